@@ -1,0 +1,521 @@
+"""numpy restatement of meep_torch's FDTD hot path (TEST INFRASTRUCTURE ONLY).
+
+This is the oracle the CUDA path is checked against. It is never imported by
+the product package. Arrays are numpy; ``dtype`` (float32 or float64) is the
+grid dtype, and every arithmetic step runs in that dtype in the same order as
+the reference so that float32 runs round like the reference's float32 runs.
+
+Scope (what the north-star configs use): PEC or PMC-in-y walls, CPML, scalar
+eps, no dispersion / conductivity / nonlinearity / symmetry folds.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+# ---------------------------------------------------------------- CPML / grid
+
+def side_counts(n_or_pair):
+    """(lo, hi) cell counts from an int or a pair (core/pml.py:8-14)."""
+    if isinstance(n_or_pair, (tuple, list)):
+        lo, hi = n_or_pair
+        return int(lo), int(hi)
+    return int(n_or_pair), int(n_or_pair)
+
+
+def cpml_profiles(n, npml, offset, dt, dx, m=3, R0=1e-6, alpha_max=0.05,
+                  dtype=np.float64):
+    """CFS-PML 1D profiles (b, a, kappa) at positions i + offset.
+
+    Follows core/pml.py:17-59: polynomial grading u^m of sigma with
+    sigma_max = -(m+1) ln R0 / (2 n dx); alpha = alpha_max (1-u) inside the
+    layer; kappa = 1; b = exp(-(sigma/kappa + alpha) dt);
+    a = sigma (b-1) / (kappa (sigma + kappa alpha)) where sigma > 0.
+    The high wall is anchored at n-1+2*offset (core/pml.py:43-49).
+    """
+    dtype = np.dtype(dtype)
+    n_lo, n_hi = side_counts(npml)
+    x = np.arange(n, dtype=dtype) + dtype.type(offset)
+    u = np.zeros(n, dtype=dtype)
+    sigma = np.zeros(n, dtype=dtype)
+    if n_lo > 0:
+        u_lo = np.maximum((dtype.type(n_lo) - x) / dtype.type(n_lo), dtype.type(0))
+        u = u + u_lo
+        smax = -(m + 1) * math.log(R0) / (2.0 * n_lo * dx)
+        sigma = sigma + dtype.type(smax) * u_lo ** m
+    if n_hi > 0:
+        wall = n - 1 + 2.0 * offset
+        u_hi = np.maximum((x - dtype.type(wall - n_hi)) / dtype.type(n_hi), dtype.type(0))
+        u = u + u_hi
+        smax = -(m + 1) * math.log(R0) / (2.0 * n_hi * dx)
+        sigma = sigma + dtype.type(smax) * u_hi ** m
+    u = np.minimum(u, dtype.type(1.0))
+    alpha = np.where(u > 0, dtype.type(alpha_max) * (dtype.type(1.0) - u),
+                     np.zeros_like(u)).astype(dtype)
+    kappa = np.ones_like(u)
+    b = np.exp(-(sigma / kappa + alpha) * dtype.type(dt)).astype(dtype)
+    denom = kappa * (sigma + kappa * alpha)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        a = np.where(sigma > 0, sigma * (b - dtype.type(1.0)) /
+                     np.maximum(denom, dtype.type(1e-300) if dtype == np.float64
+                                else np.finfo(dtype).tiny),
+                     np.zeros_like(b)).astype(dtype)
+    return b, a, kappa
+
+
+def _axis_sides(npml):
+    """((x_lo, x_hi), (y_lo, y_hi)) from an int or pair-of-pairs (core/coeffs.py:12-18)."""
+    if isinstance(npml, (tuple, list)):
+        px, py = npml
+        return side_counts(px), side_counts(py)
+    return (int(npml), int(npml)), (int(npml), int(npml))
+
+
+# ---------------------------------------------------------------- 2D TM
+
+def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
+              dtype=np.float64):
+    """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
+
+    Profiles are sliced to the live derivative nodes exactly as
+    core/coeffs.py:251-278: H side at half nodes (n-1 long); E side on the
+    interior [1:-1] (or the full axis under y_pmc)."""
+    dtype = np.dtype(dtype)
+    dt = courant * dx
+    e = (np.ones((nx, ny), dtype=dtype) if eps is None
+         else np.asarray(eps, dtype=dtype).copy())
+    px, py = _axis_sides(npml)
+    if sum(px) >= nx or (sum(py) >= ny and not y_pmc):
+        raise ValueError("npml too large for grid")
+    yprof = py if not y_pmc else 0
+    b_hy, a_hy, k_hy = cpml_profiles(ny - 1, yprof, 0.5, dt, dx, dtype=dtype)
+    b_hx, a_hx, k_hx = cpml_profiles(nx - 1, px, 0.5, dt, dx, dtype=dtype)
+    b_ex, a_ex, k_ex = (v[1:-1] for v in cpml_profiles(nx, px, 0.0, dt, dx, dtype=dtype))
+    b_eyf, a_eyf, k_eyf = cpml_profiles(ny, yprof, 0.0, dt, dx, dtype=dtype)
+    if y_pmc:
+        b_ey, a_ey, k_ey = b_eyf, a_eyf, k_eyf
+    else:
+        b_ey, a_ey, k_ey = b_eyf[1:-1], a_eyf[1:-1], k_eyf[1:-1]
+    return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc,
+                b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
+                b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
+                b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
+                b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :])
+
+
+def tm_state(c):
+    """Zero TM state with the reference's shapes (core/stepper_tm.py:37-71)."""
+    nx, ny, dt = c["nx"], c["ny"], c["dtype"]
+    ny_e = ny if c["y_pmc"] else ny - 2
+    z = lambda *s: np.zeros(s, dtype=dt)
+    return dict(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
+                psi_Ezy=z(nx, ny - 1), psi_Ezx=z(nx - 1, ny),
+                psi_Hyx=z(nx - 2, ny_e), psi_Hxy=z(nx - 2, ny_e))
+
+
+def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
+    """One TM step in the phase order of core/stepper_tm.py:234-254.
+
+    step_db(B) (:85-128) -> step_source(B) (:186-196) -> step_db(D)
+    (:130-166) -> step_source(D) (:197-200) -> update_eh(E) (:224-231).
+    Returns a new state dict."""
+    dt, dx, T = c["dt"], c["dx"], c["dtype"].type
+    Ez = s["Ez"]
+    dEz_dy = (Ez[:, 1:] - Ez[:, :-1]) / T(dx)
+    psi_Ezy = c["b_hy"] * s["psi_Ezy"] + c["a_hy"] * dEz_dy
+    curl_hx = dEz_dy / c["k_hy"] + psi_Ezy
+    dEz_dx = (Ez[1:, :] - Ez[:-1, :]) / T(dx)
+    psi_Ezx = c["b_hx"] * s["psi_Ezx"] + c["a_hx"] * dEz_dx
+    curl_hy = dEz_dx / c["k_hx"] + psi_Ezx
+    Hx = s["Hx"] - T(dt) * curl_hx
+    Hy = s["Hy"] + T(dt) * curl_hy
+    # magnetic sheet current (mode sources), subtracted (core/stepper_tm.py:186-196)
+    if hy_mask is not None:
+        Hy = Hy - T(dt * amp_h) * hy_mask
+    if hx_mask is not None:
+        Hx = Hx - T(dt * amp_h) * hx_mask
+    # D update with PEC (zero-pad) or PMC-in-y ghosts (core/stepper_tm.py:136-166)
+    if c["y_pmc"]:
+        Hxp = np.pad(Hx, ((0, 0), (1, 1)))
+        dHx_dy = (Hxp[1:-1, 1:] - Hxp[1:-1, :-1]) / T(dx)
+        dHy_dx = (Hy[1:, :] - Hy[:-1, :]) / T(dx)
+        pad = ((1, 1), (0, 0))
+    else:
+        dHx_dy = (Hx[1:-1, 1:] - Hx[1:-1, :-1]) / T(dx)
+        dHy_dx = (Hy[1:, 1:-1] - Hy[:-1, 1:-1]) / T(dx)
+        pad = ((1, 1), (1, 1))
+    psi_Hyx = c["b_ex"] * s["psi_Hyx"] + c["a_ex"] * dHy_dx
+    psi_Hxy = c["b_ey"] * s["psi_Hxy"] + c["a_ey"] * dHx_dy
+    curl = dHy_dx / c["k_ex"] + psi_Hyx - dHx_dy / c["k_ey"] - psi_Hxy
+    Dz = s["Dz"] + T(dt) * np.pad(curl, pad)
+    if mask is not None:
+        Dz = Dz - T(dt * amp) * mask
+    Ez_new = Dz / c["eps"]
+    return dict(Ez=Ez_new, Hx=Hx, Hy=Hy, Dz=Dz, psi_Ezy=psi_Ezy, psi_Ezx=psi_Ezx,
+                psi_Hyx=psi_Hyx, psi_Hxy=psi_Hxy)
+
+
+# ---------------------------------------------------------------- 2D TE
+
+def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64):
+    """TE coefficient set (core/coeffs.py:357-503, PEC path only).
+
+    eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
+    (core/coeffs.py:347-354)."""
+    dtype = np.dtype(dtype)
+    dt = courant * dx
+    e = (np.ones((nx, ny), dtype=dtype) if eps is None
+         else np.asarray(eps, dtype=dtype).copy())
+    h = dtype.type(0.5)
+    eps_x = h * (e[:-1, :] + e[1:, :])
+    eps_y = h * (e[:, :-1] + e[:, 1:])
+    px, py = _axis_sides(npml)
+    if sum(px) >= nx or sum(py) >= ny:
+        raise ValueError("npml too large for grid")
+    b_hx, a_hx, k_hx = cpml_profiles(nx - 1, px, 0.5, dt, dx, dtype=dtype)
+    b_hy, a_hy, k_hy = cpml_profiles(ny - 1, py, 0.5, dt, dx, dtype=dtype)
+    b_ey, a_ey, k_ey = (v[1:-1] for v in cpml_profiles(ny, py, 0.0, dt, dx, dtype=dtype))
+    b_ex, a_ex, k_ex = (v[1:-1] for v in cpml_profiles(nx, px, 0.0, dt, dx, dtype=dtype))
+    return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e,
+                eps_x=eps_x, eps_y=eps_y,
+                b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
+                b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
+                b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
+                b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None])
+
+
+def te_state(c):
+    """Zero TE state with the reference's shapes (core/stepper_te.py:27-49)."""
+    nx, ny, dt = c["nx"], c["ny"], c["dtype"]
+    z = lambda *s: np.zeros(s, dtype=dt)
+    return dict(Hz=z(nx - 1, ny - 1), Ex=z(nx - 1, ny), Ey=z(nx, ny - 1),
+                Dx=z(nx - 1, ny), Dy=z(nx, ny - 1),
+                psi_Eyx=z(nx - 1, ny - 1), psi_Exy=z(nx - 1, ny - 1),
+                psi_Hzy=z(nx - 1, ny - 2), psi_Hzx=z(nx - 2, ny - 1))
+
+
+def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
+    """One TE step, entered at the D half (core/stepper_te.py:178-190):
+    step_db(D) (:79-111) -> step_source(D) into Dy (:120-134) -> update_eh(E)
+    (:150-175) -> step_db(B) Hz (:113-117) -> step_source(B) into Hz."""
+    dt, dx, T = c["dt"], c["dx"], c["dtype"].type
+    Hz = s["Hz"]
+    dHz_dy = (Hz[:, 1:] - Hz[:, :-1]) / T(dx)
+    psi_Hzy = c["b_ey"] * s["psi_Hzy"] + c["a_ey"] * dHz_dy
+    curl_x = np.pad(dHz_dy / c["k_ey"] + psi_Hzy, ((0, 0), (1, 1)))
+    dHz_dx = (Hz[1:, :] - Hz[:-1, :]) / T(dx)
+    psi_Hzx = c["b_ex"] * s["psi_Hzx"] + c["a_ex"] * dHz_dx
+    curl_y = np.pad(dHz_dx / c["k_ex"] + psi_Hzx, ((1, 1), (0, 0)))
+    Dx = s["Dx"] + T(dt) * curl_x
+    Dy = s["Dy"] - T(dt) * curl_y
+    if mask_ey is not None:
+        Dy = Dy - T(dt * amp) * mask_ey
+    Ex = Dx / c["eps_x"]
+    Ey = Dy / c["eps_y"]
+    dEy_dx = (Ey[1:, :] - Ey[:-1, :]) / T(dx)
+    dEx_dy = (Ex[:, 1:] - Ex[:, :-1]) / T(dx)
+    psi_Eyx = c["b_hx"] * s["psi_Eyx"] + c["a_hx"] * dEy_dx
+    psi_Exy = c["b_hy"] * s["psi_Exy"] + c["a_hy"] * dEx_dy
+    curl_z = dEy_dx / c["k_hx"] + psi_Eyx - dEx_dy / c["k_hy"] - psi_Exy
+    Hz_new = Hz - T(dt) * curl_z
+    if hz_mask is not None:
+        Hz_new = Hz_new - T(dt * amp_h) * hz_mask
+    return dict(Hz=Hz_new, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy, psi_Eyx=psi_Eyx,
+                psi_Exy=psi_Exy, psi_Hzy=psi_Hzy, psi_Hzx=psi_Hzx)
+
+
+# ---------------------------------------------------------------- sources
+
+def gaussian_pulse(fcen, fwidth, cutoff=5.0):
+    """Time profile cos(2 pi f (t-t0)) exp(-(t-t0)^2/(2 w^2)), w = 1/fwidth,
+    t0 = cutoff*w (core/sources.py:26-36). Returns a float -> float callable."""
+    w = 1.0 / fwidth
+    t0 = cutoff * w
+
+    def amplitude(t):
+        return math.cos(2 * math.pi * fcen * (t - t0)) * math.exp(-((t - t0) ** 2) / (2 * w ** 2))
+    return amplitude
+
+
+def line_source_mask(nx, ny, dx, ix, j0, j1, dtype=np.float64):
+    """LineSource mask (core/sources.py:49-91): 1 on x=ix, y in [j0, j1),
+    scaled by dx/dx^2 for an extended line and 1/dx^2 for a single cell."""
+    dtype = np.dtype(dtype)
+    mask = np.zeros((nx, ny), dtype=dtype)
+    mask[ix, j0:j1] = 1.0
+    per_cell = dx if (j1 - j0) > 1 else 1.0
+    return (mask * dtype.type(per_cell / dx ** 2)).astype(dtype)
+
+
+def src_time(t_idx, dt):
+    """Soft sources sample their profile at (t_idx + 1/2) dt (core/sources.py:90-91)."""
+    return (t_idx + 0.5) * dt
+
+
+# ---------------------------------------------------------------- 2D monitors
+
+def dft_sample(F, t_idx, dt, freqs, component, dtype):
+    """DFTFieldsMonitor.sample (core/monitors.py:40-46): dt*[cos(wt) F, -sin(wt) F]
+    with t = (t_idx + 1) dt for E components and (t_idx + 1/2) dt for H; the
+    phase is evaluated in the grid dtype like the reference."""
+    T = np.dtype(dtype).type
+    off = 1.0 if component.startswith("E") else 0.5
+    t = (t_idx + off) * dt
+    w = (T(2 * math.pi) * np.asarray(freqs, dtype=dtype))[:, None, None]
+    wt = w * T(t)
+    return T(dt) * np.stack([np.cos(wt) * F, -np.sin(wt) * F], axis=1)
+
+
+def _line_dft(E, H, tE, tH, dt, freqs, dtype):
+    T = np.dtype(dtype).type
+    w = (T(2 * math.pi) * np.asarray(freqs, dtype=dtype))[:, None]
+    wE, wH = w * T(tE), w * T(tH)
+    return T(dt) * np.stack([np.cos(wE) * E, -np.sin(wE) * E,
+                             np.cos(wH) * H, -np.sin(wH) * H], axis=1)
+
+
+def flux_tm_sample(s, t_idx, dt, freqs, x_normal, idx, lo, hi, dtype):
+    """FluxMonitorTM.sample (core/monitors.py:71-95): Ez on the line and the
+    2-point average of Hy (x-normal) or Hx (y-normal); E at (t+1)dt, H at (t+1/2)dt."""
+    T = np.dtype(dtype).type
+    if x_normal:
+        E = s["Ez"][idx, lo:hi]
+        H = T(0.5) * (s["Hy"][idx - 1, lo:hi] + s["Hy"][idx, lo:hi])
+    else:
+        E = s["Ez"][lo:hi, idx]
+        H = T(0.5) * (s["Hx"][lo:hi, idx - 1] + s["Hx"][lo:hi, idx])
+    return _line_dft(E, H, (t_idx + 1.0) * dt, (t_idx + 0.5) * dt, dt, freqs, dtype)
+
+
+def flux_te_sample(s, t_idx, dt, freqs, ix, lo, hi, dtype):
+    """FluxMonitorTE.sample (core/monitors.py:112-122): Ey and the averaged Hz,
+    E at (t+1/2)dt, H at (t+1)dt."""
+    T = np.dtype(dtype).type
+    E = s["Ey"][ix, lo:hi]
+    H = T(0.5) * (s["Hz"][ix - 1, lo:hi] + s["Hz"][ix, lo:hi])
+    return _line_dft(E, H, (t_idx + 0.5) * dt, (t_idx + 1.0) * dt, dt, freqs, dtype)
+
+
+def flux_tey_sample(s, t_idx, dt, freqs, iy, lo, hi, dtype):
+    """FluxMonitorTEY.sample (core/monitors.py:141-151): Ex and Hz averaged in y."""
+    T = np.dtype(dtype).type
+    E = s["Ex"][lo:hi, iy]
+    H = T(0.5) * (s["Hz"][lo:hi, iy - 1] + s["Hz"][lo:hi, iy])
+    return _line_dft(E, H, (t_idx + 0.5) * dt, (t_idx + 1.0) * dt, dt, freqs, dtype)
+
+
+def line_flux(acc, dx, sign):
+    """Flux from 4 line accumulators: sign*1/2*sum(ReE ReH + ImE ImH)*dx
+    (core/monitors.py:97-100, :124-126, :153-155)."""
+    ReE, ImE, ReH, ImH = (acc[:, k] for k in range(4))
+    return sign * 0.5 * (ReE * ReH + ImE * ImH).sum(-1) * dx
+
+
+def run_2d(step, s, c, n_steps, amp_fn=None, mask=None, monitors=(), t0=0):
+    """Per-step loop of core/run.py:10-40: step, then every monitor samples the
+    new state and sum-folds. ``monitors`` are callables (state, t_idx) -> sample."""
+    acc = [None] * len(monitors)
+    for k in range(n_steps):
+        t = t0 + k
+        if amp_fn is not None:
+            s = step(s, c, amp_fn(t), mask)
+        else:
+            s = step(s, c)
+        for i, mon in enumerate(monitors):
+            smp = mon(s, t)
+            acc[i] = smp if acc[i] is None else acc[i] + smp
+    return s, acc
+
+
+# ---------------------------------------------------------------- 3D
+
+def _avg(v, axis):
+    a = [slice(None)] * 3
+    b = [slice(None)] * 3
+    a[axis] = slice(None, -1)
+    b[axis] = slice(1, None)
+    return v.dtype.type(0.5) * (v[tuple(a)] + v[tuple(b)])
+
+
+def _d(v, axis):
+    a = [slice(None)] * 3
+    b = [slice(None)] * 3
+    a[axis] = slice(None, -1)
+    b[axis] = slice(1, None)
+    return v[tuple(b)] - v[tuple(a)]
+
+
+def _bc(v, ax):
+    sh = [1, 1, 1]
+    sh[ax] = v.shape[0]
+    return v.reshape(sh)
+
+
+def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64):
+    """3D CPML coefficient set (core/stepper_3d.py:150-266, CPML path, no
+    conductivity, no poles). dt = 0.5 dx / sqrt(3). H-side profiles on the
+    n-1 half nodes, E-side on the interior [1:-1]."""
+    dtype = np.dtype(dtype)
+    dt = 0.5 * dx / math.sqrt(3.0)
+    e = (np.ones((nx, ny, nz), dtype=dtype) if eps is None
+         else np.asarray(eps, dtype=dtype).copy())
+    dims = (nx, ny, nz)
+    cp = {}
+    for ax, kh, ke in ((0, "hx", "ex"), (1, "hy", "ey"), (2, "hz", "ez")):
+        n = dims[ax]
+        b, a, k = cpml_profiles(n - 1, npml, 0.5, dt, dx, dtype=dtype)
+        cp[kh] = (_bc(b, ax), _bc(a, ax), _bc(k, ax))
+        b, a, k = cpml_profiles(n, npml, 0.0, dt, dx, dtype=dtype)
+        cp[ke] = (_bc(b[1:-1], ax), _bc(a[1:-1], ax), _bc(k[1:-1], ax))
+    # sigma = 0: damping pair (1, dt) (core/stepper_3d.py:241-251)
+    one = dtype.type((1 - 0.0) / (1 + 0.0))
+    d2 = dtype.type(dt / (1 + 0.0))
+    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, d1=one, d2=d2)
+
+
+def state_3d(c):
+    """Zero 3D state with CPML memory (core/stepper_3d.py:269-292)."""
+    nx, ny, nz = c["dims"]
+    z = lambda *s: np.zeros(s, dtype=c["dtype"])
+    return dict(
+        Ex=z(nx - 1, ny, nz), Ey=z(nx, ny - 1, nz), Ez=z(nx, ny, nz - 1),
+        Hx=z(nx, ny - 1, nz - 1), Hy=z(nx - 1, ny, nz - 1), Hz=z(nx - 1, ny - 1, nz),
+        psi_Ez_y=z(nx, ny - 1, nz - 1), psi_Ey_z=z(nx, ny - 1, nz - 1),
+        psi_Ex_z=z(nx - 1, ny, nz - 1), psi_Ez_x=z(nx - 1, ny, nz - 1),
+        psi_Ey_x=z(nx - 1, ny - 1, nz), psi_Ex_y=z(nx - 1, ny - 1, nz),
+        psi_Hz_y=z(nx - 1, ny - 2, nz), psi_Hy_z=z(nx - 1, ny, nz - 2),
+        psi_Hx_z=z(nx, ny - 1, nz - 2), psi_Hz_x=z(nx - 2, ny - 1, nz),
+        psi_Hy_x=z(nx - 2, ny, nz - 1), psi_Hx_y=z(nx, ny - 2, nz - 1))
+
+
+def _pad_interior(t, axes):
+    pad = [(0, 0)] * 3
+    for a in axes:
+        pad[a] = (1, 1)
+    return np.pad(t, pad)
+
+
+def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
+    """One 3D leapfrog step, CPML path of core/stepper_3d.py:363-445, then the
+    soft source of :448-482. ``src`` is ("Ez", i, j, k) for a point current
+    (the functional stepper ADDS dt*amp/eps there, :474-480; ``point_sign=-1``
+    gives the lean stepper's subtraction, core/stepper_3d_lean.py:293-296) or
+    ("Ez", mask) for an area current (subtracted, :452-461)."""
+    dx, T = c["dx"], c["dtype"].type
+    cp = c["cpml"]
+    d1, d2 = c["d1"], c["d2"]
+    X = T(dx)
+
+    def ce(F, ax, key, psi):
+        b, a, k = cp[key]
+        d = _d(F, ax) / X
+        p = b * psi + a * d
+        return d / k + p, p
+
+    out = {}
+    ce_y, out["psi_Ez_y"] = ce(s["Ez"], 1, "hy", s["psi_Ez_y"])
+    ce_z, out["psi_Ey_z"] = ce(s["Ey"], 2, "hz", s["psi_Ey_z"])
+    Hx = d1 * s["Hx"] - d2 * (ce_y - ce_z)
+    ce_z2, out["psi_Ex_z"] = ce(s["Ex"], 2, "hz", s["psi_Ex_z"])
+    ce_x, out["psi_Ez_x"] = ce(s["Ez"], 0, "hx", s["psi_Ez_x"])
+    Hy = d1 * s["Hy"] - d2 * (ce_z2 - ce_x)
+    ce_x2, out["psi_Ey_x"] = ce(s["Ey"], 0, "hx", s["psi_Ey_x"])
+    ce_y2, out["psi_Ex_y"] = ce(s["Ex"], 1, "hy", s["psi_Ex_y"])
+    Hz = d1 * s["Hz"] - d2 * (ce_x2 - ce_y2)
+
+    eps = c["eps"]
+    eps_x = _avg(eps, 0)
+    ch_y, out["psi_Hz_y"] = ce(Hz, 1, "ey", s["psi_Hz_y"])
+    ch_z, out["psi_Hy_z"] = ce(Hy, 2, "ez", s["psi_Hy_z"])
+    curl_x = _pad_interior(ch_y[:, :, 1:-1] - ch_z[:, 1:-1, :], (1, 2))
+    Ex = (d1 * s["Ex"] * eps_x + d2 * curl_x) / eps_x
+    eps_y = _avg(eps, 1)
+    ch_z2, out["psi_Hx_z"] = ce(Hx, 2, "ez", s["psi_Hx_z"])
+    ch_x, out["psi_Hz_x"] = ce(Hz, 0, "ex", s["psi_Hz_x"])
+    curl_y = _pad_interior(ch_z2[1:-1, :, :] - ch_x[:, :, 1:-1], (0, 2))
+    Ey = (d1 * s["Ey"] * eps_y + d2 * curl_y) / eps_y
+    eps_z = _avg(eps, 2)
+    ch_x2, out["psi_Hy_x"] = ce(Hy, 0, "ex", s["psi_Hy_x"])
+    ch_y2, out["psi_Hx_y"] = ce(Hx, 1, "ey", s["psi_Hx_y"])
+    curl_z = _pad_interior(ch_x2[:, 1:-1, :] - ch_y2[1:-1, :, :], (0, 1))
+    Ez = (d1 * s["Ez"] * eps_z + d2 * curl_z) / eps_z
+    out.update(Ex=Ex, Ey=Ey, Ez=Ez, Hx=Hx, Hy=Hy, Hz=Hz)
+    if src is not None and amp != 0.0:
+        comp = src[0]
+        epsc = {"Ex": eps_x, "Ey": eps_y, "Ez": eps_z}[comp]
+        F = out[comp]
+        if isinstance(src[1], np.ndarray):
+            out[comp] = F - T(c["dt"] * amp) * src[1] / epsc
+        else:
+            i, j, k = src[1], src[2], src[3]
+            F = F.copy()
+            if point_sign > 0:
+                F[i, j, k] = F[i, j, k] + T(c["dt"] * amp) / epsc[i, j, k]
+            else:
+                F[i, j, k] = F[i, j, k] - T(c["dt"] * amp) * (T(1.0) / epsc[i, j, k])
+            out[comp] = F
+    return out
+
+
+def flux3d_planes(s, normal, idx, win=None, ap=0):
+    """FluxMonitor3D._plane (core/monitors_3d.py:124-162): the two tangential
+    E/H pairs on the plane (H averaged across it), cropped to the common
+    min shape and then to ``win`` = (l0, h0, l1, h1) or the ``ap`` margin."""
+    h = s["Ex"].dtype.type(0.5)
+    if normal == "z":
+        k = idx
+        Ea = s["Ex"][:, :, k]; Ha = h * (s["Hy"][:, :, k - 1] + s["Hy"][:, :, k])
+        Eb = s["Ey"][:, :, k]; Hb = h * (s["Hx"][:, :, k - 1] + s["Hx"][:, :, k])
+    elif normal == "x":
+        i = idx
+        Ea = s["Ey"][i]; Ha = h * (s["Hz"][i - 1] + s["Hz"][i])
+        Eb = s["Ez"][i]; Hb = h * (s["Hy"][i - 1] + s["Hy"][i])
+    else:
+        j = idx
+        Ea = s["Ez"][:, j, :]; Ha = h * (s["Hx"][:, j - 1, :] + s["Hx"][:, j, :])
+        Eb = s["Ex"][:, j, :]; Hb = h * (s["Hz"][:, j - 1, :] + s["Hz"][:, j, :])
+    ts = [Ea, Ha, Eb, Hb]
+    m0 = min(t.shape[0] for t in ts)
+    m1 = min(t.shape[1] for t in ts)
+    if win is not None:
+        l0, h0, l1, h1 = win
+    else:
+        l0, h0, l1, h1 = ap, m0 - ap, ap, m1 - ap
+    l0 = max(0, l0); l1 = max(0, l1)
+    h0 = min(m0, h0); h1 = min(m1, h1)
+    return [t[l0:h0, l1:h1] for t in ts]
+
+
+def flux3d_sample(s, t_idx, dt, freqs, normal, idx, win=None, ap=0):
+    """FluxMonitor3D.sample (core/monitors_3d.py:164-182): 8 accumulators,
+    E at (t+1)dt and H at (t+1/2)dt, phase in the field dtype."""
+    Ea, Ha, Eb, Hb = flux3d_planes(s, normal, idx, win, ap)
+    dtype = Ea.dtype
+    T = dtype.type
+    f = np.asarray(freqs, dtype=dtype)
+    w = (T(2 * math.pi) * f)[:, None, None]
+    wE, wH = w * T((t_idx + 1.0) * dt), w * T((t_idx + 0.5) * dt)
+    cE, sE, cH, sH = np.cos(wE), -np.sin(wE), np.cos(wH), -np.sin(wH)
+    return T(dt) * np.stack([cE * Ea, sE * Ea, cH * Ha, sH * Ha,
+                             cE * Eb, sE * Eb, cH * Hb, sH * Hb], axis=1)
+
+
+def flux3d(acc, dx):
+    """FluxMonitor3D.flux (core/monitors_3d.py:184-189): 1/2 sum(sa - sb) dx^2."""
+    sa = acc[:, 0] * acc[:, 2] + acc[:, 1] * acc[:, 3]
+    sb = acc[:, 4] * acc[:, 6] + acc[:, 5] * acc[:, 7]
+    return 0.5 * (sa - sb).sum(axis=(1, 2)) * dx * dx
+
+
+def run_3d(s, c, n_steps, amp_fn=None, src=None, monitors=(), point_sign=+1.0):
+    """Loop of core/monitors_3d.py:192-210: step_3d, then sample and sum-fold."""
+    acc = [None] * len(monitors)
+    for t in range(n_steps):
+        amp = amp_fn(t) if amp_fn is not None else 0.0
+        s = step_3d(s, c, amp, src, point_sign=point_sign)
+        for i, mon in enumerate(monitors):
+            smp = mon(s, t)
+            acc[i] = smp if acc[i] is None else acc[i] + smp
+    return s, acc

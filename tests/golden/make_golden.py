@@ -1,0 +1,203 @@
+"""Generate the golden fixtures in this folder by running the REFERENCE itself.
+
+Imports meep_torch from the reference checkout (``MEEP_TORCH_REF``, default
+``/root/reference``; read-only, no bytecode written) and runs small seeded
+cases of the hot path through its own public functions:
+
+* ``Grid`` / ``build_tm_coeffs`` / ``LineSource`` / ``FluxMonitorTM`` /
+  ``DFTFieldsMonitor`` / ``run_tm``            (core/run.py:125)
+* ``build_te_coeffs`` / ``FluxMonitorTE`` / ``FluxMonitorTEY`` / ``run_te``
+* ``build_3d_coeffs`` / ``PointSource3D`` / ``FluxMonitor3D`` / ``run_3d``
+  (core/monitors_3d.py:192) and ``build_lean`` / ``run_3d_lean``
+* ``cpml_profiles``                              (core/pml.py:17)
+
+in float64 and float32. Inputs (eps maps, parameters) and outputs (final
+state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
+fixtures are what pins the oracle (tests/test_oracle_golden.py) and the CUDA
+path (tests/test_gpu_parity.py); this script is only re-run by hand.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+sys.dont_write_bytecode = True
+REF = os.environ.get("MEEP_TORCH_REF", "/root/reference")
+sys.path.insert(0, REF)
+
+import torch  # noqa: E402
+
+from meep_torch.core.coeffs import build_te_coeffs, build_tm_coeffs  # noqa: E402
+from meep_torch.core.grid import Grid  # noqa: E402
+from meep_torch.core.monitors import (DFTFieldsMonitor, FluxMonitorTE,  # noqa: E402
+                                      FluxMonitorTEY, FluxMonitorTM)
+from meep_torch.core.monitors_3d import FluxMonitor3D, PointSource3D, run_3d  # noqa: E402
+from meep_torch.core.pml import cpml_profiles  # noqa: E402
+from meep_torch.core.run import run_te, run_tm  # noqa: E402
+from meep_torch.core.sources import GaussianPulse, LineSource  # noqa: E402
+from meep_torch.core.stepper_3d import build_3d_coeffs, init_3d_state  # noqa: E402
+from meep_torch.core.stepper_3d_lean import build_lean, run_3d_lean  # noqa: E402
+from meep_torch.core.stepper_te import init_te_state  # noqa: E402
+from meep_torch.core.stepper_tm import init_tm_state  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DT = {"f64": torch.float64, "f32": torch.float32}
+
+
+def _np(t):
+    return t.detach().cpu().to(torch.float64).numpy()
+
+
+def tm_case(prec, y_pmc=False, point=False):
+    rng = np.random.default_rng(11)
+    nx, ny, dx, npml = 48, 36, 0.05, 8
+    eps = np.ones((nx, ny))
+    eps[:, 15:21] = 12.0                          # guide along x
+    eps[20:30, 8:14] = rng.uniform(2.0, 6.0)      # a block
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
+    m = build_tm_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml,
+                        y_pmc=y_pmc)
+    prof = GaussianPulse(0.65, 0.4)
+    if point:
+        src = LineSource(g, ix=12, j0=18, j1=19, profile=prof)
+    else:
+        src = LineSource(g, ix=12, j0=10, j1=26, profile=prof)
+    freqs = [0.55, 0.65, 0.75]
+    monx = FluxMonitorTM(g, freqs, x_normal=True, idx=36, lo=9, hi=27)
+    mony = FluxMonitorTM(g, freqs, x_normal=False, idx=26, lo=10, hi=38)
+    dft = DFTFieldsMonitor(g, freqs, component="Ez")
+    s0 = init_tm_state(g, y_pmc=y_pmc)
+    n = 300
+    with torch.no_grad():
+        st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft])
+    out = dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, eps=eps, freqs=np.array(freqs),
+               fcen=0.65, fwidth=0.4, src_ix=12, src_j0=18 if point else 10,
+               src_j1=19 if point else 26, y_pmc=int(y_pmc),
+               monx=np.array([36, 9, 27]), mony=np.array([26, 10, 38]),
+               acc_x=_np(ax), acc_y=_np(ay), acc_dft=_np(ad),
+               flux_x=_np(monx.flux(ax, dx)), flux_y=_np(mony.flux(ay, dx)),
+               mask=_np(src.mask))
+    for k in st._fields:
+        v = getattr(st, k)
+        if v is not None and v.numel():
+            out["s_" + k] = _np(v)
+    for k in ("b_hy", "a_hy", "b_hx", "a_hx", "b_ex", "a_ex", "b_ey", "a_ey"):
+        out["c_" + k] = _np(getattr(m, k))
+    return out
+
+
+def te_case(prec):
+    rng = np.random.default_rng(12)
+    nx, ny, dx, npml = 44, 40, 0.05, 8
+    eps = np.ones((nx, ny))
+    eps[:, 17:23] = 12.0
+    eps[18:28, 26:32] = rng.uniform(2.0, 6.0)
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
+    m = build_te_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml)
+    prof = GaussianPulse(0.65, 0.4)
+    src = LineSource(g, ix=12, j0=12, j1=28, profile=prof)
+
+    class _TESrc:                                   # Simulation's TE binding:
+        mask = src.mask[:, :-1]                     # mask[:, :-1] -> Dy (mp/simulation.py:867-869)
+        amplitude = staticmethod(src.amplitude)
+
+    freqs = [0.55, 0.65, 0.75]
+    monx = FluxMonitorTE(g, freqs, ix=32, lo=9, hi=31)
+    mony = FluxMonitorTEY(g, freqs, iy=30, lo=9, hi=35)
+    dft = DFTFieldsMonitor(g, freqs, component="Hz")
+    s0 = init_te_state(g)
+    n = 300
+    with torch.no_grad():
+        st, (ax, ay, ad) = run_te(s0, m, n, source=_TESrc(), monitors=[monx, mony, dft])
+    out = dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, eps=eps, freqs=np.array(freqs),
+               fcen=0.65, fwidth=0.4, src_ix=12, src_j0=12, src_j1=28,
+               monx=np.array([32, 9, 31]), mony=np.array([30, 9, 35]),
+               acc_x=_np(ax), acc_y=_np(ay), acc_dft=_np(ad),
+               flux_x=_np(monx.flux(ax, dx)), flux_y=_np(mony.flux(ay, dx)),
+               mask=_np(_TESrc.mask))
+    for k in st._fields:
+        v = getattr(st, k)
+        if v is not None and v.numel():
+            out["s_" + k] = _np(v)
+    return out
+
+
+FACES = [("x", 5), ("x", 18), ("y", 5), ("y", 16), ("z", 5), ("z", 14)]
+
+
+def case_3d(prec, lean=False):
+    rng = np.random.default_rng(13)
+    nx, ny, nz, dx, npml = 24, 22, 20, 1.0 / 16, 4
+    eps = np.ones((nx, ny, nz))
+    for _ in range(6):                                # a few spheres, draw order
+        c = rng.uniform(4, [nx - 4, ny - 4, nz - 4])
+        r = rng.uniform(1.5, 3.5)
+        e = rng.uniform(2, 12)
+        X, Y, Z = np.meshgrid(np.arange(nx) + 0.5, np.arange(ny) + 0.5,
+                              np.arange(nz) + 0.5, indexing="ij")
+        eps[(X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r] = e
+    epst = torch.tensor(eps, dtype=DT[prec])
+    freqs = [0.4, 0.5, 0.6, 0.7]
+    win = (4, 17, 4, 15)
+    prof = GaussianPulse(0.5, 0.3)
+    n = 120
+    src_ijk = (12, 11, 10)
+    if lean:
+        c = build_lean(nx, ny, nz, dx, epst, npml, dtype=DT[prec], device="cpu")
+        src = PointSource3D(c.dt, "Ez", *src_ijk, prof)
+        mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=i, win=win, dtype=DT[prec])
+                for a, i in FACES]
+        view, accs = run_3d_lean(c, n, source=src, monitors=mons)
+        st = {k: getattr(view, k) for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
+    else:
+        c = build_3d_coeffs(nx, ny, nz, dx, eps=epst, npml=npml, dtype=DT[prec])
+        src = PointSource3D(c.dt, "Ez", *src_ijk, prof)
+        mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=i, win=win, dtype=DT[prec])
+                for a, i in FACES]
+        s0 = init_3d_state(nx, ny, nz, npml=npml, dtype=DT[prec])
+        with torch.no_grad():
+            stt, accs = run_3d(s0, c, n, source=src, monitors=mons)
+        st = {k: getattr(stt, k) for k in stt._fields if getattr(stt, k) is not None}
+    out = dict(nx=nx, ny=ny, nz=nz, dx=dx, npml=npml, n_steps=n, eps=eps,
+               freqs=np.array(freqs), fcen=0.5, fwidth=0.3, src=np.array(src_ijk),
+               faces=json.dumps(FACES), win=np.array(win))
+    for k, v in st.items():
+        out["s_" + k] = _np(v)
+    for i, (a, mon) in enumerate(zip(accs, mons)):
+        out[f"acc_{i}"] = _np(a)
+        out[f"flux_{i}"] = _np(mon.flux(a, dx))
+    return out
+
+
+def pml_case():
+    out = {}
+    cases = [(40, 8, 0.5, 0.025, 0.05), (40, 8, 0.0, 0.025, 0.05),
+             (33, (5, 9), 0.5, 0.02, 0.04), (64, 16, 0.0, 0.018042, 1 / 16),
+             (30, (0, 6), 0.0, 0.025, 0.05)]
+    for i, (n, npml, off, dt, dx) in enumerate(cases):
+        for prec in ("f64", "f32"):
+            b, a, k = cpml_profiles(n, npml, off, dt, dx, dtype=DT[prec])
+            out[f"{i}_{prec}_b"], out[f"{i}_{prec}_a"], out[f"{i}_{prec}_k"] = _np(b), _np(a), _np(k)
+    out["cases"] = json.dumps(cases)
+    return out
+
+
+def main():
+    torch.set_num_threads(4)
+    np.savez_compressed(os.path.join(HERE, "golden_pml.npz"), **pml_case())
+    for prec in ("f64", "f32"):
+        np.savez_compressed(os.path.join(HERE, f"golden_tm_{prec}.npz"), **tm_case(prec))
+        np.savez_compressed(os.path.join(HERE, f"golden_tm_point_pmc_{prec}.npz"),
+                            **tm_case(prec, y_pmc=True, point=True))
+        np.savez_compressed(os.path.join(HERE, f"golden_te_{prec}.npz"), **te_case(prec))
+        np.savez_compressed(os.path.join(HERE, f"golden_3d_{prec}.npz"), **case_3d(prec))
+        np.savez_compressed(os.path.join(HERE, f"golden_3d_lean_{prec}.npz"),
+                            **case_3d(prec, lean=True))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
