@@ -1,0 +1,293 @@
+/*
+ * meep_b200.h -- C ABI of the B200 (sm_100a) FDTD time-stepping hot path.
+ *
+ * Plain C: device pointers, sizes and POD descriptors; no torch types. Every
+ * entry point returns an mtb status code; mtb_last_error() gives the text of
+ * the last failure on the calling thread. Nothing here throws.
+ *
+ * Each entry point replaces one seam of the reference (meep_torch):
+ *
+ *   mtb_yee2d_plan_create / mtb_yee2d_run
+ *       replace the per-step loop core/run.py:10-40 (_run_chunk) driving
+ *       core/stepper_tm.py:234 (step_tm) or core/stepper_te.py:178 (step_te)
+ *       together with core/sources.py:90 (soft-source injection) and the
+ *       sum-folded monitors of core/monitors.py:24-155; reached through
+ *       run_tm / run_te (core/run.py:125-126) and fields.step_n
+ *       (mp/cpp/core.py:802). A plan is a batch of independent structures.
+ *   mtb_yee3d_plan_create / mtb_yee3d_run
+ *       replace the loop core/monitors_3d.py:192-210 (run_3d over
+ *       core/stepper_3d.py:303 step_3d, CPML path :363-445, source :448-482)
+ *       and core/stepper_3d_lean.py:307 (run_3d_lean), with FluxMonitor3D /
+ *       DFTFieldsMonitor3D (core/monitors_3d.py:70-189) accumulation.
+ *   mtb_pack / mtb_unpack
+ *       move the reference's per-component tensors (TMState / TEState /
+ *       State3D, core/stepper_tm.py:12, core/stepper_te.py:11,
+ *       core/stepper_3d.py:38) into and out of the padded box layout the
+ *       kernels use.
+ *
+ * Ownership: the caller allocates every field, coefficient, source list and
+ * accumulator array (device memory) and keeps it alive while a plan uses it.
+ * A plan owns only its scratch (sample ring, phase/amplitude tables, work
+ * list), allocated at creation and released by the matching destroy call.
+ * Threading: a plan is not re-entrant; use one plan per stream.
+ */
+#ifndef MEEP_B200_H
+#define MEEP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the Python layer maps them to ValueError /
+ * NotImplementedError / RuntimeError like core/coeffs.py:81, :179) */
+#define MTB_OK 0
+#define MTB_INVALID_ARG 1
+#define MTB_UNSUPPORTED 2
+#define MTB_DEVICE_TIMEOUT 3
+#define MTB_CUDA_ERROR 4
+
+#define MTB_ABI_VERSION 1
+
+/* polarisations */
+#define MTB_TM 0
+#define MTB_TE 1
+
+/* 2D component ids: 0 = the integer-step field (TM Ez, TE Hz),
+ * 1 = the x component (TM Hx, TE Ex), 2 = the y component (TM Hy, TE Ey).
+ * Sampling an E component samples E = D / eps, computed in the kernel. */
+#define MTB_C2_MAIN 0
+#define MTB_C2_X 1
+#define MTB_C2_Y 2
+
+/* 3D component ids */
+#define MTB_EX 0
+#define MTB_EY 1
+#define MTB_EZ 2
+#define MTB_HX 3
+#define MTB_HY 4
+#define MTB_HZ 5
+
+/* A soft current as a list of cells sorted by row (CSR over the rows of
+ * the target component's box array). The cell (row r, col c) receives
+ *     F[r, c] -= amp_tbl[t, amp_col] * w
+ * where amp_tbl[t, col] = float32(coef[t][col]) of the run call's FP64
+ * coefficient table (dt * amplitude(t) for the reference, rounded once, as
+ * core/stepper_tm.py:197-200 computes dt * amp * mask). */
+typedef struct mtb_cells {
+    const int32_t *row_ptr; /* rows+1 entries, device; NULL = no cells     */
+    const int32_t *col;     /* n entries, device                           */
+    const float *w;         /* n entries, device                           */
+    int32_t n;              /* number of cells                             */
+    int32_t amp_col;        /* amplitude-table column this list reads      */
+} mtb_cells;
+
+/* One raw line of field values copied into the sample ring each step:
+ * kind 0 = a row segment F[index, lo:hi], kind 1 = a column segment
+ * F[lo:hi, index]. Element p of the segment goes to
+ * ring[slot * slot_elems + ring_off + p]. */
+typedef struct mtb_line_sample {
+    int32_t comp;     /* MTB_C2_*                                       */
+    int32_t kind;     /* 0 = row, 1 = column                            */
+    int32_t index;    /* row (kind 0) or column (kind 1)                */
+    int32_t lo, hi;   /* segment bounds along the other axis            */
+    int32_t pad_;
+    int64_t ring_off;
+} mtb_line_sample;
+
+/* One 2D structure (one TMState/TMCoeffs or TEState/TECoeffs pair).
+ * Box layout: every 2D array is nx rows x pitch floats, row-major, the
+ * component's reference array (e.g. Hx of shape (nx, ny-1)) occupying its
+ * top-left corner, every other cell zero. pitch >= ny, pitch % 4 == 0, and
+ * every base pointer 16-byte aligned.
+ * Evolving arrays come in ping-pong pairs [2]: a step reads buffer `cur`
+ * and writes buffer cur^1 (a fused H+E pass recomputes halo cells from the
+ * old values of its neighbours, so it cannot update in place). Both buffers
+ * of a pair start equal; mtb_yee2d_current() says which one is live. */
+typedef struct mtb_yee2d_struct {
+    int32_t pol;            /* MTB_TM / MTB_TE                              */
+    int32_t nx, ny, pitch;
+    int32_t y_pmc;          /* TM: PMC walls in y (core/coeffs.py y_pmc)    */
+    int32_t explicit_e;     /* TM: 1 = read old Ez from e_explicit this run's
+                               first step (imported Ez != Dz/eps)           */
+    float dt, dx;
+    float *f_main[2];       /* TM Dz | TE Hz                                */
+    float *f_x[2];          /* TM Hx | TE Dx                                */
+    float *f_y[2];          /* TM Hy | TE Dy                                */
+    const float *eps_a;     /* TM eps_inf | TE eps_x                        */
+    const float *eps_b;     /* TM unused  | TE eps_y                        */
+    const float *e_explicit;/* TM: Ez box array when explicit_e             */
+    /* CPML memory, box layout at the position of the field it feeds:
+     * TM: [0] psi_Ezy (Hx), [1] psi_Ezx (Hy), [2] psi_Hyx (Dz), [3] psi_Hxy (Dz)
+     * TE: [0] psi_Hzy (Dx), [1] psi_Hzx (Dy), [2] psi_Eyx (Hz), [3] psi_Exy (Hz) */
+    float *psi[4][2];
+    /* CPML (b, a) profiles, kappa == 1: half nodes along x (nx-1), half
+     * nodes along y (ny-1), integer nodes along x (nx), along y (ny). */
+    const float *hx_b, *hx_a, *hy_b, *hy_a, *ex_b, *ex_a, *ey_b, *ey_a;
+    mtb_cells src_e;        /* TM -> Dz rows | TE -> Dy rows                */
+    mtb_cells src_h1;       /* TM -> Hy rows | TE -> Hz rows                */
+    mtb_cells src_h2;       /* TM -> Hx rows | TE unused                    */
+    const mtb_line_sample *lines; /* device array of line samples          */
+    int32_t n_lines;
+    int32_t pad_;
+    int64_t ring_full[3];   /* full-grid sample of comp c to ring offset, -1 = off */
+} mtb_yee2d_struct;
+
+/* A DFT phase group: frequencies sharing one table. The plan evaluates
+ *   P(t, f, s) = dt * (cos(w (t + s/2) dt), -sin(w (t + s/2) dt)),  s in {1, 2}
+ * in FP64 (mode 0) or with the reference's float32 phase arithmetic
+ * w = float32(2 pi) * float32(f), float32(w * float32(t)) (mode 1,
+ * core/monitors.py:43-46), then rounds to float32. */
+typedef struct mtb_phase_group {
+    const double *freqs;    /* host pointer, nf entries                     */
+    int32_t nf;
+    int32_t mode;
+    double dt;
+} mtb_phase_group;
+
+/* A DFT accumulation region: rows x cols sample channels read from the
+ * ring (offset a, optionally averaged 0.5*(a+b) with offset b, as the flux
+ * monitors average H across the plane), folded into a caller accumulator:
+ *   acc[re_off + f*f_stride + r*acc_pitch + c] += sum_t Re P(t,f) * x
+ *   acc[im_off + f*f_stride + r*acc_pitch + c] += sum_t Im P(t,f) * x
+ * toff = 1 samples at (t + 1/2) dt, toff = 2 at (t + 1) dt. */
+typedef struct mtb_dft_region {
+    float *acc;             /* device accumulator base                      */
+    int64_t re_off, im_off, f_stride;
+    int64_t ring_a, ring_b; /* ring offsets; ring_b = -1: no averaging      */
+    int32_t rows, cols;
+    int32_t ring_pitch, acc_pitch;
+    int32_t group, toff;
+} mtb_dft_region;
+
+/* Tuning knobs (0 = library default). */
+typedef struct mtb_tuning {
+    int32_t rows_per_warp;  /* 2D: rows one warp marches through            */
+    int32_t ring_slots;     /* steps buffered before one DFT contraction    */
+    int32_t threads;        /* threads per block                            */
+    int32_t reserved;
+} mtb_tuning;
+
+typedef struct mtb_yee2d_plan mtb_yee2d_plan;
+
+/* Create a plan for n_structs structures. `structs`, `regions`, `groups`
+ * are host arrays copied by the call. ring_slot_elems is the number of
+ * floats one step of samples occupies (max ring offset + extent). */
+int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs, int32_t n_structs,
+                          const mtb_dft_region *regions, int32_t n_regions,
+                          const mtb_phase_group *groups, int32_t n_groups,
+                          int64_t ring_slot_elems, int32_t n_amp_cols,
+                          const mtb_tuning *tuning, mtb_yee2d_plan **out);
+
+/* Advance every structure k steps, t0 .. t0+k-1 (t is the reference's
+ * t_idx). coef_e / coef_h: host arrays [k][n_amp_cols] of per-step mask
+ * coefficients in FP64 -- for the reference that is dt * source.amplitude(t)
+ * (resp. dt * h_amplitude(t)); the plan rounds them to float32. NULL if
+ * unused. All monitor contributions of the k steps are folded into the
+ * accumulators before the call's work completes on `stream`. */
+int mtb_yee2d_run(mtb_yee2d_plan *plan, int64_t t0, int32_t k,
+                  const double *coef_e, const double *coef_h, void *stream);
+
+/* Which buffer of every ping-pong pair holds the current state (0 or 1). */
+int32_t mtb_yee2d_current(const mtb_yee2d_plan *plan);
+
+/* Number of kernel launches the last mtb_yee2d_run issued. */
+int64_t mtb_yee2d_last_launches(const mtb_yee2d_plan *plan);
+
+void mtb_yee2d_plan_destroy(mtb_yee2d_plan *plan);
+
+/* ---------------------------------------------------------------- 3D */
+
+/* One 3D structure (State3D / Coeffs3D, CPML path, sigma = 0, no poles).
+ * Box layout: every array nx x ny x zpitch floats, zpitch % 4 == 0,
+ * zpitch >= nz; the component's reference array in the low corner.
+ * E is stored (the functional stepper's primary), eps is cell-centred. */
+typedef struct mtb_yee3d_struct {
+    int32_t nx, ny, nz, zpitch;
+    float dt, dx;
+    int32_t point_sign;     /* +1 step_3d (adds), -1 lean (subtracts)       */
+    int32_t pad_;
+    float *f[6][2];         /* Ex Ey Ez Hx Hy Hz, ping-pong pairs           */
+    const float *eps;       /* cell-centred eps (nx, ny, nz) in box layout  */
+    /* CPML memory in box layout, order of core/stepper_3d.py:46-57:
+     * Ez_y Ey_z Ex_z Ez_x Ey_x Ex_y Hz_y Hy_z Hx_z Hz_x Hy_x Hx_y */
+    float *psi[12][2];
+    /* (b, a) profiles: [axis][0] half nodes (n-1), [axis][1] integer nodes (n) */
+    const float *prof_b[3][2];
+    const float *prof_a[3][2];
+    /* soft current: cells (i, j, k) on component src_comp, CSR over the
+     * (i, j) rows (row_ptr has nx*ny+1 entries, row i*ny+j; col = k).
+     * Point sources follow point_sign; mask sources always subtract
+     * (core/stepper_3d.py:452-461). amp_col must be 0. */
+    int32_t src_comp;
+    int32_t src_is_point;
+    mtb_cells src;
+    /* plane samples: component `comp` at plane `index` normal to `axis`,
+     * window [lo0, hi0) x [lo1, hi1) of the two in-plane axes (in order),
+     * copied row-major to ring_off. */
+    const int32_t *planes;  /* device int32[n_planes][8]:
+                               comp, axis, index, lo0, hi0, lo1, hi1, unused */
+    const int64_t *plane_ring_off; /* device int64[n_planes]               */
+    int32_t n_planes;
+    int32_t pad2_;
+} mtb_yee3d_struct;
+
+typedef struct mtb_yee3d_plan mtb_yee3d_plan;
+
+int mtb_yee3d_plan_create(const mtb_yee3d_struct *s,
+                          const mtb_dft_region *regions, int32_t n_regions,
+                          const mtb_phase_group *groups, int32_t n_groups,
+                          int64_t ring_slot_elems, const mtb_tuning *tuning,
+                          mtb_yee3d_plan **out);
+int mtb_yee3d_run(mtb_yee3d_plan *plan, int64_t t0, int32_t k,
+                  const double *coef, void *stream);
+int32_t mtb_yee3d_current(const mtb_yee3d_plan *plan);
+int64_t mtb_yee3d_last_launches(const mtb_yee3d_plan *plan);
+void mtb_yee3d_plan_destroy(mtb_yee3d_plan *plan);
+
+/* ------------------------------------------------------------ layout */
+
+/* Strided copy of an n0 x n1 x n2 block between a dense reference array
+ * (strides s0, s1, 1 in elements) and a box array (strides b0, b1, 1).
+ * mtb_pack writes box[i,j,k] = src[i,j,k] for the block and zero for the
+ * rest of the box row range [0, b_rows) x [0, b1_extent); mtb_unpack copies
+ * the block back. Both run on `stream`. */
+int mtb_pack(const float *src, int64_t n0, int64_t n1, int64_t n2,
+             int64_t s0, int64_t s1, float *box, int64_t box_n0,
+             int64_t box_n1, int64_t box_n2, int64_t b0, int64_t b1,
+             int64_t off0, int64_t off1, int64_t off2, void *stream);
+int mtb_unpack(const float *box, int64_t n0, int64_t n1, int64_t n2,
+               int64_t b0, int64_t b1, int64_t off0, int64_t off1,
+               int64_t off2, float *dst, int64_t s0, int64_t s1, void *stream);
+/* As mtb_unpack, dividing by a second box array of the same layout:
+ * dst = box / den (E = D / eps when exporting a 2D state, the reference's
+ * update_eh(E), core/stepper_tm.py:224-231). */
+int mtb_unpack_ratio(const float *box, const float *den, int64_t n0, int64_t n1,
+                     int64_t n2, int64_t b0, int64_t b1, int64_t off0,
+                     int64_t off1, int64_t off2, float *dst, int64_t s0,
+                     int64_t s1, void *stream);
+
+/* Count entries of x (n floats) whose |x| > 0 where mask_row (per leading
+ * index, n0 entries) and mask_col (per last index) are both zero -- used to
+ * check CPML memory is zero outside the absorbing layers on import. */
+int mtb_count_outside(const float *x, int64_t n0, int64_t n1, int64_t s0,
+                      const uint8_t *active0, const uint8_t *active1,
+                      int64_t *count_dev, void *stream);
+
+/* ------------------------------------------------------------ misc */
+
+const char *mtb_last_error(void);
+int32_t mtb_abi_version(void);
+/* sizeof of the ABI structs, for binding checks: 0 mtb_cells,
+ * 1 mtb_line_sample, 2 mtb_yee2d_struct, 3 mtb_phase_group,
+ * 4 mtb_dft_region, 5 mtb_tuning, 6 mtb_yee3d_struct */
+int64_t mtb_struct_size(int32_t which);
+/* Kernels launched by this library since load (all entry points). */
+int64_t mtb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEEP_B200_H */

@@ -1,0 +1,71 @@
+"""TM state (reference: core/stepper_tm.py:12-71) and a one-step driver."""
+from typing import NamedTuple
+
+import torch
+
+from .grid import Grid
+
+
+class TMState(NamedTuple):
+    Ez: torch.Tensor       # (nx, ny)        at n
+    Hx: torch.Tensor       # (nx, ny-1)      at n-1/2
+    Hy: torch.Tensor       # (nx-1, ny)      at n-1/2
+    Dz: torch.Tensor       # (nx, ny)
+    P_cur: torch.Tensor    # (n_poles, nx, ny) -- n_poles == 0 on the B200 path
+    P_prev: torch.Tensor
+    psi_Ezy: torch.Tensor  # (nx, ny-1)      CPML memory of dEz/dy (Hx update)
+    psi_Ezx: torch.Tensor  # (nx-1, ny)      dEz/dx (Hy update)
+    psi_Hyx: torch.Tensor  # (nx-2, ny_e)    dHy/dx (Dz update, live Ez region)
+    psi_Hxy: torch.Tensor  # (nx-2, ny_e)    dHx/dy
+    Bx: torch.Tensor | None = None
+    By: torch.Tensor | None = None
+    Mx_cur: torch.Tensor | None = None
+    Mx_prev: torch.Tensor | None = None
+    My_cur: torch.Tensor | None = None
+    My_prev: torch.Tensor | None = None
+    Hx0: torch.Tensor | None = None
+    Hy0: torch.Tensor | None = None
+
+
+def init_tm_state(grid: Grid, n_poles: int = 0, y_pmc: bool = False, **kw) -> TMState:
+    """Zero TM state; psi_Hyx/psi_Hxy cover the interior (ny_e = ny-2) or
+    every row under y_pmc (ny_e = ny), as core/stepper_tm.py:41-71."""
+    for k, v in kw.items():
+        if v:
+            raise NotImplementedError(f"{k}: not implemented on the B200 path")
+    if n_poles:
+        raise NotImplementedError("dispersive poles: not implemented on the B200 path")
+    nx, ny = grid.nx, grid.ny
+    ny_e = ny if y_pmc else ny - 2
+    z = grid.zeros
+    return TMState(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
+                   P_cur=z(0, nx, ny), P_prev=z(0, nx, ny), psi_Ezy=z(nx, ny - 1),
+                   psi_Ezx=z(nx - 1, ny), psi_Hyx=z(nx - 2, ny_e), psi_Hxy=z(nx - 2, ny_e))
+
+
+def step_tm(state, m, src_amp=0.0, src_mask=None, src_h_amp: float = 0.0,
+            src_hy_mask=None, src_hx_mask=None):
+    """One TM step (core/stepper_tm.py:234-254 phase order) on the GPU.
+    Convenience wrapper: a run of k steps should use run_tm / _run_chunk."""
+    from ..engine2d import Engine2D
+    src = _OneStepSource(src_amp, src_mask, src_h_amp,
+                         {k: v for k, v in (("src_hy_mask", src_hy_mask),
+                                            ("src_hx_mask", src_hx_mask)) if v is not None})
+    eng = Engine2D([(state, m, src if (src_mask is not None or src.h_masks) else None, [])])
+    eng.run(0, 1)
+    out = eng.state(0)
+    eng.close()
+    return out
+
+
+class _OneStepSource:
+    """Adapter: a fixed amplitude for the single step of step_tm / step_te."""
+
+    def __init__(self, amp, mask, h_amp, h_masks):
+        self._a, self.mask, self._h, self.h_masks = float(amp), mask, float(h_amp), h_masks
+
+    def amplitude(self, t_idx):
+        return self._a
+
+    def h_amplitude(self, t_idx):
+        return self._h

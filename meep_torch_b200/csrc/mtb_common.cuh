@@ -1,0 +1,118 @@
+// Shared internals of the B200 FDTD library: error state, launch counting,
+// vector helpers. Device code targets sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/meep_b200.h"
+
+namespace mtb {
+
+// Last error text, one per host thread (mtb_last_error()).
+void set_error(const char *fmt, ...);
+int fail(int code, const char *fmt, ...);
+void count_launch(int64_t n = 1);
+
+#define MTB_CUDA_TRY(expr)                                                    \
+    do {                                                                      \
+        cudaError_t e_ = (expr);                                              \
+        if (e_ != cudaSuccess)                                                \
+            return ::mtb::fail(MTB_CUDA_ERROR, "%s failed: %s (%s:%d)", #expr, \
+                               cudaGetErrorString(e_), __FILE__, __LINE__);   \
+    } while (0)
+
+#define MTB_CHECK_LAUNCH()                                                    \
+    do {                                                                      \
+        cudaError_t e_ = cudaGetLastError();                                  \
+        if (e_ != cudaSuccess)                                                \
+            return ::mtb::fail(MTB_CUDA_ERROR, "kernel launch failed: %s (%s:%d)", \
+                               cudaGetErrorString(e_), __FILE__, __LINE__);   \
+        ::mtb::count_launch();                                                \
+    } while (0)
+
+// A device buffer owned by a plan (plan scratch only; fields, coefficients
+// and accumulators always belong to the caller).
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n) {
+        if (n <= bytes) return MTB_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (n == 0) return MTB_OK;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess)
+            return fail(MTB_CUDA_ERROR, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
+        bytes = n;
+        return MTB_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// Pinned host staging buffer.
+struct HostBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n) {
+        if (n <= bytes) return MTB_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        if (n == 0) return MTB_OK;
+        cudaError_t e = cudaMallocHost(&p, n);
+        if (e != cudaSuccess)
+            return fail(MTB_CUDA_ERROR, "cudaMallocHost(%zu) failed: %s", n, cudaGetErrorString(e));
+        bytes = n;
+        return MTB_OK;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------- DFT
+// Phase tables and the ring contraction shared by the 2D and 3D plans.
+struct DftState {
+    // host copies
+    std::string err;
+    int n_regions = 0, n_groups = 0;
+    mtb_dft_region *regions_h = nullptr;   // host copy
+    int *group_nf = nullptr;               // host
+    int *group_mode = nullptr;
+    double *group_dt = nullptr;
+    double *freqs_h = nullptr;             // concatenated
+    int *freq_off = nullptr;               // per group offset into freqs_h
+    int total_nf = 0;                      // sum of nf
+    // device
+    DevBuf regions_d, blk_start_d, phase_d, ring_d;
+    HostBuf phase_h;
+    int64_t slot_elems = 0;
+    int slots = 0;                         // ring depth K
+    int64_t n_blocks = 0;                  // contraction blocks
+    int *blk_start_h = nullptr;
+
+    int init(const mtb_dft_region *regions, int n_regions, const mtb_phase_group *groups,
+             int n_groups, int64_t slot_elems, int slots);
+    // Fill the phase table for steps [t0, t0+k) and upload it on `st`.
+    int upload_phases(int64_t t0, int k, cudaStream_t st);
+    // Fold ring slots [0, n) (steps t_first .. t_first+n-1, relative row
+    // `row0` of the uploaded table) into the accumulators.
+    int contract(int row0, int n, cudaStream_t st);
+    void release();
+};
+
+}  // namespace mtb

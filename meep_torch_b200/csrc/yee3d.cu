@@ -1,0 +1,627 @@
+// 3D Yee step with CPML (the functional stepper's CPML path,
+// core/stepper_3d.py:363-445, and its soft source :448-482) for sm_100a.
+//
+// A block owns TY consecutive y rows of one x segment and the whole z
+// extent; warp (wy, wz) owns row j0+wy and z columns wz*128 + 4*lane .. +3
+// (one float4 per array). The block marches along x. Per plane i:
+//   A  E(n) of plane i for rows j0-1 .. j0+TY and eps(i) go to shared memory
+//      (own rows from registers, the two halo rows loaded by halo warps);
+//      every warp loads E(n) and eps of plane i+1 into registers.
+//   B  __syncthreads
+//   C  H(n+1/2) of plane i for rows j0-1 .. j0+TY-1 (row j0-1 is recomputed
+//      by the halo warps and never stored) -> shared memory and HBM.
+//   D  __syncthreads
+//   E  E(n+1) of plane i for the own rows; source cells; store.
+// E is stored (as in the functional stepper), eps is cell-centred and
+// Yee-averaged in the kernel exactly as core/stepper_3d.py:_avg does.
+// Evolving arrays are ping-pong pairs because of the halo recomputation.
+#include <algorithm>
+#include <vector>
+
+#include "mtb_common.cuh"
+
+namespace mtb {
+
+constexpr int TY3 = 4;          // own rows per block
+constexpr int MAXNZ = 4;        // z warps per row (zpitch <= 512)
+
+struct Ctx3D {
+    const float *amp;           // coefficient of this step
+    int par;
+};
+
+__device__ __forceinline__ void ld4v(const float *p, float (&v)[4]) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void st4v(float *p, const float (&v)[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void z4(float (&v)[4]) { v[0] = v[1] = v[2] = v[3] = 0.f; }
+
+// profile activity (psi is touched only where the layer is active)
+__device__ __forceinline__ bool pact(float b, float a) { return a != 0.f || b != 1.f; }
+
+template <int NZW>
+__global__ void __launch_bounds__(32 * NZW * (TY3 + 2)) k_yee3d_step(
+    const mtb_yee3d_struct *__restrict__ SS, int rows_per_seg, Ctx3D C) {
+    const mtb_yee3d_struct &S = *SS;
+    const int nx = S.nx, ny = S.ny, nz = S.nz;
+    const int ZP = S.zpitch;
+    const int ZS = ZP + 4;                       // shared row stride (floats)
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wy = warp / NZW, wz = warp % NZW;
+    const int j0 = blockIdx.x * TY3;
+    const int i0 = blockIdx.y * rows_per_seg;
+    const int i1 = min(i0 + rows_per_seg, nx);
+    const int kb = wz * 128 + 4 * lane;
+    const bool kact = kb < ZP;
+    // role: own row, H halo row (j0-1) or E halo row (j0+TY)
+    const bool own = wy < TY3;
+    const bool hhalo = wy == TY3;
+    const bool ehalo = wy == TY3 + 1;
+    const int j = own ? j0 + wy : (hhalo ? j0 - 1 : j0 + TY3);
+    const bool jok = j >= 0 && j < ny;
+    const bool act = kact && jok;
+    const int sr = own ? wy + 1 : (hhalo ? 0 : TY3 + 1);   // shared row of j
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int par = C.par;
+    const int64_t NYZ = (int64_t)ny * ZP;
+    auto gidx = [&](int i, int jj) -> int64_t { return (int64_t)i * NYZ + (int64_t)jj * ZP + kb; };
+
+    extern __shared__ float sm[];
+    // E(n) plane i, rows j0-1 .. j0+TY: sE[c][row][z]; eps(i) sEp[row][z]
+    float *sE = sm;
+    float *sEp = sE + 3 * (TY3 + 2) * ZS;
+    // H(n+1/2) plane i, rows j0-1 .. j0+TY-1: sH[c][row][z]
+    float *sH = sEp + (TY3 + 2) * ZS;
+    auto SE = [&](int c, int r) -> float * { return sE + (c * (TY3 + 2) + r) * ZS; };
+    auto SH = [&](int c, int r) -> float * { return sH + (c * (TY3 + 1) + r) * ZS; };
+
+    const float *Eo[3] = {S.f[0][par], S.f[1][par], S.f[2][par]};
+    float *En[3] = {S.f[0][par ^ 1], S.f[1][par ^ 1], S.f[2][par ^ 1]};
+    const float *Ho[3] = {S.f[3][par], S.f[4][par], S.f[5][par]};
+    float *Hn[3] = {S.f[3][par ^ 1], S.f[4][par ^ 1], S.f[5][par ^ 1]};
+    const float *eps = S.eps;
+
+    // lane-constant z profiles (half nodes for H, integer nodes for E)
+    bool vzH[4], vzE[4], hzA[4], ezA[4], kin[4];
+    float hzb[4], hza[4], ezb[4], eza[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = kb + q;
+        vzH[q] = k <= nz - 2;
+        vzE[q] = k < nz;
+        kin[q] = k >= 1 && k <= nz - 2;
+        hzb[q] = vzH[q] ? __ldg(S.prof_b[2][0] + k) : 1.f;
+        hza[q] = vzH[q] ? __ldg(S.prof_a[2][0] + k) : 0.f;
+        ezb[q] = vzE[q] ? __ldg(S.prof_b[2][1] + k) : 1.f;
+        eza[q] = vzE[q] ? __ldg(S.prof_a[2][1] + k) : 0.f;
+        hzA[q] = vzH[q] && pact(hzb[q], hza[q]);
+        ezA[q] = kin[q] && pact(ezb[q], eza[q]);
+    }
+    const bool anyHz = act && (hzA[0] || hzA[1] || hzA[2] || hzA[3]);
+    const bool anyEz = act && (ezA[0] || ezA[1] || ezA[2] || ezA[3]);
+    // row-uniform y profiles
+    const bool vyH = j >= 0 && j <= ny - 2;
+    const bool jin = j >= 1 && j <= ny - 2;
+    float hyb = 1.f, hya = 0.f, eyb = 1.f, eya = 0.f;
+    if (vyH) { hyb = __ldg(S.prof_b[1][0] + j); hya = __ldg(S.prof_a[1][0] + j); }
+    if (jok) { eyb = __ldg(S.prof_b[1][1] + j); eya = __ldg(S.prof_a[1][1] + j); }
+    const bool hyA = act && vyH && pact(hyb, hya);
+    const bool eyA = act && jin && pact(eyb, eya);
+    const int kl = wz * 128 + 128;               // first column of the next z warp
+
+    float e1[3][4], ep1[4];                       // E(n), eps of plane i+1 (registers)
+    float hyP[4], hzP[4];                         // H(n+1/2) of plane i-1 (own rows)
+    z4(hyP); z4(hzP);
+
+    auto load_plane = [&](int i, float (&e)[3][4], float (&ep)[4]) {
+        if (act && i >= 0 && i < nx) {
+            const int64_t g = gidx(i, j);
+            ld4v(Eo[0] + g, e[0]); ld4v(Eo[1] + g, e[1]); ld4v(Eo[2] + g, e[2]);
+            const float4 x = __ldg(reinterpret_cast<const float4 *>(eps + g));
+            ep[0] = x.x; ep[1] = x.y; ep[2] = x.z; ep[3] = x.w;
+        } else {
+            z4(e[0]); z4(e[1]); z4(e[2]);
+            ep[0] = ep[1] = ep[2] = ep[3] = 1.f;
+        }
+    };
+
+    const int ifirst = (i0 > 0) ? i0 - 1 : i0;
+    {   // E(n) of plane ifirst into registers (becomes "plane i" at the first A)
+        load_plane(ifirst, e1, ep1);
+    }
+    for (int i = ifirst; i < i1; ++i) {
+        const bool work = i >= i0;               // plane i0-1 only prepares H(i0-1)
+        // ---- A: publish E(n), eps of plane i; fetch plane i+1
+        if (kact) {
+            st4v(SE(0, sr) + kb, e1[0]);
+            st4v(SE(1, sr) + kb, e1[1]);
+            st4v(SE(2, sr) + kb, e1[2]);
+            st4v(sEp + sr * ZS + kb, ep1);
+        }
+        float ec[3][4], epc[4];                   // E(n), eps of plane i (own)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ec[c][q] = e1[c][q];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) epc[q] = ep1[q];
+        if (!ehalo) load_plane(i + 1, e1, ep1);
+        else { z4(e1[0]); z4(e1[1]); z4(e1[2]); ep1[0] = ep1[1] = ep1[2] = ep1[3] = 1.f; }
+        __syncthreads();
+        if (ehalo) {   // the E-halo warps only load the next plane for the next A
+            if (i + 1 < i1) load_plane(i + 1, e1, ep1);
+        }
+
+        // ---- C: H(n+1/2) of plane i, rows j (own and H-halo)
+        // eps neighbours for step E's Yee averages, eps(i, j+1) and
+        // eps(i, k+1), are read here: the next plane's step A overwrites sEp
+        // and no barrier separates it from this plane's step E.
+        float epj1[4];
+        if (kact && !ehalo) ld4v(sEp + (sr + 1) * ZS + kb, epj1); else z4(epj1);
+        float epk1 = __shfl_down_sync(0xffffffffu, epc[0], 1);
+        if (lane == 31) epk1 = (kl < ZP && !ehalo) ? sEp[sr * ZS + kl] : 1.f;
+        float hn[3][4];
+        if (!ehalo) {
+            const bool xok = i <= nx - 2;
+            float hxb = 1.f, hxa = 0.f;
+            if (xok) { hxb = __ldg(S.prof_b[0][0] + i); hxa = __ldg(S.prof_a[0][0] + i); }
+            const bool hxA = act && xok && pact(hxb, hxa);
+            // neighbours: E(j+1) row, E(k+1) column
+            float ezj1[4], exj1[4];
+            if (kact) { ld4v(SE(2, sr + 1) + kb, ezj1); ld4v(SE(0, sr + 1) + kb, exj1); }
+            else { z4(ezj1); z4(exj1); }
+            float eyk1 = __shfl_down_sync(0xffffffffu, ec[1][0], 1);
+            float exk1 = __shfl_down_sync(0xffffffffu, ec[0][0], 1);
+            if (lane == 31) {
+                eyk1 = (kl < ZP) ? SE(1, sr)[kl] : 0.f;
+                exk1 = (kl < ZP) ? SE(0, sr)[kl] : 0.f;
+            }
+            const int64_t g = act ? gidx(i, j) : 0;
+            const bool store = own && work && act;
+            // Hx (core/stepper_3d.py:368-375): valid j <= ny-2, k <= nz-2
+            {
+                float h[4], pY[4], pZ[4];
+                if (act) ld4v(Ho[0] + g, h); else z4(h);
+                if (hyA) ld4v(S.psi[0][par] + g, pY); else z4(pY);
+                if (anyHz && vyH) ld4v(S.psi[1][par] + g, pZ); else z4(pZ);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!(vyH && vzH[q])) continue;
+                    const float eyn = (q < 3) ? ec[1][q + 1] : eyk1;
+                    const float dy = (ezj1[q] - ec[2][q]) * rdx;
+                    const float dz = (eyn - ec[1][q]) * rdx;
+                    float cy = dy, cz = dz;
+                    if (hyA) { pY[q] = hyb * pY[q] + hya * dy; cy = dy + pY[q]; }
+                    if (hzA[q]) { pZ[q] = hzb[q] * pZ[q] + hza[q] * dz; cz = dz + pZ[q]; }
+                    h[q] = h[q] - dt * (cy - cz);
+                }
+                if (store) {
+                    st4v(Hn[0] + g, h);
+                    if (hyA) st4v(S.psi[0][par ^ 1] + g, pY);
+                    if (anyHz && vyH) st4v(S.psi[1][par ^ 1] + g, pZ);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) hn[0][q] = h[q];
+            }
+            // Hy (core/stepper_3d.py:377-384): valid i <= nx-2, k <= nz-2
+            {
+                float h[4], pZ[4], pX[4];
+                if (act) ld4v(Ho[1] + g, h); else z4(h);
+                if (anyHz && xok) ld4v(S.psi[2][par] + g, pZ); else z4(pZ);
+                if (hxA) ld4v(S.psi[3][par] + g, pX); else z4(pX);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!(xok && vzH[q])) continue;
+                    const float exn = (q < 3) ? ec[0][q + 1] : exk1;
+                    const float dz = (exn - ec[0][q]) * rdx;
+                    const float dx = (e1[2][q] - ec[2][q]) * rdx;
+                    float cz = dz, cx = dx;
+                    if (hzA[q]) { pZ[q] = hzb[q] * pZ[q] + hza[q] * dz; cz = dz + pZ[q]; }
+                    if (hxA) { pX[q] = hxb * pX[q] + hxa * dx; cx = dx + pX[q]; }
+                    h[q] = h[q] - dt * (cz - cx);
+                }
+                if (store) {
+                    st4v(Hn[1] + g, h);
+                    if (anyHz && xok) st4v(S.psi[2][par ^ 1] + g, pZ);
+                    if (hxA) st4v(S.psi[3][par ^ 1] + g, pX);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) hn[1][q] = h[q];
+            }
+            // Hz (core/stepper_3d.py:386-393): valid i <= nx-2, j <= ny-2
+            {
+                float h[4], pX[4], pY[4];
+                if (act) ld4v(Ho[2] + g, h); else z4(h);
+                if (hxA && vyH) ld4v(S.psi[4][par] + g, pX); else z4(pX);
+                if (hyA && xok) ld4v(S.psi[5][par] + g, pY); else z4(pY);
+                if (xok && vyH) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (!vzE[q]) continue;
+                        const float dx = (e1[1][q] - ec[1][q]) * rdx;
+                        const float dy = (exj1[q] - ec[0][q]) * rdx;
+                        float cx = dx, cy = dy;
+                        if (hxA) { pX[q] = hxb * pX[q] + hxa * dx; cx = dx + pX[q]; }
+                        if (hyA) { pY[q] = hyb * pY[q] + hya * dy; cy = dy + pY[q]; }
+                        h[q] = h[q] - dt * (cx - cy);
+                    }
+                }
+                if (store) {
+                    st4v(Hn[2] + g, h);
+                    if (hxA && vyH) st4v(S.psi[4][par ^ 1] + g, pX);
+                    if (hyA && xok) st4v(S.psi[5][par ^ 1] + g, pY);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) hn[2][q] = h[q];
+            }
+            if (kact) {
+                const int hr = own ? wy + 1 : 0;
+                st4v(SH(0, hr) + kb, hn[0]);
+                st4v(SH(1, hr) + kb, hn[1]);
+                st4v(SH(2, hr) + kb, hn[2]);
+            }
+        }
+        __syncthreads();
+
+        // ---- E: E(n+1) of plane i, own rows
+        if (own && work) {
+            const int hr = wy + 1;                      // shared H row of j; j-1 is hr-1
+            const bool iin = i >= 1 && i <= nx - 2;
+            float exb = 1.f, exa = 0.f;
+            if (i < nx) { exb = __ldg(S.prof_b[0][1] + i); exa = __ldg(S.prof_a[0][1] + i); }
+            const bool exA = act && iin && pact(exb, exa);
+            float hzm[4], hxm[4];                       // H(j-1) rows
+            if (kact) { ld4v(SH(2, hr - 1) + kb, hzm); ld4v(SH(0, hr - 1) + kb, hxm); }
+            else { z4(hzm); z4(hxm); }
+            float hyk = __shfl_up_sync(0xffffffffu, hn[1][3], 1);   // H(k-1)
+            float hxk = __shfl_up_sync(0xffffffffu, hn[0][3], 1);
+            if (lane == 0) {
+                const int kk = wz * 128 - 1;
+                hyk = (kk >= 0) ? SH(1, hr)[kk] : 0.f;
+                hxk = (kk >= 0) ? SH(0, hr)[kk] : 0.f;
+            }
+            const int64_t g = act ? gidx(i, j) : 0;
+            float en[3][4];
+            // The psi recursions run over their own arrays' full extent
+            // (core/stepper_3d.py:79-101 State3D shapes), wider than the
+            // interior where the curl is applied (_pad_interior).
+            // Ex (core/stepper_3d.py:397-409): valid i <= nx-2
+            {
+                float pY[4], pZ[4];
+                const bool xok = i <= nx - 2;
+                const bool ldY = eyA && xok, ldZ = anyEz && xok;
+                if (ldY) ld4v(S.psi[6][par] + g, pY); else z4(pY);
+                if (ldZ) ld4v(S.psi[7][par] + g, pZ); else z4(pZ);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float hym = (q == 0) ? hyk : hn[1][q - 1];
+                    const float dy = (hn[2][q] - hzm[q]) * rdx;      // psi_Hz_y: j interior, all k
+                    const float dz = (hn[1][q] - hym) * rdx;         // psi_Hy_z: k interior, all j
+                    float cy = dy, cz = dz;
+                    if (ldY && vzE[q]) { pY[q] = eyb * pY[q] + eya * dy; cy = dy + pY[q]; }
+                    if (ldZ && ezA[q]) { pZ[q] = ezb[q] * pZ[q] + eza[q] * dz; cz = dz + pZ[q]; }
+                    const float curl = (xok && jin && kin[q]) ? (cy - cz) : 0.f;
+                    float v = ec[0][q];
+                    if (xok && vzE[q] && act) {
+                        const float e_x = 0.5f * (epc[q] + ep1[q]);
+                        v = (v * e_x + dt * curl) / e_x;
+                    }
+                    en[0][q] = v;
+                }
+                if (ldY) st4v(S.psi[6][par ^ 1] + g, pY);
+                if (ldZ) st4v(S.psi[7][par ^ 1] + g, pZ);
+            }
+            // Ey (core/stepper_3d.py:411-422): valid j <= ny-2
+            {
+                float pZ[4], pX[4];
+                const bool ldZ = anyEz && vyH, ldX = exA && vyH;
+                if (ldZ) ld4v(S.psi[8][par] + g, pZ); else z4(pZ);
+                if (ldX) ld4v(S.psi[9][par] + g, pX); else z4(pX);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float hxkm = (q == 0) ? hxk : hn[0][q - 1];
+                    const float dz = (hn[0][q] - hxkm) * rdx;        // psi_Hx_z: k interior, all i
+                    const float dx = (hn[2][q] - hzP[q]) * rdx;      // psi_Hz_x: i interior, all k
+                    float cz = dz, cx = dx;
+                    if (ldZ && ezA[q]) { pZ[q] = ezb[q] * pZ[q] + eza[q] * dz; cz = dz + pZ[q]; }
+                    if (ldX && vzE[q]) { pX[q] = exb * pX[q] + exa * dx; cx = dx + pX[q]; }
+                    const float curl = (vyH && iin && kin[q]) ? (cz - cx) : 0.f;
+                    float v = ec[1][q];
+                    if (vyH && vzE[q] && act) {
+                        const float e_y = 0.5f * (epc[q] + epj1[q]);
+                        v = (v * e_y + dt * curl) / e_y;
+                    }
+                    en[1][q] = v;
+                }
+                if (ldZ) st4v(S.psi[8][par ^ 1] + g, pZ);
+                if (ldX) st4v(S.psi[9][par ^ 1] + g, pX);
+            }
+            // Ez (core/stepper_3d.py:424-437): valid k <= nz-2
+            {
+                float pX[4], pY[4];
+                const bool ldX = exA, ldY = eyA;
+                if (ldX) ld4v(S.psi[10][par] + g, pX); else z4(pX);
+                if (ldY) ld4v(S.psi[11][par] + g, pY); else z4(pY);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float dx = (hn[1][q] - hyP[q]) * rdx;      // psi_Hy_x: i interior, all j
+                    const float dy = (hn[0][q] - hxm[q]) * rdx;      // psi_Hx_y: j interior, all i
+                    float cx = dx, cy = dy;
+                    if (ldX && vzH[q]) { pX[q] = exb * pX[q] + exa * dx; cx = dx + pX[q]; }
+                    if (ldY && vzH[q]) { pY[q] = eyb * pY[q] + eya * dy; cy = dy + pY[q]; }
+                    const float curl = (iin && jin && vzH[q]) ? (cx - cy) : 0.f;
+                    float v = ec[2][q];
+                    if (vzH[q] && act) {
+                        const float e_z = 0.5f * (epc[q] + ((q < 3) ? epc[q + 1] : epk1));
+                        v = (v * e_z + dt * curl) / e_z;
+                    }
+                    en[2][q] = v;
+                }
+                if (ldX) st4v(S.psi[10][par ^ 1] + g, pX);
+                if (ldY) st4v(S.psi[11][par ^ 1] + g, pY);
+            }
+            // soft current cells of row (i, j) on component src_comp
+            if (act && S.src.n > 0) {
+                const int r = i * ny + j;
+                const int e0 = __ldg(S.src.row_ptr + r), e1x = __ldg(S.src.row_ptr + r + 1);
+                if (e0 < e1x) {
+                    const int c = S.src_comp;
+                    const float a = __ldg(C.amp + S.src.amp_col);
+                    const float sgn = S.src_is_point ? (float)S.point_sign : -1.f;
+                    for (int e = e0; e < e1x; ++e) {
+                        const int kq = __ldg(S.src.col + e) - kb;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            if (kq != q) continue;
+                            float epc_ = epc[q];
+                            float epn;
+                            if (c == 0) epn = ep1[q];
+                            else if (c == 1) epn = epj1[q];
+                            else epn = (q < 3) ? epc[q + 1] : epk1;
+                            const float ecomp = 0.5f * (epc_ + epn);
+                            const float v = a * __ldg(S.src.w + e);
+                            if (S.src_is_point) en[c][q] += sgn * (v * (1.0f / ecomp));
+                            else en[c][q] -= v / ecomp;
+                        }
+                    }
+                }
+            }
+            if (act) {
+                st4v(En[0] + g, en[0]);
+                st4v(En[1] + g, en[1]);
+                st4v(En[2] + g, en[2]);
+            }
+        }
+        if (own) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { hyP[q] = hn[1][q]; hzP[q] = hn[2][q]; }
+        }
+    }
+}
+
+// Copy the plane samples of the (new) state into one ring slot.
+__global__ void k_sample3d(const mtb_yee3d_struct *__restrict__ SS, const int64_t *__restrict__ pstart,
+                           int n_planes, int cur, float *__restrict__ ring) {
+    const mtb_yee3d_struct &S = *SS;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= pstart[n_planes]) return;
+    int lo = 0, hi = n_planes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pstart[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    const int *pl = S.planes + 8 * lo;
+    const int comp = pl[0], axis = pl[1], index = pl[2];
+    const int w1 = pl[6] - pl[5];
+    const int64_t p = e - pstart[lo];
+    const int a = pl[3] + (int)(p / w1), b = pl[5] + (int)(p % w1);
+    int i, j, k;
+    if (axis == 0) { i = index; j = a; k = b; }
+    else if (axis == 1) { i = a; j = index; k = b; }
+    else { i = a; j = b; k = index; }
+    const float *F = S.f[comp][cur];
+    ring[S.plane_ring_off[lo] + p] = F[((int64_t)i * S.ny + j) * S.zpitch + k];
+}
+
+}  // namespace mtb
+
+using namespace mtb;
+
+struct mtb_yee3d_plan {
+    mtb_yee3d_struct s{};
+    DevBuf s_d, pstart_d, amp_d;
+    HostBuf amp_h;
+    int rows = 32;
+    int nzw = 1;
+    int par = 0;
+    int n_planes = 0;
+    int64_t n_samples = 0;
+    size_t smem = 0;
+    int64_t last_launches = 0;
+    DftState dft;
+};
+
+template <int NZW>
+static int launch3d(mtb_yee3d_plan *p, Ctx3D C, cudaStream_t st) {
+    const dim3 grid((p->s.ny + TY3 - 1) / TY3, (p->s.nx + p->rows - 1) / p->rows);
+    k_yee3d_step<NZW><<<grid, 32 * NZW * (TY3 + 2), p->smem, st>>>(p->s_d.as<mtb_yee3d_struct>(),
+                                                                    p->rows, C);
+    MTB_CHECK_LAUNCH();
+    return MTB_OK;
+}
+
+template <int NZW>
+static int set_smem3d(size_t smem) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(k_yee3d_step<NZW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    return MTB_OK;
+}
+
+extern "C" {
+
+int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regions,
+                          int32_t n_regions, const mtb_phase_group *groups, int32_t n_groups,
+                          int64_t ring_slot_elems, const mtb_tuning *tuning,
+                          mtb_yee3d_plan **out) {
+    if (!out || !s) return fail(MTB_INVALID_ARG, "null argument");
+    *out = nullptr;
+    const mtb_yee3d_struct &S = *s;
+    if (S.nx < 3 || S.ny < 3 || S.nz < 3)
+        return fail(MTB_INVALID_ARG, "nx, ny, nz must be >= 3");
+    if (S.zpitch < S.nz || (S.zpitch & 3))
+        return fail(MTB_INVALID_ARG, "zpitch %d must be >= nz and a multiple of 4", S.zpitch);
+    if (S.zpitch > 128 * MAXNZ)
+        return fail(MTB_UNSUPPORTED, "zpitch %d > %d not supported", S.zpitch, 128 * MAXNZ);
+    if ((int64_t)S.nx * S.ny * S.zpitch >= (1LL << 34))
+        return fail(MTB_UNSUPPORTED, "grid too large");
+    if ((int64_t)S.nx * S.ny >= (1LL << 31)) return fail(MTB_UNSUPPORTED, "nx*ny too large");
+    if (!(S.dt > 0.f) || !(S.dx > 0.f)) return fail(MTB_INVALID_ARG, "dt, dx must be > 0");
+    if (S.point_sign != 1 && S.point_sign != -1)
+        return fail(MTB_INVALID_ARG, "point_sign must be +1 or -1");
+    for (int c = 0; c < 6; ++c)
+        for (int b = 0; b < 2; ++b)
+            if (!S.f[c][b] || (reinterpret_cast<uintptr_t>(S.f[c][b]) & 15))
+                return fail(MTB_INVALID_ARG, "field %d buffer %d null or not 16-byte aligned", c, b);
+    for (int c = 0; c < 12; ++c)
+        for (int b = 0; b < 2; ++b)
+            if (!S.psi[c][b] || (reinterpret_cast<uintptr_t>(S.psi[c][b]) & 15))
+                return fail(MTB_INVALID_ARG, "psi %d buffer %d null or not 16-byte aligned", c, b);
+    if (!S.eps || (reinterpret_cast<uintptr_t>(S.eps) & 15))
+        return fail(MTB_INVALID_ARG, "eps null or not 16-byte aligned");
+    for (int a = 0; a < 3; ++a)
+        for (int h = 0; h < 2; ++h)
+            if (!S.prof_b[a][h] || !S.prof_a[a][h])
+                return fail(MTB_INVALID_ARG, "null CPML profile");
+    if (S.src.n < 0) return fail(MTB_INVALID_ARG, "negative source cell count");
+    if (S.src.n > 0) {
+        if (!S.src.row_ptr || !S.src.col || !S.src.w || S.src.amp_col != 0)
+            return fail(MTB_INVALID_ARG, "source cells: null arrays or amp_col != 0");
+        if (S.src_comp < 0 || S.src_comp > 2)
+            return fail(MTB_INVALID_ARG, "src_comp must be Ex, Ey or Ez");
+    }
+    if (S.n_planes < 0 || (S.n_planes > 0 && (!S.planes || !S.plane_ring_off)))
+        return fail(MTB_INVALID_ARG, "bad plane sample list");
+    mtb_yee3d_plan *p = new mtb_yee3d_plan();
+    p->s = S;
+    p->rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
+    const int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
+    p->nzw = (S.zpitch + 127) / 128;
+    p->smem = sizeof(float) * (size_t)(S.zpitch + 4) * (4 * (TY3 + 2) + 3 * (TY3 + 1));
+    p->n_planes = S.n_planes;
+    int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
+    if (!rc) rc = p->s_d.ensure(sizeof(mtb_yee3d_struct));
+    if (!rc) rc = p->pstart_d.ensure(sizeof(int64_t) * (S.n_planes + 1));
+    if (!rc) {
+        switch (p->nzw) {
+            case 1: rc = set_smem3d<1>(p->smem); break;
+            case 2: rc = set_smem3d<2>(p->smem); break;
+            case 3: rc = set_smem3d<3>(p->smem); break;
+            default: rc = set_smem3d<4>(p->smem); break;
+        }
+    }
+    if (rc) { p->dft.release(); delete p; return rc; }
+    // plane sample extents (host copy of the device list)
+    std::vector<int64_t> ps(S.n_planes + 1, 0);
+    if (S.n_planes > 0) {
+        std::vector<int32_t> pl(8 * S.n_planes);
+        cudaError_t e = cudaMemcpy(pl.data(), S.planes, sizeof(int32_t) * 8 * S.n_planes,
+                                   cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            p->dft.release(); delete p;
+            return fail(MTB_CUDA_ERROR, "reading plane list: %s", cudaGetErrorString(e));
+        }
+        const int dims[3] = {S.nx, S.ny, S.nz};
+        for (int q = 0; q < S.n_planes; ++q) {
+            const int *d = &pl[8 * q];
+            const int comp = d[0], axis = d[1], index = d[2];
+            const int a0 = (axis == 0) ? 1 : 0, a1 = (axis == 2) ? 1 : 2;
+            if (comp < 0 || comp > 5 || axis < 0 || axis > 2 || index < 0 ||
+                index >= dims[axis] || d[3] < 0 || d[4] > dims[a0] || d[3] > d[4] || d[5] < 0 ||
+                d[6] > dims[a1] || d[5] > d[6]) {
+                p->dft.release(); delete p;
+                return fail(MTB_INVALID_ARG, "plane sample %d out of range", q);
+            }
+            ps[q + 1] = ps[q] + (int64_t)(d[4] - d[3]) * (d[6] - d[5]);
+        }
+    }
+    p->n_samples = ps[S.n_planes];
+    cudaError_t e = cudaMemcpy(p->s_d.p, &S, sizeof(S), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->pstart_d.p, ps.data(), sizeof(int64_t) * ps.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        p->dft.release(); delete p;
+        return fail(MTB_CUDA_ERROR, "plan upload failed: %s", cudaGetErrorString(e));
+    }
+    *out = p;
+    return MTB_OK;
+}
+
+int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (k < 0) return fail(MTB_INVALID_ARG, "k < 0");
+    p->last_launches = 0;
+    if (k == 0) return MTB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if ((rc = p->amp_h.ensure(sizeof(float) * k))) return rc;
+    if ((rc = p->amp_d.ensure(sizeof(float) * k))) return rc;
+    if ((rc = p->dft.upload_phases(t0, k, st))) return rc;   // syncs the stream first
+    float *ah = p->amp_h.as<float>();
+    for (int s = 0; s < k; ++s) ah[s] = coef ? (float)coef[s] : 0.f;
+    MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, p->amp_h.p, sizeof(float) * k, cudaMemcpyHostToDevice,
+                                 st));
+    int slot = 0;
+    const bool sampling = p->dft.n_regions > 0 && p->n_samples > 0;
+    for (int s = 0; s < k; ++s) {
+        Ctx3D C;
+        C.amp = p->amp_d.as<float>() + s;
+        C.par = p->par;
+        switch (p->nzw) {
+            case 1: rc = launch3d<1>(p, C, st); break;
+            case 2: rc = launch3d<2>(p, C, st); break;
+            case 3: rc = launch3d<3>(p, C, st); break;
+            default: rc = launch3d<4>(p, C, st); break;
+        }
+        if (rc) return rc;
+        ++p->last_launches;
+        p->par ^= 1;
+        if (sampling) {
+            float *ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;
+            const int64_t nb = (p->n_samples + 255) / 256;
+            k_sample3d<<<(unsigned)nb, 256, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(),
+                                                    p->pstart_d.as<int64_t>(), p->n_planes, p->par,
+                                                    ring);
+            MTB_CHECK_LAUNCH();
+            ++p->last_launches;
+        }
+        ++slot;
+        if (slot == p->dft.slots || s == k - 1) {
+            if (sampling) {
+                if ((rc = p->dft.contract(s + 1 - slot, slot, st))) return rc;
+                ++p->last_launches;
+            }
+            slot = 0;
+        }
+    }
+    return MTB_OK;
+}
+
+int32_t mtb_yee3d_current(const mtb_yee3d_plan *p) { return p ? p->par : -1; }
+
+int64_t mtb_yee3d_last_launches(const mtb_yee3d_plan *p) { return p ? p->last_launches : -1; }
+
+void mtb_yee3d_plan_destroy(mtb_yee3d_plan *p) {
+    if (!p) return;
+    p->s_d.release();
+    p->pstart_d.release();
+    p->amp_d.release();
+    p->amp_h.release();
+    p->dft.release();
+    delete p;
+}
+
+}  // extern "C"

@@ -1,0 +1,558 @@
+"""2D engine: turns the reference's state / coeffs / source / monitor objects
+into one C plan (include/meep_b200.h, mtb_yee2d_*) and back.
+
+The objects are duck-typed on the reference's interfaces so both this
+package's mirror classes and the reference's own (meep_torch.core) work:
+
+* state  -- ``TMState`` (core/stepper_tm.py:12-34) or ``TEState``
+  (core/stepper_te.py:11-24): torch tensors on one CUDA device, float32.
+* coeffs -- ``TMCoeffs`` / ``TECoeffs`` (core/coeffs.py:21-74, :294-344).
+* source -- ``.amplitude(t)``, ``.mask``, optional ``.h_masks`` /
+  ``.h_amplitude(t)`` (core/run.py:17-24, core/sources.py:49-91).
+* monitors -- ``DFTFieldsMonitor`` / ``FluxMonitorTM`` / ``FluxMonitorTE`` /
+  ``FluxMonitorTEY`` (core/monitors.py:24-155), reduce == "sum".
+
+Anything outside that set raises ``MtbUnsupported`` (a NotImplementedError)
+before any device work; there is no CPU or torch fallback in this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._lib import MtbUnsupported
+
+PHASE_MODES = {"exact": 0, "reference_fp32": 1}
+
+
+def _round4(n: int) -> int:
+    return (n + 3) // 4 * 4
+
+
+def _is_te(state) -> bool:
+    return hasattr(state, "Hz") and not hasattr(state, "Ez")
+
+
+def _need(cond, msg):
+    if not cond:
+        raise MtbUnsupported(msg)
+
+
+def _opt_none(obj, names):
+    for n in names:
+        v = getattr(obj, n, None)
+        _need(v is None or (isinstance(v, (int, bool)) and not v),
+              f"{type(obj).__name__}.{n} is set: not supported by the B200 path")
+
+
+def coef_table(source, attr: str, t0: int, k: int, dt: float) -> np.ndarray:
+    """FP64 per-step mask coefficients dt * amplitude(t), t = t0 .. t0+k-1.
+
+    Known profiles of core/sources.py are evaluated vectorised in FP64 with the
+    same formula; anything else calls the source's own method per step."""
+    t_idx = np.arange(t0, t0 + k, dtype=np.float64)
+    fn = getattr(source, attr)
+    prof = getattr(source, "profile", None)
+    src_dt = getattr(source, "dt", None)
+    if attr == "amplitude" and prof is not None and src_dt is not None and \
+            type(fn).__name__ == "method" and fn.__func__.__name__ == "amplitude" and \
+            _plain_half_step(source):
+        t = (t_idx + 0.5) * src_dt
+        amp = _profile_vec(prof, t)
+        if amp is not None:
+            return dt * amp
+    return np.array([dt * float(fn(int(t))) for t in range(t0, t0 + k)], dtype=np.float64)
+
+
+def _plain_half_step(source) -> bool:
+    # LineSource / SoftSource / PlaneSource / PointSource3D sample their profile
+    # at (t_idx + 1/2) dt (core/sources.py:90-91, :116-117, monitors_3d.py:48, :66)
+    return type(source).__name__ in ("LineSource", "SoftSource", "PlaneSource", "PointSource3D")
+
+
+def _profile_vec(prof, t: np.ndarray):
+    name = type(prof).__name__
+    if name == "GaussianPulse" and hasattr(prof, "t0") and hasattr(prof, "w"):
+        # core/sources.py:33-36
+        d = t - prof.t0
+        return np.cos(2 * math.pi * prof.fcen * d) * np.exp(-(d ** 2) / (2 * prof.w ** 2))
+    if name == "CWRamp":
+        # core/sources.py:44-46
+        return np.sin(2 * math.pi * prof.fcen * t) * np.minimum(1.0, t / prof.t_ramp)
+    if name == "ContinuousSource" and hasattr(prof, "t_ramp"):
+        # core/sources.py:105-111
+        ramp = (0.5 - 0.5 * np.cos(math.pi * np.minimum(1.0, t / prof.t_ramp))
+                if prof.t_ramp > 0 else 1.0)
+        return np.sin(2 * math.pi * prof.fcen * t) * ramp
+    return None
+
+
+def _cells(mask: torch.Tensor, n_rows: int, device) -> tuple:
+    """CSR-by-row list of the nonzero cells of a 2D mask (rows = box rows)."""
+    m = mask.detach().to(device=device, dtype=torch.float32)
+    idx = torch.nonzero(m, as_tuple=False)
+    if idx.numel() == 0:
+        return None
+    rows = idx[:, 0]
+    counts = torch.bincount(rows, minlength=n_rows)
+    row_ptr = torch.zeros(n_rows + 1, dtype=torch.int32, device=device)
+    row_ptr[1:] = torch.cumsum(counts, 0).to(torch.int32)
+    col = idx[:, 1].to(torch.int32).contiguous()
+    w = m[idx[:, 0], idx[:, 1]].contiguous()
+    return row_ptr, col, w
+
+
+@dataclass
+class _Item:
+    state: object
+    coeffs: object
+    source: object
+    monitors: list
+    te: bool = False
+    nx: int = 0
+    ny: int = 0
+    pitch: int = 0
+    box: dict = field(default_factory=dict)      # name -> [buf0, buf1] or tensor
+    keep: list = field(default_factory=list)     # tensors the plan points at
+    accs: list = field(default_factory=list)
+    amp_col: int = -1
+    hamp_col: int = -1
+
+
+class Engine2D:
+    """A batch of independent 2D structures advanced by one mtb_yee2d plan.
+
+    ``items``: iterable of (state, coeffs, source, monitors). States are
+    imported into box-layout ping-pong buffers at construction; ``run``
+    advances every structure; ``state(b)`` / ``accumulators(b)`` export in
+    the reference's types and shapes."""
+
+    def __init__(self, items, *, phase_mode: str = "exact", rows_per_warp: int = 0,
+                 ring_slots: int = 0, stream=None):
+        self.lib = L.load()
+        self.items = [_Item(*it) for it in items]
+        _need(len(self.items) > 0, "empty batch")
+        self.device = None
+        self.phase_mode = PHASE_MODES[phase_mode]
+        self.stream = stream
+        self.t = None
+        for it in self.items:
+            self._validate(it)
+        self._build(rows_per_warp, ring_slots)
+
+    # ---------------------------------------------------------------- import
+    def _validate(self, it: _Item):
+        s, c = it.state, it.coeffs
+        it.te = _is_te(s)
+        main = s.Hz if it.te else s.Ez
+        _need(isinstance(main, torch.Tensor) and main.is_cuda,
+              "state tensors must be CUDA tensors (the B200 path has no CPU mode)")
+        _need(main.dtype == torch.float32, f"state dtype {main.dtype}: the B200 path computes "
+              "in float32 (convert the grid to float32)")
+        if self.device is None:
+            self.device = main.device
+        _need(main.device == self.device, "all structures of a batch must share one device")
+        if it.te:
+            it.nx, it.ny = main.shape[0] + 1, main.shape[1] + 1
+            _need(s.Px_cur.shape[0] == 0 and s.Py_cur.shape[0] == 0, "dispersive poles")
+            _opt_none(c, ["d1x", "hz1", "inv_xx_x", "c3xy", "c3yx", "has_chi2",
+                          "y_mirror_lo", "x_mirror_lo"])
+        else:
+            it.nx, it.ny = main.shape
+            _need(s.P_cur.shape[0] == 0, "dispersive poles")
+            _opt_none(s, ["Bx", "Hx0", "Hy0"])
+            _opt_none(c, ["d1", "h1x", "mc1x", "has_chi2", "y_mirror_lo", "x_mirror_lo",
+                          "y_rot2_lo", "rot4_lo"])
+        _need(not getattr(c, "has_kerr", False), "Kerr (chi3) media")
+        for k in ("k_hx", "k_hy", "k_ex", "k_ey"):
+            kv = getattr(c, k)
+            _need(bool(torch.all(kv == 1)), f"CPML kappa != 1 ({k})")
+        for mon in it.monitors:
+            _need(getattr(mon, "reduce", "sum") == "sum",
+                  f"{type(mon).__name__}: only sum-reduced monitors run on the B200 path")
+        it.pitch = _round4(it.ny)
+
+    def _pack(self, src: torch.Tensor, nx, pitch, off=(0, 0)) -> torch.Tensor:
+        box = torch.empty((nx, pitch), dtype=torch.float32, device=self.device)
+        src = src.detach().to(dtype=torch.float32).contiguous()
+        n0, n1 = (src.shape[0], src.shape[1]) if src.dim() == 2 else (0, 0)
+        L.check(self.lib.mtb_pack(L.ptr(src) if src.numel() else 0, n0, n1, 1, n1, 1,
+                                  L.ptr(box), nx, pitch, 1, pitch, 1, off[0], off[1], 0,
+                                  self._sptr()), "pack")
+        return box
+
+    def _pair(self, src, nx, pitch, off=(0, 0)):
+        a = self._pack(src, nx, pitch, off)
+        return [a, a.clone()]
+
+    def _sptr(self):
+        st = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
+        return st.cuda_stream
+
+    def _profiles(self, it: _Item):
+        c, nx, ny = it.coeffs, it.nx, it.ny
+        dev = self.device
+
+        def flat(t):
+            return t.detach().reshape(-1).to(device=dev, dtype=torch.float32).contiguous()
+
+        def node(b, a, n):
+            # interior-sliced node profile -> full n nodes; walls inert (b=1, a=0)
+            b, a = flat(b), flat(a)
+            fb = torch.ones(n, dtype=torch.float32, device=dev)
+            fa = torch.zeros(n, dtype=torch.float32, device=dev)
+            if b.numel() == n:
+                fb.copy_(b); fa.copy_(a)
+            elif b.numel() == n - 2:
+                fb[1:-1] = b; fa[1:-1] = a
+            else:
+                raise MtbUnsupported(f"unexpected CPML profile length {b.numel()} for n={n}")
+            return fb, fa
+
+        hx = (flat(c.b_hx), flat(c.a_hx))
+        hy = (flat(c.b_hy), flat(c.a_hy))
+        _need(hx[0].numel() == nx - 1 and hy[0].numel() == ny - 1, "CPML half-node profile length")
+        ex = node(c.b_ex, c.a_ex, nx)
+        ey = node(c.b_ey, c.a_ey, ny)
+        it.keep += [*hx, *hy, *ex, *ey]
+        return hx, hy, ex, ey
+
+    def _build(self, rows_per_warp, ring_slots):
+        lib = self.lib
+        dev = self.device
+        structs = (L.Yee2DStruct * len(self.items))()
+        regions, groups, group_key = [], [], {}
+        ring = 0
+        amp_cols = 0
+        self._amp_sources = []      # (column, source, attr, dt)
+        col_of = {}
+
+        def group(freqs, dt):
+            f = tuple(float(x) for x in torch.as_tensor(freqs).detach().reshape(-1).cpu()
+                      .to(torch.float64).tolist())
+            key = (f, float(dt))
+            if key not in group_key:
+                arr = (C.c_double * len(f))(*f)
+                group_key[key] = len(groups)
+                groups.append((arr, len(f), float(dt)))
+            return group_key[key], len(f)
+
+        def alloc_ring(n):
+            nonlocal ring
+            off = ring
+            ring += _round4(n)
+            return off
+
+        for b, it in enumerate(self.items):
+            s, c, te = it.state, it.coeffs, it.te
+            nx, ny, P = it.nx, it.ny, it.pitch
+            S = structs[b]
+            S.pol = L.MTB_TE if te else L.MTB_TM
+            S.nx, S.ny, S.pitch = nx, ny, P
+            S.y_pmc = 1 if (not te and getattr(c, "y_pmc", False)) else 0
+            S.dt, S.dx = float(c.dt), float(c.dx)
+            eps_b = None
+            if te:
+                f_main, f_x, f_y = self._pair(s.Hz, nx, P), self._pair(s.Dx, nx, P), \
+                    self._pair(s.Dy, nx, P)
+                eps_a = self._pack(c.eps_x, nx, P)
+                eps_b = self._pack(c.eps_y, nx, P)
+                psis = [self._pair(s.psi_Hzy, nx, P, (0, 1)), self._pair(s.psi_Hzx, nx, P, (1, 0)),
+                        self._pair(s.psi_Eyx, nx, P), self._pair(s.psi_Exy, nx, P)]
+                S.eps_b = L.ptr(eps_b)
+                it.keep.append(eps_b)
+            else:
+                f_main, f_x, f_y = self._pair(s.Dz, nx, P), self._pair(s.Hx, nx, P), \
+                    self._pair(s.Hy, nx, P)
+                eps_a = self._pack(c.eps_inf, nx, P)
+                yoff = 0 if S.y_pmc else 1
+                psis = [self._pair(s.psi_Ezy, nx, P), self._pair(s.psi_Ezx, nx, P),
+                        self._pair(s.psi_Hyx, nx, P, (1, yoff)),
+                        self._pair(s.psi_Hxy, nx, P, (1, yoff))]
+                # Ez is normally Dz/eps exactly (update_eh); an imported state
+                # where it is not is honoured on the first step
+                ez_ref = s.Dz / c.eps_inf.to(s.Dz.dtype)
+                if not torch.equal(ez_ref, s.Ez):
+                    eex = self._pack(s.Ez, nx, P)
+                    S.explicit_e = 1
+                    S.e_explicit = L.ptr(eex)
+                    it.keep.append(eex)
+            it.box = dict(main=f_main, x=f_x, y=f_y, psi=psis, eps_a=eps_a, eps_b=eps_b)
+            it.keep += [*f_main, *f_x, *f_y, eps_a] + [t for p in psis for t in p]
+            S.f_main[0], S.f_main[1] = L.ptr(f_main[0]), L.ptr(f_main[1])
+            S.f_x[0], S.f_x[1] = L.ptr(f_x[0]), L.ptr(f_x[1])
+            S.f_y[0], S.f_y[1] = L.ptr(f_y[0]), L.ptr(f_y[1])
+            S.eps_a = L.ptr(eps_a)
+            for k in range(4):
+                S.psi[k][0], S.psi[k][1] = L.ptr(psis[k][0]), L.ptr(psis[k][1])
+            self._check_psi_outside(it)
+            hx, hy, ex, ey = self._profiles(it)
+            S.hx_b, S.hx_a = L.ptr(hx[0]), L.ptr(hx[1])
+            S.hy_b, S.hy_a = L.ptr(hy[0]), L.ptr(hy[1])
+            S.ex_b, S.ex_a = L.ptr(ex[0]), L.ptr(ex[1])
+            S.ey_b, S.ey_a = L.ptr(ey[0]), L.ptr(ey[1])
+
+            # ---- sources
+            src = it.source
+            if src is not None:
+                mask = getattr(src, "mask", None)
+                if mask is not None:
+                    want = (nx, ny - 1) if te else (nx, ny)
+                    _need(tuple(mask.shape) == want,
+                          f"source mask shape {tuple(mask.shape)} != {want}")
+                    cl = _cells(mask, nx, dev)
+                    if cl is not None:
+                        it.amp_col = col_of.setdefault((id(src), "amplitude"), amp_cols)
+                        if it.amp_col == amp_cols:
+                            amp_cols += 1
+                            self._amp_sources.append((it.amp_col, src, "amplitude", float(c.dt), "e"))
+                        self._set_cells(S.src_e, cl, it.amp_col, it)
+                h_masks = getattr(src, "h_masks", None) or {}
+                if h_masks:
+                    key = (id(src), "h_amplitude")
+                    hcol = col_of.setdefault(key, amp_cols)
+                    if hcol == amp_cols:
+                        amp_cols += 1
+                        self._amp_sources.append((hcol, src, "h_amplitude", float(c.dt), "h"))
+                    for name, m in h_masks.items():
+                        if m is None:
+                            continue
+                        if te:
+                            _need(name == "src_hz_mask", f"TE magnetic source {name}")
+                            _need(tuple(m.shape) == (nx - 1, ny - 1), "src_hz_mask shape")
+                            target = S.src_h1
+                        elif name == "src_hy_mask":
+                            _need(tuple(m.shape) == (nx - 1, ny), "src_hy_mask shape")
+                            target = S.src_h1
+                        elif name == "src_hx_mask":
+                            _need(tuple(m.shape) == (nx, ny - 1), "src_hx_mask shape")
+                            target = S.src_h2
+                        else:
+                            raise MtbUnsupported(f"magnetic source {name}")
+                        cl = _cells(m, nx, dev)
+                        if cl is not None:
+                            self._set_cells(target, cl, hcol, it)
+
+            # ---- monitors
+            lines = []
+            ring_full = [-1, -1, -1]
+            it.accs = []
+            for mon in it.monitors:
+                kind = type(mon).__name__
+                g, nf = group(mon.freqs, mon.dt)
+                if kind == "DFTFieldsMonitor":
+                    comp = mon.component
+                    names = ("Hz", "Ex", "Ey") if te else ("Ez", "Hx", "Hy")
+                    _need(comp in names, f"DFTFieldsMonitor on {comp}")
+                    ci = names.index(comp)
+                    shp = {"Ez": (nx, ny), "Hx": (nx, ny - 1), "Hy": (nx - 1, ny),
+                           "Hz": (nx - 1, ny - 1), "Ex": (nx - 1, ny), "Ey": (nx, ny - 1)}[comp]
+                    if ring_full[ci] < 0:
+                        ring_full[ci] = alloc_ring(nx * P)
+                    acc = torch.zeros((nf, 2) + shp, dtype=torch.float32, device=dev)
+                    n = shp[0] * shp[1]
+                    regions.append(self._region(acc, 0, n, 2 * n, ring_full[ci], -1, shp[0],
+                                                shp[1], P, shp[1], g,
+                                                2 if comp.startswith("E") else 1))
+                elif kind in ("FluxMonitorTM", "FluxMonitorTE", "FluxMonitorTEY"):
+                    lo, hi = int(mon.lo), int(mon.hi)
+                    Ln = hi - lo
+                    _need(Ln > 0, "empty flux line")
+                    if kind == "FluxMonitorTM":
+                        _need(not te, "FluxMonitorTM on a TE state")
+                        idx = int(mon.idx)
+                        if mon.x_normal:      # Ez row idx; Hy rows idx-1, idx
+                            e_line = (L.C2_MAIN, 0, idx)
+                            h_lines = [(L.C2_Y, 0, idx - 1), (L.C2_Y, 0, idx)]
+                        else:                 # Ez column idx; Hx columns idx-1, idx
+                            e_line = (L.C2_MAIN, 1, idx)
+                            h_lines = [(L.C2_X, 1, idx - 1), (L.C2_X, 1, idx)]
+                        toff_e, toff_h = 2, 1
+                    elif kind == "FluxMonitorTE":
+                        _need(te, "FluxMonitorTE on a TM state")
+                        idx = int(mon.ix)     # Ey row ix; Hz rows ix-1, ix
+                        e_line = (L.C2_Y, 0, idx)
+                        h_lines = [(L.C2_MAIN, 0, idx - 1), (L.C2_MAIN, 0, idx)]
+                        toff_e, toff_h = 1, 2
+                    else:
+                        _need(te, "FluxMonitorTEY on a TM state")
+                        idx = int(mon.iy)     # Ex column iy; Hz columns iy-1, iy
+                        e_line = (L.C2_X, 1, idx)
+                        h_lines = [(L.C2_MAIN, 1, idx - 1), (L.C2_MAIN, 1, idx)]
+                        toff_e, toff_h = 1, 2
+                    offs = []
+                    for comp, kd, index in [e_line] + h_lines:
+                        o = alloc_ring(Ln)
+                        lines.append((comp, kd, index, lo, hi, o))
+                        offs.append(o)
+                    acc = torch.zeros((nf, 4, Ln), dtype=torch.float32, device=dev)
+                    regions.append(self._region(acc, 0, Ln, 4 * Ln, offs[0], -1, 1, Ln, Ln, Ln,
+                                                g, toff_e))
+                    regions.append(self._region(acc, 2 * Ln, 3 * Ln, 4 * Ln, offs[1], offs[2], 1,
+                                                Ln, Ln, Ln, g, toff_h))
+                else:
+                    raise MtbUnsupported(f"monitor {kind}")
+                it.accs.append(acc)
+                it.keep.append(acc)
+            _need(len(lines) <= 16, "more than 16 monitor lines on one structure")
+            if lines:
+                arr = (L.LineSample * len(lines))()
+                for q, (comp, kd, index, lo, hi, o) in enumerate(lines):
+                    arr[q].comp, arr[q].kind, arr[q].index = comp, kd, index
+                    arr[q].lo, arr[q].hi, arr[q].ring_off = lo, hi, o
+                raw = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to(dev)
+                it.keep.append(raw)
+                S.lines = L.ptr(raw)
+                S.n_lines = len(lines)
+            for ci in range(3):
+                S.ring_full[ci] = ring_full[ci]
+
+        self.n_amp_cols = amp_cols
+        self.ring_elems = ring
+        reg_arr = (L.DftRegion * max(1, len(regions)))(*regions) if regions else None
+        grp_arr = (L.PhaseGroup * max(1, len(groups)))()
+        for q, (arr, nf, dt) in enumerate(groups):
+            grp_arr[q].freqs = C.cast(arr, C.POINTER(C.c_double))
+            grp_arr[q].nf, grp_arr[q].mode, grp_arr[q].dt = nf, self.phase_mode, dt
+        self._groups = groups
+        tun = L.Tuning(rows_per_warp, ring_slots, 0, 0)
+        plan = C.c_void_p()
+        L.check(lib.mtb_yee2d_plan_create(structs, len(self.items), reg_arr, len(regions),
+                                          grp_arr, len(groups), ring, amp_cols, C.byref(tun),
+                                          C.byref(plan)), "mtb_yee2d_plan_create")
+        self.plan = plan
+        self.structs = structs
+
+    def _set_cells(self, target, cl, col, it):
+        row_ptr, colv, w = cl
+        it.keep += [row_ptr, colv, w]
+        target.row_ptr, target.col, target.w = L.ptr(row_ptr), L.ptr(colv), L.ptr(w)
+        target.n, target.amp_col = int(colv.numel()), col
+
+    @staticmethod
+    def _region(acc, re_off, im_off, f_stride, ring_a, ring_b, rows, cols, ring_pitch,
+                acc_pitch, grp, toff):
+        r = L.DftRegion()
+        r.acc = L.ptr(acc)
+        r.re_off, r.im_off, r.f_stride = re_off, im_off, f_stride
+        r.ring_a, r.ring_b = ring_a, ring_b
+        r.rows, r.cols, r.ring_pitch, r.acc_pitch = rows, cols, ring_pitch, acc_pitch
+        r.group, r.toff = grp, toff
+        return r
+
+    def _check_psi_outside(self, it: _Item):
+        """CPML memory must vanish where its profile is inert (b == 1, a == 0):
+        the kernels never touch it there (the reference keeps it at zero)."""
+        c = it.coeffs
+
+        def inert(b, a):
+            return (b.detach().reshape(-1) == 1) & (a.detach().reshape(-1) == 0)
+
+        s = it.state
+        if it.te:
+            checks = [(s.psi_Hzy, None, inert(c.b_ey, c.a_ey)), (s.psi_Hzx, inert(c.b_ex, c.a_ex), None),
+                      (s.psi_Eyx, inert(c.b_hx, c.a_hx), None), (s.psi_Exy, None, inert(c.b_hy, c.a_hy))]
+        else:
+            checks = [(s.psi_Ezy, None, inert(c.b_hy, c.a_hy)), (s.psi_Ezx, inert(c.b_hx, c.a_hx), None),
+                      (s.psi_Hyx, inert(c.b_ex, c.a_ex), None), (s.psi_Hxy, None, inert(c.b_ey, c.a_ey))]
+        for psi, rows, cols in checks:
+            if psi.numel() == 0:
+                continue
+            m = psi != 0
+            if rows is not None:
+                m = m & rows.to(psi.device)[:, None]
+            if cols is not None:
+                m = m & cols.to(psi.device)[None, :]
+            _need(not bool(m.any()), "CPML memory is nonzero outside its absorbing layer")
+
+    # ------------------------------------------------------------------ run
+    def run(self, t0: int, k: int):
+        """Advance every structure k steps starting at step index t0."""
+        if k <= 0:
+            return
+        nc = max(self.n_amp_cols, 1)
+        ce = np.zeros((k, nc), dtype=np.float64)
+        ch = np.zeros((k, nc), dtype=np.float64)
+        have_e = have_h = False
+        for col, src, attr, dt, kind in self._amp_sources:
+            v = coef_table(src, attr, t0, k, dt)
+            if kind == "e":
+                ce[:, col] = v
+                have_e = True
+            else:
+                ch[:, col] = v
+                have_h = True
+        pe = ce.ctypes.data_as(C.POINTER(C.c_double)) if have_e else None
+        ph = ch.ctypes.data_as(C.POINTER(C.c_double)) if have_h else None
+        L.check(self.lib.mtb_yee2d_run(self.plan, t0, k, pe, ph, self._sptr()), "mtb_yee2d_run")
+        self.last_launches = self.lib.mtb_yee2d_last_launches(self.plan)
+
+    @property
+    def current(self) -> int:
+        return self.lib.mtb_yee2d_current(self.plan)
+
+    # ---------------------------------------------------------------- export
+    def _unpack(self, box, shape, off=(0, 0), den=None, den_off=None):
+        out = torch.empty(shape, dtype=torch.float32, device=self.device)
+        if out.numel() == 0:
+            return out
+        P = box.shape[1]
+        if den is None:
+            L.check(self.lib.mtb_unpack(L.ptr(box), shape[0], shape[1], 1, P, 1, off[0], off[1],
+                                        0, L.ptr(out), shape[1], 1, self._sptr()), "unpack")
+        else:
+            L.check(self.lib.mtb_unpack_ratio(L.ptr(box), L.ptr(den), shape[0], shape[1], 1, P,
+                                              1, off[0], off[1], 0, L.ptr(out), shape[1], 1,
+                                              self._sptr()), "unpack")
+        return out
+
+    def state(self, b: int = 0):
+        """Current state of structure b, as the input state's own type."""
+        it = self.items[b]
+        cur = self.current
+        s, nx, ny, bx = it.state, it.nx, it.ny, it.box
+        if it.te:
+            Hz = self._unpack(bx["main"][cur], (nx - 1, ny - 1))
+            Dx = self._unpack(bx["x"][cur], (nx - 1, ny))
+            Dy = self._unpack(bx["y"][cur], (nx, ny - 1))
+            Ex = self._unpack(bx["x"][cur], (nx - 1, ny), den=bx["eps_a"])
+            Ey = self._unpack(bx["y"][cur], (nx, ny - 1), den=bx["eps_b"])
+            ps = bx["psi"]
+            return s._replace(
+                Hz=Hz, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy,
+                psi_Hzy=self._unpack(ps[0][cur], (nx - 1, ny - 2), (0, 1)),
+                psi_Hzx=self._unpack(ps[1][cur], (nx - 2, ny - 1), (1, 0)),
+                psi_Eyx=self._unpack(ps[2][cur], (nx - 1, ny - 1)),
+                psi_Exy=self._unpack(ps[3][cur], (nx - 1, ny - 1)))
+        Dz = self._unpack(bx["main"][cur], (nx, ny))
+        Ez = self._unpack(bx["main"][cur], (nx, ny), den=bx["eps_a"])
+        ps = bx["psi"]
+        ny_e = s.psi_Hyx.shape[1]
+        yoff = 0 if ny_e == ny else 1
+        return s._replace(
+            Ez=Ez, Dz=Dz,
+            Hx=self._unpack(bx["x"][cur], (nx, ny - 1)),
+            Hy=self._unpack(bx["y"][cur], (nx - 1, ny)),
+            psi_Ezy=self._unpack(ps[0][cur], (nx, ny - 1)),
+            psi_Ezx=self._unpack(ps[1][cur], (nx - 1, ny)),
+            psi_Hyx=self._unpack(ps[2][cur], (nx - 2, ny_e), (1, yoff)),
+            psi_Hxy=self._unpack(ps[3][cur], (nx - 2, ny_e), (1, yoff)))
+
+    def accumulators(self, b: int = 0):
+        return list(self.items[b].accs)
+
+    def close(self):
+        if getattr(self, "plan", None):
+            self.lib.mtb_yee2d_plan_destroy(self.plan)
+            self.plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,173 @@
+"""CPU-side checks of the C ABI and the host logic (no GPU needed).
+
+* the shared library loads and exports every function include/meep_b200.h
+  declares, with ctypes struct layouts matching the C sizes;
+* argument validation fails with the documented status codes before any
+  device work;
+* the host mirror builds the same coefficients as the oracle, and the host
+  helpers (coefficient tables, flux windows) match the reference's rules.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fdtd as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from meep_torch_b200 import _lib, build
+    build.build()
+    return _lib.load()
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "meep_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(mtb_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = header_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_binding_covers_header():
+    from meep_torch_b200 import _lib
+    assert set(header_functions()) == set(_lib.SIGNATURES)
+
+
+def test_struct_layouts(lib):
+    from meep_torch_b200 import _lib
+    for i, cls in enumerate(_lib.STRUCTS):
+        assert lib.mtb_struct_size(i) == C.sizeof(cls), cls.__name__
+    assert lib.mtb_abi_version() == 1
+
+
+def test_plan_validation_errors(lib):
+    from meep_torch_b200 import _lib as L
+    plan = C.c_void_p()
+    rc = lib.mtb_yee2d_plan_create(None, 0, None, 0, None, 0, 0, 0, None, C.byref(plan))
+    assert rc == L.MTB_INVALID_ARG
+    assert b"structure" in lib.mtb_last_error()
+    s = (L.Yee2DStruct * 1)()
+    s[0].pol, s[0].nx, s[0].ny, s[0].pitch = 7, 10, 10, 12
+    assert lib.mtb_yee2d_plan_create(s, 1, None, 0, None, 0, 0, 0, None,
+                                     C.byref(plan)) == L.MTB_INVALID_ARG
+    s[0].pol, s[0].nx, s[0].ny, s[0].pitch = 0, 10, 10, 10      # pitch not % 4
+    assert lib.mtb_yee2d_plan_create(s, 1, None, 0, None, 0, 0, 0, None,
+                                     C.byref(plan)) == L.MTB_INVALID_ARG
+    s[0].pitch, s[0].dt, s[0].dx = 12, 0.025, 0.05               # null field pointers
+    assert lib.mtb_yee2d_plan_create(s, 1, None, 0, None, 0, 0, 0, None,
+                                     C.byref(plan)) == L.MTB_INVALID_ARG
+    assert b"null" in lib.mtb_last_error()
+    s3 = L.Yee3DStruct()
+    s3.nx, s3.ny, s3.nz, s3.zpitch = 10, 10, 10, 10
+    assert lib.mtb_yee3d_plan_create(C.byref(s3), None, 0, None, 0, 0, None,
+                                     C.byref(plan)) == L.MTB_INVALID_ARG
+    s3.zpitch = 1024
+    assert lib.mtb_yee3d_plan_create(C.byref(s3), None, 0, None, 0, 0, None,
+                                     C.byref(plan)) == L.MTB_UNSUPPORTED
+    assert lib.mtb_yee2d_run(None, 0, 1, None, None, None) == L.MTB_INVALID_ARG
+    assert lib.mtb_pack(None, 1, 1, 1, 1, 1, None, 1, 1, 1, 1, 1, 0, 0, 0, None) == \
+        L.MTB_INVALID_ARG
+
+
+def test_check_maps_status_to_exceptions(lib):
+    from meep_torch_b200 import _lib as L
+    with pytest.raises(ValueError):
+        L.check(L.MTB_INVALID_ARG)
+    with pytest.raises(NotImplementedError):
+        L.check(L.MTB_UNSUPPORTED)
+    with pytest.raises(RuntimeError):
+        L.check(L.MTB_CUDA_ERROR)
+
+
+@pytest.mark.parametrize("npml,pmc", [(8, False), (((4, 6), (0, 5)), False), (6, True)])
+def test_tm_coeffs_match_oracle(npml, pmc):
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    g = Grid(nx=40, ny=30, dx=0.05, device="cpu")
+    m = build_tm_coeffs(g, npml=npml, y_pmc=pmc)
+    o = O.tm_coeffs(40, 30, 0.05, npml=npml, y_pmc=pmc, dtype=np.float32)
+    for k in ("b_hy", "a_hy", "b_hx", "a_hx", "b_ex", "a_ex", "b_ey", "a_ey"):
+        np.testing.assert_allclose(getattr(m, k).numpy(), o[k], rtol=2e-6, atol=1e-7)
+
+
+def test_te_and_3d_coeffs_match_oracle():
+    from meep_torch_b200.core.coeffs import build_te_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs
+    rng = np.random.default_rng(0)
+    eps = rng.uniform(1, 12, (33, 27))
+    m = build_te_coeffs(Grid(nx=33, ny=27, dx=0.05, device="cpu"),
+                        eps_inf=torch.tensor(eps, dtype=torch.float32), npml=5)
+    o = O.te_coeffs(33, 27, 0.05, eps=eps, npml=5, dtype=np.float32)
+    np.testing.assert_array_equal(m.eps_x.numpy(), o["eps_x"])
+    np.testing.assert_array_equal(m.eps_y.numpy(), o["eps_y"])
+    for k in ("b_hx", "a_hx", "b_hy", "a_hy", "b_ex", "a_ex", "b_ey", "a_ey"):
+        np.testing.assert_allclose(getattr(m, k).numpy(), o[k], rtol=2e-6, atol=1e-7)
+    c = build_3d_coeffs(20, 18, 16, 1 / 16, npml=4, device="cpu")
+    o3 = O.coeffs_3d(20, 18, 16, 1 / 16, npml=4, dtype=np.float32)
+    for k in ("hx", "hy", "hz", "ex", "ey", "ez"):
+        for a, b in zip(c.cpml[k], o3["cpml"][k]):
+            np.testing.assert_allclose(a.numpy(), b, rtol=2e-6, atol=1e-7)
+
+
+def test_unsupported_features_raise():
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    g = Grid(nx=20, ny=20, dx=0.05, device="cpu")
+    with pytest.raises(NotImplementedError):
+        build_tm_coeffs(g, poles=[(1.0, 0.1, 1.0)])
+    with pytest.raises(NotImplementedError):
+        build_tm_coeffs(g, sigma_d=torch.ones(20, 20))
+    with pytest.raises(ValueError):
+        build_tm_coeffs(g, npml=10)
+
+
+def test_coef_table_matches_per_step_amplitudes():
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.sources import CustomSource, GaussianPulse, LineSource
+    from meep_torch_b200.engine2d import coef_table
+    g = Grid(nx=40, ny=30, dx=0.05, device="cpu")
+    for prof in (GaussianPulse(0.65, 0.2), CustomSource(lambda t: np.sin(t) ** 2)):
+        src = LineSource(g, 5, 3, 20, prof)
+        v = coef_table(src, "amplitude", 100, 400, g.dt)
+        ref = np.array([g.dt * src.amplitude(t) for t in range(100, 500)])
+        np.testing.assert_allclose(v, ref, rtol=1e-13, atol=1e-16)
+        # float32 rounding of the coefficient is what the kernel sees
+        assert np.array_equal(v.astype(np.float32), ref.astype(np.float32)) or \
+            np.max(np.abs(v.astype(np.float32) - ref.astype(np.float32))) <= \
+            np.max(np.abs(ref)) * 2 ** -23
+
+
+def test_line_source_mask_matches_oracle():
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource
+    g = Grid(nx=40, ny=30, dx=0.05, device="cpu")
+    for j0, j1 in ((3, 20), (7, 8)):
+        m = LineSource(g, 5, j0, j1, GaussianPulse(0.5, 0.2)).mask.numpy()
+        np.testing.assert_array_equal(m, O.line_source_mask(40, 30, 0.05, 5, j0, j1,
+                                                            dtype=np.float32))
+
+
+@pytest.mark.parametrize("normal,idx,win,ap", [("x", 5, (2, 15, 3, 12), 0), ("y", 6, None, 2),
+                                               ("z", 4, (0, 99, 1, 10), 0)])
+def test_flux_window_matches_oracle(normal, idx, win, ap):
+    from meep_torch_b200.engine3d import flux_window
+    nx, ny, nz = 20, 18, 16
+    s = {k: np.zeros(sh, np.float32) for k, sh in
+         (("Ex", (nx - 1, ny, nz)), ("Ey", (nx, ny - 1, nz)), ("Ez", (nx, ny, nz - 1)),
+          ("Hx", (nx, ny - 1, nz - 1)), ("Hy", (nx - 1, ny, nz - 1)), ("Hz", (nx - 1, ny - 1, nz)))}
+    planes = O.flux3d_planes(s, normal, idx, win, ap)
+    pairs, (l0, h0, l1, h1) = flux_window(normal, idx, nx, ny, nz, win, ap)
+    assert planes[0].shape == (h0 - l0, h1 - l1)
