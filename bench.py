@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FDTD hot path (one JSON line on rank 0).
+
+Workload (default ``cfg2``): 256 batched 2D TE/TM bend variants, grids
+uniform in 256^2..768^2, resolution 20, 1 um CPML, Gaussian line source,
+full-grid DFT of Ez/Hz at 3 frequencies plus 2 flux lines, 5000 time steps.
+One bench step = one whole run of that batch (reset to t = 0, 5000 steps,
+every DFT contribution folded). Metric: Gcell-updates/s = sum(nx*ny) *
+5000 / s over all ranks.
+
+* ``value``: inputs resident in HBM (engine built once, reset per step).
+* ``e2e``: the public API from host buffers: pinned eps maps copied in,
+  coefficients / sources / monitors / states built on the GPU, the run, and
+  the DFT + flux accumulators copied back -- all inside the timed region.
+* ``roofline``: the step kernel (k_yee2d_step), CUDA-event time per launch on
+  the plan's stream over the timed region, against algorithmic bytes per
+  launch (fields + eps + CPML layers; the DFT ring and contraction are
+  reported separately).
+* ``cpu_baseline``: the oracle (numpy restatement of the reference's TM/TE
+  step and monitors) on a bounded sample of the same batch, on the host cores.
+* ``--impl reference``: the same sample through the oracle only (the
+  reference is a Python/torch package that cannot be installed on the GPU
+  box; the oracle is its restatement, pinned against it by the golden tests).
+Multi-GPU (torchrun): every rank advances its own 256-structure batch
+(seed 2 + 1009*rank), no collective in the data path: weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STEPS_PER_RUN = {"cfg2": 5000, "cfg3": 2000, "cfg1": 4000}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}",
+                                       f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines()]
+        except OSError:
+            rows = []
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU sample
+
+def cpu_sample(specs, steps, threads):
+    """Oracle run of `steps` steps on every spec (threads over structures).
+    Returns (cell-updates, seconds)."""
+    import numpy as np
+
+    from meep_torch_b200 import workloads as W
+    from oracle import fdtd as O
+
+    def one(spec):
+        nx, ny, eps = spec["nx"], spec["ny"], spec["eps"]
+        f32 = np.float32
+        prof = O.gaussian_pulse(0.65, 0.2)
+        mask = O.line_source_mask(nx, ny, W.DX2D, spec["src_ix"], *spec["src_j"], dtype=f32)
+        freqs = W.CFG2_FREQS
+        fx, fy = spec["flux_x"], spec["flux_y"]
+        if spec["pol"] == "tm":
+            c = O.tm_coeffs(nx, ny, W.DX2D, eps=eps, npml=W.NPML2D, dtype=f32)
+            dt = c["dt"]
+            mons = [lambda s, t: O.dft_sample(s["Ez"], t, dt, freqs, "Ez", f32),
+                    lambda s, t: O.flux_tm_sample(s, t, dt, freqs, True, *fx, f32),
+                    lambda s, t: O.flux_tm_sample(s, t, dt, freqs, False, *fy, f32)]
+            step, s0 = O.tm_step, O.tm_state(c)
+        else:
+            c = O.te_coeffs(nx, ny, W.DX2D, eps=eps, npml=W.NPML2D, dtype=f32)
+            dt = c["dt"]
+            mask = mask[:, :-1]
+            mons = [lambda s, t: O.dft_sample(s["Hz"], t, dt, freqs, "Hz", f32),
+                    lambda s, t: O.flux_te_sample(s, t, dt, freqs, *fx, f32),
+                    lambda s, t: O.flux_tey_sample(s, t, dt, freqs, *fy, f32)]
+            step, s0 = O.te_step, O.te_state(c)
+        O.run_2d(step, s0, c, steps, amp_fn=lambda t: prof(O.src_time(t, dt)), mask=mask,
+                 monitors=mons)
+        return nx * ny * steps
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        cells = sum(ex.map(one, specs))
+    return cells, time.perf_counter() - t0
+
+
+def cpu_baseline_line(n_struct, steps, threads):
+    from meep_torch_b200 import workloads as W
+    specs = W.cfg2_specs()[:n_struct]
+    cells, sec = cpu_sample(specs, steps, threads)
+    return {"value": cells / sec / 1e9, "unit": "Gcell-updates/s", "cores": threads,
+            "kind": "port",
+            "sample": f"oracle (numpy float32) on cfg2 structures 0..{n_struct - 1} x {steps} "
+                      f"steps, {threads} threads over structures, {sec:.1f} s"}
+
+
+# ------------------------------------------------------------------ GPU bench
+
+def run_cfg2(args, rank, world, dev):
+    import numpy as np
+    import torch
+
+    from meep_torch_b200 import _lib
+    from meep_torch_b200 import workloads as W
+    from meep_torch_b200.engine2d import Engine2D
+
+    lib = _lib.load()
+    nsteps = args.run_steps
+    specs = W.cfg2_specs(n=args.structs, seed=2 + 1009 * rank)
+    cells = sum(s["nx"] * s["ny"] for s in specs)
+    items = [W.cfg2_item(s, dev) for s in specs]
+    eng = Engine2D(items, rows_per_warp=args.rows, ring_slots=args.ring)
+    stream = torch.cuda.current_stream(dev)
+
+    def bench_step():
+        eng.reset()
+        eng.run(0, nsteps)
+
+    for _ in range(args.warmup):
+        bench_step()
+    torch.cuda.synchronize(dev)
+    eng.set_timing(True)
+    barrier(world)
+    n0 = lib.mtb_launch_count()
+    with Clocks(dev.index if dev.index is not None else 0) as clk:
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            bench_step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+    launches = lib.mtb_launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    step_ms, step_n, dft_ms, dft_n = eng.timing()
+    eng.set_timing(False)
+    ms_max = allreduce_max(ms, world, dev)
+    clocks = clk.summary()
+    bytes_launch = W.cfg2_bytes_per_step(specs)
+    res = dict(cells=cells, nsteps=nsteps, ms=ms_max, launches=launches, clocks=clocks,
+               step_ms=step_ms, step_n=step_n, dft_ms=dft_ms, dft_n=dft_n,
+               bytes_launch=bytes_launch, ring_elems=eng.ring_elems)
+    eng.close()
+    del eng, items
+    torch.cuda.empty_cache()
+
+    if args.no_e2e:
+        res.update(e2e_s=float("nan"), h2d=0, d2h=0)
+        return res
+    # ---- e2e: host buffers through the public API
+    host_eps = [torch.from_numpy(s["eps"]).pin_memory() for s in specs]
+    h2d = sum(t.numel() * 4 for t in host_eps)
+    d2h = 0
+
+    def e2e_step():
+        nonlocal d2h
+        dev_eps = [t.to(dev, non_blocking=True) for t in host_eps]
+        its = [W.cfg2_item(s, dev, eps_t=e) for s, e in zip(specs, dev_eps)]
+        e = Engine2D(its, rows_per_warp=args.rows, ring_slots=args.ring)
+        e.run(0, nsteps)
+        outs = []
+        nb = 0
+        for b in range(len(its)):
+            for a in e.accumulators(b):
+                outs.append(a.to("cpu", non_blocking=True))
+                nb += a.numel() * 4
+        torch.cuda.synchronize(dev)
+        e.close()
+        d2h = nb
+        return outs
+
+    e2e_step()                                   # warm
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    e2e_s = allreduce_max(time.perf_counter() - t0, world, dev)
+    barrier(world)
+    res.update(e2e_s=e2e_s, h2d=h2d, d2h=d2h)
+    return res
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, world, dev):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2"])
+    ap.add_argument("--rows", type=int, default=0, help="rows per warp (0 = library default)")
+    ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
+    ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
+    ap.add_argument("--cpu-steps", type=int, default=300)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--structs", type=int, default=256,
+                    help="structures per rank (profiling runs use fewer)")
+    ap.add_argument("--run-steps", type=int, default=5000,
+                    help="time steps per run (profiling runs use fewer)")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    threads = os.cpu_count() or 1
+    if args.cpu_structs <= 0:
+        args.cpu_structs = min(max(8, threads), 64)
+    config = {"workload": "cfg2: 256 batched 2D TE/TM bend variants (256..768)^2, res 20, "
+                          "1 um CPML, Gaussian line source, full-grid DFT 3 freqs + 2 flux "
+                          "lines, 5000 steps per run",
+              "structures_per_rank": args.structs, "time_steps": args.run_steps, "seed": "2 + 1009*rank",
+              "l2": "inputs larger than L2 (~1.1 GB of field state per rank)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        line = {"metric": "Gcell-updates/s", "unit": "Gcell-updates/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "impl": "reference", "dtype": "f32", "data": "synthetic", "config": config}
+        vals = []
+        from meep_torch_b200 import workloads as W
+        specs = W.cfg2_specs()[:args.cpu_structs]
+        for _ in range(args.warmup and 1):
+            cpu_sample(specs[:1], 2, 1)
+        t_all = time.perf_counter()
+        for _ in range(args.steps):
+            cells, sec = cpu_sample(specs, args.cpu_steps, threads)
+            vals.append(cells / sec / 1e9)
+        wall = time.perf_counter() - t_all
+        v = statistics.median(vals)
+        line.update(value=v, ms_per_step=wall / max(args.steps, 1) * 1e3,
+                    cpu_baseline={"value": v, "unit": "Gcell-updates/s", "cores": threads,
+                                  "kind": "port",
+                                  "sample": f"oracle numpy float32 TM/TE step + DFT/flux "
+                                            f"monitors, cfg2 structures 0..{len(specs) - 1} x "
+                                            f"{args.cpu_steps} steps per bench step, {threads} "
+                                            "threads over structures"},
+                    e2e={"value": v, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dev = torch.device("cuda", local)
+    else:
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+    from meep_torch_b200 import build as B
+    if rank == 0:
+        B.build()
+    barrier(world)
+
+    r = run_cfg2(args, rank, world, dev)
+    peak, peak_kind = peaks()
+    total_updates = r["cells"] * r["nsteps"] * args.steps * world
+    value = total_updates / (r["ms"] / 1e3) / 1e9
+    step_avg_ms = r["step_ms"] / max(r["step_n"], 1)
+    achieved = r["bytes_launch"] / (step_avg_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "yee2d_step_cfg2_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    e2e_val = r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
+    line = {
+        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(config, parallelism=f"independent batch per rank x{world}",
+                       cells_per_rank=r["cells"]),
+        "roofline": {"bound": "hbm", "kernel": "k_yee2d_step", "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "alg_bytes_per_launch": r["bytes_launch"],
+                     "launch_ms": step_avg_ms, "launches": r["step_n"],
+                     "dft_contract_ms_total": r["dft_ms"], "dft_contract_launches": r["dft_n"],
+                     "step_kernel_share": r["step_ms"] / max(r["ms"], 1e-9)},
+        "e2e": {"value": e2e_val, "unit": "Gcell-updates/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "clocks": r["clocks"],
+        "gpu_launches": r["launches"],
+    }
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_line(args.cpu_structs, args.cpu_steps, threads)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -196,6 +196,14 @@ int32_t mtb_yee2d_current(const mtb_yee2d_plan *plan);
 /* Number of kernel launches the last mtb_yee2d_run issued. */
 int64_t mtb_yee2d_last_launches(const mtb_yee2d_plan *plan);
 
+/* Opt-in device timing: with enable = 1 every later run records a CUDA
+ * event pair around each step-kernel launch and each DFT-contraction launch
+ * on its stream, and waits for them at its end; mtb_yee2d_timing returns the
+ * summed device milliseconds and launch counts since timing was enabled. */
+int mtb_yee2d_set_timing(mtb_yee2d_plan *plan, int32_t enable);
+int mtb_yee2d_timing(const mtb_yee2d_plan *plan, double *step_ms, int64_t *step_launches,
+                     double *dft_ms, int64_t *dft_launches);
+
 void mtb_yee2d_plan_destroy(mtb_yee2d_plan *plan);
 
 /* ---------------------------------------------------------------- 3D */
@@ -245,6 +253,9 @@ int mtb_yee3d_run(mtb_yee3d_plan *plan, int64_t t0, int32_t k,
                   const double *coef, void *stream);
 int32_t mtb_yee3d_current(const mtb_yee3d_plan *plan);
 int64_t mtb_yee3d_last_launches(const mtb_yee3d_plan *plan);
+int mtb_yee3d_set_timing(mtb_yee3d_plan *plan, int32_t enable);
+int mtb_yee3d_timing(const mtb_yee3d_plan *plan, double *step_ms, int64_t *step_launches,
+                     double *dft_ms, int64_t *dft_launches);
 void mtb_yee3d_plan_destroy(mtb_yee3d_plan *plan);
 
 /* ------------------------------------------------------------ layout */

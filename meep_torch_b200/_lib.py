@@ -85,6 +85,9 @@ SIGNATURES = {
     "mtb_yee2d_current": (C.c_int32, [vp]),
     "mtb_yee2d_last_launches": (C.c_int64, [vp]),
     "mtb_yee2d_plan_destroy": (None, [vp]),
+    "mtb_yee2d_set_timing": (C.c_int, [vp, C.c_int32]),
+    "mtb_yee2d_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "mtb_yee3d_plan_create": (C.c_int, [C.POINTER(Yee3DStruct), C.POINTER(DftRegion), C.c_int32,
                                         C.POINTER(PhaseGroup), C.c_int32, C.c_int64,
                                         C.POINTER(Tuning), C.POINTER(vp)]),
@@ -92,6 +95,9 @@ SIGNATURES = {
     "mtb_yee3d_current": (C.c_int32, [vp]),
     "mtb_yee3d_last_launches": (C.c_int64, [vp]),
     "mtb_yee3d_plan_destroy": (None, [vp]),
+    "mtb_yee3d_set_timing": (C.c_int, [vp, C.c_int32]),
+    "mtb_yee3d_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "mtb_pack": (C.c_int, [vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, vp,
                            C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
                            C.c_int64, C.c_int64, vp]),

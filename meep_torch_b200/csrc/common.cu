@@ -31,6 +31,47 @@ int fail(int code, const char *fmt, ...) {
 
 void count_launch(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// ------------------------------------------------------------ launch timer
+
+int LaunchTimer::begin(cudaStream_t st, int k) {
+    if (!on) return MTB_OK;
+    while (pool.size() < used + 2) {
+        cudaEvent_t e;
+        MTB_CUDA_TRY(cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    kind.resize(pool.size() / 2 + 1);
+    kind[used / 2] = k;
+    MTB_CUDA_TRY(cudaEventRecord(pool[used], st));
+    return MTB_OK;
+}
+
+int LaunchTimer::end(cudaStream_t st) {
+    if (!on) return MTB_OK;
+    MTB_CUDA_TRY(cudaEventRecord(pool[used + 1], st));
+    used += 2;
+    return MTB_OK;
+}
+
+int LaunchTimer::collect() {
+    if (!on || used == 0) return MTB_OK;
+    MTB_CUDA_TRY(cudaEventSynchronize(pool[used - 1]));
+    for (size_t i = 0; i < used; i += 2) {
+        float t = 0.f;
+        MTB_CUDA_TRY(cudaEventElapsedTime(&t, pool[i], pool[i + 1]));
+        ms[kind[i / 2]] += t;
+        count[kind[i / 2]] += 1;
+    }
+    used = 0;
+    return MTB_OK;
+}
+
+void LaunchTimer::release() {
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+    used = 0;
+}
+
 // ------------------------------------------------------------ layout kernels
 
 // Writes the whole box: the block [off, off+n) gets src, the rest zero.
@@ -280,7 +321,7 @@ int DftState::upload_phases(int64_t t0, int k, cudaStream_t st) {
     return MTB_OK;
 }
 
-int DftState::contract(int row0, int n, cudaStream_t st) {
+int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm) {
     if (n_regions == 0 || n <= 0 || n_blocks == 0) return MTB_OK;
     int maxnf = 1;
     for (int g = 0; g < n_groups; ++g) maxnf = std::max(maxnf, group_nf[g]);
@@ -294,11 +335,14 @@ int DftState::contract(int row0, int n, cudaStream_t st) {
     }
     const int *gd = reinterpret_cast<const int *>(blk_start_d.as<int64_t>() + (n_regions + 1));
     if (n_blocks > 0x7fffffffLL) return fail(MTB_INVALID_ARG, "too many contraction blocks");
+    int rc;
+    if (tm && (rc = tm->begin(st, 1))) return rc;
     k_dft_contract<<<(unsigned)n_blocks, CT, smem, st>>>(
         regions_d.as<mtb_dft_region>(), blk_start_d.as<int64_t>(), n_regions, gd,
         gd + (n_groups + 1), total_nf, phase_d.as<float>(), row0, n, ring_d.as<float>(),
         slot_elems);
     MTB_CHECK_LAUNCH();
+    if (tm && (rc = tm->end(st))) return rc;
     return MTB_OK;
 }
 

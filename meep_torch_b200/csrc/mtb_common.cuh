@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/meep_b200.h"
 
@@ -84,6 +85,20 @@ struct HostBuf {
     template <class T> T *as() const { return reinterpret_cast<T *>(p); }
 };
 
+// Opt-in per-launch device timing (event pairs around launches).
+struct LaunchTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<int> kind;          // 0 = step kernel, 1 = DFT contraction
+    double ms[2] = {0, 0};
+    int64_t count[2] = {0, 0};
+    int begin(cudaStream_t st, int k);   // record the start event of a launch
+    int end(cudaStream_t st);            // record the end event
+    int collect();                       // wait and sum; resets the pool cursor
+    void release();
+};
+
 // ---------------------------------------------------------------- DFT
 // Phase tables and the ring contraction shared by the 2D and 3D plans.
 struct DftState {
@@ -111,7 +126,7 @@ struct DftState {
     int upload_phases(int64_t t0, int k, cudaStream_t st);
     // Fold ring slots [0, n) (steps t_first .. t_first+n-1, relative row
     // `row0` of the uploaded table) into the accumulators.
-    int contract(int row0, int n, cudaStream_t st);
+    int contract(int row0, int n, cudaStream_t st, LaunchTimer *tm = nullptr);
     void release();
 };
 

@@ -548,6 +548,7 @@ struct mtb_yee2d_plan {
     int first = 1;
     int64_t last_launches = 0;
     DftState dft;
+    LaunchTimer timer;
 };
 
 static int check_ptr(const void *p, const char *what, int s) {
@@ -698,21 +699,41 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
         C.ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;
         C.par = p->par;
         C.first = p->first;
+        if ((rc = p->timer.begin(st, 0))) return rc;
         k_yee2d_step<<<blocks, 32 * WARPS2D, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
                                                       p->work_d.as<int4>(), p->n_work, C);
         MTB_CHECK_LAUNCH();
+        if ((rc = p->timer.end(st))) return rc;
         ++p->last_launches;
         p->par ^= 1;
         p->first = 0;
         ++slot;
         if (slot == p->dft.slots || s == k - 1) {
             if (p->dft.n_regions > 0) {
-                if ((rc = p->dft.contract(s + 1 - slot, slot, st))) return rc;
+                if ((rc = p->dft.contract(s + 1 - slot, slot, st, &p->timer))) return rc;
                 ++p->last_launches;
             }
             slot = 0;
         }
     }
+    return p->timer.collect();
+}
+
+int mtb_yee2d_set_timing(mtb_yee2d_plan *p, int32_t enable) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    p->timer.on = enable != 0;
+    p->timer.ms[0] = p->timer.ms[1] = 0;
+    p->timer.count[0] = p->timer.count[1] = 0;
+    return MTB_OK;
+}
+
+int mtb_yee2d_timing(const mtb_yee2d_plan *p, double *step_ms, int64_t *step_launches,
+                     double *dft_ms, int64_t *dft_launches) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (step_ms) *step_ms = p->timer.ms[0];
+    if (step_launches) *step_launches = p->timer.count[0];
+    if (dft_ms) *dft_ms = p->timer.ms[1];
+    if (dft_launches) *dft_launches = p->timer.count[1];
     return MTB_OK;
 }
 
@@ -727,6 +748,7 @@ void mtb_yee2d_plan_destroy(mtb_yee2d_plan *p) {
     p->amp_d.release();
     p->amp_h.release();
     p->dft.release();
+    p->timer.release();
     delete p;
 }
 

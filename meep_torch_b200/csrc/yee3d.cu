@@ -443,6 +443,7 @@ struct mtb_yee3d_plan {
     size_t smem = 0;
     int64_t last_launches = 0;
     DftState dft;
+    LaunchTimer timer;
 };
 
 template <int NZW>
@@ -580,6 +581,7 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
         Ctx3D C;
         C.amp = p->amp_d.as<float>() + s;
         C.par = p->par;
+        if ((rc = p->timer.begin(st, 0))) return rc;
         switch (p->nzw) {
             case 1: rc = launch3d<1>(p, C, st); break;
             case 2: rc = launch3d<2>(p, C, st); break;
@@ -587,6 +589,7 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
             default: rc = launch3d<4>(p, C, st); break;
         }
         if (rc) return rc;
+        if ((rc = p->timer.end(st))) return rc;
         ++p->last_launches;
         p->par ^= 1;
         if (sampling) {
@@ -601,12 +604,30 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
         ++slot;
         if (slot == p->dft.slots || s == k - 1) {
             if (sampling) {
-                if ((rc = p->dft.contract(s + 1 - slot, slot, st))) return rc;
+                if ((rc = p->dft.contract(s + 1 - slot, slot, st, &p->timer))) return rc;
                 ++p->last_launches;
             }
             slot = 0;
         }
     }
+    return p->timer.collect();
+}
+
+int mtb_yee3d_set_timing(mtb_yee3d_plan *p, int32_t enable) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    p->timer.on = enable != 0;
+    p->timer.ms[0] = p->timer.ms[1] = 0;
+    p->timer.count[0] = p->timer.count[1] = 0;
+    return MTB_OK;
+}
+
+int mtb_yee3d_timing(const mtb_yee3d_plan *p, double *step_ms, int64_t *step_launches,
+                     double *dft_ms, int64_t *dft_launches) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (step_ms) *step_ms = p->timer.ms[0];
+    if (step_launches) *step_launches = p->timer.count[0];
+    if (dft_ms) *dft_ms = p->timer.ms[1];
+    if (dft_launches) *dft_launches = p->timer.count[1];
     return MTB_OK;
 }
 
@@ -621,6 +642,7 @@ void mtb_yee3d_plan_destroy(mtb_yee3d_plan *p) {
     p->amp_d.release();
     p->amp_h.release();
     p->dft.release();
+    p->timer.release();
     delete p;
 }
 

@@ -492,6 +492,27 @@ class Engine2D:
         L.check(self.lib.mtb_yee2d_run(self.plan, t0, k, pe, ph, self._sptr()), "mtb_yee2d_run")
         self.last_launches = self.lib.mtb_yee2d_last_launches(self.plan)
 
+    def reset(self):
+        """Zero every field, CPML and accumulator buffer (both ping-pong halves)
+        with the library's own fill kernel -- a fresh t = 0 run of the same batch."""
+        for it in self.items:
+            bufs = [*it.box["main"], *it.box["x"], *it.box["y"]] + \
+                [t for p in it.box["psi"] for t in p] + list(it.accs)
+            for t in bufs:
+                n = t.numel()
+                L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
+                                          self._sptr()), "reset")
+
+    def set_timing(self, on: bool = True):
+        L.check(self.lib.mtb_yee2d_set_timing(self.plan, 1 if on else 0), "set_timing")
+
+    def timing(self):
+        """(step_ms, step_launches, dft_ms, dft_launches) since set_timing(True)."""
+        a, b, c, d = C.c_double(), C.c_int64(), C.c_double(), C.c_int64()
+        L.check(self.lib.mtb_yee2d_timing(self.plan, C.byref(a), C.byref(b), C.byref(c),
+                                          C.byref(d)), "timing")
+        return a.value, b.value, c.value, d.value
+
     @property
     def current(self) -> int:
         return self.lib.mtb_yee2d_current(self.plan)

@@ -305,6 +305,23 @@ class Engine3D:
         L.check(self.lib.mtb_yee3d_run(self.plan, t0, k, coef, self._sptr()), "mtb_yee3d_run")
         self.last_launches = self.lib.mtb_yee3d_last_launches(self.plan)
 
+    def reset(self):
+        """Zero every field, CPML and accumulator buffer (t = 0 again)."""
+        bufs = [t for p in self.box.values() for t in p] + list(self.accs)
+        for t in bufs:
+            n = t.numel()
+            L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
+                                      self._sptr()), "reset")
+
+    def set_timing(self, on: bool = True):
+        L.check(self.lib.mtb_yee3d_set_timing(self.plan, 1 if on else 0), "set_timing")
+
+    def timing(self):
+        a, b, c, d = C.c_double(), C.c_int64(), C.c_double(), C.c_int64()
+        L.check(self.lib.mtb_yee3d_timing(self.plan, C.byref(a), C.byref(b), C.byref(c),
+                                          C.byref(d)), "timing")
+        return a.value, b.value, c.value, d.value
+
     @property
     def current(self):
         return self.lib.mtb_yee3d_current(self.plan)
