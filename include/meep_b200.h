@@ -82,6 +82,8 @@ typedef struct mtb_cells {
     const float *w;         /* n entries, device                           */
     int32_t n;              /* number of cells                             */
     int32_t amp_col;        /* amplitude-table column this list reads      */
+    int32_t row_lo, row_hi; /* first / last row holding cells; the plan
+                               fills these (caller values are ignored)     */
 } mtb_cells;
 
 /* One raw line of field values copied into the sample ring each step:
@@ -116,8 +118,9 @@ typedef struct mtb_yee2d_struct {
     float *f_main[2];       /* TM Dz | TE Hz                                */
     float *f_x[2];          /* TM Hx | TE Dx                                */
     float *f_y[2];          /* TM Hy | TE Dy                                */
-    const float *eps_a;     /* TM eps_inf | TE eps_x                        */
-    const float *eps_b;     /* TM unused  | TE eps_y                        */
+    const float *inv_eps_a; /* 1/eps: TM 1/eps_inf | TE 1/eps_x (E = D/eps
+                               is evaluated as D * (1/eps))                 */
+    const float *inv_eps_b; /* TM unused  | TE 1/eps_y                      */
     const float *e_explicit;/* TM: Ez box array when explicit_e             */
     /* CPML memory, box layout at the position of the field it feeds:
      * TM: [0] psi_Ezy (Hx), [1] psi_Ezx (Hy), [2] psi_Hyx (Dz), [3] psi_Hxy (Dz)
@@ -131,6 +134,10 @@ typedef struct mtb_yee2d_struct {
     mtb_cells src_h2;       /* TM -> Hx rows | TE unused                    */
     const mtb_line_sample *lines; /* device array of line samples          */
     int32_t n_lines;
+    int32_t xband[4];       /* plan-filled (caller values ignored): the hx
+                               profile is active on rows r < xband[0] or
+                               r >= xband[1], the ex profile on rows
+                               r < xband[2] or r >= xband[3]              */
     int32_t pad_;
     int64_t ring_full[3];   /* full-grid sample of comp c to ring offset, -1 = off */
 } mtb_yee2d_struct;
@@ -192,6 +199,11 @@ int mtb_yee2d_run(mtb_yee2d_plan *plan, int64_t t0, int32_t k,
 
 /* Which buffer of every ping-pong pair holds the current state (0 or 1). */
 int32_t mtb_yee2d_current(const mtb_yee2d_plan *plan);
+
+/* Waits for the plan's work on `stream` and reports a bounded device wait
+ * that expired in any earlier run (MTB_DEVICE_TIMEOUT) -- the kernels never
+ * spin forever; a wait that gives up sets this flag and the step returns. */
+int mtb_yee2d_check(mtb_yee2d_plan *plan, void *stream);
 
 /* Number of kernel launches the last mtb_yee2d_run issued. */
 int64_t mtb_yee2d_last_launches(const mtb_yee2d_plan *plan);

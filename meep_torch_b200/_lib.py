@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libmeep_b200.so")
+# MEEP_B200_LIB selects another build of the same library (tuning variants)
+LIB_PATH = os.environ.get("MEEP_B200_LIB") or os.path.join(HERE, "lib", "libmeep_b200.so")
 
 MTB_OK, MTB_INVALID_ARG, MTB_UNSUPPORTED, MTB_DEVICE_TIMEOUT, MTB_CUDA_ERROR = 0, 1, 2, 3, 4
 MTB_TM, MTB_TE = 0, 1
@@ -22,7 +23,8 @@ vp = C.c_void_p
 
 
 class Cells(C.Structure):
-    _fields_ = [("row_ptr", vp), ("col", vp), ("w", vp), ("n", C.c_int32), ("amp_col", C.c_int32)]
+    _fields_ = [("row_ptr", vp), ("col", vp), ("w", vp), ("n", C.c_int32), ("amp_col", C.c_int32),
+                ("row_lo", C.c_int32), ("row_hi", C.c_int32)]
 
 
 class LineSample(C.Structure):
@@ -36,13 +38,13 @@ class Yee2DStruct(C.Structure):
                 ("y_pmc", C.c_int32), ("explicit_e", C.c_int32),
                 ("dt", C.c_float), ("dx", C.c_float),
                 ("f_main", vp * 2), ("f_x", vp * 2), ("f_y", vp * 2),
-                ("eps_a", vp), ("eps_b", vp), ("e_explicit", vp),
+                ("inv_eps_a", vp), ("inv_eps_b", vp), ("e_explicit", vp),
                 ("psi", (vp * 2) * 4),
                 ("hx_b", vp), ("hx_a", vp), ("hy_b", vp), ("hy_a", vp),
                 ("ex_b", vp), ("ex_a", vp), ("ey_b", vp), ("ey_a", vp),
                 ("src_e", Cells), ("src_h1", Cells), ("src_h2", Cells),
-                ("lines", vp), ("n_lines", C.c_int32), ("pad_", C.c_int32),
-                ("ring_full", C.c_int64 * 3)]
+                ("lines", vp), ("n_lines", C.c_int32), ("xband", C.c_int32 * 4),
+                ("pad_", C.c_int32), ("ring_full", C.c_int64 * 3)]
 
 
 class PhaseGroup(C.Structure):
@@ -83,6 +85,7 @@ SIGNATURES = {
     "mtb_yee2d_run": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double),
                                 C.POINTER(C.c_double), vp]),
     "mtb_yee2d_current": (C.c_int32, [vp]),
+    "mtb_yee2d_check": (C.c_int, [vp, vp]),
     "mtb_yee2d_last_launches": (C.c_int64, [vp]),
     "mtb_yee2d_plan_destroy": (None, [vp]),
     "mtb_yee2d_set_timing": (C.c_int, [vp, C.c_int32]),

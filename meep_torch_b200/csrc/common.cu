@@ -150,22 +150,20 @@ static int grid_for(int64_t total, int threads = 256) {
 constexpr int KMAX = 64;       // deepest ring supported by the contraction
 constexpr int CT = 256;        // channels per contraction block
 
-// One block folds CT channels of one region. Phase values for the region's
-// (group, toff) are staged in shared memory: sP[s * nf + f] = (Re, Im).
+// One block folds CT channels of one region (region of the block from a
+// per-block table). Phase values of the region's (group, toff) are staged
+// in shared memory, sP[s * nf + f] = (Re, Im); each thread keeps NFC
+// frequencies of its channel in registers and streams its n ring samples.
+constexpr int NFC = 4;
 __global__ void __launch_bounds__(CT) k_dft_contract(
-    const mtb_dft_region *__restrict__ regions, const int64_t *__restrict__ blk_start,
-    int n_regions, const int *__restrict__ group_nf, const int *__restrict__ group_off,
-    int total_nf, const float *__restrict__ phase, int row0, int n,
-    const float *__restrict__ ring, int64_t slot_elems) {
+    const mtb_dft_region *__restrict__ regions, const int *__restrict__ blk_region,
+    const int64_t *__restrict__ blk_start, const int *__restrict__ group_nf,
+    const int *__restrict__ group_off, int total_nf, const float *__restrict__ phase, int row0,
+    int n, const float *__restrict__ ring, int64_t slot_elems) {
     extern __shared__ float2 sP[];
-    // region of this block (binary search over the block prefix)
     const int64_t b = blockIdx.x;
-    int lo = 0, hi = n_regions - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (blk_start[mid] <= b) lo = mid; else hi = mid - 1;
-    }
-    const mtb_dft_region R = regions[lo];
+    const int rg = blk_region[b];
+    const mtb_dft_region R = regions[rg];
     const int nf = group_nf[R.group];
     const int foff = group_off[R.group];
     const int sel = (R.toff == 2) ? 2 : 0;
@@ -175,40 +173,46 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
         sP[e] = make_float2(p[0], p[1]);
     }
     __syncthreads();
-    const int64_t ch = (b - blk_start[lo]) * CT + threadIdx.x;
+    const int64_t ch = (b - blk_start[rg]) * CT + threadIdx.x;
     const int64_t nch = (int64_t)R.rows * R.cols;
     if (ch >= nch) return;
     const int r = (int)(ch / R.cols), c = (int)(ch - (int64_t)r * R.cols);
-    const int64_t ia = R.ring_a + (int64_t)r * R.ring_pitch + c;
-    float x[KMAX];
-#pragma unroll
-    for (int s = 0; s < KMAX; ++s) {
-        float v = 0.f;
-        if (s < n) {
-            v = ring[s * slot_elems + ia];
-            if (R.ring_b >= 0) {
-                const float w = ring[s * slot_elems + R.ring_b + (int64_t)r * R.ring_pitch + c];
-                v = 0.5f * (v + w);
-            }
-        }
-        x[s] = v;
-    }
+    const float *xa = ring + R.ring_a + (int64_t)r * R.ring_pitch + c;
+    const float *xb = (R.ring_b >= 0) ? ring + R.ring_b + (int64_t)r * R.ring_pitch + c : nullptr;
     float *acc = R.acc;
     const int64_t base = (int64_t)r * R.acc_pitch + c;
-    for (int f = 0; f < nf; ++f) {
-        float re = 0.f, im = 0.f;
+    for (int f0 = 0; f0 < nf; f0 += NFC) {
+        float *pr[NFC], *pi[NFC];
+        float re[NFC], im[NFC];
 #pragma unroll
-        for (int s = 0; s < KMAX; ++s) {
-            if (s < n) {
-                const float2 p = sP[s * nf + f];
-                re = fmaf(p.x, x[s], re);
-                im = fmaf(p.y, x[s], im);
+        for (int q = 0; q < NFC; ++q) {
+            const int f = min(f0 + q, nf - 1);
+            pr[q] = acc + R.re_off + f * R.f_stride + base;
+            pi[q] = acc + R.im_off + f * R.f_stride + base;
+            re[q] = 0.f;
+            im[q] = 0.f;
+        }
+#pragma unroll 4
+        for (int s = 0; s < n; ++s) {
+            float x = xa[s * slot_elems];
+            if (xb) x = 0.5f * (x + xb[s * slot_elems]);
+            const float2 *ps = sP + s * nf + f0;
+#pragma unroll
+            for (int q = 0; q < NFC; ++q) {
+                if (f0 + q < nf) {
+                    const float2 p = ps[q];
+                    re[q] = fmaf(p.x, x, re[q]);
+                    im[q] = fmaf(p.y, x, im[q]);
+                }
             }
         }
-        float *pr = acc + R.re_off + f * R.f_stride + base;
-        float *pi = acc + R.im_off + f * R.f_stride + base;
-        *pr += re;
-        *pi += im;
+#pragma unroll
+        for (int q = 0; q < NFC; ++q) {
+            if (f0 + q < nf) {
+                *pr[q] += re[q];
+                *pi[q] += im[q];
+            }
+        }
     }
 }
 
@@ -264,7 +268,14 @@ int DftState::init(const mtb_dft_region *regions, int nreg, const mtb_phase_grou
     }
     bs[nreg] = nb;
     n_blocks = nb;
+    if (nb > 0x7fffffffLL) return fail(MTB_INVALID_ARG, "too many DFT channels");
+    std::vector<int> br((size_t)nb + 1, 0);
+    for (int r = 0; r < nreg; ++r)
+        for (int64_t q = bs[r]; q < bs[r + 1]; ++q) br[q] = r;
     int rc;
+    if ((rc = blk_region_d.ensure(sizeof(int) * (br.size())))) return rc;
+    MTB_CUDA_TRY(cudaMemcpy(blk_region_d.p, br.data(), sizeof(int) * br.size(),
+                            cudaMemcpyHostToDevice));
     if ((rc = regions_d.ensure(sizeof(mtb_dft_region) * (nreg + 1)))) return rc;
     if ((rc = blk_start_d.ensure(sizeof(int64_t) * (nreg + 1) + 2 * sizeof(int) * (ngrp + 1))))
         return rc;
@@ -338,7 +349,7 @@ int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm) {
     int rc;
     if (tm && (rc = tm->begin(st, 1))) return rc;
     k_dft_contract<<<(unsigned)n_blocks, CT, smem, st>>>(
-        regions_d.as<mtb_dft_region>(), blk_start_d.as<int64_t>(), n_regions, gd,
+        regions_d.as<mtb_dft_region>(), blk_region_d.as<int>(), blk_start_d.as<int64_t>(), gd,
         gd + (n_groups + 1), total_nf, phase_d.as<float>(), row0, n, ring_d.as<float>(),
         slot_elems);
     MTB_CHECK_LAUNCH();
@@ -349,6 +360,7 @@ int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm) {
 void DftState::release() {
     regions_d.release();
     blk_start_d.release();
+    blk_region_d.release();
     phase_d.release();
     ring_d.release();
     phase_h.release();

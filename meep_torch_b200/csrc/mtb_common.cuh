@@ -113,7 +113,7 @@ struct DftState {
     int *freq_off = nullptr;               // per group offset into freqs_h
     int total_nf = 0;                      // sum of nf
     // device
-    DevBuf regions_d, blk_start_d, phase_d, ring_d;
+    DevBuf regions_d, blk_start_d, blk_region_d, phase_d, ring_d;
     HostBuf phase_h;
     int64_t slot_elems = 0;
     int slots = 0;                         // ring depth K

@@ -1,20 +1,28 @@
 // Batched 2D Yee step (TM and TE) for sm_100a.
 //
 // One warp marches down rows i0..i1-1 of a 128-column strip of one
-// structure: lane L owns columns c0+4L .. c0+4L+3 (one float4 per array and
-// row). Each iteration fuses the reference's whole step for one row:
+// structure: lane L owns columns c0+4L .. c0+4L+3. Each iteration fuses the
+// reference's whole step for one row:
 //   TM (core/stepper_tm.py:234-254): H(n+1/2) of row i from Ez(n) of rows
 //      i, i+1 -> magnetic sheet source -> Dz(n+1) of row i from H rows
 //      i-1, i -> electric source -> Ez = Dz / eps.
 //   TE (core/stepper_te.py:178-190): D/E(n+1/2) of row i+1 from Hz(n) rows
 //      i, i+1 -> source into Dy -> E = D / eps -> Hz(n+1) of row i.
-// Ez (TM) and Ex/Ey (TE) are not stored: they are D / eps, recomputed where
-// needed, so the per-cell traffic is read+write of the three stored fields
-// plus one (TM) or two (TE) eps reads. Halo values (the row above the strip,
-// the columns left/right of it) are recomputed from the neighbours' old
-// values, which is why every evolving array is a ping-pong pair.
-// CPML memory is only touched where its profile is active (a != 0 or
-// b != 1); outside the layers it is identically zero, as in the reference.
+// Ez (TM) and Ex/Ey (TE) are not stored: they are D * (1/eps), recomputed
+// where needed, so the per-cell traffic is read+write of the three stored
+// fields plus one (TM) or two (TE) 1/eps reads.
+//
+// Input rows are staged in shared memory by a per-warp pipeline of bulk
+// copies (cp.async.bulk, completion counted on one mbarrier per stage):
+// NST stages, each holding one row of every input array over the column
+// window c0-4 .. c0+131 (the strip plus the 4-aligned halo the stencil needs),
+// issued NST-1 rows ahead of use. Waits are bounded by %globaltimer; a wait
+// that expires raises the plan's error flag and the warp stops.
+// Halo values (the row above the strip, the columns left/right of it) are
+// recomputed from the neighbours' old values, which is why every evolving
+// array is a ping-pong pair. CPML memory is only touched where its profile is
+// active (a != 0 or b != 1); outside the layers it is identically zero, as in
+// the reference.
 #include <algorithm>
 #include <vector>
 
@@ -24,21 +32,63 @@ namespace mtb {
 
 constexpr int MAXL = 16;          // line samples per structure
 constexpr int WARPS2D = 4;        // warps per block
+constexpr int NST = 4;            // pipeline stages per warp
+constexpr int EXT = 136;          // staged row: columns c0-4 .. c0+131
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // bounded wait: 2 s
 
 struct Ctx2D {
     const float *amp_e;           // coefficient row of this step [n_cols]
     const float *amp_h;
     float *ring;                  // ring slot of this step
+    int *err;                     // device error flag (1 = a bounded wait expired)
     int par;                      // buffer holding the old state
     int first;                    // first step executed by the plan
 };
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(float *dst, const float *src, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ void ld4(const float *p, float (&v)[4]) {
     const float4 x = *reinterpret_cast<const float4 *>(p);
     v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
 }
-__device__ __forceinline__ void ldg4(const float *p, float (&v)[4]) {
-    const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
+__device__ __forceinline__ void lds4(const float *p, float (&v)[4]) {   // shared memory
+    const float4 x = *reinterpret_cast<const float4 *>(p);
     v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
 }
 __device__ __forceinline__ void st4(float *p, const float (&v)[4]) {
@@ -49,10 +99,68 @@ __device__ __forceinline__ void copy4(float (&d)[4], const float (&s)[4]) {
     d[0] = s[0]; d[1] = s[1]; d[2] = s[2]; d[3] = s[3];
 }
 
+// ---------------------------------------------------------------- row pipeline
+// Rows r = i0-1+k (k = 0 .. nrows-1) go through stage k % NST. Rows outside
+// [0, nx) get an arrive without a copy so every stage's phase parity stays
+// k / NST; their shared data is never read.
+template <int NA>
+struct Pipe {
+    float *buf;                   // NST * NA * EXT floats (this warp's)
+    uint64_t *bar;                // NST mbarriers
+    const float *const *src;      // base of each staged global array (shared memory)
+    int64_t P;                    // row pitch
+    int w0;                       // first staged global column
+    int dst;                      // float offset of w0 inside a staged row
+    uint32_t bytes;               // bytes per staged row copy
+    int i0m1, nx, nrows;
+    int lane;
+    static constexpr int STG = NA * EXT;
+
+    // lane 0 arms the stage's barrier, lanes 0..NA-1 each issue one array's copy
+    __device__ void issue(int k) const {
+        if (k >= nrows) return;
+        const int r = i0m1 + k;
+        uint64_t *b = bar + (k % NST);
+        if (r < 0 || r >= nx) {
+            if (lane == 0) mbar_arrive(b);
+            return;
+        }
+        if (lane == 0) mbar_expect_tx(b, bytes * NA);
+        if (lane < NA)
+            bulk_g2s(buf + (k % NST) * STG + lane * EXT + dst, src[lane] + r * P + w0, bytes, b);
+    }
+    // true when stage k is ready; false (error flag raised) when the bounded
+    // wait expired
+    __device__ bool wait(int k, int *err) const {
+        uint64_t *b = bar + (k % NST);
+        const uint32_t par = (k / NST) & 1;
+        if (mbar_try_wait(b, par)) return true;
+        const unsigned long long t0 = gtimer();
+        while (!mbar_try_wait(b, par)) {
+            if (gtimer() - t0 > WAIT_NS) {
+                if (lane == 0) atomicExch(err, 1);
+                return false;
+            }
+        }
+        return true;
+    }
+    // after an expired wait: let this warp's copies in flight land (bounded)
+    __device__ void drain(int k_from, int k_to) const {
+        for (int k = k_from; k < k_to && k < nrows; ++k) {
+            uint64_t *b = bar + (k % NST);
+            const uint32_t par = (k / NST) & 1;
+            const unsigned long long t0 = gtimer();
+            while (!mbar_try_wait(b, par) && gtimer() - t0 < WAIT_NS) {
+            }
+        }
+    }
+    __device__ const float *row(int k, int a) const { return buf + (k % NST) * STG + a * EXT; }
+};
+
 // F[row, jb+q] -= amp * w for the cells of `row` in `cl` (CSR by row).
 __device__ __forceinline__ void apply_cells(const mtb_cells &cl, int row, const float *amp,
                                             int jb, float (&v)[4]) {
-    if (cl.n == 0) return;
+    if (cl.n == 0 || row < cl.row_lo || row > cl.row_hi) return;
     const int e0 = __ldg(cl.row_ptr + row), e1 = __ldg(cl.row_ptr + row + 1);
     if (e0 == e1) return;
     const float a = __ldg(amp + cl.amp_col);
@@ -64,10 +172,9 @@ __device__ __forceinline__ void apply_cells(const mtb_cells &cl, int row, const 
             if (c == q) v[q] -= a * w;
     }
 }
-// scalar variant for a halo cell (row, col)
 __device__ __forceinline__ float apply_cell1(const mtb_cells &cl, int row, int col,
                                              const float *amp, float v) {
-    if (cl.n == 0) return v;
+    if (cl.n == 0 || row < cl.row_lo || row > cl.row_hi) return v;
     const int e0 = __ldg(cl.row_ptr + row), e1 = __ldg(cl.row_ptr + row + 1);
     if (e0 == e1) return v;
     const float a = __ldg(amp + cl.amp_col);
@@ -76,7 +183,7 @@ __device__ __forceinline__ float apply_cell1(const mtb_cells &cl, int row, int c
     return v;
 }
 
-// Copy this row's values of component `comp` into the line samples.
+// Copy this row's values of component `comp` into the (pre-filtered) line samples.
 __device__ __forceinline__ void sample_row(const mtb_line_sample *L, int nl, int comp, int i,
                                            int jb, bool act, const float (&v)[4], float *ring) {
     if (!act) return;
@@ -101,11 +208,17 @@ __device__ __forceinline__ void sample_row(const mtb_line_sample *L, int nl, int
 }
 
 // ------------------------------------------------------------------ TM
+// Column validity is folded into per-lane step coefficients (dt/dx times a
+// 0/1 mask): a masked cell is left unchanged and box padding (where 1/eps is
+// 0) stays zero, so the row body carries no per-element predicates. CPML
+// memory is touched only on x-layer rows (row-uniform branch) and in y-layer
+// lanes (bit masks, bit q = column jb+q), where the profiles are read from L1.
+#define BIT(m, q) (((m) >> (q)) & 1u)
 
 template <bool EXPL>
 __device__ __forceinline__ void tm_warp(const mtb_yee2d_struct &S, const int i0, const int i1,
-                                        const int c0, const Ctx2D &C,
-                                        const mtb_line_sample *L, const int nl) {
+                                        const int c0, const Ctx2D &C, const mtb_line_sample *L,
+                                        const int nl, Pipe<4> pp) {
     const int lane = threadIdx.x & 31;
     const int nx = S.nx, ny = S.ny;
     const int64_t P = S.pitch;
@@ -113,189 +226,213 @@ __device__ __forceinline__ void tm_warp(const mtb_yee2d_struct &S, const int i0,
     const bool act = jb < S.pitch;
     const float dt = S.dt;
     const float rdx = 1.0f / S.dx;
+    const float kdt = dt * rdx;
     const int par = C.par;
-    const float *__restrict__ Dz = S.f_main[par];
     float *__restrict__ Dzn = S.f_main[par ^ 1];
-    const float *__restrict__ Hx = S.f_x[par];
     float *__restrict__ Hxn = S.f_x[par ^ 1];
-    const float *__restrict__ Hy = S.f_y[par];
     float *__restrict__ Hyn = S.f_y[par ^ 1];
-    const float *__restrict__ eps = S.eps_a;
-    const float *__restrict__ Eex = S.e_explicit;
-    const float *__restrict__ pEzy = S.psi[0][par];
-    float *__restrict__ pEzyN = S.psi[0][par ^ 1];
-    const float *__restrict__ pEzx = S.psi[1][par];
-    float *__restrict__ pEzxN = S.psi[1][par ^ 1];
-    const float *__restrict__ pHyx = S.psi[2][par];
-    float *__restrict__ pHyxN = S.psi[2][par ^ 1];
-    const float *__restrict__ pHxy = S.psi[3][par];
-    float *__restrict__ pHxyN = S.psi[3][par ^ 1];
-    const bool pmc = S.y_pmc != 0;
     float *ring = C.ring;
+    const int64_t rf0 = S.ring_full[0], rf1 = S.ring_full[1], rf2 = S.ring_full[2];
+    const int xb0 = S.xband[0], xb1 = S.xband[1], xe0 = S.xband[2], xe1 = S.xband[3];
+    const int selo = S.src_e.row_lo, sehi = S.src_e.row_hi;
+    const int h1lo = S.src_h1.row_lo, h1hi = S.src_h1.row_hi;
+    const int h2lo = S.src_h2.row_lo, h2hi = S.src_h2.row_hi;
 
-    // lane-constant column data
-    bool vC[4], vHx[4], vDz[4], hyA[4], eyA[4];
-    float hyb[4], hya[4], eyb[4], eya[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = jb + q;
-        vC[q] = j < ny;
-        vHx[q] = j <= ny - 2;
-        vDz[q] = pmc ? (j < ny) : (j >= 1 && j <= ny - 2);
-        hyb[q] = vHx[q] ? __ldg(S.hy_b + j) : 1.f;
-        hya[q] = vHx[q] ? __ldg(S.hy_a + j) : 0.f;
-        eyb[q] = vC[q] ? __ldg(S.ey_b + j) : 1.f;
-        eya[q] = vC[q] ? __ldg(S.ey_a + j) : 0.f;
-        hyA[q] = vHx[q] && (hya[q] != 0.f || hyb[q] != 1.f);
-        eyA[q] = vDz[q] && (eya[q] != 0.f || eyb[q] != 1.f);
+    // staged arrays: 0 Dz, 1 1/eps, 2 Hx, 3 Hy
+    if (lane == 0) {
+        const float **sp = const_cast<const float **>(pp.src);
+        sp[0] = S.f_main[par];
+        sp[1] = S.inv_eps_a;
+        sp[2] = S.f_x[par];
+        sp[3] = S.f_y[par];
     }
-    const bool anyHy = act && (hyA[0] || hyA[1] || hyA[2] || hyA[3]);
-    const bool anyEy = act && (eyA[0] || eyA[1] || eyA[2] || eyA[3]);
-    // left halo column (lane 0): Hx(i, c0-1)
-    const int jl = c0 - 1;
-    const bool hasL = (lane == 0) && jl >= 0 && jl <= ny - 2;
-    float hybL = 1.f, hyaL = 0.f;
-    if (hasL) { hybL = __ldg(S.hy_b + jl); hyaL = __ldg(S.hy_a + jl); }
-    const bool hyAL = hasL && (hyaL != 0.f || hybL != 1.f);
-    const int jr = c0 + 128;   // right halo column (lane 31): Ez(i, c0+128)
+    __syncwarp();
 
-    auto ezrow = [&](int i, float (&dz)[4], float (&ep)[4], float (&ez)[4]) {
-        if (act && i >= 0 && i < nx) {
-            ld4(Dz + i * P + jb, dz);
-            ldg4(eps + i * P + jb, ep);
-            if (EXPL) {
-                ldg4(Eex + i * P + jb, ez);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) ez[q] = vC[q] ? dz[q] / ep[q] : 0.f;
-            }
-        } else {
-            zero4(dz); zero4(ez);
-            ep[0] = ep[1] = ep[2] = ep[3] = 1.f;
-        }
-    };
-    auto ezat = [&](int i, int j) -> float {
-        if (i < 0 || i >= nx || j < 0 || j >= ny) return 0.f;
-        if (EXPL) return __ldg(Eex + i * P + j);
-        return Dz[i * P + j] / __ldg(eps + i * P + j);
-    };
-    // Hy(n+1/2) of row i from Ez rows i (ea) and i+1 (eb) (core/stepper_tm.py:97-100, :119-128)
-    auto hy_new = [&](int i, const float (&ea)[4], const float (&eb)[4], float (&out)[4],
-                      bool own) {
-        if (!(act && i >= 0 && i < nx)) { zero4(out); return; }
-        ld4(Hy + i * P + jb, out);
-        if (i > nx - 2) return;                       // padding row of the box
-        const float b = __ldg(S.hx_b + i), a = __ldg(S.hx_a + i);
-        const bool pa = (a != 0.f) || (b != 1.f);
-        float ps[4];
-        if (pa) ld4(pEzx + i * P + jb, ps); else zero4(ps);
+    float kH[4], kD[4];                    // dt/dx on live Hx / Dz columns, else 0
+    unsigned hyA = 0, eyA = 0;             // y-layer columns of this lane
+    {
+        const bool pmc = S.y_pmc != 0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            if (!vC[q]) continue;
-            const float d = (eb[q] - ea[q]) * rdx;
-            float c = d;
-            if (pa) { ps[q] = b * ps[q] + a * d; c = d + ps[q]; }
-            out[q] = out[q] + dt * c;
+            const int j = jb + q;
+            const bool hx = j <= ny - 2;
+            const bool dz = pmc ? (j < ny) : (j >= 1 && j <= ny - 2);
+            kH[q] = hx ? kdt : 0.f;
+            kD[q] = dz ? kdt : 0.f;
+            if (act && hx && (__ldg(S.hy_a + j) != 0.f || __ldg(S.hy_b + j) != 1.f)) hyA |= 1u << q;
+            if (act && dz && (__ldg(S.ey_a + j) != 0.f || __ldg(S.ey_b + j) != 1.f)) eyA |= 1u << q;
         }
-        if (pa && own) st4(pEzxN + i * P + jb, ps);
-        apply_cells(S.src_h1, i, C.amp_h, jb, out);
+    }
+    // halo columns: c0-1 (left of lane 0) and c0+128 (right of lane 31); the
+    // halo values are computed by the whole warp (uniform) and selected
+    const int jl = c0 - 1;
+    const bool hasL = jl >= 0 && jl <= ny - 2;
+    const bool hyAL = hasL && (__ldg(S.hy_a + jl) != 0.f || __ldg(S.hy_b + jl) != 1.f);
+    const int jr = c0 + 128;
+    const int so = 4 + 4 * lane;           // lane offset in a staged row
+
+    // Ez = Dz / eps of staged row k (own 4, halos c0-1, c0+128)
+    auto ez_of = [&](int k, int r, float (&ez)[4], float &ezl, float &ezr) {
+        ezl = ezr = 0.f;
+        if (r < 0 || r >= nx) { zero4(ez); return; }
+        if (EXPL) {
+            const float *Eex = S.e_explicit;
+            if (act) ld4(Eex + r * P + jb, ez); else zero4(ez);
+            if (jl >= 0) ezl = Eex[r * P + jl];
+            if (jr < ny) ezr = Eex[r * P + jr];
+            return;
+        }
+        const float *dz = pp.row(k, 0), *ie = pp.row(k, 1);
+        float d[4], e[4];
+        lds4(dz + so, d);
+        lds4(ie + so, e);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ez[q] = d[q] * e[q];
+        if (!act) zero4(ez);
+        if (jl >= 0) ezl = dz[3] * ie[3];
+        if (jr < ny) ezr = dz[132] * ie[132];
+    };
+    // Hy(n+1/2) of row r from Ez rows r (ea), r+1 (eb) (core/stepper_tm.py:97-100, :119-128)
+    auto hy_new = [&](int k, int r, const float (&ea)[4], const float (&eb)[4], float (&out)[4],
+                      bool own) {
+        if (r < 0 || r >= nx) { zero4(out); return; }
+        lds4(pp.row(k, 3) + so, out);
+        if (r > nx - 2) return;                       // padding row of the box
+        if (r >= xb0 && r < xb1) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) out[q] = fmaf(kdt, eb[q] - ea[q], out[q]);
+        } else if (act) {                             // inside the x layer
+            const float b = __ldg(S.hx_b + r), a = __ldg(S.hx_a + r);
+            const int64_t o = r * P + jb;
+            float ps[4];
+            ld4(S.psi[1][par] + o, ps);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float d = (eb[q] - ea[q]) * rdx;
+                ps[q] = b * ps[q] + a * d;
+                out[q] = out[q] + dt * (d + ps[q]);
+            }
+            if (own) st4(S.psi[1][par ^ 1] + o, ps);
+        }
+        if (r >= h1lo && r <= h1hi && act) apply_cells(S.src_h1, r, C.amp_h, jb, out);
     };
 
-    // ---- prologue: Ez rows i0-1 and i0, Hy(n+1/2) of row i0-1 (halo)
-    float dzB[4], epB[4], ezB[4], hyP[4];
+    // ---- prologue: rows i0-1 (stage 0) and i0 (stage 1)
+    for (int k = 0; k < NST; ++k) pp.issue(k);
+    if (!pp.wait(0, C.err) || !pp.wait(1, C.err)) { pp.drain(0, NST); return; }
+    float ezB[4], hyP[4], ezLB, ezRB;
     {
-        float dA[4], eA[4], zA[4];
-        ezrow(i0 - 1, dA, eA, zA);
-        ezrow(i0, dzB, epB, ezB);
-        if (i0 >= 1) hy_new(i0 - 1, zA, ezB, hyP, false); else zero4(hyP);
+        float ezA[4], l, r;
+        ez_of(0, i0 - 1, ezA, l, r);
+        ez_of(1, i0, ezB, ezLB, ezRB);
+        if (i0 >= 1) hy_new(0, i0 - 1, ezA, ezB, hyP, false); else zero4(hyP);
     }
-    float ezLB = (lane == 0) ? ezat(i0, jl) : 0.f;
-    float ezRB = (lane == 31) ? ezat(i0, jr) : 0.f;
+    __syncwarp();
+    pp.issue(NST);                          // stage 0 is free
 
     for (int i = i0; i < i1; ++i) {
-        float dzC[4], epC[4], ezC[4];
-        ezrow(i + 1, dzC, epC, ezC);
-        const float ezLC = (lane == 0) ? ezat(i + 1, jl) : 0.f;
-        const float ezRC = (lane == 31) ? ezat(i + 1, jr) : 0.f;
+        const int kc = i - i0 + 1, kn = kc + 1;
+        if (!pp.wait(kn, C.err)) { pp.drain(kn + 1, kc + NST); return; }
+        float ezC[4], ezLC, ezRC;
+        ez_of(kn, i + 1, ezC, ezLC, ezRC);
         const int64_t ro = i * P + jb;
 
-        // Hy(n+1/2), row i
         float hyN[4];
-        hy_new(i, ezB, ezC, hyN, true);
+        hy_new(kc, i, ezB, ezC, hyN, true);
 
         // Hx(n+1/2), row i (core/stepper_tm.py:91-94, :121-128)
         float hxN[4];
-        {
-            float ezr = __shfl_down_sync(0xffffffffu, ezB[0], 1);
-            if (lane == 31) ezr = ezRB;
-            if (act) ld4(Hx + ro, hxN); else zero4(hxN);
-            float ps[4];
-            if (anyHy) ld4(pEzy + ro, ps); else zero4(ps);
+        const float *hxs = pp.row(kc, 2);
+        float ezr = __shfl_down_sync(0xffffffffu, ezB[0], 1);
+        ezr = (lane == 31) ? ezRB : ezr;
+        lds4(hxs + so, hxN);
+        if (!hyA) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                if (!vHx[q]) continue;
+                const float er = (q < 3) ? ezB[q + 1] : ezr;
+                hxN[q] = fmaf(-kH[q], er - ezB[q], hxN[q]);
+            }
+        } else {
+            float ps[4];
+            ld4(S.psi[0][par] + ro, ps);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
                 const float er = (q < 3) ? ezB[q + 1] : ezr;
                 const float d = (er - ezB[q]) * rdx;
                 float c = d;
-                if (hyA[q]) { ps[q] = hyb[q] * ps[q] + hya[q] * d; c = d + ps[q]; }
-                hxN[q] = hxN[q] - dt * c;
+                if (BIT(hyA, q)) {
+                    ps[q] = __ldg(S.hy_b + jb + q) * ps[q] + __ldg(S.hy_a + jb + q) * d;
+                    c = d + ps[q];
+                }
+                hxN[q] = kH[q] != 0.f ? hxN[q] - dt * c : hxN[q];
             }
-            if (anyHy) st4(pEzyN + ro, ps);
-            if (act) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
+            st4(S.psi[0][par ^ 1] + ro, ps);
         }
-        // left neighbour Hx(n+1/2)(i, j-1)
+        if (i >= h2lo && i <= h2hi && act) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
+        if (!act) zero4(hxN);
+        // left neighbour Hx(n+1/2)(i, j-1): lane 0's is the halo column,
+        // recomputed by the whole warp from Ez(i, c0-1), Ez(i, c0)
         float hxl0 = __shfl_up_sync(0xffffffffu, hxN[3], 1);
-        if (lane == 0) {
+        {
+            const float ez0 = __shfl_sync(0xffffffffu, ezB[0], 0);
             float v = 0.f;
             if (hasL) {
-                const float d = (ezB[0] - ezLB) * rdx;
+                const float d = (ez0 - ezLB) * rdx;
                 float c = d;
-                if (hyAL) c = d + (hybL * pEzy[i * P + jl] + hyaL * d);
-                v = Hx[i * P + jl] - dt * c;
-                v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
+                if (hyAL)
+                    c = d + (__ldg(S.hy_b + jl) * S.psi[0][par][i * P + jl] + __ldg(S.hy_a + jl) * d);
+                v = hxs[3] - dt * c;
+                if (i >= h2lo && i <= h2hi) v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
             }
-            hxl0 = v;
+            hxl0 = (lane == 0) ? v : hxl0;
         }
 
         // Dz(n+1), row i (core/stepper_tm.py:136-166), then source and E
-        float dzN[4], ezN[4];
-        {
-            const bool irow = (i >= 1 && i <= nx - 2);
-            float bx = 1.f, ax = 0.f;
-            if (irow) { bx = __ldg(S.ex_b + i); ax = __ldg(S.ex_a + i); }
-            const bool pxA = act && irow && (ax != 0.f || bx != 1.f);
-            const bool pyA = irow && anyEy;
-            float px[4], py[4];
-            if (pxA) ld4(pHyx + ro, px); else zero4(px);
-            if (pyA) ld4(pHxy + ro, py); else zero4(py);
+        float dzN[4], ezN[4], ieB[4];
+        lds4(pp.row(kc, 0) + so, dzN);
+        lds4(pp.row(kc, 1) + so, ieB);
+        if (i >= 1 && i <= nx - 2) {
+            const bool pxA = act && (i < xe0 || i >= xe1);
+            if (!pxA && !eyA) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                float dz = dzB[q];
-                if (irow && vDz[q]) {
+                for (int q = 0; q < 4; ++q) {
+                    const float hxm = (q == 0) ? hxl0 : hxN[q - 1];
+                    dzN[q] = fmaf(kD[q], (hyN[q] - hyP[q]) - (hxN[q] - hxm), dzN[q]);
+                }
+            } else {
+                float bx = 1.f, ax = 0.f;
+                if (pxA) { bx = __ldg(S.ex_b + i); ax = __ldg(S.ex_a + i); }
+                float px[4], py[4];
+                if (pxA) ld4(S.psi[2][par] + ro, px); else zero4(px);
+                if (eyA) ld4(S.psi[3][par] + ro, py); else zero4(py);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (kD[q] == 0.f) continue;
                     const float hxm = (q == 0) ? hxl0 : hxN[q - 1];
                     const float dhy = (hyN[q] - hyP[q]) * rdx;
                     const float dhx = (hxN[q] - hxm) * rdx;
                     float p1 = 0.f, p2 = 0.f;
                     if (pxA) { p1 = bx * px[q] + ax * dhy; px[q] = p1; }
-                    if (eyA[q]) { p2 = eyb[q] * py[q] + eya[q] * dhx; py[q] = p2; }
-                    const float curl = ((dhy + p1) - dhx) - p2;
-                    dz = dz + dt * curl;
+                    if (BIT(eyA, q)) {
+                        p2 = __ldg(S.ey_b + jb + q) * py[q] + __ldg(S.ey_a + jb + q) * dhx;
+                        py[q] = p2;
+                    }
+                    dzN[q] = dzN[q] + dt * (((dhy + p1) - dhx) - p2);
                 }
-                dzN[q] = dz;
+                if (pxA) st4(S.psi[2][par ^ 1] + ro, px);
+                if (eyA) st4(S.psi[3][par ^ 1] + ro, py);
             }
-            if (pxA) st4(pHyxN + ro, px);
-            if (pyA) st4(pHxyN + ro, py);
-            if (act) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) ezN[q] = vC[q] ? dzN[q] / epB[q] : 0.f;
         }
+        if (i >= selo && i <= sehi && act) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ezN[q] = dzN[q] * ieB[q];
         if (act) {
             st4(Hxn + ro, hxN);
             st4(Hyn + ro, hyN);
             st4(Dzn + ro, dzN);
-            if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, ezN);
-            if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, hxN);
-            if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, hyN);
+            if (rf0 >= 0) st4(ring + rf0 + ro, ezN);
+            if (rf1 >= 0) st4(ring + rf1 + ro, hxN);
+            if (rf2 >= 0) st4(ring + rf2 + ro, hyN);
         }
         if (nl) {
             sample_row(L, nl, MTB_C2_MAIN, i, jb, act, ezN, ring);
@@ -303,19 +440,19 @@ __device__ __forceinline__ void tm_warp(const mtb_yee2d_struct &S, const int i0,
             sample_row(L, nl, MTB_C2_Y, i, jb, act, hyN, ring);
         }
         copy4(hyP, hyN);
-        copy4(dzB, dzC);
-        copy4(epB, epC);
         copy4(ezB, ezC);
         ezLB = ezLC;
         ezRB = ezRC;
+        __syncwarp();
+        pp.issue(kc + NST);                   // row i's stage is free
     }
 }
 
 // ------------------------------------------------------------------ TE
 
 __device__ __forceinline__ void te_warp(const mtb_yee2d_struct &S, const int i0, const int i1,
-                                        const int c0, const Ctx2D &C,
-                                        const mtb_line_sample *L, const int nl) {
+                                        const int c0, const Ctx2D &C, const mtb_line_sample *L,
+                                        const int nl, Pipe<5> pp) {
     const int lane = threadIdx.x & 31;
     const int nx = S.nx, ny = S.ny;
     const int64_t P = S.pitch;
@@ -323,131 +460,145 @@ __device__ __forceinline__ void te_warp(const mtb_yee2d_struct &S, const int i0,
     const bool act = jb < S.pitch;
     const float dt = S.dt;
     const float rdx = 1.0f / S.dx;
+    const float kdt = dt * rdx;
     const int par = C.par;
-    const float *__restrict__ Hz = S.f_main[par];
     float *__restrict__ Hzn = S.f_main[par ^ 1];
-    const float *__restrict__ Dx = S.f_x[par];
     float *__restrict__ Dxn = S.f_x[par ^ 1];
-    const float *__restrict__ Dy = S.f_y[par];
     float *__restrict__ Dyn = S.f_y[par ^ 1];
-    const float *__restrict__ epx = S.eps_a;
-    const float *__restrict__ epy = S.eps_b;
-    const float *__restrict__ pHzy = S.psi[0][par];
-    float *__restrict__ pHzyN = S.psi[0][par ^ 1];
-    const float *__restrict__ pHzx = S.psi[1][par];
-    float *__restrict__ pHzxN = S.psi[1][par ^ 1];
-    const float *__restrict__ pEyx = S.psi[2][par];
-    float *__restrict__ pEyxN = S.psi[2][par ^ 1];
-    const float *__restrict__ pExy = S.psi[3][par];
-    float *__restrict__ pExyN = S.psi[3][par ^ 1];
     float *ring = C.ring;
+    const int64_t rf0 = S.ring_full[0], rf1 = S.ring_full[1], rf2 = S.ring_full[2];
+    const int xb0 = S.xband[0], xb1 = S.xband[1], xe0 = S.xband[2], xe1 = S.xband[3];
+    const int selo = S.src_e.row_lo, sehi = S.src_e.row_hi;
+    const int h1lo = S.src_h1.row_lo, h1hi = S.src_h1.row_hi;
 
-    bool vHz[4], vEx[4], vDxU[4], vEy[4], eyA[4], hyA[4];
-    float eyb[4], eya[4], hyb[4], hya[4];
+    // staged arrays: 0 Hz, 1 Dx, 2 Dy, 3 1/eps_x, 4 1/eps_y
+    if (lane == 0) {
+        const float **sp = const_cast<const float **>(pp.src);
+        sp[0] = S.f_main[par];
+        sp[1] = S.f_x[par];
+        sp[2] = S.f_y[par];
+        sp[3] = S.inv_eps_a;
+        sp[4] = S.inv_eps_b;
+    }
+    __syncwarp();
+
+    float kDx[4], kDy[4];                  // dt/dx on updated Dx / live Dy, Hz columns
+    unsigned eyA = 0, hyA = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
-        vHz[q] = j <= ny - 2;
-        vEx[q] = j < ny;
-        vDxU[q] = j >= 1 && j <= ny - 2;
-        vEy[q] = j <= ny - 2;
-        eyb[q] = vEx[q] ? __ldg(S.ey_b + j) : 1.f;
-        eya[q] = vEx[q] ? __ldg(S.ey_a + j) : 0.f;
-        hyb[q] = vHz[q] ? __ldg(S.hy_b + j) : 1.f;
-        hya[q] = vHz[q] ? __ldg(S.hy_a + j) : 0.f;
-        eyA[q] = vDxU[q] && (eya[q] != 0.f || eyb[q] != 1.f);
-        hyA[q] = vHz[q] && (hya[q] != 0.f || hyb[q] != 1.f);
+        const bool hz = j <= ny - 2, dxu = j >= 1 && j <= ny - 2;
+        kDx[q] = dxu ? kdt : 0.f;
+        kDy[q] = hz ? kdt : 0.f;           // Dy and Hz live on columns j <= ny-2
+        if (act && dxu && (__ldg(S.ey_a + j) != 0.f || __ldg(S.ey_b + j) != 1.f)) eyA |= 1u << q;
+        if (act && hz && (__ldg(S.hy_a + j) != 0.f || __ldg(S.hy_b + j) != 1.f)) hyA |= 1u << q;
     }
-    const bool anyEy = act && (eyA[0] || eyA[1] || eyA[2] || eyA[3]);
-    const bool anyHy = act && (hyA[0] || hyA[1] || hyA[2] || hyA[3]);
     const int jl = c0 - 1;          // left halo: Hz(r, c0-1)
-    const int jr = c0 + 128;        // right halo: Ex(n+1/2)(r, c0+128)
-    const bool hasR = (lane == 31) && jr <= ny - 1;
-    float eybR = 1.f, eyaR = 0.f;
+    const int jr = c0 + 128;        // right halo: Ex(n+1/2)(r, c0+128), uniform
+    const bool hasR = jr <= ny - 1;
     const bool updR = hasR && jr >= 1 && jr <= ny - 2;
-    if (updR) { eybR = __ldg(S.ey_b + jr); eyaR = __ldg(S.ey_a + jr); }
-    const bool eyAR = updR && (eyaR != 0.f || eybR != 1.f);
+    const bool eyAR = updR && (__ldg(S.ey_a + jr) != 0.f || __ldg(S.ey_b + jr) != 1.f);
+    const int so = 4 + 4 * lane;
 
-    auto hzrow = [&](int r, float (&v)[4]) {
-        if (act && r >= 0 && r < nx) ld4(Hz + r * P + jb, v); else zero4(v);
-    };
-    auto hzat = [&](int r, int j) -> float {
-        if (r < 0 || r > nx - 2 || j < 0 || j > ny - 2) return 0.f;
-        return Hz[r * P + j];
+    // Hz(n) of staged row k (zero outside the Hz array)
+    auto hz_of = [&](int k, int r, float (&v)[4], float &hl, float &hr) {
+        hl = hr = 0.f;
+        if (!(r >= 0 && r <= nx - 2)) { zero4(v); return; }
+        const float *h = pp.row(k, 0);
+        lds4(h + so, v);
+        if (!act) zero4(v);
+        if (jl >= 0 && jl <= ny - 2) hl = h[3];
+        if (jr <= ny - 2) hr = h[132];
     };
 
-    // D/E(n+1/2) of row r from Hz(n) rows r-1 (hp) and r (hc)
+    // D/E(n+1/2) of row r (stage k) from Hz(n) rows r-1 (hp) and r (hc)
     // (core/stepper_te.py:79-111 D update, :120-134 source, :150-175 E)
-    auto e_row = [&](int r, const float (&hp)[4], const float (&hc)[4], float hzL, float hzR,
-                     bool own, float (&ex)[4], float (&ey)[4], float &exR) {
+    auto e_row = [&](int k, int r, const float (&hp)[4], const float (&hc)[4], float hzL,
+                     float hzR, bool own, float (&ex)[4], float (&ey)[4], float &exR) {
         exR = 0.f;
         if (r < 0 || r >= nx) { zero4(ex); zero4(ey); return; }
         const int64_t ro = r * P + jb;
-        // Dx, row r (valid rows 0..nx-2)
+        const float *sdx = pp.row(k, 1), *sdy = pp.row(k, 2), *siex = pp.row(k, 3),
+                    *siey = pp.row(k, 4);
         float dxN[4];
-        if (act) ld4(Dx + ro, dxN); else zero4(dxN);
+        lds4(sdx + so, dxN);
         float hl = __shfl_up_sync(0xffffffffu, hc[3], 1);
-        if (lane == 0) hl = hzL;
+        hl = (lane == 0) ? hzL : hl;
         if (r <= nx - 2) {
-            float py[4];
-            if (anyEy) ld4(pHzy + ro, py); else zero4(py);
+            if (!eyA) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (!vDxU[q]) continue;
-                const float hm = (q == 0) ? hl : hc[q - 1];
-                const float d = (hc[q] - hm) * rdx;
-                float c = d;
-                if (eyA[q]) { py[q] = eyb[q] * py[q] + eya[q] * d; c = d + py[q]; }
-                dxN[q] = dxN[q] + dt * c;
-            }
-            if (anyEy && own) st4(pHzyN + ro, py);
-            float ep[4];
-            if (act) ldg4(epx + ro, ep); else ep[0] = ep[1] = ep[2] = ep[3] = 1.f;
+                for (int q = 0; q < 4; ++q) {
+                    const float hm = (q == 0) ? hl : hc[q - 1];
+                    dxN[q] = fmaf(kDx[q], hc[q] - hm, dxN[q]);
+                }
+            } else {
+                float py[4];
+                ld4(S.psi[0][par] + ro, py);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) ex[q] = vEx[q] ? dxN[q] / ep[q] : 0.f;
-            if (hasR) {
-                float dxr = Dx[r * P + jr];
-                if (updR) {
-                    const float d = (hzR - hc[3]) * rdx;
+                for (int q = 0; q < 4; ++q) {
+                    if (kDx[q] == 0.f) continue;
+                    const float hm = (q == 0) ? hl : hc[q - 1];
+                    const float d = (hc[q] - hm) * rdx;
                     float c = d;
-                    if (eyAR) c = d + (eybR * pHzy[r * P + jr] + eyaR * d);
+                    if (BIT(eyA, q)) {
+                        py[q] = __ldg(S.ey_b + jb + q) * py[q] + __ldg(S.ey_a + jb + q) * d;
+                        c = d + py[q];
+                    }
+                    dxN[q] = dxN[q] + dt * c;
+                }
+                if (own) st4(S.psi[0][par ^ 1] + ro, py);
+            }
+            float ie[4];
+            lds4(siex + so, ie);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ex[q] = dxN[q] * ie[q];
+            if (hasR) {
+                float dxr = sdx[132];
+                if (updR) {
+                    const float hc127 = __shfl_sync(0xffffffffu, hc[3], 31);
+                    const float d = (hzR - hc127) * rdx;
+                    float c = d;
+                    if (eyAR)
+                        c = d + (__ldg(S.ey_b + jr) * S.psi[0][par][r * P + jr] +
+                                 __ldg(S.ey_a + jr) * d);
                     dxr = dxr + dt * c;
                 }
-                exR = dxr / __ldg(epx + r * P + jr);
+                exR = dxr * siex[132];
             }
         } else {
             zero4(ex);
         }
-        // Dy, row r (valid rows 0..nx-1; updated 1..nx-2)
         float dyN[4];
-        if (act) ld4(Dy + ro, dyN); else zero4(dyN);
-        const bool irow = r >= 1 && r <= nx - 2;
-        float bx = 1.f, ax = 0.f;
-        if (irow) { bx = __ldg(S.ex_b + r); ax = __ldg(S.ex_a + r); }
-        const bool pxA = act && irow && (ax != 0.f || bx != 1.f);
-        float px[4];
-        if (pxA) ld4(pHzx + ro, px); else zero4(px);
-        if (irow) {
+        lds4(sdy + so, dyN);
+        if (r >= 1 && r <= nx - 2) {
+            if (!(act && (r < xe0 || r >= xe1))) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (!vEy[q]) continue;
-                const float d = (hc[q] - hp[q]) * rdx;
-                float c = d;
-                if (pxA) { px[q] = bx * px[q] + ax * d; c = d + px[q]; }
-                dyN[q] = dyN[q] - dt * c;
+                for (int q = 0; q < 4; ++q) dyN[q] = fmaf(-kDy[q], hc[q] - hp[q], dyN[q]);
+            } else {
+                const float bx = __ldg(S.ex_b + r), ax = __ldg(S.ex_a + r);
+                float px[4];
+                ld4(S.psi[1][par] + ro, px);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (kDy[q] == 0.f) continue;
+                    const float d = (hc[q] - hp[q]) * rdx;
+                    px[q] = bx * px[q] + ax * d;
+                    dyN[q] = dyN[q] - dt * (d + px[q]);
+                }
+                if (own) st4(S.psi[1][par ^ 1] + ro, px);
             }
         }
-        if (pxA && own) st4(pHzxN + ro, px);
-        if (act) apply_cells(S.src_e, r, C.amp_e, jb, dyN);
-        float ep[4];
-        if (act) ldg4(epy + ro, ep); else ep[0] = ep[1] = ep[2] = ep[3] = 1.f;
+        if (r >= selo && r <= sehi && act) apply_cells(S.src_e, r, C.amp_e, jb, dyN);
+        float ie[4];
+        lds4(siey + so, ie);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) ey[q] = vEy[q] ? dyN[q] / ep[q] : 0.f;
+        for (int q = 0; q < 4; ++q) ey[q] = dyN[q] * ie[q];
+        if (!act) { zero4(ex); zero4(ey); }
         if (own && act) {
             st4(Dxn + ro, dxN);
             st4(Dyn + ro, dyN);
-            if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, ex);
-            if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, ey);
+            if (rf1 >= 0) st4(ring + rf1 + ro, ex);
+            if (rf2 >= 0) st4(ring + rf2 + ro, ey);
         }
         if (own && nl) {
             sample_row(L, nl, MTB_C2_X, r, jb, act, ex, ring);
@@ -455,82 +606,185 @@ __device__ __forceinline__ void te_warp(const mtb_yee2d_struct &S, const int i0,
         }
     };
 
-    // ---- prologue
-    float hzA[4], hzB[4], exB[4], eyB[4], exRB;
-    hzrow(i0 - 1, hzA);
-    hzrow(i0, hzB);
-    float hzLB = (lane == 0) ? hzat(i0, jl) : 0.f;
-    float hzRB = (lane == 31) ? hzat(i0, jr) : 0.f;
-    e_row(i0, hzA, hzB, hzLB, hzRB, true, exB, eyB, exRB);
+    // ---- prologue: rows i0-1 (stage 0), i0 (stage 1)
+    for (int k = 0; k < NST; ++k) pp.issue(k);
+    if (!pp.wait(0, C.err) || !pp.wait(1, C.err)) { pp.drain(0, NST); return; }
+    float hzB[4], exB[4], eyB[4], exRB;
+    {
+        float hzA[4], l0, r0, lB, rB;
+        hz_of(0, i0 - 1, hzA, l0, r0);
+        hz_of(1, i0, hzB, lB, rB);
+        e_row(1, i0, hzA, hzB, lB, rB, true, exB, eyB, exRB);
+    }
+    __syncwarp();
+    pp.issue(NST);
 
     for (int i = i0; i < i1; ++i) {
-        float hzC[4], exC[4], eyC[4], exRC;
-        hzrow(i + 1, hzC);
-        const float hzLC = (lane == 0) ? hzat(i + 1, jl) : 0.f;
-        const float hzRC = (lane == 31) ? hzat(i + 1, jr) : 0.f;
-        e_row(i + 1, hzB, hzC, hzLC, hzRC, i + 1 < i1, exC, eyC, exRC);
+        const int kc = i - i0 + 1, kn = kc + 1;
+        if (!pp.wait(kn, C.err)) { pp.drain(kn + 1, kc + NST); return; }
+        float hzC[4], exC[4], eyC[4], exRC, lC, rC;
+        hz_of(kn, i + 1, hzC, lC, rC);
+        e_row(kn, i + 1, hzB, hzC, lC, rC, i + 1 < i1, exC, eyC, exRC);
 
         // Hz(n+1), row i (core/stepper_te.py:113-117)
         const int64_t ro = i * P + jb;
         float hzN[4];
         copy4(hzN, hzB);
         if (i <= nx - 2) {
-            const float bx = __ldg(S.hx_b + i), ax = __ldg(S.hx_a + i);
-            const bool pxA = act && (ax != 0.f || bx != 1.f);
-            float p1v[4], p2v[4];
-            if (pxA) ld4(pEyx + ro, p1v); else zero4(p1v);
-            if (anyHy) ld4(pExy + ro, p2v); else zero4(p2v);
             float exr = __shfl_down_sync(0xffffffffu, exB[0], 1);
-            if (lane == 31) exr = exRB;
+            exr = (lane == 31) ? exRB : exr;
+            const bool pxA = act && (i < xb0 || i >= xb1);
+            if (!pxA && !hyA) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (!vHz[q]) continue;
-                const float exn = (q < 3) ? exB[q + 1] : exr;
-                const float dey = (eyC[q] - eyB[q]) * rdx;
-                const float dex = (exn - exB[q]) * rdx;
-                float p1 = 0.f, p2 = 0.f;
-                if (pxA) { p1 = bx * p1v[q] + ax * dey; p1v[q] = p1; }
-                if (hyA[q]) { p2 = hyb[q] * p2v[q] + hya[q] * dex; p2v[q] = p2; }
-                const float curl = ((dey + p1) - dex) - p2;
-                hzN[q] = hzN[q] - dt * curl;
+                for (int q = 0; q < 4; ++q) {
+                    const float exn = (q < 3) ? exB[q + 1] : exr;
+                    hzN[q] = fmaf(-kDy[q], (eyC[q] - eyB[q]) - (exn - exB[q]), hzN[q]);
+                }
+            } else {
+                float bx = 1.f, ax = 0.f;
+                if (pxA) { bx = __ldg(S.hx_b + i); ax = __ldg(S.hx_a + i); }
+                float p1v[4], p2v[4];
+                if (pxA) ld4(S.psi[2][par] + ro, p1v); else zero4(p1v);
+                if (hyA) ld4(S.psi[3][par] + ro, p2v); else zero4(p2v);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (kDy[q] == 0.f) continue;
+                    const float exn = (q < 3) ? exB[q + 1] : exr;
+                    const float dey = (eyC[q] - eyB[q]) * rdx;
+                    const float dex = (exn - exB[q]) * rdx;
+                    float p1 = 0.f, p2 = 0.f;
+                    if (pxA) { p1 = bx * p1v[q] + ax * dey; p1v[q] = p1; }
+                    if (BIT(hyA, q)) {
+                        p2 = __ldg(S.hy_b + jb + q) * p2v[q] + __ldg(S.hy_a + jb + q) * dex;
+                        p2v[q] = p2;
+                    }
+                    hzN[q] = hzN[q] - dt * (((dey + p1) - dex) - p2);
+                }
+                if (pxA) st4(S.psi[2][par ^ 1] + ro, p1v);
+                if (hyA) st4(S.psi[3][par ^ 1] + ro, p2v);
             }
-            if (pxA) st4(pEyxN + ro, p1v);
-            if (anyHy) st4(pExyN + ro, p2v);
-            if (act) apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
+            if (i >= h1lo && i <= h1hi && act) apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
         }
         if (act) {
             st4(Hzn + ro, hzN);
-            if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, hzN);
+            if (rf0 >= 0) st4(ring + rf0 + ro, hzN);
         }
         if (nl) sample_row(L, nl, MTB_C2_MAIN, i, jb, act, hzN, ring);
         copy4(hzB, hzC);
         copy4(exB, exC);
         copy4(eyB, eyC);
         exRB = exRC;
+        __syncwarp();
+        pp.issue(kc + NST);
     }
 }
 
-__global__ void __launch_bounds__(32 * WARPS2D) k_yee2d_step(
-    const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
-    Ctx2D C) {
-    __shared__ mtb_line_sample sl[WARPS2D][MAXL];
+// Shared memory per block: per warp its NST staged rows (first: bulk-copy
+// destinations need 16-byte alignment), its mbarriers, its structure copy and
+// its filtered line samples.
+template <int NA>
+struct __align__(16) WarpSmem {
+    float buf[NST * NA * EXT];
+    uint64_t bar[NST];
+    const float *src[8];
+    mtb_yee2d_struct s;
+    mtb_line_sample lines[MAXL];
+};
+static_assert((NST * 4 * EXT * sizeof(float)) % 16 == 0, "stage buffers must be 16-byte aligned");
+static_assert(sizeof(WarpSmem<4>) % 16 == 0 && sizeof(WarpSmem<5>) % 16 == 0,
+              "per-warp shared block must keep 16-byte alignment");
+
+// Per-warp setup shared by the TM and TE kernels: descriptor copy, barrier
+// init, line-sample filter, pipeline geometry.
+template <int NA>
+__device__ __forceinline__ bool warp_setup(const mtb_yee2d_struct *__restrict__ SS,
+                                           const int4 *__restrict__ work, int n_work,
+                                           WarpSmem<NA> *&Wp, int4 &w, int &nl) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    WarpSmem<NA> *ws = reinterpret_cast<WarpSmem<NA> *>(smraw);
     const int wib = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x * WARPS2D + wib;
-    if (wid >= n_work) return;
-    const int4 w = work[wid];
-    const mtb_yee2d_struct &S = SS[w.x];
-    const int nl = S.n_lines;
-    if (lane < nl) sl[wib][lane] = S.lines[lane];
-    __syncwarp();
-    if (S.pol == MTB_TM) {
-        if (C.first && S.explicit_e)
-            tm_warp<true>(S, w.y, w.z, w.w, C, sl[wib], nl);
-        else
-            tm_warp<false>(S, w.y, w.z, w.w, C, sl[wib], nl);
-    } else {
-        te_warp(S, w.y, w.z, w.w, C, sl[wib], nl);
+    if (wid >= n_work) return false;             // whole warp
+    WarpSmem<NA> &W = ws[wib];
+    Wp = &W;
+    w = work[wid];
+    {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(SS + w.x);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&W.s);
+        for (int e = lane; e < (int)(sizeof(mtb_yee2d_struct) / 4); e += 32) dst[e] = src[e];
     }
+    if (lane == 0) {
+        for (int k = 0; k < NST; ++k) mbar_init(&W.bar[k], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    const mtb_yee2d_struct &S = W.s;
+    const int i0 = w.y, i1 = w.z, c0 = w.w;
+    {   // line samples that touch this warp's rows [i0, i1) x columns [c0, c0+128)
+        const int n_all = S.n_lines;
+        bool keep = false;
+        mtb_line_sample ln{};
+        if (lane < n_all) {
+            ln = S.lines[lane];
+            if (ln.kind == 0)
+                keep = ln.index >= i0 && ln.index < i1 && ln.lo < c0 + 128 && ln.hi > c0;
+            else
+                keep = ln.index >= c0 && ln.index < c0 + 128 && ln.lo < i1 && ln.hi > i0;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) W.lines[__popc(m & ((1u << lane) - 1))] = ln;
+        nl = __popc(m);
+    }
+    __syncwarp();
+    return true;
+}
+
+template <int NA>
+__device__ __forceinline__ Pipe<NA> make_pipe(WarpSmem<NA> &W, int i0, int i1, int c0) {
+    Pipe<NA> pp;
+    const mtb_yee2d_struct &S = W.s;
+    pp.buf = W.buf;
+    pp.bar = W.bar;
+    pp.src = W.src;
+    pp.P = S.pitch;
+    pp.w0 = max(c0 - 4, 0);
+    const int w1 = min(c0 + 132, S.pitch);
+    pp.dst = pp.w0 - (c0 - 4);
+    pp.bytes = (uint32_t)(w1 - pp.w0) * 4u;
+    pp.i0m1 = i0 - 1;
+    pp.nx = S.nx;
+    pp.nrows = i1 - i0 + 2;
+    pp.lane = threadIdx.x & 31;
+    return pp;
+}
+
+// TM step; FIRST = the plan's first step, where a structure imported with an
+// Ez that is not Dz/eps reads it from e_explicit.
+template <bool FIRST>
+__global__ void __launch_bounds__(32 * WARPS2D, 4) k_yee2d_tm(
+    const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
+    Ctx2D C) {
+    WarpSmem<4> *W;
+    int4 w;
+    int nl;
+    if (!warp_setup<4>(SS, work, n_work, W, w, nl)) return;
+    Pipe<4> pp = make_pipe<4>(*W, w.y, w.z, w.w);
+    if (FIRST && W->s.explicit_e)
+        tm_warp<true>(W->s, w.y, w.z, w.w, C, W->lines, nl, pp);
+    else
+        tm_warp<false>(W->s, w.y, w.z, w.w, C, W->lines, nl, pp);
+}
+
+__global__ void __launch_bounds__(32 * WARPS2D, 4) k_yee2d_te(
+    const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
+    Ctx2D C) {
+    WarpSmem<5> *W;
+    int4 w;
+    int nl;
+    if (!warp_setup<5>(SS, work, n_work, W, w, nl)) return;
+    Pipe<5> pp = make_pipe<5>(*W, w.y, w.z, w.w);
+    te_warp(W->s, w.y, w.z, w.w, C, W->lines, nl, pp);
 }
 
 }  // namespace mtb
@@ -539,9 +793,10 @@ using namespace mtb;
 
 struct mtb_yee2d_plan {
     int n_structs = 0;
-    DevBuf structs_d, work_d, amp_d;
+    DevBuf structs_d, work_d, amp_d, err_d;
     HostBuf amp_h;
     int n_work = 0;
+    int n_work_tm = 0;                 // work items [0, n_work_tm) are TM, the rest TE
     int n_cols = 0;
     int rows = 32;
     int par = 0;
@@ -558,23 +813,74 @@ static int check_ptr(const void *p, const char *what, int s) {
     return MTB_OK;
 }
 
+// Fill row_lo / row_hi of a cell list from its row pointer (device -> host).
+static int cell_rows(mtb_cells &cl, int rows, int s) {
+    cl.row_lo = 1;
+    cl.row_hi = 0;
+    if (cl.n <= 0) return MTB_OK;
+    std::vector<int32_t> rp(rows + 1);
+    cudaError_t e = cudaMemcpy(rp.data(), cl.row_ptr, sizeof(int32_t) * (rows + 1),
+                               cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return fail(MTB_CUDA_ERROR, "structure %d: reading source rows: %s", s,
+                    cudaGetErrorString(e));
+    if (rp[0] != 0 || rp[rows] != cl.n)
+        return fail(MTB_INVALID_ARG, "structure %d: source row_ptr does not cover %d cells", s,
+                    cl.n);
+    for (int r = 0; r < rows; ++r) {
+        if (rp[r + 1] < rp[r]) return fail(MTB_INVALID_ARG, "structure %d: row_ptr decreasing", s);
+        if (rp[r + 1] > rp[r]) {
+            if (cl.row_lo > cl.row_hi) cl.row_lo = r;
+            cl.row_hi = r;
+        }
+    }
+    return MTB_OK;
+}
+
+// Rows where an x profile may be active, conservatively: [0, lo_end) holds
+// every active node (a != 0 or b != 1) of the low half, [hi_begin, n) every
+// active node of the high half. Inert nodes inside a band are harmless (their
+// CPML memory stays zero and the effective derivative is the plain one).
+static int profile_band(const float *b_d, const float *a_d, int n, int32_t &lo_end,
+                        int32_t &hi_begin, int s) {
+    std::vector<float> b(n), a(n);
+    cudaError_t e = cudaMemcpy(b.data(), b_d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(a.data(), a_d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return fail(MTB_CUDA_ERROR, "structure %d: reading CPML profile: %s", s,
+                    cudaGetErrorString(e));
+    const int half = n / 2;
+    lo_end = 0;
+    for (int i = 0; i < half; ++i)
+        if (a[i] != 0.f || b[i] != 1.f) lo_end = i + 1;
+    hi_begin = n;
+    for (int i = n - 1; i >= half; --i)
+        if (a[i] != 0.f || b[i] != 1.f) hi_begin = i;
+    return MTB_OK;
+}
+
+static size_t smem_tm() { return sizeof(WarpSmem<4>) * WARPS2D; }
+static size_t smem_te() { return sizeof(WarpSmem<5>) * WARPS2D; }
+
 extern "C" {
 
-int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs, int32_t n, const mtb_dft_region *regions,
-                          int32_t n_regions, const mtb_phase_group *groups, int32_t n_groups,
+int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
+                          const mtb_dft_region *regions, int32_t n_regions,
+                          const mtb_phase_group *groups, int32_t n_groups,
                           int64_t ring_slot_elems, int32_t n_amp_cols, const mtb_tuning *tuning,
                           mtb_yee2d_plan **out) {
     if (!out) return fail(MTB_INVALID_ARG, "out is null");
     *out = nullptr;
-    if (n < 1 || !structs) return fail(MTB_INVALID_ARG, "need at least one structure");
+    if (n < 1 || !structs_in) return fail(MTB_INVALID_ARG, "need at least one structure");
     if (n_amp_cols < 0) return fail(MTB_INVALID_ARG, "n_amp_cols < 0");
     int rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
-    int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 16;
+    int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     if (ring_slot_elems < 0 || (ring_slot_elems & 3))
         return fail(MTB_INVALID_ARG, "ring_slot_elems must be a non-negative multiple of 4");
+    std::vector<mtb_yee2d_struct> structs(structs_in, structs_in + n);
     int64_t n_work = 0;
     for (int s = 0; s < n; ++s) {
-        const mtb_yee2d_struct &S = structs[s];
+        mtb_yee2d_struct &S = structs[s];
         if (S.pol != MTB_TM && S.pol != MTB_TE)
             return fail(MTB_INVALID_ARG, "structure %d: pol must be MTB_TM or MTB_TE", s);
         if (S.nx < 3 || S.ny < 3)
@@ -583,6 +889,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs, int32_t n, const mtb_
         if (S.pitch < S.ny || (S.pitch & 3))
             return fail(MTB_INVALID_ARG, "structure %d: pitch %d must be >= ny and a multiple of 4",
                         s, S.pitch);
+        if ((int64_t)S.nx * S.pitch >= (1LL << 31))
+            return fail(MTB_UNSUPPORTED, "structure %d: grid too large", s);
         if (!(S.dt > 0.f) || !(S.dx > 0.f))
             return fail(MTB_INVALID_ARG, "structure %d: dt, dx must be > 0", s);
         if (S.pol == MTB_TE && S.y_pmc)
@@ -595,19 +903,20 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs, int32_t n, const mtb_
             for (int k = 0; k < 4; ++k)
                 if ((rc = check_ptr(S.psi[k][b], "psi", s))) return rc;
         }
-        if ((rc = check_ptr(S.eps_a, "eps_a", s))) return rc;
-        if (S.pol == MTB_TE && (rc = check_ptr(S.eps_b, "eps_b", s))) return rc;
+        if ((rc = check_ptr(S.inv_eps_a, "inv_eps_a", s))) return rc;
+        if (S.pol == MTB_TE && (rc = check_ptr(S.inv_eps_b, "inv_eps_b", s))) return rc;
         if (S.pol == MTB_TM && S.explicit_e && (rc = check_ptr(S.e_explicit, "e_explicit", s)))
             return rc;
         if (!S.hx_b || !S.hx_a || !S.hy_b || !S.hy_a || !S.ex_b || !S.ex_a || !S.ey_b || !S.ey_a)
             return fail(MTB_INVALID_ARG, "structure %d: null CPML profile", s);
-        const mtb_cells *cl[3] = {&S.src_e, &S.src_h1, &S.src_h2};
+        mtb_cells *cl[3] = {&S.src_e, &S.src_h1, &S.src_h2};
         for (int c = 0; c < 3; ++c) {
             if (cl[c]->n < 0) return fail(MTB_INVALID_ARG, "structure %d: negative cell count", s);
             if (cl[c]->n > 0 && (!cl[c]->row_ptr || !cl[c]->col || !cl[c]->w ||
                                  cl[c]->amp_col < 0 || cl[c]->amp_col >= n_amp_cols))
                 return fail(MTB_INVALID_ARG, "structure %d: source list %d has null arrays or "
                             "amp_col out of [0, %d)", s, c, n_amp_cols);
+            if ((rc = cell_rows(*cl[c], S.nx, s))) return rc;
         }
         if (S.pol == MTB_TE && S.src_h2.n > 0)
             return fail(MTB_INVALID_ARG, "structure %d: TE has no second magnetic source", s);
@@ -638,6 +947,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs, int32_t n, const mtb_
                 return fail(MTB_INVALID_ARG, "structure %d: full-grid ring offset %lld invalid", s,
                             (long long)o);
         }
+        if ((rc = profile_band(S.hx_b, S.hx_a, S.nx - 1, S.xband[0], S.xband[1], s))) return rc;
+        if ((rc = profile_band(S.ex_b, S.ex_a, S.nx, S.xband[2], S.xband[3], s))) return rc;
         n_work += (int64_t)((S.nx + rows - 1) / rows) * ((S.pitch + 127) / 128);
     }
     if (n_work > (1LL << 30)) return fail(MTB_INVALID_ARG, "batch too large");
@@ -649,23 +960,55 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs, int32_t n, const mtb_
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->structs_d.ensure(sizeof(mtb_yee2d_struct) * n);
     if (!rc) rc = p->work_d.ensure(sizeof(int4) * n_work);
+    if (!rc) rc = p->err_d.ensure(sizeof(int));
+    if (!rc) {
+        cudaError_t e = cudaFuncSetAttribute(k_yee2d_tm<false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_tm());
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_yee2d_tm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_tm());
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_yee2d_te, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_te());
+        if (e != cudaSuccess)
+            rc = fail(MTB_CUDA_ERROR, "shared memory attribute: %s", cudaGetErrorString(e));
+    }
     if (rc) { p->dft.release(); delete p; return rc; }
     std::vector<int4> work;
     work.reserve(n_work);
-    for (int s = 0; s < n; ++s)
-        for (int i0 = 0; i0 < structs[s].nx; i0 += rows)
-            for (int c0 = 0; c0 < structs[s].pitch; c0 += 128)
-                work.push_back(make_int4(s, i0, std::min(i0 + rows, structs[s].nx), c0));
-    cudaError_t e = cudaMemcpy(p->structs_d.p, structs, sizeof(mtb_yee2d_struct) * n,
+    for (int pol = 0; pol < 2; ++pol) {
+        if (pol == 1) p->n_work_tm = (int)work.size();
+        for (int s = 0; s < n; ++s) {
+            if (structs[s].pol != (pol == 0 ? MTB_TM : MTB_TE)) continue;
+            for (int i0 = 0; i0 < structs[s].nx; i0 += rows)
+                for (int c0 = 0; c0 < structs[s].pitch; c0 += 128)
+                    work.push_back(make_int4(s, i0, std::min(i0 + rows, structs[s].nx), c0));
+        }
+    }
+    cudaError_t e = cudaMemcpy(p->structs_d.p, structs.data(), sizeof(mtb_yee2d_struct) * n,
                                cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(p->work_d.p, work.data(), sizeof(int4) * n_work, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(p->err_d.p, 0, sizeof(int));
     if (e != cudaSuccess) {
         p->dft.release();
         delete p;
         return fail(MTB_CUDA_ERROR, "plan upload failed: %s", cudaGetErrorString(e));
     }
     *out = p;
+    return MTB_OK;
+}
+
+int mtb_yee2d_check(mtb_yee2d_plan *p, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    int flag = 0;
+    MTB_CUDA_TRY(cudaMemcpyAsync(&flag, p->err_d.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                 (cudaStream_t)stream));
+    MTB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    if (flag)
+        return fail(MTB_DEVICE_TIMEOUT, "a bounded wait for a staged row copy expired on the "
+                    "device; the affected steps are incomplete");
     return MTB_OK;
 }
 
@@ -676,12 +1019,13 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     p->last_launches = 0;
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if ((rc = mtb_yee2d_check(p, stream))) return rc;        // also orders the staging reuse
     const int nc = std::max(p->n_cols, 1);
     const size_t per = (size_t)k * nc;
-    int rc;
     if ((rc = p->amp_h.ensure(2 * per * sizeof(float)))) return rc;
     if ((rc = p->amp_d.ensure(2 * per * sizeof(float)))) return rc;
-    if ((rc = p->dft.upload_phases(t0, k, st))) return rc;   // syncs the stream first
+    if ((rc = p->dft.upload_phases(t0, k, st))) return rc;
     float *ah = p->amp_h.as<float>();
     for (size_t i = 0; i < per; ++i) {
         ah[i] = coef_e ? (float)coef_e[i] : 0.f;
@@ -690,21 +1034,36 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, p->amp_h.p, 2 * per * sizeof(float),
                                  cudaMemcpyHostToDevice, st));
     const float *ad = p->amp_d.as<float>();
-    const int blocks = (p->n_work + WARPS2D - 1) / WARPS2D;
+    const int n_tm = p->n_work_tm, n_te = p->n_work - p->n_work_tm;
+    const int blocks_tm = (n_tm + WARPS2D - 1) / WARPS2D;
+    const int blocks_te = (n_te + WARPS2D - 1) / WARPS2D;
     int slot = 0;
     for (int s = 0; s < k; ++s) {
         Ctx2D C;
         C.amp_e = ad + (size_t)s * nc;
         C.amp_h = ad + per + (size_t)s * nc;
         C.ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;
+        C.err = p->err_d.as<int>();
         C.par = p->par;
         C.first = p->first;
         if ((rc = p->timer.begin(st, 0))) return rc;
-        k_yee2d_step<<<blocks, 32 * WARPS2D, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
-                                                      p->work_d.as<int4>(), p->n_work, C);
-        MTB_CHECK_LAUNCH();
+        if (n_tm > 0) {
+            if (p->first)
+                k_yee2d_tm<true><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(
+                    p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>(), n_tm, C);
+            else
+                k_yee2d_tm<false><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(
+                    p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>(), n_tm, C);
+            MTB_CHECK_LAUNCH();
+            ++p->last_launches;
+        }
+        if (n_te > 0) {
+            k_yee2d_te<<<blocks_te, 32 * WARPS2D, smem_te(), st>>>(
+                p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>() + n_tm, n_te, C);
+            MTB_CHECK_LAUNCH();
+            ++p->last_launches;
+        }
         if ((rc = p->timer.end(st))) return rc;
-        ++p->last_launches;
         p->par ^= 1;
         p->first = 0;
         ++slot;
@@ -746,6 +1105,7 @@ void mtb_yee2d_plan_destroy(mtb_yee2d_plan *p) {
     p->structs_d.release();
     p->work_d.release();
     p->amp_d.release();
+    p->err_d.release();
     p->amp_h.release();
     p->dft.release();
     p->timer.release();

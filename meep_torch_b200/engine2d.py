@@ -262,14 +262,17 @@ class Engine2D:
                     self._pair(s.Dy, nx, P)
                 eps_a = self._pack(c.eps_x, nx, P)
                 eps_b = self._pack(c.eps_y, nx, P)
+                inv_a = self._pack(torch.reciprocal(c.eps_x.to(torch.float32)), nx, P)
+                inv_b = self._pack(torch.reciprocal(c.eps_y.to(torch.float32)), nx, P)
                 psis = [self._pair(s.psi_Hzy, nx, P, (0, 1)), self._pair(s.psi_Hzx, nx, P, (1, 0)),
                         self._pair(s.psi_Eyx, nx, P), self._pair(s.psi_Exy, nx, P)]
-                S.eps_b = L.ptr(eps_b)
-                it.keep.append(eps_b)
+                S.inv_eps_b = L.ptr(inv_b)
+                it.keep += [eps_b, inv_b]
             else:
                 f_main, f_x, f_y = self._pair(s.Dz, nx, P), self._pair(s.Hx, nx, P), \
                     self._pair(s.Hy, nx, P)
                 eps_a = self._pack(c.eps_inf, nx, P)
+                inv_a = self._pack(torch.reciprocal(c.eps_inf.to(torch.float32)), nx, P)
                 yoff = 0 if S.y_pmc else 1
                 psis = [self._pair(s.psi_Ezy, nx, P), self._pair(s.psi_Ezx, nx, P),
                         self._pair(s.psi_Hyx, nx, P, (1, yoff)),
@@ -287,7 +290,8 @@ class Engine2D:
             S.f_main[0], S.f_main[1] = L.ptr(f_main[0]), L.ptr(f_main[1])
             S.f_x[0], S.f_x[1] = L.ptr(f_x[0]), L.ptr(f_x[1])
             S.f_y[0], S.f_y[1] = L.ptr(f_y[0]), L.ptr(f_y[1])
-            S.eps_a = L.ptr(eps_a)
+            S.inv_eps_a = L.ptr(inv_a)
+            it.keep.append(inv_a)
             for k in range(4):
                 S.psi[k][0], S.psi[k][1] = L.ptr(psis[k][0]), L.ptr(psis[k][1])
             self._check_psi_outside(it)
