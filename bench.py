@@ -247,6 +247,51 @@ def run_cfg2(args, rank, world, dev):
     return res
 
 
+def run_cfg3(args, rank, world, dev):
+    """cfg3: one 256^3 structure per rank, 2000 steps per run."""
+    import torch
+
+    from meep_torch_b200 import _lib
+    from meep_torch_b200 import workloads as W
+    from meep_torch_b200.engine3d import Engine3D
+
+    lib = _lib.load()
+    n = args.n3
+    nsteps = args.run_steps if args.run_steps != 5000 else 2000
+    s, c, src, mons = W.cfg3_setup(dev, n=n)
+    eng = Engine3D(s, c, src, mons, rows_per_seg=args.rows, ring_slots=args.ring)
+    stream = torch.cuda.current_stream(dev)
+
+    def bench_step():
+        eng.reset()
+        eng.run(0, nsteps)
+
+    for _ in range(args.warmup):
+        bench_step()
+    torch.cuda.synchronize(dev)
+    eng.set_timing(True)
+    barrier(world)
+    n0 = lib.mtb_launch_count()
+    with Clocks(dev.index if dev.index is not None else 0) as clk:
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            bench_step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+    launches = lib.mtb_launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    step_ms, step_n, dft_ms, dft_n = eng.timing()
+    eng.close()
+    return dict(cells=n ** 3, nsteps=nsteps, ms=allreduce_max(ms, world, dev), launches=launches,
+                clocks=clk.summary(), step_ms=step_ms, step_n=step_n, dft_ms=dft_ms,
+                dft_n=dft_n, bytes_launch=W.cfg3_bytes_per_step(n), e2e_s=float("nan"), h2d=0,
+                d2h=0)
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -269,7 +314,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3"])
     ap.add_argument("--rows", type=int, default=0, help="rows per warp (0 = library default)")
     ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
     ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
@@ -280,6 +325,7 @@ def main():
     ap.add_argument("--run-steps", type=int, default=5000,
                     help="time steps per run (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--n3", type=int, default=256, help="cfg3 grid side")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -337,7 +383,7 @@ def main():
         B.build()
     barrier(world)
 
-    r = run_cfg2(args, rank, world, dev)
+    r = run_cfg3(args, rank, world, dev) if args.workload == "cfg3" else run_cfg2(args, rank, world, dev)
     peak, peak_kind = peaks()
     total_updates = r["cells"] * r["nsteps"] * args.steps * world
     value = total_updates / (r["ms"] / 1e3) / 1e9
