@@ -200,6 +200,31 @@ int mtb_yee2d_run(mtb_yee2d_plan *plan, int64_t t0, int32_t k,
 /* Which buffer of every ping-pong pair holds the current state (0 or 1). */
 int32_t mtb_yee2d_current(const mtb_yee2d_plan *plan);
 
+/* Run ONE 2D structure k steps without allocating anything (no counterpart
+ * in the reference). For callers that must not call cudaMalloc / cudaFree:
+ * a host that gives this library a fixed device-memory budget, or a
+ * latency-critical loop that cannot absorb cudaMalloc's implicit device
+ * synchronisation. Everything a plan would allocate (descriptor copy, work
+ * list, DFT tables, sample ring, error flag) lives in one file-scope device
+ * array of MTB_NOALLOC_SCRATCH_BYTES, which every GPU that loads the library
+ * holds until exit; a configuration that needs more is rejected with
+ * MTB_INVALID_ARG and the byte count in mtb_last_error(). The caller passes
+ * the inputs and outputs exactly as for mtb_yee2d_plan_create (struct,
+ * regions, groups; amp_col 0 is the only coefficient column) plus `parity`,
+ * the ping-pong buffer holding the current state; after the call the state is
+ * in buffer parity ^ (k & 1). The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and sets kernel attributes, so make
+ * it before any stream capture. Every call shares the one array: calls whose
+ * work overlaps on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller. The call waits for its work on `stream`
+ * before returning (it reads back the bounded-wait error flag). */
+#define MTB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_region *regions,
+                          int32_t n_regions, const mtb_phase_group *groups,
+                          int32_t n_groups, int64_t ring_slot_elems, int32_t ring_slots,
+                          int32_t parity, int64_t t0, int32_t k, const double *coef_e,
+                          const double *coef_h, void *stream);
+
 /* Waits for the plan's work on `stream` and reports a bounded device wait
  * that expired in any earlier run (MTB_DEVICE_TIMEOUT) -- the kernels never
  * spin forever; a wait that gives up sets this flag and the step returns. */

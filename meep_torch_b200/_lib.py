@@ -86,6 +86,10 @@ SIGNATURES = {
                                 C.POINTER(C.c_double), vp]),
     "mtb_yee2d_current": (C.c_int32, [vp]),
     "mtb_yee2d_check": (C.c_int, [vp, vp]),
+    "mtb_yee2d_run_noalloc": (C.c_int, [C.POINTER(Yee2DStruct), C.POINTER(DftRegion), C.c_int32,
+                                        C.POINTER(PhaseGroup), C.c_int32, C.c_int64, C.c_int32,
+                                        C.c_int32, C.c_int64, C.c_int32, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), vp]),
     "mtb_yee2d_last_launches": (C.c_int64, [vp]),
     "mtb_yee2d_plan_destroy": (None, [vp]),
     "mtb_yee2d_set_timing": (C.c_int, [vp, C.c_int32]),

@@ -1113,3 +1113,379 @@ void mtb_yee2d_plan_destroy(mtb_yee2d_plan *p) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- no-allocation run
+// mtb_yee2d_run_noalloc: the plan's scratch (descriptor copy, work list, DFT
+// tables, sample ring, error flag) is carved out of one file-scope device
+// array instead of cudaMalloc'd buffers; the tables a plan builds on the host
+// are built here by small set-up kernels. The step and contraction kernels
+// are the plan's own.
+namespace mtb {
+
+__global__ void k_dft_contract(const mtb_dft_region *__restrict__ regions,
+                               const int *__restrict__ blk_region,
+                               const int64_t *__restrict__ blk_start,
+                               const int *__restrict__ group_nf, const int *__restrict__ group_off,
+                               int total_nf, const float *__restrict__ phase, int row0, int n,
+                               const float *__restrict__ ring, int64_t slot_elems);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MTB_NOALLOC_SCRATCH_BYTES];
+constexpr int NA_MAX_DEV = 64;
+constexpr int NA_MAX_REGIONS = 64;
+constexpr int NA_MAX_GROUPS = 16;
+constexpr int NA_CT = 256;              // contraction block size (common.cu)
+static unsigned char *g_noalloc_dev[NA_MAX_DEV];   // device address of the array, per device
+
+// x-layer bands and source row ranges of the descriptor copy (what
+// mtb_yee2d_plan_create computes on the host)
+__global__ void k_na_struct(mtb_yee2d_struct *S) {
+    __shared__ int lh, hh, le, he, rlo[3], rhi[3];
+    const int nx = S->nx;
+    const int nh = nx - 1, ne = nx;
+    if (threadIdx.x == 0) {
+        lh = 0; hh = nh; le = 0; he = ne;
+        for (int c = 0; c < 3; ++c) { rlo[c] = 0x7fffffff; rhi[c] = -1; }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+        if (i < nh && (S->hx_a[i] != 0.f || S->hx_b[i] != 1.f)) {
+            if (i < nh / 2) atomicMax(&lh, i + 1); else atomicMin(&hh, i);
+        }
+        if (S->ex_a[i] != 0.f || S->ex_b[i] != 1.f) {
+            if (i < ne / 2) atomicMax(&le, i + 1); else atomicMin(&he, i);
+        }
+    }
+    const mtb_cells *cl[3] = {&S->src_e, &S->src_h1, &S->src_h2};
+    for (int c = 0; c < 3; ++c) {
+        if (cl[c]->n <= 0) continue;
+        for (int r = threadIdx.x; r < nx; r += blockDim.x)
+            if (cl[c]->row_ptr[r + 1] > cl[c]->row_ptr[r]) {
+                atomicMin(&rlo[c], r);
+                atomicMax(&rhi[c], r);
+            }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        S->xband[0] = lh; S->xband[1] = hh; S->xband[2] = le; S->xband[3] = he;
+        mtb_cells *w[3] = {&S->src_e, &S->src_h1, &S->src_h2};
+        for (int c = 0; c < 3; ++c) {
+            if (rhi[c] < 0) { w[c]->row_lo = 1; w[c]->row_hi = 0; }
+            else { w[c]->row_lo = rlo[c]; w[c]->row_hi = rhi[c]; }
+        }
+    }
+}
+
+__global__ void k_na_work(int4 *work, int nx, int rows, int nch, int n_work) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_work) return;
+    const int seg = e / nch, c = e - seg * nch;
+    const int i0 = seg * rows;
+    work[e] = make_int4(0, i0, min(i0 + rows, nx), c * 128);
+}
+
+__global__ void k_na_blk(int *blk_region, const int64_t *blk_start, int n_regions,
+                         int64_t n_blocks) {
+    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (b >= n_blocks) return;
+    int r = 0;
+    while (r + 1 < n_regions && blk_start[r + 1] <= b) ++r;
+    blk_region[b] = r;
+}
+
+// phase table rows [0, k) for steps t0 .. t0+k-1, same layout and formulas
+// as DftState::upload_phases (FP64 mode 0, reference float32 mode 1)
+__global__ void k_na_phase(float *phase, const double *freqs, const int *group_nf,
+                           const int *group_off, const double *group_dt, const int *group_mode,
+                           int n_groups, int total_nf, int64_t t0, int k) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= (int64_t)k * total_nf) return;
+    const int s = (int)(e / total_nf), fi = (int)(e - (int64_t)s * total_nf);
+    int g = 0;
+    while (g + 1 < n_groups && group_off[g + 1] <= fi) ++g;
+    const double dt = group_dt[g], fr = freqs[fi];
+    const double two_pi = 6.283185307179586;
+    float *p = phase + e * 4;
+    for (int h = 0; h < 2; ++h) {
+        const double tt = ((double)(t0 + s) + 0.5 * (h + 1)) * dt;
+        float c, sn;
+        if (group_mode[g] == 0) {
+            const double arg = two_pi * fr * tt;
+            c = (float)(dt * cos(arg));
+            sn = (float)(-dt * sin(arg));
+        } else {
+            const float arg = ((float)two_pi * (float)fr) * (float)tt;
+            c = (float)dt * cosf(arg);
+            sn = (float)dt * -sinf(arg);
+        }
+        p[2 * h] = c;
+        p[2 * h + 1] = sn;
+    }
+}
+
+__global__ void k_na_amp(float *amp, const double *coef, int k, int has_e, int has_h) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= k) return;
+    amp[s] = has_e ? (float)coef[s] : 0.f;
+    amp[k + s] = has_h ? (float)coef[k + s] : 0.f;
+}
+
+static size_t na_align(size_t n) { return (n + 255) & ~(size_t)255; }
+
+}  // namespace mtb
+
+extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_region *regions,
+                                     int32_t n_regions, const mtb_phase_group *groups,
+                                     int32_t n_groups, int64_t ring_slot_elems,
+                                     int32_t ring_slots, int32_t parity, int64_t t0, int32_t k,
+                                     const double *coef_e, const double *coef_h, void *stream) {
+    using namespace mtb;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!s) return fail(MTB_INVALID_ARG, "noalloc: structure is null");
+    if (k < 0) return fail(MTB_INVALID_ARG, "noalloc: k < 0");
+    if (parity != 0 && parity != 1) return fail(MTB_INVALID_ARG, "noalloc: parity must be 0 or 1");
+    const mtb_yee2d_struct &S = *s;
+    if (S.pol != MTB_TM && S.pol != MTB_TE)
+        return fail(MTB_INVALID_ARG, "noalloc: pol must be MTB_TM or MTB_TE");
+    if (S.nx < 3 || S.ny < 3 || S.pitch < S.ny || (S.pitch & 3) ||
+        (int64_t)S.nx * S.pitch >= (1LL << 31))
+        return fail(MTB_INVALID_ARG, "noalloc: bad extents nx=%d ny=%d pitch=%d", S.nx, S.ny,
+                    S.pitch);
+    if (!(S.dt > 0.f) || !(S.dx > 0.f)) return fail(MTB_INVALID_ARG, "noalloc: dt, dx must be > 0");
+    if (S.pol == MTB_TE && (S.y_pmc || S.src_h2.n > 0))
+        return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
+    int rc;
+    for (int b = 0; b < 2; ++b) {
+        if ((rc = check_ptr(S.f_main[b], "f_main", 0)) || (rc = check_ptr(S.f_x[b], "f_x", 0)) ||
+            (rc = check_ptr(S.f_y[b], "f_y", 0)))
+            return rc;
+        for (int q = 0; q < 4; ++q)
+            if ((rc = check_ptr(S.psi[q][b], "psi", 0))) return rc;
+    }
+    if ((rc = check_ptr(S.inv_eps_a, "inv_eps_a", 0))) return rc;
+    if (S.pol == MTB_TE && (rc = check_ptr(S.inv_eps_b, "inv_eps_b", 0))) return rc;
+    if (S.pol == MTB_TM && S.explicit_e && (rc = check_ptr(S.e_explicit, "e_explicit", 0)))
+        return rc;
+    if (!S.hx_b || !S.hx_a || !S.hy_b || !S.hy_a || !S.ex_b || !S.ex_a || !S.ey_b || !S.ey_a)
+        return fail(MTB_INVALID_ARG, "noalloc: null CPML profile");
+    const mtb_cells *cl[3] = {&S.src_e, &S.src_h1, &S.src_h2};
+    for (int c = 0; c < 3; ++c)
+        if (cl[c]->n < 0 || (cl[c]->n > 0 && (!cl[c]->row_ptr || !cl[c]->col || !cl[c]->w ||
+                                              cl[c]->amp_col != 0)))
+            return fail(MTB_INVALID_ARG, "noalloc: source list %d: null arrays or amp_col != 0", c);
+    if (S.n_lines < 0 || S.n_lines > MAXL || (S.n_lines > 0 && !S.lines))
+        return fail(MTB_INVALID_ARG, "noalloc: bad line sample list");
+    if (ring_slots < 1 || ring_slots > 64)
+        return fail(MTB_INVALID_ARG, "noalloc: ring_slots must be in [1, 64]");
+    if (n_regions == 0 && (S.n_lines > 0 || S.ring_full[0] >= 0 || S.ring_full[1] >= 0 ||
+                           S.ring_full[2] >= 0))
+        return fail(MTB_INVALID_ARG, "noalloc: samples requested but no DFT region reads them");
+    if (ring_slot_elems < 0 || (ring_slot_elems & 3))
+        return fail(MTB_INVALID_ARG, "noalloc: ring_slot_elems must be a multiple of 4");
+    for (int c = 0; c < 3; ++c) {
+        const int64_t o = S.ring_full[c];
+        if (o >= 0 && ((o & 3) || o + (int64_t)S.nx * S.pitch > ring_slot_elems))
+            return fail(MTB_INVALID_ARG, "noalloc: full-grid ring offset invalid");
+    }
+    if (S.n_lines > 0) {
+        mtb_line_sample ls[MAXL];
+        cudaError_t e = cudaMemcpy(ls, S.lines, sizeof(mtb_line_sample) * S.n_lines,
+                                   cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess)
+            return fail(MTB_CUDA_ERROR, "noalloc: reading line samples: %s", cudaGetErrorString(e));
+        for (int l = 0; l < S.n_lines; ++l) {
+            const mtb_line_sample &q = ls[l];
+            const int along = q.kind == 0 ? S.ny : S.nx, across = q.kind == 0 ? S.nx : S.ny;
+            if (q.comp < 0 || q.comp > 2 || (q.kind != 0 && q.kind != 1) || q.index < 0 ||
+                q.index >= across || q.lo < 0 || q.hi > along || q.lo >= q.hi || q.ring_off < 0 ||
+                q.ring_off + (q.hi - q.lo) > ring_slot_elems)
+                return fail(MTB_INVALID_ARG, "noalloc: line sample %d out of range", l);
+        }
+    }
+    if (n_regions < 0 || n_regions > NA_MAX_REGIONS || n_groups < 0 || n_groups > NA_MAX_GROUPS ||
+        (n_regions > 0 && (!regions || !groups)))
+        return fail(MTB_INVALID_ARG, "noalloc: at most %d regions and %d phase groups",
+                    NA_MAX_REGIONS, NA_MAX_GROUPS);
+    // phase groups and region block prefix on the stack (host)
+    int gnf[NA_MAX_GROUPS + 1], goff[NA_MAX_GROUPS + 1], gmode[NA_MAX_GROUPS + 1];
+    double gdt[NA_MAX_GROUPS + 1];
+    int total_nf = 0, maxnf = 1;
+    for (int g = 0; g < n_groups; ++g) {
+        if (groups[g].nf < 1 || groups[g].nf > 256 || !groups[g].freqs ||
+            (groups[g].mode != 0 && groups[g].mode != 1))
+            return fail(MTB_INVALID_ARG, "noalloc: phase group %d invalid", g);
+        gnf[g] = groups[g].nf;
+        goff[g] = total_nf;
+        gmode[g] = groups[g].mode;
+        gdt[g] = groups[g].dt;
+        total_nf += groups[g].nf;
+        maxnf = std::max(maxnf, groups[g].nf);
+    }
+    gnf[n_groups] = goff[n_groups] = gmode[n_groups] = 0;
+    gdt[n_groups] = 0.0;
+    goff[n_groups] = total_nf;
+    int64_t bs[NA_MAX_REGIONS + 1];
+    int64_t n_blocks = 0;
+    for (int r = 0; r < n_regions; ++r) {
+        const mtb_dft_region &R = regions[r];
+        if (R.group < 0 || R.group >= n_groups || (R.toff != 1 && R.toff != 2) || R.rows < 0 ||
+            R.cols < 0 || !R.acc || R.ring_a < 0 ||
+            R.ring_a + (int64_t)(R.rows - 1) * R.ring_pitch + R.cols > ring_slot_elems ||
+            (R.ring_b >= 0 && R.ring_b + (int64_t)(R.rows - 1) * R.ring_pitch + R.cols >
+                                  ring_slot_elems))
+            return fail(MTB_INVALID_ARG, "noalloc: region %d invalid", r);
+        bs[r] = n_blocks;
+        n_blocks += ((int64_t)R.rows * R.cols + NA_CT - 1) / NA_CT;
+    }
+    bs[n_regions] = n_blocks;
+    const int rows = 32;
+    const int nch = (S.pitch + 127) / 128;
+    const int n_work = ((S.nx + rows - 1) / rows) * nch;
+    // scratch layout
+    const size_t fixed = na_align(sizeof(mtb_yee2d_struct)) + 256 +
+                         na_align(sizeof(mtb_dft_region) * (n_regions + 1)) +
+                         na_align(sizeof(int64_t) * (n_regions + 1)) +
+                         4 * na_align(sizeof(double) * (NA_MAX_GROUPS + 1)) +
+                         na_align(sizeof(double) * (total_nf + 1)) +
+                         na_align(sizeof(int) * (n_blocks + 1)) + na_align(sizeof(int4) * n_work) +
+                         (n_regions > 0 ? na_align(sizeof(float) * (size_t)ring_slots *
+                                                   ring_slot_elems) : 0);
+    int CH = 256;
+    auto per_chunk = [&](int ch) {
+        return na_align(sizeof(double) * 2 * ch) + na_align(sizeof(float) * 2 * ch) +
+               na_align(sizeof(float) * 4 * (size_t)ch * std::max(total_nf, 1));
+    };
+    while (CH > 1 && fixed + per_chunk(CH) > MTB_NOALLOC_SCRATCH_BYTES) CH /= 2;
+    if (fixed + per_chunk(CH) > MTB_NOALLOC_SCRATCH_BYTES)
+        return fail(MTB_INVALID_ARG, "noalloc: this structure needs %zu bytes of scratch, more "
+                    "than the %zu-byte array (reduce ring_slots or the sampled region)",
+                    fixed + per_chunk(1), (size_t)MTB_NOALLOC_SCRATCH_BYTES);
+    // set-up, once per device: the array's device address and kernel attributes
+    int dev = 0;
+    MTB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEV) return fail(MTB_UNSUPPORTED, "noalloc: device ordinal %d", dev);
+    if (!g_noalloc_dev[dev]) {
+        void *p = nullptr;
+        MTB_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        MTB_CUDA_TRY(cudaFuncSetAttribute(k_yee2d_tm<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_tm()));
+        MTB_CUDA_TRY(cudaFuncSetAttribute(k_yee2d_tm<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_tm()));
+        MTB_CUDA_TRY(cudaFuncSetAttribute(k_yee2d_te, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_te()));
+        MTB_CUDA_TRY(cudaFuncSetAttribute(k_dft_contract,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(sizeof(float2) * 64 * 256)));
+        g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+    }
+    unsigned char *base = g_noalloc_dev[dev];
+    size_t off = 0;
+    auto take = [&](size_t bytes) { unsigned char *q = base + off; off += na_align(bytes); return q; };
+    mtb_yee2d_struct *dS = reinterpret_cast<mtb_yee2d_struct *>(take(sizeof(mtb_yee2d_struct)));
+    int *dErr = reinterpret_cast<int *>(take(256));
+    mtb_dft_region *dReg = reinterpret_cast<mtb_dft_region *>(
+        take(sizeof(mtb_dft_region) * (n_regions + 1)));
+    int64_t *dBs = reinterpret_cast<int64_t *>(take(sizeof(int64_t) * (n_regions + 1)));
+    int *dGnf = reinterpret_cast<int *>(take(sizeof(double) * (NA_MAX_GROUPS + 1)));
+    int *dGoff = reinterpret_cast<int *>(take(sizeof(double) * (NA_MAX_GROUPS + 1)));
+    int *dGmode = reinterpret_cast<int *>(take(sizeof(double) * (NA_MAX_GROUPS + 1)));
+    double *dGdt = reinterpret_cast<double *>(take(sizeof(double) * (NA_MAX_GROUPS + 1)));
+    double *dFreq = reinterpret_cast<double *>(take(sizeof(double) * (total_nf + 1)));
+    int *dBlk = reinterpret_cast<int *>(take(sizeof(int) * (n_blocks + 1)));
+    int4 *dWork = reinterpret_cast<int4 *>(take(sizeof(int4) * n_work));
+    float *dRing = n_regions > 0 ? reinterpret_cast<float *>(
+                                       take(sizeof(float) * (size_t)ring_slots * ring_slot_elems))
+                                 : nullptr;
+    double *dCoef = reinterpret_cast<double *>(take(sizeof(double) * 2 * CH));
+    float *dAmp = reinterpret_cast<float *>(take(sizeof(float) * 2 * CH));
+    float *dPhase = reinterpret_cast<float *>(take(sizeof(float) * 4 * (size_t)CH *
+                                                   std::max(total_nf, 1)));
+    // descriptors in; the error flag must start at zero
+    MTB_CUDA_TRY(cudaMemcpyAsync(dS, s, sizeof(mtb_yee2d_struct), cudaMemcpyHostToDevice, st));
+    MTB_CUDA_TRY(cudaMemsetAsync(dErr, 0, sizeof(int), st));
+    if (n_regions > 0) {
+        MTB_CUDA_TRY(cudaMemcpyAsync(dReg, regions, sizeof(mtb_dft_region) * n_regions,
+                                     cudaMemcpyHostToDevice, st));
+        MTB_CUDA_TRY(cudaMemcpyAsync(dBs, bs, sizeof(int64_t) * (n_regions + 1),
+                                     cudaMemcpyHostToDevice, st));
+        MTB_CUDA_TRY(cudaMemcpyAsync(dGnf, gnf, sizeof(int) * (n_groups + 1),
+                                     cudaMemcpyHostToDevice, st));
+        MTB_CUDA_TRY(cudaMemcpyAsync(dGoff, goff, sizeof(int) * (n_groups + 1),
+                                     cudaMemcpyHostToDevice, st));
+        MTB_CUDA_TRY(cudaMemcpyAsync(dGmode, gmode, sizeof(int) * (n_groups + 1),
+                                     cudaMemcpyHostToDevice, st));
+        MTB_CUDA_TRY(cudaMemcpyAsync(dGdt, gdt, sizeof(double) * (n_groups + 1),
+                                     cudaMemcpyHostToDevice, st));
+        for (int g = 0; g < n_groups; ++g)
+            MTB_CUDA_TRY(cudaMemcpyAsync(dFreq + goff[g], groups[g].freqs,
+                                         sizeof(double) * gnf[g], cudaMemcpyHostToDevice, st));
+    }
+    k_na_struct<<<1, 256, 0, st>>>(dS);
+    MTB_CHECK_LAUNCH();
+    k_na_work<<<(n_work + 255) / 256, 256, 0, st>>>(dWork, S.nx, rows, nch, n_work);
+    MTB_CHECK_LAUNCH();
+    if (n_blocks > 0) {
+        k_na_blk<<<(unsigned)((n_blocks + 255) / 256), 256, 0, st>>>(dBlk, dBs, n_regions,
+                                                                     n_blocks);
+        MTB_CHECK_LAUNCH();
+    }
+    const int blocks = (n_work + WARPS2D - 1) / WARPS2D;
+    int par = parity;
+    bool first = true;
+    for (int c0 = 0; c0 < k; c0 += CH) {
+        const int n = std::min(CH, k - c0);
+        if (coef_e)
+            MTB_CUDA_TRY(cudaMemcpyAsync(dCoef, coef_e + c0, sizeof(double) * n,
+                                         cudaMemcpyHostToDevice, st));
+        if (coef_h)
+            MTB_CUDA_TRY(cudaMemcpyAsync(dCoef + n, coef_h + c0, sizeof(double) * n,
+                                         cudaMemcpyHostToDevice, st));
+        k_na_amp<<<(n + 255) / 256, 256, 0, st>>>(dAmp, dCoef, n, coef_e != nullptr,
+                                                  coef_h != nullptr);
+        MTB_CHECK_LAUNCH();
+        if (n_regions > 0) {
+            const int64_t ne = (int64_t)n * total_nf;
+            k_na_phase<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(
+                dPhase, dFreq, dGnf, dGoff, dGdt, dGmode, n_groups, total_nf, t0 + c0, n);
+            MTB_CHECK_LAUNCH();
+        }
+        int slot = 0;
+        for (int q = 0; q < n; ++q) {
+            Ctx2D C;
+            C.amp_e = dAmp + q;
+            C.amp_h = dAmp + n + q;
+            C.ring = dRing ? dRing + (size_t)slot * ring_slot_elems : nullptr;
+            C.err = dErr;
+            C.par = par;
+            C.first = first ? 1 : 0;
+            if (S.pol == MTB_TM) {
+                if (first)
+                    k_yee2d_tm<true><<<blocks, 32 * WARPS2D, smem_tm(), st>>>(dS, dWork, n_work, C);
+                else
+                    k_yee2d_tm<false><<<blocks, 32 * WARPS2D, smem_tm(), st>>>(dS, dWork, n_work, C);
+            } else {
+                k_yee2d_te<<<blocks, 32 * WARPS2D, smem_te(), st>>>(dS, dWork, n_work, C);
+            }
+            MTB_CHECK_LAUNCH();
+            par ^= 1;
+            first = false;
+            ++slot;
+            if ((slot == ring_slots || q == n - 1) && n_regions > 0 && n_blocks > 0) {
+                k_dft_contract<<<(unsigned)n_blocks, NA_CT, sizeof(float2) * slot * maxnf, st>>>(
+                    dReg, dBlk, dBs, dGnf, dGoff, total_nf, dPhase, q + 1 - slot, slot, dRing,
+                    ring_slot_elems);
+                MTB_CHECK_LAUNCH();
+                slot = 0;
+            } else if (slot == ring_slots || q == n - 1) {
+                slot = 0;
+            }
+        }
+    }
+    int flag = 0;
+    MTB_CUDA_TRY(cudaMemcpyAsync(&flag, dErr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MTB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (flag)
+        return fail(MTB_DEVICE_TIMEOUT, "noalloc: a bounded wait for a staged row copy expired");
+    return MTB_OK;
+}

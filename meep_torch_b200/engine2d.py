@@ -424,6 +424,10 @@ class Engine2D:
             grp_arr[q].freqs = C.cast(arr, C.POINTER(C.c_double))
             grp_arr[q].nf, grp_arr[q].mode, grp_arr[q].dt = nf, self.phase_mode, dt
         self._groups = groups
+        self.regions = reg_arr           # host descriptors the plan was built from
+        self.n_regions = len(regions)
+        self.groups = grp_arr
+        self.n_groups = len(groups)
         tun = L.Tuning(rows_per_warp, ring_slots, 0, 0)
         plan = C.c_void_p()
         L.check(lib.mtb_yee2d_plan_create(structs, len(self.items), reg_arr, len(regions),
