@@ -259,7 +259,8 @@ def run_cfg3(args, rank, world, dev):
     n = args.n3
     nsteps = args.run_steps if args.run_steps != 5000 else 2000
     s, c, src, mons = W.cfg3_setup(dev, n=n)
-    eng = Engine3D(s, c, src, mons, rows_per_seg=args.rows, ring_slots=args.ring)
+    eng = Engine3D(s, c, src, mons, rows_per_seg=args.rows, ring_slots=args.ring,
+                   variant=args.variant)
     stream = torch.cuda.current_stream(dev)
 
     def bench_step():
@@ -326,6 +327,8 @@ def main():
                     help="time steps per run (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--n3", type=int, default=256, help="cfg3 grid side")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="3D kernel: 0 library default, 1 fused x-march, 2 split H / E")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

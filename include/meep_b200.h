@@ -171,10 +171,12 @@ typedef struct mtb_dft_region {
 
 /* Tuning knobs (0 = library default). */
 typedef struct mtb_tuning {
-    int32_t rows_per_warp;  /* 2D: rows one warp marches through            */
+    int32_t rows_per_warp;  /* 2D: rows one warp marches through; 3D: x planes
+                               one fused-march block covers                 */
     int32_t ring_slots;     /* steps buffered before one DFT contraction    */
     int32_t threads;        /* threads per block                            */
-    int32_t reserved;
+    int32_t variant;        /* 3D kernel: 0 default (split), 1 fused x-march,
+                               2 split H / E streaming kernels              */
 } mtb_tuning;
 
 typedef struct mtb_yee2d_plan mtb_yee2d_plan;

@@ -85,13 +85,13 @@ class FluxMonitor3D:
 
 
 def run_3d(state, coeffs, n_steps: int, *, source=None, monitors=(), phase_mode="exact",
-           rows_per_seg: int = 0, ring_slots: int = 0):
+           rows_per_seg: int = 0, ring_slots: int = 0, variant: int = 0):
     """Forward 3D run (core/monitors_3d.py:192-210) on the B200 kernels."""
     monitors = list(monitors)
     if n_steps <= 0:
         return state, [None] * len(monitors)
     eng = Engine3D(state, coeffs, source, monitors, point_sign=+1, phase_mode=phase_mode,
-                   rows_per_seg=rows_per_seg, ring_slots=ring_slots)
+                   rows_per_seg=rows_per_seg, ring_slots=ring_slots, variant=variant)
     try:
         eng.run(0, n_steps)
         return eng.state(), list(eng.accs)

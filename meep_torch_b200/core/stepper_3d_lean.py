@@ -41,10 +41,12 @@ def build_lean(nx, ny, nz, dx, eps, npml, poles=(), pole_masks=None, dtype=torch
 
 
 def run_3d_lean(c: Lean3D, n_steps: int, *, source=None, monitors=(), compile: bool = False,
-                phase_mode="exact"):
-    """``compile`` is accepted for signature parity; the kernels are already fused."""
+                phase_mode="exact", variant: int = 0):
+    """``compile`` is accepted for signature parity; the kernels are already fused.
+    ``variant`` selects the 3D kernel (0 default, 1 fused x-march, 2 split H / E)."""
     monitors = list(monitors)
-    eng = Engine3D(dict(c.F), c.coeffs, source, monitors, point_sign=-1, phase_mode=phase_mode)
+    eng = Engine3D(dict(c.F), c.coeffs, source, monitors, point_sign=-1, phase_mode=phase_mode,
+                   variant=variant)
     try:
         eng.run(0, n_steps)
         c.F = eng.state()

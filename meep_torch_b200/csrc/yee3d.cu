@@ -403,6 +403,291 @@ __global__ void __launch_bounds__(32 * NZW * (TY3 + 2)) k_yee3d_step(
     }
 }
 
+// ---------------------------------------------------------------- split H / E kernels
+// Streaming variant: one kernel advances H, a second E. A thread updates one
+// float4 of z (4 cells) of one (i, j) row; a block is 32 x 8 threads = 128 z
+// x 8 y of one x plane. Neighbours in y and x come from L1/L2 (the blocks of
+// planes i and i+1 run concurrently), z+-1 from a warp shuffle. Every load a
+// thread needs is issued before the first use of any of them: the CPML
+// memory is gated by the plan's band limits (geometry), not by the loaded
+// profile values, so a cell costs one memory round trip. DRAM traffic is
+// ~76 B per cell and step plus the CPML memory inside the layers.
+constexpr int SPLIT_Y = 8;
+
+// Index k of an axis lies in a CPML band iff k < lo or k >= hi. Superset of
+// the profile's active nodes; psi is loaded / stored there and updated only
+// where the profile is active. [axis][0 H-side, 1 E-side]
+struct Band3 {
+    int lo[3][2];
+    int hi[3][2];
+};
+__device__ __forceinline__ bool inband(const Band3 &B, int a, int h, int k) {
+    return k < B.lo[a][h] || k >= B.hi[a][h];
+}
+
+__device__ __forceinline__ void ldg4v(const float *p, float (&v)[4]) {
+    const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void one4(float (&v)[4]) { v[0] = v[1] = v[2] = v[3] = 1.f; }
+
+// CPML-corrected derivative: psi <- b psi + a d; d + psi (kappa = 1)
+__device__ __forceinline__ float cpml(bool on, float b, float a, float d, float &psi) {
+    if (!on) return d;
+    psi = b * psi + a * d;
+    return d + psi;
+}
+
+// H(n+1/2) from E(n): core/stepper_3d.py:367-393
+__global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const mtb_yee3d_struct *__restrict__ SS,
+                                                             int par, Band3 B) {
+    const mtb_yee3d_struct &S = *SS;
+    const int nx = S.nx, ny = S.ny, nz = S.nz, ZP = S.zpitch;
+    const int lane = threadIdx.x;
+    const int j = blockIdx.y * SPLIT_Y + threadIdx.y;
+    const int i = blockIdx.z;
+    const int kb = blockIdx.x * 128 + 4 * lane;
+    const bool act = j < ny && kb < ZP;
+    const int64_t NYZ = (int64_t)ny * ZP;
+    const int64_t g = (int64_t)i * NYZ + (int64_t)j * ZP + kb;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int pn = par ^ 1;
+    const bool xok = i <= nx - 2, vyH = j <= ny - 2;
+    const bool bx = xok && inband(B, 0, 0, i), by = vyH && inband(B, 1, 0, j);
+    bool bz = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bz |= kb + q <= nz - 2 && inband(B, 2, 0, kb + q);
+    const float *__restrict__ Ex = S.f[0][par];
+    const float *__restrict__ Ey = S.f[1][par];
+    const float *__restrict__ Ez = S.f[2][par];
+    float ex[4], ey[4], ez[4], ezj[4], exj[4], ezi[4], eyi[4], hx[4], hy[4], hz[4];
+    float p0[4], p1[4], p2[4], p3[4], p4[4], p5[4];
+    float eyk = 0.f, exk = 0.f;
+    z4(ex); z4(ey); z4(ez); z4(ezj); z4(exj); z4(ezi); z4(eyi);
+    z4(p0); z4(p1); z4(p2); z4(p3); z4(p4); z4(p5);
+    if (act) {
+        ldg4v(Ex + g, ex); ldg4v(Ey + g, ey); ldg4v(Ez + g, ez);
+        if (j + 1 < ny) { ldg4v(Ez + g + ZP, ezj); ldg4v(Ex + g + ZP, exj); }
+        if (i + 1 < nx) { ldg4v(Ez + g + NYZ, ezi); ldg4v(Ey + g + NYZ, eyi); }
+        if (lane == 31 && kb + 4 < ZP) { eyk = __ldg(Ey + g + 4); exk = __ldg(Ex + g + 4); }
+        ldg4v(S.f[3][par] + g, hx); ldg4v(S.f[4][par] + g, hy); ldg4v(S.f[5][par] + g, hz);
+        if (vyH && by) ld4v(S.psi[0][par] + g, p0);
+        if (vyH && bz) ld4v(S.psi[1][par] + g, p1);
+        if (xok && bz) ld4v(S.psi[2][par] + g, p2);
+        if (bx) ld4v(S.psi[3][par] + g, p3);
+        if (vyH && bx) ld4v(S.psi[4][par] + g, p4);
+        if (xok && by) ld4v(S.psi[5][par] + g, p5);
+    }
+    // profiles (tiny, cache resident)
+    float hxb = 1.f, hxa = 0.f, hyb = 1.f, hya = 0.f, hzb[4], hza[4];
+    if (bx) { hxb = __ldg(S.prof_b[0][0] + i); hxa = __ldg(S.prof_a[0][0] + i); }
+    if (by) { hyb = __ldg(S.prof_b[1][0] + j); hya = __ldg(S.prof_a[1][0] + j); }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool on = bz && kb + q <= nz - 2;
+        hzb[q] = on ? __ldg(S.prof_b[2][0] + kb + q) : 1.f;
+        hza[q] = on ? __ldg(S.prof_a[2][0] + kb + q) : 0.f;
+    }
+    {
+        const float t0 = __shfl_down_sync(0xffffffffu, ey[0], 1);   // E(k+1) of q = 3
+        const float t1 = __shfl_down_sync(0xffffffffu, ex[0], 1);
+        if (lane != 31) { eyk = t0; exk = t1; }
+    }
+    if (!act) return;
+    const bool hxA = bx && pact(hxb, hxa), hyA = by && pact(hyb, hya);
+    // Hx: valid j <= ny-2, k <= nz-2
+    if (vyH) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (kb + q > nz - 2) continue;
+            const float eyn = (q < 3) ? ey[q + 1] : eyk;
+            const float cy = cpml(hyA, hyb, hya, (ezj[q] - ez[q]) * rdx, p0[q]);
+            const float cz = cpml(pact(hzb[q], hza[q]), hzb[q], hza[q], (eyn - ey[q]) * rdx, p1[q]);
+            hx[q] = hx[q] - dt * (cy - cz);
+        }
+        if (by) st4v(S.psi[0][pn] + g, p0);
+        if (bz) st4v(S.psi[1][pn] + g, p1);
+    }
+    // Hy: valid i <= nx-2, k <= nz-2
+    if (xok) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (kb + q > nz - 2) continue;
+            const float exn = (q < 3) ? ex[q + 1] : exk;
+            const float cz = cpml(pact(hzb[q], hza[q]), hzb[q], hza[q], (exn - ex[q]) * rdx, p2[q]);
+            const float cx = cpml(hxA, hxb, hxa, (ezi[q] - ez[q]) * rdx, p3[q]);
+            hy[q] = hy[q] - dt * (cz - cx);
+        }
+        if (bz) st4v(S.psi[2][pn] + g, p2);
+        if (bx) st4v(S.psi[3][pn] + g, p3);
+    }
+    // Hz: valid i <= nx-2, j <= ny-2, all k < nz
+    if (xok && vyH) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (kb + q >= nz) continue;
+            const float cx = cpml(hxA, hxb, hxa, (eyi[q] - ey[q]) * rdx, p4[q]);
+            const float cy = cpml(hyA, hyb, hya, (exj[q] - ex[q]) * rdx, p5[q]);
+            hz[q] = hz[q] - dt * (cx - cy);
+        }
+        if (bx) st4v(S.psi[4][pn] + g, p4);
+        if (by) st4v(S.psi[5][pn] + g, p5);
+    }
+    st4v(S.f[3][pn] + g, hx);
+    st4v(S.f[4][pn] + g, hy);
+    st4v(S.f[5][pn] + g, hz);
+}
+
+// E(n+1) from H(n+1/2) (buffer par^1) and E(n) (buffer par):
+// core/stepper_3d.py:395-437, source :448-482. The E-side psi recursions run
+// over their arrays' full extent (core/stepper_3d.py:79-101 State3D shapes),
+// wider than the interior where the curl is applied (_pad_interior).
+__global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const mtb_yee3d_struct *__restrict__ SS,
+                                                             int par, const float *__restrict__ amp,
+                                                             Band3 B) {
+    const mtb_yee3d_struct &S = *SS;
+    const int nx = S.nx, ny = S.ny, nz = S.nz, ZP = S.zpitch;
+    const int lane = threadIdx.x;
+    const int j = blockIdx.y * SPLIT_Y + threadIdx.y;
+    const int i = blockIdx.z;
+    const int kb = blockIdx.x * 128 + 4 * lane;
+    const bool act = j < ny && kb < ZP;
+    const int64_t NYZ = (int64_t)ny * ZP;
+    const int64_t g = (int64_t)i * NYZ + (int64_t)j * ZP + kb;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int pn = par ^ 1;
+    const bool iin = i >= 1 && i <= nx - 2, jin = j >= 1 && j <= ny - 2;
+    const bool xok = i <= nx - 2, vyH = j <= ny - 2;
+    const bool bx = iin && inband(B, 0, 1, i), by = jin && inband(B, 1, 1, j);
+    bool bz = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = kb + q;
+        bz |= k >= 1 && k <= nz - 2 && inband(B, 2, 1, k);
+    }
+    const float *__restrict__ Hx = S.f[3][pn];
+    const float *__restrict__ Hy = S.f[4][pn];
+    const float *__restrict__ Hz = S.f[5][pn];
+    const float *__restrict__ eps = S.eps;
+    float hx[4], hy[4], hz[4], ep[4], hzm[4], hxm[4], hzp[4], hyp[4], epj[4], epi[4], en[3][4];
+    float p6[4], p7[4], p8[4], p9[4], p10[4], p11[4];
+    float hyk = 0.f, hxk = 0.f, epk = 1.f;
+    z4(hx); z4(hy); z4(hz); one4(ep); z4(hzm); z4(hxm); z4(hzp); z4(hyp); one4(epj); one4(epi);
+    z4(p6); z4(p7); z4(p8); z4(p9); z4(p10); z4(p11);
+    z4(en[0]); z4(en[1]); z4(en[2]);
+    if (act) {
+        ldg4v(Hx + g, hx); ldg4v(Hy + g, hy); ldg4v(Hz + g, hz); ldg4v(eps + g, ep);
+        if (j >= 1) { ldg4v(Hz + g - ZP, hzm); ldg4v(Hx + g - ZP, hxm); }
+        if (i >= 1) { ldg4v(Hz + g - NYZ, hzp); ldg4v(Hy + g - NYZ, hyp); }
+        if (j + 1 < ny) ldg4v(eps + g + ZP, epj);
+        if (i + 1 < nx) ldg4v(eps + g + NYZ, epi);
+        if (lane == 0 && kb >= 1) { hyk = __ldg(Hy + g - 1); hxk = __ldg(Hx + g - 1); }
+        if (lane == 31 && kb + 4 < ZP) epk = __ldg(eps + g + 4);
+        ldg4v(S.f[0][par] + g, en[0]); ldg4v(S.f[1][par] + g, en[1]); ldg4v(S.f[2][par] + g, en[2]);
+        if (xok && by) ld4v(S.psi[6][par] + g, p6);
+        if (xok && bz) ld4v(S.psi[7][par] + g, p7);
+        if (vyH && bz) ld4v(S.psi[8][par] + g, p8);
+        if (vyH && bx) ld4v(S.psi[9][par] + g, p9);
+        if (bx) ld4v(S.psi[10][par] + g, p10);
+        if (by) ld4v(S.psi[11][par] + g, p11);
+    }
+    float exb = 1.f, exa = 0.f, eyb = 1.f, eya = 0.f, ezb[4], eza[4];
+    if (bx) { exb = __ldg(S.prof_b[0][1] + i); exa = __ldg(S.prof_a[0][1] + i); }
+    if (by) { eyb = __ldg(S.prof_b[1][1] + j); eya = __ldg(S.prof_a[1][1] + j); }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = kb + q;
+        const bool on = bz && k >= 1 && k <= nz - 2;
+        ezb[q] = on ? __ldg(S.prof_b[2][1] + k) : 1.f;
+        eza[q] = on ? __ldg(S.prof_a[2][1] + k) : 0.f;
+    }
+    {
+        const float t0 = __shfl_up_sync(0xffffffffu, hy[3], 1);     // H(k-1) of q = 0
+        const float t1 = __shfl_up_sync(0xffffffffu, hx[3], 1);
+        const float t2 = __shfl_down_sync(0xffffffffu, ep[0], 1);   // eps(k+1) of q = 3
+        if (lane != 0) { hyk = t0; hxk = t1; }
+        if (lane != 31) epk = t2;
+    }
+    if (!act) return;
+    const bool exA = bx && pact(exb, exa), eyA = by && pact(eyb, eya);
+    // Ex: valid i <= nx-2
+    if (xok) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = kb + q;
+            if (k >= nz) continue;
+            const float hym = (q == 0) ? hyk : hy[q - 1];
+            const float cy = cpml(eyA, eyb, eya, (hz[q] - hzm[q]) * rdx, p6[q]);
+            const float cz = cpml(pact(ezb[q], eza[q]), ezb[q], eza[q], (hy[q] - hym) * rdx, p7[q]);
+            const float curl = (jin && k >= 1 && k <= nz - 2) ? (cy - cz) : 0.f;
+            const float e_x = 0.5f * (ep[q] + epi[q]);
+            en[0][q] = (en[0][q] * e_x + dt * curl) / e_x;
+        }
+        if (by) st4v(S.psi[6][pn] + g, p6);
+        if (bz) st4v(S.psi[7][pn] + g, p7);
+    }
+    // Ey: valid j <= ny-2
+    if (vyH) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = kb + q;
+            if (k >= nz) continue;
+            const float hxkm = (q == 0) ? hxk : hx[q - 1];
+            const float cz = cpml(pact(ezb[q], eza[q]), ezb[q], eza[q], (hx[q] - hxkm) * rdx, p8[q]);
+            const float cx = cpml(exA, exb, exa, (hz[q] - hzp[q]) * rdx, p9[q]);
+            const float curl = (iin && k >= 1 && k <= nz - 2) ? (cz - cx) : 0.f;
+            const float e_y = 0.5f * (ep[q] + epj[q]);
+            en[1][q] = (en[1][q] * e_y + dt * curl) / e_y;
+        }
+        if (bz) st4v(S.psi[8][pn] + g, p8);
+        if (bx) st4v(S.psi[9][pn] + g, p9);
+    }
+    // Ez: valid k <= nz-2
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (kb + q > nz - 2) continue;
+        const float cx = cpml(exA, exb, exa, (hy[q] - hyp[q]) * rdx, p10[q]);
+        const float cy = cpml(eyA, eyb, eya, (hx[q] - hxm[q]) * rdx, p11[q]);
+        const float curl = (iin && jin) ? (cx - cy) : 0.f;
+        const float e_z = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
+        en[2][q] = (en[2][q] * e_z + dt * curl) / e_z;
+    }
+    if (bx) st4v(S.psi[10][pn] + g, p10);
+    if (by) st4v(S.psi[11][pn] + g, p11);
+    // soft current cells of row (i, j) on component src_comp
+    if (S.src.n > 0) {
+        const int r = i * ny + j;
+        const int e0 = __ldg(S.src.row_ptr + r), e1x = __ldg(S.src.row_ptr + r + 1);
+        if (e0 < e1x) {
+            const int c = S.src_comp;
+            const float a = __ldg(amp + S.src.amp_col);
+            const float sgn = S.src_is_point ? (float)S.point_sign : -1.f;
+            for (int e = e0; e < e1x; ++e) {
+                const int kq = __ldg(S.src.col + e) - kb;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (kq != q) continue;
+                    float epn;
+                    if (c == 0) epn = epi[q];
+                    else if (c == 1) epn = epj[q];
+                    else epn = (q < 3) ? ep[q + 1] : epk;
+                    const float ecomp = 0.5f * (ep[q] + epn);
+                    const float v = a * __ldg(S.src.w + e);
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {     // static component index
+                        if (cc != c) continue;
+                        if (S.src_is_point) en[cc][q] += sgn * (v * (1.0f / ecomp));
+                        else en[cc][q] -= v / ecomp;
+                    }
+                }
+            }
+        }
+    }
+    st4v(S.f[0][pn] + g, en[0]);
+    st4v(S.f[1][pn] + g, en[1]);
+    st4v(S.f[2][pn] + g, en[2]);
+}
+
 // Copy the plane samples of the (new) state into one ring slot.
 __global__ void k_sample3d(const mtb_yee3d_struct *__restrict__ SS, const int64_t *__restrict__ pstart,
                            int n_planes, int cur, float *__restrict__ ring) {
@@ -437,6 +722,8 @@ struct mtb_yee3d_plan {
     HostBuf amp_h;
     int rows = 32;
     int nzw = 1;
+    int variant = 2;               // 1 fused x-march, 2 split H / E
+    Band3 band{};
     int par = 0;
     int n_planes = 0;
     int64_t n_samples = 0;
@@ -445,6 +732,22 @@ struct mtb_yee3d_plan {
     DftState dft;
     LaunchTimer timer;
 };
+
+// CPML band limits of one profile (device arrays of length len): every
+// active node k (a != 0 or b != 1) satisfies k < lo or k >= hi.
+static int profile_band3(const float *b_d, const float *a_d, int len, int &lo, int &hi) {
+    std::vector<float> b(len), a(len);
+    cudaError_t e = cudaMemcpy(b.data(), b_d, sizeof(float) * len, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(a.data(), a_d, sizeof(float) * len, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(MTB_CUDA_ERROR, "reading CPML profile: %s", cudaGetErrorString(e));
+    lo = 0;
+    hi = len;
+    for (int k = 0; k < len / 2; ++k)
+        if (a[k] != 0.f || b[k] != 1.f) lo = k + 1;
+    for (int k = len - 1; k >= len / 2; --k)
+        if (a[k] != 0.f || b[k] != 1.f) hi = k;
+    return MTB_OK;
+}
 
 template <int NZW>
 static int launch3d(mtb_yee3d_plan *p, Ctx3D C, cudaStream_t st) {
@@ -475,8 +778,12 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
         return fail(MTB_INVALID_ARG, "nx, ny, nz must be >= 3");
     if (S.zpitch < S.nz || (S.zpitch & 3))
         return fail(MTB_INVALID_ARG, "zpitch %d must be >= nz and a multiple of 4", S.zpitch);
-    if (S.zpitch > 128 * MAXNZ)
-        return fail(MTB_UNSUPPORTED, "zpitch %d > %d not supported", S.zpitch, 128 * MAXNZ);
+    const int variant = (tuning && tuning->variant == 1) ? 1 : 2;
+    if (variant == 1 && S.zpitch > 128 * MAXNZ)
+        return fail(MTB_UNSUPPORTED, "fused kernel: zpitch %d > %d not supported", S.zpitch,
+                    128 * MAXNZ);
+    if (variant == 2 && (S.nx > 65535 || (S.ny + SPLIT_Y - 1) / SPLIT_Y > 65535))
+        return fail(MTB_UNSUPPORTED, "split kernels: nx <= 65535 and ny <= %d", 65535 * SPLIT_Y);
     if ((int64_t)S.nx * S.ny * S.zpitch >= (1LL << 34))
         return fail(MTB_UNSUPPORTED, "grid too large");
     if ((int64_t)S.nx * S.ny >= (1LL << 31)) return fail(MTB_UNSUPPORTED, "nx*ny too large");
@@ -509,6 +816,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     mtb_yee3d_plan *p = new mtb_yee3d_plan();
     p->s = S;
     p->rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
+    p->variant = variant;
     const int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     p->nzw = (S.zpitch + 127) / 128;
     p->smem = sizeof(float) * (size_t)(S.zpitch + 4) * (4 * (TY3 + 2) + 3 * (TY3 + 1));
@@ -516,7 +824,14 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->s_d.ensure(sizeof(mtb_yee3d_struct));
     if (!rc) rc = p->pstart_d.ensure(sizeof(int64_t) * (S.n_planes + 1));
-    if (!rc) {
+    if (!rc && variant == 2) {
+        const int dims[3] = {S.nx, S.ny, S.nz};
+        for (int a = 0; a < 3 && !rc; ++a)
+            for (int h = 0; h < 2 && !rc; ++h)
+                rc = profile_band3(S.prof_b[a][h], S.prof_a[a][h], dims[a] - 1 + h,
+                                   p->band.lo[a][h], p->band.hi[a][h]);
+    }
+    if (!rc && variant == 1) {
         switch (p->nzw) {
             case 1: rc = set_smem3d<1>(p->smem); break;
             case 2: rc = set_smem3d<2>(p->smem); break;
@@ -582,15 +897,26 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
         C.amp = p->amp_d.as<float>() + s;
         C.par = p->par;
         if ((rc = p->timer.begin(st, 0))) return rc;
-        switch (p->nzw) {
-            case 1: rc = launch3d<1>(p, C, st); break;
-            case 2: rc = launch3d<2>(p, C, st); break;
-            case 3: rc = launch3d<3>(p, C, st); break;
-            default: rc = launch3d<4>(p, C, st); break;
+        if (p->variant == 1) {
+            switch (p->nzw) {
+                case 1: rc = launch3d<1>(p, C, st); break;
+                case 2: rc = launch3d<2>(p, C, st); break;
+                case 3: rc = launch3d<3>(p, C, st); break;
+                default: rc = launch3d<4>(p, C, st); break;
+            }
+            if (rc) return rc;
+            ++p->last_launches;
+        } else {
+            const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, p->s.nx);
+            const dim3 block(32, SPLIT_Y);
+            k_yee3d_h<<<grid, block, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(), p->par, p->band);
+            MTB_CHECK_LAUNCH();
+            k_yee3d_e<<<grid, block, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(), p->par, C.amp,
+                                              p->band);
+            MTB_CHECK_LAUNCH();
+            p->last_launches += 2;
         }
-        if (rc) return rc;
         if ((rc = p->timer.end(st))) return rc;
-        ++p->last_launches;
         p->par ^= 1;
         if (sampling) {
             float *ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;

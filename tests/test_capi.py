@@ -73,7 +73,11 @@ def test_plan_validation_errors(lib):
     s3.nx, s3.ny, s3.nz, s3.zpitch = 10, 10, 10, 10
     assert lib.mtb_yee3d_plan_create(C.byref(s3), None, 0, None, 0, 0, None,
                                      C.byref(plan)) == L.MTB_INVALID_ARG
-    s3.zpitch = 1024
+    s3.zpitch = 1024                              # the fused kernel holds z <= 512
+    fused = L.Tuning(0, 0, 0, 1)
+    assert lib.mtb_yee3d_plan_create(C.byref(s3), None, 0, None, 0, 0, C.byref(fused),
+                                     C.byref(plan)) == L.MTB_UNSUPPORTED
+    s3.nx = 70000                                 # split kernels: nx is a grid dimension
     assert lib.mtb_yee3d_plan_create(C.byref(s3), None, 0, None, 0, 0, None,
                                      C.byref(plan)) == L.MTB_UNSUPPORTED
     assert lib.mtb_yee2d_run(None, 0, 1, None, None, None) == L.MTB_INVALID_ARG

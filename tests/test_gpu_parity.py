@@ -129,7 +129,7 @@ def test_te_matches_reference():
     assert not bad, bad
 
 
-def _run3d(lean):
+def _run3d(lean, variant=0):
     from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D, run_3d
     from meep_torch_b200.core.sources import GaussianPulse
     from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
@@ -152,18 +152,20 @@ def _run3d(lean):
     src = PointSource3D(dt, "Ez", i, j, k, prof)
     mons = [FluxMonitor3D(dt, freqs, normal=a, idx=idx, win=win) for a, idx in faces]
     if lean:
-        view, accs = run_3d_lean(c, int(g["n_steps"]), source=src, monitors=mons)
+        view, accs = run_3d_lean(c, int(g["n_steps"]), source=src, monitors=mons,
+                                 variant=variant)
         st = {kk: getattr(view, kk) for kk in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
     else:
         s, accs = run_3d(init_3d_state(nx, ny, nz, npml=npml, device=dev()), c,
-                         int(g["n_steps"]), source=src, monitors=mons)
+                         int(g["n_steps"]), source=src, monitors=mons, variant=variant)
         st = s._asdict()
     return st, accs, mons, dx
 
 
+@pytest.mark.parametrize("variant", [1, 2])
 @pytest.mark.parametrize("lean", [False, True])
-def test_3d_matches_reference(lean):
-    st, accs, mons, dx = _run3d(lean)
+def test_3d_matches_reference(lean, variant):
+    st, accs, mons, dx = _run3d(lean, variant)
     name = "3d_lean" if lean else "3d"
     e32, e64 = {}, {}
     for prec, errs in (("f32", e32), ("f64", e64)):
@@ -317,3 +319,44 @@ def test_energy_conserved_in_pec_box():
         s, _ = run_tm(s, m, 99)
     u = np.array(us)
     assert (u.max() - u.min()) / u.mean() < 1e-4
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_3d_wide_z_matches_oracle(variant):
+    """z extent 300 (three 128-column blocks, a partial last one) with the
+    point source and a z flux face on a block boundary, CPML on all faces."""
+    from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D, run_3d
+    from meep_torch_b200.core.sources import GaussianPulse
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    nx, ny, nz, dx, npml, n = 14, 13, 300, 0.05, 4, 60
+    rng = np.random.default_rng(11)
+    eps = (1.0 + 3.0 * rng.random((nx, ny, nz))).astype(np.float32)
+    c = build_3d_coeffs(nx, ny, nz, dx, eps=torch.from_numpy(eps), npml=npml, device=dev())
+    freqs = [0.8, 1.1]
+    prof = GaussianPulse(1.0, 2.0)
+    src = PointSource3D(c.dt, "Ez", 7, 6, 128, prof)
+    mons = [FluxMonitor3D(c.dt, freqs, normal="z", idx=127, win=(2, 12, 2, 11)),
+            FluxMonitor3D(c.dt, freqs, normal="x", idx=8, win=(2, 11, 100, 260))]
+    oc = O.coeffs_3d(nx, ny, nz, dx, eps=eps, npml=npml, dtype=np.float32)
+    s0 = O.state_3d(oc)
+    for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):      # random start: waves in every layer
+        s0[k] = rng.standard_normal(s0[k].shape).astype(np.float32)
+    init = init_3d_state(nx, ny, nz, npml=npml, device=dev())
+    init = init._replace(**{k: torch.from_numpy(s0[k]).to(dev())
+                            for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
+    st, accs = run_3d(init, c, n, source=src, monitors=mons, variant=variant)
+    dt = oc["dt"]
+    om = [lambda s, t: O.flux3d_sample(s, t, dt, freqs, "z", 127, (2, 12, 2, 11)),
+          lambda s, t: O.flux3d_sample(s, t, dt, freqs, "x", 8, (2, 11, 100, 260))]
+    oprof = O.gaussian_pulse(1.0, 2.0)
+    os_, oacc = O.run_3d(s0, oc, n, amp_fn=lambda t: oprof(O.src_time(t, dt)),
+                         src=("Ez", 7, 6, 128), monitors=om)
+    errs = {}
+    sd = st._asdict()
+    for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "psi_Hy_z", "psi_Ex_z", "psi_Hz_x",
+              "psi_Ez_y", "psi_Hx_y", "psi_Ey_x"):
+        errs[k] = rel_l2(sd[k].cpu().numpy(), os_[k])
+    for q in range(2):
+        errs[f"acc_{q}"] = rel_l2(accs[q].cpu().numpy(), oacc[q])
+    bad = {k: v for k, v in errs.items() if not v < TOL}
+    assert not bad, bad
