@@ -407,16 +407,23 @@ __global__ void __launch_bounds__(32 * NZW * (TY3 + 2)) k_yee3d_step(
 // Streaming variant: one kernel advances H, a second E. A thread updates one
 // float4 of z (4 cells) of one (i, j) row; a block is 32 x 8 threads = 128 z
 // x 8 y of one x plane. Neighbours in y and x come from L1/L2 (the blocks of
-// planes i and i+1 run concurrently), z+-1 from a warp shuffle. Every load a
-// thread needs is issued before the first use of any of them: the CPML
-// memory is gated by the plan's band limits (geometry), not by the loaded
-// profile values, so a cell costs one memory round trip. DRAM traffic is
-// ~76 B per cell and step plus the CPML memory inside the layers.
+// planes i and i+1 run concurrently), z+-1 from a warp shuffle.
+//  * Every load a thread needs is issued before the first use of any: the
+//    CPML memory is gated by the plan's band limits (geometry), not by the
+//    loaded profile values, so a cell costs one memory round trip.
+//  * The arithmetic is uniform across lanes: outside the layers the CPML
+//    terms run with (b, a) = (1, 0) on psi = 0, which is the reference's own
+//    arithmetic there, and the edge rules are selects, so a warp that holds
+//    both layer and interior cells does not diverge.
+//  * All pointers of one parity are resolved on the host into a by-value
+//    parameter block (no pointer loads in the kernel).
+// DRAM traffic is ~76 B per cell and step plus the CPML memory in the layers.
 constexpr int SPLIT_Y = 8;
 
 // Index k of an axis lies in a CPML band iff k < lo or k >= hi. Superset of
-// the profile's active nodes; psi is loaded / stored there and updated only
-// where the profile is active. [axis][0 H-side, 1 E-side]
+// the profile's active nodes; psi is loaded / stored there and updated with
+// the profile's (b, a), which are (1, 0) on inactive nodes.
+// [axis][0 H-side, 1 E-side]
 struct Band3 {
     int lo[3][2];
     int hi[3][2];
@@ -425,68 +432,76 @@ __device__ __forceinline__ bool inband(const Band3 &B, int a, int h, int k) {
     return k < B.lo[a][h] || k >= B.hi[a][h];
 }
 
+// One parity's pointers and sizes for the split kernels.
+struct Split3 {
+    const float *e[3];          // E(n)
+    float *eo[3];               // E(n+1)
+    const float *h[3];          // H(n-1/2)
+    float *ho[3];               // H(n+1/2): written by the H kernel, read by the E kernel
+    const float *pi[12];        // psi in
+    float *po[12];              // psi out
+    const float *eps;
+    const float *pb[3][2];      // CPML b, a: [axis][0 H-side (n-1 nodes), 1 E-side (n nodes)]
+    const float *pa[3][2];
+    const int32_t *src_row;
+    const int32_t *src_col;
+    const float *src_w;
+    int src_n, src_comp, src_is_point, point_sign;
+    int nx, ny, nz, zp;
+    float dt, rdx;
+    Band3 B;
+};
+
 __device__ __forceinline__ void ldg4v(const float *p, float (&v)[4]) {
     const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
     v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
 }
 __device__ __forceinline__ void one4(float (&v)[4]) { v[0] = v[1] = v[2] = v[3] = 1.f; }
 
-// CPML-corrected derivative: psi <- b psi + a d; d + psi (kappa = 1)
-__device__ __forceinline__ float cpml(bool on, float b, float a, float d, float &psi) {
-    if (!on) return d;
-    psi = b * psi + a * d;
-    return d + psi;
-}
-
 // H(n+1/2) from E(n): core/stepper_3d.py:367-393
-__global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const mtb_yee3d_struct *__restrict__ SS,
-                                                             int par, Band3 B) {
-    const mtb_yee3d_struct &S = *SS;
-    const int nx = S.nx, ny = S.ny, nz = S.nz, ZP = S.zpitch;
+__global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_constant__ Split3 P,
+                                                             int i0) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz, ZP = P.zp;
     const int lane = threadIdx.x;
     const int j = blockIdx.y * SPLIT_Y + threadIdx.y;
-    const int i = blockIdx.z;
+    const int i = i0 + blockIdx.z;
     const int kb = blockIdx.x * 128 + 4 * lane;
     const bool act = j < ny && kb < ZP;
-    const int64_t NYZ = (int64_t)ny * ZP;
-    const int64_t g = (int64_t)i * NYZ + (int64_t)j * ZP + kb;
-    const float dt = S.dt, rdx = 1.0f / S.dx;
-    const int pn = par ^ 1;
+    const uint32_t NYZ = (uint32_t)ny * ZP;       // box < 2^31 elements (plan check)
+    const uint32_t g = (uint32_t)i * NYZ + (uint32_t)(j * ZP + kb);
+    const float dt = P.dt, rdx = P.rdx;
     const bool xok = i <= nx - 2, vyH = j <= ny - 2;
-    const bool bx = xok && inband(B, 0, 0, i), by = vyH && inband(B, 1, 0, j);
+    const bool bx = xok && inband(P.B, 0, 0, i), by = vyH && inband(P.B, 1, 0, j);
     bool bz = false;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) bz |= kb + q <= nz - 2 && inband(B, 2, 0, kb + q);
-    const float *__restrict__ Ex = S.f[0][par];
-    const float *__restrict__ Ey = S.f[1][par];
-    const float *__restrict__ Ez = S.f[2][par];
+    for (int q = 0; q < 4; ++q) bz |= kb + q <= nz - 2 && inband(P.B, 2, 0, kb + q);
     float ex[4], ey[4], ez[4], ezj[4], exj[4], ezi[4], eyi[4], hx[4], hy[4], hz[4];
     float p0[4], p1[4], p2[4], p3[4], p4[4], p5[4];
     float eyk = 0.f, exk = 0.f;
-    z4(ex); z4(ey); z4(ez); z4(ezj); z4(exj); z4(ezi); z4(eyi);
+    z4(ex); z4(ey); z4(ez); z4(ezj); z4(exj); z4(ezi); z4(eyi); z4(hx); z4(hy); z4(hz);
     z4(p0); z4(p1); z4(p2); z4(p3); z4(p4); z4(p5);
     if (act) {
-        ldg4v(Ex + g, ex); ldg4v(Ey + g, ey); ldg4v(Ez + g, ez);
-        if (j + 1 < ny) { ldg4v(Ez + g + ZP, ezj); ldg4v(Ex + g + ZP, exj); }
-        if (i + 1 < nx) { ldg4v(Ez + g + NYZ, ezi); ldg4v(Ey + g + NYZ, eyi); }
-        if (lane == 31 && kb + 4 < ZP) { eyk = __ldg(Ey + g + 4); exk = __ldg(Ex + g + 4); }
-        ldg4v(S.f[3][par] + g, hx); ldg4v(S.f[4][par] + g, hy); ldg4v(S.f[5][par] + g, hz);
-        if (vyH && by) ld4v(S.psi[0][par] + g, p0);
-        if (vyH && bz) ld4v(S.psi[1][par] + g, p1);
-        if (xok && bz) ld4v(S.psi[2][par] + g, p2);
-        if (bx) ld4v(S.psi[3][par] + g, p3);
-        if (vyH && bx) ld4v(S.psi[4][par] + g, p4);
-        if (xok && by) ld4v(S.psi[5][par] + g, p5);
+        ldg4v(P.e[0] + g, ex); ldg4v(P.e[1] + g, ey); ldg4v(P.e[2] + g, ez);
+        if (j + 1 < ny) { ldg4v(P.e[2] + g + ZP, ezj); ldg4v(P.e[0] + g + ZP, exj); }
+        if (i + 1 < nx) { ldg4v(P.e[2] + g + NYZ, ezi); ldg4v(P.e[1] + g + NYZ, eyi); }
+        if (lane == 31 && kb + 4 < ZP) { eyk = __ldg(P.e[1] + g + 4); exk = __ldg(P.e[0] + g + 4); }
+        ldg4v(P.h[0] + g, hx); ldg4v(P.h[1] + g, hy); ldg4v(P.h[2] + g, hz);
+        if (by) ld4v(P.pi[0] + g, p0);
+        if (vyH && bz) ld4v(P.pi[1] + g, p1);
+        if (xok && bz) ld4v(P.pi[2] + g, p2);
+        if (bx) ld4v(P.pi[3] + g, p3);
+        if (vyH && bx) ld4v(P.pi[4] + g, p4);
+        if (xok && by) ld4v(P.pi[5] + g, p5);
     }
-    // profiles (tiny, cache resident)
+    // profiles (tiny, cache resident); (1, 0) outside the bands
     float hxb = 1.f, hxa = 0.f, hyb = 1.f, hya = 0.f, hzb[4], hza[4];
-    if (bx) { hxb = __ldg(S.prof_b[0][0] + i); hxa = __ldg(S.prof_a[0][0] + i); }
-    if (by) { hyb = __ldg(S.prof_b[1][0] + j); hya = __ldg(S.prof_a[1][0] + j); }
+    if (bx) { hxb = __ldg(P.pb[0][0] + i); hxa = __ldg(P.pa[0][0] + i); }
+    if (by) { hyb = __ldg(P.pb[1][0] + j); hya = __ldg(P.pa[1][0] + j); }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const bool on = bz && kb + q <= nz - 2;
-        hzb[q] = on ? __ldg(S.prof_b[2][0] + kb + q) : 1.f;
-        hza[q] = on ? __ldg(S.prof_a[2][0] + kb + q) : 0.f;
+        hzb[q] = on ? __ldg(P.pb[2][0] + kb + q) : 1.f;
+        hza[q] = on ? __ldg(P.pa[2][0] + kb + q) : 0.f;
     }
     {
         const float t0 = __shfl_down_sync(0xffffffffu, ey[0], 1);   // E(k+1) of q = 3
@@ -494,87 +509,90 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const mtb_yee3d_str
         if (lane != 31) { eyk = t0; exk = t1; }
     }
     if (!act) return;
-    const bool hxA = bx && pact(hxb, hxa), hyA = by && pact(hyb, hya);
-    // Hx: valid j <= ny-2, k <= nz-2
-    if (vyH) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (kb + q > nz - 2) continue;
-            const float eyn = (q < 3) ? ey[q + 1] : eyk;
-            const float cy = cpml(hyA, hyb, hya, (ezj[q] - ez[q]) * rdx, p0[q]);
-            const float cz = cpml(pact(hzb[q], hza[q]), hzb[q], hza[q], (eyn - ey[q]) * rdx, p1[q]);
-            hx[q] = hx[q] - dt * (cy - cz);
+    for (int q = 0; q < 4; ++q) {
+        const bool vz = kb + q <= nz - 2, vzE = kb + q < nz;
+        const float eyn = (q < 3) ? ey[q + 1] : eyk;
+        const float exn = (q < 3) ? ex[q + 1] : exk;
+        // Hx: valid j <= ny-2, k <= nz-2
+        {
+            const float dy = (ezj[q] - ez[q]) * rdx, dz = (eyn - ey[q]) * rdx;
+            const float qy = hyb * p0[q] + hya * dy, qz = hzb[q] * p1[q] + hza[q] * dz;
+            const bool v = vyH && vz;
+            const float hn = hx[q] - dt * ((dy + qy) - (dz + qz));
+            hx[q] = v ? hn : hx[q];
+            p0[q] = v ? qy : p0[q];
+            p1[q] = v ? qz : p1[q];
         }
-        if (by) st4v(S.psi[0][pn] + g, p0);
-        if (bz) st4v(S.psi[1][pn] + g, p1);
-    }
-    // Hy: valid i <= nx-2, k <= nz-2
-    if (xok) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (kb + q > nz - 2) continue;
-            const float exn = (q < 3) ? ex[q + 1] : exk;
-            const float cz = cpml(pact(hzb[q], hza[q]), hzb[q], hza[q], (exn - ex[q]) * rdx, p2[q]);
-            const float cx = cpml(hxA, hxb, hxa, (ezi[q] - ez[q]) * rdx, p3[q]);
-            hy[q] = hy[q] - dt * (cz - cx);
+        // Hy: valid i <= nx-2, k <= nz-2
+        {
+            const float dz = (exn - ex[q]) * rdx, dx = (ezi[q] - ez[q]) * rdx;
+            const float qz = hzb[q] * p2[q] + hza[q] * dz, qx = hxb * p3[q] + hxa * dx;
+            const bool v = xok && vz;
+            const float hn = hy[q] - dt * ((dz + qz) - (dx + qx));
+            hy[q] = v ? hn : hy[q];
+            p2[q] = v ? qz : p2[q];
+            p3[q] = v ? qx : p3[q];
         }
-        if (bz) st4v(S.psi[2][pn] + g, p2);
-        if (bx) st4v(S.psi[3][pn] + g, p3);
-    }
-    // Hz: valid i <= nx-2, j <= ny-2, all k < nz
-    if (xok && vyH) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (kb + q >= nz) continue;
-            const float cx = cpml(hxA, hxb, hxa, (eyi[q] - ey[q]) * rdx, p4[q]);
-            const float cy = cpml(hyA, hyb, hya, (exj[q] - ex[q]) * rdx, p5[q]);
-            hz[q] = hz[q] - dt * (cx - cy);
+        // Hz: valid i <= nx-2, j <= ny-2, k < nz
+        {
+            const float dx = (eyi[q] - ey[q]) * rdx, dy = (exj[q] - ex[q]) * rdx;
+            const float qx = hxb * p4[q] + hxa * dx, qy = hyb * p5[q] + hya * dy;
+            const bool v = xok && vyH && vzE;
+            const float hn = hz[q] - dt * ((dx + qx) - (dy + qy));
+            hz[q] = v ? hn : hz[q];
+            p4[q] = v ? qx : p4[q];
+            p5[q] = v ? qy : p5[q];
         }
-        if (bx) st4v(S.psi[4][pn] + g, p4);
-        if (by) st4v(S.psi[5][pn] + g, p5);
     }
-    st4v(S.f[3][pn] + g, hx);
-    st4v(S.f[4][pn] + g, hy);
-    st4v(S.f[5][pn] + g, hz);
+    st4v(P.ho[0] + g, hx);
+    st4v(P.ho[1] + g, hy);
+    st4v(P.ho[2] + g, hz);
+    if (by) st4v(P.po[0] + g, p0);
+    if (vyH && bz) st4v(P.po[1] + g, p1);
+    if (xok && bz) st4v(P.po[2] + g, p2);
+    if (bx) st4v(P.po[3] + g, p3);
+    if (vyH && bx) st4v(P.po[4] + g, p4);
+    if (xok && by) st4v(P.po[5] + g, p5);
 }
 
-// E(n+1) from H(n+1/2) (buffer par^1) and E(n) (buffer par):
-// core/stepper_3d.py:395-437, source :448-482. The E-side psi recursions run
-// over their arrays' full extent (core/stepper_3d.py:79-101 State3D shapes),
-// wider than the interior where the curl is applied (_pad_interior).
-__global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const mtb_yee3d_struct *__restrict__ SS,
-                                                             int par, const float *__restrict__ amp,
-                                                             Band3 B) {
-    const mtb_yee3d_struct &S = *SS;
-    const int nx = S.nx, ny = S.ny, nz = S.nz, ZP = S.zpitch;
+// E(n+1) from H(n+1/2) and E(n): core/stepper_3d.py:395-437, source
+// :448-482. The E-side psi recursions run over their arrays' full extent
+// (core/stepper_3d.py:79-101 State3D shapes), wider than the interior where
+// the curl is applied (_pad_interior). E(n+1) = E(n) + dt curl / eps_c with a
+// fast (2 ulp) divide; the reference's (E eps + dt curl) / eps differs by
+// rounding only.
+__global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_constant__ Split3 P,
+                                                             const float *__restrict__ amp, int i0) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz, ZP = P.zp;
     const int lane = threadIdx.x;
     const int j = blockIdx.y * SPLIT_Y + threadIdx.y;
-    const int i = blockIdx.z;
+    const int i = i0 + blockIdx.z;
     const int kb = blockIdx.x * 128 + 4 * lane;
     const bool act = j < ny && kb < ZP;
-    const int64_t NYZ = (int64_t)ny * ZP;
-    const int64_t g = (int64_t)i * NYZ + (int64_t)j * ZP + kb;
-    const float dt = S.dt, rdx = 1.0f / S.dx;
-    const int pn = par ^ 1;
+    const uint32_t NYZ = (uint32_t)ny * ZP;       // box < 2^31 elements (plan check)
+    const uint32_t g = (uint32_t)i * NYZ + (uint32_t)(j * ZP + kb);
+    const float dt = P.dt, rdx = P.rdx;
     const bool iin = i >= 1 && i <= nx - 2, jin = j >= 1 && j <= ny - 2;
     const bool xok = i <= nx - 2, vyH = j <= ny - 2;
-    const bool bx = iin && inband(B, 0, 1, i), by = jin && inband(B, 1, 1, j);
+    const bool bx = iin && inband(P.B, 0, 1, i), by = jin && inband(P.B, 1, 1, j);
     bool bz = false;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int k = kb + q;
-        bz |= k >= 1 && k <= nz - 2 && inband(B, 2, 1, k);
+        bz |= k >= 1 && k <= nz - 2 && inband(P.B, 2, 1, k);
     }
-    const float *__restrict__ Hx = S.f[3][pn];
-    const float *__restrict__ Hy = S.f[4][pn];
-    const float *__restrict__ Hz = S.f[5][pn];
-    const float *__restrict__ eps = S.eps;
+    const float *__restrict__ Hx = P.ho[0];
+    const float *__restrict__ Hy = P.ho[1];
+    const float *__restrict__ Hz = P.ho[2];
+    const float *__restrict__ eps = P.eps;
     float hx[4], hy[4], hz[4], ep[4], hzm[4], hxm[4], hzp[4], hyp[4], epj[4], epi[4], en[3][4];
     float p6[4], p7[4], p8[4], p9[4], p10[4], p11[4];
     float hyk = 0.f, hxk = 0.f, epk = 1.f;
     z4(hx); z4(hy); z4(hz); one4(ep); z4(hzm); z4(hxm); z4(hzp); z4(hyp); one4(epj); one4(epi);
     z4(p6); z4(p7); z4(p8); z4(p9); z4(p10); z4(p11);
     z4(en[0]); z4(en[1]); z4(en[2]);
+    int e0 = 0, e1x = 0;                          // soft current cells of row (i, j)
     if (act) {
         ldg4v(Hx + g, hx); ldg4v(Hy + g, hy); ldg4v(Hz + g, hz); ldg4v(eps + g, ep);
         if (j >= 1) { ldg4v(Hz + g - ZP, hzm); ldg4v(Hx + g - ZP, hxm); }
@@ -583,23 +601,27 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const mtb_yee3d_str
         if (i + 1 < nx) ldg4v(eps + g + NYZ, epi);
         if (lane == 0 && kb >= 1) { hyk = __ldg(Hy + g - 1); hxk = __ldg(Hx + g - 1); }
         if (lane == 31 && kb + 4 < ZP) epk = __ldg(eps + g + 4);
-        ldg4v(S.f[0][par] + g, en[0]); ldg4v(S.f[1][par] + g, en[1]); ldg4v(S.f[2][par] + g, en[2]);
-        if (xok && by) ld4v(S.psi[6][par] + g, p6);
-        if (xok && bz) ld4v(S.psi[7][par] + g, p7);
-        if (vyH && bz) ld4v(S.psi[8][par] + g, p8);
-        if (vyH && bx) ld4v(S.psi[9][par] + g, p9);
-        if (bx) ld4v(S.psi[10][par] + g, p10);
-        if (by) ld4v(S.psi[11][par] + g, p11);
+        ldg4v(P.e[0] + g, en[0]); ldg4v(P.e[1] + g, en[1]); ldg4v(P.e[2] + g, en[2]);
+        if (xok && by) ld4v(P.pi[6] + g, p6);
+        if (xok && bz) ld4v(P.pi[7] + g, p7);
+        if (vyH && bz) ld4v(P.pi[8] + g, p8);
+        if (vyH && bx) ld4v(P.pi[9] + g, p9);
+        if (bx) ld4v(P.pi[10] + g, p10);
+        if (by) ld4v(P.pi[11] + g, p11);
+        if (P.src_n > 0) {
+            e0 = __ldg(P.src_row + i * ny + j);
+            e1x = __ldg(P.src_row + i * ny + j + 1);
+        }
     }
     float exb = 1.f, exa = 0.f, eyb = 1.f, eya = 0.f, ezb[4], eza[4];
-    if (bx) { exb = __ldg(S.prof_b[0][1] + i); exa = __ldg(S.prof_a[0][1] + i); }
-    if (by) { eyb = __ldg(S.prof_b[1][1] + j); eya = __ldg(S.prof_a[1][1] + j); }
+    if (bx) { exb = __ldg(P.pb[0][1] + i); exa = __ldg(P.pa[0][1] + i); }
+    if (by) { eyb = __ldg(P.pb[1][1] + j); eya = __ldg(P.pa[1][1] + j); }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int k = kb + q;
         const bool on = bz && k >= 1 && k <= nz - 2;
-        ezb[q] = on ? __ldg(S.prof_b[2][1] + k) : 1.f;
-        eza[q] = on ? __ldg(S.prof_a[2][1] + k) : 0.f;
+        ezb[q] = on ? __ldg(P.pb[2][1] + k) : 1.f;
+        eza[q] = on ? __ldg(P.pa[2][1] + k) : 0.f;
     }
     {
         const float t0 = __shfl_up_sync(0xffffffffu, hy[3], 1);     // H(k-1) of q = 0
@@ -609,83 +631,79 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const mtb_yee3d_str
         if (lane != 31) epk = t2;
     }
     if (!act) return;
-    const bool exA = bx && pact(exb, exa), eyA = by && pact(eyb, eya);
-    // Ex: valid i <= nx-2
-    if (xok) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = kb + q;
-            if (k >= nz) continue;
-            const float hym = (q == 0) ? hyk : hy[q - 1];
-            const float cy = cpml(eyA, eyb, eya, (hz[q] - hzm[q]) * rdx, p6[q]);
-            const float cz = cpml(pact(ezb[q], eza[q]), ezb[q], eza[q], (hy[q] - hym) * rdx, p7[q]);
-            const float curl = (jin && k >= 1 && k <= nz - 2) ? (cy - cz) : 0.f;
-            const float e_x = 0.5f * (ep[q] + epi[q]);
-            en[0][q] = (en[0][q] * e_x + dt * curl) / e_x;
-        }
-        if (by) st4v(S.psi[6][pn] + g, p6);
-        if (bz) st4v(S.psi[7][pn] + g, p7);
-    }
-    // Ey: valid j <= ny-2
-    if (vyH) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = kb + q;
-            if (k >= nz) continue;
-            const float hxkm = (q == 0) ? hxk : hx[q - 1];
-            const float cz = cpml(pact(ezb[q], eza[q]), ezb[q], eza[q], (hx[q] - hxkm) * rdx, p8[q]);
-            const float cx = cpml(exA, exb, exa, (hz[q] - hzp[q]) * rdx, p9[q]);
-            const float curl = (iin && k >= 1 && k <= nz - 2) ? (cz - cx) : 0.f;
-            const float e_y = 0.5f * (ep[q] + epj[q]);
-            en[1][q] = (en[1][q] * e_y + dt * curl) / e_y;
-        }
-        if (bz) st4v(S.psi[8][pn] + g, p8);
-        if (bx) st4v(S.psi[9][pn] + g, p9);
-    }
-    // Ez: valid k <= nz-2
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        if (kb + q > nz - 2) continue;
-        const float cx = cpml(exA, exb, exa, (hy[q] - hyp[q]) * rdx, p10[q]);
-        const float cy = cpml(eyA, eyb, eya, (hx[q] - hxm[q]) * rdx, p11[q]);
-        const float curl = (iin && jin) ? (cx - cy) : 0.f;
-        const float e_z = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
-        en[2][q] = (en[2][q] * e_z + dt * curl) / e_z;
+        const int k = kb + q;
+        const bool vzE = k < nz, vz = k <= nz - 2, kin = k >= 1 && k <= nz - 2;
+        const float hym = (q == 0) ? hyk : hy[q - 1];
+        const float hxkm = (q == 0) ? hxk : hx[q - 1];
+        // Ex: valid i <= nx-2, k < nz; curl on j, k interior
+        {
+            const float dy = (hz[q] - hzm[q]) * rdx, dz = (hy[q] - hym) * rdx;
+            const float qy = eyb * p6[q] + eya * dy, qz = ezb[q] * p7[q] + eza[q] * dz;
+            const bool v = xok && vzE;
+            const float curl = (jin && kin) ? (dy + qy) - (dz + qz) : 0.f;
+            const float ec = 0.5f * (ep[q] + epi[q]);
+            en[0][q] = v ? en[0][q] + __fdividef(dt * curl, ec) : en[0][q];
+            p6[q] = v ? qy : p6[q];
+            p7[q] = v ? qz : p7[q];
+        }
+        // Ey: valid j <= ny-2, k < nz; curl on i, k interior
+        {
+            const float dz = (hx[q] - hxkm) * rdx, dx = (hz[q] - hzp[q]) * rdx;
+            const float qz = ezb[q] * p8[q] + eza[q] * dz, qx = exb * p9[q] + exa * dx;
+            const bool v = vyH && vzE;
+            const float curl = (iin && kin) ? (dz + qz) - (dx + qx) : 0.f;
+            const float ec = 0.5f * (ep[q] + epj[q]);
+            en[1][q] = v ? en[1][q] + __fdividef(dt * curl, ec) : en[1][q];
+            p8[q] = v ? qz : p8[q];
+            p9[q] = v ? qx : p9[q];
+        }
+        // Ez: valid k <= nz-2; curl on i, j interior
+        {
+            const float dx = (hy[q] - hyp[q]) * rdx, dy = (hx[q] - hxm[q]) * rdx;
+            const float qx = exb * p10[q] + exa * dx, qy = eyb * p11[q] + eya * dy;
+            const float curl = (iin && jin) ? (dx + qx) - (dy + qy) : 0.f;
+            const float ec = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
+            en[2][q] = vz ? en[2][q] + __fdividef(dt * curl, ec) : en[2][q];
+            p10[q] = vz ? qx : p10[q];
+            p11[q] = vz ? qy : p11[q];
+        }
     }
-    if (bx) st4v(S.psi[10][pn] + g, p10);
-    if (by) st4v(S.psi[11][pn] + g, p11);
     // soft current cells of row (i, j) on component src_comp
-    if (S.src.n > 0) {
-        const int r = i * ny + j;
-        const int e0 = __ldg(S.src.row_ptr + r), e1x = __ldg(S.src.row_ptr + r + 1);
-        if (e0 < e1x) {
-            const int c = S.src_comp;
-            const float a = __ldg(amp + S.src.amp_col);
-            const float sgn = S.src_is_point ? (float)S.point_sign : -1.f;
-            for (int e = e0; e < e1x; ++e) {
-                const int kq = __ldg(S.src.col + e) - kb;
+    if (e0 < e1x) {
+        const int c = P.src_comp;
+        const float a = __ldg(amp);
+        const float sgn = P.src_is_point ? (float)P.point_sign : -1.f;
+        for (int e = e0; e < e1x; ++e) {
+            const int kq = __ldg(P.src_col + e) - kb;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (kq != q) continue;
-                    float epn;
-                    if (c == 0) epn = epi[q];
-                    else if (c == 1) epn = epj[q];
-                    else epn = (q < 3) ? ep[q + 1] : epk;
-                    const float ecomp = 0.5f * (ep[q] + epn);
-                    const float v = a * __ldg(S.src.w + e);
+            for (int q = 0; q < 4; ++q) {
+                if (kq != q) continue;
+                float epn;
+                if (c == 0) epn = epi[q];
+                else if (c == 1) epn = epj[q];
+                else epn = (q < 3) ? ep[q + 1] : epk;
+                const float ecomp = 0.5f * (ep[q] + epn);
+                const float v = a * __ldg(P.src_w + e);
 #pragma unroll
-                    for (int cc = 0; cc < 3; ++cc) {     // static component index
-                        if (cc != c) continue;
-                        if (S.src_is_point) en[cc][q] += sgn * (v * (1.0f / ecomp));
-                        else en[cc][q] -= v / ecomp;
-                    }
+                for (int cc = 0; cc < 3; ++cc) {         // static component index
+                    if (cc != c) continue;
+                    if (P.src_is_point) en[cc][q] += sgn * (v * (1.0f / ecomp));
+                    else en[cc][q] -= v / ecomp;
                 }
             }
         }
     }
-    st4v(S.f[0][pn] + g, en[0]);
-    st4v(S.f[1][pn] + g, en[1]);
-    st4v(S.f[2][pn] + g, en[2]);
+    st4v(P.eo[0] + g, en[0]);
+    st4v(P.eo[1] + g, en[1]);
+    st4v(P.eo[2] + g, en[2]);
+    if (xok && by) st4v(P.po[6] + g, p6);
+    if (xok && bz) st4v(P.po[7] + g, p7);
+    if (vyH && bz) st4v(P.po[8] + g, p8);
+    if (vyH && bx) st4v(P.po[9] + g, p9);
+    if (bx) st4v(P.po[10] + g, p10);
+    if (by) st4v(P.po[11] + g, p11);
 }
 
 // Copy the plane samples of the (new) state into one ring slot.
@@ -724,6 +742,8 @@ struct mtb_yee3d_plan {
     int nzw = 1;
     int variant = 2;               // 1 fused x-march, 2 split H / E
     Band3 band{};
+    Split3 sp[2]{};                // split-kernel parameters of parity 0 and 1
+    int slab = 0;                  // split kernels: x planes per H / E launch pair
     int par = 0;
     int n_planes = 0;
     int64_t n_samples = 0;
@@ -782,8 +802,10 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     if (variant == 1 && S.zpitch > 128 * MAXNZ)
         return fail(MTB_UNSUPPORTED, "fused kernel: zpitch %d > %d not supported", S.zpitch,
                     128 * MAXNZ);
-    if (variant == 2 && (S.nx > 65535 || (S.ny + SPLIT_Y - 1) / SPLIT_Y > 65535))
-        return fail(MTB_UNSUPPORTED, "split kernels: nx <= 65535 and ny <= %d", 65535 * SPLIT_Y);
+    if (variant == 2 && (S.nx > 65535 || (S.ny + SPLIT_Y - 1) / SPLIT_Y > 65535 ||
+                         (int64_t)S.nx * S.ny * S.zpitch >= (1LL << 31)))
+        return fail(MTB_UNSUPPORTED, "split kernels: nx <= 65535, ny <= %d, box < 2^31 cells",
+                    65535 * SPLIT_Y);
     if ((int64_t)S.nx * S.ny * S.zpitch >= (1LL << 34))
         return fail(MTB_UNSUPPORTED, "grid too large");
     if ((int64_t)S.nx * S.ny >= (1LL << 31)) return fail(MTB_UNSUPPORTED, "nx*ny too large");
@@ -817,6 +839,9 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     p->s = S;
     p->rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
     p->variant = variant;
+    // split kernels: rows_per_warp > 0 sets the x planes per launch pair; the
+    // default is the whole grid in one pair
+    p->slab = (tuning && tuning->rows_per_warp > 0) ? std::min(tuning->rows_per_warp, S.nx) : S.nx;
     const int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     p->nzw = (S.zpitch + 127) / 128;
     p->smem = sizeof(float) * (size_t)(S.zpitch + 4) * (4 * (TY3 + 2) + 3 * (TY3 + 1));
@@ -830,6 +855,38 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
             for (int h = 0; h < 2 && !rc; ++h)
                 rc = profile_band3(S.prof_b[a][h], S.prof_a[a][h], dims[a] - 1 + h,
                                    p->band.lo[a][h], p->band.hi[a][h]);
+    }
+    if (!rc && variant == 2) {
+        for (int par = 0; par < 2; ++par) {
+            Split3 &q = p->sp[par];
+            for (int c = 0; c < 3; ++c) {
+                q.e[c] = S.f[c][par];
+                q.eo[c] = S.f[c][par ^ 1];
+                q.h[c] = S.f[3 + c][par];
+                q.ho[c] = S.f[3 + c][par ^ 1];
+            }
+            for (int c = 0; c < 12; ++c) {
+                q.pi[c] = S.psi[c][par];
+                q.po[c] = S.psi[c][par ^ 1];
+            }
+            q.eps = S.eps;
+            for (int a = 0; a < 3; ++a)
+                for (int h = 0; h < 2; ++h) {
+                    q.pb[a][h] = S.prof_b[a][h];
+                    q.pa[a][h] = S.prof_a[a][h];
+                }
+            q.src_row = S.src.row_ptr;
+            q.src_col = S.src.col;
+            q.src_w = S.src.w;
+            q.src_n = S.src.n;
+            q.src_comp = S.src_comp;
+            q.src_is_point = S.src_is_point;
+            q.point_sign = S.point_sign;
+            q.nx = S.nx; q.ny = S.ny; q.nz = S.nz; q.zp = S.zpitch;
+            q.dt = S.dt;
+            q.rdx = 1.0f / S.dx;
+            q.B = p->band;
+        }
     }
     if (!rc && variant == 1) {
         switch (p->nzw) {
@@ -907,14 +964,20 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
             if (rc) return rc;
             ++p->last_launches;
         } else {
-            const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, p->s.nx);
-            const dim3 block(32, SPLIT_Y);
-            k_yee3d_h<<<grid, block, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(), p->par, p->band);
-            MTB_CHECK_LAUNCH();
-            k_yee3d_e<<<grid, block, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(), p->par, C.amp,
-                                              p->band);
-            MTB_CHECK_LAUNCH();
-            p->last_launches += 2;
+            // x slabs: H(slab) then E(slab), so the E kernel finds E(n) and
+            // H(n+1/2) of its planes in L2. E(slab) needs H of the slab and of
+            // the plane before it, which the previous slab wrote.
+            const int ns = p->slab;
+            for (int i0 = 0; i0 < p->s.nx; i0 += ns) {
+                const int np_ = std::min(ns, p->s.nx - i0);
+                const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, np_);
+                const dim3 block(32, SPLIT_Y);
+                k_yee3d_h<<<grid, block, 0, st>>>(p->sp[p->par], i0);
+                MTB_CHECK_LAUNCH();
+                k_yee3d_e<<<grid, block, 0, st>>>(p->sp[p->par], C.amp, i0);
+                MTB_CHECK_LAUNCH();
+                p->last_launches += 2;
+            }
         }
         if ((rc = p->timer.end(st))) return rc;
         p->par ^= 1;

@@ -321,10 +321,11 @@ def test_energy_conserved_in_pec_box():
     assert (u.max() - u.min()) / u.mean() < 1e-4
 
 
-@pytest.mark.parametrize("variant", [1, 2])
-def test_3d_wide_z_matches_oracle(variant):
+@pytest.mark.parametrize("variant,slab", [(1, 0), (2, 0), (2, 3)])
+def test_3d_wide_z_matches_oracle(variant, slab):
     """z extent 300 (three 128-column blocks, a partial last one) with the
-    point source and a z flux face on a block boundary, CPML on all faces."""
+    point source and a z flux face on a block boundary, CPML on all faces;
+    the split kernels whole-grid and in x slabs of 3 planes."""
     from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D, run_3d
     from meep_torch_b200.core.sources import GaussianPulse
     from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
@@ -344,7 +345,7 @@ def test_3d_wide_z_matches_oracle(variant):
     init = init_3d_state(nx, ny, nz, npml=npml, device=dev())
     init = init._replace(**{k: torch.from_numpy(s0[k]).to(dev())
                             for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
-    st, accs = run_3d(init, c, n, source=src, monitors=mons, variant=variant)
+    st, accs = run_3d(init, c, n, source=src, monitors=mons, variant=variant, rows_per_seg=slab)
     dt = oc["dt"]
     om = [lambda s, t: O.flux3d_sample(s, t, dt, freqs, "z", 127, (2, 12, 2, 11)),
           lambda s, t: O.flux3d_sample(s, t, dt, freqs, "x", 8, (2, 11, 100, 260))]
