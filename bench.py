@@ -172,7 +172,7 @@ def run_cfg2(args, rank, world, dev):
     specs = W.cfg2_specs(n=args.structs, seed=2 + 1009 * rank)
     cells = sum(s["nx"] * s["ny"] for s in specs)
     items = [W.cfg2_item(s, dev) for s in specs]
-    eng = Engine2D(items, rows_per_warp=args.rows, ring_slots=args.ring)
+    eng = Engine2D(items, rows_per_warp=args.rows, ring_slots=args.ring, variant=args.variant)
     stream = torch.cuda.current_stream(dev)
 
     def bench_step():
@@ -221,7 +221,7 @@ def run_cfg2(args, rank, world, dev):
         nonlocal d2h
         dev_eps = [t.to(dev, non_blocking=True) for t in host_eps]
         its = [W.cfg2_item(s, dev, eps_t=e) for s, e in zip(specs, dev_eps)]
-        e = Engine2D(its, rows_per_warp=args.rows, ring_slots=args.ring)
+        e = Engine2D(its, rows_per_warp=args.rows, ring_slots=args.ring, variant=args.variant)
         e.run(0, nsteps)
         outs = []
         nb = 0
@@ -328,7 +328,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--n3", type=int, default=256, help="cfg3 grid side")
     ap.add_argument("--variant", type=int, default=0,
-                    help="3D kernel: 0 library default, 1 fused x-march, 2 split H / E")
+                    help="kernel variant, 0 library default; 2D: 1 row march, 2 tiles; "
+                         "3D: 1 fused x-march, 2 split H / E")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

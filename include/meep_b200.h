@@ -138,6 +138,9 @@ typedef struct mtb_yee2d_struct {
                                profile is active on rows r < xband[0] or
                                r >= xband[1], the ex profile on rows
                                r < xband[2] or r >= xband[3]              */
+    int32_t yband[4];       /* plan-filled: the hy profile is active on
+                               columns j < yband[0] or j >= yband[1], the ey
+                               profile on j < yband[2] or j >= yband[3]   */
     int32_t pad_;
     int64_t ring_full[3];   /* full-grid sample of comp c to ring offset, -1 = off */
 } mtb_yee2d_struct;
@@ -171,11 +174,13 @@ typedef struct mtb_dft_region {
 
 /* Tuning knobs (0 = library default). */
 typedef struct mtb_tuning {
-    int32_t rows_per_warp;  /* 2D: rows one warp marches through; 3D: x planes
-                               one fused-march block covers                 */
+    int32_t rows_per_warp;  /* 2D row march: rows one warp marches through;
+                               3D fused: x planes one block covers; 3D split:
+                               x planes per H / E launch pair (0 = all)     */
     int32_t ring_slots;     /* steps buffered before one DFT contraction    */
     int32_t threads;        /* threads per block                            */
-    int32_t variant;        /* 3D kernel: 0 default (split), 1 fused x-march,
+    int32_t variant;        /* 2D: 0 default (row march), 1 row march, 2 tiles;
+                               3D: 0 default (split), 1 fused x-march,
                                2 split H / E streaming kernels              */
 } mtb_tuning;
 

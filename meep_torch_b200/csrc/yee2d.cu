@@ -787,6 +787,429 @@ __global__ void __launch_bounds__(32 * WARPS2D, 4) k_yee2d_te(
     te_warp(W->s, w.y, w.z, w.w, C, W->lines, nl, pp);
 }
 
+// ================================================================== tiles
+// Tile kernels: a block owns TROWS rows x 128 columns of one structure;
+// thread (lane, row) updates one float4 (columns jb .. jb+3) of one row and
+// issues every load it needs before using any. The one-row / one-column
+// halos of the fused step are recomputed from the old state (hence the
+// ping-pong buffers); neighbouring rows come from L1/L2, neighbouring columns
+// from warp shuffles (lane 0 and lane 31 load their outer column). The CPML
+// memory is gated by the plan's band limits (geometry); inside a band the
+// recursion runs with the profile's (b, a), which are (1, 0) on inert nodes,
+// so lanes of one warp run the same arithmetic whether or not they are in a
+// layer, and the edge rules are selects.
+constexpr int TROWS = 8;
+
+struct TileSmem {
+    mtb_yee2d_struct s;
+    mtb_line_sample lines[MAXL];
+    int nl;
+};
+
+// Block setup: work item, structure copy, line samples touching the tile.
+__device__ __forceinline__ bool tile_setup(const mtb_yee2d_struct *__restrict__ SS,
+                                           const int4 *__restrict__ work, int n_work,
+                                           TileSmem &T, int4 &w) {
+    if ((int)blockIdx.x >= n_work) return false;
+    w = __ldg(work + blockIdx.x);
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(SS + w.x);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&T.s);
+        for (int e = tid; e < (int)(sizeof(mtb_yee2d_struct) / 4); e += 32 * TROWS)
+            dst[e] = __ldg(src + e);
+    }
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        const int i0 = w.y, i1 = min(w.y + TROWS, T.s.nx), c0 = w.z;
+        const int n_all = T.s.n_lines;
+        bool keep = false;
+        mtb_line_sample ln{};
+        if (threadIdx.x < n_all) {
+            ln = T.s.lines[threadIdx.x];
+            if (ln.kind == 0)
+                keep = ln.index >= i0 && ln.index < i1 && ln.lo < c0 + 128 && ln.hi > c0;
+            else
+                keep = ln.index >= c0 && ln.index < c0 + 128 && ln.lo < i1 && ln.hi > i0;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) T.lines[__popc(m & ((1u << threadIdx.x) - 1))] = ln;
+        if (threadIdx.x == 0) T.nl = __popc(m);
+    }
+    __syncthreads();
+    return true;
+}
+
+__device__ __forceinline__ bool in_band(int k, int lo, int hi) { return k < lo || k >= hi; }
+// any of columns jb .. jb+3 in a band
+__device__ __forceinline__ bool band4(int jb, int lo, int hi) { return jb < lo || jb + 3 >= hi; }
+
+// Hy(n+1/2) of one row from Ez rows r (ea), r+1 (eb): core/stepper_tm.py:97-100,
+// :119-128, magnetic sheet source :116-118. `valid` = r <= nx-2.
+__device__ __forceinline__ void tm_hy(const mtb_yee2d_struct &S, int r, bool valid, bool act,
+                                      int jb, float b, float a, float dt, float rdx,
+                                      const float (&ea)[4], const float (&eb)[4],
+                                      const float (&hy)[4], float (&ps)[4], float (&out)[4],
+                                      const float *amp_h) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float d = (eb[q] - ea[q]) * rdx;
+        const float pv = b * ps[q] + a * d;
+        const float hn = hy[q] + dt * (d + pv);
+        out[q] = valid ? hn : hy[q];
+        ps[q] = valid ? pv : ps[q];
+    }
+    if (valid && act && r >= S.src_h1.row_lo && r <= S.src_h1.row_hi)
+        apply_cells(S.src_h1, r, amp_h, jb, out);
+}
+
+template <bool EXPL>
+__device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, const int c0,
+                                        const Ctx2D &C, const mtb_line_sample *L, const int nl) {
+    const int lane = threadIdx.x;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    const int jb = c0 + 4 * lane;
+    const bool act = jb < P;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int par = C.par;
+    const uint32_t ro = (uint32_t)i * P + jb;        // box < 2^31 cells (plan check)
+    const float *__restrict__ Dz = S.f_main[par];
+    const float *__restrict__ Hx = S.f_x[par];
+    const float *__restrict__ Hy = S.f_y[par];
+    const float *__restrict__ ie = S.inv_eps_a;
+    const bool hyRow = i <= nx - 2, dzRow = i >= 1 && i <= nx - 2;
+    const bool bxH = hyRow && in_band(i, S.xband[0], S.xband[1]);
+    const bool bxHp = i >= 1 && in_band(i - 1, S.xband[0], S.xband[1]);
+    const bool bxE = dzRow && in_band(i, S.xband[2], S.xband[3]);
+    const bool byH = act && band4(jb, S.yband[0], S.yband[1]);
+    const bool byE = act && dzRow && band4(jb, S.yband[2], S.yband[3]);
+    const int jl = jb - 1;
+    const bool hasL = lane == 0 && jl >= 0 && jl <= ny - 2;
+    const bool byHL = hasL && in_band(jl, S.yband[0], S.yband[1]);
+
+    float ez0[4], ez1[4], ez2[4], d1[4], e1[4], hx[4], hy[4], hyp[4];
+    float p0[4], p1[4], p1p[4], p2[4], p3[4];
+    float ezl = 0.f, ezr = 0.f, hxl = 0.f, p0l = 0.f;
+    zero4(ez0); zero4(ez1); zero4(ez2); zero4(d1); zero4(e1); zero4(hx); zero4(hy); zero4(hyp);
+    zero4(p0); zero4(p1); zero4(p1p); zero4(p2); zero4(p3);
+    if (act) {
+        ld4(Dz + ro, d1);
+        ld4(ie + ro, e1);
+        if (EXPL) {
+            const float *Eex = S.e_explicit;
+            ld4(Eex + ro, ez1);
+            if (i >= 1) ld4(Eex + ro - P, ez0);
+            if (i + 1 < nx) ld4(Eex + ro + P, ez2);
+            if (lane == 0 && jb >= 1) ezl = Eex[ro - 1];
+            if (lane == 31 && jb + 4 < ny) ezr = Eex[ro + 4];
+        } else {
+            float d0[4], e0[4], d2[4], e2[4];
+            zero4(d0); zero4(e0); zero4(d2); zero4(e2);
+            if (i >= 1) { ld4(Dz + ro - P, d0); ld4(ie + ro - P, e0); }
+            if (i + 1 < nx) { ld4(Dz + ro + P, d2); ld4(ie + ro + P, e2); }
+            if (lane == 0 && jb >= 1) ezl = Dz[ro - 1] * ie[ro - 1];
+            if (lane == 31 && jb + 4 < P) ezr = Dz[ro + 4] * ie[ro + 4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ez0[q] = d0[q] * e0[q];
+                ez1[q] = d1[q] * e1[q];
+                ez2[q] = d2[q] * e2[q];
+            }
+        }
+        ld4(Hx + ro, hx);
+        ld4(Hy + ro, hy);
+        if (i >= 1) ld4(Hy + ro - P, hyp);
+        if (hasL) {
+            hxl = Hx[ro - 1];
+            if (byHL) p0l = S.psi[0][par][ro - 1];
+        }
+        if (byH) ld4(S.psi[0][par] + ro, p0);
+        if (bxH) ld4(S.psi[1][par] + ro, p1);
+        if (bxHp) ld4(S.psi[1][par] + ro - P, p1p);
+        if (bxE) ld4(S.psi[2][par] + ro, p2);
+        if (byE) ld4(S.psi[3][par] + ro, p3);
+    }
+    // profiles: (1, 0) outside the bands
+    float hxb = 1.f, hxa = 0.f, hxbp = 1.f, hxap = 0.f, exb = 1.f, exa = 0.f;
+    if (bxH) { hxb = __ldg(S.hx_b + i); hxa = __ldg(S.hx_a + i); }
+    if (bxHp) { hxbp = __ldg(S.hx_b + i - 1); hxap = __ldg(S.hx_a + i - 1); }
+    if (bxE) { exb = __ldg(S.ex_b + i); exa = __ldg(S.ex_a + i); }
+    const bool pmc = S.y_pmc != 0;
+    float hyb[4], hya[4], eyb[4], eya[4];
+    bool vH[4], vD[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        vH[q] = act && j <= ny - 2;
+        vD[q] = act && dzRow && (pmc ? (j < ny) : (j >= 1 && j <= ny - 2));
+        const bool oh = byH && j <= ny - 2, oe = byE && j < ny;
+        hyb[q] = oh ? __ldg(S.hy_b + j) : 1.f;
+        hya[q] = oh ? __ldg(S.hy_a + j) : 0.f;
+        eyb[q] = oe ? __ldg(S.ey_b + j) : 1.f;
+        eya[q] = oe ? __ldg(S.ey_a + j) : 0.f;
+    }
+    float ezR = __shfl_down_sync(0xffffffffu, ez1[0], 1);
+    if (lane == 31) ezR = ezr;
+
+    // Hy(n+1/2) rows i-1 (recomputed halo) and i
+    float hyP[4], hyN[4];
+    tm_hy(S, i - 1, i >= 1, act, jb, hxbp, hxap, dt, rdx, ez0, ez1, hyp, p1p, hyP, C.amp_h);
+    if (i < 1) zero4(hyP);
+    tm_hy(S, i, hyRow, act, jb, hxb, hxa, dt, rdx, ez1, ez2, hy, p1, hyN, C.amp_h);
+
+    // Hx(n+1/2) row i (core/stepper_tm.py:91-94, :121-128)
+    float hxN[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float er = (q < 3) ? ez1[q + 1] : ezR;
+        const float d = (er - ez1[q]) * rdx;
+        const float pv = hyb[q] * p0[q] + hya[q] * d;
+        const float hn = hx[q] - dt * (d + pv);
+        hxN[q] = vH[q] ? hn : hx[q];
+        p0[q] = vH[q] ? pv : p0[q];
+    }
+    if (act && i >= S.src_h2.row_lo && i <= S.src_h2.row_hi) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
+    // Hx(n+1/2)(i, jb-1): the left lane's last column; lane 0 recomputes its own
+    float hxm0 = __shfl_up_sync(0xffffffffu, hxN[3], 1);
+    if (lane == 0) {
+        float v = 0.f;
+        if (hasL) {
+            const float d = (ez1[0] - ezl) * rdx;
+            float c = d;
+            if (byHL) c = d + (__ldg(S.hy_b + jl) * p0l + __ldg(S.hy_a + jl) * d);
+            v = hxl - dt * c;
+            if (i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
+                v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
+        }
+        hxm0 = v;
+    }
+
+    // Dz(n+1) row i (core/stepper_tm.py:136-166), electric source, Ez = Dz / eps
+    float dzN[4], ezN[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float hxm = (q == 0) ? hxm0 : hxN[q - 1];
+        const float dhy = (hyN[q] - hyP[q]) * rdx;
+        const float dhx = (hxN[q] - hxm) * rdx;
+        const float q2 = exb * p2[q] + exa * dhy;
+        const float q3 = eyb[q] * p3[q] + eya[q] * dhx;
+        const float dn = d1[q] + dt * ((dhy + q2) - (dhx + q3));
+        dzN[q] = vD[q] ? dn : d1[q];
+        p2[q] = vD[q] ? q2 : p2[q];
+        p3[q] = vD[q] ? q3 : p3[q];
+    }
+    if (act && i >= S.src_e.row_lo && i <= S.src_e.row_hi) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ezN[q] = dzN[q] * e1[q];
+    if (!act) return;
+    const int pn = par ^ 1;
+    st4(S.f_main[pn] + ro, dzN);
+    st4(S.f_x[pn] + ro, hxN);
+    st4(S.f_y[pn] + ro, hyN);
+    if (byH) st4(S.psi[0][pn] + ro, p0);
+    if (bxH) st4(S.psi[1][pn] + ro, p1);
+    if (bxE) st4(S.psi[2][pn] + ro, p2);
+    if (byE) st4(S.psi[3][pn] + ro, p3);
+    float *ring = C.ring;
+    if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, ezN);
+    if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, hxN);
+    if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, hyN);
+    if (nl) {
+        sample_row(L, nl, MTB_C2_MAIN, i, jb, true, ezN, ring);
+        sample_row(L, nl, MTB_C2_X, i, jb, true, hxN, ring);
+        sample_row(L, nl, MTB_C2_Y, i, jb, true, hyN, ring);
+    }
+}
+
+// Dy(n+1/2) of one row from Hz rows r-1 (hp), r (hc): core/stepper_te.py:79-111,
+// source :120-134. `valid` = 1 <= r <= nx-2.
+__device__ __forceinline__ void te_dy(const mtb_yee2d_struct &S, int r, bool valid, bool act,
+                                      int jb, float b, float a, float dt, float rdx,
+                                      const float (&hp)[4], const float (&hc)[4],
+                                      const float (&dy)[4], float (&ps)[4], float (&out)[4],
+                                      const float *amp_e) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool v = valid && act && jb + q <= S.ny - 2;
+        const float d = (hc[q] - hp[q]) * rdx;
+        const float pv = b * ps[q] + a * d;
+        const float dn = dy[q] - dt * (d + pv);
+        out[q] = v ? dn : dy[q];
+        ps[q] = v ? pv : ps[q];
+    }
+    if (act && r >= S.src_e.row_lo && r <= S.src_e.row_hi) apply_cells(S.src_e, r, amp_e, jb, out);
+}
+
+__device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, const int c0,
+                                        const Ctx2D &C, const mtb_line_sample *L, const int nl) {
+    const int lane = threadIdx.x;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    const int jb = c0 + 4 * lane;
+    const bool act = jb < P;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int par = C.par;
+    const uint32_t ro = (uint32_t)i * P + jb;
+    const float *__restrict__ Hz = S.f_main[par];
+    const float *__restrict__ Dx = S.f_x[par];
+    const float *__restrict__ Dy = S.f_y[par];
+    const float *__restrict__ iex = S.inv_eps_a;
+    const float *__restrict__ iey = S.inv_eps_b;
+    const bool hzRow = i <= nx - 2;                     // Hz, Dx (Ex) rows
+    const bool dyRow = i >= 1 && i <= nx - 2, dyRowN = i + 1 <= nx - 2;
+    const bool bxH = hzRow && in_band(i, S.xband[0], S.xband[1]);
+    const bool bxE = dyRow && in_band(i, S.xband[2], S.xband[3]);
+    const bool bxEn = dyRowN && in_band(i + 1, S.xband[2], S.xband[3]);
+    const bool byE = act && hzRow && band4(jb, S.yband[2], S.yband[3]);
+    const bool byH = act && hzRow && band4(jb, S.yband[0], S.yband[1]);
+    const int jr = jb + 4;
+    const bool hasR = lane == 31 && hzRow && jr <= ny - 1;
+    const bool updR = hasR && jr >= 1 && jr <= ny - 2;
+    const bool byER = updR && in_band(jr, S.yband[2], S.yband[3]);
+
+    float hc[4], hp[4], hn[4], dx[4], dy[4], dyn[4], ix[4], iy[4], iyn[4];
+    float p0[4], p1[4], p1n[4], p2[4], p3[4];
+    float hzL = 0.f, hzR = 0.f, dxr = 0.f, ixr = 0.f, p0r = 0.f;
+    zero4(hc); zero4(hp); zero4(hn); zero4(dx); zero4(dy); zero4(dyn); zero4(ix); zero4(iy);
+    zero4(iyn); zero4(p0); zero4(p1); zero4(p1n); zero4(p2); zero4(p3);
+    if (act) {
+        ld4(Hz + ro, hc);
+        ld4(Dx + ro, dx);
+        ld4(Dy + ro, dy);
+        ld4(iex + ro, ix);
+        ld4(iey + ro, iy);
+        if (i >= 1) ld4(Hz + ro - P, hp);
+        if (i + 1 < nx) { ld4(Hz + ro + P, hn); ld4(Dy + ro + P, dyn); ld4(iey + ro + P, iyn); }
+        if (lane == 0 && jb >= 1) hzL = Hz[ro - 1];
+        if (hasR) {
+            hzR = Hz[ro + 4];
+            dxr = Dx[ro + 4];
+            ixr = iex[ro + 4];
+            if (byER) p0r = S.psi[0][par][ro + 4];
+        }
+        if (byE) ld4(S.psi[0][par] + ro, p0);
+        if (bxE) ld4(S.psi[1][par] + ro, p1);
+        if (bxEn) ld4(S.psi[1][par] + ro + P, p1n);
+        if (bxH) ld4(S.psi[2][par] + ro, p2);
+        if (byH) ld4(S.psi[3][par] + ro, p3);
+    }
+    float hxb = 1.f, hxa = 0.f, exb = 1.f, exa = 0.f, exbn = 1.f, exan = 0.f;
+    if (bxH) { hxb = __ldg(S.hx_b + i); hxa = __ldg(S.hx_a + i); }
+    if (bxE) { exb = __ldg(S.ex_b + i); exa = __ldg(S.ex_a + i); }
+    if (bxEn) { exbn = __ldg(S.ex_b + i + 1); exan = __ldg(S.ex_a + i + 1); }
+    float hyb[4], hya[4], eyb[4], eya[4];
+    bool vX[4], vZ[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        vX[q] = act && hzRow && j >= 1 && j <= ny - 2;
+        vZ[q] = act && hzRow && j <= ny - 2;
+        const bool oe = byE && j >= 1 && j <= ny - 2, oh = byH && j <= ny - 2;
+        eyb[q] = oe ? __ldg(S.ey_b + j) : 1.f;
+        eya[q] = oe ? __ldg(S.ey_a + j) : 0.f;
+        hyb[q] = oh ? __ldg(S.hy_b + j) : 1.f;
+        hya[q] = oh ? __ldg(S.hy_a + j) : 0.f;
+    }
+    float hm0 = __shfl_up_sync(0xffffffffu, hc[3], 1);
+    if (lane == 0) hm0 = hzL;
+
+    // Dx / Ex(n+1/2) row i (core/stepper_te.py:79-95, :150-160)
+    float dxN[4], ex[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float hm = (q == 0) ? hm0 : hc[q - 1];
+        const float d = (hc[q] - hm) * rdx;
+        const float pv = eyb[q] * p0[q] + eya[q] * d;
+        const float dn = dx[q] + dt * (d + pv);
+        dxN[q] = vX[q] ? dn : dx[q];
+        p0[q] = vX[q] ? pv : p0[q];
+        ex[q] = hzRow ? dxN[q] * ix[q] : 0.f;
+    }
+    // Ex(n+1/2)(i, jb+4): lane 31's right neighbour column
+    float exR = 0.f;
+    if (hasR) {
+        float v = dxr;
+        if (updR) {
+            const float d = (hzR - hc[3]) * rdx;
+            float c = d;
+            if (byER) c = d + (__ldg(S.ey_b + jr) * p0r + __ldg(S.ey_a + jr) * d);
+            v = dxr + dt * c;
+        }
+        exR = v * ixr;
+    }
+    // Dy / Ey(n+1/2) rows i and i+1 (recomputed halo)
+    float dyN[4], ey[4], dyNn[4], eyn[4];
+    te_dy(S, i, dyRow, act, jb, exb, exa, dt, rdx, hp, hc, dy, p1, dyN, C.amp_e);
+    te_dy(S, i + 1, dyRowN, act, jb, exbn, exan, dt, rdx, hc, hn, dyn, p1n, dyNn, C.amp_e);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        ey[q] = dyN[q] * iy[q];
+        eyn[q] = (i + 1 < nx) ? dyNn[q] * iyn[q] : 0.f;
+    }
+    float exr = __shfl_down_sync(0xffffffffu, ex[0], 1);
+    if (lane == 31) exr = exR;
+
+    // Hz(n+1) row i (core/stepper_te.py:113-117)
+    float hzN[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float exn = (q < 3) ? ex[q + 1] : exr;
+        const float dey = (eyn[q] - ey[q]) * rdx;
+        const float dex = (exn - ex[q]) * rdx;
+        const float q2 = hxb * p2[q] + hxa * dey;
+        const float q3 = hyb[q] * p3[q] + hya[q] * dex;
+        const float hn_ = hc[q] - dt * ((dey + q2) - (dex + q3));
+        hzN[q] = vZ[q] ? hn_ : hc[q];
+        p2[q] = vZ[q] ? q2 : p2[q];
+        p3[q] = vZ[q] ? q3 : p3[q];
+    }
+    if (act && hzRow && i >= S.src_h1.row_lo && i <= S.src_h1.row_hi)
+        apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
+    if (!act) return;
+    const int pn = par ^ 1;
+    st4(S.f_main[pn] + ro, hzN);
+    st4(S.f_x[pn] + ro, dxN);
+    st4(S.f_y[pn] + ro, dyN);
+    if (byE) st4(S.psi[0][pn] + ro, p0);
+    if (bxE) st4(S.psi[1][pn] + ro, p1);
+    if (bxH) st4(S.psi[2][pn] + ro, p2);
+    if (byH) st4(S.psi[3][pn] + ro, p3);
+    float *ring = C.ring;
+    if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, hzN);
+    if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, ex);
+    if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, ey);
+    if (nl) {
+        sample_row(L, nl, MTB_C2_MAIN, i, jb, true, hzN, ring);
+        sample_row(L, nl, MTB_C2_X, i, jb, true, ex, ring);
+        sample_row(L, nl, MTB_C2_Y, i, jb, true, ey, ring);
+    }
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
+    const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
+    Ctx2D C) {
+    __shared__ TileSmem T;
+    int4 w;
+    if (!tile_setup(SS, work, n_work, T, w)) return;
+    const int i = w.y + threadIdx.y;
+    if (i >= T.s.nx) return;                       // whole warp
+    if (FIRST && T.s.explicit_e)
+        tm_tile<true>(T.s, i, w.z, C, T.lines, T.nl);
+    else
+        tm_tile<false>(T.s, i, w.z, C, T.lines, T.nl);
+}
+
+__global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
+    const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
+    Ctx2D C) {
+    __shared__ TileSmem T;
+    int4 w;
+    if (!tile_setup(SS, work, n_work, T, w)) return;
+    const int i = w.y + threadIdx.y;
+    if (i >= T.s.nx) return;
+    te_tile(T.s, i, w.z, C, T.lines, T.nl);
+}
+
 }  // namespace mtb
 
 using namespace mtb;
@@ -799,6 +1222,7 @@ struct mtb_yee2d_plan {
     int n_work_tm = 0;                 // work items [0, n_work_tm) are TM, the rest TE
     int n_cols = 0;
     int rows = 32;
+    int variant = 1;                   // 1 row march, 2 tiles
     int par = 0;
     int first = 1;
     int64_t last_launches = 0;
@@ -873,7 +1297,9 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     *out = nullptr;
     if (n < 1 || !structs_in) return fail(MTB_INVALID_ARG, "need at least one structure");
     if (n_amp_cols < 0) return fail(MTB_INVALID_ARG, "n_amp_cols < 0");
+    const int variant = (tuning && tuning->variant == 2) ? 2 : 1;
     int rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
+    if (variant == 2) rows = TROWS;
     int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     if (ring_slot_elems < 0 || (ring_slot_elems & 3))
         return fail(MTB_INVALID_ARG, "ring_slot_elems must be a non-negative multiple of 4");
@@ -949,12 +1375,15 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         }
         if ((rc = profile_band(S.hx_b, S.hx_a, S.nx - 1, S.xband[0], S.xband[1], s))) return rc;
         if ((rc = profile_band(S.ex_b, S.ex_a, S.nx, S.xband[2], S.xband[3], s))) return rc;
+        if ((rc = profile_band(S.hy_b, S.hy_a, S.ny - 1, S.yband[0], S.yband[1], s))) return rc;
+        if ((rc = profile_band(S.ey_b, S.ey_a, S.ny, S.yband[2], S.yband[3], s))) return rc;
         n_work += (int64_t)((S.nx + rows - 1) / rows) * ((S.pitch + 127) / 128);
     }
     if (n_work > (1LL << 30)) return fail(MTB_INVALID_ARG, "batch too large");
     mtb_yee2d_plan *p = new mtb_yee2d_plan();
     p->n_structs = n;
     p->rows = rows;
+    p->variant = variant;
     p->n_cols = n_amp_cols;
     p->n_work = (int)n_work;
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
@@ -983,7 +1412,9 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
             if (structs[s].pol != (pol == 0 ? MTB_TM : MTB_TE)) continue;
             for (int i0 = 0; i0 < structs[s].nx; i0 += rows)
                 for (int c0 = 0; c0 < structs[s].pitch; c0 += 128)
-                    work.push_back(make_int4(s, i0, std::min(i0 + rows, structs[s].nx), c0));
+                    work.push_back(variant == 1
+                                       ? make_int4(s, i0, std::min(i0 + rows, structs[s].nx), c0)
+                                       : make_int4(s, i0, c0, 0));
         }
     }
     cudaError_t e = cudaMemcpy(p->structs_d.p, structs.data(), sizeof(mtb_yee2d_struct) * n,
@@ -1047,7 +1478,25 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
         C.par = p->par;
         C.first = p->first;
         if ((rc = p->timer.begin(st, 0))) return rc;
-        if (n_tm > 0) {
+        if (p->variant == 2) {
+            const dim3 blk(32, TROWS);
+            if (n_tm > 0) {
+                if (p->first)
+                    k_tile_tm<true><<<n_tm, blk, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
+                                                         p->work_d.as<int4>(), n_tm, C);
+                else
+                    k_tile_tm<false><<<n_tm, blk, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
+                                                          p->work_d.as<int4>(), n_tm, C);
+                MTB_CHECK_LAUNCH();
+                ++p->last_launches;
+            }
+            if (n_te > 0) {
+                k_tile_te<<<n_te, blk, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
+                                                p->work_d.as<int4>() + n_tm, n_te, C);
+                MTB_CHECK_LAUNCH();
+                ++p->last_launches;
+            }
+        } else if (n_tm > 0) {
             if (p->first)
                 k_yee2d_tm<true><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(
                     p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>(), n_tm, C);
@@ -1057,7 +1506,7 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
             MTB_CHECK_LAUNCH();
             ++p->last_launches;
         }
-        if (n_te > 0) {
+        if (p->variant == 1 && n_te > 0) {
             k_yee2d_te<<<blocks_te, 32 * WARPS2D, smem_te(), st>>>(
                 p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>() + n_tm, n_te, C);
             MTB_CHECK_LAUNCH();

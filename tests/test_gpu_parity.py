@@ -215,7 +215,8 @@ def _oracle_te(nx, ny, dx, eps, npml, n, ix, j0, j1, freqs, fcen=0.65, fw=0.3, m
                     amp_fn=lambda t: prof(O.src_time(t, dt)), mask=mask, monitors=mons)
 
 
-def test_batched_mixed_tm_te_matches_oracle():
+@pytest.mark.parametrize("variant", [1, 2])
+def test_batched_mixed_tm_te_matches_oracle(variant):
     """One plan advancing TM and TE structures of different, odd sizes whose
     widths span several 128-column strips and rows several warp segments."""
     from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
@@ -255,7 +256,7 @@ def test_batched_mixed_tm_te_matches_oracle():
             items.append((init_te_state(grid), m, TESource(src), mons))
             refs.append(_oracle_te(nx, ny, 0.05, eps, 8, n, 12, ny // 2 - 8, ny // 2 + 8,
                                    freqs, mon=(mx, my)))
-    eng = Engine2D(items, rows_per_warp=16, ring_slots=7)
+    eng = Engine2D(items, rows_per_warp=16, ring_slots=7, variant=variant)
     eng.run(0, 50)
     eng.run(50, n - 50)                      # two calls: t0 continuity
     for b, ((pol, nx, ny), (s_ref, acc_ref)) in enumerate(zip(specs, refs)):
@@ -359,5 +360,60 @@ def test_3d_wide_z_matches_oracle(variant, slab):
         errs[k] = rel_l2(sd[k].cpu().numpy(), os_[k])
     for q in range(2):
         errs[f"acc_{q}"] = rel_l2(accs[q].cpu().numpy(), oacc[q])
+    bad = {k: v for k, v in errs.items() if not v < TOL}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_random_state_batched_matches_oracle(variant):
+    """Random initial fields (waves in every CPML layer from the first step),
+    a batch of TM, TM with PMC y walls and TE structures whose widths are not
+    multiples of 128 and whose heights are not multiples of the tile rows;
+    fields and CPML memory against the oracle."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    from meep_torch_b200.engine2d import Engine2D
+    rng = np.random.default_rng(17)
+    specs = [("tm", 37, 300, False), ("te", 50, 261, False), ("tm", 29, 131, True),
+             ("te", 19, 45, False)]
+    n, npml, dx = 40, 8, 0.05
+    items, refs = [], []
+    for pol, nx, ny, pmc in specs:
+        eps = (1.0 + 5.0 * rng.random((nx, ny))).astype(np.float32)
+        grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+        if pol == "tm":
+            c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, y_pmc=pmc, dtype=np.float32)
+            so = O.tm_state(c)
+            for k in ("Dz", "Hx", "Hy"):
+                so[k] = rng.standard_normal(so[k].shape).astype(np.float32)
+            m = build_tm_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml, y_pmc=pmc)
+            so["Ez"] = (torch.from_numpy(so["Dz"]) / m.eps_inf.cpu()).numpy()
+            s0 = init_tm_state(grid, y_pmc=pmc)._replace(
+                **{k: torch.from_numpy(so[k]).to(dev()) for k in ("Ez", "Dz", "Hx", "Hy")})
+            step = O.tm_step
+        else:
+            c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32)
+            so = O.te_state(c)
+            for k in ("Hz", "Dx", "Dy", "Ex", "Ey"):
+                so[k] = rng.standard_normal(so[k].shape).astype(np.float32)
+            m = build_te_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml)
+            s0 = init_te_state(grid)._replace(
+                **{k: torch.from_numpy(so[k]).to(dev()) for k in ("Hz", "Dx", "Dy", "Ex", "Ey")})
+            step = O.te_step
+        items.append((s0, m, None, []))
+        refs.append(O.run_2d(step, so, c, n)[0])
+    eng = Engine2D(items, variant=variant)
+    eng.run(0, n)
+    errs = {}
+    for b, ((pol, nx, ny, pmc), ref) in enumerate(zip(specs, refs)):
+        st = eng.state(b)
+        names = (("Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy")
+                 if pol == "tm" else
+                 ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"))
+        for k in names:
+            errs[(b, k)] = rel_l2(getattr(st, k).cpu().numpy(), ref[k])
+    eng.close()
     bad = {k: v for k, v in errs.items() if not v < TOL}
     assert not bad, bad

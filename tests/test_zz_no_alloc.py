@@ -76,8 +76,11 @@ def test_noalloc_matches_plan_two_calls(pol):
     build.build()
     lib = L.load()
     dev = "cuda"
-    ref = Engine2D([_items(pol, dev)], ring_slots=8)       # plan path
-    new = Engine2D([_items(pol, dev)], ring_slots=8)       # its buffers feed the no-alloc call
+    # the no-alloc entry point runs the row-march kernels: the plan path is
+    # pinned to the same kernels (variant 1), so the comparison is of the
+    # entry points, not of two kernels' rounding
+    ref = Engine2D([_items(pol, dev)], ring_slots=8, variant=1)   # plan path
+    new = Engine2D([_items(pol, dev)], ring_slots=8, variant=1)   # buffers for the no-alloc call
     stream = torch.cuda.current_stream().cuda_stream
     parity = 0
     t0 = 0
