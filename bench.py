@@ -287,10 +287,41 @@ def run_cfg3(args, rank, world, dev):
     ms = ev0.elapsed_time(ev1)
     step_ms, step_n, dft_ms, dft_n = eng.timing()
     eng.close()
-    return dict(cells=n ** 3, nsteps=nsteps, ms=allreduce_max(ms, world, dev), launches=launches,
-                clocks=clk.summary(), step_ms=step_ms, step_n=step_n, dft_ms=dft_ms,
-                dft_n=dft_n, bytes_launch=W.cfg3_bytes_per_step(n), e2e_s=float("nan"), h2d=0,
-                d2h=0)
+    res = dict(cells=n ** 3, nsteps=nsteps, ms=allreduce_max(ms, world, dev), launches=launches,
+               clocks=clk.summary(), step_ms=step_ms, step_n=step_n, dft_ms=dft_ms,
+               dft_n=dft_n, bytes_launch=W.cfg3_bytes_per_step(n), e2e_s=float("nan"), h2d=0,
+               d2h=0)
+    del eng, s, c, src, mons
+    torch.cuda.empty_cache()
+    if args.no_e2e:
+        return res
+    # ---- e2e: host eps through the public API (run_3d), flux accumulators back
+    from meep_torch_b200.core.monitors_3d import run_3d
+    from meep_torch_b200.core.stepper_3d import init_3d_state
+    host_eps = torch.from_numpy(W.cfg3_eps(n)).pin_memory()
+    d2h = 0
+
+    def e2e_step():
+        nonlocal d2h
+        e = host_eps.to(dev, non_blocking=True)
+        s_, c_, src_, mons_ = W.cfg3_setup(dev, n=n, eps=e)
+        _, accs = run_3d(s_, c_, nsteps, source=src_, monitors=mons_, rows_per_seg=args.rows,
+                         ring_slots=args.ring, variant=args.variant)
+        outs = [a.to("cpu", non_blocking=True) for a in accs]
+        torch.cuda.synchronize(dev)
+        d2h = sum(a.numel() * 4 for a in accs)
+        return outs
+
+    e2e_step()                                   # warm
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    res.update(e2e_s=allreduce_max(time.perf_counter() - t0, world, dev),
+               h2d=host_eps.numel() * 4, d2h=d2h)
+    return res
 
 
 def barrier(world):
@@ -336,11 +367,23 @@ def main():
     threads = os.cpu_count() or 1
     if args.cpu_structs <= 0:
         args.cpu_structs = min(max(8, threads), 64)
-    config = {"workload": "cfg2: 256 batched 2D TE/TM bend variants (256..768)^2, res 20, "
-                          "1 um CPML, Gaussian line source, full-grid DFT 3 freqs + 2 flux "
-                          "lines, 5000 steps per run",
-              "structures_per_rank": args.structs, "time_steps": args.run_steps, "seed": "2 + 1009*rank",
-              "l2": "inputs larger than L2 (~1.1 GB of field state per rank)"}
+    if args.workload == "cfg3":
+        n3 = args.n3
+        steps3 = args.run_steps if args.run_steps != 5000 else 2000
+        config = {"workload": f"cfg3: 3D {n3}^3 at res 16, 16-cell CPML on all faces, 200 "
+                              "random dielectric spheres, Gaussian Ez point dipole, six "
+                              "20-frequency flux faces, 2000 steps per run",
+                  "grid": [n3, n3, n3], "time_steps": steps3, "seed": 3,
+                  "kernel_variant": args.variant or "library default (split H / E)",
+                  "l2": f"inputs larger than L2 (~{37 * 4 * n3 ** 3 / 1e9:.1f} GB of field "
+                        "state)"}
+    else:
+        config = {"workload": "cfg2: 256 batched 2D TE/TM bend variants (256..768)^2, res 20, "
+                              "1 um CPML, Gaussian line source, full-grid DFT 3 freqs + 2 flux "
+                              "lines, 5000 steps per run",
+                  "structures_per_rank": args.structs, "time_steps": args.run_steps,
+                  "seed": "2 + 1009*rank",
+                  "l2": "inputs larger than L2 (~1.1 GB of field state per rank)"}
 
     if args.impl == "reference":
         if rank != 0:
@@ -394,11 +437,20 @@ def main():
     step_avg_ms = r["step_ms"] / max(r["step_n"], 1)
     achieved = r["bytes_launch"] / (step_avg_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "yee2d_step_cfg2_traffic.json")
+    cfg3 = args.workload == "cfg3"
+    prof = os.path.join(ROOT, "profiles", "yee3d_step_cfg3_traffic.json" if cfg3
+                        else "yee2d_step_cfg2_traffic.json")
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
-    e2e_val = r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
+            tr = json.load(f)
+        if tr.get("variant", 0) in (0, args.variant):
+            traffic = tr.get("dram_bytes_per_launch")
+    e2e_val = (r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
+               if r["e2e_s"] == r["e2e_s"] else None)
+    kernel = ("k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else
+              "k_yee3d_step (one step)" if cfg3 else
+              "k_tile_tm + k_tile_te (one step)" if args.variant == 2 else
+              "k_yee2d_tm + k_yee2d_te (one step)")
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -406,7 +458,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(config, parallelism=f"independent batch per rank x{world}",
                        cells_per_rank=r["cells"]),
-        "roofline": {"bound": "hbm", "kernel": "k_yee2d_step", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": r["bytes_launch"],
