@@ -443,7 +443,8 @@ def main():
     if os.path.exists(prof):
         with open(prof) as f:
             tr = json.load(f)
-        if tr.get("variant", 0) in (0, args.variant):
+        eff = args.variant or (2 if cfg3 else 1)          # library defaults
+        if tr.get("variant") == eff:
             traffic = tr.get("dram_bytes_per_launch")
     e2e_val = (r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
                if r["e2e_s"] == r["e2e_s"] else None)
