@@ -157,7 +157,100 @@ def cpu_baseline_line(n_struct, steps, threads):
                       f"steps, {threads} threads over structures, {sec:.1f} s"}
 
 
+def cpu_sample_cfg1(steps):
+    """Oracle run of `steps` steps of cfg1 (one thread). Returns (cell-updates, seconds)."""
+    import numpy as np
+
+    from meep_torch_b200 import workloads as W
+    from oracle import fdtd as O
+    spec = W.cfg1_spec()
+    nx, ny, f32 = spec["nx"], spec["ny"], np.float32
+    c = O.tm_coeffs(nx, ny, W.DX2D, eps=spec["eps"], npml=W.NPML2D, dtype=f32)
+    dt = c["dt"]
+    i, j = spec["src"]
+    mask = O.line_source_mask(nx, ny, W.DX2D, i, j, j + 1, dtype=f32)
+    prof = O.gaussian_pulse(0.15, 0.1)
+    ix, lo, hi = spec["flux"]
+    mons = [lambda s, t: O.flux_tm_sample(s, t, dt, spec["freqs"], True, ix, lo, hi, f32)]
+    t0 = time.perf_counter()
+    O.run_2d(O.tm_step, O.tm_state(c), c, steps, amp_fn=lambda t: prof(O.src_time(t, dt)),
+             mask=mask, monitors=mons)
+    return nx * ny * steps, time.perf_counter() - t0
+
+
 # ------------------------------------------------------------------ GPU bench
+
+def run_cfg1(args, rank, world, dev):
+    """cfg1: one 320 x 160 TM structure per rank, 4000 steps per run. The working
+    set is L2-resident and the step is launch/latency-bound: whole ring flushes
+    are replayed as CUDA graphs (per-launch timing stays off)."""
+    import torch
+
+    from meep_torch_b200 import _lib
+    from meep_torch_b200 import workloads as W
+    from meep_torch_b200.core.run import run_tm
+    from meep_torch_b200.engine2d import Engine2D
+
+    lib = _lib.load()
+    spec = W.cfg1_spec()
+    nsteps = args.run_steps if args.run_steps != 5000 else spec["steps"]
+    eng = Engine2D([W.cfg1_item(dev, spec)], rows_per_warp=args.rows, ring_slots=args.ring,
+                   variant=args.variant)
+    stream = torch.cuda.current_stream(dev)
+
+    def bench_step():
+        eng.reset()
+        eng.run(0, nsteps)
+
+    for _ in range(args.warmup):
+        bench_step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    n0 = lib.mtb_launch_count()
+    with Clocks(dev.index if dev.index is not None else 0) as clk:
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            bench_step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+    launches = lib.mtb_launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    eng.close()
+    cells = spec["nx"] * spec["ny"]
+    spec2 = dict(spec, pol="tm")
+    per_step_ms = ms / (args.steps * nsteps)
+    res = dict(cells=cells, nsteps=nsteps, ms=allreduce_max(ms, world, dev), launches=launches,
+               clocks=clk.summary(), step_ms=per_step_ms * args.steps * nsteps,
+               step_n=args.steps * nsteps, dft_ms=0.0, dft_n=0,
+               bytes_launch=W.cfg2_bytes_per_step([spec2]), e2e_s=float("nan"), h2d=0, d2h=0)
+    if args.no_e2e:
+        return res
+    # ---- e2e: host eps through run_tm, flux accumulator back
+    host_eps = torch.from_numpy(spec["eps"]).pin_memory()
+
+    def e2e_step():
+        e = host_eps.to(dev, non_blocking=True)
+        st, m, src, mons = W.cfg1_item(dev, spec, eps_t=e)
+        _, accs = run_tm(st, m, nsteps, source=src, monitors=mons)
+        out = [a.to("cpu", non_blocking=True) for a in accs]
+        torch.cuda.synchronize(dev)
+        return out, sum(a.numel() * 4 for a in accs)
+
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, d2h = e2e_step()
+    torch.cuda.synchronize(dev)
+    res.update(e2e_s=allreduce_max(time.perf_counter() - t0, world, dev),
+               h2d=host_eps.numel() * 4, d2h=d2h)
+    return res
+
 
 def run_cfg2(args, rank, world, dev):
     import numpy as np
@@ -346,7 +439,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
     ap.add_argument("--rows", type=int, default=0, help="rows per warp (0 = library default)")
     ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
     ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
@@ -367,7 +460,14 @@ def main():
     threads = os.cpu_count() or 1
     if args.cpu_structs <= 0:
         args.cpu_structs = min(max(8, threads), 64)
-    if args.workload == "cfg3":
+    if args.workload == "cfg1":
+        config = {"workload": "cfg1: 2D TM waveguide 320 x 160 (16 x 8 um at res 20), 1 um "
+                              "CPML, eps 12 guide, Gaussian Ez source (0.15, 0.1), one "
+                              "50-frequency flux line, 4000 steps per run",
+                  "time_steps": args.run_steps if args.run_steps != 5000 else 4000,
+                  "l2": "L2-resident working set (~1.4 MB): latency-bound; whole DFT ring "
+                        "flushes replayed as CUDA graphs"}
+    elif args.workload == "cfg3":
         n3 = args.n3
         steps3 = args.run_steps if args.run_steps != 5000 else 2000
         config = {"workload": f"cfg3: 3D {n3}^3 at res 16, 16-cell CPML on all faces, 200 "
@@ -430,7 +530,8 @@ def main():
         B.build()
     barrier(world)
 
-    r = run_cfg3(args, rank, world, dev) if args.workload == "cfg3" else run_cfg2(args, rank, world, dev)
+    r = {"cfg1": run_cfg1, "cfg2": run_cfg2, "cfg3": run_cfg3}[args.workload](args, rank, world,
+                                                                            dev)
     peak, peak_kind = peaks()
     total_updates = r["cells"] * r["nsteps"] * args.steps * world
     value = total_updates / (r["ms"] / 1e3) / 1e9
@@ -440,7 +541,7 @@ def main():
     cfg3 = args.workload == "cfg3"
     prof = os.path.join(ROOT, "profiles", "yee3d_step_cfg3_traffic.json" if cfg3
                         else "yee2d_step_cfg2_traffic.json")
-    if os.path.exists(prof):
+    if os.path.exists(prof) and args.workload in ("cfg2", "cfg3"):
         with open(prof) as f:
             tr = json.load(f)
         eff = args.variant or (2 if cfg3 else 1)          # library defaults
@@ -448,7 +549,11 @@ def main():
             traffic = tr.get("dram_bytes_per_launch")
     e2e_val = (r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
                if r["e2e_s"] == r["e2e_s"] else None)
-    kernel = ("k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else
+    kernel = ("k_tile_tm (one step; graph replays, step time = run time / steps)"
+              if args.workload == "cfg1" and args.variant != 1 else
+              "k_yee2d_tm (one step; graph replays, step time = run time / steps)"
+              if args.workload == "cfg1" else
+              "k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else
               "k_yee3d_step (one step)" if cfg3 else
               "k_tile_tm + k_tile_te (one step)" if args.variant == 2 else
               "k_yee2d_tm + k_yee2d_te (one step)")
@@ -472,7 +577,14 @@ def main():
         "gpu_launches": r["launches"],
     }
     if rank == 0 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline_line(args.cpu_structs, args.cpu_steps, threads)
+        if args.workload == "cfg1":
+            cells, sec = cpu_sample_cfg1(4000)
+            line["cpu_baseline"] = {"value": cells / sec / 1e9, "unit": "Gcell-updates/s",
+                                    "cores": 1, "kind": "port",
+                                    "sample": f"oracle (numpy float32) cfg1, the full 4000-step "
+                                              f"run, one thread, {sec:.1f} s"}
+        else:
+            line["cpu_baseline"] = cpu_baseline_line(args.cpu_structs, args.cpu_steps, threads)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -332,7 +332,8 @@ int DftState::upload_phases(int64_t t0, int k, cudaStream_t st) {
     return MTB_OK;
 }
 
-int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm) {
+int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm,
+                       const float *phase_base) {
     if (n_regions == 0 || n <= 0 || n_blocks == 0) return MTB_OK;
     int maxnf = 1;
     for (int g = 0; g < n_groups; ++g) maxnf = std::max(maxnf, group_nf[g]);
@@ -350,7 +351,8 @@ int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm) {
     if (tm && (rc = tm->begin(st, 1))) return rc;
     k_dft_contract<<<(unsigned)n_blocks, CT, smem, st>>>(
         regions_d.as<mtb_dft_region>(), blk_region_d.as<int>(), blk_start_d.as<int64_t>(), gd,
-        gd + (n_groups + 1), total_nf, phase_d.as<float>(), row0, n, ring_d.as<float>(),
+        gd + (n_groups + 1), total_nf, phase_base ? phase_base : phase_d.as<float>(), row0, n,
+        ring_d.as<float>(),
         slot_elems);
     MTB_CHECK_LAUNCH();
     if (tm && (rc = tm->end(st))) return rc;

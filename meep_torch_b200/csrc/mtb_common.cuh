@@ -125,8 +125,10 @@ struct DftState {
     // Fill the phase table for steps [t0, t0+k) and upload it on `st`.
     int upload_phases(int64_t t0, int k, cudaStream_t st);
     // Fold ring slots [0, n) (steps t_first .. t_first+n-1, relative row
-    // `row0` of the uploaded table) into the accumulators.
-    int contract(int row0, int n, cudaStream_t st, LaunchTimer *tm = nullptr);
+    // `row0` of the uploaded table, or of `phase_base` when given) into the
+    // accumulators.
+    int contract(int row0, int n, cudaStream_t st, LaunchTimer *tm = nullptr,
+                 const float *phase_base = nullptr);
     void release();
 };
 

@@ -799,6 +799,9 @@ __global__ void __launch_bounds__(32 * WARPS2D, 4) k_yee2d_te(
 // so lanes of one warp run the same arithmetic whether or not they are in a
 // layer, and the edge rules are selects.
 constexpr int TROWS = 8;
+// row-march warps below which the library default is the tile kernels
+// (148 SMs x 8 warps)
+constexpr int64_t ROW_MARCH_MIN_WARPS = 148 * 8;
 
 struct TileSmem {
     mtb_yee2d_struct s;
@@ -1223,6 +1226,11 @@ struct mtb_yee2d_plan {
     int n_cols = 0;
     int rows = 32;
     int variant = 1;                   // 1 row march, 2 tiles
+    int graph_mode = 0;                // 0 graphs when eligible, -1 off
+    cudaStream_t cap = nullptr;        // private capture stream
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // ring flush graph per start parity
+    int64_t gkern[2] = {0, 0};         // kernels per graph replay
+    DevBuf stage_d;                    // coefficient and phase rows of one flush
     int par = 0;
     int first = 1;
     int64_t last_launches = 0;
@@ -1297,8 +1305,18 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     *out = nullptr;
     if (n < 1 || !structs_in) return fail(MTB_INVALID_ARG, "need at least one structure");
     if (n_amp_cols < 0) return fail(MTB_INVALID_ARG, "n_amp_cols < 0");
-    const int variant = (tuning && tuning->variant == 2) ? 2 : 1;
+    int variant = (tuning && (tuning->variant == 1 || tuning->variant == 2)) ? tuning->variant : 0;
     int rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
+    if (variant == 0) {
+        // library default: the row march needs enough (rows / rows_per_warp) x strips
+        // warps to fill the GPU; small batches (a single L2-resident structure)
+        // leave most SMs idle and serialise rows, so they use the tiles
+        int64_t warps = 0;
+        for (int s = 0; s < n; ++s)
+            warps += (int64_t)((structs_in[s].nx + rows - 1) / rows) *
+                     ((structs_in[s].pitch + 127) / 128);
+        variant = warps >= ROW_MARCH_MIN_WARPS ? 1 : 2;
+    }
     if (variant == 2) rows = TROWS;
     int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     if (ring_slot_elems < 0 || (ring_slot_elems & 3))
@@ -1384,6 +1402,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     p->n_structs = n;
     p->rows = rows;
     p->variant = variant;
+    p->graph_mode = (tuning && tuning->graph < 0) ? -1 : 0;
     p->n_cols = n_amp_cols;
     p->n_work = (int)n_work;
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
@@ -1443,6 +1462,91 @@ int mtb_yee2d_check(mtb_yee2d_plan *p, void *stream) {
     return MTB_OK;
 }
 
+// One step's kernels on `st`.
+static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
+    const int n_tm = p->n_work_tm, n_te = p->n_work - p->n_work_tm;
+    const mtb_yee2d_struct *SS = p->structs_d.as<mtb_yee2d_struct>();
+    const int4 *W = p->work_d.as<int4>();
+    if (p->variant == 2) {
+        const dim3 blk(32, TROWS);
+        if (n_tm > 0) {
+            if (C.first)
+                k_tile_tm<true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+            else
+                k_tile_tm<false><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+            MTB_CHECK_LAUNCH();
+            ++p->last_launches;
+        }
+        if (n_te > 0) {
+            k_tile_te<<<n_te, blk, 0, st>>>(SS, W + n_tm, n_te, C);
+            MTB_CHECK_LAUNCH();
+            ++p->last_launches;
+        }
+        return MTB_OK;
+    }
+    const int blocks_tm = (n_tm + WARPS2D - 1) / WARPS2D;
+    const int blocks_te = (n_te + WARPS2D - 1) / WARPS2D;
+    if (n_tm > 0) {
+        if (C.first)
+            k_yee2d_tm<true><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(SS, W, n_tm, C);
+        else
+            k_yee2d_tm<false><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(SS, W, n_tm, C);
+        MTB_CHECK_LAUNCH();
+        ++p->last_launches;
+    }
+    if (n_te > 0) {
+        k_yee2d_te<<<blocks_te, 32 * WARPS2D, smem_te(), st>>>(SS, W + n_tm, n_te, C);
+        MTB_CHECK_LAUNCH();
+        ++p->last_launches;
+    }
+    return MTB_OK;
+}
+
+// Capture one ring flush (G steps from parity par0, then the contraction)
+// reading its coefficient and phase rows from the plan's staging buffer.
+static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
+    const int G = p->dft.slots;
+    if (!p->cap) MTB_CUDA_TRY(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    const float *stage = p->stage_d.as<float>();
+    const float *phase = stage + 2 * (size_t)G * nc;
+    const int64_t l0 = mtb_launch_count(), ll0 = p->last_launches;
+    MTB_CUDA_TRY(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+    int rc = MTB_OK;
+    int par = par0;
+    for (int s = 0; s < G && !rc; ++s) {
+        Ctx2D C;
+        C.amp_e = stage + (size_t)s * nc;
+        C.amp_h = stage + (size_t)G * nc + (size_t)s * nc;
+        C.ring = p->dft.ring_d.as<float>() + (size_t)s * p->dft.slot_elems;
+        C.err = p->err_d.as<int>();
+        C.par = par;
+        C.first = 0;
+        rc = launch_step(p, C, p->cap);
+        par ^= 1;
+    }
+    if (!rc && p->dft.n_regions > 0) {
+        rc = p->dft.contract(0, G, p->cap, nullptr, phase);
+        if (!rc) ++p->last_launches;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(p->cap, &g);
+    const int64_t nk = mtb_launch_count() - l0;
+    count_launch(-nk);                           // captured, not launched
+    p->last_launches = ll0;
+    if (!rc && e != cudaSuccess)
+        rc = fail(MTB_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(e));
+    if (!rc) {
+        const cudaError_t ei = cudaGraphInstantiate(&p->gexec[par0], g, 0);
+        if (ei != cudaSuccess) {
+            p->gexec[par0] = nullptr;
+            rc = fail(MTB_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ei));
+        }
+    }
+    if (g) cudaGraphDestroy(g);
+    p->gkern[par0] = nk;
+    return rc;
+}
+
 int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e,
                   const double *coef_h, void *stream) {
     if (!p) return fail(MTB_INVALID_ARG, "plan is null");
@@ -1465,11 +1569,34 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, p->amp_h.p, 2 * per * sizeof(float),
                                  cudaMemcpyHostToDevice, st));
     const float *ad = p->amp_d.as<float>();
-    const int n_tm = p->n_work_tm, n_te = p->n_work - p->n_work_tm;
-    const int blocks_tm = (n_tm + WARPS2D - 1) / WARPS2D;
-    const int blocks_te = (n_te + WARPS2D - 1) / WARPS2D;
+    const int G = p->dft.slots;
+    const size_t prow = (size_t)p->dft.total_nf * 4;         // floats per phase row
+    const bool graphs = p->graph_mode >= 0 && !p->timer.on && G >= 2 && k >= 2 * G;
+    if (graphs && (rc = p->stage_d.ensure(sizeof(float) * (2 * (size_t)G * nc + G * prow))))
+        return rc;
     int slot = 0;
-    for (int s = 0; s < k; ++s) {
+    int s = 0;
+    while (s < k) {
+        if (graphs && slot == 0 && !p->first && k - s >= G) {
+            // one ring flush as a graph replay: stage its rows, launch
+            float *stage = p->stage_d.as<float>();
+            MTB_CUDA_TRY(cudaMemcpyAsync(stage, ad + (size_t)s * nc, sizeof(float) * G * nc,
+                                         cudaMemcpyDeviceToDevice, st));
+            MTB_CUDA_TRY(cudaMemcpyAsync(stage + (size_t)G * nc, ad + per + (size_t)s * nc,
+                                         sizeof(float) * G * nc, cudaMemcpyDeviceToDevice, st));
+            if (prow > 0 && p->dft.n_regions > 0)
+                MTB_CUDA_TRY(cudaMemcpyAsync(stage + 2 * (size_t)G * nc,
+                                             p->dft.phase_d.as<float>() + (size_t)s * prow,
+                                             sizeof(float) * G * prow, cudaMemcpyDeviceToDevice,
+                                             st));
+            if (!p->gexec[p->par] && (rc = build_flush_graph(p, p->par, nc))) return rc;
+            MTB_CUDA_TRY(cudaGraphLaunch(p->gexec[p->par], st));
+            count_launch(p->gkern[p->par]);
+            p->last_launches += p->gkern[p->par];
+            p->par ^= (G & 1);
+            s += G;
+            continue;
+        }
         Ctx2D C;
         C.amp_e = ad + (size_t)s * nc;
         C.amp_h = ad + per + (size_t)s * nc;
@@ -1478,51 +1605,19 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
         C.par = p->par;
         C.first = p->first;
         if ((rc = p->timer.begin(st, 0))) return rc;
-        if (p->variant == 2) {
-            const dim3 blk(32, TROWS);
-            if (n_tm > 0) {
-                if (p->first)
-                    k_tile_tm<true><<<n_tm, blk, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
-                                                         p->work_d.as<int4>(), n_tm, C);
-                else
-                    k_tile_tm<false><<<n_tm, blk, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
-                                                          p->work_d.as<int4>(), n_tm, C);
-                MTB_CHECK_LAUNCH();
-                ++p->last_launches;
-            }
-            if (n_te > 0) {
-                k_tile_te<<<n_te, blk, 0, st>>>(p->structs_d.as<mtb_yee2d_struct>(),
-                                                p->work_d.as<int4>() + n_tm, n_te, C);
-                MTB_CHECK_LAUNCH();
-                ++p->last_launches;
-            }
-        } else if (n_tm > 0) {
-            if (p->first)
-                k_yee2d_tm<true><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(
-                    p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>(), n_tm, C);
-            else
-                k_yee2d_tm<false><<<blocks_tm, 32 * WARPS2D, smem_tm(), st>>>(
-                    p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>(), n_tm, C);
-            MTB_CHECK_LAUNCH();
-            ++p->last_launches;
-        }
-        if (p->variant == 1 && n_te > 0) {
-            k_yee2d_te<<<blocks_te, 32 * WARPS2D, smem_te(), st>>>(
-                p->structs_d.as<mtb_yee2d_struct>(), p->work_d.as<int4>() + n_tm, n_te, C);
-            MTB_CHECK_LAUNCH();
-            ++p->last_launches;
-        }
+        if ((rc = launch_step(p, C, st))) return rc;
         if ((rc = p->timer.end(st))) return rc;
         p->par ^= 1;
         p->first = 0;
         ++slot;
-        if (slot == p->dft.slots || s == k - 1) {
+        if (slot == G || s == k - 1) {
             if (p->dft.n_regions > 0) {
                 if ((rc = p->dft.contract(s + 1 - slot, slot, st, &p->timer))) return rc;
                 ++p->last_launches;
             }
             slot = 0;
         }
+        ++s;
     }
     return p->timer.collect();
 }
@@ -1551,6 +1646,10 @@ int64_t mtb_yee2d_last_launches(const mtb_yee2d_plan *p) { return p ? p->last_la
 
 void mtb_yee2d_plan_destroy(mtb_yee2d_plan *p) {
     if (!p) return;
+    for (int q = 0; q < 2; ++q)
+        if (p->gexec[q]) cudaGraphExecDestroy(p->gexec[q]);
+    if (p->cap) cudaStreamDestroy(p->cap);
+    p->stage_d.release();
     p->structs_d.release();
     p->work_d.release();
     p->amp_d.release();

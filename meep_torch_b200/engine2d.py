@@ -133,7 +133,7 @@ class Engine2D:
     the reference's types and shapes."""
 
     def __init__(self, items, *, phase_mode: str = "exact", rows_per_warp: int = 0,
-                 ring_slots: int = 0, variant: int = 0, stream=None):
+                 ring_slots: int = 0, variant: int = 0, graph: bool = True, stream=None):
         self.lib = L.load()
         self.items = [_Item(*it) for it in items]
         _need(len(self.items) > 0, "empty batch")
@@ -143,7 +143,7 @@ class Engine2D:
         self.t = None
         for it in self.items:
             self._validate(it)
-        self._build(rows_per_warp, ring_slots, variant)
+        self._build(rows_per_warp, ring_slots, variant, graph)
 
     # ---------------------------------------------------------------- import
     def _validate(self, it: _Item):
@@ -222,7 +222,7 @@ class Engine2D:
         it.keep += [*hx, *hy, *ex, *ey]
         return hx, hy, ex, ey
 
-    def _build(self, rows_per_warp, ring_slots, variant=0):
+    def _build(self, rows_per_warp, ring_slots, variant=0, graph=True):
         lib = self.lib
         dev = self.device
         structs = (L.Yee2DStruct * len(self.items))()
@@ -428,7 +428,7 @@ class Engine2D:
         self.n_regions = len(regions)
         self.groups = grp_arr
         self.n_groups = len(groups)
-        tun = L.Tuning(rows_per_warp, ring_slots, 0, variant)
+        tun = L.Tuning(rows_per_warp, ring_slots, 0 if graph else -1, variant)
         plan = C.c_void_p()
         L.check(lib.mtb_yee2d_plan_create(structs, len(self.items), reg_arr, len(regions),
                                           grp_arr, len(groups), ring, amp_cols, C.byref(tun),

@@ -104,7 +104,7 @@ def cfg1_spec():
                 freqs=tuple(np.linspace(0.1, 0.2, 50).tolist()), steps=4000)
 
 
-def cfg1_item(device, spec=None):
+def cfg1_item(device, spec=None, eps_t=None):
     from .core.coeffs import build_tm_coeffs
     from .core.grid import Grid
     from .core.monitors import FluxMonitorTM
@@ -112,7 +112,8 @@ def cfg1_item(device, spec=None):
     from .core.stepper_tm import init_tm_state
     spec = spec or cfg1_spec()
     g = Grid(nx=spec["nx"], ny=spec["ny"], dx=DX2D, device=device)
-    m = build_tm_coeffs(g, eps_inf=torch.from_numpy(spec["eps"]).to(device), npml=NPML2D)
+    eps = eps_t if eps_t is not None else torch.from_numpy(spec["eps"]).to(device)
+    m = build_tm_coeffs(g, eps_inf=eps, npml=NPML2D)
     i, j = spec["src"]
     src = LineSource(g, ix=i, j0=j, j1=j + 1, profile=GaussianPulse(0.15, 0.1))
     ix, lo, hi = spec["flux"]
