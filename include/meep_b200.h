@@ -255,6 +255,49 @@ int mtb_yee2d_timing(const mtb_yee2d_plan *plan, double *step_ms, int64_t *step_
 
 void mtb_yee2d_plan_destroy(mtb_yee2d_plan *plan);
 
+/* The plan's DFT sample ring: slot s (0 <= s < ring_slots) of the last run
+ * holds the samples of that run's step s (ring + s * slot_elems), in the
+ * layout the structures' ring_full / lines offsets describe. */
+int mtb_yee2d_ring(const mtb_yee2d_plan *plan, float **ring, int64_t *slot_elems,
+                   int32_t *ring_slots);
+
+/* ------------------------------------------------------- 2D TM adjoint */
+/* Discrete adjoint (reverse mode) of the TM step, the transpose of
+ * core/stepper_tm.py:234-254 with CPML (PEC walls, sigma = 0, no poles) and
+ * of the DFT / flux sampling (core/monitors.py:24-100): what torch autograd
+ * computes through the reference's run_tm (core/run.py:43-120).
+ *
+ * Adjoint state (box layout of the structure, nx x pitch floats each, one
+ * buffer per array), holding on entry d J / d (state after the last step of
+ * the call) and on return d J / d (state before its first step):
+ *   g[0] Ez, g[1] Hx, g[2] Hy, g[3] Dz, g_psi[0..3] as mtb_yee2d_struct psi.
+ * tmp[0..3]: scratch of the same size. g_eps accumulates d J / d eps_inf
+ * (box layout; the caller zeroes it once). */
+typedef struct mtb_adj2d_buffers {
+    float *g[4];
+    float *g_psi[4];
+    float *tmp[4];
+    float *g_eps;
+} mtb_adj2d_buffers;
+
+typedef struct mtb_yee2d_adjoint mtb_yee2d_adjoint;
+
+/* `s` is the forward structure (its ring_full / lines give the sample
+ * layout of the forward ring, slot size ring_slot_elems); `regions` are the
+ * forward DFT regions with `acc` pointing at d J / d acc (read only). */
+int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers *bufs,
+                             const mtb_dft_region *regions, int32_t n_regions,
+                             const mtb_phase_group *groups, int32_t n_groups,
+                             int64_t ring_slot_elems, int32_t ring_slots,
+                             mtb_yee2d_adjoint **out);
+/* Reverse steps t0+k-1 .. t0 (k <= ring_slots). `rec` slot q holds the
+ * forward Ez after step t0+q at element rec_offset + box index (the ring of
+ * a forward plan that ran these k steps with a full-grid Ez sample). */
+int mtb_yee2d_adjoint_run(mtb_yee2d_adjoint *p, int64_t t0, int32_t k, const float *rec,
+                          int64_t rec_slot_elems, int64_t rec_offset, void *stream);
+int64_t mtb_yee2d_adjoint_last_launches(const mtb_yee2d_adjoint *p);
+void mtb_yee2d_adjoint_destroy(mtb_yee2d_adjoint *p);
+
 /* ---------------------------------------------------------------- 3D */
 
 /* One 3D structure (State3D / Coeffs3D, CPML path, sigma = 0, no poles).
@@ -342,7 +385,7 @@ const char *mtb_last_error(void);
 int32_t mtb_abi_version(void);
 /* sizeof of the ABI structs, for binding checks: 0 mtb_cells,
  * 1 mtb_line_sample, 2 mtb_yee2d_struct, 3 mtb_phase_group,
- * 4 mtb_dft_region, 5 mtb_tuning, 6 mtb_yee3d_struct */
+ * 4 mtb_dft_region, 5 mtb_tuning, 6 mtb_yee3d_struct, 7 mtb_adj2d_buffers */
 int64_t mtb_struct_size(int32_t which);
 /* Kernels launched by this library since load (all entry points). */
 int64_t mtb_launch_count(void);

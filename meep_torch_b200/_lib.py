@@ -75,7 +75,12 @@ class Yee3DStruct(C.Structure):
                 ("pad2_", C.c_int32)]
 
 
-STRUCTS = [Cells, LineSample, Yee2DStruct, PhaseGroup, DftRegion, Tuning, Yee3DStruct]
+class Adj2DBuffers(C.Structure):
+    _fields_ = [("g", vp * 4), ("g_psi", vp * 4), ("tmp", vp * 4), ("g_eps", vp)]
+
+
+STRUCTS = [Cells, LineSample, Yee2DStruct, PhaseGroup, DftRegion, Tuning, Yee3DStruct,
+           Adj2DBuffers]
 
 # name -> (restype, argtypes); the exported C ABI (include/meep_b200.h)
 SIGNATURES = {
@@ -92,6 +97,16 @@ SIGNATURES = {
                                         C.POINTER(C.c_double), vp]),
     "mtb_yee2d_last_launches": (C.c_int64, [vp]),
     "mtb_yee2d_plan_destroy": (None, [vp]),
+    "mtb_yee2d_ring": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int32)]),
+    "mtb_yee2d_adjoint_create": (C.c_int, [C.POINTER(Yee2DStruct), C.POINTER(Adj2DBuffers),
+                                           C.POINTER(DftRegion), C.c_int32,
+                                           C.POINTER(PhaseGroup), C.c_int32, C.c_int64,
+                                           C.c_int32, C.POINTER(vp)]),
+    "mtb_yee2d_adjoint_run": (C.c_int, [vp, C.c_int64, C.c_int32, vp, C.c_int64, C.c_int64,
+                                        vp]),
+    "mtb_yee2d_adjoint_last_launches": (C.c_int64, [vp]),
+    "mtb_yee2d_adjoint_destroy": (None, [vp]),
     "mtb_yee2d_set_timing": (C.c_int, [vp, C.c_int32]),
     "mtb_yee2d_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

@@ -1,0 +1,181 @@
+"""Reverse-mode gradients of the 2D TM run through the B200 kernels.
+
+The reference gets dJ/d eps from torch autograd through ``run_tm`` (core/run.py:43-120),
+optionally checkpointed (``checkpoint_every``). Here the same derivative comes from the
+library's discrete-adjoint kernels (``mtb_yee2d_adjoint_*``): the exact transpose of the
+forward TM step with CPML and of the DFT / flux sampling, run backwards in time.
+
+Forward: the run goes in chunks of ``chunk`` steps (the ring depth); the live state at each
+chunk start is kept (box layout). Backward, chunk by chunk from the last: the chunk is
+re-run from its snapshot on a recording plan whose ring keeps the full-grid Ez of every step
+(needed for d/d eps of E = D / eps), then the adjoint plan sweeps the chunk's steps in
+reverse. Gradients reach ``coeffs.eps_inf``; other coefficient tensors and the initial state
+receive none (a gradient request for them raises NotImplementedError).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib as L
+from .engine2d import Engine2D
+
+STATE_TM = ("Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy")
+
+
+class _Grid:
+    """The attributes a DFTFieldsMonitor takes from a Grid."""
+
+    def __init__(self, dt, device):
+        self.dt, self.dtype, self.device = dt, torch.float32, device
+
+
+def _record_monitor(dt, device):
+    from .core.monitors import DFTFieldsMonitor
+    return DFTFieldsMonitor(_Grid(dt, device), [1.0], "Ez")
+
+
+class TMGradRun:
+    """One differentiable TM run: forward() keeps chunk snapshots, backward()
+    turns output gradients into d J / d eps_inf."""
+
+    def __init__(self, state, coeffs, n_steps, source, monitors, chunk=32,
+                 phase_mode="exact"):
+        if type(state).__name__ != "TMState" and not hasattr(state, "Ez"):
+            raise L.MtbUnsupported("gradients: TM states only on the B200 path")
+        if getattr(coeffs, "y_pmc", False):
+            raise L.MtbUnsupported("gradients: PEC walls only (y_pmc)")
+        self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
+        self.source, self.monitors = source, list(monitors)
+        self.chunk = max(1, min(int(chunk), 64))
+        self.phase_mode = phase_mode
+        self.chunks = [(s0, min(self.chunk, self.n - s0)) for s0 in range(0, self.n, self.chunk)]
+
+    def forward(self):
+        eng = Engine2D([(self.state0, self.coeffs, self.source, self.monitors)],
+                       phase_mode=self.phase_mode, ring_slots=self.chunk, graph=False)
+        self.snaps = []
+        for s0, k in self.chunks:
+            self.snaps.append(eng.snapshot(0))
+            eng.run(s0, k)
+        st = eng.state(0)
+        self.out_state = st
+        self.accs = [a.clone() for a in eng.accumulators(0)]
+        self.eng = eng
+        return [getattr(st, f) for f in STATE_TM] + self.accs
+
+    def backward(self, grads):
+        eng, lib = self.eng, L.load()
+        it = eng.items[0]
+        nx, ny = it.nx, it.ny
+        P = int(eng.structs[0].pitch)
+        dev = eng.device
+        box = lambda: torch.zeros((nx, P), dtype=torch.float32, device=dev)  # noqa: E731
+        g, gpsi, tmp, geps = [box() for _ in range(4)], [box() for _ in range(4)], \
+            [box() for _ in range(4)], box()
+        targets = g + gpsi
+        yoff = 0 if self.out_state.psi_Hyx.shape[1] == ny else 1
+        offs = [(0, 0)] * 6 + [(1, yoff), (1, yoff)]
+        ns = len(STATE_TM)
+        for q, name in enumerate(STATE_TM):
+            gr = grads[q]
+            if gr is None or gr.numel() == 0:
+                continue
+            targets[q].copy_(eng._pack(gr, nx, P, offs[q]))
+        # d J / d acc in the forward regions' layout
+        gaccs = []
+        for q, a in enumerate(self.accs):
+            gr = grads[ns + q]
+            gaccs.append(torch.zeros_like(a) if gr is None
+                         else gr.detach().to(torch.float32).contiguous())
+        by_ptr = {L.ptr(a): q for q, a in enumerate(it.accs)}
+        nreg = eng.n_regions
+        regs = (L.DftRegion * max(1, nreg))()
+        for r in range(nreg):
+            C.memmove(C.addressof(regs[r]), C.addressof(eng.regions[r]), C.sizeof(L.DftRegion))
+            regs[r].acc = L.ptr(gaccs[by_ptr[int(eng.regions[r].acc)]])
+        bufs = L.Adj2DBuffers()
+        for q in range(4):
+            bufs.g[q], bufs.g_psi[q], bufs.tmp[q] = L.ptr(g[q]), L.ptr(gpsi[q]), L.ptr(tmp[q])
+        bufs.g_eps = L.ptr(geps)
+        adj = C.c_void_p()
+        L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
+                                             regs if nreg else None, nreg, eng.groups,
+                                             eng.n_groups, eng.ring_elems, self.chunk,
+                                             C.byref(adj)), "mtb_yee2d_adjoint_create")
+        keep = [gaccs, g, gpsi, tmp, geps]
+        stream = eng._sptr()
+        try:
+            rec_mon = _record_monitor(float(self.coeffs.dt), dev)
+            zero = type(self.state0)(*[torch.zeros_like(t) if torch.is_tensor(t) else t
+                                       for t in self.state0])
+            rec = None
+            for c in range(len(self.chunks) - 1, -1, -1):
+                s0, k = self.chunks[c]
+                if c == 0:       # the initial state as imported (explicit Ez honoured)
+                    if rec is not None:
+                        rec.close()
+                    rec = Engine2D([(self.state0, self.coeffs, self.source, [rec_mon])],
+                                   phase_mode=self.phase_mode, ring_slots=self.chunk,
+                                   graph=False)
+                else:
+                    if rec is None:
+                        rec = Engine2D([(zero, self.coeffs, self.source, [rec_mon])],
+                                       phase_mode=self.phase_mode, ring_slots=self.chunk,
+                                       graph=False)
+                    rec.restore(0, self.snaps[c])
+                rec.run(s0, k)
+                ring, selems, nslots = C.c_void_p(), C.c_int64(), C.c_int32()
+                L.check(lib.mtb_yee2d_ring(rec.plan, C.byref(ring), C.byref(selems),
+                                           C.byref(nslots)), "mtb_yee2d_ring")
+                L.check(lib.mtb_yee2d_adjoint_run(adj, s0, k, ring, selems.value,
+                                                  int(rec.structs[0].ring_full[0]), stream),
+                        "mtb_yee2d_adjoint_run")
+            if rec is not None:
+                rec.close()
+        finally:
+            lib.mtb_yee2d_adjoint_destroy(adj)
+        del keep
+        return eng._unpack(geps, (nx, ny))
+
+    def release(self):
+        if getattr(self, "eng", None) is not None:
+            self.eng.close()
+            self.eng = None
+        self.snaps = []
+
+
+class _TMRunFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, eps_inf, runner):
+        outs = runner.forward()
+        ctx.runner = runner
+        return tuple(outs)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        runner = ctx.runner
+        try:
+            g_eps = runner.backward(grads)
+        finally:
+            runner.release()
+        return g_eps.to(dtype=runner.coeffs.eps_inf.dtype), None
+
+
+def run_tm_grad(state, coeffs, n_steps, *, source=None, monitors=(), checkpoint_every=0,
+                phase_mode="exact"):
+    """Differentiable run_tm: returns (state, accs) connected to coeffs.eps_inf."""
+    for f in getattr(coeffs, "_fields", ()):
+        t = getattr(coeffs, f)
+        if torch.is_tensor(t) and t.requires_grad and f != "eps_inf":
+            raise L.MtbUnsupported(f"gradients with respect to coeffs.{f} on the B200 path")
+    for t in state:
+        if torch.is_tensor(t) and t.requires_grad:
+            raise L.MtbUnsupported("gradients with respect to the initial state on the B200 path")
+    chunk = checkpoint_every if 0 < checkpoint_every <= 64 else 32
+    runner = TMGradRun(state, coeffs, n_steps, source, monitors, chunk, phase_mode)
+    outs = _TMRunFn.apply(coeffs.eps_inf, runner)
+    ns = len(STATE_TM)
+    st = runner.out_state._replace(**dict(zip(STATE_TM, outs[:ns])))
+    return st, list(outs[ns:])

@@ -1,0 +1,300 @@
+// Discrete adjoint of the 2D TM step for sm_100a: the exact transpose of the
+// forward update (core/stepper_tm.py:234-254: B phase :85-128, D phase
+// :130-166, E = D / eps :221-231) with CPML (kappa = 1, PEC walls, sigma = 0,
+// no poles), and of the monitors' sampling (core/monitors.py:24-100). This is
+// what torch autograd computes through the reference's run_tm
+// (core/run.py:43-120); the source terms are additive constants and have no
+// adjoint.
+//
+// Reverse of forward step t (state_t -> state_{t+1}), adjoint state A holding
+// dJ/d state_{t+1} on entry and dJ/d state_t on exit, three kernels:
+//   k_adj_tm_e   (Ez/Dz nodes) monitor samples of Ez_{t+1} into gEz;
+//                E = D / eps:  gD = gDz + gEz / eps, g_eps -= gEz Ez_{t+1} / eps;
+//                D += dt pad(curl): g_curl = dt gD on the interior; the two psi
+//                recursions of the curl; writes gDz, g_psi2, g_psi3 and the
+//                adjoints of dHy/dx (tmp0) and dHx/dy (tmp1).
+//   k_adj_tm_h   (H nodes) monitor samples of H_{t+1/2} into gHx, gHy; the
+//                transposed differences of tmp0 / tmp1; H += -/+ dt curl E
+//                with its psi recursions; writes gHx, gHy, g_psi0, g_psi1 and
+//                the adjoints of dEz/dx (tmp2) and dEz/dy (tmp3).
+//   k_adj_tm_ez  (Ez nodes) gEz = transposed differences of tmp2 / tmp3.
+// The monitor adjoint of a whole chunk comes first: DftState::expand fills
+// ring slot q with dJ/d(sample of step t0+q) in the forward ring's layout, and
+// the kernels add it back at the cells the forward kernels sampled.
+#include <algorithm>
+
+#include "mtb_common.cuh"
+
+namespace mtb {
+
+constexpr int AROWS = 8;          // rows per block (one warp per row)
+
+__device__ __forceinline__ void ldv(const float *p, float (&v)[4]) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void stv(float *p, const float (&v)[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// Add the adjoint ring's values for the forward samples of component `comp`
+// at row i, columns jb .. jb+3 (the transpose of the forward kernels'
+// full-grid sample and line samples).
+__device__ __forceinline__ void inject(const mtb_yee2d_struct &S, int comp, int i, int jb,
+                                       uint32_t g, const float *__restrict__ radj,
+                                       float (&v)[4]) {
+    const int64_t rf = S.ring_full[comp];
+    if (rf >= 0) {
+        float r[4];
+        ldv(radj + rf + g, r);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] += r[q];
+    }
+    for (int l = 0; l < S.n_lines; ++l) {
+        const mtb_line_sample ln = S.lines[l];
+        if (ln.comp != comp) continue;
+        if (ln.kind == 0) {
+            if (ln.index != i) continue;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = jb + q;
+                if (j >= ln.lo && j < ln.hi) v[q] += radj[ln.ring_off + (j - ln.lo)];
+            }
+        } else {
+            if (i < ln.lo || i >= ln.hi) continue;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (jb + q == ln.index) v[q] += radj[ln.ring_off + (i - ln.lo)];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__ mtb_yee2d_struct S,
+                                                         const __grid_constant__ mtb_adj2d_buffers B,
+                                                         const float *__restrict__ radj,
+                                                         const float *__restrict__ rec) {
+    const int i = blockIdx.y * AROWS + threadIdx.y;
+    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    if (i >= nx || jb >= P) return;
+    const uint32_t g = (uint32_t)i * P + jb;
+    const float dt = S.dt;
+    float gez[4], gdz[4], gp2[4], gp3[4], ez[4], ie[4], ge[4];
+    ldv(B.g[0] + g, gez);
+    ldv(B.g[3] + g, gdz);
+    ldv(B.g_psi[2] + g, gp2);
+    ldv(B.g_psi[3] + g, gp3);
+    ldv(rec + g, ez);
+    ldv(S.inv_eps_a + g, ie);
+    ldv(B.g_eps + g, ge);
+    inject(S, MTB_C2_MAIN, i, jb, g, radj, gez);
+    const bool rowin = i >= 1 && i <= nx - 2;
+    float bex = 1.f, aex = 0.f;
+    if (rowin) { bex = S.ex_b[i]; aex = S.ex_a[i]; }
+    float t1[4], t2[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        const bool inside = j < ny;
+        const bool interior = rowin && j >= 1 && j <= ny - 2;
+        const float gd = gdz[q] + gez[q] * ie[q];
+        ge[q] -= gez[q] * ez[q] * ie[q];
+        const float gc = interior ? dt * gd : 0.f;
+        const float g2 = gp2[q] + gc, g3 = gp3[q] - gc;
+        const float bey = interior ? S.ey_b[j] : 1.f, aey = interior ? S.ey_a[j] : 0.f;
+        t1[q] = interior ? gc + aex * g2 : 0.f;
+        t2[q] = interior ? -gc + aey * g3 : 0.f;
+        gp2[q] = interior ? bex * g2 : gp2[q];
+        gp3[q] = interior ? bey * g3 : gp3[q];
+        gdz[q] = inside ? gd : 0.f;
+    }
+    stv(B.g[3] + g, gdz);
+    stv(B.g_psi[2] + g, gp2);
+    stv(B.g_psi[3] + g, gp3);
+    stv(B.tmp[0] + g, t1);
+    stv(B.tmp[1] + g, t2);
+    stv(B.g_eps + g, ge);
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__ mtb_yee2d_struct S,
+                                                         const __grid_constant__ mtb_adj2d_buffers B,
+                                                         const float *__restrict__ radj) {
+    const int i = blockIdx.y * AROWS + threadIdx.y;
+    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    if (i >= nx || jb >= P) return;
+    const uint32_t g = (uint32_t)i * P + jb;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    float ghx[4], ghy[4], gp0[4], gp1[4], t1[4], t1n[4], t2[4];
+    ldv(B.g[1] + g, ghx);
+    ldv(B.g[2] + g, ghy);
+    ldv(B.g_psi[0] + g, gp0);
+    ldv(B.g_psi[1] + g, gp1);
+    ldv(B.tmp[0] + g, t1);
+    ldv(B.tmp[1] + g, t2);
+    if (i + 1 < nx) ldv(B.tmp[0] + g + P, t1n);
+    else t1n[0] = t1n[1] = t1n[2] = t1n[3] = 0.f;
+    const float t2r = (jb + 4 < P) ? B.tmp[1][g + 4] : 0.f;
+    inject(S, MTB_C2_X, i, jb, g, radj, ghx);
+    inject(S, MTB_C2_Y, i, jb, g, radj, ghy);
+    const bool vrow = i <= nx - 2;
+    float bhx = 1.f, ahx = 0.f;
+    if (vrow) { bhx = S.hx_b[i]; ahx = S.hx_a[i]; }
+    float t3[4], t4[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        const float t2n = (q < 3) ? t2[q + 1] : t2r;
+        const float gyp = ghy[q] + (t1[q] - t1n[q]) * rdx;
+        const float gxp = ghx[q] + (t2[q] - t2n) * rdx;
+        const bool vy = vrow && j < ny, vx = j <= ny - 2;
+        // Hy += dt (dEz/dx + psi_Ezx'), psi_Ezx' = b_hx psi + a_hx dEz/dx
+        const float g1 = gp1[q] + dt * gyp;
+        t3[q] = vy ? dt * gyp + ahx * g1 : 0.f;
+        gp1[q] = vy ? bhx * g1 : gp1[q];
+        ghy[q] = vy ? gyp : 0.f;
+        // Hx -= dt (dEz/dy + psi_Ezy'), psi_Ezy' = b_hy psi + a_hy dEz/dy
+        const float bhy = vx ? S.hy_b[j] : 1.f, ahy = vx ? S.hy_a[j] : 0.f;
+        const float g0 = gp0[q] - dt * gxp;
+        t4[q] = vx ? -dt * gxp + ahy * g0 : 0.f;
+        gp0[q] = vx ? bhy * g0 : gp0[q];
+        ghx[q] = vx ? gxp : 0.f;
+    }
+    stv(B.g[1] + g, ghx);
+    stv(B.g[2] + g, ghy);
+    stv(B.g_psi[0] + g, gp0);
+    stv(B.g_psi[1] + g, gp1);
+    stv(B.tmp[2] + g, t3);
+    stv(B.tmp[3] + g, t4);
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant__ mtb_yee2d_struct S,
+                                                          const __grid_constant__ mtb_adj2d_buffers B) {
+    const int i = blockIdx.y * AROWS + threadIdx.y;
+    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    if (i >= nx || jb >= P) return;
+    const uint32_t g = (uint32_t)i * P + jb;
+    const float rdx = 1.0f / S.dx;
+    float t3[4], t3p[4], t4[4];
+    ldv(B.tmp[2] + g, t3);
+    if (i >= 1) ldv(B.tmp[2] + g - P, t3p);
+    else t3p[0] = t3p[1] = t3p[2] = t3p[3] = 0.f;
+    ldv(B.tmp[3] + g, t4);
+    const float t4l = (jb >= 1) ? B.tmp[3][g - 1] : 0.f;
+    float gez[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float t4m = (q == 0) ? t4l : t4[q - 1];
+        gez[q] = (jb + q < ny) ? (t3p[q] - t3[q]) * rdx + (t4m - t4[q]) * rdx : 0.f;
+    }
+    stv(B.g[0] + g, gez);
+}
+
+}  // namespace mtb
+
+using namespace mtb;
+
+struct mtb_yee2d_adjoint {
+    mtb_yee2d_struct s{};
+    mtb_adj2d_buffers b{};
+    DftState dft;
+    int64_t last_launches = 0;
+};
+
+extern "C" {
+
+int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers *bufs,
+                             const mtb_dft_region *regions, int32_t n_regions,
+                             const mtb_phase_group *groups, int32_t n_groups,
+                             int64_t ring_slot_elems, int32_t ring_slots,
+                             mtb_yee2d_adjoint **out) {
+    if (!out || !s || !bufs) return fail(MTB_INVALID_ARG, "null argument");
+    *out = nullptr;
+    const mtb_yee2d_struct &S = *s;
+    if (S.pol != MTB_TM) return fail(MTB_UNSUPPORTED, "adjoint: TM structures only");
+    if (S.y_pmc) return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc)");
+    if (S.nx < 3 || S.ny < 3 || S.pitch < S.ny || (S.pitch & 3))
+        return fail(MTB_INVALID_ARG, "adjoint: bad grid %d x %d, pitch %d", S.nx, S.ny, S.pitch);
+    if ((int64_t)S.nx * S.pitch >= (1LL << 31)) return fail(MTB_UNSUPPORTED, "grid too large");
+    if (S.nx > 65535 * AROWS) return fail(MTB_UNSUPPORTED, "adjoint: nx too large");
+    auto bad = [](const void *p) { return !p || (reinterpret_cast<uintptr_t>(p) & 15); };
+    for (int c = 0; c < 4; ++c)
+        if (bad(bufs->g[c]) || bad(bufs->g_psi[c]) || bad(bufs->tmp[c]))
+            return fail(MTB_INVALID_ARG, "adjoint: null or unaligned buffer");
+    if (bad(bufs->g_eps) || bad(S.inv_eps_a))
+        return fail(MTB_INVALID_ARG, "adjoint: null or unaligned g_eps / inv_eps");
+    if (!S.hx_b || !S.hx_a || !S.hy_b || !S.hy_a || !S.ex_b || !S.ex_a || !S.ey_b || !S.ey_a)
+        return fail(MTB_INVALID_ARG, "adjoint: null CPML profile");
+    if (S.n_lines < 0 || (S.n_lines > 0 && !S.lines))
+        return fail(MTB_INVALID_ARG, "adjoint: bad line samples");
+    for (int c = 0; c < 3; ++c) {
+        const int64_t o = S.ring_full[c];
+        if (o >= 0 && ((o & 3) || o + (int64_t)S.nx * S.pitch > ring_slot_elems))
+            return fail(MTB_INVALID_ARG, "adjoint: full-grid ring offset %lld invalid",
+                        (long long)o);
+    }
+    if (ring_slot_elems & 3) return fail(MTB_INVALID_ARG, "ring_slot_elems must be a multiple of 4");
+    mtb_yee2d_adjoint *p = new mtb_yee2d_adjoint();
+    p->s = S;
+    p->b = *bufs;
+    const int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems,
+                               ring_slots > 0 ? ring_slots : 32);
+    if (rc) { p->dft.release(); delete p; return rc; }
+    // the adjoint ring must exist even without regions (line / full samples read it)
+    if (n_regions == 0) {
+        const int rc2 = p->dft.ring_d.ensure(sizeof(float) * (size_t)std::max<int64_t>(
+                                                                ring_slot_elems, 4) * p->dft.slots);
+        if (rc2) { p->dft.release(); delete p; return rc2; }
+    }
+    *out = p;
+    return MTB_OK;
+}
+
+int mtb_yee2d_adjoint_run(mtb_yee2d_adjoint *p, int64_t t0, int32_t k, const float *rec,
+                          int64_t rec_slot_elems, int64_t rec_offset, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "adjoint plan is null");
+    p->last_launches = 0;
+    if (k <= 0) return MTB_OK;
+    if (k > p->dft.slots) return fail(MTB_INVALID_ARG, "k %d > ring slots %d", k, p->dft.slots);
+    if (!rec || (rec_offset & 3) || (rec_slot_elems & 3) ||
+        (reinterpret_cast<uintptr_t>(rec) & 15))
+        return fail(MTB_INVALID_ARG, "adjoint: bad forward record");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if ((rc = p->dft.upload_phases(t0, k, st))) return rc;
+    if (p->dft.n_regions > 0) {
+        if ((rc = p->dft.expand(0, k, st))) return rc;
+        ++p->last_launches;
+    } else {
+        MTB_CUDA_TRY(cudaMemsetAsync(p->dft.ring_d.p, 0,
+                                     sizeof(float) * (size_t)p->dft.slot_elems * k, st));
+    }
+    const mtb_yee2d_struct &S = p->s;
+    const dim3 blk(32, AROWS);
+    const dim3 grid((S.pitch / 4 + 31) / 32, (S.nx + AROWS - 1) / AROWS);
+    for (int q = k - 1; q >= 0; --q) {
+        const float *radj = p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems;
+        const float *rq = rec + (size_t)q * rec_slot_elems + rec_offset;
+        k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq);
+        MTB_CHECK_LAUNCH();
+        k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
+        MTB_CHECK_LAUNCH();
+        k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
+        MTB_CHECK_LAUNCH();
+        p->last_launches += 3;
+    }
+    return MTB_OK;
+}
+
+int64_t mtb_yee2d_adjoint_last_launches(const mtb_yee2d_adjoint *p) {
+    return p ? p->last_launches : -1;
+}
+
+void mtb_yee2d_adjoint_destroy(mtb_yee2d_adjoint *p) {
+    if (!p) return;
+    p->dft.release();
+    delete p;
+}
+
+}  // extern "C"

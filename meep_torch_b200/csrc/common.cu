@@ -216,6 +216,54 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
     }
 }
 
+// Transpose of k_dft_contract (the adjoint of DFT sampling): for ring slot
+// s of the n staged steps, every channel of a region receives
+//   sum_f Re P(s, f) acc_re[f, ch] + Im P(s, f) acc_im[f, ch]
+// (acc = d J / d accumulator), split 1/2 : 1/2 onto ring_a / ring_b where
+// the forward averaged two samples. Regions may share ring elements, so the
+// ring (zeroed by the caller) is accumulated atomically.
+__global__ void __launch_bounds__(CT) k_dft_expand(
+    const mtb_dft_region *__restrict__ regions, const int *__restrict__ blk_region,
+    const int64_t *__restrict__ blk_start, const int *__restrict__ group_nf,
+    const int *__restrict__ group_off, int total_nf, const float *__restrict__ phase, int row0,
+    int n, float *__restrict__ ring, int64_t slot_elems) {
+    extern __shared__ float2 sP[];
+    const int64_t b = blockIdx.x;
+    const int rg = blk_region[b];
+    const mtb_dft_region R = regions[rg];
+    const int nf = group_nf[R.group];
+    const int foff = group_off[R.group];
+    const int sel = (R.toff == 2) ? 2 : 0;
+    for (int e = threadIdx.x; e < n * nf; e += CT) {
+        const int s = e / nf, f = e - s * nf;
+        const float *p = phase + ((int64_t)(row0 + s) * total_nf + foff + f) * 4 + sel;
+        sP[e] = make_float2(p[0], p[1]);
+    }
+    __syncthreads();
+    const int64_t ch = (b - blk_start[rg]) * CT + threadIdx.x;
+    const int64_t nch = (int64_t)R.rows * R.cols;
+    if (ch >= nch) return;
+    const int r = (int)(ch / R.cols), c = (int)(ch - (int64_t)r * R.cols);
+    float *xa = ring + R.ring_a + (int64_t)r * R.ring_pitch + c;
+    float *xb = (R.ring_b >= 0) ? ring + R.ring_b + (int64_t)r * R.ring_pitch + c : nullptr;
+    const float *acc = R.acc;
+    const int64_t base = (int64_t)r * R.acc_pitch + c;
+    for (int s = 0; s < n; ++s) {
+        float g = 0.f;
+        for (int f = 0; f < nf; ++f) {
+            const float2 p = sP[s * nf + f];
+            g = fmaf(p.x, __ldg(acc + R.re_off + f * R.f_stride + base), g);
+            g = fmaf(p.y, __ldg(acc + R.im_off + f * R.f_stride + base), g);
+        }
+        if (xb) {
+            atomicAdd(xa + s * slot_elems, 0.5f * g);
+            atomicAdd(xb + s * slot_elems, 0.5f * g);
+        } else {
+            atomicAdd(xa + s * slot_elems, g);
+        }
+    }
+}
+
 int DftState::init(const mtb_dft_region *regions, int nreg, const mtb_phase_group *groups,
                    int ngrp, int64_t selems, int nslots) {
     n_regions = nreg;
@@ -359,6 +407,28 @@ int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm,
     return MTB_OK;
 }
 
+int DftState::expand(int row0, int n, cudaStream_t st) {
+    if (n <= 0) return MTB_OK;
+    MTB_CUDA_TRY(cudaMemsetAsync(ring_d.p, 0, sizeof(float) * (size_t)slot_elems * n, st));
+    if (n_regions == 0 || n_blocks == 0) return MTB_OK;
+    int maxnf = 1;
+    for (int g = 0; g < n_groups; ++g) maxnf = std::max(maxnf, group_nf[g]);
+    const size_t smem = sizeof(float2) * (size_t)n * maxnf;
+    static bool attr_set = false;
+    if (!attr_set) {
+        MTB_CUDA_TRY(cudaFuncSetAttribute(k_dft_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          sizeof(float2) * KMAX * 256));
+        attr_set = true;
+    }
+    const int *gd = reinterpret_cast<const int *>(blk_start_d.as<int64_t>() + (n_regions + 1));
+    k_dft_expand<<<(unsigned)n_blocks, CT, smem, st>>>(
+        regions_d.as<mtb_dft_region>(), blk_region_d.as<int>(), blk_start_d.as<int64_t>(), gd,
+        gd + (n_groups + 1), total_nf, phase_d.as<float>(), row0, n, ring_d.as<float>(),
+        slot_elems);
+    MTB_CHECK_LAUNCH();
+    return MTB_OK;
+}
+
 void DftState::release() {
     regions_d.release();
     blk_start_d.release();
@@ -399,6 +469,7 @@ int64_t mtb_struct_size(int32_t which) {
         case 4: return sizeof(mtb_dft_region);
         case 5: return sizeof(mtb_tuning);
         case 6: return sizeof(mtb_yee3d_struct);
+        case 7: return sizeof(mtb_adj2d_buffers);
         default: return -1;
     }
 }

@@ -129,6 +129,9 @@ struct DftState {
     // accumulators.
     int contract(int row0, int n, cudaStream_t st, LaunchTimer *tm = nullptr,
                  const float *phase_base = nullptr);
+    // Transposed contraction: zero ring slots [0, n) and fill them with the
+    // adjoint of the samples of the n staged steps (region acc = d J / d acc).
+    int expand(int row0, int n, cudaStream_t st);
     void release();
 };
 

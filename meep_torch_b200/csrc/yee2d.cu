@@ -1644,6 +1644,14 @@ int32_t mtb_yee2d_current(const mtb_yee2d_plan *p) { return p ? p->par : -1; }
 
 int64_t mtb_yee2d_last_launches(const mtb_yee2d_plan *p) { return p ? p->last_launches : -1; }
 
+int mtb_yee2d_ring(const mtb_yee2d_plan *p, float **ring, int64_t *slot_elems, int32_t *slots) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (ring) *ring = const_cast<float *>(p->dft.ring_d.as<float>());
+    if (slot_elems) *slot_elems = p->dft.slot_elems;
+    if (slots) *slots = p->dft.slots;
+    return MTB_OK;
+}
+
 void mtb_yee2d_plan_destroy(mtb_yee2d_plan *p) {
     if (!p) return;
     for (int q = 0; q < 2; ++q)

@@ -511,6 +511,21 @@ class Engine2D:
                 L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
                                           self._sptr()), "reset")
 
+    def _live_buffers(self, b: int):
+        """The buffers of structure b the next step reads: fields, then CPML memory."""
+        it, cur = self.items[b], self.current
+        return [it.box["main"][cur], it.box["x"][cur], it.box["y"][cur]] + \
+            [p[cur] for p in it.box["psi"]]
+
+    def snapshot(self, b: int = 0):
+        """Copy of structure b's live state (box layout) for restore()."""
+        return [t.clone() for t in self._live_buffers(b)]
+
+    def restore(self, b: int, snap):
+        """Make a snapshot() structure b's live state again (t_idx is the caller's)."""
+        for dst, src in zip(self._live_buffers(b), snap):
+            dst.copy_(src)
+
     def set_timing(self, on: bool = True):
         L.check(self.lib.mtb_yee2d_set_timing(self.plan, 1 if on else 0), "set_timing")
 

@@ -10,6 +10,8 @@ cases of the hot path through its own public functions:
 * ``build_3d_coeffs`` / ``PointSource3D`` / ``FluxMonitor3D`` / ``run_3d``
   (core/monitors_3d.py:192) and ``build_lean`` / ``run_3d_lean``
 * ``cpml_profiles``                              (core/pml.py:17)
+* d J / d eps through the reference's autograd of ``run_tm`` with
+  ``checkpoint_every`` (``python make_golden.py grad`` writes only these)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -185,7 +187,49 @@ def pml_case():
     return out
 
 
+def grad_loss(st, ax, ay, ad, mx, my, dx):
+    """The scalar loss of the gradient fixtures: both flux lines (frequency
+    weights), the energy of the full-grid DFT and of the final fields."""
+    w = torch.tensor([1.0, -0.5, 0.25], dtype=ax.dtype)
+    return ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
+            + 1e-3 * (ad * ad).sum() + 0.1 * (st.Ez * st.Ez).sum()
+            + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
+
+
+def grad_tm_case(prec):
+    """d J / d eps through the reference's autograd (run_tm with
+    checkpoint_every, core/run.py:81-120) on the TM case's geometry."""
+    rng = np.random.default_rng(11)
+    nx, ny, dx, npml = 48, 36, 0.05, 8
+    eps = np.ones((nx, ny))
+    eps[:, 15:21] = 12.0
+    eps[20:30, 8:14] = rng.uniform(2.0, 6.0)
+    eps[30:38, 20:30] = 1.0 + 4.0 * rng.random((8, 10))       # a pixelated design patch
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
+    e = torch.tensor(eps, dtype=DT[prec], requires_grad=True)
+    m = build_tm_coeffs(g, eps_inf=e, npml=npml)
+    src = LineSource(g, ix=12, j0=10, j1=26, profile=GaussianPulse(0.65, 0.4))
+    freqs = [0.55, 0.65, 0.75]
+    monx = FluxMonitorTM(g, freqs, x_normal=True, idx=36, lo=9, hi=27)
+    mony = FluxMonitorTM(g, freqs, x_normal=False, idx=26, lo=10, hi=38)
+    dft = DFTFieldsMonitor(g, freqs, component="Ez")
+    n, ce = 200, 50
+    st, (ax, ay, ad) = run_tm(init_tm_state(g), m, n, source=src, monitors=[monx, mony, dft],
+                              checkpoint_every=ce)
+    J = grad_loss(st, ax, ay, ad, monx, mony, dx)
+    J.backward()
+    return dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, checkpoint_every=ce, eps=eps,
+                freqs=np.array(freqs), fcen=0.65, fwidth=0.4, src_ix=12, src_j0=10, src_j1=26,
+                monx=np.array([36, 9, 27]), mony=np.array([26, 10, 38]),
+                J=float(J.detach()), grad=_np(e.grad))
+
+
 def main():
+    if sys.argv[1:] == ["grad"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_grad_tm_{prec}.npz"),
+                                **grad_tm_case(prec))
+        return
     torch.set_num_threads(4)
     np.savez_compressed(os.path.join(HERE, "golden_pml.npz"), **pml_case())
     for prec in ("f64", "f32"):

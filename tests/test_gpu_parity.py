@@ -444,3 +444,52 @@ def test_graph_replay_bitwise_equal_to_direct_launches(variant):
                 assert torch.equal(x, y), (b, name)
         for x, y in zip(a0[b], a1[b]):
             assert torch.equal(x, y), b
+
+
+def _grad_setup(g, dev_, requires_grad=True):
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor, FluxMonitorTM
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    nx, ny, dx, npml = int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"])
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=dev_)
+    e = torch.tensor(g["eps"], dtype=torch.float32, device=dev_, requires_grad=requires_grad)
+    m = build_tm_coeffs(grid, eps_inf=e, npml=npml)
+    src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
+                     profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
+    freqs = [float(f) for f in g["freqs"]]
+    mx, my = (int(v) for v in g["monx"]), (int(v) for v in g["mony"])
+    mx, my = list(mx), list(my)
+    monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=mx[0], lo=mx[1], hi=mx[2])
+    mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=my[0], lo=my[1], hi=my[2])
+    dft = DFTFieldsMonitor(grid, freqs, "Ez")
+    return e, m, src, [monx, mony, dft], init_tm_state(grid), dx
+
+
+def _grad_loss(st, ax, ay, ad, mx, my, dx):
+    """The fixtures' loss (tests/golden/make_golden.py grad_loss)."""
+    w = torch.tensor([1.0, -0.5, 0.25], dtype=ax.dtype, device=ax.device)
+    return ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
+            + 1e-3 * (ad * ad).sum() + 0.1 * (st.Ez * st.Ez).sum()
+            + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
+
+
+@pytest.mark.parametrize("chunk", [50, 32, 7])
+def test_tm_gradient_matches_reference_autograd(chunk):
+    """d J / d eps from the library's discrete-adjoint kernels against the
+    reference's own autograd through run_tm(checkpoint_every=50) (fixtures
+    made by tests/golden/make_golden.py grad), for several checkpoint lengths."""
+    from meep_torch_b200.core.run import run_tm
+    g32, g64 = load_golden("grad_tm_f32"), load_golden("grad_tm_f64")
+    e, m, src, mons, s0, dx = _grad_setup(g32, dev())
+    st, (ax, ay, ad) = run_tm(s0, m, int(g32["n_steps"]), source=src, monitors=mons,
+                              checkpoint_every=chunk)
+    J = _grad_loss(st, ax, ay, ad, mons[0], mons[1], dx)
+    J.backward()
+    got = e.grad.cpu().numpy()
+    e32, e64 = rel_l2(got, g32["grad"]), rel_l2(got, g64["grad"])
+    print(f"grad chunk {chunk}: rel L2 vs reference f32 {e32:.3e}, vs f64 {e64:.3e}; "
+          f"J {float(J):.6e} vs {float(g32['J']):.6e}")
+    assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
+    assert e32 < 1e-4, e32

@@ -143,3 +143,43 @@ def test_3d_lean_sign_convention(prec):
         assert rel_l2(s[k], g["s_" + k]) < tol, k
     for n, a in enumerate(acc):
         assert rel_l2(a, g[f"acc_{n}"]) < tol
+
+
+def test_reference_gradient_matches_oracle_finite_differences():
+    """The golden d J / d eps (reference autograd, float64) against central
+    finite differences of the oracle's float64 run at a few pixels."""
+    g = load_golden("grad_tm_f64")
+    nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
+                           int(g["n_steps"]))
+    freqs = [float(f) for f in g["freqs"]]
+    mxi, mxl, mxh = (int(v) for v in g["monx"])
+    myi, myl, myh = (int(v) for v in g["mony"])
+
+    def J_of(eps):
+        c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float64)
+        dt = c["dt"]
+        mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
+                                  int(g["src_j1"]), dtype=np.float64)
+        prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
+        mons = [lambda s, t: O.flux_tm_sample(s, t, dt, freqs, True, mxi, mxl, mxh, np.float64),
+                lambda s, t: O.flux_tm_sample(s, t, dt, freqs, False, myi, myl, myh, np.float64),
+                lambda s, t: O.dft_sample(s["Ez"], t, dt, freqs, "Ez", np.float64)]
+        s, (ax, ay, ad) = O.run_2d(O.tm_step, O.tm_state(c), c, n,
+                                   amp_fn=lambda t: prof(O.src_time(t, dt)), mask=mask,
+                                   monitors=mons)
+        w = np.array([1.0, -0.5, 0.25])
+        fx, fy = O.line_flux(ax, dx, -1.0), O.line_flux(ay, dx, +1.0)
+        return float((w * fx).sum() + (w[::-1] * fy).sum() + 1e-3 * (ad * ad).sum()
+                     + 0.1 * (s["Ez"] ** 2).sum() + 0.05 * (s["Hy"] ** 2).sum()
+                     - 0.02 * (s["Hx"] ** 2).sum())
+
+    eps = g["eps"].astype(np.float64)
+    assert abs(J_of(eps) - float(g["J"])) <= 1e-9 * abs(float(g["J"]))
+    h = 1e-4
+    for (i, j) in [(33, 24), (24, 17), (36, 12)]:
+        ep, em = eps.copy(), eps.copy()
+        ep[i, j] += h
+        em[i, j] -= h
+        fd = (J_of(ep) - J_of(em)) / (2 * h)
+        ref = float(g["grad"][i, j])
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-16, (i, j, fd, ref)
