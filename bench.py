@@ -180,6 +180,74 @@ def cpu_sample_cfg1(steps):
 
 # ------------------------------------------------------------------ GPU bench
 
+def run_cfg4(args, rank, world, dev):
+    """cfg4: gradient evaluations (design chain + 8000-step TM run + adjoint sweep)."""
+    import torch
+
+    from meep_torch_b200 import _lib
+    from meep_torch_b200 import workloads as W
+
+    lib = _lib.load()
+    steps = args.run_steps if args.run_steps != 5000 else W.CFG4["steps"]
+    opt, n = W.cfg4_setup(dev, seed=4 + 1009 * rank, steps=steps)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        opt()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    n0 = lib.mtb_launch_count()
+    with Clocks(dev.index if dev.index is not None else 0) as clk:
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            opt()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+    launches = lib.mtb_launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    c = W.CFG4
+    res = dict(cells=c["nx"] * c["ny"], nsteps=n, ms=allreduce_max(ms, world, dev),
+               launches=launches, clocks=clk.summary(), grad_evals=args.steps * world)
+    if args.no_e2e:
+        res.update(e2e_s=float("nan"), h2d=0, d2h=0)
+        return res
+    host_rho = opt.rho.detach().cpu().pin_memory()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        opt.rho = host_rho.to(dev, non_blocking=True)
+        _, grad = opt()                              # dJ/drho comes back as numpy
+    torch.cuda.synchronize(dev)
+    res.update(e2e_s=allreduce_max(time.perf_counter() - t0, world, dev),
+               h2d=host_rho.numel() * 4, d2h=grad.size * 4)
+    return res
+
+
+def cpu_sample_cfg4(steps):
+    """Oracle forward of `steps` steps on the cfg4 grid (one thread)."""
+    import numpy as np
+
+    from meep_torch_b200 import workloads as W
+    from oracle import fdtd as O
+    c = W.CFG4
+    nx, ny, dx = c["nx"], c["ny"], c["dx"]
+    eps = np.full((nx, ny), c["eps_bg"], dtype=np.float32)
+    eps[:, ny // 2 - 10: ny // 2 + 10] = c["eps_core"]
+    oc = O.tm_coeffs(nx, ny, dx, eps=eps, npml=c["npml"], dtype=np.float32)
+    dt = oc["dt"]
+    mask = O.line_source_mask(nx, ny, dx, c["npml"] + 10, ny // 2 - 20, ny // 2 + 20,
+                              dtype=np.float32)
+    prof = O.gaussian_pulse(0.645, 0.12)
+    t0 = time.perf_counter()
+    O.run_2d(O.tm_step, O.tm_state(oc), oc, steps, amp_fn=lambda t: prof(O.src_time(t, dt)),
+             mask=mask)
+    return time.perf_counter() - t0
+
+
 def run_cfg1(args, rank, world, dev):
     """cfg1: one 320 x 160 TM structure per rank, 4000 steps per run. The working
     set is L2-resident and the step is launch/latency-bound: whole ring flushes
@@ -439,7 +507,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--rows", type=int, default=0, help="rows per warp (0 = library default)")
     ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
     ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
@@ -460,7 +528,16 @@ def main():
     threads = os.cpu_count() or 1
     if args.cpu_structs <= 0:
         args.cpu_structs = min(max(8, threads), 64)
-    if args.workload == "cfg1":
+    if args.workload == "cfg4":
+        config = {"workload": "cfg4: gradient of a 600 x 400 TM mode-converter-shaped problem "
+                              "(res 25, 25-cell CPML, 160 x 160 design, conic filter + tanh "
+                              "projection, line source across the input guide standing in for "
+                              "the mode source, output-port flux at 3 wavelengths), 8000 steps "
+                              "forward + adjoint sweep per gradient",
+                  "time_steps": args.run_steps if args.run_steps != 5000 else 8000,
+                  "checkpoint_every": 32, "seed": "4 + 1009*rank",
+                  "l2": "L2-resident working set (~10 MB of state): latency-bound"}
+    elif args.workload == "cfg1":
         config = {"workload": "cfg1: 2D TM waveguide 320 x 160 (16 x 8 um at res 20), 1 um "
                               "CPML, eps 12 guide, Gaussian Ez source (0.15, 0.1), one "
                               "50-frequency flux line, 4000 steps per run",
@@ -530,6 +607,41 @@ def main():
         B.build()
     barrier(world)
 
+    if args.workload == "cfg4":
+        r = run_cfg4(args, rank, world, dev)
+        value = r["grad_evals"] / (r["ms"] / 1e3)
+        line = {"metric": "gradient-evaluations/s", "value": value,
+                "unit": "gradient-evaluations/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": dict(config, parallelism=f"independent problem per rank x{world}"),
+                "roofline": {"bound": "latency (L2-resident)", "achieved": None,
+                             "peak": peaks()[0], "unit": "GB/s", "frac": None, "traffic": None,
+                             "note": "600 x 400 fits in L2; each step is a few microsecond "
+                                     "launches, so the HBM roofline does not apply"},
+                "e2e": {"value": (args.steps * world / r["e2e_s"]
+                                  if r["e2e_s"] == r["e2e_s"] else None),
+                        "unit": "gradient-evaluations/s", "h2d_bytes_per_step": r["h2d"],
+                        "d2h_bytes_per_step": r["d2h"]},
+                "clocks": r["clocks"], "gpu_launches": r["launches"]}
+        if rank == 0 and not args.no_cpu:
+            sec = cpu_sample_cfg4(300)
+            per_grad = sec / 300 * 2 * r["nsteps"]
+            line["cpu_baseline"] = {"value": 1.0 / per_grad, "unit": "gradient-evaluations/s",
+                                    "cores": 1, "kind": "port",
+                                    "sample": f"oracle (numpy float32) forward, 300 steps of the "
+                                              f"cfg4 grid in {sec:.1f} s, one thread; a gradient "
+                                              f"costed as 2 x {r['nsteps']} steps (the reverse "
+                                              "sweep at the forward's cost); the oracle has no "
+                                              "reverse mode"}
+        if rank == 0:
+            print(json.dumps(line))
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     r = {"cfg1": run_cfg1, "cfg2": run_cfg2, "cfg3": run_cfg3}[args.workload](args, rank, world,
                                                                             dev)
     peak, peak_kind = peaks()

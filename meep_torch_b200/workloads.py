@@ -167,3 +167,55 @@ def cfg3_bytes_per_step(n: int = 256, npml: int = 16) -> float:
     3 axes x 4 psi x 8 B x (2 npml / n))."""
     cells = n ** 3
     return cells * (48 + 4) + 3 * 4 * 8 * cells * (2 * npml / n)
+
+
+# ------------------------------------------------------------------ cfg4
+
+CFG4 = dict(nx=600, ny=400, dx=0.04, npml=25, eps_bg=2.1, eps_core=12.0, guide_w=20,
+            design=160, steps=8000, radius=0.15, beta=8.0, eta=0.5,
+            freqs=(1 / 1.60, 1 / 1.55, 1 / 1.50))
+
+
+def cfg4_setup(device, seed: int = 4, steps: int = None):
+    """cfg4-shaped gradient problem: 600 x 400 TM grid at res 25, 25-cell CPML,
+    eps 2.1 background with an eps 12, 0.8 um wide input and output guide along x
+    meeting a centred 160 x 160 design region (rho0 ~ U(0.4, 0.6), default_rng(4)),
+    conic filter 0.15 um, tanh projection beta 8 / eta 0.5. A Gaussian line source
+    across the input guide (fcen 0.645, fwidth 0.12: the 1.50-1.60 um band) stands in
+    for the reference's mode source, and the objective is the mean transmitted flux
+    through the output guide at the three wavelengths. Returns the
+    OptimizationProblem (design.py) and the step count."""
+    from .core.coeffs import build_tm_coeffs
+    from .core.grid import Grid
+    from .core.monitors import FluxMonitorTM
+    from .core.run import run_tm
+    from .core.sources import GaussianPulse, LineSource
+    from .core.stepper_tm import init_tm_state
+    from .design import DesignRegion, MaterialGrid, OptimizationProblem
+    c = CFG4
+    nx, ny, dx, npml = c["nx"], c["ny"], c["dx"], c["npml"]
+    n = steps or c["steps"]
+    rng = np.random.default_rng(seed)
+    base = torch.full((nx, ny), c["eps_bg"], dtype=torch.float32)
+    y0, y1 = ny // 2 - c["guide_w"] // 2, ny // 2 + c["guide_w"] // 2
+    base[:, y0:y1] = c["eps_core"]
+    d = c["design"]
+    ix0, iy0 = nx // 2 - d // 2, ny // 2 - d // 2
+    reg = DesignRegion(MaterialGrid((d, d), c["eps_bg"], c["eps_core"]), ix0=ix0, ix1=ix0 + d,
+                       iy0=iy0, iy1=iy0 + d)
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=device)
+    src = LineSource(grid, ix=npml + 10, j0=y0 - 10, j1=y1 + 10,
+                     profile=GaussianPulse(0.645, 0.12))
+    mon = FluxMonitorTM(grid, list(c["freqs"]), x_normal=True, idx=nx - npml - 10,
+                        lo=y0 - 20, hi=y1 + 20)
+
+    def run_fn(eps):
+        m = build_tm_coeffs(grid, eps_inf=eps, npml=npml)
+        _, (acc,) = run_tm(init_tm_state(grid), m, n, source=src, monitors=[mon],
+                           checkpoint_every=32)
+        return mon.flux(acc, dx).mean()
+
+    rho0 = torch.tensor(rng.uniform(0.4, 0.6, (d, d)), dtype=torch.float32, device=device)
+    opt = OptimizationProblem(run_fn, base.to(device), reg, filter_radius=c["radius"], dx=dx,
+                              beta=c["beta"], eta=c["eta"], rho0=rho0)
+    return opt, n

@@ -12,6 +12,8 @@ cases of the hot path through its own public functions:
 * ``cpml_profiles``                              (core/pml.py:17)
 * d J / d eps through the reference's autograd of ``run_tm`` with
   ``checkpoint_every`` (``python make_golden.py grad`` writes only these)
+* the design chain (``conic_filter``, ``tanh_projection``, ``MaterialGrid``,
+  ``DesignRegion``, ``OptimizationProblem``; ``python make_golden.py design``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -224,7 +226,47 @@ def grad_tm_case(prec):
                 J=float(J.detach()), grad=_np(e.grad))
 
 
+def design_case():
+    """The design chain (adjoint/filters.py, adjoint/problem.py): conic filter,
+    tanh projection, MaterialGrid / DesignRegion paint, and the gradient of an
+    OptimizationProblem whose run function is the TM run of grad_tm_case."""
+    from meep_torch.adjoint.filters import conic_filter, tanh_projection
+    from meep_torch.adjoint.problem import DesignRegion, MaterialGrid, OptimizationProblem
+    rng = np.random.default_rng(4)
+    rho = rng.uniform(0.0, 1.0, (20, 16))
+    r = torch.tensor(rho, dtype=torch.float64)
+    filt = conic_filter(r, 0.15, 0.04)
+    proj = tanh_projection(filt, 8.0, 0.5)
+    mg = MaterialGrid((20, 16), 2.1, 12.0)
+    base = torch.full((48, 36), 2.1, dtype=torch.float64)
+    base[:, 15:21] = 12.0
+    reg = DesignRegion(mg, ix0=22, ix1=32, iy0=10, iy1=26)
+    painted = reg.paint(base, proj)
+    # problem: TM run on the fixture grid, objective = transmitted flux
+    nx, ny, dx, npml = 48, 36, 0.05, 8
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=torch.float64, device="cpu")
+    src = LineSource(g, ix=12, j0=12, j1=24, profile=GaussianPulse(0.65, 0.4))
+    freqs = [0.6, 0.7]
+    mon = FluxMonitorTM(g, freqs, x_normal=True, idx=38, lo=9, hi=27)
+
+    def run_fn(eps):
+        m = build_tm_coeffs(g, eps_inf=eps, npml=npml)
+        st, (acc,) = run_tm(init_tm_state(g), m, 200, source=src, monitors=[mon],
+                            checkpoint_every=50)
+        return mon.flux(acc, dx).mean() * 1e9
+
+    rho0 = torch.tensor(rng.uniform(0.3, 0.7, (20, 16)), dtype=torch.float64)
+    opt = OptimizationProblem(run_fn, base, reg, filter_radius=0.1, dx=dx, beta=4.0, eta=0.5,
+                              rho0=rho0)
+    f0, grad = opt()
+    return dict(rho=rho, filt=_np(filt), proj=_np(proj), base=_np(base), painted=_np(painted),
+                box=np.array(reg.box), rho0=_np(rho0), f0=f0, grad=grad)
+
+
 def main():
+    if sys.argv[1:] == ["design"]:
+        np.savez_compressed(os.path.join(HERE, "golden_design.npz"), **design_case())
+        return
     if sys.argv[1:] == ["grad"]:
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_grad_tm_{prec}.npz"),
