@@ -656,7 +656,7 @@ def main():
     if os.path.exists(prof) and args.workload in ("cfg2", "cfg3"):
         with open(prof) as f:
             tr = json.load(f)
-        eff = args.variant or (2 if cfg3 else 1)          # library defaults
+        eff = args.variant or 2                           # library default: tiles / split
         if tr.get("variant") == eff:
             traffic = tr.get("dram_bytes_per_launch")
     e2e_val = (r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
@@ -667,8 +667,8 @@ def main():
               if args.workload == "cfg1" else
               "k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else
               "k_yee3d_step (one step)" if cfg3 else
-              "k_tile_tm + k_tile_te (one step)" if args.variant == 2 else
-              "k_yee2d_tm + k_yee2d_te (one step)")
+              "k_yee2d_tm + k_yee2d_te (one step)" if args.variant == 1 else
+              "k_tile_tm + k_tile_te (one step)")
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -174,17 +174,18 @@ typedef struct mtb_dft_region {
 
 /* Tuning knobs (0 = library default). */
 typedef struct mtb_tuning {
-    int32_t rows_per_warp;  /* 2D row march: rows one warp marches through;
-                               3D fused: x planes one block covers; 3D split:
-                               x planes per H / E launch pair (0 = all)     */
+    int32_t rows_per_warp;  /* 2D tiles: rows per warp (>= 4: four, register-
+                               blocked; 1-3: one; 0: four when the batch fills
+                               the GPU, else one); 2D row march: rows one warp
+                               marches through; 3D fused: x planes one block
+                               covers; 3D split: x planes per H / E launch pair
+                               (0 = all)                                     */
     int32_t ring_slots;     /* steps buffered before one DFT contraction    */
     int32_t graph;          /* 2D: replay whole ring flushes (ring_slots steps
                                + one contraction) as a CUDA graph: 0 default
                                (on for runs of >= 2 flushes while per-launch
                                timing is off), -1 off                       */
-    int32_t variant;        /* 2D: 0 default (row march for batches that fill
-                               the GPU, tiles for small ones), 1 row march,
-                               2 tiles;
+    int32_t variant;        /* 2D: 0 default (tiles), 1 row march, 2 tiles;
                                3D: 0 default (split), 1 fused x-march,
                                2 split H / E streaming kernels              */
 } mtb_tuning;

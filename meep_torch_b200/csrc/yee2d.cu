@@ -43,6 +43,7 @@ struct Ctx2D {
     int *err;                     // device error flag (1 = a bounded wait expired)
     int par;                      // buffer holding the old state
     int first;                    // first step executed by the plan
+    int wr;                       // tile kernels: rows per warp (1 or WROWS)
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -798,10 +799,12 @@ __global__ void __launch_bounds__(32 * WARPS2D, 4) k_yee2d_te(
 // recursion runs with the profile's (b, a), which are (1, 0) on inert nodes,
 // so lanes of one warp run the same arithmetic whether or not they are in a
 // layer, and the edge rules are selects.
-constexpr int TROWS = 8;
-// row-march warps below which the library default is the tile kernels
-// (148 SMs x 8 warps)
-constexpr int64_t ROW_MARCH_MIN_WARPS = 148 * 8;
+constexpr int TROWS = 8;            // warps per tile block
+constexpr int WROWS = 4;            // rows per warp
+constexpr int TILE_ROWS = TROWS * WROWS;
+// tile blocks (of WROWS rows per warp) below which the tiles use one row per
+// warp: 148 SMs x 2 resident blocks x 4 waves
+constexpr int64_t TILE_MIN_BLOCKS = 148 * 2 * 4;
 
 struct TileSmem {
     mtb_yee2d_struct s;
@@ -811,7 +814,7 @@ struct TileSmem {
 
 // Block setup: work item, structure copy, line samples touching the tile.
 __device__ __forceinline__ bool tile_setup(const mtb_yee2d_struct *__restrict__ SS,
-                                           const int4 *__restrict__ work, int n_work,
+                                           const int4 *__restrict__ work, int n_work, int wr,
                                            TileSmem &T, int4 &w) {
     if ((int)blockIdx.x >= n_work) return false;
     w = __ldg(work + blockIdx.x);
@@ -824,7 +827,7 @@ __device__ __forceinline__ bool tile_setup(const mtb_yee2d_struct *__restrict__ 
     }
     __syncthreads();
     if (threadIdx.y == 0) {
-        const int i0 = w.y, i1 = min(w.y + TROWS, T.s.nx), c0 = w.z;
+        const int i0 = w.y, i1 = min(w.y + TROWS * wr, T.s.nx), c0 = w.z;
         const int n_all = T.s.n_lines;
         bool keep = false;
         mtb_line_sample ln{};
@@ -1187,19 +1190,395 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     }
 }
 
+// Lean TM rows: rows ib .. ib+R-1 of one warp, all in [1, nx-2] and outside
+// the x layers (no x-direction CPML memory), columns jb .. jb+3 of one lane.
+// The R rows share their neighbour rows' loads (R+2 rows of Dz and 1/eps,
+// R+1 of Hy): per cell a fraction of tm_tile's loads and index work. YPSI adds
+// the y-direction CPML of lanes inside a y layer. Same arithmetic as tm_tile
+// (the x-CPML terms there are b psi + a d = 0 here), so either path may
+// recompute a neighbour's halo row.
+template <int R, bool YPSI>
+__device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib, const int c0,
+                                        const Ctx2D &C, const mtb_line_sample *L, const int nl) {
+    const int lane = threadIdx.x;
+    const int ny = S.ny, P = S.pitch;
+    const int jb = c0 + 4 * lane;
+    const bool act = jb < P;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int par = C.par;
+    const float *__restrict__ Dz = S.f_main[par];
+    const float *__restrict__ Hx = S.f_x[par];
+    const float *__restrict__ Hy = S.f_y[par];
+    const float *__restrict__ ie = S.inv_eps_a;
+    const uint32_t o0 = (uint32_t)ib * P + jb;          // own row 0
+    const uint32_t om = o0 - P;                         // row ib-1 (ib >= 1)
+    const int jl = jb - 1;
+    const bool hasL = lane == 0 && jl >= 0 && jl <= ny - 2;
+    const bool byH = YPSI && act && band4(jb, S.yband[0], S.yband[1]);
+    const bool byE = YPSI && act && band4(jb, S.yband[2], S.yband[3]);
+    const bool byHL = YPSI && hasL && in_band(jl, S.yband[0], S.yband[1]);
+    const bool rok = lane == 31 && jb + 4 < P;
+
+    float dv[R + 2][4], iv[R + 2][4];                  // Dz, 1/eps rows ib-1 .. ib+R
+    float hx[R][4], hy[R + 1][4];                      // Hx own rows; Hy rows ib-1 .. ib+R-1
+    float ezl[R], ezr[R], hxl[R], p0l[R];
+    float p0[R][4], p3[R][4];
+#pragma unroll
+    for (int k = 0; k < R + 2; ++k) { zero4(dv[k]); zero4(iv[k]); }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        zero4(hx[r]); zero4(p0[r]); zero4(p3[r]);
+        ezl[r] = ezr[r] = hxl[r] = p0l[r] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < R + 1; ++k) zero4(hy[k]);
+    if (act) {
+#pragma unroll
+        for (int k = 0; k < R + 2; ++k) {
+            ld4(Dz + om + k * P, dv[k]);
+            ld4(ie + om + k * P, iv[k]);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) ld4(Hx + o0 + r * P, hx[r]);
+#pragma unroll
+        for (int k = 0; k < R + 1; ++k) ld4(Hy + om + k * P, hy[k]);
+        if (lane == 0 && jl >= 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                ezl[r] = Dz[o0 + r * P - 1] * ie[o0 + r * P - 1];
+                if (hasL) hxl[r] = Hx[o0 + r * P - 1];
+                if (byHL) p0l[r] = S.psi[0][par][o0 + r * P - 1];
+            }
+        }
+        if (rok) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) ezr[r] = Dz[o0 + r * P + 4] * ie[o0 + r * P + 4];
+        }
+        if (YPSI) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (byH) ld4(S.psi[0][par] + o0 + r * P, p0[r]);
+                if (byE) ld4(S.psi[3][par] + o0 + r * P, p3[r]);
+            }
+        }
+    }
+    const bool pmc = S.y_pmc != 0;
+    float hyb[4], hya[4], eyb[4], eya[4];
+    bool vH[4], vD[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        vH[q] = act && j <= ny - 2;
+        vD[q] = act && (pmc ? (j < ny) : (j >= 1 && j <= ny - 2));
+        hyb[q] = 1.f; hya[q] = 0.f; eyb[q] = 1.f; eya[q] = 0.f;
+        if (YPSI) {
+            const bool oh = byH && j <= ny - 2, oe = byE && j < ny;
+            if (oh) { hyb[q] = __ldg(S.hy_b + j); hya[q] = __ldg(S.hy_a + j); }
+            if (oe) { eyb[q] = __ldg(S.ey_b + j); eya[q] = __ldg(S.ey_a + j); }
+        }
+    }
+    float ez[R + 2][4];
+#pragma unroll
+    for (int k = 0; k < R + 2; ++k)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ez[k][q] = dv[k][q] * iv[k][q];
+
+    // Hy(n+1/2) rows ib-1 .. ib+R-1 (all <= nx-2, outside the x layers)
+    float hyN[R + 1][4];
+#pragma unroll
+    for (int k = 0; k < R + 1; ++k) {
+        const int row = ib - 1 + k;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float d = (ez[k + 1][q] - ez[k][q]) * rdx;
+            const float pv = 1.f * 0.f + 0.f * d;
+            hyN[k][q] = hy[k][q] + dt * (d + pv);
+        }
+        if (act && row >= S.src_h1.row_lo && row <= S.src_h1.row_hi)
+            apply_cells(S.src_h1, row, C.amp_h, jb, hyN[k]);
+    }
+    float *ring = C.ring;
+    const int pn = par ^ 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = ib + r;
+        const uint32_t ro = o0 + r * P;
+        // Hx(n+1/2) row i
+        float ezR = __shfl_down_sync(0xffffffffu, ez[r + 1][0], 1);
+        if (lane == 31) ezR = ezr[r];
+        float hxN[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float er = (q < 3) ? ez[r + 1][q + 1] : ezR;
+            const float d = (er - ez[r + 1][q]) * rdx;
+            const float pv = hyb[q] * p0[r][q] + hya[q] * d;
+            const float hn = hx[r][q] - dt * (d + pv);
+            hxN[q] = vH[q] ? hn : hx[r][q];
+            p0[r][q] = vH[q] ? pv : p0[r][q];
+        }
+        if (act && i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
+            apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
+        if (!act) zero4(hxN);
+        float hxm0 = __shfl_up_sync(0xffffffffu, hxN[3], 1);
+        if (lane == 0) {
+            float v = 0.f;
+            if (hasL) {
+                const float d = (ez[r + 1][0] - ezl[r]) * rdx;
+                float c = d;
+                if (byHL) c = d + (__ldg(S.hy_b + jl) * p0l[r] + __ldg(S.hy_a + jl) * d);
+                v = hxl[r] - dt * c;
+                if (i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
+                    v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
+            }
+            hxm0 = v;
+        }
+        // Dz(n+1) row i, electric source, Ez = Dz / eps
+        float dzN[4], ezN[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float hxm = (q == 0) ? hxm0 : hxN[q - 1];
+            const float dhy = (hyN[r + 1][q] - hyN[r][q]) * rdx;
+            const float dhx = (hxN[q] - hxm) * rdx;
+            const float q2 = 1.f * 0.f + 0.f * dhy;
+            const float q3 = eyb[q] * p3[r][q] + eya[q] * dhx;
+            const float dn = dv[r + 1][q] + dt * ((dhy + q2) - (dhx + q3));
+            dzN[q] = vD[q] ? dn : dv[r + 1][q];
+            p3[r][q] = vD[q] ? q3 : p3[r][q];
+        }
+        if (act && i >= S.src_e.row_lo && i <= S.src_e.row_hi)
+            apply_cells(S.src_e, i, C.amp_e, jb, dzN);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ezN[q] = dzN[q] * iv[r + 1][q];
+        if (act) {
+            st4(S.f_main[pn] + ro, dzN);
+            st4(S.f_x[pn] + ro, hxN);
+            st4(S.f_y[pn] + ro, hyN[r + 1]);
+            if (YPSI && byH) st4(S.psi[0][pn] + ro, p0[r]);
+            if (YPSI && byE) st4(S.psi[3][pn] + ro, p3[r]);
+            if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, ezN);
+            if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, hxN);
+            if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, hyN[r + 1]);
+            if (nl) {
+                sample_row(L, nl, MTB_C2_MAIN, i, jb, true, ezN, ring);
+                sample_row(L, nl, MTB_C2_X, i, jb, true, hxN, ring);
+                sample_row(L, nl, MTB_C2_Y, i, jb, true, hyN[r + 1], ring);
+            }
+        }
+    }
+}
+
 template <bool FIRST>
 __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
     Ctx2D C) {
     __shared__ TileSmem T;
     int4 w;
-    if (!tile_setup(SS, work, n_work, T, w)) return;
-    const int i = w.y + threadIdx.y;
-    if (i >= T.s.nx) return;                       // whole warp
-    if (FIRST && T.s.explicit_e)
-        tm_tile<true>(T.s, i, w.z, C, T.lines, T.nl);
-    else
-        tm_tile<false>(T.s, i, w.z, C, T.lines, T.nl);
+    if (!tile_setup(SS, work, n_work, C.wr, T, w)) return;
+    const mtb_yee2d_struct &S = T.s;
+    const int ib = w.y + threadIdx.y * C.wr;           // this warp's rows ib .. ib+wr-1
+    if (ib >= S.nx) return;                             // whole warp
+    const bool expl = FIRST && S.explicit_e;
+    // lean rows: interior rows outside the x layers, imported Ez not pending
+    const int last = ib + WROWS - 1;
+    const bool lean = C.wr == WROWS && !expl && ib >= 1 && last <= S.nx - 2 &&
+                      ib - 1 >= S.xband[0] && last < S.xband[1] &&
+                      ib >= S.xband[2] && last < S.xband[3];
+    if (lean) {
+        const int jb = w.z + 4 * threadIdx.x;
+        const bool yb = jb < S.pitch &&
+                        (band4(jb, S.yband[0], S.yband[1]) || band4(jb, S.yband[2], S.yband[3]) ||
+                         (threadIdx.x == 0 && jb >= 1 && in_band(jb - 1, S.yband[0], S.yband[1])));
+        if (!__any_sync(0xffffffffu, yb)) {
+            tm_rows<WROWS, false>(S, ib, w.z, C, T.lines, T.nl);
+        } else {
+#pragma unroll 1
+            for (int h = 0; h < WROWS; h += 2) tm_rows<2, true>(S, ib + h, w.z, C, T.lines, T.nl);
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int r = 0; r < C.wr; ++r) {
+        if (ib + r >= S.nx) break;
+        if (FIRST && expl)
+            tm_tile<true>(S, ib + r, w.z, C, T.lines, T.nl);
+        else
+            tm_tile<false>(S, ib + r, w.z, C, T.lines, T.nl);
+    }
+}
+
+// Lean TE rows: Hz rows ib .. ib+R-1 of one warp with their Dx / Ex rows and
+// the Dy / Ey rows ib .. ib+R (the last one is the halo the Hz update needs),
+// all in [1, nx-2] and outside the x layers; y-direction CPML when YPSI. Same
+// arithmetic as te_tile / te_dy.
+template <int R, bool YPSI>
+__device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib, const int c0,
+                                        const Ctx2D &C, const mtb_line_sample *L, const int nl) {
+    const int lane = threadIdx.x;
+    const int ny = S.ny, P = S.pitch;
+    const int jb = c0 + 4 * lane;
+    const bool act = jb < P;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    const int par = C.par;
+    const float *__restrict__ Hz = S.f_main[par];
+    const float *__restrict__ Dx = S.f_x[par];
+    const float *__restrict__ Dy = S.f_y[par];
+    const float *__restrict__ iex = S.inv_eps_a;
+    const float *__restrict__ iey = S.inv_eps_b;
+    const uint32_t o0 = (uint32_t)ib * P + jb;
+    const uint32_t om = o0 - P;                         // row ib-1 (ib >= 1)
+    const int jr = jb + 4;
+    const bool hasR = lane == 31 && jr <= ny - 1;
+    const bool updR = hasR && jr <= ny - 2;             // jr >= 1 always
+    const bool byE = YPSI && act && band4(jb, S.yband[2], S.yband[3]);
+    const bool byH = YPSI && act && band4(jb, S.yband[0], S.yband[1]);
+    const bool byER = YPSI && updR && in_band(jr, S.yband[2], S.yband[3]);
+
+    float hz[R + 2][4];                                 // Hz rows ib-1 .. ib+R
+    float dx[R][4], ix[R][4];                           // Dx, 1/eps_x own rows
+    float dy[R + 1][4], iy[R + 1][4];                   // Dy, 1/eps_y rows ib .. ib+R
+    float hzL[R], hzR[R], dxr[R], ixr[R], p0r[R];
+    float p0[R][4], p3[R][4];
+#pragma unroll
+    for (int k = 0; k < R + 2; ++k) zero4(hz[k]);
+#pragma unroll
+    for (int k = 0; k < R + 1; ++k) { zero4(dy[k]); zero4(iy[k]); }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        zero4(dx[r]); zero4(ix[r]); zero4(p0[r]); zero4(p3[r]);
+        hzL[r] = hzR[r] = dxr[r] = ixr[r] = p0r[r] = 0.f;
+    }
+    if (act) {
+#pragma unroll
+        for (int k = 0; k < R + 2; ++k) ld4(Hz + om + k * P, hz[k]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            ld4(Dx + o0 + r * P, dx[r]);
+            ld4(iex + o0 + r * P, ix[r]);
+        }
+#pragma unroll
+        for (int k = 0; k < R + 1; ++k) {
+            ld4(Dy + o0 + k * P, dy[k]);
+            ld4(iey + o0 + k * P, iy[k]);
+        }
+        if (lane == 0 && jb >= 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) hzL[r] = Hz[o0 + r * P - 1];
+        }
+        if (hasR) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                hzR[r] = Hz[o0 + r * P + 4];
+                dxr[r] = Dx[o0 + r * P + 4];
+                ixr[r] = iex[o0 + r * P + 4];
+                if (byER) p0r[r] = S.psi[0][par][o0 + r * P + 4];
+            }
+        }
+        if (YPSI) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (byE) ld4(S.psi[0][par] + o0 + r * P, p0[r]);
+                if (byH) ld4(S.psi[3][par] + o0 + r * P, p3[r]);
+            }
+        }
+    }
+    float hyb[4], hya[4], eyb[4], eya[4];
+    bool vX[4], vZ[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        vX[q] = act && j >= 1 && j <= ny - 2;
+        vZ[q] = act && j <= ny - 2;
+        hyb[q] = 1.f; hya[q] = 0.f; eyb[q] = 1.f; eya[q] = 0.f;
+        if (YPSI) {
+            const bool oe = byE && j >= 1 && j <= ny - 2, oh = byH && j <= ny - 2;
+            if (oe) { eyb[q] = __ldg(S.ey_b + j); eya[q] = __ldg(S.ey_a + j); }
+            if (oh) { hyb[q] = __ldg(S.hy_b + j); hya[q] = __ldg(S.hy_a + j); }
+        }
+    }
+    // Dy / Ey(n+1/2) rows ib .. ib+R (te_dy with the x-CPML terms b psi + a d = 0)
+    float ey[R + 1][4], dyN[R + 1][4];
+#pragma unroll
+    for (int k = 0; k < R + 1; ++k) {
+        const int row = ib + k;
+        float ps[4];
+        zero4(ps);
+        te_dy(S, row, true, act, jb, 1.f, 0.f, dt, rdx, hz[k], hz[k + 1], dy[k], ps, dyN[k],
+              C.amp_e);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ey[k][q] = dyN[k][q] * iy[k][q];
+    }
+    float *ring = C.ring;
+    const int pn = par ^ 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = ib + r;
+        const uint32_t ro = o0 + r * P;
+        const float (&hc)[4] = hz[r + 1];
+        // Dx / Ex(n+1/2) row i
+        float hm0 = __shfl_up_sync(0xffffffffu, hc[3], 1);
+        if (lane == 0) hm0 = hzL[r];
+        float dxN[4], ex[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float hm = (q == 0) ? hm0 : hc[q - 1];
+            const float d = (hc[q] - hm) * rdx;
+            const float pv = eyb[q] * p0[r][q] + eya[q] * d;
+            const float dn = dx[r][q] + dt * (d + pv);
+            dxN[q] = vX[q] ? dn : dx[r][q];
+            p0[r][q] = vX[q] ? pv : p0[r][q];
+            ex[q] = dxN[q] * ix[r][q];
+        }
+        float exR = 0.f;
+        if (hasR) {
+            float v = dxr[r];
+            if (updR) {
+                const float d = (hzR[r] - hc[3]) * rdx;
+                float c = d;
+                if (byER) c = d + (__ldg(S.ey_b + jr) * p0r[r] + __ldg(S.ey_a + jr) * d);
+                v = dxr[r] + dt * c;
+            }
+            exR = v * ixr[r];
+        }
+        if (!act) { zero4(ex); }
+        float exr = __shfl_down_sync(0xffffffffu, ex[0], 1);
+        if (lane == 31) exr = exR;
+        // Hz(n+1) row i
+        float hzN[4];
+        float eyo[4], eyn[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            eyo[q] = act ? ey[r][q] : 0.f;
+            eyn[q] = act ? ey[r + 1][q] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float exn = (q < 3) ? ex[q + 1] : exr;
+            const float dey = (eyn[q] - eyo[q]) * rdx;
+            const float dex = (exn - ex[q]) * rdx;
+            const float q2 = 1.f * 0.f + 0.f * dey;
+            const float q3 = hyb[q] * p3[r][q] + hya[q] * dex;
+            const float hn = hc[q] - dt * ((dey + q2) - (dex + q3));
+            hzN[q] = vZ[q] ? hn : hc[q];
+            p3[r][q] = vZ[q] ? q3 : p3[r][q];
+        }
+        if (act && i >= S.src_h1.row_lo && i <= S.src_h1.row_hi)
+            apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
+        if (act) {
+            st4(S.f_main[pn] + ro, hzN);
+            st4(S.f_x[pn] + ro, dxN);
+            st4(S.f_y[pn] + ro, dyN[r]);
+            if (YPSI && byE) st4(S.psi[0][pn] + ro, p0[r]);
+            if (YPSI && byH) st4(S.psi[3][pn] + ro, p3[r]);
+            if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, hzN);
+            if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, ex);
+            if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, eyo);
+            if (nl) {
+                sample_row(L, nl, MTB_C2_MAIN, i, jb, true, hzN, ring);
+                sample_row(L, nl, MTB_C2_X, i, jb, true, ex, ring);
+                sample_row(L, nl, MTB_C2_Y, i, jb, true, eyo, ring);
+            }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
@@ -1207,10 +1586,35 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
     Ctx2D C) {
     __shared__ TileSmem T;
     int4 w;
-    if (!tile_setup(SS, work, n_work, T, w)) return;
-    const int i = w.y + threadIdx.y;
-    if (i >= T.s.nx) return;
-    te_tile(T.s, i, w.z, C, T.lines, T.nl);
+    if (!tile_setup(SS, work, n_work, C.wr, T, w)) return;
+    const mtb_yee2d_struct &S = T.s;
+    const int ib = w.y + threadIdx.y * C.wr;
+    if (ib >= S.nx) return;
+    const int last = ib + WROWS - 1;
+    // lean rows: Dy rows ib .. last+1 interior, Hz rows outside the H x layer,
+    // Dy rows outside the E x layer
+    const bool lean = C.wr == WROWS && ib >= 1 && last + 1 <= S.nx - 2 && ib >= S.xband[0] &&
+                      last < S.xband[1] &&
+                      ib >= S.xband[2] && last + 1 < S.xband[3];
+    if (lean) {
+        const int jb = w.z + 4 * threadIdx.x;
+        const bool yb = jb < S.pitch &&
+                        (band4(jb, S.yband[0], S.yband[1]) || band4(jb, S.yband[2], S.yband[3]) ||
+                         (threadIdx.x == 31 && in_band(jb + 4, S.yband[2], S.yband[3])));
+        if (!__any_sync(0xffffffffu, yb)) {
+#pragma unroll 1
+            for (int h = 0; h < WROWS; h += 2) te_rows<2, false>(S, ib + h, w.z, C, T.lines, T.nl);
+        } else {
+#pragma unroll 1
+            for (int h = 0; h < WROWS; h += 2) te_rows<2, true>(S, ib + h, w.z, C, T.lines, T.nl);
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int r = 0; r < C.wr; ++r) {
+        if (ib + r >= S.nx) break;
+        te_tile(S, ib + r, w.z, C, T.lines, T.nl);
+    }
 }
 
 }  // namespace mtb
@@ -1225,7 +1629,8 @@ struct mtb_yee2d_plan {
     int n_work_tm = 0;                 // work items [0, n_work_tm) are TM, the rest TE
     int n_cols = 0;
     int rows = 32;
-    int variant = 1;                   // 1 row march, 2 tiles
+    int variant = 2;                   // 1 row march, 2 tiles
+    int wr = 1;                        // tiles: rows per warp
     int graph_mode = 0;                // 0 graphs when eligible, -1 off
     cudaStream_t cap = nullptr;        // private capture stream
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // ring flush graph per start parity
@@ -1305,19 +1710,22 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     *out = nullptr;
     if (n < 1 || !structs_in) return fail(MTB_INVALID_ARG, "need at least one structure");
     if (n_amp_cols < 0) return fail(MTB_INVALID_ARG, "n_amp_cols < 0");
-    int variant = (tuning && (tuning->variant == 1 || tuning->variant == 2)) ? tuning->variant : 0;
+    const int variant = (tuning && tuning->variant == 1) ? 1 : 2;   // default: tiles
     int rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
-    if (variant == 0) {
-        // library default: the row march needs enough (rows / rows_per_warp) x strips
-        // warps to fill the GPU; small batches (a single L2-resident structure)
-        // leave most SMs idle and serialise rows, so they use the tiles
-        int64_t warps = 0;
+    int wr = 1;
+    if (variant == 2) {
+        // rows per warp: WROWS (register-blocked lean rows) when the batch still
+        // fills the GPU with 2 blocks per SM, else one (small, L2-resident
+        // batches need the parallelism more than the amortisation)
+        int64_t blocks = 0;
         for (int s = 0; s < n; ++s)
-            warps += (int64_t)((structs_in[s].nx + rows - 1) / rows) *
-                     ((structs_in[s].pitch + 127) / 128);
-        variant = warps >= ROW_MARCH_MIN_WARPS ? 1 : 2;
+            blocks += (int64_t)((structs_in[s].nx + TILE_ROWS - 1) / TILE_ROWS) *
+                      ((structs_in[s].pitch + 127) / 128);
+        wr = (tuning && tuning->rows_per_warp > 0)
+                 ? (tuning->rows_per_warp >= WROWS ? WROWS : 1)
+                 : (blocks >= TILE_MIN_BLOCKS ? WROWS : 1);
+        rows = TROWS * wr;
     }
-    if (variant == 2) rows = TROWS;
     int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     if (ring_slot_elems < 0 || (ring_slot_elems & 3))
         return fail(MTB_INVALID_ARG, "ring_slot_elems must be a non-negative multiple of 4");
@@ -1402,6 +1810,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     p->n_structs = n;
     p->rows = rows;
     p->variant = variant;
+    p->wr = wr;
     p->graph_mode = (tuning && tuning->graph < 0) ? -1 : 0;
     p->n_cols = n_amp_cols;
     p->n_work = (int)n_work;
@@ -1521,6 +1930,7 @@ static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
         C.err = p->err_d.as<int>();
         C.par = par;
         C.first = 0;
+        C.wr = p->wr;
         rc = launch_step(p, C, p->cap);
         par ^= 1;
     }
@@ -1604,6 +2014,7 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
         C.err = p->err_d.as<int>();
         C.par = p->par;
         C.first = p->first;
+        C.wr = p->wr;
         if ((rc = p->timer.begin(st, 0))) return rc;
         if ((rc = launch_step(p, C, st))) return rc;
         if ((rc = p->timer.end(st))) return rc;
@@ -2015,6 +2426,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
             C.err = dErr;
             C.par = par;
             C.first = first ? 1 : 0;
+            C.wr = 1;                              // unused by the row-march kernels
             if (S.pol == MTB_TM) {
                 if (first)
                     k_yee2d_tm<true><<<blocks, 32 * WARPS2D, smem_tm(), st>>>(dS, dWork, n_work, C);
