@@ -493,3 +493,83 @@ def test_tm_gradient_matches_reference_autograd(chunk):
           f"J {float(J):.6e} vs {float(g32['J']):.6e}")
     assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
     assert e32 < 1e-4, e32
+
+
+class _Sheets:
+    """A TFSF-style source with the shape of the reference's mode sources
+    (ports/mode_source.py:21-128): an electric current sheet (``mask``) and a
+    magnetic sheet (``h_masks``) half a cell upstream, the magnetic amplitude
+    delayed and signed. The kernels see only this protocol."""
+
+    def __init__(self, prof, dt, mask, h_masks, te=False, delay=0.0, hsign=-1.0):
+        self.prof, self.dt, self.mask, self.h_masks = prof, dt, mask, h_masks
+        self.te, self.delay, self.hsign = te, delay, hsign
+
+    def amplitude(self, t):
+        return self.prof.amplitude((t if self.te else t + 0.5) * self.dt)
+
+    def h_amplitude(self, t):
+        return self.hsign * self.prof.amplitude((t + 0.5 if self.te else t) * self.dt
+                                                - self.delay)
+
+
+@pytest.mark.parametrize("case", ["tm_x", "tm_y", "te_x"])
+def test_magnetic_sheet_sources_match_oracle(case):
+    """Electric + magnetic sheet pairs (the mode-source path: src_hy_mask,
+    src_hx_mask, src_hz_mask) through run_tm / run_te against the oracle."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.run import run_te, run_tm
+    from meep_torch_b200.core.sources import GaussianPulse
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    nx, ny, dx, npml, n = 70, 58, 0.05, 8, 150
+    eps = np.ones((nx, ny), dtype=np.float32)
+    eps[:, 24:34] = 12.0
+    eps[24:34, :] = np.maximum(eps[24:34, :], 6.0)
+    prof = GaussianPulse(0.65, 0.3)
+    oprof = O.gaussian_pulse(0.65, 0.3)
+    shape = np.sin(np.linspace(0.2, np.pi - 0.2, 14)).astype(np.float32)
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    delay = 2.5 * dx / 2.0
+    if case.startswith("tm"):
+        c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32)
+        m = build_tm_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml)
+        mask = np.zeros((nx, ny), np.float32)
+        if case == "tm_x":
+            mask[14, 22:36] = 2.5 * shape / dx
+            hm = np.zeros((nx - 1, ny), np.float32)
+            hm[13, 22:36] = shape / dx
+            key = "src_hy_mask"
+        else:
+            mask[22:36, 14] = -2.5 * shape / dx
+            hm = np.zeros((nx, ny - 1), np.float32)
+            hm[22:36, 13] = shape / dx
+            key = "src_hx_mask"
+        src = _Sheets(prof, c["dt"], torch.from_numpy(mask).to(dev()),
+                      {key: torch.from_numpy(hm).to(dev())}, delay=delay)
+        st, _ = run_tm(init_tm_state(grid), m, n, source=src)
+        s = O.tm_state(c)
+        for t in range(n):
+            kw = {"hy_mask" if case == "tm_x" else "hx_mask": hm}
+            s = O.tm_step(s, c, amp=oprof((t + 0.5) * c["dt"]), mask=mask,
+                          amp_h=-oprof(t * c["dt"] - delay), **kw)
+        names = ("Ez", "Hx", "Hy", "Dz")
+    else:
+        c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32)
+        m = build_te_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml)
+        mask = np.zeros((nx, ny - 1), np.float32)
+        mask[14, 22:36] = shape / dx
+        hm = np.zeros((nx - 1, ny - 1), np.float32)
+        hm[13, 22:36] = 2.0 * shape / dx
+        src = _Sheets(prof, c["dt"], torch.from_numpy(mask).to(dev()),
+                      {"src_hz_mask": torch.from_numpy(hm).to(dev())}, te=True, delay=delay,
+                      hsign=1.0)
+        st, _ = run_te(init_te_state(grid), m, n, source=src)
+        s = O.te_state(c)
+        for t in range(n):
+            s = O.te_step(s, c, amp=oprof(t * c["dt"]), mask_ey=mask,
+                          amp_h=oprof((t + 0.5) * c["dt"] - delay), hz_mask=hm)
+        names = ("Hz", "Ex", "Ey", "Dx", "Dy")
+    errs = {k: rel_l2(getattr(st, k).cpu().numpy(), s[k]) for k in names}
+    assert all(v < TOL for v in errs.values()), errs
