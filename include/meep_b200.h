@@ -183,8 +183,8 @@ typedef struct mtb_tuning {
     int32_t ring_slots;     /* steps buffered before one DFT contraction    */
     int32_t graph;          /* 2D: replay whole ring flushes (ring_slots steps
                                + one contraction) as a CUDA graph: 0 default
-                               (on for runs of >= 2 flushes while per-launch
-                               timing is off), -1 off                       */
+                               (every whole flush after the plan's first step
+                               while per-launch timing is off), -1 off      */
     int32_t variant;        /* 2D: 0 default (tiles), 1 row march, 2 tiles;
                                3D: 0 default (split), 1 fused x-march,
                                2 split H / E streaming kernels              */

@@ -200,7 +200,42 @@ struct mtb_yee2d_adjoint {
     mtb_adj2d_buffers b{};
     DftState dft;
     int64_t last_launches = 0;
+    // a whole chunk (ring_slots reverse steps with its sample adjoint) replayed
+    // as a CUDA graph, valid for the forward record it was captured with
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const float *g_rec = nullptr;
+    int64_t g_rec_slot = -1, g_rec_off = -1, gkern = 0;
 };
+
+// The device work of one chunk of k reverse steps on `st` (after the phases
+// of its steps are uploaded).
+static int adjoint_chunk(mtb_yee2d_adjoint *p, int k, const float *rec, int64_t rec_slot_elems,
+                         int64_t rec_offset, cudaStream_t st) {
+    int rc;
+    if (p->dft.n_regions > 0) {
+        if ((rc = p->dft.expand(0, k, st))) return rc;
+        ++p->last_launches;
+    } else {
+        MTB_CUDA_TRY(cudaMemsetAsync(p->dft.ring_d.p, 0,
+                                     sizeof(float) * (size_t)p->dft.slot_elems * k, st));
+    }
+    const mtb_yee2d_struct &S = p->s;
+    const dim3 blk(32, AROWS);
+    const dim3 grid((S.pitch / 4 + 31) / 32, (S.nx + AROWS - 1) / AROWS);
+    for (int q = k - 1; q >= 0; --q) {
+        const float *radj = p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems;
+        const float *rq = rec + (size_t)q * rec_slot_elems + rec_offset;
+        k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq);
+        MTB_CHECK_LAUNCH();
+        k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
+        MTB_CHECK_LAUNCH();
+        k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
+        MTB_CHECK_LAUNCH();
+        p->last_launches += 3;
+    }
+    return MTB_OK;
+}
 
 extern "C" {
 
@@ -263,28 +298,41 @@ int mtb_yee2d_adjoint_run(mtb_yee2d_adjoint *p, int64_t t0, int32_t k, const flo
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
     if ((rc = p->dft.upload_phases(t0, k, st))) return rc;
-    if (p->dft.n_regions > 0) {
-        if ((rc = p->dft.expand(0, k, st))) return rc;
-        ++p->last_launches;
-    } else {
-        MTB_CUDA_TRY(cudaMemsetAsync(p->dft.ring_d.p, 0,
-                                     sizeof(float) * (size_t)p->dft.slot_elems * k, st));
+    const bool whole = k == p->dft.slots;
+    if (whole && !p->gexec) {                  // capture the whole-chunk graph once
+        if (!p->cap) MTB_CUDA_TRY(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+        const int64_t l0 = mtb_launch_count();
+        MTB_CUDA_TRY(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+        rc = adjoint_chunk(p, k, rec, rec_slot_elems, rec_offset, p->cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(p->cap, &g);
+        const int64_t nk = mtb_launch_count() - l0;
+        count_launch(-nk);                     // captured, not launched
+        if (!rc && e != cudaSuccess)
+            rc = fail(MTB_CUDA_ERROR, "adjoint graph capture: %s", cudaGetErrorString(e));
+        if (!rc) {
+            const cudaError_t ei = cudaGraphInstantiate(&p->gexec, g, 0);
+            if (ei != cudaSuccess) {
+                p->gexec = nullptr;
+                rc = fail(MTB_CUDA_ERROR, "adjoint graph instantiate: %s", cudaGetErrorString(ei));
+            }
+        }
+        if (g) cudaGraphDestroy(g);
+        if (rc) return rc;
+        p->gkern = nk;
+        p->g_rec = rec;
+        p->g_rec_slot = rec_slot_elems;
+        p->g_rec_off = rec_offset;
     }
-    const mtb_yee2d_struct &S = p->s;
-    const dim3 blk(32, AROWS);
-    const dim3 grid((S.pitch / 4 + 31) / 32, (S.nx + AROWS - 1) / AROWS);
-    for (int q = k - 1; q >= 0; --q) {
-        const float *radj = p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems;
-        const float *rq = rec + (size_t)q * rec_slot_elems + rec_offset;
-        k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq);
-        MTB_CHECK_LAUNCH();
-        k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
-        MTB_CHECK_LAUNCH();
-        k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
-        MTB_CHECK_LAUNCH();
-        p->last_launches += 3;
+    p->last_launches = 0;
+    if (whole && p->gexec && p->g_rec == rec && p->g_rec_slot == rec_slot_elems &&
+        p->g_rec_off == rec_offset) {
+        MTB_CUDA_TRY(cudaGraphLaunch(p->gexec, st));
+        count_launch(p->gkern);
+        p->last_launches = p->gkern;
+        return MTB_OK;
     }
-    return MTB_OK;
+    return adjoint_chunk(p, k, rec, rec_slot_elems, rec_offset, st);
 }
 
 int64_t mtb_yee2d_adjoint_last_launches(const mtb_yee2d_adjoint *p) {
@@ -293,6 +341,8 @@ int64_t mtb_yee2d_adjoint_last_launches(const mtb_yee2d_adjoint *p) {
 
 void mtb_yee2d_adjoint_destroy(mtb_yee2d_adjoint *p) {
     if (!p) return;
+    if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    if (p->cap) cudaStreamDestroy(p->cap);
     p->dft.release();
     delete p;
 }

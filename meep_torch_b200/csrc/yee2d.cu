@@ -1981,7 +1981,7 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     const float *ad = p->amp_d.as<float>();
     const int G = p->dft.slots;
     const size_t prow = (size_t)p->dft.total_nf * 4;         // floats per phase row
-    const bool graphs = p->graph_mode >= 0 && !p->timer.on && G >= 2 && k >= 2 * G;
+    const bool graphs = p->graph_mode >= 0 && !p->timer.on && G >= 2 && k >= G;
     if (graphs && (rc = p->stage_d.ensure(sizeof(float) * (2 * (size_t)G * nc + G * prow))))
         return rc;
     int slot = 0;
