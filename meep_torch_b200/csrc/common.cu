@@ -343,11 +343,10 @@ int DftState::upload_phases(int64_t t0, int k, cudaStream_t st) {
     if (n_regions == 0) return MTB_OK;
     const size_t n = (size_t)k * total_nf * 4;
     int rc;
-    if ((rc = phase_h.ensure(n * sizeof(float)))) return rc;
+    void *hp = nullptr;
+    if ((rc = phase_h.acquire(n * sizeof(float), &hp))) return rc;
     if ((rc = phase_d.ensure(n * sizeof(float)))) return rc;
-    // the previous upload may still be in flight from the staging buffer
-    MTB_CUDA_TRY(cudaStreamSynchronize(st));
-    float *P = phase_h.as<float>();
+    float *P = static_cast<float *>(hp);
     const double two_pi = 2.0 * M_PI;
     for (int g = 0; g < n_groups; ++g) {
         const double dt = group_dt[g];
@@ -375,9 +374,8 @@ int DftState::upload_phases(int64_t t0, int k, cudaStream_t st) {
             }
         }
     }
-    MTB_CUDA_TRY(cudaMemcpyAsync(phase_d.p, phase_h.p, n * sizeof(float), cudaMemcpyHostToDevice,
-                                 st));
-    return MTB_OK;
+    MTB_CUDA_TRY(cudaMemcpyAsync(phase_d.p, P, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    return phase_h.queued(st);
 }
 
 int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm,

@@ -86,6 +86,48 @@ struct HostBuf {
 };
 
 // Opt-in per-launch device timing (event pairs around launches).
+// Two pinned host staging buffers used alternately for host -> device
+// uploads: a buffer is refilled only after its previous upload completed
+// (an event), so back-to-back runs on one stream never wait for the GPU.
+struct PinnedPair {
+    HostBuf h[2];
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool pending[2] = {false, false};
+    int next = 0;
+    // a staging buffer of at least `bytes` that may be overwritten now
+    int acquire(size_t bytes, void **out) {
+        const int b = next;
+        if (pending[b]) {
+            MTB_CUDA_TRY(cudaEventSynchronize(ev[b]));
+            pending[b] = false;
+        }
+        const int rc = h[b].ensure(bytes);
+        if (rc) return rc;
+        *out = h[b].p;
+        return MTB_OK;
+    }
+    // the upload from the last acquired buffer has been queued on `st`
+    int queued(cudaStream_t st) {
+        const int b = next;
+        if (!ev[b]) MTB_CUDA_TRY(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+        MTB_CUDA_TRY(cudaEventRecord(ev[b], st));
+        pending[b] = true;
+        next ^= 1;
+        return MTB_OK;
+    }
+    void release() {
+        for (int b = 0; b < 2; ++b) {
+            if (ev[b]) {
+                cudaEventSynchronize(ev[b]);
+                cudaEventDestroy(ev[b]);
+            }
+            ev[b] = nullptr;
+            pending[b] = false;
+            h[b].release();
+        }
+    }
+};
+
 struct LaunchTimer {
     bool on = false;
     std::vector<cudaEvent_t> pool;
@@ -114,7 +156,7 @@ struct DftState {
     int total_nf = 0;                      // sum of nf
     // device
     DevBuf regions_d, blk_start_d, blk_region_d, phase_d, ring_d;
-    HostBuf phase_h;
+    PinnedPair phase_h;
     int64_t slot_elems = 0;
     int slots = 0;                         // ring depth K
     int64_t n_blocks = 0;                  // contraction blocks

@@ -1624,7 +1624,7 @@ using namespace mtb;
 struct mtb_yee2d_plan {
     int n_structs = 0;
     DevBuf structs_d, work_d, amp_d, err_d;
-    HostBuf amp_h;
+    PinnedPair amp_h;
     int n_work = 0;
     int n_work_tm = 0;                 // work items [0, n_work_tm) are TM, the rest TE
     int n_cols = 0;
@@ -1965,19 +1965,22 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    if ((rc = mtb_yee2d_check(p, stream))) return rc;        // also orders the staging reuse
+    // the row march's bounded waits may have raised the error flag (tiles never wait)
+    if (p->variant == 1 && (rc = mtb_yee2d_check(p, stream))) return rc;
     const int nc = std::max(p->n_cols, 1);
     const size_t per = (size_t)k * nc;
-    if ((rc = p->amp_h.ensure(2 * per * sizeof(float)))) return rc;
+    void *hp = nullptr;
+    if ((rc = p->amp_h.acquire(2 * per * sizeof(float), &hp))) return rc;
     if ((rc = p->amp_d.ensure(2 * per * sizeof(float)))) return rc;
     if ((rc = p->dft.upload_phases(t0, k, st))) return rc;
-    float *ah = p->amp_h.as<float>();
+    float *ah = static_cast<float *>(hp);
     for (size_t i = 0; i < per; ++i) {
         ah[i] = coef_e ? (float)coef_e[i] : 0.f;
         ah[per + i] = coef_h ? (float)coef_h[i] : 0.f;
     }
-    MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, p->amp_h.p, 2 * per * sizeof(float),
+    MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, ah, 2 * per * sizeof(float),
                                  cudaMemcpyHostToDevice, st));
+    if ((rc = p->amp_h.queued(st))) return rc;
     const float *ad = p->amp_d.as<float>();
     const int G = p->dft.slots;
     const size_t prow = (size_t)p->dft.total_nf * 4;         // floats per phase row

@@ -737,7 +737,7 @@ using namespace mtb;
 struct mtb_yee3d_plan {
     mtb_yee3d_struct s{};
     DevBuf s_d, pstart_d, amp_d;
-    HostBuf amp_h;
+    PinnedPair amp_h;
     int rows = 32;
     int nzw = 1;
     int variant = 2;               // 1 fused x-march, 2 split H / E
@@ -940,13 +940,14 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    if ((rc = p->amp_h.ensure(sizeof(float) * k))) return rc;
+    void *hp = nullptr;
+    if ((rc = p->amp_h.acquire(sizeof(float) * k, &hp))) return rc;
     if ((rc = p->amp_d.ensure(sizeof(float) * k))) return rc;
-    if ((rc = p->dft.upload_phases(t0, k, st))) return rc;   // syncs the stream first
-    float *ah = p->amp_h.as<float>();
+    if ((rc = p->dft.upload_phases(t0, k, st))) return rc;
+    float *ah = static_cast<float *>(hp);
     for (int s = 0; s < k; ++s) ah[s] = coef ? (float)coef[s] : 0.f;
-    MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, p->amp_h.p, sizeof(float) * k, cudaMemcpyHostToDevice,
-                                 st));
+    MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, ah, sizeof(float) * k, cudaMemcpyHostToDevice, st));
+    if ((rc = p->amp_h.queued(st))) return rc;
     int slot = 0;
     const bool sampling = p->dft.n_regions > 0 && p->n_samples > 0;
     for (int s = 0; s < k; ++s) {
