@@ -351,6 +351,36 @@ int mtb_yee3d_timing(const mtb_yee3d_plan *plan, double *step_ms, int64_t *step_
                      double *dft_ms, int64_t *dft_launches);
 void mtb_yee3d_plan_destroy(mtb_yee3d_plan *plan);
 
+/* ------------------------------------------------------- 3D adjoint */
+/* Discrete adjoint of the 3D CPML step (core/stepper_3d.py:363-482) and of
+ * the plane sampling (core/monitors_3d.py:70-189): the reverse sweep of the
+ * reference's run_3d_adjoint (core/adjoint3d.py:56-115).
+ *   g[0..5]   d J / d (Ex, Ey, Ez, Hx, Hy, Hz), box layout (nx x ny x zpitch)
+ *   g_psi     d J / d psi (12, as mtb_yee3d_struct psi)
+ *   tmp[0..14] scratch boxes; g_eps accumulates d J / d eps (cell-centred). */
+typedef struct mtb_adj3d_buffers {
+    float *g[6];
+    float *g_psi[12];
+    float *tmp[15];
+    float *g_eps;
+} mtb_adj3d_buffers;
+
+typedef struct mtb_yee3d_adjoint mtb_yee3d_adjoint;
+
+int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers *bufs,
+                             const mtb_dft_region *regions, int32_t n_regions,
+                             const mtb_phase_group *groups, int32_t n_groups,
+                             int64_t ring_slot_elems, int32_t ring_slots,
+                             mtb_yee3d_adjoint **out);
+/* Reverse steps t0+k-1 .. t0 (k <= ring_slots). E component c (0..2) of
+ * record slot q (0..k) is at rec + q * rec_slot_stride + c * rec_comp_stride
+ * (box layout): slot 0 holds E before step t0, slot q the E after step
+ * t0+q-1. */
+int mtb_yee3d_adjoint_run(mtb_yee3d_adjoint *p, int64_t t0, int32_t k, const float *rec,
+                          int64_t rec_comp_stride, int64_t rec_slot_stride, void *stream);
+int64_t mtb_yee3d_adjoint_last_launches(const mtb_yee3d_adjoint *p);
+void mtb_yee3d_adjoint_destroy(mtb_yee3d_adjoint *p);
+
 /* ------------------------------------------------------------ layout */
 
 /* Strided copy of an n0 x n1 x n2 block between a dense reference array
@@ -386,7 +416,8 @@ const char *mtb_last_error(void);
 int32_t mtb_abi_version(void);
 /* sizeof of the ABI structs, for binding checks: 0 mtb_cells,
  * 1 mtb_line_sample, 2 mtb_yee2d_struct, 3 mtb_phase_group,
- * 4 mtb_dft_region, 5 mtb_tuning, 6 mtb_yee3d_struct, 7 mtb_adj2d_buffers */
+ * 4 mtb_dft_region, 5 mtb_tuning, 6 mtb_yee3d_struct, 7 mtb_adj2d_buffers,
+ * 8 mtb_adj3d_buffers */
 int64_t mtb_struct_size(int32_t which);
 /* Kernels launched by this library since load (all entry points). */
 int64_t mtb_launch_count(void);

@@ -79,8 +79,12 @@ class Adj2DBuffers(C.Structure):
     _fields_ = [("g", vp * 4), ("g_psi", vp * 4), ("tmp", vp * 4), ("g_eps", vp)]
 
 
+class Adj3DBuffers(C.Structure):
+    _fields_ = [("g", vp * 6), ("g_psi", vp * 12), ("tmp", vp * 15), ("g_eps", vp)]
+
+
 STRUCTS = [Cells, LineSample, Yee2DStruct, PhaseGroup, DftRegion, Tuning, Yee3DStruct,
-           Adj2DBuffers]
+           Adj2DBuffers, Adj3DBuffers]
 
 # name -> (restype, argtypes); the exported C ABI (include/meep_b200.h)
 SIGNATURES = {
@@ -117,6 +121,13 @@ SIGNATURES = {
     "mtb_yee3d_current": (C.c_int32, [vp]),
     "mtb_yee3d_last_launches": (C.c_int64, [vp]),
     "mtb_yee3d_plan_destroy": (None, [vp]),
+    "mtb_yee3d_adjoint_create": (C.c_int, [C.POINTER(Yee3DStruct), C.POINTER(Adj3DBuffers),
+                                           C.POINTER(DftRegion), C.c_int32,
+                                           C.POINTER(PhaseGroup), C.c_int32, C.c_int64,
+                                           C.c_int32, C.POINTER(vp)]),
+    "mtb_yee3d_adjoint_run": (C.c_int, [vp, C.c_int64, C.c_int32, vp, C.c_int64, C.c_int64, vp]),
+    "mtb_yee3d_adjoint_last_launches": (C.c_int64, [vp]),
+    "mtb_yee3d_adjoint_destroy": (None, [vp]),
     "mtb_yee3d_set_timing": (C.c_int, [vp, C.c_int32]),
     "mtb_yee3d_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

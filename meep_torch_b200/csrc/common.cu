@@ -468,6 +468,7 @@ int64_t mtb_struct_size(int32_t which) {
         case 5: return sizeof(mtb_tuning);
         case 6: return sizeof(mtb_yee3d_struct);
         case 7: return sizeof(mtb_adj2d_buffers);
+        case 8: return sizeof(mtb_adj3d_buffers);
         default: return -1;
     }
 }

@@ -197,6 +197,9 @@ class Engine3D:
                 "mtb_yee3d_plan_create")
         self.plan = plan
         self.S = S
+        self.regions, self.n_regions = reg_arr, len(regions)
+        self.groups, self.n_groups = grp_arr, len(groups)
+        self.ring_elems = ring
 
     # ------------------------------------------------------------ helpers
     def _sptr(self):
@@ -325,6 +328,24 @@ class Engine3D:
     @property
     def current(self):
         return self.lib.mtb_yee3d_current(self.plan)
+
+    def _live_buffers(self):
+        cur = self.current
+        return [self.box[k][cur] for k in FIELDS + PSI]
+
+    def snapshot(self):
+        """Copy of the live state (box layout: six fields, then twelve psi) for restore()."""
+        return [t.clone() for t in self._live_buffers()]
+
+    def restore(self, snap):
+        """Make a snapshot() the live state again (t_idx is the caller's)."""
+        for dst, src in zip(self._live_buffers(), snap):
+            dst.copy_(src)
+
+    def live_e(self):
+        """The live Ex, Ey, Ez boxes (views; the next step overwrites the other buffer)."""
+        cur = self.current
+        return [self.box[k][cur] for k in FIELDS[:3]]
 
     def fields(self):
         """Current fields and CPML memory as reference-shaped tensors."""

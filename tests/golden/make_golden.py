@@ -14,6 +14,7 @@ cases of the hot path through its own public functions:
   ``checkpoint_every`` (``python make_golden.py grad`` writes only these)
 * the design chain (``conic_filter``, ``tanh_projection``, ``MaterialGrid``,
   ``DesignRegion``, ``OptimizationProblem``; ``python make_golden.py design``)
+* d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -263,7 +264,47 @@ def design_case():
                 box=np.array(reg.box), rho0=_np(rho0), f0=f0, grad=grad)
 
 
+def grad3d_case(prec):
+    """d J / d eps of the reference's run_3d_adjoint (core/adjoint3d.py:56) on a
+    small CPML grid with spheres, an Ez point dipole and two flux faces."""
+    from meep_torch.core.adjoint3d import run_3d_adjoint
+    rng = np.random.default_rng(13)
+    n, dx, npml = 20, 1.0 / 16, 4
+    eps = np.ones((n, n, n))
+    ax = (np.arange(n) + 0.5) * dx
+    for _ in range(6):
+        cc = rng.uniform(0.35, 0.9, 3)
+        r = rng.uniform(0.08, 0.2)
+        inside = ((ax[:, None, None] - cc[0]) ** 2 + (ax[None, :, None] - cc[1]) ** 2 +
+                  (ax[None, None, :] - cc[2]) ** 2) <= r * r
+        eps[inside] = rng.uniform(2.0, 8.0)
+    e = torch.tensor(eps, dtype=DT[prec], requires_grad=True)
+    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device="cpu")
+    src = PointSource3D(c.dt, "Ez", 10, 9, 11, GaussianPulse(0.9, 0.6))
+    freqs = [0.7, 0.9, 1.1]
+    mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=15, win=(5, 15, 5, 15)),
+            FluxMonitor3D(c.dt, freqs, normal="z", idx=6, win=(5, 15, 5, 15))]
+    w = torch.tensor([1.0, -0.7, 0.4], dtype=DT[prec])
+
+    def loss_fn(accs):
+        return 1e15 * ((w * mons[0].flux(accs[0], dx)).sum()
+                       + (w.flip(0) * mons[1].flux(accs[1], dx)).sum()
+                       + 1e-3 * sum((a * a).sum() for a in accs))
+
+    s0 = init_3d_state(n, n, n, npml=npml, dtype=DT[prec], device="cpu")
+    n_steps, chunk = 70, 25
+    L, accs = run_3d_adjoint(c, n_steps, chunk, src, mons, loss_fn, s0)
+    return dict(n=n, dx=dx, npml=npml, eps=eps, freqs=np.array(freqs), src=np.array([10, 9, 11]),
+                fcen=0.9, fwidth=0.6, n_steps=n_steps, chunk=chunk, L=float(L),
+                grad=_np(e.grad), acc_0=_np(accs[0]), acc_1=_np(accs[1]))
+
+
 def main():
+    if sys.argv[1:] == ["grad3d"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_grad3d_{prec}.npz"),
+                                **grad3d_case(prec))
+        return
     if sys.argv[1:] == ["design"]:
         np.savez_compressed(os.path.join(HERE, "golden_design.npz"), **design_case())
         return

@@ -573,3 +573,38 @@ def test_magnetic_sheet_sources_match_oracle(case):
         names = ("Hz", "Ex", "Ey", "Dx", "Dy")
     errs = {k: rel_l2(getattr(st, k).cpu().numpy(), s[k]) for k in names}
     assert all(v < TOL for v in errs.values()), errs
+
+
+def test_3d_gradient_matches_reference_run_3d_adjoint():
+    """d J / d eps of run_3d_adjoint on the library's 3D adjoint kernels against the
+    reference's own run_3d_adjoint (core/adjoint3d.py:56-115; fixtures made by
+    tests/golden/make_golden.py grad3d), chunked differently on each side."""
+    from meep_torch_b200.core.adjoint3d import run_3d_adjoint
+    from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D
+    from meep_torch_b200.core.sources import GaussianPulse
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    g32, g64 = load_golden("grad3d_f32"), load_golden("grad3d_f64")
+    n, dx, npml = int(g32["n"]), float(g32["dx"]), int(g32["npml"])
+    e = torch.tensor(g32["eps"], dtype=torch.float32, device=dev(), requires_grad=True)
+    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device=dev())
+    i, j, k = (int(v) for v in g32["src"])
+    src = PointSource3D(c.dt, "Ez", i, j, k, GaussianPulse(float(g32["fcen"]), float(g32["fwidth"])))
+    freqs = [float(f) for f in g32["freqs"]]
+    mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=15, win=(5, 15, 5, 15)),
+            FluxMonitor3D(c.dt, freqs, normal="z", idx=6, win=(5, 15, 5, 15))]
+    w = torch.tensor([1.0, -0.7, 0.4], dtype=torch.float32, device=dev())
+
+    def loss_fn(accs):
+        return 1e15 * ((w * mons[0].flux(accs[0], dx)).sum()
+                       + (w.flip(0) * mons[1].flux(accs[1], dx)).sum()
+                       + 1e-3 * sum((a * a).sum() for a in accs))
+
+    L, accs = run_3d_adjoint(c, int(g32["n_steps"]), 16, src, mons, loss_fn,
+                             init_3d_state(n, n, n, npml=npml, device=dev()))
+    got = e.grad.cpu().numpy()
+    e32, e64 = rel_l2(got, g32["grad"]), rel_l2(got, g64["grad"])
+    print(f"3D grad: rel L2 vs reference f32 {e32:.3e}, vs f64 {e64:.3e}; "
+          f"L {L:.6e} vs {float(g32['L']):.6e}")
+    assert abs(L - float(g32["L"])) <= 1e-4 * abs(float(g32["L"]))
+    assert rel_l2(accs[0].cpu().numpy(), g32["acc_0"]) < TOL
+    assert e32 < TOL, e32
