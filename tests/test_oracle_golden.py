@@ -183,3 +183,35 @@ def test_reference_gradient_matches_oracle_finite_differences():
         fd = (J_of(ep) - J_of(em)) / (2 * h)
         ref = float(g["grad"][i, j])
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-16, (i, j, fd, ref)
+
+
+def test_reference_3d_gradient_matches_oracle_finite_differences():
+    """The golden d J / d eps of run_3d_adjoint (float64) against central finite
+    differences of the oracle's float64 3D run at two cells."""
+    g = load_golden("grad3d_f64")
+    n, dx, npml, steps = int(g["n"]), float(g["dx"]), int(g["npml"]), int(g["n_steps"])
+    freqs = [float(f) for f in g["freqs"]]
+    si, sj, sk = (int(v) for v in g["src"])
+    prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
+    w = np.array([1.0, -0.7, 0.4])
+
+    def J_of(eps):
+        c = O.coeffs_3d(n, n, n, dx, eps=eps, npml=npml, dtype=np.float64)
+        dt = c["dt"]
+        mons = [lambda s, t: O.flux3d_sample(s, t, dt, freqs, "x", 15, (5, 15, 5, 15)),
+                lambda s, t: O.flux3d_sample(s, t, dt, freqs, "z", 6, (5, 15, 5, 15))]
+        _, (a0, a1) = O.run_3d(O.state_3d(c), c, steps, amp_fn=lambda t: prof(O.src_time(t, dt)),
+                               src=("Ez", si, sj, sk), monitors=mons)
+        return 1e15 * float((w * O.flux3d(a0, dx)).sum() + (w[::-1] * O.flux3d(a1, dx)).sum()
+                            + 1e-3 * ((a0 * a0).sum() + (a1 * a1).sum()))
+
+    eps = g["eps"].astype(np.float64)
+    assert abs(J_of(eps) - float(g["L"])) <= 1e-9 * abs(float(g["L"]))
+    h = 1e-4
+    for (i, j, k) in [(12, 9, 11), (14, 12, 8)]:
+        ep, em = eps.copy(), eps.copy()
+        ep[i, j, k] += h
+        em[i, j, k] -= h
+        fd = (J_of(ep) - J_of(em)) / (2 * h)
+        ref = float(g["grad"][i, j, k])
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-12, (i, j, k, fd, ref)
