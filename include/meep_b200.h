@@ -262,23 +262,26 @@ void mtb_yee2d_plan_destroy(mtb_yee2d_plan *plan);
 int mtb_yee2d_ring(const mtb_yee2d_plan *plan, float **ring, int64_t *slot_elems,
                    int32_t *ring_slots);
 
-/* ------------------------------------------------------- 2D TM adjoint */
-/* Discrete adjoint (reverse mode) of the TM step, the transpose of
- * core/stepper_tm.py:234-254 with CPML (PEC walls, sigma = 0, no poles) and
- * of the DFT / flux sampling (core/monitors.py:24-100): what torch autograd
- * computes through the reference's run_tm (core/run.py:43-120).
+/* ---------------------------------------------------------- 2D adjoint */
+/* Discrete adjoint (reverse mode) of the TM and TE steps, the transpose of
+ * core/stepper_tm.py:234-254 / core/stepper_te.py:178-190 with CPML (PEC
+ * walls, sigma = 0, no poles) and of the DFT / flux sampling
+ * (core/monitors.py:24-155): what torch autograd computes through the
+ * reference's run_tm / run_te (core/run.py:43-126).
  *
  * Adjoint state (box layout of the structure, nx x pitch floats each, one
  * buffer per array), holding on entry d J / d (state after the last step of
  * the call) and on return d J / d (state before its first step):
- *   g[0] Ez, g[1] Hx, g[2] Hy, g[3] Dz, g_psi[0..3] as mtb_yee2d_struct psi.
- * tmp[0..3]: scratch of the same size. g_eps accumulates d J / d eps_inf
- * (box layout; the caller zeroes it once). */
+ *   TM: g[0] Ez, g[1] Hx, g[2] Hy, g[3] Dz;  TE: g[0] Hz, g[1] Ex, g[2] Ey,
+ *   g[3] Dx, g[4] Dy;  g_psi[0..3] as mtb_yee2d_struct psi.
+ * tmp[0..3]: scratch of the same size. g_eps accumulates d J / d eps (box
+ * layout; the caller zeroes it once): TM g_eps[0] = eps_inf; TE g_eps[0] =
+ * eps_x (Ex nodes), g_eps[1] = eps_y (Ey nodes). */
 typedef struct mtb_adj2d_buffers {
-    float *g[4];
+    float *g[5];
     float *g_psi[4];
     float *tmp[4];
-    float *g_eps;
+    float *g_eps[2];
 } mtb_adj2d_buffers;
 
 typedef struct mtb_yee2d_adjoint mtb_yee2d_adjoint;
@@ -291,11 +294,13 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
                              const mtb_phase_group *groups, int32_t n_groups,
                              int64_t ring_slot_elems, int32_t ring_slots,
                              mtb_yee2d_adjoint **out);
-/* Reverse steps t0+k-1 .. t0 (k <= ring_slots). `rec` slot q holds the
- * forward Ez after step t0+q at element rec_offset + box index (the ring of
- * a forward plan that ran these k steps with a full-grid Ez sample). */
+/* Reverse steps t0+k-1 .. t0 (k <= ring_slots). `rec` slot q (slot size
+ * rec_slot_elems) holds the forward E of step t0+q (the ring of a forward
+ * plan that ran these k steps with full-grid E samples): TM Ez after the step
+ * at rec_offset[0] + box index; TE Ex, Ey of the step at rec_offset[0],
+ * rec_offset[1]. */
 int mtb_yee2d_adjoint_run(mtb_yee2d_adjoint *p, int64_t t0, int32_t k, const float *rec,
-                          int64_t rec_slot_elems, int64_t rec_offset, void *stream);
+                          int64_t rec_slot_elems, const int64_t *rec_offset, void *stream);
 int64_t mtb_yee2d_adjoint_last_launches(const mtb_yee2d_adjoint *p);
 void mtb_yee2d_adjoint_destroy(mtb_yee2d_adjoint *p);
 

@@ -76,7 +76,7 @@ class Yee3DStruct(C.Structure):
 
 
 class Adj2DBuffers(C.Structure):
-    _fields_ = [("g", vp * 4), ("g_psi", vp * 4), ("tmp", vp * 4), ("g_eps", vp)]
+    _fields_ = [("g", vp * 5), ("g_psi", vp * 4), ("tmp", vp * 4), ("g_eps", vp * 2)]
 
 
 class Adj3DBuffers(C.Structure):
@@ -107,8 +107,8 @@ SIGNATURES = {
                                            C.POINTER(DftRegion), C.c_int32,
                                            C.POINTER(PhaseGroup), C.c_int32, C.c_int64,
                                            C.c_int32, C.POINTER(vp)]),
-    "mtb_yee2d_adjoint_run": (C.c_int, [vp, C.c_int64, C.c_int32, vp, C.c_int64, C.c_int64,
-                                        vp]),
+    "mtb_yee2d_adjoint_run": (C.c_int, [vp, C.c_int64, C.c_int32, vp, C.c_int64,
+                                        C.POINTER(C.c_int64), vp]),
     "mtb_yee2d_adjoint_last_launches": (C.c_int64, [vp]),
     "mtb_yee2d_adjoint_destroy": (None, [vp]),
     "mtb_yee2d_set_timing": (C.c_int, [vp, C.c_int32]),

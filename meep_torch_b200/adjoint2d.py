@@ -1,4 +1,4 @@
-"""Reverse-mode gradients of the 2D TM run through the B200 kernels.
+"""Reverse-mode gradients of the 2D TM and TE runs through the B200 kernels.
 
 The reference gets dJ/d eps from torch autograd through ``run_tm`` (core/run.py:43-120),
 optionally checkpointed (``checkpoint_every``). Here the same derivative comes from the
@@ -7,10 +7,12 @@ forward TM step with CPML and of the DFT / flux sampling, run backwards in time.
 
 Forward: the run goes in chunks of ``chunk`` steps (the ring depth); the live state at each
 chunk start is kept (box layout). Backward, chunk by chunk from the last: the chunk is
-re-run from its snapshot on a recording plan whose ring keeps the full-grid Ez of every step
-(needed for d/d eps of E = D / eps), then the adjoint plan sweeps the chunk's steps in
-reverse. Gradients reach ``coeffs.eps_inf``; other coefficient tensors and the initial state
-receive none (a gradient request for them raises NotImplementedError).
+re-run from its snapshot on a recording plan whose ring keeps the full-grid E of every step
+(Ez for TM, Ex and Ey for TE: needed for d/d eps of E = D / eps), then the adjoint plan
+sweeps the chunk's steps in reverse. Gradients reach ``coeffs.eps_inf`` (TM) or
+``coeffs.eps_x`` / ``coeffs.eps_y`` (TE, and through them ``eps_inf``); other coefficient
+tensors and the initial state receive none (a gradient request for them raises
+NotImplementedError).
 """
 from __future__ import annotations
 
@@ -22,6 +24,7 @@ from . import _lib as L
 from .engine2d import Engine2D
 
 STATE_TM = ("Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy")
+STATE_TE = ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Hzy", "psi_Hzx", "psi_Eyx", "psi_Exy")
 
 
 class _Grid:
@@ -31,21 +34,22 @@ class _Grid:
         self.dt, self.dtype, self.device = dt, torch.float32, device
 
 
-def _record_monitor(dt, device):
+def _record_monitors(dt, device, te):
     from .core.monitors import DFTFieldsMonitor
-    return DFTFieldsMonitor(_Grid(dt, device), [1.0], "Ez")
+    comps = ("Ex", "Ey") if te else ("Ez",)
+    return [DFTFieldsMonitor(_Grid(dt, device), [1.0], c) for c in comps]
 
 
-class TMGradRun:
-    """One differentiable TM run: forward() keeps chunk snapshots, backward()
-    turns output gradients into d J / d eps_inf."""
+class GradRun2D:
+    """One differentiable TM or TE run: forward() keeps chunk snapshots, backward()
+    turns output gradients into d J / d eps (TM eps_inf; TE eps_x, eps_y)."""
 
     def __init__(self, state, coeffs, n_steps, source, monitors, chunk=32,
                  phase_mode="exact"):
-        if type(state).__name__ != "TMState" and not hasattr(state, "Ez"):
-            raise L.MtbUnsupported("gradients: TM states only on the B200 path")
+        self.te = hasattr(state, "Hz")
         if getattr(coeffs, "y_pmc", False):
             raise L.MtbUnsupported("gradients: PEC walls only (y_pmc)")
+        self.names = STATE_TE if self.te else STATE_TM
         self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
         self.source, self.monitors = source, list(monitors)
         self.chunk = max(1, min(int(chunk), 64))
@@ -63,7 +67,7 @@ class TMGradRun:
         self.out_state = st
         self.accs = [a.clone() for a in eng.accumulators(0)]
         self.eng = eng
-        return [getattr(st, f) for f in STATE_TM] + self.accs
+        return [getattr(st, f) for f in self.names] + self.accs
 
     def backward(self, grads):
         eng, lib = self.eng, L.load()
@@ -72,13 +76,18 @@ class TMGradRun:
         P = int(eng.structs[0].pitch)
         dev = eng.device
         box = lambda: torch.zeros((nx, P), dtype=torch.float32, device=dev)  # noqa: E731
-        g, gpsi, tmp, geps = [box() for _ in range(4)], [box() for _ in range(4)], \
-            [box() for _ in range(4)], box()
+        nfld = 5 if self.te else 4
+        g, gpsi, tmp = [box() for _ in range(nfld)], [box() for _ in range(4)], \
+            [box() for _ in range(4)]
+        geps = [box() for _ in range(2 if self.te else 1)]
         targets = g + gpsi
-        yoff = 0 if self.out_state.psi_Hyx.shape[1] == ny else 1
-        offs = [(0, 0)] * 6 + [(1, yoff), (1, yoff)]
-        ns = len(STATE_TM)
-        for q, name in enumerate(STATE_TM):
+        if self.te:
+            offs = [(0, 0)] * 5 + [(0, 1), (1, 0), (0, 0), (0, 0)]
+        else:
+            yoff = 0 if self.out_state.psi_Hyx.shape[1] == ny else 1
+            offs = [(0, 0)] * 6 + [(1, yoff), (1, yoff)]
+        ns = len(self.names)
+        for q, name in enumerate(self.names):
             gr = grads[q]
             if gr is None or gr.numel() == 0:
                 continue
@@ -96,9 +105,12 @@ class TMGradRun:
             C.memmove(C.addressof(regs[r]), C.addressof(eng.regions[r]), C.sizeof(L.DftRegion))
             regs[r].acc = L.ptr(gaccs[by_ptr[int(eng.regions[r].acc)]])
         bufs = L.Adj2DBuffers()
+        for q in range(nfld):
+            bufs.g[q] = L.ptr(g[q])
         for q in range(4):
-            bufs.g[q], bufs.g_psi[q], bufs.tmp[q] = L.ptr(g[q]), L.ptr(gpsi[q]), L.ptr(tmp[q])
-        bufs.g_eps = L.ptr(geps)
+            bufs.g_psi[q], bufs.tmp[q] = L.ptr(gpsi[q]), L.ptr(tmp[q])
+        for q in range(len(geps)):
+            bufs.g_eps[q] = L.ptr(geps[q])
         adj = C.c_void_p()
         L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
                                              regs if nreg else None, nreg, eng.groups,
@@ -107,7 +119,7 @@ class TMGradRun:
         keep = [gaccs, g, gpsi, tmp, geps]
         stream = eng._sptr()
         try:
-            rec_mon = _record_monitor(float(self.coeffs.dt), dev)
+            rec_mons = _record_monitors(float(self.coeffs.dt), dev, self.te)
             zero = type(self.state0)(*[torch.zeros_like(t) if torch.is_tensor(t) else t
                                        for t in self.state0])
             rec = None
@@ -116,12 +128,12 @@ class TMGradRun:
                 if c == 0:       # the initial state as imported (explicit Ez honoured)
                     if rec is not None:
                         rec.close()
-                    rec = Engine2D([(self.state0, self.coeffs, self.source, [rec_mon])],
+                    rec = Engine2D([(self.state0, self.coeffs, self.source, rec_mons)],
                                    phase_mode=self.phase_mode, ring_slots=self.chunk,
                                    graph=False)
                 else:
                     if rec is None:
-                        rec = Engine2D([(zero, self.coeffs, self.source, [rec_mon])],
+                        rec = Engine2D([(zero, self.coeffs, self.source, rec_mons)],
                                        phase_mode=self.phase_mode, ring_slots=self.chunk,
                                        graph=False)
                     rec.restore(0, self.snaps[c])
@@ -129,15 +141,19 @@ class TMGradRun:
                 ring, selems, nslots = C.c_void_p(), C.c_int64(), C.c_int32()
                 L.check(lib.mtb_yee2d_ring(rec.plan, C.byref(ring), C.byref(selems),
                                            C.byref(nslots)), "mtb_yee2d_ring")
-                L.check(lib.mtb_yee2d_adjoint_run(adj, s0, k, ring, selems.value,
-                                                  int(rec.structs[0].ring_full[0]), stream),
-                        "mtb_yee2d_adjoint_run")
+                rf = rec.structs[0].ring_full
+                offs2 = (C.c_int64 * 2)(*((int(rf[1]), int(rf[2])) if self.te
+                                          else (int(rf[0]), int(rf[0]))))
+                L.check(lib.mtb_yee2d_adjoint_run(adj, s0, k, ring, selems.value, offs2,
+                                                  stream), "mtb_yee2d_adjoint_run")
             if rec is not None:
                 rec.close()
         finally:
             lib.mtb_yee2d_adjoint_destroy(adj)
         del keep
-        return eng._unpack(geps, (nx, ny))
+        if self.te:
+            return (eng._unpack(geps[0], (nx - 1, ny)), eng._unpack(geps[1], (nx, ny - 1)))
+        return (eng._unpack(geps[0], (nx, ny)),)
 
     def release(self):
         if getattr(self, "eng", None) is not None:
@@ -146,11 +162,15 @@ class TMGradRun:
         self.snaps = []
 
 
-class _TMRunFn(torch.autograd.Function):
+class _RunFn2D(torch.autograd.Function):
+    """Inputs: the eps tensors the kernels read (TM eps_inf; TE eps_x, eps_y) and
+    the runner; outputs: the final state's tensors and the accumulators."""
+
     @staticmethod
-    def forward(ctx, eps_inf, runner):
+    def forward(ctx, runner, *eps):
         outs = runner.forward()
         ctx.runner = runner
+        ctx.dtypes = [e.dtype for e in eps]
         return tuple(outs)
 
     @staticmethod
@@ -160,22 +180,28 @@ class _TMRunFn(torch.autograd.Function):
             g_eps = runner.backward(grads)
         finally:
             runner.release()
-        return g_eps.to(dtype=runner.coeffs.eps_inf.dtype), None
+        return (None,) + tuple(gr.to(dtype=dt) for gr, dt in zip(g_eps, ctx.dtypes))
 
 
-def run_tm_grad(state, coeffs, n_steps, *, source=None, monitors=(), checkpoint_every=0,
-                phase_mode="exact"):
-    """Differentiable run_tm: returns (state, accs) connected to coeffs.eps_inf."""
+def run_grad(state, coeffs, n_steps, *, source=None, monitors=(), checkpoint_every=0,
+             phase_mode="exact"):
+    """Differentiable run_tm / run_te: returns (state, accs) connected to the
+    coefficients' eps tensors (TM eps_inf; TE eps_x, eps_y)."""
+    te = hasattr(state, "Hz")
+    eps_names = ("eps_x", "eps_y") if te else ("eps_inf",)
     for f in getattr(coeffs, "_fields", ()):
         t = getattr(coeffs, f)
-        if torch.is_tensor(t) and t.requires_grad and f != "eps_inf":
+        if torch.is_tensor(t) and t.requires_grad and f not in eps_names and f != "eps_inf":
             raise L.MtbUnsupported(f"gradients with respect to coeffs.{f} on the B200 path")
     for t in state:
         if torch.is_tensor(t) and t.requires_grad:
             raise L.MtbUnsupported("gradients with respect to the initial state on the B200 path")
     chunk = checkpoint_every if 0 < checkpoint_every <= 64 else 32
-    runner = TMGradRun(state, coeffs, n_steps, source, monitors, chunk, phase_mode)
-    outs = _TMRunFn.apply(coeffs.eps_inf, runner)
-    ns = len(STATE_TM)
-    st = runner.out_state._replace(**dict(zip(STATE_TM, outs[:ns])))
+    runner = GradRun2D(state, coeffs, n_steps, source, monitors, chunk, phase_mode)
+    outs = _RunFn2D.apply(runner, *[getattr(coeffs, f) for f in eps_names])
+    ns = len(runner.names)
+    st = runner.out_state._replace(**dict(zip(runner.names, outs[:ns])))
     return st, list(outs[ns:])
+
+
+run_tm_grad = run_grad

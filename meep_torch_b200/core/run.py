@@ -7,7 +7,6 @@ DFT contraction per ring of steps, instead of ~30 torch ops per step.
 """
 import torch
 
-from .._lib import MtbUnsupported
 from ..engine2d import Engine2D
 
 
@@ -28,20 +27,20 @@ def _run_chunk(step_fn, state, coeffs, step0: int, k: int, source, monitors,
 def _make_runner(kind):
     def run(state, coeffs, n_steps: int, *, source=None, monitors=(), checkpoint_every: int = 0,
             phase_mode: str = "exact"):
-        """core/run.py:44-122. When coeffs.eps_inf requires grad (and grad mode
-        is on) the TM run is differentiable through the library's adjoint
-        kernels, checkpointed every ``checkpoint_every`` steps (<= 64; the
-        default 32); otherwise checkpoint_every has no effect on a forward run."""
+        """core/run.py:44-122. When the eps the kernels read requires grad (TM
+        coeffs.eps_inf; TE coeffs.eps_x / eps_y, e.g. built from an eps_inf that
+        requires grad) and grad mode is on, the run is differentiable through the
+        library's adjoint kernels, checkpointed every ``checkpoint_every`` steps
+        (<= 64; the default 32); otherwise checkpoint_every has no effect."""
         monitors = list(monitors)
         if n_steps <= 0:
             return state, [None] * len(monitors)
-        eps = getattr(coeffs, "eps_inf", None)
-        if torch.is_grad_enabled() and torch.is_tensor(eps) and eps.requires_grad:
-            if kind != "tm":
-                raise MtbUnsupported("gradients: TE runs are not on the B200 adjoint path")
-            from ..adjoint2d import run_tm_grad
-            return run_tm_grad(state, coeffs, n_steps, source=source, monitors=monitors,
-                               checkpoint_every=checkpoint_every, phase_mode=phase_mode)
+        eps = [getattr(coeffs, f, None) for f in (("eps_x", "eps_y") if kind == "te"
+                                                 else ("eps_inf",))]
+        if torch.is_grad_enabled() and any(torch.is_tensor(e) and e.requires_grad for e in eps):
+            from ..adjoint2d import run_grad
+            return run_grad(state, coeffs, n_steps, source=source, monitors=monitors,
+                            checkpoint_every=checkpoint_every, phase_mode=phase_mode)
         state, acc = _run_chunk(None, state, coeffs, 0, n_steps, source, monitors,
                                 phase_mode=phase_mode)
         return state, acc

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__
     ldv(B.g_psi[3] + g, gp3);
     ldv(rec + g, ez);
     ldv(S.inv_eps_a + g, ie);
-    ldv(B.g_eps + g, ge);
+    ldv(B.g_eps[0] + g, ge);
     inject(S, MTB_C2_MAIN, i, jb, g, radj, gez);
     const bool rowin = i >= 1 && i <= nx - 2;
     float bex = 1.f, aex = 0.f;
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__
     stv(B.g_psi[3] + g, gp3);
     stv(B.tmp[0] + g, t1);
     stv(B.tmp[1] + g, t2);
-    stv(B.g_eps + g, ge);
+    stv(B.g_eps[0] + g, ge);
 }
 
 __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__ mtb_yee2d_struct S,
@@ -191,6 +191,155 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant_
     stv(B.g[0] + g, gez);
 }
 
+// ------------------------------------------------------------------ TE
+// Reverse of TE step t (core/stepper_te.py:178-190: D from Hz(n), E = D / eps,
+// Hz from E(n+1/2)), state_{t+1} = (Hz_{t+1}, E/D_{t+1/2}):
+//   k_adj_te_h   (Hz nodes) samples of Hz_{t+1} into gHz; Hz -= dt ((dEy/dx + psi2')
+//                - (dEx/dy + psi3')): g_psi2, g_psi3 and the adjoints of the two E
+//                differences (tmp0 dEy/dx, tmp1 dEx/dy); gHz passes through.
+//   k_adj_te_e   (E nodes) samples of Ex, Ey into gEx, gEy; transposed differences of
+//                tmp0 / tmp1; E = D / eps: gD += gE / eps, g_eps -= gE E / eps (E of the
+//                step from the record); D += dt (dHz/dy + psi0'), D -= dt (dHz/dx + psi1'):
+//                g_psi0, g_psi1 and the adjoints of the two Hz differences (tmp2 at Dx
+//                nodes, tmp3 at Dy nodes); gEx = gEy = 0 (E is recomputed every step).
+//   k_adj_te_hz  (Hz nodes) gHz += transposed differences of tmp2 / tmp3.
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_h(const __grid_constant__ mtb_yee2d_struct S,
+                                                         const __grid_constant__ mtb_adj2d_buffers B,
+                                                         const float *__restrict__ radj) {
+    const int i = blockIdx.y * AROWS + threadIdx.y;
+    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    if (i >= nx || jb >= P) return;
+    const uint32_t g = (uint32_t)i * P + jb;
+    const float dt = S.dt;
+    float ghz[4], gp2[4], gp3[4];
+    ldv(B.g[0] + g, ghz);
+    ldv(B.g_psi[2] + g, gp2);
+    ldv(B.g_psi[3] + g, gp3);
+    inject(S, MTB_C2_MAIN, i, jb, g, radj, ghz);
+    const bool vrow = i <= nx - 2;
+    float hxb = 1.f, hxa = 0.f;
+    if (vrow) { hxb = S.hx_b[i]; hxa = S.hx_a[i]; }
+    float u0[4], u1[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        const bool v = vrow && j <= ny - 2;
+        const float hyb = v ? S.hy_b[j] : 1.f, hya = v ? S.hy_a[j] : 0.f;
+        const float c2 = -dt * ghz[q], c3 = dt * ghz[q];
+        const float g2 = gp2[q] + c2, g3 = gp3[q] + c3;
+        u0[q] = v ? c2 + hxa * g2 : 0.f;                  // dEy/dx
+        u1[q] = v ? c3 + hya * g3 : 0.f;                  // dEx/dy
+        gp2[q] = v ? hxb * g2 : gp2[q];
+        gp3[q] = v ? hyb * g3 : gp3[q];
+    }
+    stv(B.g[0] + g, ghz);
+    stv(B.g_psi[2] + g, gp2);
+    stv(B.g_psi[3] + g, gp3);
+    stv(B.tmp[0] + g, u0);
+    stv(B.tmp[1] + g, u1);
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_e(const __grid_constant__ mtb_yee2d_struct S,
+                                                         const __grid_constant__ mtb_adj2d_buffers B,
+                                                         const float *__restrict__ radj,
+                                                         const float *__restrict__ rex,
+                                                         const float *__restrict__ rey) {
+    const int i = blockIdx.y * AROWS + threadIdx.y;
+    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    if (i >= nx || jb >= P) return;
+    const uint32_t g = (uint32_t)i * P + jb;
+    const float dt = S.dt, rdx = 1.0f / S.dx;
+    float gex[4], gey[4], gdx[4], gdy[4], gp0[4], gp1[4], ex[4], ey[4], ix[4], iy[4];
+    float u0[4], u0p[4], u1[4], gex_e[4], gey_e[4];
+    ldv(B.g[1] + g, gex);
+    ldv(B.g[2] + g, gey);
+    ldv(B.g[3] + g, gdx);
+    ldv(B.g[4] + g, gdy);
+    ldv(B.g_psi[0] + g, gp0);
+    ldv(B.g_psi[1] + g, gp1);
+    ldv(rex + g, ex);
+    ldv(rey + g, ey);
+    ldv(S.inv_eps_a + g, ix);
+    ldv(S.inv_eps_b + g, iy);
+    ldv(B.g_eps[0] + g, gex_e);
+    ldv(B.g_eps[1] + g, gey_e);
+    ldv(B.tmp[0] + g, u0);
+    ldv(B.tmp[1] + g, u1);
+    if (i >= 1) ldv(B.tmp[0] + g - P, u0p);
+    else u0p[0] = u0p[1] = u0p[2] = u0p[3] = 0.f;
+    const float u1l = (jb >= 1) ? B.tmp[1][g - 1] : 0.f;
+    inject(S, MTB_C2_X, i, jb, g, radj, gex);
+    inject(S, MTB_C2_Y, i, jb, g, radj, gey);
+    const bool xrow = i <= nx - 2, yrow = i >= 1 && i <= nx - 2;
+    float exb = 1.f, exa = 0.f;
+    if (yrow) { exb = S.ex_b[i]; exa = S.ex_a[i]; }
+    float t2[4], t3[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        // Hz used dEx/dy = (Ex(j+1) - Ex(j)) and dEy/dx = (Ey(i+1) - Ey(i))
+        const float u1m = (q == 0) ? u1l : u1[q - 1];
+        const float gX = gex[q] + (u1m - u1[q]) * rdx;
+        const float gY = gey[q] + (u0p[q] - u0[q]) * rdx;
+        // E = D / eps (Ex on rows <= nx-2 only)
+        const float gdX = gdx[q] + (xrow ? gX * ix[q] : 0.f);
+        const float gdY = gdy[q] + gY * iy[q];
+        gex_e[q] -= xrow ? gX * ex[q] * ix[q] : 0.f;
+        gey_e[q] -= gY * ey[q] * iy[q];
+        // Dx += dt (d + psi0'): valid i <= nx-2, 1 <= j <= ny-2
+        const bool vx = xrow && j >= 1 && j <= ny - 2;
+        const float eyb = vx ? S.ey_b[j] : 1.f, eya = vx ? S.ey_a[j] : 0.f;
+        const float c0 = dt * gdX, g0 = gp0[q] + c0;
+        t2[q] = vx ? c0 + eya * g0 : 0.f;
+        gp0[q] = vx ? eyb * g0 : gp0[q];
+        // Dy -= dt (d + psi1'): valid 1 <= i <= nx-2, j <= ny-2
+        const bool vy = yrow && j <= ny - 2;
+        const float c1 = -dt * gdY, g1 = gp1[q] + c1;
+        t3[q] = vy ? c1 + exa * g1 : 0.f;
+        gp1[q] = vy ? exb * g1 : gp1[q];
+        gdx[q] = gdX;
+        gdy[q] = gdY;
+        gex[q] = 0.f;
+        gey[q] = 0.f;
+    }
+    stv(B.g[1] + g, gex);
+    stv(B.g[2] + g, gey);
+    stv(B.g[3] + g, gdx);
+    stv(B.g[4] + g, gdy);
+    stv(B.g_psi[0] + g, gp0);
+    stv(B.g_psi[1] + g, gp1);
+    stv(B.g_eps[0] + g, gex_e);
+    stv(B.g_eps[1] + g, gey_e);
+    stv(B.tmp[2] + g, t2);
+    stv(B.tmp[3] + g, t3);
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_hz(const __grid_constant__ mtb_yee2d_struct S,
+                                                          const __grid_constant__ mtb_adj2d_buffers B) {
+    const int i = blockIdx.y * AROWS + threadIdx.y;
+    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    if (i >= nx || jb >= P) return;
+    const uint32_t g = (uint32_t)i * P + jb;
+    const float rdx = 1.0f / S.dx;
+    float ghz[4], t2[4], t3[4], t3n[4];
+    ldv(B.g[0] + g, ghz);
+    ldv(B.tmp[2] + g, t2);
+    ldv(B.tmp[3] + g, t3);
+    if (i + 1 < nx) ldv(B.tmp[3] + g + P, t3n);
+    else t3n[0] = t3n[1] = t3n[2] = t3n[3] = 0.f;
+    const float t2r = (jb + 4 < P) ? B.tmp[2][g + 4] : 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float t2n = (q < 3) ? t2[q + 1] : t2r;
+        const bool v = i <= nx - 2 && jb + q <= ny - 2;
+        ghz[q] = v ? ghz[q] + (t2[q] - t2n) * rdx + (t3[q] - t3n[q]) * rdx : 0.f;
+    }
+    stv(B.g[0] + g, ghz);
+}
+
 }  // namespace mtb
 
 using namespace mtb;
@@ -205,13 +354,13 @@ struct mtb_yee2d_adjoint {
     cudaStream_t cap = nullptr;
     cudaGraphExec_t gexec = nullptr;
     const float *g_rec = nullptr;
-    int64_t g_rec_slot = -1, g_rec_off = -1, gkern = 0;
+    int64_t g_rec_slot = -1, g_rec_off[2] = {-1, -1}, gkern = 0;
 };
 
 // The device work of one chunk of k reverse steps on `st` (after the phases
 // of its steps are uploaded).
 static int adjoint_chunk(mtb_yee2d_adjoint *p, int k, const float *rec, int64_t rec_slot_elems,
-                         int64_t rec_offset, cudaStream_t st) {
+                         const int64_t *rec_offset, cudaStream_t st) {
     int rc;
     if (p->dft.n_regions > 0) {
         if ((rc = p->dft.expand(0, k, st))) return rc;
@@ -225,13 +374,22 @@ static int adjoint_chunk(mtb_yee2d_adjoint *p, int k, const float *rec, int64_t 
     const dim3 grid((S.pitch / 4 + 31) / 32, (S.nx + AROWS - 1) / AROWS);
     for (int q = k - 1; q >= 0; --q) {
         const float *radj = p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems;
-        const float *rq = rec + (size_t)q * rec_slot_elems + rec_offset;
-        k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq);
-        MTB_CHECK_LAUNCH();
-        k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
-        MTB_CHECK_LAUNCH();
-        k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
-        MTB_CHECK_LAUNCH();
+        const float *rq = rec + (size_t)q * rec_slot_elems;
+        if (S.pol == MTB_TM) {
+            k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0]);
+            MTB_CHECK_LAUNCH();
+            k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
+            MTB_CHECK_LAUNCH();
+            k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
+            MTB_CHECK_LAUNCH();
+        } else {
+            k_adj_te_h<<<grid, blk, 0, st>>>(S, p->b, radj);
+            MTB_CHECK_LAUNCH();
+            k_adj_te_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0], rq + rec_offset[1]);
+            MTB_CHECK_LAUNCH();
+            k_adj_te_hz<<<grid, blk, 0, st>>>(S, p->b);
+            MTB_CHECK_LAUNCH();
+        }
         p->last_launches += 3;
     }
     return MTB_OK;
@@ -247,18 +405,20 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     if (!out || !s || !bufs) return fail(MTB_INVALID_ARG, "null argument");
     *out = nullptr;
     const mtb_yee2d_struct &S = *s;
-    if (S.pol != MTB_TM) return fail(MTB_UNSUPPORTED, "adjoint: TM structures only");
+    if (S.pol != MTB_TM && S.pol != MTB_TE) return fail(MTB_INVALID_ARG, "adjoint: bad pol");
     if (S.y_pmc) return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc)");
     if (S.nx < 3 || S.ny < 3 || S.pitch < S.ny || (S.pitch & 3))
         return fail(MTB_INVALID_ARG, "adjoint: bad grid %d x %d, pitch %d", S.nx, S.ny, S.pitch);
     if ((int64_t)S.nx * S.pitch >= (1LL << 31)) return fail(MTB_UNSUPPORTED, "grid too large");
     if (S.nx > 65535 * AROWS) return fail(MTB_UNSUPPORTED, "adjoint: nx too large");
     auto bad = [](const void *p) { return !p || (reinterpret_cast<uintptr_t>(p) & 15); };
+    const bool te = S.pol == MTB_TE;
     for (int c = 0; c < 4; ++c)
         if (bad(bufs->g[c]) || bad(bufs->g_psi[c]) || bad(bufs->tmp[c]))
             return fail(MTB_INVALID_ARG, "adjoint: null or unaligned buffer");
-    if (bad(bufs->g_eps) || bad(S.inv_eps_a))
-        return fail(MTB_INVALID_ARG, "adjoint: null or unaligned g_eps / inv_eps");
+    if ((te && bad(bufs->g[4])) || bad(bufs->g_eps[0]) || bad(S.inv_eps_a) ||
+        (te && (bad(bufs->g_eps[1]) || bad(S.inv_eps_b))))
+        return fail(MTB_INVALID_ARG, "adjoint: null or unaligned g / g_eps / inv_eps");
     if (!S.hx_b || !S.hx_a || !S.hy_b || !S.hy_a || !S.ex_b || !S.ex_a || !S.ey_b || !S.ey_a)
         return fail(MTB_INVALID_ARG, "adjoint: null CPML profile");
     if (S.n_lines < 0 || (S.n_lines > 0 && !S.lines))
@@ -287,13 +447,16 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
 }
 
 int mtb_yee2d_adjoint_run(mtb_yee2d_adjoint *p, int64_t t0, int32_t k, const float *rec,
-                          int64_t rec_slot_elems, int64_t rec_offset, void *stream) {
+                          int64_t rec_slot_elems, const int64_t *rec_offset_in, void *stream) {
     if (!p) return fail(MTB_INVALID_ARG, "adjoint plan is null");
     p->last_launches = 0;
     if (k <= 0) return MTB_OK;
     if (k > p->dft.slots) return fail(MTB_INVALID_ARG, "k %d > ring slots %d", k, p->dft.slots);
-    if (!rec || (rec_offset & 3) || (rec_slot_elems & 3) ||
-        (reinterpret_cast<uintptr_t>(rec) & 15))
+    if (!rec_offset_in) return fail(MTB_INVALID_ARG, "adjoint: null record offsets");
+    const int64_t rec_offset[2] = {rec_offset_in[0],
+                                   p->s.pol == MTB_TE ? rec_offset_in[1] : rec_offset_in[0]};
+    if (!rec || (rec_offset[0] & 3) || (rec_offset[1] & 3) || rec_offset[0] < 0 ||
+        rec_offset[1] < 0 || (rec_slot_elems & 3) || (reinterpret_cast<uintptr_t>(rec) & 15))
         return fail(MTB_INVALID_ARG, "adjoint: bad forward record");
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
@@ -322,11 +485,12 @@ int mtb_yee2d_adjoint_run(mtb_yee2d_adjoint *p, int64_t t0, int32_t k, const flo
         p->gkern = nk;
         p->g_rec = rec;
         p->g_rec_slot = rec_slot_elems;
-        p->g_rec_off = rec_offset;
+        p->g_rec_off[0] = rec_offset[0];
+        p->g_rec_off[1] = rec_offset[1];
     }
     p->last_launches = 0;
     if (whole && p->gexec && p->g_rec == rec && p->g_rec_slot == rec_slot_elems &&
-        p->g_rec_off == rec_offset) {
+        p->g_rec_off[0] == rec_offset[0] && p->g_rec_off[1] == rec_offset[1]) {
         MTB_CUDA_TRY(cudaGraphLaunch(p->gexec, st));
         count_launch(p->gkern);
         p->last_launches = p->gkern;

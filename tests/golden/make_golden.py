@@ -15,6 +15,7 @@ cases of the hot path through its own public functions:
 * the design chain (``conic_filter``, ``tanh_projection``, ``MaterialGrid``,
   ``DesignRegion``, ``OptimizationProblem``; ``python make_golden.py design``)
 * d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
+  and of ``run_te`` (``make_golden.py grad_te``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -299,7 +300,54 @@ def grad3d_case(prec):
                 grad=_np(e.grad), acc_0=_np(accs[0]), acc_1=_np(accs[1]))
 
 
+def grad_loss_te(st, ad, ax, ay, mx, my, dx):
+    """The loss of the TE gradient fixtures: both flux lines (frequency weights),
+    the energy of the full-grid Hz DFT and of the final fields."""
+    w = torch.tensor([1.0, -0.5, 0.25], dtype=ax.dtype)
+    return 1e6 * ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
+                  + 1e-3 * (ad * ad).sum() + 0.1 * (st.Hz * st.Hz).sum()
+                  + 0.05 * (st.Ex * st.Ex).sum() - 0.02 * (st.Ey * st.Ey).sum())
+
+
+def grad_te_case(prec):
+    """d J / d eps_inf through the reference's autograd of run_te
+    (checkpoint_every, core/run.py:81-120) on the TE case's geometry."""
+    rng = np.random.default_rng(12)
+    nx, ny, dx, npml = 44, 40, 0.05, 8
+    eps = np.ones((nx, ny))
+    eps[:, 16:24] = 12.0
+    eps[26:34, 22:32] = 1.0 + 4.0 * rng.random((8, 10))
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
+    e = torch.tensor(eps, dtype=DT[prec], requires_grad=True)
+    m = build_te_coeffs(g, eps_inf=e, npml=npml)
+    line = LineSource(g, ix=12, j0=14, j1=26, profile=GaussianPulse(0.65, 0.4))
+
+    class _TESrc:                                   # TE binding: mask[:, :-1] -> Dy
+        mask = line.mask[:, :-1]
+        amplitude = staticmethod(line.amplitude)
+
+    src = _TESrc()
+    freqs = [0.55, 0.65, 0.75]
+    dft = DFTFieldsMonitor(g, freqs, component="Hz")
+    monx = FluxMonitorTE(g, freqs, ix=33, lo=10, hi=30)
+    mony = FluxMonitorTEY(g, freqs, iy=30, lo=10, hi=34)
+    n, ce = 180, 60
+    st, (ad, ax, ay) = run_te(init_te_state(g), m, n, source=src, monitors=[dft, monx, mony],
+                              checkpoint_every=ce)
+    J = grad_loss_te(st, ad, ax, ay, monx, mony, dx)
+    J.backward()
+    return dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, checkpoint_every=ce, eps=eps,
+                freqs=np.array(freqs), fcen=0.65, fwidth=0.4, src_ix=12, src_j0=14, src_j1=26,
+                monx=np.array([33, 10, 30]), mony=np.array([30, 10, 34]),
+                J=float(J.detach()), grad=_np(e.grad))
+
+
 def main():
+    if sys.argv[1:] == ["grad_te"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_grad_te_{prec}.npz"),
+                                **grad_te_case(prec))
+        return
     if sys.argv[1:] == ["grad3d"]:
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_grad3d_{prec}.npz"),

@@ -608,3 +608,42 @@ def test_3d_gradient_matches_reference_run_3d_adjoint():
     assert abs(L - float(g32["L"])) <= 1e-4 * abs(float(g32["L"]))
     assert rel_l2(accs[0].cpu().numpy(), g32["acc_0"]) < TOL
     assert e32 < TOL, e32
+
+
+@pytest.mark.parametrize("chunk", [60, 32])
+def test_te_gradient_matches_reference_autograd(chunk):
+    """d J / d eps_inf of a TE run (gradients through eps_x / eps_y to eps_inf) from
+    the adjoint kernels against the reference's autograd through run_te
+    (fixtures: tests/golden/make_golden.py grad_te)."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor, FluxMonitorTE, FluxMonitorTEY
+    from meep_torch_b200.core.run import run_te
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource, TESource
+    from meep_torch_b200.core.stepper_te import init_te_state
+    g32, g64 = load_golden("grad_te_f32"), load_golden("grad_te_f64")
+    nx, ny, dx, npml = int(g32["nx"]), int(g32["ny"]), float(g32["dx"]), int(g32["npml"])
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    e = torch.tensor(g32["eps"], dtype=torch.float32, device=dev(), requires_grad=True)
+    m = build_te_coeffs(grid, eps_inf=e, npml=npml)
+    src = TESource(LineSource(grid, ix=int(g32["src_ix"]), j0=int(g32["src_j0"]),
+                              j1=int(g32["src_j1"]),
+                              profile=GaussianPulse(float(g32["fcen"]), float(g32["fwidth"]))))
+    freqs = [float(f) for f in g32["freqs"]]
+    mx, my = [int(v) for v in g32["monx"]], [int(v) for v in g32["mony"]]
+    dft = DFTFieldsMonitor(grid, freqs, "Hz")
+    monx = FluxMonitorTE(grid, freqs, ix=mx[0], lo=mx[1], hi=mx[2])
+    mony = FluxMonitorTEY(grid, freqs, iy=my[0], lo=my[1], hi=my[2])
+    st, (ad, ax, ay) = run_te(init_te_state(grid), m, int(g32["n_steps"]), source=src,
+                              monitors=[dft, monx, mony], checkpoint_every=chunk)
+    w = torch.tensor([1.0, -0.5, 0.25], dtype=torch.float32, device=dev())
+    J = 1e6 * ((w * monx.flux(ax, dx)).sum() + (w.flip(0) * mony.flux(ay, dx)).sum()
+               + 1e-3 * (ad * ad).sum() + 0.1 * (st.Hz * st.Hz).sum()
+               + 0.05 * (st.Ex * st.Ex).sum() - 0.02 * (st.Ey * st.Ey).sum())
+    J.backward()
+    got = e.grad.cpu().numpy()
+    e32, e64 = rel_l2(got, g32["grad"]), rel_l2(got, g64["grad"])
+    print(f"TE grad chunk {chunk}: rel L2 vs reference f32 {e32:.3e}, vs f64 {e64:.3e}; "
+          f"J {float(J):.6e} vs {float(g32['J']):.6e}")
+    assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
+    assert e32 < TOL, e32

@@ -215,3 +215,43 @@ def test_reference_3d_gradient_matches_oracle_finite_differences():
         fd = (J_of(ep) - J_of(em)) / (2 * h)
         ref = float(g["grad"][i, j, k])
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-12, (i, j, k, fd, ref)
+
+
+def test_reference_te_gradient_matches_oracle_finite_differences():
+    """The golden TE d J / d eps_inf (reference autograd, float64) against central
+    finite differences of the oracle's float64 TE run at two pixels."""
+    g = load_golden("grad_te_f64")
+    nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
+                           int(g["n_steps"]))
+    freqs = [float(f) for f in g["freqs"]]
+    mxi, mxl, mxh = (int(v) for v in g["monx"])
+    myi, myl, myh = (int(v) for v in g["mony"])
+
+    def J_of(eps):
+        c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float64)
+        dt = c["dt"]
+        mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
+                                  int(g["src_j1"]), dtype=np.float64)[:, :-1]
+        prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
+        mons = [lambda s, t: O.dft_sample(s["Hz"], t, dt, freqs, "Hz", np.float64),
+                lambda s, t: O.flux_te_sample(s, t, dt, freqs, mxi, mxl, mxh, np.float64),
+                lambda s, t: O.flux_tey_sample(s, t, dt, freqs, myi, myl, myh, np.float64)]
+        s, (ad, ax, ay) = O.run_2d(O.te_step, O.te_state(c), c, n,
+                                   amp_fn=lambda t: prof(O.src_time(t, dt)), mask=mask,
+                                   monitors=mons)
+        w = np.array([1.0, -0.5, 0.25])
+        fx, fy = O.line_flux(ax, dx, +1.0), O.line_flux(ay, dx, -1.0)
+        return 1e6 * float((w * fx).sum() + (w[::-1] * fy).sum() + 1e-3 * (ad * ad).sum()
+                           + 0.1 * (s["Hz"] ** 2).sum() + 0.05 * (s["Ex"] ** 2).sum()
+                           - 0.02 * (s["Ey"] ** 2).sum())
+
+    eps = g["eps"].astype(np.float64)
+    assert abs(J_of(eps) - float(g["J"])) <= 1e-9 * abs(float(g["J"]))
+    h = 1e-4
+    for (i, j) in [(30, 26), (20, 18)]:
+        ep, em = eps.copy(), eps.copy()
+        ep[i, j] += h
+        em[i, j] -= h
+        fd = (J_of(ep) - J_of(em)) / (2 * h)
+        ref = float(g["grad"][i, j])
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-12, (i, j, fd, ref)
