@@ -682,7 +682,13 @@ def main():
                      "alg_bytes_per_launch": r["bytes_launch"],
                      "launch_ms": step_avg_ms, "launches": r["step_n"],
                      "dft_contract_ms_total": r["dft_ms"], "dft_contract_launches": r["dft_n"],
-                     "step_kernel_share": r["step_ms"] / max(r["ms"], 1e-9)},
+                     "step_kernel_share": r["step_ms"] / max(r["ms"], 1e-9),
+                     # the measured DRAM bytes of a step (ncu, profiles/) over the live step
+                     # time: the raw-bytes rate, beside the algorithmic one above
+                     "achieved_raw": (traffic / (step_avg_ms / 1e3) / 1e9
+                                      if traffic else None),
+                     "frac_raw": (traffic / (step_avg_ms / 1e3) / 1e9 / peak
+                                  if traffic else None)},
         "e2e": {"value": e2e_val, "unit": "Gcell-updates/s", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"]},
         "clocks": r["clocks"],
