@@ -12,10 +12,13 @@ every DFT contribution folded). Metric: Gcell-updates/s = sum(nx*ny) *
 * ``e2e``: the public API from host buffers: pinned eps maps copied in,
   coefficients / sources / monitors / states built on the GPU, the run, and
   the DFT + flux accumulators copied back -- all inside the timed region.
-* ``roofline``: the step kernel (k_yee2d_step), CUDA-event time per launch on
-  the plan's stream over the timed region, against algorithmic bytes per
-  launch (fields + eps + CPML layers; the DFT ring and contraction are
-  reported separately).
+* ``roofline``: the step kernels of one time step (cfg2: k_tile_tm + k_tile_te),
+  CUDA-event time per step on the plan's stream over the timed region, against
+  algorithmic bytes per step (fields + eps + CPML layers; the DFT ring and
+  contraction are reported separately); ``achieved_raw`` / ``frac_raw`` use the
+  measured DRAM bytes (``traffic``) instead.
+* ``--workload cfg1 | cfg3 | cfg4``: the single-structure TM run, the 256^3 3D
+  run and the 600 x 400 gradient problem, on the same line format.
 * ``cpu_baseline``: the oracle (numpy restatement of the reference's TM/TE
   step and monitors) on a bounded sample of the same batch, on the host cores.
 * ``--impl reference``: the same sample through the oracle only (the
