@@ -333,7 +333,15 @@ def run_cfg2(args, rank, world, dev):
 
     lib = _lib.load()
     nsteps = args.run_steps
-    specs = W.cfg2_specs(n=args.structs, seed=2 + 1009 * rank)
+    fixed = args.shard == "fixed"
+    if fixed:       # one batch split across the ranks (LPT on cells): strong scaling
+        from meep_torch_b200.shard import lpt_partition
+        all_specs = W.cfg2_specs(n=args.structs, seed=2)
+        costs = [s["nx"] * s["ny"] for s in all_specs]
+        parts = lpt_partition(costs, world)
+        specs = [all_specs[i] for i in parts[rank]]
+    else:           # every rank its own batch: weak scaling
+        specs = W.cfg2_specs(n=args.structs, seed=2 + 1009 * rank)
     cells = sum(s["nx"] * s["ny"] for s in specs)
     items = [W.cfg2_item(s, dev) for s in specs]
     eng = Engine2D(items, rows_per_warp=args.rows, ring_slots=args.ring, variant=args.variant)
@@ -381,22 +389,30 @@ def run_cfg2(args, rank, world, dev):
     h2d = sum(t.numel() * 4 for t in host_eps)
     d2h = 0
 
-    def e2e_step():
+    def run_share(idx):
+        """Structures idx of this rank's specs: eps in, run, accumulators out."""
         nonlocal d2h
-        dev_eps = [t.to(dev, non_blocking=True) for t in host_eps]
-        its = [W.cfg2_item(s, dev, eps_t=e) for s, e in zip(specs, dev_eps)]
+        dev_eps = [host_eps[i].to(dev, non_blocking=True) for i in idx]
+        its = [W.cfg2_item(specs[i], dev, eps_t=e) for i, e in zip(idx, dev_eps)]
         e = Engine2D(its, rows_per_warp=args.rows, ring_slots=args.ring, variant=args.variant)
         e.run(0, nsteps)
         outs = []
         nb = 0
         for b in range(len(its)):
-            for a in e.accumulators(b):
-                outs.append(a.to("cpu", non_blocking=True))
-                nb += a.numel() * 4
+            outs.append([a.to("cpu", non_blocking=True) for a in e.accumulators(b)])
+            nb += sum(a.numel() * 4 for a in e.accumulators(b))
         torch.cuda.synchronize(dev)
         e.close()
         d2h = nb
         return outs
+
+    def e2e_step():
+        if fixed:   # every structure's accumulators end on rank 0, in batch order
+            from meep_torch_b200.shard import run_sharded
+            local = iter(range(len(specs)))
+            return run_sharded(costs, lambda idx: run_share([next(local) for _ in idx]),
+                               rank=rank, world=world)
+        return run_share(list(range(len(specs))))
 
     e2e_step()                                   # warm
     torch.cuda.synchronize(dev)
@@ -494,6 +510,16 @@ def barrier(world):
         dist.barrier()
 
 
+def allreduce_sum(x, world, dev):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def allreduce_max(x, world, dev):
     if world == 1:
         return x
@@ -522,6 +548,10 @@ def main():
                     help="time steps per run (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--n3", type=int, default=256, help="cfg3 grid side")
+    ap.add_argument("--shard", default="none", choices=["none", "fixed"],
+                    help="cfg2 under torchrun: none = every rank its own batch (weak "
+                         "scaling); fixed = one batch split across the ranks by LPT on "
+                         "cells, accumulators gathered on rank 0 (strong scaling)")
     ap.add_argument("--variant", type=int, default=0,
                     help="kernel variant, 0 library default; 2D: 1 row march, 2 tiles; "
                          "3D: 1 fused x-march, 2 split H / E")
@@ -648,7 +678,8 @@ def main():
     r = {"cfg1": run_cfg1, "cfg2": run_cfg2, "cfg3": run_cfg3}[args.workload](args, rank, world,
                                                                             dev)
     peak, peak_kind = peaks()
-    total_updates = r["cells"] * r["nsteps"] * args.steps * world
+    cells_total = allreduce_sum(r["cells"], world, dev)       # every rank's own cells
+    total_updates = cells_total * r["nsteps"] * args.steps
     value = total_updates / (r["ms"] / 1e3) / 1e9
     step_avg_ms = r["step_ms"] / max(r["step_n"], 1)
     achieved = r["bytes_launch"] / (step_avg_ms / 1e3) / 1e9
@@ -662,7 +693,7 @@ def main():
         eff = args.variant or 2                           # library default: tiles / split
         if tr.get("variant") == eff:
             traffic = tr.get("dram_bytes_per_launch")
-    e2e_val = (r["cells"] * r["nsteps"] * args.steps * world / r["e2e_s"] / 1e9
+    e2e_val = (total_updates / r["e2e_s"] / 1e9
                if r["e2e_s"] == r["e2e_s"] else None)
     kernel = ("k_tile_tm (one step; graph replays, step time = run time / steps)"
               if args.workload == "cfg1" and args.variant != 1 else
@@ -675,9 +706,13 @@ def main():
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "strong" if (args.shard == "fixed" and args.workload == "cfg2") else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(config, parallelism=f"independent batch per rank x{world}",
+        "config": dict(config, parallelism=(
+            f"one batch split across {world} ranks (LPT on cells), accumulators gathered on "
+            "rank 0" if (args.shard == "fixed" and args.workload == "cfg2")
+            else f"independent batch per rank x{world}"),
                        cells_per_rank=r["cells"]),
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
