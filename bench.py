@@ -504,6 +504,98 @@ def run_cfg3(args, rank, world, dev):
     return res
 
 
+def run_cfg3_slabs(args, rank, world, dev):
+    """cfg3 as one 256^3 grid split along x into ``world`` slabs, one per rank: halo
+    planes (Ey, Ez after each E update, Hy, Hz after each H update) travel between
+    neighbours over torch.distributed point-to-point (NCCL), flux accumulators are
+    summed onto rank 0 at the end. Strong scaling."""
+    import torch
+
+    from meep_torch_b200 import _lib
+    from meep_torch_b200 import slab3d as SL
+    from meep_torch_b200 import workloads as W
+    from meep_torch_b200.engine3d import Engine3D
+
+    lib = _lib.load()
+    n = args.n3
+    nsteps = args.run_steps if args.run_steps != 5000 else 2000
+    s, c, src, mons = W.cfg3_setup(dev, n=n)
+    sl = SL.slab_bounds(n, world)[rank]
+    parts = SL.slice_monitors(mons, sl, n, n)
+    eng = Engine3D(SL.slice_state(s, sl), SL.slice_coeffs(c, sl), SL.slice_source(src, sl),
+                   [p.monitor for p in parts if p is not None], own=sl.own_local,
+                   ring_slots=args.ring)
+    del s, c, src
+    torch.cuda.empty_cache()
+    halo = SL.DistHalo(eng, sl) if world > 1 else SL.LocalHalo([eng], [sl])
+    drv = SL.SlabDriver([eng], halo)
+    stream = torch.cuda.current_stream(dev)
+
+    def bench_step():
+        eng.reset()
+        drv.run(0, nsteps)
+
+    for _ in range(args.warmup):
+        bench_step()
+    torch.cuda.synchronize(dev)
+    eng.set_timing(True)
+    barrier(world)
+    n0 = lib.mtb_launch_count()
+    with Clocks(dev.index if dev.index is not None else 0) as clk:
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            bench_step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+    launches = lib.mtb_launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    step_ms, step_n, dft_ms, dft_n = eng.timing()
+    eng.close()
+    own = (sl.x1 - sl.x0) * n * n
+    res = dict(cells=own, nsteps=nsteps, ms=allreduce_max(ms, world, dev), launches=launches,
+               clocks=clk.summary(), step_ms=step_ms, step_n=step_n, dft_ms=dft_ms,
+               dft_n=dft_n, bytes_launch=W.cfg3_bytes_per_step(n) * (sl.x1 - sl.x0) / n,
+               e2e_s=float("nan"), h2d=0, d2h=0)
+    del eng
+    torch.cuda.empty_cache()
+    if args.no_e2e:
+        return res
+    # ---- e2e: host eps through the public API (run_3d_distributed), flux
+    # accumulators summed onto rank 0 and read back there
+    host_eps = torch.from_numpy(W.cfg3_eps(n)).pin_memory()
+    d2h = 0
+
+    def e2e_step():
+        nonlocal d2h
+        e = host_eps.to(dev, non_blocking=True)
+        s_, c_, src_, mons_ = W.cfg3_setup(dev, n=n, eps=e)
+        if world > 1:
+            _, accs = SL.run_3d_distributed(s_, c_, nsteps, source=src_, monitors=mons_,
+                                            rank=rank, world=world, ring_slots=args.ring)
+        else:
+            _, accs = SL.run_3d_slabs(s_, c_, nsteps, source=src_, monitors=mons_, n_slabs=1,
+                                      ring_slots=args.ring)
+        outs = [a.to("cpu", non_blocking=True) for a in accs] if accs is not None else []
+        torch.cuda.synchronize(dev)
+        d2h = sum(a.numel() * 4 for a in outs)
+        return outs
+
+    e2e_step()                                   # warm
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    res.update(e2e_s=allreduce_max(time.perf_counter() - t0, world, dev),
+               h2d=host_eps.numel() * 4, d2h=d2h)
+    return res
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -549,9 +641,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--n3", type=int, default=256, help="cfg3 grid side")
     ap.add_argument("--shard", default="none", choices=["none", "fixed"],
-                    help="cfg2 under torchrun: none = every rank its own batch (weak "
-                         "scaling); fixed = one batch split across the ranks by LPT on "
-                         "cells, accumulators gathered on rank 0 (strong scaling)")
+                    help="under torchrun: none = every rank its own problem (weak "
+                         "scaling); fixed = one problem split across the ranks (strong "
+                         "scaling): cfg2's batch by LPT on cells with the accumulators "
+                         "gathered on rank 0, cfg3's grid into x slabs with halo planes "
+                         "exchanged every half step")
     ap.add_argument("--variant", type=int, default=0,
                     help="kernel variant, 0 library default; 2D: 1 row march, 2 tiles; "
                          "3D: 1 fused x-march, 2 split H / E")
@@ -675,8 +769,9 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    r = {"cfg1": run_cfg1, "cfg2": run_cfg2, "cfg3": run_cfg3}[args.workload](args, rank, world,
-                                                                            dev)
+    slabs3 = args.workload == "cfg3" and args.shard == "fixed"
+    r = {"cfg1": run_cfg1, "cfg2": run_cfg2,
+         "cfg3": run_cfg3_slabs if slabs3 else run_cfg3}[args.workload](args, rank, world, dev)
     peak, peak_kind = peaks()
     cells_total = allreduce_sum(r["cells"], world, dev)       # every rank's own cells
     total_updates = cells_total * r["nsteps"] * args.steps
@@ -707,12 +802,14 @@ def main():
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
-        "scaling": "strong" if (args.shard == "fixed" and args.workload == "cfg2") else "weak",
+        "scaling": "strong" if args.shard == "fixed" else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(config, parallelism=(
             f"one batch split across {world} ranks (LPT on cells), accumulators gathered on "
             "rank 0" if (args.shard == "fixed" and args.workload == "cfg2")
-            else f"independent batch per rank x{world}"),
+            else f"one grid split along x into {world} slabs, halo planes over NCCL "
+            "point-to-point, flux accumulators reduced onto rank 0" if slabs3
+            else f"independent problem per rank x{world}"),
                        cells_per_rank=r["cells"]),
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",

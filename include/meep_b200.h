@@ -349,6 +349,22 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s,
                           mtb_yee3d_plan **out);
 int mtb_yee3d_run(mtb_yee3d_plan *plan, int64_t t0, int32_t k,
                   const double *coef, void *stream);
+/* x-slab decomposition (core/monitors_3d.py:192-210 run_3d split across
+ * ranks along x). The plan holds planes [lo, hi) of a larger grid as its own
+ * nx planes: its first plane is the left neighbour's last plane (a halo)
+ * unless lo == 0, its last the right neighbour's first unless hi == the global
+ * nx. set_slab restricts the updates to the plan's planes [own_lo, own_hi);
+ * the halo planes are the caller's to fill. Split kernels only. */
+int mtb_yee3d_set_slab(mtb_yee3d_plan *plan, int32_t own_lo, int32_t own_hi);
+/* Half steps, so that a caller can exchange halo planes between the H and E
+ * updates: begin stages steps t0 .. t0+k-1 (amplitudes coef[0..k-1] as in
+ * mtb_yee3d_run); then per step half(0) = H(n+1/2) from E(n) (written to
+ * the buffer mtb_yee3d_current() ^ 1) and half(1) = E(n+1), the plane
+ * samples and the ring fold (the buffers flip). Same results as
+ * mtb_yee3d_run of the k steps. */
+int mtb_yee3d_begin(mtb_yee3d_plan *plan, int64_t t0, int32_t k, const double *coef,
+                    void *stream);
+int mtb_yee3d_half(mtb_yee3d_plan *plan, int32_t part, void *stream);
 int32_t mtb_yee3d_current(const mtb_yee3d_plan *plan);
 int64_t mtb_yee3d_last_launches(const mtb_yee3d_plan *plan);
 int mtb_yee3d_set_timing(mtb_yee3d_plan *plan, int32_t enable);

@@ -118,6 +118,9 @@ SIGNATURES = {
                                         C.POINTER(PhaseGroup), C.c_int32, C.c_int64,
                                         C.POINTER(Tuning), C.POINTER(vp)]),
     "mtb_yee3d_run": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double), vp]),
+    "mtb_yee3d_set_slab": (C.c_int, [vp, C.c_int32, C.c_int32]),
+    "mtb_yee3d_begin": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double), vp]),
+    "mtb_yee3d_half": (C.c_int, [vp, C.c_int32, vp]),
     "mtb_yee3d_current": (C.c_int32, [vp]),
     "mtb_yee3d_last_launches": (C.c_int64, [vp]),
     "mtb_yee3d_plan_destroy": (None, [vp]),

@@ -744,6 +744,11 @@ struct mtb_yee3d_plan {
     Band3 band{};
     Split3 sp[2]{};                // split-kernel parameters of parity 0 and 1
     int slab = 0;                  // split kernels: x planes per H / E launch pair
+    int own_lo = 0, own_hi = 0;    // split kernels: x planes this plan updates
+    // chunk staged by mtb_yee3d_begin: k steps from t0, next step c_s, next
+    // half c_half (0 H, 1 E), ring slot c_slot
+    int64_t c_t0 = 0;
+    int c_k = 0, c_s = 0, c_half = 0, c_slot = 0;
     int par = 0;
     int n_planes = 0;
     int64_t n_samples = 0;
@@ -842,6 +847,8 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     // split kernels: rows_per_warp > 0 sets the x planes per launch pair; the
     // default is the whole grid in one pair
     p->slab = (tuning && tuning->rows_per_warp > 0) ? std::min(tuning->rows_per_warp, S.nx) : S.nx;
+    p->own_lo = 0;
+    p->own_hi = S.nx;
     const int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     p->nzw = (S.zpitch + 127) / 128;
     p->smem = sizeof(float) * (size_t)(S.zpitch + 4) * (4 * (TY3 + 2) + 3 * (TY3 + 1));
@@ -933,12 +940,10 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     return MTB_OK;
 }
 
-int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, void *stream) {
-    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
-    if (k < 0) return fail(MTB_INVALID_ARG, "k < 0");
-    p->last_launches = 0;
-    if (k == 0) return MTB_OK;
-    cudaStream_t st = (cudaStream_t)stream;
+}  // extern "C"
+
+// Stage the source amplitudes and DFT phases of steps [t0, t0+k) on `st`.
+static int stage_chunk(mtb_yee3d_plan *p, int64_t t0, int k, const double *coef, cudaStream_t st) {
     int rc;
     void *hp = nullptr;
     if ((rc = p->amp_h.acquire(sizeof(float) * k, &hp))) return rc;
@@ -948,14 +953,74 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
     for (int s = 0; s < k; ++s) ah[s] = coef ? (float)coef[s] : 0.f;
     MTB_CUDA_TRY(cudaMemcpyAsync(p->amp_d.p, ah, sizeof(float) * k, cudaMemcpyHostToDevice, st));
     if ((rc = p->amp_h.queued(st))) return rc;
-    int slot = 0;
+    p->c_t0 = t0;
+    p->c_k = k;
+    p->c_s = 0;
+    p->c_half = 0;
+    p->c_slot = 0;
+    return MTB_OK;
+}
+
+// Split-kernel H (part 0) or E (part 1) update of x planes [i0, i1), step s
+// of the staged chunk.
+static int launch_split(mtb_yee3d_plan *p, int part, int i0, int i1, int s, cudaStream_t st) {
+    if (i1 <= i0) return MTB_OK;
+    const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, i1 - i0);
+    const dim3 block(32, SPLIT_Y);
+    if (part == 0)
+        k_yee3d_h<<<grid, block, 0, st>>>(p->sp[p->par], i0);
+    else
+        k_yee3d_e<<<grid, block, 0, st>>>(p->sp[p->par], p->amp_d.as<float>() + s, i0);
+    MTB_CHECK_LAUNCH();
+    ++p->last_launches;
+    return MTB_OK;
+}
+
+// After the E update of step c_s: flip the buffers, sample the planes into
+// the ring, fold a full ring (or the chunk's last steps) into the accumulators.
+static int finish_step(mtb_yee3d_plan *p, cudaStream_t st) {
+    int rc;
+    p->par ^= 1;
     const bool sampling = p->dft.n_regions > 0 && p->n_samples > 0;
+    if (sampling) {
+        float *ring = p->dft.ring_d.as<float>() + (size_t)p->c_slot * p->dft.slot_elems;
+        const int64_t nb = (p->n_samples + 255) / 256;
+        k_sample3d<<<(unsigned)nb, 256, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(),
+                                                p->pstart_d.as<int64_t>(), p->n_planes, p->par,
+                                                ring);
+        MTB_CHECK_LAUNCH();
+        ++p->last_launches;
+    }
+    const int s = p->c_s;
+    ++p->c_slot;
+    if (p->c_slot == p->dft.slots || s == p->c_k - 1) {
+        if (sampling) {
+            if ((rc = p->dft.contract(s + 1 - p->c_slot, p->c_slot, st, &p->timer))) return rc;
+            ++p->last_launches;
+        }
+        p->c_slot = 0;
+    }
+    ++p->c_s;
+    p->c_half = 0;
+    return p->c_s == p->c_k ? p->timer.collect() : MTB_OK;
+}
+
+extern "C" {
+
+int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (k < 0) return fail(MTB_INVALID_ARG, "k < 0");
+    p->last_launches = 0;
+    if (k == 0) return MTB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if ((rc = stage_chunk(p, t0, k, coef, st))) return rc;
     for (int s = 0; s < k; ++s) {
-        Ctx3D C;
-        C.amp = p->amp_d.as<float>() + s;
-        C.par = p->par;
         if ((rc = p->timer.begin(st, 0))) return rc;
         if (p->variant == 1) {
+            Ctx3D C;
+            C.amp = p->amp_d.as<float>() + s;
+            C.par = p->par;
             switch (p->nzw) {
                 case 1: rc = launch3d<1>(p, C, st); break;
                 case 2: rc = launch3d<2>(p, C, st); break;
@@ -969,38 +1034,52 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
             // H(n+1/2) of its planes in L2. E(slab) needs H of the slab and of
             // the plane before it, which the previous slab wrote.
             const int ns = p->slab;
-            for (int i0 = 0; i0 < p->s.nx; i0 += ns) {
-                const int np_ = std::min(ns, p->s.nx - i0);
-                const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, np_);
-                const dim3 block(32, SPLIT_Y);
-                k_yee3d_h<<<grid, block, 0, st>>>(p->sp[p->par], i0);
-                MTB_CHECK_LAUNCH();
-                k_yee3d_e<<<grid, block, 0, st>>>(p->sp[p->par], C.amp, i0);
-                MTB_CHECK_LAUNCH();
-                p->last_launches += 2;
+            for (int i0 = p->own_lo; i0 < p->own_hi; i0 += ns) {
+                const int i1 = std::min(i0 + ns, p->own_hi);
+                if ((rc = launch_split(p, 0, i0, i1, s, st))) return rc;
+                if ((rc = launch_split(p, 1, i0, i1, s, st))) return rc;
             }
         }
         if ((rc = p->timer.end(st))) return rc;
-        p->par ^= 1;
-        if (sampling) {
-            float *ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;
-            const int64_t nb = (p->n_samples + 255) / 256;
-            k_sample3d<<<(unsigned)nb, 256, 0, st>>>(p->s_d.as<mtb_yee3d_struct>(),
-                                                    p->pstart_d.as<int64_t>(), p->n_planes, p->par,
-                                                    ring);
-            MTB_CHECK_LAUNCH();
-            ++p->last_launches;
-        }
-        ++slot;
-        if (slot == p->dft.slots || s == k - 1) {
-            if (sampling) {
-                if ((rc = p->dft.contract(s + 1 - slot, slot, st, &p->timer))) return rc;
-                ++p->last_launches;
-            }
-            slot = 0;
-        }
+        if ((rc = finish_step(p, st))) return rc;
     }
-    return p->timer.collect();
+    return MTB_OK;
+}
+
+int mtb_yee3d_set_slab(mtb_yee3d_plan *p, int32_t own_lo, int32_t own_hi) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (p->variant != 2) return fail(MTB_UNSUPPORTED, "x slabs need the split kernels");
+    if (own_lo < 0 || own_hi > p->s.nx || own_lo >= own_hi)
+        return fail(MTB_INVALID_ARG, "slab [%d, %d) outside [0, %d)", own_lo, own_hi, p->s.nx);
+    p->own_lo = own_lo;
+    p->own_hi = own_hi;
+    return MTB_OK;
+}
+
+int mtb_yee3d_begin(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (p->variant != 2) return fail(MTB_UNSUPPORTED, "half steps need the split kernels");
+    if (k <= 0) return fail(MTB_INVALID_ARG, "k must be > 0");
+    p->last_launches = 0;
+    return stage_chunk(p, t0, k, coef, (cudaStream_t)stream);
+}
+
+int mtb_yee3d_half(mtb_yee3d_plan *p, int32_t part, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (p->c_s >= p->c_k) return fail(MTB_INVALID_ARG, "no staged step left (mtb_yee3d_begin)");
+    if (part != p->c_half)
+        return fail(MTB_INVALID_ARG, "half %d out of order (expected %d)", part, p->c_half);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (part == 0) {
+        if ((rc = p->timer.begin(st, 0))) return rc;
+        if ((rc = launch_split(p, 0, p->own_lo, p->own_hi, p->c_s, st))) return rc;
+        p->c_half = 1;
+        return MTB_OK;
+    }
+    if ((rc = launch_split(p, 1, p->own_lo, p->own_hi, p->c_s, st))) return rc;
+    if ((rc = p->timer.end(st))) return rc;
+    return finish_step(p, st);
 }
 
 int mtb_yee3d_set_timing(mtb_yee3d_plan *p, int32_t enable) {

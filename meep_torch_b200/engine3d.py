@@ -57,7 +57,7 @@ class Engine3D:
 
     def __init__(self, state, coeffs, source=None, monitors=(), *, point_sign: int = 1,
                  phase_mode: str = "exact", rows_per_seg: int = 0, ring_slots: int = 0,
-                 variant: int = 0, stream=None):
+                 variant: int = 0, stream=None, own=None):
         self.lib = L.load()
         self.stream = stream
         self.keep = []
@@ -169,8 +169,10 @@ class Engine3D:
                 comp = mon.component
                 shp = shapes[comp]
                 a0, a1 = [a for a in range(3) if a != axis]
-                w = (0, shp[a0], 0, shp[a1])
-                rows, cols = shp[a0], shp[a1]
+                w = getattr(mon, "win", None) or (0, shp[a0], 0, shp[a1])
+                _need(0 <= w[0] <= w[1] <= shp[a0] and 0 <= w[2] <= w[3] <= shp[a1],
+                      "DFT plane window")
+                rows, cols = w[1] - w[0], w[3] - w[2]
                 M = rows * cols
                 acc = torch.zeros((nf, 2, rows, cols), dtype=torch.float32, device=self.device)
                 o = add_plane(comp, axis, int(idx), w)
@@ -197,6 +199,10 @@ class Engine3D:
                 "mtb_yee3d_plan_create")
         self.plan = plan
         self.S = S
+        if own is not None:
+            L.check(self.lib.mtb_yee3d_set_slab(plan, int(own[0]), int(own[1])),
+                    "mtb_yee3d_set_slab")
+        self.own = (0, nx) if own is None else (int(own[0]), int(own[1]))
         self.regions, self.n_regions = reg_arr, len(regions)
         self.groups, self.n_groups = grp_arr, len(groups)
         self.ring_elems = ring
@@ -307,6 +313,25 @@ class Engine3D:
             coef = self._coef.ctypes.data_as(C.POINTER(C.c_double))
         L.check(self.lib.mtb_yee3d_run(self.plan, t0, k, coef, self._sptr()), "mtb_yee3d_run")
         self.last_launches = self.lib.mtb_yee3d_last_launches(self.plan)
+
+    def begin(self, t0: int, k: int):
+        """Stage steps t0 .. t0+k-1 for half(); the amplitudes as in run()."""
+        coef = None
+        if self.source is not None:
+            v = coef_table(self.source, "amplitude", t0, k, self._dt)
+            self._coef = np.ascontiguousarray(v, dtype=np.float64)
+            coef = self._coef.ctypes.data_as(C.POINTER(C.c_double))
+        L.check(self.lib.mtb_yee3d_begin(self.plan, t0, k, coef, self._sptr()), "mtb_yee3d_begin")
+
+    def half(self, part: int):
+        """H (part 0) or E (part 1) update of the next staged step."""
+        L.check(self.lib.mtb_yee3d_half(self.plan, int(part), self._sptr()), "mtb_yee3d_half")
+
+    def plane(self, comp: str, i: int, nxt: bool = False):
+        """Box plane i (ny x zpitch, contiguous) of a field: the live buffer, or the
+        other one (where a half(0) put H(n+1/2)) when ``nxt``."""
+        cur = self.current
+        return self.box[comp][cur ^ 1 if nxt else cur][i]
 
     def reset(self):
         """Zero every field, CPML and accumulator buffer (t = 0 again)."""

@@ -5,7 +5,7 @@ the product package. Arrays are numpy; ``dtype`` (float32 or float64) is the
 grid dtype, and every arithmetic step runs in that dtype in the same order as
 the reference so that float32 runs round like the reference's float32 runs.
 
-Scope (what the north-star configs use): PEC or PMC-in-y walls, CPML, scalar
+Scope (what the benchmark workloads use): PEC or PMC-in-y walls, CPML, scalar
 eps, no dispersion / conductivity / nonlinearity / symmetry folds.
 """
 from __future__ import annotations
@@ -397,15 +397,9 @@ def _pad_interior(t, axes):
     return np.pad(t, pad)
 
 
-def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
-    """One 3D leapfrog step, CPML path of core/stepper_3d.py:363-445, then the
-    soft source of :448-482. ``src`` is ("Ez", i, j, k) for a point current
-    (the functional stepper ADDS dt*amp/eps there, :474-480; ``point_sign=-1``
-    gives the lean stepper's subtraction, core/stepper_3d_lean.py:293-296) or
-    ("Ez", mask) for an area current (subtracted, :452-461)."""
+def _ce3(c):
     dx, T = c["dx"], c["dtype"].type
     cp = c["cpml"]
-    d1, d2 = c["d1"], c["d2"]
     X = T(dx)
 
     def ce(F, ax, key, psi):
@@ -413,7 +407,24 @@ def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
         d = _d(F, ax) / X
         p = b * psi + a * d
         return d / k + p, p
+    return ce
 
+
+def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
+    """One 3D leapfrog step, CPML path of core/stepper_3d.py:363-445, then the
+    soft source of :448-482. ``src`` is ("Ez", i, j, k) for a point current
+    (the functional stepper ADDS dt*amp/eps there, :474-480; ``point_sign=-1``
+    gives the lean stepper's subtraction, core/stepper_3d_lean.py:293-296) or
+    ("Ez", mask) for an area current (subtracted, :452-461)."""
+    out = step_3d_h(s, c)
+    out.update(step_3d_e(s, c, out, amp, src, point_sign))
+    return out
+
+
+def step_3d_h(s, c):
+    """H(n+1/2) and the H-side CPML memory of step_3d (core/stepper_3d.py:367-393)."""
+    ce = _ce3(c)
+    d1, d2 = c["d1"], c["d2"]
     out = {}
     ce_y, out["psi_Ez_y"] = ce(s["Ez"], 1, "hy", s["psi_Ez_y"])
     ce_z, out["psi_Ey_z"] = ce(s["Ey"], 2, "hz", s["psi_Ey_z"])
@@ -424,7 +435,18 @@ def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
     ce_x2, out["psi_Ey_x"] = ce(s["Ey"], 0, "hx", s["psi_Ey_x"])
     ce_y2, out["psi_Ex_y"] = ce(s["Ex"], 1, "hy", s["psi_Ex_y"])
     Hz = d1 * s["Hz"] - d2 * (ce_x2 - ce_y2)
+    out.update(Hx=Hx, Hy=Hy, Hz=Hz)
+    return out
 
+
+def step_3d_e(s, c, h, amp=0.0, src=None, point_sign=+1.0):
+    """E(n+1), the E-side CPML memory and the soft source of step_3d
+    (core/stepper_3d.py:395-482) from the state ``s`` and H(n+1/2) in ``h``."""
+    ce = _ce3(c)
+    d1, d2 = c["d1"], c["d2"]
+    T = c["dtype"].type
+    Hx, Hy, Hz = h["Hx"], h["Hy"], h["Hz"]
+    out = {}
     eps = c["eps"]
     eps_x = _avg(eps, 0)
     ch_y, out["psi_Hz_y"] = ce(Hz, 1, "ey", s["psi_Hz_y"])
@@ -441,7 +463,7 @@ def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
     ch_y2, out["psi_Hx_y"] = ce(Hx, 1, "ey", s["psi_Hx_y"])
     curl_z = _pad_interior(ch_x2[:, 1:-1, :] - ch_y2[1:-1, :, :], (0, 1))
     Ez = (d1 * s["Ez"] * eps_z + d2 * curl_z) / eps_z
-    out.update(Ex=Ex, Ey=Ey, Ez=Ez, Hx=Hx, Hy=Hy, Hz=Hz)
+    out.update(Ex=Ex, Ey=Ey, Ez=Ez)
     if src is not None and amp != 0.0:
         comp = src[0]
         epsc = {"Ex": eps_x, "Ey": eps_y, "Ez": eps_z}[comp]

@@ -2,7 +2,7 @@
 meep_torch itself) and with the oracle, through the package's public API and
 therefore the C ABI.
 
-Bar: relative L2 <= 1e-4 against the reference's
+Bar (the parity tolerance): relative L2 <= 1e-4 against the reference's
 float32 run on fields, DFT accumulators and fluxes. The error against the
 reference's float64 run is computed and printed for each case.
 """
@@ -647,3 +647,43 @@ def test_te_gradient_matches_reference_autograd(chunk):
           f"J {float(J):.6e} vs {float(g32['J']):.6e}")
     assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
     assert e32 < TOL, e32
+
+
+@pytest.mark.parametrize("n_slabs", [1, 2, 3])
+@pytest.mark.parametrize("plane_source", [False, True])
+def test_3d_slabs_bitwise_equal_to_whole_grid(n_slabs, plane_source):
+    """One grid split into x slabs (a plan per slab on its owned planes, halo planes
+    copied between the H and E halves) reproduces the whole-grid run bit for bit:
+    fields, CPML memory and the flux / DFT accumulators of planes of every
+    orientation, some crossing slab boundaries. n_slabs = 1 checks the half-step
+    entry points against mtb_yee3d_run."""
+    from meep_torch_b200.core.monitors_3d import (DFTFieldsMonitor3D, FluxMonitor3D,
+                                                  PlaneSource, PointSource3D, run_3d)
+    from meep_torch_b200.core.sources import GaussianPulse
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    from meep_torch_b200.slab3d import run_3d_slabs
+    nx, ny, nz, dx, npml, n = 23, 17, 40, 0.05, 4, 50
+    rng = np.random.default_rng(12)
+    eps = (1.0 + 3.0 * rng.random((nx, ny, nz))).astype(np.float32)
+    c = build_3d_coeffs(nx, ny, nz, dx, eps=torch.from_numpy(eps), npml=npml, device=dev())
+    freqs = [0.8, 1.1, 1.4]
+    prof = GaussianPulse(1.0, 2.0)
+    if plane_source:
+        src = PlaneSource(nx, ny, nz, c.dt, "Ez", 1, 8, prof, lo=3, hi=19, device=dev())
+    else:
+        src = PointSource3D(c.dt, "Ez", 11, 8, 20, prof)
+    mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=8, win=(2, 14, 3, 30)),
+            FluxMonitor3D(c.dt, freqs, normal="x", idx=16, ap=2),
+            FluxMonitor3D(c.dt, freqs, normal="y", idx=10, win=(3, 20, 2, 35)),
+            FluxMonitor3D(c.dt, freqs, normal="z", idx=21, ap=1),
+            DFTFieldsMonitor3D(c.dt, freqs, component="Ez", plane=(2, 17)),
+            DFTFieldsMonitor3D(c.dt, freqs, component="Hy", plane=(0, 12))]
+    init = init_3d_state(nx, ny, nz, npml=npml, device=dev())
+    init = init._replace(**{k: torch.randn(getattr(init, k).shape, device=dev())
+                            for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
+    ref_s, ref_a = run_3d(init, c, n, source=src, monitors=mons)
+    st, accs = run_3d_slabs(init, c, n, source=src, monitors=mons, n_slabs=n_slabs)
+    bad = [k for k, v in ref_s._asdict().items()
+           if v is not None and not torch.equal(v, getattr(st, k))]
+    bad += [f"acc_{q}" for q, (a, b) in enumerate(zip(accs, ref_a)) if not torch.equal(a, b)]
+    assert not bad, bad
