@@ -1299,6 +1299,20 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
     }
     float *ring = C.ring;
     const int pn = par ^ 1;
+    // descriptor fields used after the first global store, held in registers
+    // (the stores could alias the shared descriptor, which would force reloads)
+    const int h2_lo = S.src_h2.row_lo, h2_hi = S.src_h2.row_hi;
+    const int e_lo = S.src_e.row_lo, e_hi = S.src_e.row_hi;
+    float *__restrict__ dzo = S.f_main[pn];
+    float *__restrict__ hxo = S.f_x[pn];
+    float *__restrict__ hyo = S.f_y[pn];
+    float *__restrict__ ps0o = S.psi[0][pn];
+    float *__restrict__ ps3o = S.psi[3][pn];
+    float *__restrict__ rE = S.ring_full[0] >= 0 ? ring + S.ring_full[0] : nullptr;
+    float *__restrict__ rX = S.ring_full[1] >= 0 ? ring + S.ring_full[1] : nullptr;
+    float *__restrict__ rY = S.ring_full[2] >= 0 ? ring + S.ring_full[2] : nullptr;
+    float hylb = 0.f, hyla = 0.f;
+    if (YPSI && byHL) { hylb = __ldg(S.hy_b + jl); hyla = __ldg(S.hy_a + jl); }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int i = ib + r;
@@ -1316,8 +1330,7 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
             hxN[q] = vH[q] ? hn : hx[r][q];
             p0[r][q] = vH[q] ? pv : p0[r][q];
         }
-        if (act && i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
-            apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
+        if (act && i >= h2_lo && i <= h2_hi) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
         if (!act) zero4(hxN);
         float hxm0 = __shfl_up_sync(0xffffffffu, hxN[3], 1);
         if (lane == 0) {
@@ -1325,10 +1338,9 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
             if (hasL) {
                 const float d = (ez[r + 1][0] - ezl[r]) * rdx;
                 float c = d;
-                if (byHL) c = d + (__ldg(S.hy_b + jl) * p0l[r] + __ldg(S.hy_a + jl) * d);
+                if (byHL) c = d + (hylb * p0l[r] + hyla * d);
                 v = hxl[r] - dt * c;
-                if (i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
-                    v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
+                if (i >= h2_lo && i <= h2_hi) v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
             }
             hxm0 = v;
         }
@@ -1345,19 +1357,18 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
             dzN[q] = vD[q] ? dn : dv[r + 1][q];
             p3[r][q] = vD[q] ? q3 : p3[r][q];
         }
-        if (act && i >= S.src_e.row_lo && i <= S.src_e.row_hi)
-            apply_cells(S.src_e, i, C.amp_e, jb, dzN);
+        if (act && i >= e_lo && i <= e_hi) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
 #pragma unroll
         for (int q = 0; q < 4; ++q) ezN[q] = dzN[q] * iv[r + 1][q];
         if (act) {
-            st4(S.f_main[pn] + ro, dzN);
-            st4(S.f_x[pn] + ro, hxN);
-            st4(S.f_y[pn] + ro, hyN[r + 1]);
-            if (YPSI && byH) st4(S.psi[0][pn] + ro, p0[r]);
-            if (YPSI && byE) st4(S.psi[3][pn] + ro, p3[r]);
-            if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, ezN);
-            if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, hxN);
-            if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, hyN[r + 1]);
+            st4(dzo + ro, dzN);
+            st4(hxo + ro, hxN);
+            st4(hyo + ro, hyN[r + 1]);
+            if (YPSI && byH) st4(ps0o + ro, p0[r]);
+            if (YPSI && byE) st4(ps3o + ro, p3[r]);
+            if (rE) st4(rE + ro, ezN);
+            if (rX) st4(rX + ro, hxN);
+            if (rY) st4(rY + ro, hyN[r + 1]);
             if (nl) {
                 sample_row(L, nl, MTB_C2_MAIN, i, jb, true, ezN, ring);
                 sample_row(L, nl, MTB_C2_X, i, jb, true, hxN, ring);
@@ -1509,6 +1520,19 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
     }
     float *ring = C.ring;
     const int pn = par ^ 1;
+    // descriptor fields used after the first global store, held in registers
+    // (the stores could alias the shared descriptor, which would force reloads)
+    const int h1_lo = S.src_h1.row_lo, h1_hi = S.src_h1.row_hi;
+    float *__restrict__ hzo = S.f_main[pn];
+    float *__restrict__ dxo = S.f_x[pn];
+    float *__restrict__ dyo = S.f_y[pn];
+    float *__restrict__ ps0o = S.psi[0][pn];
+    float *__restrict__ ps3o = S.psi[3][pn];
+    float *__restrict__ rZ = S.ring_full[0] >= 0 ? ring + S.ring_full[0] : nullptr;
+    float *__restrict__ rX = S.ring_full[1] >= 0 ? ring + S.ring_full[1] : nullptr;
+    float *__restrict__ rY = S.ring_full[2] >= 0 ? ring + S.ring_full[2] : nullptr;
+    float eyrb = 0.f, eyra = 0.f;
+    if (YPSI && byER) { eyrb = __ldg(S.ey_b + jr); eyra = __ldg(S.ey_a + jr); }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int i = ib + r;
@@ -1534,7 +1558,7 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
             if (updR) {
                 const float d = (hzR[r] - hc[3]) * rdx;
                 float c = d;
-                if (byER) c = d + (__ldg(S.ey_b + jr) * p0r[r] + __ldg(S.ey_a + jr) * d);
+                if (byER) c = d + (eyrb * p0r[r] + eyra * d);
                 v = dxr[r] + dt * c;
             }
             exR = v * ixr[r];
@@ -1561,17 +1585,16 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
             hzN[q] = vZ[q] ? hn : hc[q];
             p3[r][q] = vZ[q] ? q3 : p3[r][q];
         }
-        if (act && i >= S.src_h1.row_lo && i <= S.src_h1.row_hi)
-            apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
+        if (act && i >= h1_lo && i <= h1_hi) apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
         if (act) {
-            st4(S.f_main[pn] + ro, hzN);
-            st4(S.f_x[pn] + ro, dxN);
-            st4(S.f_y[pn] + ro, dyN[r]);
-            if (YPSI && byE) st4(S.psi[0][pn] + ro, p0[r]);
-            if (YPSI && byH) st4(S.psi[3][pn] + ro, p3[r]);
-            if (S.ring_full[0] >= 0) st4(ring + S.ring_full[0] + ro, hzN);
-            if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, ex);
-            if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, eyo);
+            st4(hzo + ro, hzN);
+            st4(dxo + ro, dxN);
+            st4(dyo + ro, dyN[r]);
+            if (YPSI && byE) st4(ps0o + ro, p0[r]);
+            if (YPSI && byH) st4(ps3o + ro, p3[r]);
+            if (rZ) st4(rZ + ro, hzN);
+            if (rX) st4(rX + ro, ex);
+            if (rY) st4(rY + ro, eyo);
             if (nl) {
                 sample_row(L, nl, MTB_C2_MAIN, i, jb, true, hzN, ring);
                 sample_row(L, nl, MTB_C2_X, i, jb, true, ex, ring);
