@@ -1290,9 +1290,7 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
         const int row = ib - 1 + k;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float d = (ez[k + 1][q] - ez[k][q]) * rdx;
-            const float pv = 1.f * 0.f + 0.f * d;
-            hyN[k][q] = hy[k][q] + dt * (d + pv);
+            hyN[k][q] = hy[k][q] + dt * ((ez[k + 1][q] - ez[k][q]) * rdx);
         }
         if (act && row >= S.src_h1.row_lo && row <= S.src_h1.row_hi)
             apply_cells(S.src_h1, row, C.amp_h, jb, hyN[k]);
@@ -1325,10 +1323,15 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
         for (int q = 0; q < 4; ++q) {
             const float er = (q < 3) ? ez[r + 1][q + 1] : ezR;
             const float d = (er - ez[r + 1][q]) * rdx;
-            const float pv = hyb[q] * p0[r][q] + hya[q] * d;
-            const float hn = hx[r][q] - dt * (d + pv);
+            float hn;
+            if (YPSI) {
+                const float pv = hyb[q] * p0[r][q] + hya[q] * d;
+                hn = hx[r][q] - dt * (d + pv);
+                p0[r][q] = vH[q] ? pv : p0[r][q];
+            } else {
+                hn = hx[r][q] - dt * d;
+            }
             hxN[q] = vH[q] ? hn : hx[r][q];
-            p0[r][q] = vH[q] ? pv : p0[r][q];
         }
         if (act && i >= h2_lo && i <= h2_hi) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
         if (!act) zero4(hxN);
@@ -1351,11 +1354,15 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
             const float hxm = (q == 0) ? hxm0 : hxN[q - 1];
             const float dhy = (hyN[r + 1][q] - hyN[r][q]) * rdx;
             const float dhx = (hxN[q] - hxm) * rdx;
-            const float q2 = 1.f * 0.f + 0.f * dhy;
-            const float q3 = eyb[q] * p3[r][q] + eya[q] * dhx;
-            const float dn = dv[r + 1][q] + dt * ((dhy + q2) - (dhx + q3));
+            float dn;
+            if (YPSI) {
+                const float q3 = eyb[q] * p3[r][q] + eya[q] * dhx;
+                dn = dv[r + 1][q] + dt * (dhy - (dhx + q3));
+                p3[r][q] = vD[q] ? q3 : p3[r][q];
+            } else {
+                dn = dv[r + 1][q] + dt * (dhy - dhx);
+            }
             dzN[q] = vD[q] ? dn : dv[r + 1][q];
-            p3[r][q] = vD[q] ? q3 : p3[r][q];
         }
         if (act && i >= e_lo && i <= e_hi) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
 #pragma unroll
@@ -1506,15 +1513,18 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
             if (oh) { hyb[q] = __ldg(S.hy_b + j); hya[q] = __ldg(S.hy_a + j); }
         }
     }
-    // Dy / Ey(n+1/2) rows ib .. ib+R (te_dy with the x-CPML terms b psi + a d = 0)
+    // Dy / Ey(n+1/2) rows ib .. ib+R (te_dy outside the x layers)
     float ey[R + 1][4], dyN[R + 1][4];
 #pragma unroll
     for (int k = 0; k < R + 1; ++k) {
         const int row = ib + k;
-        float ps[4];
-        zero4(ps);
-        te_dy(S, row, true, act, jb, 1.f, 0.f, dt, rdx, hz[k], hz[k + 1], dy[k], ps, dyN[k],
-              C.amp_e);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float dn = dy[k][q] - dt * ((hz[k + 1][q] - hz[k][q]) * rdx);
+            dyN[k][q] = vZ[q] ? dn : dy[k][q];
+        }
+        if (act && row >= S.src_e.row_lo && row <= S.src_e.row_hi)
+            apply_cells(S.src_e, row, C.amp_e, jb, dyN[k]);
 #pragma unroll
         for (int q = 0; q < 4; ++q) ey[k][q] = dyN[k][q] * iy[k][q];
     }
@@ -1546,10 +1556,15 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
         for (int q = 0; q < 4; ++q) {
             const float hm = (q == 0) ? hm0 : hc[q - 1];
             const float d = (hc[q] - hm) * rdx;
-            const float pv = eyb[q] * p0[r][q] + eya[q] * d;
-            const float dn = dx[r][q] + dt * (d + pv);
+            float dn;
+            if (YPSI) {
+                const float pv = eyb[q] * p0[r][q] + eya[q] * d;
+                dn = dx[r][q] + dt * (d + pv);
+                p0[r][q] = vX[q] ? pv : p0[r][q];
+            } else {
+                dn = dx[r][q] + dt * d;
+            }
             dxN[q] = vX[q] ? dn : dx[r][q];
-            p0[r][q] = vX[q] ? pv : p0[r][q];
             ex[q] = dxN[q] * ix[r][q];
         }
         float exR = 0.f;
@@ -1579,11 +1594,15 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
             const float exn = (q < 3) ? ex[q + 1] : exr;
             const float dey = (eyn[q] - eyo[q]) * rdx;
             const float dex = (exn - ex[q]) * rdx;
-            const float q2 = 1.f * 0.f + 0.f * dey;
-            const float q3 = hyb[q] * p3[r][q] + hya[q] * dex;
-            const float hn = hc[q] - dt * ((dey + q2) - (dex + q3));
+            float hn;
+            if (YPSI) {
+                const float q3 = hyb[q] * p3[r][q] + hya[q] * dex;
+                hn = hc[q] - dt * (dey - (dex + q3));
+                p3[r][q] = vZ[q] ? q3 : p3[r][q];
+            } else {
+                hn = hc[q] - dt * (dey - dex);
+            }
             hzN[q] = vZ[q] ? hn : hc[q];
-            p3[r][q] = vZ[q] ? q3 : p3[r][q];
         }
         if (act && i >= h1_lo && i <= h1_hi) apply_cells(S.src_h1, i, C.amp_h, jb, hzN);
         if (act) {
