@@ -1210,7 +1210,9 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
     const float *__restrict__ Hx = S.f_x[par];
     const float *__restrict__ Hy = S.f_y[par];
     const float *__restrict__ ie = S.inv_eps_a;
-    const uint32_t o0 = (uint32_t)ib * P + jb;          // own row 0
+    // lanes past the row end (last strip) read the row's last float4 instead:
+    // their results are never stored and feed only masked neighbour cells
+    const uint32_t o0 = (uint32_t)ib * P + (act ? jb : P - 4);   // own row 0
     const uint32_t om = o0 - P;                         // row ib-1 (ib >= 1)
     const int jl = jb - 1;
     const bool hasL = lane == 0 && jl >= 0 && jl <= ny - 2;
@@ -1224,24 +1226,20 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
     float ezl[R], ezr[R], hxl[R], p0l[R];
     float p0[R][4], p3[R][4];
 #pragma unroll
-    for (int k = 0; k < R + 2; ++k) { zero4(dv[k]); zero4(iv[k]); }
-#pragma unroll
     for (int r = 0; r < R; ++r) {
-        zero4(hx[r]); zero4(p0[r]); zero4(p3[r]);
+        zero4(p0[r]); zero4(p3[r]);
         ezl[r] = ezr[r] = hxl[r] = p0l[r] = 0.f;
     }
 #pragma unroll
-    for (int k = 0; k < R + 1; ++k) zero4(hy[k]);
+    for (int k = 0; k < R + 2; ++k) {
+        ld4(Dz + om + k * P, dv[k]);
+        ld4(ie + om + k * P, iv[k]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) ld4(Hx + o0 + r * P, hx[r]);
+#pragma unroll
+    for (int k = 0; k < R + 1; ++k) ld4(Hy + om + k * P, hy[k]);
     if (act) {
-#pragma unroll
-        for (int k = 0; k < R + 2; ++k) {
-            ld4(Dz + om + k * P, dv[k]);
-            ld4(ie + om + k * P, iv[k]);
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r) ld4(Hx + o0 + r * P, hx[r]);
-#pragma unroll
-        for (int k = 0; k < R + 1; ++k) ld4(Hy + om + k * P, hy[k]);
         if (lane == 0 && jl >= 0) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -1334,7 +1332,6 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
             hxN[q] = vH[q] ? hn : hx[r][q];
         }
         if (act && i >= h2_lo && i <= h2_hi) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
-        if (!act) zero4(hxN);
         float hxm0 = __shfl_up_sync(0xffffffffu, hxN[3], 1);
         if (lane == 0) {
             float v = 0.f;
@@ -1442,7 +1439,9 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
     const float *__restrict__ Dy = S.f_y[par];
     const float *__restrict__ iex = S.inv_eps_a;
     const float *__restrict__ iey = S.inv_eps_b;
-    const uint32_t o0 = (uint32_t)ib * P + jb;
+    // lanes past the row end (last strip) read the row's last float4 instead:
+    // their results are never stored and feed only masked neighbour cells
+    const uint32_t o0 = (uint32_t)ib * P + (act ? jb : P - 4);
     const uint32_t om = o0 - P;                         // row ib-1 (ib >= 1)
     const int jr = jb + 4;
     const bool hasR = lane == 31 && jr <= ny - 1;
@@ -1457,27 +1456,23 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
     float hzL[R], hzR[R], dxr[R], ixr[R], p0r[R];
     float p0[R][4], p3[R][4];
 #pragma unroll
-    for (int k = 0; k < R + 2; ++k) zero4(hz[k]);
-#pragma unroll
-    for (int k = 0; k < R + 1; ++k) { zero4(dy[k]); zero4(iy[k]); }
-#pragma unroll
     for (int r = 0; r < R; ++r) {
-        zero4(dx[r]); zero4(ix[r]); zero4(p0[r]); zero4(p3[r]);
+        zero4(p0[r]); zero4(p3[r]);
         hzL[r] = hzR[r] = dxr[r] = ixr[r] = p0r[r] = 0.f;
     }
+#pragma unroll
+    for (int k = 0; k < R + 2; ++k) ld4(Hz + om + k * P, hz[k]);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        ld4(Dx + o0 + r * P, dx[r]);
+        ld4(iex + o0 + r * P, ix[r]);
+    }
+#pragma unroll
+    for (int k = 0; k < R + 1; ++k) {
+        ld4(Dy + o0 + k * P, dy[k]);
+        ld4(iey + o0 + k * P, iy[k]);
+    }
     if (act) {
-#pragma unroll
-        for (int k = 0; k < R + 2; ++k) ld4(Hz + om + k * P, hz[k]);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            ld4(Dx + o0 + r * P, dx[r]);
-            ld4(iex + o0 + r * P, ix[r]);
-        }
-#pragma unroll
-        for (int k = 0; k < R + 1; ++k) {
-            ld4(Dy + o0 + k * P, dy[k]);
-            ld4(iey + o0 + k * P, iy[k]);
-        }
         if (lane == 0 && jb >= 1) {
 #pragma unroll
             for (int r = 0; r < R; ++r) hzL[r] = Hz[o0 + r * P - 1];
@@ -1578,17 +1573,12 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
             }
             exR = v * ixr[r];
         }
-        if (!act) { zero4(ex); }
         float exr = __shfl_down_sync(0xffffffffu, ex[0], 1);
         if (lane == 31) exr = exR;
         // Hz(n+1) row i
         float hzN[4];
-        float eyo[4], eyn[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            eyo[q] = act ? ey[r][q] : 0.f;
-            eyn[q] = act ? ey[r + 1][q] : 0.f;
-        }
+        const float (&eyo)[4] = ey[r];
+        const float (&eyn)[4] = ey[r + 1];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float exn = (q < 3) ? ex[q + 1] : exr;
