@@ -143,6 +143,14 @@ typedef struct mtb_yee2d_struct {
                                profile on j < yband[2] or j >= yband[3]   */
     int32_t pad_;
     int64_t ring_full[3];   /* full-grid sample of comp c to ring offset, -1 = off */
+    /* electric conductivity (core/coeffs.py sigma_d; core/stepper_tm.py:158-163,
+     * core/stepper_te.py D update): null = none. Box arrays at the D
+     * component's position: D' = d1 D + d2 curl H, and the soft current on D
+     * is scaled by d2 instead of dt. TM uses [0] (Dz); TE [0] (Dx), [1] (Dy).
+     * Tile kernels only (variant 2); other variants and the adjoint return
+     * MTB_UNSUPPORTED. */
+    const float *cond_d1[2];
+    const float *cond_d2[2];
 } mtb_yee2d_struct;
 
 /* A DFT phase group: frequencies sharing one table. The plan evaluates

@@ -44,7 +44,8 @@ class Yee2DStruct(C.Structure):
                 ("ex_b", vp), ("ex_a", vp), ("ey_b", vp), ("ey_a", vp),
                 ("src_e", Cells), ("src_h1", Cells), ("src_h2", Cells),
                 ("lines", vp), ("n_lines", C.c_int32), ("xband", C.c_int32 * 4),
-                ("yband", C.c_int32 * 4), ("pad_", C.c_int32), ("ring_full", C.c_int64 * 3)]
+                ("yband", C.c_int32 * 4), ("pad_", C.c_int32), ("ring_full", C.c_int64 * 3),
+                ("cond_d1", vp * 2), ("cond_d2", vp * 2)]
 
 
 class PhaseGroup(C.Structure):

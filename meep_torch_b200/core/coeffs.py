@@ -3,9 +3,10 @@
 
 The NamedTuple field names are the reference's, so either side's objects can
 be handed to either side's run drivers. The builders cover the B200 path's
-feature set -- scalar eps, CPML (kappa = 1), PEC walls or TM PMC-in-y walls;
-the reference's dispersive / conductive / nonlinear / symmetry options raise
-NotImplementedError here (the reference itself still runs them).
+feature set -- scalar eps, CPML (kappa = 1), PEC walls or TM PMC-in-y walls,
+electric conductivity (sigma_d); the reference's dispersive, magnetic-conductive,
+nonlinear and symmetry options raise NotImplementedError here (the reference itself
+still runs them).
 """
 from typing import NamedTuple
 
@@ -120,7 +121,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("poles", "pole_masks", "chi3", "chi2", "sigma_d", "sigma_b", "mu", "m_poles",
+_UNSUPPORTED = ("poles", "pole_masks", "chi3", "chi2", "sigma_b", "mu", "m_poles",
                 "m_pole_masks", "y_mirror", "x_mirror", "y_rot2", "rot4", "eps_tensor",
                 "poles_x", "poles_y", "pole_masks_x", "pole_masks_y", "poles_tensor",
                 "pole_masks_tensor")
@@ -137,10 +138,45 @@ def _reject(kw):
             f"{k}: not implemented on the B200 path (use the reference stepper)")
 
 
-def build_tm_coeffs(grid: Grid, eps_inf=None, npml=0, y_pmc: bool = False, **kw) -> TMCoeffs:
+def _cond_tm(grid: Grid, sigma_d):
+    """Electric conductivity pairs of core/coeffs.py:161-175 with sigma_b = 0 and mu = 1:
+    d1 = (1 - sd dt/2) / (1 + sd dt/2), d2 = dt / (1 + sd dt/2) on Dz, and the inert
+    magnetic pairs h1 = 1, h2 = dt the reference builds alongside them."""
+    if sigma_d is None:
+        return {}
+    dt = grid.dt
+    sd = _as_field(sigma_d, grid, 0.0)
+    sb = _as_field(None, grid, 0.0)
+    mu_ = _as_field(None, grid, 1.0)
+    sbx, mux = 0.5 * (sb[:, :-1] + sb[:, 1:]), 0.5 * (mu_[:, :-1] + mu_[:, 1:])
+    sby, muy = 0.5 * (sb[:-1, :] + sb[1:, :]), 0.5 * (mu_[:-1, :] + mu_[1:, :])
+    return dict(d1=(1 - sd * dt / 2) / (1 + sd * dt / 2), d2=dt / (1 + sd * dt / 2),
+                h1x=(1 - sbx * dt / 2) / (1 + sbx * dt / 2), h2x=dt / (mux * (1 + sbx * dt / 2)),
+                h1y=(1 - sby * dt / 2) / (1 + sby * dt / 2), h2y=dt / (muy * (1 + sby * dt / 2)))
+
+
+def _cond_te(grid: Grid, sigma_d):
+    """TE pairs of core/coeffs.py:401-415: sigma_d averaged to Ex / Ey, inert Hz pair."""
+    if sigma_d is None:
+        return {}
+    dt = grid.dt
+    sd = _as_field(sigma_d, grid, 0.0)
+    sb = _as_field(None, grid, 0.0)
+    mu_ = _as_field(None, grid, 1.0)
+    sdx, sdy = _avg_to_ex(sd), _avg_to_ey(sd)
+    sbz = 0.25 * (sb[:-1, :-1] + sb[1:, :-1] + sb[:-1, 1:] + sb[1:, 1:])
+    muz = 0.25 * (mu_[:-1, :-1] + mu_[1:, :-1] + mu_[:-1, 1:] + mu_[1:, 1:])
+    return dict(d1x=(1 - sdx * dt / 2) / (1 + sdx * dt / 2), d2x=dt / (1 + sdx * dt / 2),
+                d1y=(1 - sdy * dt / 2) / (1 + sdy * dt / 2), d2y=dt / (1 + sdy * dt / 2),
+                hz1=(1 - sbz * dt / 2) / (1 + sbz * dt / 2), hz2=dt / (muz * (1 + sbz * dt / 2)))
+
+
+def build_tm_coeffs(grid: Grid, eps_inf=None, npml=0, y_pmc: bool = False, sigma_d=None,
+                    **kw) -> TMCoeffs:
     """TM coefficients: eps map, CPML profiles sliced to the live nodes --
     H side on the n-1 half nodes, E side on the interior [1:-1] (the full
-    axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291."""
+    axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291;
+    ``sigma_d`` (scalar or (nx, ny)) gives the conductivity pairs of :161-175."""
     _reject(kw)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
@@ -167,7 +203,7 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, npml=0, y_pmc: bool = False, **kw)
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
-        chi2=zero.clone(), has_chi2=False)
+        chi2=zero.clone(), has_chi2=False, **_cond_tm(grid, sigma_d))
 
 
 def _avg_to_ex(v):
@@ -178,9 +214,10 @@ def _avg_to_ey(v):
     return 0.5 * (v[:, :-1] + v[:, 1:])
 
 
-def build_te_coeffs(grid: Grid, eps_inf=None, npml=0, **kw) -> TECoeffs:
+def build_te_coeffs(grid: Grid, eps_inf=None, npml=0, sigma_d=None, **kw) -> TECoeffs:
     """TE coefficients: eps Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1)
-    (core/coeffs.py:347-354, :387-388) and the CPML slices of :480-491."""
+    (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491 and, with
+    ``sigma_d``, the conductivity pairs of :401-415."""
     _reject(kw)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
@@ -206,4 +243,5 @@ def build_te_coeffs(grid: Grid, eps_inf=None, npml=0, **kw) -> TECoeffs:
         b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
-        chi2_x=_avg_to_ex(zero), chi2_y=_avg_to_ey(zero), has_chi2=False)
+        chi2_x=_avg_to_ex(zero), chi2_y=_avg_to_ey(zero), has_chi2=False,
+        **_cond_te(grid, sigma_d))

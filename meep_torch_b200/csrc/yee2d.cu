@@ -990,7 +990,14 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
         hxm0 = v;
     }
 
-    // Dz(n+1) row i (core/stepper_tm.py:136-166), electric source, Ez = Dz / eps
+    // Dz(n+1) row i (core/stepper_tm.py:136-166), electric source, Ez = Dz / eps;
+    // with conductivity Dz' = c1 Dz + c2 curl, curl zero outside the updated cells
+    const bool cond = S.cond_d1[0] != nullptr;
+    float c1[4], c2[4];
+    if (cond && act) {
+        ld4(S.cond_d1[0] + ro, c1);
+        ld4(S.cond_d2[0] + ro, c2);
+    }
     float dzN[4], ezN[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -999,8 +1006,9 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
         const float dhx = (hxN[q] - hxm) * rdx;
         const float q2 = exb * p2[q] + exa * dhy;
         const float q3 = eyb[q] * p3[q] + eya[q] * dhx;
-        const float dn = d1[q] + dt * ((dhy + q2) - (dhx + q3));
-        dzN[q] = vD[q] ? dn : d1[q];
+        const float curl = (dhy + q2) - (dhx + q3);
+        const float dn = cond ? c1[q] * d1[q] + c2[q] * curl : d1[q] + dt * curl;
+        dzN[q] = vD[q] ? dn : (cond ? c1[q] * d1[q] : d1[q]);
         p2[q] = vD[q] ? q2 : p2[q];
         p3[q] = vD[q] ? q3 : p3[q];
     }
@@ -1034,13 +1042,25 @@ __device__ __forceinline__ void te_dy(const mtb_yee2d_struct &S, int r, bool val
                                       const float (&hp)[4], const float (&hc)[4],
                                       const float (&dy)[4], float (&ps)[4], float (&out)[4],
                                       const float *amp_e) {
+    // conductivity: Dy' = c1 Dy - c2 curl, curl zero outside the updated cells
+    // (core/stepper_te.py D update with d1y / d2y); rows past the grid keep Dy
+    const bool cond = S.cond_d1[1] != nullptr;
+    float c1[4], c2[4];
+    if (cond && act && r < S.nx) {
+        const uint32_t o = (uint32_t)r * S.pitch + jb;
+        ld4(S.cond_d1[1] + o, c1);
+        ld4(S.cond_d2[1] + o, c2);
+    } else {
+        c1[0] = c1[1] = c1[2] = c1[3] = 1.f;
+        zero4(c2);
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const bool v = valid && act && jb + q <= S.ny - 2;
         const float d = (hc[q] - hp[q]) * rdx;
         const float pv = b * ps[q] + a * d;
-        const float dn = dy[q] - dt * (d + pv);
-        out[q] = v ? dn : dy[q];
+        const float dn = cond ? c1[q] * dy[q] - c2[q] * (d + pv) : dy[q] - dt * (d + pv);
+        out[q] = v ? dn : (cond ? c1[q] * dy[q] : dy[q]);
         ps[q] = v ? pv : ps[q];
     }
     if (act && r >= S.src_e.row_lo && r <= S.src_e.row_hi) apply_cells(S.src_e, r, amp_e, jb, out);
@@ -1120,13 +1140,20 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
 
     // Dx / Ex(n+1/2) row i (core/stepper_te.py:79-95, :150-160)
     float dxN[4], ex[4];
+    // conductivity: Dx' = c1 Dx + c2 curl (core/stepper_te.py D update, d1x / d2x)
+    const bool cond = S.cond_d1[0] != nullptr;
+    float c1[4], c2[4];
+    if (cond && act) {
+        ld4(S.cond_d1[0] + ro, c1);
+        ld4(S.cond_d2[0] + ro, c2);
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float hm = (q == 0) ? hm0 : hc[q - 1];
         const float d = (hc[q] - hm) * rdx;
         const float pv = eyb[q] * p0[q] + eya[q] * d;
-        const float dn = dx[q] + dt * (d + pv);
-        dxN[q] = vX[q] ? dn : dx[q];
+        const float dn = cond ? c1[q] * dx[q] + c2[q] * (d + pv) : dx[q] + dt * (d + pv);
+        dxN[q] = vX[q] ? dn : (cond ? c1[q] * dx[q] : dx[q]);
         p0[q] = vX[q] ? pv : p0[q];
         ex[q] = hzRow ? dxN[q] * ix[q] : 0.f;
     }
@@ -1134,11 +1161,14 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     float exR = 0.f;
     if (hasR) {
         float v = dxr;
+        const float c1r = cond ? S.cond_d1[0][ro + 4] : 1.f;
         if (updR) {
             const float d = (hzR - hc[3]) * rdx;
             float c = d;
             if (byER) c = d + (__ldg(S.ey_b + jr) * p0r + __ldg(S.ey_a + jr) * d);
-            v = dxr + dt * c;
+            v = cond ? c1r * dxr + S.cond_d2[0][ro + 4] * c : dxr + dt * c;
+        } else if (cond) {
+            v = c1r * dxr;
         }
         exR = v * ixr;
     }
@@ -1397,7 +1427,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const int last = ib + WROWS - 1;
     const bool lean = C.wr == WROWS && !expl && ib >= 1 && last <= S.nx - 2 &&
                       ib - 1 >= S.xband[0] && last < S.xband[1] &&
-                      ib >= S.xband[2] && last < S.xband[3];
+                      ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr;
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1627,7 +1657,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
     // Dy rows outside the E x layer
     const bool lean = C.wr == WROWS && ib >= 1 && last + 1 <= S.nx - 2 && ib >= S.xband[0] &&
                       last < S.xband[1] &&
-                      ib >= S.xband[2] && last + 1 < S.xband[3];
+                      ib >= S.xband[2] && last + 1 < S.xband[3] && S.cond_d1[0] == nullptr;
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1788,6 +1818,20 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
                 if ((rc = check_ptr(S.psi[k][b], "psi", s))) return rc;
         }
         if ((rc = check_ptr(S.inv_eps_a, "inv_eps_a", s))) return rc;
+        const int n_cond = S.pol == MTB_TE ? 2 : 1;
+        if (S.cond_d1[0] || S.cond_d1[1]) {
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: conductivity needs the tile "
+                            "kernels (variant 2)", s);
+            for (int k = 0; k < n_cond; ++k) {
+                if ((rc = check_ptr(S.cond_d1[k], "cond_d1", s))) return rc;
+                if ((rc = check_ptr(S.cond_d2[k], "cond_d2", s))) return rc;
+            }
+            if (S.pol == MTB_TM && (S.cond_d1[1] || S.cond_d2[1]))
+                return fail(MTB_INVALID_ARG, "structure %d: TM conductivity uses slot 0 only", s);
+        } else if (S.cond_d2[0] || S.cond_d2[1]) {
+            return fail(MTB_INVALID_ARG, "structure %d: cond_d2 without cond_d1", s);
+        }
         if (S.pol == MTB_TE && (rc = check_ptr(S.inv_eps_b, "inv_eps_b", s))) return rc;
         if (S.pol == MTB_TM && S.explicit_e && (rc = check_ptr(S.e_explicit, "e_explicit", s)))
             return rc;
@@ -2255,6 +2299,8 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     if (!(S.dt > 0.f) || !(S.dx > 0.f)) return fail(MTB_INVALID_ARG, "noalloc: dt, dx must be > 0");
     if (S.pol == MTB_TE && (S.y_pmc || S.src_h2.n > 0))
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
+    if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1])
+        return fail(MTB_UNSUPPORTED, "noalloc: conductivity needs the tile kernels");
     int rc;
     for (int b = 0; b < 2; ++b) {
         if ((rc = check_ptr(S.f_main[b], "f_main", 0)) || (rc = check_ptr(S.f_x[b], "f_x", 0)) ||

@@ -50,6 +50,20 @@ def _opt_none(obj, names):
               f"{type(obj).__name__}.{n} is set: not supported by the B200 path")
 
 
+def _inert_magnetic(c, pairs):
+    """The reference builds the magnetic pairs (h1, h2) whenever it builds the electric
+    conductivity ones (core/coeffs.py:161-175, :401-415); they run here only inert:
+    h1 = 1 and h2 = dt (no sigma_b, mu = 1), where H' = h1 H - h2 curl is the plain step."""
+    dt = torch.tensor(float(c.dt), dtype=torch.float32)
+    for n1, n2 in pairs:
+        h1, h2 = getattr(c, n1, None), getattr(c, n2, None)
+        if h1 is None and h2 is None:
+            continue
+        _need(h1 is not None and h2 is not None and bool(torch.all(h1 == 1)) and
+              bool(torch.all(h2.to(torch.float32) == dt.to(h2.device))),
+              f"magnetic conductivity / mu ({n1}, {n2}): not supported by the B200 path")
+
+
 def coef_table(source, attr: str, t0: int, k: int, dt: float) -> np.ndarray:
     """FP64 per-step mask coefficients dt * amplitude(t), t = t0 .. t0+k-1.
 
@@ -122,6 +136,7 @@ class _Item:
     accs: list = field(default_factory=list)
     amp_col: int = -1
     hamp_col: int = -1
+    src_scale: object = None     # conductivity: d2 / dt on the electric source cells
 
 
 class Engine2D:
@@ -160,14 +175,15 @@ class Engine2D:
         if it.te:
             it.nx, it.ny = main.shape[0] + 1, main.shape[1] + 1
             _need(s.Px_cur.shape[0] == 0 and s.Py_cur.shape[0] == 0, "dispersive poles")
-            _opt_none(c, ["d1x", "hz1", "inv_xx_x", "c3xy", "c3yx", "has_chi2",
-                          "y_mirror_lo", "x_mirror_lo"])
+            _opt_none(c, ["inv_xx_x", "c3xy", "c3yx", "has_chi2", "y_mirror_lo", "x_mirror_lo"])
+            _inert_magnetic(c, [("hz1", "hz2")])
         else:
             it.nx, it.ny = main.shape
             _need(s.P_cur.shape[0] == 0, "dispersive poles")
             _opt_none(s, ["Bx", "Hx0", "Hy0"])
-            _opt_none(c, ["d1", "h1x", "mc1x", "has_chi2", "y_mirror_lo", "x_mirror_lo",
-                          "y_rot2_lo", "rot4_lo"])
+            _opt_none(c, ["mc1x", "has_chi2", "y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
+                          "rot4_lo"])
+            _inert_magnetic(c, [("h1x", "h2x"), ("h1y", "h2y")])
         _need(not getattr(c, "has_kerr", False), "Kerr (chi3) media")
         for k in ("k_hx", "k_hy", "k_ex", "k_ey"):
             kv = getattr(c, k)
@@ -294,6 +310,19 @@ class Engine2D:
             it.keep.append(inv_a)
             for k in range(4):
                 S.psi[k][0], S.psi[k][1] = L.ptr(psis[k][0]), L.ptr(psis[k][1])
+            # electric conductivity (sigma_d): D' = d1 D + d2 curl H, and the soft
+            # current on D scaled by d2 (core/stepper_tm.py:158-163, :197-200;
+            # core/stepper_te.py D update and step_source)
+            it.src_scale = None
+            cond = ([("d1x", "d2x"), ("d1y", "d2y")] if te else [("d1", "d2")])
+            if getattr(c, cond[0][0], None) is not None:
+                for k, (n1, n2) in enumerate(cond):
+                    b1 = self._pack(getattr(c, n1), nx, P)
+                    b2 = self._pack(getattr(c, n2), nx, P)
+                    S.cond_d1[k], S.cond_d2[k] = L.ptr(b1), L.ptr(b2)
+                    it.keep += [b1, b2]
+                d2e = getattr(c, cond[-1][1])
+                it.src_scale = d2e.to(device=dev, dtype=torch.float32) / float(c.dt)
             self._check_psi_outside(it)
             hx, hy, ex, ey = self._profiles(it)
             S.hx_b, S.hx_a = L.ptr(hx[0]), L.ptr(hx[1])
@@ -309,6 +338,10 @@ class Engine2D:
                     want = (nx, ny - 1) if te else (nx, ny)
                     _need(tuple(mask.shape) == want,
                           f"source mask shape {tuple(mask.shape)} != {want}")
+                    if it.src_scale is not None:
+                        # the plan subtracts (dt amp) w; under conductivity the
+                        # reference subtracts d2 amp mask
+                        mask = mask.to(device=dev, dtype=torch.float32) * it.src_scale
                     cl = _cells(mask, nx, dev)
                     if cl is not None:
                         it.amp_col = col_of.setdefault((id(src), "amplitude"), amp_cols)

@@ -75,13 +75,19 @@ def _axis_sides(npml):
 
 # ---------------------------------------------------------------- 2D TM
 
+def _cond_pair(sd, dt):
+    """(d1, d2) of an electric conductivity map (core/coeffs.py:165-166, :406-409)."""
+    return (1 - sd * dt / 2) / (1 + sd * dt / 2), dt / (1 + sd * dt / 2)
+
+
 def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
-              dtype=np.float64):
+              dtype=np.float64, sigma=None):
     """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
 
     Profiles are sliced to the live derivative nodes exactly as
     core/coeffs.py:251-278: H side at half nodes (n-1 long); E side on the
-    interior [1:-1] (or the full axis under y_pmc)."""
+    interior [1:-1] (or the full axis under y_pmc). ``sigma`` (nx, ny): the
+    electric conductivity pair (d1, d2) of :161-166 on Dz."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -98,7 +104,10 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
         b_ey, a_ey, k_ey = b_eyf, a_eyf, k_eyf
     else:
         b_ey, a_ey, k_ey = b_eyf[1:-1], a_eyf[1:-1], k_eyf[1:-1]
-    return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc,
+    cond = {}
+    if sigma is not None:
+        cond["d1"], cond["d2"] = _cond_pair(np.asarray(sigma, dtype=dtype), dt)
+    return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc, **cond,
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
                 b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
@@ -149,9 +158,15 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
     psi_Hyx = c["b_ex"] * s["psi_Hyx"] + c["a_ex"] * dHy_dx
     psi_Hxy = c["b_ey"] * s["psi_Hxy"] + c["a_ey"] * dHx_dy
     curl = dHy_dx / c["k_ex"] + psi_Hyx - dHx_dy / c["k_ey"] - psi_Hxy
-    Dz = s["Dz"] + T(dt) * np.pad(curl, pad)
-    if mask is not None:
-        Dz = Dz - T(dt * amp) * mask
+    if "d1" in c:
+        # conductivity (core/stepper_tm.py:158-161); the source scaled by d2 (:197-200)
+        Dz = c["d1"] * s["Dz"] + c["d2"] * np.pad(curl, pad)
+        if mask is not None:
+            Dz = Dz - c["d2"] * T(amp) * mask
+    else:
+        Dz = s["Dz"] + T(dt) * np.pad(curl, pad)
+        if mask is not None:
+            Dz = Dz - T(dt * amp) * mask
     Ez_new = Dz / c["eps"]
     return dict(Ez=Ez_new, Hx=Hx, Hy=Hy, Dz=Dz, psi_Ezy=psi_Ezy, psi_Ezx=psi_Ezx,
                 psi_Hyx=psi_Hyx, psi_Hxy=psi_Hxy)
@@ -159,11 +174,12 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
 
 # ---------------------------------------------------------------- 2D TE
 
-def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64):
+def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
-    (core/coeffs.py:347-354)."""
+    (core/coeffs.py:347-354); so is ``sigma`` for the conductivity pairs of
+    :401-409 on Dx and Dy."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -178,7 +194,12 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64):
     b_hy, a_hy, k_hy = cpml_profiles(ny - 1, py, 0.5, dt, dx, dtype=dtype)
     b_ey, a_ey, k_ey = (v[1:-1] for v in cpml_profiles(ny, py, 0.0, dt, dx, dtype=dtype))
     b_ex, a_ex, k_ex = (v[1:-1] for v in cpml_profiles(nx, px, 0.0, dt, dx, dtype=dtype))
-    return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e,
+    cond = {}
+    if sigma is not None:
+        sd = np.asarray(sigma, dtype=dtype)
+        cond["d1x"], cond["d2x"] = _cond_pair(h * (sd[:-1, :] + sd[1:, :]), dt)
+        cond["d1y"], cond["d2y"] = _cond_pair(h * (sd[:, :-1] + sd[:, 1:]), dt)
+    return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, **cond,
                 eps_x=eps_x, eps_y=eps_y,
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
@@ -208,10 +229,17 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
     dHz_dx = (Hz[1:, :] - Hz[:-1, :]) / T(dx)
     psi_Hzx = c["b_ex"] * s["psi_Hzx"] + c["a_ex"] * dHz_dx
     curl_y = np.pad(dHz_dx / c["k_ex"] + psi_Hzx, ((1, 1), (0, 0)))
-    Dx = s["Dx"] + T(dt) * curl_x
-    Dy = s["Dy"] - T(dt) * curl_y
-    if mask_ey is not None:
-        Dy = Dy - T(dt * amp) * mask_ey
+    if "d1x" in c:
+        # conductivity (core/stepper_te.py D update); the source scaled by d2y
+        Dx = c["d1x"] * s["Dx"] + c["d2x"] * curl_x
+        Dy = c["d1y"] * s["Dy"] - c["d2y"] * curl_y
+        if mask_ey is not None:
+            Dy = Dy - c["d2y"] * T(amp) * mask_ey
+    else:
+        Dx = s["Dx"] + T(dt) * curl_x
+        Dy = s["Dy"] - T(dt) * curl_y
+        if mask_ey is not None:
+            Dy = Dy - T(dt * amp) * mask_ey
     Ex = Dx / c["eps_x"]
     Ey = Dy / c["eps_y"]
     dEy_dx = (Ey[1:, :] - Ey[:-1, :]) / T(dx)

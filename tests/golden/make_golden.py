@@ -16,6 +16,8 @@ cases of the hot path through its own public functions:
   ``DesignRegion``, ``OptimizationProblem``; ``python make_golden.py design``)
 * d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
   and of ``run_te`` (``make_golden.py grad_te``)
+* the TM and TE cases with an electric conductivity map (``sigma_d``;
+  ``make_golden.py sigma``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -57,15 +59,26 @@ def _np(t):
     return t.detach().cpu().to(torch.float64).numpy()
 
 
-def tm_case(prec, y_pmc=False, point=False):
+def sigma_map(nx, ny, seed):
+    """Electric conductivity: a lossy slab across the grid and a graded patch."""
+    rng = np.random.default_rng(seed)
+    sig = np.zeros((nx, ny))
+    sig[26:31, :] = 1.5
+    sig[14:20, 24:30] = rng.uniform(0.5, 4.0, (6, 6))
+    return sig
+
+
+def tm_case(prec, y_pmc=False, point=False, sigma=False):
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
     eps[:, 15:21] = 12.0                          # guide along x
     eps[20:30, 8:14] = rng.uniform(2.0, 6.0)      # a block
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
+    sig = sigma_map(nx, ny, 21) if sigma else None
+    kw = {} if sig is None else {"sigma_d": torch.tensor(sig, dtype=DT[prec])}
     m = build_tm_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml,
-                        y_pmc=y_pmc)
+                        y_pmc=y_pmc, **kw)
     prof = GaussianPulse(0.65, 0.4)
     if point:
         src = LineSource(g, ix=12, j0=18, j1=19, profile=prof)
@@ -86,6 +99,8 @@ def tm_case(prec, y_pmc=False, point=False):
                acc_x=_np(ax), acc_y=_np(ay), acc_dft=_np(ad),
                flux_x=_np(monx.flux(ax, dx)), flux_y=_np(mony.flux(ay, dx)),
                mask=_np(src.mask))
+    if sig is not None:
+        out["sigma"] = sig
     for k in st._fields:
         v = getattr(st, k)
         if v is not None and v.numel():
@@ -95,14 +110,16 @@ def tm_case(prec, y_pmc=False, point=False):
     return out
 
 
-def te_case(prec):
+def te_case(prec, sigma=False):
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
     eps[:, 17:23] = 12.0
     eps[18:28, 26:32] = rng.uniform(2.0, 6.0)
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
-    m = build_te_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml)
+    sig = sigma_map(nx, ny, 22) if sigma else None
+    kw = {} if sig is None else {"sigma_d": torch.tensor(sig, dtype=DT[prec])}
+    m = build_te_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml, **kw)
     prof = GaussianPulse(0.65, 0.4)
     src = LineSource(g, ix=12, j0=12, j1=28, profile=prof)
 
@@ -124,6 +141,8 @@ def te_case(prec):
                acc_x=_np(ax), acc_y=_np(ay), acc_dft=_np(ad),
                flux_x=_np(monx.flux(ax, dx)), flux_y=_np(mony.flux(ay, dx)),
                mask=_np(_TESrc.mask))
+    if sig is not None:
+        out["sigma"] = sig
     for k in st._fields:
         v = getattr(st, k)
         if v is not None and v.numel():
@@ -343,6 +362,13 @@ def grad_te_case(prec):
 
 
 def main():
+    if sys.argv[1:] == ["sigma"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_tm_sigma_{prec}.npz"),
+                                **tm_case(prec, sigma=True))
+            np.savez_compressed(os.path.join(HERE, f"golden_te_sigma_{prec}.npz"),
+                                **te_case(prec, sigma=True))
+        return
     if sys.argv[1:] == ["grad_te"]:
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_grad_te_{prec}.npz"),

@@ -133,9 +133,31 @@ def test_unsupported_features_raise():
     with pytest.raises(NotImplementedError):
         build_tm_coeffs(g, poles=[(1.0, 0.1, 1.0)])
     with pytest.raises(NotImplementedError):
-        build_tm_coeffs(g, sigma_d=torch.ones(20, 20))
+        build_tm_coeffs(g, sigma_b=torch.ones(20, 20))
     with pytest.raises(ValueError):
         build_tm_coeffs(g, npml=10)
+
+
+def test_conductivity_coefficients_match_oracle():
+    """sigma_d gives the reference's (d1, d2) pairs on D (core/coeffs.py:161-166,
+    :401-409; the oracle's restatement is pinned by the golden runs) and inert magnetic
+    pairs (h1 = 1, h2 = dt)."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    rng = np.random.default_rng(3)
+    sig = (3.0 * rng.random((20, 24))).astype(np.float32)
+    g = Grid(nx=20, ny=24, dx=0.05, device="cpu")
+    m = build_tm_coeffs(g, sigma_d=torch.from_numpy(sig))
+    c = O.tm_coeffs(20, 24, 0.05, dtype=np.float32, sigma=sig)
+    # torch's scalar / tensor division and numpy's differ in the last bit
+    np.testing.assert_allclose(m.d1.numpy(), c["d1"], rtol=2.5e-7, atol=0)
+    np.testing.assert_allclose(m.d2.numpy(), c["d2"], rtol=2.5e-7, atol=0)
+    assert bool(torch.all(m.h1x == 1)) and bool(torch.all(m.h2y == torch.tensor(g.dt)))
+    t = build_te_coeffs(g, sigma_d=torch.from_numpy(sig))
+    ct = O.te_coeffs(20, 24, 0.05, dtype=np.float32, sigma=sig)
+    for k in ("d1x", "d2x", "d1y", "d2y"):
+        np.testing.assert_allclose(getattr(t, k).numpy(), ct[k], rtol=2.5e-7, atol=0)
+    assert bool(torch.all(t.hz1 == 1))
 
 
 def test_coef_table_matches_per_step_amplitudes():

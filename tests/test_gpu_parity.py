@@ -48,8 +48,10 @@ def run_tm_case(case, phase_mode="exact"):
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
     pmc = bool(g["y_pmc"])
     grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    sig = g.get("sigma")
     m = build_tm_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
-                        npml=int(g["npml"]), y_pmc=pmc)
+                        npml=int(g["npml"]), y_pmc=pmc,
+                        sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32))
     src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
                      profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
     freqs = [float(f) for f in g["freqs"]]
@@ -65,7 +67,7 @@ def run_tm_case(case, phase_mode="exact"):
     return st, accs, (fx, fy)
 
 
-@pytest.mark.parametrize("case", ["tm", "tm_point_pmc"])
+@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma"])
 def test_tm_matches_reference(case):
     st, accs, (fx, fy) = run_tm_case(case)
     e32, e64 = {}, {}
@@ -91,18 +93,21 @@ def test_tm_reference_phase_mode():
         assert rel_l2(a.cpu().numpy(), g[key]) < TOL, key
 
 
-def test_te_matches_reference():
+@pytest.mark.parametrize("case", ["te", "te_sigma"])
+def test_te_matches_reference(case):
     from meep_torch_b200.core.coeffs import build_te_coeffs
     from meep_torch_b200.core.grid import Grid
     from meep_torch_b200.core.monitors import DFTFieldsMonitor, FluxMonitorTE, FluxMonitorTEY
     from meep_torch_b200.core.run import run_te
     from meep_torch_b200.core.sources import GaussianPulse, LineSource, TESource
     from meep_torch_b200.core.stepper_te import init_te_state
-    g = load_golden("te_f32")
+    g = load_golden(f"{case}_f32")
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
     grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    sig = g.get("sigma")
     m = build_te_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
-                        npml=int(g["npml"]))
+                        npml=int(g["npml"]),
+                        sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32))
     src = TESource(LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]),
                               j1=int(g["src_j1"]),
                               profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"]))))
@@ -117,14 +122,14 @@ def test_te_matches_reference():
     fx, fy = monx.flux(accs[0], dx), mony.flux(accs[1], dx)
     e32, e64 = {}, {}
     for prec, errs in (("f32", e32), ("f64", e64)):
-        gg = load_golden(f"te_{prec}")
+        gg = load_golden(f"{case}_{prec}")
         for k in ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"):
             errs[k] = rel_l2(getattr(st, k).cpu().numpy(), gg["s_" + k])
         for a, key in zip(accs, ("acc_x", "acc_y", "acc_dft")):
             errs[key] = rel_l2(a.cpu().numpy(), gg[key])
         errs["flux_x"] = rel_l2(fx.cpu().numpy(), gg["flux_x"])
         errs["flux_y"] = rel_l2(fy.cpu().numpy(), gg["flux_y"])
-    _report("te", e32, e64)
+    _report(case, e32, e64)
     bad = {k: v for k, v in e32.items() if not v < TOL}
     assert not bad, bad
 
@@ -687,3 +692,80 @@ def test_3d_slabs_bitwise_equal_to_whole_grid(n_slabs, plane_source):
            if v is not None and not torch.equal(v, getattr(st, k))]
     bad += [f"acc_{q}" for q, (a, b) in enumerate(zip(accs, ref_a)) if not torch.equal(a, b)]
     assert not bad, bad
+
+
+def test_autotune_picks_a_candidate_that_matches_the_default():
+    """autotune_2d times every candidate launch shape on the batch and returns the fastest;
+    the batch advanced with it agrees with the library default (different kernels, same
+    arithmetic up to rounding)."""
+    from meep_torch_b200 import workloads as W
+    from meep_torch_b200.engine2d import Engine2D
+    from meep_torch_b200.tune import DEFAULT_CANDIDATES, autotune_2d
+    specs = W.cfg2_specs(n=6, seed=4, lo=96, hi=260)
+    items = [W.cfg2_item(s, dev()) for s in specs]
+    best, table = autotune_2d(items, steps=40, warmup=8)
+    assert len(table) == len(DEFAULT_CANDIDATES) and all(ms > 0 for _, ms in table)
+    assert best in [dict(c) for c in DEFAULT_CANDIDATES]
+    outs = []
+    for kw in ({}, best):
+        eng = Engine2D([W.cfg2_item(s, dev()) for s in specs], **kw)
+        eng.run(0, 70)
+        outs.append([eng.state(b) for b in range(len(specs))])
+        eng.close()
+    for a, b in zip(*outs):
+        main = "Ez" if hasattr(a, "Dz") else "Hz"
+        assert rel_l2(getattr(a, main).cpu().numpy(), getattr(b, main).cpu().numpy()) < 1e-5
+
+
+def test_conductivity_batched_tiles_match_oracle_and_other_paths_refuse():
+    """Electric conductivity in a batch large enough for four rows per warp (the tiles
+    then run the general rows on every warp of a conductive structure), from random
+    fields, against the oracle; the row march refuses it (MTB_UNSUPPORTED)."""
+    from meep_torch_b200._lib import MtbUnsupported
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    from meep_torch_b200.engine2d import Engine2D
+    rng = np.random.default_rng(23)
+    n, npml, dx = 30, 8, 0.05
+    specs = [("tm", 300, 260), ("te", 280, 300)] * 40
+    items, refs = [], []
+    for q, (pol, nx, ny) in enumerate(specs):
+        eps = (1.0 + 3.0 * rng.random((nx, ny))).astype(np.float32)
+        sig = np.zeros((nx, ny), dtype=np.float32)
+        sig[nx // 3: nx // 2, :] = 2.0
+        grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+        kw = dict(eps_inf=torch.from_numpy(eps), npml=npml, sigma_d=torch.from_numpy(sig))
+        if pol == "tm":
+            c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32, sigma=sig)
+            so = O.tm_state(c)
+            for k in ("Dz", "Hx", "Hy"):
+                so[k] = rng.standard_normal(so[k].shape).astype(np.float32)
+            m = build_tm_coeffs(grid, **kw)
+            so["Ez"] = (torch.from_numpy(so["Dz"]) / m.eps_inf.cpu()).numpy()
+            s0 = init_tm_state(grid)._replace(
+                **{k: torch.from_numpy(so[k]).to(dev()) for k in ("Ez", "Dz", "Hx", "Hy")})
+            step = O.tm_step
+        else:
+            c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32, sigma=sig)
+            so = O.te_state(c)
+            for k in ("Hz", "Dx", "Dy"):
+                so[k] = rng.standard_normal(so[k].shape).astype(np.float32)
+            so["Ex"], so["Ey"] = so["Dx"] / c["eps_x"], so["Dy"] / c["eps_y"]
+            m = build_te_coeffs(grid, **kw)
+            s0 = init_te_state(grid)._replace(
+                **{k: torch.from_numpy(so[k]).to(dev()) for k in ("Hz", "Dx", "Dy", "Ex", "Ey")})
+            step = O.te_step
+        items.append((s0, m, None, []))
+        if q < 2:
+            refs.append(O.run_2d(step, so, c, n)[0])
+    eng = Engine2D(items)
+    eng.run(0, n)
+    for b, ref in enumerate(refs):
+        st = eng.state(b)
+        for k in (("Ez", "Dz", "Hx", "Hy") if b == 0 else ("Hz", "Dx", "Dy", "Ex", "Ey")):
+            assert rel_l2(getattr(st, k).cpu().numpy(), ref[k]) < TOL, (b, k)
+    eng.close()
+    with pytest.raises(MtbUnsupported):
+        Engine2D(items[:1], variant=1)

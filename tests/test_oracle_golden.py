@@ -35,7 +35,7 @@ def run_tm_oracle(g, prec):
     dt_np = NPD[prec]
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
     c = O.tm_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]),
-                    y_pmc=bool(g["y_pmc"]), dtype=dt_np)
+                    y_pmc=bool(g["y_pmc"]), dtype=dt_np, sigma=g.get("sigma"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -52,7 +52,7 @@ def run_tm_oracle(g, prec):
     return c, mask, s, acc
 
 
-@pytest.mark.parametrize("case", ["tm", "tm_point_pmc"])
+@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_tm_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
@@ -73,7 +73,8 @@ def test_tm_oracle_matches_reference(case, prec):
 def run_te_oracle(g, prec):
     dt_np = NPD[prec]
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
-    c = O.te_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np)
+    c = O.te_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
+                    sigma=g.get("sigma"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)[:, :-1]
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -90,9 +91,10 @@ def run_te_oracle(g, prec):
     return c, mask, s, acc
 
 
+@pytest.mark.parametrize("case", ["te", "te_sigma"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_te_oracle_matches_reference(prec):
-    g = load_golden(f"te_{prec}")
+def test_te_oracle_matches_reference(case, prec):
+    g = load_golden(f"{case}_{prec}")
     c, mask, s, acc = run_te_oracle(g, prec)
     np.testing.assert_allclose(mask, g["mask"], rtol=1e-7)
     for k in ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"):
