@@ -151,7 +151,21 @@ typedef struct mtb_yee2d_struct {
      * MTB_UNSUPPORTED. */
     const float *cond_d1[2];
     const float *cond_d2[2];
+    /* dispersive poles on TM Ez (ADE Lorentz / Drude, core/stepper_tm.py:203-231):
+     * n_poles (<= MTB_MAX_POLES) planes of nx x pitch floats each, plane k at
+     * k * nx * pitch. pol_p[2] is a ping-pong pair: buffer `cur` holds P(n) and
+     * the other P(n-1), which the step overwrites with
+     *     P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n);
+     * then Ez(n+1) = (Dz(n+1) - sum_k P_k(n+1)) / eps. pol_c = c1, c2, c3.
+     * TM and the tile kernels only (variant 2); other variants, TE and the
+     * adjoint return MTB_UNSUPPORTED. */
+    int32_t n_poles;
+    int32_t pad3_;
+    float *pol_p[2];
+    const float *pol_c[3];
 } mtb_yee2d_struct;
+
+#define MTB_MAX_POLES 8
 
 /* A DFT phase group: frequencies sharing one table. The plan evaluates
  *   P(t, f, s) = dt * (cos(w (t + s/2) dt), -sin(w (t + s/2) dt)),  s in {1, 2}

@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("MEEP_B200_LIB") or os.path.join(HERE, "lib", "libmeep_b200.so")
 
 MTB_OK, MTB_INVALID_ARG, MTB_UNSUPPORTED, MTB_DEVICE_TIMEOUT, MTB_CUDA_ERROR = 0, 1, 2, 3, 4
+MTB_MAX_POLES = 8
 MTB_TM, MTB_TE = 0, 1
 C2_MAIN, C2_X, C2_Y = 0, 1, 2
 EX, EY, EZ, HX, HY, HZ = range(6)
@@ -45,7 +46,9 @@ class Yee2DStruct(C.Structure):
                 ("src_e", Cells), ("src_h1", Cells), ("src_h2", Cells),
                 ("lines", vp), ("n_lines", C.c_int32), ("xband", C.c_int32 * 4),
                 ("yband", C.c_int32 * 4), ("pad_", C.c_int32), ("ring_full", C.c_int64 * 3),
-                ("cond_d1", vp * 2), ("cond_d2", vp * 2)]
+                ("cond_d1", vp * 2), ("cond_d2", vp * 2),
+                ("n_poles", C.c_int32), ("pad3_", C.c_int32), ("pol_p", vp * 2),
+                ("pol_c", vp * 3)]
 
 
 class PhaseGroup(C.Structure):

@@ -8,6 +8,7 @@ electric conductivity (sigma_d); the reference's dispersive, magnetic-conductive
 nonlinear and symmetry options raise NotImplementedError here (the reference itself
 still runs them).
 """
+import math
 from typing import NamedTuple
 
 import torch
@@ -121,7 +122,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("poles", "pole_masks", "chi3", "chi2", "sigma_b", "mu", "m_poles",
+_UNSUPPORTED = ("chi3", "chi2", "sigma_b", "mu", "m_poles",
                 "m_pole_masks", "y_mirror", "x_mirror", "y_rot2", "rot4", "eps_tensor",
                 "poles_x", "poles_y", "pole_masks_x", "pole_masks_y", "poles_tensor",
                 "pole_masks_tensor")
@@ -171,12 +172,38 @@ def _cond_te(grid: Grid, sigma_d):
                 hz1=(1 - sbz * dt / 2) / (1 + sbz * dt / 2), hz2=dt / (muz * (1 + sbz * dt / 2)))
 
 
-def build_tm_coeffs(grid: Grid, eps_inf=None, npml=0, y_pmc: bool = False, sigma_d=None,
-                    **kw) -> TMCoeffs:
+def _pole_recurrence(pole, dt):
+    """ADE recurrence scalars (c1, c2, c3) of one pole, as core/coeffs.py:87-106:
+    pole = (fn, gamma, sigma[, fc]); w0 = 2 pi fn drives c1 / c2, wc = 2 pi fc (fc = fn
+    by default: Lorentz; fn = 0, fc = plasma frequency: Drude) drives c3."""
+    fn, gamma, sigma = pole[0], pole[1], pole[2]
+    fc = pole[3] if len(pole) > 3 else fn
+    w0, wc, G = 2 * math.pi * fn, 2 * math.pi * fc, 2 * math.pi * gamma
+    den = 1.0 + G * dt / 2.0
+    return ((2.0 - w0 * w0 * dt * dt) / den, -(1.0 - G * dt / 2.0) / den,
+            sigma * wc * wc * dt * dt / den)
+
+
+def _poles_tm(grid: Grid, eps, poles, pole_masks):
+    """(c1, c2, c3), each (n_poles, nx, ny), as core/coeffs.py:195-203."""
+    n = len(poles)
+    c1, c2, c3 = (grid.zeros(n, grid.nx, grid.ny) for _ in range(3))
+    for k, pole in enumerate(poles):
+        cv1, cv2, cv3 = _pole_recurrence(pole, grid.dt)
+        mask = pole_masks[k] if pole_masks is not None else torch.ones_like(eps)
+        c1[k] = cv1 * torch.ones_like(eps)
+        c2[k] = cv2 * torch.ones_like(eps)
+        c3[k] = cv3 * mask.to(eps)
+    return c1, c2, c3
+
+
+def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
+                    y_pmc: bool = False, sigma_d=None, **kw) -> TMCoeffs:
     """TM coefficients: eps map, CPML profiles sliced to the live nodes --
     H side on the n-1 half nodes, E side on the interior [1:-1] (the full
     axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291;
-    ``sigma_d`` (scalar or (nx, ny)) gives the conductivity pairs of :161-175."""
+    ``sigma_d`` (scalar or (nx, ny)) gives the conductivity pairs of :161-175,
+    ``poles`` / ``pole_masks`` the ADE recurrences of :87-106, :195-203."""
     _reject(kw)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
@@ -195,10 +222,10 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, npml=0, y_pmc: bool = False, sigma
     b_ey, a_ey, k_ey = prof(grid.ny, 0.0, py, use=not y_pmc)
     if not y_pmc:
         b_ey, a_ey, k_ey = b_ey[1:-1], a_ey[1:-1], k_ey[1:-1]
-    empty = grid.zeros(0, grid.nx, grid.ny)
+    c1, c2, c3 = _poles_tm(grid, eps, list(poles), pole_masks)
     return TMCoeffs(
-        dt=dt, dx=dx, eps_inf=eps, chi3=zero, has_kerr=False, c1=empty, c2=empty.clone(),
-        c3=empty.clone(), y_pmc=y_pmc,
+        dt=dt, dx=dx, eps_inf=eps, chi3=zero, has_kerr=False, c1=c1, c2=c2, c3=c3,
+        y_pmc=y_pmc,
         b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],

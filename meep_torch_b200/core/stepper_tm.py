@@ -11,7 +11,7 @@ class TMState(NamedTuple):
     Hx: torch.Tensor       # (nx, ny-1)      at n-1/2
     Hy: torch.Tensor       # (nx-1, ny)      at n-1/2
     Dz: torch.Tensor       # (nx, ny)
-    P_cur: torch.Tensor    # (n_poles, nx, ny) -- n_poles == 0 on the B200 path
+    P_cur: torch.Tensor    # (n_poles, nx, ny) ADE polarisation of each pole
     P_prev: torch.Tensor
     psi_Ezy: torch.Tensor  # (nx, ny-1)      CPML memory of dEz/dy (Hx update)
     psi_Ezx: torch.Tensor  # (nx-1, ny)      dEz/dx (Hy update)
@@ -29,17 +29,16 @@ class TMState(NamedTuple):
 
 def init_tm_state(grid: Grid, n_poles: int = 0, y_pmc: bool = False, **kw) -> TMState:
     """Zero TM state; psi_Hyx/psi_Hxy cover the interior (ny_e = ny-2) or
-    every row under y_pmc (ny_e = ny), as core/stepper_tm.py:41-71."""
+    every row under y_pmc (ny_e = ny), as core/stepper_tm.py:41-71; P_cur /
+    P_prev hold one (nx, ny) plane per dispersive pole."""
     for k, v in kw.items():
         if v:
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
-    if n_poles:
-        raise NotImplementedError("dispersive poles: not implemented on the B200 path")
     nx, ny = grid.nx, grid.ny
     ny_e = ny if y_pmc else ny - 2
     z = grid.zeros
     return TMState(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
-                   P_cur=z(0, nx, ny), P_prev=z(0, nx, ny), psi_Ezy=z(nx, ny - 1),
+                   P_cur=z(n_poles, nx, ny), P_prev=z(n_poles, nx, ny), psi_Ezy=z(nx, ny - 1),
                    psi_Ezx=z(nx - 1, ny), psi_Hyx=z(nx - 2, ny_e), psi_Hxy=z(nx - 2, ny_e))
 
 

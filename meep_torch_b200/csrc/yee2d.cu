@@ -913,13 +913,38 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             zero4(d0); zero4(e0); zero4(d2); zero4(e2);
             if (i >= 1) { ld4(Dz + ro - P, d0); ld4(ie + ro - P, e0); }
             if (i + 1 < nx) { ld4(Dz + ro + P, d2); ld4(ie + ro + P, e2); }
-            if (lane == 0 && jb >= 1) ezl = Dz[ro - 1] * ie[ro - 1];
-            if (lane == 31 && jb + 4 < P) ezr = Dz[ro + 4] * ie[ro + 4];
+            // dispersive poles: Ez = (Dz - sum_k P_k) / eps (core/stepper_tm.py:220-224)
+            float s0[4], s1[4], s2[4], sl = 0.f, sr = 0.f;
+            zero4(s0); zero4(s1); zero4(s2);
+            const float *Pc = S.pol_p[par];
+            const uint32_t pl = (uint32_t)nx * P;
+#pragma unroll 1
+            for (int k = 0; k < S.n_poles; ++k) {
+                const float *Pk = Pc + k * pl;
+                float t[4];
+                ld4(Pk + ro, t);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) s1[q] += t[q];
+                if (i >= 1) {
+                    ld4(Pk + ro - P, t);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) s0[q] += t[q];
+                }
+                if (i + 1 < nx) {
+                    ld4(Pk + ro + P, t);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) s2[q] += t[q];
+                }
+                if (lane == 0 && jb >= 1) sl += Pk[ro - 1];
+                if (lane == 31 && jb + 4 < P) sr += Pk[ro + 4];
+            }
+            if (lane == 0 && jb >= 1) ezl = (Dz[ro - 1] - sl) * ie[ro - 1];
+            if (lane == 31 && jb + 4 < P) ezr = (Dz[ro + 4] - sr) * ie[ro + 4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                ez0[q] = d0[q] * e0[q];
-                ez1[q] = d1[q] * e1[q];
-                ez2[q] = d2[q] * e2[q];
+                ez0[q] = (d0[q] - s0[q]) * e0[q];
+                ez1[q] = (d1[q] - s1[q]) * e1[q];
+                ez2[q] = (d2[q] - s2[q]) * e2[q];
             }
         }
         ld4(Hx + ro, hx);
@@ -1013,8 +1038,33 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
         p3[q] = vD[q] ? q3 : p3[q];
     }
     if (act && i >= S.src_e.row_lo && i <= S.src_e.row_hi) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
+    // ADE update P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n) over the old buffer
+    // (core/stepper_tm.py:203-207), then Ez = (Dz - sum_k P_k) / eps
+    float psN[4];
+    zero4(psN);
+    if (S.n_poles > 0 && act) {
+        const float *Pc = S.pol_p[par];
+        float *Po = S.pol_p[par ^ 1];
+        const uint32_t pl = (uint32_t)nx * P;
+#pragma unroll 1
+        for (int k = 0; k < S.n_poles; ++k) {
+            const uint32_t o = k * pl + ro;
+            float pc[4], pp[4], a1[4], a2[4], a3[4];
+            ld4(Pc + o, pc);
+            ld4(Po + o, pp);
+            ld4(S.pol_c[0] + o, a1);
+            ld4(S.pol_c[1] + o, a2);
+            ld4(S.pol_c[2] + o, a3);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) ezN[q] = dzN[q] * e1[q];
+            for (int q = 0; q < 4; ++q) {
+                pc[q] = a1[q] * pc[q] + a2[q] * pp[q] + a3[q] * ez1[q];
+                psN[q] += pc[q];
+            }
+            st4(Po + o, pc);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ezN[q] = (dzN[q] - psN[q]) * e1[q];
     if (!act) return;
     const int pn = par ^ 1;
     st4(S.f_main[pn] + ro, dzN);
@@ -1427,7 +1477,8 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const int last = ib + WROWS - 1;
     const bool lean = C.wr == WROWS && !expl && ib >= 1 && last <= S.nx - 2 &&
                       ib - 1 >= S.xband[0] && last < S.xband[1] &&
-                      ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr;
+                      ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr &&
+                      S.n_poles == 0;
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1831,6 +1882,22 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
                 return fail(MTB_INVALID_ARG, "structure %d: TM conductivity uses slot 0 only", s);
         } else if (S.cond_d2[0] || S.cond_d2[1]) {
             return fail(MTB_INVALID_ARG, "structure %d: cond_d2 without cond_d1", s);
+        }
+        if (S.n_poles < 0 || S.n_poles > MTB_MAX_POLES)
+            return fail(MTB_INVALID_ARG, "structure %d: n_poles %d outside [0, %d]", s,
+                        S.n_poles, MTB_MAX_POLES);
+        if (S.n_poles > 0) {
+            if (S.pol != MTB_TM)
+                return fail(MTB_UNSUPPORTED, "structure %d: poles are a TM option here", s);
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: poles need the tile kernels "
+                            "(variant 2)", s);
+            for (int b = 0; b < 2; ++b)
+                if ((rc = check_ptr(S.pol_p[b], "pol_p", s))) return rc;
+            for (int k = 0; k < 3; ++k)
+                if ((rc = check_ptr(S.pol_c[k], "pol_c", s))) return rc;
+            if ((int64_t)S.n_poles * S.nx * S.pitch >= (1LL << 31))
+                return fail(MTB_UNSUPPORTED, "structure %d: pole planes too large", s);
         }
         if (S.pol == MTB_TE && (rc = check_ptr(S.inv_eps_b, "inv_eps_b", s))) return rc;
         if (S.pol == MTB_TM && S.explicit_e && (rc = check_ptr(S.e_explicit, "e_explicit", s)))
@@ -2299,8 +2366,8 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     if (!(S.dt > 0.f) || !(S.dx > 0.f)) return fail(MTB_INVALID_ARG, "noalloc: dt, dx must be > 0");
     if (S.pol == MTB_TE && (S.y_pmc || S.src_h2.n > 0))
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
-    if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1])
-        return fail(MTB_UNSUPPORTED, "noalloc: conductivity needs the tile kernels");
+    if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles)
+        return fail(MTB_UNSUPPORTED, "noalloc: conductivity and poles need the tile kernels");
     int rc;
     for (int b = 0; b < 2; ++b) {
         if ((rc = check_ptr(S.f_main[b], "f_main", 0)) || (rc = check_ptr(S.f_x[b], "f_x", 0)) ||

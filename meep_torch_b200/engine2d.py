@@ -179,7 +179,9 @@ class Engine2D:
             _inert_magnetic(c, [("hz1", "hz2")])
         else:
             it.nx, it.ny = main.shape
-            _need(s.P_cur.shape[0] == 0, "dispersive poles")
+            np_ = s.P_cur.shape[0]
+            _need(np_ <= L.MTB_MAX_POLES, f"{np_} dispersive poles (at most {L.MTB_MAX_POLES})")
+            _need(tuple(c.c1.shape) == (np_, it.nx, it.ny), "pole coefficients c1 shape")
             _opt_none(s, ["Bx", "Hx0", "Hy0"])
             _opt_none(c, ["mc1x", "has_chi2", "y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
                           "rot4_lo"])
@@ -273,6 +275,7 @@ class Engine2D:
             S.y_pmc = 1 if (not te and getattr(c, "y_pmc", False)) else 0
             S.dt, S.dx = float(c.dt), float(c.dx)
             eps_b = None
+            pol_bufs = None
             if te:
                 f_main, f_x, f_y = self._pair(s.Hz, nx, P), self._pair(s.Dx, nx, P), \
                     self._pair(s.Dy, nx, P)
@@ -293,15 +296,33 @@ class Engine2D:
                 psis = [self._pair(s.psi_Ezy, nx, P), self._pair(s.psi_Ezx, nx, P),
                         self._pair(s.psi_Hyx, nx, P, (1, yoff)),
                         self._pair(s.psi_Hxy, nx, P, (1, yoff))]
-                # Ez is normally Dz/eps exactly (update_eh); an imported state
-                # where it is not is honoured on the first step
-                ez_ref = s.Dz / c.eps_inf.to(s.Dz.dtype)
+                # dispersive poles: P planes (ping-pong) and c1, c2, c3
+                # (core/stepper_tm.py:203-231)
+                n_p = s.P_cur.shape[0]
+                S.n_poles = n_p
+                psum = 0.0
+                if n_p:
+                    pp = [self._pack(s.P_cur.reshape(n_p * nx, ny), n_p * nx, P),
+                          self._pack(s.P_prev.reshape(n_p * nx, ny), n_p * nx, P)]
+                    pc = [self._pack(getattr(c, k).reshape(n_p * nx, ny), n_p * nx, P)
+                          for k in ("c1", "c2", "c3")]
+                    S.pol_p[0], S.pol_p[1] = L.ptr(pp[0]), L.ptr(pp[1])
+                    for k in range(3):
+                        S.pol_c[k] = L.ptr(pc[k])
+                    pol_bufs = pp
+                    it.keep += pp + pc
+                    psum = s.P_cur.sum(0)
+                # Ez is normally (Dz - sum P)/eps exactly (update_eh); an imported
+                # state where it is not is honoured on the first step
+                ez_ref = (s.Dz - psum) / c.eps_inf.to(s.Dz.dtype)
                 if not torch.equal(ez_ref, s.Ez):
                     eex = self._pack(s.Ez, nx, P)
                     S.explicit_e = 1
                     S.e_explicit = L.ptr(eex)
                     it.keep.append(eex)
             it.box = dict(main=f_main, x=f_x, y=f_y, psi=psis, eps_a=eps_a, eps_b=eps_b)
+            if pol_bufs is not None:
+                it.box["pol"] = pol_bufs
             it.keep += [*f_main, *f_x, *f_y, eps_a] + [t for p in psis for t in p]
             S.f_main[0], S.f_main[1] = L.ptr(f_main[0]), L.ptr(f_main[1])
             S.f_x[0], S.f_x[1] = L.ptr(f_x[0]), L.ptr(f_x[1])
@@ -538,7 +559,8 @@ class Engine2D:
         with the library's own fill kernel -- a fresh t = 0 run of the same batch."""
         for it in self.items:
             bufs = [*it.box["main"], *it.box["x"], *it.box["y"]] + \
-                [t for p in it.box["psi"] for t in p] + list(it.accs)
+                [t for p in it.box["psi"] for t in p] + list(it.accs) + \
+                list(it.box.get("pol", []))
             for t in bufs:
                 n = t.numel()
                 L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
@@ -547,8 +569,9 @@ class Engine2D:
     def _live_buffers(self, b: int):
         """The buffers of structure b the next step reads: fields, then CPML memory."""
         it, cur = self.items[b], self.current
+        pol = it.box.get("pol")
         return [it.box["main"][cur], it.box["x"][cur], it.box["y"][cur]] + \
-            [p[cur] for p in it.box["psi"]]
+            [p[cur] for p in it.box["psi"]] + ([pol[cur], pol[cur ^ 1]] if pol else [])
 
     def snapshot(self, b: int = 0):
         """Copy of structure b's live state (box layout) for restore()."""
@@ -607,12 +630,20 @@ class Engine2D:
                 psi_Eyx=self._unpack(ps[2][cur], (nx - 1, ny - 1)),
                 psi_Exy=self._unpack(ps[3][cur], (nx - 1, ny - 1)))
         Dz = self._unpack(bx["main"][cur], (nx, ny))
-        Ez = self._unpack(bx["main"][cur], (nx, ny), den=bx["eps_a"])
+        pol = {}
+        if "pol" in bx:
+            n_p = s.P_cur.shape[0]
+            pc = self._unpack(bx["pol"][cur], (n_p * nx, ny)).reshape(n_p, nx, ny)
+            pp = self._unpack(bx["pol"][cur ^ 1], (n_p * nx, ny)).reshape(n_p, nx, ny)
+            pol = dict(P_cur=pc, P_prev=pp)
+            Ez = (Dz - pc.sum(0)) / it.coeffs.eps_inf.to(Dz)
+        else:
+            Ez = self._unpack(bx["main"][cur], (nx, ny), den=bx["eps_a"])
         ps = bx["psi"]
         ny_e = s.psi_Hyx.shape[1]
         yoff = 0 if ny_e == ny else 1
         return s._replace(
-            Ez=Ez, Dz=Dz,
+            Ez=Ez, Dz=Dz, **pol,
             Hx=self._unpack(bx["x"][cur], (nx, ny - 1)),
             Hy=self._unpack(bx["y"][cur], (nx - 1, ny)),
             psi_Ezy=self._unpack(ps[0][cur], (nx, ny - 1)),

@@ -80,8 +80,20 @@ def _cond_pair(sd, dt):
     return (1 - sd * dt / 2) / (1 + sd * dt / 2), dt / (1 + sd * dt / 2)
 
 
+def pole_recurrence(pole, dt):
+    """(c1, c2, c3) of one ADE pole (core/coeffs.py:87-106): pole = (fn, gamma,
+    sigma[, fc]); Lorentz with fc = fn, Drude with fn = 0 and fc the plasma
+    frequency."""
+    fn, gamma, sig = pole[0], pole[1], pole[2]
+    fc = pole[3] if len(pole) > 3 else fn
+    w0, wc, G = 2 * math.pi * fn, 2 * math.pi * fc, 2 * math.pi * gamma
+    den = 1.0 + G * dt / 2.0
+    return (2.0 - w0 * w0 * dt * dt) / den, -(1.0 - G * dt / 2.0) / den, \
+        sig * wc * wc * dt * dt / den
+
+
 def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
-              dtype=np.float64, sigma=None):
+              dtype=np.float64, sigma=None, poles=(), pole_masks=None):
     """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
 
     Profiles are sliced to the live derivative nodes exactly as
@@ -107,6 +119,16 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
     cond = {}
     if sigma is not None:
         cond["d1"], cond["d2"] = _cond_pair(np.asarray(sigma, dtype=dtype), dt)
+    n_p = len(poles)
+    c1, c2, c3 = (np.zeros((n_p, nx, ny), dtype=dtype) for _ in range(3))
+    for k, pole in enumerate(poles):        # core/coeffs.py:195-203
+        cv1, cv2, cv3 = pole_recurrence(pole, dt)
+        m = (np.ones((nx, ny), dtype=dtype) if pole_masks is None
+             else np.asarray(pole_masks[k], dtype=dtype))
+        c1[k] = dtype.type(cv1)
+        c2[k] = dtype.type(cv2)
+        c3[k] = dtype.type(cv3) * m
+    cond.update(c1=c1, c2=c2, c3=c3)
     return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc, **cond,
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
@@ -119,7 +141,9 @@ def tm_state(c):
     nx, ny, dt = c["nx"], c["ny"], c["dtype"]
     ny_e = ny if c["y_pmc"] else ny - 2
     z = lambda *s: np.zeros(s, dtype=dt)
+    n_p = c["c1"].shape[0]
     return dict(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
+                P_cur=z(n_p, nx, ny), P_prev=z(n_p, nx, ny),
                 psi_Ezy=z(nx, ny - 1), psi_Ezx=z(nx - 1, ny),
                 psi_Hyx=z(nx - 2, ny_e), psi_Hxy=z(nx - 2, ny_e))
 
@@ -167,9 +191,16 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
         Dz = s["Dz"] + T(dt) * np.pad(curl, pad)
         if mask is not None:
             Dz = Dz - T(dt * amp) * mask
-    Ez_new = Dz / c["eps"]
-    return dict(Ez=Ez_new, Hx=Hx, Hy=Hy, Dz=Dz, psi_Ezy=psi_Ezy, psi_Ezx=psi_Ezx,
-                psi_Hyx=psi_Hyx, psi_Hxy=psi_Hxy)
+    out = dict(Hx=Hx, Hy=Hy, Dz=Dz, psi_Ezy=psi_Ezy, psi_Ezx=psi_Ezx, psi_Hyx=psi_Hyx,
+               psi_Hxy=psi_Hxy)
+    if c["c1"].shape[0]:
+        # update_pols (core/stepper_tm.py:203-207) on the old Ez, then
+        # update_eh(E): Ez = (Dz - sum P) / eps_inf (:220-224)
+        P_new = c["c1"] * s["P_cur"] + c["c2"] * s["P_prev"] + c["c3"] * Ez
+        out.update(P_cur=P_new, P_prev=s["P_cur"], Ez=(Dz - P_new.sum(0)) / c["eps"])
+    else:
+        out.update(Ez=Dz / c["eps"], P_cur=s.get("P_cur"), P_prev=s.get("P_prev"))
+    return out
 
 
 # ---------------------------------------------------------------- 2D TE

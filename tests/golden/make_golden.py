@@ -17,7 +17,8 @@ cases of the hot path through its own public functions:
 * d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
   and of ``run_te`` (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
-  ``make_golden.py sigma``)
+  ``make_golden.py sigma``) and the TM case with a Lorentz and a Drude pole
+  (``make_golden.py poles``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -68,7 +69,19 @@ def sigma_map(nx, ny, seed):
     return sig
 
 
-def tm_case(prec, y_pmc=False, point=False, sigma=False):
+POLES = [(0.7, 0.05, 1.5), (0.0, 0.1, 1.0, 0.9)]   # a Lorentz and a Drude pole
+
+
+def pole_masks(nx, ny):
+    """The Lorentz pole on a block across the guide, the Drude pole on a patch."""
+    m0 = np.zeros((nx, ny))
+    m0[22:30, 12:24] = 1.0
+    m1 = np.zeros((nx, ny))
+    m1[32:38, 6:12] = 1.0
+    return [m0, m1]
+
+
+def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False):
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -77,6 +90,9 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False):
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
     sig = sigma_map(nx, ny, 21) if sigma else None
     kw = {} if sig is None else {"sigma_d": torch.tensor(sig, dtype=DT[prec])}
+    pm = pole_masks(nx, ny) if poles else None
+    if poles:
+        kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
     m = build_tm_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml,
                         y_pmc=y_pmc, **kw)
     prof = GaussianPulse(0.65, 0.4)
@@ -88,7 +104,7 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False):
     monx = FluxMonitorTM(g, freqs, x_normal=True, idx=36, lo=9, hi=27)
     mony = FluxMonitorTM(g, freqs, x_normal=False, idx=26, lo=10, hi=38)
     dft = DFTFieldsMonitor(g, freqs, component="Ez")
-    s0 = init_tm_state(g, y_pmc=y_pmc)
+    s0 = init_tm_state(g, y_pmc=y_pmc, n_poles=len(POLES) if poles else 0)
     n = 300
     with torch.no_grad():
         st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft])
@@ -101,6 +117,9 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False):
                mask=_np(src.mask))
     if sig is not None:
         out["sigma"] = sig
+    if poles:
+        out["poles"] = json.dumps(POLES)
+        out["pole_masks"] = np.stack(pm)
     for k in st._fields:
         v = getattr(st, k)
         if v is not None and v.numel():
@@ -362,6 +381,11 @@ def grad_te_case(prec):
 
 
 def main():
+    if sys.argv[1:] == ["poles"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_tm_poles_{prec}.npz"),
+                                **tm_case(prec, poles=True))
+        return
     if sys.argv[1:] == ["sigma"]:
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_tm_sigma_{prec}.npz"),

@@ -131,11 +131,26 @@ def test_unsupported_features_raise():
     from meep_torch_b200.core.grid import Grid
     g = Grid(nx=20, ny=20, dx=0.05, device="cpu")
     with pytest.raises(NotImplementedError):
-        build_tm_coeffs(g, poles=[(1.0, 0.1, 1.0)])
+        build_tm_coeffs(g, m_poles=[(1.0, 0.1, 1.0)])
     with pytest.raises(NotImplementedError):
         build_tm_coeffs(g, sigma_b=torch.ones(20, 20))
     with pytest.raises(ValueError):
         build_tm_coeffs(g, npml=10)
+
+
+def test_pole_coefficients_match_oracle():
+    """poles / pole_masks give the reference's ADE planes (core/coeffs.py:87-106,
+    :195-203), as the oracle restates them."""
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    poles = [(0.7, 0.05, 1.5), (0.0, 0.1, 1.0, 0.9)]
+    masks = [np.zeros((20, 24), dtype=np.float32), np.ones((20, 24), dtype=np.float32)]
+    masks[0][5:9, 3:10] = 1.0
+    g = Grid(nx=20, ny=24, dx=0.05, device="cpu")
+    m = build_tm_coeffs(g, poles=poles, pole_masks=[torch.from_numpy(x) for x in masks])
+    c = O.tm_coeffs(20, 24, 0.05, dtype=np.float32, poles=poles, pole_masks=masks)
+    for k in ("c1", "c2", "c3"):
+        np.testing.assert_array_equal(getattr(m, k).numpy(), c[k])
 
 
 def test_conductivity_coefficients_match_oracle():

@@ -49,9 +49,12 @@ def run_tm_case(case, phase_mode="exact"):
     pmc = bool(g["y_pmc"])
     grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
     sig = g.get("sigma")
+    poles = json.loads(str(g["poles"])) if "poles" in g else ()
+    pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
     m = build_tm_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
                         npml=int(g["npml"]), y_pmc=pmc,
-                        sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32))
+                        sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32),
+                        poles=poles, pole_masks=pm)
     src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
                      profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
     freqs = [float(f) for f in g["freqs"]]
@@ -61,19 +64,22 @@ def run_tm_case(case, phase_mode="exact"):
     monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=ix, lo=xlo, hi=xhi)
     mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=iy, lo=ylo, hi=yhi)
     dft = DFTFieldsMonitor(grid, freqs, "Ez")
-    st, accs = run_tm(init_tm_state(grid, y_pmc=pmc), m, int(g["n_steps"]), source=src,
-                      monitors=[monx, mony, dft], phase_mode=phase_mode)
+    st, accs = run_tm(init_tm_state(grid, y_pmc=pmc, n_poles=len(poles)), m, int(g["n_steps"]),
+                      source=src, monitors=[monx, mony, dft], phase_mode=phase_mode)
     fx, fy = monx.flux(accs[0], dx), mony.flux(accs[1], dx)
     return st, accs, (fx, fy)
 
 
-@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma"])
+@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles"])
 def test_tm_matches_reference(case):
     st, accs, (fx, fy) = run_tm_case(case)
     e32, e64 = {}, {}
     for prec, errs in (("f32", e32), ("f64", e64)):
         g = load_golden(f"{case}_{prec}")
-        for k in ("Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"):
+        names = ["Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"]
+        if "s_P_cur" in g:
+            names += ["P_cur", "P_prev"]
+        for k in names:
             errs[k] = rel_l2(getattr(st, k).cpu().numpy(), g["s_" + k])
         for a, key in zip(accs, ("acc_x", "acc_y", "acc_dft")):
             errs[key] = rel_l2(a.cpu().numpy(), g[key])
@@ -765,6 +771,57 @@ def test_conductivity_batched_tiles_match_oracle_and_other_paths_refuse():
     for b, ref in enumerate(refs):
         st = eng.state(b)
         for k in (("Ez", "Dz", "Hx", "Hy") if b == 0 else ("Hz", "Dx", "Dy", "Ex", "Ey")):
+            assert rel_l2(getattr(st, k).cpu().numpy(), ref[k]) < TOL, (b, k)
+    eng.close()
+    with pytest.raises(MtbUnsupported):
+        Engine2D(items[:1], variant=1)
+
+
+def test_poles_batched_tiles_match_oracle_from_random_state():
+    """Lorentz and Drude poles in a batch that gets four rows per warp, from random
+    fields and polarisations, against the oracle (fields, CPML memory, both P buffers);
+    a pole-free structure in the same batch keeps the lean rows. The row march refuses
+    poles (MTB_UNSUPPORTED)."""
+    from meep_torch_b200._lib import MtbUnsupported
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    from meep_torch_b200.engine2d import Engine2D
+    rng = np.random.default_rng(31)
+    n, npml, dx = 30, 8, 0.05
+    poles = [(0.7, 0.05, 1.5), (0.0, 0.1, 1.0, 0.9)]
+    items, refs = [], []
+    for q in range(60):
+        nx, ny = (300, 260) if q % 2 == 0 else (260, 300)
+        use = q % 3 != 2
+        eps = (1.0 + 3.0 * rng.random((nx, ny))).astype(np.float32)
+        masks = [(rng.random((nx, ny)) < 0.5).astype(np.float32) for _ in poles] if use else None
+        grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+        pl = poles if use else ()
+        c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32, poles=pl,
+                        pole_masks=masks)
+        so = O.tm_state(c)
+        for k in ("Dz", "Hx", "Hy", "P_cur", "P_prev"):
+            so[k] = (0.1 if k.startswith("P") else 1.0) * \
+                rng.standard_normal(so[k].shape).astype(np.float32)
+        so["Ez"] = (so["Dz"] - so["P_cur"].sum(0)) / c["eps"]
+        m = build_tm_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml, poles=pl,
+                            pole_masks=None if masks is None else
+                            [torch.from_numpy(x) for x in masks])
+        s0 = init_tm_state(grid, n_poles=len(pl))._replace(
+            **{k: torch.from_numpy(so[k]).to(dev())
+               for k in ("Ez", "Dz", "Hx", "Hy", "P_cur", "P_prev")})
+        items.append((s0, m, None, []))
+        if q < 3:
+            refs.append(O.run_2d(O.tm_step, so, c, n)[0])
+    eng = Engine2D(items)
+    eng.run(0, n)
+    for b, ref in enumerate(refs):
+        st = eng.state(b)
+        names = ["Ez", "Dz", "Hx", "Hy", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"]
+        if b % 3 != 2:
+            names += ["P_cur", "P_prev"]
+        for k in names:
             assert rel_l2(getattr(st, k).cpu().numpy(), ref[k]) < TOL, (b, k)
     eng.close()
     with pytest.raises(MtbUnsupported):

@@ -34,8 +34,10 @@ def test_cpml_profiles_match_reference():
 def run_tm_oracle(g, prec):
     dt_np = NPD[prec]
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
+    poles = json.loads(str(g["poles"])) if "poles" in g else ()
     c = O.tm_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]),
-                    y_pmc=bool(g["y_pmc"]), dtype=dt_np, sigma=g.get("sigma"))
+                    y_pmc=bool(g["y_pmc"]), dtype=dt_np, sigma=g.get("sigma"),
+                    poles=poles, pole_masks=g.get("pole_masks"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -52,7 +54,7 @@ def run_tm_oracle(g, prec):
     return c, mask, s, acc
 
 
-@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma"])
+@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_tm_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
@@ -60,7 +62,10 @@ def test_tm_oracle_matches_reference(case, prec):
     np.testing.assert_allclose(mask, g["mask"], rtol=1e-7)
     for k in ("b_hy", "a_hy", "b_hx", "a_hx", "b_ex", "a_ex", "b_ey", "a_ey"):
         np.testing.assert_allclose(c[k], g["c_" + k], rtol=1e-6, atol=1e-6)
-    for k in ("Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"):
+    names = ["Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"]
+    if "s_P_cur" in g:
+        names += ["P_cur", "P_prev"]
+    for k in names:
         assert rel_l2(s[k], g["s_" + k]) < TOL[prec], k
     for a, key in zip(acc, ("acc_x", "acc_y", "acc_dft")):
         assert rel_l2(a, g[key]) < TOL[prec], key
