@@ -869,7 +869,7 @@ __device__ __forceinline__ void tm_hy(const mtb_yee2d_struct &S, int r, bool val
         apply_cells(S.src_h1, r, amp_h, jb, out);
 }
 
-template <bool EXPL>
+template <bool EXPL, bool EXT>
 __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, const int c0,
                                         const Ctx2D &C, const mtb_line_sample *L, const int nl) {
     const int lane = threadIdx.x;
@@ -919,7 +919,7 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             const float *Pc = S.pol_p[par];
             const uint32_t pl = (uint32_t)nx * P;
 #pragma unroll 1
-            for (int k = 0; k < S.n_poles; ++k) {
+            for (int k = 0; k < (EXT ? S.n_poles : 0); ++k) {
                 const float *Pk = Pc + k * pl;
                 float t[4];
                 ld4(Pk + ro, t);
@@ -1017,7 +1017,7 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
 
     // Dz(n+1) row i (core/stepper_tm.py:136-166), electric source, Ez = Dz / eps;
     // with conductivity Dz' = c1 Dz + c2 curl, curl zero outside the updated cells
-    const bool cond = S.cond_d1[0] != nullptr;
+    const bool cond = EXT && S.cond_d1[0] != nullptr;
     float c1[4], c2[4];
     if (cond && act) {
         ld4(S.cond_d1[0] + ro, c1);
@@ -1042,12 +1042,12 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
     // (core/stepper_tm.py:203-207), then Ez = (Dz - sum_k P_k) / eps
     float psN[4];
     zero4(psN);
-    if (S.n_poles > 0 && act) {
+    if (EXT && S.n_poles > 0 && act) {
         const float *Pc = S.pol_p[par];
         float *Po = S.pol_p[par ^ 1];
         const uint32_t pl = (uint32_t)nx * P;
 #pragma unroll 1
-        for (int k = 0; k < S.n_poles; ++k) {
+        for (int k = 0; k < (EXT ? S.n_poles : 0); ++k) {
             const uint32_t o = k * pl + ro;
             float pc[4], pp[4], a1[4], a2[4], a3[4];
             ld4(Pc + o, pc);
@@ -1087,6 +1087,7 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
 
 // Dy(n+1/2) of one row from Hz rows r-1 (hp), r (hc): core/stepper_te.py:79-111,
 // source :120-134. `valid` = 1 <= r <= nx-2.
+template <bool EXT>
 __device__ __forceinline__ void te_dy(const mtb_yee2d_struct &S, int r, bool valid, bool act,
                                       int jb, float b, float a, float dt, float rdx,
                                       const float (&hp)[4], const float (&hc)[4],
@@ -1094,7 +1095,7 @@ __device__ __forceinline__ void te_dy(const mtb_yee2d_struct &S, int r, bool val
                                       const float *amp_e) {
     // conductivity: Dy' = c1 Dy - c2 curl, curl zero outside the updated cells
     // (core/stepper_te.py D update with d1y / d2y); rows past the grid keep Dy
-    const bool cond = S.cond_d1[1] != nullptr;
+    const bool cond = EXT && S.cond_d1[1] != nullptr;
     float c1[4], c2[4];
     if (cond && act && r < S.nx) {
         const uint32_t o = (uint32_t)r * S.pitch + jb;
@@ -1116,6 +1117,7 @@ __device__ __forceinline__ void te_dy(const mtb_yee2d_struct &S, int r, bool val
     if (act && r >= S.src_e.row_lo && r <= S.src_e.row_hi) apply_cells(S.src_e, r, amp_e, jb, out);
 }
 
+template <bool EXT>
 __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, const int c0,
                                         const Ctx2D &C, const mtb_line_sample *L, const int nl) {
     const int lane = threadIdx.x;
@@ -1191,7 +1193,7 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     // Dx / Ex(n+1/2) row i (core/stepper_te.py:79-95, :150-160)
     float dxN[4], ex[4];
     // conductivity: Dx' = c1 Dx + c2 curl (core/stepper_te.py D update, d1x / d2x)
-    const bool cond = S.cond_d1[0] != nullptr;
+    const bool cond = EXT && S.cond_d1[0] != nullptr;
     float c1[4], c2[4];
     if (cond && act) {
         ld4(S.cond_d1[0] + ro, c1);
@@ -1224,8 +1226,8 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     }
     // Dy / Ey(n+1/2) rows i and i+1 (recomputed halo)
     float dyN[4], ey[4], dyNn[4], eyn[4];
-    te_dy(S, i, dyRow, act, jb, exb, exa, dt, rdx, hp, hc, dy, p1, dyN, C.amp_e);
-    te_dy(S, i + 1, dyRowN, act, jb, exbn, exan, dt, rdx, hc, hn, dyn, p1n, dyNn, C.amp_e);
+    te_dy<EXT>(S, i, dyRow, act, jb, exb, exa, dt, rdx, hp, hc, dy, p1, dyN, C.amp_e);
+    te_dy<EXT>(S, i + 1, dyRowN, act, jb, exbn, exan, dt, rdx, hc, hn, dyn, p1n, dyNn, C.amp_e);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         ey[q] = dyN[q] * iy[q];
@@ -1462,7 +1464,7 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
     }
 }
 
-template <bool FIRST>
+template <bool FIRST, bool EXT>
 __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
     Ctx2D C) {
@@ -1496,9 +1498,9 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     for (int r = 0; r < C.wr; ++r) {
         if (ib + r >= S.nx) break;
         if (FIRST && expl)
-            tm_tile<true>(S, ib + r, w.z, C, T.lines, T.nl);
+            tm_tile<true, EXT>(S, ib + r, w.z, C, T.lines, T.nl);
         else
-            tm_tile<false>(S, ib + r, w.z, C, T.lines, T.nl);
+            tm_tile<false, EXT>(S, ib + r, w.z, C, T.lines, T.nl);
     }
 }
 
@@ -1694,6 +1696,7 @@ __device__ __forceinline__ void te_rows(const mtb_yee2d_struct &S, const int ib,
     }
 }
 
+template <bool EXT>
 __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
     const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
     Ctx2D C) {
@@ -1726,7 +1729,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
 #pragma unroll 1
     for (int r = 0; r < C.wr; ++r) {
         if (ib + r >= S.nx) break;
-        te_tile(S, ib + r, w.z, C, T.lines, T.nl);
+        te_tile<EXT>(S, ib + r, w.z, C, T.lines, T.nl);
     }
 }
 
@@ -1744,6 +1747,7 @@ struct mtb_yee2d_plan {
     int rows = 32;
     int variant = 2;                   // 1 row march, 2 tiles
     int wr = 1;                        // tiles: rows per warp
+    bool ext = false;                  // a structure has conductivity or poles
     int graph_mode = 0;                // 0 graphs when eligible, -1 off
     cudaStream_t cap = nullptr;        // private capture stream
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // ring flush graph per start parity
@@ -1957,6 +1961,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     p->graph_mode = (tuning && tuning->graph < 0) ? -1 : 0;
     p->n_cols = n_amp_cols;
     p->n_work = (int)n_work;
+    for (int s = 0; s < n; ++s)
+        if (structs[s].cond_d1[0] || structs[s].n_poles > 0) p->ext = true;
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->structs_d.ensure(sizeof(mtb_yee2d_struct) * n);
     if (!rc) rc = p->work_d.ensure(sizeof(int4) * n_work);
@@ -2022,15 +2028,22 @@ static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
     if (p->variant == 2) {
         const dim3 blk(32, TROWS);
         if (n_tm > 0) {
-            if (C.first)
-                k_tile_tm<true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+            if (C.first && p->ext)
+                k_tile_tm<true, true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+            else if (C.first)
+                k_tile_tm<true, false><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+            else if (p->ext)
+                k_tile_tm<false, true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
             else
-                k_tile_tm<false><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+                k_tile_tm<false, false><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
             MTB_CHECK_LAUNCH();
             ++p->last_launches;
         }
         if (n_te > 0) {
-            k_tile_te<<<n_te, blk, 0, st>>>(SS, W + n_tm, n_te, C);
+            if (p->ext)
+                k_tile_te<true><<<n_te, blk, 0, st>>>(SS, W + n_tm, n_te, C);
+            else
+                k_tile_te<false><<<n_te, blk, 0, st>>>(SS, W + n_tm, n_te, C);
             MTB_CHECK_LAUNCH();
             ++p->last_launches;
         }
