@@ -151,18 +151,22 @@ typedef struct mtb_yee2d_struct {
      * MTB_UNSUPPORTED. */
     const float *cond_d1[2];
     const float *cond_d2[2];
-    /* dispersive poles on TM Ez (ADE Lorentz / Drude, core/stepper_tm.py:203-231):
-     * n_poles (<= MTB_MAX_POLES) planes of nx x pitch floats each, plane k at
-     * k * nx * pitch. pol_p[2] is a ping-pong pair: buffer `cur` holds P(n) and
-     * the other P(n-1), which the step overwrites with
-     *     P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n);
-     * then Ez(n+1) = (Dz(n+1) - sum_k P_k(n+1)) / eps. pol_c = c1, c2, c3.
-     * TM and the tile kernels only (variant 2); other variants, TE and the
-     * adjoint return MTB_UNSUPPORTED. */
+    /* dispersive poles (ADE Lorentz / Drude; TM core/stepper_tm.py:203-231, TE
+     * core/stepper_te.py:136-175): n_poles (<= MTB_MAX_POLES) planes of
+     * nx x pitch floats each, plane k at k * nx * pitch, on TM Ez or TE Ex.
+     * pol_p[2] is a ping-pong pair: buffer `cur` holds P(n) and the other
+     * P(n-1), which the step overwrites with
+     *     P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n);
+     * then E(n+1) = (D(n+1) - sum_k P_k(n+1)) / eps. pol_c = c1, c2, c3.
+     * TE's Ey poles are the second set (n_poles_y, pol_py, pol_cy). Tile
+     * kernels only (variant 2); the other variants and the adjoint return
+     * MTB_UNSUPPORTED. */
     int32_t n_poles;
-    int32_t pad3_;
+    int32_t n_poles_y;
     float *pol_p[2];
     const float *pol_c[3];
+    float *pol_py[2];
+    const float *pol_cy[3];
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

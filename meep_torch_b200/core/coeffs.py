@@ -124,8 +124,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
 
 _UNSUPPORTED = ("chi3", "chi2", "sigma_b", "mu", "m_poles",
                 "m_pole_masks", "y_mirror", "x_mirror", "y_rot2", "rot4", "eps_tensor",
-                "poles_x", "poles_y", "pole_masks_x", "pole_masks_y", "poles_tensor",
-                "pole_masks_tensor")
+                "poles_tensor", "pole_masks_tensor")
 
 
 def _reject(kw):
@@ -241,10 +240,32 @@ def _avg_to_ey(v):
     return 0.5 * (v[:, :-1] + v[:, 1:])
 
 
-def build_te_coeffs(grid: Grid, eps_inf=None, npml=0, sigma_d=None, **kw) -> TECoeffs:
+def _axis_poles(grid: Grid, eps, shared, axis_poles, shared_masks, axis_masks, shape, avg):
+    """(c1, c2, c3) of one TE E axis (core/coeffs.py:109-131): the shared poles, then the
+    axis-only ones; masks are Yee-averaged from cell centres onto the E nodes."""
+    allp = list(shared) + list(axis_poles)
+    c1, c2, c3 = (grid.zeros(len(allp), *shape) for _ in range(3))
+    ns = len(shared)
+    for k, pole in enumerate(allp):
+        cv1, cv2, cv3 = _pole_recurrence(pole, grid.dt)
+        if k < ns:
+            m = shared_masks[k] if shared_masks is not None else None
+        else:
+            m = axis_masks[k - ns] if axis_masks is not None else None
+        mask = (m if m is not None else torch.ones_like(eps)).to(eps)
+        c1[k] = cv1
+        c2[k] = cv2
+        c3[k] = cv3 * avg(mask)
+    return c1, c2, c3
+
+
+def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
+                    sigma_d=None, poles_x=(), poles_y=(), pole_masks_x=None,
+                    pole_masks_y=None, **kw) -> TECoeffs:
     """TE coefficients: eps Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1)
-    (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491 and, with
-    ``sigma_d``, the conductivity pairs of :401-415."""
+    (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491, with
+    ``sigma_d`` the conductivity pairs of :401-415, and the per-axis ADE pole stacks
+    of :416-425 (shared ``poles`` on both axes, ``poles_x`` / ``poles_y`` on one)."""
     _reject(kw)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
@@ -260,12 +281,14 @@ def build_te_coeffs(grid: Grid, eps_inf=None, npml=0, sigma_d=None, **kw) -> TEC
     b_hy, a_hy, k_hy = prof(grid.ny - 1, 0.5, py)
     b_ey, a_ey, k_ey = (v[1:-1] for v in prof(grid.ny, 0.0, py))
     b_ex, a_ex, k_ex = (v[1:-1] for v in prof(grid.nx, 0.0, px))
-    ex0 = grid.zeros(0, grid.nx - 1, grid.ny)
-    ey0 = grid.zeros(0, grid.nx, grid.ny - 1)
+    c1x, c2x, c3x = _axis_poles(grid, eps, poles, poles_x, pole_masks, pole_masks_x,
+                                (grid.nx - 1, grid.ny), _avg_to_ex)
+    c1y, c2y, c3y = _axis_poles(grid, eps, poles, poles_y, pole_masks, pole_masks_y,
+                                (grid.nx, grid.ny - 1), _avg_to_ey)
     return TECoeffs(
         dt=dt, dx=dx, eps_x=_avg_to_ex(eps), eps_y=_avg_to_ey(eps),
         chi3_x=_avg_to_ex(zero), chi3_y=_avg_to_ey(zero), has_kerr=False,
-        c1x=ex0, c2x=ex0.clone(), c3x=ex0.clone(), c1y=ey0, c2y=ey0.clone(), c3y=ey0.clone(),
+        c1x=c1x, c2x=c2x, c3x=c3x, c1y=c1y, c2y=c2y, c3y=c3y,
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],

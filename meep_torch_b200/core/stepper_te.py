@@ -13,9 +13,9 @@ class TEState(NamedTuple):
     Ey: torch.Tensor       # (nx, ny-1)   at n-1/2
     Dx: torch.Tensor       # (nx-1, ny)
     Dy: torch.Tensor       # (nx, ny-1)
-    Px_cur: torch.Tensor   # (0, nx-1, ny) on the B200 path
+    Px_cur: torch.Tensor   # (n_poles, nx-1, ny) ADE polarisation on Ex
     Px_prev: torch.Tensor
-    Py_cur: torch.Tensor   # (0, nx, ny-1)
+    Py_cur: torch.Tensor   # (n_poles_y, nx, ny-1) on Ey
     Py_prev: torch.Tensor
     psi_Eyx: torch.Tensor  # (nx-1, ny-1)
     psi_Exy: torch.Tensor  # (nx-1, ny-1)
@@ -24,13 +24,15 @@ class TEState(NamedTuple):
 
 
 def init_te_state(grid: Grid, n_poles: int = 0, n_poles_y: int | None = None) -> TEState:
-    if n_poles or n_poles_y:
-        raise NotImplementedError("dispersive poles: not implemented on the B200 path")
+    """Zero TE state (core/stepper_te.py:27-49); n_poles sizes the Ex pole stack and
+    n_poles_y (default n_poles: shared poles) the Ey one."""
     nx, ny = grid.nx, grid.ny
+    npy = n_poles if n_poles_y is None else n_poles_y
     z = grid.zeros
     return TEState(Hz=z(nx - 1, ny - 1), Ex=z(nx - 1, ny), Ey=z(nx, ny - 1), Dx=z(nx - 1, ny),
-                   Dy=z(nx, ny - 1), Px_cur=z(0, nx - 1, ny), Px_prev=z(0, nx - 1, ny),
-                   Py_cur=z(0, nx, ny - 1), Py_prev=z(0, nx, ny - 1),
+                   Dy=z(nx, ny - 1), Px_cur=z(n_poles, nx - 1, ny),
+                   Px_prev=z(n_poles, nx - 1, ny), Py_cur=z(npy, nx, ny - 1),
+                   Py_prev=z(npy, nx, ny - 1),
                    psi_Eyx=z(nx - 1, ny - 1), psi_Exy=z(nx - 1, ny - 1),
                    psi_Hzy=z(nx - 1, ny - 2), psi_Hzx=z(nx - 2, ny - 1))
 

@@ -1087,6 +1087,45 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
 
 // Dy(n+1/2) of one row from Hz rows r-1 (hp), r (hc): core/stepper_te.py:79-111,
 // source :120-134. `valid` = 1 <= r <= nx-2.
+// Sum over a pole stack (planes pl floats apart) of one float4 at offset o.
+__device__ __forceinline__ void pole_sum4(const float *Pc, int np, uint32_t pl, uint32_t o,
+                                          float (&s)[4]) {
+    zero4(s);
+#pragma unroll 1
+    for (int k = 0; k < np; ++k) {
+        float t[4];
+        ld4(Pc + k * pl + o, t);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s[q] += t[q];
+    }
+}
+
+// ADE step of one float4 of a pole stack: P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n)
+// (core/stepper_tm.py:203-207, core/stepper_te.py:136-146), written over P(n-1)
+// when STORE (the owner of the cells), and sum_k P_k(n+1) into s.
+template <bool STORE>
+__device__ __forceinline__ void pole_step4(const float *Pc, float *Po, const float *const *c,
+                                           int np, uint32_t pl, uint32_t o,
+                                           const float (&e)[4], float (&s)[4]) {
+    zero4(s);
+#pragma unroll 1
+    for (int k = 0; k < np; ++k) {
+        const uint32_t ok = k * pl + o;
+        float pc[4], pp[4], a1[4], a2[4], a3[4];
+        ld4(Pc + ok, pc);
+        ld4(Po + ok, pp);
+        ld4(c[0] + ok, a1);
+        ld4(c[1] + ok, a2);
+        ld4(c[2] + ok, a3);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            pc[q] = a1[q] * pc[q] + a2[q] * pp[q] + a3[q] * e[q];
+            s[q] += pc[q];
+        }
+        if (STORE) st4(Po + ok, pc);
+    }
+}
+
 template <bool EXT>
 __device__ __forceinline__ void te_dy(const mtb_yee2d_struct &S, int r, bool valid, bool act,
                                       int jb, float b, float a, float dt, float rdx,
@@ -1209,6 +1248,20 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
         p0[q] = vX[q] ? pv : p0[q];
         ex[q] = hzRow ? dxN[q] * ix[q] : 0.f;
     }
+    // dispersive poles on Ex / Ey (core/stepper_te.py:136-175): the ADE step on
+    // the old E, then E = (D - sum P) / eps; the halo cells (lane 31's column,
+    // row i+1 of Ey) recompute their poles without storing them
+    const int npx = EXT ? S.n_poles : 0, npy = EXT ? S.n_poles_y : 0;
+    const uint32_t pl = (uint32_t)nx * P;
+    if (npx > 0 && act) {
+        float sc[4], eo[4], sn[4];
+        pole_sum4(S.pol_p[par], npx, pl, ro, sc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) eo[q] = (dx[q] - sc[q]) * ix[q];
+        pole_step4<true>(S.pol_p[par], S.pol_p[par ^ 1], S.pol_c, npx, pl, ro, eo, sn);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ex[q] = hzRow ? (dxN[q] - sn[q]) * ix[q] : 0.f;
+    }
     // Ex(n+1/2)(i, jb+4): lane 31's right neighbour column
     float exR = 0.f;
     if (hasR) {
@@ -1222,7 +1275,18 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
         } else if (cond) {
             v = c1r * dxr;
         }
-        exR = v * ixr;
+        float sN = 0.f;
+        if (npx > 0) {
+            const float *Pc = S.pol_p[par], *Pp = S.pol_p[par ^ 1];
+            float sc = 0.f;
+            for (int k = 0; k < npx; ++k) sc += Pc[k * pl + ro + 4];
+            const float eo = (dxr - sc) * ixr;
+            for (int k = 0; k < npx; ++k) {
+                const uint32_t ok = k * pl + ro + 4;
+                sN += S.pol_c[0][ok] * Pc[ok] + S.pol_c[1][ok] * Pp[ok] + S.pol_c[2][ok] * eo;
+            }
+        }
+        exR = (v - sN) * ixr;
     }
     // Dy / Ey(n+1/2) rows i and i+1 (recomputed halo)
     float dyN[4], ey[4], dyNn[4], eyn[4];
@@ -1232,6 +1296,24 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     for (int q = 0; q < 4; ++q) {
         ey[q] = dyN[q] * iy[q];
         eyn[q] = (i + 1 < nx) ? dyNn[q] * iyn[q] : 0.f;
+    }
+    if (npy > 0 && act) {
+        float sc[4], eo[4], sn[4];
+        pole_sum4(S.pol_py[par], npy, pl, ro, sc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) eo[q] = (dy[q] - sc[q]) * iy[q];
+        pole_step4<true>(S.pol_py[par], S.pol_py[par ^ 1], S.pol_cy, npy, pl, ro, eo, sn);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ey[q] = (dyN[q] - sn[q]) * iy[q];
+        if (i + 1 < nx) {
+            pole_sum4(S.pol_py[par], npy, pl, ro + P, sc);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) eo[q] = (dyn[q] - sc[q]) * iyn[q];
+            pole_step4<false>(S.pol_py[par], S.pol_py[par ^ 1], S.pol_cy, npy, pl, ro + P, eo,
+                              sn);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) eyn[q] = (dyNn[q] - sn[q]) * iyn[q];
+        }
     }
     float exr = __shfl_down_sync(0xffffffffu, ex[0], 1);
     if (lane == 31) exr = exR;
@@ -1711,7 +1793,8 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
     // Dy rows outside the E x layer
     const bool lean = C.wr == WROWS && ib >= 1 && last + 1 <= S.nx - 2 && ib >= S.xband[0] &&
                       last < S.xband[1] &&
-                      ib >= S.xband[2] && last + 1 < S.xband[3] && S.cond_d1[0] == nullptr;
+                      ib >= S.xband[2] && last + 1 < S.xband[3] && S.cond_d1[0] == nullptr &&
+                      S.n_poles == 0 && S.n_poles_y == 0;
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1887,20 +1970,24 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         } else if (S.cond_d2[0] || S.cond_d2[1]) {
             return fail(MTB_INVALID_ARG, "structure %d: cond_d2 without cond_d1", s);
         }
-        if (S.n_poles < 0 || S.n_poles > MTB_MAX_POLES)
-            return fail(MTB_INVALID_ARG, "structure %d: n_poles %d outside [0, %d]", s,
-                        S.n_poles, MTB_MAX_POLES);
-        if (S.n_poles > 0) {
-            if (S.pol != MTB_TM)
-                return fail(MTB_UNSUPPORTED, "structure %d: poles are a TM option here", s);
+        for (int a = 0; a < 2; ++a) {
+            const int np = a ? S.n_poles_y : S.n_poles;
+            if (np < 0 || np > MTB_MAX_POLES)
+                return fail(MTB_INVALID_ARG, "structure %d: %d poles outside [0, %d]", s, np,
+                            MTB_MAX_POLES);
+            if (np == 0) continue;
+            if (a == 1 && S.pol != MTB_TE)
+                return fail(MTB_INVALID_ARG, "structure %d: n_poles_y is a TE field", s);
             if (variant != 2)
                 return fail(MTB_UNSUPPORTED, "structure %d: poles need the tile kernels "
                             "(variant 2)", s);
+            float *const *pp = a ? S.pol_py : S.pol_p;
+            const float *const *pc = a ? S.pol_cy : S.pol_c;
             for (int b = 0; b < 2; ++b)
-                if ((rc = check_ptr(S.pol_p[b], "pol_p", s))) return rc;
+                if ((rc = check_ptr(pp[b], "pole planes", s))) return rc;
             for (int k = 0; k < 3; ++k)
-                if ((rc = check_ptr(S.pol_c[k], "pol_c", s))) return rc;
-            if ((int64_t)S.n_poles * S.nx * S.pitch >= (1LL << 31))
+                if ((rc = check_ptr(pc[k], "pole coefficients", s))) return rc;
+            if ((int64_t)np * S.nx * S.pitch >= (1LL << 31))
                 return fail(MTB_UNSUPPORTED, "structure %d: pole planes too large", s);
         }
         if (S.pol == MTB_TE && (rc = check_ptr(S.inv_eps_b, "inv_eps_b", s))) return rc;
@@ -1962,7 +2049,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     p->n_cols = n_amp_cols;
     p->n_work = (int)n_work;
     for (int s = 0; s < n; ++s)
-        if (structs[s].cond_d1[0] || structs[s].n_poles > 0) p->ext = true;
+        if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0)
+            p->ext = true;
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->structs_d.ensure(sizeof(mtb_yee2d_struct) * n);
     if (!rc) rc = p->work_d.ensure(sizeof(int4) * n_work);
@@ -2379,7 +2467,8 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     if (!(S.dt > 0.f) || !(S.dx > 0.f)) return fail(MTB_INVALID_ARG, "noalloc: dt, dx must be > 0");
     if (S.pol == MTB_TE && (S.y_pmc || S.src_h2.n > 0))
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
-    if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles)
+    if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles ||
+        S.n_poles_y)
         return fail(MTB_UNSUPPORTED, "noalloc: conductivity and poles need the tile kernels");
     int rc;
     for (int b = 0; b < 2; ++b) {

@@ -174,7 +174,9 @@ class Engine2D:
         _need(main.device == self.device, "all structures of a batch must share one device")
         if it.te:
             it.nx, it.ny = main.shape[0] + 1, main.shape[1] + 1
-            _need(s.Px_cur.shape[0] == 0 and s.Py_cur.shape[0] == 0, "dispersive poles")
+            for n_, cn in ((s.Px_cur.shape[0], "c1x"), (s.Py_cur.shape[0], "c1y")):
+                _need(n_ <= L.MTB_MAX_POLES, f"{n_} dispersive poles (at most {L.MTB_MAX_POLES})")
+                _need(getattr(c, cn).shape[0] == n_, f"pole coefficients {cn} count")
             _opt_none(c, ["inv_xx_x", "c3xy", "c3yx", "has_chi2", "y_mirror_lo", "x_mirror_lo"])
             _inert_magnetic(c, [("hz1", "hz2")])
         else:
@@ -203,6 +205,19 @@ class Engine2D:
                                   L.ptr(box), nx, pitch, 1, pitch, 1, off[0], off[1], 0,
                                   self._sptr()), "pack")
         return box
+
+    def _pack_stack(self, t3, nx, pitch):
+        """A (n, r, c) stack of planes -> (n * nx, pitch) box planes, plane k at rows
+        k * nx (each plane in the box layout of an nx-row array)."""
+        n = t3.shape[0]
+        box = torch.zeros((n * nx, pitch), dtype=torch.float32, device=self.device)
+        for k in range(n):
+            box[k * nx:(k + 1) * nx].copy_(self._pack(t3[k], nx, pitch))
+        return box
+
+    def _unpack_stack(self, box, n, nx, shape):
+        return torch.stack([self._unpack(box[k * nx:(k + 1) * nx], shape) for k in range(n)]) \
+            if n else torch.zeros((0, *shape), dtype=torch.float32, device=self.device)
 
     def _pair(self, src, nx, pitch, off=(0, 0)):
         a = self._pack(src, nx, pitch, off)
@@ -287,6 +302,29 @@ class Engine2D:
                         self._pair(s.psi_Eyx, nx, P), self._pair(s.psi_Exy, nx, P)]
                 S.inv_eps_b = L.ptr(inv_b)
                 it.keep += [eps_b, inv_b]
+                # dispersive poles on Ex and Ey (core/stepper_te.py:136-175)
+                pol_bufs = {}
+                for ax, (pcur, pprev, cs) in enumerate(
+                        ((s.Px_cur, s.Px_prev, ("c1x", "c2x", "c3x")),
+                         (s.Py_cur, s.Py_prev, ("c1y", "c2y", "c3y")))):
+                    n_p = pcur.shape[0]
+                    if not n_p:
+                        continue
+                    pp = [self._pack_stack(pcur, nx, P), self._pack_stack(pprev, nx, P)]
+                    pc = [self._pack_stack(getattr(c, k), nx, P) for k in cs]
+                    if ax == 0:
+                        S.n_poles = n_p
+                        S.pol_p[0], S.pol_p[1] = L.ptr(pp[0]), L.ptr(pp[1])
+                        for k in range(3):
+                            S.pol_c[k] = L.ptr(pc[k])
+                    else:
+                        S.n_poles_y = n_p
+                        S.pol_py[0], S.pol_py[1] = L.ptr(pp[0]), L.ptr(pp[1])
+                        for k in range(3):
+                            S.pol_cy[k] = L.ptr(pc[k])
+                    pol_bufs["x" if ax == 0 else "y"] = pp
+                    it.keep += pp + pc
+                pol_bufs = pol_bufs or None
             else:
                 f_main, f_x, f_y = self._pair(s.Dz, nx, P), self._pair(s.Hx, nx, P), \
                     self._pair(s.Hy, nx, P)
@@ -322,7 +360,11 @@ class Engine2D:
                     it.keep.append(eex)
             it.box = dict(main=f_main, x=f_x, y=f_y, psi=psis, eps_a=eps_a, eps_b=eps_b)
             if pol_bufs is not None:
-                it.box["pol"] = pol_bufs
+                if te:
+                    for ax, bufs in pol_bufs.items():
+                        it.box["pol_" + ax] = bufs
+                else:
+                    it.box["pol"] = pol_bufs
             it.keep += [*f_main, *f_x, *f_y, eps_a] + [t for p in psis for t in p]
             S.f_main[0], S.f_main[1] = L.ptr(f_main[0]), L.ptr(f_main[1])
             S.f_x[0], S.f_x[1] = L.ptr(f_x[0]), L.ptr(f_x[1])
@@ -560,7 +602,8 @@ class Engine2D:
         for it in self.items:
             bufs = [*it.box["main"], *it.box["x"], *it.box["y"]] + \
                 [t for p in it.box["psi"] for t in p] + list(it.accs) + \
-                list(it.box.get("pol", []))
+                list(it.box.get("pol", [])) + list(it.box.get("pol_x", [])) + \
+                list(it.box.get("pol_y", []))
             for t in bufs:
                 n = t.numel()
                 L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
@@ -569,9 +612,9 @@ class Engine2D:
     def _live_buffers(self, b: int):
         """The buffers of structure b the next step reads: fields, then CPML memory."""
         it, cur = self.items[b], self.current
-        pol = it.box.get("pol")
+        pols = [it.box[k] for k in ("pol", "pol_x", "pol_y") if k in it.box]
         return [it.box["main"][cur], it.box["x"][cur], it.box["y"][cur]] + \
-            [p[cur] for p in it.box["psi"]] + ([pol[cur], pol[cur ^ 1]] if pol else [])
+            [p[cur] for p in it.box["psi"]] + [b for pol in pols for b in (pol[cur], pol[cur ^ 1])]
 
     def snapshot(self, b: int = 0):
         """Copy of structure b's live state (box layout) for restore()."""
@@ -620,11 +663,26 @@ class Engine2D:
             Hz = self._unpack(bx["main"][cur], (nx - 1, ny - 1))
             Dx = self._unpack(bx["x"][cur], (nx - 1, ny))
             Dy = self._unpack(bx["y"][cur], (nx, ny - 1))
-            Ex = self._unpack(bx["x"][cur], (nx - 1, ny), den=bx["eps_a"])
-            Ey = self._unpack(bx["y"][cur], (nx, ny - 1), den=bx["eps_b"])
+            pol = {}
+            if "pol_x" in bx:
+                n_p = s.Px_cur.shape[0]
+                pc = self._unpack_stack(bx["pol_x"][cur], n_p, nx, (nx - 1, ny))
+                pol.update(Px_cur=pc, Px_prev=self._unpack_stack(bx["pol_x"][cur ^ 1], n_p, nx,
+                                                                 (nx - 1, ny)))
+                Ex = (Dx - pc.sum(0)) / it.coeffs.eps_x.to(Dx)
+            else:
+                Ex = self._unpack(bx["x"][cur], (nx - 1, ny), den=bx["eps_a"])
+            if "pol_y" in bx:
+                n_p = s.Py_cur.shape[0]
+                pc = self._unpack_stack(bx["pol_y"][cur], n_p, nx, (nx, ny - 1))
+                pol.update(Py_cur=pc, Py_prev=self._unpack_stack(bx["pol_y"][cur ^ 1], n_p, nx,
+                                                                 (nx, ny - 1)))
+                Ey = (Dy - pc.sum(0)) / it.coeffs.eps_y.to(Dy)
+            else:
+                Ey = self._unpack(bx["y"][cur], (nx, ny - 1), den=bx["eps_b"])
             ps = bx["psi"]
             return s._replace(
-                Hz=Hz, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy,
+                Hz=Hz, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy, **pol,
                 psi_Hzy=self._unpack(ps[0][cur], (nx - 1, ny - 2), (0, 1)),
                 psi_Hzx=self._unpack(ps[1][cur], (nx - 2, ny - 1), (1, 0)),
                 psi_Eyx=self._unpack(ps[2][cur], (nx - 1, ny - 1)),

@@ -205,7 +205,8 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
 
 # ---------------------------------------------------------------- 2D TE
 
-def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None):
+def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None,
+              poles=(), pole_masks=None):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
@@ -230,6 +231,19 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
         sd = np.asarray(sigma, dtype=dtype)
         cond["d1x"], cond["d2x"] = _cond_pair(h * (sd[:-1, :] + sd[1:, :]), dt)
         cond["d1y"], cond["d2y"] = _cond_pair(h * (sd[:, :-1] + sd[:, 1:]), dt)
+    # shared ADE poles on both E axes, masks Yee-averaged (core/coeffs.py:109-131, :416-425)
+    for ax, shape in (("x", (nx - 1, ny)), ("y", (nx, ny - 1))):
+        n_p = len(poles)
+        c1, c2, c3 = (np.zeros((n_p,) + shape, dtype=dtype) for _ in range(3))
+        for k, pole in enumerate(poles):
+            cv1, cv2, cv3 = pole_recurrence(pole, dt)
+            m = (np.ones((nx, ny), dtype=dtype) if pole_masks is None
+                 else np.asarray(pole_masks[k], dtype=dtype))
+            mavg = h * (m[:-1, :] + m[1:, :]) if ax == "x" else h * (m[:, :-1] + m[:, 1:])
+            c1[k] = dtype.type(cv1)
+            c2[k] = dtype.type(cv2)
+            c3[k] = dtype.type(cv3) * mavg
+        cond.update({"c1" + ax: c1, "c2" + ax: c2, "c3" + ax: c3})
     return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, **cond,
                 eps_x=eps_x, eps_y=eps_y,
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
@@ -242,8 +256,11 @@ def te_state(c):
     """Zero TE state with the reference's shapes (core/stepper_te.py:27-49)."""
     nx, ny, dt = c["nx"], c["ny"], c["dtype"]
     z = lambda *s: np.zeros(s, dtype=dt)
+    npx, npy = c["c1x"].shape[0], c["c1y"].shape[0]
     return dict(Hz=z(nx - 1, ny - 1), Ex=z(nx - 1, ny), Ey=z(nx, ny - 1),
                 Dx=z(nx - 1, ny), Dy=z(nx, ny - 1),
+                Px_cur=z(npx, nx - 1, ny), Px_prev=z(npx, nx - 1, ny),
+                Py_cur=z(npy, nx, ny - 1), Py_prev=z(npy, nx, ny - 1),
                 psi_Eyx=z(nx - 1, ny - 1), psi_Exy=z(nx - 1, ny - 1),
                 psi_Hzy=z(nx - 1, ny - 2), psi_Hzx=z(nx - 2, ny - 1))
 
@@ -271,8 +288,18 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
         Dy = s["Dy"] - T(dt) * curl_y
         if mask_ey is not None:
             Dy = Dy - T(dt * amp) * mask_ey
-    Ex = Dx / c["eps_x"]
-    Ey = Dy / c["eps_y"]
+    pol = {}
+    if c["c1x"].shape[0] or c["c1y"].shape[0]:
+        # update_pols on the old E (core/stepper_te.py:136-146), update_eh(E) (:159-169)
+        Px = c["c1x"] * s["Px_cur"] + c["c2x"] * s["Px_prev"] + c["c3x"] * s["Ex"]
+        Py = c["c1y"] * s["Py_cur"] + c["c2y"] * s["Py_prev"] + c["c3y"] * s["Ey"]
+        pol = dict(Px_cur=Px, Px_prev=s["Px_cur"], Py_cur=Py, Py_prev=s["Py_cur"])
+        Ex = (Dx - Px.sum(0)) / c["eps_x"]
+        Ey = (Dy - Py.sum(0)) / c["eps_y"]
+    else:
+        pol = {k: s.get(k) for k in ("Px_cur", "Px_prev", "Py_cur", "Py_prev")}
+        Ex = Dx / c["eps_x"]
+        Ey = Dy / c["eps_y"]
     dEy_dx = (Ey[1:, :] - Ey[:-1, :]) / T(dx)
     dEx_dy = (Ex[:, 1:] - Ex[:, :-1]) / T(dx)
     psi_Eyx = c["b_hx"] * s["psi_Eyx"] + c["a_hx"] * dEy_dx
@@ -282,7 +309,7 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
     if hz_mask is not None:
         Hz_new = Hz_new - T(dt * amp_h) * hz_mask
     return dict(Hz=Hz_new, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy, psi_Eyx=psi_Eyx,
-                psi_Exy=psi_Exy, psi_Hzy=psi_Hzy, psi_Hzx=psi_Hzx)
+                psi_Exy=psi_Exy, psi_Hzy=psi_Hzy, psi_Hzx=psi_Hzx, **pol)
 
 
 # ---------------------------------------------------------------- sources

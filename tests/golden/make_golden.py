@@ -17,7 +17,7 @@ cases of the hot path through its own public functions:
 * d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
   and of ``run_te`` (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
-  ``make_golden.py sigma``) and the TM case with a Lorentz and a Drude pole
+  ``make_golden.py sigma``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
@@ -129,7 +129,7 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False):
     return out
 
 
-def te_case(prec, sigma=False):
+def te_case(prec, sigma=False, poles=False):
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -138,6 +138,9 @@ def te_case(prec, sigma=False):
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
     sig = sigma_map(nx, ny, 22) if sigma else None
     kw = {} if sig is None else {"sigma_d": torch.tensor(sig, dtype=DT[prec])}
+    pm = pole_masks(nx, ny) if poles else None
+    if poles:
+        kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
     m = build_te_coeffs(g, eps_inf=torch.tensor(eps, dtype=DT[prec]), npml=npml, **kw)
     prof = GaussianPulse(0.65, 0.4)
     src = LineSource(g, ix=12, j0=12, j1=28, profile=prof)
@@ -150,7 +153,7 @@ def te_case(prec, sigma=False):
     monx = FluxMonitorTE(g, freqs, ix=32, lo=9, hi=31)
     mony = FluxMonitorTEY(g, freqs, iy=30, lo=9, hi=35)
     dft = DFTFieldsMonitor(g, freqs, component="Hz")
-    s0 = init_te_state(g)
+    s0 = init_te_state(g, n_poles=len(POLES) if poles else 0)
     n = 300
     with torch.no_grad():
         st, (ax, ay, ad) = run_te(s0, m, n, source=_TESrc(), monitors=[monx, mony, dft])
@@ -162,6 +165,9 @@ def te_case(prec, sigma=False):
                mask=_np(_TESrc.mask))
     if sig is not None:
         out["sigma"] = sig
+    if poles:
+        out["poles"] = json.dumps(POLES)
+        out["pole_masks"] = np.stack(pm)
     for k in st._fields:
         v = getattr(st, k)
         if v is not None and v.numel():
@@ -385,6 +391,8 @@ def main():
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_tm_poles_{prec}.npz"),
                                 **tm_case(prec, poles=True))
+            np.savez_compressed(os.path.join(HERE, f"golden_te_poles_{prec}.npz"),
+                                **te_case(prec, poles=True))
         return
     if sys.argv[1:] == ["sigma"]:
         for prec in ("f64", "f32"):

@@ -151,6 +151,11 @@ def test_pole_coefficients_match_oracle():
     c = O.tm_coeffs(20, 24, 0.05, dtype=np.float32, poles=poles, pole_masks=masks)
     for k in ("c1", "c2", "c3"):
         np.testing.assert_array_equal(getattr(m, k).numpy(), c[k])
+    from meep_torch_b200.core.coeffs import build_te_coeffs
+    t = build_te_coeffs(g, poles=poles, pole_masks=[torch.from_numpy(x) for x in masks])
+    ct = O.te_coeffs(20, 24, 0.05, dtype=np.float32, poles=poles, pole_masks=masks)
+    for k in ("c1x", "c2x", "c3x", "c1y", "c2y", "c3y"):
+        np.testing.assert_allclose(getattr(t, k).numpy(), ct[k], rtol=2.5e-7, atol=0)
 
 
 def test_conductivity_coefficients_match_oracle():

@@ -99,7 +99,7 @@ def test_tm_reference_phase_mode():
         assert rel_l2(a.cpu().numpy(), g[key]) < TOL, key
 
 
-@pytest.mark.parametrize("case", ["te", "te_sigma"])
+@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles"])
 def test_te_matches_reference(case):
     from meep_torch_b200.core.coeffs import build_te_coeffs
     from meep_torch_b200.core.grid import Grid
@@ -111,8 +111,10 @@ def test_te_matches_reference(case):
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
     grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
     sig = g.get("sigma")
+    poles = json.loads(str(g["poles"])) if "poles" in g else ()
+    pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
     m = build_te_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
-                        npml=int(g["npml"]),
+                        npml=int(g["npml"]), poles=poles, pole_masks=pm,
                         sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32))
     src = TESource(LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]),
                               j1=int(g["src_j1"]),
@@ -123,13 +125,16 @@ def test_te_matches_reference(case):
     monx = FluxMonitorTE(grid, freqs, ix=ix, lo=xlo, hi=xhi)
     mony = FluxMonitorTEY(grid, freqs, iy=iy, lo=ylo, hi=yhi)
     dft = DFTFieldsMonitor(grid, freqs, "Hz")
-    st, accs = run_te(init_te_state(grid), m, int(g["n_steps"]), source=src,
-                      monitors=[monx, mony, dft])
+    st, accs = run_te(init_te_state(grid, n_poles=len(poles)), m, int(g["n_steps"]),
+                      source=src, monitors=[monx, mony, dft])
     fx, fy = monx.flux(accs[0], dx), mony.flux(accs[1], dx)
     e32, e64 = {}, {}
     for prec, errs in (("f32", e32), ("f64", e64)):
         gg = load_golden(f"{case}_{prec}")
-        for k in ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"):
+        names = ["Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"]
+        if "s_Px_cur" in gg:
+            names += ["Px_cur", "Px_prev", "Py_cur", "Py_prev"]
+        for k in names:
             errs[k] = rel_l2(getattr(st, k).cpu().numpy(), gg["s_" + k])
         for a, key in zip(accs, ("acc_x", "acc_y", "acc_dft")):
             errs[key] = rel_l2(a.cpu().numpy(), gg[key])
@@ -826,3 +831,51 @@ def test_poles_batched_tiles_match_oracle_from_random_state():
     eng.close()
     with pytest.raises(MtbUnsupported):
         Engine2D(items[:1], variant=1)
+
+
+def test_te_poles_batched_tiles_match_oracle_from_random_state():
+    """TE with Lorentz and Drude poles on both E axes in a batch that gets four rows per
+    warp, from random fields and polarisations, against the oracle (fields, CPML memory,
+    both P buffers of each axis)."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.engine2d import Engine2D
+    rng = np.random.default_rng(37)
+    n, npml, dx = 30, 8, 0.05
+    poles = [(0.7, 0.05, 1.5), (0.0, 0.1, 1.0, 0.9)]
+    items, refs = [], []
+    for q in range(60):
+        nx, ny = (300, 260) if q % 2 == 0 else (260, 300)
+        use = q % 3 != 2
+        eps = (1.0 + 3.0 * rng.random((nx, ny))).astype(np.float32)
+        masks = [(rng.random((nx, ny)) < 0.5).astype(np.float32) for _ in poles] if use else None
+        grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+        pl = poles if use else ()
+        c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32, poles=pl,
+                        pole_masks=masks)
+        so = O.te_state(c)
+        for k in ("Hz", "Dx", "Dy", "Px_cur", "Px_prev", "Py_cur", "Py_prev"):
+            so[k] = (0.1 if k.startswith("P") else 1.0) * \
+                rng.standard_normal(so[k].shape).astype(np.float32)
+        so["Ex"] = (so["Dx"] - so["Px_cur"].sum(0)) / c["eps_x"]
+        so["Ey"] = (so["Dy"] - so["Py_cur"].sum(0)) / c["eps_y"]
+        m = build_te_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml, poles=pl,
+                            pole_masks=None if masks is None else
+                            [torch.from_numpy(x) for x in masks])
+        s0 = init_te_state(grid, n_poles=len(pl))._replace(
+            **{k: torch.from_numpy(so[k]).to(dev())
+               for k in ("Hz", "Dx", "Dy", "Ex", "Ey", "Px_cur", "Px_prev", "Py_cur", "Py_prev")})
+        items.append((s0, m, None, []))
+        if q < 3:
+            refs.append(O.run_2d(O.te_step, so, c, n)[0])
+    eng = Engine2D(items)
+    eng.run(0, n)
+    for b, ref in enumerate(refs):
+        st = eng.state(b)
+        names = ["Hz", "Dx", "Dy", "Ex", "Ey", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"]
+        if b % 3 != 2:
+            names += ["Px_cur", "Px_prev", "Py_cur", "Py_prev"]
+        for k in names:
+            assert rel_l2(getattr(st, k).cpu().numpy(), ref[k]) < TOL, (b, k)
+    eng.close()

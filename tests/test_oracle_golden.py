@@ -78,8 +78,9 @@ def test_tm_oracle_matches_reference(case, prec):
 def run_te_oracle(g, prec):
     dt_np = NPD[prec]
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
+    poles = json.loads(str(g["poles"])) if "poles" in g else ()
     c = O.te_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
-                    sigma=g.get("sigma"))
+                    sigma=g.get("sigma"), poles=poles, pole_masks=g.get("pole_masks"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)[:, :-1]
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -96,13 +97,16 @@ def run_te_oracle(g, prec):
     return c, mask, s, acc
 
 
-@pytest.mark.parametrize("case", ["te", "te_sigma"])
+@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_te_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
     c, mask, s, acc = run_te_oracle(g, prec)
     np.testing.assert_allclose(mask, g["mask"], rtol=1e-7)
-    for k in ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"):
+    names = ["Hz", "Ex", "Ey", "Dx", "Dy", "psi_Eyx", "psi_Exy", "psi_Hzy", "psi_Hzx"]
+    if "s_Px_cur" in g:
+        names += ["Px_cur", "Px_prev", "Py_cur", "Py_prev"]
+    for k in names:
         assert rel_l2(s[k], g["s_" + k]) < TOL[prec], k
     for a, key in zip(acc, ("acc_x", "acc_y", "acc_dft")):
         assert rel_l2(a, g[key]) < TOL[prec], key
