@@ -154,18 +154,19 @@ typedef struct mtb_yee2d_struct {
     /* dispersive poles (ADE Lorentz / Drude; TM core/stepper_tm.py:203-231, TE
      * core/stepper_te.py:136-175): n_poles (<= MTB_MAX_POLES) planes of
      * nx x pitch floats each, plane k at k * nx * pitch, on TM Ez or TE Ex.
-     * pol_p[2] is a ping-pong pair: buffer `cur` holds P(n) and the other
-     * P(n-1), which the step overwrites with
-     *     P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n);
+     * pol_p[3] rotate: with s = mtb_yee2d_pole_slot(plan) (0 at creation, +1
+     * mod 3 per step), buffer s holds P(n), buffer (s+2)%3 P(n-1), and the step
+     * writes P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n) into buffer (s+1)%3 (three
+     * buffers, because TE recomputes its neighbours' P(n+1) from their P(n-1));
      * then E(n+1) = (D(n+1) - sum_k P_k(n+1)) / eps. pol_c = c1, c2, c3.
      * TE's Ey poles are the second set (n_poles_y, pol_py, pol_cy). Tile
      * kernels only (variant 2); the other variants and the adjoint return
      * MTB_UNSUPPORTED. */
     int32_t n_poles;
     int32_t n_poles_y;
-    float *pol_p[2];
+    float *pol_p[3];
     const float *pol_c[3];
-    float *pol_py[2];
+    float *pol_py[3];
     const float *pol_cy[3];
 } mtb_yee2d_struct;
 
@@ -238,6 +239,8 @@ int mtb_yee2d_run(mtb_yee2d_plan *plan, int64_t t0, int32_t k,
 
 /* Which buffer of every ping-pong pair holds the current state (0 or 1). */
 int32_t mtb_yee2d_current(const mtb_yee2d_plan *plan);
+/* The pole buffer holding P(n) now (mtb_yee2d_struct.pol_p / pol_py). */
+int32_t mtb_yee2d_pole_slot(const mtb_yee2d_plan *plan);
 
 /* Run ONE 2D structure k steps without allocating anything (no counterpart
  * in the reference). For callers that must not call cudaMalloc / cudaFree:

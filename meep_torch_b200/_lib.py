@@ -47,8 +47,8 @@ class Yee2DStruct(C.Structure):
                 ("lines", vp), ("n_lines", C.c_int32), ("xband", C.c_int32 * 4),
                 ("yband", C.c_int32 * 4), ("pad_", C.c_int32), ("ring_full", C.c_int64 * 3),
                 ("cond_d1", vp * 2), ("cond_d2", vp * 2),
-                ("n_poles", C.c_int32), ("n_poles_y", C.c_int32), ("pol_p", vp * 2),
-                ("pol_c", vp * 3), ("pol_py", vp * 2), ("pol_cy", vp * 3)]
+                ("n_poles", C.c_int32), ("n_poles_y", C.c_int32), ("pol_p", vp * 3),
+                ("pol_c", vp * 3), ("pol_py", vp * 3), ("pol_cy", vp * 3)]
 
 
 class PhaseGroup(C.Structure):
@@ -98,6 +98,7 @@ SIGNATURES = {
     "mtb_yee2d_run": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double),
                                 C.POINTER(C.c_double), vp]),
     "mtb_yee2d_current": (C.c_int32, [vp]),
+    "mtb_yee2d_pole_slot": (C.c_int32, [vp]),
     "mtb_yee2d_check": (C.c_int, [vp, vp]),
     "mtb_yee2d_run_noalloc": (C.c_int, [C.POINTER(Yee2DStruct), C.POINTER(DftRegion), C.c_int32,
                                         C.POINTER(PhaseGroup), C.c_int32, C.c_int64, C.c_int32,

@@ -44,6 +44,7 @@ struct Ctx2D {
     int par;                      // buffer holding the old state
     int first;                    // first step executed by the plan
     int wr;                       // tile kernels: rows per warp (1 or WROWS)
+    int pst;                      // pole buffer holding P(n) (0..2)
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -916,7 +917,7 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             // dispersive poles: Ez = (Dz - sum_k P_k) / eps (core/stepper_tm.py:220-224)
             float s0[4], s1[4], s2[4], sl = 0.f, sr = 0.f;
             zero4(s0); zero4(s1); zero4(s2);
-            const float *Pc = S.pol_p[par];
+            const float *Pc = S.pol_p[C.pst];
             const uint32_t pl = (uint32_t)nx * P;
 #pragma unroll 1
             for (int k = 0; k < (EXT ? S.n_poles : 0); ++k) {
@@ -1038,20 +1039,21 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
         p3[q] = vD[q] ? q3 : p3[q];
     }
     if (act && i >= S.src_e.row_lo && i <= S.src_e.row_hi) apply_cells(S.src_e, i, C.amp_e, jb, dzN);
-    // ADE update P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n) over the old buffer
+    // ADE update P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n) into the third buffer
     // (core/stepper_tm.py:203-207), then Ez = (Dz - sum_k P_k) / eps
     float psN[4];
     zero4(psN);
     if (EXT && S.n_poles > 0 && act) {
-        const float *Pc = S.pol_p[par];
-        float *Po = S.pol_p[par ^ 1];
+        const float *Pc = S.pol_p[C.pst];
+        const float *Pp = S.pol_p[(C.pst + 2) % 3];
+        float *Po = S.pol_p[(C.pst + 1) % 3];
         const uint32_t pl = (uint32_t)nx * P;
 #pragma unroll 1
         for (int k = 0; k < (EXT ? S.n_poles : 0); ++k) {
             const uint32_t o = k * pl + ro;
             float pc[4], pp[4], a1[4], a2[4], a3[4];
             ld4(Pc + o, pc);
-            ld4(Po + o, pp);
+            ld4(Pp + o, pp);
             ld4(S.pol_c[0] + o, a1);
             ld4(S.pol_c[1] + o, a2);
             ld4(S.pol_c[2] + o, a3);
@@ -1101,19 +1103,19 @@ __device__ __forceinline__ void pole_sum4(const float *Pc, int np, uint32_t pl, 
 }
 
 // ADE step of one float4 of a pole stack: P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n)
-// (core/stepper_tm.py:203-207, core/stepper_te.py:136-146), written over P(n-1)
-// when STORE (the owner of the cells), and sum_k P_k(n+1) into s.
+// (core/stepper_tm.py:203-207, core/stepper_te.py:136-146), written to the third
+// buffer when STORE (the owner of the cells), and sum_k P_k(n+1) into s.
 template <bool STORE>
-__device__ __forceinline__ void pole_step4(const float *Pc, float *Po, const float *const *c,
-                                           int np, uint32_t pl, uint32_t o,
-                                           const float (&e)[4], float (&s)[4]) {
+__device__ __forceinline__ void pole_step4(const float *Pc, const float *Pp, float *Po,
+                                           const float *const *c, int np, uint32_t pl,
+                                           uint32_t o, const float (&e)[4], float (&s)[4]) {
     zero4(s);
 #pragma unroll 1
     for (int k = 0; k < np; ++k) {
         const uint32_t ok = k * pl + o;
         float pc[4], pp[4], a1[4], a2[4], a3[4];
         ld4(Pc + ok, pc);
-        ld4(Po + ok, pp);
+        ld4(Pp + ok, pp);
         ld4(c[0] + ok, a1);
         ld4(c[1] + ok, a2);
         ld4(c[2] + ok, a3);
@@ -1255,10 +1257,11 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     const uint32_t pl = (uint32_t)nx * P;
     if (npx > 0 && act) {
         float sc[4], eo[4], sn[4];
-        pole_sum4(S.pol_p[par], npx, pl, ro, sc);
+        pole_sum4(S.pol_p[C.pst], npx, pl, ro, sc);
 #pragma unroll
         for (int q = 0; q < 4; ++q) eo[q] = (dx[q] - sc[q]) * ix[q];
-        pole_step4<true>(S.pol_p[par], S.pol_p[par ^ 1], S.pol_c, npx, pl, ro, eo, sn);
+        pole_step4<true>(S.pol_p[C.pst], S.pol_p[(C.pst + 2) % 3], S.pol_p[(C.pst + 1) % 3],
+                         S.pol_c, npx, pl, ro, eo, sn);
 #pragma unroll
         for (int q = 0; q < 4; ++q) ex[q] = hzRow ? (dxN[q] - sn[q]) * ix[q] : 0.f;
     }
@@ -1277,7 +1280,7 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
         }
         float sN = 0.f;
         if (npx > 0) {
-            const float *Pc = S.pol_p[par], *Pp = S.pol_p[par ^ 1];
+            const float *Pc = S.pol_p[C.pst], *Pp = S.pol_p[(C.pst + 2) % 3];
             float sc = 0.f;
             for (int k = 0; k < npx; ++k) sc += Pc[k * pl + ro + 4];
             const float eo = (dxr - sc) * ixr;
@@ -1299,18 +1302,19 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     }
     if (npy > 0 && act) {
         float sc[4], eo[4], sn[4];
-        pole_sum4(S.pol_py[par], npy, pl, ro, sc);
+        const float *Pc = S.pol_py[C.pst], *Pp = S.pol_py[(C.pst + 2) % 3];
+        float *Po = S.pol_py[(C.pst + 1) % 3];
+        pole_sum4(Pc, npy, pl, ro, sc);
 #pragma unroll
         for (int q = 0; q < 4; ++q) eo[q] = (dy[q] - sc[q]) * iy[q];
-        pole_step4<true>(S.pol_py[par], S.pol_py[par ^ 1], S.pol_cy, npy, pl, ro, eo, sn);
+        pole_step4<true>(Pc, Pp, Po, S.pol_cy, npy, pl, ro, eo, sn);
 #pragma unroll
         for (int q = 0; q < 4; ++q) ey[q] = (dyN[q] - sn[q]) * iy[q];
         if (i + 1 < nx) {
-            pole_sum4(S.pol_py[par], npy, pl, ro + P, sc);
+            pole_sum4(Pc, npy, pl, ro + P, sc);
 #pragma unroll
             for (int q = 0; q < 4; ++q) eo[q] = (dyn[q] - sc[q]) * iyn[q];
-            pole_step4<false>(S.pol_py[par], S.pol_py[par ^ 1], S.pol_cy, npy, pl, ro + P, eo,
-                              sn);
+            pole_step4<false>(Pc, Pp, Po, S.pol_cy, npy, pl, ro + P, eo, sn);
 #pragma unroll
             for (int q = 0; q < 4; ++q) eyn[q] = (dyNn[q] - sn[q]) * iyn[q];
         }
@@ -1831,6 +1835,8 @@ struct mtb_yee2d_plan {
     int variant = 2;                   // 1 row march, 2 tiles
     int wr = 1;                        // tiles: rows per warp
     bool ext = false;                  // a structure has conductivity or poles
+    bool poles = false;                // a structure has poles (no graph replay)
+    int pst = 0;                       // pole buffer holding P(n)
     int graph_mode = 0;                // 0 graphs when eligible, -1 off
     cudaStream_t cap = nullptr;        // private capture stream
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // ring flush graph per start parity
@@ -1983,7 +1989,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
                             "(variant 2)", s);
             float *const *pp = a ? S.pol_py : S.pol_p;
             const float *const *pc = a ? S.pol_cy : S.pol_c;
-            for (int b = 0; b < 2; ++b)
+            for (int b = 0; b < 3; ++b)
                 if ((rc = check_ptr(pp[b], "pole planes", s))) return rc;
             for (int k = 0; k < 3; ++k)
                 if ((rc = check_ptr(pc[k], "pole coefficients", s))) return rc;
@@ -2049,8 +2055,11 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     p->n_cols = n_amp_cols;
     p->n_work = (int)n_work;
     for (int s = 0; s < n; ++s)
+    {
         if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0)
             p->ext = true;
+        if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
+    }
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->structs_d.ensure(sizeof(mtb_yee2d_struct) * n);
     if (!rc) rc = p->work_d.ensure(sizeof(int4) * n_work);
@@ -2175,6 +2184,7 @@ static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
         C.par = par;
         C.first = 0;
         C.wr = p->wr;
+        C.pst = 0;                               // no poles in graph-replayed plans
         rc = launch_step(p, C, p->cap);
         par ^= 1;
     }
@@ -2228,7 +2238,8 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     const float *ad = p->amp_d.as<float>();
     const int G = p->dft.slots;
     const size_t prow = (size_t)p->dft.total_nf * 4;         // floats per phase row
-    const bool graphs = p->graph_mode >= 0 && !p->timer.on && G >= 2 && k >= G;
+    // graph replay keys on the start parity; the pole buffers rotate with period 3
+    const bool graphs = p->graph_mode >= 0 && !p->timer.on && G >= 2 && k >= G && !p->poles;
     if (graphs && (rc = p->stage_d.ensure(sizeof(float) * (2 * (size_t)G * nc + G * prow))))
         return rc;
     int slot = 0;
@@ -2262,10 +2273,12 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
         C.par = p->par;
         C.first = p->first;
         C.wr = p->wr;
+        C.pst = p->pst;
         if ((rc = p->timer.begin(st, 0))) return rc;
         if ((rc = launch_step(p, C, st))) return rc;
         if ((rc = p->timer.end(st))) return rc;
         p->par ^= 1;
+        p->pst = (p->pst + 1) % 3;
         p->first = 0;
         ++slot;
         if (slot == G || s == k - 1) {
@@ -2297,6 +2310,8 @@ int mtb_yee2d_timing(const mtb_yee2d_plan *p, double *step_ms, int64_t *step_lau
     if (dft_launches) *dft_launches = p->timer.count[1];
     return MTB_OK;
 }
+
+int32_t mtb_yee2d_pole_slot(const mtb_yee2d_plan *p) { return p ? p->pst : -1; }
 
 int32_t mtb_yee2d_current(const mtb_yee2d_plan *p) { return p ? p->par : -1; }
 
@@ -2677,6 +2692,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
             C.par = par;
             C.first = first ? 1 : 0;
             C.wr = 1;                              // unused by the row-march kernels
+            C.pst = 0;
             if (S.pol == MTB_TM) {
                 if (first)
                     k_yee2d_tm<true><<<blocks, 32 * WARPS2D, smem_tm(), st>>>(dS, dWork, n_work, C);

@@ -310,18 +310,19 @@ class Engine2D:
                     n_p = pcur.shape[0]
                     if not n_p:
                         continue
-                    pp = [self._pack_stack(pcur, nx, P), self._pack_stack(pprev, nx, P)]
+                    # three rotating buffers: P(n) in slot 0, P(n-1) in slot 2
+                    pp = [self._pack_stack(pcur, nx, P), None, self._pack_stack(pprev, nx, P)]
+                    pp[1] = torch.zeros_like(pp[0])
                     pc = [self._pack_stack(getattr(c, k), nx, P) for k in cs]
+                    for k in range(3):
+                        if ax == 0:
+                            S.pol_p[k], S.pol_c[k] = L.ptr(pp[k]), L.ptr(pc[k])
+                        else:
+                            S.pol_py[k], S.pol_cy[k] = L.ptr(pp[k]), L.ptr(pc[k])
                     if ax == 0:
                         S.n_poles = n_p
-                        S.pol_p[0], S.pol_p[1] = L.ptr(pp[0]), L.ptr(pp[1])
-                        for k in range(3):
-                            S.pol_c[k] = L.ptr(pc[k])
                     else:
                         S.n_poles_y = n_p
-                        S.pol_py[0], S.pol_py[1] = L.ptr(pp[0]), L.ptr(pp[1])
-                        for k in range(3):
-                            S.pol_cy[k] = L.ptr(pc[k])
                     pol_bufs["x" if ax == 0 else "y"] = pp
                     it.keep += pp + pc
                 pol_bufs = pol_bufs or None
@@ -340,13 +341,14 @@ class Engine2D:
                 S.n_poles = n_p
                 psum = 0.0
                 if n_p:
-                    pp = [self._pack(s.P_cur.reshape(n_p * nx, ny), n_p * nx, P),
+                    # three rotating buffers: P(n) in slot 0, P(n-1) in slot 2
+                    pp = [self._pack(s.P_cur.reshape(n_p * nx, ny), n_p * nx, P), None,
                           self._pack(s.P_prev.reshape(n_p * nx, ny), n_p * nx, P)]
+                    pp[1] = torch.zeros_like(pp[0])
                     pc = [self._pack(getattr(c, k).reshape(n_p * nx, ny), n_p * nx, P)
                           for k in ("c1", "c2", "c3")]
-                    S.pol_p[0], S.pol_p[1] = L.ptr(pp[0]), L.ptr(pp[1])
                     for k in range(3):
-                        S.pol_c[k] = L.ptr(pc[k])
+                        S.pol_p[k], S.pol_c[k] = L.ptr(pp[k]), L.ptr(pc[k])
                     pol_bufs = pp
                     it.keep += pp + pc
                     psum = s.P_cur.sum(0)
@@ -613,8 +615,10 @@ class Engine2D:
         """The buffers of structure b the next step reads: fields, then CPML memory."""
         it, cur = self.items[b], self.current
         pols = [it.box[k] for k in ("pol", "pol_x", "pol_y") if k in it.box]
+        ps = self.pole_slot
         return [it.box["main"][cur], it.box["x"][cur], it.box["y"][cur]] + \
-            [p[cur] for p in it.box["psi"]] + [b for pol in pols for b in (pol[cur], pol[cur ^ 1])]
+            [p[cur] for p in it.box["psi"]] + \
+            [b for pol in pols for b in (pol[ps], pol[(ps + 2) % 3])]
 
     def snapshot(self, b: int = 0):
         """Copy of structure b's live state (box layout) for restore()."""
@@ -638,6 +642,11 @@ class Engine2D:
     @property
     def current(self) -> int:
         return self.lib.mtb_yee2d_current(self.plan)
+
+    @property
+    def pole_slot(self) -> int:
+        """The pole buffer holding P(n) (three rotate; P(n-1) is two slots on)."""
+        return self.lib.mtb_yee2d_pole_slot(self.plan)
 
     # ---------------------------------------------------------------- export
     def _unpack(self, box, shape, off=(0, 0), den=None, den_off=None):
@@ -666,17 +675,19 @@ class Engine2D:
             pol = {}
             if "pol_x" in bx:
                 n_p = s.Px_cur.shape[0]
-                pc = self._unpack_stack(bx["pol_x"][cur], n_p, nx, (nx - 1, ny))
-                pol.update(Px_cur=pc, Px_prev=self._unpack_stack(bx["pol_x"][cur ^ 1], n_p, nx,
-                                                                 (nx - 1, ny)))
+                ps_ = self.pole_slot
+                pc = self._unpack_stack(bx["pol_x"][ps_], n_p, nx, (nx - 1, ny))
+                pol.update(Px_cur=pc, Px_prev=self._unpack_stack(bx["pol_x"][(ps_ + 2) % 3], n_p,
+                                                                 nx, (nx - 1, ny)))
                 Ex = (Dx - pc.sum(0)) / it.coeffs.eps_x.to(Dx)
             else:
                 Ex = self._unpack(bx["x"][cur], (nx - 1, ny), den=bx["eps_a"])
             if "pol_y" in bx:
                 n_p = s.Py_cur.shape[0]
-                pc = self._unpack_stack(bx["pol_y"][cur], n_p, nx, (nx, ny - 1))
-                pol.update(Py_cur=pc, Py_prev=self._unpack_stack(bx["pol_y"][cur ^ 1], n_p, nx,
-                                                                 (nx, ny - 1)))
+                ps_ = self.pole_slot
+                pc = self._unpack_stack(bx["pol_y"][ps_], n_p, nx, (nx, ny - 1))
+                pol.update(Py_cur=pc, Py_prev=self._unpack_stack(bx["pol_y"][(ps_ + 2) % 3], n_p,
+                                                                 nx, (nx, ny - 1)))
                 Ey = (Dy - pc.sum(0)) / it.coeffs.eps_y.to(Dy)
             else:
                 Ey = self._unpack(bx["y"][cur], (nx, ny - 1), den=bx["eps_b"])
@@ -691,8 +702,9 @@ class Engine2D:
         pol = {}
         if "pol" in bx:
             n_p = s.P_cur.shape[0]
-            pc = self._unpack(bx["pol"][cur], (n_p * nx, ny)).reshape(n_p, nx, ny)
-            pp = self._unpack(bx["pol"][cur ^ 1], (n_p * nx, ny)).reshape(n_p, nx, ny)
+            ps_ = self.pole_slot
+            pc = self._unpack(bx["pol"][ps_], (n_p * nx, ny)).reshape(n_p, nx, ny)
+            pp = self._unpack(bx["pol"][(ps_ + 2) % 3], (n_p * nx, ny)).reshape(n_p, nx, ny)
             pol = dict(P_cur=pc, P_prev=pp)
             Ez = (Dz - pc.sum(0)) / it.coeffs.eps_inf.to(Dz)
         else:
