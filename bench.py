@@ -181,6 +181,28 @@ def cpu_sample_cfg1(steps):
     return nx * ny * steps, time.perf_counter() - t0
 
 
+def cpu_sample_cfg3(steps, n=256):
+    """Oracle run of `steps` steps of the cfg3 grid (n^3, spheres, point source, six flux
+    faces), one thread. Returns (cell-updates, seconds)."""
+    import numpy as np
+
+    from meep_torch_b200 import workloads as W
+    from oracle import fdtd as O
+    f32 = np.float32
+    c = O.coeffs_3d(n, n, n, 1.0 / 16, eps=W.cfg3_eps(n), npml=16, dtype=f32)
+    dt = c["dt"]
+    prof = O.gaussian_pulse(0.5, 0.3)
+    freqs = np.linspace(0.35, 0.65, 20)
+    lo_, hi_ = 24 * n // 256, 232 * n // 256
+    mons = [(lambda a, i: (lambda st, t: O.flux3d_sample(st, t, dt, freqs, a, i,
+                                                         win=(lo_, hi_, lo_, hi_))))(
+        a, lo_ if i == 24 else hi_) for a, i in W.CFG3_FACES]
+    t0 = time.perf_counter()
+    O.run_3d(O.state_3d(c), c, steps, amp_fn=lambda t: prof(O.src_time(t, dt)),
+             src=("Ez", n // 2, n // 2, n // 2), monitors=mons)
+    return n ** 3 * steps, time.perf_counter() - t0
+
+
 # ------------------------------------------------------------------ GPU bench
 
 def run_cfg4(args, rank, world, dev):
@@ -836,6 +858,14 @@ def main():
                                     "cores": 1, "kind": "port",
                                     "sample": f"oracle (numpy float32) cfg1, the full 4000-step "
                                               f"run, one thread, {sec:.1f} s"}
+        elif args.workload == "cfg3":
+            n3s = 8
+            cells, sec = cpu_sample_cfg3(n3s, n=args.n3)
+            line["cpu_baseline"] = {"value": cells / sec / 1e9, "unit": "Gcell-updates/s",
+                                    "cores": 1, "kind": "port",
+                                    "sample": f"oracle (numpy float32) cfg3 {args.n3}^3 grid with "
+                                              f"its source and six flux faces, {n3s} steps, one "
+                                              f"thread, {sec:.1f} s"}
         else:
             line["cpu_baseline"] = cpu_baseline_line(args.cpu_structs, args.cpu_steps, threads)
     if rank == 0:
