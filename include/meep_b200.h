@@ -367,6 +367,12 @@ typedef struct mtb_yee3d_struct {
     const int64_t *plane_ring_off; /* device int64[n_planes]               */
     int32_t n_planes;
     int32_t pad2_;
+    /* conductive damping (core/stepper_3d.py:217-235 damp pairs from sigma_d /
+     * sigma_b, applied at :375-437): per component (Ex Ey Ez Hx Hy Hz) the pair
+     * (d1, d2) as box arrays, H' = d1 H - d2 curl E, E' = d1 E + d2 curl H / eps;
+     * all null = the plain step (d1 = 1, d2 = dt). Split kernels only; the
+     * fused kernel and the adjoint return MTB_UNSUPPORTED. */
+    const float *damp[6][2];
 } mtb_yee3d_struct;
 
 typedef struct mtb_yee3d_plan mtb_yee3d_plan;

@@ -76,7 +76,7 @@ class Yee3DStruct(C.Structure):
                 ("prof_b", (vp * 2) * 3), ("prof_a", (vp * 2) * 3),
                 ("src_comp", C.c_int32), ("src_is_point", C.c_int32), ("src", Cells),
                 ("planes", vp), ("plane_ring_off", vp), ("n_planes", C.c_int32),
-                ("pad2_", C.c_int32)]
+                ("pad2_", C.c_int32), ("damp", (vp * 2) * 6)]
 
 
 class Adj2DBuffers(C.Structure):

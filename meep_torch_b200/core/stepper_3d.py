@@ -60,10 +60,21 @@ def _axis_sides3(v):
     return (side_counts(v),) * 3
 
 
+def _avg3(v, axis):
+    a = [slice(None)] * 3
+    b = [slice(None)] * 3
+    a[axis] = slice(None, -1)
+    b[axis] = slice(1, None)
+    return 0.5 * (v[tuple(a)] + v[tuple(b)])
+
+
 def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
-                    dtype=torch.float32, device="cuda", **kw) -> Coeffs3D:
+                    dtype=torch.float32, device="cuda", sigma_d=None, sigma_b=None,
+                    **kw) -> Coeffs3D:
     """CPML coefficients: H-side profiles on the n-1 half nodes, E-side on the
-    interior [1:-1] of each axis (core/stepper_3d.py:192-206)."""
+    interior [1:-1] of each axis (core/stepper_3d.py:192-206); with ``sigma_d`` /
+    ``sigma_b`` ((nx, ny, nz) cell-centred), the damping pairs of :217-235 Yee-averaged
+    onto each component."""
     for k, v in kw.items():
         if v not in (None, 0, (), []):
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
@@ -80,9 +91,20 @@ def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
         cpml[kh] = (_bc(b, ax), _bc(a, ax), _bc(k, ax))
         b, a, k = cpml_profiles(dims[ax], npml_ax[ax], 0.0, dt, dx, dtype=dtype, device=device)
         cpml[ke] = (_bc(b[1:-1], ax), _bc(a[1:-1], ax), _bc(k[1:-1], ax))
-    one = torch.ones((), dtype=dtype, device=device)
-    d2 = torch.full((), dt, dtype=dtype, device=device)
-    damp = {c: (one, d2) for c in ("ex", "ey", "ez", "hx", "hy", "hz")}
+    if sigma_d is None and sigma_b is None:
+        one = torch.ones((), dtype=dtype, device=device)
+        d2 = torch.full((), dt, dtype=dtype, device=device)
+        damp = {c: (one, d2) for c in ("ex", "ey", "ez", "hx", "hy", "hz")}
+    else:
+        zero = torch.zeros(nx, ny, nz, dtype=dtype, device=device)
+        sd = sigma_d.to(dtype=dtype, device=device) if sigma_d is not None else zero
+        sb = sigma_b.to(dtype=dtype, device=device) if sigma_b is not None else zero
+
+        def dpair(sg):
+            return (1 - sg * dt / 2) / (1 + sg * dt / 2), dt / (1 + sg * dt / 2)
+        damp = {"ex": dpair(_avg3(sd, 0)), "ey": dpair(_avg3(sd, 1)), "ez": dpair(_avg3(sd, 2)),
+                "hx": dpair(_avg3(_avg3(sb, 1), 2)), "hy": dpair(_avg3(_avg3(sb, 0), 2)),
+                "hz": dpair(_avg3(_avg3(sb, 0), 1))}
     return Coeffs3D(dt=dt, dx=dx, eps=e, damp=damp, cpml=cpml)
 
 

@@ -450,6 +450,7 @@ struct Split3 {
     int nx, ny, nz, zp;
     float dt, rdx;
     Band3 B;
+    const float *dmp[6][2];     // conductive damping (d1, d2) per component, or null
 };
 
 __device__ __forceinline__ void ldg4v(const float *p, float (&v)[4]) {
@@ -458,7 +459,8 @@ __device__ __forceinline__ void ldg4v(const float *p, float (&v)[4]) {
 }
 __device__ __forceinline__ void one4(float (&v)[4]) { v[0] = v[1] = v[2] = v[3] = 1.f; }
 
-// H(n+1/2) from E(n): core/stepper_3d.py:367-393
+// H(n+1/2) from E(n): core/stepper_3d.py:367-393; DAMP: H' = d1 H - d2 curl
+template <bool DAMP>
 __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_constant__ Split3 P,
                                                              int i0) {
     const int nx = P.nx, ny = P.ny, nz = P.nz, ZP = P.zp;
@@ -509,6 +511,14 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
         if (lane != 31) { eyk = t0; exk = t1; }
     }
     if (!act) return;
+    float a1[3][4], a2[3][4];
+    if (DAMP) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ldg4v(P.dmp[3 + c][0] + g, a1[c]);
+            ldg4v(P.dmp[3 + c][1] + g, a2[c]);
+        }
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const bool vz = kb + q <= nz - 2, vzE = kb + q < nz;
@@ -519,7 +529,8 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
             const float dy = (ezj[q] - ez[q]) * rdx, dz = (eyn - ey[q]) * rdx;
             const float qy = hyb * p0[q] + hya * dy, qz = hzb[q] * p1[q] + hza[q] * dz;
             const bool v = vyH && vz;
-            const float hn = hx[q] - dt * ((dy + qy) - (dz + qz));
+            const float cu = (dy + qy) - (dz + qz);
+            const float hn = DAMP ? a1[0][q] * hx[q] - a2[0][q] * cu : hx[q] - dt * cu;
             hx[q] = v ? hn : hx[q];
             p0[q] = v ? qy : p0[q];
             p1[q] = v ? qz : p1[q];
@@ -529,7 +540,8 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
             const float dz = (exn - ex[q]) * rdx, dx = (ezi[q] - ez[q]) * rdx;
             const float qz = hzb[q] * p2[q] + hza[q] * dz, qx = hxb * p3[q] + hxa * dx;
             const bool v = xok && vz;
-            const float hn = hy[q] - dt * ((dz + qz) - (dx + qx));
+            const float cu = (dz + qz) - (dx + qx);
+            const float hn = DAMP ? a1[1][q] * hy[q] - a2[1][q] * cu : hy[q] - dt * cu;
             hy[q] = v ? hn : hy[q];
             p2[q] = v ? qz : p2[q];
             p3[q] = v ? qx : p3[q];
@@ -539,7 +551,8 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
             const float dx = (eyi[q] - ey[q]) * rdx, dy = (exj[q] - ex[q]) * rdx;
             const float qx = hxb * p4[q] + hxa * dx, qy = hyb * p5[q] + hya * dy;
             const bool v = xok && vyH && vzE;
-            const float hn = hz[q] - dt * ((dx + qx) - (dy + qy));
+            const float cu = (dx + qx) - (dy + qy);
+            const float hn = DAMP ? a1[2][q] * hz[q] - a2[2][q] * cu : hz[q] - dt * cu;
             hz[q] = v ? hn : hz[q];
             p4[q] = v ? qx : p4[q];
             p5[q] = v ? qy : p5[q];
@@ -562,6 +575,7 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
 // the curl is applied (_pad_interior). E(n+1) = E(n) + dt curl / eps_c with a
 // fast (2 ulp) divide; the reference's (E eps + dt curl) / eps differs by
 // rounding only.
+template <bool DAMP>
 __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_constant__ Split3 P,
                                                              const float *__restrict__ amp, int i0) {
     const int nx = P.nx, ny = P.ny, nz = P.nz, ZP = P.zp;
@@ -631,6 +645,15 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
         if (lane != 31) epk = t2;
     }
     if (!act) return;
+    // conductive damping: E' = d1 E + d2 curl / eps (core/stepper_3d.py:405-437)
+    float a1[3][4], a2[3][4];
+    if (DAMP) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ldg4v(P.dmp[c][0] + g, a1[c]);
+            ldg4v(P.dmp[c][1] + g, a2[c]);
+        }
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int k = kb + q;
@@ -644,7 +667,9 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             const bool v = xok && vzE;
             const float curl = (jin && kin) ? (dy + qy) - (dz + qz) : 0.f;
             const float ec = 0.5f * (ep[q] + epi[q]);
-            en[0][q] = v ? en[0][q] + __fdividef(dt * curl, ec) : en[0][q];
+            en[0][q] = v ? (DAMP ? a1[0][q] * en[0][q] + __fdividef(a2[0][q] * curl, ec)
+                                 : en[0][q] + __fdividef(dt * curl, ec))
+                         : en[0][q];
             p6[q] = v ? qy : p6[q];
             p7[q] = v ? qz : p7[q];
         }
@@ -655,7 +680,9 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             const bool v = vyH && vzE;
             const float curl = (iin && kin) ? (dz + qz) - (dx + qx) : 0.f;
             const float ec = 0.5f * (ep[q] + epj[q]);
-            en[1][q] = v ? en[1][q] + __fdividef(dt * curl, ec) : en[1][q];
+            en[1][q] = v ? (DAMP ? a1[1][q] * en[1][q] + __fdividef(a2[1][q] * curl, ec)
+                                 : en[1][q] + __fdividef(dt * curl, ec))
+                         : en[1][q];
             p8[q] = v ? qz : p8[q];
             p9[q] = v ? qx : p9[q];
         }
@@ -665,7 +692,9 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             const float qx = exb * p10[q] + exa * dx, qy = eyb * p11[q] + eya * dy;
             const float curl = (iin && jin) ? (dx + qx) - (dy + qy) : 0.f;
             const float ec = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
-            en[2][q] = vz ? en[2][q] + __fdividef(dt * curl, ec) : en[2][q];
+            en[2][q] = vz ? (DAMP ? a1[2][q] * en[2][q] + __fdividef(a2[2][q] * curl, ec)
+                                  : en[2][q] + __fdividef(dt * curl, ec))
+                          : en[2][q];
             p10[q] = vz ? qx : p10[q];
             p11[q] = vz ? qy : p11[q];
         }
@@ -744,6 +773,7 @@ struct mtb_yee3d_plan {
     Band3 band{};
     Split3 sp[2]{};                // split-kernel parameters of parity 0 and 1
     int slab = 0;                  // split kernels: x planes per H / E launch pair
+    bool damp = false;             // conductive damping arrays given
     int own_lo = 0, own_hi = 0;    // split kernels: x planes this plan updates
     // chunk staged by mtb_yee3d_begin: k steps from t0, next step c_s, next
     // half c_half (0 H, 1 E), ring slot c_slot
@@ -840,6 +870,18 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     }
     if (S.n_planes < 0 || (S.n_planes > 0 && (!S.planes || !S.plane_ring_off)))
         return fail(MTB_INVALID_ARG, "bad plane sample list");
+    int n_damp = 0;
+    for (int c = 0; c < 6; ++c)
+        for (int h = 0; h < 2; ++h) {
+            if (!S.damp[c][h]) continue;
+            ++n_damp;
+            if (reinterpret_cast<uintptr_t>(S.damp[c][h]) & 15)
+                return fail(MTB_INVALID_ARG, "damping array %d/%d not 16-byte aligned", c, h);
+        }
+    if (n_damp != 0 && n_damp != 12)
+        return fail(MTB_INVALID_ARG, "damping: give all 12 (d1, d2) arrays or none");
+    if (n_damp && variant == 1)
+        return fail(MTB_UNSUPPORTED, "conductive damping needs the split kernels");
     mtb_yee3d_plan *p = new mtb_yee3d_plan();
     p->s = S;
     p->rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
@@ -849,6 +891,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     p->slab = (tuning && tuning->rows_per_warp > 0) ? std::min(tuning->rows_per_warp, S.nx) : S.nx;
     p->own_lo = 0;
     p->own_hi = S.nx;
+    p->damp = n_damp == 12;
     const int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     p->nzw = (S.zpitch + 127) / 128;
     p->smem = sizeof(float) * (size_t)(S.zpitch + 4) * (4 * (TY3 + 2) + 3 * (TY3 + 1));
@@ -893,6 +936,8 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
             q.dt = S.dt;
             q.rdx = 1.0f / S.dx;
             q.B = p->band;
+            for (int c = 0; c < 6; ++c)
+                for (int h = 0; h < 2; ++h) q.dmp[c][h] = S.damp[c][h];
         }
     }
     if (!rc && variant == 1) {
@@ -968,9 +1013,16 @@ static int launch_split(mtb_yee3d_plan *p, int part, int i0, int i1, int s, cuda
     const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, i1 - i0);
     const dim3 block(32, SPLIT_Y);
     if (part == 0)
-        k_yee3d_h<<<grid, block, 0, st>>>(p->sp[p->par], i0);
+        if (p->damp)
+            k_yee3d_h<true><<<grid, block, 0, st>>>(p->sp[p->par], i0);
+        else
+            k_yee3d_h<false><<<grid, block, 0, st>>>(p->sp[p->par], i0);
     else
-        k_yee3d_e<<<grid, block, 0, st>>>(p->sp[p->par], p->amp_d.as<float>() + s, i0);
+        if (p->damp)
+            k_yee3d_e<true><<<grid, block, 0, st>>>(p->sp[p->par], p->amp_d.as<float>() + s, i0);
+        else
+            k_yee3d_e<false><<<grid, block, 0, st>>>(p->sp[p->par], p->amp_d.as<float>() + s,
+                                                     i0);
     MTB_CHECK_LAUNCH();
     ++p->last_launches;
     return MTB_OK;

@@ -78,9 +78,14 @@ class Engine3D:
         _need(getattr(coeffs, "cpml", None) is not None, "matched-sigma absorber mode")
         _need(getattr(coeffs, "pols", None) is None, "dispersive poles")
         _need(not getattr(coeffs, "pmc", ()), "PMC walls")
-        for key, (d1, d2) in coeffs.damp.items():
-            _need(bool(torch.all(d1 == 1)), f"conductivity (damp[{key}] d1 != 1)")
-            _need(bool(torch.all(d2 == d2.reshape(-1)[0])), f"conductivity (damp[{key}] d2)")
+        # conductive damping (core/stepper_3d.py:217-235): the plain step when every pair
+        # is (1, dt), else the split kernels' damped form with the 12 arrays
+        dtf = torch.tensor(float(coeffs.dt), dtype=torch.float32)
+        self._damp = None
+        if any(not (bool(torch.all(d1 == 1)) and
+                    bool(torch.all(d2.to(torch.float32) == dtf.to(d2.device))))
+               for d1, d2 in coeffs.damp.values()):
+            self._damp = {k: coeffs.damp[k] for k in ("ex", "ey", "ez", "hx", "hy", "hz")}
         self.phase_mode = PHASE_MODES[phase_mode]
         S = L.Yee3DStruct()
         S.nx, S.ny, S.nz, S.zpitch = nx, ny, nz, zp
@@ -113,6 +118,14 @@ class Engine3D:
             S.prof_b[ax][1], S.prof_a[ax][1] = L.ptr(eb), L.ptr(ea)
             self.keep += [hb, ha, eb, ea]
         self._check_psi(g, cp)
+        if self._damp is not None:
+            shapes_ = field_shapes(nx, ny, nz)
+            for q, comp in enumerate(FIELDS):
+                for h, v in enumerate(self._damp[comp.lower()]):
+                    v = torch.as_tensor(v, dtype=torch.float32, device=self.device)
+                    box = self._pack(v.expand(shapes_[comp]).contiguous())
+                    self.keep.append(box)
+                    S.damp[q][h] = L.ptr(box)
         # ---- source
         self.source = source
         if source is not None:

@@ -439,7 +439,8 @@ def _bc(v, ax):
     return v.reshape(sh)
 
 
-def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64):
+def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
+              sigma_b=None):
     """3D CPML coefficient set (core/stepper_3d.py:150-266, CPML path, no
     conductivity, no poles). dt = 0.5 dx / sqrt(3). H-side profiles on the
     n-1 half nodes, E-side on the interior [1:-1]."""
@@ -455,10 +456,21 @@ def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64):
         cp[kh] = (_bc(b, ax), _bc(a, ax), _bc(k, ax))
         b, a, k = cpml_profiles(n, npml, 0.0, dt, dx, dtype=dtype)
         cp[ke] = (_bc(b[1:-1], ax), _bc(a[1:-1], ax), _bc(k[1:-1], ax))
-    # sigma = 0: damping pair (1, dt) (core/stepper_3d.py:241-251)
-    one = dtype.type((1 - 0.0) / (1 + 0.0))
-    d2 = dtype.type(dt / (1 + 0.0))
-    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, d1=one, d2=d2)
+    # damping pairs (core/stepper_3d.py:217-235): (1, dt) without conductivity, else
+    # (1 - s dt/2)/(1 + s dt/2), dt/(1 + s dt/2) with sigma_d Yee-averaged onto each E
+    # component and sigma_b onto each H component
+    if sigma_d is None and sigma_b is None:
+        one, d2 = dtype.type(1.0), dtype.type(dt)
+        damp = {k: (one, d2) for k in ("ex", "ey", "ez", "hx", "hy", "hz")}
+    else:
+        z = np.zeros((nx, ny, nz), dtype=dtype)
+        sd = z if sigma_d is None else np.asarray(sigma_d, dtype=dtype)
+        sb = z if sigma_b is None else np.asarray(sigma_b, dtype=dtype)
+        pair = lambda sg: ((1 - sg * dt / 2) / (1 + sg * dt / 2), dt / (1 + sg * dt / 2))  # noqa: E731
+        damp = {"ex": pair(_avg(sd, 0)), "ey": pair(_avg(sd, 1)), "ez": pair(_avg(sd, 2)),
+                "hx": pair(_avg(_avg(sb, 1), 2)), "hy": pair(_avg(_avg(sb, 0), 2)),
+                "hz": pair(_avg(_avg(sb, 0), 1))}
+    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, damp=damp)
 
 
 def state_3d(c):
@@ -510,17 +522,17 @@ def step_3d(s, c, amp=0.0, src=None, point_sign=+1.0):
 def step_3d_h(s, c):
     """H(n+1/2) and the H-side CPML memory of step_3d (core/stepper_3d.py:367-393)."""
     ce = _ce3(c)
-    d1, d2 = c["d1"], c["d2"]
+    dm = c["damp"]
     out = {}
     ce_y, out["psi_Ez_y"] = ce(s["Ez"], 1, "hy", s["psi_Ez_y"])
     ce_z, out["psi_Ey_z"] = ce(s["Ey"], 2, "hz", s["psi_Ey_z"])
-    Hx = d1 * s["Hx"] - d2 * (ce_y - ce_z)
+    Hx = dm["hx"][0] * s["Hx"] - dm["hx"][1] * (ce_y - ce_z)
     ce_z2, out["psi_Ex_z"] = ce(s["Ex"], 2, "hz", s["psi_Ex_z"])
     ce_x, out["psi_Ez_x"] = ce(s["Ez"], 0, "hx", s["psi_Ez_x"])
-    Hy = d1 * s["Hy"] - d2 * (ce_z2 - ce_x)
+    Hy = dm["hy"][0] * s["Hy"] - dm["hy"][1] * (ce_z2 - ce_x)
     ce_x2, out["psi_Ey_x"] = ce(s["Ey"], 0, "hx", s["psi_Ey_x"])
     ce_y2, out["psi_Ex_y"] = ce(s["Ex"], 1, "hy", s["psi_Ex_y"])
-    Hz = d1 * s["Hz"] - d2 * (ce_x2 - ce_y2)
+    Hz = dm["hz"][0] * s["Hz"] - dm["hz"][1] * (ce_x2 - ce_y2)
     out.update(Hx=Hx, Hy=Hy, Hz=Hz)
     return out
 
@@ -529,7 +541,7 @@ def step_3d_e(s, c, h, amp=0.0, src=None, point_sign=+1.0):
     """E(n+1), the E-side CPML memory and the soft source of step_3d
     (core/stepper_3d.py:395-482) from the state ``s`` and H(n+1/2) in ``h``."""
     ce = _ce3(c)
-    d1, d2 = c["d1"], c["d2"]
+    dm = c["damp"]
     T = c["dtype"].type
     Hx, Hy, Hz = h["Hx"], h["Hy"], h["Hz"]
     out = {}
@@ -538,17 +550,17 @@ def step_3d_e(s, c, h, amp=0.0, src=None, point_sign=+1.0):
     ch_y, out["psi_Hz_y"] = ce(Hz, 1, "ey", s["psi_Hz_y"])
     ch_z, out["psi_Hy_z"] = ce(Hy, 2, "ez", s["psi_Hy_z"])
     curl_x = _pad_interior(ch_y[:, :, 1:-1] - ch_z[:, 1:-1, :], (1, 2))
-    Ex = (d1 * s["Ex"] * eps_x + d2 * curl_x) / eps_x
+    Ex = (dm["ex"][0] * s["Ex"] * eps_x + dm["ex"][1] * curl_x) / eps_x
     eps_y = _avg(eps, 1)
     ch_z2, out["psi_Hx_z"] = ce(Hx, 2, "ez", s["psi_Hx_z"])
     ch_x, out["psi_Hz_x"] = ce(Hz, 0, "ex", s["psi_Hz_x"])
     curl_y = _pad_interior(ch_z2[1:-1, :, :] - ch_x[:, :, 1:-1], (0, 2))
-    Ey = (d1 * s["Ey"] * eps_y + d2 * curl_y) / eps_y
+    Ey = (dm["ey"][0] * s["Ey"] * eps_y + dm["ey"][1] * curl_y) / eps_y
     eps_z = _avg(eps, 2)
     ch_x2, out["psi_Hy_x"] = ce(Hy, 0, "ex", s["psi_Hy_x"])
     ch_y2, out["psi_Hx_y"] = ce(Hx, 1, "ey", s["psi_Hx_y"])
     curl_z = _pad_interior(ch_x2[:, 1:-1, :] - ch_y2[1:-1, :, :], (0, 1))
-    Ez = (d1 * s["Ez"] * eps_z + d2 * curl_z) / eps_z
+    Ez = (dm["ez"][0] * s["Ez"] * eps_z + dm["ez"][1] * curl_z) / eps_z
     out.update(Ex=Ex, Ey=Ey, Ez=Ez)
     if src is not None and amp != 0.0:
         comp = src[0]

@@ -18,7 +18,8 @@ cases of the hot path through its own public functions:
   and of ``run_te`` (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and the TM and TE cases with a Lorentz and a Drude pole
-  (``make_golden.py poles``)
+  (``make_golden.py poles``); the 3D case with sigma_d and sigma_b
+  (``make_golden.py sigma3d``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -178,7 +179,7 @@ def te_case(prec, sigma=False, poles=False):
 FACES = [("x", 5), ("x", 18), ("y", 5), ("y", 16), ("z", 5), ("z", 14)]
 
 
-def case_3d(prec, lean=False):
+def case_3d(prec, lean=False, sigma=False):
     rng = np.random.default_rng(13)
     nx, ny, nz, dx, npml = 24, 22, 20, 1.0 / 16, 4
     eps = np.ones((nx, ny, nz))
@@ -203,7 +204,15 @@ def case_3d(prec, lean=False):
         view, accs = run_3d_lean(c, n, source=src, monitors=mons)
         st = {k: getattr(view, k) for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
     else:
-        c = build_3d_coeffs(nx, ny, nz, dx, eps=epst, npml=npml, dtype=DT[prec])
+        kw = {}
+        if sigma:                                     # lossy slab (E) and a lossy patch (H)
+            sd = np.zeros((nx, ny, nz))
+            sd[14:18] = 2.0
+            sb = np.zeros((nx, ny, nz))
+            sb[6:10, 6:12, 8:14] = 3.0
+            kw = dict(sigma_d=torch.tensor(sd, dtype=DT[prec]),
+                      sigma_b=torch.tensor(sb, dtype=DT[prec]))
+        c = build_3d_coeffs(nx, ny, nz, dx, eps=epst, npml=npml, dtype=DT[prec], **kw)
         src = PointSource3D(c.dt, "Ez", *src_ijk, prof)
         mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=i, win=win, dtype=DT[prec])
                 for a, i in FACES]
@@ -214,6 +223,8 @@ def case_3d(prec, lean=False):
     out = dict(nx=nx, ny=ny, nz=nz, dx=dx, npml=npml, n_steps=n, eps=eps,
                freqs=np.array(freqs), fcen=0.5, fwidth=0.3, src=np.array(src_ijk),
                faces=json.dumps(FACES), win=np.array(win))
+    if sigma:
+        out["sigma_d"], out["sigma_b"] = sd, sb
     for k, v in st.items():
         out["s_" + k] = _np(v)
     for i, (a, mon) in enumerate(zip(accs, mons)):
@@ -387,6 +398,11 @@ def grad_te_case(prec):
 
 
 def main():
+    if sys.argv[1:] == ["sigma3d"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_3d_sigma_{prec}.npz"),
+                                **case_3d(prec, sigma=True))
+        return
     if sys.argv[1:] == ["poles"]:
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_tm_poles_{prec}.npz"),

@@ -145,12 +145,12 @@ def test_te_matches_reference(case):
     assert not bad, bad
 
 
-def _run3d(lean, variant=0):
+def _run3d(lean, variant=0, case=None):
     from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D, run_3d
     from meep_torch_b200.core.sources import GaussianPulse
     from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
     from meep_torch_b200.core.stepper_3d_lean import build_lean, run_3d_lean
-    g = load_golden("3d_lean_f32" if lean else "3d_f32")
+    g = load_golden(f"{case}_f32" if case else ("3d_lean_f32" if lean else "3d_f32"))
     nx, ny, nz, dx, npml = (int(g["nx"]), int(g["ny"]), int(g["nz"]), float(g["dx"]),
                             int(g["npml"]))
     eps = torch.tensor(g["eps"], dtype=torch.float32)
@@ -163,7 +163,11 @@ def _run3d(lean, variant=0):
         c = build_lean(nx, ny, nz, dx, eps, npml, device=dev())
         dt = c.dt
     else:
-        c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, device=dev())
+        kw = {}
+        if "sigma_d" in g:
+            kw = dict(sigma_d=torch.tensor(g["sigma_d"], dtype=torch.float32),
+                      sigma_b=torch.tensor(g["sigma_b"], dtype=torch.float32))
+        c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, device=dev(), **kw)
         dt = c.dt
     src = PointSource3D(dt, "Ez", i, j, k, prof)
     mons = [FluxMonitor3D(dt, freqs, normal=a, idx=idx, win=win) for a, idx in faces]
@@ -178,11 +182,13 @@ def _run3d(lean, variant=0):
     return st, accs, mons, dx
 
 
-@pytest.mark.parametrize("variant", [1, 2])
-@pytest.mark.parametrize("lean", [False, True])
-def test_3d_matches_reference(lean, variant):
-    st, accs, mons, dx = _run3d(lean, variant)
-    name = "3d_lean" if lean else "3d"
+@pytest.mark.parametrize("variant,lean,case", [(1, False, None), (2, False, None),
+                                                (1, True, None), (2, True, None),
+                                                (2, False, "3d_sigma")])
+def test_3d_matches_reference(lean, variant, case):
+    """3D golden cases; 3d_sigma adds conductive damping (sigma_d on E, sigma_b on H)."""
+    st, accs, mons, dx = _run3d(lean, variant, case)
+    name = case or ("3d_lean" if lean else "3d")
     e32, e64 = {}, {}
     for prec, errs in (("f32", e32), ("f64", e64)):
         g = load_golden(f"{name}_{prec}")
@@ -879,3 +885,21 @@ def test_te_poles_batched_tiles_match_oracle_from_random_state():
         for k in names:
             assert rel_l2(getattr(st, k).cpu().numpy(), ref[k]) < TOL, (b, k)
     eng.close()
+
+
+def test_3d_damping_refused_by_fused_kernel_and_adjoint():
+    """Conductive damping runs on the split kernels only; the fused x-march and the 3D
+    adjoint refuse it with MTB_UNSUPPORTED."""
+    from meep_torch_b200._lib import MtbUnsupported
+    from meep_torch_b200.core.adjoint3d import run_3d_adjoint
+    from meep_torch_b200.core.monitors_3d import run_3d
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    n = 12
+    sd = torch.zeros(n, n, n)
+    sd[4:8] = 1.0
+    c = build_3d_coeffs(n, n, n, 0.0625, npml=3, device=dev(), sigma_d=sd)
+    s0 = init_3d_state(n, n, n, npml=3, device=dev())
+    with pytest.raises(MtbUnsupported):
+        run_3d(s0, c, 2, variant=1)
+    with pytest.raises(MtbUnsupported):
+        run_3d_adjoint(c, 4, 2, None, [], lambda accs: torch.zeros(()), s0)

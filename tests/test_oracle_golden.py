@@ -117,7 +117,8 @@ def test_te_oracle_matches_reference(case, prec):
 def run_3d_oracle(g, prec, lean=False):
     dt_np = NPD[prec]
     nx, ny, nz, dx = int(g["nx"]), int(g["ny"]), int(g["nz"]), float(g["dx"])
-    c = O.coeffs_3d(nx, ny, nz, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np)
+    c = O.coeffs_3d(nx, ny, nz, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
+                    sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"))
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
     dt = c["dt"]
     freqs = g["freqs"]
@@ -132,9 +133,10 @@ def run_3d_oracle(g, prec, lean=False):
     return c, s, acc
 
 
+@pytest.mark.parametrize("case", ["3d", "3d_sigma"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_3d_oracle_matches_reference(prec):
-    g = load_golden(f"3d_{prec}")
+def test_3d_oracle_matches_reference(case, prec):
+    g = load_golden(f"{case}_{prec}")
     c, s, acc = run_3d_oracle(g, prec)
     for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "psi_Ez_y", "psi_Hx_y", "psi_Hz_x"):
         assert rel_l2(s[k], g["s_" + k]) < TOL[prec], k
