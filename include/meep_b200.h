@@ -373,6 +373,18 @@ typedef struct mtb_yee3d_struct {
      * all null = the plain step (d1 = 1, d2 = dt). Split kernels only; the
      * fused kernel and the adjoint return MTB_UNSUPPORTED. */
     const float *damp[6][2];
+    /* dispersive poles (core/stepper_3d.py:236-300; the functional stepper's
+     * folded-D update): n_poles (<= MTB_MAX_POLES) box planes per E component
+     * (Ex Ey Ez), plane k at k * nx * ny * zpitch. pol_p[c][2] ping-pong with the
+     * fields: buffer `cur` P(n), the other P(n-1), overwritten with
+     * P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n); c1, c2 per pole (host values),
+     * c3 per cell. Split kernels only. */
+    int32_t n_poles;
+    int32_t pad3_;
+    float *pol_p[3][2];
+    const float *pol_c3[3];
+    float pol_c1[MTB_MAX_POLES];
+    float pol_c2[MTB_MAX_POLES];
 } mtb_yee3d_struct;
 
 typedef struct mtb_yee3d_plan mtb_yee3d_plan;

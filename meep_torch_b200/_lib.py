@@ -76,7 +76,9 @@ class Yee3DStruct(C.Structure):
                 ("prof_b", (vp * 2) * 3), ("prof_a", (vp * 2) * 3),
                 ("src_comp", C.c_int32), ("src_is_point", C.c_int32), ("src", Cells),
                 ("planes", vp), ("plane_ring_off", vp), ("n_planes", C.c_int32),
-                ("pad2_", C.c_int32), ("damp", (vp * 2) * 6)]
+                ("pad2_", C.c_int32), ("damp", (vp * 2) * 6),
+                ("n_poles", C.c_int32), ("pad3_", C.c_int32), ("pol_p", (vp * 2) * 3),
+                ("pol_c3", vp * 3), ("pol_c1", C.c_float * 8), ("pol_c2", C.c_float * 8)]
 
 
 class Adj2DBuffers(C.Structure):

@@ -70,11 +70,11 @@ def _avg3(v, axis):
 
 def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
                     dtype=torch.float32, device="cuda", sigma_d=None, sigma_b=None,
-                    **kw) -> Coeffs3D:
+                    poles=(), pole_masks=None, **kw) -> Coeffs3D:
     """CPML coefficients: H-side profiles on the n-1 half nodes, E-side on the
     interior [1:-1] of each axis (core/stepper_3d.py:192-206); with ``sigma_d`` /
     ``sigma_b`` ((nx, ny, nz) cell-centred), the damping pairs of :217-235 Yee-averaged
-    onto each component."""
+    onto each component; with ``poles`` / ``pole_masks`` the ADE stacks of :236-266."""
     for k, v in kw.items():
         if v not in (None, 0, (), []):
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
@@ -105,13 +105,29 @@ def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
         damp = {"ex": dpair(_avg3(sd, 0)), "ey": dpair(_avg3(sd, 1)), "ez": dpair(_avg3(sd, 2)),
                 "hx": dpair(_avg3(_avg3(sb, 1), 2)), "hy": dpair(_avg3(_avg3(sb, 0), 2)),
                 "hz": dpair(_avg3(_avg3(sb, 0), 1))}
-    return Coeffs3D(dt=dt, dx=dx, eps=e, damp=damp, cpml=cpml)
+    pols = None
+    if len(poles):
+        from .coeffs import _pole_recurrence
+        pols = {}
+        for key, shape, ax in (("x", (nx - 1, ny, nz), 0), ("y", (nx, ny - 1, nz), 1),
+                               ("z", (nx, ny, nz - 1), 2)):
+            npl = len(poles)
+            c3 = torch.zeros(npl, *shape, dtype=dtype, device=device)
+            vs = []
+            for q, pole in enumerate(poles):
+                v1, v2, v3 = _pole_recurrence(pole, dt)
+                m = (pole_masks[q] if pole_masks is not None else
+                     torch.ones(nx, ny, nz, dtype=dtype, device=device))
+                c3[q] = v3 * _avg3(m.to(dtype=dtype, device=device), ax)
+                vs.append((v1, v2))
+            c1 = torch.tensor([v[0] for v in vs], dtype=dtype, device=device).reshape(npl, 1, 1, 1)
+            c2 = torch.tensor([v[1] for v in vs], dtype=dtype, device=device).reshape(npl, 1, 1, 1)
+            pols[key] = (c1, c2, c3)
+    return Coeffs3D(dt=dt, dx=dx, eps=e, damp=damp, cpml=cpml, pols=pols)
 
 
 def init_3d_state(nx: int, ny: int, nz: int, npml: int = 0, n_poles: int = 0,
                   dtype=torch.float32, device="cuda") -> State3D:
-    if n_poles:
-        raise NotImplementedError("dispersive poles: not implemented on the B200 path")
     z = lambda *s: torch.zeros(*s, dtype=dtype, device=device)
     psi = {}
     if npml > 0:
@@ -122,6 +138,11 @@ def init_3d_state(nx: int, ny: int, nz: int, npml: int = 0, n_poles: int = 0,
             psi_Hz_y=z(nx - 1, ny - 2, nz), psi_Hy_z=z(nx - 1, ny, nz - 2),
             psi_Hx_z=z(nx, ny - 1, nz - 2), psi_Hz_x=z(nx - 2, ny - 1, nz),
             psi_Hy_x=z(nx - 2, ny, nz - 1), psi_Hx_y=z(nx, ny - 2, nz - 1))
+    if n_poles:
+        psi.update(
+            Px_cur=z(n_poles, nx - 1, ny, nz), Px_prev=z(n_poles, nx - 1, ny, nz),
+            Py_cur=z(n_poles, nx, ny - 1, nz), Py_prev=z(n_poles, nx, ny - 1, nz),
+            Pz_cur=z(n_poles, nx, ny, nz - 1), Pz_prev=z(n_poles, nx, ny, nz - 1))
     return State3D(z(nx - 1, ny, nz), z(nx, ny - 1, nz), z(nx, ny, nz - 1),
                    z(nx, ny - 1, nz - 1), z(nx - 1, ny, nz - 1), z(nx - 1, ny - 1, nz), **psi)
 

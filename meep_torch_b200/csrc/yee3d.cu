@@ -451,6 +451,13 @@ struct Split3 {
     float dt, rdx;
     Band3 B;
     const float *dmp[6][2];     // conductive damping (d1, d2) per component, or null
+    // dispersive poles: per E component a stack of np box planes (plane floats apart),
+    // P ping-pong with the fields, c3 per cell, c1 / c2 per pole
+    float *pp[3][2];
+    const float *pc3[3];
+    float pc1[MTB_MAX_POLES], pc2[MTB_MAX_POLES];
+    int np;
+    uint32_t plane;
 };
 
 __device__ __forceinline__ void ldg4v(const float *p, float (&v)[4]) {
@@ -575,9 +582,10 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
 // the curl is applied (_pad_interior). E(n+1) = E(n) + dt curl / eps_c with a
 // fast (2 ulp) divide; the reference's (E eps + dt curl) / eps differs by
 // rounding only.
-template <bool DAMP>
+template <int MODE>                 // bit 0: damping, bit 1: poles
 __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_constant__ Split3 P,
                                                              const float *__restrict__ amp, int i0) {
+    constexpr bool DAMP = (MODE & 1) != 0, PL = (MODE & 2) != 0;
     const int nx = P.nx, ny = P.ny, nz = P.nz, ZP = P.zp;
     const int lane = threadIdx.x;
     const int j = blockIdx.y * SPLIT_Y + threadIdx.y;
@@ -654,6 +662,33 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             ldg4v(P.dmp[c][1] + g, a2[c]);
         }
     }
+    // dispersive poles (core/stepper_3d.py:295-300, :312-325): P(n+1) = c1 P(n) +
+    // c2 P(n-1) + c3 E(n) over the P(n-1) buffer, and the sums of P(n), P(n+1) that the
+    // folded-D update E(n+1) = (d1 (eps E + sum P(n)) + d2 curl - sum P(n+1)) / eps needs
+    float spc[3][4], spn[3][4];
+    if (PL) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            z4(spc[c]);
+            z4(spn[c]);
+#pragma unroll 1
+            for (int k = 0; k < P.np; ++k) {
+                const uint32_t o = k * P.plane + g;
+                float pc[4], pq[4], c3[4];
+                ld4v(P.pp[c][0] + o, pc);
+                ld4v(P.pp[c][1] + o, pq);
+                ldg4v(P.pc3[c] + o, c3);
+                const float c1 = P.pc1[k], c2 = P.pc2[k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    spc[c][q] += pc[q];
+                    pq[q] = c1 * pc[q] + c2 * pq[q] + c3[q] * en[c][q];
+                    spn[c][q] += pq[q];
+                }
+                st4v(P.pp[c][1] + o, pq);
+            }
+        }
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int k = kb + q;
@@ -667,8 +702,12 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             const bool v = xok && vzE;
             const float curl = (jin && kin) ? (dy + qy) - (dz + qz) : 0.f;
             const float ec = 0.5f * (ep[q] + epi[q]);
-            en[0][q] = v ? (DAMP ? a1[0][q] * en[0][q] + __fdividef(a2[0][q] * curl, ec)
-                                 : en[0][q] + __fdividef(dt * curl, ec))
+            en[0][q] = v ? (PL ? (DAMP ? __fdividef(a1[0][q] * (en[0][q] * ec + spc[0][q]) +
+                                                      a2[0][q] * curl - spn[0][q], ec)
+                                       : en[0][q] + __fdividef(dt * curl + spc[0][q] - spn[0][q],
+                                                               ec))
+                                 : DAMP ? a1[0][q] * en[0][q] + __fdividef(a2[0][q] * curl, ec)
+                                        : en[0][q] + __fdividef(dt * curl, ec))
                          : en[0][q];
             p6[q] = v ? qy : p6[q];
             p7[q] = v ? qz : p7[q];
@@ -680,8 +719,12 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             const bool v = vyH && vzE;
             const float curl = (iin && kin) ? (dz + qz) - (dx + qx) : 0.f;
             const float ec = 0.5f * (ep[q] + epj[q]);
-            en[1][q] = v ? (DAMP ? a1[1][q] * en[1][q] + __fdividef(a2[1][q] * curl, ec)
-                                 : en[1][q] + __fdividef(dt * curl, ec))
+            en[1][q] = v ? (PL ? (DAMP ? __fdividef(a1[1][q] * (en[1][q] * ec + spc[1][q]) +
+                                                      a2[1][q] * curl - spn[1][q], ec)
+                                       : en[1][q] + __fdividef(dt * curl + spc[1][q] - spn[1][q],
+                                                               ec))
+                                 : DAMP ? a1[1][q] * en[1][q] + __fdividef(a2[1][q] * curl, ec)
+                                        : en[1][q] + __fdividef(dt * curl, ec))
                          : en[1][q];
             p8[q] = v ? qz : p8[q];
             p9[q] = v ? qx : p9[q];
@@ -692,8 +735,12 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
             const float qx = exb * p10[q] + exa * dx, qy = eyb * p11[q] + eya * dy;
             const float curl = (iin && jin) ? (dx + qx) - (dy + qy) : 0.f;
             const float ec = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
-            en[2][q] = vz ? (DAMP ? a1[2][q] * en[2][q] + __fdividef(a2[2][q] * curl, ec)
-                                  : en[2][q] + __fdividef(dt * curl, ec))
+            en[2][q] = vz ? (PL ? (DAMP ? __fdividef(a1[2][q] * (en[2][q] * ec + spc[2][q]) +
+                                                       a2[2][q] * curl - spn[2][q], ec)
+                                        : en[2][q] + __fdividef(dt * curl + spc[2][q] - spn[2][q],
+                                                                ec))
+                                  : DAMP ? a1[2][q] * en[2][q] + __fdividef(a2[2][q] * curl, ec)
+                                         : en[2][q] + __fdividef(dt * curl, ec))
                           : en[2][q];
             p10[q] = vz ? qx : p10[q];
             p11[q] = vz ? qy : p11[q];
@@ -774,6 +821,7 @@ struct mtb_yee3d_plan {
     Split3 sp[2]{};                // split-kernel parameters of parity 0 and 1
     int slab = 0;                  // split kernels: x planes per H / E launch pair
     bool damp = false;             // conductive damping arrays given
+    bool poles = false;            // dispersive pole stacks given
     int own_lo = 0, own_hi = 0;    // split kernels: x planes this plan updates
     // chunk staged by mtb_yee3d_begin: k steps from t0, next step c_s, next
     // half c_half (0 H, 1 E), ring slot c_slot
@@ -882,6 +930,20 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
         return fail(MTB_INVALID_ARG, "damping: give all 12 (d1, d2) arrays or none");
     if (n_damp && variant == 1)
         return fail(MTB_UNSUPPORTED, "conductive damping needs the split kernels");
+    if (S.n_poles < 0 || S.n_poles > MTB_MAX_POLES)
+        return fail(MTB_INVALID_ARG, "n_poles %d outside [0, %d]", S.n_poles, MTB_MAX_POLES);
+    if (S.n_poles > 0) {
+        if (variant == 1) return fail(MTB_UNSUPPORTED, "poles need the split kernels");
+        for (int c = 0; c < 3; ++c) {
+            for (int b = 0; b < 2; ++b)
+                if (!S.pol_p[c][b] || (reinterpret_cast<uintptr_t>(S.pol_p[c][b]) & 15))
+                    return fail(MTB_INVALID_ARG, "pole buffer %d/%d null or misaligned", c, b);
+            if (!S.pol_c3[c] || (reinterpret_cast<uintptr_t>(S.pol_c3[c]) & 15))
+                return fail(MTB_INVALID_ARG, "pole c3 %d null or misaligned", c);
+        }
+        if ((int64_t)S.n_poles * S.nx * S.ny * S.zpitch >= (1LL << 31))
+            return fail(MTB_UNSUPPORTED, "pole stacks too large");
+    }
     mtb_yee3d_plan *p = new mtb_yee3d_plan();
     p->s = S;
     p->rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
@@ -892,6 +954,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     p->own_lo = 0;
     p->own_hi = S.nx;
     p->damp = n_damp == 12;
+    p->poles = S.n_poles > 0;
     const int slots = (tuning && tuning->ring_slots > 0) ? tuning->ring_slots : 32;
     p->nzw = (S.zpitch + 127) / 128;
     p->smem = sizeof(float) * (size_t)(S.zpitch + 4) * (4 * (TY3 + 2) + 3 * (TY3 + 1));
@@ -938,6 +1001,17 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
             q.B = p->band;
             for (int c = 0; c < 6; ++c)
                 for (int h = 0; h < 2; ++h) q.dmp[c][h] = S.damp[c][h];
+            q.np = S.n_poles;
+            q.plane = (uint32_t)((int64_t)S.nx * S.ny * S.zpitch);
+            for (int c = 0; c < 3; ++c) {
+                q.pp[c][0] = S.pol_p[c][par];
+                q.pp[c][1] = S.pol_p[c][par ^ 1];
+                q.pc3[c] = S.pol_c3[c];
+            }
+            for (int k = 0; k < MTB_MAX_POLES; ++k) {
+                q.pc1[k] = k < S.n_poles ? S.pol_c1[k] : 0.f;
+                q.pc2[k] = k < S.n_poles ? S.pol_c2[k] : 0.f;
+            }
         }
     }
     if (!rc && variant == 1) {
@@ -1012,17 +1086,20 @@ static int launch_split(mtb_yee3d_plan *p, int part, int i0, int i1, int s, cuda
     if (i1 <= i0) return MTB_OK;
     const dim3 grid((p->s.zpitch + 127) / 128, (p->s.ny + SPLIT_Y - 1) / SPLIT_Y, i1 - i0);
     const dim3 block(32, SPLIT_Y);
-    if (part == 0)
+    if (part == 0) {
         if (p->damp)
             k_yee3d_h<true><<<grid, block, 0, st>>>(p->sp[p->par], i0);
         else
             k_yee3d_h<false><<<grid, block, 0, st>>>(p->sp[p->par], i0);
-    else
-        if (p->damp)
-            k_yee3d_e<true><<<grid, block, 0, st>>>(p->sp[p->par], p->amp_d.as<float>() + s, i0);
-        else
-            k_yee3d_e<false><<<grid, block, 0, st>>>(p->sp[p->par], p->amp_d.as<float>() + s,
-                                                     i0);
+    } else {
+        const float *a = p->amp_d.as<float>() + s;
+        switch ((p->damp ? 1 : 0) | (p->poles ? 2 : 0)) {
+            case 0: k_yee3d_e<0><<<grid, block, 0, st>>>(p->sp[p->par], a, i0); break;
+            case 1: k_yee3d_e<1><<<grid, block, 0, st>>>(p->sp[p->par], a, i0); break;
+            case 2: k_yee3d_e<2><<<grid, block, 0, st>>>(p->sp[p->par], a, i0); break;
+            default: k_yee3d_e<3><<<grid, block, 0, st>>>(p->sp[p->par], a, i0); break;
+        }
+    }
     MTB_CHECK_LAUNCH();
     ++p->last_launches;
     return MTB_OK;

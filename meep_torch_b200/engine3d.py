@@ -19,6 +19,7 @@ from .engine2d import PHASE_MODES, _need, _round4, coef_table
 FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 PSI = ("psi_Ez_y", "psi_Ey_z", "psi_Ex_z", "psi_Ez_x", "psi_Ey_x", "psi_Ex_y",
        "psi_Hz_y", "psi_Hy_z", "psi_Hx_z", "psi_Hz_x", "psi_Hy_x", "psi_Hx_y")
+POLES = ("Px_cur", "Px_prev", "Py_cur", "Py_prev", "Pz_cur", "Pz_prev")
 # box offset of each psi array: the E-side ones cover the interior of
 # their derivative axis (core/stepper_3d.py:52-57)
 PSI_OFF = ((0, 0, 0),) * 6 + ((0, 1, 0), (0, 0, 1), (0, 0, 1), (1, 0, 0), (1, 0, 0), (0, 1, 0))
@@ -63,7 +64,7 @@ class Engine3D:
         self.keep = []
         self.state_in = state
         g = state if isinstance(state, dict) else {k: getattr(state, k, None)
-                                                    for k in FIELDS + PSI}
+                                                    for k in FIELDS + PSI + POLES}
         Ex = g["Ex"]
         _need(isinstance(Ex, torch.Tensor) and Ex.is_cuda, "3D state must be CUDA tensors")
         _need(Ex.dtype == torch.float32, f"3D state dtype {Ex.dtype}: float32 only")
@@ -76,7 +77,9 @@ class Engine3D:
             _need(tuple(g[k].shape) == shapes[k], f"{k} shape {tuple(g[k].shape)}")
         _need(all(g.get(k) is not None for k in PSI), "3D CPML memory (npml > 0) required")
         _need(getattr(coeffs, "cpml", None) is not None, "matched-sigma absorber mode")
-        _need(getattr(coeffs, "pols", None) is None, "dispersive poles")
+        pols = getattr(coeffs, "pols", None)
+        n_p = 0 if pols is None else int(pols["x"][2].shape[0])
+        _need(n_p <= L.MTB_MAX_POLES, f"{n_p} dispersive poles (at most {L.MTB_MAX_POLES})")
         _need(not getattr(coeffs, "pmc", ()), "PMC walls")
         # conductive damping (core/stepper_3d.py:217-235): the plain step when every pair
         # is (1, dt), else the split kernels' damped form with the 12 arrays
@@ -118,6 +121,28 @@ class Engine3D:
             S.prof_b[ax][1], S.prof_a[ax][1] = L.ptr(eb), L.ptr(ea)
             self.keep += [hb, ha, eb, ea]
         self._check_psi(g, cp)
+        # dispersive poles (core/stepper_3d.py:236-300): P stacks ping-pong with the fields
+        self.n_poles = n_p
+        if n_p:
+            shapes_ = field_shapes(nx, ny, nz)
+            S.n_poles = n_p
+            self.pol_box = {}
+            for ci, key in enumerate("xyz"):
+                comp = "E" + key
+                cur = g.get(f"P{key}_cur")
+                prev = g.get(f"P{key}_prev")
+                _need(cur is not None and tuple(cur.shape) == (n_p,) + shapes_[comp],
+                      f"P{key}_cur shape")
+                bufs = [self._pack_stack(cur), self._pack_stack(prev)]
+                c3 = self._pack_stack(pols[key][2])
+                self.pol_box[key] = bufs
+                self.keep += bufs + [c3]
+                S.pol_p[ci][0], S.pol_p[ci][1] = L.ptr(bufs[0]), L.ptr(bufs[1])
+                S.pol_c3[ci] = L.ptr(c3)
+            c1 = pols["x"][0].reshape(-1).tolist()
+            c2 = pols["x"][1].reshape(-1).tolist()
+            for k in range(n_p):
+                S.pol_c1[k], S.pol_c2[k] = float(c1[k]), float(c2[k])
         if self._damp is not None:
             shapes_ = field_shapes(nx, ny, nz)
             for q, comp in enumerate(FIELDS):
@@ -235,6 +260,15 @@ class Engine3D:
                                   self._sptr()), "pack")
         return box
 
+    def _pack_stack(self, t4):
+        """(n, ...) component stack -> (n * nx, ny, zpitch) box planes."""
+        n = t4.shape[0]
+        out = torch.zeros((n * self.nx, self.ny, self.zp), dtype=torch.float32,
+                          device=self.device)
+        for k in range(n):
+            out[k * self.nx:(k + 1) * self.nx].copy_(self._pack(t4[k]))
+        return out
+
     def _pair(self, src, off=(0, 0, 0)):
         a = self._pack(src, off)
         return [a, a.clone()]
@@ -348,7 +382,8 @@ class Engine3D:
 
     def reset(self):
         """Zero every field, CPML and accumulator buffer (t = 0 again)."""
-        bufs = [t for p in self.box.values() for t in p] + list(self.accs)
+        bufs = [t for p in self.box.values() for t in p] + list(self.accs) + \
+            [t for p in getattr(self, "pol_box", {}).values() for t in p]
         for t in bufs:
             n = t.numel()
             L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
@@ -399,6 +434,15 @@ class Engine3D:
                       (nx, ny - 2, nz - 1)]
         for q, k in enumerate(PSI):
             out[k] = self._unpack(self.box[k][cur], psi_shapes[q], PSI_OFF[q])
+        if self.n_poles:
+            nxb = self.nx
+            for key in "xyz":
+                shp = shapes["E" + key]
+                for name, b in (("cur", cur), ("prev", cur ^ 1)):
+                    box = self.pol_box[key][b]
+                    out[f"P{key}_{name}"] = torch.stack(
+                        [self._unpack(box[k * nxb:(k + 1) * nxb], shp)
+                         for k in range(self.n_poles)])
         return out
 
     def _unpack(self, box, shape, off=(0, 0, 0)):

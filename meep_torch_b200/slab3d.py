@@ -25,6 +25,7 @@ from __future__ import annotations
 import copy
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 from .engine3d import FIELDS, PSI, PSI_OFF, field_shapes, flux_window
@@ -92,10 +93,26 @@ def _copy(x):
     return x.clone() if isinstance(x, torch.Tensor) else x.copy()
 
 
+def _stack(parts, like):
+    return torch.stack(parts) if isinstance(like, torch.Tensor) else np.stack(parts)
+
+
+def _slice_any(k, v, sl: Slab):
+    """Rows of a state array; a pole stack (P*: one plane per pole) along its dim 1."""
+    if v is None:
+        return None
+    if k.startswith("P"):
+        if v.shape[0] == 0:
+            return _copy(v[:, sl.lo: sl.hi - (sl.nx - v.shape[1])])
+        return _stack([_copy(_rows(p, sl.nx, sl)) for p in v], v)
+    return _copy(_rows(v, sl.nx, sl))
+
+
 def slice_state(state, sl: Slab):
-    """The slab's part of a State3D (or dict): every array cropped to planes [lo, hi)."""
+    """The slab's part of a State3D (or dict): every array cropped to planes [lo, hi)
+    (pole stacks along their x axis, dim 1)."""
     g = state if isinstance(state, dict) else state._asdict()
-    out = {k: (None if v is None else _copy(_rows(v, sl.nx, sl))) for k, v in g.items()}
+    out = {k: _slice_any(k, v, sl) for k, v in g.items()}
     return out if isinstance(state, dict) else type(state)(**out)
 
 
@@ -110,6 +127,10 @@ def slice_coeffs(coeffs, sl: Slab):
     out = dict(g)
     out["cpml"] = cp
     out["eps"] = g["eps"][sl.lo: sl.hi]
+    pols = g.get("pols")
+    if isinstance(pols, dict):                           # c3 stacks along their dim 1
+        out["pols"] = {k: (c1, c2, _stack([_rows(p, nx, sl) for p in c3], c3))
+                       for k, (c1, c2, c3) in pols.items()}
     damp = g.get("damp")
     if isinstance(damp, dict):
         out["damp"] = {k: tuple(_rows(v, nx, sl) if getattr(v, "ndim", 0) == 3 else v
@@ -327,10 +348,11 @@ def owned_rows(state, sl: Slab):
     g = state if isinstance(state, dict) else state._asdict()
     out = {}
     for k, v in g.items():
-        if v is None or k not in X_OFF:
+        pole = k.startswith("P") and v is not None and v.ndim == 4
+        if v is None or (k not in X_OFF and not pole):
             continue
-        c = sl.nx_local - v.shape[0]                        # x extent nx - c
-        o = X_OFF[k]
+        c = sl.nx_local - v.shape[1 if pole else 0]         # x extent nx - c
+        o = 0 if pole else X_OFF[k]
         r0 = max(sl.x0 - o, 0)
         r1 = min(sl.x1 - o, sl.nx - c)
         out[k] = (r0, max(0, r1 - r0))
@@ -347,7 +369,9 @@ def assemble_state(state_like, slabs, local_states):
     for sl, ls in zip(slabs, local_states):
         lg = ls if isinstance(ls, dict) else ls._asdict()
         for k, (r0, n) in owned_rows(ls, sl).items():
-            if n > 0:
+            if n > 0 and k.startswith("P") and lg[k].ndim == 4:
+                out[k][:, r0: r0 + n] = lg[k][:, r0 - sl.lo: r0 - sl.lo + n]
+            elif n > 0:
                 out[k][r0: r0 + n] = lg[k][r0 - sl.lo: r0 - sl.lo + n]
     return out if isinstance(state_like, dict) else type(state_like)(**out)
 

@@ -440,7 +440,7 @@ def _bc(v, ax):
 
 
 def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
-              sigma_b=None):
+              sigma_b=None, poles=(), pole_masks=None):
     """3D CPML coefficient set (core/stepper_3d.py:150-266, CPML path, no
     conductivity, no poles). dt = 0.5 dx / sqrt(3). H-side profiles on the
     n-1 half nodes, E-side on the interior [1:-1]."""
@@ -470,14 +470,38 @@ def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
         damp = {"ex": pair(_avg(sd, 0)), "ey": pair(_avg(sd, 1)), "ez": pair(_avg(sd, 2)),
                 "hx": pair(_avg(_avg(sb, 1), 2)), "hy": pair(_avg(_avg(sb, 0), 2)),
                 "hz": pair(_avg(_avg(sb, 0), 1))}
-    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, damp=damp)
+    # ADE pole stacks per E component (core/stepper_3d.py:236-266): c1, c2 per pole,
+    # c3 = v3 x the Yee-averaged mask
+    pols = None
+    if len(poles):
+        pols = {}
+        for key, shape, ax in (("x", (nx - 1, ny, nz), 0), ("y", (nx, ny - 1, nz), 1),
+                               ("z", (nx, ny, nz - 1), 2)):
+            n_p = len(poles)
+            c3 = np.zeros((n_p,) + shape, dtype=dtype)
+            c1 = np.zeros((n_p, 1, 1, 1), dtype=dtype)
+            c2 = np.zeros((n_p, 1, 1, 1), dtype=dtype)
+            for q, pole in enumerate(poles):
+                v1, v2, v3 = pole_recurrence(pole, dt)
+                m = (np.ones((nx, ny, nz), dtype=dtype) if pole_masks is None
+                     else np.asarray(pole_masks[q], dtype=dtype))
+                c3[q] = dtype.type(v3) * _avg(m, ax)
+                c1[q], c2[q] = v1, v2
+            pols[key] = (c1, c2, c3)
+    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, damp=damp, pols=pols)
 
 
 def state_3d(c):
-    """Zero 3D state with CPML memory (core/stepper_3d.py:269-292)."""
+    """Zero 3D state with CPML memory and pole stacks (core/stepper_3d.py:269-292)."""
     nx, ny, nz = c["dims"]
     z = lambda *s: np.zeros(s, dtype=c["dtype"])
-    return dict(
+    pol = {}
+    if c.get("pols"):
+        n_p = c["pols"]["x"][2].shape[0]
+        pol = dict(Px_cur=z(n_p, nx - 1, ny, nz), Px_prev=z(n_p, nx - 1, ny, nz),
+                   Py_cur=z(n_p, nx, ny - 1, nz), Py_prev=z(n_p, nx, ny - 1, nz),
+                   Pz_cur=z(n_p, nx, ny, nz - 1), Pz_prev=z(n_p, nx, ny, nz - 1))
+    return dict(**pol,
         Ex=z(nx - 1, ny, nz), Ey=z(nx, ny - 1, nz), Ez=z(nx, ny, nz - 1),
         Hx=z(nx, ny - 1, nz - 1), Hy=z(nx - 1, ny, nz - 1), Hz=z(nx - 1, ny - 1, nz),
         psi_Ez_y=z(nx, ny - 1, nz - 1), psi_Ey_z=z(nx, ny - 1, nz - 1),
@@ -537,6 +561,21 @@ def step_3d_h(s, c):
     return out
 
 
+def _e_update(s, c, key, pair, eps_c, curl, out):
+    """E(n+1) of one component: (d1 E eps + d2 curl) / eps, or with poles the folded-D
+    form (d1 (eps E + sum P(n)) + d2 curl - sum P(n+1)) / eps after the ADE step
+    P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n) (core/stepper_3d.py:295-300, :312-325)."""
+    d1, d2 = pair
+    E = s["E" + key]
+    if not c.get("pols"):
+        return (d1 * E * eps_c + d2 * curl) / eps_c
+    c1, c2, c3 = c["pols"][key]
+    pc, pp = s[f"P{key}_cur"], s[f"P{key}_prev"]
+    pn = c1 * pc + c2 * pp + c3 * E
+    out[f"P{key}_cur"], out[f"P{key}_prev"] = pn, pc
+    return (d1 * (E * eps_c + pc.sum(0)) + d2 * curl - pn.sum(0)) / eps_c
+
+
 def step_3d_e(s, c, h, amp=0.0, src=None, point_sign=+1.0):
     """E(n+1), the E-side CPML memory and the soft source of step_3d
     (core/stepper_3d.py:395-482) from the state ``s`` and H(n+1/2) in ``h``."""
@@ -550,17 +589,17 @@ def step_3d_e(s, c, h, amp=0.0, src=None, point_sign=+1.0):
     ch_y, out["psi_Hz_y"] = ce(Hz, 1, "ey", s["psi_Hz_y"])
     ch_z, out["psi_Hy_z"] = ce(Hy, 2, "ez", s["psi_Hy_z"])
     curl_x = _pad_interior(ch_y[:, :, 1:-1] - ch_z[:, 1:-1, :], (1, 2))
-    Ex = (dm["ex"][0] * s["Ex"] * eps_x + dm["ex"][1] * curl_x) / eps_x
+    Ex = _e_update(s, c, "x", dm["ex"], eps_x, curl_x, out)
     eps_y = _avg(eps, 1)
     ch_z2, out["psi_Hx_z"] = ce(Hx, 2, "ez", s["psi_Hx_z"])
     ch_x, out["psi_Hz_x"] = ce(Hz, 0, "ex", s["psi_Hz_x"])
     curl_y = _pad_interior(ch_z2[1:-1, :, :] - ch_x[:, :, 1:-1], (0, 2))
-    Ey = (dm["ey"][0] * s["Ey"] * eps_y + dm["ey"][1] * curl_y) / eps_y
+    Ey = _e_update(s, c, "y", dm["ey"], eps_y, curl_y, out)
     eps_z = _avg(eps, 2)
     ch_x2, out["psi_Hy_x"] = ce(Hy, 0, "ex", s["psi_Hy_x"])
     ch_y2, out["psi_Hx_y"] = ce(Hx, 1, "ey", s["psi_Hx_y"])
     curl_z = _pad_interior(ch_x2[:, 1:-1, :] - ch_y2[1:-1, :, :], (0, 1))
-    Ez = (dm["ez"][0] * s["Ez"] * eps_z + dm["ez"][1] * curl_z) / eps_z
+    Ez = _e_update(s, c, "z", dm["ez"], eps_z, curl_z, out)
     out.update(Ex=Ex, Ey=Ey, Ez=Ez)
     if src is not None and amp != 0.0:
         comp = src[0]

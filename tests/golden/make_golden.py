@@ -18,8 +18,8 @@ cases of the hot path through its own public functions:
   and of ``run_te`` (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and the TM and TE cases with a Lorentz and a Drude pole
-  (``make_golden.py poles``); the 3D case with sigma_d and sigma_b
-  (``make_golden.py sigma3d``)
+  (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
+  (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
 in float64 and float32. Inputs (eps maps, parameters) and outputs (final
 state, monitor accumulators, fluxes) are stored as ``golden_*.npz``. The
@@ -179,7 +179,10 @@ def te_case(prec, sigma=False, poles=False):
 FACES = [("x", 5), ("x", 18), ("y", 5), ("y", 16), ("z", 5), ("z", 14)]
 
 
-def case_3d(prec, lean=False, sigma=False):
+POLES3 = [(0.5, 0.05, 2.0), (0.0, 0.1, 1.0, 0.8)]     # a Lorentz and a Drude pole
+
+
+def case_3d(prec, lean=False, sigma=False, poles=False):
     rng = np.random.default_rng(13)
     nx, ny, nz, dx, npml = 24, 22, 20, 1.0 / 16, 4
     eps = np.ones((nx, ny, nz))
@@ -212,11 +215,18 @@ def case_3d(prec, lean=False, sigma=False):
             sb[6:10, 6:12, 8:14] = 3.0
             kw = dict(sigma_d=torch.tensor(sd, dtype=DT[prec]),
                       sigma_b=torch.tensor(sb, dtype=DT[prec]))
+        pm3 = None
+        if poles:                                     # masks off the absorbing layers
+            pm3 = [np.zeros((nx, ny, nz)), np.zeros((nx, ny, nz))]
+            pm3[0][8:16, 6:14, 6:14] = 1.0
+            pm3[1][14:19, 12:17, 9:15] = 1.0
+            kw.update(poles=POLES3, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm3])
         c = build_3d_coeffs(nx, ny, nz, dx, eps=epst, npml=npml, dtype=DT[prec], **kw)
         src = PointSource3D(c.dt, "Ez", *src_ijk, prof)
         mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=i, win=win, dtype=DT[prec])
                 for a, i in FACES]
-        s0 = init_3d_state(nx, ny, nz, npml=npml, dtype=DT[prec])
+        s0 = init_3d_state(nx, ny, nz, npml=npml, dtype=DT[prec],
+                           n_poles=len(POLES3) if poles else 0)
         with torch.no_grad():
             stt, accs = run_3d(s0, c, n, source=src, monitors=mons)
         st = {k: getattr(stt, k) for k in stt._fields if getattr(stt, k) is not None}
@@ -225,6 +235,9 @@ def case_3d(prec, lean=False, sigma=False):
                faces=json.dumps(FACES), win=np.array(win))
     if sigma:
         out["sigma_d"], out["sigma_b"] = sd, sb
+    if poles:
+        out["poles"] = json.dumps(POLES3)
+        out["pole_masks"] = np.stack(pm3)
     for k, v in st.items():
         out["s_" + k] = _np(v)
     for i, (a, mon) in enumerate(zip(accs, mons)):
@@ -402,6 +415,11 @@ def main():
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_3d_sigma_{prec}.npz"),
                                 **case_3d(prec, sigma=True))
+        return
+    if sys.argv[1:] == ["poles3d"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_3d_poles_{prec}.npz"),
+                                **case_3d(prec, poles=True))
         return
     if sys.argv[1:] == ["poles"]:
         for prec in ("f64", "f32"):

@@ -167,6 +167,9 @@ def _run3d(lean, variant=0, case=None):
         if "sigma_d" in g:
             kw = dict(sigma_d=torch.tensor(g["sigma_d"], dtype=torch.float32),
                       sigma_b=torch.tensor(g["sigma_b"], dtype=torch.float32))
+        if "poles" in g:
+            kw = dict(poles=json.loads(str(g["poles"])),
+                      pole_masks=[torch.tensor(m, dtype=torch.float32) for m in g["pole_masks"]])
         c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, device=dev(), **kw)
         dt = c.dt
     src = PointSource3D(dt, "Ez", i, j, k, prof)
@@ -176,7 +179,8 @@ def _run3d(lean, variant=0, case=None):
                                  variant=variant)
         st = {kk: getattr(view, kk) for kk in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
     else:
-        s, accs = run_3d(init_3d_state(nx, ny, nz, npml=npml, device=dev()), c,
+        n_p = len(json.loads(str(g["poles"]))) if "poles" in g else 0
+        s, accs = run_3d(init_3d_state(nx, ny, nz, npml=npml, device=dev(), n_poles=n_p), c,
                          int(g["n_steps"]), source=src, monitors=mons, variant=variant)
         st = s._asdict()
     return st, accs, mons, dx
@@ -184,7 +188,7 @@ def _run3d(lean, variant=0, case=None):
 
 @pytest.mark.parametrize("variant,lean,case", [(1, False, None), (2, False, None),
                                                 (1, True, None), (2, True, None),
-                                                (2, False, "3d_sigma")])
+                                                (2, False, "3d_sigma"), (2, False, "3d_poles")])
 def test_3d_matches_reference(lean, variant, case):
     """3D golden cases; 3d_sigma adds conductive damping (sigma_d on E, sigma_b on H)."""
     st, accs, mons, dx = _run3d(lean, variant, case)
@@ -195,6 +199,7 @@ def test_3d_matches_reference(lean, variant, case):
         keys = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]
         if not lean:
             keys += ["psi_Ez_y", "psi_Hx_y", "psi_Hz_x", "psi_Hy_z", "psi_Ex_z"]
+            keys += [k[2:] for k in g if k.startswith("s_P")]
         for k in keys:
             errs[k] = rel_l2(st[k].cpu().numpy(), g["s_" + k])
         for n, (a, mon) in enumerate(zip(accs, mons)):
@@ -903,3 +908,30 @@ def test_3d_damping_refused_by_fused_kernel_and_adjoint():
         run_3d(s0, c, 2, variant=1)
     with pytest.raises(MtbUnsupported):
         run_3d_adjoint(c, 4, 2, None, [], lambda accs: torch.zeros(()), s0)
+
+
+def test_3d_poles_slabs_bitwise_equal_to_whole_grid():
+    """3D poles (random P stacks and fields) through the x-slab decomposition: two and three
+    slabs reproduce the whole-grid run bit for bit, pole stacks included."""
+    from meep_torch_b200.core.monitors_3d import FluxMonitor3D, run_3d
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    from meep_torch_b200.slab3d import run_3d_slabs
+    nx, ny, nz, dx, npml, n = 21, 15, 24, 0.0625, 4, 30
+    g = torch.Generator().manual_seed(5)
+    masks = [torch.zeros(nx, ny, nz), torch.zeros(nx, ny, nz)]
+    masks[0][6:15, 5:10, 6:18] = 1.0
+    masks[1][9:13, 4:11, 8:12] = 1.0
+    c = build_3d_coeffs(nx, ny, nz, dx, npml=npml, device=dev(),
+                        poles=[(0.5, 0.05, 2.0), (0.0, 0.1, 1.0, 0.8)], pole_masks=masks)
+    s0 = init_3d_state(nx, ny, nz, npml=npml, device=dev(), n_poles=2)
+    s0 = s0._replace(**{k: 0.1 * torch.randn(getattr(s0, k).shape, generator=g).to(dev())
+                        for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Px_cur", "Px_prev",
+                                  "Py_cur", "Py_prev", "Pz_cur", "Pz_prev")})
+    mons = [FluxMonitor3D(c.dt, [0.5, 0.7], normal="y", idx=7, win=(2, 18, 3, 20))]
+    ref_s, ref_a = run_3d(s0, c, n, monitors=mons)
+    for n_slabs in (2, 3):
+        st, accs = run_3d_slabs(s0, c, n, monitors=mons, n_slabs=n_slabs)
+        bad = [k for k, v in ref_s._asdict().items()
+               if v is not None and not torch.equal(v, getattr(st, k))]
+        bad += ["acc"] if not torch.equal(accs[0], ref_a[0]) else []
+        assert not bad, (n_slabs, bad)

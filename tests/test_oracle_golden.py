@@ -117,8 +117,10 @@ def test_te_oracle_matches_reference(case, prec):
 def run_3d_oracle(g, prec, lean=False):
     dt_np = NPD[prec]
     nx, ny, nz, dx = int(g["nx"]), int(g["ny"]), int(g["nz"]), float(g["dx"])
+    poles = json.loads(str(g["poles"])) if "poles" in g else ()
     c = O.coeffs_3d(nx, ny, nz, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
-                    sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"))
+                    sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"), poles=poles,
+                    pole_masks=g.get("pole_masks"))
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
     dt = c["dt"]
     freqs = g["freqs"]
@@ -133,12 +135,14 @@ def run_3d_oracle(g, prec, lean=False):
     return c, s, acc
 
 
-@pytest.mark.parametrize("case", ["3d", "3d_sigma"])
+@pytest.mark.parametrize("case", ["3d", "3d_sigma", "3d_poles"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_3d_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
     c, s, acc = run_3d_oracle(g, prec)
-    for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "psi_Ez_y", "psi_Hx_y", "psi_Hz_x"):
+    names = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "psi_Ez_y", "psi_Hx_y", "psi_Hz_x"]
+    names += [k[2:] for k in g if k.startswith("s_P")]
+    for k in names:
         assert rel_l2(s[k], g["s_" + k]) < TOL[prec], k
     for n, a in enumerate(acc):
         assert rel_l2(a, g[f"acc_{n}"]) < TOL[prec]
