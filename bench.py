@@ -19,6 +19,11 @@ every DFT contribution folded). Metric: Gcell-updates/s = sum(nx*ny) *
   measured DRAM bytes (``traffic``) instead.
 * ``--workload cfg1 | cfg3 | cfg4``: the single-structure TM run, the 256^3 3D
   run and the 600 x 400 gradient problem, on the same line format.
+* ``--workload cfg5``: the surrogate-assisted design loop. FDTD data generation and
+  FNO training come first (untimed). Then the plain adjoint loop and the surrogate
+  loop run from the same start. ``value`` is the plain loop's iteration count over
+  the surrogate loop's wall time to reach 99 % of the plain loop's final FOM, with
+  both FOMs verified by FDTD. Each bench step is one pair of loops.
 * ``cpu_baseline``: the oracle (numpy restatement of the reference's TM/TE
   step and monitors) on a bounded sample of the same batch, on the host cores.
 * ``--impl reference``: the same sample through the oracle only (the
@@ -43,6 +48,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 STEPS_PER_RUN = {"cfg2": 5000, "cfg3": 2000, "cfg1": 4000}
+S_CFG5_STEPS = 3000
 
 
 def peaks():
@@ -270,6 +276,105 @@ def cpu_sample_cfg4(steps):
     t0 = time.perf_counter()
     O.run_2d(O.tm_step, O.tm_state(oc), oc, steps, amp_fn=lambda t: prof(O.src_time(t, dt)),
              mask=mask)
+    return time.perf_counter() - t0
+
+
+def run_cfg5(args, rank, world, dev):
+    """cfg5: FDTD data generation, FNO training, then the plain adjoint design loop and
+    the surrogate-assisted loop from the same start; the surrogate loop stops once its
+    FDTD-verified FOM reaches 99 % of the plain loop's final FOM."""
+    import torch
+
+    from meep_torch_b200 import _lib
+    from meep_torch_b200 import surrogate as S
+    from meep_torch_b200 import workloads as W
+
+    lib = _lib.load()
+    torch.manual_seed(5 + 1009 * rank)
+    prob = S.Cfg5Problem(dev)
+    c = prob.c
+    n_train, n_test = args.maps, 256
+    rho = S.grf_designs(n_train + n_test, seed=5 + 1009 * rank).to(dev)
+    batch = min(1024, n_train)
+    # data generation: one plan of `batch` designs, eps repacked per chunk
+    prob.simulate(rho[:batch], batch=batch)                       # plan build + warm-up
+    eng = prob._engines[batch]
+    eng.set_timing(True)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    y = prob.simulate(rho, batch=batch)
+    torch.cuda.synchronize(dev)
+    gen_s = time.perf_counter() - t0
+    step_ms, step_n, dft_ms, dft_n = eng.timing()
+    eng.set_timing(False)
+    prob.close()
+    x = prob.fno_input(rho)
+    model = S.FNO2d().to(dev)
+    scale, train_s = S.train_fno(model, x[:n_train], y[:n_train], epochs=args.epochs)
+    model.eval()
+    test_err = S.rel_error(model, x[n_train:], y[n_train:], scale)
+    with torch.no_grad():
+        fp = torch.cat([model(x[n_train + i:n_train + i + 64]) for i in range(0, n_test, 64)])
+        ft = prob.fom(y[n_train:])
+        fom_err = float(((prob.fom(fp * scale) - ft).abs() / ft).median())
+    del y
+    rho0 = torch.full((c["design"], c["design"]), 0.5)
+    for _ in range(args.warmup):                                   # plans, cuFFT, autotune
+        S.design_loop(prob, rho0.to(dev), 2)
+        S.design_loop(prob, rho0.to(dev), 2, model=model, scale=scale)
+    torch.cuda.synchronize(dev)
+    n0 = lib.mtb_launch_count()
+    runs = []
+    with Clocks(dev.index if dev.index is not None else 0) as clk:
+        for _ in range(args.steps):
+            plain = S.design_loop(prob, rho0.to(dev), args.iters)
+            target = 0.99 * plain["fom"][-1]
+            sur = S.design_loop(prob, rho0.to(dev), args.iters, model=model, scale=scale,
+                                target=target)
+            runs.append((plain, sur, target))
+    launches = lib.mtb_launch_count() - n0
+    plain, sur, target = runs[len(runs) // 2]
+    # e2e: the surrogate loop from a pinned host design to the final design on the host
+    host = rho0.pin_memory()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    out = S.design_loop(prob, host.to(dev, non_blocking=True), args.iters, model=model,
+                        scale=scale, target=target)
+    final = out["rho"].cpu()
+    e2e_s = time.perf_counter() - t0
+    spec = [{"nx": c["n"], "ny": c["n"], "pol": "tm"}] * batch
+    return dict(plain=plain, sur=sur, target=target, e2e_s=e2e_s, e2e_reached=
+                out["fom"][-1] >= target, h2d=host.numel() * 4, d2h=final.numel() * 4,
+                gen_s=gen_s, gen_updates=(n_train + n_test) * c["n"] ** 2 * c["steps"],
+                step_ms=step_ms, step_n=step_n, dft_ms=dft_ms,
+                bytes_launch=W.cfg2_bytes_per_step(spec, c["npml"]), train_s=train_s,
+                test_err=test_err, fom_err=fom_err, launches=launches,
+                clocks=clk.summary(), n_train=n_train)
+
+
+def cpu_sample_cfg5(steps):
+    """Oracle TM forward of `steps` steps on the cfg5 grid (one thread): seconds."""
+    import numpy as np
+
+    from meep_torch_b200 import surrogate as S
+    from oracle import fdtd as O
+    c = S.CFG5
+    n = c["n"]
+    rho = S.grf_designs(1, seed=5)[0].numpy()
+    eps = np.full((n, n), c["eps_min"], dtype=np.float32)
+    d0 = (n - c["design"]) // 2
+    eps[d0:d0 + c["design"], d0:d0 + c["design"]] = c["eps_min"] + \
+        (c["eps_max"] - c["eps_min"]) * rho
+    oc = O.tm_coeffs(n, n, c["dx"], eps=eps, npml=c["npml"], dtype=np.float32)
+    dt = oc["dt"]
+    mask = O.line_source_mask(n, n, c["dx"], c["npml"] + 10, c["npml"], n - c["npml"],
+                              dtype=np.float32)
+    prof = O.gaussian_pulse(c["fcen"], c["fwidth"])
+    freqs = list(c["freqs"])
+    mons = [lambda s, t: O.dft_sample(s["Ez"], t, dt, freqs, "Ez", np.float32)]
+    t0 = time.perf_counter()
+    O.run_2d(O.tm_step, O.tm_state(oc), oc, steps, amp_fn=lambda t: prof(O.src_time(t, dt)),
+             mask=mask, monitors=mons)
     return time.perf_counter() - t0
 
 
@@ -650,7 +755,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
+    ap.add_argument("--maps", type=int, default=20000, help="cfg5 training designs")
+    ap.add_argument("--epochs", type=int, default=20, help="cfg5 FNO training epochs")
+    ap.add_argument("--iters", type=int, default=50,
+                    help="cfg5 design iterations (plain loop) / verifications (surrogate)")
     ap.add_argument("--rows", type=int, default=0, help="rows per warp (0 = library default)")
     ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
     ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
@@ -677,7 +786,24 @@ def main():
     threads = os.cpu_count() or 1
     if args.cpu_structs <= 0:
         args.cpu_structs = min(max(8, threads), 64)
-    if args.workload == "cfg4":
+    if args.workload == "cfg5":
+        config = {"workload": "cfg5: surrogate-assisted design of a 64 x 64 px region "
+                              "(eps 1..4) in a 256 x 256 TM cell at res 20, 20-cell CPML, "
+                              "Gaussian line source (0.65, 0.25), 3000 steps per FDTD run; "
+                              "objective mean |Ez|^2 of the 0.6/0.65/0.7 DFT on an 8 x 8 patch "
+                              "behind the design",
+                  "training_maps": args.maps, "test_maps": 256, "epochs": args.epochs,
+                  "maps": "Gaussian random fields, correlation 4 px (0.2 um), thresholded "
+                          "at 0, conic filter 0.1 um, seed 5",
+                  "fno": "4 layers, width 64, 24 x 24 modes, BF16 autocast (FP32 "
+                         "accumulation); FFTs in FP32",
+                  "loops": f"plain: {args.iters} Adam steps (lr 0.05) on the FDTD adjoint "
+                           "gradient; surrogate: trust region, 10 FNO steps per FDTD "
+                           "adjoint verification, first-order corrected, stops at 99 % of "
+                           "the plain loop's final FOM",
+                  "l2": "data generation batches of 1024 x 256^2 designs (~1.5 GB of "
+                        "fields): larger than L2; design loops are latency-bound"}
+    elif args.workload == "cfg4":
         config = {"workload": "cfg4: gradient of a 600 x 400 TM mode-converter-shaped problem "
                               "(res 25, 25-cell CPML, 160 x 160 design, conic filter + tanh "
                               "projection, line source across the input guide standing in for "
@@ -784,6 +910,68 @@ def main():
                                               f"costed as 2 x {r['nsteps']} steps (the reverse "
                                               "sweep at the forward's cost); the oracle has no "
                                               "reverse mode"}
+        if rank == 0:
+            print(json.dumps(line))
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.workload == "cfg5":
+        r = run_cfg5(args, rank, world, dev)
+        plain, sur = r["plain"], r["sur"]
+        reached = sur["fom"][-1] >= r["target"]
+        t_sur = sur["t"][-1]
+        n_it = len(plain["fom"])
+        peak, peak_kind = peaks()
+        step_avg = r["step_ms"] / max(r["step_n"], 1)
+        ach = r["bytes_launch"] / (step_avg / 1e3) / 1e9 if step_avg else None
+        line = {"metric": "design-iterations/s (plain-loop iterations matched per second of "
+                          "the surrogate loop, at <= 1% FOM error)",
+                "value": n_it / t_sur if reached else None,
+                "unit": "design-iterations/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": (plain["seconds"] + sur["seconds"]) * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 FDTD, bf16 FNO", "data": "synthetic",
+                "config": dict(config, parallelism=f"independent problem per rank x{world}"),
+                "plain_loop": {"iterations": n_it, "seconds": plain["seconds"],
+                               "design_iterations_per_s": n_it / plain["seconds"],
+                               "fom_start": plain["fom"][0], "fom_final": plain["fom"][-1]},
+                "surrogate_loop": {"reached_target": reached, "target_fom": r["target"],
+                                   "fom_final": sur["fom"][-1],
+                                   "fom_rel_err_vs_plain": abs(sur["fom"][-1] - plain["fom"][-1])
+                                   / plain["fom"][-1],
+                                   "seconds": t_sur, "fdtd_runs": sur["fdtd_runs"],
+                                   "surrogate_steps": sur["surrogate_steps"],
+                                   "accepted": sum(sur["accepted"]) - 1,
+                                   "speedup_vs_plain": plain["seconds"] / t_sur
+                                   if reached else None},
+                "surrogate": {"train_seconds": r["train_s"], "test_rel_l2": r["test_err"],
+                              "test_fom_rel_err_median": r["fom_err"],
+                              "training_maps": r["n_train"]},
+                "data_generation": {"seconds": r["gen_s"],
+                                    "gcell_updates_per_s": r["gen_updates"] / r["gen_s"] / 1e9},
+                "roofline": {"bound": "hbm", "kernel": "k_tile_tm (data generation, one step "
+                             "of a 1024-design batch)", "achieved": ach, "peak": peak,
+                             "peak_kind": peak_kind, "unit": "GB/s",
+                             "frac": ach / peak if ach else None, "traffic": None,
+                             "alg_bytes_per_launch": r["bytes_launch"], "launch_ms": step_avg,
+                             "launches": r["step_n"], "dft_contract_ms_total": r["dft_ms"],
+                             "note": "the design loops themselves are latency-bound (one "
+                                     "256 x 256 structure)"},
+                "e2e": {"value": n_it / r["e2e_s"] if r["e2e_reached"] else None,
+                        "unit": "design-iterations/s", "h2d_bytes_per_step": r["h2d"],
+                        "d2h_bytes_per_step": r["d2h"]},
+                "clocks": r["clocks"], "gpu_launches": r["launches"]}
+        if rank == 0 and not args.no_cpu:
+            sec = cpu_sample_cfg5(S_CFG5_STEPS)
+            line["cpu_baseline"] = {"value": 1.0 / (2 * sec), "unit": "design-iterations/s",
+                                    "cores": 1, "kind": "port",
+                                    "sample": f"oracle (numpy float32) forward with the 3-freq "
+                                              f"DFT, the full {S_CFG5_STEPS}-step run of one "
+                                              f"cfg5 design in {sec:.1f} s, one thread; one "
+                                              "plain design iteration costed as two runs "
+                                              "(forward + reverse sweep at the forward's cost)"}
         if rank == 0:
             print(json.dumps(line))
         if world > 1:

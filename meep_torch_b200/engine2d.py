@@ -360,7 +360,8 @@ class Engine2D:
                     S.explicit_e = 1
                     S.e_explicit = L.ptr(eex)
                     it.keep.append(eex)
-            it.box = dict(main=f_main, x=f_x, y=f_y, psi=psis, eps_a=eps_a, eps_b=eps_b)
+            it.box = dict(main=f_main, x=f_x, y=f_y, psi=psis, eps_a=eps_a, eps_b=eps_b,
+                          inv_a=inv_a)
             if pol_bufs is not None:
                 if te:
                     for ax, bufs in pol_bufs.items():
@@ -379,6 +380,7 @@ class Engine2D:
             # current on D scaled by d2 (core/stepper_tm.py:158-163, :197-200;
             # core/stepper_te.py D update and step_source)
             it.src_scale = None
+            it.plain = not te and not S.n_poles and not S.explicit_e
             cond = ([("d1x", "d2x"), ("d1y", "d2y")] if te else [("d1", "d2")])
             if getattr(c, cond[0][0], None) is not None:
                 for k, (n1, n2) in enumerate(cond):
@@ -386,6 +388,7 @@ class Engine2D:
                     b2 = self._pack(getattr(c, n2), nx, P)
                     S.cond_d1[k], S.cond_d2[k] = L.ptr(b1), L.ptr(b2)
                     it.keep += [b1, b2]
+                it.plain = False
                 d2e = getattr(c, cond[-1][1])
                 it.src_scale = d2e.to(device=dev, dtype=torch.float32) / float(c.dt)
             self._check_psi_outside(it)
@@ -610,6 +613,20 @@ class Engine2D:
                 n = t.numel()
                 L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
                                           self._sptr()), "reset")
+
+    def set_eps(self, b: int, eps: torch.Tensor):
+        """Replace structure b's permittivity in place (a TM structure without
+        conductivity, poles or an explicit first-step Ez): eps and 1/eps are packed
+        into the plan's own buffers, so a batch of new designs of the same shapes
+        reuses the plan (and its graphs); call reset() before the next run."""
+        it = self.items[b]
+        _need(getattr(it, "plain", False), "set_eps: TM structures without conductivity, "
+              "poles or an explicit first-step Ez only")
+        _need(tuple(eps.shape) == (it.nx, it.ny), f"set_eps: eps shape {tuple(eps.shape)} "
+              f"!= {(it.nx, it.ny)}")
+        e = eps.to(device=self.device, dtype=torch.float32)
+        it.box["eps_a"].copy_(self._pack(e, it.nx, it.pitch))
+        it.box["inv_a"].copy_(self._pack(torch.reciprocal(e), it.nx, it.pitch))
 
     def _live_buffers(self, b: int):
         """The buffers of structure b the next step reads: fields, then CPML memory."""

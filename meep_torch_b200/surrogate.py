@@ -1,0 +1,341 @@
+"""Surrogate-assisted inverse design on the FDTD engine (the cfg5 workload).
+
+The FDTD data and every verification run through the library's batched 2D TM kernels.
+The surrogate is a Fourier neural operator (FNO) trained on those runs. Its spectral
+transforms are cuFFT (torch.fft) and its channel mixes are BF16 cuBLAS GEMMs under
+autocast, with FP32 accumulation: library calls, as for any plain GEMM here.
+
+Pieces:
+
+* ``grf_designs``: seeded design maps. A Gaussian random field (correlation length in
+  pixels) is thresholded at 0, then conic-filtered (``design.conic_filter``).
+* ``Cfg5Problem``: the 256 x 256 TM cell at resolution 20. It has a 20-cell CPML, a 64 x 64
+  design painted at the centre (eps between ``eps_min`` and ``eps_max``) and a Gaussian
+  line source across the grid 10 cells inside the left absorber. The DFT of Ez at three
+  frequencies is read on the 128 x 128 region around the design.
+  ``simulate(rho)`` runs a batch of designs in one plan and returns the six real target
+  channels (Re, Im per frequency). ``fom(fields)`` is the objective: the mean |Ez|^2 over
+  a target patch behind the design, averaged over the frequencies.
+* ``FNO2d``: lift (eps, x, y) to ``width`` channels, ``layers`` Fourier layers (rfft2,
+  ``modes`` x ``modes`` low modes in each corner mixed by complex weights, plus a 1x1
+  channel mix, GELU), then a projection to the six channels.
+* ``train_fno``: Adam with a cosine schedule on the relative L2 error.
+* ``design_loop``: gradient ascent on the design latent. Without a model each
+  iteration is one FDTD run with the library's adjoint (``run_tm`` with eps requiring
+  grad): the plain loop. With one, blocks of surrogate steps on a first-order-corrected
+  FNO propose designs inside a trust region, and an FDTD adjoint run verifies each
+  proposal and re-anchors the correction.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+import torch
+import torch.nn as nn
+import torch.nn.functional as F
+
+from .design import conic_filter
+
+__all__ = ["CFG5", "grf_designs", "Cfg5Problem", "FNO2d", "train_fno", "rel_error", "design_loop"]
+
+CFG5 = dict(n=256, dx=0.05, npml=20, design=64, region=128, eps_min=1.0, eps_max=4.0,
+            freqs=(0.6, 0.65, 0.7), fcen=0.65, fwidth=0.25, steps=3000, corr_px=4.0,
+            filter_radius=0.1, target=(176, 184, 124, 132))
+
+
+def grf_designs(n: int, size: int = 64, corr_px: float = 4.0, radius: float = 0.1,
+                dx: float = 0.05, seed: int = 5, device="cpu") -> torch.Tensor:
+    """``n`` binary Gaussian-random-field maps (size x size, correlation length ``corr_px``
+    pixels, thresholded at 0), conic-filtered with ``radius``: values in [0, 1]."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    noise = torch.randn(n, size, size, generator=g)
+    k = torch.fft.fftfreq(size)
+    k2 = k[:, None] ** 2 + k[None, :] ** 2
+    kernel = torch.exp(-2.0 * (math.pi * corr_px) ** 2 * k2)
+    field = torch.fft.ifft2(torch.fft.fft2(noise) * kernel).real
+    binary = (field > 0).to(torch.float32)
+    out = torch.stack([conic_filter(b, radius, dx) for b in binary])
+    return out.to(device)
+
+
+class Cfg5Problem:
+    """The cfg5 TM cell; ``simulate`` batches designs through one Engine2D plan."""
+
+    def __init__(self, device, steps: int | None = None, **over):
+        self.c = dict(CFG5, **over)
+        if steps is not None:
+            self.c["steps"] = int(steps)
+        c = self.c
+        self.device = torch.device(device)
+        n, d, r = c["n"], c["design"], c["region"]
+        self.d0 = (n - d) // 2
+        self.r0 = (n - r) // 2
+        from .core.grid import Grid
+        from .core.sources import GaussianPulse, LineSource
+        self.grid = Grid(nx=n, ny=n, dx=c["dx"], device=self.device)
+        self.source = LineSource(self.grid, ix=c["npml"] + 10, j0=c["npml"], j1=n - c["npml"],
+                                 profile=GaussianPulse(c["fcen"], c["fwidth"]))
+
+    # -------------------------------------------------------------- geometry
+    def eps_map(self, rho: torch.Tensor) -> torch.Tensor:
+        """(B, d, d) design densities -> (B, n, n) eps."""
+        c, d0, d = self.c, self.d0, self.c["design"]
+        eps = torch.full((rho.shape[0], c["n"], c["n"]), c["eps_min"], dtype=torch.float32,
+                         device=rho.device)
+        eps[:, d0:d0 + d, d0:d0 + d] = c["eps_min"] + (c["eps_max"] - c["eps_min"]) * rho
+        return eps
+
+    def region(self, full: torch.Tensor) -> torch.Tensor:
+        r0, r = self.r0, self.c["region"]
+        return full[..., r0:r0 + r, r0:r0 + r]
+
+    def fno_input(self, rho: torch.Tensor) -> torch.Tensor:
+        """(B, d, d) -> (B, 1, region, region) normalised eps of the region."""
+        c = self.c
+        e = self.region(self.eps_map(rho))
+        return ((e - c["eps_min"]) / (c["eps_max"] - c["eps_min"]))[:, None]
+
+    # ------------------------------------------------------------------ FDTD
+    def _item(self, eps):
+        from .core.coeffs import build_tm_coeffs
+        from .core.monitors import DFTFieldsMonitor
+        from .core.stepper_tm import init_tm_state
+        m = build_tm_coeffs(self.grid, eps_inf=eps, npml=self.c["npml"])
+        mon = DFTFieldsMonitor(self.grid, list(self.c["freqs"]), "Ez")
+        return (init_tm_state(self.grid), m, self.source, [mon])
+
+    def simulate(self, rho: torch.Tensor, batch: int = 1024) -> torch.Tensor:
+        """FDTD of each design: (B, d, d) -> (B, 6, region, region) = (Re, Im) of the Ez
+        DFT at each frequency on the region. One plan per batch size is built once and
+        kept; later batches only repack eps (Engine2D.set_eps) and reset."""
+        nf, r = len(self.c["freqs"]), self.c["region"]
+        outs = []
+        with torch.no_grad():
+            for b0 in range(0, rho.shape[0], batch):
+                eps = self.eps_map(rho[b0:b0 + batch].to(self.device))
+                eng = self._engine(eps)
+                eng.run(0, self.c["steps"])
+                acc = torch.stack([eng.accumulators(b)[0] for b in range(eps.shape[0])])
+                outs.append(self.region(acc).reshape(acc.shape[0], 2 * nf, r, r))
+        return torch.cat(outs)
+
+    def _engine(self, eps):
+        from .engine2d import Engine2D
+        if not hasattr(self, "_engines"):
+            self._engines = {}
+        n = eps.shape[0]
+        eng = self._engines.get(n)
+        if eng is None:
+            eng = self._engines[n] = Engine2D([self._item(e) for e in eps])
+        else:
+            for b in range(n):
+                eng.set_eps(b, eps[b])
+            eng.reset()
+        return eng
+
+    def close(self):
+        for eng in getattr(self, "_engines", {}).values():
+            eng.close()
+        self._engines = {}
+
+    def fdtd_fom_and_grad(self, rho: torch.Tensor):
+        """(FOM, dFOM/drho) of one design by the library's adjoint (run_tm with eps
+        requiring grad)."""
+        from .core.run import run_tm
+        rho = rho.detach().clone().requires_grad_(True)
+        eps = self.eps_map(rho[None])[0]
+        st, m, src, mons = self._item(eps)
+        _, (acc,) = run_tm(st, m, self.c["steps"], source=src, monitors=mons,
+                           checkpoint_every=32)
+        nf = len(self.c["freqs"])
+        f = self.fom(self.region(acc).reshape(1, 2 * nf, self.c["region"],
+                                              self.c["region"]))[0]
+        f.backward()
+        return float(f.detach()), rho.grad.detach()
+
+    def fom(self, fields: torch.Tensor) -> torch.Tensor:
+        """Mean |Ez|^2 over the target patch and the frequencies: (B, 6, r, r) -> (B,)."""
+        i0, i1, j0, j1 = self.c["target"]
+        r0 = self.r0
+        patch = fields[:, :, i0 - r0:i1 - r0, j0 - r0:j1 - r0]
+        re, im = patch[:, 0::2], patch[:, 1::2]
+        return (re * re + im * im).mean(dim=(1, 2, 3))
+
+
+class _SpectralConv(nn.Module):
+    """Complex channel mix of the ``modes`` x ``modes`` lowest modes in the two
+    positive-frequency corners of rfft2."""
+
+    def __init__(self, width: int, modes: int):
+        super().__init__()
+        self.modes = modes
+        scale = 1.0 / (width * width)
+        self.w = nn.Parameter(scale * torch.randn(2, width, width, modes, modes,
+                                                  dtype=torch.cfloat))
+
+    def forward(self, x):
+        b, c, h, w = x.shape
+        m = self.modes
+        xf = torch.fft.rfft2(x.float())
+        out = torch.zeros(b, c, h, w // 2 + 1, dtype=torch.cfloat, device=x.device)
+        out[:, :, :m, :m] = torch.einsum("bixy,ioxy->boxy", xf[:, :, :m, :m], self.w[0])
+        out[:, :, -m:, :m] = torch.einsum("bixy,ioxy->boxy", xf[:, :, -m:, :m], self.w[1])
+        return torch.fft.irfft2(out, s=(h, w))
+
+
+class FNO2d(nn.Module):
+    """Fourier neural operator: (B, 1, r, r) normalised eps -> (B, 6, r, r) fields."""
+
+    def __init__(self, width: int = 64, modes: int = 24, layers: int = 4, out_ch: int = 6):
+        super().__init__()
+        self.lift = nn.Conv2d(3, width, 1)
+        self.spec = nn.ModuleList([_SpectralConv(width, modes) for _ in range(layers)])
+        self.mix = nn.ModuleList([nn.Conv2d(width, width, 1) for _ in range(layers)])
+        self.proj1 = nn.Conv2d(width, 128, 1)
+        self.proj2 = nn.Conv2d(128, out_ch, 1)
+
+    def forward(self, x):
+        b, _, h, w = x.shape
+        gy, gx = torch.meshgrid(torch.linspace(0, 1, h, device=x.device),
+                                torch.linspace(0, 1, w, device=x.device), indexing="ij")
+        x = torch.cat([x, gy.expand(b, 1, h, w), gx.expand(b, 1, h, w)], dim=1)
+        with torch.autocast("cuda", dtype=torch.bfloat16, enabled=x.is_cuda):
+            x = self.lift(x)
+            for k, (s, m) in enumerate(zip(self.spec, self.mix)):
+                y = s(x) + m(x)
+                x = F.gelu(y) if k < len(self.spec) - 1 else y
+            x = self.proj2(F.gelu(self.proj1(x)))
+        return x.float()
+
+
+def train_fno(model: FNO2d, x: torch.Tensor, y: torch.Tensor, *, epochs: int = 30,
+              batch: int = 32, lr: float = 2e-3, scale: float | None = None, log=None):
+    """Adam + cosine schedule on the relative L2 error of the (scaled) fields. Returns
+    (scale, seconds): targets are divided by ``scale`` (their RMS unless given)."""
+    if scale is None:
+        scale = float(y.pow(2).mean().sqrt())
+    yn = y / scale
+    opt = torch.optim.Adam(model.parameters(), lr=lr)
+    steps = epochs * max(1, x.shape[0] // batch)
+    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, steps)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    t0 = time.perf_counter()
+    for ep in range(epochs):
+        perm = torch.randperm(x.shape[0], generator=g)
+        tot = 0.0
+        for b0 in range(0, x.shape[0] - batch + 1, batch):
+            idx = perm[b0:b0 + batch].to(x.device)
+            pred = model(x[idx])
+            t = yn[idx]
+            loss = ((pred - t).flatten(1).norm(dim=1) / t.flatten(1).norm(dim=1)).mean()
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+            sched.step()
+            tot += float(loss.detach())
+        if log is not None:
+            log(ep, tot / max(1, x.shape[0] // batch))
+    if x.is_cuda:
+        torch.cuda.synchronize(x.device)
+    return scale, time.perf_counter() - t0
+
+
+def rel_error(model: FNO2d, x: torch.Tensor, y: torch.Tensor, scale: float) -> float:
+    with torch.no_grad():
+        p = torch.cat([model(x[i:i + 64]) for i in range(0, x.shape[0], 64)]) * scale
+    return float(((p - y).flatten(1).norm(dim=1) / y.flatten(1).norm(dim=1)).mean())
+
+
+def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None,
+                scale: float = 1.0, lr: float = 0.05, inner: int = 10, inner_lr: float = 0.1,
+                radius: float = 1.0, target: float | None = None):
+    """Gradient ascent on the design latent z (rho = sigmoid(z)) from ``rho0``.
+
+    Without ``model`` (the plain loop): ``iters`` Adam steps (``lr``), each on the FOM
+    and gradient of one FDTD run with its adjoint.
+
+    With ``model``: a first-order-corrected trust-region loop (surrogate management
+    after Alexandrov, Dennis, Lewis and Torczon, 1998). At an anchor z_k the FDTD
+    adjoint gives f_k and g_k = dFOM/drho. The surrogate s(rho) is shifted to agree
+    with FDTD in value and gradient there, m(rho) = s(rho) + (f_k - s_k) +
+    (g_k - grad s_k) . (rho - rho_k). ``inner`` surrogate Adam steps (``inner_lr``)
+    then maximise m with z kept within ``radius`` of z_k (max norm), and the proposal
+    is verified by an FDTD adjoint run. It is accepted if its verified FOM beats f_k;
+    the radius doubles when the gain is at least 3/4 of the predicted one and halves
+    on a rejection. At most ``iters`` verifications run, fewer once the verified FOM
+    reaches ``target``. Each verification is one FDTD run and every accepted design is
+    one; the FDTD FOM is the only one reported.
+
+    Returns dict(fom=[verified FOM after each FDTD run], t=[seconds at each],
+    accepted=[bool], seconds, surrogate_steps, fdtd_runs, rho)."""
+    dev = prob.device
+    z = torch.logit(rho0.clamp(0.02, 0.98)).detach().clone().to(dev)
+    hist, times, acc = [], [], []
+    t0 = time.perf_counter()
+
+    def mark(f, ok):
+        hist.append(f)
+        times.append(time.perf_counter() - t0)
+        acc.append(ok)
+
+    if model is None:
+        z.requires_grad_(True)
+        opt = torch.optim.Adam([z], lr=lr)
+        for _ in range(iters):
+            rho = torch.sigmoid(z).detach()
+            f, g = prob.fdtd_fom_and_grad(rho)
+            mark(f, True)
+            if target is not None and f >= target:
+                break
+            opt.zero_grad(set_to_none=True)
+            z.grad = -(g * rho * (1 - rho))          # d(-FOM)/dz
+            opt.step()
+        n_sur = 0
+    else:
+        frozen = [(p, p.requires_grad) for p in model.parameters()]
+        for p, _ in frozen:
+            p.requires_grad_(False)
+        f_k, g_k = prob.fdtd_fom_and_grad(torch.sigmoid(z))
+        mark(f_k, True)
+        n_sur = 0
+        for _ in range(iters - 1):
+            if target is not None and f_k >= target:
+                break
+            rho_k = torch.sigmoid(z).detach()
+            r = rho_k.clone().requires_grad_(True)
+            s_k = prob.fom(model(prob.fno_input(r[None])) * scale)[0]
+            (gs_k,) = torch.autograd.grad(s_k, r)
+            c0, cg = f_k - float(s_k.detach()), g_k - gs_k
+            zc = z.clone().requires_grad_(True)
+            opt = torch.optim.Adam([zc], lr=inner_lr)
+            for _ in range(inner):
+                rho = torch.sigmoid(zc)
+                m = prob.fom(model(prob.fno_input(rho[None])) * scale)[0] + c0 + \
+                    (cg * (rho - rho_k)).sum()
+                opt.zero_grad(set_to_none=True)
+                (-m).backward()
+                opt.step()
+                with torch.no_grad():
+                    zc.copy_(torch.minimum(torch.maximum(zc, z - radius), z + radius))
+                n_sur += 1
+            with torch.no_grad():
+                rho = torch.sigmoid(zc)
+                pred = float(prob.fom(model(prob.fno_input(rho[None])) * scale)[0]) + c0 + \
+                    float((cg * (rho - rho_k)).sum()) - f_k
+            f_c, g_c = prob.fdtd_fom_and_grad(rho.detach())
+            ok = f_c > f_k
+            mark(f_c, ok)
+            if ok:
+                if f_c - f_k >= 0.75 * pred:
+                    radius = min(2.0 * radius, 4.0)
+                z, f_k, g_k = zc.detach().clone(), f_c, g_c
+            else:
+                radius *= 0.5
+        for p, g in frozen:
+            p.requires_grad_(g)
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
+    return dict(fom=hist, t=times, accepted=acc, seconds=time.perf_counter() - t0,
+                surrogate_steps=n_sur, fdtd_runs=len(hist), rho=torch.sigmoid(z).detach())
