@@ -78,7 +78,8 @@ extern "C" {
  * core/stepper_tm.py:197-200 computes dt * amp * mask). */
 typedef struct mtb_cells {
     const int32_t *row_ptr; /* rows+1 entries, device; NULL = no cells     */
-    const int32_t *col;     /* n entries, device                           */
+    const int32_t *col;     /* n entries, device; ascending within a row
+                               (plans reject other orders)                 */
     const float *w;         /* n entries, device                           */
     int32_t n;              /* number of cells                             */
     int32_t amp_col;        /* amplitude-table column this list reads      */

@@ -160,14 +160,27 @@ struct Pipe {
 };
 
 // F[row, jb+q] -= amp * w for the cells of `row` in `cl` (CSR by row).
+// First e in [e0, e1) whose column is >= key (the columns of a row ascend: the
+// plan rejects other orders); e1 if there is none. Every probe stays in [e0, e1).
+__device__ __forceinline__ int lower_col(const int32_t *__restrict__ col, int e0, int e1,
+                                         int key) {
+    while (e0 < e1) {
+        const int m = (e0 + e1) >> 1;
+        if (__ldg(col + m) < key) e0 = m + 1;
+        else e1 = m;
+    }
+    return e0;
+}
 __device__ __forceinline__ void apply_cells(const mtb_cells &cl, int row, const float *amp,
                                             int jb, float (&v)[4]) {
     if (cl.n == 0 || row < cl.row_lo || row > cl.row_hi) return;
     const int e0 = __ldg(cl.row_ptr + row), e1 = __ldg(cl.row_ptr + row + 1);
     if (e0 == e1) return;
     const float a = __ldg(amp + cl.amp_col);
-    for (int e = e0; e < e1; ++e) {
+    // only the cells of columns jb .. jb+3, in list order (duplicates included)
+    for (int e = lower_col(cl.col, e0, e1, jb); e < e1; ++e) {
         const int c = __ldg(cl.col + e) - jb;
+        if (c >= 4) break;
         const float w = __ldg(cl.w + e);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -180,8 +193,8 @@ __device__ __forceinline__ float apply_cell1(const mtb_cells &cl, int row, int c
     const int e0 = __ldg(cl.row_ptr + row), e1 = __ldg(cl.row_ptr + row + 1);
     if (e0 == e1) return v;
     const float a = __ldg(amp + cl.amp_col);
-    for (int e = e0; e < e1; ++e)
-        if (__ldg(cl.col + e) == col) v -= a * __ldg(cl.w + e);
+    for (int e = lower_col(cl.col, e0, e1, col); e < e1 && __ldg(cl.col + e) == col; ++e)
+        v -= a * __ldg(cl.w + e);
     return v;
 }
 
@@ -1877,6 +1890,17 @@ static int cell_rows(mtb_cells &cl, int rows, int s) {
             cl.row_hi = r;
         }
     }
+    // the kernels binary-search a row's columns: they must ascend within each row
+    std::vector<int32_t> cv(cl.n);
+    e = cudaMemcpy(cv.data(), cl.col, sizeof(int32_t) * cl.n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return fail(MTB_CUDA_ERROR, "structure %d: reading source columns: %s", s,
+                    cudaGetErrorString(e));
+    for (int r = 0; r < rows; ++r)
+        for (int q = rp[r] + 1; q < rp[r + 1]; ++q)
+            if (cv[q] < cv[q - 1])
+                return fail(MTB_INVALID_ARG, "structure %d: source columns of row %d are not in "
+                            "ascending order", s, r);
     return MTB_OK;
 }
 
@@ -2363,11 +2387,12 @@ constexpr int NA_MAX_DEV = 64;
 constexpr int NA_MAX_REGIONS = 64;
 constexpr int NA_MAX_GROUPS = 16;
 constexpr int NA_CT = 256;              // contraction block size (common.cu)
+constexpr int NA_ERR_COLS = 1 << 30;    // error-flag bit: source columns out of order
 static unsigned char *g_noalloc_dev[NA_MAX_DEV];   // device address of the array, per device
 
 // x-layer bands and source row ranges of the descriptor copy (what
 // mtb_yee2d_plan_create computes on the host)
-__global__ void k_na_struct(mtb_yee2d_struct *S) {
+__global__ void k_na_struct(mtb_yee2d_struct *S, int *err) {
     __shared__ int lh, hh, le, he, rlo[3], rhi[3];
     const int nx = S->nx;
     const int nh = nx - 1, ne = nx;
@@ -2387,11 +2412,19 @@ __global__ void k_na_struct(mtb_yee2d_struct *S) {
     const mtb_cells *cl[3] = {&S->src_e, &S->src_h1, &S->src_h2};
     for (int c = 0; c < 3; ++c) {
         if (cl[c]->n <= 0) continue;
-        for (int r = threadIdx.x; r < nx; r += blockDim.x)
-            if (cl[c]->row_ptr[r + 1] > cl[c]->row_ptr[r]) {
+        for (int r = threadIdx.x; r < nx; r += blockDim.x) {
+            const int e0 = cl[c]->row_ptr[r], e1 = cl[c]->row_ptr[r + 1];
+            if (e1 > e0) {
                 atomicMin(&rlo[c], r);
                 atomicMax(&rhi[c], r);
             }
+            // the kernels binary-search a row's columns: flag a descending pair
+            for (int q = e0 + 1; q < e1; ++q)
+                if (cl[c]->col[q] < cl[c]->col[q - 1]) {
+                    atomicOr(err, NA_ERR_COLS);
+                    break;
+                }
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -2653,7 +2686,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
             MTB_CUDA_TRY(cudaMemcpyAsync(dFreq + goff[g], groups[g].freqs,
                                          sizeof(double) * gnf[g], cudaMemcpyHostToDevice, st));
     }
-    k_na_struct<<<1, 256, 0, st>>>(dS);
+    k_na_struct<<<1, 256, 0, st>>>(dS, dErr);
     MTB_CHECK_LAUNCH();
     k_na_work<<<(n_work + 255) / 256, 256, 0, st>>>(dWork, S.nx, rows, nch, n_work);
     MTB_CHECK_LAUNCH();
@@ -2719,6 +2752,9 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     int flag = 0;
     MTB_CUDA_TRY(cudaMemcpyAsync(&flag, dErr, sizeof(int), cudaMemcpyDeviceToHost, st));
     MTB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (flag & NA_ERR_COLS)
+        return fail(MTB_INVALID_ARG, "noalloc: source columns are not in ascending order within "
+                    "a row");
     if (flag)
         return fail(MTB_DEVICE_TIMEOUT, "noalloc: a bounded wait for a staged row copy expired");
     return MTB_OK;

@@ -46,17 +46,26 @@ CFG5 = dict(n=256, dx=0.05, npml=20, design=64, region=128, eps_min=1.0, eps_max
 
 
 def grf_designs(n: int, size: int = 64, corr_px: float = 4.0, radius: float = 0.1,
-                dx: float = 0.05, seed: int = 5, device="cpu") -> torch.Tensor:
-    """``n`` binary Gaussian-random-field maps (size x size, correlation length ``corr_px``
-    pixels, thresholded at 0), conic-filtered with ``radius``: values in [0, 1]."""
+                dx: float = 0.05, seed: int = 5, device="cpu", soft: float = 0.0,
+                beta=(0.5, 4.0)) -> torch.Tensor:
+    """``n`` Gaussian-random-field maps (size x size, correlation length ``corr_px``
+    pixels), conic-filtered with ``radius``: values in [0, 1]. The first
+    ``n - round(soft * n)`` maps are thresholded at 0 (binary); the rest are
+    soft-thresholded, sigmoid(beta * g / std(g)) with beta uniform in ``beta``, which
+    gives the grey densities a gradient-based design passes through."""
     g = torch.Generator(device="cpu").manual_seed(seed)
     noise = torch.randn(n, size, size, generator=g)
     k = torch.fft.fftfreq(size)
     k2 = k[:, None] ** 2 + k[None, :] ** 2
     kernel = torch.exp(-2.0 * (math.pi * corr_px) ** 2 * k2)
     field = torch.fft.ifft2(torch.fft.fft2(noise) * kernel).real
-    binary = (field > 0).to(torch.float32)
-    out = torch.stack([conic_filter(b, radius, dx) for b in binary])
+    rho = (field > 0).to(torch.float32)
+    n_soft = int(round(soft * n))
+    if n_soft:
+        b = beta[0] + (beta[1] - beta[0]) * torch.rand(n_soft, 1, 1, generator=g)
+        f = field[n - n_soft:]
+        rho[n - n_soft:] = torch.sigmoid(b * f / f.std(dim=(1, 2), keepdim=True))
+    out = torch.stack([conic_filter(r, radius, dx) for r in rho])
     return out.to(device)
 
 
@@ -140,19 +149,21 @@ class Cfg5Problem:
             eng.close()
         self._engines = {}
 
-    def fdtd_fom_and_grad(self, rho: torch.Tensor):
+    def fdtd_fom_and_grad(self, rho: torch.Tensor, fields: bool = False):
         """(FOM, dFOM/drho) of one design by the library's adjoint (run_tm with eps
-        requiring grad)."""
+        requiring grad); with ``fields`` also its (1, 6, region, region) DFT fields."""
         from .core.run import run_tm
         rho = rho.detach().clone().requires_grad_(True)
         eps = self.eps_map(rho[None])[0]
         st, m, src, mons = self._item(eps)
         _, (acc,) = run_tm(st, m, self.c["steps"], source=src, monitors=mons,
-                           checkpoint_every=32)
+                           checkpoint_every=64)
         nf = len(self.c["freqs"])
-        f = self.fom(self.region(acc).reshape(1, 2 * nf, self.c["region"],
-                                              self.c["region"]))[0]
+        y = self.region(acc).reshape(1, 2 * nf, self.c["region"], self.c["region"])
+        f = self.fom(y)[0]
         f.backward()
+        if fields:
+            return float(f.detach()), rho.grad.detach(), y.detach()
         return float(f.detach()), rho.grad.detach()
 
     def fom(self, fields: torch.Tensor) -> torch.Tensor:
@@ -249,31 +260,36 @@ def rel_error(model: FNO2d, x: torch.Tensor, y: torch.Tensor, scale: float) -> f
 
 
 def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None,
-                scale: float = 1.0, lr: float = 0.05, inner: int = 10, inner_lr: float = 0.1,
-                radius: float = 1.0, target: float | None = None):
+                scale: float = 1.0, lr: float = 0.05, inner: int = 40, inner_lr: float = 0.1,
+                radius: float = 1.0, probes=(5, 10, 20, 40), finetune: int = 0,
+                ft_lr: float = 2e-4, replay=None, target: float | None = None):
     """Gradient ascent on the design latent z (rho = sigmoid(z)) from ``rho0``.
 
     Without ``model`` (the plain loop): ``iters`` Adam steps (``lr``), each on the FOM
     and gradient of one FDTD run with its adjoint.
 
     With ``model``: a first-order-corrected trust-region loop (surrogate management
-    after Alexandrov, Dennis, Lewis and Torczon, 1998). At an anchor z_k the FDTD
-    adjoint gives f_k and g_k = dFOM/drho. The surrogate s(rho) is shifted to agree
-    with FDTD in value and gradient there, m(rho) = s(rho) + (f_k - s_k) +
-    (g_k - grad s_k) . (rho - rho_k). ``inner`` surrogate Adam steps (``inner_lr``)
-    then maximise m with z kept within ``radius`` of z_k (max norm), and the proposal
-    is verified by an FDTD adjoint run. It is accepted if its verified FOM beats f_k;
-    the radius doubles when the gain is at least 3/4 of the predicted one and halves
-    on a rejection. At most ``iters`` verifications run, fewer once the verified FOM
-    reaches ``target``. Each verification is one FDTD run and every accepted design is
-    one; the FDTD FOM is the only one reported.
+    after Alexandrov, Dennis, Lewis and Torczon, 1998) of at most ``iters`` blocks. At
+    an anchor z_k the FDTD adjoint gives f_k and g_k = dFOM/drho. The surrogate s(rho)
+    is shifted to agree with FDTD in value and gradient there, m(rho) = s(rho) +
+    (f_k - s_k) + (g_k - grad s_k) . (rho - rho_k). ``inner`` surrogate Adam steps
+    (``inner_lr``) maximise m with z kept within ``radius`` of z_k (max norm); the
+    designs after each count in ``probes`` are verified together by one batched
+    forward FDTD run. The best verified probe becomes the next anchor (and gets its
+    adjoint run) if it beats f_k; the radius doubles when that probe is the last one
+    and halves when no probe beats f_k. With ``finetune`` > 0 the model then takes that
+    many Adam steps (``ft_lr``) on the verified fields of this loop, mixed with
+    samples of ``replay`` = (inputs, targets / scale) when given. The loop stops
+    once a verified FOM reaches ``target``. Only FDTD FOMs are reported.
 
-    Returns dict(fom=[verified FOM after each FDTD run], t=[seconds at each],
-    accepted=[bool], seconds, surrogate_steps, fdtd_runs, rho)."""
+    Returns dict(fom=[verified FOM of each anchor / best probe], t=[seconds at each],
+    accepted=[bool], seconds, surrogate_steps, fdtd_runs (adjoint runs plus batched
+    forward runs), adjoint_runs, rho)."""
     dev = prob.device
     z = torch.logit(rho0.clamp(0.02, 0.98)).detach().clone().to(dev)
     hist, times, acc = [], [], []
     t0 = time.perf_counter()
+    n_adj = n_fwd = n_sur = 0
 
     def mark(f, ok):
         hist.append(f)
@@ -286,20 +302,32 @@ def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None
         for _ in range(iters):
             rho = torch.sigmoid(z).detach()
             f, g = prob.fdtd_fom_and_grad(rho)
+            n_adj += 1
             mark(f, True)
             if target is not None and f >= target:
                 break
             opt.zero_grad(set_to_none=True)
             z.grad = -(g * rho * (1 - rho))          # d(-FOM)/dz
             opt.step()
-        n_sur = 0
     else:
-        frozen = [(p, p.requires_grad) for p in model.parameters()]
-        for p, _ in frozen:
-            p.requires_grad_(False)
-        f_k, g_k = prob.fdtd_fom_and_grad(torch.sigmoid(z))
+        probes = sorted(set(int(p) for p in probes if 0 < int(p) <= inner)) or [inner]
+        params = list(model.parameters())
+        trainable = [p.requires_grad for p in params]
+        ft_opt = torch.optim.Adam([p for p, t in zip(params, trainable) if t], lr=ft_lr) \
+            if finetune else None
+        mem_x, mem_y = [], []
+        gen = torch.Generator(device="cpu").manual_seed(0)
+
+        def freeze(on):
+            for p, t in zip(params, trainable):
+                p.requires_grad_(t and not on)
+
+        freeze(True)
+        f_k, g_k, y_k = prob.fdtd_fom_and_grad(torch.sigmoid(z), fields=True)
+        n_adj += 1
         mark(f_k, True)
-        n_sur = 0
+        mem_x.append(prob.fno_input(torch.sigmoid(z)[None]))
+        mem_y.append(y_k / scale)
         for _ in range(iters - 1):
             if target is not None and f_k >= target:
                 break
@@ -310,7 +338,8 @@ def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None
             c0, cg = f_k - float(s_k.detach()), g_k - gs_k
             zc = z.clone().requires_grad_(True)
             opt = torch.optim.Adam([zc], lr=inner_lr)
-            for _ in range(inner):
+            cand = []
+            for j in range(1, probes[-1] + 1):
                 rho = torch.sigmoid(zc)
                 m = prob.fom(model(prob.fno_input(rho[None])) * scale)[0] + c0 + \
                     (cg * (rho - rho_k)).sum()
@@ -320,22 +349,46 @@ def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None
                 with torch.no_grad():
                     zc.copy_(torch.minimum(torch.maximum(zc, z - radius), z + radius))
                 n_sur += 1
-            with torch.no_grad():
-                rho = torch.sigmoid(zc)
-                pred = float(prob.fom(model(prob.fno_input(rho[None])) * scale)[0]) + c0 + \
-                    float((cg * (rho - rho_k)).sum()) - f_k
-            f_c, g_c = prob.fdtd_fom_and_grad(rho.detach())
-            ok = f_c > f_k
-            mark(f_c, ok)
+                if j in probes:
+                    cand.append(zc.detach().clone())
+            rhos = torch.sigmoid(torch.stack(cand))
+            y = prob.simulate(rhos, batch=len(cand))
+            n_fwd += 1
+            fc = prob.fom(y)
+            best = int(torch.argmax(fc))
+            ok = float(fc[best]) > f_k
+            if finetune:
+                mem_x.append(prob.fno_input(rhos))
+                mem_y.append(y / scale)
             if ok:
-                if f_c - f_k >= 0.75 * pred:
-                    radius = min(2.0 * radius, 4.0)
-                z, f_k, g_k = zc.detach().clone(), f_c, g_c
+                if best == len(cand) - 1:
+                    radius = min(2.0 * radius, 8.0)
+                z = cand[best]
+                f_k, g_k = prob.fdtd_fom_and_grad(torch.sigmoid(z))
+                n_adj += 1
             else:
                 radius *= 0.5
-        for p, g in frozen:
-            p.requires_grad_(g)
+            mark(f_k if ok else float(fc[best]), ok)
+            if finetune:
+                freeze(False)
+                xs, ys = torch.cat(mem_x), torch.cat(mem_y)
+                for _ in range(finetune):
+                    bx, by = xs, ys
+                    if replay is not None:
+                        idx = torch.randint(0, replay[0].shape[0], (16,), generator=gen)
+                        idx = idx.to(replay[0].device)
+                        bx = torch.cat([xs[-16:], replay[0][idx]])
+                        by = torch.cat([ys[-16:], replay[1][idx]])
+                    pred = model(bx)
+                    loss = ((pred - by).flatten(1).norm(dim=1) /
+                            by.flatten(1).norm(dim=1)).mean()
+                    ft_opt.zero_grad(set_to_none=True)
+                    loss.backward()
+                    ft_opt.step()
+                freeze(True)
+        freeze(False)
     if dev.type == "cuda":
         torch.cuda.synchronize(dev)
     return dict(fom=hist, t=times, accepted=acc, seconds=time.perf_counter() - t0,
-                surrogate_steps=n_sur, fdtd_runs=len(hist), rho=torch.sigmoid(z).detach())
+                surrogate_steps=n_sur, fdtd_runs=n_adj + n_fwd, adjoint_runs=n_adj,
+                rho=torch.sigmoid(z).detach())

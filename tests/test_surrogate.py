@@ -77,10 +77,18 @@ class _Quadratic:
         self.opt = 0.2 + 0.6 * torch.rand(8, 8, generator=g)
         self.runs = 0
 
-    def fdtd_fom_and_grad(self, rho):
+    def _f(self, rho):
+        return 10.0 - (rho - self.opt).square().sum(dim=(-2, -1)) / 64
+
+    def fdtd_fom_and_grad(self, rho, fields=False):
         self.runs += 1
-        d = rho - self.opt
-        return float(10.0 - d.square().sum() / 64), -2.0 * d / 64
+        f = float(self._f(rho))
+        g = -2.0 * (rho - self.opt) / 64
+        return (f, g, torch.full((1, 1, 1, 1), f)) if fields else (f, g)
+
+    def simulate(self, rhos, batch=0):
+        self.runs += 1
+        return self._f(rhos)[:, None, None, None]
 
     def fno_input(self, rho):
         return rho[:, None]
@@ -110,14 +118,16 @@ def test_trust_region_loop_monotone_and_reaches_target_cpu():
     assert plain["fom"][-1] > plain["fom"][0]
     model = _BiasedModel(prob.opt)
     target = 0.99999 * 10.0
-    sur = S.design_loop(prob, rho0, 40, model=model, target=target, inner=10, inner_lr=0.2)
+    sur = S.design_loop(prob, rho0, 40, model=model, target=target, inner=10, inner_lr=0.2,
+                        probes=(2, 5, 10))
     best = sur["fom"][0]
     for f, ok in zip(sur["fom"][1:], sur["accepted"][1:]):
         assert ok == (f > best)
         if ok:
             best = f
-    assert sur["fdtd_runs"] == len(sur["fom"])
-    assert sur["surrogate_steps"] == 10 * (sur["fdtd_runs"] - 1)
+    assert sur["fdtd_runs"] == prob.runs - 1 - len(plain["fom"]) + 1
+    assert sur["adjoint_runs"] == 1 + sum(sur["accepted"][1:])
+    assert sur["surrogate_steps"] == 10 * (len(sur["fom"]) - 1)
     # model parameters are left as they were (trainable, no gradient)
     assert model.w.requires_grad and model.w.grad is None
     assert max(sur["fom"]) > plain["fom"][-1]
@@ -136,11 +146,28 @@ def test_trust_region_rejects_bad_proposals_cpu():
         def forward(self, x):
             return (self.k * (x[:, 0] - 0.5).square().mean(dim=(1, 2)))[:, None, None, None]
 
-    out = S.design_loop(prob, torch.full((8, 8), 0.5), 12, model=Wrong(), inner=5)
+    out = S.design_loop(prob, torch.full((8, 8), 0.5), 12, model=Wrong(), inner=5,
+                        probes=(1, 5))
     accepted = [f for f, ok in zip(out["fom"], out["accepted"]) if ok]
     assert accepted == sorted(accepted)
-    d = out["rho"] - prob.opt
-    assert float(10.0 - d.square().sum() / 64) == pytest.approx(accepted[-1], abs=1e-5)
+    assert float(prob._f(out["rho"])) == pytest.approx(accepted[-1], abs=1e-5)
+
+
+def test_trust_region_finetunes_the_model_cpu():
+    """With finetune > 0 the surrogate learns from the verified probes (here the
+    'fields' are the FOM itself): its parameters move toward the FDTD values and are
+    left trainable afterwards."""
+    prob = _Quadratic()
+    model = _BiasedModel(prob.opt)
+    w0 = float(model.w.detach())
+    rx = torch.rand(32, 1, 8, 8)
+    ry = prob._f(rx[:, 0])[:, None, None, None]
+    out = S.design_loop(prob, torch.full((8, 8), 0.5), 6, model=model, inner=8,
+                        probes=(4, 8), finetune=5, ft_lr=0.05, replay=(rx, ry))
+    assert float(model.w.detach()) != w0
+    assert model.w.requires_grad
+    accepted = [f for f, ok in zip(out["fom"], out["accepted"]) if ok]
+    assert accepted == sorted(accepted) and len(accepted) >= 2
 
 
 # ------------------------------------------------------------------------ GPU
@@ -261,9 +288,11 @@ def test_short_end_to_end_loop():
     f, g = p.fdtd_fom_and_grad(rho[0])
     assert f == pytest.approx(float(p.fom(y[:1])[0]), rel=1e-5)
     assert g.shape == (64, 64) and torch.isfinite(g).all()
-    out = S.design_loop(p, torch.full((64, 64), 0.5), 4, model=m, scale=scale)
+    out = S.design_loop(p, torch.full((64, 64), 0.5), 4, model=m, scale=scale, finetune=2,
+                        replay=(x[:512], y[:512] / scale))
     acc = [v for v, ok in zip(out["fom"], out["accepted"]) if ok]
-    assert acc == sorted(acc) and out["fdtd_runs"] == 4
+    assert acc == sorted(acc) and len(out["fom"]) == 4
+    assert out["adjoint_runs"] == sum(out["accepted"]) and out["fdtd_runs"] == 3 + acc.__len__()
     plain = S.design_loop(p, torch.full((64, 64), 0.5), 3)
     assert plain["fom"][0] == pytest.approx(out["fom"][0], rel=1e-5)
     p.close()

@@ -138,3 +138,47 @@ def test_noalloc_rejects_oversize():
     assert rc == L.MTB_INVALID_ARG
     assert b"scratch" in lib.mtb_last_error()
     eng.close()
+
+
+
+def _reversed_rows(cells):
+    """A CSR source list with each row's columns (and weights) in descending order."""
+    row_ptr, col, w = cells
+    rp = row_ptr.cpu().tolist()
+    col, w = col.clone(), w.clone()
+    for r in range(len(rp) - 1):
+        if rp[r + 1] - rp[r] > 1:
+            col[rp[r]:rp[r + 1]] = col[rp[r]:rp[r + 1]].flip(0)
+            w[rp[r]:rp[r + 1]] = w[rp[r]:rp[r + 1]].flip(0)
+    return row_ptr, col, w
+
+
+def test_source_columns_must_ascend(monkeypatch):
+    """The kernels binary-search a row's source columns, so both entry points refuse
+    a row whose columns descend: the plan before any device work, the
+    allocation-free call with MTB_INVALID_ARG once its set-up kernel has flagged it
+    (every search probe stays inside the row's cell range either way)."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from meep_torch_b200 import _lib as L
+    from meep_torch_b200 import engine2d
+    lib = L.load()
+    orig = engine2d._cells
+    ok = engine2d.Engine2D([_items("tm", "cuda")], ring_slots=8)
+    monkeypatch.setattr(engine2d, "_cells", lambda m, n, d: _reversed_rows(orig(m, n, d)))
+    with pytest.raises(ValueError, match="ascending"):
+        engine2d.Engine2D([_items("tm", "cuda")], ring_slots=8)
+    it = ok.items[0]
+    bad = _reversed_rows(orig(it.source.mask, it.nx, "cuda"))
+    S = ok.structs[0]
+    S.src_e.row_ptr, S.src_e.col, S.src_e.w = (L.ptr(t) for t in bad)
+    stream = torch.cuda.current_stream().cuda_stream
+    ce, _ = _coefs(ok, 0, 4)
+    pe = ce.ctypes.data_as(C.POINTER(C.c_double))
+    rc = lib.mtb_yee2d_run_noalloc(ok.structs, ok.regions, ok.n_regions, ok.groups,
+                                   ok.n_groups, ok.ring_elems, 8, ok.current, 0, 4, pe, None,
+                                   stream)
+    assert rc == L.MTB_INVALID_ARG
+    assert b"ascending" in lib.mtb_last_error()
+    del bad
+    ok.close()
