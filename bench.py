@@ -294,7 +294,7 @@ def run_cfg5(args, rank, world, dev):
     prob = S.Cfg5Problem(dev)
     c = prob.c
     n_train, n_test = args.maps, 256
-    rho = S.grf_designs(n_train + n_test, seed=5 + 1009 * rank).to(dev)
+    rho = S.grf_designs(n_train + n_test, seed=5 + 1009 * rank, soft=0.5).to(dev)
     batch = min(1024, n_train)
     # data generation: one plan of `batch` designs, eps repacked per chunk
     prob.simulate(rho[:batch], batch=batch)                       # plan build + warm-up
@@ -317,11 +317,14 @@ def run_cfg5(args, rank, world, dev):
         fp = torch.cat([model(x[n_train + i:n_train + i + 64]) for i in range(0, n_test, 64)])
         ft = prob.fom(y[n_train:])
         fom_err = float(((prob.fom(fp * scale) - ft).abs() / ft).median())
+    replay = (x[:n_train], y[:n_train] / scale)
     del y
     rho0 = torch.full((c["design"], c["design"]), 0.5)
+    import copy
     for _ in range(args.warmup):                                   # plans, cuFFT, autotune
         S.design_loop(prob, rho0.to(dev), 2)
-        S.design_loop(prob, rho0.to(dev), 2, model=model, scale=scale)
+        S.design_loop(prob, rho0.to(dev), 2, model=copy.deepcopy(model), scale=scale,
+                      **CFG5_LOOP, replay=replay)
     torch.cuda.synchronize(dev)
     n0 = lib.mtb_launch_count()
     runs = []
@@ -329,8 +332,9 @@ def run_cfg5(args, rank, world, dev):
         for _ in range(args.steps):
             plain = S.design_loop(prob, rho0.to(dev), args.iters)
             target = 0.99 * plain["fom"][-1]
-            sur = S.design_loop(prob, rho0.to(dev), args.iters, model=model, scale=scale,
-                                target=target)
+            sur = S.design_loop(prob, rho0.to(dev), 2 * args.iters,
+                                model=copy.deepcopy(model), scale=scale, **CFG5_LOOP,
+                                replay=replay, target=target)
             runs.append((plain, sur, target))
     launches = lib.mtb_launch_count() - n0
     plain, sur, target = runs[len(runs) // 2]
@@ -338,8 +342,9 @@ def run_cfg5(args, rank, world, dev):
     host = rho0.pin_memory()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    out = S.design_loop(prob, host.to(dev, non_blocking=True), args.iters, model=model,
-                        scale=scale, target=target)
+    out = S.design_loop(prob, host.to(dev, non_blocking=True), 2 * args.iters,
+                        model=copy.deepcopy(model), scale=scale, **CFG5_LOOP, replay=replay,
+                        target=target)
     final = out["rho"].cpu()
     e2e_s = time.perf_counter() - t0
     spec = [{"nx": c["n"], "ny": c["n"], "pol": "tm"}] * batch
@@ -350,6 +355,12 @@ def run_cfg5(args, rank, world, dev):
                 bytes_launch=W.cfg2_bytes_per_step(spec, c["npml"]), train_s=train_s,
                 test_err=test_err, fom_err=fom_err, launches=launches,
                 clocks=clk.summary(), n_train=n_train)
+
+
+# surrogate-loop settings (chosen by a sweep of inner steps, probe sets, fine-tuning and
+# adjoint frequency on this problem)
+CFG5_LOOP = dict(inner=20, inner_lr=0.2, radius=2.0, probes=(2, 5, 10, 15, 20), finetune=2,
+                 grad_every=1)
 
 
 def cpu_sample_cfg5(steps):
@@ -757,7 +768,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--maps", type=int, default=20000, help="cfg5 training designs")
-    ap.add_argument("--epochs", type=int, default=20, help="cfg5 FNO training epochs")
+    ap.add_argument("--epochs", type=int, default=16, help="cfg5 FNO training epochs")
     ap.add_argument("--iters", type=int, default=50,
                     help="cfg5 design iterations (plain loop) / verifications (surrogate)")
     ap.add_argument("--rows", type=int, default=0, help="rows per warp (0 = library default)")
@@ -793,14 +804,18 @@ def main():
                               "objective mean |Ez|^2 of the 0.6/0.65/0.7 DFT on an 8 x 8 patch "
                               "behind the design",
                   "training_maps": args.maps, "test_maps": 256, "epochs": args.epochs,
-                  "maps": "Gaussian random fields, correlation 4 px (0.2 um), thresholded "
-                          "at 0, conic filter 0.1 um, seed 5",
+                  "maps": "Gaussian random fields, correlation 4 px (0.2 um); half thresholded "
+                          "at 0, half soft-thresholded sigmoid(beta g / std g), beta ~ U(0.5, 4); "
+                          "conic filter 0.1 um; seed 5",
                   "fno": "4 layers, width 64, 24 x 24 modes, BF16 autocast (FP32 "
                          "accumulation); FFTs in FP32",
                   "loops": f"plain: {args.iters} Adam steps (lr 0.05) on the FDTD adjoint "
-                           "gradient; surrogate: trust region, 10 FNO steps per FDTD "
-                           "adjoint verification, first-order corrected, stops at 99 % of "
-                           "the plain loop's final FOM",
+                           "gradient; surrogate: first-order-corrected trust region, blocks of "
+                           "20 FNO Adam steps (lr 0.2, radius 2 in z) probed after 2/5/10/15/20 "
+                           "steps, probes verified by one batched forward FDTD run, an adjoint "
+                           "run at each accepted probe, 2 fine-tuning steps per block on the "
+                           "verified fields plus replay; stops at 99 % of the plain loop's final "
+                           "FOM (at most 2x the plain iteration count in blocks)",
                   "l2": "data generation batches of 1024 x 256^2 designs (~1.5 GB of "
                         "fields): larger than L2; design loops are latency-bound"}
     elif args.workload == "cfg4":
@@ -943,6 +958,7 @@ def main():
                                    / plain["fom"][-1],
                                    "seconds": t_sur, "fdtd_runs": sur["fdtd_runs"],
                                    "surrogate_steps": sur["surrogate_steps"],
+                                   "adjoint_runs": sur["adjoint_runs"],
                                    "accepted": sum(sur["accepted"]) - 1,
                                    "speedup_vs_plain": plain["seconds"] / t_sur
                                    if reached else None},

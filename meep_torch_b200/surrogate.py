@@ -262,7 +262,8 @@ def rel_error(model: FNO2d, x: torch.Tensor, y: torch.Tensor, scale: float) -> f
 def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None,
                 scale: float = 1.0, lr: float = 0.05, inner: int = 40, inner_lr: float = 0.1,
                 radius: float = 1.0, probes=(5, 10, 20, 40), finetune: int = 0,
-                ft_lr: float = 2e-4, replay=None, target: float | None = None):
+                ft_lr: float = 2e-4, replay=None, grad_every: int = 1,
+                target: float | None = None):
     """Gradient ascent on the design latent z (rho = sigmoid(z)) from ``rho0``.
 
     Without ``model`` (the plain loop): ``iters`` Adam steps (``lr``), each on the FOM
@@ -275,8 +276,10 @@ def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None
     (f_k - s_k) + (g_k - grad s_k) . (rho - rho_k). ``inner`` surrogate Adam steps
     (``inner_lr``) maximise m with z kept within ``radius`` of z_k (max norm); the
     designs after each count in ``probes`` are verified together by one batched
-    forward FDTD run. The best verified probe becomes the next anchor (and gets its
-    adjoint run) if it beats f_k; the radius doubles when that probe is the last one
+    forward FDTD run. The best verified probe becomes the next anchor if it beats f_k;
+    every ``grad_every``-th new anchor gets an adjoint run, the others keep the last
+    adjoint anchor's gradient correction g - grad s with the value correction taken
+    from the verified FOM. The radius doubles when the accepted probe is the last one
     and halves when no probe beats f_k. With ``finetune`` > 0 the model then takes that
     many Adam steps (``ft_lr``) on the verified fields of this loop, mixed with
     samples of ``replay`` = (inputs, targets / scale) when given. The loop stops
@@ -328,14 +331,18 @@ def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None
         mark(f_k, True)
         mem_x.append(prob.fno_input(torch.sigmoid(z)[None]))
         mem_y.append(y_k / scale)
+        n_acc = 0
+        cg = None
         for _ in range(iters - 1):
             if target is not None and f_k >= target:
                 break
             rho_k = torch.sigmoid(z).detach()
             r = rho_k.clone().requires_grad_(True)
             s_k = prob.fom(model(prob.fno_input(r[None])) * scale)[0]
-            (gs_k,) = torch.autograd.grad(s_k, r)
-            c0, cg = f_k - float(s_k.detach()), g_k - gs_k
+            if g_k is not None or cg is None:
+                (gs_k,) = torch.autograd.grad(s_k, r)
+                cg = g_k - gs_k
+            c0 = f_k - float(s_k.detach())
             zc = z.clone().requires_grad_(True)
             opt = torch.optim.Adam([zc], lr=inner_lr)
             cand = []
@@ -364,8 +371,12 @@ def design_loop(prob: Cfg5Problem, rho0: torch.Tensor, iters: int, *, model=None
                 if best == len(cand) - 1:
                     radius = min(2.0 * radius, 8.0)
                 z = cand[best]
-                f_k, g_k = prob.fdtd_fom_and_grad(torch.sigmoid(z))
-                n_adj += 1
+                n_acc += 1
+                if n_acc % max(1, grad_every) == 0:
+                    f_k, g_k = prob.fdtd_fom_and_grad(torch.sigmoid(z))
+                    n_adj += 1
+                else:
+                    f_k, g_k = float(fc[best]), None
             else:
                 radius *= 0.5
             mark(f_k if ok else float(fc[best]), ok)

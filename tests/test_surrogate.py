@@ -296,3 +296,16 @@ def test_short_end_to_end_loop():
     plain = S.design_loop(p, torch.full((64, 64), 0.5), 3)
     assert plain["fom"][0] == pytest.approx(out["fom"][0], rel=1e-5)
     p.close()
+
+
+def test_trust_region_grad_every_cpu():
+    """grad_every = 2: every second accepted anchor gets an adjoint run; the loop
+    still only accepts verified improvements."""
+    prob = _Quadratic()
+    model = _BiasedModel(prob.opt)
+    out = S.design_loop(prob, torch.full((8, 8), 0.5), 10, model=model, inner=6,
+                        probes=(2, 4, 6), grad_every=2)
+    n_acc = sum(out["accepted"][1:])
+    assert out["adjoint_runs"] == 1 + n_acc // 2
+    accepted = [f for f, ok in zip(out["fom"], out["accepted"]) if ok]
+    assert accepted == sorted(accepted) and n_acc >= 2
