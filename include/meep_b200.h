@@ -479,6 +479,34 @@ int mtb_count_outside(const float *x, int64_t n0, int64_t n1, int64_t s0,
                       const uint8_t *active0, const uint8_t *active1,
                       int64_t *count_dev, void *stream);
 
+/* ------------------------------------------------- FNO channel mixes */
+
+/* The pointwise (1 x 1) layers of the Fourier neural operator of the surrogate
+ * design loop, on the tcgen05 tensor cores (no counterpart in the reference):
+ * BF16 operands, FP32 accumulation in TMEM. Tensors are NCHW float32 with
+ * `pixels` = H * W (a multiple of 8) per channel; built shapes: cin = 64, cout
+ * 64 or 128. All kernels run on `stream` and return at once; a bounded
+ * tensor-core wait that expired is reported by mtb_fno_status.
+ *
+ * mtb_fno_mix:    z = W x + bias + s (bias [cout] and s [batch, cout, pixels]
+ *                 optional), y = act ? GELU(z) : z (exact erf GELU); z is
+ *                 stored when non-NULL. W is [cout, cin] row-major.
+ * mtb_fno_mix_dx: dz = act ? dy * GELU'(z) : dy (stored when non-NULL),
+ *                 dx = W^T dz.
+ * mtb_fno_mix_dw: dw += dz x^T summed over images and pixels (dw [cout, cin],
+ *                 accumulated: zero it first); dz and x 16-byte aligned. */
+int mtb_fno_mix(const float *x, const float *w, const float *bias, const float *s, float *y,
+                float *z, int32_t batch, int32_t cin, int32_t cout, int64_t pixels,
+                int32_t act, void *stream);
+int mtb_fno_mix_dx(const float *dy, const float *z, const float *w, float *dz, float *dx,
+                   int32_t batch, int32_t cin, int32_t cout, int64_t pixels, int32_t act,
+                   void *stream);
+int mtb_fno_mix_dw(const float *dz, const float *x, float *dw, int32_t batch, int32_t cin,
+                   int32_t cout, int64_t pixels, void *stream);
+/* Waits for `stream`; MTB_DEVICE_TIMEOUT (and clears the flag) if a tensor-core
+ * wait of an earlier FNO launch expired. */
+int mtb_fno_status(void *stream);
+
 /* ------------------------------------------------------------ misc */
 
 const char *mtb_last_error(void);

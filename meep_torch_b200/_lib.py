@@ -154,6 +154,12 @@ SIGNATURES = {
     "mtb_abi_version": (C.c_int32, []),
     "mtb_struct_size": (C.c_int64, [C.c_int32]),
     "mtb_launch_count": (C.c_int64, []),
+    "mtb_fno_mix": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_int32,
+                              C.c_int64, C.c_int32, vp]),
+    "mtb_fno_mix_dx": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_int32,
+                                 C.c_int64, C.c_int32, vp]),
+    "mtb_fno_mix_dw": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int64, vp]),
+    "mtb_fno_status": (C.c_int, [vp]),
 }
 
 _lib = None

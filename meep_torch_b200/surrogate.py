@@ -38,7 +38,8 @@ import torch.nn.functional as F
 
 from .design import conic_filter
 
-__all__ = ["CFG5", "grf_designs", "Cfg5Problem", "FNO2d", "train_fno", "rel_error", "design_loop"]
+__all__ = ["CFG5", "grf_designs", "Cfg5Problem", "FNO2d", "channel_mix", "train_fno",
+           "rel_error", "design_loop"]
 
 CFG5 = dict(n=256, dx=0.05, npml=20, design=64, region=128, eps_min=1.0, eps_max=4.0,
             freqs=(0.6, 0.65, 0.7), fcen=0.65, fwidth=0.25, steps=3000, corr_px=4.0,
@@ -196,11 +197,73 @@ class _SpectralConv(nn.Module):
         return torch.fft.irfft2(out, s=(h, w))
 
 
-class FNO2d(nn.Module):
-    """Fourier neural operator: (B, 1, r, r) normalised eps -> (B, 6, r, r) fields."""
+class _ChannelMix(torch.autograd.Function):
+    """y = act(W x + b + s) over NCHW pixels on the library's tcgen05 kernels (BF16
+    operands, FP32 accumulation): mtb_fno_mix forward; mtb_fno_mix_dx (dz = dy *
+    GELU'(z), dx = W^T dz) and mtb_fno_mix_dw (dW = dz x^T) backward; db and ds are
+    sums / copies of dz."""
 
-    def __init__(self, width: int = 64, modes: int = 24, layers: int = 4, out_ch: int = 6):
+    @staticmethod
+    def forward(ctx, x, weight, bias, s, act):
+        from . import _lib as L
+        lib = L.load()
+        bsz, cin, h, w = x.shape
+        cout = weight.shape[0]
+        x = x.contiguous().float()
+        w2 = weight.reshape(cout, cin).contiguous().float()
+        b = bias.contiguous().float() if bias is not None else None
+        sv = s.contiguous().float() if s is not None else None
+        y = torch.empty(bsz, cout, h, w, device=x.device, dtype=torch.float32)
+        z = torch.empty_like(y) if act else None
+        st = torch.cuda.current_stream(x.device).cuda_stream
+        L.check(lib.mtb_fno_mix(L.ptr(x), L.ptr(w2), L.ptr(b) if b is not None else None,
+                                L.ptr(sv) if sv is not None else None, L.ptr(y),
+                                L.ptr(z) if z is not None else None, bsz, cin, cout, h * w,
+                                1 if act else 0, st), "mtb_fno_mix")
+        ctx.save_for_backward(x, w2, z)
+        ctx.act, ctx.has_b, ctx.has_s = bool(act), bias is not None, s is not None
+        ctx.wshape = weight.shape
+        return y
+
+    @staticmethod
+    def backward(ctx, dy):
+        from . import _lib as L
+        lib = L.load()
+        x, w2, z = ctx.saved_tensors
+        bsz, cin, h, w = x.shape
+        cout = w2.shape[0]
+        dy = dy.contiguous().float()
+        dz = torch.empty(bsz, cout, h, w, device=x.device, dtype=torch.float32)
+        dx = torch.empty_like(x)
+        dw = torch.zeros(cout, cin, device=x.device, dtype=torch.float32)
+        st = torch.cuda.current_stream(x.device).cuda_stream
+        L.check(lib.mtb_fno_mix_dx(L.ptr(dy), L.ptr(z) if z is not None else None, L.ptr(w2),
+                                   L.ptr(dz), L.ptr(dx), bsz, cin, cout, h * w,
+                                   1 if ctx.act else 0, st), "mtb_fno_mix_dx")
+        L.check(lib.mtb_fno_mix_dw(L.ptr(dz), L.ptr(x), L.ptr(dw), bsz, cin, cout, h * w, st),
+                "mtb_fno_mix_dw")
+        db = dz.sum(dim=(0, 2, 3)) if ctx.has_b else None
+        return dx, dw.reshape(ctx.wshape), db, (dz if ctx.has_s else None), None
+
+
+def channel_mix(x, weight, bias=None, s=None, act=False):
+    """act(W x + b + s) for NCHW x on the tcgen05 channel-mix kernels (CUDA only)."""
+    return _ChannelMix.apply(x, weight, bias, s, act)
+
+
+class FNO2d(nn.Module):
+    """Fourier neural operator: (B, 1, r, r) normalised eps -> (B, 6, r, r) fields.
+
+    On CUDA (``native``, the default) the four channel mixes (each fused with the
+    spectral branch's sum, the bias and GELU) and the 64 -> 128 projection run on the
+    library's tcgen05 kernels; the FFTs and per-mode complex mixes are cuFFT / cuBLAS
+    in FP32, the 3 -> 64 lift and 128 -> 6 head plain convolutions. ``native=False``
+    runs every layer through torch with BF16 autocast."""
+
+    def __init__(self, width: int = 64, modes: int = 24, layers: int = 4, out_ch: int = 6,
+                 native: bool = True):
         super().__init__()
+        self.native = native
         self.lift = nn.Conv2d(3, width, 1)
         self.spec = nn.ModuleList([_SpectralConv(width, modes) for _ in range(layers)])
         self.mix = nn.ModuleList([nn.Conv2d(width, width, 1) for _ in range(layers)])
@@ -212,6 +275,13 @@ class FNO2d(nn.Module):
         gy, gx = torch.meshgrid(torch.linspace(0, 1, h, device=x.device),
                                 torch.linspace(0, 1, w, device=x.device), indexing="ij")
         x = torch.cat([x, gy.expand(b, 1, h, w), gx.expand(b, 1, h, w)], dim=1)
+        if self.native and x.is_cuda:
+            x = self.lift(x)
+            n = len(self.spec)
+            for k, (s, m) in enumerate(zip(self.spec, self.mix)):
+                x = channel_mix(x, m.weight, m.bias, s(x), act=k < n - 1)
+            x = channel_mix(x, self.proj1.weight, self.proj1.bias, None, act=True)
+            return self.proj2(x)
         with torch.autocast("cuda", dtype=torch.bfloat16, enabled=x.is_cuda):
             x = self.lift(x)
             for k, (s, m) in enumerate(zip(self.spec, self.mix)):

@@ -309,3 +309,58 @@ def test_trust_region_grad_every_cpu():
     assert out["adjoint_runs"] == 1 + n_acc // 2
     accepted = [f for f, ok in zip(out["fom"], out["accepted"]) if ok]
     assert accepted == sorted(accepted) and n_acc >= 2
+
+
+def _bf(t):
+    return t.detach().to(torch.bfloat16).float()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cout,act,hw", [(64, True, (24, 24)), (64, False, (16, 16)),
+                                         (128, True, (32, 20))])
+def test_channel_mix_kernels_vs_fp32(cout, act, hw):
+    """The tcgen05 channel mix (forward, dx, dW) against FP32 torch on the same
+    BF16-rounded operands: only the accumulation order differs. 576 pixels exercise
+    a partial 128-pixel tile."""
+    import torch.nn.functional as F
+
+    from meep_torch_b200 import _lib as L
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(3)
+    bsz, cin = 3, 64
+    h, w = hw
+    x = torch.randn(bsz, cin, h, w, generator=g).to(dev).requires_grad_(True)
+    W = (torch.randn(cout, cin, 1, 1, generator=g) / 8).to(dev).requires_grad_(True)
+    b = torch.randn(cout, generator=g).to(dev).requires_grad_(True)
+    s = torch.randn(bsz, cout, h, w, generator=g).to(dev).requires_grad_(True)
+    y = S.channel_mix(x, W, b, s, act)
+    zr = (torch.einsum("oi,bihw->bohw", _bf(W[:, :, 0, 0]), _bf(x)) + b.detach()[None, :, None, None]
+          + s.detach()).requires_grad_(True)
+    yr = F.gelu(zr) if act else zr
+
+    def rel(a, r):
+        return float((a.detach() - r.detach()).norm() / r.detach().norm())
+    assert rel(y, yr) < 1e-5
+    dy = torch.randn(y.shape, generator=g).to(dev)
+    y.backward(dy)
+    yr.backward(dy)
+    dzr = zr.grad
+    dxr = torch.einsum("oi,bohw->bihw", _bf(W[:, :, 0, 0]), _bf(dzr))
+    dwr = torch.einsum("bohw,bihw->oi", _bf(dzr), _bf(x))
+    assert rel(x.grad, dxr) < 1e-4
+    assert rel(W.grad[:, :, 0, 0], dwr) < 1e-4
+    assert rel(b.grad, dzr.sum(dim=(0, 2, 3))) < 1e-5
+    assert rel(s.grad, dzr) < 1e-5
+    L.check(L.load().mtb_fno_status(torch.cuda.current_stream().cuda_stream), "mtb_fno_status")
+
+
+@pytest.mark.gpu
+def test_channel_mix_rejects_unbuilt_shapes():
+    from meep_torch_b200 import _lib as L
+    dev = torch.device("cuda", 0)
+    x = torch.randn(1, 32, 8, 8, device=dev)
+    with pytest.raises(L.MtbUnsupported):
+        S.channel_mix(x, torch.randn(64, 32, 1, 1, device=dev))
+    x = torch.randn(1, 64, 3, 3, device=dev)                      # 9 pixels: not a multiple of 8
+    with pytest.raises(ValueError):
+        S.channel_mix(x, torch.randn(64, 64, 1, 1, device=dev))
