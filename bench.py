@@ -807,8 +807,10 @@ def main():
                   "maps": "Gaussian random fields, correlation 4 px (0.2 um); half thresholded "
                           "at 0, half soft-thresholded sigmoid(beta g / std g), beta ~ U(0.5, 4); "
                           "conic filter 0.1 um; seed 5",
-                  "fno": "4 layers, width 64, 24 x 24 modes, BF16 autocast (FP32 "
-                         "accumulation); FFTs in FP32",
+                  "fno": "4 layers, width 64, 24 x 24 modes; channel mixes and the 64->128 "
+                         "projection on the library's tcgen05 kernels (BF16 operands, FP32 "
+                         "accumulation in TMEM), forward and backward; FFTs and per-mode "
+                         "complex mixes FP32 (cuFFT / cuBLAS)",
                   "loops": f"plain: {args.iters} Adam steps (lr 0.05) on the FDTD adjoint "
                            "gradient; surrogate: first-order-corrected trust region, blocks of "
                            "20 FNO Adam steps (lr 0.2, radius 2 in z) probed after 2/5/10/15/20 "

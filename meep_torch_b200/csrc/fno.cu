@@ -32,10 +32,13 @@ namespace mtb {
 namespace {
 
 constexpr int FNO_THREADS = 128;
-// Dynamic shared memory per CTA: large enough that at most two CTAs share an SM,
-// so their TMEM (at most 2 x 128 columns) never exceeds the SM's 512 columns and
-// tcgen05.alloc never waits on another CTA.
+// Dynamic shared memory per CTA: 100 KB, so that at most two CTAs share an SM. Their
+// TMEM (at most 2 x 128 columns) then never exceeds the SM's 512 columns and
+// tcgen05.alloc never waits on another CTA. (Smaller requests, up to 7 CTAs per SM,
+// measured 1.6-1.7x slower per launch on the cfg5 training shapes.)
 constexpr int FNO_SMEM = 100 * 1024;
+constexpr int smem_bytes(int need, int) { return need > FNO_SMEM ? need : FNO_SMEM; }
+constexpr int tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
 constexpr long long FNO_SPIN = 1LL << 24;        // polls of one mbarrier wait
 
 __device__ int g_fno_err;
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(FNO_THREADS, 1)
     unsigned char *sB = smem + A_BYTES;
     FnoShared *sh = reinterpret_cast<FnoShared *>(smem + A_BYTES + NOUT * KIN * 2);
     const int t = threadIdx.x, warp = t >> 5;
-    constexpr uint32_t NCOLS = NOUT <= 32 ? 32 : NOUT <= 64 ? 64 : NOUT <= 128 ? 128 : 256;
+    constexpr uint32_t NCOLS = tmem_cols(NOUT);
 
     // B operand: forward B[n=o][k=i] = W[o, i] (W is C_out x C_in);
     // dx        B[n=i][k=o] = W[o, i]  (here KIN = C_out, NOUT = C_in)
@@ -215,25 +218,42 @@ __global__ void __launch_bounds__(FNO_THREADS, 1)
         const int b = (int)(tile / tiles_per_img);
         const long long p = (tile % tiles_per_img) * 128 + t;
         const bool valid = p < P;
-        // A[m = pixel][k]: forward x[b, k, p]; dx dz[b, k, p] = dy * GELU'(z)
+        // A[m = pixel][k]: forward x[b, k, p]; dx dz[b, k, p] = dy * GELU'(z).
+        // 32 channels per pass: all loads first (32 or 64 in flight per thread),
+        // then the transform and the four 16-byte shared stores.
 #pragma unroll 1
-        for (int kc = 0; kc < KIN; kc += 8) {
-            float v[8];
+        for (int k0 = 0; k0 < KIN; k0 += 32) {
+            float v[32], zz[DX ? 32 : 1];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const long long g = ((long long)b * KIN + kc + j) * P + p;
-                float a = valid ? src[g] : 0.f;
-                if (DX && valid) {
-                    if (act) a *= gelu_grad(zin[g]);
-                    if (aux) aux[g] = a;
-                }
-                v[j] = a;
+            for (int j = 0; j < 32; ++j) {
+                const long long g = ((long long)b * KIN + k0 + j) * P + p;
+                v[j] = valid ? src[g] : 0.f;
+                if (DX) zz[DX ? j : 0] = (valid && act) ? zin[g] : 0.f;
             }
-            st_shared16(smem_u32(sA) + kmaj(t, kc, SBO_A), pack_bf16(v[0], v[1]),
-                        pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+            if (DX) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    if (act) v[j] *= gelu_grad(zz[DX ? j : 0]);
+                    if (aux && valid) aux[((long long)b * KIN + k0 + j) * P + p] = v[j];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                st_shared16(smem_u32(sA) + kmaj(t, k0 + 8 * c, SBO_A),
+                            pack_bf16(v[8 * c], v[8 * c + 1]), pack_bf16(v[8 * c + 2], v[8 * c + 3]),
+                            pack_bf16(v[8 * c + 4], v[8 * c + 5]),
+                            pack_bf16(v[8 * c + 6], v[8 * c + 7]));
         }
         fence_async_smem();
         __syncthreads();
+        // the spectral term of this pixel, fetched while the tensor cores run
+        constexpr bool PRE = !DX && NOUT <= 64;
+        float sp[PRE ? NOUT : 1];
+        if (PRE) {
+#pragma unroll
+            for (int o = 0; o < (PRE ? NOUT : 1); ++o)
+                sp[o] = (s && valid) ? s[((long long)b * NOUT + o) * P + p] : 0.f;
+        }
         if (t == 0) {
             fence_after();
 #pragma unroll
@@ -251,7 +271,7 @@ __global__ void __launch_bounds__(FNO_THREADS, 1)
         __syncthreads();
         if (!sh->ok) break;
         fence_after();
-#pragma unroll 1
+#pragma unroll
         for (int g = 0; g < NOUT; g += 16) {
             float v[16];
             tmem_ld16(lane_base + g, v);
@@ -263,7 +283,8 @@ __global__ void __launch_bounds__(FNO_THREADS, 1)
                 float z = v[j];
                 if (!DX) {
                     if (bias) z += bias[o];
-                    if (s) z += s[gi];
+                    if (PRE) z += sp[(PRE ? o : 0)];
+                    else if (s) z += s[gi];
                     if (aux) aux[gi] = z;
                     if (act) z = gelu(z);
                 }
@@ -293,7 +314,7 @@ __global__ void __launch_bounds__(FNO_THREADS, 1)
     unsigned char *sB = smem + A_BYTES;
     FnoShared *sh = reinterpret_cast<FnoShared *>(smem + A_BYTES + CIN * KT * 2);
     const int t = threadIdx.x, warp = t >> 5;
-    constexpr uint32_t NCOLS = CIN <= 32 ? 32 : CIN <= 64 ? 64 : CIN <= 128 ? 128 : 256;
+    constexpr uint32_t NCOLS = tmem_cols(CIN);
     // rows COUT .. 127 of A stay zero
     for (int q = t; q < (128 - COUT) * KT / 8; q += FNO_THREADS) {
         const int r = COUT + q / (KT / 8), kc = (q % (KT / 8)) * 8;
@@ -320,6 +341,7 @@ __global__ void __launch_bounds__(FNO_THREADS, 1)
         const int b = (int)(tile / tiles_per_img);
         const long long p0 = (tile % tiles_per_img) * KT;
         // 8 consecutive pixels of one row per chunk (float4 pairs; P % 8 == 0)
+#pragma unroll 4
         for (int q = t; q < (COUT + CIN) * (KT / 8); q += FNO_THREADS) {
             const int row = q / (KT / 8), kc = (q % (KT / 8)) * 8;
             const bool isA = row < COUT;
@@ -387,10 +409,25 @@ int sm_count() {
     return n;
 }
 
+// shared memory a launch of each kernel requests (operands + barrier block)
+template <int KIN, int NOUT>
+constexpr int pointwise_smem() {
+    return smem_bytes(128 * KIN * 2 + NOUT * KIN * 2 + 64, tmem_cols(NOUT));
+}
+template <int CIN>
+constexpr int dw_smem() {
+    return smem_bytes(128 * 128 * 2 + CIN * 128 * 2 + 64, tmem_cols(CIN));
+}
+
+// sets the kernel's shared-memory limit and returns its grid: one wave of the CTAs
+// the SMs can hold (at most two per SM), at most one per tile
 template <class K>
-int prepare(K kern) {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      FNO_SMEM));
+int prepare(K kern, int smem, long long tiles, int *grid) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FNO_THREADS, smem));
+    if (per_sm < 1) return fail(MTB_CUDA_ERROR, "fno: kernel does not fit on an SM");
+    *grid = (int)std::min<long long>(tiles, (long long)std::min(per_sm, 2) * sm_count());
     return MTB_OK;
 }
 
@@ -422,14 +459,16 @@ int mtb_fno_mix(const float *x, const float *w, const float *bias, const float *
     if (!x || !w || !y) return fail(MTB_INVALID_ARG, "fno_mix: null x, w or y");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long tiles = (long long)batch * ((pixels + 127) / 128);
-    const int grid = (int)std::min<long long>(tiles, 2LL * sm_count());
+    int grid = 0;
     if (cout == 64) {
-        if ((rc = prepare(k_fno_pointwise<64, 64, false>))) return rc;
-        k_fno_pointwise<64, 64, false><<<grid, FNO_THREADS, FNO_SMEM, st>>>(
+        constexpr int sm = pointwise_smem<64, 64>();
+        if ((rc = prepare(k_fno_pointwise<64, 64, false>, sm, tiles, &grid))) return rc;
+        k_fno_pointwise<64, 64, false><<<grid, FNO_THREADS, sm, st>>>(
             x, nullptr, w, bias, s, y, z, batch, pixels, act);
     } else {
-        if ((rc = prepare(k_fno_pointwise<64, 128, false>))) return rc;
-        k_fno_pointwise<64, 128, false><<<grid, FNO_THREADS, FNO_SMEM, st>>>(
+        constexpr int sm = pointwise_smem<64, 128>();
+        if ((rc = prepare(k_fno_pointwise<64, 128, false>, sm, tiles, &grid))) return rc;
+        k_fno_pointwise<64, 128, false><<<grid, FNO_THREADS, sm, st>>>(
             x, nullptr, w, bias, s, y, z, batch, pixels, act);
     }
     MTB_CHECK_LAUNCH();
@@ -444,14 +483,16 @@ int mtb_fno_mix_dx(const float *dy, const float *z, const float *w, float *dz, f
     if (!dy || !w || !dx || (act && !z)) return fail(MTB_INVALID_ARG, "fno_mix_dx: null input");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long tiles = (long long)batch * ((pixels + 127) / 128);
-    const int grid = (int)std::min<long long>(tiles, 2LL * sm_count());
+    int grid = 0;
     if (cout == 64) {
-        if ((rc = prepare(k_fno_pointwise<64, 64, true>))) return rc;
-        k_fno_pointwise<64, 64, true><<<grid, FNO_THREADS, FNO_SMEM, st>>>(
+        constexpr int sm = pointwise_smem<64, 64>();
+        if ((rc = prepare(k_fno_pointwise<64, 64, true>, sm, tiles, &grid))) return rc;
+        k_fno_pointwise<64, 64, true><<<grid, FNO_THREADS, sm, st>>>(
             dy, z, w, nullptr, nullptr, dx, dz, batch, pixels, act);
     } else {
-        if ((rc = prepare(k_fno_pointwise<128, 64, true>))) return rc;
-        k_fno_pointwise<128, 64, true><<<grid, FNO_THREADS, FNO_SMEM, st>>>(
+        constexpr int sm = pointwise_smem<128, 64>();
+        if ((rc = prepare(k_fno_pointwise<128, 64, true>, sm, tiles, &grid))) return rc;
+        k_fno_pointwise<128, 64, true><<<grid, FNO_THREADS, sm, st>>>(
             dy, z, w, nullptr, nullptr, dx, dz, batch, pixels, act);
     }
     MTB_CHECK_LAUNCH();
@@ -467,13 +508,14 @@ int mtb_fno_mix_dw(const float *dz, const float *x, float *dw, int32_t batch, in
         return fail(MTB_INVALID_ARG, "fno_mix_dw: dz and x must be 16-byte aligned");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long tiles = (long long)batch * ((pixels + 127) / 128);
-    const int grid = (int)std::min<long long>(tiles, 2LL * sm_count());
+    int grid = 0;
+    constexpr int sm = dw_smem<64>();
     if (cout == 64) {
-        if ((rc = prepare(k_fno_dw<64, 64>))) return rc;
-        k_fno_dw<64, 64><<<grid, FNO_THREADS, FNO_SMEM, st>>>(dz, x, dw, batch, pixels);
+        if ((rc = prepare(k_fno_dw<64, 64>, sm, tiles, &grid))) return rc;
+        k_fno_dw<64, 64><<<grid, FNO_THREADS, sm, st>>>(dz, x, dw, batch, pixels);
     } else {
-        if ((rc = prepare(k_fno_dw<128, 64>))) return rc;
-        k_fno_dw<128, 64><<<grid, FNO_THREADS, FNO_SMEM, st>>>(dz, x, dw, batch, pixels);
+        if ((rc = prepare(k_fno_dw<128, 64>, sm, tiles, &grid))) return rc;
+        k_fno_dw<128, 64><<<grid, FNO_THREADS, sm, st>>>(dz, x, dw, batch, pixels);
     }
     MTB_CHECK_LAUNCH();
     return MTB_OK;

@@ -1,9 +1,11 @@
 """Surrogate-assisted inverse design on the FDTD engine (the cfg5 workload).
 
 The FDTD data and every verification run through the library's batched 2D TM kernels.
-The surrogate is a Fourier neural operator (FNO) trained on those runs. Its spectral
-transforms are cuFFT (torch.fft) and its channel mixes are BF16 cuBLAS GEMMs under
-autocast, with FP32 accumulation: library calls, as for any plain GEMM here.
+The surrogate is a Fourier neural operator (FNO) trained on those runs. Its pointwise
+channel mixes (fused with the spectral branch's sum, the bias and GELU) and its
+64 -> 128 projection run forward and backward on the library's tcgen05 kernels (BF16
+operands, FP32 accumulation in TMEM). The spectral transforms are cuFFT (torch.fft),
+and the per-mode complex mixes are FP32 cuBLAS: library calls.
 
 Pieces:
 
