@@ -32,12 +32,15 @@ namespace mtb {
 namespace {
 
 constexpr int FNO_THREADS = 128;
-// Dynamic shared memory per CTA: 100 KB, so that at most two CTAs share an SM. Their
-// TMEM (at most 2 x 128 columns) then never exceeds the SM's 512 columns and
-// tcgen05.alloc never waits on another CTA. (Smaller requests, up to 7 CTAs per SM,
-// measured 1.6-1.7x slower per launch on the cfg5 training shapes.)
-constexpr int FNO_SMEM = 100 * 1024;
-constexpr int smem_bytes(int need, int) { return need > FNO_SMEM ? need : FNO_SMEM; }
+// Dynamic shared memory per CTA: at least what the operands need, and at least a
+// floor that bounds the CTAs an SM can hold (233472 bytes of shared memory, 1 KB
+// reserved per CTA) so that their TMEM never exceeds the SM's 512 columns and
+// tcgen05.alloc never waits on another CTA: 64 columns -> 29 KB floor (at most 7 CTAs,
+// 448 columns); 128 columns -> 58 KB (at most 3 CTAs, 384 columns).
+constexpr int smem_bytes(int need, int ncols) {
+    return need > (ncols <= 64 ? 29 * 1024 : 58 * 1024) ? need
+                                                        : (ncols <= 64 ? 29 * 1024 : 58 * 1024);
+}
 constexpr int tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
 constexpr long long FNO_SPIN = 1LL << 24;        // polls of one mbarrier wait
 
@@ -420,14 +423,21 @@ constexpr int dw_smem() {
 }
 
 // sets the kernel's shared-memory limit and returns its grid: one wave of the CTAs
-// the SMs can hold (at most two per SM), at most one per tile
+// the SMs hold at once (by registers, shared memory and TMEM columns), at most one
+// per tile. The residency is computed here from the kernel's register count:
+// cudaOccupancyMaxActiveBlocksPerMultiprocessor reported one CTA per SM for these
+// kernels where two and more are resident.
 template <class K>
-int prepare(K kern, int smem, long long tiles, int *grid) {
+int prepare(K kern, int smem, int ncols, long long tiles, int *grid) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int per_sm = 0;
-    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FNO_THREADS, smem));
-    if (per_sm < 1) return fail(MTB_CUDA_ERROR, "fno: kernel does not fit on an SM");
-    *grid = (int)std::min<long long>(tiles, (long long)std::min(per_sm, 2) * sm_count());
+    cudaFuncAttributes fa;
+    MTB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;     // per-warp granularity
+    const int by_regs = 65536 / (regs_warp * (FNO_THREADS / 32));
+    const int by_smem = 233472 / (smem + (int)fa.sharedSizeBytes + 1024);
+    const int by_tmem = 512 / ncols;
+    const int per_sm = std::max(1, std::min(std::min(by_regs, by_smem), by_tmem));
+    *grid = (int)std::min<long long>(tiles, (long long)per_sm * sm_count());
     return MTB_OK;
 }
 
@@ -462,12 +472,12 @@ int mtb_fno_mix(const float *x, const float *w, const float *bias, const float *
     int grid = 0;
     if (cout == 64) {
         constexpr int sm = pointwise_smem<64, 64>();
-        if ((rc = prepare(k_fno_pointwise<64, 64, false>, sm, tiles, &grid))) return rc;
+        if ((rc = prepare(k_fno_pointwise<64, 64, false>, sm, 64, tiles, &grid))) return rc;
         k_fno_pointwise<64, 64, false><<<grid, FNO_THREADS, sm, st>>>(
             x, nullptr, w, bias, s, y, z, batch, pixels, act);
     } else {
         constexpr int sm = pointwise_smem<64, 128>();
-        if ((rc = prepare(k_fno_pointwise<64, 128, false>, sm, tiles, &grid))) return rc;
+        if ((rc = prepare(k_fno_pointwise<64, 128, false>, sm, 128, tiles, &grid))) return rc;
         k_fno_pointwise<64, 128, false><<<grid, FNO_THREADS, sm, st>>>(
             x, nullptr, w, bias, s, y, z, batch, pixels, act);
     }
@@ -486,12 +496,12 @@ int mtb_fno_mix_dx(const float *dy, const float *z, const float *w, float *dz, f
     int grid = 0;
     if (cout == 64) {
         constexpr int sm = pointwise_smem<64, 64>();
-        if ((rc = prepare(k_fno_pointwise<64, 64, true>, sm, tiles, &grid))) return rc;
+        if ((rc = prepare(k_fno_pointwise<64, 64, true>, sm, 64, tiles, &grid))) return rc;
         k_fno_pointwise<64, 64, true><<<grid, FNO_THREADS, sm, st>>>(
             dy, z, w, nullptr, nullptr, dx, dz, batch, pixels, act);
     } else {
         constexpr int sm = pointwise_smem<128, 64>();
-        if ((rc = prepare(k_fno_pointwise<128, 64, true>, sm, tiles, &grid))) return rc;
+        if ((rc = prepare(k_fno_pointwise<128, 64, true>, sm, 64, tiles, &grid))) return rc;
         k_fno_pointwise<128, 64, true><<<grid, FNO_THREADS, sm, st>>>(
             dy, z, w, nullptr, nullptr, dx, dz, batch, pixels, act);
     }
@@ -511,10 +521,10 @@ int mtb_fno_mix_dw(const float *dz, const float *x, float *dw, int32_t batch, in
     int grid = 0;
     constexpr int sm = dw_smem<64>();
     if (cout == 64) {
-        if ((rc = prepare(k_fno_dw<64, 64>, sm, tiles, &grid))) return rc;
+        if ((rc = prepare(k_fno_dw<64, 64>, sm, 64, tiles, &grid))) return rc;
         k_fno_dw<64, 64><<<grid, FNO_THREADS, sm, st>>>(dz, x, dw, batch, pixels);
     } else {
-        if ((rc = prepare(k_fno_dw<128, 64>, sm, tiles, &grid))) return rc;
+        if ((rc = prepare(k_fno_dw<128, 64>, sm, 64, tiles, &grid))) return rc;
         k_fno_dw<128, 64><<<grid, FNO_THREADS, sm, st>>>(dz, x, dw, batch, pixels);
     }
     MTB_CHECK_LAUNCH();
