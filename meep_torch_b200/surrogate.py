@@ -41,7 +41,7 @@ import torch.nn.functional as F
 from .design import conic_filter
 
 __all__ = ["CFG5", "grf_designs", "Cfg5Problem", "FNO2d", "channel_mix", "train_fno",
-           "rel_error", "design_loop"]
+           "rel_error", "design_loop", "shard_range"]
 
 CFG5 = dict(n=256, dx=0.05, npml=20, design=64, region=128, eps_min=1.0, eps_max=4.0,
             freqs=(0.6, 0.65, 0.7), fcen=0.65, fwidth=0.25, steps=3000, corr_px=4.0,
@@ -293,33 +293,93 @@ class FNO2d(nn.Module):
         return x.float()
 
 
+def shard_range(n: int, rank: int, world: int) -> tuple:
+    """Contiguous [start, stop) of n designs owned by ``rank`` of ``world``; shard sizes
+    differ by at most one. Data generation runs each shard on its own rank with no
+    collective (the designs are independent)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of world {world}")
+    base, extra = divmod(n, world)
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+def _dist(group):
+    """(torch.distributed, world size) when a process group is up, else (None, 1)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return None, 1
+    return dist, dist.get_world_size(group)
+
+
+def _real_views(ts):
+    return [torch.view_as_real(t) if t.is_complex() else t for t in ts]
+
+
+def _allreduce_mean_grads(params, dist, group, world):
+    """Mean of every parameter gradient over the ranks, through one flat buffer
+    (complex gradients travel as their real and imaginary parts)."""
+    for p in params:
+        if p.grad is None:
+            p.grad = torch.zeros_like(p)
+    views = _real_views([p.grad for p in params])
+    flat = torch.cat([v.reshape(-1) for v in views])
+    dist.all_reduce(flat, group=group)
+    flat /= world
+    off = 0
+    for v in views:
+        v.copy_(flat[off:off + v.numel()].view_as(v))
+        off += v.numel()
+
+
 def train_fno(model: FNO2d, x: torch.Tensor, y: torch.Tensor, *, epochs: int = 30,
-              batch: int = 32, lr: float = 2e-3, scale: float | None = None, log=None):
+              batch: int = 32, lr: float = 2e-3, scale: float | None = None, log=None,
+              group=None):
     """Adam + cosine schedule on the relative L2 error of the (scaled) fields. Returns
-    (scale, seconds): targets are divided by ``scale`` (their RMS unless given)."""
+    (scale, seconds): targets are divided by ``scale`` (their RMS unless given).
+
+    Under torch.distributed (a process group is initialised) the training is data-parallel:
+    x, y are this rank's shard, ``batch`` is per rank, rank 0's parameters are broadcast
+    first, every step all-reduces the mean gradient (one flat buffer), the RMS scale is
+    global, and every rank takes the smallest shard's number of steps per epoch."""
+    dist, world = _dist(group)
+    params = list(model.parameters())
+    if world > 1:
+        for v in _real_views([p.data for p in params]):
+            dist.broadcast(v, 0, group=group)
     if scale is None:
-        scale = float(y.pow(2).mean().sqrt())
+        ss = torch.tensor([float(y.pow(2).sum(dtype=torch.float64)), float(y.numel())],
+                          dtype=torch.float64, device=y.device)
+        if world > 1:
+            dist.all_reduce(ss, group=group)
+        scale = float((ss[0] / ss[1]).sqrt())
+    spe = max(1, x.shape[0] // batch)
+    if world > 1:
+        n = torch.tensor([spe], dtype=torch.int64, device=y.device)
+        dist.all_reduce(n, op=dist.ReduceOp.MIN, group=group)
+        spe = int(n.item())
     yn = y / scale
-    opt = torch.optim.Adam(model.parameters(), lr=lr)
-    steps = epochs * max(1, x.shape[0] // batch)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, steps)
+    opt = torch.optim.Adam(params, lr=lr)
+    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, epochs * spe)
     g = torch.Generator(device="cpu").manual_seed(0)
     t0 = time.perf_counter()
     for ep in range(epochs):
         perm = torch.randperm(x.shape[0], generator=g)
         tot = 0.0
-        for b0 in range(0, x.shape[0] - batch + 1, batch):
-            idx = perm[b0:b0 + batch].to(x.device)
+        for k in range(spe):
+            idx = perm[k * batch:(k + 1) * batch].to(x.device)
             pred = model(x[idx])
             t = yn[idx]
             loss = ((pred - t).flatten(1).norm(dim=1) / t.flatten(1).norm(dim=1)).mean()
             opt.zero_grad(set_to_none=True)
             loss.backward()
+            if world > 1:
+                _allreduce_mean_grads(params, dist, group, world)
             opt.step()
             sched.step()
             tot += float(loss.detach())
         if log is not None:
-            log(ep, tot / max(1, x.shape[0] // batch))
+            log(ep, tot / spe)
     if x.is_cuda:
         torch.cuda.synchronize(x.device)
     return scale, time.perf_counter() - t0
