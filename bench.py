@@ -49,6 +49,8 @@ sys.path.insert(0, ROOT)
 
 STEPS_PER_RUN = {"cfg2": 5000, "cfg3": 2000, "cfg1": 4000}
 S_CFG5_STEPS = 3000
+CFG5_METRIC = ("design-iterations/s (plain-loop iterations matched per second of the surrogate "
+               "loop, at <= 1% FOM error)")
 
 
 def peaks():
@@ -734,6 +736,70 @@ def run_cfg3_slabs(args, rank, world, dev):
     return res
 
 
+def reference_line(args, config, threads):
+    """The reference arm: the oracle port of the reference's CPU path, timed on the
+    host cores on a bounded sample of the chosen workload, in that workload's metric."""
+    from meep_torch_b200 import workloads as W
+    wl = args.workload
+    vals = []
+    t_all = time.perf_counter()
+    if wl == "cfg2":
+        unit = "Gcell-updates/s"
+        specs = W.cfg2_specs()[:args.cpu_structs]
+        for _ in range(args.warmup and 1):
+            cpu_sample(specs[:1], 2, 1)
+        t_all = time.perf_counter()
+        for _ in range(args.steps):
+            cells, sec = cpu_sample(specs, args.cpu_steps, threads)
+            vals.append(cells / sec / 1e9)
+        cores = threads
+        sample = (f"oracle numpy float32 TM/TE step + DFT/flux monitors, cfg2 structures "
+                  f"0..{len(specs) - 1} x {args.cpu_steps} steps per bench step, {threads} "
+                  "threads over structures")
+    elif wl == "cfg1":
+        unit, cores = "Gcell-updates/s", 1
+        for _ in range(args.steps):
+            cells, sec = cpu_sample_cfg1(4000)
+            vals.append(cells / sec / 1e9)
+        sample = "oracle numpy float32 cfg1, the full 4000-step run per bench step, one thread"
+    elif wl == "cfg3":
+        unit, cores = "Gcell-updates/s", 1
+        for _ in range(args.steps):
+            cells, sec = cpu_sample_cfg3(8, n=args.n3)
+            vals.append(cells / sec / 1e9)
+        sample = (f"oracle numpy float32 cfg3 {args.n3}^3 grid with its source and six flux "
+                  "faces, 8 steps per bench step, one thread")
+    elif wl == "cfg4":
+        unit, cores = "gradient-evaluations/s", 1
+        n = args.run_steps if args.run_steps != 5000 else W.CFG4["steps"]
+        for _ in range(args.steps):
+            sec = cpu_sample_cfg4(300)
+            vals.append(1.0 / (sec / 300 * 2 * n))
+        sample = (f"oracle numpy float32 forward, 300 steps of the cfg4 grid per bench step, "
+                  f"one thread; a gradient costed as 2 x {n} steps (the oracle has no reverse "
+                  "mode)")
+    else:
+        unit, cores = "design-iterations/s", 1
+        for _ in range(args.steps):
+            sec = cpu_sample_cfg5(S_CFG5_STEPS)
+            vals.append(1.0 / (2 * sec))
+        sample = (f"oracle numpy float32 forward with the 3-frequency DFT, the full "
+                  f"{S_CFG5_STEPS}-step run of one cfg5 design per bench step, one thread; a "
+                  "plain design iteration costed as two runs (the oracle has no reverse mode "
+                  "and no surrogate)")
+    wall = time.perf_counter() - t_all
+    v = statistics.median(vals)
+    metric = CFG5_METRIC if wl == "cfg5" else unit
+    return {"metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall / max(args.steps, 1) * 1e3,
+            "higher_is_better": True, "impl": "reference", "dtype": "f32",
+            "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -857,30 +923,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        line = {"metric": "Gcell-updates/s", "unit": "Gcell-updates/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                "impl": "reference", "dtype": "f32", "data": "synthetic", "config": config}
-        vals = []
-        from meep_torch_b200 import workloads as W
-        specs = W.cfg2_specs()[:args.cpu_structs]
-        for _ in range(args.warmup and 1):
-            cpu_sample(specs[:1], 2, 1)
-        t_all = time.perf_counter()
-        for _ in range(args.steps):
-            cells, sec = cpu_sample(specs, args.cpu_steps, threads)
-            vals.append(cells / sec / 1e9)
-        wall = time.perf_counter() - t_all
-        v = statistics.median(vals)
-        line.update(value=v, ms_per_step=wall / max(args.steps, 1) * 1e3,
-                    cpu_baseline={"value": v, "unit": "Gcell-updates/s", "cores": threads,
-                                  "kind": "port",
-                                  "sample": f"oracle numpy float32 TM/TE step + DFT/flux "
-                                            f"monitors, cfg2 structures 0..{len(specs) - 1} x "
-                                            f"{args.cpu_steps} steps per bench step, {threads} "
-                                            "threads over structures"},
-                    e2e={"value": v, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
-                         "d2h_bytes_per_step": 0})
-        print(json.dumps(line))
+        print(json.dumps(reference_line(args, config, threads)))
         return
 
     import torch
@@ -943,8 +986,7 @@ def main():
         peak, peak_kind = peaks()
         step_avg = r["step_ms"] / max(r["step_n"], 1)
         ach = r["bytes_launch"] / (step_avg / 1e3) / 1e9 if step_avg else None
-        line = {"metric": "design-iterations/s (plain-loop iterations matched per second of "
-                          "the surrogate loop, at <= 1% FOM error)",
+        line = {"metric": CFG5_METRIC,
                 "value": n_it / t_sur if reached else None,
                 "unit": "design-iterations/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": (plain["seconds"] + sur["seconds"]) * 1e3,
