@@ -300,7 +300,7 @@ def run_cfg5(args, rank, world, dev):
     batch = min(1024, n_train)
     # data generation: one plan of `batch` designs, eps repacked per chunk
     prob.simulate(rho[:batch], batch=batch)                       # plan build + warm-up
-    eng = prob._engines[batch]
+    eng = prob.plan(batch)
     eng.set_timing(True)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()

@@ -147,6 +147,10 @@ class Cfg5Problem:
             eng.reset()
         return eng
 
+    def plan(self, n: int):
+        """The Engine2D kept for batches of ``n`` designs (None before the first)."""
+        return getattr(self, "_engines", {}).get(n)
+
     def close(self):
         for eng in getattr(self, "_engines", {}).values():
             eng.close()
