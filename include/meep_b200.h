@@ -169,6 +169,15 @@ typedef struct mtb_yee2d_struct {
     const float *pol_c[3];
     float *pol_py[3];
     const float *pol_cy[3];
+    /* Magnetic conductivity / permeability (core/coeffs.py:161-175, :410-414):
+     * H' = h1 H - h2 curl E (TM Hx, TE Hz) or h1 H + h2 curl E (TM Hy), with
+     * h1 = (1 - sigma_b dt/2) / (1 + sigma_b dt/2), h2 = dt / (mu (1 + sigma_b dt/2))
+     * Yee-averaged onto the H nodes. TM: slot 0 = Hx (h1x, h2x), slot 1 = Hy
+     * (h1y, h2y); TE: slot 0 = Hz (hz1, hz2), slot 1 unused. Box layout like
+     * the field; NULL = the plain step (h1 = 1, h2 = dt). Tile kernels only
+     * (variant 2); the other variants and the adjoint return MTB_UNSUPPORTED. */
+    const float *mag_h1[2];
+    const float *mag_h2[2];
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

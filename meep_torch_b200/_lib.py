@@ -48,7 +48,8 @@ class Yee2DStruct(C.Structure):
                 ("yband", C.c_int32 * 4), ("pad_", C.c_int32), ("ring_full", C.c_int64 * 3),
                 ("cond_d1", vp * 2), ("cond_d2", vp * 2),
                 ("n_poles", C.c_int32), ("n_poles_y", C.c_int32), ("pol_p", vp * 3),
-                ("pol_c", vp * 3), ("pol_py", vp * 3), ("pol_cy", vp * 3)]
+                ("pol_c", vp * 3), ("pol_py", vp * 3), ("pol_cy", vp * 3),
+                ("mag_h1", vp * 2), ("mag_h2", vp * 2)]
 
 
 class PhaseGroup(C.Structure):

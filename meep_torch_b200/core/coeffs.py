@@ -122,7 +122,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("chi3", "chi2", "sigma_b", "mu", "m_poles",
+_UNSUPPORTED = ("chi3", "chi2", "m_poles",
                 "m_pole_masks", "y_mirror", "x_mirror", "y_rot2", "rot4", "eps_tensor",
                 "poles_tensor", "pole_masks_tensor")
 
@@ -138,16 +138,17 @@ def _reject(kw):
             f"{k}: not implemented on the B200 path (use the reference stepper)")
 
 
-def _cond_tm(grid: Grid, sigma_d):
-    """Electric conductivity pairs of core/coeffs.py:161-175 with sigma_b = 0 and mu = 1:
-    d1 = (1 - sd dt/2) / (1 + sd dt/2), d2 = dt / (1 + sd dt/2) on Dz, and the inert
-    magnetic pairs h1 = 1, h2 = dt the reference builds alongside them."""
-    if sigma_d is None:
+def _cond_tm(grid: Grid, sigma_d, sigma_b=None, mu=None):
+    """Conductivity / permeability pairs of core/coeffs.py:161-175, built when any of
+    sigma_d, sigma_b, mu is given: d1 = (1 - sd dt/2) / (1 + sd dt/2), d2 = dt / (1 +
+    sd dt/2) on Dz; h1 = (1 - sb dt/2) / (1 + sb dt/2), h2 = dt / (mu (1 + sb dt/2)) with
+    sigma_b and mu averaged onto Hx (along y) and Hy (along x)."""
+    if sigma_d is None and sigma_b is None and mu is None:
         return {}
     dt = grid.dt
     sd = _as_field(sigma_d, grid, 0.0)
-    sb = _as_field(None, grid, 0.0)
-    mu_ = _as_field(None, grid, 1.0)
+    sb = _as_field(sigma_b, grid, 0.0)
+    mu_ = _as_field(mu, grid, 1.0)
     sbx, mux = 0.5 * (sb[:, :-1] + sb[:, 1:]), 0.5 * (mu_[:, :-1] + mu_[:, 1:])
     sby, muy = 0.5 * (sb[:-1, :] + sb[1:, :]), 0.5 * (mu_[:-1, :] + mu_[1:, :])
     return dict(d1=(1 - sd * dt / 2) / (1 + sd * dt / 2), d2=dt / (1 + sd * dt / 2),
@@ -155,14 +156,15 @@ def _cond_tm(grid: Grid, sigma_d):
                 h1y=(1 - sby * dt / 2) / (1 + sby * dt / 2), h2y=dt / (muy * (1 + sby * dt / 2)))
 
 
-def _cond_te(grid: Grid, sigma_d):
-    """TE pairs of core/coeffs.py:401-415: sigma_d averaged to Ex / Ey, inert Hz pair."""
-    if sigma_d is None:
+def _cond_te(grid: Grid, sigma_d, sigma_b=None, mu=None):
+    """TE pairs of core/coeffs.py:401-415: sigma_d averaged to Ex / Ey, sigma_b and mu
+    averaged over the four nodes around Hz."""
+    if sigma_d is None and sigma_b is None and mu is None:
         return {}
     dt = grid.dt
     sd = _as_field(sigma_d, grid, 0.0)
-    sb = _as_field(None, grid, 0.0)
-    mu_ = _as_field(None, grid, 1.0)
+    sb = _as_field(sigma_b, grid, 0.0)
+    mu_ = _as_field(mu, grid, 1.0)
     sdx, sdy = _avg_to_ex(sd), _avg_to_ey(sd)
     sbz = 0.25 * (sb[:-1, :-1] + sb[1:, :-1] + sb[:-1, 1:] + sb[1:, 1:])
     muz = 0.25 * (mu_[:-1, :-1] + mu_[1:, :-1] + mu_[:-1, 1:] + mu_[1:, 1:])
@@ -197,12 +199,14 @@ def _poles_tm(grid: Grid, eps, poles, pole_masks):
 
 
 def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
-                    y_pmc: bool = False, sigma_d=None, **kw) -> TMCoeffs:
+                    y_pmc: bool = False, sigma_d=None, sigma_b=None, mu=None,
+                    **kw) -> TMCoeffs:
     """TM coefficients: eps map, CPML profiles sliced to the live nodes --
     H side on the n-1 half nodes, E side on the interior [1:-1] (the full
     axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291;
-    ``sigma_d`` (scalar or (nx, ny)) gives the conductivity pairs of :161-175,
-    ``poles`` / ``pole_masks`` the ADE recurrences of :87-106, :195-203."""
+    ``sigma_d``, ``sigma_b``, ``mu`` (scalars or (nx, ny)) give the conductivity and
+    permeability pairs of :161-175, ``poles`` / ``pole_masks`` the ADE recurrences of
+    :87-106, :195-203."""
     _reject(kw)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
@@ -229,7 +233,7 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
-        chi2=zero.clone(), has_chi2=False, **_cond_tm(grid, sigma_d))
+        chi2=zero.clone(), has_chi2=False, **_cond_tm(grid, sigma_d, sigma_b, mu))
 
 
 def _avg_to_ex(v):
@@ -261,11 +265,12 @@ def _axis_poles(grid: Grid, eps, shared, axis_poles, shared_masks, axis_masks, s
 
 def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     sigma_d=None, poles_x=(), poles_y=(), pole_masks_x=None,
-                    pole_masks_y=None, **kw) -> TECoeffs:
+                    pole_masks_y=None, sigma_b=None, mu=None, **kw) -> TECoeffs:
     """TE coefficients: eps Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1)
     (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491, with
-    ``sigma_d`` the conductivity pairs of :401-415, and the per-axis ADE pole stacks
-    of :416-425 (shared ``poles`` on both axes, ``poles_x`` / ``poles_y`` on one)."""
+    ``sigma_d``, ``sigma_b``, ``mu`` the conductivity and permeability pairs of
+    :401-415, and the per-axis ADE pole stacks of :416-425 (shared ``poles`` on both
+    axes, ``poles_x`` / ``poles_y`` on one)."""
     _reject(kw)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
@@ -294,4 +299,4 @@ def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         chi2_x=_avg_to_ex(zero), chi2_y=_avg_to_ey(zero), has_chi2=False,
-        **_cond_te(grid, sigma_d))
+        **_cond_te(grid, sigma_d, sigma_b, mu))

@@ -407,7 +407,8 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     const mtb_yee2d_struct &S = *s;
     if (S.pol != MTB_TM && S.pol != MTB_TE) return fail(MTB_INVALID_ARG, "adjoint: bad pol");
     if (S.y_pmc) return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc)");
-    if (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y)
+    if (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y || S.mag_h1[0] ||
+        S.mag_h1[1])
         return fail(MTB_UNSUPPORTED, "adjoint: conductivity and poles are forward-only");
     if (S.nx < 3 || S.ny < 3 || S.pitch < S.ny || (S.pitch & 3))
         return fail(MTB_INVALID_ARG, "adjoint: bad grid %d x %d, pitch %d", S.nx, S.ny, S.pitch);

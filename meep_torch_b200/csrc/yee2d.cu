@@ -866,16 +866,25 @@ __device__ __forceinline__ bool band4(int jb, int lo, int hi) { return jb < lo |
 
 // Hy(n+1/2) of one row from Ez rows r (ea), r+1 (eb): core/stepper_tm.py:97-100,
 // :119-128, magnetic sheet source :116-118. `valid` = r <= nx-2.
+// With magnetic conductivity / permeability (`h1`, `h2` non-null, box layout):
+// Hy' = h1 Hy + h2 curl (core/stepper_tm.py:121-125).
 __device__ __forceinline__ void tm_hy(const mtb_yee2d_struct &S, int r, bool valid, bool act,
                                       int jb, float b, float a, float dt, float rdx,
                                       const float (&ea)[4], const float (&eb)[4],
                                       const float (&hy)[4], float (&ps)[4], float (&out)[4],
-                                      const float *amp_h) {
+                                      const float *amp_h, const float *h1 = nullptr,
+                                      const float *h2 = nullptr) {
+    float m1[4] = {1.f, 1.f, 1.f, 1.f}, m2[4] = {dt, dt, dt, dt};
+    if (h1 && valid && act) {
+        const uint32_t o = (uint32_t)r * S.pitch + jb;
+        ld4(h1 + o, m1);
+        ld4(h2 + o, m2);
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float d = (eb[q] - ea[q]) * rdx;
         const float pv = b * ps[q] + a * d;
-        const float hn = hy[q] + dt * (d + pv);
+        const float hn = h1 ? m1[q] * hy[q] + m2[q] * (d + pv) : hy[q] + dt * (d + pv);
         out[q] = valid ? hn : hy[q];
         ps[q] = valid ? pv : ps[q];
     }
@@ -996,20 +1005,30 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
     float ezR = __shfl_down_sync(0xffffffffu, ez1[0], 1);
     if (lane == 31) ezR = ezr;
 
-    // Hy(n+1/2) rows i-1 (recomputed halo) and i
+    // Hy(n+1/2) rows i-1 (recomputed halo) and i; magnetic conductivity /
+    // permeability pairs when the structure has them
+    const float *mh1y = EXT ? S.mag_h1[1] : nullptr, *mh2y = EXT ? S.mag_h2[1] : nullptr;
     float hyP[4], hyN[4];
-    tm_hy(S, i - 1, i >= 1, act, jb, hxbp, hxap, dt, rdx, ez0, ez1, hyp, p1p, hyP, C.amp_h);
+    tm_hy(S, i - 1, i >= 1, act, jb, hxbp, hxap, dt, rdx, ez0, ez1, hyp, p1p, hyP, C.amp_h,
+          mh1y, mh2y);
     if (i < 1) zero4(hyP);
-    tm_hy(S, i, hyRow, act, jb, hxb, hxa, dt, rdx, ez1, ez2, hy, p1, hyN, C.amp_h);
+    tm_hy(S, i, hyRow, act, jb, hxb, hxa, dt, rdx, ez1, ez2, hy, p1, hyN, C.amp_h, mh1y, mh2y);
 
-    // Hx(n+1/2) row i (core/stepper_tm.py:91-94, :121-128)
+    // Hx(n+1/2) row i (core/stepper_tm.py:91-94, :121-128): Hx' = Hx - dt curl, or
+    // h1x Hx - h2x curl with magnetic pairs
+    const bool magx = EXT && S.mag_h1[0] != nullptr;
+    float mx1[4] = {1.f, 1.f, 1.f, 1.f}, mx2[4] = {dt, dt, dt, dt};
+    if (magx && act) {
+        ld4(S.mag_h1[0] + ro, mx1);
+        ld4(S.mag_h2[0] + ro, mx2);
+    }
     float hxN[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float er = (q < 3) ? ez1[q + 1] : ezR;
         const float d = (er - ez1[q]) * rdx;
         const float pv = hyb[q] * p0[q] + hya[q] * d;
-        const float hn = hx[q] - dt * (d + pv);
+        const float hn = magx ? mx1[q] * hx[q] - mx2[q] * (d + pv) : hx[q] - dt * (d + pv);
         hxN[q] = vH[q] ? hn : hx[q];
         p0[q] = vH[q] ? pv : p0[q];
     }
@@ -1022,7 +1041,7 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             const float d = (ez1[0] - ezl) * rdx;
             float c = d;
             if (byHL) c = d + (__ldg(S.hy_b + jl) * p0l + __ldg(S.hy_a + jl) * d);
-            v = hxl - dt * c;
+            v = magx ? S.mag_h1[0][ro - 1] * hxl - S.mag_h2[0][ro - 1] * c : hxl - dt * c;
             if (i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
                 v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
         }
@@ -1335,7 +1354,14 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     float exr = __shfl_down_sync(0xffffffffu, ex[0], 1);
     if (lane == 31) exr = exR;
 
-    // Hz(n+1) row i (core/stepper_te.py:113-117)
+    // Hz(n+1) row i (core/stepper_te.py:113-117): Hz' = Hz - dt curl, or
+    // hz1 Hz - hz2 curl with magnetic conductivity / permeability
+    const bool magz = EXT && S.mag_h1[0] != nullptr;
+    float mz1[4] = {1.f, 1.f, 1.f, 1.f}, mz2[4] = {dt, dt, dt, dt};
+    if (magz && act) {
+        ld4(S.mag_h1[0] + ro, mz1);
+        ld4(S.mag_h2[0] + ro, mz2);
+    }
     float hzN[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -1344,7 +1370,8 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
         const float dex = (exn - ex[q]) * rdx;
         const float q2 = hxb * p2[q] + hxa * dey;
         const float q3 = hyb[q] * p3[q] + hya[q] * dex;
-        const float hn_ = hc[q] - dt * ((dey + q2) - (dex + q3));
+        const float cz = (dey + q2) - (dex + q3);
+        const float hn_ = magz ? mz1[q] * hc[q] - mz2[q] * cz : hc[q] - dt * cz;
         hzN[q] = vZ[q] ? hn_ : hc[q];
         p2[q] = vZ[q] ? q2 : p2[q];
         p3[q] = vZ[q] ? q3 : p3[q];
@@ -1579,7 +1606,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const bool lean = C.wr == WROWS && !expl && ib >= 1 && last <= S.nx - 2 &&
                       ib - 1 >= S.xband[0] && last < S.xband[1] &&
                       ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr &&
-                      S.n_poles == 0;
+                      S.n_poles == 0 && S.mag_h1[0] == nullptr && S.mag_h1[1] == nullptr;
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1811,7 +1838,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
     const bool lean = C.wr == WROWS && ib >= 1 && last + 1 <= S.nx - 2 && ib >= S.xband[0] &&
                       last < S.xband[1] &&
                       ib >= S.xband[2] && last + 1 < S.xband[3] && S.cond_d1[0] == nullptr &&
-                      S.n_poles == 0 && S.n_poles_y == 0;
+                      S.n_poles == 0 && S.n_poles_y == 0 && S.mag_h1[0] == nullptr;
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -2000,6 +2027,17 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         } else if (S.cond_d2[0] || S.cond_d2[1]) {
             return fail(MTB_INVALID_ARG, "structure %d: cond_d2 without cond_d1", s);
         }
+        for (int k = 0; k < 2; ++k) {
+            if (!S.mag_h1[k] && !S.mag_h2[k]) continue;
+            if (k == 1 && S.pol == MTB_TE)
+                return fail(MTB_INVALID_ARG, "structure %d: TE magnetic pairs use slot 0 only",
+                            s);
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: magnetic conductivity needs the "
+                            "tile kernels (variant 2)", s);
+            if ((rc = check_ptr(S.mag_h1[k], "mag_h1", s))) return rc;
+            if ((rc = check_ptr(S.mag_h2[k], "mag_h2", s))) return rc;
+        }
         for (int a = 0; a < 2; ++a) {
             const int np = a ? S.n_poles_y : S.n_poles;
             if (np < 0 || np > MTB_MAX_POLES)
@@ -2080,7 +2118,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     p->n_work = (int)n_work;
     for (int s = 0; s < n; ++s)
     {
-        if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0)
+        if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0 ||
+            structs[s].mag_h1[0] || structs[s].mag_h1[1])
             p->ext = true;
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
     }
@@ -2516,7 +2555,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     if (S.pol == MTB_TE && (S.y_pmc || S.src_h2.n > 0))
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
     if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles ||
-        S.n_poles_y)
+        S.n_poles_y || S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1])
         return fail(MTB_UNSUPPORTED, "noalloc: conductivity and poles need the tile kernels");
     int rc;
     for (int b = 0; b < 2; ++b) {

@@ -50,18 +50,22 @@ def _opt_none(obj, names):
               f"{type(obj).__name__}.{n} is set: not supported by the B200 path")
 
 
-def _inert_magnetic(c, pairs):
-    """The reference builds the magnetic pairs (h1, h2) whenever it builds the electric
-    conductivity ones (core/coeffs.py:161-175, :401-415); they run here only inert:
-    h1 = 1 and h2 = dt (no sigma_b, mu = 1), where H' = h1 H - h2 curl is the plain step."""
+def _magnetic_pairs(c, pairs):
+    """The magnetic pairs (h1, h2) of core/coeffs.py:161-175, :401-415, one entry per H
+    component named in ``pairs``: None where they are absent or inert (h1 = 1 and h2 =
+    dt, where H' = h1 H - h2 curl is the plain step), else the two tensors."""
     dt = torch.tensor(float(c.dt), dtype=torch.float32)
+    out = []
     for n1, n2 in pairs:
         h1, h2 = getattr(c, n1, None), getattr(c, n2, None)
         if h1 is None and h2 is None:
+            out.append(None)
             continue
-        _need(h1 is not None and h2 is not None and bool(torch.all(h1 == 1)) and
-              bool(torch.all(h2.to(torch.float32) == dt.to(h2.device))),
-              f"magnetic conductivity / mu ({n1}, {n2}): not supported by the B200 path")
+        _need(h1 is not None and h2 is not None, f"magnetic pair ({n1}, {n2}) incomplete")
+        inert = bool(torch.all(h1 == 1)) and \
+            bool(torch.all(h2.to(torch.float32) == dt.to(h2.device)))
+        out.append(None if inert else (h1, h2))
+    return out
 
 
 def coef_table(source, attr: str, t0: int, k: int, dt: float) -> np.ndarray:
@@ -178,7 +182,7 @@ class Engine2D:
                 _need(n_ <= L.MTB_MAX_POLES, f"{n_} dispersive poles (at most {L.MTB_MAX_POLES})")
                 _need(getattr(c, cn).shape[0] == n_, f"pole coefficients {cn} count")
             _opt_none(c, ["inv_xx_x", "c3xy", "c3yx", "has_chi2", "y_mirror_lo", "x_mirror_lo"])
-            _inert_magnetic(c, [("hz1", "hz2")])
+            it.mag = _magnetic_pairs(c, [("hz1", "hz2")])
         else:
             it.nx, it.ny = main.shape
             np_ = s.P_cur.shape[0]
@@ -187,7 +191,7 @@ class Engine2D:
             _opt_none(s, ["Bx", "Hx0", "Hy0"])
             _opt_none(c, ["mc1x", "has_chi2", "y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
                           "rot4_lo"])
-            _inert_magnetic(c, [("h1x", "h2x"), ("h1y", "h2y")])
+            it.mag = _magnetic_pairs(c, [("h1x", "h2x"), ("h1y", "h2y")])
         _need(not getattr(c, "has_kerr", False), "Kerr (chi3) media")
         for k in ("k_hx", "k_hy", "k_ex", "k_ey"):
             kv = getattr(c, k)
@@ -391,6 +395,15 @@ class Engine2D:
                 it.plain = False
                 d2e = getattr(c, cond[-1][1])
                 it.src_scale = d2e.to(device=dev, dtype=torch.float32) / float(c.dt)
+            # magnetic conductivity / permeability: H' = h1 H -/+ h2 curl
+            # (core/stepper_tm.py:121-125, core/stepper_te.py:112-114)
+            for k, pr in enumerate(it.mag):
+                if pr is None:
+                    continue
+                b1, b2 = self._pack(pr[0], nx, P), self._pack(pr[1], nx, P)
+                S.mag_h1[k], S.mag_h2[k] = L.ptr(b1), L.ptr(b2)
+                it.keep += [b1, b2]
+                it.plain = False
             self._check_psi_outside(it)
             hx, hy, ex, ey = self._profiles(it)
             S.hx_b, S.hx_a = L.ptr(hx[0]), L.ptr(hx[1])

@@ -80,6 +80,12 @@ def _cond_pair(sd, dt):
     return (1 - sd * dt / 2) / (1 + sd * dt / 2), dt / (1 + sd * dt / 2)
 
 
+def _mag_pair(sb, mu, dt):
+    """(h1, h2) of a magnetic conductivity / permeability pair on the H nodes
+    (core/coeffs.py:171-175, :413-414)."""
+    return (1 - sb * dt / 2) / (1 + sb * dt / 2), dt / (mu * (1 + sb * dt / 2))
+
+
 def pole_recurrence(pole, dt):
     """(c1, c2, c3) of one ADE pole (core/coeffs.py:87-106): pole = (fn, gamma,
     sigma[, fc]); Lorentz with fc = fn, Drude with fn = 0 and fc the plasma
@@ -93,13 +99,15 @@ def pole_recurrence(pole, dt):
 
 
 def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
-              dtype=np.float64, sigma=None, poles=(), pole_masks=None):
+              dtype=np.float64, sigma=None, poles=(), pole_masks=None, sigma_b=None, mu=None):
     """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
 
     Profiles are sliced to the live derivative nodes exactly as
     core/coeffs.py:251-278: H side at half nodes (n-1 long); E side on the
     interior [1:-1] (or the full axis under y_pmc). ``sigma`` (nx, ny): the
-    electric conductivity pair (d1, d2) of :161-166 on Dz."""
+    electric conductivity pair (d1, d2) of :161-166 on Dz; ``sigma_b`` and ``mu``
+    (nx, ny): the magnetic pairs of :167-175, averaged onto Hx along y and onto Hy
+    along x. Any of the three builds all the pairs, as the reference does."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -117,8 +125,17 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
     else:
         b_ey, a_ey, k_ey = b_eyf[1:-1], a_eyf[1:-1], k_eyf[1:-1]
     cond = {}
-    if sigma is not None:
-        cond["d1"], cond["d2"] = _cond_pair(np.asarray(sigma, dtype=dtype), dt)
+    if sigma is not None or sigma_b is not None or mu is not None:
+        z, one = np.zeros((nx, ny), dtype=dtype), np.ones((nx, ny), dtype=dtype)
+        sd = z if sigma is None else np.asarray(sigma, dtype=dtype)
+        sb = z if sigma_b is None else np.asarray(sigma_b, dtype=dtype)
+        mu_ = one if mu is None else np.asarray(mu, dtype=dtype)
+        h = dtype.type(0.5)
+        cond["d1"], cond["d2"] = _cond_pair(sd, dt)
+        cond["h1x"], cond["h2x"] = _mag_pair(h * (sb[:, :-1] + sb[:, 1:]),
+                                             h * (mu_[:, :-1] + mu_[:, 1:]), dt)
+        cond["h1y"], cond["h2y"] = _mag_pair(h * (sb[:-1, :] + sb[1:, :]),
+                                             h * (mu_[:-1, :] + mu_[1:, :]), dt)
     n_p = len(poles)
     c1, c2, c3 = (np.zeros((n_p, nx, ny), dtype=dtype) for _ in range(3))
     for k, pole in enumerate(poles):        # core/coeffs.py:195-203
@@ -162,8 +179,13 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
     dEz_dx = (Ez[1:, :] - Ez[:-1, :]) / T(dx)
     psi_Ezx = c["b_hx"] * s["psi_Ezx"] + c["a_hx"] * dEz_dx
     curl_hy = dEz_dx / c["k_hx"] + psi_Ezx
-    Hx = s["Hx"] - T(dt) * curl_hx
-    Hy = s["Hy"] + T(dt) * curl_hy
+    if "h1x" in c:
+        # magnetic conductivity / permeability (core/stepper_tm.py:121-125)
+        Hx = c["h1x"] * s["Hx"] - c["h2x"] * curl_hx
+        Hy = c["h1y"] * s["Hy"] + c["h2y"] * curl_hy
+    else:
+        Hx = s["Hx"] - T(dt) * curl_hx
+        Hy = s["Hy"] + T(dt) * curl_hy
     # magnetic sheet current (mode sources), subtracted (core/stepper_tm.py:186-196)
     if hy_mask is not None:
         Hy = Hy - T(dt * amp_h) * hy_mask
@@ -206,12 +228,13 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
 # ---------------------------------------------------------------- 2D TE
 
 def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None,
-              poles=(), pole_masks=None):
+              poles=(), pole_masks=None, sigma_b=None, mu=None):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
     (core/coeffs.py:347-354); so is ``sigma`` for the conductivity pairs of
-    :401-409 on Dx and Dy."""
+    :401-409 on Dx and Dy. ``sigma_b`` and ``mu`` give the Hz pair of :410-414,
+    averaged over the four nodes around each Hz. Any of the three builds all pairs."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -227,10 +250,17 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
     b_ey, a_ey, k_ey = (v[1:-1] for v in cpml_profiles(ny, py, 0.0, dt, dx, dtype=dtype))
     b_ex, a_ex, k_ex = (v[1:-1] for v in cpml_profiles(nx, px, 0.0, dt, dx, dtype=dtype))
     cond = {}
-    if sigma is not None:
-        sd = np.asarray(sigma, dtype=dtype)
+    if sigma is not None or sigma_b is not None or mu is not None:
+        z, one = np.zeros((nx, ny), dtype=dtype), np.ones((nx, ny), dtype=dtype)
+        sd = z if sigma is None else np.asarray(sigma, dtype=dtype)
+        sb = z if sigma_b is None else np.asarray(sigma_b, dtype=dtype)
+        mu_ = one if mu is None else np.asarray(mu, dtype=dtype)
+        q = dtype.type(0.25)
         cond["d1x"], cond["d2x"] = _cond_pair(h * (sd[:-1, :] + sd[1:, :]), dt)
         cond["d1y"], cond["d2y"] = _cond_pair(h * (sd[:, :-1] + sd[:, 1:]), dt)
+        cond["hz1"], cond["hz2"] = _mag_pair(
+            q * (sb[:-1, :-1] + sb[1:, :-1] + sb[:-1, 1:] + sb[1:, 1:]),
+            q * (mu_[:-1, :-1] + mu_[1:, :-1] + mu_[:-1, 1:] + mu_[1:, 1:]), dt)
     # shared ADE poles on both E axes, masks Yee-averaged (core/coeffs.py:109-131, :416-425)
     for ax, shape in (("x", (nx - 1, ny)), ("y", (nx, ny - 1))):
         n_p = len(poles)
@@ -305,7 +335,11 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
     psi_Eyx = c["b_hx"] * s["psi_Eyx"] + c["a_hx"] * dEy_dx
     psi_Exy = c["b_hy"] * s["psi_Exy"] + c["a_hy"] * dEx_dy
     curl_z = dEy_dx / c["k_hx"] + psi_Eyx - dEx_dy / c["k_hy"] - psi_Exy
-    Hz_new = Hz - T(dt) * curl_z
+    if "hz1" in c:
+        # magnetic conductivity / permeability (core/stepper_te.py:112-114)
+        Hz_new = c["hz1"] * Hz - c["hz2"] * curl_z
+    else:
+        Hz_new = Hz - T(dt) * curl_z
     if hz_mask is not None:
         Hz_new = Hz_new - T(dt * amp_h) * hz_mask
     return dict(Hz=Hz_new, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy, psi_Eyx=psi_Eyx,

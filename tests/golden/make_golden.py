@@ -17,7 +17,8 @@ cases of the hot path through its own public functions:
 * d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
   and of ``run_te`` (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
-  ``make_golden.py sigma``) and the TM and TE cases with a Lorentz and a Drude pole
+  ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
+  (``sigma_b``, ``mu``; ``make_golden.py magnetic``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -70,6 +71,18 @@ def sigma_map(nx, ny, seed):
     return sig
 
 
+def magnetic_maps(nx, ny, seed):
+    """Magnetic conductivity (a lossy slab and a graded patch) and permeability (a
+    block of mu in [1.5, 3])."""
+    rng = np.random.default_rng(seed)
+    sb = np.zeros((nx, ny))
+    sb[30:34, :] = 2.0
+    sb[10:16, 22:28] = rng.uniform(0.5, 3.0, (6, 6))
+    mu = np.ones((nx, ny))
+    mu[18:26, 6:14] = rng.uniform(1.5, 3.0, (8, 8))
+    return sb, mu
+
+
 POLES = [(0.7, 0.05, 1.5), (0.0, 0.1, 1.0, 0.9)]   # a Lorentz and a Drude pole
 
 
@@ -82,7 +95,7 @@ def pole_masks(nx, ny):
     return [m0, m1]
 
 
-def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False):
+def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=False):
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -91,6 +104,9 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False):
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
     sig = sigma_map(nx, ny, 21) if sigma else None
     kw = {} if sig is None else {"sigma_d": torch.tensor(sig, dtype=DT[prec])}
+    sbm, mum = magnetic_maps(nx, ny, 23) if magnetic else (None, None)
+    if magnetic:
+        kw.update(sigma_b=torch.tensor(sbm, dtype=DT[prec]), mu=torch.tensor(mum, dtype=DT[prec]))
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -118,6 +134,8 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False):
                mask=_np(src.mask))
     if sig is not None:
         out["sigma"] = sig
+    if magnetic:
+        out["sigma_b"], out["mu"] = sbm, mum
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -130,7 +148,7 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False):
     return out
 
 
-def te_case(prec, sigma=False, poles=False):
+def te_case(prec, sigma=False, poles=False, magnetic=False):
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -139,6 +157,9 @@ def te_case(prec, sigma=False, poles=False):
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
     sig = sigma_map(nx, ny, 22) if sigma else None
     kw = {} if sig is None else {"sigma_d": torch.tensor(sig, dtype=DT[prec])}
+    sbm, mum = magnetic_maps(nx, ny, 24) if magnetic else (None, None)
+    if magnetic:
+        kw.update(sigma_b=torch.tensor(sbm, dtype=DT[prec]), mu=torch.tensor(mum, dtype=DT[prec]))
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -166,6 +187,8 @@ def te_case(prec, sigma=False, poles=False):
                mask=_np(_TESrc.mask))
     if sig is not None:
         out["sigma"] = sig
+    if magnetic:
+        out["sigma_b"], out["mu"] = sbm, mum
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -427,6 +450,13 @@ def main():
                                 **tm_case(prec, poles=True))
             np.savez_compressed(os.path.join(HERE, f"golden_te_poles_{prec}.npz"),
                                 **te_case(prec, poles=True))
+        return
+    if sys.argv[1:] == ["magnetic"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_tm_magnetic_{prec}.npz"),
+                                **tm_case(prec, magnetic=True))
+            np.savez_compressed(os.path.join(HERE, f"golden_te_magnetic_{prec}.npz"),
+                                **te_case(prec, magnetic=True))
         return
     if sys.argv[1:] == ["sigma"]:
         for prec in ("f64", "f32"):

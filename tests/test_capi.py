@@ -133,7 +133,7 @@ def test_unsupported_features_raise():
     with pytest.raises(NotImplementedError):
         build_tm_coeffs(g, m_poles=[(1.0, 0.1, 1.0)])
     with pytest.raises(NotImplementedError):
-        build_tm_coeffs(g, sigma_b=torch.ones(20, 20))
+        build_tm_coeffs(g, chi3=torch.ones(20, 20))
     with pytest.raises(ValueError):
         build_tm_coeffs(g, npml=10)
 
@@ -217,3 +217,25 @@ def test_flux_window_matches_oracle(normal, idx, win, ap):
     planes = O.flux3d_planes(s, normal, idx, win, ap)
     pairs, (l0, h0, l1, h1) = flux_window(normal, idx, nx, ny, nz, win, ap)
     assert planes[0].shape == (h0 - l0, h1 - l1)
+
+
+def test_magnetic_coefficients_match_oracle():
+    """sigma_b and mu give the reference's magnetic pairs (core/coeffs.py:167-175,
+    :410-414), averaged onto Hx / Hy (TM) and Hz (TE) as the oracle restates them;
+    the electric pair is built alongside (d1 = 1, d2 = dt without sigma_d)."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    rng = np.random.default_rng(4)
+    sb = (3.0 * rng.random((20, 24))).astype(np.float32)
+    mu = (1.0 + 2.0 * rng.random((20, 24))).astype(np.float32)
+    g = Grid(nx=20, ny=24, dx=0.05, device="cpu")
+    m = build_tm_coeffs(g, sigma_b=torch.from_numpy(sb), mu=torch.from_numpy(mu))
+    c = O.tm_coeffs(20, 24, 0.05, dtype=np.float32, sigma_b=sb, mu=mu)
+    for k in ("h1x", "h2x", "h1y", "h2y", "d1", "d2"):
+        np.testing.assert_allclose(getattr(m, k).numpy(), c[k], rtol=5e-7, atol=0, err_msg=k)
+    assert m.h1x.shape == (20, 23) and m.h1y.shape == (19, 24)
+    t = build_te_coeffs(g, sigma_b=torch.from_numpy(sb), mu=torch.from_numpy(mu))
+    ct = O.te_coeffs(20, 24, 0.05, dtype=np.float32, sigma_b=sb, mu=mu)
+    for k in ("hz1", "hz2", "d1x", "d2y"):
+        np.testing.assert_allclose(getattr(t, k).numpy(), ct[k], rtol=5e-7, atol=0, err_msg=k)
+    assert t.hz1.shape == (19, 23)

@@ -51,10 +51,11 @@ def run_tm_case(case, phase_mode="exact"):
     sig = g.get("sigma")
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
+    mag = {k: torch.tensor(g[k], dtype=torch.float32) for k in ("sigma_b", "mu") if k in g}
     m = build_tm_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
                         npml=int(g["npml"]), y_pmc=pmc,
                         sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32),
-                        poles=poles, pole_masks=pm)
+                        poles=poles, pole_masks=pm, **mag)
     src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
                      profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
     freqs = [float(f) for f in g["freqs"]]
@@ -70,7 +71,8 @@ def run_tm_case(case, phase_mode="exact"):
     return st, accs, (fx, fy)
 
 
-@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles"])
+@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles",
+                                  "tm_magnetic"])
 def test_tm_matches_reference(case):
     st, accs, (fx, fy) = run_tm_case(case)
     e32, e64 = {}, {}
@@ -99,7 +101,7 @@ def test_tm_reference_phase_mode():
         assert rel_l2(a.cpu().numpy(), g[key]) < TOL, key
 
 
-@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles"])
+@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic"])
 def test_te_matches_reference(case):
     from meep_torch_b200.core.coeffs import build_te_coeffs
     from meep_torch_b200.core.grid import Grid
@@ -113,9 +115,11 @@ def test_te_matches_reference(case):
     sig = g.get("sigma")
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
+    mag = {k: torch.tensor(g[k], dtype=torch.float32) for k in ("sigma_b", "mu") if k in g}
     m = build_te_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
                         npml=int(g["npml"]), poles=poles, pole_masks=pm,
-                        sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32))
+                        sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32),
+                        **mag)
     src = TESource(LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]),
                               j1=int(g["src_j1"]),
                               profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"]))))
@@ -791,6 +795,79 @@ def test_conductivity_batched_tiles_match_oracle_and_other_paths_refuse():
     eng.close()
     with pytest.raises(MtbUnsupported):
         Engine2D(items[:1], variant=1)
+
+
+def test_magnetic_batched_tiles_match_oracle_and_other_paths_refuse():
+    """Magnetic conductivity and permeability (with an electric conductivity slab) in
+    a batch large enough for four rows per warp, from random fields, against the
+    oracle: every H site of the tiles (TM Hx, Hy and the recomputed Hy row and Hx
+    column; TE Hz) applies the (h1, h2) pairs. The row march and the adjoint refuse
+    them (MTB_UNSUPPORTED)."""
+    from meep_torch_b200._lib import MtbUnsupported
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor
+    from meep_torch_b200.core.run import run_tm
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    from meep_torch_b200.engine2d import Engine2D
+    rng = np.random.default_rng(29)
+    n, npml, dx = 30, 8, 0.05
+    specs = [("tm", 300, 260), ("te", 280, 300)] * 40
+    items, refs = [], []
+    for q, (pol, nx, ny) in enumerate(specs):
+        eps = (1.0 + 3.0 * rng.random((nx, ny))).astype(np.float32)
+        sig = np.zeros((nx, ny), dtype=np.float32)
+        sig[nx // 3: nx // 2, :] = 1.0
+        sb = np.zeros((nx, ny), dtype=np.float32)
+        sb[:, ny // 4: ny // 3] = 2.5
+        sb[nx // 2:, :] += (2.0 * rng.random((nx - nx // 2, ny))).astype(np.float32)
+        mu = (1.0 + 2.0 * rng.random((nx, ny))).astype(np.float32)
+        grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+        kw = dict(eps_inf=torch.from_numpy(eps), npml=npml, sigma_d=torch.from_numpy(sig),
+                  sigma_b=torch.from_numpy(sb), mu=torch.from_numpy(mu))
+        okw = dict(eps=eps, npml=npml, dtype=np.float32, sigma=sig, sigma_b=sb, mu=mu)
+        if pol == "tm":
+            c = O.tm_coeffs(nx, ny, dx, **okw)
+            so = O.tm_state(c)
+            for k in ("Dz", "Hx", "Hy"):
+                so[k] = rng.standard_normal(so[k].shape).astype(np.float32)
+            m = build_tm_coeffs(grid, **kw)
+            so["Ez"] = (torch.from_numpy(so["Dz"]) / m.eps_inf.cpu()).numpy()
+            s0 = init_tm_state(grid)._replace(
+                **{k: torch.from_numpy(so[k]).to(dev()) for k in ("Ez", "Dz", "Hx", "Hy")})
+            step = O.tm_step
+        else:
+            c = O.te_coeffs(nx, ny, dx, **okw)
+            so = O.te_state(c)
+            for k in ("Hz", "Dx", "Dy"):
+                so[k] = rng.standard_normal(so[k].shape).astype(np.float32)
+            so["Ex"], so["Ey"] = so["Dx"] / c["eps_x"], so["Dy"] / c["eps_y"]
+            m = build_te_coeffs(grid, **kw)
+            s0 = init_te_state(grid)._replace(
+                **{k: torch.from_numpy(so[k]).to(dev()) for k in ("Hz", "Dx", "Dy", "Ex", "Ey")})
+            step = O.te_step
+        items.append((s0, m, None, []))
+        if q < 2:
+            refs.append(O.run_2d(step, so, c, n)[0])
+    eng = Engine2D(items)
+    eng.run(0, n)
+    for b, ref in enumerate(refs):
+        st = eng.state(b)
+        for k in (("Ez", "Dz", "Hx", "Hy") if b == 0 else ("Hz", "Dx", "Dy", "Ex", "Ey")):
+            assert rel_l2(getattr(st, k).cpu().numpy(), ref[k]) < TOL, (b, k)
+    eng.close()
+    with pytest.raises(MtbUnsupported):
+        Engine2D(items[:1], variant=1)
+    grid = Grid(nx=40, ny=40, dx=dx, device=dev())
+    eps = torch.ones(40, 40, device=dev(), requires_grad=True)
+    m = build_tm_coeffs(grid, eps_inf=eps, npml=8, sigma_b=torch.full((40, 40), 0.5))
+    src = LineSource(grid, ix=20, j0=15, j1=25, profile=GaussianPulse(0.5, 0.3))
+    _, (acc,) = run_tm(init_tm_state(grid), m, 10, source=src,
+                       monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
+    with pytest.raises(MtbUnsupported):
+        acc.sum().backward()
 
 
 def test_poles_batched_tiles_match_oracle_from_random_state():

@@ -37,7 +37,8 @@ def run_tm_oracle(g, prec):
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     c = O.tm_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]),
                     y_pmc=bool(g["y_pmc"]), dtype=dt_np, sigma=g.get("sigma"),
-                    poles=poles, pole_masks=g.get("pole_masks"))
+                    poles=poles, pole_masks=g.get("pole_masks"), sigma_b=g.get("sigma_b"),
+                    mu=g.get("mu"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -54,7 +55,8 @@ def run_tm_oracle(g, prec):
     return c, mask, s, acc
 
 
-@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles"])
+@pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles",
+                                  "tm_magnetic"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_tm_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
@@ -80,7 +82,8 @@ def run_te_oracle(g, prec):
     nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     c = O.te_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
-                    sigma=g.get("sigma"), poles=poles, pole_masks=g.get("pole_masks"))
+                    sigma=g.get("sigma"), poles=poles, pole_masks=g.get("pole_masks"),
+                    sigma_b=g.get("sigma_b"), mu=g.get("mu"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)[:, :-1]
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -97,7 +100,7 @@ def run_te_oracle(g, prec):
     return c, mask, s, acc
 
 
-@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles"])
+@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_te_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
