@@ -99,7 +99,8 @@ def pole_recurrence(pole, dt):
 
 
 def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
-              dtype=np.float64, sigma=None, poles=(), pole_masks=None, sigma_b=None, mu=None):
+              dtype=np.float64, sigma=None, poles=(), pole_masks=None, sigma_b=None, mu=None,
+              y_mirror=0, x_mirror=0, y_rot2=0, rot4=0):
     """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
 
     Profiles are sliced to the live derivative nodes exactly as
@@ -107,21 +108,48 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
     interior [1:-1] (or the full axis under y_pmc). ``sigma`` (nx, ny): the
     electric conductivity pair (d1, d2) of :161-166 on Dz; ``sigma_b`` and ``mu``
     (nx, ny): the magnetic pairs of :167-175, averaged onto Hx along y and onto Hy
-    along x. Any of the three builds all the pairs, as the reference does."""
+    along x. Any of the three builds all the pairs, as the reference does.
+
+    Symmetry folds (:213-278): ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd) cut the
+    low-y / low-x edge; ``y_rot2`` (C2 about the low-y cut) and ``rot4`` (C4, both low
+    edges, square grids) likewise. A cut replaces the low-side PML, and the D-side
+    profiles then keep the cut row / column (0 .. n-2) instead of the interior."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
          else np.asarray(eps, dtype=dtype).copy())
+    for v in (y_mirror, x_mirror, y_rot2, rot4):
+        if v not in (0, 1, -1):
+            raise ValueError("symmetry parity must be 0, +1 or -1")
+    if y_mirror and y_rot2:
+        raise ValueError("y_mirror and y_rot2 both cut the low-y edge")
+    if rot4 and (y_mirror or x_mirror or y_rot2):
+        raise ValueError("rot4 cuts both low edges on its own")
+    if rot4 and nx != ny:
+        raise ValueError("rot4 needs a square grid")
+    if y_pmc and (y_mirror or x_mirror or y_rot2 or rot4):
+        raise ValueError("symmetry cuts and y_pmc are mutually exclusive")
+    ycut, xcut = bool(y_mirror or y_rot2 or rot4), bool(x_mirror or rot4)
     px, py = _axis_sides(npml)
+    if ycut:
+        py = (0, py[1])
+    if xcut:
+        px = (0, px[1])
     if sum(px) >= nx or (sum(py) >= ny and not y_pmc):
         raise ValueError("npml too large for grid")
     yprof = py if not y_pmc else 0
     b_hy, a_hy, k_hy = cpml_profiles(ny - 1, yprof, 0.5, dt, dx, dtype=dtype)
     b_hx, a_hx, k_hx = cpml_profiles(nx - 1, px, 0.5, dt, dx, dtype=dtype)
-    b_ex, a_ex, k_ex = (v[1:-1] for v in cpml_profiles(nx, px, 0.0, dt, dx, dtype=dtype))
+    b_exf, a_exf, k_exf = cpml_profiles(nx, px, 0.0, dt, dx, dtype=dtype)
+    if xcut:
+        b_ex, a_ex, k_ex = b_exf[:-1], a_exf[:-1], k_exf[:-1]
+    else:
+        b_ex, a_ex, k_ex = b_exf[1:-1], a_exf[1:-1], k_exf[1:-1]
     b_eyf, a_eyf, k_eyf = cpml_profiles(ny, yprof, 0.0, dt, dx, dtype=dtype)
     if y_pmc:
         b_ey, a_ey, k_ey = b_eyf, a_eyf, k_eyf
+    elif ycut:
+        b_ey, a_ey, k_ey = b_eyf[:-1], a_eyf[:-1], k_eyf[:-1]
     else:
         b_ey, a_ey, k_ey = b_eyf[1:-1], a_eyf[1:-1], k_eyf[1:-1]
     cond = {}
@@ -147,6 +175,7 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
         c3[k] = dtype.type(cv3) * m
     cond.update(c1=c1, c2=c2, c3=c3)
     return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc, **cond,
+                y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4,
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
                 b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
@@ -154,15 +183,25 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
 
 
 def tm_state(c):
-    """Zero TM state with the reference's shapes (core/stepper_tm.py:37-71)."""
+    """Zero TM state with the reference's shapes (core/stepper_tm.py:37-71): with a
+    low-y (low-x) cut the E-side CPML memory keeps the cut row (column); an odd y
+    mirror, Rotate2 or Rotate4 carries the live on-plane Hx row (Hx0, (nx,)), an odd x
+    mirror or Rotate4 the on-plane Hy column (Hy0, (ny,))."""
     nx, ny, dt = c["nx"], c["ny"], c["dtype"]
-    ny_e = ny if c["y_pmc"] else ny - 2
+    ym, xm, r2, r4 = (c.get(k, 0) for k in ("y_mirror", "x_mirror", "y_rot2", "rot4"))
+    ny_e = ny if c["y_pmc"] else (ny - 1 if (ym or r2 or r4) else ny - 2)
+    nx_e = nx - 1 if (xm or r4) else nx - 2
     z = lambda *s: np.zeros(s, dtype=dt)
     n_p = c["c1"].shape[0]
-    return dict(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
-                P_cur=z(n_p, nx, ny), P_prev=z(n_p, nx, ny),
-                psi_Ezy=z(nx, ny - 1), psi_Ezx=z(nx - 1, ny),
-                psi_Hyx=z(nx - 2, ny_e), psi_Hxy=z(nx - 2, ny_e))
+    st = dict(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
+              P_cur=z(n_p, nx, ny), P_prev=z(n_p, nx, ny),
+              psi_Ezy=z(nx, ny - 1), psi_Ezx=z(nx - 1, ny),
+              psi_Hyx=z(nx_e, ny_e), psi_Hxy=z(nx_e, ny_e))
+    if ym == -1 or r2 or r4:
+        st["Hx0"] = z(nx)
+    if xm == -1 or r4:
+        st["Hy0"] = z(ny)
+    return st
 
 
 def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
@@ -186,21 +225,52 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
     else:
         Hx = s["Hx"] - T(dt) * curl_hx
         Hy = s["Hy"] + T(dt) * curl_hy
+    # on-plane H of an odd mirror / Rotate2 / Rotate4 cut (core/stepper_tm.py:94-115):
+    # the ghost Ez beyond the cut is -Ez (odd), the cut row reversed times the parity
+    # (C2), or the other cut's line times the parity (C4)
+    r2, r4 = c.get("y_rot2", 0), c.get("rot4", 0)
+    mir = {}
+    if "Hx0" in s:
+        ez0 = Ez[:, 0]
+        ghost = r4 * Ez[0, :] if r4 else (r2 * ez0[::-1] if r2 else -ez0)
+        mir["Hx0"] = s["Hx0"] - T(dt) * (ez0 - ghost) / T(dx)
+    if "Hy0" in s:
+        ez0x = Ez[0, :]
+        ghost_x = r4 * Ez[:, 0] if r4 else -ez0x
+        mir["Hy0"] = s["Hy0"] + T(dt) * (ez0x - ghost_x) / T(dx)
     # magnetic sheet current (mode sources), subtracted (core/stepper_tm.py:186-196)
     if hy_mask is not None:
         Hy = Hy - T(dt * amp_h) * hy_mask
     if hx_mask is not None:
         Hx = Hx - T(dt * amp_h) * hx_mask
-    # D update with PEC (zero-pad) or PMC-in-y ghosts (core/stepper_tm.py:136-166)
+    # D update (core/stepper_tm.py:130-166): ghost / plane H beyond each wall, then
+    # differences over the live Ez region -- interior (PEC), all rows (y-PMC), or from
+    # the cut up (even mirror: H = 0 ghost; odd / C2 / C4: the plane node)
+    ym, xm = c.get("y_mirror", 0), c.get("x_mirror", 0)
     if c["y_pmc"]:
-        Hxp = np.pad(Hx, ((0, 0), (1, 1)))
-        dHx_dy = (Hxp[1:-1, 1:] - Hxp[1:-1, :-1]) / T(dx)
-        dHy_dx = (Hy[1:, :] - Hy[:-1, :]) / T(dx)
-        pad = ((1, 1), (0, 0))
+        Hxg = np.pad(Hx, ((0, 0), (1, 1)))
+        pad_y, ys = (0, 0), slice(None)
+    elif ym == 1:
+        Hxg = np.pad(Hx, ((0, 0), (1, 0)))
+        pad_y, ys = (0, 1), slice(None, -1)
+    elif ym == -1 or r2 or r4:
+        Hxg = np.concatenate([mir["Hx0"][:, None], Hx], axis=1)
+        pad_y, ys = (0, 1), slice(None, -1)
     else:
-        dHx_dy = (Hx[1:-1, 1:] - Hx[1:-1, :-1]) / T(dx)
-        dHy_dx = (Hy[1:, 1:-1] - Hy[:-1, 1:-1]) / T(dx)
-        pad = ((1, 1), (1, 1))
+        Hxg = Hx
+        pad_y, ys = (1, 1), slice(1, -1)
+    if xm == 1:
+        Hyg = np.pad(Hy, ((1, 0), (0, 0)))
+        pad_x, xs = (0, 1), slice(None, -1)
+    elif xm == -1 or r4:
+        Hyg = np.concatenate([mir["Hy0"][None, :], Hy], axis=0)
+        pad_x, xs = (0, 1), slice(None, -1)
+    else:
+        Hyg = Hy
+        pad_x, xs = (1, 1), slice(1, -1)
+    dHx_dy = (Hxg[xs, 1:] - Hxg[xs, :-1]) / T(dx)
+    dHy_dx = (Hyg[1:, ys] - Hyg[:-1, ys]) / T(dx)
+    pad = (pad_x, pad_y)
     psi_Hyx = c["b_ex"] * s["psi_Hyx"] + c["a_ex"] * dHy_dx
     psi_Hxy = c["b_ey"] * s["psi_Hxy"] + c["a_ey"] * dHx_dy
     curl = dHy_dx / c["k_ex"] + psi_Hyx - dHx_dy / c["k_ey"] - psi_Hxy
@@ -214,7 +284,7 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
         if mask is not None:
             Dz = Dz - T(dt * amp) * mask
     out = dict(Hx=Hx, Hy=Hy, Dz=Dz, psi_Ezy=psi_Ezy, psi_Ezx=psi_Ezx, psi_Hyx=psi_Hyx,
-               psi_Hxy=psi_Hxy)
+               psi_Hxy=psi_Hxy, **mir)
     if c["c1"].shape[0]:
         # update_pols (core/stepper_tm.py:203-207) on the old Ez, then
         # update_eh(E): Ez = (Dz - sum P) / eps_inf (:220-224)
@@ -228,13 +298,15 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
 # ---------------------------------------------------------------- 2D TE
 
 def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None,
-              poles=(), pole_masks=None, sigma_b=None, mu=None):
+              poles=(), pole_masks=None, sigma_b=None, mu=None, y_mirror=0, x_mirror=0):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
     (core/coeffs.py:347-354); so is ``sigma`` for the conductivity pairs of
     :401-409 on Dx and Dy. ``sigma_b`` and ``mu`` give the Hz pair of :410-414,
-    averaged over the four nodes around each Hz. Any of the three builds all pairs."""
+    averaged over the four nodes around each Hz. Any of the three builds all pairs.
+    ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd) replace the low-side PML with the
+    mirror wall (:457-469)."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -242,7 +314,13 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
     h = dtype.type(0.5)
     eps_x = h * (e[:-1, :] + e[1:, :])
     eps_y = h * (e[:, :-1] + e[:, 1:])
+    if y_mirror not in (0, 1, -1) or x_mirror not in (0, 1, -1):
+        raise ValueError("mirror parity must be 0, +1 or -1")
     px, py = _axis_sides(npml)
+    if y_mirror:
+        py = (0, py[1])
+    if x_mirror:
+        px = (0, px[1])
     if sum(px) >= nx or sum(py) >= ny:
         raise ValueError("npml too large for grid")
     b_hx, a_hx, k_hx = cpml_profiles(nx - 1, px, 0.5, dt, dx, dtype=dtype)
@@ -275,7 +353,7 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
             c3[k] = dtype.type(cv3) * mavg
         cond.update({"c1" + ax: c1, "c2" + ax: c2, "c3" + ax: c3})
     return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, **cond,
-                eps_x=eps_x, eps_y=eps_y,
+                eps_x=eps_x, eps_y=eps_y, y_mirror=y_mirror, x_mirror=x_mirror,
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
                 b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
@@ -307,6 +385,12 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
     dHz_dx = (Hz[1:, :] - Hz[:-1, :]) / T(dx)
     psi_Hzx = c["b_ex"] * s["psi_Hzx"] + c["a_ex"] * dHz_dx
     curl_y = np.pad(dHz_dx / c["k_ex"] + psi_Hzx, ((1, 1), (0, 0)))
+    # even mirror: the on-plane tangential E row / column is live, its curl from the
+    # odd Hz ghost 2 Hz[0] / dx (core/stepper_te.py:87-96); odd: the zero pad stays
+    if c.get("y_mirror", 0) == 1:
+        curl_x = np.concatenate([T(2.0) * Hz[:, :1] / T(dx), curl_x[:, 1:]], axis=1)
+    if c.get("x_mirror", 0) == 1:
+        curl_y = np.concatenate([T(2.0) * Hz[:1, :] / T(dx), curl_y[1:, :]], axis=0)
     if "d1x" in c:
         # conductivity (core/stepper_te.py D update); the source scaled by d2y
         Dx = c["d1x"] * s["Dx"] + c["d2x"] * curl_x

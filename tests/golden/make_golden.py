@@ -18,7 +18,8 @@ cases of the hot path through its own public functions:
   and of ``run_te`` (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
-  (``sigma_b``, ``mu``; ``make_golden.py magnetic``) and the TM and TE cases with a Lorentz and a Drude pole
+  (``sigma_b``, ``mu``; ``make_golden.py magnetic``), and the symmetry-folded TM and TE
+  runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -192,6 +193,56 @@ def te_case(prec, sigma=False, poles=False, magnetic=False):
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
+    for k in st._fields:
+        v = getattr(st, k)
+        if v is not None and v.numel():
+            out["s_" + k] = _np(v)
+    return out
+
+
+TM_FOLDS = {"ym_even": dict(y_mirror=1), "ym_odd": dict(y_mirror=-1),
+            "xm_even": dict(x_mirror=1), "xm_odd_ym_even": dict(x_mirror=-1, y_mirror=1),
+            "rot2_even": dict(y_rot2=1), "rot2_odd": dict(y_rot2=-1),
+            "rot4_even": dict(rot4=1), "rot4_odd": dict(rot4=-1)}
+TE_FOLDS = {"ym_even_xm_odd": dict(y_mirror=1, x_mirror=-1),
+            "ym_odd_xm_even": dict(y_mirror=-1, x_mirror=1)}
+
+
+def fold_case(prec, pol, fold):
+    """A symmetry-folded 2D run (the low-x / low-y edges are the cuts): 40 x 40 cells,
+    PML on the far sides, a dielectric block and a line source near the cut, 250
+    steps, the full-grid DFT of the main component at three frequencies."""
+    rng = np.random.default_rng(31)
+    nx = ny = 40
+    dx, npml, n = 0.05, 8, 250
+    eps = np.ones((nx, ny))
+    eps[6:16, 4:12] = rng.uniform(2.0, 6.0)
+    eps[:, 20:24] = 8.0
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
+    e = torch.tensor(eps, dtype=DT[prec])
+    freqs = [0.55, 0.65, 0.75]
+    src = LineSource(g, ix=5, j0=3, j1=18, profile=GaussianPulse(0.65, 0.4))
+    if pol == "tm":
+        m = build_tm_coeffs(g, eps_inf=e, npml=npml, **fold)
+        s0 = init_tm_state(g, **fold)
+        dft = DFTFieldsMonitor(g, freqs, component="Ez")
+        with torch.no_grad():
+            st, (ad,) = run_tm(s0, m, n, source=src, monitors=[dft])
+        mask = _np(src.mask)
+    else:
+        m = build_te_coeffs(g, eps_inf=e, npml=npml, **fold)
+        s0 = init_te_state(g)
+
+        class _TESrc:
+            mask = src.mask[:, :-1]
+            amplitude = staticmethod(src.amplitude)
+        dft = DFTFieldsMonitor(g, freqs, component="Hz")
+        with torch.no_grad():
+            st, (ad,) = run_te(s0, m, n, source=_TESrc(), monitors=[dft])
+        mask = _np(_TESrc.mask)
+    out = dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, eps=eps, freqs=np.array(freqs),
+               fcen=0.65, fwidth=0.4, src_ix=5, src_j0=3, src_j1=18, mask=mask,
+               acc_dft=_np(ad), fold=json.dumps(fold))
     for k in st._fields:
         v = getattr(st, k)
         if v is not None and v.numel():
@@ -450,6 +501,13 @@ def main():
                                 **tm_case(prec, poles=True))
             np.savez_compressed(os.path.join(HERE, f"golden_te_poles_{prec}.npz"),
                                 **te_case(prec, poles=True))
+        return
+    if sys.argv[1:] == ["folds"]:
+        for prec in ("f64", "f32"):
+            for pol, folds in (("tm", TM_FOLDS), ("te", TE_FOLDS)):
+                for name, fold in folds.items():
+                    np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
+                                        **fold_case(prec, pol, fold))
         return
     if sys.argv[1:] == ["magnetic"]:
         for prec in ("f64", "f32"):
