@@ -100,7 +100,7 @@ def pole_recurrence(pole, dt):
 
 def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
               dtype=np.float64, sigma=None, poles=(), pole_masks=None, sigma_b=None, mu=None,
-              y_mirror=0, x_mirror=0, y_rot2=0, rot4=0):
+              y_mirror=0, x_mirror=0, y_rot2=0, rot4=0, chi2=None, chi3=None):
     """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
 
     Profiles are sliced to the live derivative nodes exactly as
@@ -113,7 +113,8 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
     Symmetry folds (:213-278): ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd) cut the
     low-y / low-x edge; ``y_rot2`` (C2 about the low-y cut) and ``rot4`` (C4, both low
     edges, square grids) likewise. A cut replaces the low-side PML, and the D-side
-    profiles then keep the cut row / column (0 .. n-2) instead of the interior."""
+    profiles then keep the cut row / column (0 .. n-2) instead of the interior.
+    ``chi2`` / ``chi3`` (nx, ny): the instantaneous nonlinearity of :154-158."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -174,8 +175,15 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
         c2[k] = dtype.type(cv2)
         c3[k] = dtype.type(cv3) * m
     cond.update(c1=c1, c2=c2, c3=c3)
+    nl = {}
+    if chi2 is not None or chi3 is not None:
+        z = np.zeros((nx, ny), dtype=dtype)
+        x2 = z if chi2 is None else np.asarray(chi2, dtype=dtype)
+        x3 = z if chi3 is None else np.asarray(chi3, dtype=dtype)
+        if (x2 != 0).any() or (x3 != 0).any():
+            nl = dict(chi2=x2, chi3=x3)
     return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc, **cond,
-                y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4,
+                **nl, y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4,
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
                 b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
@@ -289,16 +297,26 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
         # update_pols (core/stepper_tm.py:203-207) on the old Ez, then
         # update_eh(E): Ez = (Dz - sum P) / eps_inf (:220-224)
         P_new = c["c1"] * s["P_cur"] + c["c2"] * s["P_prev"] + c["c3"] * Ez
-        out.update(P_cur=P_new, P_prev=s["P_cur"], Ez=(Dz - P_new.sum(0)) / c["eps"])
+        rhs = Dz - P_new.sum(0)
+        out.update(P_cur=P_new, P_prev=s["P_cur"])
     else:
-        out.update(Ez=Dz / c["eps"], P_cur=s.get("P_cur"), P_prev=s.get("P_prev"))
+        rhs = Dz
+        out.update(P_cur=s.get("P_cur"), P_prev=s.get("P_prev"))
+    Ez_new = rhs / c["eps"]
+    if "chi3" in c:
+        # instantaneous chi2 / chi3: three fixed-point sweeps of
+        # E = rhs / (eps + chi2 E + chi3 E^2) (core/stepper_tm.py:225-230)
+        for _ in range(3):
+            Ez_new = rhs / (c["eps"] + c["chi2"] * Ez_new + c["chi3"] * Ez_new * Ez_new)
+    out["Ez"] = Ez_new
     return out
 
 
 # ---------------------------------------------------------------- 2D TE
 
 def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None,
-              poles=(), pole_masks=None, sigma_b=None, mu=None, y_mirror=0, x_mirror=0):
+              poles=(), pole_masks=None, sigma_b=None, mu=None, y_mirror=0, x_mirror=0,
+              chi2=None, chi3=None):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
@@ -306,7 +324,8 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
     :401-409 on Dx and Dy. ``sigma_b`` and ``mu`` give the Hz pair of :410-414,
     averaged over the four nodes around each Hz. Any of the three builds all pairs.
     ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd) replace the low-side PML with the
-    mirror wall (:457-469)."""
+    mirror wall (:457-469). ``chi2`` / ``chi3`` (nx, ny) are Yee-averaged to Ex / Ey
+    (:382-387)."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -352,12 +371,33 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
             c2[k] = dtype.type(cv2)
             c3[k] = dtype.type(cv3) * mavg
         cond.update({"c1" + ax: c1, "c2" + ax: c2, "c3" + ax: c3})
-    return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, **cond,
+    nl = {}
+    if chi2 is not None or chi3 is not None:
+        z = np.zeros((nx, ny), dtype=dtype)
+        x2 = z if chi2 is None else np.asarray(chi2, dtype=dtype)
+        x3 = z if chi3 is None else np.asarray(chi3, dtype=dtype)
+        if (x2 != 0).any() or (x3 != 0).any():
+            nl = dict(chi2_x=h * (x2[:-1, :] + x2[1:, :]), chi2_y=h * (x2[:, :-1] + x2[:, 1:]),
+                      chi3_x=h * (x3[:-1, :] + x3[1:, :]), chi3_y=h * (x3[:, :-1] + x3[:, 1:]))
+    return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, **cond, **nl,
                 eps_x=eps_x, eps_y=eps_y, y_mirror=y_mirror, x_mirror=x_mirror,
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
                 b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
                 b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None])
+
+
+def _avg4_to_ex(Ey):
+    """Ey (nx, ny-1) at the Ex nodes (nx-1, ny), zero beyond the y walls
+    (core/stepper_te.py:52-55)."""
+    p = np.pad(Ey, ((0, 0), (1, 1)))
+    return Ey.dtype.type(0.25) * (p[:-1, :-1] + p[:-1, 1:] + p[1:, :-1] + p[1:, 1:])
+
+
+def _avg4_to_ey(Ex):
+    """Ex (nx-1, ny) at the Ey nodes (nx, ny-1), zero beyond the x walls (:58-61)."""
+    p = np.pad(Ex, ((1, 1), (0, 0)))
+    return Ex.dtype.type(0.25) * (p[:-1, :-1] + p[:-1, 1:] + p[1:, :-1] + p[1:, 1:])
 
 
 def te_state(c):
@@ -414,6 +454,16 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
         pol = {k: s.get(k) for k in ("Px_cur", "Px_prev", "Py_cur", "Py_prev")}
         Ex = Dx / c["eps_x"]
         Ey = Dy / c["eps_y"]
+    if "chi3_x" in c:
+        # instantaneous chi2 / chi3 (core/stepper_te.py:157-174): three fixed-point
+        # sweeps with |E|^2 from the other component averaged over four nodes
+        rhs_x = Dx - pol["Px_cur"].sum(0) if pol.get("Px_cur") is not None else Dx
+        rhs_y = Dy - pol["Py_cur"].sum(0) if pol.get("Py_cur") is not None else Dy
+        for _ in range(3):
+            E2x = Ex * Ex + _avg4_to_ex(Ey) ** 2
+            E2y = Ey * Ey + _avg4_to_ey(Ex) ** 2
+            Ex = rhs_x / (c["eps_x"] + c["chi2_x"] * Ex + c["chi3_x"] * E2x)
+            Ey = rhs_y / (c["eps_y"] + c["chi2_y"] * Ey + c["chi3_y"] * E2y)
     dEy_dx = (Ey[1:, :] - Ey[:-1, :]) / T(dx)
     dEx_dy = (Ex[:, 1:] - Ex[:, :-1]) / T(dx)
     psi_Eyx = c["b_hx"] * s["psi_Eyx"] + c["a_hx"] * dEy_dx

@@ -19,7 +19,8 @@ cases of the hot path through its own public functions:
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
   (``sigma_b``, ``mu``; ``make_golden.py magnetic``), and the symmetry-folded TM and TE
-  runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``) and the TM and TE cases with a Lorentz and a Drude pole
+  runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``), and chi2 / chi3 runs
+  (``make_golden.py nonlinear``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -96,7 +97,19 @@ def pole_masks(nx, ny):
     return [m0, m1]
 
 
-def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=False):
+def chi_maps(nx, ny, seed):
+    """Kerr chi3 along a band and chi2 on a patch (instantaneous nonlinearity), strong
+    enough at these field amplitudes to change the run well beyond the tolerances."""
+    rng = np.random.default_rng(seed)
+    x3 = np.zeros((nx, ny))
+    x3[:, 14:22] = 100.0
+    x2 = np.zeros((nx, ny))
+    x2[24:32, 8:16] = rng.uniform(5.0, 20.0, (8, 8))
+    return x2, x3
+
+
+def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=False,
+            nonlinear=False):
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -108,6 +121,9 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
     sbm, mum = magnetic_maps(nx, ny, 23) if magnetic else (None, None)
     if magnetic:
         kw.update(sigma_b=torch.tensor(sbm, dtype=DT[prec]), mu=torch.tensor(mum, dtype=DT[prec]))
+    x2m, x3m = chi_maps(nx, ny, 25) if nonlinear else (None, None)
+    if nonlinear:
+        kw.update(chi2=torch.tensor(x2m, dtype=DT[prec]), chi3=torch.tensor(x3m, dtype=DT[prec]))
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -137,6 +153,8 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
         out["sigma"] = sig
     if magnetic:
         out["sigma_b"], out["mu"] = sbm, mum
+    if nonlinear:
+        out["chi2"], out["chi3"] = x2m, x3m
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -149,7 +167,7 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
     return out
 
 
-def te_case(prec, sigma=False, poles=False, magnetic=False):
+def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False):
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -161,6 +179,9 @@ def te_case(prec, sigma=False, poles=False, magnetic=False):
     sbm, mum = magnetic_maps(nx, ny, 24) if magnetic else (None, None)
     if magnetic:
         kw.update(sigma_b=torch.tensor(sbm, dtype=DT[prec]), mu=torch.tensor(mum, dtype=DT[prec]))
+    x2m, x3m = chi_maps(nx, ny, 26) if nonlinear else (None, None)
+    if nonlinear:
+        kw.update(chi2=torch.tensor(x2m, dtype=DT[prec]), chi3=torch.tensor(x3m, dtype=DT[prec]))
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -190,6 +211,8 @@ def te_case(prec, sigma=False, poles=False, magnetic=False):
         out["sigma"] = sig
     if magnetic:
         out["sigma_b"], out["mu"] = sbm, mum
+    if nonlinear:
+        out["chi2"], out["chi3"] = x2m, x3m
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -508,6 +531,13 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["nonlinear"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_tm_nonlinear_{prec}.npz"),
+                                **tm_case(prec, nonlinear=True))
+            np.savez_compressed(os.path.join(HERE, f"golden_te_nonlinear_{prec}.npz"),
+                                **te_case(prec, nonlinear=True))
         return
     if sys.argv[1:] == ["magnetic"]:
         for prec in ("f64", "f32"):

@@ -38,7 +38,7 @@ def run_tm_oracle(g, prec):
     c = O.tm_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]),
                     y_pmc=bool(g["y_pmc"]), dtype=dt_np, sigma=g.get("sigma"),
                     poles=poles, pole_masks=g.get("pole_masks"), sigma_b=g.get("sigma_b"),
-                    mu=g.get("mu"))
+                    mu=g.get("mu"), chi2=g.get("chi2"), chi3=g.get("chi3"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -56,7 +56,7 @@ def run_tm_oracle(g, prec):
 
 
 @pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles",
-                                  "tm_magnetic"])
+                                  "tm_magnetic", "tm_nonlinear"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_tm_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
@@ -83,7 +83,8 @@ def run_te_oracle(g, prec):
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     c = O.te_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
                     sigma=g.get("sigma"), poles=poles, pole_masks=g.get("pole_masks"),
-                    sigma_b=g.get("sigma_b"), mu=g.get("mu"))
+                    sigma_b=g.get("sigma_b"), mu=g.get("mu"), chi2=g.get("chi2"),
+                    chi3=g.get("chi3"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)[:, :-1]
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -100,7 +101,8 @@ def run_te_oracle(g, prec):
     return c, mask, s, acc
 
 
-@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic"])
+@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic",
+                                  "te_nonlinear"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_te_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
