@@ -100,7 +100,8 @@ def pole_recurrence(pole, dt):
 
 def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
               dtype=np.float64, sigma=None, poles=(), pole_masks=None, sigma_b=None, mu=None,
-              y_mirror=0, x_mirror=0, y_rot2=0, rot4=0, chi2=None, chi3=None):
+              y_mirror=0, x_mirror=0, y_rot2=0, rot4=0, chi2=None, chi3=None,
+              m_poles=(), m_pole_masks=None):
     """TM coefficient set (core/coeffs.py:134-291, PEC/PMC path only).
 
     Profiles are sliced to the live derivative nodes exactly as
@@ -114,7 +115,9 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
     low-y / low-x edge; ``y_rot2`` (C2 about the low-y cut) and ``rot4`` (C4, both low
     edges, square grids) likewise. A cut replaces the low-side PML, and the D-side
     profiles then keep the cut row / column (0 .. n-2) instead of the interior.
-    ``chi2`` / ``chi3`` (nx, ny): the instantaneous nonlinearity of :154-158."""
+    ``chi2`` / ``chi3`` (nx, ny): the instantaneous nonlinearity of :154-158.
+    ``m_poles`` = [(fn, gamma, sigma), ...] with ``m_pole_masks``: magnetic Lorentz
+    poles (:177-193), the masks averaged onto Hx (along y) and Hy (along x)."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -182,6 +185,23 @@ def tm_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, y_pmc=False,
         x3 = z if chi3 is None else np.asarray(chi3, dtype=dtype)
         if (x2 != 0).any() or (x3 != 0).any():
             nl = dict(chi2=x2, chi3=x3)
+    if m_poles:
+        if "d1" in cond:
+            raise NotImplementedError("m_poles with sigma_d / sigma_b / mu")
+        nm, h = len(m_poles), dtype.type(0.5)
+        for suf, shape, avg in (("x", (nx, ny - 1), lambda v: h * (v[:, :-1] + v[:, 1:])),
+                                ("y", (nx - 1, ny), lambda v: h * (v[:-1, :] + v[1:, :]))):
+            c1m, c2m, c3m = (np.zeros((nm,) + shape, dtype=dtype) for _ in range(3))
+            for k, pole in enumerate(m_poles):
+                fn, gamma, sig = pole[0], pole[1], pole[2]
+                w0, G = 2 * math.pi * fn, 2 * math.pi * gamma
+                den = 1.0 + G * dt / 2.0
+                msk = (np.ones((nx, ny), dtype=dtype) if m_pole_masks is None
+                       else np.asarray(m_pole_masks[k], dtype=dtype))
+                c1m[k] = dtype.type((2.0 - w0 * w0 * dt * dt) / den)
+                c2m[k] = dtype.type(-(1.0 - G * dt / 2.0) / den)
+                c3m[k] = dtype.type(sig * w0 * w0 * dt * dt / den) * avg(msk)
+            nl.update({"mc1" + suf: c1m, "mc2" + suf: c2m, "mc3" + suf: c3m})
     return dict(pol="tm", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, y_pmc=y_pmc, **cond,
                 **nl, y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4,
                 b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
@@ -209,6 +229,11 @@ def tm_state(c):
         st["Hx0"] = z(nx)
     if xm == -1 or r4:
         st["Hy0"] = z(ny)
+    if "mc1x" in c:                     # magnetic poles: B and the M histories
+        nm = c["mc1x"].shape[0]
+        st.update(Bx=z(nx, ny - 1), By=z(nx - 1, ny), Mx_cur=z(nm, nx, ny - 1),
+                  Mx_prev=z(nm, nx, ny - 1), My_cur=z(nm, nx - 1, ny),
+                  My_prev=z(nm, nx - 1, ny))
     return st
 
 
@@ -226,7 +251,13 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
     dEz_dx = (Ez[1:, :] - Ez[:-1, :]) / T(dx)
     psi_Ezx = c["b_hx"] * s["psi_Ezx"] + c["a_hx"] * dEz_dx
     curl_hy = dEz_dx / c["k_hx"] + psi_Ezx
-    if "h1x" in c:
+    mpol = {}
+    if "mc1x" in c:
+        # magnetic poles: B integrates the curl (core/stepper_tm.py:115-119); H is
+        # formed below by update_eh(H)
+        Bx = s["Bx"] - T(dt) * curl_hx
+        By = s["By"] + T(dt) * curl_hy
+    elif "h1x" in c:
         # magnetic conductivity / permeability (core/stepper_tm.py:121-125)
         Hx = c["h1x"] * s["Hx"] - c["h2x"] * curl_hx
         Hy = c["h1y"] * s["Hy"] + c["h2y"] * curl_hy
@@ -246,11 +277,25 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
         ez0x = Ez[0, :]
         ghost_x = r4 * Ez[:, 0] if r4 else -ez0x
         mir["Hy0"] = s["Hy0"] + T(dt) * (ez0x - ghost_x) / T(dx)
-    # magnetic sheet current (mode sources), subtracted (core/stepper_tm.py:186-196)
-    if hy_mask is not None:
-        Hy = Hy - T(dt * amp_h) * hy_mask
-    if hx_mask is not None:
-        Hx = Hx - T(dt * amp_h) * hx_mask
+    # magnetic sheet current (mode sources), subtracted (core/stepper_tm.py:186-196),
+    # into B when magnetic poles carry it
+    if "mc1x" in c:
+        if hy_mask is not None:
+            By = By - T(dt * amp_h) * hy_mask
+        if hx_mask is not None:
+            Bx = Bx - T(dt * amp_h) * hx_mask
+        # update_eh(H) (:215-224): M(n+1) = mc1 M(n) + mc2 M(n-1) + mc3 H(n-1/2),
+        # H = B - sum M
+        Mx = c["mc1x"] * s["Mx_cur"] + c["mc2x"] * s["Mx_prev"] + c["mc3x"] * s["Hx"]
+        My = c["mc1y"] * s["My_cur"] + c["mc2y"] * s["My_prev"] + c["mc3y"] * s["Hy"]
+        Hx, Hy = Bx - Mx.sum(0), By - My.sum(0)
+        mpol = dict(Bx=Bx, By=By, Mx_cur=Mx, Mx_prev=s["Mx_cur"], My_cur=My,
+                    My_prev=s["My_cur"])
+    else:
+        if hy_mask is not None:
+            Hy = Hy - T(dt * amp_h) * hy_mask
+        if hx_mask is not None:
+            Hx = Hx - T(dt * amp_h) * hx_mask
     # D update (core/stepper_tm.py:130-166): ghost / plane H beyond each wall, then
     # differences over the live Ez region -- interior (PEC), all rows (y-PMC), or from
     # the cut up (even mirror: H = 0 ghost; odd / C2 / C4: the plane node)
@@ -292,7 +337,7 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
         if mask is not None:
             Dz = Dz - T(dt * amp) * mask
     out = dict(Hx=Hx, Hy=Hy, Dz=Dz, psi_Ezy=psi_Ezy, psi_Ezx=psi_Ezx, psi_Hyx=psi_Hyx,
-               psi_Hxy=psi_Hxy, **mir)
+               psi_Hxy=psi_Hxy, **mir, **mpol)
     if c["c1"].shape[0]:
         # update_pols (core/stepper_tm.py:203-207) on the old Ez, then
         # update_eh(E): Ez = (Dz - sum P) / eps_inf (:220-224)

@@ -19,8 +19,9 @@ cases of the hot path through its own public functions:
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
   (``sigma_b``, ``mu``; ``make_golden.py magnetic``), and the symmetry-folded TM and TE
-  runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``), and chi2 / chi3 runs
-  (``make_golden.py nonlinear``) and the TM and TE cases with a Lorentz and a Drude pole
+  runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``), chi2 / chi3 runs
+  (``make_golden.py nonlinear``) and a TM run with magnetic Lorentz poles
+  (``make_golden.py mpoles``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -108,8 +109,11 @@ def chi_maps(nx, ny, seed):
     return x2, x3
 
 
+M_POLES = [(0.6, 0.05, 0.8), (0.9, 0.1, 0.4)]      # two magnetic Lorentz poles
+
+
 def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=False,
-            nonlinear=False):
+            nonlinear=False, mpoles=False):
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -124,6 +128,9 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
     x2m, x3m = chi_maps(nx, ny, 25) if nonlinear else (None, None)
     if nonlinear:
         kw.update(chi2=torch.tensor(x2m, dtype=DT[prec]), chi3=torch.tensor(x3m, dtype=DT[prec]))
+    mpm = pole_masks(nx, ny) if mpoles else None
+    if mpoles:
+        kw.update(m_poles=M_POLES, m_pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in mpm])
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -138,7 +145,8 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
     monx = FluxMonitorTM(g, freqs, x_normal=True, idx=36, lo=9, hi=27)
     mony = FluxMonitorTM(g, freqs, x_normal=False, idx=26, lo=10, hi=38)
     dft = DFTFieldsMonitor(g, freqs, component="Ez")
-    s0 = init_tm_state(g, y_pmc=y_pmc, n_poles=len(POLES) if poles else 0)
+    s0 = init_tm_state(g, y_pmc=y_pmc, n_poles=len(POLES) if poles else 0,
+                       n_mpoles=len(M_POLES) if mpoles else 0)
     n = 300
     with torch.no_grad():
         st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft])
@@ -155,6 +163,9 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
         out["sigma_b"], out["mu"] = sbm, mum
     if nonlinear:
         out["chi2"], out["chi3"] = x2m, x3m
+    if mpoles:
+        out["m_poles"] = json.dumps(M_POLES)
+        out["m_pole_masks"] = np.stack(mpm)
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -531,6 +542,11 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["mpoles"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_tm_mpoles_{prec}.npz"),
+                                **tm_case(prec, mpoles=True))
         return
     if sys.argv[1:] == ["nonlinear"]:
         for prec in ("f64", "f32"):

@@ -38,7 +38,9 @@ def run_tm_oracle(g, prec):
     c = O.tm_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]),
                     y_pmc=bool(g["y_pmc"]), dtype=dt_np, sigma=g.get("sigma"),
                     poles=poles, pole_masks=g.get("pole_masks"), sigma_b=g.get("sigma_b"),
-                    mu=g.get("mu"), chi2=g.get("chi2"), chi3=g.get("chi3"))
+                    mu=g.get("mu"), chi2=g.get("chi2"), chi3=g.get("chi3"),
+                    m_poles=json.loads(str(g["m_poles"])) if "m_poles" in g else (),
+                    m_pole_masks=g.get("m_pole_masks"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -56,7 +58,7 @@ def run_tm_oracle(g, prec):
 
 
 @pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles",
-                                  "tm_magnetic", "tm_nonlinear"])
+                                  "tm_magnetic", "tm_nonlinear", "tm_mpoles"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_tm_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
@@ -67,6 +69,8 @@ def test_tm_oracle_matches_reference(case, prec):
     names = ["Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"]
     if "s_P_cur" in g:
         names += ["P_cur", "P_prev"]
+    if "s_Mx_cur" in g:
+        names += ["Bx", "By", "Mx_cur", "Mx_prev", "My_cur", "My_prev"]
     for k in names:
         assert rel_l2(s[k], g["s_" + k]) < TOL[prec], k
     for a, key in zip(acc, ("acc_x", "acc_y", "acc_dft")):
