@@ -361,7 +361,7 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
 
 def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None,
               poles=(), pole_masks=None, sigma_b=None, mu=None, y_mirror=0, x_mirror=0,
-              chi2=None, chi3=None):
+              chi2=None, chi3=None, eps_tensor=None):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
@@ -370,7 +370,8 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
     averaged over the four nodes around each Hz. Any of the three builds all pairs.
     ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd) replace the low-side PML with the
     mirror wall (:457-469). ``chi2`` / ``chi3`` (nx, ny) are Yee-averaged to Ex / Ey
-    (:382-387)."""
+    (:382-387). ``eps_tensor`` = (exx, exy, eyy) at cell centres: the in-plane
+    inverse tensor's components Yee-averaged to the E nodes (:390-400)."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -424,6 +425,13 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
         if (x2 != 0).any() or (x3 != 0).any():
             nl = dict(chi2_x=h * (x2[:-1, :] + x2[1:, :]), chi2_y=h * (x2[:, :-1] + x2[:, 1:]),
                       chi3_x=h * (x3[:-1, :] + x3[1:, :]), chi3_y=h * (x3[:, :-1] + x3[:, 1:]))
+    if eps_tensor is not None:
+        exx, exy, eyy = (np.asarray(v, dtype=dtype) for v in eps_tensor)
+        det = exx * eyy - exy * exy
+        ax = lambda v: h * (v[:-1, :] + v[1:, :])          # noqa: E731
+        ay = lambda v: h * (v[:, :-1] + v[:, 1:])          # noqa: E731
+        nl.update(inv_xx_x=ax(eyy / det), inv_xy_x=ax(-exy / det),
+                  inv_yy_y=ay(exx / det), inv_xy_y=ay(-exy / det))
     return dict(pol="te", dt=dt, dx=dx, nx=nx, ny=ny, dtype=dtype, eps=e, **cond, **nl,
                 eps_x=eps_x, eps_y=eps_y, y_mirror=y_mirror, x_mirror=x_mirror,
                 b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
@@ -493,17 +501,21 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
         Px = c["c1x"] * s["Px_cur"] + c["c2x"] * s["Px_prev"] + c["c3x"] * s["Ex"]
         Py = c["c1y"] * s["Py_cur"] + c["c2y"] * s["Py_prev"] + c["c3y"] * s["Ey"]
         pol = dict(Px_cur=Px, Px_prev=s["Px_cur"], Py_cur=Py, Py_prev=s["Py_cur"])
-        Ex = (Dx - Px.sum(0)) / c["eps_x"]
-        Ey = (Dy - Py.sum(0)) / c["eps_y"]
+        rhs_x, rhs_y = Dx - Px.sum(0), Dy - Py.sum(0)
     else:
         pol = {k: s.get(k) for k in ("Px_cur", "Px_prev", "Py_cur", "Py_prev")}
-        Ex = Dx / c["eps_x"]
-        Ey = Dy / c["eps_y"]
+        rhs_x, rhs_y = Dx, Dy
+    if "inv_xx_x" in c:
+        # in-plane tensor eps (core/stepper_te.py:162-165): E = eps^-1 (D - P), the
+        # cross terms from the other component averaged over four nodes
+        Ex = c["inv_xx_x"] * rhs_x + c["inv_xy_x"] * _avg4_to_ex(rhs_y)
+        Ey = c["inv_yy_y"] * rhs_y + c["inv_xy_y"] * _avg4_to_ey(rhs_x)
+    else:
+        Ex = rhs_x / c["eps_x"]
+        Ey = rhs_y / c["eps_y"]
     if "chi3_x" in c:
         # instantaneous chi2 / chi3 (core/stepper_te.py:157-174): three fixed-point
         # sweeps with |E|^2 from the other component averaged over four nodes
-        rhs_x = Dx - pol["Px_cur"].sum(0) if pol.get("Px_cur") is not None else Dx
-        rhs_y = Dy - pol["Py_cur"].sum(0) if pol.get("Py_cur") is not None else Dy
         for _ in range(3):
             E2x = Ex * Ex + _avg4_to_ex(Ey) ** 2
             E2y = Ey * Ey + _avg4_to_ey(Ex) ** 2

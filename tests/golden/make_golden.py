@@ -20,8 +20,9 @@ cases of the hot path through its own public functions:
   ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
   (``sigma_b``, ``mu``; ``make_golden.py magnetic``), and the symmetry-folded TM and TE
   runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``), chi2 / chi3 runs
-  (``make_golden.py nonlinear``) and a TM run with magnetic Lorentz poles
-  (``make_golden.py mpoles``) and the TM and TE cases with a Lorentz and a Drude pole
+  (``make_golden.py nonlinear``), a TM run with magnetic Lorentz poles
+  (``make_golden.py mpoles``) and a TE run with an in-plane tensor eps
+  (``make_golden.py tensor``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -178,7 +179,15 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
     return out
 
 
-def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False):
+def tensor_maps(eps):
+    """An in-plane anisotropic block: exx raised, a 0.5 off-diagonal on a patch."""
+    exx, exy, eyy = eps.copy(), np.zeros_like(eps), eps.copy()
+    exx[10:30, 6:16] += 2.0
+    exy[14:26, 8:14] = 0.5
+    return exx, exy, eyy
+
+
+def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False, tensor=False):
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -193,6 +202,9 @@ def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False):
     x2m, x3m = chi_maps(nx, ny, 26) if nonlinear else (None, None)
     if nonlinear:
         kw.update(chi2=torch.tensor(x2m, dtype=DT[prec]), chi3=torch.tensor(x3m, dtype=DT[prec]))
+    tens = tensor_maps(eps) if tensor else None
+    if tensor:
+        kw.update(eps_tensor=tuple(torch.tensor(v, dtype=DT[prec]) for v in tens))
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -224,6 +236,8 @@ def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False):
         out["sigma_b"], out["mu"] = sbm, mum
     if nonlinear:
         out["chi2"], out["chi3"] = x2m, x3m
+    if tensor:
+        out["eps_tensor"] = np.stack(tens)
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -542,6 +556,11 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["tensor"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_te_tensor_{prec}.npz"),
+                                **te_case(prec, tensor=True))
         return
     if sys.argv[1:] == ["mpoles"]:
         for prec in ("f64", "f32"):
