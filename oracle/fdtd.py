@@ -664,33 +664,86 @@ def _bc(v, ax):
     return v.reshape(sh)
 
 
+def _per_axis3(v):
+    """Per-axis layer counts of a 3D box (core/stepper_3d.py:142-147): an int (or a
+    (lo, hi) pair) for all three axes, or a 3-sequence of int-or-pair."""
+    if isinstance(v, (tuple, list)):
+        return tuple(v)
+    return (v, v, v)
+
+
+def absorber_sigma(n, nabs, dx, R0=1e-15, m=2, dtype=np.float64):
+    """Matched-sigma absorber profile along one axis (core/pml.py:62-80): a
+    quadratic (order m) ramp on each edge's nabs cells, peak -(m+1) ln R0 / (2 nc dx)."""
+    n_lo, n_hi = side_counts(nabs)
+    p = np.zeros(n, dtype=dtype)
+
+    def ramp(nc):
+        smax = -(m + 1) * math.log(R0) / (2.0 * nc * dx)
+        i = np.arange(nc, dtype=dtype)
+        return smax * ((nc - i - 0.5) / nc) ** m
+    if n_lo > 0:
+        p[:n_lo] = ramp(n_lo)
+    if n_hi > 0:
+        p[n - n_hi:] = ramp(n_hi)[::-1]
+    return p
+
+
 def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
-              sigma_b=None, poles=(), pole_masks=None):
-    """3D CPML coefficient set (core/stepper_3d.py:150-266, CPML path, no
-    conductivity, no poles). dt = 0.5 dx / sqrt(3). H-side profiles on the
-    n-1 half nodes, E-side on the interior [1:-1]."""
+              sigma_b=None, poles=(), pole_masks=None, n_abs=0, absorber_axes=(),
+              absorber_m=2, absorber_R0=1e-15):
+    """3D coefficient set (core/stepper_3d.py:150-266). dt = 0.5 dx / sqrt(3). H-side
+    CPML profiles on the n-1 half nodes, E-side on the interior [1:-1].
+
+    Boundary modes (:170-215): CPML (npml > 0); the matched-sigma absorber (npml = 0,
+    ``n_abs`` > 0) -- plain derivatives and the absorber sigma added to both the
+    electric and magnetic damping; or mixed (both), the absorber on ``absorber_axes``
+    and CPML on the others. A plain derivative is written here as the identity
+    profile (b = 0, a = 0, k = 1): the memory then stays 0 and d / 1 + 0 = d exactly,
+    the reference's own form for the absorber axes of mixed mode (:132-147)."""
     dtype = np.dtype(dtype)
     dt = 0.5 * dx / math.sqrt(3.0)
     e = (np.ones((nx, ny, nz), dtype=dtype) if eps is None
          else np.asarray(eps, dtype=dtype).copy())
     dims = (nx, ny, nz)
+    npml_ax = [side_counts(v) for v in _per_axis3(npml)]
+    nabs_ax = [side_counts(v) for v in _per_axis3(n_abs)]
+    has_pml = any(lo or hi for lo, hi in npml_ax)
+    has_abs = any(lo or hi for lo, hi in nabs_ax)
+    mixed = has_pml and has_abs
+    plain_axes = set(absorber_axes) if mixed else ({0, 1, 2} if not has_pml else set())
     cp = {}
     for ax, kh, ke in ((0, "hx", "ex"), (1, "hy", "ey"), (2, "hz", "ez")):
         n = dims[ax]
-        b, a, k = cpml_profiles(n - 1, npml, 0.5, dt, dx, dtype=dtype)
+        if ax in plain_axes:
+            ident = lambda L: tuple(_bc(v, ax) for v in (np.zeros(L, dtype=dtype),  # noqa: E731
+                                                          np.zeros(L, dtype=dtype),
+                                                          np.ones(L, dtype=dtype)))
+            cp[kh], cp[ke] = ident(n - 1), ident(n - 2)
+            continue
+        b, a, k = cpml_profiles(n - 1, npml_ax[ax], 0.5, dt, dx, dtype=dtype)
         cp[kh] = (_bc(b, ax), _bc(a, ax), _bc(k, ax))
-        b, a, k = cpml_profiles(n, npml, 0.0, dt, dx, dtype=dtype)
+        b, a, k = cpml_profiles(n, npml_ax[ax], 0.0, dt, dx, dtype=dtype)
         cp[ke] = (_bc(b[1:-1], ax), _bc(a[1:-1], ax), _bc(k[1:-1], ax))
+    sig_bound = None
+    if has_abs:
+        sig_bound = np.zeros((nx, ny, nz), dtype=dtype)
+        for ax in (absorber_axes if mixed else (0, 1, 2)):
+            sa = absorber_sigma(dims[ax], nabs_ax[ax], dx, R0=absorber_R0, m=absorber_m,
+                                dtype=dtype)
+            sig_bound = np.maximum(sig_bound, _bc(sa, ax))
     # damping pairs (core/stepper_3d.py:217-235): (1, dt) without conductivity, else
-    # (1 - s dt/2)/(1 + s dt/2), dt/(1 + s dt/2) with sigma_d Yee-averaged onto each E
-    # component and sigma_b onto each H component
-    if sigma_d is None and sigma_b is None:
+    # (1 - s dt/2)/(1 + s dt/2), dt/(1 + s dt/2) with sigma_d (+ the absorber) Yee-averaged
+    # onto each E component and sigma_b (+ the absorber) onto each H component
+    if sigma_d is None and sigma_b is None and sig_bound is None:
         one, d2 = dtype.type(1.0), dtype.type(dt)
         damp = {k: (one, d2) for k in ("ex", "ey", "ez", "hx", "hy", "hz")}
     else:
         z = np.zeros((nx, ny, nz), dtype=dtype)
         sd = z if sigma_d is None else np.asarray(sigma_d, dtype=dtype)
         sb = z if sigma_b is None else np.asarray(sigma_b, dtype=dtype)
+        if sig_bound is not None:
+            sd, sb = sig_bound + sd, sig_bound + sb
         pair = lambda sg: ((1 - sg * dt / 2) / (1 + sg * dt / 2), dt / (1 + sg * dt / 2))  # noqa: E731
         damp = {"ex": pair(_avg(sd, 0)), "ey": pair(_avg(sd, 1)), "ez": pair(_avg(sd, 2)),
                 "hx": pair(_avg(_avg(sb, 1), 2)), "hy": pair(_avg(_avg(sb, 0), 2)),

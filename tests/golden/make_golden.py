@@ -21,8 +21,9 @@ cases of the hot path through its own public functions:
   (``sigma_b``, ``mu``; ``make_golden.py magnetic``), and the symmetry-folded TM and TE
   runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``), chi2 / chi3 runs
   (``make_golden.py nonlinear``), a TM run with magnetic Lorentz poles
-  (``make_golden.py mpoles``) and a TE run with an in-plane tensor eps
-  (``make_golden.py tensor``) and the TM and TE cases with a Lorentz and a Drude pole
+  (``make_golden.py mpoles``), a TE run with an in-plane tensor eps
+  (``make_golden.py tensor``) and the 3D matched-sigma absorber, alone and beside CPML
+  (``make_golden.py absorber3d``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -304,9 +305,13 @@ FACES = [("x", 5), ("x", 18), ("y", 5), ("y", 16), ("z", 5), ("z", 14)]
 POLES3 = [(0.5, 0.05, 2.0), (0.0, 0.1, 1.0, 0.8)]     # a Lorentz and a Drude pole
 
 
-def case_3d(prec, lean=False, sigma=False, poles=False):
+def case_3d(prec, lean=False, sigma=False, poles=False, absorber=None):
     rng = np.random.default_rng(13)
     nx, ny, nz, dx, npml = 24, 22, 20, 1.0 / 16, 4
+    # matched-sigma absorber on every face (npml 0), or on z beside x / y CPML
+    ab = {None: {}, "abs": dict(n_abs=5), "mixed": dict(n_abs=5, absorber_axes=(2,))}[absorber]
+    if absorber == "abs":
+        npml = 0
     eps = np.ones((nx, ny, nz))
     for _ in range(6):                                # a few spheres, draw order
         c = rng.uniform(4, [nx - 4, ny - 4, nz - 4])
@@ -343,7 +348,7 @@ def case_3d(prec, lean=False, sigma=False, poles=False):
             pm3[0][8:16, 6:14, 6:14] = 1.0
             pm3[1][14:19, 12:17, 9:15] = 1.0
             kw.update(poles=POLES3, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm3])
-        c = build_3d_coeffs(nx, ny, nz, dx, eps=epst, npml=npml, dtype=DT[prec], **kw)
+        c = build_3d_coeffs(nx, ny, nz, dx, eps=epst, npml=npml, dtype=DT[prec], **kw, **ab)
         src = PointSource3D(c.dt, "Ez", *src_ijk, prof)
         mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=i, win=win, dtype=DT[prec])
                 for a, i in FACES]
@@ -357,6 +362,9 @@ def case_3d(prec, lean=False, sigma=False, poles=False):
                faces=json.dumps(FACES), win=np.array(win))
     if sigma:
         out["sigma_d"], out["sigma_b"] = sd, sb
+    if ab:
+        out["n_abs"] = ab["n_abs"]
+        out["absorber_axes"] = np.array(ab.get("absorber_axes", ()), dtype=np.int64)
     if poles:
         out["poles"] = json.dumps(POLES3)
         out["pole_masks"] = np.stack(pm3)
@@ -556,6 +564,12 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["absorber3d"]:
+        for prec in ("f64", "f32"):
+            for mode in ("abs", "mixed"):
+                np.savez_compressed(os.path.join(HERE, f"golden_3d_{mode}_{prec}.npz"),
+                                    **case_3d(prec, absorber=mode))
         return
     if sys.argv[1:] == ["tensor"]:
         for prec in ("f64", "f32"):
