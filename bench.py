@@ -617,7 +617,6 @@ def run_cfg3(args, rank, world, dev):
         return res
     # ---- e2e: host eps through the public API (run_3d), flux accumulators back
     from meep_torch_b200.core.monitors_3d import run_3d
-    from meep_torch_b200.core.stepper_3d import init_3d_state
     host_eps = torch.from_numpy(W.cfg3_eps(n)).pin_memory()
     d2h = 0
 
