@@ -1,7 +1,4 @@
 """3D sources, monitors and the forward runner (reference: core/monitors_3d.py:18-210)."""
-import math
-from typing import Sequence
-
 import torch
 
 from ..engine3d import Engine3D
