@@ -361,7 +361,7 @@ def tm_step(s, c, amp=0.0, mask=None, amp_h=0.0, hy_mask=None, hx_mask=None):
 
 def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma=None,
               poles=(), pole_masks=None, sigma_b=None, mu=None, y_mirror=0, x_mirror=0,
-              chi2=None, chi3=None, eps_tensor=None):
+              chi2=None, chi3=None, eps_tensor=None, poles_tensor=(), pole_masks_tensor=None):
     """TE coefficient set (core/coeffs.py:357-503, PEC path only).
 
     eps is Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1) positions
@@ -371,7 +371,10 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
     ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd) replace the low-side PML with the
     mirror wall (:457-469). ``chi2`` / ``chi3`` (nx, ny) are Yee-averaged to Ex / Ey
     (:382-387). ``eps_tensor`` = (exx, exy, eyy) at cell centres: the in-plane
-    inverse tensor's components Yee-averaged to the E nodes (:390-400)."""
+    inverse tensor's components Yee-averaged to the E nodes (:390-400).
+    ``poles_tensor`` = [(fn, gamma, (sxx, sxy, syy)[, fc]), ...]: oriented poles
+    (:426-452) appended to both axis stacks, sxx / syy on the diagonal c3 and sxy in
+    the cross terms c3xy (Px from Ey) and c3yx (Py from Ex)."""
     dtype = np.dtype(dtype)
     dt = courant * dx
     e = (np.ones((nx, ny), dtype=dtype) if eps is None
@@ -417,6 +420,27 @@ def te_coeffs(nx, ny, dx, eps=None, npml=0, courant=0.5, dtype=np.float64, sigma
             c2[k] = dtype.type(cv2)
             c3[k] = dtype.type(cv3) * mavg
         cond.update({"c1" + ax: c1, "c2" + ax: c2, "c3" + ax: c3})
+    if len(poles_tensor):
+        # oriented poles (core/coeffs.py:426-452): one extra pole per axis stack, the
+        # cross drive zero for the plain poles before them
+        for ax, shape in (("x", (nx - 1, ny)), ("y", (nx, ny - 1))):
+            nt = len(poles_tensor)
+            t1, t2, t3, tc = (np.zeros((nt,) + shape, dtype=dtype) for _ in range(4))
+            for k, pole in enumerate(poles_tensor):
+                fn, gamma, (sxx, sxy, syy) = pole[0], pole[1], pole[2]
+                fc = pole[3] if len(pole) > 3 else fn
+                cv1, cv2, cv3 = pole_recurrence((fn, gamma, 1.0, fc), dt)
+                m = (np.ones((nx, ny), dtype=dtype) if pole_masks_tensor is None
+                     else np.asarray(pole_masks_tensor[k], dtype=dtype))
+                mavg = h * (m[:-1, :] + m[1:, :]) if ax == "x" else h * (m[:, :-1] + m[:, 1:])
+                t1[k], t2[k] = dtype.type(cv1), dtype.type(cv2)
+                t3[k] = dtype.type(cv3 * (sxx if ax == "x" else syy)) * mavg
+                tc[k] = dtype.type(cv3 * sxy) * mavg
+            n0 = cond["c1" + ax].shape[0]
+            for key, t in (("c1", t1), ("c2", t2), ("c3", t3)):
+                cond[key + ax] = np.concatenate([cond[key + ax], t])
+            cond["c3xy" if ax == "x" else "c3yx"] = np.concatenate(
+                [np.zeros((n0,) + shape, dtype=dtype), tc])
     nl = {}
     if chi2 is not None or chi3 is not None:
         z = np.zeros((nx, ny), dtype=dtype)
@@ -500,6 +524,10 @@ def te_step(s, c, amp=0.0, mask_ey=None, amp_h=0.0, hz_mask=None):
         # update_pols on the old E (core/stepper_te.py:136-146), update_eh(E) (:159-169)
         Px = c["c1x"] * s["Px_cur"] + c["c2x"] * s["Px_prev"] + c["c3x"] * s["Ex"]
         Py = c["c1y"] * s["Py_cur"] + c["c2y"] * s["Py_prev"] + c["c3y"] * s["Ey"]
+        if "c3xy" in c:
+            # oriented poles: the off-diagonal drive (core/stepper_te.py:142-145)
+            Px = Px + c["c3xy"] * _avg4_to_ex(s["Ey"])
+            Py = Py + c["c3yx"] * _avg4_to_ey(s["Ex"])
         pol = dict(Px_cur=Px, Px_prev=s["Px_cur"], Py_cur=Py, Py_prev=s["Py_cur"])
         rhs_x, rhs_y = Dx - Px.sum(0), Dy - Py.sum(0)
     else:

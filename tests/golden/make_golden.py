@@ -35,6 +35,7 @@ path (tests/test_gpu_parity.py); this script is only re-run by hand.
 from __future__ import annotations
 
 import json
+import math
 import os
 import sys
 
@@ -188,7 +189,13 @@ def tensor_maps(eps):
     return exx, exy, eyy
 
 
-def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False, tensor=False):
+_TH = math.radians(30.0)
+POLES_T = [(0.65, 0.05, (math.cos(_TH) ** 2, math.cos(_TH) * math.sin(_TH),
+                         math.sin(_TH) ** 2))]              # one pole, optic axis at 30 deg
+
+
+def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False, tensor=False,
+            tensor_poles=False):
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -206,6 +213,10 @@ def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False, ten
     tens = tensor_maps(eps) if tensor else None
     if tensor:
         kw.update(eps_tensor=tuple(torch.tensor(v, dtype=DT[prec]) for v in tens))
+    tpm = pole_masks(nx, ny) if tensor_poles else None
+    if tensor_poles:                      # a plain shared pole, then the oriented one
+        kw.update(poles=POLES[:1], pole_masks=[torch.tensor(tpm[0], dtype=DT[prec])],
+                  poles_tensor=POLES_T, pole_masks_tensor=[torch.tensor(tpm[1], dtype=DT[prec])])
     pm = pole_masks(nx, ny) if poles else None
     if poles:
         kw.update(poles=POLES, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
@@ -221,7 +232,7 @@ def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False, ten
     monx = FluxMonitorTE(g, freqs, ix=32, lo=9, hi=31)
     mony = FluxMonitorTEY(g, freqs, iy=30, lo=9, hi=35)
     dft = DFTFieldsMonitor(g, freqs, component="Hz")
-    s0 = init_te_state(g, n_poles=len(POLES) if poles else 0)
+    s0 = init_te_state(g, n_poles=len(POLES) if poles else (2 if tensor_poles else 0))
     n = 300
     with torch.no_grad():
         st, (ax, ay, ad) = run_te(s0, m, n, source=_TESrc(), monitors=[monx, mony, dft])
@@ -239,6 +250,11 @@ def te_case(prec, sigma=False, poles=False, magnetic=False, nonlinear=False, ten
         out["chi2"], out["chi3"] = x2m, x3m
     if tensor:
         out["eps_tensor"] = np.stack(tens)
+    if tensor_poles:
+        out["poles"] = json.dumps(POLES[:1])
+        out["pole_masks"] = tpm[:1]
+        out["poles_tensor"] = json.dumps(POLES_T)
+        out["pole_masks_tensor"] = tpm[1:]
     if poles:
         out["poles"] = json.dumps(POLES)
         out["pole_masks"] = np.stack(pm)
@@ -575,6 +591,8 @@ def main():
         for prec in ("f64", "f32"):
             np.savez_compressed(os.path.join(HERE, f"golden_te_tensor_{prec}.npz"),
                                 **te_case(prec, tensor=True))
+            np.savez_compressed(os.path.join(HERE, f"golden_te_tensor_poles_{prec}.npz"),
+                                **te_case(prec, tensor_poles=True))
         return
     if sys.argv[1:] == ["mpoles"]:
         for prec in ("f64", "f32"):

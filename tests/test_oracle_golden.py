@@ -88,7 +88,9 @@ def run_te_oracle(g, prec):
     c = O.te_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
                     sigma=g.get("sigma"), poles=poles, pole_masks=g.get("pole_masks"),
                     sigma_b=g.get("sigma_b"), mu=g.get("mu"), chi2=g.get("chi2"),
-                    chi3=g.get("chi3"), eps_tensor=g.get("eps_tensor"))
+                    chi3=g.get("chi3"), eps_tensor=g.get("eps_tensor"),
+                    poles_tensor=json.loads(str(g["poles_tensor"])) if "poles_tensor" in g else (),
+                    pole_masks_tensor=g.get("pole_masks_tensor"))
     mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                               int(g["src_j1"]), dtype=dt_np)[:, :-1]
     prof = O.gaussian_pulse(float(g["fcen"]), float(g["fwidth"]))
@@ -106,7 +108,7 @@ def run_te_oracle(g, prec):
 
 
 @pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic",
-                                  "te_nonlinear", "te_tensor"])
+                                  "te_nonlinear", "te_tensor", "te_tensor_poles"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_te_oracle_matches_reference(case, prec):
     g = load_golden(f"{case}_{prec}")
