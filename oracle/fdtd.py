@@ -719,7 +719,7 @@ def absorber_sigma(n, nabs, dx, R0=1e-15, m=2, dtype=np.float64):
 
 def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
               sigma_b=None, poles=(), pole_masks=None, n_abs=0, absorber_axes=(),
-              absorber_m=2, absorber_R0=1e-15):
+              absorber_m=2, absorber_R0=1e-15, pmc_axes=()):
     """3D coefficient set (core/stepper_3d.py:150-266). dt = 0.5 dx / sqrt(3). H-side
     CPML profiles on the n-1 half nodes, E-side on the interior [1:-1].
 
@@ -728,7 +728,9 @@ def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
     electric and magnetic damping; or mixed (both), the absorber on ``absorber_axes``
     and CPML on the others. A plain derivative is written here as the identity
     profile (b = 0, a = 0, k = 1): the memory then stays 0 and d / 1 + 0 = d exactly,
-    the reference's own form for the absorber axes of mixed mode (:132-147)."""
+    the reference's own form for the absorber axes of mixed mode (:132-147).
+    ``pmc_axes``: PMC walls instead of PEC on those axes (plain derivatives there; the
+    E update keeps the wall values, see _term_pmc)."""
     dtype = np.dtype(dtype)
     dt = 0.5 * dx / math.sqrt(3.0)
     e = (np.ones((nx, ny, nz), dtype=dtype) if eps is None
@@ -740,6 +742,7 @@ def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
     has_abs = any(lo or hi for lo, hi in nabs_ax)
     mixed = has_pml and has_abs
     plain_axes = set(absorber_axes) if mixed else ({0, 1, 2} if not has_pml else set())
+    plain_axes |= set(pmc_axes)
     cp = {}
     for ax, kh, ke in ((0, "hx", "ex"), (1, "hy", "ey"), (2, "hz", "ez")):
         n = dims[ax]
@@ -794,7 +797,8 @@ def coeffs_3d(nx, ny, nz, dx, eps=None, npml=0, dtype=np.float64, sigma_d=None,
                 c3[q] = dtype.type(v3) * _avg(m, ax)
                 c1[q], c2[q] = v1, v2
             pols[key] = (c1, c2, c3)
-    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, damp=damp, pols=pols)
+    return dict(dt=dt, dx=dx, dims=dims, dtype=dtype, eps=e, cpml=cp, damp=damp, pols=pols,
+                pmc=tuple(pmc_axes))
 
 
 def state_3d(c):
@@ -818,11 +822,31 @@ def state_3d(c):
         psi_Hy_x=z(nx - 2, ny, nz - 1), psi_Hx_y=z(nx, ny - 2, nz - 1))
 
 
-def _pad_interior(t, axes):
+def _pad_interior(t, axes, pmc=()):
+    """Zero pad of one cell on both sides of each axis in ``axes`` (the PEC edge of the
+    tangential E), skipping PMC axes, whose terms _term_pmc already brought to full
+    length (core/stepper_3d.py:86-96)."""
     pad = [(0, 0)] * 3
     for a in axes:
-        pad[a] = (1, 1)
+        if a not in pmc:
+            pad[a] = (1, 1)
     return np.pad(t, pad)
+
+
+def _term_pmc(t, padaxes, fullax, pmc):
+    """One curl term of an E update (core/stepper_3d.py:99-121): the term that is
+    full-length along ``fullax`` keeps its wall values on a PMC axis and is trimmed to
+    the interior otherwise; a term along a PMC axis is zero-padded to the wall."""
+    sl = [slice(None)] * 3
+    pad = [(0, 0)] * 3
+    for a in padaxes:
+        if a == fullax:
+            if a not in pmc:
+                sl[a] = slice(1, -1)
+        elif a in pmc:
+            pad[a] = (1, 1)
+    t = t[tuple(sl)]
+    return np.pad(t, pad) if any(p != (0, 0) for p in pad) else t
 
 
 def _ce3(c):
@@ -892,19 +916,23 @@ def step_3d_e(s, c, h, amp=0.0, src=None, point_sign=+1.0):
     out = {}
     eps = c["eps"]
     eps_x = _avg(eps, 0)
+    pmc = c.get("pmc", ())
     ch_y, out["psi_Hz_y"] = ce(Hz, 1, "ey", s["psi_Hz_y"])
     ch_z, out["psi_Hy_z"] = ce(Hy, 2, "ez", s["psi_Hy_z"])
-    curl_x = _pad_interior(ch_y[:, :, 1:-1] - ch_z[:, 1:-1, :], (1, 2))
+    curl_x = _pad_interior(_term_pmc(ch_y, (1, 2), 2, pmc) - _term_pmc(ch_z, (1, 2), 1, pmc),
+                           (1, 2), pmc)
     Ex = _e_update(s, c, "x", dm["ex"], eps_x, curl_x, out)
     eps_y = _avg(eps, 1)
     ch_z2, out["psi_Hx_z"] = ce(Hx, 2, "ez", s["psi_Hx_z"])
     ch_x, out["psi_Hz_x"] = ce(Hz, 0, "ex", s["psi_Hz_x"])
-    curl_y = _pad_interior(ch_z2[1:-1, :, :] - ch_x[:, :, 1:-1], (0, 2))
+    curl_y = _pad_interior(_term_pmc(ch_z2, (0, 2), 0, pmc) - _term_pmc(ch_x, (0, 2), 2, pmc),
+                           (0, 2), pmc)
     Ey = _e_update(s, c, "y", dm["ey"], eps_y, curl_y, out)
     eps_z = _avg(eps, 2)
     ch_x2, out["psi_Hy_x"] = ce(Hy, 0, "ex", s["psi_Hy_x"])
     ch_y2, out["psi_Hx_y"] = ce(Hx, 1, "ey", s["psi_Hx_y"])
-    curl_z = _pad_interior(ch_x2[:, 1:-1, :] - ch_y2[1:-1, :, :], (0, 1))
+    curl_z = _pad_interior(_term_pmc(ch_x2, (0, 1), 1, pmc) - _term_pmc(ch_y2, (0, 1), 0, pmc),
+                           (0, 1), pmc)
     Ez = _e_update(s, c, "z", dm["ez"], eps_z, curl_z, out)
     out.update(Ex=Ex, Ey=Ey, Ez=Ez)
     if src is not None and amp != 0.0:

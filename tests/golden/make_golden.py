@@ -22,8 +22,8 @@ cases of the hot path through its own public functions:
   runs (mirrors, Rotate2, Rotate4; ``make_golden.py folds``), chi2 / chi3 runs
   (``make_golden.py nonlinear``), a TM run with magnetic Lorentz poles
   (``make_golden.py mpoles``), a TE run with an in-plane tensor eps
-  (``make_golden.py tensor``) and the 3D matched-sigma absorber, alone and beside CPML
-  (``make_golden.py absorber3d``) and the TM and TE cases with a Lorentz and a Drude pole
+  (``make_golden.py tensor``) and the 3D matched-sigma absorber, alone and beside CPML,
+  and PMC walls (``make_golden.py absorber3d``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -321,11 +321,13 @@ FACES = [("x", 5), ("x", 18), ("y", 5), ("y", 16), ("z", 5), ("z", 14)]
 POLES3 = [(0.5, 0.05, 2.0), (0.0, 0.1, 1.0, 0.8)]     # a Lorentz and a Drude pole
 
 
-def case_3d(prec, lean=False, sigma=False, poles=False, absorber=None):
+def case_3d(prec, lean=False, sigma=False, poles=False, absorber=None, pmc=False):
     rng = np.random.default_rng(13)
     nx, ny, nz, dx, npml = 24, 22, 20, 1.0 / 16, 4
     # matched-sigma absorber on every face (npml 0), or on z beside x / y CPML
     ab = {None: {}, "abs": dict(n_abs=5), "mixed": dict(n_abs=5, absorber_axes=(2,))}[absorber]
+    if pmc:                                           # PMC walls on y beside x / z CPML
+        ab = dict(ab, pmc_axes=(1,))
     if absorber == "abs":
         npml = 0
     eps = np.ones((nx, ny, nz))
@@ -378,9 +380,11 @@ def case_3d(prec, lean=False, sigma=False, poles=False, absorber=None):
                faces=json.dumps(FACES), win=np.array(win))
     if sigma:
         out["sigma_d"], out["sigma_b"] = sd, sb
-    if ab:
+    if "n_abs" in ab:
         out["n_abs"] = ab["n_abs"]
         out["absorber_axes"] = np.array(ab.get("absorber_axes", ()), dtype=np.int64)
+    if pmc:
+        out["pmc_axes"] = np.array(ab["pmc_axes"], dtype=np.int64)
     if poles:
         out["poles"] = json.dumps(POLES3)
         out["pole_masks"] = np.stack(pm3)
@@ -586,6 +590,8 @@ def main():
             for mode in ("abs", "mixed"):
                 np.savez_compressed(os.path.join(HERE, f"golden_3d_{mode}_{prec}.npz"),
                                     **case_3d(prec, absorber=mode))
+            np.savez_compressed(os.path.join(HERE, f"golden_3d_pmc_{prec}.npz"),
+                                **case_3d(prec, pmc=True))
         return
     if sys.argv[1:] == ["tensor"]:
         for prec in ("f64", "f32"):

@@ -132,6 +132,8 @@ def run_3d_oracle(g, prec, lean=False):
     ab = {}
     if "n_abs" in g:
         ab = dict(n_abs=int(g["n_abs"]), absorber_axes=tuple(int(a) for a in g["absorber_axes"]))
+    if "pmc_axes" in g:
+        ab["pmc_axes"] = tuple(int(a) for a in g["pmc_axes"])
     c = O.coeffs_3d(nx, ny, nz, dx, eps=g["eps"], npml=int(g["npml"]), dtype=dt_np,
                     sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"), poles=poles,
                     pole_masks=g.get("pole_masks"), **ab)
@@ -149,12 +151,13 @@ def run_3d_oracle(g, prec, lean=False):
     return c, s, acc
 
 
-@pytest.mark.parametrize("case", ["3d", "3d_sigma", "3d_poles", "3d_abs", "3d_mixed"])
+@pytest.mark.parametrize("case", ["3d", "3d_sigma", "3d_poles", "3d_abs", "3d_mixed",
+                                  "3d_pmc"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_3d_oracle_matches_reference(case, prec):
     """3D cases; 3d_abs runs the matched-sigma absorber on every face (no CPML, so
     the reference state carries no CPML memory), 3d_mixed the absorber on z beside
-    x / y CPML."""
+    x / y CPML, 3d_pmc PMC walls on y beside x / z CPML."""
     g = load_golden(f"{case}_{prec}")
     c, s, acc = run_3d_oracle(g, prec)
     names = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]
