@@ -1012,3 +1012,119 @@ def run_3d(s, c, n_steps, amp_fn=None, src=None, monitors=(), point_sign=+1.0):
             smp = mon(s, t)
             acc[i] = smp if acc[i] is None else acc[i] + smp
     return s, acc
+
+
+# ---------------------------------------------------------------- CW solve (2D TM)
+
+def bicgstab_l(ell, A, b, x, tol=1e-8, maxiters=10000, breaktol=1e-30):
+    """BiCGSTAB(ell) of Sleijpen and Fokkema (ETNA 1, 11-32, 1993), in place on the
+    complex vector ``x``, with the real inner product <p, q> = Re(conj(p) . q) that
+    meep's solver uses (the reference's core/bicgstab.py). Stops when
+    |r| <= tol |b|; returns (ierr, outer iterations): 0 converged, 1 out of
+    iterations, -1 breakdown."""
+    if ell < 1:
+        raise ValueError("ell >= 1")
+
+    def ip(p, q):
+        return float(np.vdot(p, q).real)
+
+    def nrm(p):
+        return float(np.linalg.norm(p))
+    bn = nrm(b) or 1.0
+    r = [np.zeros_like(b) for _ in range(ell + 1)]
+    u = [np.zeros_like(b) for _ in range(ell + 1)]
+    r[0] = b - A(x)
+    n0 = nrm(r[0])
+    if n0 == 0.0:
+        return 0, 0
+    rt = r[0] / n0                                   # shadow residual, normalised
+    rho0, alpha, omega = 1.0, 0.0, 1.0
+    it = 0
+    while nrm(r[0]) > tol * bn:
+        if it >= maxiters:
+            return 1, it
+        it += 1
+        rho0 = -omega * rho0
+        # BiCG part: ell steps, building r_0..r_ell and u_0..u_ell
+        for j in range(ell):
+            if abs(rho0) < breaktol:
+                return -1, it
+            rho1 = ip(r[j], rt)
+            beta = alpha * rho1 / rho0
+            rho0 = rho1
+            for i in range(j + 1):
+                u[i] = r[i] - beta * u[i]
+            u[j + 1] = A(u[j])
+            alpha = rho0 / ip(u[j + 1], rt)
+            for i in range(j + 1):
+                r[i] = r[i] - alpha * u[i + 1]
+            r[j + 1] = A(r[j])
+            x += alpha * u[0]
+        # minimal-residual part: modified Gram-Schmidt on r_1..r_ell
+        tau = np.zeros((ell + 1, ell + 1))
+        sig = np.zeros(ell + 1)
+        gp = np.zeros(ell + 1)
+        for j in range(1, ell + 1):
+            for i in range(1, j):
+                tau[i, j] = ip(r[j], r[i]) / sig[i]
+                r[j] = r[j] - tau[i, j] * r[i]
+            sig[j] = ip(r[j], r[j])
+            gp[j] = ip(r[0], r[j]) / sig[j]
+        g = np.zeros(ell + 1)
+        g[ell] = gp[ell]
+        omega = g[ell]
+        for j in range(ell - 1, 0, -1):
+            g[j] = gp[j] - sum(tau[j, i] * g[i] for i in range(j + 1, ell + 1))
+        gpp = np.zeros(ell + 1)
+        for j in range(1, ell):
+            gpp[j] = g[j + 1] + sum(tau[j, i] * g[i + 1] for i in range(j + 1, ell))
+        x += g[1] * r[0]
+        r[0] = r[0] - gp[ell] * r[ell]
+        u[0] = u[0] - g[ell] * u[ell]
+        for j in range(1, ell):
+            u[0] = u[0] - g[j] * u[j]
+            x += gpp[j] * r[j]
+            r[0] = r[0] - gp[j] * r[j]
+    return 0, it
+
+
+def cw_tm(c, freq):
+    """meep's CW operator on a 2D TM coefficient set (mp/cpp/core.py:721-778):
+    A x = (step(x) - x) / dt + i Omega x, Omega = (1 - exp(-2 pi i f dt)) / i dt, over
+    the unknowns the step carries forward (every state array but Ez, which update_eh
+    re-derives from Dz - sum P after each unpack). Returns (names, pack, unpack, A)."""
+    s0 = tm_state(c)
+    names = tuple(k for k in ("Hx", "Hy", "Dz", "P_cur", "P_prev", "psi_Ezy", "psi_Ezx",
+                              "psi_Hyx", "psi_Hxy", "Hx0", "Hy0") if k in s0)
+    shapes = {k: s0[k].shape for k in names}
+    dt = c["dt"]
+    iomega = (1.0 - np.exp(-2j * np.pi * freq * dt)) / dt
+
+    def pack(re, im):
+        return np.concatenate([re[k].ravel() for k in names]) + \
+            1j * np.concatenate([im[k].ravel() for k in names])
+
+    def unpack(x):
+        re, im, i = dict(tm_state(c)), dict(tm_state(c)), 0
+        for k in names:
+            n = int(np.prod(shapes[k]))
+            re[k] = x[i:i + n].real.reshape(shapes[k]).astype(c["dtype"])
+            im[k] = x[i:i + n].imag.reshape(shapes[k]).astype(c["dtype"])
+            i += n
+        for st in (re, im):
+            st["Ez"] = (st["Dz"] - st["P_cur"].sum(0)) / c["eps"]
+        return re, im
+
+    def A(x):
+        re, im = unpack(x)
+        return (pack(tm_step(re, c), tm_step(im, c)) - x) / dt + iomega * x
+    return names, pack, unpack, A
+
+
+def cw_rhs_tm(c, names, pack, amp, mask):
+    """meep's right-hand side (mp/cpp/core.py:704-719): one step of source current
+    into zero fields, read back and scaled by -1/dt -- amp * mask on Dz."""
+    re, im = dict(tm_state(c)), dict(tm_state(c))
+    re["Dz"] = re["Dz"] - c["dt"] * amp.real * mask
+    im["Dz"] = im["Dz"] - c["dt"] * amp.imag * mask
+    return pack(re, im) * (-1.0 / c["dt"])

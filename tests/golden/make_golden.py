@@ -23,7 +23,8 @@ cases of the hot path through its own public functions:
   (``make_golden.py nonlinear``), a TM run with magnetic Lorentz poles
   (``make_golden.py mpoles``), a TE run with an in-plane tensor eps
   (``make_golden.py tensor``) and the 3D matched-sigma absorber, alone and beside CPML,
-  and PMC walls (``make_golden.py absorber3d``) and the TM and TE cases with a Lorentz and a Drude pole
+  and PMC walls (``make_golden.py absorber3d``), and meep's CW solve on a 2D TM
+  cell (``make_golden.py cw``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -315,6 +316,62 @@ def fold_case(prec, pol, fold):
     return out
 
 
+def cw_case():
+    """meep's CW solve on a small 2D TM cell, assembled from the reference's own parts the
+    way its Simulation.solve_cw does (mp/cpp/core.py:667-778): the unknowns are every
+    state array but Ez, A x = (step(x) - x) / dt + i Omega x with update_eh(E) after each
+    unpack, b = amp * mask on Dz, and its bicgstabL (L = 2). FP64. Also A applied to two
+    seeded random vectors, which pins the operator itself."""
+    from meep_torch.core.bicgstab import bicgstabL
+    from meep_torch.core.stepper_tm import step_tm, update_eh
+    nx, ny, dx, npml, freq = 40, 30, 0.05, 6, 0.6
+    eps = np.ones((nx, ny))
+    eps[:, 12:18] = 6.0
+    g = Grid(nx=nx, ny=ny, dx=dx, dtype=torch.float64, device="cpu")
+    m = build_tm_coeffs(g, eps_inf=torch.tensor(eps), npml=npml)
+    st0 = init_tm_state(g)
+    names = tuple(n for n in st0._fields if n != "Ez" and getattr(st0, n) is not None)
+    shapes = tuple(tuple(getattr(st0, n).shape) for n in names)
+    dt = m.dt
+    iomega = complex((1.0 - np.exp(-2j * np.pi * freq * dt)) / dt)
+
+    def pack(re, im):
+        return (torch.cat([getattr(re, n).reshape(-1) for n in names])
+                + 1j * torch.cat([getattr(im, n).reshape(-1) for n in names]))
+
+    def unpack(x):
+        out_re, out_im, i = {}, {}, 0
+        for n, sh in zip(names, shapes):
+            k = int(np.prod(sh))
+            out_re[n] = x[i:i + k].real.reshape(sh).contiguous()
+            out_im[n] = x[i:i + k].imag.reshape(sh).contiguous()
+            i += k
+        return (update_eh(st0._replace(**out_re), m, "E"),
+                update_eh(st0._replace(**out_im), m, "E"))
+
+    def A(x):
+        re, im = unpack(x)
+        return (pack(step_tm(re, m), step_tm(im, m)) - x) / dt + iomega * x
+
+    src = LineSource(g, ix=10, j0=13, j1=17, profile=GaussianPulse(freq, 0.2))
+    mask = src.mask
+    b = pack(st0._replace(Dz=mask.clone()), st0._replace(Dz=torch.zeros_like(mask)))
+    x = torch.zeros_like(b)
+    ierr, iters = bicgstabL(2, A, b, x, tol=1e-8, maxiters=5000)
+    rng = np.random.default_rng(41)
+    n = b.numel()
+    vs = [torch.tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n)) for _ in range(2)]
+    re, im = unpack(x)
+    out = dict(nx=nx, ny=ny, dx=dx, npml=npml, eps=eps, freq=freq, src_ix=10, src_j0=13,
+               src_j1=17, mask=_np(mask), ierr=ierr, iters=iters, names=json.dumps(names),
+               b=b.numpy(), v0=vs[0].numpy(), v1=vs[1].numpy(), Av0=A(vs[0]).numpy(),
+               Av1=A(vs[1]).numpy())
+    for k in names:
+        out["re_" + k], out["im_" + k] = _np(getattr(re, k)), _np(getattr(im, k))
+    out["re_Ez"], out["im_Ez"] = _np(re.Ez), _np(im.Ez)
+    return out
+
+
 FACES = [("x", 5), ("x", 18), ("y", 5), ("y", 16), ("z", 5), ("z", 14)]
 
 
@@ -584,6 +641,9 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["cw"]:
+        np.savez_compressed(os.path.join(HERE, "golden_cw_tm_f64.npz"), **cw_case())
         return
     if sys.argv[1:] == ["absorber3d"]:
         for prec in ("f64", "f32"):

@@ -330,3 +330,32 @@ def test_fold_oracle_matches_reference(pol, name, prec):
         assert s[k].shape == g["s_" + k].shape, k
         assert rel_l2(s[k], g["s_" + k]) < TOL[prec], k
     assert rel_l2(acc, g["acc_dft"]) < TOL[prec]
+
+
+def test_cw_operator_and_solve_match_reference():
+    """meep's CW solve on a 2D TM cell: the oracle's operator A x = (step(x) - x)/dt +
+    i Omega x matches the reference's on seeded random vectors (FP64 rounding), its
+    right-hand side matches, and its BiCGSTAB(2) reaches the reference's solution
+    (both stop at |r| <= 1e-8 |b|) in about the same number of iterations."""
+    g = load_golden("cw_tm_f64")
+    nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
+    c = O.tm_coeffs(nx, ny, dx, eps=g["eps"], npml=int(g["npml"]), dtype=np.float64)
+    names, pack, unpack, A = O.cw_tm(c, float(g["freq"]))
+    assert list(names) == json.loads(str(g["names"]))
+    def crel(a, r):                                  # complex relative L2
+        return float(np.linalg.norm(np.asarray(a) - r) / np.linalg.norm(r))
+    for v, av in (("v0", "Av0"), ("v1", "Av1")):
+        assert crel(A(g[v]), g[av]) < 1e-12, v
+    mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]), int(g["src_j1"]))
+    np.testing.assert_allclose(mask, g["mask"], rtol=1e-12)
+    b = O.cw_rhs_tm(c, names, pack, 1.0 + 0.0j, mask)
+    assert crel(b, g["b"]) < 1e-14
+    x = np.zeros_like(b)
+    ierr, it = O.bicgstab_l(2, A, b, x, tol=1e-8, maxiters=5000)
+    assert ierr == 0 and abs(it - int(g["iters"])) <= max(5, int(g["iters"]) // 10)
+    assert float(np.linalg.norm(A(x) - b)) <= 1e-8 * float(np.linalg.norm(b)) * 1.01
+    re, im = unpack(x)
+    for k in list(names) + ["Ez"]:
+        if re[k].size:
+            assert rel_l2(re[k], g["re_" + k]) < 1e-6, k
+            assert rel_l2(im[k], g["im_" + k]) < 1e-6, k
