@@ -26,6 +26,18 @@ def _line(*args):
 def test_reference_arm_line(args, unit):
     d = _line(*args, "--steps", "1", "--warmup", "0")
     assert d["impl"] == "reference" and d["unit"] == unit and d["metric"] == unit
+    _common(d, unit)
+
+
+def test_reference_arm_cfg5_line():
+    """cfg5's reference arm: one full oracle run of a cfg5 design on the host, a plain
+    design iteration costed as two, in the surrogate metric's unit and name."""
+    d = _line("--workload", "cfg5", "--steps", "1", "--warmup", "0")
+    assert d["unit"] == "design-iterations/s" and d["metric"].startswith("design-iterations/s")
+    _common(d, "design-iterations/s")
+
+
+def _common(d, unit):
     assert d["value"] > 0 and d["higher_is_better"] is True
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": unit, "h2d_bytes_per_step": 0,
