@@ -43,7 +43,8 @@ import sys
 import numpy as np
 
 sys.dont_write_bytecode = True
-REF = os.environ.get("MEEP_TORCH_REF", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from reference_path import REF  # noqa: E402
 sys.path.insert(0, REF)
 
 import torch  # noqa: E402

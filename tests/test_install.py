@@ -96,8 +96,6 @@ def test_routing_and_fallback_rules(fake_pkg):
 
 
 def test_cuda_f32_predicate():
-    class T:
-        pass
     assert not I.cuda_f32(((torch.zeros(2), 1),), {})
     assert not I.cuda_f32((None, 3), {})
     if torch.cuda.is_available():
@@ -106,7 +104,7 @@ def test_cuda_f32_predicate():
 
 
 def test_install_on_the_reference_package():
-    ref = os.environ.get("MEEP_TORCH_REF", "/root/reference")
+    from tests.golden.reference_path import REF as ref
     if not os.path.isdir(os.path.join(ref, "meep_torch")):
         pytest.skip("reference checkout not present")
     sys.path.insert(0, ref)
