@@ -24,6 +24,18 @@ def test_grf_designs_seeded_and_bounded():
     assert not torch.equal(S.grf_designs(2, seed=1), S.grf_designs(2, seed=2))
 
 
+def test_grf_soft_half_is_grey():
+    """With soft = 0.5 the second half of the maps is soft-thresholded: far more grey
+    pixels (0.2 < rho < 0.8) than the thresholded half, whose grey pixels are only the
+    filtered edges; the first half equals the all-binary maps of the same seed."""
+    hard = S.grf_designs(16, seed=4)
+    mixed = S.grf_designs(16, seed=4, soft=0.5)
+    assert torch.equal(mixed[:8], hard[:8])
+    grey = lambda r: float(((r > 0.2) & (r < 0.8)).float().mean())  # noqa: E731
+    assert grey(mixed[8:]) > 2.0 * grey(mixed[:8])
+    assert float(mixed.min()) >= 0.0 and float(mixed.max()) <= 1.0
+
+
 def test_problem_geometry_cpu():
     p = S.Cfg5Problem("cpu")
     rho = torch.zeros(2, 64, 64)
