@@ -24,7 +24,8 @@ cases of the hot path through its own public functions:
   (``make_golden.py mpoles``), a TE run with an in-plane tensor eps
   (``make_golden.py tensor``) and the 3D matched-sigma absorber, alone and beside CPML,
   and PMC walls (``make_golden.py absorber3d``), and meep's CW solve on a 2D TM
-  cell (``make_golden.py cw``) and the TM and TE cases with a Lorentz and a Drude pole
+  cell (``make_golden.py cw``), and the lean 3D stepper with poles
+  (``make_golden.py lean_poles``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -403,7 +404,13 @@ def case_3d(prec, lean=False, sigma=False, poles=False, absorber=None, pmc=False
     n = 120
     src_ijk = (12, 11, 10)
     if lean:
-        c = build_lean(nx, ny, nz, dx, epst, npml, dtype=DT[prec], device="cpu")
+        lk = {}
+        if poles:                                     # the same pole masks as the functional case
+            pm3 = [np.zeros((nx, ny, nz)), np.zeros((nx, ny, nz))]
+            pm3[0][8:16, 6:14, 6:14] = 1.0
+            pm3[1][14:19, 12:17, 9:15] = 1.0
+            lk = dict(poles=POLES3, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm3])
+        c = build_lean(nx, ny, nz, dx, epst, npml, dtype=DT[prec], device="cpu", **lk)
         src = PointSource3D(c.dt, "Ez", *src_ijk, prof)
         mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=i, win=win, dtype=DT[prec])
                 for a, i in FACES]
@@ -642,6 +649,11 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["lean_poles"]:
+        for prec in ("f64", "f32"):
+            np.savez_compressed(os.path.join(HERE, f"golden_3d_lean_poles_{prec}.npz"),
+                                **case_3d(prec, lean=True, poles=True))
         return
     if sys.argv[1:] == ["cw"]:
         np.savez_compressed(os.path.join(HERE, "golden_cw_tm_f64.npz"), **cw_case())

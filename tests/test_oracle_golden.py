@@ -170,11 +170,13 @@ def test_3d_oracle_matches_reference(case, prec):
         assert rel_l2(O.flux3d(a, float(g["dx"])), g[f"flux_{n}"]) < TOL[prec]
 
 
+@pytest.mark.parametrize("case", ["3d_lean", "3d_lean_poles"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_3d_lean_sign_convention(prec):
+def test_3d_lean_sign_convention(case, prec):
     """The lean stepper subtracts the point current and multiplies by 1/eps;
-    the oracle's point_sign=-1 reproduces it to the rounding of that form."""
-    g = load_golden(f"3d_lean_{prec}")
+    the oracle's point_sign=-1 reproduces it to the rounding of that form. With
+    poles the lean stepper's folded-D update is the functional stepper's."""
+    g = load_golden(f"{case}_{prec}")
     c, s, acc = run_3d_oracle(g, prec, lean=True)
     tol = 1e-9 if prec == "f64" else 1e-4
     for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
