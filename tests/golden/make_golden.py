@@ -24,8 +24,9 @@ cases of the hot path through its own public functions:
   (``make_golden.py mpoles``), a TE run with an in-plane tensor eps
   (``make_golden.py tensor``) and the 3D matched-sigma absorber, alone and beside CPML,
   and PMC walls (``make_golden.py absorber3d``), and meep's CW solve on a 2D TM
-  cell (``make_golden.py cw``), and the lean 3D stepper with poles
-  (``make_golden.py lean_poles``) and the TM and TE cases with a Lorentz and a Drude pole
+  cell (``make_golden.py cw``), the lean 3D stepper with poles
+  (``make_golden.py lean_poles``), and the TM gradient of lossy and dispersive runs
+  (``make_golden.py grad_extra``) and the TM and TE cases with a Lorentz and a Drude pole
   (``make_golden.py poles``); the 3D cases with sigma_d and sigma_b
   (``make_golden.py sigma3d``) and with poles (``make_golden.py poles3d``)
 
@@ -483,9 +484,10 @@ def grad_loss(st, ax, ay, ad, mx, my, dx):
             + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
 
 
-def grad_tm_case(prec):
+def grad_tm_case(prec, extra=None):
     """d J / d eps through the reference's autograd (run_tm with
-    checkpoint_every, core/run.py:81-120) on the TM case's geometry."""
+    checkpoint_every, core/run.py:81-120) on the TM case's geometry; ``extra`` =
+    "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole."""
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -494,21 +496,33 @@ def grad_tm_case(prec):
     eps[30:38, 20:30] = 1.0 + 4.0 * rng.random((8, 10))       # a pixelated design patch
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
     e = torch.tensor(eps, dtype=DT[prec], requires_grad=True)
-    m = build_tm_coeffs(g, eps_inf=e, npml=npml)
+    kw, out_extra = {}, {}
+    if extra == "lossy":
+        sd = sigma_map(nx, ny, 21)
+        sbm, mum = magnetic_maps(nx, ny, 23)
+        kw = dict(sigma_d=torch.tensor(sd, dtype=DT[prec]), sigma_b=torch.tensor(sbm, dtype=DT[prec]),
+                  mu=torch.tensor(mum, dtype=DT[prec]))
+        out_extra = dict(sigma=sd, sigma_b=sbm, mu=mum)
+    elif extra == "poles":
+        pm = pole_masks(nx, ny)
+        kw = dict(poles=POLES, pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
+        out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
+    m = build_tm_coeffs(g, eps_inf=e, npml=npml, **kw)
     src = LineSource(g, ix=12, j0=10, j1=26, profile=GaussianPulse(0.65, 0.4))
     freqs = [0.55, 0.65, 0.75]
     monx = FluxMonitorTM(g, freqs, x_normal=True, idx=36, lo=9, hi=27)
     mony = FluxMonitorTM(g, freqs, x_normal=False, idx=26, lo=10, hi=38)
     dft = DFTFieldsMonitor(g, freqs, component="Ez")
     n, ce = 200, 50
-    st, (ax, ay, ad) = run_tm(init_tm_state(g), m, n, source=src, monitors=[monx, mony, dft],
+    s0 = init_tm_state(g, n_poles=len(POLES) if extra == "poles" else 0)
+    st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft],
                               checkpoint_every=ce)
     J = grad_loss(st, ax, ay, ad, monx, mony, dx)
     J.backward()
     return dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, checkpoint_every=ce, eps=eps,
                 freqs=np.array(freqs), fcen=0.65, fwidth=0.4, src_ix=12, src_j0=10, src_j1=26,
                 monx=np.array([36, 9, 27]), mony=np.array([26, 10, 38]),
-                J=float(J.detach()), grad=_np(e.grad))
+                J=float(J.detach()), grad=_np(e.grad), **out_extra)
 
 
 def design_case():
@@ -649,6 +663,11 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["grad_extra"]:
+        for extra in ("lossy", "poles"):
+            np.savez_compressed(os.path.join(HERE, f"golden_grad_tm_{extra}_f64.npz"),
+                                **grad_tm_case("f64", extra))
         return
     if sys.argv[1:] == ["lean_poles"]:
         for prec in ("f64", "f32"):

@@ -185,10 +185,16 @@ def test_3d_lean_sign_convention(case, prec):
         assert rel_l2(a, g[f"acc_{n}"]) < tol
 
 
-def test_reference_gradient_matches_oracle_finite_differences():
+@pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles"])
+def test_reference_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps (reference autograd, float64) against central
-    finite differences of the oracle's float64 run at a few pixels."""
-    g = load_golden("grad_tm_f64")
+    finite differences of the oracle's float64 run at a few pixels; the lossy case
+    adds sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole (the
+    gradients a future adjoint of those runs must reproduce)."""
+    g = load_golden(f"{case}_f64")
+    extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"))
+    if "poles" in g:
+        extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
                            int(g["n_steps"]))
     freqs = [float(f) for f in g["freqs"]]
@@ -196,7 +202,7 @@ def test_reference_gradient_matches_oracle_finite_differences():
     myi, myl, myh = (int(v) for v in g["mony"])
 
     def J_of(eps):
-        c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float64)
+        c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float64, **extra)
         dt = c["dt"]
         mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                                   int(g["src_j1"]), dtype=np.float64)
