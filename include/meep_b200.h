@@ -266,10 +266,18 @@ int32_t mtb_yee2d_pole_slot(const mtb_yee2d_plan *plan);
  * the ping-pong buffer holding the current state; after the call the state is
  * in buffer parity ^ (k & 1). The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) and sets kernel attributes, so make
- * it before any stream capture. Every call shares the one array: calls whose
- * work overlaps on the GPU (other streams, other host threads) race and must
- * be serialised by the caller. The call waits for its work on `stream`
- * before returning (it reads back the bounded-wait error flag). */
+ * it before any stream capture; that set-up is guarded by a lock, so host
+ * threads may make first calls concurrently. The cached address belongs to
+ * the device's primary context: after cudaDeviceReset the entry point must
+ * not be called on that device again (unsupported). Every call shares the
+ * one array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.
+ * Before any step kernel runs, the call checks on the device each source
+ * list's row_ptr (starts at 0, ends at n, never decreases), the column order
+ * within each row and the line samples, and waits for that verdict on
+ * `stream`: a rejected call (MTB_INVALID_ARG) leaves the caller's fields,
+ * CPML memory and accumulators untouched. The call also waits for its work
+ * on `stream` before returning (it reads back the bounded-wait error flag). */
 #define MTB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_region *regions,
                           int32_t n_regions, const mtb_phase_group *groups,

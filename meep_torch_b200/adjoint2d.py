@@ -5,11 +5,13 @@ optionally checkpointed (``checkpoint_every``). Here the same derivative comes f
 library's discrete-adjoint kernels (``mtb_yee2d_adjoint_*``): the exact transpose of the
 forward TM step with CPML and of the DFT / flux sampling, run backwards in time.
 
-Forward: the run goes in chunks of ``chunk`` steps (the ring depth); the live state at each
-chunk start is kept (box layout). Backward, chunk by chunk from the last: the chunk is
-re-run from its snapshot on a recording plan whose ring keeps the full-grid E of every step
-(Ez for TM, Ex and Ey for TE: needed for d/d eps of E = D / eps), then the adjoint plan
-sweeps the chunk's steps in reverse. Gradients reach ``coeffs.eps_inf`` (TM) or
+Forward: the run goes in chunks of ``chunk`` steps (the checkpoint interval); the live
+state at each chunk start is kept (box layout). Backward, chunk by chunk from the last: the
+chunk is re-run from its snapshot on a recording plan whose ring keeps the full-grid E of
+every step (Ez for TM, Ex and Ey for TE: needed for d/d eps of E = D / eps), then the
+adjoint plan sweeps the chunk's steps in reverse. The ring holds at most 64 steps, so a
+longer chunk is walked forward once keeping the state at the start of each 64-step
+sub-chunk, and the sub-chunks are then recorded and reversed from the last. Gradients reach ``coeffs.eps_inf`` (TM) or
 ``coeffs.eps_x`` / ``coeffs.eps_y`` (TE, and through them ``eps_inf``); other coefficient
 tensors and the initial state receive none (a gradient request for them raises
 NotImplementedError).
@@ -52,13 +54,14 @@ class GradRun2D:
         self.names = STATE_TE if self.te else STATE_TM
         self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
         self.source, self.monitors = source, list(monitors)
-        self.chunk = max(1, min(int(chunk), 64))
+        self.chunk = max(1, int(chunk))
+        self.sub = min(self.chunk, 64)                    # recording ring depth
         self.phase_mode = phase_mode
         self.chunks = [(s0, min(self.chunk, self.n - s0)) for s0 in range(0, self.n, self.chunk)]
 
     def forward(self):
         eng = Engine2D([(self.state0, self.coeffs, self.source, self.monitors)],
-                       phase_mode=self.phase_mode, ring_slots=self.chunk, graph=False)
+                       phase_mode=self.phase_mode, ring_slots=self.sub, graph=False)
         self.snaps = []
         for s0, k in self.chunks:
             self.snaps.append(eng.snapshot(0))
@@ -114,7 +117,7 @@ class GradRun2D:
         adj = C.c_void_p()
         L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
                                              regs if nreg else None, nreg, eng.groups,
-                                             eng.n_groups, eng.ring_elems, self.chunk,
+                                             eng.n_groups, eng.ring_elems, self.sub,
                                              C.byref(adj)), "mtb_yee2d_adjoint_create")
         keep = [gaccs, g, gpsi, tmp, geps]
         stream = eng._sptr()
@@ -123,29 +126,49 @@ class GradRun2D:
             zero = type(self.state0)(*[torch.zeros_like(t) if torch.is_tensor(t) else t
                                        for t in self.state0])
             rec = None
+
+            def from_state0():      # the initial state as imported (explicit Ez honoured)
+                nonlocal rec
+                if rec is not None:
+                    rec.close()
+                rec = Engine2D([(self.state0, self.coeffs, self.source, rec_mons)],
+                               phase_mode=self.phase_mode, ring_slots=self.sub, graph=False)
+
+            def restored(snap):
+                nonlocal rec
+                if rec is None:
+                    rec = Engine2D([(zero, self.coeffs, self.source, rec_mons)],
+                                   phase_mode=self.phase_mode, ring_slots=self.sub,
+                                   graph=False)
+                rec.restore(0, snap)
+
             for c in range(len(self.chunks) - 1, -1, -1):
                 s0, k = self.chunks[c]
-                if c == 0:       # the initial state as imported (explicit Ez honoured)
-                    if rec is not None:
-                        rec.close()
-                    rec = Engine2D([(self.state0, self.coeffs, self.source, rec_mons)],
-                                   phase_mode=self.phase_mode, ring_slots=self.chunk,
-                                   graph=False)
-                else:
-                    if rec is None:
-                        rec = Engine2D([(zero, self.coeffs, self.source, rec_mons)],
-                                       phase_mode=self.phase_mode, ring_slots=self.chunk,
-                                       graph=False)
-                    rec.restore(0, self.snaps[c])
-                rec.run(s0, k)
-                ring, selems, nslots = C.c_void_p(), C.c_int64(), C.c_int32()
-                L.check(lib.mtb_yee2d_ring(rec.plan, C.byref(ring), C.byref(selems),
-                                           C.byref(nslots)), "mtb_yee2d_ring")
-                rf = rec.structs[0].ring_full
-                offs2 = (C.c_int64 * 2)(*((int(rf[1]), int(rf[2])) if self.te
-                                          else (int(rf[0]), int(rf[0]))))
-                L.check(lib.mtb_yee2d_adjoint_run(adj, s0, k, ring, selems.value, offs2,
-                                                  stream), "mtb_yee2d_adjoint_run")
+                subs = [(s0 + o, min(self.sub, k - o)) for o in range(0, k, self.sub)]
+                starts = [self.snaps[c]] + [None] * (len(subs) - 1)
+                if len(subs) > 1:         # keep each sub-chunk's starting state
+                    if c == 0:
+                        from_state0()
+                    else:
+                        restored(self.snaps[c])
+                    for q, (u0, uk) in enumerate(subs[:-1]):
+                        rec.run(u0, uk)
+                        starts[q + 1] = rec.snapshot(0)
+                for q in range(len(subs) - 1, -1, -1):
+                    u0, uk = subs[q]
+                    if c == 0 and q == 0:
+                        from_state0()
+                    else:
+                        restored(starts[q])
+                    rec.run(u0, uk)
+                    ring, selems, nslots = C.c_void_p(), C.c_int64(), C.c_int32()
+                    L.check(lib.mtb_yee2d_ring(rec.plan, C.byref(ring), C.byref(selems),
+                                               C.byref(nslots)), "mtb_yee2d_ring")
+                    rf = rec.structs[0].ring_full
+                    offs2 = (C.c_int64 * 2)(*((int(rf[1]), int(rf[2])) if self.te
+                                              else (int(rf[0]), int(rf[0]))))
+                    L.check(lib.mtb_yee2d_adjoint_run(adj, u0, uk, ring, selems.value, offs2,
+                                                      stream), "mtb_yee2d_adjoint_run")
             if rec is not None:
                 rec.close()
         finally:
@@ -196,7 +219,7 @@ def run_grad(state, coeffs, n_steps, *, source=None, monitors=(), checkpoint_eve
     for t in state:
         if torch.is_tensor(t) and t.requires_grad:
             raise L.MtbUnsupported("gradients with respect to the initial state on the B200 path")
-    chunk = checkpoint_every if 0 < checkpoint_every <= 64 else 32
+    chunk = checkpoint_every if checkpoint_every > 0 else 32
     runner = GradRun2D(state, coeffs, n_steps, source, monitors, chunk, phase_mode)
     outs = _RunFn2D.apply(runner, *[getattr(coeffs, f) for f in eps_names])
     ns = len(runner.names)

@@ -31,7 +31,7 @@ def _make_runner(kind):
         coeffs.eps_inf; TE coeffs.eps_x / eps_y, e.g. built from an eps_inf that
         requires grad) and grad mode is on, the run is differentiable through the
         library's adjoint kernels, checkpointed every ``checkpoint_every`` steps
-        (<= 64; the default 32); otherwise checkpoint_every has no effect."""
+        (the default 32); otherwise checkpoint_every has no effect."""
         monitors = list(monitors)
         if n_steps <= 0:
             return state, [None] * len(monitors)

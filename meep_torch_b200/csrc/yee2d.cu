@@ -24,6 +24,7 @@
 // active (a != 0 or b != 1); outside the layers it is identically zero, as in
 // the reference.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "mtb_common.cuh"
@@ -2427,17 +2428,47 @@ constexpr int NA_MAX_REGIONS = 64;
 constexpr int NA_MAX_GROUPS = 16;
 constexpr int NA_CT = 256;              // contraction block size (common.cu)
 constexpr int NA_ERR_COLS = 1 << 30;    // error-flag bit: source columns out of order
-static unsigned char *g_noalloc_dev[NA_MAX_DEV];   // device address of the array, per device
+constexpr int NA_ERR_ROWS = 1 << 29;    // error-flag bit: a source row_ptr is malformed
+constexpr int NA_ERR_LINES = 1 << 28;   // error-flag bit: a line sample is out of range
+// device address of the array, per device, filled once under g_noalloc_mu
+static unsigned char *g_noalloc_dev[NA_MAX_DEV];
+static std::mutex g_noalloc_mu;
 
-// x-layer bands and source row ranges of the descriptor copy (what
-// mtb_yee2d_plan_create computes on the host)
-__global__ void k_na_struct(mtb_yee2d_struct *S, int *err) {
-    __shared__ int lh, hh, le, he, rlo[3], rhi[3];
+// Checks and derived fields of the descriptor copy (what mtb_yee2d_plan_create
+// computes on the host): each source list's row pointer (rp[0] == 0,
+// rp[nx] == n, non-decreasing) before any of its columns is read, the column
+// order within a row, the line samples against the ring slot, the x-layer
+// bands and the source row ranges. Failures set bits of *err; the host reads
+// them back before any step kernel runs.
+__global__ void k_na_struct(mtb_yee2d_struct *S, int *err, int64_t ring_slot_elems) {
+    __shared__ int lh, hh, le, he, rlo[3], rhi[3], bad[3];
     const int nx = S->nx;
     const int nh = nx - 1, ne = nx;
+    const mtb_cells *cl[3] = {&S->src_e, &S->src_h1, &S->src_h2};
     if (threadIdx.x == 0) {
         lh = 0; hh = nh; le = 0; he = ne;
-        for (int c = 0; c < 3; ++c) { rlo[c] = 0x7fffffff; rhi[c] = -1; }
+        for (int c = 0; c < 3; ++c) {
+            rlo[c] = 0x7fffffff; rhi[c] = -1;
+            const int n = cl[c]->n;
+            bad[c] = n > 0 && (cl[c]->row_ptr[0] != 0 || cl[c]->row_ptr[nx] != n);
+        }
+    }
+    __syncthreads();
+    for (int c = 0; c < 3; ++c) {
+        const int n = cl[c]->n;
+        if (n <= 0) continue;
+        for (int r = threadIdx.x; r < nx; r += blockDim.x) {
+            const int e0 = cl[c]->row_ptr[r], e1 = cl[c]->row_ptr[r + 1];
+            if (e0 < 0 || e1 < e0 || e1 > n) atomicOr(&bad[c], 1);
+        }
+    }
+    for (int l = threadIdx.x; l < S->n_lines; l += blockDim.x) {
+        const mtb_line_sample q = S->lines[l];
+        const int along = q.kind == 0 ? S->ny : S->nx, across = q.kind == 0 ? S->nx : S->ny;
+        if (q.comp < 0 || q.comp > 2 || (q.kind != 0 && q.kind != 1) || q.index < 0 ||
+            q.index >= across || q.lo < 0 || q.hi > along || q.lo >= q.hi || q.ring_off < 0 ||
+            q.ring_off + (q.hi - q.lo) > ring_slot_elems)
+            atomicOr(err, NA_ERR_LINES);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < ne; i += blockDim.x) {
@@ -2448,9 +2479,12 @@ __global__ void k_na_struct(mtb_yee2d_struct *S, int *err) {
             if (i < ne / 2) atomicMax(&le, i + 1); else atomicMin(&he, i);
         }
     }
-    const mtb_cells *cl[3] = {&S->src_e, &S->src_h1, &S->src_h2};
     for (int c = 0; c < 3; ++c) {
         if (cl[c]->n <= 0) continue;
+        if (bad[c]) {                      // columns are only read through a valid row_ptr
+            if (threadIdx.x == 0) atomicOr(err, NA_ERR_ROWS);
+            continue;
+        }
         for (int r = threadIdx.x; r < nx; r += blockDim.x) {
             const int e0 = cl[c]->row_ptr[r], e1 = cl[c]->row_ptr[r + 1];
             if (e1 > e0) {
@@ -2590,21 +2624,6 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
         if (o >= 0 && ((o & 3) || o + (int64_t)S.nx * S.pitch > ring_slot_elems))
             return fail(MTB_INVALID_ARG, "noalloc: full-grid ring offset invalid");
     }
-    if (S.n_lines > 0) {
-        mtb_line_sample ls[MAXL];
-        cudaError_t e = cudaMemcpy(ls, S.lines, sizeof(mtb_line_sample) * S.n_lines,
-                                   cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess)
-            return fail(MTB_CUDA_ERROR, "noalloc: reading line samples: %s", cudaGetErrorString(e));
-        for (int l = 0; l < S.n_lines; ++l) {
-            const mtb_line_sample &q = ls[l];
-            const int along = q.kind == 0 ? S.ny : S.nx, across = q.kind == 0 ? S.nx : S.ny;
-            if (q.comp < 0 || q.comp > 2 || (q.kind != 0 && q.kind != 1) || q.index < 0 ||
-                q.index >= across || q.lo < 0 || q.hi > along || q.lo >= q.hi || q.ring_off < 0 ||
-                q.ring_off + (q.hi - q.lo) > ring_slot_elems)
-                return fail(MTB_INVALID_ARG, "noalloc: line sample %d out of range", l);
-        }
-    }
     if (n_regions < 0 || n_regions > NA_MAX_REGIONS || n_groups < 0 || n_groups > NA_MAX_GROUPS ||
         (n_regions > 0 && (!regions || !groups)))
         return fail(MTB_INVALID_ARG, "noalloc: at most %d regions and %d phase groups",
@@ -2667,6 +2686,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     int dev = 0;
     MTB_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NA_MAX_DEV) return fail(MTB_UNSUPPORTED, "noalloc: device ordinal %d", dev);
+    std::unique_lock<std::mutex> setup_lock(g_noalloc_mu);
     if (!g_noalloc_dev[dev]) {
         void *p = nullptr;
         MTB_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -2684,6 +2704,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
         g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
     }
     unsigned char *base = g_noalloc_dev[dev];
+    setup_lock.unlock();
     size_t off = 0;
     auto take = [&](size_t bytes) { unsigned char *q = base + off; off += na_align(bytes); return q; };
     mtb_yee2d_struct *dS = reinterpret_cast<mtb_yee2d_struct *>(take(sizeof(mtb_yee2d_struct)));
@@ -2725,8 +2746,20 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
             MTB_CUDA_TRY(cudaMemcpyAsync(dFreq + goff[g], groups[g].freqs,
                                          sizeof(double) * gnf[g], cudaMemcpyHostToDevice, st));
     }
-    k_na_struct<<<1, 256, 0, st>>>(dS, dErr);
+    k_na_struct<<<1, 256, 0, st>>>(dS, dErr, ring_slot_elems);
     MTB_CHECK_LAUNCH();
+    // the checks' verdict before any step kernel: a rejected call leaves the
+    // caller's fields, CPML memory and accumulators untouched
+    int flag = 0;
+    MTB_CUDA_TRY(cudaMemcpyAsync(&flag, dErr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MTB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (flag & NA_ERR_ROWS)
+        return fail(MTB_INVALID_ARG, "noalloc: a source row_ptr does not start at 0, end at n "
+                    "and never decrease");
+    if (flag & NA_ERR_LINES) return fail(MTB_INVALID_ARG, "noalloc: a line sample is out of range");
+    if (flag & NA_ERR_COLS)
+        return fail(MTB_INVALID_ARG, "noalloc: source columns are not in ascending order within "
+                    "a row");
     k_na_work<<<(n_work + 255) / 256, 256, 0, st>>>(dWork, S.nx, rows, nch, n_work);
     MTB_CHECK_LAUNCH();
     if (n_blocks > 0) {
@@ -2788,12 +2821,8 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
             }
         }
     }
-    int flag = 0;
     MTB_CUDA_TRY(cudaMemcpyAsync(&flag, dErr, sizeof(int), cudaMemcpyDeviceToHost, st));
     MTB_CUDA_TRY(cudaStreamSynchronize(st));
-    if (flag & NA_ERR_COLS)
-        return fail(MTB_INVALID_ARG, "noalloc: source columns are not in ascending order within "
-                    "a row");
     if (flag)
         return fail(MTB_DEVICE_TIMEOUT, "noalloc: a bounded wait for a staged row copy expired");
     return MTB_OK;

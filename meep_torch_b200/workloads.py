@@ -212,7 +212,7 @@ def cfg4_setup(device, seed: int = 4, steps: int = None):
     def run_fn(eps):
         m = build_tm_coeffs(grid, eps_inf=eps, npml=npml)
         _, (acc,) = run_tm(init_tm_state(grid), m, n, source=src, monitors=[mon],
-                           checkpoint_every=32)
+                           checkpoint_every=256)
         return mon.flux(acc, dx).mean()
 
     rho0 = torch.tensor(rng.uniform(0.4, 0.6, (d, d)), dtype=torch.float32, device=device)

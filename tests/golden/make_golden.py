@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder by running the REFERENCE itself.
 
-Imports meep_torch from the reference checkout (``MEEP_TORCH_REF``, default
-``/root/reference``; read-only, no bytecode written) and runs small seeded
+Imports meep_torch from the reference checkout named by ``MEEP_TORCH_REF`` (read-only,
+no bytecode written) and runs small seeded
 cases of the hot path through its own public functions:
 
 * ``Grid`` / ``build_tm_coeffs`` / ``LineSource`` / ``FluxMonitorTM`` /
@@ -46,8 +46,8 @@ import numpy as np
 
 sys.dont_write_bytecode = True
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from reference_path import REF  # noqa: E402
-sys.path.insert(0, REF)
+from reference_path import reference_root  # noqa: E402
+sys.path.insert(0, reference_root())
 
 import torch  # noqa: E402
 

@@ -6,9 +6,14 @@ cudaMalloc's device synchronisation. For them, mtb_yee2d_run_noalloc runs one
 2D structure with all of its scratch in one fixed-size device array. This
 test drives it through the C ABI on the same inputs as mtb_yee2d_plan_create
 + mtb_yee2d_run, for two calls in a row (the second continuing the first,
-with the time index and ping-pong buffer carried over), and compares fields
-and DFT/flux accumulators within the parity tolerance used elsewhere (1e-4
-relative L2). The file is named so pytest collects it last.
+with the time index and ping-pong buffer carried over; the second call is
+longer than the entry point's 256-step table chunk, so a chunk boundary is
+crossed), and compares fields and DFT/flux accumulators within the parity
+tolerance used elsewhere (1e-4 relative L2). It also checks the property the
+entry point exists for: once the library is loaded and the first call has
+done its one-time set-up, a call leaves the device's free memory unchanged.
+Calls the entry point rejects leave the caller's arrays untouched. The file is
+named so pytest collects it last.
 """
 import ctypes as C
 
@@ -84,7 +89,7 @@ def test_noalloc_matches_plan_two_calls(pol):
     stream = torch.cuda.current_stream().cuda_stream
     parity = 0
     t0 = 0
-    for k in (70, 53):                                    # two calls in a row
+    for k in (70, 300):                                   # two calls in a row
         ref.run(t0, k)
         ce, ch = _coefs(new, t0, k)
         pe = ce.ctypes.data_as(C.POINTER(C.c_double)) if ce is not None else None
@@ -124,6 +129,82 @@ def test_noalloc_matches_plan_two_calls(pol):
     new.close()
 
 
+def _snapshot(eng):
+    """Copies of every device array a call may write: fields, CPML memory, accumulators."""
+    out = []
+    for it in eng.items:
+        for key in ("main", "x", "y"):
+            out += [t.clone() for t in it.box[key]]
+        for pr in it.box["psi"]:
+            out += [t.clone() for t in pr]
+    out += [a.clone() for a in eng.accumulators(0)]
+    return out
+
+
+def _same(a, b):
+    return all(torch.equal(x, y) for x, y in zip(a, b))
+
+
+def test_noalloc_allocates_nothing():
+    """After a first call (which may do the one-time set-up), further calls leave
+    the device's free memory exactly where it was."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from meep_torch_b200 import _lib as L
+    from meep_torch_b200.engine2d import Engine2D
+    lib = L.load()
+    eng = Engine2D([_items("tm", "cuda")], ring_slots=8, variant=1)
+    stream = torch.cuda.current_stream().cuda_stream
+    parity = eng.current
+    ce, ch = _coefs(eng, 0, 600)
+
+    def call(t, k):
+        ph = (ch[t:].ctypes.data_as(C.POINTER(C.c_double)) if ch is not None else None)
+        rc = lib.mtb_yee2d_run_noalloc(eng.structs, eng.regions, eng.n_regions, eng.groups,
+                                       eng.n_groups, eng.ring_elems, 8, parity ^ (t & 1), t, k,
+                                       ce[t:].ctypes.data_as(C.POINTER(C.c_double)), ph,
+                                       stream)
+        L.check(rc, "mtb_yee2d_run_noalloc")
+
+    call(0, 20)                                           # warm-up: one-time set-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    call(20, 300)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    eng.close()
+
+
+def test_noalloc_rejects_bad_row_ptr_before_any_step():
+    """A source row_ptr that does not start at 0 is refused, and the state is untouched:
+    the check runs on the device and its verdict is read back before any step kernel."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from meep_torch_b200 import _lib as L
+    from meep_torch_b200 import engine2d
+    lib = L.load()
+    ok = engine2d.Engine2D([_items("tm", "cuda")], ring_slots=8, variant=1)
+    it = ok.items[0]
+    row_ptr, col, w = engine2d._cells(it.source.mask, it.nx, "cuda")
+    bad_rp = row_ptr.clone()
+    bad_rp[0] = 5                                         # rp[0] != 0: the list is malformed
+    S = ok.structs[0]
+    S.src_e.row_ptr, S.src_e.col, S.src_e.w = (L.ptr(t) for t in (bad_rp, col, w))
+    stream = torch.cuda.current_stream().cuda_stream
+    ce, _ = _coefs(ok, 0, 4)
+    before = _snapshot(ok)
+    rc = lib.mtb_yee2d_run_noalloc(ok.structs, ok.regions, ok.n_regions, ok.groups,
+                                   ok.n_groups, ok.ring_elems, 8, ok.current, 0, 4,
+                                   ce.ctypes.data_as(C.POINTER(C.c_double)), None, stream)
+    assert rc == L.MTB_INVALID_ARG
+    assert b"row_ptr" in lib.mtb_last_error()
+    torch.cuda.synchronize()
+    assert _same(before, _snapshot(ok))
+    del bad_rp, row_ptr, col, w
+    ok.close()
+
+
 def test_noalloc_rejects_oversize():
     if not torch.cuda.is_available():
         pytest.skip("needs a CUDA device")
@@ -156,8 +237,9 @@ def _reversed_rows(cells):
 def test_source_columns_must_ascend(monkeypatch):
     """The kernels binary-search a row's source columns, so both entry points refuse
     a row whose columns descend: the plan before any device work, the
-    allocation-free call with MTB_INVALID_ARG once its set-up kernel has flagged it
-    (every search probe stays inside the row's cell range either way)."""
+    allocation-free call with MTB_INVALID_ARG once its set-up kernel has flagged it,
+    before any step kernel, so the state is untouched (every search probe stays inside
+    the row's cell range either way)."""
     if not torch.cuda.is_available():
         pytest.skip("needs a CUDA device")
     from meep_torch_b200 import _lib as L
@@ -175,10 +257,13 @@ def test_source_columns_must_ascend(monkeypatch):
     stream = torch.cuda.current_stream().cuda_stream
     ce, _ = _coefs(ok, 0, 4)
     pe = ce.ctypes.data_as(C.POINTER(C.c_double))
+    before = _snapshot(ok)
     rc = lib.mtb_yee2d_run_noalloc(ok.structs, ok.regions, ok.n_regions, ok.groups,
                                    ok.n_groups, ok.ring_elems, 8, ok.current, 0, 4, pe, None,
                                    stream)
     assert rc == L.MTB_INVALID_ARG
     assert b"ascending" in lib.mtb_last_error()
+    torch.cuda.synchronize()
+    assert _same(before, _snapshot(ok))                   # rejected before any step kernel
     del bad
     ok.close()
