@@ -516,7 +516,8 @@ def run_cfg2(args, rank, world, dev):
     bytes_launch = W.cfg2_bytes_per_step(specs)
     res = dict(cells=cells, nsteps=nsteps, ms=ms_max, launches=launches, clocks=clocks,
                step_ms=step_ms, step_n=step_n, dft_ms=dft_ms, dft_n=dft_n,
-               bytes_launch=bytes_launch, ring_elems=eng.ring_elems)
+               timed_steps=nsteps * args.steps, bytes_launch=bytes_launch,
+               ring_elems=eng.ring_elems)
     eng.close()
     del eng, items
     torch.cuda.empty_cache()
@@ -735,6 +736,206 @@ def run_cfg3_slabs(args, rank, world, dev):
     return res
 
 
+# ------------------------------------------------------------------ reference arm
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def reference_module():
+    """The reference (meep_torch) installed beside the repository by
+    baseline/install_reference.py, or None when it is not there."""
+    if not os.path.isdir(os.path.join(REF_DIR, "meep_torch")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    import meep_torch
+    return meep_torch
+
+
+def ref_cfg2(specs, steps):
+    """The reference's own run_tm / run_te (core/run.py:125-126) on cfg2 structures:
+    its Grid, build_tm_coeffs / build_te_coeffs, LineSource, DFTFieldsMonitor and flux
+    monitors, float32, no_grad, all host threads (torch intra-op). Returns
+    (cell-updates, seconds); set-up is outside the timed region."""
+    import torch
+    from meep_torch.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch.core.grid import Grid
+    from meep_torch.core.monitors import (DFTFieldsMonitor, FluxMonitorTE, FluxMonitorTEY,
+                                          FluxMonitorTM)
+    from meep_torch.core.run import run_te, run_tm
+    from meep_torch.core.sources import GaussianPulse, LineSource
+    from meep_torch.core.stepper_te import init_te_state
+    from meep_torch.core.stepper_tm import init_tm_state
+
+    from meep_torch_b200 import workloads as W
+    cells, sec = 0, 0.0
+    for spec in specs:
+        nx, ny = spec["nx"], spec["ny"]
+        g = Grid(nx=nx, ny=ny, dx=W.DX2D, dtype=torch.float32, device="cpu")
+        eps = torch.from_numpy(spec["eps"])
+        line = LineSource(g, ix=spec["src_ix"], j0=spec["src_j"][0], j1=spec["src_j"][1],
+                          profile=GaussianPulse(0.65, 0.2))
+        fx, fy = spec["flux_x"], spec["flux_y"]
+        freqs = list(W.CFG2_FREQS)
+        if spec["pol"] == "tm":
+            m = build_tm_coeffs(g, eps_inf=eps, npml=W.NPML2D)
+            mons = [DFTFieldsMonitor(g, freqs, "Ez"),
+                    FluxMonitorTM(g, freqs, x_normal=True, idx=fx[0], lo=fx[1], hi=fx[2]),
+                    FluxMonitorTM(g, freqs, x_normal=False, idx=fy[0], lo=fy[1], hi=fy[2])]
+            run, st0, src = run_tm, init_tm_state(g), line
+        else:
+            m = build_te_coeffs(g, eps_inf=eps, npml=W.NPML2D)
+
+            class _TESrc:                   # Simulation's TE binding: mask[:, :-1] -> Dy
+                mask = line.mask[:, :-1]
+                amplitude = staticmethod(line.amplitude)
+
+            mons = [DFTFieldsMonitor(g, freqs, "Hz"),
+                    FluxMonitorTE(g, freqs, ix=fx[0], lo=fx[1], hi=fx[2]),
+                    FluxMonitorTEY(g, freqs, iy=fy[0], lo=fy[1], hi=fy[2])]
+            run, st0, src = run_te, init_te_state(g), _TESrc()
+        with torch.no_grad():
+            t0 = time.perf_counter()
+            run(st0, m, steps, source=src, monitors=mons)
+            sec += time.perf_counter() - t0
+        cells += nx * ny * steps
+    return cells, sec
+
+
+def ref_cfg1(steps=4000):
+    """The reference's run_tm on cfg1 (the full run by default). (cell-updates, s)."""
+    import torch
+    from meep_torch.core.coeffs import build_tm_coeffs
+    from meep_torch.core.grid import Grid
+    from meep_torch.core.monitors import FluxMonitorTM
+    from meep_torch.core.run import run_tm
+    from meep_torch.core.sources import GaussianPulse, LineSource
+    from meep_torch.core.stepper_tm import init_tm_state
+
+    from meep_torch_b200 import workloads as W
+    sp = W.cfg1_spec()
+    g = Grid(nx=sp["nx"], ny=sp["ny"], dx=W.DX2D, dtype=torch.float32, device="cpu")
+    m = build_tm_coeffs(g, eps_inf=torch.from_numpy(sp["eps"]), npml=W.NPML2D)
+    i, j = sp["src"]
+    src = LineSource(g, ix=i, j0=j, j1=j + 1, profile=GaussianPulse(0.15, 0.1))
+    ix, lo, hi = sp["flux"]
+    mon = FluxMonitorTM(g, list(sp["freqs"]), x_normal=True, idx=ix, lo=lo, hi=hi)
+    with torch.no_grad():
+        t0 = time.perf_counter()
+        run_tm(init_tm_state(g), m, steps, source=src, monitors=[mon])
+        sec = time.perf_counter() - t0
+    return sp["nx"] * sp["ny"] * steps, sec
+
+
+def ref_cfg3(steps, n=256):
+    """The reference's run_3d (core/monitors_3d.py:192) on the cfg3 grid with its point
+    source and six flux faces, `steps` steps. (cell-updates, s)."""
+    import numpy as np
+    import torch
+    from meep_torch.core.monitors_3d import FluxMonitor3D, PointSource3D, run_3d
+    from meep_torch.core.sources import GaussianPulse
+    from meep_torch.core.stepper_3d import build_3d_coeffs, init_3d_state
+
+    from meep_torch_b200 import workloads as W
+    dx, npml = 1.0 / 16, 16
+    c = build_3d_coeffs(n, n, n, dx, eps=torch.from_numpy(W.cfg3_eps(n)), npml=npml,
+                        dtype=torch.float32)
+    s0 = init_3d_state(n, n, n, npml=npml, dtype=torch.float32)
+    src = PointSource3D(c.dt, "Ez", n // 2, n // 2, n // 2, GaussianPulse(0.5, 0.3))
+    lo_, hi_ = 24 * n // 256, 232 * n // 256
+    freqs = np.linspace(0.35, 0.65, 20).tolist()
+    mons = [FluxMonitor3D(c.dt, freqs, normal=a, idx=(lo_ if i == 24 else hi_),
+                          win=(lo_, hi_, lo_, hi_), dtype=torch.float32)
+            for a, i in W.CFG3_FACES]
+    with torch.no_grad():
+        t0 = time.perf_counter()
+        run_3d(s0, c, steps, source=src, monitors=mons)
+        sec = time.perf_counter() - t0
+    return n ** 3 * steps, sec
+
+
+def ref_cfg4(steps):
+    """One gradient of the cfg4-shaped problem through the reference's design chain and
+    autograd of run_tm(checkpoint_every=256), `steps` time steps. Returns seconds."""
+    import numpy as np
+    import torch
+    from meep_torch.adjoint.problem import DesignRegion, MaterialGrid, OptimizationProblem
+    from meep_torch.core.coeffs import build_tm_coeffs
+    from meep_torch.core.grid import Grid
+    from meep_torch.core.monitors import FluxMonitorTM
+    from meep_torch.core.run import run_tm
+    from meep_torch.core.sources import GaussianPulse, LineSource
+    from meep_torch.core.stepper_tm import init_tm_state
+
+    from meep_torch_b200 import workloads as W
+    c = W.CFG4
+    nx, ny, dx, npml = c["nx"], c["ny"], c["dx"], c["npml"]
+    base = torch.full((nx, ny), c["eps_bg"], dtype=torch.float32)
+    y0, y1 = ny // 2 - c["guide_w"] // 2, ny // 2 + c["guide_w"] // 2
+    base[:, y0:y1] = c["eps_core"]
+    d = c["design"]
+    ix0, iy0 = nx // 2 - d // 2, ny // 2 - d // 2
+    reg = DesignRegion(MaterialGrid((d, d), c["eps_bg"], c["eps_core"]), ix0=ix0, ix1=ix0 + d,
+                       iy0=iy0, iy1=iy0 + d)
+    grid = Grid(nx=nx, ny=ny, dx=dx, dtype=torch.float32, device="cpu")
+    src = LineSource(grid, ix=npml + 10, j0=y0 - 10, j1=y1 + 10,
+                     profile=GaussianPulse(0.645, 0.12))
+    mon = FluxMonitorTM(grid, list(c["freqs"]), x_normal=True, idx=nx - npml - 10,
+                        lo=y0 - 20, hi=y1 + 20)
+
+    def run_fn(eps):
+        m = build_tm_coeffs(grid, eps_inf=eps, npml=npml)
+        _, (acc,) = run_tm(init_tm_state(grid), m, steps, source=src, monitors=[mon],
+                           checkpoint_every=256)
+        return mon.flux(acc, dx).mean()
+
+    rho0 = torch.tensor(np.random.default_rng(4).uniform(0.4, 0.6, (d, d)), dtype=torch.float32)
+    opt = OptimizationProblem(run_fn, base, reg, filter_radius=c["radius"], dx=dx,
+                              beta=c["beta"], eta=c["eta"], rho0=rho0)
+    t0 = time.perf_counter()
+    opt()
+    return time.perf_counter() - t0
+
+
+def reference_cpu(wl, args, threads):
+    """(value, unit, cores, sample, kind) of the reference's own CPU path on a bounded
+    sample of workload `wl`, or None when the reference is not installed (cfg5: the
+    reference has no surrogate, so None)."""
+    if wl == "cfg5" or reference_module() is None:
+        return None
+    import torch
+    torch.set_num_threads(os.cpu_count() or 1)
+    cores = torch.get_num_threads()
+    from meep_torch_b200 import workloads as W
+    if wl == "cfg2":
+        n_s, steps = args.ref_structs, args.ref_steps or 150
+        cells, sec = ref_cfg2(W.cfg2_specs()[:n_s], steps)
+        return (cells / sec / 1e9, "Gcell-updates/s", cores,
+                f"reference meep_torch run_tm / run_te (float32, no_grad, {cores} torch "
+                f"threads) on cfg2 structures 0..{n_s - 1} x {steps} steps with the cfg2 DFT and "
+                f"flux monitors, {sec:.1f} s", "reference")
+    if wl == "cfg1":
+        cells, sec = ref_cfg1(4000)
+        return (cells / sec / 1e9, "Gcell-updates/s", cores,
+                f"reference meep_torch run_tm (float32, no_grad, {cores} torch threads), the "
+                f"full 4000-step cfg1 run, {sec:.1f} s", "reference")
+    if wl == "cfg3":
+        steps = 6
+        cells, sec = ref_cfg3(steps, n=args.n3)
+        return (cells / sec / 1e9, "Gcell-updates/s", cores,
+                f"reference meep_torch run_3d (float32, no_grad, {cores} torch threads) on the "
+                f"cfg3 {args.n3}^3 grid with its source and six flux faces, {steps} steps, "
+                f"{sec:.1f} s", "reference")
+    if wl == "cfg4":
+        steps = args.ref_steps or 256
+        n = args.run_steps if args.run_steps != 5000 else W.CFG4["steps"]
+        sec = ref_cfg4(steps)
+        return (1.0 / (sec * n / steps), "gradient-evaluations/s", cores,
+                f"reference meep_torch OptimizationProblem gradient (design chain + autograd "
+                f"of run_tm, checkpoint_every=256, float32, {cores} torch threads) over {steps} "
+                f"steps in {sec:.1f} s, scaled to the {n}-step run", "reference")
+    return None
+
+
 def reference_line(args, config, threads):
     """The reference arm: the oracle port of the reference's CPU path, timed on the
     host cores on a bounded sample of the chosen workload, in that workload's metric."""
@@ -742,7 +943,18 @@ def reference_line(args, config, threads):
     wl = args.workload
     vals = []
     t_all = time.perf_counter()
-    if wl == "cfg2":
+    kind = "port"
+    if reference_module() is not None and wl != "cfg5":
+        kind = "reference"
+        if wl == "cfg2" and args.warmup:
+            ref_cfg2(W.cfg2_specs()[:1], 5)                                  # warm-up
+            t_all = time.perf_counter()
+        sample = unit = None
+        cores = 1
+        for _ in range(args.steps):
+            v_, unit, cores, sample, _k = reference_cpu(wl, args, threads)
+            vals.append(v_)
+    elif wl == "cfg2":
         unit = "Gcell-updates/s"
         specs = W.cfg2_specs()[:args.cpu_structs]
         for _ in range(args.warmup and 1):
@@ -793,7 +1005,7 @@ def reference_line(args, config, threads):
             "warmup": args.warmup, "ms_per_step": wall / max(args.steps, 1) * 1e3,
             "higher_is_better": True, "impl": "reference", "dtype": "f32",
             "data": "synthetic", "config": config,
-            "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -840,6 +1052,10 @@ def main():
     ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
     ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
     ap.add_argument("--cpu-steps", type=int, default=300)
+    ap.add_argument("--ref-structs", type=int, default=4,
+                    help="cfg2 structures of the reference's own CPU run (reference arm)")
+    ap.add_argument("--ref-steps", type=int, default=0,
+                    help="time steps of the reference's own CPU sample (0 = per workload)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--structs", type=int, default=256,
                     help="structures per rank (profiling runs use fewer)")
@@ -1046,7 +1262,10 @@ def main():
     total_updates = cells_total * r["nsteps"] * args.steps
     value = total_updates / (r["ms"] / 1e3) / 1e9
     step_avg_ms = r["step_ms"] / max(r["step_n"], 1)
-    achieved = r["bytes_launch"] / (step_avg_ms / 1e3) / 1e9
+    # time steps one step-kernel launch advances: 1 for the one-step kernels, up to 4
+    # for the temporally blocked ones (every timed step is covered by a timed launch)
+    steps_per_launch = (r.get("timed_steps", r["step_n"]) / max(r["step_n"], 1))
+    achieved = r["bytes_launch"] * steps_per_launch / (step_avg_ms / 1e3) / 1e9
     traffic = None
     cfg3 = args.workload == "cfg3"
     prof = os.path.join(ROOT, "profiles", "yee3d_step_cfg3_traffic.json" if cfg3
@@ -1054,7 +1273,7 @@ def main():
     if os.path.exists(prof) and args.workload in ("cfg2", "cfg3"):
         with open(prof) as f:
             tr = json.load(f)
-        eff = args.variant or 2                           # library default: tiles / split
+        eff = args.variant or (3 if args.workload == "cfg2" else 2)   # library defaults
         if tr.get("variant") == eff:
             traffic = tr.get("dram_bytes_per_launch")
     e2e_val = (total_updates / r["e2e_s"] / 1e9
@@ -1066,7 +1285,8 @@ def main():
               "k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else
               "k_yee3d_step (one step)" if cfg3 else
               "k_yee2d_tm + k_yee2d_te (one step)" if args.variant == 1 else
-              "k_tile_tm + k_tile_te (one step)")
+              "k_tile_tm + k_tile_te (one step)" if args.variant == 2 else
+              "k_tb_tm + k_tb_te (temporally blocked: up to 4 steps per launch)")
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1083,7 +1303,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "alg_bytes_per_launch": r["bytes_launch"],
+                     "alg_bytes_per_step": r["bytes_launch"],
+                     "steps_per_launch": steps_per_launch,
+                     "alg_bytes_per_launch": r["bytes_launch"] * steps_per_launch,
                      "launch_ms": step_avg_ms, "launches": r["step_n"],
                      "dft_contract_ms_total": r["dft_ms"], "dft_contract_launches": r["dft_n"],
                      "step_kernel_share": r["step_ms"] / max(r["ms"], 1e-9),
@@ -1098,7 +1320,13 @@ def main():
         "clocks": r["clocks"],
         "gpu_launches": r["launches"],
     }
-    if rank == 0 and not args.no_cpu:
+    ref_cpu = (reference_cpu(args.workload, args, threads)
+               if rank == 0 and not args.no_cpu else None)
+    if ref_cpu is not None:
+        v_, u_, cores_, sample_, kind_ = ref_cpu
+        line["cpu_baseline"] = {"value": v_, "unit": u_, "cores": cores_, "kind": kind_,
+                                "sample": sample_}
+    elif rank == 0 and not args.no_cpu:
         if args.workload == "cfg1":
             cells, sec = cpu_sample_cfg1(4000)
             line["cpu_baseline"] = {"value": cells / sec / 1e9, "unit": "Gcell-updates/s",

@@ -222,7 +222,13 @@ typedef struct mtb_tuning {
                                + one contraction) as a CUDA graph: 0 default
                                (every whole flush after the plan's first step
                                while per-launch timing is off), -1 off      */
-    int32_t variant;        /* 2D: 0 default (tiles), 1 row march, 2 tiles;
+    int32_t variant;        /* 2D: 0 default (3 when every structure is
+                               eligible, else 2), 1 row march, 2 one-step
+                               tiles, 3 temporally blocked tiles (up to 4
+                               steps per launch from TMA-staged 32 x 128
+                               tiles; PEC structures without conductivity,
+                               poles or magnetic pairs; the plan's first
+                               step runs on the one-step tiles);
                                3D: 0 default (split), 1 fused x-march,
                                2 split H / E streaming kernels              */
 } mtb_tuning;

@@ -4,46 +4,48 @@ import torch
 from ..engine3d import Engine3D
 
 
-class PlaneSource:
-    """Soft area current on the plane idx normal to ``axis`` on an E component
-    (mask subtracted, core/stepper_3d.py:452-461)."""
+class _Sampled3D:
+    """Shared by the 3D sources: the profile sampled at half steps (t_idx + 1/2) dt."""
+
+    def amplitude(self, t_idx: int) -> float:
+        return self.profile.amplitude((t_idx + 0.5) * self.dt)
+
+
+# array shape of each E component (its staggered axis is one node shorter)
+_E_AXIS = {"Ex": 0, "Ey": 1, "Ez": 2}
+
+
+class PlaneSource(_Sampled3D):
+    """A soft area current with unit weight on the plane idx normal to ``axis`` of one E
+    component, optionally limited to [lo, hi) along the two in-plane axes; run_3d
+    subtracts dt amp mask / eps (core/stepper_3d.py:452-461)."""
 
     def __init__(self, nx, ny, nz, dt, comp, axis, idx, profile, lo=None, hi=None, device=None):
-        shape = {"Ex": (nx - 1, ny, nz), "Ey": (nx, ny - 1, nz), "Ez": (nx, ny, nz - 1)}[comp]
-        mask = torch.zeros(shape, dtype=torch.float32, device=device)
-        sl = [slice(None)] * 3
-        sl[axis] = idx
-        mask[tuple(sl)] = 1.0
+        shape = [nx, ny, nz]
+        shape[_E_AXIS[comp]] -= 1
+        region = [slice(None)] * 3
+        region[axis] = idx
         if lo is not None and hi is not None:
-            sel = [slice(None)] * 3
-            for a in range(3):
-                if a != axis:
-                    sel[a] = slice(lo, hi)
-            window = mask[tuple(sel)].clone()
-            mask = torch.zeros_like(mask)
-            mask[tuple(sel)] = window
+            for other in {0, 1, 2} - {axis}:
+                region[other] = slice(lo, hi)
+        mask = torch.zeros(shape, dtype=torch.float32, device=device)
+        mask[tuple(region)] = 1.0
+        self.src = (comp, mask)
         self.profile = profile
         self.dt = dt
-        self.src = (comp, mask)
-
-    def amplitude(self, t_idx: int) -> float:
-        return self.profile.amplitude((t_idx + 0.5) * self.dt)
 
 
-class PointSource3D:
-    """Soft point current; run_3d ADDS dt*amp/eps (core/stepper_3d.py:474-480),
-    run_3d_lean subtracts (core/stepper_3d_lean.py:293-296)."""
-    _COMP = {"Ex", "Ey", "Ez"}
+class PointSource3D(_Sampled3D):
+    """A soft current at one node (i, j, k) of an E component. The functional stepper
+    adds dt amp / eps there (core/stepper_3d.py:474-480); the lean stepper subtracts it
+    (core/stepper_3d_lean.py:293-296)."""
 
     def __init__(self, dt, comp, i, j, k, profile):
-        if comp not in self._COMP:
-            raise ValueError(f"PointSource3D comp must be Ex/Ey/Ez, got {comp!r}")
-        self.dt = dt
-        self.profile = profile
+        if comp not in _E_AXIS:
+            raise ValueError(f"PointSource3D drives Ex, Ey or Ez, not {comp!r}")
         self.src = (comp, int(i), int(j), int(k))
-
-    def amplitude(self, t_idx: int) -> float:
-        return self.profile.amplitude((t_idx + 0.5) * self.dt)
+        self.profile = profile
+        self.dt = dt
 
 
 class DFTFieldsMonitor3D:

@@ -24,7 +24,10 @@
 // active (a != 0 or b != 1); outside the layers it is identically zero, as in
 // the reference.
 #include <algorithm>
+#include <cstring>
 #include <mutex>
+
+#include <cudaTypedefs.h>
 #include <vector>
 
 #include "mtb_common.cuh"
@@ -1863,6 +1866,8 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
 
 }  // namespace mtb
 
+#include "yee2d_tb.cuh"
+
 using namespace mtb;
 
 struct mtb_yee2d_plan {
@@ -1883,12 +1888,225 @@ struct mtb_yee2d_plan {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // ring flush graph per start parity
     int64_t gkern[2] = {0, 0};         // kernels per graph replay
     DevBuf stage_d;                    // coefficient and phase rows of one flush
+    int gend[2] = {0, 1};              // parity after a replay, per start parity
+    bool tb = false;                   // temporally blocked kernels after the first step
+    DevBuf tb_work_d, tmaps_d;         // TB tile list (TM first), tensor maps
+    DevBuf tb_meta_d, tb_prof_d;       // TB records, padded profiles
+    int n_tb_tm = 0, n_tb_te = 0, tb_grid = 148;
     int par = 0;
     int first = 1;
     int64_t last_launches = 0;
     DftState dft;
     LaunchTimer timer;
 };
+
+// ---------------------------------------------------------------- TB set-up
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+// A 2D float32 tensor map over one box array (nx rows x pitch floats), box of
+// bc columns x br rows; reads outside the array return zero.
+static int tmap_2d(CUtensorMap *m, const float *base, int nx, int pitch, int bc, int br, int s) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    if (!enc) return fail(MTB_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)nx};
+    const cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)bc, (cuuint32_t)br};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(MTB_CUDA_ERROR, "structure %d: tensor map encoding failed (%d)", s, (int)r);
+    return MTB_OK;
+}
+
+// Structures the TB kernels take: no conductivity, poles, magnetic pairs or
+// PMC walls (those run on the tile kernels' extended variant).
+static bool tb_eligible(const mtb_yee2d_struct &S) {
+    return !S.cond_d1[0] && !S.cond_d1[1] && !S.n_poles && !S.n_poles_y && !S.mag_h1[0] &&
+           !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc;
+}
+
+// Copy n floats of a device array to the host.
+static int d2h_floats(std::vector<float> &h, const float *d, int n, int s) {
+    h.assign(std::max(n, 0), 0.f);
+    if (n <= 0) return MTB_OK;
+    const cudaError_t e = cudaMemcpy(h.data(), d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return fail(MTB_CUDA_ERROR, "structure %d: reading a profile: %s", s,
+                    cudaGetErrorString(e));
+    return MTB_OK;
+}
+
+// Tensor maps, per-structure records (descriptor + line samples), padded
+// profiles and the tile list (TM tiles first, then TE) of a TB plan. A
+// structure's padded profiles are 4 y rows (hy b, a; ey b, a) of pitch + 128
+// floats, column j at index j + 4, then 4 x rows (hx b, a; ex b, a) of
+// nx + 32 floats, row i at index i + 4; inert (1, 0) off the arrays.
+static int tb_setup_plan(mtb_yee2d_plan *p, const std::vector<mtb_yee2d_struct> &structs) {
+    const int n = (int)structs.size();
+    std::vector<CUtensorMap> maps((size_t)n * TBM_N);
+    std::vector<TbMeta> metas(n);
+    std::vector<int64_t> poff(n, 0), xoff(n, 0);
+    std::vector<float> prof;
+    std::vector<int4> work;
+    int rc;
+    for (int s = 0; s < n; ++s) {                  // records and padded profiles
+        const mtb_yee2d_struct &S = structs[s];
+        std::memset(&metas[s], 0, sizeof(TbMeta));
+        metas[s].s = S;
+        if (S.n_lines > 0) {
+            const cudaError_t e = cudaMemcpy(metas[s].lines, S.lines,
+                                             sizeof(mtb_line_sample) * S.n_lines,
+                                             cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess)
+                return fail(MTB_CUDA_ERROR, "structure %d: reading line samples: %s", s,
+                            cudaGetErrorString(e));
+        }
+        const int row = S.pitch + 128, xrow = (S.nx + 32 + 3) & ~3;
+        poff[s] = (int64_t)prof.size();
+        xoff[s] = poff[s] + 4 * (int64_t)row;
+        prof.resize(prof.size() + 4 * (size_t)row + 4 * (size_t)xrow);
+        float *pp = prof.data() + poff[s], *xp = prof.data() + xoff[s];
+        for (int q = 0; q < row; ++q) {
+            pp[q] = 1.f; pp[row + q] = 0.f; pp[2 * row + q] = 1.f; pp[3 * row + q] = 0.f;
+        }
+        for (int q = 0; q < xrow; ++q) {
+            xp[q] = 1.f; xp[xrow + q] = 0.f; xp[2 * xrow + q] = 1.f; xp[3 * xrow + q] = 0.f;
+        }
+        std::vector<float> hb, ha, eb, ea;
+        if ((rc = d2h_floats(hb, S.hy_b, S.ny - 1, s)) ||
+            (rc = d2h_floats(ha, S.hy_a, S.ny - 1, s)) ||
+            (rc = d2h_floats(eb, S.ey_b, S.ny, s)) || (rc = d2h_floats(ea, S.ey_a, S.ny, s)))
+            return rc;
+        for (int j = 0; j < S.ny - 1; ++j) { pp[j + 4] = hb[j]; pp[row + j + 4] = ha[j]; }
+        for (int j = 0; j < S.ny; ++j) { pp[2 * row + j + 4] = eb[j]; pp[3 * row + j + 4] = ea[j]; }
+        if ((rc = d2h_floats(hb, S.hx_b, S.nx - 1, s)) ||
+            (rc = d2h_floats(ha, S.hx_a, S.nx - 1, s)) ||
+            (rc = d2h_floats(eb, S.ex_b, S.nx, s)) || (rc = d2h_floats(ea, S.ex_a, S.nx, s)))
+            return rc;
+        for (int i = 0; i < S.nx - 1; ++i) { xp[i + 4] = hb[i]; xp[xrow + i + 4] = ha[i]; }
+        for (int i = 0; i < S.nx; ++i) { xp[2 * xrow + i + 4] = eb[i]; xp[3 * xrow + i + 4] = ea[i]; }
+    }
+    for (int pol = 0; pol < 2; ++pol) {
+        for (int s = 0; s < n; ++s) {
+            const mtb_yee2d_struct &S = structs[s];
+            if (S.pol != (pol == 0 ? MTB_TM : MTB_TE)) continue;
+            const int nx = S.nx, P = S.pitch;
+            CUtensorMap *m = maps.data() + (size_t)s * TBM_N;
+            for (int b = 0; b < 2; ++b) {
+                if ((rc = tmap_2d(m + TBM_MAIN + b, S.f_main[b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_X + b, S.f_x[b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_Y + b, S.f_y[b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_P1 + b, S.psi[1][b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_P2 + b, S.psi[2][b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_P0W + b, S.psi[0][b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_P3W + b, S.psi[3][b], nx, P, TB_C, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_P0N + b, S.psi[0][b], nx, P, TB_NARROW, TB_R, s)) ||
+                    (rc = tmap_2d(m + TBM_P3N + b, S.psi[3][b], nx, P, TB_NARROW, TB_R, s)))
+                    return rc;
+            }
+            if ((rc = tmap_2d(m + TBM_IEA, S.inv_eps_a, nx, P, TB_C, TB_R, s))) return rc;
+            if ((rc = tmap_2d(m + TBM_IEB, S.pol == MTB_TE ? S.inv_eps_b : S.inv_eps_a, nx, P,
+                              TB_C, TB_R, s)))
+                return rc;
+            // layer extents: rows [0, XL) and [XH, nx), columns [0, YL) and [YH, ny)
+            const int XL = std::max(S.xband[0], S.xband[2]), XH = std::min(S.xband[1], S.xband[3]);
+            const int YL = std::max(S.yband[0], S.yband[2]), YH = std::min(S.yband[1], S.yband[3]);
+            const mtb_line_sample *ls = metas[s].lines;
+            for (int r0 = 0; r0 < nx; r0 += TB_OUTR) {
+                const int wr0 = r0 - TB_T, wr1 = r0 - TB_T + TB_R;
+                const bool xl = wr0 < XL || wr1 > XH;
+                const int or1 = std::min(r0 + TB_OUTR, nx);
+                for (int c0 = 0; c0 < P; c0 += TB_OUTC) {
+                    const int wc0 = c0 - 4, wc1 = c0 - 4 + TB_C, oc1 = c0 + TB_OUTC;
+                    const int la = std::max(wc0, 0), lb = std::min(wc1, YL);
+                    const int ha = std::max(wc0, YH), hb = std::min(wc1, S.ny);
+                    const bool lo = lb > la, hi = hb > ha;
+                    int flags = xl ? TBF_XPSI : 0;
+                    if (lo || hi) {
+                        const int a = lo ? la : ha, b = lo ? lb : hb;
+                        const int xs = a & ~3;
+                        if (lo && hi) {
+                            flags |= TBF_YWIDE << TBF_YSHIFT;
+                        } else if (b <= xs + TB_NARROW) {
+                            flags |= (TBF_YNARROW << TBF_YSHIFT) | ((xs - wc0) << TBF_XS_SHIFT);
+                        } else {
+                            flags |= TBF_YWIDE << TBF_YSHIFT;
+                        }
+                    }
+                    unsigned lmask = 0;
+                    for (int l = 0; l < S.n_lines; ++l) {
+                        const mtb_line_sample &q = ls[l];
+                        const bool t = q.kind == 0
+                                           ? (q.index >= r0 && q.index < or1 && q.lo < oc1 &&
+                                              q.hi > c0)
+                                           : (q.index >= c0 && q.index < oc1 && q.lo < or1 &&
+                                              q.hi > r0);
+                        if (t) lmask |= 1u << l;
+                    }
+                    flags |= (int)(lmask << TBF_LINE_SHIFT);
+                    if (!xl && !(lo || hi) && wr0 >= 1 && wr1 <= nx - 1 && wc0 >= 1 &&
+                        wc1 <= S.ny - 1)
+                        flags |= TBF_LEAN;
+                    const int64_t yo = poff[s] + c0, xo = xoff[s] + r0;
+                    const int meta_bytes = (int)(sizeof(mtb_yee2d_struct) +
+                                                 S.n_lines * sizeof(mtb_line_sample));
+                    work.push_back(make_int4(s, r0, c0, flags));
+                    work.push_back(make_int4(meta_bytes, S.pitch + 128, (int)(uint32_t)yo,
+                                             (int)(yo >> 32)));
+                    work.push_back(make_int4((int)(uint32_t)xo, (int)(xo >> 32),
+                                             (S.nx + 32 + 3) & ~3, 0));
+                }
+            }
+        }
+        if (pol == 0) p->n_tb_tm = (int)(work.size() / TB_WORK);
+    }
+    p->n_tb_te = (int)(work.size() / TB_WORK) - p->n_tb_tm;
+    if ((rc = p->tmaps_d.ensure(sizeof(CUtensorMap) * maps.size())) ||
+        (rc = p->tb_work_d.ensure(sizeof(int4) * std::max<size_t>(work.size(), 1))) ||
+        (rc = p->tb_meta_d.ensure(sizeof(TbMeta) * metas.size())) ||
+        (rc = p->tb_prof_d.ensure(sizeof(float) * prof.size())))
+        return rc;
+    cudaError_t e = cudaMemcpy(p->tmaps_d.p, maps.data(), sizeof(CUtensorMap) * maps.size(),
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !work.empty())
+        e = cudaMemcpy(p->tb_work_d.p, work.data(), sizeof(int4) * work.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->tb_meta_d.p, metas.data(), sizeof(TbMeta) * metas.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->tb_prof_d.p, prof.data(), sizeof(float) * prof.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tb_tm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tb_smem<false>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tb_te, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tb_smem<true>());
+    int dev = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return fail(MTB_CUDA_ERROR, "TB set-up: %s", cudaGetErrorString(e));
+    p->tb_grid = std::max(sms, 1);
+    p->tb = true;
+    return MTB_OK;
+}
+
 
 static int check_ptr(const void *p, const char *what, int s) {
     if (!p) return fail(MTB_INVALID_ARG, "structure %d: %s is null", s, what);
@@ -1968,7 +2186,11 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     *out = nullptr;
     if (n < 1 || !structs_in) return fail(MTB_INVALID_ARG, "need at least one structure");
     if (n_amp_cols < 0) return fail(MTB_INVALID_ARG, "n_amp_cols < 0");
-    const int variant = (tuning && tuning->variant == 1) ? 1 : 2;   // default: tiles
+    // default (0) and variant 3: the temporally blocked kernels after the first
+    // step when every structure is eligible, else tiles; 2: tiles only
+    const int tv = tuning ? tuning->variant : 0;
+    const int variant = tv == 1 ? 1 : 2;
+    bool want_tb = tv == 3 || tv == 0;
     int rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
     int wr = 1;
     if (variant == 2) {
@@ -2124,6 +2346,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
             p->ext = true;
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
     }
+    for (int s = 0; s < n; ++s) want_tb = want_tb && tb_eligible(structs[s]);
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->structs_d.ensure(sizeof(mtb_yee2d_struct) * n);
     if (!rc) rc = p->work_d.ensure(sizeof(int4) * n_work);
@@ -2164,6 +2387,10 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         p->dft.release();
         delete p;
         return fail(MTB_CUDA_ERROR, "plan upload failed: %s", cudaGetErrorString(e));
+    }
+    if (want_tb && (rc = tb_setup_plan(p, structs))) {
+        mtb_yee2d_plan_destroy(p);
+        return rc;
     }
     *out = p;
     return MTB_OK;
@@ -2228,6 +2455,42 @@ static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
     return MTB_OK;
 }
 
+// One TB launch pair (TM tiles, then TE tiles) advancing C.nsub steps.
+static int launch_tb(mtb_yee2d_plan *p, const TbCtx &C, cudaStream_t st) {
+    const CUtensorMap *M = p->tmaps_d.as<CUtensorMap>();
+    const int4 *W = p->tb_work_d.as<int4>();
+    if (p->n_tb_tm > 0) {
+        k_tb_tm<<<std::min(p->tb_grid, p->n_tb_tm), TB_THREADS, tb_smem<false>(), st>>>(
+            M, W, p->n_tb_tm, C);
+        MTB_CHECK_LAUNCH();
+        ++p->last_launches;
+    }
+    if (p->n_tb_te > 0) {
+        k_tb_te<<<std::min(p->tb_grid, p->n_tb_te), TB_THREADS, tb_smem<true>(), st>>>(
+            M, W + (size_t)TB_WORK * p->n_tb_tm, p->n_tb_te, C);
+        MTB_CHECK_LAUNCH();
+        ++p->last_launches;
+    }
+    return MTB_OK;
+}
+
+// Launch context of n TB sub-steps whose first sample goes to ring slot `slot`.
+static TbCtx tb_ctx(const mtb_yee2d_plan *p, const float *amp_e, const float *amp_h, int nc,
+                    int n, int slot, int par) {
+    TbCtx C;
+    C.meta = p->tb_meta_d.as<TbMeta>();
+    C.prof = p->tb_prof_d.as<float>();
+    C.amp_e = amp_e;
+    C.amp_h = amp_h;
+    C.ncols = nc;
+    C.nsub = n;
+    C.ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;
+    C.slot_elems = p->dft.slot_elems;
+    C.err = p->err_d.as<int>();
+    C.par = par;
+    return C;
+}
+
 // Capture one ring flush (G steps from parity par0, then the contraction)
 // reading its coefficient and phase rows from the plan's staging buffer.
 static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
@@ -2239,7 +2502,16 @@ static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
     MTB_CUDA_TRY(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
     int rc = MTB_OK;
     int par = par0;
-    for (int s = 0; s < G && !rc; ++s) {
+    for (int s = 0; s < G && !rc;) {
+        if (p->tb) {                             // TB launches of up to TB_T steps
+            const int n = std::min(TB_T, G - s);
+            const TbCtx C = tb_ctx(p, stage + (size_t)s * nc,
+                                   stage + (size_t)G * nc + (size_t)s * nc, nc, n, s, par);
+            rc = launch_tb(p, C, p->cap);
+            par ^= 1;
+            s += n;
+            continue;
+        }
         Ctx2D C;
         C.amp_e = stage + (size_t)s * nc;
         C.amp_h = stage + (size_t)G * nc + (size_t)s * nc;
@@ -2251,7 +2523,9 @@ static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
         C.pst = 0;                               // no poles in graph-replayed plans
         rc = launch_step(p, C, p->cap);
         par ^= 1;
+        ++s;
     }
+    p->gend[par0] = par;
     if (!rc && p->dft.n_regions > 0) {
         rc = p->dft.contract(0, G, p->cap, nullptr, phase);
         if (!rc) ++p->last_launches;
@@ -2325,8 +2599,28 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
             MTB_CUDA_TRY(cudaGraphLaunch(p->gexec[p->par], st));
             count_launch(p->gkern[p->par]);
             p->last_launches += p->gkern[p->par];
-            p->par ^= (G & 1);
+            p->par = p->gend[p->par];
             s += G;
+            continue;
+        }
+        if (p->tb && !p->first) {
+            // TB: up to TB_T steps per launch, never past the ring's end
+            const int n = std::min(TB_T, std::min(G - slot, k - s));
+            const TbCtx C = tb_ctx(p, ad + (size_t)s * nc, ad + per + (size_t)s * nc, nc, n, slot,
+                                   p->par);
+            if ((rc = p->timer.begin(st, 0))) return rc;
+            if ((rc = launch_tb(p, C, st))) return rc;
+            if ((rc = p->timer.end(st))) return rc;
+            p->par ^= 1;
+            s += n;
+            slot += n;
+            if (slot == G || s == k) {
+                if (p->dft.n_regions > 0) {
+                    if ((rc = p->dft.contract(s - slot, slot, st, &p->timer))) return rc;
+                    ++p->last_launches;
+                }
+                slot = 0;
+            }
             continue;
         }
         Ctx2D C;
@@ -2395,6 +2689,10 @@ void mtb_yee2d_plan_destroy(mtb_yee2d_plan *p) {
         if (p->gexec[q]) cudaGraphExecDestroy(p->gexec[q]);
     if (p->cap) cudaStreamDestroy(p->cap);
     p->stage_d.release();
+    p->tb_work_d.release();
+    p->tmaps_d.release();
+    p->tb_meta_d.release();
+    p->tb_prof_d.release();
     p->structs_d.release();
     p->work_d.release();
     p->amp_d.release();

@@ -18,7 +18,9 @@ from .engine2d import Engine2D
 __all__ = ["DEFAULT_CANDIDATES", "autotune_2d"]
 
 DEFAULT_CANDIDATES = (
-    {"variant": 2, "rows_per_warp": 0, "ring_slots": 32},     # library default
+    {"variant": 3, "rows_per_warp": 0, "ring_slots": 32},     # library default: TB tiles
+    {"variant": 3, "rows_per_warp": 0, "ring_slots": 16},
+    {"variant": 2, "rows_per_warp": 0, "ring_slots": 32},     # one-step tiles
     {"variant": 2, "rows_per_warp": 1, "ring_slots": 32},     # tiles, one row per warp
     {"variant": 2, "rows_per_warp": 4, "ring_slots": 32},     # tiles, register-blocked rows
     {"variant": 1, "rows_per_warp": 0, "ring_slots": 32},     # row march

@@ -246,7 +246,7 @@ def _oracle_te(nx, ny, dx, eps, npml, n, ix, j0, j1, freqs, fcen=0.65, fw=0.3, m
                     amp_fn=lambda t: prof(O.src_time(t, dt)), mask=mask, monitors=mons)
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_batched_mixed_tm_te_matches_oracle(variant):
     """One plan advancing TM and TE structures of different, odd sizes whose
     widths span several 128-column strips and rows several warp segments."""
@@ -395,21 +395,24 @@ def test_3d_wide_z_matches_oracle(variant, slab):
     assert not bad, bad
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_random_state_batched_matches_oracle(variant):
     """Random initial fields (waves in every CPML layer from the first step),
     a batch of TM, TM with PMC y walls and TE structures whose widths are not
     multiples of 128 and whose heights are not multiples of the tile rows;
-    fields and CPML memory against the oracle."""
+    fields and CPML memory against the oracle. The temporally blocked kernels
+    (variant 3) take PEC structures only, so their batch swaps the PMC one for a
+    PEC one of the same shape; it runs 41 steps (a first single step, then ten
+    4-step launches)."""
     from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
     from meep_torch_b200.core.grid import Grid
     from meep_torch_b200.core.stepper_te import init_te_state
     from meep_torch_b200.core.stepper_tm import init_tm_state
     from meep_torch_b200.engine2d import Engine2D
     rng = np.random.default_rng(17)
-    specs = [("tm", 37, 300, False), ("te", 50, 261, False), ("tm", 29, 131, True),
+    specs = [("tm", 37, 300, False), ("te", 50, 261, False), ("tm", 29, 131, variant != 3),
              ("te", 19, 45, False)]
-    n, npml, dx = 40, 8, 0.05
+    n, npml, dx = (41 if variant == 3 else 40), 8, 0.05
     items, refs = [], []
     for pol, nx, ny, pmc in specs:
         eps = (1.0 + 5.0 * rng.random((nx, ny))).astype(np.float32)
@@ -450,7 +453,7 @@ def test_random_state_batched_matches_oracle(variant):
     assert not bad, bad
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_graph_replay_bitwise_equal_to_direct_launches(variant):
     """Whole ring flushes replayed as a CUDA graph (coefficient and phase rows
     staged per flush) give bit-identical fields and accumulators to the same
@@ -475,6 +478,40 @@ def test_graph_replay_bitwise_equal_to_direct_launches(variant):
                 assert torch.equal(x, y), (b, name)
         for x, y in zip(a0[b], a1[b]):
             assert torch.equal(x, y), b
+
+
+def test_tb_matches_tiles_on_a_cfg2_batch():
+    """The temporally blocked kernels (4 steps per launch from TMA-staged tiles)
+    against the one-step tile kernels on a cfg2-shaped batch of TM and TE bends
+    (line sources, full-grid DFT, two flux lines), over ring flushes of 32 steps
+    and a partial last launch: fields, CPML memory and accumulators agree to
+    float32 rounding, and the TB plan issues about a quarter of the launches."""
+    from meep_torch_b200 import workloads as W
+    from meep_torch_b200.engine2d import Engine2D
+    specs = W.cfg2_specs(n=6, seed=11, lo=120, hi=420)
+    outs, launches = [], []
+    for variant in (2, 3):
+        items = [W.cfg2_item(s, dev()) for s in specs]
+        eng = Engine2D(items, variant=variant, graph=False)
+        eng.run(0, 1)
+        eng.run(1, 130)
+        launches.append(int(eng.last_launches))
+        outs.append(([eng.state(b) for b in range(len(specs))],
+                     [[a.clone() for a in eng.accumulators(b)] for b in range(len(specs))]))
+        eng.close()
+    (s0, a0), (s1, a1) = outs
+    errs = {}
+    for b in range(len(specs)):
+        for name in s0[b]._fields:
+            x, y = getattr(s0[b], name), getattr(s1[b], name)
+            if isinstance(x, torch.Tensor) and x.numel():
+                errs[(b, name)] = rel_l2(y.cpu().numpy(), x.cpu().numpy())
+        for q, (x, y) in enumerate(zip(a0[b], a1[b])):
+            errs[(b, f"acc{q}")] = rel_l2(y.cpu().numpy(), x.cpu().numpy())
+    print(f"\n[tb vs tiles] max relL2 {max(errs.values()):.2e}; launches {launches}")
+    bad = {k: v for k, v in errs.items() if not v < 1e-5}
+    assert not bad, bad
+    assert launches[1] < launches[0] / 2, launches
 
 
 def _grad_setup(g, dev_, requires_grad=True):
