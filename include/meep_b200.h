@@ -315,6 +315,15 @@ void mtb_yee2d_plan_destroy(mtb_yee2d_plan *plan);
 int mtb_yee2d_ring(const mtb_yee2d_plan *plan, float **ring, int64_t *slot_elems,
                    int32_t *ring_slots);
 
+/* Copy samples out of the plan's ring after a run of n_slots <= ring_slots
+ * steps (one flush): out[s * n_off + j] = ring[s * slot_elems + offsets[j]]
+ * for s < n_slots (offsets and out are device arrays; an offset outside the
+ * slot reads 0). This is the "stack" reduction of core/run.py:28-38 for
+ * probes such as PointProbe (core/monitors.py:11-21): one value per step
+ * instead of a running sum. */
+int mtb_yee2d_ring_gather(const mtb_yee2d_plan *plan, const int64_t *offsets, int32_t n_off,
+                          int32_t n_slots, float *out, void *stream);
+
 /* ---------------------------------------------------------- 2D adjoint */
 /* Discrete adjoint (reverse mode) of the TM and TE steps, the transpose of
  * core/stepper_tm.py:234-254 / core/stepper_te.py:178-190 with CPML (PEC

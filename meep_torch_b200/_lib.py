@@ -111,6 +111,7 @@ SIGNATURES = {
     "mtb_yee2d_plan_destroy": (None, [vp]),
     "mtb_yee2d_ring": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_int64),
                                  C.POINTER(C.c_int32)]),
+    "mtb_yee2d_ring_gather": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp]),
     "mtb_yee2d_adjoint_create": (C.c_int, [C.POINTER(Yee2DStruct), C.POINTER(Adj2DBuffers),
                                            C.POINTER(DftRegion), C.c_int32,
                                            C.POINTER(PhaseGroup), C.c_int32, C.c_int64,

@@ -219,6 +219,9 @@ def run_grad(state, coeffs, n_steps, *, source=None, monitors=(), checkpoint_eve
     for t in state:
         if torch.is_tensor(t) and t.requires_grad:
             raise L.MtbUnsupported("gradients with respect to the initial state on the B200 path")
+    for mon in monitors:
+        if getattr(mon, "reduce", "sum") != "sum":
+            raise L.MtbUnsupported(f"gradients through {type(mon).__name__} (stack-reduced)")
     chunk = checkpoint_every if checkpoint_every > 0 else 32
     runner = GradRun2D(state, coeffs, n_steps, source, monitors, chunk, phase_mode)
     outs = _RunFn2D.apply(runner, *[getattr(coeffs, f) for f in eps_names])

@@ -1,4 +1,4 @@
-"""2D DFT / flux monitors (reference: core/monitors.py:24-155).
+"""2D point probes, DFT and flux monitors (reference: core/monitors.py:11-155).
 
 On the B200 path the monitors are descriptors: the kernels sample the
 fields into a ring and a contraction kernel folds dt*[cos(wt) F, -sin(wt) F]
@@ -11,6 +11,17 @@ from typing import Sequence
 import torch
 
 from .grid import Grid
+
+
+class PointProbe:
+    """Ez at node (ix, iy) after every step; a run returns the k values of its steps as
+    one (k,) tensor (stack-reduced; reference interface core/monitors.py:11-21). The
+    kernels copy the node into the sample ring each step and the engine gathers the
+    ring after every flush."""
+    reduce = "stack"
+
+    def __init__(self, ix: int, iy: int):
+        self.ix, self.iy = int(ix), int(iy)
 
 
 class DFTFieldsMonitor:

@@ -155,6 +155,7 @@ constexpr int CT = 256;        // channels per contraction block
 // in shared memory, sP[s * nf + f] = (Re, Im); each thread keeps NFC
 // frequencies of its channel in registers and streams its n ring samples.
 constexpr int NFC = 4;
+constexpr int KFULL = 32;      // ring depth with a fully unrolled contraction (the default)
 __global__ void __launch_bounds__(CT) k_dft_contract(
     const mtb_dft_region *__restrict__ regions, const int *__restrict__ blk_region,
     const int64_t *__restrict__ blk_start, const int *__restrict__ group_nf,
@@ -181,6 +182,28 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
     const float *xb = (R.ring_b >= 0) ? ring + R.ring_b + (int64_t)r * R.ring_pitch + c : nullptr;
     float *acc = R.acc;
     const int64_t base = (int64_t)r * R.acc_pitch + c;
+    if (n == KFULL) {
+        // a whole ring: every sample of the channel in flight at once
+        float x[KFULL];
+#pragma unroll
+        for (int s = 0; s < KFULL; ++s) x[s] = __ldg(xa + s * slot_elems);
+        if (xb) {
+#pragma unroll
+            for (int s = 0; s < KFULL; ++s) x[s] = 0.5f * (x[s] + __ldg(xb + s * slot_elems));
+        }
+        for (int f = 0; f < nf; ++f) {
+            float re = 0.f, im = 0.f;
+#pragma unroll
+            for (int s = 0; s < KFULL; ++s) {
+                const float2 p = sP[s * nf + f];
+                re = fmaf(p.x, x[s], re);
+                im = fmaf(p.y, x[s], im);
+            }
+            acc[R.re_off + f * R.f_stride + base] += re;
+            acc[R.im_off + f * R.f_stride + base] += im;
+        }
+        return;
+    }
     for (int f0 = 0; f0 < nf; f0 += NFC) {
         float *pr[NFC], *pi[NFC];
         float re[NFC], im[NFC];
@@ -335,7 +358,8 @@ int DftState::init(const mtb_dft_region *regions, int nreg, const mtb_phase_grou
     MTB_CUDA_TRY(cudaMemcpy(gd, group_nf, sizeof(int) * (ngrp + 1), cudaMemcpyHostToDevice));
     MTB_CUDA_TRY(cudaMemcpy(gd + (ngrp + 1), freq_off, sizeof(int) * (ngrp + 1),
                             cudaMemcpyHostToDevice));
-    if (nreg && (rc = ring_d.ensure(sizeof(float) * (size_t)selems * nslots))) return rc;
+    // the ring exists whenever samples are written (DFT regions or stacked probes)
+    if (selems > 0 && (rc = ring_d.ensure(sizeof(float) * (size_t)selems * nslots))) return rc;
     return MTB_OK;
 }
 

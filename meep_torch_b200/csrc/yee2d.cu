@@ -2455,6 +2455,17 @@ static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
     return MTB_OK;
 }
 
+// out[s * n_off + j] = ring slot s at offset off[j]; offsets outside the slot read 0.
+__global__ void k_ring_gather(const float *__restrict__ ring, int64_t slot_elems,
+                              const int64_t *__restrict__ off, int n_off, int n_slots,
+                              float *__restrict__ out) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n_off * n_slots) return;
+    const int s = (int)(e / n_off), j = (int)(e - (int64_t)s * n_off);
+    const int64_t o = off[j];
+    out[e] = (o >= 0 && o < slot_elems) ? ring[s * slot_elems + o] : 0.f;
+}
+
 // One TB launch pair (TM tiles, then TE tiles) advancing C.nsub steps.
 static int launch_tb(mtb_yee2d_plan *p, const TbCtx &C, cudaStream_t st) {
     const CUtensorMap *M = p->tmaps_d.as<CUtensorMap>();
@@ -2674,6 +2685,22 @@ int32_t mtb_yee2d_pole_slot(const mtb_yee2d_plan *p) { return p ? p->pst : -1; }
 int32_t mtb_yee2d_current(const mtb_yee2d_plan *p) { return p ? p->par : -1; }
 
 int64_t mtb_yee2d_last_launches(const mtb_yee2d_plan *p) { return p ? p->last_launches : -1; }
+
+int mtb_yee2d_ring_gather(const mtb_yee2d_plan *p, const int64_t *offsets, int32_t n_off,
+                          int32_t n_slots, float *out, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (n_off < 0 || n_slots < 0 || n_slots > p->dft.slots)
+        return fail(MTB_INVALID_ARG, "ring gather: %d offsets x %d slots (ring of %d)", n_off,
+                    n_slots, p->dft.slots);
+    if ((int64_t)n_off * n_slots == 0) return MTB_OK;
+    if (!offsets || !out || !p->dft.ring_d.p)
+        return fail(MTB_INVALID_ARG, "ring gather: null offsets, output or ring");
+    const int64_t n = (int64_t)n_off * n_slots;
+    k_ring_gather<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        p->dft.ring_d.as<float>(), p->dft.slot_elems, offsets, n_off, n_slots, out);
+    MTB_CHECK_LAUNCH();
+    return MTB_OK;
+}
 
 int mtb_yee2d_ring(const mtb_yee2d_plan *p, float **ring, int64_t *slot_elems, int32_t *slots) {
     if (!p) return fail(MTB_INVALID_ARG, "plan is null");

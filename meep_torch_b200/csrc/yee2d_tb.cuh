@@ -366,8 +366,9 @@ __global__ void __launch_bounds__(TB_THREADS, 1) k_tb_tm(
         const float exb = bxE ? xpr[2 * TB_R] : 1.f, exa = bxE ? xpr[3 * TB_R] : 0.f;
         const bool byH = act && band4(jb, S.yband[0], S.yband[1]);
         const bool byE = act && dzRow && band4(jb, S.yband[2], S.yband[3]);
-        const bool yl = act && (band4(jb, S.yband[0], S.yband[1]) ||
-                                band4(jb, S.yband[2], S.yband[3]));
+        // every lane of a tile that reaches a y layer runs the CPML arithmetic (inert
+        // profiles and zero memory off the layer give the plain update): no divergence
+        const bool yl = ((wk.w >> TBF_YSHIFT) & 3) != TBF_YNONE;
         float *yp0 = L.yp + cell, *yp3 = L.yp + TB_PLANE + cell;
         const float *pr = L.prof + (k & 1) * 4 * TB_C + 4 * lane;
         const bool outC = act && lane >= 1 && lane <= 30;
@@ -617,8 +618,9 @@ __global__ void __launch_bounds__(TB_THREADS, 1) k_tb_te(
         const float exb = bxE ? xpr[2 * TB_R] : 1.f, exa = bxE ? xpr[3 * TB_R] : 0.f;
         const bool byE = act && hzRow && band4(jb, S.yband[2], S.yband[3]);
         const bool byH = act && hzRow && band4(jb, S.yband[0], S.yband[1]);
-        const bool yl = act && (band4(jb, S.yband[0], S.yband[1]) ||
-                                band4(jb, S.yband[2], S.yband[3]));
+        // every lane of a tile that reaches a y layer runs the CPML arithmetic (inert
+        // profiles and zero memory off the layer give the plain update): no divergence
+        const bool yl = ((wk.w >> TBF_YSHIFT) & 3) != TBF_YNONE;
         float *yp0 = L.yp + cell, *yp3 = L.yp + TB_PLANE + cell;
         const float *pr = L.prof + (k & 1) * 4 * TB_C + 4 * lane;
         const bool outC = act && lane >= 1 && lane <= 30;

@@ -138,6 +138,7 @@ class _Item:
     box: dict = field(default_factory=dict)      # name -> [buf0, buf1] or tensor
     keep: list = field(default_factory=list)     # tensors the plan points at
     accs: list = field(default_factory=list)
+    stacks: list = field(default_factory=list)   # point probes: (acc index, ring offset)
     amp_col: int = -1
     hamp_col: int = -1
     src_scale: object = None     # conductivity: d2 / dt on the electric source cells
@@ -197,8 +198,10 @@ class Engine2D:
             kv = getattr(c, k)
             _need(bool(torch.all(kv == 1)), f"CPML kappa != 1 ({k})")
         for mon in it.monitors:
-            _need(getattr(mon, "reduce", "sum") == "sum",
-                  f"{type(mon).__name__}: only sum-reduced monitors run on the B200 path")
+            red = getattr(mon, "reduce", "sum")
+            _need(red == "sum" or (red == "stack" and hasattr(mon, "ix") and hasattr(mon, "iy")),
+                  f"{type(mon).__name__}: only sum-reduced monitors and point probes run on "
+                  "the B200 path")
         it.pitch = _round4(it.ny)
 
     def _pack(self, src: torch.Tensor, nx, pitch, off=(0, 0)) -> torch.Tensor:
@@ -460,8 +463,20 @@ class Engine2D:
             lines = []
             ring_full = [-1, -1, -1]
             it.accs = []
+            it.stacks = []                   # (monitor index, ring offset) of point probes
             for mon in it.monitors:
                 kind = type(mon).__name__
+                if getattr(mon, "reduce", "sum") == "stack":
+                    # a point probe (core/monitors.py:11-21): Ez of one node, one value
+                    # per step (stack-reduced, core/run.py:28-38)
+                    _need(not te, f"{kind} samples Ez: a TM state")
+                    ix, iy = int(mon.ix), int(mon.iy)
+                    _need(0 <= ix < nx and 0 <= iy < ny, f"{kind} at ({ix}, {iy}) outside the grid")
+                    o = alloc_ring(1)
+                    lines.append((L.C2_MAIN, 0, ix, iy, iy + 1, o))
+                    it.stacks.append((len(it.accs), o))
+                    it.accs.append(torch.zeros(0, dtype=torch.float32, device=dev))
+                    continue
                 g, nf = group(mon.freqs, mon.dt)
                 if kind == "DFTFieldsMonitor":
                     comp = mon.component
@@ -594,9 +609,42 @@ class Engine2D:
 
     # ------------------------------------------------------------------ run
     def run(self, t0: int, k: int):
-        """Advance every structure k steps starting at step index t0."""
+        """Advance every structure k steps starting at step index t0. Point probes
+        (stack-reduced) hold the k values of this call afterwards."""
         if k <= 0:
             return
+        if any(it.stacks for it in self.items):
+            self._run_stacked(t0, k)
+            return
+        self._run(t0, k)
+
+    def _run_stacked(self, t0: int, k: int):
+        """Run in pieces of one ring flush and copy the probes' samples out after each:
+        the ring holds the samples of the last flush only."""
+        lib = self.lib
+        ring, selems, nslots = C.c_void_p(), C.c_int64(), C.c_int32()
+        L.check(lib.mtb_yee2d_ring(self.plan, C.byref(ring), C.byref(selems), C.byref(nslots)),
+                "mtb_yee2d_ring")
+        G = int(nslots.value)
+        offs, where = [], []
+        for b, it in enumerate(self.items):
+            for q, o in it.stacks:
+                where.append((b, q))
+                offs.append(o)
+        off_d = torch.tensor(offs, dtype=torch.int64, device=self.device)
+        out = torch.empty((k, len(offs)), dtype=torch.float32, device=self.device)
+        s = 0
+        while s < k:
+            n = min(G, k - s)
+            self._run(t0 + s, n)
+            L.check(lib.mtb_yee2d_ring_gather(self.plan, L.ptr(off_d), len(offs), n,
+                                              L.ptr(out[s:]), self._sptr()),
+                    "mtb_yee2d_ring_gather")
+            s += n
+        for j, (b, q) in enumerate(where):
+            self.items[b].accs[q] = out[:, j].clone()
+
+    def _run(self, t0: int, k: int):
         nc = max(self.n_amp_cols, 1)
         ce = np.zeros((k, nc), dtype=np.float64)
         ch = np.zeros((k, nc), dtype=np.float64)
@@ -624,6 +672,8 @@ class Engine2D:
                 list(it.box.get("pol_y", []))
             for t in bufs:
                 n = t.numel()
+                if n == 0:
+                    continue
                 L.check(self.lib.mtb_pack(0, 0, 0, 0, 0, 0, L.ptr(t), 1, 1, n, n, n, 0, 0, 0,
                                           self._sptr()), "reset")
 

@@ -57,3 +57,38 @@ def run_sharded(costs: Sequence[float], run_share: Callable[[list[int]], list], 
         for i, res in share:
             out[i] = res
     return out
+
+
+def distributed_gradient(term_grad: Callable[[list[int]], tuple], n_terms: int, *,
+                         rank: int = 0, world: int = 1, group=None, costs=None):
+    """Objective and design gradient of a sum of independent terms, split across ranks.
+
+    Design objectives are often sums of terms that each need their own forward + adjoint
+    FDTD pair: one per narrowband wavelength, per excitation, or per fabrication scenario
+    (nominal / eroded / dilated) of a robust design. ``term_grad(indices)`` evaluates the
+    terms ``indices`` on this rank and returns (sum of their objective values, sum of their
+    gradients as one tensor). The terms are split by LPT on ``costs`` (default: equal), and
+    one all-reduce sums the objectives and gradients, so every rank returns the same
+    (J, dJ/drho). A rank with no term contributes zeros (it still joins the collective)."""
+    import torch
+    parts = lpt_partition(costs if costs is not None else [1.0] * n_terms, world)
+    mine = parts[rank]
+    J, g = term_grad(mine) if mine else (0.0, None)
+    if world == 1:
+        return float(J), g
+    import torch.distributed as dist
+    # the gradient's shape is the same on every rank; ranks without a term learn it here
+    shape = torch.tensor(list(g.shape) if g is not None else [], dtype=torch.int64)
+    meta = [None] * world
+    dist.all_gather_object(meta, (tuple(shape.tolist()), str(g.dtype) if g is not None
+                                  else None), group=group)
+    ref_shape, ref_dtype = next(m for m in meta if m[1] is not None)
+    dev = g.device if g is not None else torch.device("cpu")
+    flat = torch.zeros(1 + int(torch.tensor(ref_shape).prod()), dtype=torch.float64,
+                       device=dev)
+    flat[0] = float(J)
+    if g is not None:
+        flat[1:] = g.detach().reshape(-1).to(torch.float64)
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    out_dtype = getattr(torch, ref_dtype.replace("torch.", ""))
+    return float(flat[0]), flat[1:].reshape(ref_shape).to(out_dtype)

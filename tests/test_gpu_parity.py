@@ -514,6 +514,57 @@ def test_tb_matches_tiles_on_a_cfg2_batch():
     assert launches[1] < launches[0] / 2, launches
 
 
+@pytest.mark.parametrize("variant", [2, 3])
+def test_point_probes_stack_every_step(variant):
+    """PointProbe (reduce "stack", core/monitors.py:11-21) next to a flux line: the run
+    returns Ez at the probe node after every step, over several ring flushes and two
+    run calls, equal to the oracle's per-step values; the flux accumulator still sums."""
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import FluxMonitorTM, PointProbe
+    from meep_torch_b200.core.run import _run_chunk
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    nx, ny, dx, npml = 60, 140, 0.05, 8
+    rng = np.random.default_rng(31)
+    eps = np.ones((nx, ny), dtype=np.float32)
+    eps[:, 60:80] = 12.0
+    eps[30:40, 20:50] = rng.uniform(2, 8, (10, 30))
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    m = build_tm_coeffs(grid, eps_inf=torch.from_numpy(eps), npml=npml)
+    src = LineSource(grid, ix=12, j0=60, j1=80, profile=GaussianPulse(0.65, 0.3))
+    probes = [PointProbe(20, 70), PointProbe(45, 130)]
+    freqs = [0.6, 0.7]
+    flux = FluxMonitorTM(grid, freqs, x_normal=True, idx=40, lo=10, hi=130)
+    c = O.tm_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float32)
+    mask = O.line_source_mask(nx, ny, dx, 12, 60, 80, dtype=np.float32)
+    op = O.gaussian_pulse(0.65, 0.3)
+    rec = []
+    so, (ao,) = O.run_2d(
+        O.tm_step, O.tm_state(c), c, 90, amp_fn=lambda t: op(O.src_time(t, c["dt"])),
+        mask=mask, monitors=[lambda s, t: (rec.append([s["Ez"][20, 70], s["Ez"][45, 130]]),
+                                           O.flux_tm_sample(s, t, c["dt"], freqs, True, 40, 10,
+                                                            130, np.float32))[1]])
+    rec = np.array(rec, dtype=np.float64)
+    from meep_torch_b200.engine2d import Engine2D
+    eng = Engine2D([(init_tm_state(grid), m, src, [probes[0], flux, probes[1]])],
+                   variant=variant, ring_slots=16)
+    eng.run(0, 50)
+    p0a, _, p1a = eng.accumulators(0)
+    eng.run(50, 40)
+    p0b, acc, p1b = eng.accumulators(0)
+    eng.close()
+    got = np.stack([torch.cat([p0a, p0b]).cpu().double().numpy(),
+                    torch.cat([p1a, p1b]).cpu().double().numpy()], axis=1)
+    assert got.shape == (90, 2)
+    assert rel_l2(got, rec) < TOL, rel_l2(got, rec)
+    assert rel_l2(acc.cpu().numpy(), ao) < TOL
+    # through the reference's seam: _run_chunk returns the stack as the probe's output
+    st, outs = _run_chunk(None, init_tm_state(grid), m, 0, 20, src, [probes[0]])
+    assert outs[0].shape == (20,)
+    assert rel_l2(outs[0].cpu().numpy(), rec[:20, 0]) < TOL
+
+
 def _grad_setup(g, dev_, requires_grad=True):
     from meep_torch_b200.core.coeffs import build_tm_coeffs
     from meep_torch_b200.core.grid import Grid

@@ -88,3 +88,60 @@ def test_run_sharded_gathers_in_batch_order_two_ranks():
 def test_run_sharded_single_rank_needs_no_collective():
     out = run_sharded([3, 1, 2], lambda idx: [i * 2 for i in idx])
     assert out == [0, 2, 4]
+
+
+def _term(i):
+    """A stand-in objective term i and its gradient over a 4 x 5 design."""
+    import torch
+    rho = torch.linspace(0, 1, 20, dtype=torch.float64).reshape(4, 5)
+    return float((i + 1) * rho.sum()), (i + 1) * torch.cos(rho + i)
+
+
+def _grad_worker(rank, world, port, n_terms, q):
+    import torch
+    import torch.distributed as dist
+
+    from meep_torch_b200.shard import distributed_gradient
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        seen = []
+
+        def term_grad(idx):
+            seen.extend(idx)
+            J, g = 0.0, torch.zeros(4, 5, dtype=torch.float64)
+            for i in idx:
+                a, b = _term(i)
+                J, g = J + a, g + b
+            return J, g
+
+        J, g = distributed_gradient(term_grad, n_terms, rank=rank, world=world)
+        q.put((rank, seen, J, g.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n_terms", [(2, 3), (3, 2)])
+def test_distributed_gradient_sums_terms_across_ranks(world, n_terms):
+    """Objective terms (wavelengths / scenarios) split over gloo ranks: every rank ends with
+    the single-process sum of objectives and gradients, each term evaluated exactly once;
+    a rank without a term (3 ranks, 2 terms) still joins the all-reduce."""
+    import torch
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_grad_worker, args=(r, world, port, n_terms, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    J_ref = sum(_term(i)[0] for i in range(n_terms))
+    g_ref = sum(_term(i)[1] for i in range(n_terms))
+    assert sorted(i for r in res for i in r[1]) == list(range(n_terms))
+    for rank, seen, J, g in res:
+        assert abs(J - J_ref) < 1e-12 * abs(J_ref)
+        assert torch.allclose(torch.tensor(g, dtype=torch.float64), g_ref, rtol=1e-14)
