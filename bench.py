@@ -907,7 +907,7 @@ def reference_cpu(wl, args, threads):
     cores = torch.get_num_threads()
     from meep_torch_b200 import workloads as W
     if wl == "cfg2":
-        n_s, steps = args.ref_structs, args.ref_steps or 150
+        n_s, steps = args.ref_structs, args.ref_steps or 500
         cells, sec = ref_cfg2(W.cfg2_specs()[:n_s], steps)
         return (cells / sec / 1e9, "Gcell-updates/s", cores,
                 f"reference meep_torch run_tm / run_te (float32, no_grad, {cores} torch "
@@ -1052,7 +1052,7 @@ def main():
     ap.add_argument("--ring", type=int, default=0, help="DFT ring depth (0 = default)")
     ap.add_argument("--cpu-structs", type=int, default=0, help="0 = host threads, 8..64")
     ap.add_argument("--cpu-steps", type=int, default=300)
-    ap.add_argument("--ref-structs", type=int, default=4,
+    ap.add_argument("--ref-structs", type=int, default=16,
                     help="cfg2 structures of the reference's own CPU run (reference arm)")
     ap.add_argument("--ref-steps", type=int, default=0,
                     help="time steps of the reference's own CPU sample (0 = per workload)")
@@ -1274,12 +1274,16 @@ def main():
         with open(prof) as f:
             tr = json.load(f)
         eff = args.variant or (3 if args.workload == "cfg2" else 2)   # library defaults
-        if tr.get("variant") == eff:
-            traffic = tr.get("dram_bytes_per_launch")
+        entry = tr.get("variants", {}).get(str(eff)) if "variants" in tr else (
+            tr if tr.get("variant") == eff else None)
+        if entry and round(entry.get("steps_per_launch", 1)) == round(steps_per_launch):
+            traffic = entry.get("dram_bytes_per_launch")
     e2e_val = (total_updates / r["e2e_s"] / 1e9
                if r["e2e_s"] == r["e2e_s"] else None)
-    kernel = ("k_tile_tm (one step; graph replays, step time = run time / steps)"
-              if args.workload == "cfg1" and args.variant != 1 else
+    kernel = ("k_tb_tm (temporally blocked, 4 steps per launch; graph replays, step time = "
+              "run time / steps)" if args.workload == "cfg1" and args.variant in (0, 3) else
+              "k_tile_tm (one step; graph replays, step time = run time / steps)"
+              if args.workload == "cfg1" and args.variant == 2 else
               "k_yee2d_tm (one step; graph replays, step time = run time / steps)"
               if args.workload == "cfg1" else
               "k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else

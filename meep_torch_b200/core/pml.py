@@ -54,3 +54,24 @@ def cpml_profiles(n, npml, offset, dt, dx, m=3, R0=1e-6, alpha_max=0.05,
     a[active] = sigma[active] * (b[active] - 1.0) / (sigma[active] + alpha[active])
     out = lambda v: torch.tensor(v, dtype=dtype, device=device)  # noqa: E731
     return out(b), out(a), torch.ones(n, dtype=dtype, device=device)
+
+
+def absorber_sigma(n: int, nabs, dx: float, *, R0: float = 1e-15, m: int = 2,
+                   dtype=torch.float32, device="cpu") -> torch.Tensor:
+    """Conductivity of a matched absorber (meep's Absorber; reference interface
+    core/pml.py:62-80) along an axis of n cells: zero inside, and over the n_side cells
+    of each layer a ramp sigma_max u^m of the cell-centre depth u = (n_side - i - 1/2) /
+    n_side counted from the outer edge, with sigma_max = (m + 1) ln(1 / R0) / (2 n_side
+    dx). The same curve damps D and B (sigma_d = sigma_b)."""
+    n_lo, n_hi = side_counts(nabs)
+    sig = np.zeros(n)
+    for count, edge in ((n_lo, "lo"), (n_hi, "hi")):
+        if count <= 0:
+            continue
+        peak = (m + 1) * math.log(1.0 / R0) / (2.0 * count * dx)
+        ramp = peak * ((count - np.arange(count) - 0.5) / count) ** m
+        if edge == "lo":
+            sig[:count] = ramp
+        else:
+            sig[n - count:] = ramp[::-1]
+    return torch.tensor(sig, dtype=dtype, device=device)

@@ -1,14 +1,15 @@
 """3D coefficients and state (reference: core/stepper_3d.py:28-67, :150-292).
 
-CPML boundary only (the reference's matched-sigma absorber, conductivity,
-poles and PMC walls are not on the B200 path). dt = 0.5 dx / sqrt(3).
+Boundaries: CPML, the matched-sigma absorber, or CPML on some axes and the absorber on
+others; conductivity and ADE poles. PMC walls are not on the B200 path. dt = 0.5 dx /
+sqrt(3).
 """
 import math
 from typing import NamedTuple
 
 import torch
 
-from .pml import cpml_profiles, side_counts
+from .pml import absorber_sigma, cpml_profiles, side_counts
 
 
 class Coeffs3D(NamedTuple):
@@ -68,13 +69,28 @@ def _avg3(v, axis):
     return 0.5 * (v[tuple(a)] + v[tuple(b)])
 
 
+def _inert(n, ax, dtype, device):
+    """A profile that leaves the derivative plain and the CPML memory at zero (b = 1,
+    a = 0, kappa = 1): the kernels never touch the memory of such a node."""
+    sh = [1, 1, 1]
+    sh[ax] = n
+    return (torch.ones(sh, dtype=dtype, device=device), torch.zeros(sh, dtype=dtype,
+                                                                     device=device),
+            torch.ones(sh, dtype=dtype, device=device))
+
+
 def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
                     dtype=torch.float32, device="cuda", sigma_d=None, sigma_b=None,
-                    poles=(), pole_masks=None, **kw) -> Coeffs3D:
-    """CPML coefficients: H-side profiles on the n-1 half nodes, E-side on the
-    interior [1:-1] of each axis (core/stepper_3d.py:192-206); with ``sigma_d`` /
-    ``sigma_b`` ((nx, ny, nz) cell-centred), the damping pairs of :217-235 Yee-averaged
-    onto each component; with ``poles`` / ``pole_masks`` the ADE stacks of :236-266."""
+                    poles=(), pole_masks=None, n_abs=0, absorber_axes=(), absorber_m: int = 2,
+                    absorber_R0: float = 1e-15, **kw) -> Coeffs3D:
+    """Coefficients of the 3D step (core/stepper_3d.py:150-266). Boundaries as the
+    reference offers them: CPML (``npml``), the matched-sigma absorber (``n_abs`` with
+    ``npml = 0``: no CPML, the absorber's conductivity damps D and B), or both (CPML on
+    the axes not in ``absorber_axes``, plain derivatives plus the absorber on those).
+    CPML profiles: H side on the n-1 half nodes, E side on the interior [1:-1] of each
+    axis (:192-206). With ``sigma_d`` / ``sigma_b`` ((nx, ny, nz) cell-centred, added to
+    the absorber's), the damping pairs of :217-235 Yee-averaged onto each component;
+    with ``poles`` / ``pole_masks`` the ADE stacks of :236-266."""
     for k, v in kw.items():
         if v not in (None, 0, (), []):
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
@@ -82,15 +98,37 @@ def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
     e = (eps.to(dtype=dtype, device=device) if isinstance(eps, torch.Tensor)
          else torch.ones(nx, ny, nz, dtype=dtype, device=device))
     dims = (nx, ny, nz)
-    npml_ax = _axis_sides3(npml)
-    if not any(l or h for l, h in npml_ax):
-        raise NotImplementedError("npml = 0 (absorber / PEC box): the B200 path runs the CPML form")
-    cpml = {}
-    for ax, kh, ke in ((0, "hx", "ex"), (1, "hy", "ey"), (2, "hz", "ez")):
-        b, a, k = cpml_profiles(dims[ax] - 1, npml_ax[ax], 0.5, dt, dx, dtype=dtype, device=device)
-        cpml[kh] = (_bc(b, ax), _bc(a, ax), _bc(k, ax))
-        b, a, k = cpml_profiles(dims[ax], npml_ax[ax], 0.0, dt, dx, dtype=dtype, device=device)
-        cpml[ke] = (_bc(b[1:-1], ax), _bc(a[1:-1], ax), _bc(k[1:-1], ax))
+    npml_ax, nabs_ax = _axis_sides3(npml), _axis_sides3(n_abs)
+    has_pml = any(l or h for l, h in npml_ax)
+    has_abs = any(l or h for l, h in nabs_ax)
+    if not has_pml and not has_abs:
+        raise NotImplementedError("a PEC box without CPML or absorber is not on the B200 path")
+    abs_axes = set(absorber_axes) if (has_pml and has_abs) else {0, 1, 2} if has_abs else set()
+    cpml = None
+    if has_pml:
+        cpml = {}
+        for ax, kh, ke in ((0, "hx", "ex"), (1, "hy", "ey"), (2, "hz", "ez")):
+            if ax in abs_axes:
+                cpml[kh] = _inert(dims[ax] - 1, ax, dtype, device)
+                cpml[ke] = _inert(dims[ax] - 2, ax, dtype, device)
+                continue
+            b, a, k = cpml_profiles(dims[ax] - 1, npml_ax[ax], 0.5, dt, dx, dtype=dtype,
+                                    device=device)
+            cpml[kh] = (_bc(b, ax), _bc(a, ax), _bc(k, ax))
+            b, a, k = cpml_profiles(dims[ax], npml_ax[ax], 0.0, dt, dx, dtype=dtype, device=device)
+            cpml[ke] = (_bc(b[1:-1], ax), _bc(a[1:-1], ax), _bc(k[1:-1], ax))
+    sig_abs = None
+    if abs_axes:
+        # the boundary conductivity is the largest of the absorbing axes' ramps
+        sig_abs = torch.zeros(nx, ny, nz, dtype=dtype, device=device)
+        for ax in sorted(abs_axes):
+            ramp = absorber_sigma(dims[ax], nabs_ax[ax], dx, R0=absorber_R0, m=absorber_m,
+                                  dtype=dtype, device=device)
+            sig_abs = torch.maximum(sig_abs, _bc(ramp, ax).expand(nx, ny, nz))
+        sigma_d = sig_abs + (sigma_d.to(dtype=dtype, device=device) if sigma_d is not None
+                             else 0.0)
+        sigma_b = sig_abs + (sigma_b.to(dtype=dtype, device=device) if sigma_b is not None
+                             else 0.0)
     if sigma_d is None and sigma_b is None:
         one = torch.ones((), dtype=dtype, device=device)
         d2 = torch.full((), dt, dtype=dtype, device=device)

@@ -33,10 +33,13 @@ class _StateView:
 
 def build_lean(nx, ny, nz, dx, eps, npml, poles=(), pole_masks=None, dtype=torch.float32,
                device="cuda") -> Lean3D:
-    if len(poles):
-        raise NotImplementedError("dispersive poles: not implemented on the B200 path")
-    c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, dtype=dtype, device=device)
-    st = init_3d_state(nx, ny, nz, npml=npml, dtype=dtype, device=device)
+    """With ``poles`` / ``pole_masks`` the lean stepper's ADE poles
+    (core/stepper_3d_lean.py:143-150): the same folded-D update as the functional
+    stepper, which the split kernels' pole variant runs."""
+    c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, dtype=dtype, device=device,
+                        poles=poles, pole_masks=pole_masks)
+    st = init_3d_state(nx, ny, nz, npml=npml, dtype=dtype, device=device,
+                       n_poles=len(poles))
     return Lean3D(dt=c.dt, dx=dx, nx=nx, ny=ny, nz=nz, npml=npml, coeffs=c, F=st._asdict())
 
 

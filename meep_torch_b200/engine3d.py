@@ -25,6 +25,24 @@ POLES = ("Px_cur", "Px_prev", "Py_cur", "Py_prev", "Pz_cur", "Pz_prev")
 PSI_OFF = ((0, 0, 0),) * 6 + ((0, 1, 0), (0, 0, 1), (0, 0, 1), (1, 0, 0), (1, 0, 0), (0, 1, 0))
 
 
+def _plain_profiles(cpml, dims):
+    """The CPML profiles the kernels read: inert (b = 1, a = 0, kappa = 1) on every axis
+    when there is no CPML (the absorber-only boundary, cpml None), and inert where the
+    reference writes its plain-derivative profile (b = 0, a = 0: the memory is reset to
+    zero every step, so b = 1 with memory left at zero is the same update)."""
+    out = {}
+    for ax, (kh, ke) in enumerate((("hx", "ex"), ("hy", "ey"), ("hz", "ez"))):
+        for key, n in ((kh, dims[ax] - 1), (ke, dims[ax] - 2)):
+            if cpml is None:
+                b, a, k = (torch.ones(n), torch.zeros(n), torch.ones(n))
+            else:
+                b, a, k = cpml[key]
+                plain = (a == 0) & (b == 0)
+                b = torch.where(plain, torch.ones_like(b), b)
+            out[key] = (b, a, k)
+    return out
+
+
 def field_shapes(nx, ny, nz):
     return {"Ex": (nx - 1, ny, nz), "Ey": (nx, ny - 1, nz), "Ez": (nx, ny, nz - 1),
             "Hx": (nx, ny - 1, nz - 1), "Hy": (nx - 1, ny, nz - 1), "Hz": (nx - 1, ny - 1, nz)}
@@ -75,8 +93,11 @@ class Engine3D:
         shapes = field_shapes(nx, ny, nz)
         for k in FIELDS:
             _need(tuple(g[k].shape) == shapes[k], f"{k} shape {tuple(g[k].shape)}")
-        _need(all(g.get(k) is not None for k in PSI), "3D CPML memory (npml > 0) required")
-        _need(getattr(coeffs, "cpml", None) is not None, "matched-sigma absorber mode")
+        # without CPML memory in the state (the absorber-only boundary) the engine keeps
+        # zero memory of its own, which inert profiles leave untouched
+        self.own_psi = all(g.get(k) is None for k in PSI)
+        _need(self.own_psi or all(g.get(k) is not None for k in PSI),
+              "3D CPML memory: all twelve arrays or none")
         pols = getattr(coeffs, "pols", None)
         n_p = 0 if pols is None else int(pols["x"][2].shape[0])
         _need(n_p <= L.MTB_MAX_POLES, f"{n_p} dispersive poles (at most {L.MTB_MAX_POLES})")
@@ -100,15 +121,22 @@ class Engine3D:
             pair = self._pair(g[k])
             self.box[k] = pair
             S.f[q][0], S.f[q][1] = L.ptr(pair[0]), L.ptr(pair[1])
+        zero_box = (torch.zeros((nx, ny, zp), dtype=torch.float32, device=self.device)
+                    if self.own_psi else None)
         for q, k in enumerate(PSI):
-            pair = self._pair(g[k], PSI_OFF[q])
+            if self.own_psi:
+                # inert profiles everywhere: the kernels never read or write this memory,
+                # so one zero box serves all twelve arrays and both buffers
+                pair = [zero_box, zero_box]
+            else:
+                pair = self._pair(g[k], PSI_OFF[q])
             self.box[k] = pair
             S.psi[q][0], S.psi[q][1] = L.ptr(pair[0]), L.ptr(pair[1])
         eps = coeffs.eps
         _need(tuple(eps.shape) == (nx, ny, nz), "eps must be cell-centred (nx, ny, nz)")
         self.eps_box = self._pack(eps.to(self.device))
         S.eps = L.ptr(self.eps_box)
-        cp = coeffs.cpml
+        cp = _plain_profiles(coeffs.cpml, (nx, ny, nz))
         dims = (nx, ny, nz)
         for ax, (kh, ke) in enumerate((("hx", "ex"), ("hy", "ey"), ("hz", "ez"))):
             bH, aH, kH = cp[kh]
@@ -120,7 +148,8 @@ class Engine3D:
             S.prof_b[ax][0], S.prof_a[ax][0] = L.ptr(hb), L.ptr(ha)
             S.prof_b[ax][1], S.prof_a[ax][1] = L.ptr(eb), L.ptr(ea)
             self.keep += [hb, ha, eb, ea]
-        self._check_psi(g, cp)
+        if not self.own_psi:
+            self._check_psi(g, cp)
         # dispersive poles (core/stepper_3d.py:236-300): P stacks ping-pong with the fields
         self.n_poles = n_p
         if n_p:
@@ -433,7 +462,8 @@ class Engine3D:
                       (nx, ny - 1, nz - 2), (nx - 2, ny - 1, nz), (nx - 2, ny, nz - 1),
                       (nx, ny - 2, nz - 1)]
         for q, k in enumerate(PSI):
-            out[k] = self._unpack(self.box[k][cur], psi_shapes[q], PSI_OFF[q])
+            out[k] = (None if self.own_psi else
+                      self._unpack(self.box[k][cur], psi_shapes[q], PSI_OFF[q]))
         if self.n_poles:
             nxb = self.nx
             for key in "xyz":

@@ -14,7 +14,8 @@ float32 (the parity target) and float64 (the error floor), on all host threads:
   faces, ``build_3d_coeffs`` + ``run_3d`` (core/monitors_3d.py:192), 2000 steps;
 * cfg4: the 600 x 400 design problem's objective and d J / d rho through the reference's
   ``OptimizationProblem`` (adjoint/problem.py:97) over ``run_tm(checkpoint_every=256)``,
-  8000 steps.
+  8000 steps; and (``cfg4fd``, float64 only) central finite differences of the objective on
+  32 random design pixels.
 
 The inputs are the seeded synthetic configurations of ``meep_torch_b200.workloads``
 (numpy only). The fixtures stay small: monitor accumulators and flux spectra in full
@@ -208,10 +209,56 @@ def cfg4_case(prec, steps=None):
     return dict(n_steps=n, rho0=rho0, J=float(J), grad=np.asarray(g, dtype=np.float64))
 
 
+def cfg4_fd_case(n_pix=32, h=1e-4, steps=None):
+    """Central differences of the float64 reference objective on n_pix random design
+    pixels (np.random.default_rng(4): rho0 first, then the pixels), step h:
+    (J(rho + h e_p) - J(rho - h e_p)) / 2h through OptimizationProblem.eval_at_delta
+    (adjoint/problem.py:105-110), 8000 steps, checkpointing irrelevant (no_grad)."""
+    from meep_torch.adjoint.problem import DesignRegion, MaterialGrid, OptimizationProblem
+    c = W.CFG4
+    nx, ny, dx, npml = c["nx"], c["ny"], c["dx"], c["npml"]
+    n = steps or c["steps"]
+    dt_ = torch.float64
+    rng = np.random.default_rng(4)
+    rho0 = rng.uniform(0.4, 0.6, (c["design"], c["design"]))
+    pix = rng.choice(c["design"] * c["design"], n_pix, replace=False)
+    base = torch.full((nx, ny), c["eps_bg"], dtype=dt_)
+    y0, y1 = ny // 2 - c["guide_w"] // 2, ny // 2 + c["guide_w"] // 2
+    base[:, y0:y1] = c["eps_core"]
+    d = c["design"]
+    ix0, iy0 = nx // 2 - d // 2, ny // 2 - d // 2
+    reg = DesignRegion(MaterialGrid((d, d), c["eps_bg"], c["eps_core"]),
+                       ix0=ix0, ix1=ix0 + d, iy0=iy0, iy1=iy0 + d)
+    grid = Grid(nx=nx, ny=ny, dx=dx, dtype=dt_, device="cpu")
+    src = LineSource(grid, ix=npml + 10, j0=y0 - 10, j1=y1 + 10,
+                     profile=GaussianPulse(0.645, 0.12))
+    mon = FluxMonitorTM(grid, list(c["freqs"]), x_normal=True, idx=nx - npml - 10,
+                        lo=y0 - 20, hi=y1 + 20)
+
+    def run_fn(eps):
+        m = build_tm_coeffs(grid, eps_inf=eps, npml=npml)
+        _, (acc,) = run_tm(init_tm_state(grid), m, n, source=src, monitors=[mon])
+        return mon.flux(acc, dx).mean()
+
+    opt = OptimizationProblem(run_fn, base, reg, filter_radius=c["radius"], dx=dx,
+                              beta=c["beta"], eta=c["eta"], rho0=torch.tensor(rho0, dtype=dt_))
+    fd = []
+    for p in pix:
+        i, j = int(p) // d, int(p) % d
+        fd.append((opt.eval_at_delta(i, j, h) - opt.eval_at_delta(i, j, -h)) / (2 * h))
+        print(f"  pixel {i},{j}: {fd[-1]:.6e}", flush=True)
+    return dict(n_steps=n, h=h, pixels=np.asarray(pix), fd=np.asarray(fd))
+
+
 def main(argv):
     torch.set_num_threads(os.cpu_count() or 1)
-    which = argv or ["cfg1", "cfg2", "cfg3", "cfg4"]
+    which = argv or ["cfg1", "cfg2", "cfg3", "cfg4", "cfg4fd"]
     for w in which:
+        if w == "cfg4fd":                       # float64 only
+            t0 = time.time()
+            np.savez_compressed(os.path.join(HERE, "config_cfg4_fd_f64.npz"), **cfg4_fd_case())
+            print(f"cfg4fd f64: {time.time() - t0:.1f} s", flush=True)
+            continue
         for prec in ("f32", "f64"):
             t0 = time.time()
             if w == "cfg1":

@@ -158,3 +158,18 @@ def test_cfg4_gradient_matches_reference():
           f"dJ/drho relL2 vs ref fp32 {out['f32'][1]:.2e} fp64 {out['f64'][1]:.2e}")
     assert out["f64"][0] < TOL and out["f32"][0] < TOL, out
     assert out["f64"][1] < GRAD_TOL, out
+
+
+def test_cfg4_gradient_matches_central_differences():
+    """The kernels' d J / d rho (float32 adjoint) on the 32 random design pixels against
+    central differences of the reference's float64 objective (h = 1e-4, 8000 steps)."""
+    from meep_torch_b200 import workloads as W
+    fd = _fixture("cfg4_fd_f64")
+    g64 = _fixture("cfg4_f64")
+    opt, n = W.cfg4_setup("cuda", steps=int(fd["n_steps"]))
+    opt.rho = torch.tensor(g64["rho0"], dtype=torch.float32, device="cuda")
+    _, g = opt()
+    g = np.asarray(g, dtype=np.float64).reshape(-1)[fd["pixels"]]
+    e = rel_l2(g, fd["fd"])
+    print(f"\n[cfg4 FD] {len(g)} pixels: dJ/drho relL2 vs central differences {e:.2e}")
+    assert e < GRAD_TOL, e

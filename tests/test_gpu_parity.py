@@ -164,7 +164,11 @@ def _run3d(lean, variant=0, case=None):
     prof = GaussianPulse(float(g["fcen"]), float(g["fwidth"]))
     i, j, k = (int(v) for v in g["src"])
     if lean:
-        c = build_lean(nx, ny, nz, dx, eps, npml, device=dev())
+        lk = {}
+        if "poles" in g:
+            lk = dict(poles=json.loads(str(g["poles"])),
+                      pole_masks=[torch.tensor(m, dtype=torch.float32) for m in g["pole_masks"]])
+        c = build_lean(nx, ny, nz, dx, eps, npml, device=dev(), **lk)
         dt = c.dt
     else:
         kw = {}
@@ -174,6 +178,9 @@ def _run3d(lean, variant=0, case=None):
         if "poles" in g:
             kw = dict(poles=json.loads(str(g["poles"])),
                       pole_masks=[torch.tensor(m, dtype=torch.float32) for m in g["pole_masks"]])
+        if "n_abs" in g:
+            kw.update(n_abs=int(g["n_abs"]),
+                      absorber_axes=tuple(int(a) for a in g["absorber_axes"]))
         c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, device=dev(), **kw)
         dt = c.dt
     src = PointSource3D(dt, "Ez", i, j, k, prof)
@@ -192,16 +199,20 @@ def _run3d(lean, variant=0, case=None):
 
 @pytest.mark.parametrize("variant,lean,case", [(1, False, None), (2, False, None),
                                                 (1, True, None), (2, True, None),
-                                                (2, False, "3d_sigma"), (2, False, "3d_poles")])
+                                                (2, False, "3d_sigma"), (2, False, "3d_poles"),
+                                                (2, False, "3d_abs"), (2, False, "3d_mixed"),
+                                                (2, True, "3d_lean_poles")])
 def test_3d_matches_reference(lean, variant, case):
-    """3D golden cases; 3d_sigma adds conductive damping (sigma_d on E, sigma_b on H)."""
+    """3D golden cases; 3d_sigma adds conductive damping (sigma_d on E, sigma_b on H);
+    3d_abs is the matched-sigma absorber on every face (no CPML), 3d_mixed the absorber
+    on z beside x / y CPML (core/stepper_3d.py:150-235)."""
     st, accs, mons, dx = _run3d(lean, variant, case)
     name = case or ("3d_lean" if lean else "3d")
     e32, e64 = {}, {}
     for prec, errs in (("f32", e32), ("f64", e64)):
         g = load_golden(f"{name}_{prec}")
         keys = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]
-        if not lean:
+        if not lean and case != "3d_abs":
             keys += ["psi_Ez_y", "psi_Hx_y", "psi_Hz_x", "psi_Hy_z", "psi_Ex_z"]
             keys += [k[2:] for k in g if k.startswith("s_P")]
         for k in keys:
