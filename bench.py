@@ -936,6 +936,40 @@ def reference_cpu(wl, args, threads):
     return None
 
 
+def config_suite(args, rank, world, dev):
+    """The other single-GPU configurations measured in the same run as the default line
+    (cfg1 4000-step TM run, cfg3 256^3 2000-step run, cfg4 gradient), each with its own
+    value and, for the HBM-bound cfg3, its roofline; two warm-up and two timed steps."""
+    out = {}
+    peak, _ = peaks()
+    for wl in ("cfg1", "cfg3", "cfg4"):
+        a = argparse.Namespace(**dict(vars(args)))
+        a.workload, a.steps, a.warmup, a.no_e2e, a.run_steps = wl, 2, 2, True, 5000
+        a.rows = a.ring = 0
+        a.variant = 0
+        if wl == "cfg4":
+            r = run_cfg4(a, rank, world, dev)
+            out[wl] = {"metric": "gradient-evaluations/s",
+                       "value": r["grad_evals"] / (r["ms"] / 1e3),
+                       "ms_per_step": r["ms"] / a.steps, "steps": a.steps,
+                       "time_steps": r["nsteps"], "checkpoint_every": 256}
+            continue
+        r = (run_cfg1 if wl == "cfg1" else run_cfg3)(a, rank, world, dev)
+        total = r["cells"] * r["nsteps"] * a.steps
+        ent = {"metric": "Gcell-updates/s", "value": total / (r["ms"] / 1e3) / 1e9,
+               "ms_per_step": r["ms"] / a.steps, "steps": a.steps, "time_steps": r["nsteps"],
+               "cells": r["cells"]}
+        if wl == "cfg3":
+            avg = r["step_ms"] / max(r["step_n"], 1)
+            ach = r["bytes_launch"] / (avg / 1e3) / 1e9
+            ent["roofline"] = {"bound": "hbm", "kernel": "k_yee3d_h + k_yee3d_e (one step)",
+                               "achieved": ach, "peak": peak, "unit": "GB/s",
+                               "frac": ach / peak, "alg_bytes_per_step": r["bytes_launch"],
+                               "launch_ms": avg}
+        out[wl] = ent
+    return out
+
+
 def reference_line(args, config, threads):
     """The reference arm: the oracle port of the reference's CPU path, timed on the
     host cores on a bounded sample of the chosen workload, in that workload's metric."""
@@ -1062,6 +1096,8 @@ def main():
     ap.add_argument("--run-steps", type=int, default=5000,
                     help="time steps per run (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-suite", action="store_true",
+                    help="cfg2 at one GPU: skip the cfg1 / cfg3 / cfg4 lines measured after it")
     ap.add_argument("--n3", type=int, default=256, help="cfg3 grid side")
     ap.add_argument("--shard", default="none", choices=["none", "fixed"],
                     help="under torchrun: none = every rank its own problem (weak "
@@ -1347,6 +1383,8 @@ def main():
                                               f"thread, {sec:.1f} s"}
         else:
             line["cpu_baseline"] = cpu_baseline_line(args.cpu_structs, args.cpu_steps, threads)
+    if args.workload == "cfg2" and world == 1 and not args.no_suite:
+        line["other_configs"] = config_suite(args, rank, world, dev)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
