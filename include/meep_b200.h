@@ -229,8 +229,13 @@ typedef struct mtb_tuning {
                                tiles; PEC structures without conductivity,
                                poles or magnetic pairs; the plan's first
                                step runs on the one-step tiles);
-                               3D: 0 default (split), 1 fused x-march,
-                               2 split H / E streaming kernels              */
+                               3D: 0 default (3 where it applies, else 2),
+                               1 fused x-march (register-staged), 2 split
+                               H / E streaming kernels, 3 one-pass x-march
+                               (H and E of a plane in one kernel from
+                               TMA-staged planes; no damping or poles,
+                               zpitch <= 256; half steps and x slabs move
+                               a default plan to 2)                         */
 } mtb_tuning;
 
 typedef struct mtb_yee2d_plan mtb_yee2d_plan;
@@ -429,6 +434,11 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s,
                           mtb_yee3d_plan **out);
 int mtb_yee3d_run(mtb_yee3d_plan *plan, int64_t t0, int32_t k,
                   const double *coef, void *stream);
+/* Error flag of the one-pass kernel (variant 3): MTB_DEVICE_TIMEOUT if one of
+ * its bounded waits for a staged plane copy expired since the plan was made
+ * (the steps of that launch are incomplete). Synchronises `stream`.
+ * mtb_yee3d_run checks it before its first launch. */
+int mtb_yee3d_check(mtb_yee3d_plan *plan, void *stream);
 /* x-slab decomposition (core/monitors_3d.py:192-210 run_3d split across
  * ranks along x). The plan holds planes [lo, hi) of a larger grid as its own
  * nx planes: its first plane is the left neighbour's last plane (a halo)

@@ -127,6 +127,7 @@ SIGNATURES = {
                                         C.POINTER(PhaseGroup), C.c_int32, C.c_int64,
                                         C.POINTER(Tuning), C.POINTER(vp)]),
     "mtb_yee3d_run": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double), vp]),
+    "mtb_yee3d_check": (C.c_int, [vp, vp]),
     "mtb_yee3d_set_slab": (C.c_int, [vp, C.c_int32, C.c_int32]),
     "mtb_yee3d_begin": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double), vp]),
     "mtb_yee3d_half": (C.c_int, [vp, C.c_int32, vp]),

@@ -16,7 +16,10 @@
 // Yee-averaged in the kernel exactly as core/stepper_3d.py:_avg does.
 // Evolving arrays are ping-pong pairs because of the halo recomputation.
 #include <algorithm>
+#include <mutex>
 #include <vector>
+
+#include <cudaTypedefs.h>
 
 #include "mtb_common.cuh"
 
@@ -432,6 +435,49 @@ __device__ __forceinline__ bool inband(const Band3 &B, int a, int h, int k) {
     return k < B.lo[a][h] || k >= B.hi[a][h];
 }
 
+// Rounding of the 3D updates, written out (no multiply-add contraction is left to the
+// compiler), so that the split kernels and both paths of the one-pass kernel round
+// alike and agree bit for bit.
+__device__ __forceinline__ float y3_d(float a, float b, float rdx) {      // (a - b) / dx
+    return __fmul_rn(__fsub_rn(a, b), rdx);
+}
+// CPML-stretched derivative d + q with q = b psi + a d (kappa = 1); q is the new psi
+__device__ __forceinline__ float y3_s(float d, float b, float a, float psi, float &q) {
+    q = __fmaf_rn(b, psi, __fmul_rn(a, d));
+    return __fadd_rn(d, q);
+}
+__device__ __forceinline__ float y3_ec(float e0, float e1) {            // Yee-averaged eps
+    return __fmul_rn(0.5f, __fadd_rn(e0, e1));
+}
+// H' = H - dt curl; with damping d1 H - d2 curl
+__device__ __forceinline__ float y3_h(float h, float cu, float dt) { return __fmaf_rn(-dt, cu, h); }
+__device__ __forceinline__ float y3_hd(float h, float cu, float d1, float d2) {
+    return __fmaf_rn(-d2, cu, __fmul_rn(d1, h));
+}
+// E' = E + dt curl / eps_c (fast divide); with damping d1 E + d2 curl / eps_c; with
+// poles the folded-D forms E + (dt curl + sum P(n) - sum P(n+1)) / eps_c and
+// (d1 (eps_c E + sum P(n)) + d2 curl - sum P(n+1)) / eps_c
+__device__ __forceinline__ float y3_e(float e, float curl, float dt, float ec) {
+    return __fadd_rn(e, __fdividef(__fmul_rn(dt, curl), ec));
+}
+__device__ __forceinline__ float y3_ed(float e, float curl, float d1, float d2, float ec) {
+    return __fadd_rn(__fmul_rn(d1, e), __fdividef(__fmul_rn(d2, curl), ec));
+}
+__device__ __forceinline__ float y3_ep(float e, float curl, float dt, float ec, float spc,
+                                       float spn) {
+    return __fadd_rn(e, __fdividef(__fsub_rn(__fmaf_rn(dt, curl, spc), spn), ec));
+}
+__device__ __forceinline__ float y3_epd(float e, float curl, float d1, float d2, float ec,
+                                        float spc, float spn) {
+    return __fdividef(__fsub_rn(__fmaf_rn(d2, curl, __fmul_rn(d1, __fmaf_rn(e, ec, spc))), spn),
+                      ec);
+}
+// soft current of one cell: E + sgn v / eps_c (point) or E - v / eps_c (area / plane)
+__device__ __forceinline__ float y3_src(float e, float v, float ecomp, bool point, float sgn) {
+    return point ? __fadd_rn(e, sgn * __fmul_rn(v, __fdiv_rn(1.0f, ecomp)))
+                 : __fsub_rn(e, __fdiv_rn(v, ecomp));
+}
+
 // One parity's pointers and sizes for the split kernels.
 struct Split3 {
     const float *e[3];          // E(n)
@@ -533,33 +579,33 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_h(const __grid_consta
         const float exn = (q < 3) ? ex[q + 1] : exk;
         // Hx: valid j <= ny-2, k <= nz-2
         {
-            const float dy = (ezj[q] - ez[q]) * rdx, dz = (eyn - ey[q]) * rdx;
-            const float qy = hyb * p0[q] + hya * dy, qz = hzb[q] * p1[q] + hza[q] * dz;
+            float qy, qz;
+            const float cu = __fsub_rn(y3_s(y3_d(ezj[q], ez[q], rdx), hyb, hya, p0[q], qy),
+                                       y3_s(y3_d(eyn, ey[q], rdx), hzb[q], hza[q], p1[q], qz));
             const bool v = vyH && vz;
-            const float cu = (dy + qy) - (dz + qz);
-            const float hn = DAMP ? a1[0][q] * hx[q] - a2[0][q] * cu : hx[q] - dt * cu;
+            const float hn = DAMP ? y3_hd(hx[q], cu, a1[0][q], a2[0][q]) : y3_h(hx[q], cu, dt);
             hx[q] = v ? hn : hx[q];
             p0[q] = v ? qy : p0[q];
             p1[q] = v ? qz : p1[q];
         }
         // Hy: valid i <= nx-2, k <= nz-2
         {
-            const float dz = (exn - ex[q]) * rdx, dx = (ezi[q] - ez[q]) * rdx;
-            const float qz = hzb[q] * p2[q] + hza[q] * dz, qx = hxb * p3[q] + hxa * dx;
+            float qz, qx;
+            const float cu = __fsub_rn(y3_s(y3_d(exn, ex[q], rdx), hzb[q], hza[q], p2[q], qz),
+                                       y3_s(y3_d(ezi[q], ez[q], rdx), hxb, hxa, p3[q], qx));
             const bool v = xok && vz;
-            const float cu = (dz + qz) - (dx + qx);
-            const float hn = DAMP ? a1[1][q] * hy[q] - a2[1][q] * cu : hy[q] - dt * cu;
+            const float hn = DAMP ? y3_hd(hy[q], cu, a1[1][q], a2[1][q]) : y3_h(hy[q], cu, dt);
             hy[q] = v ? hn : hy[q];
             p2[q] = v ? qz : p2[q];
             p3[q] = v ? qx : p3[q];
         }
         // Hz: valid i <= nx-2, j <= ny-2, k < nz
         {
-            const float dx = (eyi[q] - ey[q]) * rdx, dy = (exj[q] - ex[q]) * rdx;
-            const float qx = hxb * p4[q] + hxa * dx, qy = hyb * p5[q] + hya * dy;
+            float qx, qy;
+            const float cu = __fsub_rn(y3_s(y3_d(eyi[q], ey[q], rdx), hxb, hxa, p4[q], qx),
+                                       y3_s(y3_d(exj[q], ex[q], rdx), hyb, hya, p5[q], qy));
             const bool v = xok && vyH && vzE;
-            const float cu = (dx + qx) - (dy + qy);
-            const float hn = DAMP ? a1[2][q] * hz[q] - a2[2][q] * cu : hz[q] - dt * cu;
+            const float hn = DAMP ? y3_hd(hz[q], cu, a1[2][q], a2[2][q]) : y3_h(hz[q], cu, dt);
             hz[q] = v ? hn : hz[q];
             p4[q] = v ? qx : p4[q];
             p5[q] = v ? qy : p5[q];
@@ -682,7 +728,7 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     spc[c][q] += pc[q];
-                    pq[q] = c1 * pc[q] + c2 * pq[q] + c3[q] * en[c][q];
+                    pq[q] = __fmaf_rn(c3[q], en[c][q], __fmaf_rn(c2, pq[q], __fmul_rn(c1, pc[q])));
                     spn[c][q] += pq[q];
                 }
                 st4v(P.pp[c][1] + o, pq);
@@ -697,50 +743,50 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
         const float hxkm = (q == 0) ? hxk : hx[q - 1];
         // Ex: valid i <= nx-2, k < nz; curl on j, k interior
         {
-            const float dy = (hz[q] - hzm[q]) * rdx, dz = (hy[q] - hym) * rdx;
-            const float qy = eyb * p6[q] + eya * dy, qz = ezb[q] * p7[q] + eza[q] * dz;
+            float qy, qz;
+            const float cs = __fsub_rn(y3_s(y3_d(hz[q], hzm[q], rdx), eyb, eya, p6[q], qy),
+                                       y3_s(y3_d(hy[q], hym, rdx), ezb[q], eza[q], p7[q], qz));
             const bool v = xok && vzE;
-            const float curl = (jin && kin) ? (dy + qy) - (dz + qz) : 0.f;
-            const float ec = 0.5f * (ep[q] + epi[q]);
-            en[0][q] = v ? (PL ? (DAMP ? __fdividef(a1[0][q] * (en[0][q] * ec + spc[0][q]) +
-                                                      a2[0][q] * curl - spn[0][q], ec)
-                                       : en[0][q] + __fdividef(dt * curl + spc[0][q] - spn[0][q],
-                                                               ec))
-                                 : DAMP ? a1[0][q] * en[0][q] + __fdividef(a2[0][q] * curl, ec)
-                                        : en[0][q] + __fdividef(dt * curl, ec))
+            const float curl = (jin && kin) ? cs : 0.f;
+            const float ec = y3_ec(ep[q], epi[q]);
+            en[0][q] = v ? (PL ? (DAMP ? y3_epd(en[0][q], curl, a1[0][q], a2[0][q], ec, spc[0][q],
+                                                spn[0][q])
+                                       : y3_ep(en[0][q], curl, dt, ec, spc[0][q], spn[0][q]))
+                                 : DAMP ? y3_ed(en[0][q], curl, a1[0][q], a2[0][q], ec)
+                                        : y3_e(en[0][q], curl, dt, ec))
                          : en[0][q];
             p6[q] = v ? qy : p6[q];
             p7[q] = v ? qz : p7[q];
         }
         // Ey: valid j <= ny-2, k < nz; curl on i, k interior
         {
-            const float dz = (hx[q] - hxkm) * rdx, dx = (hz[q] - hzp[q]) * rdx;
-            const float qz = ezb[q] * p8[q] + eza[q] * dz, qx = exb * p9[q] + exa * dx;
+            float qz, qx;
+            const float cs = __fsub_rn(y3_s(y3_d(hx[q], hxkm, rdx), ezb[q], eza[q], p8[q], qz),
+                                       y3_s(y3_d(hz[q], hzp[q], rdx), exb, exa, p9[q], qx));
             const bool v = vyH && vzE;
-            const float curl = (iin && kin) ? (dz + qz) - (dx + qx) : 0.f;
-            const float ec = 0.5f * (ep[q] + epj[q]);
-            en[1][q] = v ? (PL ? (DAMP ? __fdividef(a1[1][q] * (en[1][q] * ec + spc[1][q]) +
-                                                      a2[1][q] * curl - spn[1][q], ec)
-                                       : en[1][q] + __fdividef(dt * curl + spc[1][q] - spn[1][q],
-                                                               ec))
-                                 : DAMP ? a1[1][q] * en[1][q] + __fdividef(a2[1][q] * curl, ec)
-                                        : en[1][q] + __fdividef(dt * curl, ec))
+            const float curl = (iin && kin) ? cs : 0.f;
+            const float ec = y3_ec(ep[q], epj[q]);
+            en[1][q] = v ? (PL ? (DAMP ? y3_epd(en[1][q], curl, a1[1][q], a2[1][q], ec, spc[1][q],
+                                                spn[1][q])
+                                       : y3_ep(en[1][q], curl, dt, ec, spc[1][q], spn[1][q]))
+                                 : DAMP ? y3_ed(en[1][q], curl, a1[1][q], a2[1][q], ec)
+                                        : y3_e(en[1][q], curl, dt, ec))
                          : en[1][q];
             p8[q] = v ? qz : p8[q];
             p9[q] = v ? qx : p9[q];
         }
         // Ez: valid k <= nz-2; curl on i, j interior
         {
-            const float dx = (hy[q] - hyp[q]) * rdx, dy = (hx[q] - hxm[q]) * rdx;
-            const float qx = exb * p10[q] + exa * dx, qy = eyb * p11[q] + eya * dy;
-            const float curl = (iin && jin) ? (dx + qx) - (dy + qy) : 0.f;
-            const float ec = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
-            en[2][q] = vz ? (PL ? (DAMP ? __fdividef(a1[2][q] * (en[2][q] * ec + spc[2][q]) +
-                                                       a2[2][q] * curl - spn[2][q], ec)
-                                        : en[2][q] + __fdividef(dt * curl + spc[2][q] - spn[2][q],
-                                                                ec))
-                                  : DAMP ? a1[2][q] * en[2][q] + __fdividef(a2[2][q] * curl, ec)
-                                         : en[2][q] + __fdividef(dt * curl, ec))
+            float qx, qy;
+            const float cs = __fsub_rn(y3_s(y3_d(hy[q], hyp[q], rdx), exb, exa, p10[q], qx),
+                                       y3_s(y3_d(hx[q], hxm[q], rdx), eyb, eya, p11[q], qy));
+            const float curl = (iin && jin) ? cs : 0.f;
+            const float ec = y3_ec(ep[q], (q < 3) ? ep[q + 1] : epk);
+            en[2][q] = vz ? (PL ? (DAMP ? y3_epd(en[2][q], curl, a1[2][q], a2[2][q], ec, spc[2][q],
+                                                 spn[2][q])
+                                        : y3_ep(en[2][q], curl, dt, ec, spc[2][q], spn[2][q]))
+                                  : DAMP ? y3_ed(en[2][q], curl, a1[2][q], a2[2][q], ec)
+                                         : y3_e(en[2][q], curl, dt, ec))
                           : en[2][q];
             p10[q] = vz ? qx : p10[q];
             p11[q] = vz ? qy : p11[q];
@@ -760,13 +806,12 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
                 if (c == 0) epn = epi[q];
                 else if (c == 1) epn = epj[q];
                 else epn = (q < 3) ? ep[q + 1] : epk;
-                const float ecomp = 0.5f * (ep[q] + epn);
-                const float v = a * __ldg(P.src_w + e);
+                const float ecomp = y3_ec(ep[q], epn);
+                const float v = __fmul_rn(a, __ldg(P.src_w + e));
 #pragma unroll
                 for (int cc = 0; cc < 3; ++cc) {         // static component index
                     if (cc != c) continue;
-                    if (P.src_is_point) en[cc][q] += sgn * (v * (1.0f / ecomp));
-                    else en[cc][q] -= v / ecomp;
+                    en[cc][q] = y3_src(en[cc][q], v, ecomp, P.src_is_point != 0, sgn);
                 }
             }
         }
@@ -808,6 +853,8 @@ __global__ void k_sample3d(const mtb_yee3d_struct *__restrict__ SS, const int64_
 
 }  // namespace mtb
 
+#include "yee3d_xm.cuh"
+
 using namespace mtb;
 
 struct mtb_yee3d_plan {
@@ -816,7 +863,14 @@ struct mtb_yee3d_plan {
     PinnedPair amp_h;
     int rows = 32;
     int nzw = 1;
-    int variant = 2;               // 1 fused x-march, 2 split H / E
+    int variant = 2;               // 1 fused x-march, 2 split H / E, 3 one-pass TMA x-march
+    bool chosen = false;           // variant 3 picked by default (half steps and slabs
+                                   // fall back to the split kernels)
+    XmMaps xm{};                   // variant 3: tensor maps of E (both buffers) and eps
+    int xm_v = 0, xm_grid = 0, xm_tiles = 0;
+    DevBuf err_d;                  // variant 3: bounded-wait error flag
+    DevBuf ptab_d;                 // variant 3: masked CPML profiles (XmMaps::ptab)
+    DevBuf share_d;                // variant 3: unit range of each block (xm_grid + 1)
     Band3 band{};
     Split3 sp[2]{};                // split-kernel parameters of parity 0 and 1
     int slab = 0;                  // split kernels: x planes per H / E launch pair
@@ -868,6 +922,164 @@ static int set_smem3d(size_t smem) {
     return MTB_OK;
 }
 
+// ---------------------------------------------------------------- one-pass x-march set-up
+static PFN_cuTensorMapEncodeTiled_v12000 tmap3_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+// A 3D float32 tensor map over one box array (nx planes x ny rows x zp floats), box
+// of bz x by x 1; reads outside the array return zero.
+static int tmap_3d(CUtensorMap *m, const float *base, int nx, int ny, int zp, int bz, int by) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap3_encoder();
+    if (!enc) return fail(MTB_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[3] = {(cuuint64_t)zp, (cuuint64_t)ny, (cuuint64_t)nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)zp * sizeof(float),
+                                   (cuuint64_t)zp * ny * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MTB_CUDA_ERROR, "3D tensor map encoding failed (%d)", (int)r);
+    return MTB_OK;
+}
+
+// tile height per z width: (TY + 1) * V warps within 64 KB of registers without spills
+template <int V> constexpr int xm_ty() { return V == 1 ? 8 : 5; }
+static_assert(sizeof(Split3) + sizeof(XmMaps) + 64 <= 4096, "kernel parameters exceed 4 KB");
+
+template <int V>
+static int xm_setup(mtb_yee3d_plan *p) {
+    constexpr int TY = xm_ty<V>();
+    using Sh = XmShape<V, TY>;
+    const mtb_yee3d_struct &S = p->s;
+    int rc;
+    // z-layer boxes: every float4 of z-layer cells (H or E side) lies below zl or at /
+    // above zh, both multiples of 4, each box XM_BZ wide
+    const Band3 &B = p->band;
+    const int lo = std::max(B.lo[2][0], B.lo[2][1]), hi = std::min(B.hi[2][0], B.hi[2][1]);
+    const int zl = (lo + 3) / 4 * 4, zh = hi / 4 * 4;
+    p->xm.npz = (lo > 0 || hi < S.nz - 1) ? 1 : 0;
+    p->xm.zl = p->xm.npz ? zl : 0;
+    p->xm.zh = p->xm.npz ? zh : (1 << 30);
+    if (p->xm.npz && (zl > XM_BZ || S.zpitch - zh > XM_BZ || zh < 0))
+        return fail(MTB_UNSUPPORTED, "one-pass 3D kernel: z CPML layers wider than %d cells",
+                    XM_BZ - 4);
+    for (int b = 0; b < 2; ++b) {
+        for (int c = 0; c < 3; ++c) {
+            if ((rc = tmap_3d(&p->xm.e[b][c], S.f[c][b], S.nx, S.ny, S.zpitch, Sh::ZB, Sh::EROWS)) ||
+                (rc = tmap_3d(&p->xm.h[b][c], S.f[3 + c][b], S.nx, S.ny, S.zpitch, Sh::ZB,
+                              Sh::SLOTS)))
+                return rc;
+        }
+        const int pzi[4] = {1, 2, 7, 8};
+        for (int a = 0; a < 4; ++a)
+            if ((rc = tmap_3d(&p->xm.pz[b][a], S.psi[pzi[a]][b], S.nx, S.ny, S.zpitch, XM_BZ,
+                              Sh::SLOTS)))
+                return rc;
+    }
+    if ((rc = tmap_3d(&p->xm.eps, S.eps, S.nx, S.ny, S.zpitch, Sh::ZB, Sh::PROWS))) return rc;
+    // profiles as the split kernels apply them: the H-side node k of an axis of n cells
+    // is updated for k <= n-2, the E-side curl for 1 <= k <= n-2; (1, 0) elsewhere
+    {
+        const int dims[3] = {S.nx, S.ny, S.zpitch};
+        const int real[3] = {S.nx, S.ny, S.nz};
+        std::vector<float> tab;
+        for (int a = 0; a < 3; ++a) {
+            const int n = dims[a], nr = real[a];
+            std::vector<float> prof[2][2];
+            for (int h = 0; h < 2; ++h) {
+                const int len = nr - 1 + h;
+                for (int v = 0; v < 2; ++v) {
+                    prof[h][v].resize(len);
+                    const float *src = v ? S.prof_a[a][h] : S.prof_b[a][h];
+                    MTB_CUDA_TRY(cudaMemcpy(prof[h][v].data(), src, sizeof(float) * len,
+                                            cudaMemcpyDeviceToHost));
+                }
+            }
+            for (int h = 0; h < 2; ++h)
+                for (int v = 0; v < 2; ++v)
+                    for (int k = 0; k < n; ++k) {
+                        const bool on = h == 0 ? k <= nr - 2 : (k >= 1 && k <= nr - 2);
+                        tab.push_back(on ? prof[h][v][k] : (v ? 0.f : 1.f));
+                    }
+        }
+        if ((rc = p->ptab_d.ensure(sizeof(float) * tab.size()))) return rc;
+        MTB_CUDA_TRY(cudaMemcpy(p->ptab_d.p, tab.data(), sizeof(float) * tab.size(),
+                                cudaMemcpyHostToDevice));
+        p->xm.ptab = p->ptab_d.as<float>();
+    }
+    MTB_CUDA_TRY(cudaFuncSetAttribute(k_yee3d_xm<V, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)Sh::SMEM));
+    int dev = 0, sms = 0, occ = 0;
+    MTB_CUDA_TRY(cudaGetDevice(&dev));
+    MTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_yee3d_xm<V, TY>, Sh::THREADS,
+                                                               Sh::SMEM));
+    if (occ < 1) return fail(MTB_UNSUPPORTED, "one-pass 3D kernel does not fit on an SM");
+    p->xm_tiles = (S.ny + TY - 1) / TY;
+    // one share of the (tile, plane) sequence per resident block, at least four planes
+    // per share so that the recomputed halo planes stay a small part; shares of equal
+    // estimated cost: a (tile, plane) pair costs XM_LAYER_COST when its plane or one of
+    // its rows lies in an x / y CPML layer (memory read from HBM, the full update)
+    const int64_t units = (int64_t)p->xm_tiles * S.nx;
+    p->xm_grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * occ, units / 4));
+    p->xm_v = V;
+    {
+        constexpr double XM_LAYER_COST = 1.6;
+        auto band = [&](int a, int k) {
+            return k < B.lo[a][0] || k >= B.hi[a][0] || k < B.lo[a][1] || k >= B.hi[a][1];
+        };
+        std::vector<char> xb(S.nx), yb(p->xm_tiles, 0);
+        for (int i = 0; i < S.nx; ++i) xb[i] = band(0, i);
+        for (int t = 0; t < p->xm_tiles; ++t)
+            for (int r = std::max(t * TY - 1, 0); r < std::min(t * TY + TY, S.ny); ++r)
+                yb[t] |= band(1, r);
+        std::vector<double> cum(units + 1, 0.0);
+        for (int64_t u = 0; u < units; ++u) {
+            const int t = (int)(u / S.nx), i = (int)(u % S.nx);
+            cum[u + 1] = cum[u] + ((xb[i] || yb[t]) ? XM_LAYER_COST : 1.0);
+        }
+        std::vector<int64_t> share(p->xm_grid + 1);
+        int64_t u = 0;
+        for (int b = 0; b <= p->xm_grid; ++b) {
+            const double target = cum[units] * b / p->xm_grid;
+            while (u < units && cum[u] < target) ++u;
+            share[b] = (b == p->xm_grid) ? units : u;
+        }
+        if ((rc = p->share_d.ensure(sizeof(int64_t) * share.size()))) return rc;
+        MTB_CUDA_TRY(cudaMemcpy(p->share_d.p, share.data(), sizeof(int64_t) * share.size(),
+                                cudaMemcpyHostToDevice));
+    }
+    return p->err_d.ensure(sizeof(int));
+}
+
+static int launch_xm(mtb_yee3d_plan *p, int s, cudaStream_t st) {
+    const float *a = p->amp_d.as<float>() + s;
+    using S1 = XmShape<1, xm_ty<1>()>;
+    using S2 = XmShape<2, xm_ty<2>()>;
+    if (p->xm_v == 1)
+        k_yee3d_xm<1, xm_ty<1>()><<<p->xm_grid, S1::THREADS, S1::SMEM, st>>>(
+            p->sp[p->par], p->xm, a, p->par, p->share_d.as<int64_t>(), p->err_d.as<int>());
+    else
+        k_yee3d_xm<2, xm_ty<2>()><<<p->xm_grid, S2::THREADS, S2::SMEM, st>>>(
+            p->sp[p->par], p->xm, a, p->par, p->share_d.as<int64_t>(), p->err_d.as<int>());
+    MTB_CHECK_LAUNCH();
+    ++p->last_launches;
+    return MTB_OK;
+}
+
 extern "C" {
 
 int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regions,
@@ -881,11 +1093,21 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
         return fail(MTB_INVALID_ARG, "nx, ny, nz must be >= 3");
     if (S.zpitch < S.nz || (S.zpitch & 3))
         return fail(MTB_INVALID_ARG, "zpitch %d must be >= nz and a multiple of 4", S.zpitch);
-    const int variant = (tuning && tuning->variant == 1) ? 1 : 2;
+    // variant 3 (one pass per step) by default where it applies: no conductive
+    // damping or poles, zpitch <= 256
+    const int asked = tuning ? tuning->variant : 0;
+    if (asked < 0 || asked > 3) return fail(MTB_INVALID_ARG, "3D variant %d not in 0..3", asked);
+    int n_damp0 = 0;
+    for (int c = 0; c < 6; ++c)
+        for (int h = 0; h < 2; ++h) n_damp0 += S.damp[c][h] != nullptr;
+    const bool xm_ok = n_damp0 == 0 && S.n_poles == 0 && S.zpitch <= 256;
+    if (asked == 3 && !xm_ok)
+        return fail(MTB_UNSUPPORTED, "one-pass 3D kernel: no damping or poles, zpitch <= 256");
+    const int variant = asked == 1 ? 1 : (asked == 3 || (asked == 0 && xm_ok)) ? 3 : 2;
     if (variant == 1 && S.zpitch > 128 * MAXNZ)
         return fail(MTB_UNSUPPORTED, "fused kernel: zpitch %d > %d not supported", S.zpitch,
                     128 * MAXNZ);
-    if (variant == 2 && (S.nx > 65535 || (S.ny + SPLIT_Y - 1) / SPLIT_Y > 65535 ||
+    if (variant != 1 && (S.nx > 65535 || (S.ny + SPLIT_Y - 1) / SPLIT_Y > 65535 ||
                          (int64_t)S.nx * S.ny * S.zpitch >= (1LL << 31)))
         return fail(MTB_UNSUPPORTED, "split kernels: nx <= 65535, ny <= %d, box < 2^31 cells",
                     65535 * SPLIT_Y);
@@ -948,6 +1170,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     p->s = S;
     p->rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
     p->variant = variant;
+    p->chosen = variant == 3 && asked == 0;
     // split kernels: rows_per_warp > 0 sets the x planes per launch pair; the
     // default is the whole grid in one pair
     p->slab = (tuning && tuning->rows_per_warp > 0) ? std::min(tuning->rows_per_warp, S.nx) : S.nx;
@@ -962,14 +1185,14 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->s_d.ensure(sizeof(mtb_yee3d_struct));
     if (!rc) rc = p->pstart_d.ensure(sizeof(int64_t) * (S.n_planes + 1));
-    if (!rc && variant == 2) {
+    if (!rc && variant != 1) {
         const int dims[3] = {S.nx, S.ny, S.nz};
         for (int a = 0; a < 3 && !rc; ++a)
             for (int h = 0; h < 2 && !rc; ++h)
                 rc = profile_band3(S.prof_b[a][h], S.prof_a[a][h], dims[a] - 1 + h,
                                    p->band.lo[a][h], p->band.hi[a][h]);
     }
-    if (!rc && variant == 2) {
+    if (!rc && variant != 1) {
         for (int par = 0; par < 2; ++par) {
             Split3 &q = p->sp[par];
             for (int c = 0; c < 3; ++c) {
@@ -1022,7 +1245,15 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
             default: rc = set_smem3d<4>(p->smem); break;
         }
     }
-    if (rc) { p->dft.release(); delete p; return rc; }
+    if (!rc && variant == 3) {
+        rc = S.zpitch <= 128 ? xm_setup<1>(p) : xm_setup<2>(p);
+        if (rc && p->chosen) {          // default choice only: keep the split kernels
+            rc = MTB_OK;
+            p->variant = 2;
+            p->chosen = false;
+        }
+    }
+    if (rc) { mtb_yee3d_plan_destroy(p); return rc; }
     // plane sample extents (host copy of the device list)
     std::vector<int64_t> ps(S.n_planes + 1, 0);
     if (S.n_planes > 0) {
@@ -1030,7 +1261,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
         cudaError_t e = cudaMemcpy(pl.data(), S.planes, sizeof(int32_t) * 8 * S.n_planes,
                                    cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) {
-            p->dft.release(); delete p;
+            mtb_yee3d_plan_destroy(p);
             return fail(MTB_CUDA_ERROR, "reading plane list: %s", cudaGetErrorString(e));
         }
         const int dims[3] = {S.nx, S.ny, S.nz};
@@ -1041,7 +1272,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
             if (comp < 0 || comp > 5 || axis < 0 || axis > 2 || index < 0 ||
                 index >= dims[axis] || d[3] < 0 || d[4] > dims[a0] || d[3] > d[4] || d[5] < 0 ||
                 d[6] > dims[a1] || d[5] > d[6]) {
-                p->dft.release(); delete p;
+                mtb_yee3d_plan_destroy(p);
                 return fail(MTB_INVALID_ARG, "plane sample %d out of range", q);
             }
             ps[q + 1] = ps[q] + (int64_t)(d[4] - d[3]) * (d[6] - d[5]);
@@ -1051,8 +1282,9 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
     cudaError_t e = cudaMemcpy(p->s_d.p, &S, sizeof(S), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(p->pstart_d.p, ps.data(), sizeof(int64_t) * ps.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && p->err_d.p) e = cudaMemset(p->err_d.p, 0, sizeof(int));
     if (e != cudaSuccess) {
-        p->dft.release(); delete p;
+        mtb_yee3d_plan_destroy(p);
         return fail(MTB_CUDA_ERROR, "plan upload failed: %s", cudaGetErrorString(e));
     }
     *out = p;
@@ -1143,10 +1375,14 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
+    // the one-pass kernel's bounded waits may have raised the error flag
+    if (p->variant == 3 && (rc = mtb_yee3d_check(p, stream))) return rc;
     if ((rc = stage_chunk(p, t0, k, coef, st))) return rc;
     for (int s = 0; s < k; ++s) {
         if ((rc = p->timer.begin(st, 0))) return rc;
-        if (p->variant == 1) {
+        if (p->variant == 3) {
+            if ((rc = launch_xm(p, s, st))) return rc;
+        } else if (p->variant == 1) {
             Ctx3D C;
             C.amp = p->amp_d.as<float>() + s;
             C.par = p->par;
@@ -1175,9 +1411,30 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
     return MTB_OK;
 }
 
+int mtb_yee3d_check(mtb_yee3d_plan *p, void *stream) {
+    if (!p) return fail(MTB_INVALID_ARG, "plan is null");
+    if (!p->err_d.p) return MTB_OK;
+    int flag = 0;
+    MTB_CUDA_TRY(cudaMemcpyAsync(&flag, p->err_d.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                 (cudaStream_t)stream));
+    MTB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    if (flag)
+        return fail(MTB_DEVICE_TIMEOUT, "a bounded wait for a staged plane copy expired on the "
+                    "device; the affected steps are incomplete");
+    return MTB_OK;
+}
+
+// Half steps and x slabs run on the split kernels: a plan that took the one-pass
+// kernel by default moves to them (same results); an explicit request is refused.
+static int need_split(mtb_yee3d_plan *p, const char *what) {
+    if (p->variant == 3 && p->chosen) p->variant = 2;
+    if (p->variant != 2) return fail(MTB_UNSUPPORTED, "%s need the split kernels", what);
+    return MTB_OK;
+}
+
 int mtb_yee3d_set_slab(mtb_yee3d_plan *p, int32_t own_lo, int32_t own_hi) {
     if (!p) return fail(MTB_INVALID_ARG, "plan is null");
-    if (p->variant != 2) return fail(MTB_UNSUPPORTED, "x slabs need the split kernels");
+    if (int rc = need_split(p, "x slabs")) return rc;
     if (own_lo < 0 || own_hi > p->s.nx || own_lo >= own_hi)
         return fail(MTB_INVALID_ARG, "slab [%d, %d) outside [0, %d)", own_lo, own_hi, p->s.nx);
     p->own_lo = own_lo;
@@ -1187,7 +1444,7 @@ int mtb_yee3d_set_slab(mtb_yee3d_plan *p, int32_t own_lo, int32_t own_hi) {
 
 int mtb_yee3d_begin(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, void *stream) {
     if (!p) return fail(MTB_INVALID_ARG, "plan is null");
-    if (p->variant != 2) return fail(MTB_UNSUPPORTED, "half steps need the split kernels");
+    if (int rc = need_split(p, "half steps")) return rc;
     if (k <= 0) return fail(MTB_INVALID_ARG, "k must be > 0");
     p->last_launches = 0;
     return stage_chunk(p, t0, k, coef, (cudaStream_t)stream);
@@ -1241,6 +1498,9 @@ void mtb_yee3d_plan_destroy(mtb_yee3d_plan *p) {
     p->amp_h.release();
     p->dft.release();
     p->timer.release();
+    p->err_d.release();
+    p->ptab_d.release();
+    p->share_d.release();
     delete p;
 }
 

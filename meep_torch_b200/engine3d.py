@@ -449,8 +449,13 @@ class Engine3D:
         cur = self.current
         return [self.box[k][cur] for k in FIELDS[:3]]
 
+    def check(self):
+        """Raise if a bounded wait of the one-pass kernel expired (synchronises)."""
+        L.check(self.lib.mtb_yee3d_check(self.plan, self._sptr()), "mtb_yee3d_check")
+
     def fields(self):
         """Current fields and CPML memory as reference-shaped tensors."""
+        self.check()
         cur = self.current
         nx, ny, nz, zp = self.nx, self.ny, self.nz, self.zp
         shapes = field_shapes(nx, ny, nz)

@@ -198,7 +198,8 @@ def _run3d(lean, variant=0, case=None):
 
 
 @pytest.mark.parametrize("variant,lean,case", [(1, False, None), (2, False, None),
-                                                (1, True, None), (2, True, None),
+                                                (3, False, None), (1, True, None),
+                                                (2, True, None), (3, True, None),
                                                 (2, False, "3d_sigma"), (2, False, "3d_poles"),
                                                 (2, False, "3d_abs"), (2, False, "3d_mixed"),
                                                 (2, True, "3d_lean_poles")])
@@ -777,6 +778,62 @@ def test_te_gradient_matches_reference_autograd(chunk):
           f"J {float(J):.6e} vs {float(g32['J']):.6e}")
     assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
     assert e32 < TOL, e32
+
+
+@pytest.mark.parametrize("shape", [(23, 17, 40), (9, 30, 128), (31, 13, 131), (6, 22, 256),
+                                   (40, 8, 77)])
+def test_3d_one_pass_bitwise_equal_to_split(shape):
+    """The one-pass x-march (variant 3: H and E of a plane in one kernel, TMA-staged
+    planes, a persistent grid cutting the (tile, plane) sequence into segments with
+    recomputed halo planes) gives the split kernels' results bit for bit: fields, CPML
+    memory and flux / DFT accumulators from a random start, for z widths on both
+    kernel shapes (zpitch <= 128 and <= 256), y extents that leave a partial tile and
+    grids small enough that every block owns a few planes only."""
+    from meep_torch_b200.core.monitors_3d import (DFTFieldsMonitor3D, FluxMonitor3D,
+                                                  PointSource3D, run_3d)
+    from meep_torch_b200.core.sources import GaussianPulse
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    nx, ny, nz = shape
+    dx, npml, n = 0.05, 3, 24
+    rng = np.random.default_rng(nx * 1000 + ny)
+    eps = (1.0 + 3.0 * rng.random((nx, ny, nz))).astype(np.float32)
+    c = build_3d_coeffs(nx, ny, nz, dx, eps=torch.from_numpy(eps), npml=npml, device=dev())
+    freqs = [0.8, 1.1]
+    prof = GaussianPulse(1.0, 2.0)
+    src = PointSource3D(c.dt, "Ez", nx // 2, ny // 2, nz // 2, prof)
+    mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=nx // 3, ap=1),
+            FluxMonitor3D(c.dt, freqs, normal="z", idx=nz - 5, ap=1),
+            DFTFieldsMonitor3D(c.dt, freqs, component="Hy", plane=(1, ny // 2))]
+    init = init_3d_state(nx, ny, nz, npml=npml, device=dev())
+    gen = torch.Generator(device="cpu").manual_seed(nx + ny + nz)
+    init = init._replace(**{k: torch.randn(getattr(init, k).shape, generator=gen).to(dev())
+                            for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
+    ref_s, ref_a = run_3d(init, c, n, source=src, monitors=mons, variant=2)
+    st, accs = run_3d(init, c, n, source=src, monitors=mons, variant=3)
+    bad = [k for k, v in ref_s._asdict().items()
+           if v is not None and not torch.equal(v, getattr(st, k))]
+    bad += [f"acc_{q}" for q, (a, b) in enumerate(zip(accs, ref_a)) if not torch.equal(a, b)]
+    assert not bad, bad
+
+
+def test_3d_one_pass_refuses_damping_and_wide_z():
+    """Variant 3 asked for explicitly on a plan it does not cover (conductive damping,
+    zpitch > 256) is refused before any device work; the default falls back to the
+    split kernels there."""
+    from meep_torch_b200.core.monitors_3d import run_3d
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    from meep_torch_b200._lib import MtbUnsupported
+    c = build_3d_coeffs(8, 8, 300, 0.05, eps=2.0, npml=2, device=dev())
+    s0 = init_3d_state(8, 8, 300, npml=2, device=dev())
+    with pytest.raises(MtbUnsupported):
+        run_3d(s0, c, 2, variant=3)
+    run_3d(s0, c, 2)
+    sig = torch.full((8, 8, 8), 0.3)
+    c = build_3d_coeffs(8, 8, 8, 0.05, eps=2.0, npml=2, sigma_d=sig, sigma_b=sig, device=dev())
+    s0 = init_3d_state(8, 8, 8, npml=2, device=dev())
+    with pytest.raises(MtbUnsupported):
+        run_3d(s0, c, 2, variant=3)
+    run_3d(s0, c, 2)
 
 
 @pytest.mark.parametrize("n_slabs", [1, 2, 3])
