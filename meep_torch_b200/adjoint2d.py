@@ -83,6 +83,10 @@ class GradRun2D:
         g, gpsi, tmp = [box() for _ in range(nfld)], [box() for _ in range(4)], \
             [box() for _ in range(4)]
         geps = [box() for _ in range(2 if self.te else 1)]
+        # TM poles: d J / d P(n), d J / d P(n-1) (zero at the end: P is not an output)
+        n_p = 0 if self.te else int(eng.structs[0].n_poles)
+        gpol = [torch.zeros((n_p * nx, P), dtype=torch.float32, device=dev) for _ in range(2)] \
+            if n_p else []
         targets = g + gpsi
         if self.te:
             offs = [(0, 0)] * 5 + [(0, 1), (1, 0), (0, 0), (0, 0)]
@@ -114,12 +118,14 @@ class GradRun2D:
             bufs.g_psi[q], bufs.tmp[q] = L.ptr(gpsi[q]), L.ptr(tmp[q])
         for q in range(len(geps)):
             bufs.g_eps[q] = L.ptr(geps[q])
+        for q in range(len(gpol)):
+            bufs.g_pol[q] = L.ptr(gpol[q])
         adj = C.c_void_p()
         L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
                                              regs if nreg else None, nreg, eng.groups,
                                              eng.n_groups, eng.ring_elems, self.sub,
                                              C.byref(adj)), "mtb_yee2d_adjoint_create")
-        keep = [gaccs, g, gpsi, tmp, geps]
+        keep = [gaccs, g, gpsi, tmp, geps, gpol]
         stream = eng._sptr()
         try:
             rec_mons = _record_monitors(float(self.coeffs.dt), dev, self.te)

@@ -1,10 +1,11 @@
 // Discrete adjoint of the 2D TM step for sm_100a: the exact transpose of the
 // forward update (core/stepper_tm.py:234-254: B phase :85-128, D phase
-// :130-166, E = D / eps :221-231) with CPML (kappa = 1, PEC walls, sigma = 0,
-// no poles), and of the monitors' sampling (core/monitors.py:24-100). This is
-// what torch autograd computes through the reference's run_tm
-// (core/run.py:43-120); the source terms are additive constants and have no
-// adjoint.
+// :130-166, update_pols :203-208, E = (D - sum P) / eps :221-231) with CPML
+// (kappa = 1, PEC walls), electric conductivity (D' = d1 D + d2 curl), magnetic
+// conductivity / permeability (H' = h1 H -/+ h2 curl) and dispersive ADE poles,
+// and of the monitors' sampling (core/monitors.py:24-100). This is what torch
+// autograd computes through the reference's run_tm (core/run.py:43-120); the
+// source terms are additive constants and have no adjoint. (TE: CPML only.)
 //
 // Reverse of forward step t (state_t -> state_{t+1}), adjoint state A holding
 // dJ/d state_{t+1} on entry and dJ/d state_t on exit, three kernels:
@@ -17,7 +18,11 @@
 //                transposed differences of tmp0 / tmp1; H += -/+ dt curl E
 //                with its psi recursions; writes gHx, gHy, g_psi0, g_psi1 and
 //                the adjoints of dEz/dx (tmp2) and dEz/dy (tmp3).
-//   k_adj_tm_ez  (Ez nodes) gEz = transposed differences of tmp2 / tmp3.
+//   k_adj_tm_ez  (Ez nodes) gEz = transposed differences of tmp2 / tmp3 (plus, with
+//                poles, what k_adj_tm_e left in gEz).
+// Poles, P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n) with Ez(n+1) = (Dz - sum P(n+1)) / eps:
+// with gA = d J / d P(n+1), gB = d J / d P(n) on entry, gPn = gA - gEz(n+1) / eps, and
+// on exit gA = c1 gPn + gB, gB = c2 gPn, gEz(n) gets sum_k c3 gPn.
 // The monitor adjoint of a whole chunk comes first: DftState::expand fills
 // ring slot q with dJ/d(sample of step t0+q) in the forward ring's layout, and
 // the kernels add it back at the cells the forward kernels sampled.
@@ -91,6 +96,32 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__
     const bool rowin = i >= 1 && i <= nx - 2;
     float bex = 1.f, aex = 0.f;
     if (rowin) { bex = S.ex_b[i]; aex = S.ex_a[i]; }
+    // electric conductivity: D' = d1 D + d2 pad(curl)
+    float d1[4] = {1.f, 1.f, 1.f, 1.f}, d2[4] = {dt, dt, dt, dt};
+    if (S.cond_d1[0]) { ldv(S.cond_d1[0] + g, d1); ldv(S.cond_d2[0] + g, d2); }
+    // poles: the gradient of P(n+1) and its transpose through the ADE recursion
+    float gpe[4] = {0.f, 0.f, 0.f, 0.f};            // sum_k c3 gPn -> gEz(n)
+    if (S.n_poles > 0) {
+        const uint32_t pl = (uint32_t)nx * P;
+        for (int k = 0; k < S.n_poles; ++k) {
+            const uint32_t o = k * pl + g;
+            float ga[4], gb[4], c1[4], c2[4], c3[4];
+            ldv(B.g_pol[0] + o, ga);
+            ldv(B.g_pol[1] + o, gb);
+            ldv(S.pol_c[0] + o, c1);
+            ldv(S.pol_c[1] + o, c2);
+            ldv(S.pol_c[2] + o, c3);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float gpn = ga[q] - gez[q] * ie[q];
+                ga[q] = c1[q] * gpn + gb[q];
+                gb[q] = c2[q] * gpn;
+                gpe[q] += c3[q] * gpn;
+            }
+            stv(B.g_pol[0] + o, ga);
+            stv(B.g_pol[1] + o, gb);
+        }
+    }
     float t1[4], t2[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -99,15 +130,17 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__
         const bool interior = rowin && j >= 1 && j <= ny - 2;
         const float gd = gdz[q] + gez[q] * ie[q];
         ge[q] -= gez[q] * ez[q] * ie[q];
-        const float gc = interior ? dt * gd : 0.f;
+        const float gc = interior ? d2[q] * gd : 0.f;
         const float g2 = gp2[q] + gc, g3 = gp3[q] - gc;
         const float bey = interior ? S.ey_b[j] : 1.f, aey = interior ? S.ey_a[j] : 0.f;
         t1[q] = interior ? gc + aex * g2 : 0.f;
         t2[q] = interior ? -gc + aey * g3 : 0.f;
         gp2[q] = interior ? bex * g2 : gp2[q];
         gp3[q] = interior ? bey * g3 : gp3[q];
-        gdz[q] = inside ? gd : 0.f;
+        gdz[q] = inside ? d1[q] * gd : 0.f;
+        gpe[q] = inside ? gpe[q] : 0.f;
     }
+    if (S.n_poles > 0) stv(B.g[0] + g, gpe);     // gEz(n) from the poles; k_adj_tm_ez adds
     stv(B.g[3] + g, gdz);
     stv(B.g_psi[2] + g, gp2);
     stv(B.g_psi[3] + g, gp3);
@@ -140,6 +173,11 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__
     const bool vrow = i <= nx - 2;
     float bhx = 1.f, ahx = 0.f;
     if (vrow) { bhx = S.hx_b[i]; ahx = S.hx_a[i]; }
+    // magnetic conductivity / permeability: Hx' = h1 Hx - h2 curl, Hy' = h1 Hy + h2 curl
+    float h1x[4] = {1.f, 1.f, 1.f, 1.f}, h2x[4] = {dt, dt, dt, dt};
+    float h1y[4] = {1.f, 1.f, 1.f, 1.f}, h2y[4] = {dt, dt, dt, dt};
+    if (S.mag_h1[0]) { ldv(S.mag_h1[0] + g, h1x); ldv(S.mag_h2[0] + g, h2x); }
+    if (S.mag_h1[1]) { ldv(S.mag_h1[1] + g, h1y); ldv(S.mag_h2[1] + g, h2y); }
     float t3[4], t4[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -148,17 +186,19 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__
         const float gyp = ghy[q] + (t1[q] - t1n[q]) * rdx;
         const float gxp = ghx[q] + (t2[q] - t2n) * rdx;
         const bool vy = vrow && j < ny, vx = j <= ny - 2;
-        // Hy += dt (dEz/dx + psi_Ezx'), psi_Ezx' = b_hx psi + a_hx dEz/dx
-        const float g1 = gp1[q] + dt * gyp;
-        t3[q] = vy ? dt * gyp + ahx * g1 : 0.f;
+        // Hy = h1 Hy + h2 (dEz/dx + psi_Ezx'), psi_Ezx' = b_hx psi + a_hx dEz/dx
+        const float cy = h2y[q] * gyp;
+        const float g1 = gp1[q] + cy;
+        t3[q] = vy ? cy + ahx * g1 : 0.f;
         gp1[q] = vy ? bhx * g1 : gp1[q];
-        ghy[q] = vy ? gyp : 0.f;
-        // Hx -= dt (dEz/dy + psi_Ezy'), psi_Ezy' = b_hy psi + a_hy dEz/dy
+        ghy[q] = vy ? h1y[q] * gyp : 0.f;
+        // Hx = h1 Hx - h2 (dEz/dy + psi_Ezy'), psi_Ezy' = b_hy psi + a_hy dEz/dy
         const float bhy = vx ? S.hy_b[j] : 1.f, ahy = vx ? S.hy_a[j] : 0.f;
-        const float g0 = gp0[q] - dt * gxp;
-        t4[q] = vx ? -dt * gxp + ahy * g0 : 0.f;
+        const float cx = -h2x[q] * gxp;
+        const float g0 = gp0[q] + cx;
+        t4[q] = vx ? cx + ahy * g0 : 0.f;
         gp0[q] = vx ? bhy * g0 : gp0[q];
-        ghx[q] = vx ? gxp : 0.f;
+        ghx[q] = vx ? h1x[q] * gxp : 0.f;
     }
     stv(B.g[1] + g, ghx);
     stv(B.g[2] + g, ghy);
@@ -182,11 +222,12 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant_
     else t3p[0] = t3p[1] = t3p[2] = t3p[3] = 0.f;
     ldv(B.tmp[3] + g, t4);
     const float t4l = (jb >= 1) ? B.tmp[3][g - 1] : 0.f;
-    float gez[4];
+    float gez[4] = {0.f, 0.f, 0.f, 0.f};
+    if (S.n_poles > 0) ldv(B.g[0] + g, gez);      // the poles' share, from k_adj_tm_e
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float t4m = (q == 0) ? t4l : t4[q - 1];
-        gez[q] = (jb + q < ny) ? (t3p[q] - t3[q]) * rdx + (t4m - t4[q]) * rdx : 0.f;
+        gez[q] = (jb + q < ny) ? gez[q] + ((t3p[q] - t3[q]) * rdx + (t4m - t4[q]) * rdx) : 0.f;
     }
     stv(B.g[0] + g, gez);
 }
@@ -407,9 +448,18 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     const mtb_yee2d_struct &S = *s;
     if (S.pol != MTB_TM && S.pol != MTB_TE) return fail(MTB_INVALID_ARG, "adjoint: bad pol");
     if (S.y_pmc) return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc)");
-    if (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y || S.mag_h1[0] ||
-        S.mag_h1[1])
-        return fail(MTB_UNSUPPORTED, "adjoint: conductivity and poles are forward-only");
+    if (S.pol == MTB_TE && (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y ||
+                            S.mag_h1[0] || S.mag_h1[1]))
+        return fail(MTB_UNSUPPORTED, "adjoint: TE conductivity, poles and magnetic pairs are "
+                    "forward-only");
+    if ((S.cond_d1[0] && !S.cond_d2[0]) || (S.mag_h1[0] && !S.mag_h2[0]) ||
+        (S.mag_h1[1] && !S.mag_h2[1]))
+        return fail(MTB_INVALID_ARG, "adjoint: damping pairs need both arrays");
+    if (S.n_poles > 0 && (!bufs->g_pol[0] || !bufs->g_pol[1] ||
+                          (reinterpret_cast<uintptr_t>(bufs->g_pol[0]) & 15) ||
+                          (reinterpret_cast<uintptr_t>(bufs->g_pol[1]) & 15) || !S.pol_c[0] ||
+                          !S.pol_c[1] || !S.pol_c[2]))
+        return fail(MTB_INVALID_ARG, "adjoint: poles need g_pol[0..1] and the c1..c3 arrays");
     if (S.nx < 3 || S.ny < 3 || S.pitch < S.ny || (S.pitch & 3))
         return fail(MTB_INVALID_ARG, "adjoint: bad grid %d x %d, pitch %d", S.nx, S.ny, S.pitch);
     if ((int64_t)S.nx * S.pitch >= (1LL << 31)) return fail(MTB_UNSUPPORTED, "grid too large");

@@ -577,7 +577,7 @@ def test_point_probes_stack_every_step(variant):
     assert rel_l2(outs[0].cpu().numpy(), rec[:20, 0]) < TOL
 
 
-def _grad_setup(g, dev_, requires_grad=True):
+def _grad_setup(g, dev_, requires_grad=True, extra=None):
     from meep_torch_b200.core.coeffs import build_tm_coeffs
     from meep_torch_b200.core.grid import Grid
     from meep_torch_b200.core.monitors import DFTFieldsMonitor, FluxMonitorTM
@@ -586,7 +586,16 @@ def _grad_setup(g, dev_, requires_grad=True):
     nx, ny, dx, npml = int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"])
     grid = Grid(nx=nx, ny=ny, dx=dx, device=dev_)
     e = torch.tensor(g["eps"], dtype=torch.float32, device=dev_, requires_grad=requires_grad)
-    m = build_tm_coeffs(grid, eps_inf=e, npml=npml)
+    kw, n_p = {}, 0
+    if extra == "lossy":
+        kw = {k: torch.tensor(g[f], dtype=torch.float32, device=dev_)
+              for k, f in (("sigma_d", "sigma"), ("sigma_b", "sigma_b"), ("mu", "mu"))}
+    elif extra == "poles":
+        poles = json.loads(str(g["poles"]))
+        kw = dict(poles=poles, pole_masks=[torch.tensor(v, dtype=torch.float32, device=dev_)
+                                           for v in g["pole_masks"]])
+        n_p = len(poles)
+    m = build_tm_coeffs(grid, eps_inf=e, npml=npml, **kw)
     src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
                      profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
     freqs = [float(f) for f in g["freqs"]]
@@ -595,7 +604,7 @@ def _grad_setup(g, dev_, requires_grad=True):
     monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=mx[0], lo=mx[1], hi=mx[2])
     mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=my[0], lo=my[1], hi=my[2])
     dft = DFTFieldsMonitor(grid, freqs, "Ez")
-    return e, m, src, [monx, mony, dft], init_tm_state(grid), dx
+    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p), dx
 
 
 def _grad_loss(st, ax, ay, ad, mx, my, dx):
@@ -624,6 +633,28 @@ def test_tm_gradient_matches_reference_autograd(chunk):
           f"J {float(J):.6e} vs {float(g32['J']):.6e}")
     assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
     assert e32 < 1e-4, e32
+
+
+@pytest.mark.parametrize("extra", ["lossy", "poles"])
+@pytest.mark.parametrize("chunk", [50, 13])
+def test_tm_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
+    """d J / d eps of lossy (sigma_d on E, sigma_b and mu on H) and dispersive (a
+    Lorentz and a Drude pole) TM runs from the adjoint kernels, against the reference's
+    float64 autograd through run_tm(checkpoint_every=50) (tests/golden/make_golden.py
+    grad_extra); the float32 forward and adjoint agree with it to 1e-4."""
+    from meep_torch_b200.core.run import run_tm
+    g64 = load_golden(f"grad_tm_{extra}_f64")
+    e, m, src, mons, s0, dx = _grad_setup(g64, dev(), extra=extra)
+    st, (ax, ay, ad) = run_tm(s0, m, int(g64["n_steps"]), source=src, monitors=mons,
+                              checkpoint_every=chunk)
+    J = _grad_loss(st, ax, ay, ad, mons[0], mons[1], dx)
+    J.backward()
+    got = e.grad.cpu().numpy()
+    e64 = rel_l2(got, g64["grad"])
+    print(f"grad {extra} chunk {chunk}: rel L2 vs reference f64 {e64:.3e}; "
+          f"J {float(J):.6e} vs {float(g64['J']):.6e}")
+    assert abs(float(J) - float(g64["J"])) <= 1e-4 * abs(float(g64["J"]))
+    assert e64 < 1e-4, e64
 
 
 class _Sheets:
@@ -957,13 +988,13 @@ def test_magnetic_batched_tiles_match_oracle_and_other_paths_refuse():
     """Magnetic conductivity and permeability (with an electric conductivity slab) in
     a batch large enough for four rows per warp, from random fields, against the
     oracle: every H site of the tiles (TM Hx, Hy and the recomputed Hy row and Hx
-    column; TE Hz) applies the (h1, h2) pairs. The row march and the adjoint refuse
+    column; TE Hz) applies the (h1, h2) pairs. The row march and the TE adjoint refuse
     them (MTB_UNSUPPORTED)."""
     from meep_torch_b200._lib import MtbUnsupported
     from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
     from meep_torch_b200.core.grid import Grid
     from meep_torch_b200.core.monitors import DFTFieldsMonitor
-    from meep_torch_b200.core.run import run_tm
+    from meep_torch_b200.core.run import run_te
     from meep_torch_b200.core.sources import GaussianPulse, LineSource
     from meep_torch_b200.core.stepper_te import init_te_state
     from meep_torch_b200.core.stepper_tm import init_tm_state
@@ -1016,12 +1047,13 @@ def test_magnetic_batched_tiles_match_oracle_and_other_paths_refuse():
     eng.close()
     with pytest.raises(MtbUnsupported):
         Engine2D(items[:1], variant=1)
+    # gradients: TM magnetic pairs have an adjoint, TE ones do not (refused)
     grid = Grid(nx=40, ny=40, dx=dx, device=dev())
     eps = torch.ones(40, 40, device=dev(), requires_grad=True)
-    m = build_tm_coeffs(grid, eps_inf=eps, npml=8, sigma_b=torch.full((40, 40), 0.5))
+    m = build_te_coeffs(grid, eps_inf=eps, npml=8, sigma_b=torch.full((40, 40), 0.5))
     src = LineSource(grid, ix=20, j0=15, j1=25, profile=GaussianPulse(0.5, 0.3))
-    _, (acc,) = run_tm(init_tm_state(grid), m, 10, source=src,
-                       monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
+    _, (acc,) = run_te(init_te_state(grid), m, 10, source=src,
+                       monitors=[DFTFieldsMonitor(grid, [0.5], "Hz")])
     with pytest.raises(MtbUnsupported):
         acc.sum().backward()
 
