@@ -177,6 +177,11 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
     const int64_t ch = (b - blk_start[rg]) * CT + threadIdx.x;
     const int64_t nch = (int64_t)R.rows * R.cols;
     if (ch >= nch) return;
+    // frequencies [fa, fb) of this block row (small channel counts split the
+    // frequency loop over gridDim.y block rows; each sum is formed as without it)
+    const int per = (nf + gridDim.y - 1) / gridDim.y;
+    const int fa = blockIdx.y * per, fb = min(nf, fa + per);
+    if (fa >= fb) return;
     const int r = (int)(ch / R.cols), c = (int)(ch - (int64_t)r * R.cols);
     const float *xa = ring + R.ring_a + (int64_t)r * R.ring_pitch + c;
     const float *xb = (R.ring_b >= 0) ? ring + R.ring_b + (int64_t)r * R.ring_pitch + c : nullptr;
@@ -191,7 +196,7 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
 #pragma unroll
             for (int s = 0; s < KFULL; ++s) x[s] = 0.5f * (x[s] + __ldg(xb + s * slot_elems));
         }
-        for (int f = 0; f < nf; ++f) {
+        for (int f = fa; f < fb; ++f) {
             float re = 0.f, im = 0.f;
 #pragma unroll
             for (int s = 0; s < KFULL; ++s) {
@@ -204,12 +209,12 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
         }
         return;
     }
-    for (int f0 = 0; f0 < nf; f0 += NFC) {
+    for (int f0 = fa; f0 < fb; f0 += NFC) {
         float *pr[NFC], *pi[NFC];
         float re[NFC], im[NFC];
 #pragma unroll
         for (int q = 0; q < NFC; ++q) {
-            const int f = min(f0 + q, nf - 1);
+            const int f = min(f0 + q, fb - 1);
             pr[q] = acc + R.re_off + f * R.f_stride + base;
             pi[q] = acc + R.im_off + f * R.f_stride + base;
             re[q] = 0.f;
@@ -222,7 +227,7 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
             const float2 *ps = sP + s * nf + f0;
 #pragma unroll
             for (int q = 0; q < NFC; ++q) {
-                if (f0 + q < nf) {
+                if (f0 + q < fb) {
                     const float2 p = ps[q];
                     re[q] = fmaf(p.x, x, re[q]);
                     im[q] = fmaf(p.y, x, im[q]);
@@ -231,7 +236,7 @@ __global__ void __launch_bounds__(CT) k_dft_contract(
         }
 #pragma unroll
         for (int q = 0; q < NFC; ++q) {
-            if (f0 + q < nf) {
+            if (f0 + q < fb) {
                 *pr[q] += re[q];
                 *pi[q] += im[q];
             }
@@ -419,7 +424,11 @@ int DftState::contract(int row0, int n, cudaStream_t st, LaunchTimer *tm,
     if (n_blocks > 0x7fffffffLL) return fail(MTB_INVALID_ARG, "too many contraction blocks");
     int rc;
     if (tm && (rc = tm->begin(st, 1))) return rc;
-    k_dft_contract<<<(unsigned)n_blocks, CT, smem, st>>>(
+    // few channels: split every channel's frequencies over block rows (four or more
+    // frequencies each) until the launch has about 2^17 threads
+    const int64_t want = ((int64_t)1 << 17) / std::max<int64_t>(n_blocks * CT, 1);
+    const int fsplit = (int)std::max<int64_t>(1, std::min<int64_t>(want, (maxnf + 3) / 4));
+    k_dft_contract<<<dim3((unsigned)n_blocks, fsplit), CT, smem, st>>>(
         regions_d.as<mtb_dft_region>(), blk_region_d.as<int>(), blk_start_d.as<int64_t>(), gd,
         gd + (n_groups + 1), total_nf, phase_base ? phase_base : phase_d.as<float>(), row0, n,
         ring_d.as<float>(),

@@ -175,6 +175,22 @@ __device__ __forceinline__ int lower_col(const int32_t *__restrict__ col, int e0
     }
     return e0;
 }
+// the cells of columns jb .. jb+3 of `row` with amplitude a (the cluster kernel stages
+// its amplitudes in shared memory, so this form takes the value)
+__device__ __forceinline__ void apply_cells_a(const mtb_cells &cl, int row, float a, int jb,
+                                              float (&v)[4]) {
+    if (cl.n == 0 || row < cl.row_lo || row > cl.row_hi) return;
+    const int e0 = __ldg(cl.row_ptr + row), e1 = __ldg(cl.row_ptr + row + 1);
+    if (e0 == e1) return;
+    for (int e = lower_col(cl.col, e0, e1, jb); e < e1; ++e) {
+        const int c = __ldg(cl.col + e) - jb;
+        if (c >= 4) break;
+        const float w = __ldg(cl.w + e);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (c == q) v[q] -= a * w;
+    }
+}
 __device__ __forceinline__ void apply_cells(const mtb_cells &cl, int row, const float *amp,
                                             int jb, float (&v)[4]) {
     if (cl.n == 0 || row < cl.row_lo || row > cl.row_hi) return;
@@ -1867,6 +1883,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
 }  // namespace mtb
 
 #include "yee2d_tb.cuh"
+#include "yee2d_cl.cuh"
 
 using namespace mtb;
 
@@ -1890,6 +1907,10 @@ struct mtb_yee2d_plan {
     DevBuf stage_d;                    // coefficient and phase rows of one flush
     int gend[2] = {0, 1};              // parity after a replay, per start parity
     bool tb = false;                   // temporally blocked kernels after the first step
+    bool cl = false;                   // cluster-resident kernel after the first step
+    int cl_size = 0, cl_rows = 0;      // CTAs per cluster, rows per CTA
+    size_t cl_bytes = 0;               // shared memory per CTA (with the sample staging)
+    int cl_nmax = 0, cl_stage = 0;     // steps per launch; line samples staged
     DevBuf tb_work_d, tmaps_d;         // TB tile list (TM first), tensor maps
     DevBuf tb_meta_d, tb_prof_d;       // TB records, padded profiles
     int n_tb_tm = 0, n_tb_te = 0, tb_grid = 148;
@@ -2177,6 +2198,10 @@ static size_t smem_te() { return sizeof(WarpSmem<5>) * WARPS2D; }
 
 extern "C" {
 
+static int cl_setup_plan(mtb_yee2d_plan *p, const std::vector<mtb_yee2d_struct> &structs,
+                         bool must);
+
+
 int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
                           const mtb_dft_region *regions, int32_t n_regions,
                           const mtb_phase_group *groups, int32_t n_groups,
@@ -2189,8 +2214,10 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     // default (0) and variant 3: the temporally blocked kernels after the first
     // step when every structure is eligible, else tiles; 2: tiles only
     const int tv = tuning ? tuning->variant : 0;
+    if (tv < 0 || tv > 4) return fail(MTB_INVALID_ARG, "2D variant %d not in 0..4", tv);
     const int variant = tv == 1 ? 1 : 2;
     bool want_tb = tv == 3 || tv == 0;
+    bool want_cl = tv == 4 || tv == 0;
     int rows = (tuning && tuning->rows_per_warp > 0) ? tuning->rows_per_warp : 32;
     int wr = 1;
     if (variant == 2) {
@@ -2347,6 +2374,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
     }
     for (int s = 0; s < n; ++s) want_tb = want_tb && tb_eligible(structs[s]);
+    for (int s = 0; s < n; ++s)
+        want_cl = want_cl && structs[s].pol == MTB_TM && tb_eligible(structs[s]);
     int rc = p->dft.init(regions, n_regions, groups, n_groups, ring_slot_elems, slots);
     if (!rc) rc = p->structs_d.ensure(sizeof(mtb_yee2d_struct) * n);
     if (!rc) rc = p->work_d.ensure(sizeof(int4) * n_work);
@@ -2388,7 +2417,11 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         delete p;
         return fail(MTB_CUDA_ERROR, "plan upload failed: %s", cudaGetErrorString(e));
     }
-    if (want_tb && (rc = tb_setup_plan(p, structs))) {
+    if (want_cl && (rc = cl_setup_plan(p, structs, tv == 4))) {
+        mtb_yee2d_plan_destroy(p);
+        return rc;
+    }
+    if (want_tb && !p->cl && (rc = tb_setup_plan(p, structs))) {
         mtb_yee2d_plan_destroy(p);
         return rc;
     }
@@ -2502,6 +2535,120 @@ static TbCtx tb_ctx(const mtb_yee2d_plan *p, const float *amp_e, const float *am
     return C;
 }
 
+// Cluster-resident kernel: every structure fits the shared memory of one cluster
+// (rows split over its CTAs) and the batch occupies at most one cluster per ~16
+// SMs, i.e. a launch-latency-bound plan; asked for explicitly, only the fit counts.
+// Not applicable leaves p->cl false (or fails when `must`).
+static int cl_setup_plan(mtb_yee2d_plan *p, const std::vector<mtb_yee2d_struct> &structs,
+                         bool must) {
+    const int n = (int)structs.size();
+    int nx = 0, pitch = 0;
+    for (const auto &S : structs) {
+        nx = std::max(nx, S.nx);
+        pitch = std::max(pitch, S.pitch);
+    }
+    int dev = 0, sms = 0, optin = 0;
+    MTB_CUDA_TRY(cudaGetDevice(&dev));
+    MTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MTB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    int size = CL_MAX;
+    if (cudaFuncSetAttribute(k_cl_tm, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        size = 8;
+    }
+    const int rows = (nx + size - 1) / size;
+    size_t bytes = cl_smem(rows, pitch);
+    const bool fits = bytes <= (size_t)optin && (int64_t)rows * (pitch / 4) <= CL_THREADS;
+    // line samples staged in shared memory for a whole launch (written to the ring at its
+    // end, so that no global store sits before a cluster barrier): as many steps per
+    // launch as the remaining shared memory holds, at most a ring's worth
+    int64_t span = 0;
+    for (const auto &S : structs) {
+        if (S.n_lines <= 0) continue;
+        mtb_line_sample ls[MAXL];
+        MTB_CUDA_TRY(cudaMemcpy(ls, S.lines, sizeof(mtb_line_sample) * S.n_lines,
+                                cudaMemcpyDeviceToHost));
+        int64_t lo = 0, hi = 0;
+        cl_line_span(ls, S.n_lines, lo, hi);
+        span = std::max(span, hi - lo);
+    }
+    const int G = p->dft.slots;
+    int nmax = G, stage = 0;
+    if (fits && span > 0) {
+        const int64_t room = ((int64_t)optin - (int64_t)bytes) / (int64_t)(sizeof(float) * span);
+        if (room >= std::min(G, 8)) {
+            nmax = (int)std::min<int64_t>(G, room);
+            stage = 1;
+            bytes = cl_smem_staged(rows, pitch, span, nmax);
+        }
+    }
+    if (!fits || (!must && (int64_t)n * size > sms)) {
+        if (must)
+            return fail(MTB_UNSUPPORTED, "cluster kernel: %zu bytes of shared memory per CTA "
+                        "(%d rows x pitch %d) exceed %d", bytes, rows, pitch, optin);
+        return MTB_OK;
+    }
+    MTB_CUDA_TRY(cudaFuncSetAttribute(k_cl_tm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bytes));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = size;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(size * n);
+    cfg.blockDim = dim3(CL_THREADS);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_cl_tm, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        if (must) return fail(MTB_UNSUPPORTED, "cluster kernel: no cluster of %d CTAs fits", size);
+        return MTB_OK;
+    }
+    p->cl = true;
+    p->cl_size = size;
+    p->cl_rows = rows;
+    p->cl_bytes = bytes;
+    p->cl_nmax = nmax;
+    p->cl_stage = stage;
+    return MTB_OK;
+}
+
+// n cluster-resident steps from parity par; samples from ring slot `slot` on.
+static int launch_cl(mtb_yee2d_plan *p, const float *amp_e, const float *amp_h, int nc, int n,
+                     int slot, int par, cudaStream_t st) {
+    ClCtx C;
+    C.structs = p->structs_d.as<mtb_yee2d_struct>();
+    C.amp_e = amp_e;
+    C.amp_h = amp_h;
+    C.ncols = nc;
+    C.nsub = n;
+    C.ring = p->dft.ring_d.as<float>() + (size_t)slot * p->dft.slot_elems;
+    C.slot_elems = p->dft.slot_elems;
+    C.par = par;
+    C.rows = p->cl_rows;
+    C.stage = p->cl_stage;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = p->cl_size;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(p->cl_size * p->n_structs);
+    cfg.blockDim = dim3(CL_THREADS);
+    cfg.dynamicSmemBytes = p->cl_bytes;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    MTB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_cl_tm, C));
+    MTB_CHECK_LAUNCH();
+    ++p->last_launches;
+    return MTB_OK;
+}
+
 // Capture one ring flush (G steps from parity par0, then the contraction)
 // reading its coefficient and phase rows from the plan's staging buffer.
 static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
@@ -2514,6 +2661,14 @@ static int build_flush_graph(mtb_yee2d_plan *p, int par0, int nc) {
     int rc = MTB_OK;
     int par = par0;
     for (int s = 0; s < G && !rc;) {
+        if (p->cl) {                             // cluster launches of up to cl_nmax steps
+            const int n = std::min(p->cl_nmax, G - s);
+            rc = launch_cl(p, stage + (size_t)s * nc, stage + (size_t)G * nc + (size_t)s * nc, nc,
+                           n, s, par, p->cap);
+            par ^= n & 1;
+            s += n;
+            continue;
+        }
         if (p->tb) {                             // TB launches of up to TB_T steps
             const int n = std::min(TB_T, G - s);
             const TbCtx C = tb_ctx(p, stage + (size_t)s * nc,
@@ -2568,8 +2723,9 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    // the row march's bounded waits may have raised the error flag (tiles never wait)
-    if (p->variant == 1 && (rc = mtb_yee2d_check(p, stream))) return rc;
+    // the row march's and the TB kernels' bounded waits may have raised the error flag
+    // (the one-step tiles and the cluster kernel never wait)
+    if ((p->variant == 1 || p->tb) && (rc = mtb_yee2d_check(p, stream))) return rc;
     const int nc = std::max(p->n_cols, 1);
     const size_t per = (size_t)k * nc;
     void *hp = nullptr;
@@ -2612,6 +2768,26 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
             p->last_launches += p->gkern[p->par];
             p->par = p->gend[p->par];
             s += G;
+            continue;
+        }
+        if (p->cl && !p->first) {
+            // cluster-resident: the rest of the ring in one launch
+            const int n = std::min(p->cl_nmax, std::min(G - slot, k - s));
+            if ((rc = p->timer.begin(st, 0))) return rc;
+            if ((rc = launch_cl(p, ad + (size_t)s * nc, ad + per + (size_t)s * nc, nc, n, slot,
+                                p->par, st)))
+                return rc;
+            if ((rc = p->timer.end(st))) return rc;
+            p->par ^= n & 1;
+            s += n;
+            slot += n;
+            if (slot == G || s == k) {
+                if (p->dft.n_regions > 0) {
+                    if ((rc = p->dft.contract(s - slot, slot, st, &p->timer))) return rc;
+                    ++p->last_launches;
+                }
+                slot = 0;
+            }
             continue;
         }
         if (p->tb && !p->first) {

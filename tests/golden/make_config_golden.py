@@ -176,7 +176,9 @@ def cfg3_case(prec, n_steps=2000):
 def cfg4_case(prec, steps=None):
     """J and d J / d rho of the cfg4-shaped problem through the reference's design
     chain (conic_filter, tanh_projection, MaterialGrid, DesignRegion, OptimizationProblem)
-    and its autograd through run_tm(checkpoint_every=256)."""
+    and its autograd through run_tm(checkpoint_every=256) in float32; float64 checkpoints
+    every 64 steps (the same gradient; 256-step float64 segments exceed this machine's
+    memory)."""
     from meep_torch.adjoint.problem import DesignRegion, MaterialGrid, OptimizationProblem
     c = W.CFG4
     nx, ny, dx, npml = c["nx"], c["ny"], c["dx"], c["npml"]
@@ -199,7 +201,7 @@ def cfg4_case(prec, steps=None):
     def run_fn(eps):
         m = build_tm_coeffs(grid, eps_inf=eps, npml=npml)
         _, (acc,) = run_tm(init_tm_state(grid), m, n, source=src, monitors=[mon],
-                           checkpoint_every=256)
+                           checkpoint_every=256 if prec == "f32" else 64)
         return mon.flux(acc, dx).mean()
 
     rho0 = rng.uniform(0.4, 0.6, (d, d))
@@ -253,13 +255,20 @@ def cfg4_fd_case(n_pix=32, h=1e-4, steps=None):
 def main(argv):
     torch.set_num_threads(os.cpu_count() or 1)
     which = argv or ["cfg1", "cfg2", "cfg3", "cfg4", "cfg4fd"]
-    for w in which:
+    for arg in which:
+        # "cfg4:f64" makes one precision; "cfg4:f64:4000" also shortens the run (the file
+        # name then carries the step count)
+        w, _, rest = arg.partition(":")
+        only, _, nst = rest.partition(":")
+        steps = int(nst) if nst else None
         if w == "cfg4fd":                       # float64 only
             t0 = time.time()
             np.savez_compressed(os.path.join(HERE, "config_cfg4_fd_f64.npz"), **cfg4_fd_case())
             print(f"cfg4fd f64: {time.time() - t0:.1f} s", flush=True)
             continue
         for prec in ("f32", "f64"):
+            if only and prec != only:
+                continue
             t0 = time.time()
             if w == "cfg1":
                 np.savez_compressed(os.path.join(HERE, f"config_cfg1_{prec}.npz"),
@@ -273,8 +282,9 @@ def main(argv):
                 np.savez_compressed(os.path.join(HERE, f"config_cfg3_{prec}.npz"),
                                     **cfg3_case(prec))
             elif w == "cfg4":
-                np.savez_compressed(os.path.join(HERE, f"config_cfg4_{prec}.npz"),
-                                    **cfg4_case(prec))
+                tag = f"_{steps}" if steps else ""
+                np.savez_compressed(os.path.join(HERE, f"config_cfg4{tag}_{prec}.npz"),
+                                    **cfg4_case(prec, steps))
             print(f"{w} {prec}: {time.time() - t0:.1f} s", flush=True)
 
 

@@ -526,6 +526,58 @@ def test_tb_matches_tiles_on_a_cfg2_batch():
     assert launches[1] < launches[0] / 2, launches
 
 
+@pytest.mark.parametrize("shape", [(320, 160), (77, 50), (30, 301), (200, 96)])
+@pytest.mark.parametrize("graph", [False, True])
+def test_cluster_kernel_matches_tiles(shape, graph):
+    """The cluster-resident TM kernel (variant 4: the structure's rows split over the
+    shared memory of one thread-block cluster, a ring's worth of steps per launch,
+    neighbour rows through distributed shared memory) against the one-step tiles from
+    a random start: the cfg1 320 x 160 case and shapes whose rows do not split evenly
+    over the cluster, a single-cell source, a flux line, a full-grid DFT, run lengths of
+    both parities over several calls and ring flushes (graph-replayed or not)."""
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor, FluxMonitorTM
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    from meep_torch_b200.engine2d import Engine2D
+    nx, ny = shape
+    rng = np.random.default_rng(nx * 7 + ny)
+    eps = torch.from_numpy((1.0 + 5.0 * rng.random((nx, ny))).astype(np.float32)).to(dev())
+    grid = Grid(nx=nx, ny=ny, dx=0.05, device=dev())
+    outs, launches = [], []
+    for variant in (2, 4):
+        m = build_tm_coeffs(grid, eps_inf=eps, npml=10)
+        src = LineSource(grid, ix=nx // 4, j0=ny // 2, j1=ny // 2 + 1,
+                         profile=GaussianPulse(0.6, 0.3))
+        mons = [FluxMonitorTM(grid, [0.5, 0.6, 0.7], x_normal=True, idx=3 * nx // 4, lo=12,
+                              hi=ny - 12),
+                DFTFieldsMonitor(grid, [0.55, 0.65], "Ez")]
+        s0 = init_tm_state(grid)
+        g = torch.Generator().manual_seed(3)
+        s0 = s0._replace(**{k: 0.1 * torch.randn(getattr(s0, k).shape, generator=g).to(dev())
+                            for k in ("Hx", "Hy")})
+        eng = Engine2D([(s0, m, src, mons)], variant=variant, ring_slots=16, graph=graph)
+        eng.run(0, 1)
+        eng.run(1, 47)
+        eng.run(48, 33)
+        launches.append(int(eng.last_launches))
+        outs.append((eng.state(0), [a.clone() for a in eng.accumulators(0)]))
+        eng.close()
+    (s0, a0), (s1, a1) = outs
+    errs = {}
+    for name in s0._fields:
+        x, y = getattr(s0, name), getattr(s1, name)
+        if isinstance(x, torch.Tensor) and x.numel():
+            errs[name] = rel_l2(y.cpu().numpy(), x.cpu().numpy())
+    for q, (x, y) in enumerate(zip(a0, a1)):
+        errs[f"acc{q}"] = rel_l2(y.cpu().numpy(), x.cpu().numpy())
+    print(f"\n[cluster vs tiles {shape}] max relL2 {max(errs.values()):.2e}; launches {launches}")
+    bad = {k: v for k, v in errs.items() if not v < 1e-6}
+    assert not bad, bad
+    assert launches[1] < launches[0] / 4, launches
+
+
 @pytest.mark.parametrize("variant", [2, 3])
 def test_point_probes_stack_every_step(variant):
     """PointProbe (reduce "stack", core/monitors.py:11-21) next to a flux line: the run
@@ -1051,8 +1103,7 @@ def test_magnetic_batched_tiles_match_oracle_and_other_paths_refuse():
     grid = Grid(nx=40, ny=40, dx=dx, device=dev())
     eps = torch.ones(40, 40, device=dev(), requires_grad=True)
     m = build_te_coeffs(grid, eps_inf=eps, npml=8, sigma_b=torch.full((40, 40), 0.5))
-    src = LineSource(grid, ix=20, j0=15, j1=25, profile=GaussianPulse(0.5, 0.3))
-    _, (acc,) = run_te(init_te_state(grid), m, 10, source=src,
+    _, (acc,) = run_te(init_te_state(grid), m, 10,
                        monitors=[DFTFieldsMonitor(grid, [0.5], "Hz")])
     with pytest.raises(MtbUnsupported):
         acc.sum().backward()
