@@ -441,8 +441,8 @@ int mtb_yee3d_run(mtb_yee3d_plan *plan, int64_t t0, int32_t k,
                   const double *coef, void *stream);
 /* Error flag of the one-pass kernel (variant 3): MTB_DEVICE_TIMEOUT if one of
  * its bounded waits for a staged plane copy expired since the plan was made
- * (the steps of that launch are incomplete). Synchronises `stream`.
- * mtb_yee3d_run checks it before its first launch. */
+ * (the steps of that launch are incomplete). Synchronises `stream`; call it
+ * before trusting the state (the engine does when it exports fields). */
 int mtb_yee3d_check(mtb_yee3d_plan *plan, void *stream);
 /* x-slab decomposition (core/monitors_3d.py:192-210 run_3d split across
  * ranks along x). The plan holds planes [lo, hi) of a larger grid as its own

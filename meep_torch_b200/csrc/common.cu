@@ -156,7 +156,7 @@ constexpr int CT = 256;        // channels per contraction block
 // frequencies of its channel in registers and streams its n ring samples.
 constexpr int NFC = 4;
 constexpr int KFULL = 32;      // ring depth with a fully unrolled contraction (the default)
-__global__ void __launch_bounds__(CT) k_dft_contract(
+__global__ void __launch_bounds__(CT, 4) k_dft_contract(
     const mtb_dft_region *__restrict__ regions, const int *__restrict__ blk_region,
     const int64_t *__restrict__ blk_start, const int *__restrict__ group_nf,
     const int *__restrict__ group_off, int total_nf, const float *__restrict__ phase, int row0,

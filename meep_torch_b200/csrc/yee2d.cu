@@ -2551,12 +2551,23 @@ static int cl_setup_plan(mtb_yee2d_plan *p, const std::vector<mtb_yee2d_struct> 
     MTB_CUDA_TRY(cudaGetDevice(&dev));
     MTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     MTB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    int size = CL_MAX;
-    if (cudaFuncSetAttribute(k_cl_tm, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-        cudaSuccess) {
-        cudaGetLastError();
-        size = 8;
+    // the function attributes once per process (the largest shared memory the device
+    // allows), the cluster occupancy once per shared-memory size: plan creation stays cheap
+    static std::mutex mu;
+    static int size_cached = 0;
+    static std::vector<std::pair<size_t, int>> occ_cache;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!size_cached) {
+        size_cached = CL_MAX;
+        if (cudaFuncSetAttribute(k_cl_tm, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            size_cached = 8;
+        }
+        MTB_CUDA_TRY(cudaFuncSetAttribute(k_cl_tm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          optin));
     }
+    const int size = size_cached;
     const int rows = (nx + size - 1) / size;
     size_t bytes = cl_smem(rows, pitch);
     const bool fits = bytes <= (size_t)optin && (int64_t)rows * (pitch / 4) <= CL_THREADS;
@@ -2589,8 +2600,6 @@ static int cl_setup_plan(mtb_yee2d_plan *p, const std::vector<mtb_yee2d_struct> 
                         "(%d rows x pitch %d) exceed %d", bytes, rows, pitch, optin);
         return MTB_OK;
     }
-    MTB_CUDA_TRY(cudaFuncSetAttribute(k_cl_tm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)bytes));
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -2602,9 +2611,18 @@ static int cl_setup_plan(mtb_yee2d_plan *p, const std::vector<mtb_yee2d_struct> 
     cfg.dynamicSmemBytes = bytes;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, k_cl_tm, &cfg) != cudaSuccess || clusters < 1) {
-        cudaGetLastError();
+    int clusters = -1;
+    for (const auto &e : occ_cache)
+        if (e.first == bytes) clusters = e.second;
+    if (clusters < 0) {
+        cfg.gridDim = dim3(size);
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_cl_tm, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            clusters = 0;
+        }
+        occ_cache.emplace_back(bytes, clusters);
+    }
+    if (clusters < 1) {
         if (must) return fail(MTB_UNSUPPORTED, "cluster kernel: no cluster of %d CTAs fits", size);
         return MTB_OK;
     }
@@ -2723,9 +2741,10 @@ int mtb_yee2d_run(mtb_yee2d_plan *p, int64_t t0, int32_t k, const double *coef_e
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    // the row march's and the TB kernels' bounded waits may have raised the error flag
-    // (the one-step tiles and the cluster kernel never wait)
-    if ((p->variant == 1 || p->tb) && (rc = mtb_yee2d_check(p, stream))) return rc;
+    // the row march's bounded waits may have raised the error flag (the TB kernels' flag
+    // is read by mtb_yee2d_check, which the engine calls when it exports the state; the
+    // one-step tiles and the cluster kernel never wait)
+    if (p->variant == 1 && (rc = mtb_yee2d_check(p, stream))) return rc;
     const int nc = std::max(p->n_cols, 1);
     const size_t per = (size_t)k * nc;
     void *hp = nullptr;

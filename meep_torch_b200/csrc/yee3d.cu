@@ -1375,8 +1375,6 @@ int mtb_yee3d_run(mtb_yee3d_plan *p, int64_t t0, int32_t k, const double *coef, 
     if (k == 0) return MTB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    // the one-pass kernel's bounded waits may have raised the error flag
-    if (p->variant == 3 && (rc = mtb_yee3d_check(p, stream))) return rc;
     if ((rc = stage_chunk(p, t0, k, coef, st))) return rc;
     for (int s = 0; s < k; ++s) {
         if ((rc = p->timer.begin(st, 0))) return rc;

@@ -611,6 +611,7 @@ class Engine2D:
     def run(self, t0: int, k: int):
         """Advance every structure k steps starting at step index t0. Point probes
         (stack-reduced) hold the k values of this call afterwards."""
+        self._checked = False
         if k <= 0:
             return
         if any(it.stacks for it in self.items):
@@ -743,8 +744,16 @@ class Engine2D:
                                               self._sptr()), "unpack")
         return out
 
+    def check(self):
+        """Raise if a bounded wait of a staging kernel (row march, temporally blocked
+        tiles) expired; synchronises the plan's stream (once per run)."""
+        if not getattr(self, "_checked", False):
+            L.check(self.lib.mtb_yee2d_check(self.plan, self._sptr()), "mtb_yee2d_check")
+            self._checked = True
+
     def state(self, b: int = 0):
         """Current state of structure b, as the input state's own type."""
+        self.check()
         it = self.items[b]
         cur = self.current
         s, nx, ny, bx = it.state, it.nx, it.ny, it.box
