@@ -962,7 +962,7 @@ def config_suite(args, rank, world, dev):
         if wl == "cfg3":
             avg = r["step_ms"] / max(r["step_n"], 1)
             ach = r["bytes_launch"] / (avg / 1e3) / 1e9
-            ent["roofline"] = {"bound": "hbm", "kernel": "k_yee3d_h + k_yee3d_e (one step)",
+            ent["roofline"] = {"bound": "hbm", "kernel": "k_yee3d_xm (one pass per step)",
                                "achieved": ach, "peak": peak, "unit": "GB/s",
                                "frac": ach / peak, "alg_bytes_per_step": r["bytes_launch"],
                                "launch_ms": avg}
@@ -1144,7 +1144,7 @@ def main():
                               "the mode source, output-port flux at 3 wavelengths), 8000 steps "
                               "forward + adjoint sweep per gradient",
                   "time_steps": args.run_steps if args.run_steps != 5000 else 8000,
-                  "checkpoint_every": 32, "seed": "4 + 1009*rank",
+                  "checkpoint_every": 256, "seed": "4 + 1009*rank",
                   "l2": "L2-resident working set (~10 MB of state): latency-bound"}
     elif args.workload == "cfg1":
         config = {"workload": "cfg1: 2D TM waveguide 320 x 160 (16 x 8 um at res 20), 1 um "
@@ -1309,20 +1309,24 @@ def main():
     if os.path.exists(prof) and args.workload in ("cfg2", "cfg3"):
         with open(prof) as f:
             tr = json.load(f)
-        eff = args.variant or (3 if args.workload == "cfg2" else 2)   # library defaults
+        eff = args.variant or 3                  # library defaults: TB tiles (2D), one pass (3D)
         entry = tr.get("variants", {}).get(str(eff)) if "variants" in tr else (
             tr if tr.get("variant") == eff else None)
         if entry and round(entry.get("steps_per_launch", 1)) == round(steps_per_launch):
             traffic = entry.get("dram_bytes_per_launch")
     e2e_val = (total_updates / r["e2e_s"] / 1e9
                if r["e2e_s"] == r["e2e_s"] else None)
-    kernel = ("k_tb_tm (temporally blocked, 4 steps per launch; graph replays, step time = "
-              "run time / steps)" if args.workload == "cfg1" and args.variant in (0, 3) else
+    kernel = ("k_cl_tm (cluster-resident, a ring of steps per launch; graph replays, step "
+              "time = run time / steps)" if args.workload == "cfg1" and args.variant in (0, 4)
+              else
+              "k_tb_tm (temporally blocked, 4 steps per launch; graph replays, step time = "
+              "run time / steps)" if args.workload == "cfg1" and args.variant == 3 else
               "k_tile_tm (one step; graph replays, step time = run time / steps)"
               if args.workload == "cfg1" and args.variant == 2 else
               "k_yee2d_tm (one step; graph replays, step time = run time / steps)"
               if args.workload == "cfg1" else
-              "k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant != 1 else
+              "k_yee3d_xm (one pass per step)" if cfg3 and args.variant in (0, 3) else
+              "k_yee3d_h + k_yee3d_e (one step)" if cfg3 and args.variant == 2 else
               "k_yee3d_step (one step)" if cfg3 else
               "k_yee2d_tm + k_yee2d_te (one step)" if args.variant == 1 else
               "k_tile_tm + k_tile_te (one step)" if args.variant == 2 else
