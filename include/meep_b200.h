@@ -423,7 +423,11 @@ typedef struct mtb_yee3d_struct {
      * P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n); c1, c2 per pole (host values),
      * c3 per cell. Split kernels only. */
     int32_t n_poles;
-    int32_t pad3_;
+    /* PMC walls instead of PEC on these axes (bit 0 x, 1 y, 2 z; core/stepper_3d.py
+     * _term_pmc :99-121): the tangential E stays live at the wall and the curl term
+     * that differentiates along the axis is zero there. Split and one-pass kernels;
+     * the register-staged march and the adjoint refuse it. */
+    int32_t pmc_axes;
     float *pol_p[3][2];
     const float *pol_c3[3];
     float pol_c1[MTB_MAX_POLES];

@@ -78,7 +78,7 @@ class Yee3DStruct(C.Structure):
                 ("src_comp", C.c_int32), ("src_is_point", C.c_int32), ("src", Cells),
                 ("planes", vp), ("plane_ring_off", vp), ("n_planes", C.c_int32),
                 ("pad2_", C.c_int32), ("damp", (vp * 2) * 6),
-                ("n_poles", C.c_int32), ("pad3_", C.c_int32), ("pol_p", (vp * 2) * 3),
+                ("n_poles", C.c_int32), ("pmc_axes", C.c_int32), ("pol_p", (vp * 2) * 3),
                 ("pol_c3", vp * 3), ("pol_c1", C.c_float * 8), ("pol_c2", C.c_float * 8)]
 
 

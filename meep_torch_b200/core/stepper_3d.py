@@ -82,7 +82,7 @@ def _inert(n, ax, dtype, device):
 def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
                     dtype=torch.float32, device="cuda", sigma_d=None, sigma_b=None,
                     poles=(), pole_masks=None, n_abs=0, absorber_axes=(), absorber_m: int = 2,
-                    absorber_R0: float = 1e-15, **kw) -> Coeffs3D:
+                    absorber_R0: float = 1e-15, pmc_axes=(), **kw) -> Coeffs3D:
     """Coefficients of the 3D step (core/stepper_3d.py:150-266). Boundaries as the
     reference offers them: CPML (``npml``), the matched-sigma absorber (``n_abs`` with
     ``npml = 0``: no CPML, the absorber's conductivity damps D and B), or both (CPML on
@@ -90,7 +90,8 @@ def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
     CPML profiles: H side on the n-1 half nodes, E side on the interior [1:-1] of each
     axis (:192-206). With ``sigma_d`` / ``sigma_b`` ((nx, ny, nz) cell-centred, added to
     the absorber's), the damping pairs of :217-235 Yee-averaged onto each component;
-    with ``poles`` / ``pole_masks`` the ADE stacks of :236-266."""
+    with ``poles`` / ``pole_masks`` the ADE stacks of :236-266. ``pmc_axes``: PMC walls
+    instead of PEC on those axes, whose CPML profile is the plain derivative (:186-189)."""
     for k, v in kw.items():
         if v not in (None, 0, (), []):
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
@@ -108,7 +109,7 @@ def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
     if has_pml:
         cpml = {}
         for ax, kh, ke in ((0, "hx", "ex"), (1, "hy", "ey"), (2, "hz", "ez")):
-            if ax in abs_axes:
+            if ax in abs_axes or ax in pmc_axes:
                 cpml[kh] = _inert(dims[ax] - 1, ax, dtype, device)
                 cpml[ke] = _inert(dims[ax] - 2, ax, dtype, device)
                 continue
@@ -161,7 +162,8 @@ def build_3d_coeffs(nx: int, ny: int, nz: int, dx: float, eps=None, npml=0,
             c1 = torch.tensor([v[0] for v in vs], dtype=dtype, device=device).reshape(npl, 1, 1, 1)
             c2 = torch.tensor([v[1] for v in vs], dtype=dtype, device=device).reshape(npl, 1, 1, 1)
             pols[key] = (c1, c2, c3)
-    return Coeffs3D(dt=dt, dx=dx, eps=e, damp=damp, cpml=cpml, pols=pols)
+    return Coeffs3D(dt=dt, dx=dx, eps=e, damp=damp, cpml=cpml, pols=pols,
+                    pmc=tuple(int(a) for a in pmc_axes))
 
 
 def init_3d_state(nx: int, ny: int, nz: int, npml: int = 0, n_poles: int = 0,

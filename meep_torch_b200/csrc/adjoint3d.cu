@@ -338,6 +338,7 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
         if (S.damp[c][0] || S.damp[c][1])
             return fail(MTB_UNSUPPORTED, "3D adjoint: conductive damping is forward-only");
     if (S.n_poles) return fail(MTB_UNSUPPORTED, "3D adjoint: poles are forward-only");
+    if (S.pmc_axes) return fail(MTB_UNSUPPORTED, "3D adjoint: PMC walls are forward-only");
     if (S.nx < 3 || S.ny < 3 || S.nz < 3 || S.zpitch < S.nz || (S.zpitch & 3))
         return fail(MTB_INVALID_ARG, "3D adjoint: bad grid");
     if ((int64_t)S.nx * S.ny * S.zpitch >= (1LL << 31) || S.nx > 65535 ||

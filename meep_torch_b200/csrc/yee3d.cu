@@ -472,6 +472,13 @@ __device__ __forceinline__ float y3_epd(float e, float curl, float d1, float d2,
     return __fdividef(__fsub_rn(__fmaf_rn(d2, curl, __fmul_rn(d1, __fmaf_rn(e, ec, spc))), spn),
                       ec);
 }
+// One E-update curl ta - tb (core/stepper_3d.py:395-437 with _term_pmc / _pad_interior,
+// :86-121): wa / wb mark a cell on a wall of the axis that term a / b differentiates
+// along; on a PEC wall (pa / pb clear) the tangential E keeps its value (curl 0), on a
+// PMC wall that term alone is zero. Without PMC this is (wa || wb) ? 0 : ta - tb.
+__device__ __forceinline__ float y3_curl(float ta, bool wa, bool pa, float tb, bool wb, bool pb) {
+    return ((wa && !pa) || (wb && !pb)) ? 0.f : __fsub_rn(wa ? 0.f : ta, wb ? 0.f : tb);
+}
 // soft current of one cell: E + sgn v / eps_c (point) or E - v / eps_c (area / plane)
 __device__ __forceinline__ float y3_src(float e, float v, float ecomp, bool point, float sgn) {
     return point ? __fadd_rn(e, sgn * __fmul_rn(v, __fdiv_rn(1.0f, ecomp)))
@@ -504,6 +511,7 @@ struct Split3 {
     float pc1[MTB_MAX_POLES], pc2[MTB_MAX_POLES];
     int np;
     uint32_t plane;
+    int pmc;                    // PMC wall axes: bit 0 x, 1 y, 2 z (PEC otherwise)
 };
 
 __device__ __forceinline__ void ldg4v(const float *p, float (&v)[4]) {
@@ -642,6 +650,7 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
     const uint32_t g = (uint32_t)i * NYZ + (uint32_t)(j * ZP + kb);
     const float dt = P.dt, rdx = P.rdx;
     const bool iin = i >= 1 && i <= nx - 2, jin = j >= 1 && j <= ny - 2;
+    const bool pmx = P.pmc & 1, pmy = (P.pmc >> 1) & 1, pmz = (P.pmc >> 2) & 1;
     const bool xok = i <= nx - 2, vyH = j <= ny - 2;
     const bool bx = iin && inband(P.B, 0, 1, i), by = jin && inband(P.B, 1, 1, j);
     bool bz = false;
@@ -744,10 +753,10 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
         // Ex: valid i <= nx-2, k < nz; curl on j, k interior
         {
             float qy, qz;
-            const float cs = __fsub_rn(y3_s(y3_d(hz[q], hzm[q], rdx), eyb, eya, p6[q], qy),
-                                       y3_s(y3_d(hy[q], hym, rdx), ezb[q], eza[q], p7[q], qz));
+            const float ty = y3_s(y3_d(hz[q], hzm[q], rdx), eyb, eya, p6[q], qy);
+            const float tz = y3_s(y3_d(hy[q], hym, rdx), ezb[q], eza[q], p7[q], qz);
             const bool v = xok && vzE;
-            const float curl = (jin && kin) ? cs : 0.f;
+            const float curl = y3_curl(ty, !jin, pmy, tz, !kin, pmz);
             const float ec = y3_ec(ep[q], epi[q]);
             en[0][q] = v ? (PL ? (DAMP ? y3_epd(en[0][q], curl, a1[0][q], a2[0][q], ec, spc[0][q],
                                                 spn[0][q])
@@ -761,10 +770,10 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
         // Ey: valid j <= ny-2, k < nz; curl on i, k interior
         {
             float qz, qx;
-            const float cs = __fsub_rn(y3_s(y3_d(hx[q], hxkm, rdx), ezb[q], eza[q], p8[q], qz),
-                                       y3_s(y3_d(hz[q], hzp[q], rdx), exb, exa, p9[q], qx));
+            const float tz = y3_s(y3_d(hx[q], hxkm, rdx), ezb[q], eza[q], p8[q], qz);
+            const float tx = y3_s(y3_d(hz[q], hzp[q], rdx), exb, exa, p9[q], qx);
             const bool v = vyH && vzE;
-            const float curl = (iin && kin) ? cs : 0.f;
+            const float curl = y3_curl(tz, !kin, pmz, tx, !iin, pmx);
             const float ec = y3_ec(ep[q], epj[q]);
             en[1][q] = v ? (PL ? (DAMP ? y3_epd(en[1][q], curl, a1[1][q], a2[1][q], ec, spc[1][q],
                                                 spn[1][q])
@@ -778,9 +787,9 @@ __global__ void __launch_bounds__(32 * SPLIT_Y, 2) k_yee3d_e(const __grid_consta
         // Ez: valid k <= nz-2; curl on i, j interior
         {
             float qx, qy;
-            const float cs = __fsub_rn(y3_s(y3_d(hy[q], hyp[q], rdx), exb, exa, p10[q], qx),
-                                       y3_s(y3_d(hx[q], hxm[q], rdx), eyb, eya, p11[q], qy));
-            const float curl = (iin && jin) ? cs : 0.f;
+            const float tx = y3_s(y3_d(hy[q], hyp[q], rdx), exb, exa, p10[q], qx);
+            const float ty = y3_s(y3_d(hx[q], hxm[q], rdx), eyb, eya, p11[q], qy);
+            const float curl = y3_curl(tx, !iin, pmx, ty, !jin, pmy);
             const float ec = y3_ec(ep[q], (q < 3) ? ep[q + 1] : epk);
             en[2][q] = vz ? (PL ? (DAMP ? y3_epd(en[2][q], curl, a1[2][q], a2[2][q], ec, spc[2][q],
                                                  spn[2][q])
@@ -1152,6 +1161,10 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
         return fail(MTB_INVALID_ARG, "damping: give all 12 (d1, d2) arrays or none");
     if (n_damp && variant == 1)
         return fail(MTB_UNSUPPORTED, "conductive damping needs the split kernels");
+    if (S.pmc_axes < 0 || S.pmc_axes > 7)
+        return fail(MTB_INVALID_ARG, "pmc_axes %d is not a mask of x / y / z", S.pmc_axes);
+    if (S.pmc_axes && variant == 1)
+        return fail(MTB_UNSUPPORTED, "PMC walls need the split or one-pass kernels");
     if (S.n_poles < 0 || S.n_poles > MTB_MAX_POLES)
         return fail(MTB_INVALID_ARG, "n_poles %d outside [0, %d]", S.n_poles, MTB_MAX_POLES);
     if (S.n_poles > 0) {
@@ -1226,6 +1239,7 @@ int mtb_yee3d_plan_create(const mtb_yee3d_struct *s, const mtb_dft_region *regio
                 for (int h = 0; h < 2; ++h) q.dmp[c][h] = S.damp[c][h];
             q.np = S.n_poles;
             q.plane = (uint32_t)((int64_t)S.nx * S.ny * S.zpitch);
+            q.pmc = S.pmc_axes;
             for (int c = 0; c < 3; ++c) {
                 q.pp[c][0] = S.pol_p[c][par];
                 q.pp[c][1] = S.pol_p[c][par ^ 1];

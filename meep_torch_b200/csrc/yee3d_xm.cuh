@@ -232,6 +232,7 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
     // E phase of this warp (warp-uniform) and its flags
     const bool eact = !tail && !halo && slot > 0 && j < ny;
     const bool iin = i >= 1 && i <= nx - 2, jin = j >= 1 && j <= ny - 2;
+    const bool pmx = P.pmc & 1, pmy = (P.pmc >> 1) & 1, pmz = (P.pmc >> 2) & 1;
     const bool bxe = XY && eact && act && iin && inband(P.B, 0, 1, i);
     const bool bye = XY && eact && act && jin && inband(P.B, 1, 1, j);
     // x / y layer memory (band planes / tiles only) and the row's soft current cells
@@ -426,10 +427,10 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
             {
                 float qy = 0.f, qz;
                 const float dy = y3_d(hz[q], hzm[q], rdx);
-                const float cs = __fsub_rn(XY ? y3_s(dy, eyb, eya, p6[q], qy) : dy,
-                                           y3_s(y3_d(hy[q], hym, rdx), ezb[q], eza[q], p7[q], qz));
+                const float ty = XY ? y3_s(dy, eyb, eya, p6[q], qy) : dy;
+                const float tz = y3_s(y3_d(hy[q], hym, rdx), ezb[q], eza[q], p7[q], qz);
                 const bool v = xok && vzE;
-                const float curl = (jin && kin) ? cs : 0.f;
+                const float curl = y3_curl(ty, !jin, pmy, tz, !kin, pmz);
                 const float en1 = y3_e(en[0][q], curl, dt, y3_ec(ep[q], epi[q]));
                 en[0][q] = v ? en1 : en[0][q];
                 if (XY) p6[q] = v ? qy : p6[q];
@@ -438,10 +439,10 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
             {
                 float qz, qx = 0.f;
                 const float dx = y3_d(hz[q], c.hzp[q], rdx);
-                const float cs = __fsub_rn(y3_s(y3_d(hx[q], hxkm, rdx), ezb[q], eza[q], p8[q], qz),
-                                           XY ? y3_s(dx, exb, exa, p9[q], qx) : dx);
+                const float tz = y3_s(y3_d(hx[q], hxkm, rdx), ezb[q], eza[q], p8[q], qz);
+                const float tx = XY ? y3_s(dx, exb, exa, p9[q], qx) : dx;
                 const bool v = vyH && vzE;
-                const float curl = (iin && kin) ? cs : 0.f;
+                const float curl = y3_curl(tz, !kin, pmz, tx, !iin, pmx);
                 const float en1 = y3_e(en[1][q], curl, dt, y3_ec(ep[q], epj[q]));
                 en[1][q] = v ? en1 : en[1][q];
                 p8[q] = v ? qz : p8[q];
@@ -450,10 +451,9 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
             {
                 float qx = 0.f, qy = 0.f;
                 const float dx = y3_d(hy[q], c.hyp[q], rdx), dy = y3_d(hx[q], hxm[q], rdx);
-                const float cs = XY ? __fsub_rn(y3_s(dx, exb, exa, p10[q], qx),
-                                                y3_s(dy, eyb, eya, p11[q], qy))
-                                    : __fsub_rn(dx, dy);
-                const float curl = (iin && jin) ? cs : 0.f;
+                const float tx = XY ? y3_s(dx, exb, exa, p10[q], qx) : dx;
+                const float ty = XY ? y3_s(dy, eyb, eya, p11[q], qy) : dy;
+                const float curl = y3_curl(tx, !iin, pmx, ty, !jin, pmy);
                 const float en1 = y3_e(en[2][q], curl, dt, y3_ec(ep[q], (q < 3) ? ep[q + 1] : epk));
                 en[2][q] = vz ? en1 : en[2][q];
                 if (XY) {

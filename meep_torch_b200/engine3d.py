@@ -101,7 +101,6 @@ class Engine3D:
         pols = getattr(coeffs, "pols", None)
         n_p = 0 if pols is None else int(pols["x"][2].shape[0])
         _need(n_p <= L.MTB_MAX_POLES, f"{n_p} dispersive poles (at most {L.MTB_MAX_POLES})")
-        _need(not getattr(coeffs, "pmc", ()), "PMC walls")
         # conductive damping (core/stepper_3d.py:217-235): the plain step when every pair
         # is (1, dt), else the split kernels' damped form with the 12 arrays
         dtf = torch.tensor(float(coeffs.dt), dtype=torch.float32)
@@ -116,6 +115,8 @@ class Engine3D:
         S.dt, S.dx = float(coeffs.dt), float(coeffs.dx)
         self._dt = float(coeffs.dt)
         S.point_sign = int(point_sign)
+        # PMC walls (core/stepper_3d.py _term_pmc): bit a set for a PMC wall on axis a
+        S.pmc_axes = sum(1 << int(a) for a in set(getattr(coeffs, "pmc", ()) or ()))
         self.box = {}
         for q, k in enumerate(FIELDS):
             pair = self._pair(g[k])

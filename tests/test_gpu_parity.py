@@ -181,6 +181,8 @@ def _run3d(lean, variant=0, case=None):
         if "n_abs" in g:
             kw.update(n_abs=int(g["n_abs"]),
                       absorber_axes=tuple(int(a) for a in g["absorber_axes"]))
+        if "pmc_axes" in g:
+            kw.update(pmc_axes=tuple(int(a) for a in g["pmc_axes"]))
         c = build_3d_coeffs(nx, ny, nz, dx, eps=eps, npml=npml, device=dev(), **kw)
         dt = c.dt
     src = PointSource3D(dt, "Ez", i, j, k, prof)
@@ -202,11 +204,14 @@ def _run3d(lean, variant=0, case=None):
                                                 (2, True, None), (3, True, None),
                                                 (2, False, "3d_sigma"), (2, False, "3d_poles"),
                                                 (2, False, "3d_abs"), (2, False, "3d_mixed"),
+                                                (2, False, "3d_pmc"), (3, False, "3d_pmc"),
                                                 (2, True, "3d_lean_poles")])
 def test_3d_matches_reference(lean, variant, case):
     """3D golden cases; 3d_sigma adds conductive damping (sigma_d on E, sigma_b on H);
     3d_abs is the matched-sigma absorber on every face (no CPML), 3d_mixed the absorber
-    on z beside x / y CPML (core/stepper_3d.py:150-235)."""
+    on z beside x / y CPML (core/stepper_3d.py:150-235); 3d_pmc puts PMC walls on y
+    beside x / z CPML (core/stepper_3d.py _term_pmc / _pad_interior), on the split and the
+    one-pass kernels."""
     st, accs, mons, dx = _run3d(lean, variant, case)
     name = case or ("3d_lean" if lean else "3d")
     e32, e64 = {}, {}
