@@ -178,6 +178,29 @@ typedef struct mtb_yee2d_struct {
      * (variant 2); the other variants and the adjoint return MTB_UNSUPPORTED. */
     const float *mag_h1[2];
     const float *mag_h2[2];
+    /* Symmetry cuts at the low-y / low-x edges (core/coeffs.py:148-285 y_mirror,
+     * x_mirror, y_rot2, rot4 and :375-503; core/stepper_tm.py:85-166,
+     * core/stepper_te.py:73-111). The cut row / column of the D component is
+     * live and the far wall stays PEC. cut_y / cut_x:
+     *   0  no cut;
+     *   1  TM: the H ghost beyond the cut is zero (even mirror);
+     *      TE: the D row on the cut takes dHz/dn = 2 Hz / dx (even mirror;
+     *      an odd TE mirror changes only the CPML profiles: pass 0);
+     *   2  TM: the on-plane H line beyond the cut is live (odd mirror, Rotate2,
+     *      Rotate4), held in f_x0 (nx floats, the Hx row at the y cut) or
+     *      f_y0 (ny floats, the Hy column at the x cut) and advanced from the
+     *      ghost Ez = cut_ph * Ez(partner): cut_map 0 = the cut cell itself,
+     *      1 = reversed along the cut (Rotate2, y cut only), 2 = the transposed
+     *      cell of the other cut (Rotate4, square grids).
+     * The caller packs the E-side CPML memory and the (b, a) node profiles
+     * from the cut row (offset 0). Tile kernels only (variant 2); the other
+     * variants, the no-alloc entry and the adjoint return MTB_UNSUPPORTED. */
+    int32_t cut_y, cut_x;
+    int32_t cut_map_y, cut_map_x;
+    float cut_ph_y, cut_ph_x;
+    int32_t pad2_[2];
+    float *f_x0[2];
+    float *f_y0[2];
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

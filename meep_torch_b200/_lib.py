@@ -49,7 +49,11 @@ class Yee2DStruct(C.Structure):
                 ("cond_d1", vp * 2), ("cond_d2", vp * 2),
                 ("n_poles", C.c_int32), ("n_poles_y", C.c_int32), ("pol_p", vp * 3),
                 ("pol_c", vp * 3), ("pol_py", vp * 3), ("pol_cy", vp * 3),
-                ("mag_h1", vp * 2), ("mag_h2", vp * 2)]
+                ("mag_h1", vp * 2), ("mag_h2", vp * 2),
+                ("cut_y", C.c_int32), ("cut_x", C.c_int32), ("cut_map_y", C.c_int32),
+                ("cut_map_x", C.c_int32), ("cut_ph_y", C.c_float), ("cut_ph_x", C.c_float),
+                ("pad2_", C.c_int32 * 2),
+                ("f_x0", vp * 2), ("f_y0", vp * 2)]
 
 
 class PhaseGroup(C.Structure):

@@ -3,10 +3,10 @@
 
 The NamedTuple field names are the reference's, so either side's objects can
 be handed to either side's run drivers. The builders cover the B200 path's
-feature set -- scalar eps, CPML (kappa = 1), PEC walls or TM PMC-in-y walls,
-electric conductivity (sigma_d); the reference's dispersive, magnetic-conductive,
-nonlinear and symmetry options raise NotImplementedError here (the reference itself
-still runs them).
+feature set -- scalar eps, CPML (kappa = 1), PEC walls, TM PMC-in-y walls and the
+low-edge symmetry cuts (mirrors; TM Rotate2 / Rotate4), conductivity, permeability and
+dispersive poles; the reference's nonlinear, magnetic-pole and tensor options raise
+NotImplementedError here (the reference itself still runs them).
 """
 import math
 from typing import NamedTuple
@@ -122,9 +122,27 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("chi3", "chi2", "m_poles",
-                "m_pole_masks", "y_mirror", "x_mirror", "y_rot2", "rot4", "eps_tensor",
+_UNSUPPORTED = ("chi3", "chi2", "m_poles", "m_pole_masks", "y_rot2", "rot4", "eps_tensor",
                 "poles_tensor", "pole_masks_tensor")
+
+
+def _check_parity(**kw):
+    for k, v in kw.items():
+        if v not in (0, 1, -1):
+            raise ValueError(f"symmetry parity {k}={v}: must be 0, +1 or -1")
+
+
+def _cut_axes(grid, px, py, y_cut, x_cut, y_pmc=False):
+    """A low-edge symmetry cut takes the place of that side's absorber: the kept half
+    spans the cut plane to the far edge, so the low layer count drops to zero before the
+    fit check (core/coeffs.py:209-220, :459-469)."""
+    if y_cut:
+        py = (0, py[1])
+    if x_cut:
+        px = (0, px[1])
+    if sum(px) >= grid.nx or (sum(py) >= grid.ny and not y_pmc):
+        raise ValueError(f"npml too large for grid {grid.nx}x{grid.ny}")
+    return px, py
 
 
 def _reject(kw):
@@ -200,35 +218,56 @@ def _poles_tm(grid: Grid, eps, poles, pole_masks):
 
 def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     y_pmc: bool = False, sigma_d=None, sigma_b=None, mu=None,
+                    y_mirror: int = 0, x_mirror: int = 0, y_rot2: int = 0, rot4: int = 0,
                     **kw) -> TMCoeffs:
     """TM coefficients: eps map, CPML profiles sliced to the live nodes --
     H side on the n-1 half nodes, E side on the interior [1:-1] (the full
     axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291;
     ``sigma_d``, ``sigma_b``, ``mu`` (scalars or (nx, ny)) give the conductivity and
     permeability pairs of :161-175, ``poles`` / ``pole_masks`` the ADE recurrences of
-    :87-106, :195-203."""
+    :87-106, :195-203. ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd), ``y_rot2`` and
+    ``rot4`` (phase +-1) cut the low-y / low-x edge (:209-285): no absorber on the cut
+    side, and the E-side profiles run from the cut node to the node before the far wall."""
     _reject(kw)
+    _check_parity(y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4)
+    if y_mirror and y_rot2:
+        raise ValueError("y_mirror and y_rot2 both cut the low-y edge")
+    if rot4 and (y_mirror or x_mirror or y_rot2):
+        raise ValueError("rot4 cuts both low edges by itself")
+    if rot4 and grid.nx != grid.ny:
+        raise ValueError(f"rot4 needs a square grid, got {grid.nx}x{grid.ny}")
+    y_cut, x_cut = bool(y_mirror or y_rot2 or rot4), bool(x_mirror or rot4)
+    if y_pmc and (y_cut or x_cut):
+        raise ValueError("symmetry cuts and y_pmc exclude each other")
+    live_line = y_mirror == -1 or x_mirror == -1 or y_rot2 or rot4
+    if live_line and (sigma_b is not None or mu is not None):
+        raise NotImplementedError("odd mirror / Rotate2 / Rotate4 with sigma_b or mu: the "
+                                  "on-plane H line has no magnetic coefficients")
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
     zero = _as_field(None, grid, 0.0)
-    px, py = _axis_sides(npml)
-    if sum(px) >= grid.nx or (sum(py) >= grid.ny and not y_pmc):
-        raise ValueError(f"npml={npml} too large for grid {grid.nx}x{grid.ny}")
+    px, py = _cut_axes(grid, *_axis_sides(npml), y_cut, x_cut, y_pmc)
 
     def prof(n, offset, pair, use=True):
         return cpml_profiles(n, pair if use else 0, offset, dt, dx, dtype=grid.dtype,
                              device=grid.device)
 
+    def e_side(n, pair, cut, full=False):
+        # the E-side (integer node) profile over the nodes whose D is updated
+        v = prof(n, 0.0, pair, use=not full)
+        if full:
+            return v
+        return tuple(t[:-1] for t in v) if cut else tuple(t[1:-1] for t in v)
+
     b_hy, a_hy, k_hy = prof(grid.ny - 1, 0.5, py, use=not y_pmc)
     b_hx, a_hx, k_hx = prof(grid.nx - 1, 0.5, px)
-    b_ex, a_ex, k_ex = (v[1:-1] for v in prof(grid.nx, 0.0, px))
-    b_ey, a_ey, k_ey = prof(grid.ny, 0.0, py, use=not y_pmc)
-    if not y_pmc:
-        b_ey, a_ey, k_ey = b_ey[1:-1], a_ey[1:-1], k_ey[1:-1]
+    b_ex, a_ex, k_ex = e_side(grid.nx, px, x_cut)
+    b_ey, a_ey, k_ey = e_side(grid.ny, py, y_cut, full=y_pmc)
     c1, c2, c3 = _poles_tm(grid, eps, list(poles), pole_masks)
     return TMCoeffs(
         dt=dt, dx=dx, eps_inf=eps, chi3=zero, has_kerr=False, c1=c1, c2=c2, c3=c3,
-        y_pmc=y_pmc,
+        y_pmc=y_pmc, y_mirror_lo=y_mirror, x_mirror_lo=x_mirror, y_rot2_lo=y_rot2,
+        rot4_lo=rot4,
         b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
@@ -265,19 +304,20 @@ def _axis_poles(grid: Grid, eps, shared, axis_poles, shared_masks, axis_masks, s
 
 def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     sigma_d=None, poles_x=(), poles_y=(), pole_masks_x=None,
-                    pole_masks_y=None, sigma_b=None, mu=None, **kw) -> TECoeffs:
+                    pole_masks_y=None, sigma_b=None, mu=None, y_mirror: int = 0,
+                    x_mirror: int = 0, **kw) -> TECoeffs:
     """TE coefficients: eps Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1)
     (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491, with
     ``sigma_d``, ``sigma_b``, ``mu`` the conductivity and permeability pairs of
     :401-415, and the per-axis ADE pole stacks of :416-425 (shared ``poles`` on both
-    axes, ``poles_x`` / ``poles_y`` on one)."""
+    axes, ``poles_x`` / ``poles_y`` on one). ``y_mirror`` / ``x_mirror`` (+-1) cut the
+    low edge (:457-469): no absorber there; the profiles keep their interior slices."""
     _reject(kw)
+    _check_parity(y_mirror=y_mirror, x_mirror=x_mirror)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
     zero = _as_field(None, grid, 0.0)
-    px, py = _axis_sides(npml)
-    if sum(px) >= grid.nx or sum(py) >= grid.ny:
-        raise ValueError(f"npml={npml} too large for grid {grid.nx}x{grid.ny}")
+    px, py = _cut_axes(grid, *_axis_sides(npml), bool(y_mirror), bool(x_mirror))
 
     def prof(n, offset, pair):
         return cpml_profiles(n, pair, offset, dt, dx, dtype=grid.dtype, device=grid.device)
@@ -299,4 +339,5 @@ def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         chi2_x=_avg_to_ex(zero), chi2_y=_avg_to_ey(zero), has_chi2=False,
+        y_mirror_lo=y_mirror, x_mirror_lo=x_mirror,
         **_cond_te(grid, sigma_d, sigma_b, mu))

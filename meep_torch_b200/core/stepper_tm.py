@@ -15,31 +15,38 @@ class TMState(NamedTuple):
     P_prev: torch.Tensor
     psi_Ezy: torch.Tensor  # (nx, ny-1)      CPML memory of dEz/dy (Hx update)
     psi_Ezx: torch.Tensor  # (nx-1, ny)      dEz/dx (Hy update)
-    psi_Hyx: torch.Tensor  # (nx-2, ny_e)    dHy/dx (Dz update, live Ez region)
-    psi_Hxy: torch.Tensor  # (nx-2, ny_e)    dHx/dy
+    psi_Hyx: torch.Tensor  # (nx_e, ny_e)    dHy/dx (Dz update, live Ez region)
+    psi_Hxy: torch.Tensor  # (nx_e, ny_e)    dHx/dy
     Bx: torch.Tensor | None = None
     By: torch.Tensor | None = None
     Mx_cur: torch.Tensor | None = None
     Mx_prev: torch.Tensor | None = None
     My_cur: torch.Tensor | None = None
     My_prev: torch.Tensor | None = None
-    Hx0: torch.Tensor | None = None
-    Hy0: torch.Tensor | None = None
+    Hx0: torch.Tensor | None = None   # (nx,) on-plane Hx row at a live low-y cut
+    Hy0: torch.Tensor | None = None   # (ny,) on-plane Hy column at a live low-x cut
 
 
-def init_tm_state(grid: Grid, n_poles: int = 0, y_pmc: bool = False, **kw) -> TMState:
-    """Zero TM state; psi_Hyx/psi_Hxy cover the interior (ny_e = ny-2) or
-    every row under y_pmc (ny_e = ny), as core/stepper_tm.py:41-71; P_cur /
-    P_prev hold one (nx, ny) plane per dispersive pole."""
+def init_tm_state(grid: Grid, n_poles: int = 0, y_pmc: bool = False, y_mirror: int = 0,
+                  x_mirror: int = 0, y_rot2: int = 0, rot4: int = 0, **kw) -> TMState:
+    """Zero TM state, as core/stepper_tm.py:41-71: psi_Hyx / psi_Hxy cover the live
+    Ez region -- the interior, every column under y_pmc, or from the cut row / column
+    of a low-edge symmetry cut; P_cur / P_prev hold one (nx, ny) plane per dispersive
+    pole; Hx0 / Hy0 are the on-plane H lines that an odd mirror, Rotate2 or Rotate4
+    keeps live."""
     for k, v in kw.items():
         if v:
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
     nx, ny = grid.nx, grid.ny
-    ny_e = ny if y_pmc else ny - 2
+    y_cut, x_cut = bool(y_mirror or y_rot2 or rot4), bool(x_mirror or rot4)
+    ny_e = ny if y_pmc else (ny - 1 if y_cut else ny - 2)
+    nx_e = nx - 1 if x_cut else nx - 2
     z = grid.zeros
     return TMState(Ez=z(nx, ny), Hx=z(nx, ny - 1), Hy=z(nx - 1, ny), Dz=z(nx, ny),
                    P_cur=z(n_poles, nx, ny), P_prev=z(n_poles, nx, ny), psi_Ezy=z(nx, ny - 1),
-                   psi_Ezx=z(nx - 1, ny), psi_Hyx=z(nx - 2, ny_e), psi_Hxy=z(nx - 2, ny_e))
+                   psi_Ezx=z(nx - 1, ny), psi_Hyx=z(nx_e, ny_e), psi_Hxy=z(nx_e, ny_e),
+                   Hx0=z(nx) if (y_mirror == -1 or y_rot2 or rot4) else None,
+                   Hy0=z(ny) if (x_mirror == -1 or rot4) else None)
 
 
 def step_tm(state, m, src_amp=0.0, src_mask=None, src_h_amp: float = 0.0,

@@ -912,6 +912,39 @@ __device__ __forceinline__ void tm_hy(const mtb_yee2d_struct &S, int r, bool val
         apply_cells(S.src_h1, r, amp_h, jb, out);
 }
 
+// Ez(n) of one cell as tm_tile forms it for its own rows: the imported Ez on an
+// explicit first step, else (Dz - sum_k P_k) / eps with the poles summed in order.
+template <bool EXPL, bool EXT>
+__device__ __forceinline__ float tm_ez_at(const mtb_yee2d_struct &S, const Ctx2D &C, int i,
+                                          int j) {
+    const uint32_t o = (uint32_t)i * S.pitch + j;
+    if (EXPL) return S.e_explicit[o];
+    float sp = 0.f;
+    const float *Pc = S.pol_p[C.pst];
+    const uint32_t pl = (uint32_t)S.nx * S.pitch;
+#pragma unroll 1
+    for (int k = 0; k < (EXT ? S.n_poles : 0); ++k) sp += Pc[k * pl + o];
+    return (S.f_main[C.par][o] - sp) * S.inv_eps_a[o];
+}
+
+// The live on-plane H line beyond a TM symmetry cut (core/stepper_tm.py:95-113):
+// H0' = H0 -/+ dt (Ez_cut - ghost) / dx, ghost = ph * Ez(partner). `a` = 0 for
+// the Hx row at the y cut (cell (k, 0), minus), 1 for the Hy column at the x cut
+// (cell (0, k), plus); ez is Ez(n) of the cut cell.
+template <bool EXPL, bool EXT>
+__device__ __forceinline__ float tm_cut_line(const mtb_yee2d_struct &S, const Ctx2D &C, int a,
+                                             int k, float ez, float dt, float rdx) {
+    const int map = a ? S.cut_map_x : S.cut_map_y;
+    const float ph = a ? S.cut_ph_x : S.cut_ph_y;
+    float partner = ez;
+    if (map == 1) partner = tm_ez_at<EXPL, EXT>(S, C, S.nx - 1 - k, 0);
+    else if (map == 2) partner = a ? tm_ez_at<EXPL, EXT>(S, C, k, 0)
+                                   : tm_ez_at<EXPL, EXT>(S, C, 0, k);
+    const float d = (ez - ph * partner) * rdx;
+    const float *h0 = a ? S.f_y0[C.par] : S.f_x0[C.par];
+    return a ? h0[k] + dt * d : h0[k] - dt * d;
+}
+
 template <bool EXPL, bool EXT>
 __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, const int c0,
                                         const Ctx2D &C, const mtb_line_sample *L, const int nl) {
@@ -926,7 +959,9 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
     const float *__restrict__ Hx = S.f_x[par];
     const float *__restrict__ Hy = S.f_y[par];
     const float *__restrict__ ie = S.inv_eps_a;
-    const bool hyRow = i <= nx - 2, dzRow = i >= 1 && i <= nx - 2;
+    // symmetry cuts: the cut row (x) / column (y) of Dz is live
+    const bool cutx = EXT && S.cut_x != 0, cuty = EXT && S.cut_y != 0;
+    const bool hyRow = i <= nx - 2, dzRow = (i >= 1 || cutx) && i <= nx - 2;
     const bool bxH = hyRow && in_band(i, S.xband[0], S.xband[1]);
     const bool bxHp = i >= 1 && in_band(i - 1, S.xband[0], S.xband[1]);
     const bool bxE = dzRow && in_band(i, S.xband[2], S.xband[3]);
@@ -1015,7 +1050,7 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
         vH[q] = act && j <= ny - 2;
-        vD[q] = act && dzRow && (pmc ? (j < ny) : (j >= 1 && j <= ny - 2));
+        vD[q] = act && dzRow && (pmc ? (j < ny) : ((j >= 1 || cuty) && j <= ny - 2));
         const bool oh = byH && j <= ny - 2, oe = byE && j < ny;
         hyb[q] = oh ? __ldg(S.hy_b + j) : 1.f;
         hya[q] = oh ? __ldg(S.hy_a + j) : 0.f;
@@ -1032,6 +1067,17 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
     tm_hy(S, i - 1, i >= 1, act, jb, hxbp, hxap, dt, rdx, ez0, ez1, hyp, p1p, hyP, C.amp_h,
           mh1y, mh2y);
     if (i < 1) zero4(hyP);
+    if (EXT && i == 0 && S.cut_x == 2 && act) {
+        // odd x mirror / Rotate4: the on-plane Hy column is the ghost of row 0
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = jb + q;
+            if (j < ny) {
+                hyP[q] = tm_cut_line<EXPL, EXT>(S, C, 1, j, ez1[q], dt, rdx);
+                S.f_y0[par ^ 1][j] = hyP[q];
+            }
+        }
+    }
     tm_hy(S, i, hyRow, act, jb, hxb, hxa, dt, rdx, ez1, ez2, hy, p1, hyN, C.amp_h, mh1y, mh2y);
 
     // Hx(n+1/2) row i (core/stepper_tm.py:91-94, :121-128): Hx' = Hx - dt curl, or
@@ -1064,6 +1110,10 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             v = magx ? S.mag_h1[0][ro - 1] * hxl - S.mag_h2[0][ro - 1] * c : hxl - dt * c;
             if (i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
                 v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
+        } else if (EXT && jb == 0 && S.cut_y == 2) {
+            // odd y mirror / Rotate2 / Rotate4: the on-plane Hx row is the ghost of column 0
+            v = tm_cut_line<EXPL, EXT>(S, C, 0, i, ez1[0], dt, rdx);
+            S.f_x0[par ^ 1][i] = v;
         }
         hxm0 = v;
     }
@@ -1225,8 +1275,11 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     const float *__restrict__ Dy = S.f_y[par];
     const float *__restrict__ iex = S.inv_eps_a;
     const float *__restrict__ iey = S.inv_eps_b;
+    // even symmetry cuts (core/stepper_te.py:88-97): the cut row of Dy (x cut) and
+    // column of Dx (y cut) are live with dHz/dn = 2 Hz / dx (odd Hz ghost)
+    const bool cutx = EXT && S.cut_x != 0, cuty = EXT && S.cut_y != 0;
     const bool hzRow = i <= nx - 2;                     // Hz, Dx (Ex) rows
-    const bool dyRow = i >= 1 && i <= nx - 2, dyRowN = i + 1 <= nx - 2;
+    const bool dyRow = (i >= 1 || cutx) && i <= nx - 2, dyRowN = i + 1 <= nx - 2;
     const bool bxH = hzRow && in_band(i, S.xband[0], S.xband[1]);
     const bool bxE = dyRow && in_band(i, S.xband[2], S.xband[3]);
     const bool bxEn = dyRowN && in_band(i + 1, S.xband[2], S.xband[3]);
@@ -1272,7 +1325,7 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
-        vX[q] = act && hzRow && j >= 1 && j <= ny - 2;
+        vX[q] = act && hzRow && (j >= 1 || cuty) && j <= ny - 2;
         vZ[q] = act && hzRow && j <= ny - 2;
         const bool oe = byE && j >= 1 && j <= ny - 2, oh = byH && j <= ny - 2;
         eyb[q] = oe ? __ldg(S.ey_b + j) : 1.f;
@@ -1281,7 +1334,7 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
         hya[q] = oh ? __ldg(S.hy_a + j) : 0.f;
     }
     float hm0 = __shfl_up_sync(0xffffffffu, hc[3], 1);
-    if (lane == 0) hm0 = hzL;
+    if (lane == 0) hm0 = (cuty && jb == 0) ? -hc[0] : hzL;
 
     // Dx / Ex(n+1/2) row i (core/stepper_te.py:79-95, :150-160)
     float dxN[4], ex[4];
@@ -1345,6 +1398,10 @@ __device__ __forceinline__ void te_tile(const mtb_yee2d_struct &S, const int i, 
     }
     // Dy / Ey(n+1/2) rows i and i+1 (recomputed halo)
     float dyN[4], ey[4], dyNn[4], eyn[4];
+    if (cutx && i == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) hp[q] = -hc[q];
+    }
     te_dy<EXT>(S, i, dyRow, act, jb, exb, exa, dt, rdx, hp, hc, dy, p1, dyN, C.amp_e);
     te_dy<EXT>(S, i + 1, dyRowN, act, jb, exbn, exan, dt, rdx, hc, hn, dyn, p1n, dyNn, C.amp_e);
 #pragma unroll
@@ -1626,7 +1683,8 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const bool lean = C.wr == WROWS && !expl && ib >= 1 && last <= S.nx - 2 &&
                       ib - 1 >= S.xband[0] && last < S.xband[1] &&
                       ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr &&
-                      S.n_poles == 0 && S.mag_h1[0] == nullptr && S.mag_h1[1] == nullptr;
+                      S.n_poles == 0 && S.mag_h1[0] == nullptr && S.mag_h1[1] == nullptr &&
+                      !(EXT && S.cut_y && w.z == 0);
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1858,7 +1916,8 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
     const bool lean = C.wr == WROWS && ib >= 1 && last + 1 <= S.nx - 2 && ib >= S.xband[0] &&
                       last < S.xband[1] &&
                       ib >= S.xband[2] && last + 1 < S.xband[3] && S.cond_d1[0] == nullptr &&
-                      S.n_poles == 0 && S.n_poles_y == 0 && S.mag_h1[0] == nullptr;
+                      S.n_poles == 0 && S.n_poles_y == 0 && S.mag_h1[0] == nullptr &&
+                      !(EXT && S.cut_y && w.z == 0);
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1954,11 +2013,11 @@ static int tmap_2d(CUtensorMap *m, const float *base, int nx, int pitch, int bc,
     return MTB_OK;
 }
 
-// Structures the TB kernels take: no conductivity, poles, magnetic pairs or
-// PMC walls (those run on the tile kernels' extended variant).
+// Structures the TB kernels take: no conductivity, poles, magnetic pairs, PMC
+// walls or symmetry cuts (those run on the tile kernels' extended variant).
 static bool tb_eligible(const mtb_yee2d_struct &S) {
     return !S.cond_d1[0] && !S.cond_d1[1] && !S.n_poles && !S.n_poles_y && !S.mag_h1[0] &&
-           !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc;
+           !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc && !S.cut_y && !S.cut_x;
 }
 
 // Copy n floats of a device array to the host.
@@ -2255,6 +2314,34 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         if (S.pol == MTB_TE && S.y_pmc)
             return fail(MTB_UNSUPPORTED, "structure %d: y_pmc is a TM option", s);
         int rc;
+        if (S.cut_y || S.cut_x) {
+            if (S.cut_y < 0 || S.cut_y > 2 || S.cut_x < 0 || S.cut_x > 2)
+                return fail(MTB_INVALID_ARG, "structure %d: cut_y / cut_x must be 0, 1 or 2", s);
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: symmetry cuts need the tile kernels "
+                            "(variant 2)", s);
+            if (S.y_pmc)
+                return fail(MTB_INVALID_ARG, "structure %d: symmetry cuts and y_pmc exclude "
+                            "each other", s);
+            if (S.pol == MTB_TE && (S.cut_y == 2 || S.cut_x == 2))
+                return fail(MTB_INVALID_ARG, "structure %d: TE cuts are 0 or 1", s);
+            for (int a = 0; a < 2; ++a) {
+                const int cut = a ? S.cut_x : S.cut_y, map = a ? S.cut_map_x : S.cut_map_y;
+                const float ph = a ? S.cut_ph_x : S.cut_ph_y;
+                if (cut != 2) continue;
+                if (map < 0 || map > 2 || (a == 1 && map == 1) || (ph != 1.f && ph != -1.f))
+                    return fail(MTB_INVALID_ARG, "structure %d: cut map %d / phase %g", s, map,
+                                (double)ph);
+                if (map == 2 && S.nx != S.ny)
+                    return fail(MTB_INVALID_ARG, "structure %d: Rotate4 needs a square grid", s);
+                for (int b = 0; b < 2; ++b)
+                    if ((rc = check_ptr(a ? S.f_y0[b] : S.f_x0[b], "f_x0 / f_y0", s))) return rc;
+                // the on-plane H line carries no magnetic pair (core/coeffs.py:240-244)
+                if (S.mag_h1[a ? 1 : 0] || S.mag_h2[a ? 1 : 0])
+                    return fail(MTB_UNSUPPORTED, "structure %d: a live on-plane H line with "
+                                "magnetic conductivity / permeability", s);
+            }
+        }
         for (int b = 0; b < 2; ++b) {
             if ((rc = check_ptr(S.f_main[b], "f_main", s))) return rc;
             if ((rc = check_ptr(S.f_x[b], "f_x", s))) return rc;
@@ -2369,7 +2456,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     for (int s = 0; s < n; ++s)
     {
         if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0 ||
-            structs[s].mag_h1[0] || structs[s].mag_h1[1])
+            structs[s].mag_h1[0] || structs[s].mag_h1[1] || structs[s].cut_y || structs[s].cut_x)
             p->ext = true;
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
     }
@@ -3109,8 +3196,10 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
     if (S.pol == MTB_TE && (S.y_pmc || S.src_h2.n > 0))
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
     if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles ||
-        S.n_poles_y || S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1])
-        return fail(MTB_UNSUPPORTED, "noalloc: conductivity and poles need the tile kernels");
+        S.n_poles_y || S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1] || S.cut_y ||
+        S.cut_x)
+        return fail(MTB_UNSUPPORTED, "noalloc: conductivity, poles and symmetry cuts need the "
+                    "tile kernels");
     int rc;
     for (int b = 0; b < 2; ++b) {
         if ((rc = check_ptr(S.f_main[b], "f_main", 0)) || (rc = check_ptr(S.f_x[b], "f_x", 0)) ||

@@ -50,6 +50,39 @@ def _opt_none(obj, names):
               f"{type(obj).__name__}.{n} is set: not supported by the B200 path")
 
 
+def _cuts(c, te):
+    """The symmetry cuts of a coefficient tuple as the struct's (cut, map, phase) per
+    axis (y, x): core/coeffs.py y_mirror / x_mirror / y_rot2 / rot4 (TM) and y_mirror /
+    x_mirror (TE). TM: 1 = even mirror (zero H ghost), 2 = a live on-plane H line whose
+    ghost Ez is phase * Ez(partner), map 0 the cut cell, 1 reversed (Rotate2), 2 the
+    other cut's transposed cell (Rotate4). TE: only the even mirror touches the step."""
+    ym = int(getattr(c, "y_mirror_lo", 0) or 0)
+    xm = int(getattr(c, "x_mirror_lo", 0) or 0)
+    if te:
+        return (1 if ym == 1 else 0, 0, 1.0), (1 if xm == 1 else 0, 0, 1.0)
+    r2 = int(getattr(c, "y_rot2_lo", 0) or 0)
+    r4 = int(getattr(c, "rot4_lo", 0) or 0)
+    if ym == 1:
+        cy = (1, 0, 1.0)
+    elif ym == -1:
+        cy = (2, 0, -1.0)
+    elif r2:
+        cy = (2, 1, float(r2))
+    elif r4:
+        cy = (2, 2, float(r4))
+    else:
+        cy = (0, 0, 1.0)
+    if xm == 1:
+        cx = (1, 0, 1.0)
+    elif xm == -1:
+        cx = (2, 0, -1.0)
+    elif r4:
+        cx = (2, 2, float(r4))
+    else:
+        cx = (0, 0, 1.0)
+    return cy, cx
+
+
 def _magnetic_pairs(c, pairs):
     """The magnetic pairs (h1, h2) of core/coeffs.py:161-175, :401-415, one entry per H
     component named in ``pairs``: None where they are absent or inert (h1 = 1 and h2 =
@@ -182,17 +215,24 @@ class Engine2D:
             for n_, cn in ((s.Px_cur.shape[0], "c1x"), (s.Py_cur.shape[0], "c1y")):
                 _need(n_ <= L.MTB_MAX_POLES, f"{n_} dispersive poles (at most {L.MTB_MAX_POLES})")
                 _need(getattr(c, cn).shape[0] == n_, f"pole coefficients {cn} count")
-            _opt_none(c, ["inv_xx_x", "c3xy", "c3yx", "has_chi2", "y_mirror_lo", "x_mirror_lo"])
+            _opt_none(c, ["inv_xx_x", "c3xy", "c3yx", "has_chi2"])
             it.mag = _magnetic_pairs(c, [("hz1", "hz2")])
         else:
             it.nx, it.ny = main.shape
             np_ = s.P_cur.shape[0]
             _need(np_ <= L.MTB_MAX_POLES, f"{np_} dispersive poles (at most {L.MTB_MAX_POLES})")
             _need(tuple(c.c1.shape) == (np_, it.nx, it.ny), "pole coefficients c1 shape")
-            _opt_none(s, ["Bx", "Hx0", "Hy0"])
-            _opt_none(c, ["mc1x", "has_chi2", "y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
-                          "rot4_lo"])
+            _opt_none(s, ["Bx"])
+            _opt_none(c, ["mc1x", "has_chi2"])
             it.mag = _magnetic_pairs(c, [("h1x", "h2x"), ("h1y", "h2y")])
+        it.cuts = _cuts(c, it.te)
+        if not it.te:
+            # the live on-plane H lines of the cuts (init_tm_state Hx0 / Hy0)
+            for (cut, _, _), name, n in ((it.cuts[0], "Hx0", it.nx), (it.cuts[1], "Hy0", it.ny)):
+                h0 = getattr(s, name, None)
+                _need((cut == 2) == (h0 is not None),
+                      f"TMState.{name} does not match the coefficients' symmetry cut")
+                _need(h0 is None or tuple(h0.shape) == (n,), f"TMState.{name} shape")
         _need(not getattr(c, "has_kerr", False), "Kerr (chi3) media")
         for k in ("k_hx", "k_hy", "k_ex", "k_ey"):
             kv = getattr(c, k)
@@ -250,6 +290,8 @@ class Engine2D:
                 fb.copy_(b); fa.copy_(a)
             elif b.numel() == n - 2:
                 fb[1:-1] = b; fa[1:-1] = a
+            elif b.numel() == n - 1 and not it.te:
+                fb[:-1] = b; fa[:-1] = a                  # from the cut row (TM cuts)
             else:
                 raise MtbUnsupported(f"unexpected CPML profile length {b.numel()} for n={n}")
             return fb, fa
@@ -338,10 +380,13 @@ class Engine2D:
                     self._pair(s.Hy, nx, P)
                 eps_a = self._pack(c.eps_inf, nx, P)
                 inv_a = self._pack(torch.reciprocal(c.eps_inf.to(torch.float32)), nx, P)
-                yoff = 0 if S.y_pmc else 1
+                # the E-side CPML memory covers the interior, or from the cut row /
+                # column (symmetry cuts), or every column (y PMC)
+                xoff = 1 if s.psi_Hyx.shape[0] == nx - 2 else 0
+                yoff = 1 if s.psi_Hyx.shape[1] == ny - 2 else 0
                 psis = [self._pair(s.psi_Ezy, nx, P), self._pair(s.psi_Ezx, nx, P),
-                        self._pair(s.psi_Hyx, nx, P, (1, yoff)),
-                        self._pair(s.psi_Hxy, nx, P, (1, yoff))]
+                        self._pair(s.psi_Hyx, nx, P, (xoff, yoff)),
+                        self._pair(s.psi_Hxy, nx, P, (xoff, yoff))]
                 # dispersive poles: P planes (ping-pong) and c1, c2, c3
                 # (core/stepper_tm.py:203-231)
                 n_p = s.P_cur.shape[0]
@@ -369,6 +414,16 @@ class Engine2D:
                     it.keep.append(eex)
             it.box = dict(main=f_main, x=f_x, y=f_y, psi=psis, eps_a=eps_a, eps_b=eps_b,
                           inv_a=inv_a)
+            (S.cut_y, S.cut_map_y, S.cut_ph_y), (S.cut_x, S.cut_map_x, S.cut_ph_x) = it.cuts
+            for name, attr in (("Hx0", "f_x0"), ("Hy0", "f_y0")):
+                h0 = None if te else getattr(s, name, None)
+                if h0 is None:
+                    continue
+                buf = torch.zeros((2, _round4(h0.shape[0])), dtype=torch.float32, device=dev)
+                buf[:, :h0.shape[0]] = h0.detach().to(device=dev, dtype=torch.float32)
+                getattr(S, attr)[0], getattr(S, attr)[1] = L.ptr(buf[0]), L.ptr(buf[1])
+                it.box[name] = buf
+                it.keep.append(buf)
             if pol_bufs is not None:
                 if te:
                     for ax, bufs in pol_bufs.items():
@@ -387,7 +442,7 @@ class Engine2D:
             # current on D scaled by d2 (core/stepper_tm.py:158-163, :197-200;
             # core/stepper_te.py D update and step_source)
             it.src_scale = None
-            it.plain = not te and not S.n_poles and not S.explicit_e
+            it.plain = not te and not S.n_poles and not S.explicit_e and not (S.cut_y or S.cut_x)
             cond = ([("d1x", "d2x"), ("d1y", "d2y")] if te else [("d1", "d2")])
             if getattr(c, cond[0][0], None) is not None:
                 for k, (n1, n2) in enumerate(cond):
@@ -799,16 +854,19 @@ class Engine2D:
         else:
             Ez = self._unpack(bx["main"][cur], (nx, ny), den=bx["eps_a"])
         ps = bx["psi"]
-        ny_e = s.psi_Hyx.shape[1]
-        yoff = 0 if ny_e == ny else 1
+        nx_e, ny_e = s.psi_Hyx.shape
+        xoff, yoff = int(nx_e == nx - 2), int(ny_e == ny - 2)
+        for name, n in (("Hx0", nx), ("Hy0", ny)):
+            if name in bx:
+                pol[name] = bx[name][cur, :n].clone()
         return s._replace(
             Ez=Ez, Dz=Dz, **pol,
             Hx=self._unpack(bx["x"][cur], (nx, ny - 1)),
             Hy=self._unpack(bx["y"][cur], (nx - 1, ny)),
             psi_Ezy=self._unpack(ps[0][cur], (nx, ny - 1)),
             psi_Ezx=self._unpack(ps[1][cur], (nx - 1, ny)),
-            psi_Hyx=self._unpack(ps[2][cur], (nx - 2, ny_e), (1, yoff)),
-            psi_Hxy=self._unpack(ps[3][cur], (nx - 2, ny_e), (1, yoff)))
+            psi_Hyx=self._unpack(ps[2][cur], (nx_e, ny_e), (xoff, yoff)),
+            psi_Hxy=self._unpack(ps[3][cur], (nx_e, ny_e), (xoff, yoff)))
 
     def accumulators(self, b: int = 0):
         return list(self.items[b].accs)

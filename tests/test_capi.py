@@ -106,6 +106,38 @@ def test_tm_coeffs_match_oracle(npml, pmc):
         np.testing.assert_allclose(getattr(m, k).numpy(), o[k], rtol=2e-6, atol=1e-7)
 
 
+FOLDS_TM = [dict(y_mirror=1), dict(y_mirror=-1), dict(x_mirror=1),
+            dict(x_mirror=-1, y_mirror=1), dict(y_rot2=1), dict(y_rot2=-1), dict(rot4=1),
+            dict(rot4=-1)]
+
+
+@pytest.mark.parametrize("fold", FOLDS_TM + [dict(y_mirror=1, x_mirror=-1, te=1),
+                                             dict(y_mirror=-1, x_mirror=1, te=1)])
+def test_fold_coeffs_and_state_match_oracle(fold):
+    """Symmetry cuts: the profiles (no absorber on the cut side, E-side slices from the
+    cut node) and the TM state shapes (psi over the live Ez region, Hx0 / Hy0)."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    fold = dict(fold)
+    te = fold.pop("te", 0)
+    g = Grid(nx=40, ny=40, dx=0.05, device="cpu")
+    if te:
+        m = build_te_coeffs(g, npml=8, **fold)
+        o = O.te_coeffs(40, 40, 0.05, npml=8, dtype=np.float32, **fold)
+    else:
+        m = build_tm_coeffs(g, npml=8, **fold)
+        o = O.tm_coeffs(40, 40, 0.05, npml=8, dtype=np.float32, **fold)
+        s, so = init_tm_state(g, **fold), O.tm_state(o)
+        for k in ("psi_Hyx", "psi_Hxy", "Hx0", "Hy0"):
+            a, b = getattr(s, k), so.get(k)
+            assert (a is None) == (b is None), k
+            if a is not None:
+                assert tuple(a.shape) == b.shape, k
+    for k in ("b_hy", "a_hy", "b_hx", "a_hx", "b_ex", "a_ex", "b_ey", "a_ey"):
+        np.testing.assert_allclose(getattr(m, k).numpy(), o[k], rtol=2e-6, atol=1e-7)
+
+
 def test_te_and_3d_coeffs_match_oracle():
     from meep_torch_b200.core.coeffs import build_te_coeffs
     from meep_torch_b200.core.grid import Grid

@@ -92,6 +92,59 @@ def test_tm_matches_reference(case):
     assert not bad, bad
 
 
+FOLD_CASES = [("tm", "ym_even"), ("tm", "ym_odd"), ("tm", "xm_even"), ("tm", "xm_odd_ym_even"),
+              ("tm", "rot2_even"), ("tm", "rot2_odd"), ("tm", "rot4_even"), ("tm", "rot4_odd"),
+              ("te", "ym_even_xm_odd"), ("te", "ym_odd_xm_even")]
+
+
+@pytest.mark.parametrize("pol,fold", FOLD_CASES)
+def test_fold_matches_reference(pol, fold):
+    """Symmetry-folded runs (core/stepper_tm.py:85-166, core/stepper_te.py:73-111):
+    mirrors, Rotate2 and Rotate4 at the low-x / low-y edges, absorber on the far sides, a
+    line source beside the cut; every state array (the on-plane Hx0 / Hy0 lines and the
+    CPML memory from the cut row included) and the full-grid DFT, 250 steps."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor
+    from meep_torch_b200.core.run import run_te, run_tm
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource, TESource
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    name = f"{pol}_fold_{fold}"
+    g = load_golden(f"{name}_f32")
+    kw = json.loads(str(g["fold"]))
+    nx, ny, dx = int(g["nx"]), int(g["ny"]), float(g["dx"])
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    eps = torch.tensor(g["eps"], dtype=torch.float32)
+    src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
+                     profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
+    freqs = [float(f) for f in g["freqs"]]
+    if pol == "tm":
+        m = build_tm_coeffs(grid, eps_inf=eps, npml=int(g["npml"]), **kw)
+        dft = DFTFieldsMonitor(grid, freqs, "Ez")
+        st, (acc,) = run_tm(init_tm_state(grid, **kw), m, int(g["n_steps"]), source=src,
+                            monitors=[dft])
+    else:
+        m = build_te_coeffs(grid, eps_inf=eps, npml=int(g["npml"]), **kw)
+        src = TESource(src)
+        dft = DFTFieldsMonitor(grid, freqs, "Hz")
+        st, (acc,) = run_te(init_te_state(grid), m, int(g["n_steps"]), source=src,
+                            monitors=[dft])
+    np.testing.assert_array_equal(src.mask.cpu().numpy(), g["mask"])
+    e32, e64 = {}, {}
+    for prec, errs in (("f32", e32), ("f64", e64)):
+        gg = load_golden(f"{name}_{prec}")
+        keys = [k[2:] for k in gg if k.startswith("s_")]
+        assert not [k for k in st._fields if getattr(st, k) is not None
+                    and getattr(st, k).numel() and k not in keys]
+        for k in keys:
+            errs[k] = rel_l2(getattr(st, k).cpu().numpy(), gg["s_" + k])
+        errs["acc_dft"] = rel_l2(acc.cpu().numpy(), gg["acc_dft"])
+    _report(name, e32, e64)
+    bad = {k: v for k, v in e32.items() if not v < TOL}
+    assert not bad, bad
+
+
 def test_tm_reference_phase_mode():
     """The float32 phase emulation reproduces the reference's own float32
     DFT phase arithmetic (core/monitors.py:43-46)."""
