@@ -186,8 +186,10 @@ class Engine2D:
     the reference's types and shapes."""
 
     def __init__(self, items, *, phase_mode: str = "exact", rows_per_warp: int = 0,
-                 ring_slots: int = 0, variant: int = 0, graph: bool = True, stream=None):
+                 ring_slots: int = 0, variant: int = 0, graph: bool = True, stream=None,
+                 arena: bool = False):
         self.lib = L.load()
+        self.use_arena = bool(arena)
         self.items = [_Item(*it) for it in items]
         _need(len(self.items) > 0, "empty batch")
         self.device = None
@@ -612,6 +614,8 @@ class Engine2D:
         self.n_regions = len(regions)
         self.groups = grp_arr
         self.n_groups = len(groups)
+        if self.use_arena:
+            self._make_arena(structs)
         tun = L.Tuning(rows_per_warp, ring_slots, 0 if graph else -1, variant)
         plan = C.c_void_p()
         L.check(lib.mtb_yee2d_plan_create(structs, len(self.items), reg_arr, len(regions),
@@ -619,6 +623,46 @@ class Engine2D:
                                           C.byref(plan)), "mtb_yee2d_plan_create")
         self.plan = plan
         self.structs = structs
+
+    def _make_arena(self, structs):
+        """Move every structure's stepped fields (main, x, y, the four CPML memories and
+        the on-plane cut lines) into one flat buffer per parity, ``self.arena`` (2, n):
+        structure b owns ``arena[p, it.arena_off : it.arena_off + it.arena_len]``, its
+        arrays back to back in that order (``it.arena_segs``: name, offset, shape). A
+        caller can then read or write a whole state with one copy (the CW operator's
+        Krylov vectors live in this layout). Pole stacks stay outside (they rotate
+        through three buffers)."""
+        segs, total = [], 0
+        for b, it in enumerate(self.items):
+            bx = it.box
+            lst = [("main", bx["main"]), ("x", bx["x"]), ("y", bx["y"])]
+            lst += [(f"psi{k}", bx["psi"][k]) for k in range(4)]
+            lst += [(n, [bx[n][0], bx[n][1]]) for n in ("Hx0", "Hy0") if n in bx]
+            it.arena_off, it.arena_segs = total, []
+            for name, pair in lst:
+                segs.append((it, name, pair, total))
+                it.arena_segs.append((name, total, tuple(pair[0].shape)))
+                total += pair[0].numel()
+            it.arena_len = total - it.arena_off
+        arena = torch.zeros((2, total), dtype=torch.float32, device=self.device)
+        remap = {}
+        for it, name, pair, off in segs:
+            views = []
+            for p in range(2):
+                v = arena[p, off:off + pair[p].numel()].view(pair[p].shape)
+                v.copy_(pair[p])
+                remap[L.ptr(pair[p])] = L.ptr(v)
+                views.append(v)
+            if name.startswith("psi"):
+                it.box["psi"][int(name[3])] = views
+            else:
+                it.box[name] = views
+        for S in structs:
+            for arr in (S.f_main, S.f_x, S.f_y, S.f_x0, S.f_y0, *S.psi):
+                for p in range(2):
+                    if arr[p]:
+                        arr[p] = remap.get(arr[p], arr[p])
+        self.arena = arena
 
     def _set_cells(self, target, cl, col, it):
         row_ptr, colv, w = cl
@@ -858,7 +902,7 @@ class Engine2D:
         xoff, yoff = int(nx_e == nx - 2), int(ny_e == ny - 2)
         for name, n in (("Hx0", nx), ("Hy0", ny)):
             if name in bx:
-                pol[name] = bx[name][cur, :n].clone()
+                pol[name] = bx[name][cur][:n].clone()
         return s._replace(
             Ez=Ez, Dz=Dz, **pol,
             Hx=self._unpack(bx["x"][cur], (nx, ny - 1)),

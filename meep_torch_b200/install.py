@@ -11,6 +11,7 @@ reference (module : name)                 this package
 ``core.monitors_3d : run_3d`` (:192)      ``meep_torch_b200.core.monitors_3d.run_3d``
 ``core.stepper_3d_lean : run_3d_lean``    ``meep_torch_b200.core.stepper_3d_lean.run_3d_lean``
 ``core.adjoint3d : run_3d_adjoint``       ``meep_torch_b200.core.adjoint3d.run_3d_adjoint``
+``mp.cpp.core : fields.solve_cw``         ``meep_torch_b200.cw.solve_cw_fields``
 ========================================  ==============================================
 
 Modules that bound one of these names by ``from ... import`` (``mp/cpp/core.py``,
@@ -44,7 +45,12 @@ TARGETS = (
     ("core.adjoint3d", "run_3d_adjoint", "meep_torch_b200.core.adjoint3d", "run_3d_adjoint"),
 )
 
-_patched: list = []          # (module, attribute, original) in patch order
+# methods: (reference module, class, method, this package's module, its function)
+METHOD_TARGETS = (
+    ("mp.cpp.core", "fields", "solve_cw", "meep_torch_b200.cw", "solve_cw_fields"),
+)
+
+_patched: list = []          # (module or class, attribute, original) in patch order
 
 
 def _first_tensor(obj, depth: int = 0):
@@ -67,6 +73,14 @@ def cuda_f32(args, kwargs) -> bool:
         if t is not None:
             return bool(t.is_cuda) and t.dtype == torch.float32
     return False
+
+
+def fields_cuda_f32(args, kwargs) -> bool:
+    """True when a fields method's object (the first argument) holds a float32 CUDA
+    state."""
+    st = getattr(args[0], "_state", None) if args else None
+    t = _first_tensor(st)
+    return t is not None and bool(t.is_cuda) and t.dtype == torch.float32
 
 
 def _router(original, ours, fallback: bool, route):
@@ -116,6 +130,21 @@ def install(package: str = "meep_torch", *, fallback: bool = False, ours=None,
             if hit is not None and hit[0] is val:
                 setattr(mod, attr, hit[1])
                 _patched.append((mod, attr, val))
+    # methods of the reference's classes, routed on the object's state
+    for mod_name, cls_name, meth, our_mod, our_name in METHOD_TARGETS:
+        try:
+            mod = importlib.import_module(f"{package}.{mod_name}")
+        except ImportError:
+            continue
+        cls = getattr(mod, cls_name, None)
+        original = vars(cls).get(meth) if isinstance(cls, type) else None
+        if original is None:
+            continue
+        target = (ours or {}).get(meth)
+        if target is None:
+            target = getattr(importlib.import_module(our_mod), our_name)
+        setattr(cls, meth, _router(original, target, fallback, fields_cuda_f32))
+        _patched.append((cls, meth, original))
     return len(_patched)
 
 

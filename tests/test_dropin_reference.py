@@ -14,6 +14,7 @@ float32 on both sides, is held to 1e-3.
 """
 import importlib
 import sys
+import time
 
 import numpy as np
 import pytest
@@ -160,3 +161,43 @@ def test_mode_converter_gradient_on_the_kernels(ref):
     eJ, eg = abs(Jg - Jc) / abs(Jc), rel_l2(gg, gc)
     print(f"\n[mode converter gradient] J rel err {eJ:.2e}, dJ/deps relL2 {eg:.2e}")
     assert eJ < TOL and eg < 1e-3, (eJ, eg)
+
+
+def test_simulation_solve_cw_on_the_kernels_matches_the_reference(ref):
+    """mp.Simulation(force_complex_fields=True).solve_cw (mp/simulation.py:2290 ->
+    fields.solve_cw, mp/cpp/core.py:721) routed to the kernels' CW solve: an 80 x 80 cell
+    with an eps 12 guide and a ContinuousSource(0.15) Ez point source, PML 1. The CUDA
+    float32 solve (tol 1e-5) against the reference's own float64 solve on the CPU
+    (tol 1e-8): the complex Ez map."""
+    mp = importlib.import_module("meep_torch.mp")
+
+    def solve(device, dtype, tol):
+        sim = mp.Simulation(
+            resolution=10, cell_size=mp.Vector3(8, 8),
+            geometry=[mp.Block(size=mp.Vector3(mp.inf, 1, mp.inf),
+                               material=mp.Medium(epsilon=12))],
+            sources=[mp.Source(mp.ContinuousSource(0.15), component=mp.Ez,
+                               center=mp.Vector3(-2, 0))],
+            boundary_layers=[mp.PML(1.0)], force_complex_fields=True, dtype=dtype,
+            device=device)
+        sim.init_sim()
+        n0 = _launches()
+        t0 = time.perf_counter()
+        ok = sim.solve_cw(tol, 10000, 2)
+        if device == "cuda":
+            torch.cuda.synchronize()
+        times[device] = time.perf_counter() - t0
+        launched = _launches() - n0
+        ez = sim.get_array(component=mp.Ez)
+        ez = ez.detach().cpu().numpy() if torch.is_tensor(ez) else np.asarray(ez)
+        return ok, np.asarray(ez, dtype=np.complex128), launched
+
+    times = {}
+    ok_c, ez_c, n_c = solve("cpu", torch.float64, 1e-8)
+    ok_g, ez_g, n_g = solve("cuda", torch.float32, 1e-5)
+    assert ok_g and n_c == 0 and n_g > 0, (ok_c, ok_g, n_c, n_g)
+    e = float(np.linalg.norm(ez_g - ez_c) / np.linalg.norm(ez_c))
+    print(f"\n[Simulation solve_cw] Ez relL2 vs the reference (CPU, float64; converged "
+          f"{ok_c}): {e:.2e}; {n_g} library launches; solve {times['cuda']:.3f} s on the "
+          f"kernels, {times['cpu']:.3f} s for the reference on the CPU")
+    assert e < 1e-3, e

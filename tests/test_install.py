@@ -103,6 +103,17 @@ def test_cuda_f32_predicate():
         assert not I.cuda_f32(((torch.zeros(2, device="cuda", dtype=torch.float64),),), {})
 
 
+def test_fields_method_predicate():
+    """fields.solve_cw routes on the fields object's state, not on its arguments."""
+    class F:
+        _state = (torch.zeros(2), torch.zeros(3))
+    assert not I.fields_cuda_f32((F(),), {})
+    assert not I.fields_cuda_f32((), {})
+    if torch.cuda.is_available():
+        F._state = (torch.zeros(2, device="cuda"),)
+        assert I.fields_cuda_f32((F(),), {})
+
+
 def test_install_on_the_reference_package():
     from tests.golden.reference_path import find_reference
     ref = find_reference()
@@ -118,9 +129,12 @@ def test_install_on_the_reference_package():
             importlib.import_module(m)
         run_mod = sys.modules["meep_torch.core.run"]
         orig = {n: getattr(run_mod, n) for n in ("_run_chunk", "run_tm", "run_te")}
+        fcls = sys.modules["meep_torch.mp.cpp.core"].fields
+        orig_cw = vars(fcls)["solve_cw"]
         n = I.install("meep_torch")
         try:
-            assert n >= 6
+            assert n >= 7
+            assert getattr(vars(fcls)["solve_cw"], "_meep_b200_router", False)
             assert getattr(run_mod.run_tm, "_meep_b200_router", False)
             assert sys.modules["meep_torch.solvers"].run_tm is run_mod.run_tm
             assert getattr(sys.modules["meep_torch.mp.cpp.core"]._run_chunk,
@@ -131,6 +145,7 @@ def test_install_on_the_reference_package():
             I.uninstall()
         for k, v in orig.items():
             assert getattr(run_mod, k) is v
+        assert vars(fcls)["solve_cw"] is orig_cw
         assert mt is not None
     finally:
         sys.path.remove(ref)
