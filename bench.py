@@ -581,7 +581,7 @@ def run_cfg3(args, rank, world, dev):
     nsteps = args.run_steps if args.run_steps != 5000 else 2000
     s, c, src, mons = W.cfg3_setup(dev, n=n)
     eng = Engine3D(s, c, src, mons, rows_per_seg=args.rows, ring_slots=args.ring,
-                   variant=args.variant)
+                   variant=args.variant, geometry=args.geometry)
     stream = torch.cuda.current_stream(dev)
 
     def bench_step():
@@ -1106,8 +1106,12 @@ def main():
                          "gathered on rank 0, cfg3's grid into x slabs with halo planes "
                          "exchanged every half step")
     ap.add_argument("--variant", type=int, default=0,
-                    help="kernel variant, 0 library default; 2D: 1 row march, 2 tiles; "
-                         "3D: 1 fused x-march, 2 split H / E")
+                    help="kernel variant, 0 library default; 2D: 1 row march, 2 tiles, "
+                         "3 temporally blocked tiles, 4 cluster-resident; 3D: 1 fused "
+                         "x-march, 2 split H / E, 3 one pass")
+    ap.add_argument("--geometry", type=int, default=0,
+                    help="3D one-pass work split: 0 library default, 1 tile-major shares, "
+                         "2 lockstep tiles")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1160,7 +1164,8 @@ def main():
                               "random dielectric spheres, Gaussian Ez point dipole, six "
                               "20-frequency flux faces, 2000 steps per run",
                   "grid": [n3, n3, n3], "time_steps": steps3, "seed": 3,
-                  "kernel_variant": args.variant or "library default (split H / E)",
+                  "kernel_variant": args.variant or "library default (one pass)",
+                  "geometry": args.geometry or "library default",
                   "l2": f"inputs larger than L2 (~{37 * 4 * n3 ** 3 / 1e9:.1f} GB of field "
                         "state)"}
     else:

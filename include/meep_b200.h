@@ -259,6 +259,11 @@ typedef struct mtb_tuning {
                                TMA-staged planes; no damping or poles,
                                zpitch <= 256; half steps and x slabs move
                                a default plan to 2)                         */
+    int32_t geometry;       /* 3D one-pass kernel work split: 0 default and 1
+                               tile-major shares of equal cost, 2 lockstep
+                               (every tile cut at the same x planes, tile
+                               heights balanced by cost: fewer DRAM bytes,
+                               more issue slots)                            */
 } mtb_tuning;
 
 typedef struct mtb_yee2d_plan mtb_yee2d_plan;

@@ -70,7 +70,7 @@ class DftRegion(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("rows_per_warp", C.c_int32), ("ring_slots", C.c_int32),
-                ("graph", C.c_int32), ("variant", C.c_int32)]
+                ("graph", C.c_int32), ("variant", C.c_int32), ("geometry", C.c_int32)]
 
 
 class Yee3DStruct(C.Structure):

@@ -84,13 +84,15 @@ class FluxMonitor3D:
 
 
 def run_3d(state, coeffs, n_steps: int, *, source=None, monitors=(), phase_mode="exact",
-           rows_per_seg: int = 0, ring_slots: int = 0, variant: int = 0):
-    """Forward 3D run (core/monitors_3d.py:192-210) on the B200 kernels."""
+           rows_per_seg: int = 0, ring_slots: int = 0, variant: int = 0, geometry: int = 0):
+    """Forward 3D run (core/monitors_3d.py:192-210) on the B200 kernels. ``variant`` and
+    ``geometry`` are the plan's tuning knobs (``mtb_tuning``)."""
     monitors = list(monitors)
     if n_steps <= 0:
         return state, [None] * len(monitors)
     eng = Engine3D(state, coeffs, source, monitors, point_sign=+1, phase_mode=phase_mode,
-                   rows_per_seg=rows_per_seg, ring_slots=ring_slots, variant=variant)
+                   rows_per_seg=rows_per_seg, ring_slots=ring_slots, variant=variant,
+                   geometry=geometry)
     try:
         eng.run(0, n_steps)
         return eng.state(), list(eng.accs)

@@ -3,11 +3,13 @@
 // source, :448-482, with the arithmetic of the split kernels k_yee3d_h /
 // k_yee3d_e cell for cell (the results are bit-identical to theirs).
 //
-// Work: the y axis is cut into tiles of TY rows; (tile, x plane) pairs are
-// numbered tile-major and every block of a persistent grid takes one contiguous
-// share of that sequence (one or a few x segments of one or a few tiles), the shares
-// cut on the host so that their estimated costs (a pair in an x or y CPML layer
-// costs more) are equal.
+// Work: the y axis is cut into tiles of at most TY rows (tile t: rows ytab[t] ..
+// ytab[t+1]-1); (tile, x plane) pairs are numbered tile-major and every block of a
+// persistent grid takes one contiguous share of that sequence. The host cuts
+// tile-major shares of equal estimated cost (a pair in an x or y CPML layer costs
+// more) or, when asked, lockstep shares (every tile split at the same x planes, one
+// share per block, tile heights balanced by cost) so that y-neighbour tiles pass a
+// plane at about the same time and the halo rows one reads are still in L2.
 // Within a segment the block marches along x. Per x plane p:
 //   H phase  H(n+1/2) of plane p for the tile's rows and the row below it (that
 //            halo row is recomputed, never stored) from staged E(n) of planes p
@@ -56,6 +58,7 @@ struct XmMaps {
     int npz;               // 1: the z-layer boxes are staged
     const float *ptab;     // profiles masked as the kernels apply them, (1, 0) outside the
                            // layers: x [H b, H a, E b, E a][nx], y [..][ny], z [..][zpitch]
+    const int *ytab;       // first row of each tile, tiles + 1 entries (last = ny)
 };
 
 template <int V, int TY>
@@ -147,7 +150,7 @@ template <int V, int TY>
 __device__ __forceinline__ void xm_issue(const XmMaps &M, int par, int t, int p, float *stage,
                                          uint64_t *bar) {
     using S = XmShape<V, TY>;
-    const int y0 = t * TY;
+    const int y0 = __ldg(M.ytab + t);
     const uint32_t bytes = S::BYTES_BASE + (M.npz ? S::BYTES_PZ : 0u);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                  ::"r"(xm_s32(bar)), "r"(bytes) : "memory");
@@ -167,11 +170,10 @@ __device__ __forceinline__ void xm_issue(const XmMaps &M, int par, int t, int p,
 }
 
 // L2 prefetch (cp.async.bulk.prefetch) of the x / y layer CPML memory an element will
-// read: the rows y0-1 .. y0+TY-1 of plane p are one contiguous run per array.
-template <int TY>
-__device__ __forceinline__ void xm_l2_psi(const Split3 &P, int t, int p) {
-    const int ny = P.ny, y0 = t * TY;
-    const int r0 = max(y0 - 1, 0), r1 = min(y0 + TY, ny);
+// read: the rows y0-1 .. y1-1 of plane p are one contiguous run per array.
+__device__ __forceinline__ void xm_l2_psi(const Split3 &P, const XmMaps &M, int t, int p) {
+    const int ny = P.ny, y0 = __ldg(M.ytab + t);
+    const int r0 = max(y0 - 1, 0), r1 = min(__ldg(M.ytab + t + 1), ny);
     const bool xb = inband(P.B, 0, 0, p) || inband(P.B, 0, 1, p);
     bool yb = false;
     for (int r = r0; r < r1; ++r) yb |= inband(P.B, 1, 0, r) || inband(P.B, 1, 1, r);
@@ -219,8 +221,10 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
     const int nx = P.nx, ny = P.ny, nz = P.nz, ZP = P.zp;
     const int lane = c.lane, slot = c.slot, kb = c.kb;
     const float dt = P.dt, rdx = P.rdx;
-    const int j = t * TY - 1 + slot, i = p;
-    const bool act = j >= 0 && j < ny && kb < ZP;
+    const int j = __ldg(M.ytab + t) - 1 + slot, i = p;
+    // rows past the tile (a tile shorter than TY) are the next tile's: not stored
+    const int jend = min(__ldg(M.ytab + t + 1), ny);
+    const bool act = j >= 0 && j < jend && kb < ZP;
     const uint32_t g = (uint32_t)i * ((uint32_t)ny * ZP) + (uint32_t)(max(j, 0) * ZP + kb);
     const bool xok = i <= nx - 2, vyH = j <= ny - 2;
     const bool bx = XY && act && xok && inband(P.B, 0, 0, i);
@@ -230,7 +234,7 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
     for (int q = 0; q < 4; ++q) bz |= act && kb + q <= nz - 2 && inband(P.B, 2, 0, kb + q);
     const float *xt = M.ptab, *yt = M.ptab + 4 * nx;      // masked x / y profiles
     // E phase of this warp (warp-uniform) and its flags
-    const bool eact = !tail && !halo && slot > 0 && j < ny;
+    const bool eact = !tail && !halo && slot > 0 && j < jend;
     const bool iin = i >= 1 && i <= nx - 2, jin = j >= 1 && j <= ny - 2;
     const bool pmx = P.pmc & 1, pmy = (P.pmc >> 1) & 1, pmz = (P.pmc >> 2) & 1;
     const bool bxe = XY && eact && act && iin && inband(P.B, 0, 1, i);
@@ -374,7 +378,7 @@ __device__ __forceinline__ void xm_elem(const Split3 &P, const XmMaps &M, const 
         c.pmore = Q.next(c.pt, c.pp);
         // x / y layer memory of the element after next into L2
         int t2 = t, p2 = p;
-        if (Q.next(t2, p2) && Q.next(t2, p2)) xm_l2_psi<TY>(P, t2, p2);
+        if (Q.next(t2, p2) && Q.next(t2, p2)) xm_l2_psi(P, M, t2, p2);
     }
     if (eact) {
         // ---- E(n+1) of (i, j): core/stepper_3d.py:395-437, source :448-482
@@ -565,7 +569,7 @@ k_yee3d_xm(const __grid_constant__ Split3 P, const __grid_constant__ XmMaps M,
         const bool halo = p < xs, tail = p >= xe;
         const bool has_next = p + 1 < nx && p + 1 <= last;
         if (p == xs - 1 || (xs == 0 && p == 0)) { z4(c.hyp); z4(c.hzp); }
-        const int j = t * TY - 1 + c.slot;
+        const int j = __ldg(M.ytab + t) - 1 + c.slot;
         const bool xy = inband(P.B, 0, 0, p) || inband(P.B, 0, 1, p) ||
                         (j >= 0 && j < ny && (inband(P.B, 1, 0, j) || inband(P.B, 1, 1, j)));
         if (xy)

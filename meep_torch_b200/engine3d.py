@@ -76,7 +76,7 @@ class Engine3D:
 
     def __init__(self, state, coeffs, source=None, monitors=(), *, point_sign: int = 1,
                  phase_mode: str = "exact", rows_per_seg: int = 0, ring_slots: int = 0,
-                 variant: int = 0, stream=None, own=None):
+                 variant: int = 0, stream=None, own=None, geometry: int = 0):
         self.lib = L.load()
         self.stream = stream
         self.keep = []
@@ -260,7 +260,7 @@ class Engine3D:
             grp_arr[q].freqs = C.cast(arr, C.POINTER(C.c_double))
             grp_arr[q].nf, grp_arr[q].mode, grp_arr[q].dt = nf, self.phase_mode, dt
         self._groups = groups
-        tun = L.Tuning(rows_per_seg, ring_slots, 0, variant)
+        tun = L.Tuning(rows_per_seg, ring_slots, 0, variant, geometry)
         plan = C.c_void_p()
         L.check(self.lib.mtb_yee3d_plan_create(C.byref(S), reg_arr, len(regions), grp_arr,
                                                len(groups), ring, C.byref(tun), C.byref(plan)),

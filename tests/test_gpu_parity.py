@@ -921,15 +921,18 @@ def test_te_gradient_matches_reference_autograd(chunk):
     assert e32 < TOL, e32
 
 
+@pytest.mark.parametrize("geometry", [0, 2])
 @pytest.mark.parametrize("shape", [(23, 17, 40), (9, 30, 128), (31, 13, 131), (6, 22, 256),
-                                   (40, 8, 77)])
-def test_3d_one_pass_bitwise_equal_to_split(shape):
+                                   (40, 8, 77), (48, 256, 256)])
+def test_3d_one_pass_bitwise_equal_to_split(shape, geometry):
     """The one-pass x-march (variant 3: H and E of a plane in one kernel, TMA-staged
     planes, a persistent grid cutting the (tile, plane) sequence into segments with
     recomputed halo planes) gives the split kernels' results bit for bit: fields, CPML
     memory and flux / DFT accumulators from a random start, for z widths on both
     kernel shapes (zpitch <= 128 and <= 256), y extents that leave a partial tile and
-    grids small enough that every block owns a few planes only."""
+    grids small enough that every block owns a few planes only; with the default work
+    geometry and with the lockstep one asked for (tiles of cost-balanced heights, every
+    tile cut at the same x planes)."""
     from meep_torch_b200.core.monitors_3d import (DFTFieldsMonitor3D, FluxMonitor3D,
                                                   PointSource3D, run_3d)
     from meep_torch_b200.core.sources import GaussianPulse
@@ -950,7 +953,7 @@ def test_3d_one_pass_bitwise_equal_to_split(shape):
     init = init._replace(**{k: torch.randn(getattr(init, k).shape, generator=gen).to(dev())
                             for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
     ref_s, ref_a = run_3d(init, c, n, source=src, monitors=mons, variant=2)
-    st, accs = run_3d(init, c, n, source=src, monitors=mons, variant=3)
+    st, accs = run_3d(init, c, n, source=src, monitors=mons, variant=3, geometry=geometry)
     bad = [k for k, v in ref_s._asdict().items()
            if v is not None and not torch.equal(v, getattr(st, k))]
     bad += [f"acc_{q}" for q, (a, b) in enumerate(zip(accs, ref_a)) if not torch.equal(a, b)]
