@@ -201,6 +201,14 @@ typedef struct mtb_yee2d_struct {
     int32_t pad2_[2];
     float *f_x0[2];
     float *f_y0[2];
+    /* TM instantaneous chi2 / chi3 (core/coeffs.py:155-158; core/stepper_tm.py:222-230):
+     * box arrays of chi2, chi3 and eps_inf (all three, or all null = linear). Ez is
+     * then the fixed point rhs / (eps + chi2 Ez + chi3 Ez^2) after three sweeps from
+     * rhs / eps, rhs = Dz - sum P, wherever the step reads or writes Ez. Tile kernels
+     * only (variant 2); other variants, the no-alloc entry and the adjoint return
+     * MTB_UNSUPPORTED. */
+    const float *chi2, *chi3, *eps_nl;
+    const void *pad3_;
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

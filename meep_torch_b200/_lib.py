@@ -53,7 +53,8 @@ class Yee2DStruct(C.Structure):
                 ("cut_y", C.c_int32), ("cut_x", C.c_int32), ("cut_map_y", C.c_int32),
                 ("cut_map_x", C.c_int32), ("cut_ph_y", C.c_float), ("cut_ph_x", C.c_float),
                 ("pad2_", C.c_int32 * 2),
-                ("f_x0", vp * 2), ("f_y0", vp * 2)]
+                ("f_x0", vp * 2), ("f_y0", vp * 2),
+                ("chi2", vp), ("chi3", vp), ("eps_nl", vp), ("pad3_", vp)]
 
 
 class PhaseGroup(C.Structure):

@@ -5,7 +5,7 @@ The NamedTuple field names are the reference's, so either side's objects can
 be handed to either side's run drivers. The builders cover the B200 path's
 feature set -- scalar eps, CPML (kappa = 1), PEC walls, TM PMC-in-y walls and the
 low-edge symmetry cuts (mirrors; TM Rotate2 / Rotate4), conductivity, permeability and
-dispersive poles; the reference's nonlinear, magnetic-pole and tensor options raise
+dispersive poles and chi2 / chi3; the reference's magnetic-pole and tensor options raise
 NotImplementedError here (the reference itself still runs them).
 """
 import math
@@ -122,8 +122,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("chi3", "chi2", "m_poles", "m_pole_masks", "y_rot2", "rot4", "eps_tensor",
-                "poles_tensor", "pole_masks_tensor")
+_UNSUPPORTED = ("m_poles", "m_pole_masks", "eps_tensor", "poles_tensor", "pole_masks_tensor")
 
 
 def _check_parity(**kw):
@@ -219,7 +218,7 @@ def _poles_tm(grid: Grid, eps, poles, pole_masks):
 def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     y_pmc: bool = False, sigma_d=None, sigma_b=None, mu=None,
                     y_mirror: int = 0, x_mirror: int = 0, y_rot2: int = 0, rot4: int = 0,
-                    **kw) -> TMCoeffs:
+                    chi2=None, chi3=None, **kw) -> TMCoeffs:
     """TM coefficients: eps map, CPML profiles sliced to the live nodes --
     H side on the n-1 half nodes, E side on the interior [1:-1] (the full
     axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291;
@@ -227,7 +226,9 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
     permeability pairs of :161-175, ``poles`` / ``pole_masks`` the ADE recurrences of
     :87-106, :195-203. ``y_mirror`` / ``x_mirror`` (+1 even, -1 odd), ``y_rot2`` and
     ``rot4`` (phase +-1) cut the low-y / low-x edge (:209-285): no absorber on the cut
-    side, and the E-side profiles run from the cut node to the node before the far wall."""
+    side, and the E-side profiles run from the cut node to the node before the far wall.
+    ``chi2`` / ``chi3`` (scalars or (nx, ny)): instantaneous nonlinearity (:155-158),
+    flagged by ``has_chi2`` / ``has_kerr`` when any value is nonzero."""
     _reject(kw)
     _check_parity(y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4)
     if y_mirror and y_rot2:
@@ -245,7 +246,7 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                                   "on-plane H line has no magnetic coefficients")
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
-    zero = _as_field(None, grid, 0.0)
+    x2, x3 = _as_field(chi2, grid, 0.0), _as_field(chi3, grid, 0.0)
     px, py = _cut_axes(grid, *_axis_sides(npml), y_cut, x_cut, y_pmc)
 
     def prof(n, offset, pair, use=True):
@@ -265,14 +266,14 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
     b_ey, a_ey, k_ey = e_side(grid.ny, py, y_cut, full=y_pmc)
     c1, c2, c3 = _poles_tm(grid, eps, list(poles), pole_masks)
     return TMCoeffs(
-        dt=dt, dx=dx, eps_inf=eps, chi3=zero, has_kerr=False, c1=c1, c2=c2, c3=c3,
-        y_pmc=y_pmc, y_mirror_lo=y_mirror, x_mirror_lo=x_mirror, y_rot2_lo=y_rot2,
+        dt=dt, dx=dx, eps_inf=eps, chi3=x3, has_kerr=bool((x3 != 0).any()), c1=c1, c2=c2,
+        c3=c3, y_pmc=y_pmc, y_mirror_lo=y_mirror, x_mirror_lo=x_mirror, y_rot2_lo=y_rot2,
         rot4_lo=rot4,
         b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
-        chi2=zero.clone(), has_chi2=False, **_cond_tm(grid, sigma_d, sigma_b, mu))
+        chi2=x2, has_chi2=bool((x2 != 0).any()), **_cond_tm(grid, sigma_d, sigma_b, mu))
 
 
 def _avg_to_ex(v):
@@ -305,18 +306,20 @@ def _axis_poles(grid: Grid, eps, shared, axis_poles, shared_masks, axis_masks, s
 def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     sigma_d=None, poles_x=(), poles_y=(), pole_masks_x=None,
                     pole_masks_y=None, sigma_b=None, mu=None, y_mirror: int = 0,
-                    x_mirror: int = 0, **kw) -> TECoeffs:
+                    x_mirror: int = 0, chi2=None, chi3=None, **kw) -> TECoeffs:
     """TE coefficients: eps Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1)
     (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491, with
     ``sigma_d``, ``sigma_b``, ``mu`` the conductivity and permeability pairs of
     :401-415, and the per-axis ADE pole stacks of :416-425 (shared ``poles`` on both
     axes, ``poles_x`` / ``poles_y`` on one). ``y_mirror`` / ``x_mirror`` (+-1) cut the
-    low edge (:457-469): no absorber there; the profiles keep their interior slices."""
+    low edge (:457-469): no absorber there; the profiles keep their interior slices.
+    ``chi2`` / ``chi3`` are averaged onto Ex / Ey (:380-387); the kernels run them for TM
+    only."""
     _reject(kw)
     _check_parity(y_mirror=y_mirror, x_mirror=x_mirror)
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
-    zero = _as_field(None, grid, 0.0)
+    x2, x3 = _as_field(chi2, grid, 0.0), _as_field(chi3, grid, 0.0)
     px, py = _cut_axes(grid, *_axis_sides(npml), bool(y_mirror), bool(x_mirror))
 
     def prof(n, offset, pair):
@@ -332,12 +335,12 @@ def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                                 (grid.nx, grid.ny - 1), _avg_to_ey)
     return TECoeffs(
         dt=dt, dx=dx, eps_x=_avg_to_ex(eps), eps_y=_avg_to_ey(eps),
-        chi3_x=_avg_to_ex(zero), chi3_y=_avg_to_ey(zero), has_kerr=False,
+        chi3_x=_avg_to_ex(x3), chi3_y=_avg_to_ey(x3), has_kerr=bool((x3 != 0).any()),
         c1x=c1x, c2x=c2x, c3x=c3x, c1y=c1y, c2y=c2y, c3y=c3y,
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_hy=b_hy[None, :], a_hy=a_hy[None, :], k_hy=k_hy[None, :],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
-        chi2_x=_avg_to_ex(zero), chi2_y=_avg_to_ey(zero), has_chi2=False,
+        chi2_x=_avg_to_ex(x2), chi2_y=_avg_to_ey(x2), has_chi2=bool((x2 != 0).any()),
         y_mirror_lo=y_mirror, x_mirror_lo=x_mirror,
         **_cond_te(grid, sigma_d, sigma_b, mu))

@@ -912,6 +912,36 @@ __device__ __forceinline__ void tm_hy(const mtb_yee2d_struct &S, int r, bool val
         apply_cells(S.src_h1, r, amp_h, jb, out);
 }
 
+// Instantaneous chi2 / chi3 (core/stepper_tm.py:222-230): Ez = rhs / eps, then three
+// sweeps Ez = rhs / (eps + chi2 Ez + chi3 Ez Ez), evaluated left to right and rounded
+// like the reference's tensor expression.
+__device__ __forceinline__ float tm_nl(float rhs, float eps, float x2, float x3) {
+    float e = __fdiv_rn(rhs, eps);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        e = __fdiv_rn(rhs, __fadd_rn(__fadd_rn(eps, __fmul_rn(x2, e)),
+                                     __fmul_rn(__fmul_rn(x3, e), e)));
+    return e;
+}
+
+// Ez of one row's float4 from rhs = Dz - sum P: rhs / eps (as rhs * (1/eps)), or the
+// chi2 / chi3 fixed point when the structure has them (box offset o).
+__device__ __forceinline__ void tm_e4(const mtb_yee2d_struct &S, bool nl, uint32_t o,
+                                      const float (&rhs)[4], const float (&ie)[4],
+                                      float (&e)[4]) {
+    if (nl) {
+        float x2[4], x3[4], ep[4];
+        ld4(S.chi2 + o, x2);
+        ld4(S.chi3 + o, x3);
+        ld4(S.eps_nl + o, ep);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q] = tm_nl(rhs[q], ep[q], x2[q], x3[q]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q] = rhs[q] * ie[q];
+    }
+}
+
 // Ez(n) of one cell as tm_tile forms it for its own rows: the imported Ez on an
 // explicit first step, else (Dz - sum_k P_k) / eps with the poles summed in order.
 template <bool EXPL, bool EXT>
@@ -924,6 +954,8 @@ __device__ __forceinline__ float tm_ez_at(const mtb_yee2d_struct &S, const Ctx2D
     const uint32_t pl = (uint32_t)S.nx * S.pitch;
 #pragma unroll 1
     for (int k = 0; k < (EXT ? S.n_poles : 0); ++k) sp += Pc[k * pl + o];
+    if (EXT && S.chi2)
+        return tm_nl(S.f_main[C.par][o] - sp, S.eps_nl[o], S.chi2[o], S.chi3[o]);
     return (S.f_main[C.par][o] - sp) * S.inv_eps_a[o];
 }
 
@@ -1016,14 +1048,23 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
                 if (lane == 0 && jb >= 1) sl += Pk[ro - 1];
                 if (lane == 31 && jb + 4 < P) sr += Pk[ro + 4];
             }
-            if (lane == 0 && jb >= 1) ezl = (Dz[ro - 1] - sl) * ie[ro - 1];
-            if (lane == 31 && jb + 4 < P) ezr = (Dz[ro + 4] - sr) * ie[ro + 4];
+            const bool nl = EXT && S.chi2 != nullptr;
+            if (lane == 0 && jb >= 1)
+                ezl = nl ? tm_nl(Dz[ro - 1] - sl, S.eps_nl[ro - 1], S.chi2[ro - 1], S.chi3[ro - 1])
+                         : (Dz[ro - 1] - sl) * ie[ro - 1];
+            if (lane == 31 && jb + 4 < P)
+                ezr = nl ? tm_nl(Dz[ro + 4] - sr, S.eps_nl[ro + 4], S.chi2[ro + 4], S.chi3[ro + 4])
+                         : (Dz[ro + 4] - sr) * ie[ro + 4];
+            float r0[4], r1[4], r2[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                ez0[q] = (d0[q] - s0[q]) * e0[q];
-                ez1[q] = (d1[q] - s1[q]) * e1[q];
-                ez2[q] = (d2[q] - s2[q]) * e2[q];
+                r0[q] = d0[q] - s0[q];
+                r1[q] = d1[q] - s1[q];
+                r2[q] = d2[q] - s2[q];
             }
+            if (i >= 1) tm_e4(S, nl, ro - P, r0, e0, ez0); else zero4(ez0);
+            tm_e4(S, nl, ro, r1, e1, ez1);
+            if (i + 1 < nx) tm_e4(S, nl, ro + P, r2, e2, ez2); else zero4(ez2);
         }
         ld4(Hx + ro, hx);
         ld4(Hy + ro, hy);
@@ -1167,8 +1208,13 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             st4(Po + o, pc);
         }
     }
+    {
+        float rN[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) ezN[q] = (dzN[q] - psN[q]) * e1[q];
+        for (int q = 0; q < 4; ++q) rN[q] = dzN[q] - psN[q];
+        if (act) tm_e4(S, EXT && S.chi2 != nullptr, ro, rN, e1, ezN);
+        else zero4(ezN);
+    }
     if (!act) return;
     const int pn = par ^ 1;
     st4(S.f_main[pn] + ro, dzN);
@@ -1684,7 +1730,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
                       ib - 1 >= S.xband[0] && last < S.xband[1] &&
                       ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr &&
                       S.n_poles == 0 && S.mag_h1[0] == nullptr && S.mag_h1[1] == nullptr &&
-                      !(EXT && S.cut_y && w.z == 0);
+                      S.chi2 == nullptr && !(EXT && S.cut_y && w.z == 0);
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -2017,7 +2063,8 @@ static int tmap_2d(CUtensorMap *m, const float *base, int nx, int pitch, int bc,
 // walls or symmetry cuts (those run on the tile kernels' extended variant).
 static bool tb_eligible(const mtb_yee2d_struct &S) {
     return !S.cond_d1[0] && !S.cond_d1[1] && !S.n_poles && !S.n_poles_y && !S.mag_h1[0] &&
-           !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc && !S.cut_y && !S.cut_x;
+           !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc && !S.cut_y && !S.cut_x &&
+           !S.chi2;
 }
 
 // Copy n floats of a device array to the host.
@@ -2314,6 +2361,17 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         if (S.pol == MTB_TE && S.y_pmc)
             return fail(MTB_UNSUPPORTED, "structure %d: y_pmc is a TM option", s);
         int rc;
+        if (S.chi2 || S.chi3 || S.eps_nl) {
+            if (S.pol != MTB_TM)
+                return fail(MTB_UNSUPPORTED, "structure %d: chi2 / chi3 on the kernels are TM "
+                            "only", s);
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: chi2 / chi3 need the tile kernels "
+                            "(variant 2)", s);
+            if ((rc = check_ptr(S.chi2, "chi2", s)) || (rc = check_ptr(S.chi3, "chi3", s)) ||
+                (rc = check_ptr(S.eps_nl, "eps_nl", s)))
+                return rc;
+        }
         if (S.cut_y || S.cut_x) {
             if (S.cut_y < 0 || S.cut_y > 2 || S.cut_x < 0 || S.cut_x > 2)
                 return fail(MTB_INVALID_ARG, "structure %d: cut_y / cut_x must be 0, 1 or 2", s);
@@ -2456,7 +2514,8 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     for (int s = 0; s < n; ++s)
     {
         if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0 ||
-            structs[s].mag_h1[0] || structs[s].mag_h1[1] || structs[s].cut_y || structs[s].cut_x)
+            structs[s].mag_h1[0] || structs[s].mag_h1[1] || structs[s].cut_y || structs[s].cut_x ||
+            structs[s].chi2)
             p->ext = true;
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
     }
@@ -3197,7 +3256,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
     if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles ||
         S.n_poles_y || S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1] || S.cut_y ||
-        S.cut_x)
+        S.cut_x || S.chi2)
         return fail(MTB_UNSUPPORTED, "noalloc: conductivity, poles and symmetry cuts need the "
                     "tile kernels");
     int rc;

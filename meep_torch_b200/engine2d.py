@@ -225,7 +225,7 @@ class Engine2D:
             _need(np_ <= L.MTB_MAX_POLES, f"{np_} dispersive poles (at most {L.MTB_MAX_POLES})")
             _need(tuple(c.c1.shape) == (np_, it.nx, it.ny), "pole coefficients c1 shape")
             _opt_none(s, ["Bx"])
-            _opt_none(c, ["mc1x", "has_chi2"])
+            _opt_none(c, ["mc1x"])
             it.mag = _magnetic_pairs(c, [("h1x", "h2x"), ("h1y", "h2y")])
         it.cuts = _cuts(c, it.te)
         if not it.te:
@@ -235,7 +235,9 @@ class Engine2D:
                 _need((cut == 2) == (h0 is not None),
                       f"TMState.{name} does not match the coefficients' symmetry cut")
                 _need(h0 is None or tuple(h0.shape) == (n,), f"TMState.{name} shape")
-        _need(not getattr(c, "has_kerr", False), "Kerr (chi3) media")
+        # instantaneous chi2 / chi3: TM on the tile kernels (core/stepper_tm.py:222-230)
+        it.nl = bool(getattr(c, "has_kerr", False) or getattr(c, "has_chi2", False))
+        _need(not (it.nl and it.te), "TE chi2 / chi3 media")
         for k in ("k_hx", "k_hy", "k_ex", "k_ey"):
             kv = getattr(c, k)
             _need(bool(torch.all(kv == 1)), f"CPML kappa != 1 ({k})")
@@ -444,7 +446,14 @@ class Engine2D:
             # current on D scaled by d2 (core/stepper_tm.py:158-163, :197-200;
             # core/stepper_te.py D update and step_source)
             it.src_scale = None
-            it.plain = not te and not S.n_poles and not S.explicit_e and not (S.cut_y or S.cut_x)
+            it.plain = (not te and not S.n_poles and not S.explicit_e and not (S.cut_y or S.cut_x)
+                        and not it.nl)
+            if it.nl:
+                x2 = self._pack(c.chi2 if c.chi2 is not None else torch.zeros_like(c.eps_inf),
+                                nx, P)
+                x3 = self._pack(c.chi3, nx, P)
+                S.chi2, S.chi3, S.eps_nl = L.ptr(x2), L.ptr(x3), L.ptr(eps_a)
+                it.keep += [x2, x3]
             cond = ([("d1x", "d2x"), ("d1y", "d2y")] if te else [("d1", "d2")])
             if getattr(c, cond[0][0], None) is not None:
                 for k, (n1, n2) in enumerate(cond):
@@ -897,6 +906,16 @@ class Engine2D:
             Ez = (Dz - pc.sum(0)) / it.coeffs.eps_inf.to(Dz)
         else:
             Ez = self._unpack(bx["main"][cur], (nx, ny), den=bx["eps_a"])
+        if it.nl:
+            # the fixed point the kernels use (core/stepper_tm.py:222-230)
+            c = it.coeffs
+            rhs = Dz - (pol["P_cur"].sum(0) if pol else 0.0)
+            eps = c.eps_inf.to(Dz)
+            x2 = c.chi2.to(Dz) if c.chi2 is not None else torch.zeros_like(Dz)
+            x3 = c.chi3.to(Dz)
+            Ez = rhs / eps
+            for _ in range(3):
+                Ez = rhs / (eps + x2 * Ez + x3 * Ez * Ez)
         ps = bx["psi"]
         nx_e, ny_e = s.psi_Hyx.shape
         xoff, yoff = int(nx_e == nx - 2), int(ny_e == ny - 2)

@@ -165,7 +165,9 @@ def test_unsupported_features_raise():
     with pytest.raises(NotImplementedError):
         build_tm_coeffs(g, m_poles=[(1.0, 0.1, 1.0)])
     with pytest.raises(NotImplementedError):
-        build_tm_coeffs(g, chi3=torch.ones(20, 20))
+        build_tm_coeffs(g, eps_tensor=torch.ones(3, 20, 20))
+    m = build_tm_coeffs(g, chi3=torch.ones(20, 20))          # chi2 / chi3: built, flagged
+    assert m.has_kerr and not m.has_chi2
     with pytest.raises(ValueError):
         build_tm_coeffs(g, npml=10)
 

@@ -51,7 +51,8 @@ def run_tm_case(case, phase_mode="exact"):
     sig = g.get("sigma")
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
-    mag = {k: torch.tensor(g[k], dtype=torch.float32) for k in ("sigma_b", "mu") if k in g}
+    mag = {k: torch.tensor(g[k], dtype=torch.float32)
+           for k in ("sigma_b", "mu", "chi2", "chi3") if k in g}
     m = build_tm_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
                         npml=int(g["npml"]), y_pmc=pmc,
                         sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32),
@@ -72,7 +73,7 @@ def run_tm_case(case, phase_mode="exact"):
 
 
 @pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles",
-                                  "tm_magnetic"])
+                                  "tm_magnetic", "tm_nonlinear"])
 def test_tm_matches_reference(case):
     st, accs, (fx, fy) = run_tm_case(case)
     e32, e64 = {}, {}
