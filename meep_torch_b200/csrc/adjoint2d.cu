@@ -20,6 +20,8 @@
 //                the adjoints of dEz/dx (tmp2) and dEz/dy (tmp3).
 //   k_adj_tm_ez  (Ez nodes) gEz = transposed differences of tmp2 / tmp3 (plus, with
 //                poles, what k_adj_tm_e left in gEz).
+// k_adj_tm_ez of step q and k_adj_tm_e of step q-1 touch the same node only, so within
+// a chunk they run as one launch (k_adj_tm_eze): two launches per reverse step.
 // Poles, P(n+1) = c1 P(n) + c2 P(n-1) + c3 Ez(n) with Ez(n+1) = (Dz - sum P(n+1)) / eps:
 // with gA = d J / d P(n+1), gB = d J / d P(n) on entry, gPn = gA - gEz(n+1) / eps, and
 // on exit gA = c1 gPn + gB, gB = c2 gPn, gEz(n) gets sum_k c3 gPn.
@@ -74,12 +76,10 @@ __device__ __forceinline__ void inject(const mtb_yee2d_struct &S, int comp, int 
     }
 }
 
-__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__ mtb_yee2d_struct S,
-                                                         const __grid_constant__ mtb_adj2d_buffers B,
-                                                         const float *__restrict__ radj,
-                                                         const float *__restrict__ rec) {
-    const int i = blockIdx.y * AROWS + threadIdx.y;
-    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+__device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const float *__restrict__ radj,
+                                              const float *__restrict__ rec, const int i,
+                                              const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -149,11 +149,17 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__
     stv(B.g_eps[0] + g, ge);
 }
 
-__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__ mtb_yee2d_struct S,
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__ mtb_yee2d_struct S,
                                                          const __grid_constant__ mtb_adj2d_buffers B,
-                                                         const float *__restrict__ radj) {
-    const int i = blockIdx.y * AROWS + threadIdx.y;
-    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+                                                         const float *__restrict__ radj,
+                                                         const float *__restrict__ rec) {
+    adj_tm_e_cell(S, B, radj, rec, blockIdx.y * AROWS + threadIdx.y,
+                  (blockIdx.x * 32 + threadIdx.x) * 4);
+}
+
+__device__ __forceinline__ void adj_tm_h_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const float *__restrict__ radj, const int i,
+                                              const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -208,10 +214,16 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__
     stv(B.tmp[3] + g, t4);
 }
 
-__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant__ mtb_yee2d_struct S,
-                                                          const __grid_constant__ mtb_adj2d_buffers B) {
-    const int i = blockIdx.y * AROWS + threadIdx.y;
-    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__ mtb_yee2d_struct S,
+                                                         const __grid_constant__ mtb_adj2d_buffers B,
+                                                         const float *__restrict__ radj) {
+    adj_tm_h_cell(S, B, radj, blockIdx.y * AROWS + threadIdx.y,
+                  (blockIdx.x * 32 + threadIdx.x) * 4);
+}
+
+__device__ __forceinline__ void adj_tm_ez_cell(const mtb_yee2d_struct &S,
+                                               const mtb_adj2d_buffers &B, const int i,
+                                               const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -232,6 +244,12 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant_
     stv(B.g[0] + g, gez);
 }
 
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant__ mtb_yee2d_struct S,
+                                                          const __grid_constant__ mtb_adj2d_buffers B) {
+    adj_tm_ez_cell(S, B, blockIdx.y * AROWS + threadIdx.y,
+                  (blockIdx.x * 32 + threadIdx.x) * 4);
+}
+
 // ------------------------------------------------------------------ TE
 // Reverse of TE step t (core/stepper_te.py:178-190: D from Hz(n), E = D / eps,
 // Hz from E(n+1/2)), state_{t+1} = (Hz_{t+1}, E/D_{t+1/2}):
@@ -244,11 +262,11 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant_
 //                g_psi0, g_psi1 and the adjoints of the two Hz differences (tmp2 at Dx
 //                nodes, tmp3 at Dy nodes); gEx = gEy = 0 (E is recomputed every step).
 //   k_adj_te_hz  (Hz nodes) gHz += transposed differences of tmp2 / tmp3.
-__global__ void __launch_bounds__(32 * AROWS) k_adj_te_h(const __grid_constant__ mtb_yee2d_struct S,
-                                                         const __grid_constant__ mtb_adj2d_buffers B,
-                                                         const float *__restrict__ radj) {
-    const int i = blockIdx.y * AROWS + threadIdx.y;
-    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+// As for TM, k_adj_te_hz of step q and k_adj_te_h of step q-1 run as one launch
+// (k_adj_te_hzh).
+__device__ __forceinline__ void adj_te_h_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const float *__restrict__ radj, const int i,
+                                              const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -281,13 +299,18 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_te_h(const __grid_constant__
     stv(B.tmp[1] + g, u1);
 }
 
-__global__ void __launch_bounds__(32 * AROWS) k_adj_te_e(const __grid_constant__ mtb_yee2d_struct S,
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_h(const __grid_constant__ mtb_yee2d_struct S,
                                                          const __grid_constant__ mtb_adj2d_buffers B,
-                                                         const float *__restrict__ radj,
-                                                         const float *__restrict__ rex,
-                                                         const float *__restrict__ rey) {
-    const int i = blockIdx.y * AROWS + threadIdx.y;
-    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+                                                         const float *__restrict__ radj) {
+    adj_te_h_cell(S, B, radj, blockIdx.y * AROWS + threadIdx.y,
+                  (blockIdx.x * 32 + threadIdx.x) * 4);
+}
+
+__device__ __forceinline__ void adj_te_e_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const float *__restrict__ radj,
+                                              const float *__restrict__ rex,
+                                              const float *__restrict__ rey, const int i,
+                                              const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -357,10 +380,18 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_te_e(const __grid_constant__
     stv(B.tmp[3] + g, t3);
 }
 
-__global__ void __launch_bounds__(32 * AROWS) k_adj_te_hz(const __grid_constant__ mtb_yee2d_struct S,
-                                                          const __grid_constant__ mtb_adj2d_buffers B) {
-    const int i = blockIdx.y * AROWS + threadIdx.y;
-    const int jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_e(const __grid_constant__ mtb_yee2d_struct S,
+                                                         const __grid_constant__ mtb_adj2d_buffers B,
+                                                         const float *__restrict__ radj,
+                                                         const float *__restrict__ rex,
+                                                         const float *__restrict__ rey) {
+    adj_te_e_cell(S, B, radj, rex, rey, blockIdx.y * AROWS + threadIdx.y,
+                  (blockIdx.x * 32 + threadIdx.x) * 4);
+}
+
+__device__ __forceinline__ void adj_te_hz_cell(const mtb_yee2d_struct &S,
+                                               const mtb_adj2d_buffers &B, const int i,
+                                               const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -379,6 +410,33 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_te_hz(const __grid_constant_
         ghz[q] = v ? ghz[q] + (t2[q] - t2n) * rdx + (t3[q] - t3n[q]) * rdx : 0.f;
     }
     stv(B.g[0] + g, ghz);
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_hz(const __grid_constant__ mtb_yee2d_struct S,
+                                                          const __grid_constant__ mtb_adj2d_buffers B) {
+    adj_te_hz_cell(S, B, blockIdx.y * AROWS + threadIdx.y,
+                  (blockIdx.x * 32 + threadIdx.x) * 4);
+}
+
+// Two node-local kernels of consecutive reverse steps in one launch: the last kernel
+// of step q (gEz / gHz from the neighbours' difference adjoints, written by the
+// previous launch) and the first kernel of step q-1 on the same node, which reads only
+// that node's adjoint state. Three launches per step become two.
+__global__ void __launch_bounds__(32 * AROWS) k_adj_tm_eze(const __grid_constant__ mtb_yee2d_struct S,
+                                                           const __grid_constant__ mtb_adj2d_buffers B,
+                                                           const float *__restrict__ radj,
+                                                           const float *__restrict__ rec) {
+    const int i = blockIdx.y * AROWS + threadIdx.y, jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    adj_tm_ez_cell(S, B, i, jb);
+    adj_tm_e_cell(S, B, radj, rec, i, jb);
+}
+
+__global__ void __launch_bounds__(32 * AROWS) k_adj_te_hzh(const __grid_constant__ mtb_yee2d_struct S,
+                                                           const __grid_constant__ mtb_adj2d_buffers B,
+                                                           const float *__restrict__ radj) {
+    const int i = blockIdx.y * AROWS + threadIdx.y, jb = (blockIdx.x * 32 + threadIdx.x) * 4;
+    adj_te_hz_cell(S, B, i, jb);
+    adj_te_h_cell(S, B, radj, i, jb);
 }
 
 }  // namespace mtb
@@ -413,25 +471,40 @@ static int adjoint_chunk(mtb_yee2d_adjoint *p, int k, const float *rec, int64_t 
     const mtb_yee2d_struct &S = p->s;
     const dim3 blk(32, AROWS);
     const dim3 grid((S.pitch / 4 + 31) / 32, (S.nx + AROWS - 1) / AROWS);
+    // step q: first kernel (fused with the previous step's last, except at q = k-1),
+    // middle kernel, and the last kernel alone only at q = 0
+    auto radj_of = [&](int q) { return p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems; };
+    auto rec_of = [&](int q) { return rec + (size_t)q * rec_slot_elems; };
     for (int q = k - 1; q >= 0; --q) {
-        const float *radj = p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems;
-        const float *rq = rec + (size_t)q * rec_slot_elems;
+        const float *radj = radj_of(q);
+        const float *rq = rec_of(q);
         if (S.pol == MTB_TM) {
-            k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0]);
-            MTB_CHECK_LAUNCH();
+            if (q == k - 1) {
+                k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0]);
+                MTB_CHECK_LAUNCH();
+            }
             k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
             MTB_CHECK_LAUNCH();
-            k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
+            if (q > 0)
+                k_adj_tm_eze<<<grid, blk, 0, st>>>(S, p->b, radj_of(q - 1),
+                                                   rec_of(q - 1) + rec_offset[0]);
+            else
+                k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
             MTB_CHECK_LAUNCH();
         } else {
-            k_adj_te_h<<<grid, blk, 0, st>>>(S, p->b, radj);
-            MTB_CHECK_LAUNCH();
+            if (q == k - 1) {
+                k_adj_te_h<<<grid, blk, 0, st>>>(S, p->b, radj);
+                MTB_CHECK_LAUNCH();
+            }
             k_adj_te_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0], rq + rec_offset[1]);
             MTB_CHECK_LAUNCH();
-            k_adj_te_hz<<<grid, blk, 0, st>>>(S, p->b);
+            if (q > 0)
+                k_adj_te_hzh<<<grid, blk, 0, st>>>(S, p->b, radj_of(q - 1));
+            else
+                k_adj_te_hz<<<grid, blk, 0, st>>>(S, p->b);
             MTB_CHECK_LAUNCH();
         }
-        p->last_launches += 3;
+        p->last_launches += (q == k - 1) ? 3 : 2;
     }
     return MTB_OK;
 }
