@@ -209,6 +209,22 @@ typedef struct mtb_yee2d_struct {
      * MTB_UNSUPPORTED. */
     const float *chi2, *chi3, *eps_nl;
     const void *pad3_;
+    /* TM magnetic Lorentz poles (core/coeffs.py:177-193; core/stepper_tm.py:114-117,
+     * :186-196, :209-219): n_mpoles (<= MTB_MAX_POLES) on Hx (slot 0) and Hy (slot 1).
+     * B integrates the curl (B' = B -/+ dt curl, CPML as for H), the magnetic sheet
+     * sources go into B, M(n+1) = mc1 M(n) + mc2 M(n-1) + mc3 H(n-1/2) and
+     * H(n+1/2) = B(n+1/2) - sum_k M_k(n+1). f_b[c][2]: B, ping-pong box arrays like
+     * f_x / f_y; mpol[c][3]: stacks of n_mpoles planes rotating like pol_p (buffer s =
+     * mtb_yee2d_pole_slot holds M(n), (s+2)%3 M(n-1), (s+1)%3 receives M(n+1));
+     * mpc[c][3]: mc1, mc2, mc3 stacks. No magnetic conductivity pairs and no live
+     * symmetry-cut lines with them (core/coeffs.py:177-179, :240-244). Tile kernels
+     * only (variant 2); other variants, the no-alloc entry and the adjoint return
+     * MTB_UNSUPPORTED. */
+    int32_t n_mpoles;
+    int32_t pad4_[3];
+    float *f_b[2][2];
+    float *mpol[2][3];
+    const float *mpc[2][3];
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

@@ -54,7 +54,9 @@ class Yee2DStruct(C.Structure):
                 ("cut_map_x", C.c_int32), ("cut_ph_y", C.c_float), ("cut_ph_x", C.c_float),
                 ("pad2_", C.c_int32 * 2),
                 ("f_x0", vp * 2), ("f_y0", vp * 2),
-                ("chi2", vp), ("chi3", vp), ("eps_nl", vp), ("pad3_", vp)]
+                ("chi2", vp), ("chi3", vp), ("eps_nl", vp), ("pad3_", vp),
+                ("n_mpoles", C.c_int32), ("pad4_", C.c_int32 * 3), ("f_b", (vp * 2) * 2),
+                ("mpol", (vp * 3) * 2), ("mpc", (vp * 3) * 2)]
 
 
 class PhaseGroup(C.Structure):

@@ -122,7 +122,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("m_poles", "m_pole_masks", "eps_tensor", "poles_tensor", "pole_masks_tensor")
+_UNSUPPORTED = ("eps_tensor", "poles_tensor", "pole_masks_tensor")
 
 
 def _check_parity(**kw):
@@ -215,10 +215,33 @@ def _poles_tm(grid: Grid, eps, poles, pole_masks):
     return c1, c2, c3
 
 
+def _mpoles_tm(grid: Grid, m_poles, m_pole_masks):
+    """Magnetic Lorentz recurrences (core/coeffs.py:177-193): per pole (fn, gamma,
+    sigma), c1 = (2 - w0^2 dt^2) / den, c2 = -(1 - G dt / 2) / den, c3 = sigma w0^2 dt^2 /
+    den with w0 = 2 pi fn, G = 2 pi gamma, den = 1 + G dt / 2, c3 scaled by the pole's
+    mask averaged onto Hx (along y) and Hy (along x)."""
+    dt, nm = grid.dt, len(m_poles)
+    out = {}
+    for suf, shape, avg in (("x", (grid.nx, grid.ny - 1), lambda v: 0.5 * (v[:, :-1] + v[:, 1:])),
+                            ("y", (grid.nx - 1, grid.ny), lambda v: 0.5 * (v[:-1, :] + v[1:, :]))):
+        c1, c2, c3 = (grid.zeros(nm, *shape) for _ in range(3))
+        for k, (fn, gamma, sigma, *_) in enumerate(m_poles):
+            w0, G = 2 * math.pi * fn, 2 * math.pi * gamma
+            den = 1.0 + G * dt / 2.0
+            m = (m_pole_masks[k] if m_pole_masks is not None
+                 else torch.ones(grid.nx, grid.ny, dtype=grid.dtype, device=grid.device))
+            c1[k] = (2.0 - w0 * w0 * dt * dt) / den
+            c2[k] = -(1.0 - G * dt / 2.0) / den
+            c3[k] = (sigma * w0 * w0 * dt * dt / den) * avg(m.to(device=grid.device,
+                                                                 dtype=grid.dtype))
+        out[f"mc1{suf}"], out[f"mc2{suf}"], out[f"mc3{suf}"] = c1, c2, c3
+    return out
+
+
 def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     y_pmc: bool = False, sigma_d=None, sigma_b=None, mu=None,
                     y_mirror: int = 0, x_mirror: int = 0, y_rot2: int = 0, rot4: int = 0,
-                    chi2=None, chi3=None, **kw) -> TMCoeffs:
+                    chi2=None, chi3=None, m_poles=(), m_pole_masks=None, **kw) -> TMCoeffs:
     """TM coefficients: eps map, CPML profiles sliced to the live nodes --
     H side on the n-1 half nodes, E side on the interior [1:-1] (the full
     axis under y_pmc, where the y layer is off) -- as core/coeffs.py:246-291;
@@ -228,7 +251,9 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
     ``rot4`` (phase +-1) cut the low-y / low-x edge (:209-285): no absorber on the cut
     side, and the E-side profiles run from the cut node to the node before the far wall.
     ``chi2`` / ``chi3`` (scalars or (nx, ny)): instantaneous nonlinearity (:155-158),
-    flagged by ``has_chi2`` / ``has_kerr`` when any value is nonzero."""
+    flagged by ``has_chi2`` / ``has_kerr`` when any value is nonzero. ``m_poles`` /
+    ``m_pole_masks``: magnetic Lorentz poles (:177-193), not combined with sigma_d,
+    sigma_b or mu."""
     _reject(kw)
     _check_parity(y_mirror=y_mirror, x_mirror=x_mirror, y_rot2=y_rot2, rot4=rot4)
     if y_mirror and y_rot2:
@@ -241,9 +266,11 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
     if y_pmc and (y_cut or x_cut):
         raise ValueError("symmetry cuts and y_pmc exclude each other")
     live_line = y_mirror == -1 or x_mirror == -1 or y_rot2 or rot4
-    if live_line and (sigma_b is not None or mu is not None):
-        raise NotImplementedError("odd mirror / Rotate2 / Rotate4 with sigma_b or mu: the "
-                                  "on-plane H line has no magnetic coefficients")
+    if live_line and (sigma_b is not None or mu is not None or m_poles):
+        raise NotImplementedError("odd mirror / Rotate2 / Rotate4 with sigma_b, mu or m_poles: "
+                                  "the on-plane H line has no magnetic coefficients")
+    if m_poles and (sigma_d is not None or sigma_b is not None or mu is not None):
+        raise NotImplementedError("m_poles with sigma_b/mu not combined")
     dt, dx = grid.dt, grid.dx
     eps = _as_field(eps_inf, grid, 1.0)
     x2, x3 = _as_field(chi2, grid, 0.0), _as_field(chi3, grid, 0.0)
@@ -273,7 +300,8 @@ def build_tm_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
         b_hx=b_hx[:, None], a_hx=a_hx[:, None], k_hx=k_hx[:, None],
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         b_ey=b_ey[None, :], a_ey=a_ey[None, :], k_ey=k_ey[None, :],
-        chi2=x2, has_chi2=bool((x2 != 0).any()), **_cond_tm(grid, sigma_d, sigma_b, mu))
+        chi2=x2, has_chi2=bool((x2 != 0).any()), **_cond_tm(grid, sigma_d, sigma_b, mu),
+        **(_mpoles_tm(grid, list(m_poles), m_pole_masks) if m_poles else {}))
 
 
 def _avg_to_ex(v):

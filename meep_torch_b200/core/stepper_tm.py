@@ -28,12 +28,13 @@ class TMState(NamedTuple):
 
 
 def init_tm_state(grid: Grid, n_poles: int = 0, y_pmc: bool = False, y_mirror: int = 0,
-                  x_mirror: int = 0, y_rot2: int = 0, rot4: int = 0, **kw) -> TMState:
+                  x_mirror: int = 0, y_rot2: int = 0, rot4: int = 0, n_mpoles: int = 0,
+                  **kw) -> TMState:
     """Zero TM state, as core/stepper_tm.py:41-71: psi_Hyx / psi_Hxy cover the live
     Ez region -- the interior, every column under y_pmc, or from the cut row / column
     of a low-edge symmetry cut; P_cur / P_prev hold one (nx, ny) plane per dispersive
     pole; Hx0 / Hy0 are the on-plane H lines that an odd mirror, Rotate2 or Rotate4
-    keeps live."""
+    keeps live; ``n_mpoles`` magnetic poles add B and the M histories on Hx / Hy."""
     for k, v in kw.items():
         if v:
             raise NotImplementedError(f"{k}: not implemented on the B200 path")
@@ -46,7 +47,11 @@ def init_tm_state(grid: Grid, n_poles: int = 0, y_pmc: bool = False, y_mirror: i
                    P_cur=z(n_poles, nx, ny), P_prev=z(n_poles, nx, ny), psi_Ezy=z(nx, ny - 1),
                    psi_Ezx=z(nx - 1, ny), psi_Hyx=z(nx_e, ny_e), psi_Hxy=z(nx_e, ny_e),
                    Hx0=z(nx) if (y_mirror == -1 or y_rot2 or rot4) else None,
-                   Hy0=z(ny) if (x_mirror == -1 or rot4) else None)
+                   Hy0=z(ny) if (x_mirror == -1 or rot4) else None,
+                   **(dict(Bx=z(nx, ny - 1), By=z(nx - 1, ny),
+                           Mx_cur=z(n_mpoles, nx, ny - 1), Mx_prev=z(n_mpoles, nx, ny - 1),
+                           My_cur=z(n_mpoles, nx - 1, ny), My_prev=z(n_mpoles, nx - 1, ny))
+                      if n_mpoles else {}))
 
 
 def step_tm(state, m, src_amp=0.0, src_mask=None, src_h_amp: float = 0.0,

@@ -523,6 +523,7 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     if (S.y_pmc || S.cut_y || S.cut_x)
         return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc, symmetry cuts)");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");
+    if (S.n_mpoles) return fail(MTB_UNSUPPORTED, "adjoint: magnetic poles are forward-only");
     if (S.pol == MTB_TE && (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y ||
                             S.mag_h1[0] || S.mag_h1[1]))
         return fail(MTB_UNSUPPORTED, "adjoint: TE conductivity, poles and magnetic pairs are "

@@ -977,7 +977,54 @@ __device__ __forceinline__ float tm_cut_line(const mtb_yee2d_struct &S, const Ct
     return a ? h0[k] + dt * d : h0[k] - dt * d;
 }
 
-template <bool EXPL, bool EXT>
+// Magnetic Lorentz poles on one float4 of an H row (core/stepper_tm.py:209-219): `bh`
+// holds B(n+1/2) (the curl update and the sheet sources applied to B) and becomes
+// H(n+1/2) = B - sum_k M_k(n+1), M(n+1) = mc1 M(n) + mc2 M(n-1) + mc3 H(n-1/2) (`hold`).
+// `store` writes B and the M(n+1) stack (own rows; a recomputed halo row does not).
+__device__ __forceinline__ void tm_mpole4(const mtb_yee2d_struct &S, const Ctx2D &C, int c,
+                                          uint32_t o, bool store, const float (&hold)[4],
+                                          float (&bh)[4]) {
+    const uint32_t pl = (uint32_t)S.nx * S.pitch;
+    const float *Mc = S.mpol[c][C.pst], *Mp = S.mpol[c][(C.pst + 2) % 3];
+    float *Mo = S.mpol[c][(C.pst + 1) % 3];
+    float sm[4];
+    zero4(sm);
+#pragma unroll 1
+    for (int k = 0; k < S.n_mpoles; ++k) {
+        const uint32_t ok = k * pl + o;
+        float mc[4], mp[4], a1[4], a2[4], a3[4];
+        ld4(Mc + ok, mc);
+        ld4(Mp + ok, mp);
+        ld4(S.mpc[c][0] + ok, a1);
+        ld4(S.mpc[c][1] + ok, a2);
+        ld4(S.mpc[c][2] + ok, a3);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            mc[q] = a1[q] * mc[q] + a2[q] * mp[q] + a3[q] * hold[q];
+            sm[q] += mc[q];
+        }
+        if (store) st4(Mo + ok, mc);
+    }
+    if (store) st4(S.f_b[c][C.par ^ 1] + o, bh);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bh[q] = bh[q] - sm[q];
+}
+
+// The same for one cell (lane 0's recomputed left neighbour), not stored.
+__device__ __forceinline__ float tm_mpole1(const mtb_yee2d_struct &S, const Ctx2D &C, int c,
+                                           uint32_t o, float hold, float b) {
+    const uint32_t pl = (uint32_t)S.nx * S.pitch;
+    const float *Mc = S.mpol[c][C.pst], *Mp = S.mpol[c][(C.pst + 2) % 3];
+    float sm = 0.f;
+#pragma unroll 1
+    for (int k = 0; k < S.n_mpoles; ++k) {
+        const uint32_t ok = k * pl + o;
+        sm += S.mpc[c][0][ok] * Mc[ok] + S.mpc[c][1][ok] * Mp[ok] + S.mpc[c][2][ok] * hold;
+    }
+    return b - sm;
+}
+
+template <bool EXPL, bool EXT, bool MP = false>
 __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, const int c0,
                                         const Ctx2D &C, const mtb_line_sample *L, const int nl) {
     const int lane = threadIdx.x;
@@ -1104,9 +1151,17 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
     // Hy(n+1/2) rows i-1 (recomputed halo) and i; magnetic conductivity /
     // permeability pairs when the structure has them
     const float *mh1y = EXT ? S.mag_h1[1] : nullptr, *mh2y = EXT ? S.mag_h2[1] : nullptr;
+    // magnetic Lorentz poles: the curl updates B, H = B - sum M (tm_mpole4)
+    const bool mp = MP && S.n_mpoles > 0;
     float hyP[4], hyN[4];
-    tm_hy(S, i - 1, i >= 1, act, jb, hxbp, hxap, dt, rdx, ez0, ez1, hyp, p1p, hyP, C.amp_h,
-          mh1y, mh2y);
+    {
+        float byp[4];
+        zero4(byp);
+        if (mp && act && i >= 1) ld4(S.f_b[1][par] + ro - P, byp);
+        tm_hy(S, i - 1, i >= 1, act, jb, hxbp, hxap, dt, rdx, ez0, ez1, mp ? byp : hyp, p1p,
+              hyP, C.amp_h, mh1y, mh2y);
+    }
+    if (mp && act && i >= 1) tm_mpole4(S, C, 1, ro - P, false, hyp, hyP);
     if (i < 1) zero4(hyP);
     if (EXT && i == 0 && S.cut_x == 2 && act) {
         // odd x mirror / Rotate4: the on-plane Hy column is the ghost of row 0
@@ -1119,27 +1174,38 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             }
         }
     }
-    tm_hy(S, i, hyRow, act, jb, hxb, hxa, dt, rdx, ez1, ez2, hy, p1, hyN, C.amp_h, mh1y, mh2y);
+    {
+        float byo[4];
+        zero4(byo);
+        if (mp && act) ld4(S.f_b[1][par] + ro, byo);
+        tm_hy(S, i, hyRow, act, jb, hxb, hxa, dt, rdx, ez1, ez2, mp ? byo : hy, p1, hyN, C.amp_h,
+              mh1y, mh2y);
+    }
+    if (mp && act) tm_mpole4(S, C, 1, ro, true, hy, hyN);
 
     // Hx(n+1/2) row i (core/stepper_tm.py:91-94, :121-128): Hx' = Hx - dt curl, or
-    // h1x Hx - h2x curl with magnetic pairs
+    // h1x Hx - h2x curl with magnetic pairs (Bx with magnetic poles)
     const bool magx = EXT && S.mag_h1[0] != nullptr;
     float mx1[4] = {1.f, 1.f, 1.f, 1.f}, mx2[4] = {dt, dt, dt, dt};
     if (magx && act) {
         ld4(S.mag_h1[0] + ro, mx1);
         ld4(S.mag_h2[0] + ro, mx2);
     }
-    float hxN[4];
+    float hxN[4], bxo[4];
+    zero4(bxo);
+    if (mp && act) ld4(S.f_b[0][par] + ro, bxo);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float er = (q < 3) ? ez1[q + 1] : ezR;
         const float d = (er - ez1[q]) * rdx;
         const float pv = hyb[q] * p0[q] + hya[q] * d;
-        const float hn = magx ? mx1[q] * hx[q] - mx2[q] * (d + pv) : hx[q] - dt * (d + pv);
-        hxN[q] = vH[q] ? hn : hx[q];
+        const float f = mp ? bxo[q] : hx[q];
+        const float hn = magx ? mx1[q] * f - mx2[q] * (d + pv) : f - dt * (d + pv);
+        hxN[q] = vH[q] ? hn : f;
         p0[q] = vH[q] ? pv : p0[q];
     }
     if (act && i >= S.src_h2.row_lo && i <= S.src_h2.row_hi) apply_cells(S.src_h2, i, C.amp_h, jb, hxN);
+    if (mp && act) tm_mpole4(S, C, 0, ro, true, hx, hxN);
     // Hx(n+1/2)(i, jb-1): the left lane's last column; lane 0 recomputes its own
     float hxm0 = __shfl_up_sync(0xffffffffu, hxN[3], 1);
     if (lane == 0) {
@@ -1148,9 +1214,11 @@ __device__ __forceinline__ void tm_tile(const mtb_yee2d_struct &S, const int i, 
             const float d = (ez1[0] - ezl) * rdx;
             float c = d;
             if (byHL) c = d + (__ldg(S.hy_b + jl) * p0l + __ldg(S.hy_a + jl) * d);
-            v = magx ? S.mag_h1[0][ro - 1] * hxl - S.mag_h2[0][ro - 1] * c : hxl - dt * c;
+            const float f = mp ? S.f_b[0][par][ro - 1] : hxl;
+            v = magx ? S.mag_h1[0][ro - 1] * f - S.mag_h2[0][ro - 1] * c : f - dt * c;
             if (i >= S.src_h2.row_lo && i <= S.src_h2.row_hi)
                 v = apply_cell1(S.src_h2, i, jl, C.amp_h, v);
+            if (mp) v = tm_mpole1(S, C, 0, ro - 1, hxl, v);
         } else if (EXT && jb == 0 && S.cut_y == 2) {
             // odd y mirror / Rotate2 / Rotate4: the on-plane Hx row is the ghost of column 0
             v = tm_cut_line<EXPL, EXT>(S, C, 0, i, ez1[0], dt, rdx);
@@ -1713,7 +1781,7 @@ __device__ __forceinline__ void tm_rows(const mtb_yee2d_struct &S, const int ib,
     }
 }
 
-template <bool FIRST, bool EXT>
+template <bool FIRST, bool EXT, bool MP = false>
 __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     const mtb_yee2d_struct *__restrict__ SS, const int4 *__restrict__ work, int n_work,
     Ctx2D C) {
@@ -1730,7 +1798,7 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
                       ib - 1 >= S.xband[0] && last < S.xband[1] &&
                       ib >= S.xband[2] && last < S.xband[3] && S.cond_d1[0] == nullptr &&
                       S.n_poles == 0 && S.mag_h1[0] == nullptr && S.mag_h1[1] == nullptr &&
-                      S.chi2 == nullptr && !(EXT && S.cut_y && w.z == 0);
+                      S.chi2 == nullptr && S.n_mpoles == 0 && !(EXT && S.cut_y && w.z == 0);
     if (lean) {
         const int jb = w.z + 4 * threadIdx.x;
         const bool yb = jb < S.pitch &&
@@ -1748,9 +1816,9 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_tm(
     for (int r = 0; r < C.wr; ++r) {
         if (ib + r >= S.nx) break;
         if (FIRST && expl)
-            tm_tile<true, EXT>(S, ib + r, w.z, C, T.lines, T.nl);
+            tm_tile<true, EXT, MP>(S, ib + r, w.z, C, T.lines, T.nl);
         else
-            tm_tile<false, EXT>(S, ib + r, w.z, C, T.lines, T.nl);
+            tm_tile<false, EXT, MP>(S, ib + r, w.z, C, T.lines, T.nl);
     }
 }
 
@@ -2001,6 +2069,7 @@ struct mtb_yee2d_plan {
     int n_cols = 0;
     int rows = 32;
     int variant = 2;                   // 1 row march, 2 tiles
+    bool mpoles = false;               // a structure has magnetic Lorentz poles
     int wr = 1;                        // tiles: rows per warp
     bool ext = false;                  // a structure has conductivity or poles
     bool poles = false;                // a structure has poles (no graph replay)
@@ -2064,7 +2133,7 @@ static int tmap_2d(CUtensorMap *m, const float *base, int nx, int pitch, int bc,
 static bool tb_eligible(const mtb_yee2d_struct &S) {
     return !S.cond_d1[0] && !S.cond_d1[1] && !S.n_poles && !S.n_poles_y && !S.mag_h1[0] &&
            !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc && !S.cut_y && !S.cut_x &&
-           !S.chi2;
+           !S.chi2 && !S.n_mpoles;
 }
 
 // Copy n floats of a device array to the host.
@@ -2361,6 +2430,30 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         if (S.pol == MTB_TE && S.y_pmc)
             return fail(MTB_UNSUPPORTED, "structure %d: y_pmc is a TM option", s);
         int rc;
+        if (S.n_mpoles) {
+            if (S.n_mpoles < 0 || S.n_mpoles > MTB_MAX_POLES)
+                return fail(MTB_INVALID_ARG, "structure %d: %d magnetic poles outside [0, %d]",
+                            s, S.n_mpoles, MTB_MAX_POLES);
+            if (S.pol != MTB_TM)
+                return fail(MTB_INVALID_ARG, "structure %d: magnetic poles are a TM option", s);
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: magnetic poles need the tile "
+                            "kernels (variant 2)", s);
+            if (S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1] || S.cut_y == 2 ||
+                S.cut_x == 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: magnetic poles with magnetic "
+                            "conductivity or a live symmetry-cut line", s);
+            for (int c = 0; c < 2; ++c) {
+                for (int b = 0; b < 2; ++b)
+                    if ((rc = check_ptr(S.f_b[c][b], "f_b", s))) return rc;
+                for (int b = 0; b < 3; ++b)
+                    if ((rc = check_ptr(S.mpol[c][b], "mpol", s)) ||
+                        (rc = check_ptr(S.mpc[c][b], "mpc", s)))
+                        return rc;
+            }
+            if ((int64_t)S.n_mpoles * S.nx * S.pitch >= (1LL << 31))
+                return fail(MTB_UNSUPPORTED, "structure %d: magnetic pole planes too large", s);
+        }
         if (S.chi2 || S.chi3 || S.eps_nl) {
             if (S.pol != MTB_TM)
                 return fail(MTB_UNSUPPORTED, "structure %d: chi2 / chi3 on the kernels are TM "
@@ -2515,9 +2608,11 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     {
         if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0 ||
             structs[s].mag_h1[0] || structs[s].mag_h1[1] || structs[s].cut_y || structs[s].cut_x ||
-            structs[s].chi2)
+            structs[s].chi2 || structs[s].n_mpoles)
             p->ext = true;
-        if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0) p->poles = true;
+        if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0 || structs[s].n_mpoles > 0)
+            p->poles = true;
+        if (structs[s].n_mpoles > 0) p->mpoles = true;
     }
     for (int s = 0; s < n; ++s) want_tb = want_tb && tb_eligible(structs[s]);
     for (int s = 0; s < n; ++s)
@@ -2595,7 +2690,13 @@ static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
     if (p->variant == 2) {
         const dim3 blk(32, TROWS);
         if (n_tm > 0) {
-            if (C.first && p->ext)
+            if (p->mpoles) {
+                // magnetic Lorentz poles: their own instantiation (more live registers)
+                if (C.first)
+                    k_tile_tm<true, true, true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+                else
+                    k_tile_tm<false, true, true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
+            } else if (C.first && p->ext)
                 k_tile_tm<true, true><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
             else if (C.first)
                 k_tile_tm<true, false><<<n_tm, blk, 0, st>>>(SS, W, n_tm, C);
@@ -3256,7 +3357,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
     if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles ||
         S.n_poles_y || S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1] || S.cut_y ||
-        S.cut_x || S.chi2)
+        S.cut_x || S.chi2 || S.n_mpoles)
         return fail(MTB_UNSUPPORTED, "noalloc: conductivity, poles and symmetry cuts need the "
                     "tile kernels");
     int rc;

@@ -224,8 +224,13 @@ class Engine2D:
             np_ = s.P_cur.shape[0]
             _need(np_ <= L.MTB_MAX_POLES, f"{np_} dispersive poles (at most {L.MTB_MAX_POLES})")
             _need(tuple(c.c1.shape) == (np_, it.nx, it.ny), "pole coefficients c1 shape")
-            _opt_none(s, ["Bx"])
-            _opt_none(c, ["mc1x"])
+            it.n_mp = 0 if getattr(c, "mc1x", None) is None else int(c.mc1x.shape[0])
+            _need((getattr(s, "Bx", None) is None) == (it.n_mp == 0),
+                  "TMState.Bx and the coefficients' magnetic poles must come together")
+            _need(it.n_mp <= L.MTB_MAX_POLES,
+                  f"{it.n_mp} magnetic poles (at most {L.MTB_MAX_POLES})")
+            if it.n_mp:
+                _need(tuple(s.Mx_cur.shape[:1]) == (it.n_mp,), "TMState.Mx_cur pole count")
             it.mag = _magnetic_pairs(c, [("h1x", "h2x"), ("h1y", "h2y")])
         it.cuts = _cuts(c, it.te)
         if not it.te:
@@ -448,6 +453,27 @@ class Engine2D:
             it.src_scale = None
             it.plain = (not te and not S.n_poles and not S.explicit_e and not (S.cut_y or S.cut_x)
                         and not it.nl)
+            if not te and it.n_mp:
+                # magnetic Lorentz poles: B pairs, M stacks (M(n) in slot 0, M(n-1) in
+                # slot 2, as the electric poles) and mc1..mc3
+                nm = it.n_mp
+                S.n_mpoles = nm
+                fb = [self._pair(s.Bx, nx, P), self._pair(s.By, nx, P)]
+                mstk = []
+                for c_, (cur, prev, cs) in enumerate(
+                        ((s.Mx_cur, s.Mx_prev, ("mc1x", "mc2x", "mc3x")),
+                         (s.My_cur, s.My_prev, ("mc1y", "mc2y", "mc3y")))):
+                    mm = [self._pack_stack(cur, nx, P), None, self._pack_stack(prev, nx, P)]
+                    mm[1] = torch.zeros_like(mm[0])
+                    mc = [self._pack_stack(getattr(c, k), nx, P) for k in cs]
+                    for b in range(2):
+                        S.f_b[c_][b] = L.ptr(fb[c_][b])
+                    for k in range(3):
+                        S.mpol[c_][k], S.mpc[c_][k] = L.ptr(mm[k]), L.ptr(mc[k])
+                    mstk.append(mm)
+                    it.keep += fb[c_] + mm + mc
+                it.box["B"], it.box["M"] = fb, mstk
+                it.plain = False
             if it.nl:
                 x2 = self._pack(c.chi2 if c.chi2 is not None else torch.zeros_like(c.eps_inf),
                                 nx, P)
@@ -909,7 +935,7 @@ class Engine2D:
         if it.nl:
             # the fixed point the kernels use (core/stepper_tm.py:222-230)
             c = it.coeffs
-            rhs = Dz - (pol["P_cur"].sum(0) if pol else 0.0)
+            rhs = Dz - (pol["P_cur"].sum(0) if "P_cur" in pol else 0.0)
             eps = c.eps_inf.to(Dz)
             x2 = c.chi2.to(Dz) if c.chi2 is not None else torch.zeros_like(Dz)
             x3 = c.chi3.to(Dz)
@@ -922,6 +948,15 @@ class Engine2D:
         for name, n in (("Hx0", nx), ("Hy0", ny)):
             if name in bx:
                 pol[name] = bx[name][cur][:n].clone()
+        if "B" in bx:
+            nm, ps_ = it.n_mp, self.pole_slot
+            shp = ((nx, ny - 1), (nx - 1, ny))
+            pol.update(Bx=self._unpack(bx["B"][0][cur], shp[0]),
+                       By=self._unpack(bx["B"][1][cur], shp[1]))
+            for c_, sfx in enumerate(("x", "y")):
+                mm = bx["M"][c_]
+                pol[f"M{sfx}_cur"] = self._unpack_stack(mm[ps_], nm, nx, shp[c_])
+                pol[f"M{sfx}_prev"] = self._unpack_stack(mm[(ps_ + 2) % 3], nm, nx, shp[c_])
         return s._replace(
             Ez=Ez, Dz=Dz, **pol,
             Hx=self._unpack(bx["x"][cur], (nx, ny - 1)),

@@ -162,8 +162,8 @@ def test_unsupported_features_raise():
     from meep_torch_b200.core.coeffs import build_tm_coeffs
     from meep_torch_b200.core.grid import Grid
     g = Grid(nx=20, ny=20, dx=0.05, device="cpu")
-    with pytest.raises(NotImplementedError):
-        build_tm_coeffs(g, m_poles=[(1.0, 0.1, 1.0)])
+    with pytest.raises(NotImplementedError):          # the reference refuses the pair too
+        build_tm_coeffs(g, m_poles=[(1.0, 0.1, 1.0)], mu=2.0)
     with pytest.raises(NotImplementedError):
         build_tm_coeffs(g, eps_tensor=torch.ones(3, 20, 20))
     m = build_tm_coeffs(g, chi3=torch.ones(20, 20))          # chi2 / chi3: built, flagged
@@ -273,3 +273,23 @@ def test_magnetic_coefficients_match_oracle():
     for k in ("hz1", "hz2", "d1x", "d2y"):
         np.testing.assert_allclose(getattr(t, k).numpy(), ct[k], rtol=5e-7, atol=0, err_msg=k)
     assert t.hz1.shape == (19, 23)
+
+
+def test_magnetic_pole_coefficients_and_state_match_oracle():
+    """m_poles: the Hx / Hy recurrences with their masks averaged onto the H nodes, and
+    the state's B and M histories."""
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    rng = np.random.default_rng(5)
+    mp = [(0.6, 0.05, 0.8), (0.9, 0.1, 0.4)]
+    masks = [(rng.random((30, 24)) < 0.4).astype(np.float64) for _ in mp]
+    g = Grid(nx=30, ny=24, dx=0.05, device="cpu")
+    m = build_tm_coeffs(g, npml=5, m_poles=mp,
+                        m_pole_masks=[torch.tensor(x, dtype=torch.float32) for x in masks])
+    o = O.tm_coeffs(30, 24, 0.05, npml=5, m_poles=mp, m_pole_masks=masks, dtype=np.float32)
+    for k in ("mc1x", "mc2x", "mc3x", "mc1y", "mc2y", "mc3y"):
+        np.testing.assert_allclose(getattr(m, k).numpy(), o[k], rtol=2e-6, atol=1e-7)
+    s, so = init_tm_state(g, n_mpoles=2), O.tm_state(o)
+    for k in ("Bx", "By", "Mx_cur", "Mx_prev", "My_cur", "My_prev"):
+        assert tuple(getattr(s, k).shape) == so[k].shape, k

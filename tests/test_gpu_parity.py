@@ -53,6 +53,11 @@ def run_tm_case(case, phase_mode="exact"):
     pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
     mag = {k: torch.tensor(g[k], dtype=torch.float32)
            for k in ("sigma_b", "mu", "chi2", "chi3") if k in g}
+    n_mp = 0
+    if "m_poles" in g:
+        mag.update(m_poles=json.loads(str(g["m_poles"])),
+                   m_pole_masks=[torch.tensor(x, dtype=torch.float32) for x in g["m_pole_masks"]])
+        n_mp = len(mag["m_poles"])
     m = build_tm_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
                         npml=int(g["npml"]), y_pmc=pmc,
                         sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32),
@@ -66,14 +71,15 @@ def run_tm_case(case, phase_mode="exact"):
     monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=ix, lo=xlo, hi=xhi)
     mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=iy, lo=ylo, hi=yhi)
     dft = DFTFieldsMonitor(grid, freqs, "Ez")
-    st, accs = run_tm(init_tm_state(grid, y_pmc=pmc, n_poles=len(poles)), m, int(g["n_steps"]),
+    st, accs = run_tm(init_tm_state(grid, y_pmc=pmc, n_poles=len(poles), n_mpoles=n_mp), m,
+                      int(g["n_steps"]),
                       source=src, monitors=[monx, mony, dft], phase_mode=phase_mode)
     fx, fy = monx.flux(accs[0], dx), mony.flux(accs[1], dx)
     return st, accs, (fx, fy)
 
 
 @pytest.mark.parametrize("case", ["tm", "tm_point_pmc", "tm_sigma", "tm_poles",
-                                  "tm_magnetic", "tm_nonlinear"])
+                                  "tm_magnetic", "tm_nonlinear", "tm_mpoles"])
 def test_tm_matches_reference(case):
     st, accs, (fx, fy) = run_tm_case(case)
     e32, e64 = {}, {}
@@ -82,6 +88,8 @@ def test_tm_matches_reference(case):
         names = ["Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy"]
         if "s_P_cur" in g:
             names += ["P_cur", "P_prev"]
+        names += [k for k in ("Bx", "By", "Mx_cur", "Mx_prev", "My_cur", "My_prev")
+                  if "s_" + k in g]
         for k in names:
             errs[k] = rel_l2(getattr(st, k).cpu().numpy(), g["s_" + k])
         for a, key in zip(accs, ("acc_x", "acc_y", "acc_dft")):
