@@ -35,6 +35,7 @@
 namespace mtb {
 
 constexpr int AROWS = 8;          // rows per block (one warp per row)
+constexpr int AMAXL = 16;         // line samples per structure (the forward plan's limit)
 
 __device__ __forceinline__ void ldv(const float *p, float (&v)[4]) {
     const float4 x = *reinterpret_cast<const float4 *>(p);
@@ -44,12 +45,22 @@ __device__ __forceinline__ void stv(float *p, const float (&v)[4]) {
     *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
+// The structure's line-sample descriptors, copied to shared memory once per block
+// (every thread of the block reads them for each of its cells).
+__device__ __forceinline__ const mtb_line_sample *stage_lines(const mtb_yee2d_struct &S,
+                                                              mtb_line_sample *sl) {
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    if (t < S.n_lines) sl[t] = S.lines[t];
+    __syncthreads();
+    return sl;
+}
+
 // Add the adjoint ring's values for the forward samples of component `comp`
 // at row i, columns jb .. jb+3 (the transpose of the forward kernels'
 // full-grid sample and line samples).
-__device__ __forceinline__ void inject(const mtb_yee2d_struct &S, int comp, int i, int jb,
-                                       uint32_t g, const float *__restrict__ radj,
-                                       float (&v)[4]) {
+__device__ __forceinline__ void inject(const mtb_yee2d_struct &S, const mtb_line_sample *L,
+                                       int comp, int i, int jb, uint32_t g,
+                                       const float *__restrict__ radj, float (&v)[4]) {
     const int64_t rf = S.ring_full[comp];
     if (rf >= 0) {
         float r[4];
@@ -58,7 +69,7 @@ __device__ __forceinline__ void inject(const mtb_yee2d_struct &S, int comp, int 
         for (int q = 0; q < 4; ++q) v[q] += r[q];
     }
     for (int l = 0; l < S.n_lines; ++l) {
-        const mtb_line_sample ln = S.lines[l];
+        const mtb_line_sample ln = L[l];
         if (ln.comp != comp) continue;
         if (ln.kind == 0) {
             if (ln.index != i) continue;
@@ -77,6 +88,7 @@ __device__ __forceinline__ void inject(const mtb_yee2d_struct &S, int comp, int 
 }
 
 __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const mtb_line_sample *L,
                                               const float *__restrict__ radj,
                                               const float *__restrict__ rec, const int i,
                                               const int jb) {
@@ -92,7 +104,7 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
     ldv(rec + g, ez);
     ldv(S.inv_eps_a + g, ie);
     ldv(B.g_eps[0] + g, ge);
-    inject(S, MTB_C2_MAIN, i, jb, g, radj, gez);
+    inject(S, L, MTB_C2_MAIN, i, jb, g, radj, gez);
     const bool rowin = i >= 1 && i <= nx - 2;
     float bex = 1.f, aex = 0.f;
     if (rowin) { bex = S.ex_b[i]; aex = S.ex_a[i]; }
@@ -153,11 +165,14 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__
                                                          const __grid_constant__ mtb_adj2d_buffers B,
                                                          const float *__restrict__ radj,
                                                          const float *__restrict__ rec) {
-    adj_tm_e_cell(S, B, radj, rec, blockIdx.y * AROWS + threadIdx.y,
+    __shared__ mtb_line_sample sl[AMAXL];
+    const mtb_line_sample *L = stage_lines(S, sl);
+    adj_tm_e_cell(S, B, L, radj, rec, blockIdx.y * AROWS + threadIdx.y,
                   (blockIdx.x * 32 + threadIdx.x) * 4);
 }
 
 __device__ __forceinline__ void adj_tm_h_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const mtb_line_sample *L,
                                               const float *__restrict__ radj, const int i,
                                               const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
@@ -174,8 +189,8 @@ __device__ __forceinline__ void adj_tm_h_cell(const mtb_yee2d_struct &S, const m
     if (i + 1 < nx) ldv(B.tmp[0] + g + P, t1n);
     else t1n[0] = t1n[1] = t1n[2] = t1n[3] = 0.f;
     const float t2r = (jb + 4 < P) ? B.tmp[1][g + 4] : 0.f;
-    inject(S, MTB_C2_X, i, jb, g, radj, ghx);
-    inject(S, MTB_C2_Y, i, jb, g, radj, ghy);
+    inject(S, L, MTB_C2_X, i, jb, g, radj, ghx);
+    inject(S, L, MTB_C2_Y, i, jb, g, radj, ghy);
     const bool vrow = i <= nx - 2;
     float bhx = 1.f, ahx = 0.f;
     if (vrow) { bhx = S.hx_b[i]; ahx = S.hx_a[i]; }
@@ -217,7 +232,9 @@ __device__ __forceinline__ void adj_tm_h_cell(const mtb_yee2d_struct &S, const m
 __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__ mtb_yee2d_struct S,
                                                          const __grid_constant__ mtb_adj2d_buffers B,
                                                          const float *__restrict__ radj) {
-    adj_tm_h_cell(S, B, radj, blockIdx.y * AROWS + threadIdx.y,
+    __shared__ mtb_line_sample sl[AMAXL];
+    const mtb_line_sample *L = stage_lines(S, sl);
+    adj_tm_h_cell(S, B, L, radj, blockIdx.y * AROWS + threadIdx.y,
                   (blockIdx.x * 32 + threadIdx.x) * 4);
 }
 
@@ -265,6 +282,7 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant_
 // As for TM, k_adj_te_hz of step q and k_adj_te_h of step q-1 run as one launch
 // (k_adj_te_hzh).
 __device__ __forceinline__ void adj_te_h_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const mtb_line_sample *L,
                                               const float *__restrict__ radj, const int i,
                                               const int jb) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
@@ -275,7 +293,7 @@ __device__ __forceinline__ void adj_te_h_cell(const mtb_yee2d_struct &S, const m
     ldv(B.g[0] + g, ghz);
     ldv(B.g_psi[2] + g, gp2);
     ldv(B.g_psi[3] + g, gp3);
-    inject(S, MTB_C2_MAIN, i, jb, g, radj, ghz);
+    inject(S, L, MTB_C2_MAIN, i, jb, g, radj, ghz);
     const bool vrow = i <= nx - 2;
     float hxb = 1.f, hxa = 0.f;
     if (vrow) { hxb = S.hx_b[i]; hxa = S.hx_a[i]; }
@@ -302,11 +320,14 @@ __device__ __forceinline__ void adj_te_h_cell(const mtb_yee2d_struct &S, const m
 __global__ void __launch_bounds__(32 * AROWS) k_adj_te_h(const __grid_constant__ mtb_yee2d_struct S,
                                                          const __grid_constant__ mtb_adj2d_buffers B,
                                                          const float *__restrict__ radj) {
-    adj_te_h_cell(S, B, radj, blockIdx.y * AROWS + threadIdx.y,
+    __shared__ mtb_line_sample sl[AMAXL];
+    const mtb_line_sample *L = stage_lines(S, sl);
+    adj_te_h_cell(S, B, L, radj, blockIdx.y * AROWS + threadIdx.y,
                   (blockIdx.x * 32 + threadIdx.x) * 4);
 }
 
 __device__ __forceinline__ void adj_te_e_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
+                                              const mtb_line_sample *L,
                                               const float *__restrict__ radj,
                                               const float *__restrict__ rex,
                                               const float *__restrict__ rey, const int i,
@@ -334,8 +355,8 @@ __device__ __forceinline__ void adj_te_e_cell(const mtb_yee2d_struct &S, const m
     if (i >= 1) ldv(B.tmp[0] + g - P, u0p);
     else u0p[0] = u0p[1] = u0p[2] = u0p[3] = 0.f;
     const float u1l = (jb >= 1) ? B.tmp[1][g - 1] : 0.f;
-    inject(S, MTB_C2_X, i, jb, g, radj, gex);
-    inject(S, MTB_C2_Y, i, jb, g, radj, gey);
+    inject(S, L, MTB_C2_X, i, jb, g, radj, gex);
+    inject(S, L, MTB_C2_Y, i, jb, g, radj, gey);
     const bool xrow = i <= nx - 2, yrow = i >= 1 && i <= nx - 2;
     float exb = 1.f, exa = 0.f;
     if (yrow) { exb = S.ex_b[i]; exa = S.ex_a[i]; }
@@ -385,7 +406,9 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_te_e(const __grid_constant__
                                                          const float *__restrict__ radj,
                                                          const float *__restrict__ rex,
                                                          const float *__restrict__ rey) {
-    adj_te_e_cell(S, B, radj, rex, rey, blockIdx.y * AROWS + threadIdx.y,
+    __shared__ mtb_line_sample sl[AMAXL];
+    const mtb_line_sample *L = stage_lines(S, sl);
+    adj_te_e_cell(S, B, L, radj, rex, rey, blockIdx.y * AROWS + threadIdx.y,
                   (blockIdx.x * 32 + threadIdx.x) * 4);
 }
 
@@ -426,17 +449,21 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_eze(const __grid_constant
                                                            const __grid_constant__ mtb_adj2d_buffers B,
                                                            const float *__restrict__ radj,
                                                            const float *__restrict__ rec) {
+    __shared__ mtb_line_sample sl[AMAXL];
+    const mtb_line_sample *L = stage_lines(S, sl);
     const int i = blockIdx.y * AROWS + threadIdx.y, jb = (blockIdx.x * 32 + threadIdx.x) * 4;
     adj_tm_ez_cell(S, B, i, jb);
-    adj_tm_e_cell(S, B, radj, rec, i, jb);
+    adj_tm_e_cell(S, B, L, radj, rec, i, jb);
 }
 
 __global__ void __launch_bounds__(32 * AROWS) k_adj_te_hzh(const __grid_constant__ mtb_yee2d_struct S,
                                                            const __grid_constant__ mtb_adj2d_buffers B,
                                                            const float *__restrict__ radj) {
+    __shared__ mtb_line_sample sl[AMAXL];
+    const mtb_line_sample *L = stage_lines(S, sl);
     const int i = blockIdx.y * AROWS + threadIdx.y, jb = (blockIdx.x * 32 + threadIdx.x) * 4;
     adj_te_hz_cell(S, B, i, jb);
-    adj_te_h_cell(S, B, radj, i, jb);
+    adj_te_h_cell(S, B, L, radj, i, jb);
 }
 
 }  // namespace mtb
@@ -524,6 +551,8 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
         return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc, symmetry cuts)");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");
     if (S.n_mpoles) return fail(MTB_UNSUPPORTED, "adjoint: magnetic poles are forward-only");
+    if (S.n_lines < 0 || S.n_lines > AMAXL || (S.n_lines > 0 && !S.lines))
+        return fail(MTB_INVALID_ARG, "adjoint: %d line samples (at most %d)", S.n_lines, AMAXL);
     if (S.pol == MTB_TE && (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y ||
                             S.mag_h1[0] || S.mag_h1[1]))
         return fail(MTB_UNSUPPORTED, "adjoint: TE conductivity, poles and magnetic pairs are "
