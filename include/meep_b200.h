@@ -225,6 +225,20 @@ typedef struct mtb_yee2d_struct {
     float *f_b[2][2];
     float *mpol[2][3];
     const float *mpc[2][3];
+    /* TE in-plane tensor eps and oriented poles (core/coeffs.py:389-399, :428-456;
+     * core/stepper_te.py:136-175): te3 = 1 runs the structure as three passes (D and
+     * poles, E, Hz) with E stored in e_x (Ex, nx-1 x ny) and e_y (Ey, nx x ny-1), box
+     * layout, one buffer each, holding the state's E between steps. tinv: inv_xx and
+     * inv_xy at the Ex nodes, inv_yy and inv_xy at the Ey nodes (null: E = rhs / eps
+     * from inv_eps_a / inv_eps_b). c3xy / c3yx: the oriented poles' cross drives of Px
+     * by the four-node average of Ey and of Py by that of Ex, stacks like pol_c / pol_cy
+     * (null = none). Tile kernels only (variant 2); other variants, the no-alloc entry
+     * and the adjoint return MTB_UNSUPPORTED. */
+    int32_t te3;
+    int32_t pad5_[3];
+    const float *tinv[4];
+    float *e_x, *e_y;
+    const float *c3xy, *c3yx;
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

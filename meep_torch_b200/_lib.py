@@ -56,7 +56,9 @@ class Yee2DStruct(C.Structure):
                 ("f_x0", vp * 2), ("f_y0", vp * 2),
                 ("chi2", vp), ("chi3", vp), ("eps_nl", vp), ("pad3_", vp),
                 ("n_mpoles", C.c_int32), ("pad4_", C.c_int32 * 3), ("f_b", (vp * 2) * 2),
-                ("mpol", (vp * 3) * 2), ("mpc", (vp * 3) * 2)]
+                ("mpol", (vp * 3) * 2), ("mpc", (vp * 3) * 2),
+                ("te3", C.c_int32), ("pad5_", C.c_int32 * 3), ("tinv", vp * 4),
+                ("e_x", vp), ("e_y", vp), ("c3xy", vp), ("c3yx", vp)]
 
 
 class PhaseGroup(C.Structure):

@@ -5,8 +5,7 @@ The NamedTuple field names are the reference's, so either side's objects can
 be handed to either side's run drivers. The builders cover the B200 path's
 feature set -- scalar eps, CPML (kappa = 1), PEC walls, TM PMC-in-y walls and the
 low-edge symmetry cuts (mirrors; TM Rotate2 / Rotate4), conductivity, permeability and
-dispersive poles and chi2 / chi3; the reference's magnetic-pole and tensor options raise
-NotImplementedError here (the reference itself still runs them).
+dispersive and magnetic poles, chi2 / chi3, the TE tensor eps and oriented poles.
 """
 import math
 from typing import NamedTuple
@@ -122,7 +121,7 @@ def _as_field(val, grid: Grid, default: float) -> torch.Tensor:
     return torch.full((grid.nx, grid.ny), float(val), dtype=grid.dtype, device=grid.device)
 
 
-_UNSUPPORTED = ("eps_tensor", "poles_tensor", "pole_masks_tensor")
+_UNSUPPORTED = ()
 
 
 def _check_parity(**kw):
@@ -334,7 +333,8 @@ def _axis_poles(grid: Grid, eps, shared, axis_poles, shared_masks, axis_masks, s
 def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                     sigma_d=None, poles_x=(), poles_y=(), pole_masks_x=None,
                     pole_masks_y=None, sigma_b=None, mu=None, y_mirror: int = 0,
-                    x_mirror: int = 0, chi2=None, chi3=None, **kw) -> TECoeffs:
+                    x_mirror: int = 0, chi2=None, chi3=None, eps_tensor=None,
+                    poles_tensor=(), pole_masks_tensor=None, **kw) -> TECoeffs:
     """TE coefficients: eps Yee-averaged to Ex (nx-1, ny) and Ey (nx, ny-1)
     (core/coeffs.py:347-354, :387-388), the CPML slices of :480-491, with
     ``sigma_d``, ``sigma_b``, ``mu`` the conductivity and permeability pairs of
@@ -342,7 +342,10 @@ def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
     axes, ``poles_x`` / ``poles_y`` on one). ``y_mirror`` / ``x_mirror`` (+-1) cut the
     low edge (:457-469): no absorber there; the profiles keep their interior slices.
     ``chi2`` / ``chi3`` are averaged onto Ex / Ey (:380-387); the kernels run them for TM
-    only."""
+    only. ``eps_tensor`` = (exx, exy, eyy) at cell centres gives the inverse tensor
+    Yee-averaged onto the E nodes (:389-399); ``poles_tensor`` = [(fn, gamma, (sxx, sxy,
+    syy)[, fc]), ...] appends one oriented pole to each axis stack with the off-diagonal
+    drives c3xy / c3yx (:428-456)."""
     _reject(kw)
     _check_parity(y_mirror=y_mirror, x_mirror=x_mirror)
     dt, dx = grid.dt, grid.dx
@@ -361,6 +364,38 @@ def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
                                 (grid.nx - 1, grid.ny), _avg_to_ex)
     c1y, c2y, c3y = _axis_poles(grid, eps, poles, poles_y, pole_masks, pole_masks_y,
                                 (grid.nx, grid.ny - 1), _avg_to_ey)
+    extra = {}
+    if eps_tensor is not None:
+        exx = _as_field(eps_tensor[0], grid, 1.0)
+        exy = _as_field(eps_tensor[1], grid, 0.0)
+        eyy = _as_field(eps_tensor[2], grid, 1.0)
+        det = exx * eyy - exy * exy
+        extra.update(inv_xx_x=_avg_to_ex(eyy / det), inv_xy_x=_avg_to_ex(-exy / det),
+                     inv_yy_y=_avg_to_ey(exx / det), inv_xy_y=_avg_to_ey(-exy / det))
+    if len(poles_tensor):
+        # oriented poles: one more pole on each axis; the off-diagonal part drives Px
+        # from the averaged Ey and Py from the averaged Ex
+        nt = len(poles_tensor)
+        t = {k: grid.zeros(nt, grid.nx - 1, grid.ny) for k in ("c1x", "c2x", "c3x", "c3xy")}
+        t.update({k: grid.zeros(nt, grid.nx, grid.ny - 1) for k in ("c1y", "c2y", "c3y", "c3yx")})
+        for k, pole in enumerate(poles_tensor):
+            fn, gamma, (sxx, sxy, syy) = pole[0], pole[1], pole[2]
+            fc = pole[3] if len(pole) > 3 else fn
+            cv1, cv2, cv3 = _pole_recurrence((fn, gamma, 1.0, fc), dt)
+            m = (pole_masks_tensor[k] if pole_masks_tensor is not None
+                 else torch.ones_like(eps)).to(eps)
+            mx, my = _avg_to_ex(m), _avg_to_ey(m)
+            t["c1x"][k], t["c2x"][k] = cv1, cv2
+            t["c1y"][k], t["c2y"][k] = cv1, cv2
+            t["c3x"][k], t["c3xy"][k] = cv3 * sxx * mx, cv3 * sxy * mx
+            t["c3y"][k], t["c3yx"][k] = cv3 * syy * my, cv3 * sxy * my
+        n0x, n0y = c1x.shape[0], c1y.shape[0]
+        c1x, c2x, c3x = (torch.cat([a, t[k]]) for a, k in ((c1x, "c1x"), (c2x, "c2x"),
+                                                           (c3x, "c3x")))
+        c1y, c2y, c3y = (torch.cat([a, t[k]]) for a, k in ((c1y, "c1y"), (c2y, "c2y"),
+                                                           (c3y, "c3y")))
+        extra.update(c3xy=torch.cat([grid.zeros(n0x, grid.nx - 1, grid.ny), t["c3xy"]]),
+                     c3yx=torch.cat([grid.zeros(n0y, grid.nx, grid.ny - 1), t["c3yx"]]))
     return TECoeffs(
         dt=dt, dx=dx, eps_x=_avg_to_ex(eps), eps_y=_avg_to_ey(eps),
         chi3_x=_avg_to_ex(x3), chi3_y=_avg_to_ey(x3), has_kerr=bool((x3 != 0).any()),
@@ -371,4 +406,4 @@ def build_te_coeffs(grid: Grid, eps_inf=None, poles=(), pole_masks=None, npml=0,
         b_ex=b_ex[:, None], a_ex=a_ex[:, None], k_ex=k_ex[:, None],
         chi2_x=_avg_to_ex(x2), chi2_y=_avg_to_ey(x2), has_chi2=bool((x2 != 0).any()),
         y_mirror_lo=y_mirror, x_mirror_lo=x_mirror,
-        **_cond_te(grid, sigma_d, sigma_b, mu))
+        **_cond_te(grid, sigma_d, sigma_b, mu), **extra)

@@ -551,6 +551,7 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
         return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc, symmetry cuts)");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");
     if (S.n_mpoles) return fail(MTB_UNSUPPORTED, "adjoint: magnetic poles are forward-only");
+    if (S.te3) return fail(MTB_UNSUPPORTED, "adjoint: TE tensor eps / oriented poles");
     if (S.n_lines < 0 || S.n_lines > AMAXL || (S.n_lines > 0 && !S.lines))
         return fail(MTB_INVALID_ARG, "adjoint: %d line samples (at most %d)", S.n_lines, AMAXL);
     if (S.pol == MTB_TE && (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y ||

@@ -2055,6 +2055,12 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_tile_te(
 
 }  // namespace mtb
 
+#include "yee2d_te3.cuh"
+
+namespace mtb {
+
+}  // namespace mtb
+
 #include "yee2d_tb.cuh"
 #include "yee2d_cl.cuh"
 
@@ -2070,6 +2076,7 @@ struct mtb_yee2d_plan {
     int rows = 32;
     int variant = 2;                   // 1 row march, 2 tiles
     bool mpoles = false;               // a structure has magnetic Lorentz poles
+    int n_work_te3 = 0;                // the last work items: three-pass TE structures
     int wr = 1;                        // tiles: rows per warp
     bool ext = false;                  // a structure has conductivity or poles
     bool poles = false;                // a structure has poles (no graph replay)
@@ -2133,7 +2140,7 @@ static int tmap_2d(CUtensorMap *m, const float *base, int nx, int pitch, int bc,
 static bool tb_eligible(const mtb_yee2d_struct &S) {
     return !S.cond_d1[0] && !S.cond_d1[1] && !S.n_poles && !S.n_poles_y && !S.mag_h1[0] &&
            !S.mag_h1[1] && !S.mag_h2[0] && !S.mag_h2[1] && !S.y_pmc && !S.cut_y && !S.cut_x &&
-           !S.chi2 && !S.n_mpoles;
+           !S.chi2 && !S.n_mpoles && !S.te3;
 }
 
 // Copy n floats of a device array to the host.
@@ -2430,6 +2437,27 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         if (S.pol == MTB_TE && S.y_pmc)
             return fail(MTB_UNSUPPORTED, "structure %d: y_pmc is a TM option", s);
         int rc;
+        if (S.te3) {
+            if (S.pol != MTB_TE || S.te3 != 1)
+                return fail(MTB_INVALID_ARG, "structure %d: te3 is a TE flag (0 or 1)", s);
+            if (variant != 2)
+                return fail(MTB_UNSUPPORTED, "structure %d: tensor eps / oriented poles need "
+                            "the tile kernels (variant 2)", s);
+            if (S.cut_y || S.cut_x)
+                return fail(MTB_UNSUPPORTED, "structure %d: tensor eps / oriented poles with "
+                            "symmetry cuts", s);
+            if ((rc = check_ptr(S.e_x, "e_x", s)) || (rc = check_ptr(S.e_y, "e_y", s)))
+                return rc;
+            const bool t = S.tinv[0] || S.tinv[1] || S.tinv[2] || S.tinv[3];
+            for (int k = 0; t && k < 4; ++k)
+                if ((rc = check_ptr(S.tinv[k], "tinv", s))) return rc;
+            if ((S.c3xy && (!S.n_poles || (rc = check_ptr(S.c3xy, "c3xy", s)))) ||
+                (S.c3yx && (!S.n_poles_y || (rc = check_ptr(S.c3yx, "c3yx", s)))))
+                return rc ? rc : fail(MTB_INVALID_ARG, "structure %d: cross drives without "
+                                      "poles", s);
+        } else if (S.tinv[0] || S.c3xy || S.c3yx) {
+            return fail(MTB_INVALID_ARG, "structure %d: tensor arrays need te3 = 1", s);
+        }
         if (S.n_mpoles) {
             if (S.n_mpoles < 0 || S.n_mpoles > MTB_MAX_POLES)
                 return fail(MTB_INVALID_ARG, "structure %d: %d magnetic poles outside [0, %d]",
@@ -2608,7 +2636,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     {
         if (structs[s].cond_d1[0] || structs[s].n_poles > 0 || structs[s].n_poles_y > 0 ||
             structs[s].mag_h1[0] || structs[s].mag_h1[1] || structs[s].cut_y || structs[s].cut_x ||
-            structs[s].chi2 || structs[s].n_mpoles)
+            structs[s].chi2 || structs[s].n_mpoles || structs[s].te3)
             p->ext = true;
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0 || structs[s].n_mpoles > 0)
             p->poles = true;
@@ -2637,10 +2665,13 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
     if (rc) { p->dft.release(); delete p; return rc; }
     std::vector<int4> work;
     work.reserve(n_work);
-    for (int pol = 0; pol < 2; ++pol) {
+    size_t te3_start = 0;
+    for (int pol = 0; pol < 3; ++pol) {
         if (pol == 1) p->n_work_tm = (int)work.size();
+        if (pol == 2) te3_start = work.size();
         for (int s = 0; s < n; ++s) {
             if (structs[s].pol != (pol == 0 ? MTB_TM : MTB_TE)) continue;
+            if (pol > 0 && (structs[s].te3 != 0) != (pol == 2)) continue;
             for (int i0 = 0; i0 < structs[s].nx; i0 += rows)
                 for (int c0 = 0; c0 < structs[s].pitch; c0 += 128)
                     work.push_back(variant == 1
@@ -2648,6 +2679,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
                                        : make_int4(s, i0, c0, 0));
         }
     }
+    p->n_work_te3 = (int)(work.size() - te3_start);
     cudaError_t e = cudaMemcpy(p->structs_d.p, structs.data(), sizeof(mtb_yee2d_struct) * n,
                                cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
@@ -2707,13 +2739,25 @@ static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
             MTB_CHECK_LAUNCH();
             ++p->last_launches;
         }
-        if (n_te > 0) {
+        const int n_t3 = p->n_work_te3, n_te1 = n_te - n_t3;
+        if (n_te1 > 0) {
             if (p->ext)
-                k_tile_te<true><<<n_te, blk, 0, st>>>(SS, W + n_tm, n_te, C);
+                k_tile_te<true><<<n_te1, blk, 0, st>>>(SS, W + n_tm, n_te1, C);
             else
-                k_tile_te<false><<<n_te, blk, 0, st>>>(SS, W + n_tm, n_te, C);
+                k_tile_te<false><<<n_te1, blk, 0, st>>>(SS, W + n_tm, n_te1, C);
             MTB_CHECK_LAUNCH();
             ++p->last_launches;
+        }
+        if (n_t3 > 0) {
+            // tensor eps / oriented poles: D and poles, E, Hz as three launches
+            const int4 *W3 = W + n_tm + n_te1;
+            k_te3<0><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
+            MTB_CHECK_LAUNCH();
+            k_te3<1><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
+            MTB_CHECK_LAUNCH();
+            k_te3<2><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
+            MTB_CHECK_LAUNCH();
+            p->last_launches += 3;
         }
         return MTB_OK;
     }
@@ -3357,7 +3401,7 @@ extern "C" int mtb_yee2d_run_noalloc(const mtb_yee2d_struct *s, const mtb_dft_re
         return fail(MTB_INVALID_ARG, "noalloc: y_pmc / second magnetic source are TM options");
     if (S.cond_d1[0] || S.cond_d1[1] || S.cond_d2[0] || S.cond_d2[1] || S.n_poles ||
         S.n_poles_y || S.mag_h1[0] || S.mag_h1[1] || S.mag_h2[0] || S.mag_h2[1] || S.cut_y ||
-        S.cut_x || S.chi2 || S.n_mpoles)
+        S.cut_x || S.chi2 || S.n_mpoles || S.te3)
         return fail(MTB_UNSUPPORTED, "noalloc: conductivity, poles and symmetry cuts need the "
                     "tile kernels");
     int rc;

@@ -217,7 +217,10 @@ class Engine2D:
             for n_, cn in ((s.Px_cur.shape[0], "c1x"), (s.Py_cur.shape[0], "c1y")):
                 _need(n_ <= L.MTB_MAX_POLES, f"{n_} dispersive poles (at most {L.MTB_MAX_POLES})")
                 _need(getattr(c, cn).shape[0] == n_, f"pole coefficients {cn} count")
-            _opt_none(c, ["inv_xx_x", "c3xy", "c3yx", "has_chi2"])
+            _opt_none(c, ["has_chi2"])
+            # in-plane tensor eps / oriented poles: the three-pass TE kernels
+            it.te3 = (getattr(c, "inv_xx_x", None) is not None or
+                      getattr(c, "c3xy", None) is not None)
             it.mag = _magnetic_pairs(c, [("hz1", "hz2")])
         else:
             it.nx, it.ny = main.shape
@@ -384,6 +387,24 @@ class Engine2D:
                     pol_bufs["x" if ax == 0 else "y"] = pp
                     it.keep += pp + pc
                 pol_bufs = pol_bufs or None
+                if it.te3:
+                    # E is kept between steps (core/stepper_te.py:150-175)
+                    ebx, eby = self._pack(s.Ex, nx, P), self._pack(s.Ey, nx, P)
+                    S.te3, S.e_x, S.e_y = 1, L.ptr(ebx), L.ptr(eby)
+                    it.keep += [ebx, eby]
+                    if getattr(c, "inv_xx_x", None) is not None:
+                        tv = [self._pack(getattr(c, k), nx, P)
+                              for k in ("inv_xx_x", "inv_xy_x", "inv_yy_y", "inv_xy_y")]
+                        for k in range(4):
+                            S.tinv[k] = L.ptr(tv[k])
+                        it.keep += tv
+                    for name, attr in (("c3xy", "c3xy"), ("c3yx", "c3yx")):
+                        v = getattr(c, name, None)
+                        if v is not None:
+                            st_ = self._pack_stack(v, nx, P)
+                            setattr(S, attr, L.ptr(st_))
+                            it.keep.append(st_)
+                    it.te3_box = (ebx, eby)
             else:
                 f_main, f_x, f_y = self._pair(s.Dz, nx, P), self._pair(s.Hx, nx, P), \
                     self._pair(s.Hy, nx, P)
@@ -896,6 +917,7 @@ class Engine2D:
             Dx = self._unpack(bx["x"][cur], (nx - 1, ny))
             Dy = self._unpack(bx["y"][cur], (nx, ny - 1))
             pol = {}
+            te3 = getattr(it, "te3_box", None)
             if "pol_x" in bx:
                 n_p = s.Px_cur.shape[0]
                 ps_ = self.pole_slot
@@ -914,6 +936,9 @@ class Engine2D:
                 Ey = (Dy - pc.sum(0)) / it.coeffs.eps_y.to(Dy)
             else:
                 Ey = self._unpack(bx["y"][cur], (nx, ny - 1), den=bx["eps_b"])
+            if te3 is not None:                 # the stored E of the three-pass kernels
+                Ex = self._unpack(te3[0], (nx - 1, ny))
+                Ey = self._unpack(te3[1], (nx, ny - 1))
             ps = bx["psi"]
             return s._replace(
                 Hz=Hz, Ex=Ex, Ey=Ey, Dx=Dx, Dy=Dy, **pol,

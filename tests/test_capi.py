@@ -164,7 +164,7 @@ def test_unsupported_features_raise():
     g = Grid(nx=20, ny=20, dx=0.05, device="cpu")
     with pytest.raises(NotImplementedError):          # the reference refuses the pair too
         build_tm_coeffs(g, m_poles=[(1.0, 0.1, 1.0)], mu=2.0)
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(TypeError):                    # a TE option, as in the reference
         build_tm_coeffs(g, eps_tensor=torch.ones(3, 20, 20))
     m = build_tm_coeffs(g, chi3=torch.ones(20, 20))          # chi2 / chi3: built, flagged
     assert m.has_kerr and not m.has_chi2
@@ -293,3 +293,26 @@ def test_magnetic_pole_coefficients_and_state_match_oracle():
     s, so = init_tm_state(g, n_mpoles=2), O.tm_state(o)
     for k in ("Bx", "By", "Mx_cur", "Mx_prev", "My_cur", "My_prev"):
         assert tuple(getattr(s, k).shape) == so[k].shape, k
+
+
+def test_te_tensor_coefficients_match_oracle():
+    """eps_tensor: the inverse tensor Yee-averaged onto the E nodes; poles_tensor: the
+    oriented pole appended to each axis stack with its off-diagonal drives."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs
+    from meep_torch_b200.core.grid import Grid
+    rng = np.random.default_rng(9)
+    nx, ny = 26, 22
+    exx = rng.uniform(2, 6, (nx, ny)); eyy = rng.uniform(2, 6, (nx, ny))
+    exy = rng.uniform(-1, 1, (nx, ny))
+    pt = [(0.7, 0.1, (0.6, 0.3, 0.4))]
+    pm = [(rng.random((nx, ny)) < 0.5).astype(np.float64)]
+    g = Grid(nx=nx, ny=ny, dx=0.05, device="cpu")
+    T = lambda a: torch.tensor(a, dtype=torch.float32)  # noqa: E731
+    m = build_te_coeffs(g, npml=4, eps_tensor=(T(exx), T(exy), T(eyy)), poles=[(0.5, 0.05, 1.0)],
+                        poles_tensor=pt, pole_masks_tensor=[T(x) for x in pm])
+    o = O.te_coeffs(nx, ny, 0.05, npml=4, eps_tensor=(exx, exy, eyy), poles=[(0.5, 0.05, 1.0)],
+                    poles_tensor=pt, pole_masks_tensor=pm, dtype=np.float32)
+    for k in ("inv_xx_x", "inv_xy_x", "inv_yy_y", "inv_xy_y", "c1x", "c2x", "c3x", "c1y",
+              "c2y", "c3y", "c3xy", "c3yx"):
+        np.testing.assert_allclose(getattr(m, k).numpy(), o[k], rtol=2e-5, atol=1e-7,
+                                   err_msg=k)

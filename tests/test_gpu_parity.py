@@ -163,7 +163,8 @@ def test_tm_reference_phase_mode():
         assert rel_l2(a.cpu().numpy(), g[key]) < TOL, key
 
 
-@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic"])
+@pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic", "te_tensor",
+                                  "te_tensor_poles"])
 def test_te_matches_reference(case):
     from meep_torch_b200.core.coeffs import build_te_coeffs
     from meep_torch_b200.core.grid import Grid
@@ -178,6 +179,15 @@ def test_te_matches_reference(case):
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
     mag = {k: torch.tensor(g[k], dtype=torch.float32) for k in ("sigma_b", "mu") if k in g}
+    # in-plane tensor eps and oriented poles: the three-pass TE kernels
+    if "eps_tensor" in g:
+        mag["eps_tensor"] = tuple(torch.tensor(v, dtype=torch.float32) for v in g["eps_tensor"])
+    n_pt = 0
+    if "poles_tensor" in g:
+        pt = [(p[0], p[1], tuple(p[2]), *p[3:]) for p in json.loads(str(g["poles_tensor"]))]
+        mag.update(poles_tensor=pt, pole_masks_tensor=[torch.tensor(x, dtype=torch.float32)
+                                                       for x in g["pole_masks_tensor"]])
+        n_pt = len(pt)
     m = build_te_coeffs(grid, eps_inf=torch.tensor(g["eps"], dtype=torch.float32),
                         npml=int(g["npml"]), poles=poles, pole_masks=pm,
                         sigma_d=None if sig is None else torch.tensor(sig, dtype=torch.float32),
@@ -191,7 +201,7 @@ def test_te_matches_reference(case):
     monx = FluxMonitorTE(grid, freqs, ix=ix, lo=xlo, hi=xhi)
     mony = FluxMonitorTEY(grid, freqs, iy=iy, lo=ylo, hi=yhi)
     dft = DFTFieldsMonitor(grid, freqs, "Hz")
-    st, accs = run_te(init_te_state(grid, n_poles=len(poles)), m, int(g["n_steps"]),
+    st, accs = run_te(init_te_state(grid, n_poles=len(poles) + n_pt), m, int(g["n_steps"]),
                       source=src, monitors=[monx, mony, dft])
     fx, fy = monx.flux(accs[0], dx), mony.flux(accs[1], dx)
     e32, e64 = {}, {}
