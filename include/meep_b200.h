@@ -239,6 +239,14 @@ typedef struct mtb_yee2d_struct {
     const float *tinv[4];
     float *e_x, *e_y;
     const float *c3xy, *c3yx;
+    /* TE instantaneous chi2 / chi3 on the three-pass kernels (te3 = 1; core/coeffs.py:
+     * 380-387, core/stepper_te.py:160-174): nlx = chi2, chi3, eps at the Ex nodes, nly
+     * the same at the Ey nodes (box layout; all null = linear). E starts at rhs / eps and
+     * takes three Jacobi sweeps E = rhs / (eps + chi2 E + chi3 (E^2 + avg4(E_other)^2)),
+     * through the scratch boxes e_t (Ex, Ey). Not with the tensor eps. */
+    const float *nlx[3];
+    const float *nly[3];
+    float *e_t[2];
 } mtb_yee2d_struct;
 
 #define MTB_MAX_POLES 8

@@ -58,7 +58,8 @@ class Yee2DStruct(C.Structure):
                 ("n_mpoles", C.c_int32), ("pad4_", C.c_int32 * 3), ("f_b", (vp * 2) * 2),
                 ("mpol", (vp * 3) * 2), ("mpc", (vp * 3) * 2),
                 ("te3", C.c_int32), ("pad5_", C.c_int32 * 3), ("tinv", vp * 4),
-                ("e_x", vp), ("e_y", vp), ("c3xy", vp), ("c3yx", vp)]
+                ("e_x", vp), ("e_y", vp), ("c3xy", vp), ("c3yx", vp),
+                ("nlx", vp * 3), ("nly", vp * 3), ("e_t", vp * 2)]
 
 
 class PhaseGroup(C.Structure):

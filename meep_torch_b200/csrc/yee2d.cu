@@ -2077,6 +2077,7 @@ struct mtb_yee2d_plan {
     int variant = 2;                   // 1 row march, 2 tiles
     bool mpoles = false;               // a structure has magnetic Lorentz poles
     int n_work_te3 = 0;                // the last work items: three-pass TE structures
+    bool te_nl = false;                // a three-pass TE structure has chi2 / chi3
     int wr = 1;                        // tiles: rows per warp
     bool ext = false;                  // a structure has conductivity or poles
     bool poles = false;                // a structure has poles (no graph replay)
@@ -2451,11 +2452,21 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
             const bool t = S.tinv[0] || S.tinv[1] || S.tinv[2] || S.tinv[3];
             for (int k = 0; t && k < 4; ++k)
                 if ((rc = check_ptr(S.tinv[k], "tinv", s))) return rc;
+            const bool nlt = S.nlx[0] || S.nlx[1] || S.nlx[2] || S.nly[0] || S.nly[1] ||
+                             S.nly[2];
+            if (nlt && t)
+                return fail(MTB_UNSUPPORTED, "structure %d: TE chi2 / chi3 with the tensor eps",
+                            s);
+            for (int k = 0; nlt && k < 3; ++k)
+                if ((rc = check_ptr(S.nlx[k], "nlx", s)) || (rc = check_ptr(S.nly[k], "nly", s)))
+                    return rc;
+            for (int k = 0; nlt && k < 2; ++k)
+                if ((rc = check_ptr(S.e_t[k], "e_t", s))) return rc;
             if ((S.c3xy && (!S.n_poles || (rc = check_ptr(S.c3xy, "c3xy", s)))) ||
                 (S.c3yx && (!S.n_poles_y || (rc = check_ptr(S.c3yx, "c3yx", s)))))
                 return rc ? rc : fail(MTB_INVALID_ARG, "structure %d: cross drives without "
                                       "poles", s);
-        } else if (S.tinv[0] || S.c3xy || S.c3yx) {
+        } else if (S.tinv[0] || S.c3xy || S.c3yx || S.nlx[0] || S.nly[0]) {
             return fail(MTB_INVALID_ARG, "structure %d: tensor arrays need te3 = 1", s);
         }
         if (S.n_mpoles) {
@@ -2641,6 +2652,7 @@ int mtb_yee2d_plan_create(const mtb_yee2d_struct *structs_in, int32_t n,
         if (structs[s].n_poles > 0 || structs[s].n_poles_y > 0 || structs[s].n_mpoles > 0)
             p->poles = true;
         if (structs[s].n_mpoles > 0) p->mpoles = true;
+        if (structs[s].te3 && structs[s].nlx[0]) p->te_nl = true;
     }
     for (int s = 0; s < n; ++s) want_tb = want_tb && tb_eligible(structs[s]);
     for (int s = 0; s < n; ++s)
@@ -2755,6 +2767,15 @@ static int launch_step(mtb_yee2d_plan *p, const Ctx2D &C, cudaStream_t st) {
             MTB_CHECK_LAUNCH();
             k_te3<1><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
             MTB_CHECK_LAUNCH();
+            if (p->te_nl) {                    // chi2 / chi3: three Jacobi sweeps
+                k_te3<3><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
+                MTB_CHECK_LAUNCH();
+                k_te3<4><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
+                MTB_CHECK_LAUNCH();
+                k_te3<5><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
+                MTB_CHECK_LAUNCH();
+                p->last_launches += 3;
+            }
             k_te3<2><<<n_t3, blk, 0, st>>>(SS, W3, n_t3, C);
             MTB_CHECK_LAUNCH();
             p->last_launches += 3;

@@ -4,7 +4,7 @@
 // 136-175). The one-pass TE tile recomputes E where it needs it; here E has to
 // come from a two-node-wide neighbourhood of D, so E is kept in two box arrays
 // (e_x, e_y: the state's own Ex, Ey) and the step runs as three launches over
-// the same work items:
+// the same work items (k_te3<PASS>):
 //   k_te3_d  Dx, Dy(n+1/2) from Hz(n) with their CPML memory, conductivity and
 //            the soft current on Dy; the ADE poles P(n+1/2) = c1 P(n-1/2) +
 //            c2 P(n-3/2) + c3 E(n-1/2) (+ c3xy * avg4(Ey(n-1/2)) on Px, c3yx *
@@ -14,6 +14,8 @@
 //            samples of Ex, Ey;
 //   k_te3_h  Hz(n+1) from the stored E(n+1/2) with its CPML memory, magnetic
 //            pairs and source, the samples of Hz.
+// With chi2 / chi3 (core/stepper_te.py:160-171) pass 2 leaves the first iterate rhs / eps
+// in the scratch boxes and three Jacobi sweeps (passes 3-5, before the Hz pass) end in E.
 // avg4 is the reference's four-node Yee average with zero padding at the walls
 // (core/stepper_te.py:52-61). Padding cells of every box stay zero.
 #pragma once
@@ -194,7 +196,22 @@ __device__ __forceinline__ void te3_d_row(const mtb_yee2d_struct &S, const int i
     if (bxE) st4(S.psi[1][pn] + ro, p1);
 }
 
-// Pass 2: E(n+1/2) from D(n+1/2) and P(n+1/2), and the E samples.
+// Samples of E(n+1/2) (full-grid ring copies and line samples).
+__device__ __forceinline__ void te3_sample_e(const mtb_yee2d_struct &S, int i, int jb,
+                                             uint32_t ro, const Ctx2D &C,
+                                             const mtb_line_sample *L, int nl,
+                                             const float (&ex)[4], const float (&ey)[4]) {
+    float *ring = C.ring;
+    if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, ex);
+    if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, ey);
+    if (nl) {
+        sample_row(L, nl, MTB_C2_X, i, jb, true, ex, ring);
+        sample_row(L, nl, MTB_C2_Y, i, jb, true, ey, ring);
+    }
+}
+
+// Pass 2: E(n+1/2) from D(n+1/2) and P(n+1/2), and the E samples (with chi2 / chi3 the
+// first iterate rhs / eps, into the scratch boxes; the sweeps sample the last one).
 __device__ __forceinline__ void te3_e_row(const mtb_yee2d_struct &S, const int i, const int c0,
                                           const Ctx2D &C, const mtb_line_sample *L,
                                           const int nl) {
@@ -241,6 +258,15 @@ __device__ __forceinline__ void te3_e_row(const mtb_yee2d_struct &S, const int i
         te3_avg_ey(rxp, pr, rx, cr, ay);
 #pragma unroll
         for (int q = 0; q < 4; ++q) ey[q] = t2[q] * ry[q] + t3[q] * ay[q];
+    } else if (S.nlx[0]) {
+        float epx[4], epy[4];                           // chi: rhs / eps, divided
+        ld4(S.nlx[2] + ro, epx);
+        ld4(S.nly[2] + ro, epy);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ex[q] = __fdiv_rn(rx[q], epx[q]);
+            ey[q] = __fdiv_rn(ry[q], epy[q]);
+        }
     } else {
         float ix[4], iy[4];
         ld4(S.inv_eps_a + ro, ix);
@@ -257,15 +283,76 @@ __device__ __forceinline__ void te3_e_row(const mtb_yee2d_struct &S, const int i
         if (!(i <= nx - 2 && j <= ny - 1)) ex[q] = 0.f;
         if (!(j <= ny - 2)) ey[q] = 0.f;
     }
+    if (S.nlx[0]) {                                    // the sweeps go on from here
+        st4(S.e_t[0] + ro, ex);
+        st4(S.e_t[1] + ro, ey);
+        return;
+    }
     st4(S.e_x + ro, ex);
     st4(S.e_y + ro, ey);
-    float *ring = C.ring;
-    if (S.ring_full[1] >= 0) st4(ring + S.ring_full[1] + ro, ex);
-    if (S.ring_full[2] >= 0) st4(ring + S.ring_full[2] + ro, ey);
-    if (nl) {
-        sample_row(L, nl, MTB_C2_X, i, jb, true, ex, ring);
-        sample_row(L, nl, MTB_C2_Y, i, jb, true, ey, ring);
+    te3_sample_e(S, i, jb, ro, C, L, nl, ex, ey);
+}
+
+// One Jacobi sweep of the chi2 / chi3 fixed point (core/stepper_te.py:166-171): from the
+// iterate in (ix_, iy_) to (ox, oy); E2 = E^2 + avg4(E_other)^2 of the input iterate.
+// `last` samples the result.
+__device__ __forceinline__ void te3_sweep_row(const mtb_yee2d_struct &S, const int i,
+                                              const int c0, const Ctx2D &C,
+                                              const mtb_line_sample *L, const int nl,
+                                              const float *ix_, const float *iy_, float *ox,
+                                              float *oy, bool last) {
+    const int lane = threadIdx.x;
+    const int nx = S.nx, ny = S.ny, P = S.pitch;
+    const int jb = c0 + 4 * lane;
+    if (jb >= P) return;
+    const int pn = C.par ^ 1;
+    const uint32_t ro = (uint32_t)i * P + jb, pl = (uint32_t)nx * P;
+    const int slot = (C.pst + 1) % 3;
+    const bool hasr = jb + 4 < P;
+    float ex[4], ey[4], rx[4], ry[4], ax[4], ay[4];
+    ld4(ix_ + ro, ex);
+    ld4(iy_ + ro, ey);
+    zero4(rx);
+    if (i <= nx - 2) te3_rhs4(S.f_x[pn], S.pol_p[slot], S.n_poles, pl, ro, rx);
+    te3_rhs4(S.f_y[pn], S.pol_py[slot], S.n_poles_y, pl, ro, ry);
+    {
+        float a1[4], l0 = jb >= 1 ? iy_[ro - 1] : 0.f, l1 = 0.f;
+        zero4(a1);
+        if (i + 1 < nx) {
+            ld4(iy_ + ro + P, a1);
+            if (jb >= 1) l1 = iy_[ro + P - 1];
+        }
+        te3_avg_ex(ey, l0, a1, l1, jb, ny, ax);
     }
+    {
+        float p[4], pr = 0.f, cr = 0.f;
+        zero4(p);
+        if (i >= 1 && i - 1 <= nx - 2) {
+            ld4(ix_ + ro - P, p);
+            if (hasr) pr = ix_[ro - P + 4];
+        }
+        if (i <= nx - 2 && hasr) cr = ix_[ro + 4];
+        te3_avg_ey(p, pr, ex, cr, ay);
+    }
+    float x2[4], x3[4], xe[4], y2[4], y3[4], ye[4];
+    ld4(S.nlx[0] + ro, x2); ld4(S.nlx[1] + ro, x3); ld4(S.nlx[2] + ro, xe);
+    ld4(S.nly[0] + ro, y2); ld4(S.nly[1] + ro, y3); ld4(S.nly[2] + ro, ye);
+    float nxv[4], nyv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        const float e2x = __fadd_rn(__fmul_rn(ex[q], ex[q]), __fmul_rn(ax[q], ax[q]));
+        const float e2y = __fadd_rn(__fmul_rn(ey[q], ey[q]), __fmul_rn(ay[q], ay[q]));
+        const float vx = __fdiv_rn(rx[q], __fadd_rn(__fadd_rn(xe[q], __fmul_rn(x2[q], ex[q])),
+                                                    __fmul_rn(x3[q], e2x)));
+        const float vy = __fdiv_rn(ry[q], __fadd_rn(__fadd_rn(ye[q], __fmul_rn(y2[q], ey[q])),
+                                                    __fmul_rn(y3[q], e2y)));
+        nxv[q] = (i <= nx - 2 && j <= ny - 1) ? vx : 0.f;  // padding cells stay zero
+        nyv[q] = (j <= ny - 2) ? vy : 0.f;
+    }
+    st4(ox + ro, nxv);
+    st4(oy + ro, nyv);
+    if (last) te3_sample_e(S, i, jb, ro, C, L, nl, nxv, nyv);
 }
 
 // Pass 3: Hz(n+1) from the stored E(n+1/2) (core/stepper_te.py:103-117), its samples.
@@ -348,7 +435,14 @@ __global__ void __launch_bounds__(32 * TROWS, 2) k_te3(const mtb_yee2d_struct *_
         if (i >= S.nx) break;
         if (PASS == 0) te3_d_row(S, i, w.z, C);
         else if (PASS == 1) te3_e_row(S, i, w.z, C, T.lines, T.nl);
-        else te3_h_row(S, i, w.z, C, T.lines, T.nl);
+        else if (PASS == 2) te3_h_row(S, i, w.z, C, T.lines, T.nl);
+        // chi sweeps 1, 2, 3: scratch -> E -> scratch -> E
+        else if (PASS == 3) te3_sweep_row(S, i, w.z, C, T.lines, T.nl, S.e_t[0], S.e_t[1],
+                                          S.e_x, S.e_y, false);
+        else if (PASS == 4) te3_sweep_row(S, i, w.z, C, T.lines, T.nl, S.e_x, S.e_y,
+                                          S.e_t[0], S.e_t[1], false);
+        else te3_sweep_row(S, i, w.z, C, T.lines, T.nl, S.e_t[0], S.e_t[1], S.e_x, S.e_y,
+                           true);
     }
 }
 

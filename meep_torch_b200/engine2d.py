@@ -217,7 +217,6 @@ class Engine2D:
             for n_, cn in ((s.Px_cur.shape[0], "c1x"), (s.Py_cur.shape[0], "c1y")):
                 _need(n_ <= L.MTB_MAX_POLES, f"{n_} dispersive poles (at most {L.MTB_MAX_POLES})")
                 _need(getattr(c, cn).shape[0] == n_, f"pole coefficients {cn} count")
-            _opt_none(c, ["has_chi2"])
             # in-plane tensor eps / oriented poles: the three-pass TE kernels
             it.te3 = (getattr(c, "inv_xx_x", None) is not None or
                       getattr(c, "c3xy", None) is not None)
@@ -245,7 +244,10 @@ class Engine2D:
                 _need(h0 is None or tuple(h0.shape) == (n,), f"TMState.{name} shape")
         # instantaneous chi2 / chi3: TM on the tile kernels (core/stepper_tm.py:222-230)
         it.nl = bool(getattr(c, "has_kerr", False) or getattr(c, "has_chi2", False))
-        _need(not (it.nl and it.te), "TE chi2 / chi3 media")
+        if it.nl and it.te:
+            # TE chi2 / chi3: Jacobi sweeps on the three-pass kernels (scalar eps only)
+            _need(getattr(c, "inv_xx_x", None) is None, "TE chi2 / chi3 with the tensor eps")
+            it.te3 = True
         for k in ("k_hx", "k_hy", "k_ex", "k_ey"):
             kv = getattr(c, k)
             _need(bool(torch.all(kv == 1)), f"CPML kappa != 1 ({k})")
@@ -405,6 +407,18 @@ class Engine2D:
                             setattr(S, attr, L.ptr(st_))
                             it.keep.append(st_)
                     it.te3_box = (ebx, eby)
+                    if it.nl:
+                        z2 = torch.zeros_like(c.eps_x)
+                        nlb = [self._pack(v, nx, P) for v in
+                               (c.chi2_x if c.chi2_x is not None else z2, c.chi3_x, c.eps_x,
+                                c.chi2_y if c.chi2_y is not None else torch.zeros_like(c.eps_y),
+                                c.chi3_y, c.eps_y)]
+                        et = [torch.zeros((nx, P), dtype=torch.float32, device=dev)
+                              for _ in range(2)]
+                        for k in range(3):
+                            S.nlx[k], S.nly[k] = L.ptr(nlb[k]), L.ptr(nlb[3 + k])
+                        S.e_t[0], S.e_t[1] = L.ptr(et[0]), L.ptr(et[1])
+                        it.keep += nlb + et
             else:
                 f_main, f_x, f_y = self._pair(s.Dz, nx, P), self._pair(s.Hx, nx, P), \
                     self._pair(s.Hy, nx, P)
@@ -495,7 +509,7 @@ class Engine2D:
                     it.keep += fb[c_] + mm + mc
                 it.box["B"], it.box["M"] = fb, mstk
                 it.plain = False
-            if it.nl:
+            if it.nl and not te:
                 x2 = self._pack(c.chi2 if c.chi2 is not None else torch.zeros_like(c.eps_inf),
                                 nx, P)
                 x3 = self._pack(c.chi3, nx, P)

@@ -164,7 +164,7 @@ def test_tm_reference_phase_mode():
 
 
 @pytest.mark.parametrize("case", ["te", "te_sigma", "te_poles", "te_magnetic", "te_tensor",
-                                  "te_tensor_poles"])
+                                  "te_tensor_poles", "te_nonlinear"])
 def test_te_matches_reference(case):
     from meep_torch_b200.core.coeffs import build_te_coeffs
     from meep_torch_b200.core.grid import Grid
@@ -178,8 +178,9 @@ def test_te_matches_reference(case):
     sig = g.get("sigma")
     poles = json.loads(str(g["poles"])) if "poles" in g else ()
     pm = [torch.tensor(x, dtype=torch.float32) for x in g["pole_masks"]] if poles else None
-    mag = {k: torch.tensor(g[k], dtype=torch.float32) for k in ("sigma_b", "mu") if k in g}
-    # in-plane tensor eps and oriented poles: the three-pass TE kernels
+    mag = {k: torch.tensor(g[k], dtype=torch.float32)
+           for k in ("sigma_b", "mu", "chi2", "chi3") if k in g}
+    # in-plane tensor eps, oriented poles, chi2 / chi3: the three-pass TE kernels
     if "eps_tensor" in g:
         mag["eps_tensor"] = tuple(torch.tensor(v, dtype=torch.float32) for v in g["eps_tensor"])
     n_pt = 0
