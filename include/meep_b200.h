@@ -406,8 +406,8 @@ int mtb_yee2d_ring_gather(const mtb_yee2d_plan *plan, const int64_t *offsets, in
 /* ---------------------------------------------------------- 2D adjoint */
 /* Discrete adjoint (reverse mode) of the TM and TE steps, the transpose of
  * core/stepper_tm.py:234-254 / core/stepper_te.py:178-190 with CPML and PEC
- * walls (TM also with electric conductivity, magnetic conductivity and
- * permeability, and dispersive ADE poles; TE without them) and of the DFT / flux
+ * walls, electric conductivity, magnetic conductivity and permeability, and
+ * dispersive ADE poles (TM and TE) and of the DFT / flux
  * sampling
  * (core/monitors.py:24-155): what torch autograd computes through the
  * reference's run_tm / run_te (core/run.py:43-126).
@@ -425,9 +425,11 @@ typedef struct mtb_adj2d_buffers {
     float *g_psi[4];
     float *tmp[4];
     float *g_eps[2];
-    /* TM with dispersive poles: d J / d P(n) (g_pol[0]) and d J / d P(n-1)
-     * (g_pol[1]), n_poles planes of nx x pitch floats each; null otherwise */
+    /* With dispersive poles: d J / d P(n) (g_pol[0]) and d J / d P(n-1)
+     * (g_pol[1]), n_poles planes of nx x pitch floats each (TM P on Ez, TE Px on
+     * Ex); g_pol_y the same for TE's Py stack (n_poles_y planes); null otherwise */
     float *g_pol[2];
+    float *g_pol_y[2];
 } mtb_adj2d_buffers;
 
 typedef struct mtb_yee2d_adjoint mtb_yee2d_adjoint;

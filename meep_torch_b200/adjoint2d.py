@@ -85,10 +85,14 @@ class GradRun2D:
         g, gpsi, tmp = [box() for _ in range(nfld)], [box() for _ in range(4)], \
             [box() for _ in range(4)]
         geps = [box() for _ in range(2 if self.te else 1)]
-        # TM poles: d J / d P(n), d J / d P(n-1) (zero at the end: P is not an output)
-        n_p = 0 if self.te else int(eng.structs[0].n_poles)
+        # poles: d J / d P(n), d J / d P(n-1) (zero at the end: P is not an output); TE
+        # has a second set for its Ey stack
+        n_p = int(eng.structs[0].n_poles)
+        n_py = int(eng.structs[0].n_poles_y) if self.te else 0
         gpol = [torch.zeros((n_p * nx, P), dtype=torch.float32, device=dev) for _ in range(2)] \
             if n_p else []
+        gpol_y = [torch.zeros((n_py * nx, P), dtype=torch.float32, device=dev)
+                  for _ in range(2)] if n_py else []
         targets = g + gpsi
         if self.te:
             offs = [(0, 0)] * 5 + [(0, 1), (1, 0), (0, 0), (0, 0)]
@@ -122,12 +126,14 @@ class GradRun2D:
             bufs.g_eps[q] = L.ptr(geps[q])
         for q in range(len(gpol)):
             bufs.g_pol[q] = L.ptr(gpol[q])
+        for q in range(len(gpol_y)):
+            bufs.g_pol_y[q] = L.ptr(gpol_y[q])
         adj = C.c_void_p()
         L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
                                              regs if nreg else None, nreg, eng.groups,
                                              eng.n_groups, eng.ring_elems, self.sub,
                                              C.byref(adj)), "mtb_yee2d_adjoint_create")
-        keep = [gaccs, g, gpsi, tmp, geps, gpol]
+        keep = [gaccs, g, gpsi, tmp, geps, gpol, gpol_y]
         stream = eng._sptr()
         try:
             rec_mons = _record_monitors(float(self.coeffs.dt), dev, self.te)

@@ -5,7 +5,8 @@
 // conductivity / permeability (H' = h1 H -/+ h2 curl) and dispersive ADE poles,
 // and of the monitors' sampling (core/monitors.py:24-100). This is what torch
 // autograd computes through the reference's run_tm (core/run.py:43-120); the
-// source terms are additive constants and have no adjoint. (TE: CPML only.)
+// source terms are additive constants and have no adjoint. TE takes the same
+// conductivity, magnetic pairs and poles (Px on Ex, Py on Ey).
 //
 // Reverse of forward step t (state_t -> state_{t+1}), adjoint state A holding
 // dJ/d state_{t+1} on entry and dJ/d state_t on exit, three kernels:
@@ -297,18 +298,22 @@ __device__ __forceinline__ void adj_te_h_cell(const mtb_yee2d_struct &S, const m
     const bool vrow = i <= nx - 2;
     float hxb = 1.f, hxa = 0.f;
     if (vrow) { hxb = S.hx_b[i]; hxa = S.hx_a[i]; }
+    // magnetic conductivity / permeability: Hz' = hz1 Hz - hz2 curl (core/stepper_te.py:112-114)
+    float h1[4] = {1.f, 1.f, 1.f, 1.f}, h2[4] = {dt, dt, dt, dt};
+    if (S.mag_h1[0]) { ldv(S.mag_h1[0] + g, h1); ldv(S.mag_h2[0] + g, h2); }
     float u0[4], u1[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
         const bool v = vrow && j <= ny - 2;
         const float hyb = v ? S.hy_b[j] : 1.f, hya = v ? S.hy_a[j] : 0.f;
-        const float c2 = -dt * ghz[q], c3 = dt * ghz[q];
+        const float c2 = -h2[q] * ghz[q], c3 = h2[q] * ghz[q];
         const float g2 = gp2[q] + c2, g3 = gp3[q] + c3;
         u0[q] = v ? c2 + hxa * g2 : 0.f;                  // dEy/dx
         u1[q] = v ? c3 + hya * g3 : 0.f;                  // dEx/dy
         gp2[q] = v ? hxb * g2 : gp2[q];
         gp3[q] = v ? hyb * g3 : gp3[q];
+        ghz[q] = v ? h1[q] * ghz[q] : ghz[q];
     }
     stv(B.g[0] + g, ghz);
     stv(B.g_psi[2] + g, gp2);
@@ -360,34 +365,74 @@ __device__ __forceinline__ void adj_te_e_cell(const mtb_yee2d_struct &S, const m
     const bool xrow = i <= nx - 2, yrow = i >= 1 && i <= nx - 2;
     float exb = 1.f, exa = 0.f;
     if (yrow) { exb = S.ex_b[i]; exa = S.ex_a[i]; }
+    // electric conductivity: Dx' = d1x Dx + d2x curl, Dy' = d1y Dy - d2y curl
+    float dx1[4] = {1.f, 1.f, 1.f, 1.f}, dx2[4] = {dt, dt, dt, dt};
+    float dy1[4] = {1.f, 1.f, 1.f, 1.f}, dy2[4] = {dt, dt, dt, dt};
+    if (S.cond_d1[0]) {
+        ldv(S.cond_d1[0] + g, dx1); ldv(S.cond_d2[0] + g, dx2);
+        ldv(S.cond_d1[1] + g, dy1); ldv(S.cond_d2[1] + g, dy2);
+    }
+    float gX[4], gY[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        // Hz used dEx/dy = (Ex(j+1) - Ex(j)) and dEy/dx = (Ey(i+1) - Ey(i))
+        const float u1m = (q == 0) ? u1l : u1[q - 1];
+        gX[q] = xrow ? gex[q] + (u1m - u1[q]) * rdx : 0.f;   // Ex on rows <= nx-2 only
+        gY[q] = gey[q] + (u0p[q] - u0[q]) * rdx;
+    }
+    // poles, E = (D - sum P(n+1)) / eps with P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n)
+    // (core/stepper_te.py:136-175): gPn = gA - gE / eps, then gA = c1 gPn + gB,
+    // gB = c2 gPn, and d J / d E(n) = sum_k c3 gPn (the next reverse step's gE)
+    float pex[4] = {0.f, 0.f, 0.f, 0.f}, pey[4] = {0.f, 0.f, 0.f, 0.f};
+    const uint32_t pl = (uint32_t)nx * P;
+    for (int a = 0; a < 2; ++a) {
+        const int np = a ? S.n_poles_y : S.n_poles;
+        float *ga_ = a ? B.g_pol_y[0] : B.g_pol[0], *gb_ = a ? B.g_pol_y[1] : B.g_pol[1];
+        const float *const *pc = a ? S.pol_cy : S.pol_c;
+        const float(&gE)[4] = a ? gY : gX;
+        const float(&ie)[4] = a ? iy : ix;
+        float(&acc)[4] = a ? pey : pex;
+        for (int k = 0; k < np; ++k) {
+            const uint32_t o = k * pl + g;
+            float ga[4], gb[4], c1[4], c2[4], c3[4];
+            ldv(ga_ + o, ga); ldv(gb_ + o, gb);
+            ldv(pc[0] + o, c1); ldv(pc[1] + o, c2); ldv(pc[2] + o, c3);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float gpn = ga[q] - gE[q] * ie[q];
+                ga[q] = c1[q] * gpn + gb[q];
+                gb[q] = c2[q] * gpn;
+                acc[q] += c3[q] * gpn;
+            }
+            stv(ga_ + o, ga);
+            stv(gb_ + o, gb);
+        }
+    }
     float t2[4], t3[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
-        // Hz used dEx/dy = (Ex(j+1) - Ex(j)) and dEy/dx = (Ey(i+1) - Ey(i))
-        const float u1m = (q == 0) ? u1l : u1[q - 1];
-        const float gX = gex[q] + (u1m - u1[q]) * rdx;
-        const float gY = gey[q] + (u0p[q] - u0[q]) * rdx;
-        // E = D / eps (Ex on rows <= nx-2 only)
-        const float gdX = gdx[q] + (xrow ? gX * ix[q] : 0.f);
-        const float gdY = gdy[q] + gY * iy[q];
-        gex_e[q] -= xrow ? gX * ex[q] * ix[q] : 0.f;
-        gey_e[q] -= gY * ey[q] * iy[q];
-        // Dx += dt (d + psi0'): valid i <= nx-2, 1 <= j <= ny-2
+        // E = (D - sum P) / eps (Ex on rows <= nx-2 only)
+        const float gdX = gdx[q] + (xrow ? gX[q] * ix[q] : 0.f);
+        const float gdY = gdy[q] + gY[q] * iy[q];
+        gex_e[q] -= xrow ? gX[q] * ex[q] * ix[q] : 0.f;
+        gey_e[q] -= gY[q] * ey[q] * iy[q];
+        // Dx' = d1x Dx + d2x (d + psi0'): the curl on i <= nx-2, 1 <= j <= ny-2
         const bool vx = xrow && j >= 1 && j <= ny - 2;
         const float eyb = vx ? S.ey_b[j] : 1.f, eya = vx ? S.ey_a[j] : 0.f;
-        const float c0 = dt * gdX, g0 = gp0[q] + c0;
+        const float c0 = dx2[q] * gdX, g0 = gp0[q] + c0;
         t2[q] = vx ? c0 + eya * g0 : 0.f;
         gp0[q] = vx ? eyb * g0 : gp0[q];
-        // Dy -= dt (d + psi1'): valid 1 <= i <= nx-2, j <= ny-2
+        // Dy' = d1y Dy - d2y (d + psi1'): the curl on 1 <= i <= nx-2, j <= ny-2
         const bool vy = yrow && j <= ny - 2;
-        const float c1 = -dt * gdY, g1 = gp1[q] + c1;
+        const float c1 = -dy2[q] * gdY, g1 = gp1[q] + c1;
         t3[q] = vy ? c1 + exa * g1 : 0.f;
         gp1[q] = vy ? exb * g1 : gp1[q];
-        gdx[q] = gdX;
-        gdy[q] = gdY;
-        gex[q] = 0.f;
-        gey[q] = 0.f;
+        gdx[q] = dx1[q] * gdX;
+        gdy[q] = dy1[q] * gdY;
+        // E(n) reaches J only through the poles' recursion
+        gex[q] = xrow && j < ny ? pex[q] : 0.f;
+        gey[q] = j <= ny - 2 ? pey[q] : 0.f;
     }
     stv(B.g[1] + g, gex);
     stv(B.g[2] + g, gey);
@@ -554,13 +599,16 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     if (S.te3) return fail(MTB_UNSUPPORTED, "adjoint: TE tensor eps / oriented poles");
     if (S.n_lines < 0 || S.n_lines > AMAXL || (S.n_lines > 0 && !S.lines))
         return fail(MTB_INVALID_ARG, "adjoint: %d line samples (at most %d)", S.n_lines, AMAXL);
-    if (S.pol == MTB_TE && (S.cond_d1[0] || S.cond_d1[1] || S.n_poles || S.n_poles_y ||
-                            S.mag_h1[0] || S.mag_h1[1]))
-        return fail(MTB_UNSUPPORTED, "adjoint: TE conductivity, poles and magnetic pairs are "
-                    "forward-only");
     if ((S.cond_d1[0] && !S.cond_d2[0]) || (S.mag_h1[0] && !S.mag_h2[0]) ||
-        (S.mag_h1[1] && !S.mag_h2[1]))
+        (S.mag_h1[1] && !S.mag_h2[1]) ||
+        (S.pol == MTB_TE && S.cond_d1[0] && (!S.cond_d1[1] || !S.cond_d2[1])))
         return fail(MTB_INVALID_ARG, "adjoint: damping pairs need both arrays");
+    if (S.pol == MTB_TE && S.n_poles_y > 0 &&
+        (!bufs->g_pol_y[0] || !bufs->g_pol_y[1] ||
+         (reinterpret_cast<uintptr_t>(bufs->g_pol_y[0]) & 15) ||
+         (reinterpret_cast<uintptr_t>(bufs->g_pol_y[1]) & 15) || !S.pol_cy[0] || !S.pol_cy[1] ||
+         !S.pol_cy[2]))
+        return fail(MTB_INVALID_ARG, "adjoint: Ey poles need g_pol_y[0..1] and c1..c3");
     if (S.n_poles > 0 && (!bufs->g_pol[0] || !bufs->g_pol[1] ||
                           (reinterpret_cast<uintptr_t>(bufs->g_pol[0]) & 15) ||
                           (reinterpret_cast<uintptr_t>(bufs->g_pol[1]) & 15) || !S.pol_c[0] ||

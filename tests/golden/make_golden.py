@@ -606,9 +606,11 @@ def grad_loss_te(st, ad, ax, ay, mx, my, dx):
                   + 0.05 * (st.Ex * st.Ex).sum() - 0.02 * (st.Ey * st.Ey).sum())
 
 
-def grad_te_case(prec):
+def grad_te_case(prec, extra=None):
     """d J / d eps_inf through the reference's autograd of run_te
-    (checkpoint_every, core/run.py:81-120) on the TE case's geometry."""
+    (checkpoint_every, core/run.py:81-120) on the TE case's geometry; ``extra`` =
+    "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole on
+    both E axes."""
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -616,7 +618,18 @@ def grad_te_case(prec):
     eps[26:34, 22:32] = 1.0 + 4.0 * rng.random((8, 10))
     g = Grid(nx=nx, ny=ny, dx=dx, dtype=DT[prec], device="cpu")
     e = torch.tensor(eps, dtype=DT[prec], requires_grad=True)
-    m = build_te_coeffs(g, eps_inf=e, npml=npml)
+    kw, out_extra = {}, {}
+    if extra == "lossy":
+        sd = sigma_map(nx, ny, 21)
+        sbm, mum = magnetic_maps(nx, ny, 23)
+        kw = dict(sigma_d=torch.tensor(sd, dtype=DT[prec]), sigma_b=torch.tensor(sbm, dtype=DT[prec]),
+                  mu=torch.tensor(mum, dtype=DT[prec]))
+        out_extra = dict(sigma=sd, sigma_b=sbm, mu=mum)
+    elif extra == "poles":
+        pm = pole_masks(nx, ny)
+        kw = dict(poles=POLES, pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
+        out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
+    m = build_te_coeffs(g, eps_inf=e, npml=npml, **kw)
     line = LineSource(g, ix=12, j0=14, j1=26, profile=GaussianPulse(0.65, 0.4))
 
     class _TESrc:                                   # TE binding: mask[:, :-1] -> Dy
@@ -629,14 +642,15 @@ def grad_te_case(prec):
     monx = FluxMonitorTE(g, freqs, ix=33, lo=10, hi=30)
     mony = FluxMonitorTEY(g, freqs, iy=30, lo=10, hi=34)
     n, ce = 180, 60
-    st, (ad, ax, ay) = run_te(init_te_state(g), m, n, source=src, monitors=[dft, monx, mony],
+    s0 = init_te_state(g, n_poles=len(POLES) if extra == "poles" else 0)
+    st, (ad, ax, ay) = run_te(s0, m, n, source=src, monitors=[dft, monx, mony],
                               checkpoint_every=ce)
     J = grad_loss_te(st, ad, ax, ay, monx, mony, dx)
     J.backward()
     return dict(nx=nx, ny=ny, dx=dx, npml=npml, n_steps=n, checkpoint_every=ce, eps=eps,
                 freqs=np.array(freqs), fcen=0.65, fwidth=0.4, src_ix=12, src_j0=14, src_j1=26,
                 monx=np.array([33, 10, 30]), mony=np.array([30, 10, 34]),
-                J=float(J.detach()), grad=_np(e.grad))
+                J=float(J.detach()), grad=_np(e.grad), **out_extra)
 
 
 def main():
@@ -668,6 +682,11 @@ def main():
         for extra in ("lossy", "poles"):
             np.savez_compressed(os.path.join(HERE, f"golden_grad_tm_{extra}_f64.npz"),
                                 **grad_tm_case("f64", extra))
+        return
+    if sys.argv[1:] == ["grad_extra_te"]:
+        for extra in ("lossy", "poles"):
+            np.savez_compressed(os.path.join(HERE, f"golden_grad_te_{extra}_f64.npz"),
+                                **grad_te_case("f64", extra))
         return
     if sys.argv[1:] == ["lean_poles"]:
         for prec in ("f64", "f32"):

@@ -941,6 +941,56 @@ def test_te_gradient_matches_reference_autograd(chunk):
     assert e32 < TOL, e32
 
 
+@pytest.mark.parametrize("chunk", [60, 32])
+@pytest.mark.parametrize("extra", ["lossy", "poles"])
+def test_te_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
+    """d J / d eps_inf of lossy (sigma_d on Dx / Dy, sigma_b and mu on Hz) and
+    dispersive (a Lorentz and a Drude pole on Ex and Ey) TE runs from the adjoint kernels,
+    against the reference's float64 autograd through run_te(checkpoint_every=60)
+    (tests/golden/make_golden.py grad_extra_te, pinned by central differences of the
+    oracle); the float32 forward and adjoint agree with it to 1e-4."""
+    from meep_torch_b200.core.coeffs import build_te_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor, FluxMonitorTE, FluxMonitorTEY
+    from meep_torch_b200.core.run import run_te
+    from meep_torch_b200.core.sources import GaussianPulse, LineSource, TESource
+    from meep_torch_b200.core.stepper_te import init_te_state
+    g64 = load_golden(f"grad_te_{extra}_f64")
+    nx, ny, dx, npml = int(g64["nx"]), int(g64["ny"]), float(g64["dx"]), int(g64["npml"])
+    grid = Grid(nx=nx, ny=ny, dx=dx, device=dev())
+    e = torch.tensor(g64["eps"], dtype=torch.float32, device=dev(), requires_grad=True)
+    T = lambda a: torch.tensor(a, dtype=torch.float32)  # noqa: E731
+    kw, n_p = {}, 0
+    if extra == "lossy":
+        kw = dict(sigma_d=T(g64["sigma"]), sigma_b=T(g64["sigma_b"]), mu=T(g64["mu"]))
+    else:
+        poles = json.loads(str(g64["poles"]))
+        kw = dict(poles=poles, pole_masks=[T(x) for x in g64["pole_masks"]])
+        n_p = len(poles)
+    m = build_te_coeffs(grid, eps_inf=e, npml=npml, **kw)
+    src = TESource(LineSource(grid, ix=int(g64["src_ix"]), j0=int(g64["src_j0"]),
+                              j1=int(g64["src_j1"]),
+                              profile=GaussianPulse(float(g64["fcen"]), float(g64["fwidth"]))))
+    freqs = [float(f) for f in g64["freqs"]]
+    mx, my = [int(v) for v in g64["monx"]], [int(v) for v in g64["mony"]]
+    dft = DFTFieldsMonitor(grid, freqs, "Hz")
+    monx = FluxMonitorTE(grid, freqs, ix=mx[0], lo=mx[1], hi=mx[2])
+    mony = FluxMonitorTEY(grid, freqs, iy=my[0], lo=my[1], hi=my[2])
+    st, (ad, ax, ay) = run_te(init_te_state(grid, n_poles=n_p), m, int(g64["n_steps"]),
+                              source=src, monitors=[dft, monx, mony], checkpoint_every=chunk)
+    w = torch.tensor([1.0, -0.5, 0.25], dtype=torch.float32, device=dev())
+    J = 1e6 * ((w * monx.flux(ax, dx)).sum() + (w.flip(0) * mony.flux(ay, dx)).sum()
+               + 1e-3 * (ad * ad).sum() + 0.1 * (st.Hz * st.Hz).sum()
+               + 0.05 * (st.Ex * st.Ex).sum() - 0.02 * (st.Ey * st.Ey).sum())
+    J.backward()
+    got = e.grad.cpu().numpy()
+    e64 = rel_l2(got, g64["grad"])
+    print(f"TE grad {extra} chunk {chunk}: rel L2 vs reference f64 {e64:.3e}; "
+          f"J {float(J):.6e} vs {float(g64['J']):.6e}")
+    assert abs(float(J) - float(g64["J"])) <= 1e-4 * abs(float(g64["J"]))
+    assert e64 < 1e-4, e64
+
+
 @pytest.mark.parametrize("geometry", [0, 2])
 @pytest.mark.parametrize("shape", [(23, 17, 40), (9, 30, 128), (31, 13, 131), (6, 22, 256),
                                    (40, 8, 77), (48, 256, 256)])
@@ -1180,10 +1230,16 @@ def test_magnetic_batched_tiles_match_oracle_and_other_paths_refuse():
     eng.close()
     with pytest.raises(MtbUnsupported):
         Engine2D(items[:1], variant=1)
-    # gradients: TM magnetic pairs have an adjoint, TE ones do not (refused)
+    # gradients: TE magnetic pairs have an adjoint; a nonlinear (chi3) TE run does not
     grid = Grid(nx=40, ny=40, dx=dx, device=dev())
     eps = torch.ones(40, 40, device=dev(), requires_grad=True)
     m = build_te_coeffs(grid, eps_inf=eps, npml=8, sigma_b=torch.full((40, 40), 0.5))
+    _, (acc,) = run_te(init_te_state(grid), m, 10,
+                       monitors=[DFTFieldsMonitor(grid, [0.5], "Hz")])
+    acc.sum().backward()
+    assert bool(torch.isfinite(eps.grad).all())
+    eps2 = torch.ones(40, 40, device=dev(), requires_grad=True)
+    m = build_te_coeffs(grid, eps_inf=eps2, npml=8, chi3=torch.full((40, 40), 0.5))
     _, (acc,) = run_te(init_te_state(grid), m, 10,
                        monitors=[DFTFieldsMonitor(grid, [0.5], "Hz")])
     with pytest.raises(MtbUnsupported):

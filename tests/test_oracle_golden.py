@@ -263,10 +263,16 @@ def test_reference_3d_gradient_matches_oracle_finite_differences():
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-12, (i, j, k, fd, ref)
 
 
-def test_reference_te_gradient_matches_oracle_finite_differences():
+@pytest.mark.parametrize("case", ["grad_te", "grad_te_lossy", "grad_te_poles"])
+def test_reference_te_gradient_matches_oracle_finite_differences(case):
     """The golden TE d J / d eps_inf (reference autograd, float64) against central
-    finite differences of the oracle's float64 TE run at two pixels."""
-    g = load_golden("grad_te_f64")
+    finite differences of the oracle's float64 TE run at two pixels; the lossy case adds
+    sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole on both E
+    axes."""
+    g = load_golden(f"{case}_f64")
+    extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"))
+    if "poles" in g:
+        extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
                            int(g["n_steps"]))
     freqs = [float(f) for f in g["freqs"]]
@@ -274,7 +280,7 @@ def test_reference_te_gradient_matches_oracle_finite_differences():
     myi, myl, myh = (int(v) for v in g["mony"])
 
     def J_of(eps):
-        c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float64)
+        c = O.te_coeffs(nx, ny, dx, eps=eps, npml=npml, dtype=np.float64, **extra)
         dt = c["dt"]
         mask = O.line_source_mask(nx, ny, dx, int(g["src_ix"]), int(g["src_j0"]),
                                   int(g["src_j1"]), dtype=np.float64)[:, :-1]
