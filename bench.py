@@ -899,7 +899,18 @@ def ref_cfg4(steps):
 def reference_cpu(wl, args, threads):
     """(value, unit, cores, sample, kind) of the reference's own CPU path on a bounded
     sample of workload `wl`, or None when the reference is not installed (cfg5: the
-    reference has no surrogate, so None)."""
+    reference has no surrogate, so None). The reference runs on every host thread; the
+    process's own torch thread count is put back afterwards, so the host-side work of
+    the measurements that follow (the other configurations) is not slowed by it."""
+    import torch
+    prev = torch.get_num_threads()
+    try:
+        return _reference_cpu(wl, args, threads)
+    finally:
+        torch.set_num_threads(prev)
+
+
+def _reference_cpu(wl, args, threads):
     if wl == "cfg5" or reference_module() is None:
         return None
     import torch

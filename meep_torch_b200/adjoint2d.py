@@ -49,10 +49,9 @@ class GradRun2D:
     def __init__(self, state, coeffs, n_steps, source, monitors, chunk=32,
                  phase_mode="exact"):
         self.te = hasattr(state, "Hz")
-        if getattr(coeffs, "y_pmc", False) or any(
-                getattr(coeffs, k, 0) for k in ("y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
-                                                "rot4_lo")):
-            raise L.MtbUnsupported("gradients: PEC walls only (y_pmc, symmetry cuts)")
+        if any(getattr(coeffs, k, 0) for k in ("y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
+                                               "rot4_lo")):
+            raise L.MtbUnsupported("gradients: symmetry cuts are forward-only")
         self.names = STATE_TE if self.te else STATE_TM
         self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
         self.source, self.monitors = source, list(monitors)

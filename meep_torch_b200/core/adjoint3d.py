@@ -32,10 +32,9 @@ def run_3d_adjoint(c, n_steps: int, chunk: int, source, monitors, loss_fn, state
     eps_src = c.eps
     cd = c._replace(eps=eps_src.detach())
     eng = Engine3D(state0, cd, source, monitors, point_sign=+1, ring_slots=K)
-    if eng._damp is not None or eng.n_poles:
+    if eng.n_poles:
         eng.close()
-        raise L.MtbUnsupported("3D adjoint: conductive damping (sigma_d / sigma_b) and poles "
-                               "are forward-only on the B200 path")
+        raise L.MtbUnsupported("3D adjoint: poles are forward-only on the B200 path")
     rec = adj = None
     try:
         chunks = [(s0, min(K, n - s0)) for s0 in range(0, n, K)]

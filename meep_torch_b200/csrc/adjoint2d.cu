@@ -1,7 +1,7 @@
 // Discrete adjoint of the 2D TM step for sm_100a: the exact transpose of the
 // forward update (core/stepper_tm.py:234-254: B phase :85-128, D phase
 // :130-166, update_pols :203-208, E = (D - sum P) / eps :221-231) with CPML
-// (kappa = 1, PEC walls), electric conductivity (D' = d1 D + d2 curl), magnetic
+// (kappa = 1, PEC walls or TM PMC walls in y), electric conductivity (D' = d1 D + d2 curl), magnetic
 // conductivity / permeability (H' = h1 H -/+ h2 curl) and dispersive ADE poles,
 // and of the monitors' sampling (core/monitors.py:24-100). This is what torch
 // autograd computes through the reference's run_tm (core/run.py:43-120); the
@@ -140,7 +140,9 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
         const bool inside = j < ny;
-        const bool interior = rowin && j >= 1 && j <= ny - 2;
+        // the curl of the D update: interior columns, or every column under PMC walls in
+        // y (zero H beyond both walls, core/stepper_tm.py:143-145)
+        const bool interior = rowin && (S.y_pmc ? j < ny : (j >= 1 && j <= ny - 2));
         const float gd = gdz[q] + gez[q] * ie[q];
         ge[q] -= gez[q] * ez[q] * ie[q];
         const float gc = interior ? d2[q] * gd : 0.f;
@@ -592,8 +594,9 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     *out = nullptr;
     const mtb_yee2d_struct &S = *s;
     if (S.pol != MTB_TM && S.pol != MTB_TE) return fail(MTB_INVALID_ARG, "adjoint: bad pol");
-    if (S.y_pmc || S.cut_y || S.cut_x)
-        return fail(MTB_UNSUPPORTED, "adjoint: PEC walls only (y_pmc, symmetry cuts)");
+    if (S.cut_y || S.cut_x)
+        return fail(MTB_UNSUPPORTED, "adjoint: symmetry cuts are forward-only");
+    if (S.y_pmc && S.pol != MTB_TM) return fail(MTB_INVALID_ARG, "adjoint: y_pmc is TM only");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");
     if (S.n_mpoles) return fail(MTB_UNSUPPORTED, "adjoint: magnetic poles are forward-only");
     if (S.te3) return fail(MTB_UNSUPPORTED, "adjoint: TE tensor eps / oriented poles");

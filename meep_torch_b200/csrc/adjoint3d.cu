@@ -1,4 +1,5 @@
-// Discrete adjoint of the 3D CPML step for sm_100a: the exact transpose of
+// Discrete adjoint of the 3D CPML step for sm_100a (with conductive damping:
+// H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps): the exact transpose of
 // the split H / E update (core/stepper_3d.py:363-437, the same arithmetic as
 // k_yee3d_h / k_yee3d_e) and of the plane sampling (core/monitors_3d.py:70-189)
 // -- the reverse sweep of the reference's run_3d_adjoint
@@ -36,6 +37,7 @@ struct Adj3 {
     const float *eps;
     const float *pb[3][2];
     const float *pa[3][2];
+    const float *dmp[6][2];       // conductive damping (d1, d2) per component, or null
     int nx, ny, nz, zp;
     float dt, rdx;
 };
@@ -115,6 +117,13 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
         l4(eo_ + c * rec_comp + g, eo[c]);
     }
     for (int c = 0; c < 6; ++c) l4(B.g_psi[6 + c] + g, gp[c]);
+    // conductive damping: E' = d1 E + (d2 curl + s) / eps_c (core/stepper_3d.py:405-437)
+    const bool damp = P.dmp[0][0] != nullptr;
+    float d1[3][4], d2[3][4];
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 4; ++q) { d1[c][q] = 1.f; d2[c][q] = dt; }
+    if (damp)
+        for (int c = 0; c < 3; ++c) { l4(P.dmp[c][0] + g, d1[c]); l4(P.dmp[c][1] + g, d2[c]); }
     // E-side profiles (1, 0) on inert nodes
     const float exb = prof(P.pb[0][1], iin, 1.f, i), exa = prof(P.pa[0][1], iin, 0.f, i);
     const float eyb = prof(P.pb[1][1], jin, 1.f, j), eya = prof(P.pa[1][1], jin, 0.f, j);
@@ -129,8 +138,9 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const bool v = xok && vzE, in = v && jin && kin;
             const float e_x = 0.5f * (ep[q] + epi[q]);
             const float gE = ge[0][q];
-            t[6][q] = v ? -gE * (en[0][q] - eo[0][q]) / e_x : 0.f;
-            const float gc = in ? dt * gE / e_x : 0.f;
+            t[6][q] = v ? -gE * (en[0][q] - d1[0][q] * eo[0][q]) / e_x : 0.f;
+            const float gc = in ? d2[0][q] * gE / e_x : 0.f;
+            ge[0][q] = v ? d1[0][q] * gE : gE;         // E' = d1 E + ...: d1 gE to E
             const float g6 = gp[0][q] + gc, g7 = gp[1][q] - gc;
             const bool u6 = v && jin, u7 = v && kin;
             gp[0][q] = u6 ? eyb * g6 : gp[0][q];
@@ -143,8 +153,9 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const bool v = vyH && vzE, in = v && iin && kin;
             const float e_y = 0.5f * (ep[q] + epj[q]);
             const float gE = ge[1][q];
-            t[7][q] = v ? -gE * (en[1][q] - eo[1][q]) / e_y : 0.f;
-            const float gc = in ? dt * gE / e_y : 0.f;
+            t[7][q] = v ? -gE * (en[1][q] - d1[1][q] * eo[1][q]) / e_y : 0.f;
+            const float gc = in ? d2[1][q] * gE / e_y : 0.f;
+            ge[1][q] = v ? d1[1][q] * gE : gE;         // E' = d1 E + ...: d1 gE to E
             const float g8 = gp[2][q] + gc, g9 = gp[3][q] - gc;
             const bool u8 = v && kin, u9 = v && iin;
             gp[2][q] = u8 ? ezb * g8 : gp[2][q];
@@ -157,8 +168,9 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const bool v = vz, in = v && iin && jin;
             const float e_z = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
             const float gE = ge[2][q];
-            t[8][q] = v ? -gE * (en[2][q] - eo[2][q]) / e_z : 0.f;
-            const float gc = in ? dt * gE / e_z : 0.f;
+            t[8][q] = v ? -gE * (en[2][q] - d1[2][q] * eo[2][q]) / e_z : 0.f;
+            const float gc = in ? d2[2][q] * gE / e_z : 0.f;
+            ge[2][q] = v ? d1[2][q] * gE : gE;         // E' = d1 E + ...: d1 gE to E
             const float g10 = gp[4][q] + gc, g11 = gp[5][q] - gc;
             const bool u10 = v && iin, u11 = v && jin;
             gp[4][q] = u10 ? exb * g10 : gp[4][q];
@@ -169,6 +181,8 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
     }
     for (int c = 0; c < 6; ++c) s4(B.g_psi[6 + c] + g, gp[c]);
     for (int c = 0; c < 9; ++c) s4(B.tmp[c] + g, t[c]);
+    if (damp)
+        for (int c = 0; c < 3; ++c) s4(B.g[c] + g, ge[c]);
 }
 
 __global__ void __launch_bounds__(32 * A3Y) k_adj3_h(const __grid_constant__ Adj3 P) {
@@ -205,6 +219,12 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_h(const __grid_constant__ Adj
     for (int c = 0; c < 6; ++c) l4(B.g_psi[c] + g, gp[c]);
     const float hxb = prof(P.pb[0][0], xok, 1.f, i), hxa = prof(P.pa[0][0], xok, 0.f, i);
     const float hyb = prof(P.pb[1][0], vyH, 1.f, j), hya = prof(P.pa[1][0], vyH, 0.f, j);
+    // conductive damping: H' = d1 H - d2 curl (core/stepper_3d.py:375-393)
+    float h1[3][4], h2[3][4];
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 4; ++q) { h1[c][q] = 1.f; h2[c][q] = dt; }
+    if (P.dmp[3][0])
+        for (int c = 0; c < 3; ++c) { l4(P.dmp[3 + c][0] + g, h1[c]); l4(P.dmp[3 + c][1] + g, h2[c]); }
     float u[6][4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -220,35 +240,35 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_h(const __grid_constant__ Adj
         // Hx -= dt ((dy + psi0') - (dz + psi1')): valid j <= ny-2, k <= nz-2
         {
             const bool v = vyH && vz;
-            const float c0 = -dt * gx, c1 = dt * gx;
+            const float c0 = -h2[0][q] * gx, c1 = h2[0][q] * gx;
             const float g0 = gp[0][q] + c0, g1 = gp[1][q] + c1;
             u[0][q] = v ? c0 + hya * g0 : 0.f;                     // dy(Ez)
             u[1][q] = v ? c1 + hza * g1 : 0.f;                     // dz(Ey)
             gp[0][q] = v ? hyb * g0 : gp[0][q];
             gp[1][q] = v ? hzb * g1 : gp[1][q];
-            gh[0][q] = gx;
+            gh[0][q] = v ? h1[0][q] * gx : gx;
         }
         // Hy -= dt ((dz + psi2') - (dx + psi3')): valid i <= nx-2, k <= nz-2
         {
             const bool v = xok && vz;
-            const float c2 = -dt * gy, c3 = dt * gy;
+            const float c2 = -h2[1][q] * gy, c3 = h2[1][q] * gy;
             const float g2 = gp[2][q] + c2, g3 = gp[3][q] + c3;
             u[2][q] = v ? c2 + hza * g2 : 0.f;                     // dz(Ex)
             u[3][q] = v ? c3 + hxa * g3 : 0.f;                     // dx(Ez)
             gp[2][q] = v ? hzb * g2 : gp[2][q];
             gp[3][q] = v ? hxb * g3 : gp[3][q];
-            gh[1][q] = gy;
+            gh[1][q] = v ? h1[1][q] * gy : gy;
         }
         // Hz -= dt ((dx + psi4') - (dy + psi5')): valid i <= nx-2, j <= ny-2, k < nz
         {
             const bool v = xok && vyH && vzE;
-            const float c4 = -dt * gz, c5 = dt * gz;
+            const float c4 = -h2[2][q] * gz, c5 = h2[2][q] * gz;
             const float g4 = gp[4][q] + c4, g5 = gp[5][q] + c5;
             u[4][q] = v ? c4 + hxa * g4 : 0.f;                     // dx(Ey)
             u[5][q] = v ? c5 + hya * g5 : 0.f;                     // dy(Ex)
             gp[4][q] = v ? hxb * g4 : gp[4][q];
             gp[5][q] = v ? hyb * g5 : gp[5][q];
-            gh[2][q] = gz;
+            gh[2][q] = v ? h1[2][q] * gz : gz;
         }
     }
     for (int c = 0; c < 3; ++c) s4(B.g[3 + c] + g, gh[c]);
@@ -334,9 +354,13 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
     if (!out || !s || !bufs) return fail(MTB_INVALID_ARG, "null argument");
     *out = nullptr;
     const mtb_yee3d_struct &S = *s;
+    const bool dmp = S.damp[0][0] != nullptr;
     for (int c = 0; c < 6; ++c)
-        if (S.damp[c][0] || S.damp[c][1])
-            return fail(MTB_UNSUPPORTED, "3D adjoint: conductive damping is forward-only");
+        for (int h = 0; h < 2; ++h)
+            if ((S.damp[c][h] != nullptr) != dmp ||
+                (S.damp[c][h] && (reinterpret_cast<uintptr_t>(S.damp[c][h]) & 15)))
+                return fail(MTB_INVALID_ARG, "3D adjoint: damping needs all twelve arrays, "
+                            "16-byte aligned");
     if (S.n_poles) return fail(MTB_UNSUPPORTED, "3D adjoint: poles are forward-only");
     if (S.pmc_axes) return fail(MTB_UNSUPPORTED, "3D adjoint: PMC walls are forward-only");
     if (S.nx < 3 || S.ny < 3 || S.nz < 3 || S.zpitch < S.nz || (S.zpitch & 3))
@@ -368,6 +392,8 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
             A.pb[a][h] = S.prof_b[a][h];
             A.pa[a][h] = S.prof_a[a][h];
         }
+    for (int c = 0; c < 6; ++c)
+        for (int h = 0; h < 2; ++h) A.dmp[c][h] = S.damp[c][h];
     A.nx = S.nx; A.ny = S.ny; A.nz = S.nz; A.zp = S.zpitch;
     A.dt = S.dt;
     A.rdx = 1.0f / S.dx;

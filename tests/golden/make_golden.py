@@ -487,7 +487,8 @@ def grad_loss(st, ax, ay, ad, mx, my, dx):
 def grad_tm_case(prec, extra=None):
     """d J / d eps through the reference's autograd (run_tm with
     checkpoint_every, core/run.py:81-120) on the TM case's geometry; ``extra`` =
-    "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole."""
+    "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole,
+    "pmc" PMC walls in y."""
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -507,6 +508,8 @@ def grad_tm_case(prec, extra=None):
         pm = pole_masks(nx, ny)
         kw = dict(poles=POLES, pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
         out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
+    if extra == "pmc":
+        kw, out_extra = dict(y_pmc=True), dict(y_pmc=1)
     m = build_tm_coeffs(g, eps_inf=e, npml=npml, **kw)
     src = LineSource(g, ix=12, j0=10, j1=26, profile=GaussianPulse(0.65, 0.4))
     freqs = [0.55, 0.65, 0.75]
@@ -514,7 +517,8 @@ def grad_tm_case(prec, extra=None):
     mony = FluxMonitorTM(g, freqs, x_normal=False, idx=26, lo=10, hi=38)
     dft = DFTFieldsMonitor(g, freqs, component="Ez")
     n, ce = 200, 50
-    s0 = init_tm_state(g, n_poles=len(POLES) if extra == "poles" else 0)
+    s0 = init_tm_state(g, n_poles=len(POLES) if extra == "poles" else 0,
+                       y_pmc=extra == "pmc")
     st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft],
                               checkpoint_every=ce)
     J = grad_loss(st, ax, ay, ad, monx, mony, dx)
@@ -562,9 +566,10 @@ def design_case():
                 box=np.array(reg.box), rho0=_np(rho0), f0=f0, grad=grad)
 
 
-def grad3d_case(prec):
+def grad3d_case(prec, sigma=False):
     """d J / d eps of the reference's run_3d_adjoint (core/adjoint3d.py:56) on a
-    small CPML grid with spheres, an Ez point dipole and two flux faces."""
+    small CPML grid with spheres, an Ez point dipole and two flux faces; ``sigma`` adds a
+    lossy slab (sigma_d) and a magnetically lossy patch (sigma_b)."""
     from meep_torch.core.adjoint3d import run_3d_adjoint
     rng = np.random.default_rng(13)
     n, dx, npml = 20, 1.0 / 16, 4
@@ -577,7 +582,15 @@ def grad3d_case(prec):
                   (ax[None, None, :] - cc[2]) ** 2) <= r * r
         eps[inside] = rng.uniform(2.0, 8.0)
     e = torch.tensor(eps, dtype=DT[prec], requires_grad=True)
-    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device="cpu")
+    kw, out_extra = {}, {}
+    if sigma:
+        sd = np.zeros((n, n, n))
+        sd[12:15] = 2.0
+        sb = np.zeros((n, n, n))
+        sb[5:9, 6:12, 7:13] = 3.0
+        kw = dict(sigma_d=torch.tensor(sd, dtype=DT[prec]), sigma_b=torch.tensor(sb, dtype=DT[prec]))
+        out_extra = dict(sigma_d=sd, sigma_b=sb)
+    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device="cpu", **kw)
     src = PointSource3D(c.dt, "Ez", 10, 9, 11, GaussianPulse(0.9, 0.6))
     freqs = [0.7, 0.9, 1.1]
     mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=15, win=(5, 15, 5, 15)),
@@ -594,7 +607,7 @@ def grad3d_case(prec):
     L, accs = run_3d_adjoint(c, n_steps, chunk, src, mons, loss_fn, s0)
     return dict(n=n, dx=dx, npml=npml, eps=eps, freqs=np.array(freqs), src=np.array([10, 9, 11]),
                 fcen=0.9, fwidth=0.6, n_steps=n_steps, chunk=chunk, L=float(L),
-                grad=_np(e.grad), acc_0=_np(accs[0]), acc_1=_np(accs[1]))
+                grad=_np(e.grad), acc_0=_np(accs[0]), acc_1=_np(accs[1]), **out_extra)
 
 
 def grad_loss_te(st, ad, ax, ay, mx, my, dx):
@@ -677,6 +690,14 @@ def main():
                 for name, fold in folds.items():
                     np.savez_compressed(os.path.join(HERE, f"golden_{pol}_fold_{name}_{prec}.npz"),
                                         **fold_case(prec, pol, fold))
+        return
+    if sys.argv[1:] == ["grad3d_sigma"]:
+        np.savez_compressed(os.path.join(HERE, "golden_grad3d_sigma_f64.npz"),
+                            **grad3d_case("f64", sigma=True))
+        return
+    if sys.argv[1:] == ["grad_pmc"]:
+        np.savez_compressed(os.path.join(HERE, "golden_grad_tm_pmc_f64.npz"),
+                            **grad_tm_case("f64", "pmc"))
         return
     if sys.argv[1:] == ["grad_extra"]:
         for extra in ("lossy", "poles"):

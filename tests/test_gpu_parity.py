@@ -725,6 +725,9 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
         kw = dict(poles=poles, pole_masks=[torch.tensor(v, dtype=torch.float32, device=dev_)
                                            for v in g["pole_masks"]])
         n_p = len(poles)
+    pmc = extra == "pmc"
+    if pmc:
+        kw = dict(y_pmc=True)
     m = build_tm_coeffs(grid, eps_inf=e, npml=npml, **kw)
     src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
                      profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
@@ -734,7 +737,7 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
     monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=mx[0], lo=mx[1], hi=mx[2])
     mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=my[0], lo=my[1], hi=my[2])
     dft = DFTFieldsMonitor(grid, freqs, "Ez")
-    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p), dx
+    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p, y_pmc=pmc), dx
 
 
 def _grad_loss(st, ax, ay, ad, mx, my, dx):
@@ -765,11 +768,11 @@ def test_tm_gradient_matches_reference_autograd(chunk):
     assert e32 < 1e-4, e32
 
 
-@pytest.mark.parametrize("extra", ["lossy", "poles"])
+@pytest.mark.parametrize("extra", ["lossy", "poles", "pmc"])
 @pytest.mark.parametrize("chunk", [50, 13])
 def test_tm_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
-    """d J / d eps of lossy (sigma_d on E, sigma_b and mu on H) and dispersive (a
-    Lorentz and a Drude pole) TM runs from the adjoint kernels, against the reference's
+    """d J / d eps of lossy (sigma_d on E, sigma_b and mu on H), dispersive (a
+    Lorentz and a Drude pole) and y-PMC TM runs from the adjoint kernels, against the reference's
     float64 autograd through run_tm(checkpoint_every=50) (tests/golden/make_golden.py
     grad_extra); the float32 forward and adjoint agree with it to 1e-4."""
     from meep_torch_b200.core.run import run_tm
@@ -865,6 +868,43 @@ def test_magnetic_sheet_sources_match_oracle(case):
         names = ("Hz", "Ex", "Ey", "Dx", "Dy")
     errs = {k: rel_l2(getattr(st, k).cpu().numpy(), s[k]) for k in names}
     assert all(v < TOL for v in errs.values()), errs
+
+
+def test_3d_lossy_gradient_matches_reference_run_3d_adjoint():
+    """d J / d eps of run_3d_adjoint with conductive damping (a sigma_d slab, a sigma_b
+    patch: H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps) on the 3D adjoint kernels
+    against the reference's float64 run_3d_adjoint (tests/golden/make_golden.py
+    grad3d_sigma, pinned by central differences of the oracle)."""
+    from meep_torch_b200.core.adjoint3d import run_3d_adjoint
+    from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D
+    from meep_torch_b200.core.sources import GaussianPulse
+    from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
+    g64 = load_golden("grad3d_sigma_f64")
+    n, dx, npml = int(g64["n"]), float(g64["dx"]), int(g64["npml"])
+    e = torch.tensor(g64["eps"], dtype=torch.float32, device=dev(), requires_grad=True)
+    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device=dev(),
+                        sigma_d=torch.tensor(g64["sigma_d"], dtype=torch.float32),
+                        sigma_b=torch.tensor(g64["sigma_b"], dtype=torch.float32))
+    i, j, k = (int(v) for v in g64["src"])
+    src = PointSource3D(c.dt, "Ez", i, j, k, GaussianPulse(float(g64["fcen"]), float(g64["fwidth"])))
+    freqs = [float(f) for f in g64["freqs"]]
+    mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=15, win=(5, 15, 5, 15)),
+            FluxMonitor3D(c.dt, freqs, normal="z", idx=6, win=(5, 15, 5, 15))]
+    w = torch.tensor([1.0, -0.7, 0.4], dtype=torch.float32, device=dev())
+
+    def loss_fn(accs):
+        return 1e15 * ((w * mons[0].flux(accs[0], dx)).sum()
+                       + (w.flip(0) * mons[1].flux(accs[1], dx)).sum()
+                       + 1e-3 * sum((a * a).sum() for a in accs))
+
+    L, accs = run_3d_adjoint(c, int(g64["n_steps"]), 16, src, mons, loss_fn,
+                             init_3d_state(n, n, n, npml=npml, device=dev()))
+    got = e.grad.cpu().numpy()
+    e64 = rel_l2(got, g64["grad"])
+    print(f"3D lossy grad: rel L2 vs reference f64 {e64:.3e}; L {L:.6e} vs "
+          f"{float(g64['L']):.6e}")
+    assert abs(L - float(g64["L"])) <= 1e-4 * abs(float(g64["L"]))
+    assert e64 < 1e-4, e64
 
 
 def test_3d_gradient_matches_reference_run_3d_adjoint():
@@ -1346,8 +1386,8 @@ def test_te_poles_batched_tiles_match_oracle_from_random_state():
 
 
 def test_3d_damping_refused_by_fused_kernel_and_adjoint():
-    """Conductive damping runs on the split kernels only; the fused x-march and the 3D
-    adjoint refuse it with MTB_UNSUPPORTED."""
+    """Conductive damping runs on the split kernels only (the fused x-march refuses it
+    with MTB_UNSUPPORTED); the 3D adjoint takes damping but refuses poles."""
     from meep_torch_b200._lib import MtbUnsupported
     from meep_torch_b200.core.adjoint3d import run_3d_adjoint
     from meep_torch_b200.core.monitors_3d import run_3d
@@ -1359,8 +1399,13 @@ def test_3d_damping_refused_by_fused_kernel_and_adjoint():
     s0 = init_3d_state(n, n, n, npml=3, device=dev())
     with pytest.raises(MtbUnsupported):
         run_3d(s0, c, 2, variant=1)
+    m = torch.zeros(n, n, n)
+    m[4:8, 4:8, 4:8] = 1.0
+    cp = build_3d_coeffs(n, n, n, 0.0625, npml=3, device=dev(), poles=[(0.5, 0.05, 2.0)],
+                         pole_masks=[m])
+    sp = init_3d_state(n, n, n, npml=3, device=dev(), n_poles=1)
     with pytest.raises(MtbUnsupported):
-        run_3d_adjoint(c, 4, 2, None, [], lambda accs: torch.zeros(()), s0)
+        run_3d_adjoint(cp, 4, 2, None, [], lambda accs: torch.zeros(()), sp)
 
 
 def test_3d_poles_slabs_bitwise_equal_to_whole_grid():

@@ -185,14 +185,15 @@ def test_3d_lean_sign_convention(case, prec):
         assert rel_l2(a, g[f"acc_{n}"]) < tol
 
 
-@pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles"])
+@pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles", "grad_tm_pmc"])
 def test_reference_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps (reference autograd, float64) against central
     finite differences of the oracle's float64 run at a few pixels; the lossy case
     adds sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole (the
     gradients a future adjoint of those runs must reproduce)."""
     g = load_golden(f"{case}_f64")
-    extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"))
+    extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"),
+                 y_pmc=bool(g.get("y_pmc", 0)))
     if "poles" in g:
         extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
@@ -231,10 +232,12 @@ def test_reference_gradient_matches_oracle_finite_differences(case):
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-16, (i, j, fd, ref)
 
 
-def test_reference_3d_gradient_matches_oracle_finite_differences():
+@pytest.mark.parametrize("case", ["grad3d", "grad3d_sigma"])
+def test_reference_3d_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps of run_3d_adjoint (float64) against central finite
-    differences of the oracle's float64 3D run at two cells."""
-    g = load_golden("grad3d_f64")
+    differences of the oracle's float64 3D run at two cells; the sigma case adds a
+    lossy slab (sigma_d) and a magnetically lossy patch (sigma_b)."""
+    g = load_golden(f"{case}_f64")
     n, dx, npml, steps = int(g["n"]), float(g["dx"]), int(g["npml"]), int(g["n_steps"])
     freqs = [float(f) for f in g["freqs"]]
     si, sj, sk = (int(v) for v in g["src"])
@@ -242,7 +245,8 @@ def test_reference_3d_gradient_matches_oracle_finite_differences():
     w = np.array([1.0, -0.7, 0.4])
 
     def J_of(eps):
-        c = O.coeffs_3d(n, n, n, dx, eps=eps, npml=npml, dtype=np.float64)
+        c = O.coeffs_3d(n, n, n, dx, eps=eps, npml=npml, dtype=np.float64,
+                        sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"))
         dt = c["dt"]
         mons = [lambda s, t: O.flux3d_sample(s, t, dt, freqs, "x", 15, (5, 15, 5, 15)),
                 lambda s, t: O.flux3d_sample(s, t, dt, freqs, "z", 6, (5, 15, 5, 15))]
