@@ -497,7 +497,7 @@ typedef struct mtb_yee3d_struct {
      * (Ex Ey Ez), plane k at k * nx * ny * zpitch. pol_p[c][2] ping-pong with the
      * fields: buffer `cur` P(n), the other P(n-1), overwritten with
      * P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n); c1, c2 per pole (host values),
-     * c3 per cell. Split kernels only. */
+     * c3 per cell. Split kernels and the adjoint. */
     int32_t n_poles;
     /* PMC walls instead of PEC on these axes (bit 0 x, 1 y, 2 z; core/stepper_3d.py
      * _term_pmc :99-121): the tangential E stays live at the wall and the curl term
@@ -553,12 +553,16 @@ void mtb_yee3d_plan_destroy(mtb_yee3d_plan *plan);
  * reference's run_3d_adjoint (core/adjoint3d.py:56-115).
  *   g[0..5]   d J / d (Ex, Ey, Ez, Hx, Hy, Hz), box layout (nx x ny x zpitch)
  *   g_psi     d J / d psi (12, as mtb_yee3d_struct psi)
- *   tmp[0..14] scratch boxes; g_eps accumulates d J / d eps (cell-centred). */
+ *   tmp[0..14] scratch boxes; g_eps accumulates d J / d eps (cell-centred).
+ *   g_pol[c][0] / g_pol[c][1]  with dispersive poles: d J / d P(n) and
+ *              d J / d P(n-1) of E component c, n_poles box planes each (the
+ *              layout of mtb_yee3d_struct.pol_p); null without poles. */
 typedef struct mtb_adj3d_buffers {
     float *g[6];
     float *g_psi[12];
     float *tmp[15];
     float *g_eps;
+    float *g_pol[3][2];
 } mtb_adj3d_buffers;
 
 typedef struct mtb_yee3d_adjoint mtb_yee3d_adjoint;

@@ -98,7 +98,8 @@ class Adj2DBuffers(C.Structure):
 
 
 class Adj3DBuffers(C.Structure):
-    _fields_ = [("g", vp * 6), ("g_psi", vp * 12), ("tmp", vp * 15), ("g_eps", vp)]
+    _fields_ = [("g", vp * 6), ("g_psi", vp * 12), ("tmp", vp * 15), ("g_eps", vp),
+                ("g_pol", (vp * 2) * 3)]
 
 
 STRUCTS = [Cells, LineSample, Yee2DStruct, PhaseGroup, DftRegion, Tuning, Yee3DStruct,

@@ -9,7 +9,9 @@ sampling. Per chunk (last first) the chunk's start state is restored on a record
 which re-runs the chunk step by step keeping E after every step (d/d eps of
 E' = E + (dt curl + s) / eps_c needs the increment); the adjoint plan then sweeps the
 chunk's steps in reverse. ``chunk`` bounds that record (at most 32 steps are kept at a
-time); the gradient does not depend on it.
+time); the gradient does not depend on it. Conductive damping and dispersive poles are
+transposed with the step (the pole recurrence is linear, so its adjoint needs no record
+of P); PMC walls are refused by the library.
 """
 from __future__ import annotations
 
@@ -32,9 +34,9 @@ def run_3d_adjoint(c, n_steps: int, chunk: int, source, monitors, loss_fn, state
     eps_src = c.eps
     cd = c._replace(eps=eps_src.detach())
     eng = Engine3D(state0, cd, source, monitors, point_sign=+1, ring_slots=K)
-    if eng.n_poles:
+    if eng.S.pmc_axes:
         eng.close()
-        raise L.MtbUnsupported("3D adjoint: poles are forward-only on the B200 path")
+        raise L.MtbUnsupported("3D adjoint: PMC walls are forward-only on the B200 path")
     rec = adj = None
     try:
         chunks = [(s0, min(K, n - s0)) for s0 in range(0, n, K)]
@@ -63,6 +65,12 @@ def run_3d_adjoint(c, n_steps: int, chunk: int, source, monitors, loss_fn, state
         for q in range(15):
             bufs.tmp[q] = L.ptr(tmp[q])
         bufs.g_eps = L.ptr(geps)
+        # with poles: d J / d P(n) and d J / d P(n-1) per E component, n_poles boxes each
+        gpol = [[torch.zeros((eng.n_poles * nx, ny, zp), dtype=torch.float32, device=dev)
+                 for _ in range(2)] for _ in range(3)] if eng.n_poles else []
+        for c, pair in enumerate(gpol):
+            for h in range(2):
+                bufs.g_pol[c][h] = L.ptr(pair[h])
         by_ptr = {L.ptr(a): q for q, a in enumerate(eng.accs)}
         nreg = eng.n_regions
         regs = (L.DftRegion * max(1, nreg))()
@@ -74,7 +82,7 @@ def run_3d_adjoint(c, n_steps: int, chunk: int, source, monitors, loss_fn, state
                                              regs if nreg else None, nreg, eng.groups,
                                              eng.n_groups, eng.ring_elems, K, C.byref(adj)),
                 "mtb_yee3d_adjoint_create")
-        keep = [gf, gpsi, tmp, geps, g_accs]
+        keep = [gf, gpsi, tmp, geps, g_accs, gpol]
         N = nx * ny * zp
         record = torch.empty((K + 1, 3, nx, ny, zp), dtype=torch.float32, device=dev)
         rec = Engine3D(state0, cd, source, [], point_sign=+1, ring_slots=K)

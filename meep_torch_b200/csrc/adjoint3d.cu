@@ -1,5 +1,6 @@
 // Discrete adjoint of the 3D CPML step for sm_100a (with conductive damping:
-// H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps): the exact transpose of
+// H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps, and dispersive poles, whose
+// recurrence is linear with eps-free coefficients): the exact transpose of
 // the split H / E update (core/stepper_3d.py:363-437, the same arithmetic as
 // k_yee3d_h / k_yee3d_e) and of the plane sampling (core/monitors_3d.py:70-189)
 // -- the reverse sweep of the reference's run_3d_adjoint
@@ -38,6 +39,9 @@ struct Adj3 {
     const float *pb[3][2];
     const float *pa[3][2];
     const float *dmp[6][2];       // conductive damping (d1, d2) per component, or null
+    const float *c3[3];           // pole drives per E component (np box planes each)
+    float c1[MTB_MAX_POLES], c2[MTB_MAX_POLES];
+    int np;                       // dispersive poles (0: none)
     int nx, ny, nz, zp;
     float dt, rdx;
 };
@@ -124,6 +128,43 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
         for (int q = 0; q < 4; ++q) { d1[c][q] = 1.f; d2[c][q] = dt; }
     if (damp)
         for (int c = 0; c < 3; ++c) { l4(P.dmp[c][0] + g, d1[c]); l4(P.dmp[c][1] + g, d2[c]); }
+    // dispersive poles (core/stepper_3d.py:295-300, :311-322): P(n+1) = c1 P(n) +
+    // c2 P(n-1) + c3 E(n), E' = (d1 (E eps_c + sum P(n)) + d2 curl + s - sum P(n+1)) / eps_c.
+    // P(n+1) is the next state's P(n), so gN = d J / d P(n+1) = gPc' - gE' / eps_c, and
+    //   d J / d E(n) gains sum c3 gN,  gPc = d1 gE' / eps_c + c1 gN + gPp',  gPp = c2 gN.
+    float pe[3][4];
+    for (int c = 0; c < 3; ++c) zz(pe[c]);
+    if (P.np > 0) {
+        const size_t plane = (size_t)nx * NYZ;
+        for (int c = 0; c < 3; ++c) {
+            float ec[4];
+            bool pv[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = kb + q;
+                const float o = c == 0 ? epi[q] : c == 1 ? epj[q] : (q < 3 ? ep[q + 1] : epk);
+                ec[q] = 0.5f * (ep[q] + o);
+                pv[q] = c == 0 ? (xok && k < nz) : c == 1 ? (vyH && k < nz) : (k <= nz - 2);
+            }
+            for (int p = 0; p < P.np; ++p) {
+                float *gc_ = B.g_pol[c][0] + p * plane + g;
+                float *gq_ = B.g_pol[c][1] + p * plane + g;
+                float gpc[4], gpp[4], c3[4];
+                l4(gc_, gpc); l4(gq_, gpp); l4(P.c3[c] + p * plane + g, c3);
+                const float c1 = P.c1[p], c2 = P.c2[p];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!pv[q]) continue;
+                    const float gE = ge[c][q];
+                    const float gN = gpc[q] - gE / ec[q];
+                    pe[c][q] += c3[q] * gN;
+                    gpc[q] = d1[c][q] * gE / ec[q] + c1 * gN + gpp[q];
+                    gpp[q] = c2 * gN;
+                }
+                s4(gc_, gpc); s4(gq_, gpp);
+            }
+        }
+    }
     // E-side profiles (1, 0) on inert nodes
     const float exb = prof(P.pb[0][1], iin, 1.f, i), exa = prof(P.pa[0][1], iin, 0.f, i);
     const float eyb = prof(P.pb[1][1], jin, 1.f, j), eya = prof(P.pa[1][1], jin, 0.f, j);
@@ -140,7 +181,7 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const float gE = ge[0][q];
             t[6][q] = v ? -gE * (en[0][q] - d1[0][q] * eo[0][q]) / e_x : 0.f;
             const float gc = in ? d2[0][q] * gE / e_x : 0.f;
-            ge[0][q] = v ? d1[0][q] * gE : gE;         // E' = d1 E + ...: d1 gE to E
+            ge[0][q] = v ? d1[0][q] * gE + pe[0][q] : gE;   // d1 gE (+ poles) to E
             const float g6 = gp[0][q] + gc, g7 = gp[1][q] - gc;
             const bool u6 = v && jin, u7 = v && kin;
             gp[0][q] = u6 ? eyb * g6 : gp[0][q];
@@ -155,7 +196,7 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const float gE = ge[1][q];
             t[7][q] = v ? -gE * (en[1][q] - d1[1][q] * eo[1][q]) / e_y : 0.f;
             const float gc = in ? d2[1][q] * gE / e_y : 0.f;
-            ge[1][q] = v ? d1[1][q] * gE : gE;         // E' = d1 E + ...: d1 gE to E
+            ge[1][q] = v ? d1[1][q] * gE + pe[1][q] : gE;   // d1 gE (+ poles) to E
             const float g8 = gp[2][q] + gc, g9 = gp[3][q] - gc;
             const bool u8 = v && kin, u9 = v && iin;
             gp[2][q] = u8 ? ezb * g8 : gp[2][q];
@@ -170,7 +211,7 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const float gE = ge[2][q];
             t[8][q] = v ? -gE * (en[2][q] - d1[2][q] * eo[2][q]) / e_z : 0.f;
             const float gc = in ? d2[2][q] * gE / e_z : 0.f;
-            ge[2][q] = v ? d1[2][q] * gE : gE;         // E' = d1 E + ...: d1 gE to E
+            ge[2][q] = v ? d1[2][q] * gE + pe[2][q] : gE;   // d1 gE (+ poles) to E
             const float g10 = gp[4][q] + gc, g11 = gp[5][q] - gc;
             const bool u10 = v && iin, u11 = v && jin;
             gp[4][q] = u10 ? exb * g10 : gp[4][q];
@@ -181,7 +222,7 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
     }
     for (int c = 0; c < 6; ++c) s4(B.g_psi[6 + c] + g, gp[c]);
     for (int c = 0; c < 9; ++c) s4(B.tmp[c] + g, t[c]);
-    if (damp)
+    if (damp || P.np > 0)
         for (int c = 0; c < 3; ++c) s4(B.g[c] + g, ge[c]);
 }
 
@@ -361,7 +402,8 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
                 (S.damp[c][h] && (reinterpret_cast<uintptr_t>(S.damp[c][h]) & 15)))
                 return fail(MTB_INVALID_ARG, "3D adjoint: damping needs all twelve arrays, "
                             "16-byte aligned");
-    if (S.n_poles) return fail(MTB_UNSUPPORTED, "3D adjoint: poles are forward-only");
+    if (S.n_poles < 0 || S.n_poles > MTB_MAX_POLES)
+        return fail(MTB_INVALID_ARG, "3D adjoint: n_poles %d", S.n_poles);
     if (S.pmc_axes) return fail(MTB_UNSUPPORTED, "3D adjoint: PMC walls are forward-only");
     if (S.nx < 3 || S.ny < 3 || S.nz < 3 || S.zpitch < S.nz || (S.zpitch & 3))
         return fail(MTB_INVALID_ARG, "3D adjoint: bad grid");
@@ -376,6 +418,11 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
     for (int c = 0; c < 15; ++c)
         if (bad(bufs->tmp[c])) return fail(MTB_INVALID_ARG, "3D adjoint: bad tmp buffer");
     if (bad(bufs->g_eps) || bad(S.eps)) return fail(MTB_INVALID_ARG, "3D adjoint: bad eps");
+    if (S.n_poles > 0)
+        for (int c = 0; c < 3; ++c)
+            if (bad(S.pol_c3[c]) || bad(bufs->g_pol[c][0]) || bad(bufs->g_pol[c][1]))
+                return fail(MTB_INVALID_ARG, "3D adjoint: poles need c3 and both g_pol stacks "
+                            "per component, 16-byte aligned");
     for (int a = 0; a < 3; ++a)
         for (int h = 0; h < 2; ++h)
             if (!S.prof_b[a][h] || !S.prof_a[a][h])
@@ -394,6 +441,12 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
         }
     for (int c = 0; c < 6; ++c)
         for (int h = 0; h < 2; ++h) A.dmp[c][h] = S.damp[c][h];
+    A.np = S.n_poles;
+    for (int c = 0; c < 3; ++c) A.c3[c] = S.n_poles ? S.pol_c3[c] : nullptr;
+    for (int p = 0; p < MTB_MAX_POLES; ++p) {
+        A.c1[p] = p < S.n_poles ? S.pol_c1[p] : 0.f;
+        A.c2[p] = p < S.n_poles ? S.pol_c2[p] : 0.f;
+    }
     A.nx = S.nx; A.ny = S.ny; A.nz = S.nz; A.zp = S.zpitch;
     A.dt = S.dt;
     A.rdx = 1.0f / S.dx;

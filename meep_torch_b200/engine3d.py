@@ -1,9 +1,10 @@
 """3D engine: the reference's State3D / Coeffs3D / source / monitors
 (core/stepper_3d.py:28-67, core/monitors_3d.py:18-189) -> one mtb_yee3d plan.
 
-Supported: the CPML boundary (12 psi arrays), scalar eps, no conductivity,
-no poles, no PMC walls; point / mask / plane-indexed soft currents on Ex, Ey
-or Ez; FluxMonitor3D and plane DFTFieldsMonitor3D (sum-reduced).
+Supported: the CPML boundary (12 psi arrays) or the matched-sigma absorber, scalar
+eps, conductive damping (sigma_d, sigma_b), dispersive poles, PMC walls; point / mask /
+plane-indexed soft currents on Ex, Ey or Ez; FluxMonitor3D and plane
+DFTFieldsMonitor3D (sum-reduced).
 """
 from __future__ import annotations
 
@@ -434,10 +435,14 @@ class Engine3D:
 
     def _live_buffers(self):
         cur = self.current
-        return [self.box[k][cur] for k in FIELDS + PSI]
+        out = [self.box[k][cur] for k in FIELDS + PSI]
+        for key in ("xyz" if self.n_poles else ""):
+            out += [self.pol_box[key][cur], self.pol_box[key][cur ^ 1]]   # P(n), P(n-1)
+        return out
 
     def snapshot(self):
-        """Copy of the live state (box layout: six fields, then twelve psi) for restore()."""
+        """Copy of the live state (box layout: six fields, twelve psi, then with poles
+        P(n) and P(n-1) of Ex, Ey, Ez) for restore()."""
         return [t.clone() for t in self._live_buffers()]
 
     def restore(self, snap):

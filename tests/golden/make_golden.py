@@ -14,8 +14,9 @@ cases of the hot path through its own public functions:
   ``checkpoint_every`` (``python make_golden.py grad`` writes only these)
 * the design chain (``conic_filter``, ``tanh_projection``, ``MaterialGrid``,
   ``DesignRegion``, ``OptimizationProblem``; ``python make_golden.py design``)
-* d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``)
-  and of ``run_te`` (``make_golden.py grad_te``)
+* d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``,
+  with conductive damping ``grad3d_sigma``, with poles ``grad3d_poles``) and of ``run_te``
+  (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
   (``sigma_b``, ``mu``; ``make_golden.py magnetic``), and the symmetry-folded TM and TE
@@ -566,10 +567,11 @@ def design_case():
                 box=np.array(reg.box), rho0=_np(rho0), f0=f0, grad=grad)
 
 
-def grad3d_case(prec, sigma=False):
+def grad3d_case(prec, sigma=False, poles=False):
     """d J / d eps of the reference's run_3d_adjoint (core/adjoint3d.py:56) on a
     small CPML grid with spheres, an Ez point dipole and two flux faces; ``sigma`` adds a
-    lossy slab (sigma_d) and a magnetically lossy patch (sigma_b)."""
+    lossy slab (sigma_d) and a magnetically lossy patch (sigma_b), ``poles`` a Lorentz
+    and a Drude pole on two boxes inside the CPML layers."""
     from meep_torch.core.adjoint3d import run_3d_adjoint
     rng = np.random.default_rng(13)
     n, dx, npml = 20, 1.0 / 16, 4
@@ -590,6 +592,12 @@ def grad3d_case(prec, sigma=False):
         sb[5:9, 6:12, 7:13] = 3.0
         kw = dict(sigma_d=torch.tensor(sd, dtype=DT[prec]), sigma_b=torch.tensor(sb, dtype=DT[prec]))
         out_extra = dict(sigma_d=sd, sigma_b=sb)
+    if poles:
+        pm = [np.zeros((n, n, n)), np.zeros((n, n, n))]
+        pm[0][7:13, 5:12, 8:14] = 1.0
+        pm[1][11:15, 9:15, 6:11] = 1.0
+        kw = dict(poles=POLES3, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
+        out_extra = dict(pm0=pm[0], pm1=pm[1], poles=json.dumps(POLES3))
     c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device="cpu", **kw)
     src = PointSource3D(c.dt, "Ez", 10, 9, 11, GaussianPulse(0.9, 0.6))
     freqs = [0.7, 0.9, 1.1]
@@ -602,7 +610,8 @@ def grad3d_case(prec, sigma=False):
                        + (w.flip(0) * mons[1].flux(accs[1], dx)).sum()
                        + 1e-3 * sum((a * a).sum() for a in accs))
 
-    s0 = init_3d_state(n, n, n, npml=npml, dtype=DT[prec], device="cpu")
+    s0 = init_3d_state(n, n, n, npml=npml, dtype=DT[prec], device="cpu",
+                       n_poles=len(POLES3) if poles else 0)
     n_steps, chunk = 70, 25
     L, accs = run_3d_adjoint(c, n_steps, chunk, src, mons, loss_fn, s0)
     return dict(n=n, dx=dx, npml=npml, eps=eps, freqs=np.array(freqs), src=np.array([10, 9, 11]),
@@ -694,6 +703,10 @@ def main():
     if sys.argv[1:] == ["grad3d_sigma"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad3d_sigma_f64.npz"),
                             **grad3d_case("f64", sigma=True))
+        return
+    if sys.argv[1:] == ["grad3d_poles"]:
+        np.savez_compressed(os.path.join(HERE, "golden_grad3d_poles_f64.npz"),
+                            **grad3d_case("f64", poles=True))
         return
     if sys.argv[1:] == ["grad_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad_tm_pmc_f64.npz"),

@@ -870,21 +870,30 @@ def test_magnetic_sheet_sources_match_oracle(case):
     assert all(v < TOL for v in errs.values()), errs
 
 
-def test_3d_lossy_gradient_matches_reference_run_3d_adjoint():
+@pytest.mark.parametrize("case", ["sigma", "poles"])
+def test_3d_lossy_gradient_matches_reference_run_3d_adjoint(case):
     """d J / d eps of run_3d_adjoint with conductive damping (a sigma_d slab, a sigma_b
-    patch: H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps) on the 3D adjoint kernels
-    against the reference's float64 run_3d_adjoint (tests/golden/make_golden.py
-    grad3d_sigma, pinned by central differences of the oracle)."""
+    patch: H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps) or with a Lorentz and a Drude
+    pole (P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n), folded-D E update) on the 3D adjoint
+    kernels against the reference's float64 run_3d_adjoint (tests/golden/make_golden.py
+    grad3d_sigma / grad3d_poles, pinned by central differences of the oracle)."""
     from meep_torch_b200.core.adjoint3d import run_3d_adjoint
     from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D
     from meep_torch_b200.core.sources import GaussianPulse
     from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
-    g64 = load_golden("grad3d_sigma_f64")
+    g64 = load_golden(f"grad3d_{case}_f64")
     n, dx, npml = int(g64["n"]), float(g64["dx"]), int(g64["npml"])
     e = torch.tensor(g64["eps"], dtype=torch.float32, device=dev(), requires_grad=True)
-    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device=dev(),
-                        sigma_d=torch.tensor(g64["sigma_d"], dtype=torch.float32),
-                        sigma_b=torch.tensor(g64["sigma_b"], dtype=torch.float32))
+    if case == "sigma":
+        kw = dict(sigma_d=torch.tensor(g64["sigma_d"], dtype=torch.float32),
+                  sigma_b=torch.tensor(g64["sigma_b"], dtype=torch.float32))
+        n_p = 0
+    else:
+        poles = [tuple(p) for p in json.loads(str(g64["poles"]))]
+        kw = dict(poles=poles, pole_masks=[torch.tensor(g64[f"pm{q}"], dtype=torch.float32)
+                                           for q in range(2)])
+        n_p = len(poles)
+    c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device=dev(), **kw)
     i, j, k = (int(v) for v in g64["src"])
     src = PointSource3D(c.dt, "Ez", i, j, k, GaussianPulse(float(g64["fcen"]), float(g64["fwidth"])))
     freqs = [float(f) for f in g64["freqs"]]
@@ -898,10 +907,10 @@ def test_3d_lossy_gradient_matches_reference_run_3d_adjoint():
                        + 1e-3 * sum((a * a).sum() for a in accs))
 
     L, accs = run_3d_adjoint(c, int(g64["n_steps"]), 16, src, mons, loss_fn,
-                             init_3d_state(n, n, n, npml=npml, device=dev()))
+                             init_3d_state(n, n, n, npml=npml, device=dev(), n_poles=n_p))
     got = e.grad.cpu().numpy()
     e64 = rel_l2(got, g64["grad"])
-    print(f"3D lossy grad: rel L2 vs reference f64 {e64:.3e}; L {L:.6e} vs "
+    print(f"3D {case} grad: rel L2 vs reference f64 {e64:.3e}; L {L:.6e} vs "
           f"{float(g64['L']):.6e}")
     assert abs(L - float(g64["L"])) <= 1e-4 * abs(float(g64["L"]))
     assert e64 < 1e-4, e64
@@ -1387,7 +1396,7 @@ def test_te_poles_batched_tiles_match_oracle_from_random_state():
 
 def test_3d_damping_refused_by_fused_kernel_and_adjoint():
     """Conductive damping runs on the split kernels only (the fused x-march refuses it
-    with MTB_UNSUPPORTED); the 3D adjoint takes damping but refuses poles."""
+    with MTB_UNSUPPORTED); the 3D adjoint takes damping and poles but refuses PMC walls."""
     from meep_torch_b200._lib import MtbUnsupported
     from meep_torch_b200.core.adjoint3d import run_3d_adjoint
     from meep_torch_b200.core.monitors_3d import run_3d
@@ -1399,11 +1408,8 @@ def test_3d_damping_refused_by_fused_kernel_and_adjoint():
     s0 = init_3d_state(n, n, n, npml=3, device=dev())
     with pytest.raises(MtbUnsupported):
         run_3d(s0, c, 2, variant=1)
-    m = torch.zeros(n, n, n)
-    m[4:8, 4:8, 4:8] = 1.0
-    cp = build_3d_coeffs(n, n, n, 0.0625, npml=3, device=dev(), poles=[(0.5, 0.05, 2.0)],
-                         pole_masks=[m])
-    sp = init_3d_state(n, n, n, npml=3, device=dev(), n_poles=1)
+    cp = build_3d_coeffs(n, n, n, 0.0625, npml=3, device=dev(), pmc_axes=(1,))
+    sp = init_3d_state(n, n, n, npml=3, device=dev())
     with pytest.raises(MtbUnsupported):
         run_3d_adjoint(cp, 4, 2, None, [], lambda accs: torch.zeros(()), sp)
 

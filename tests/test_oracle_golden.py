@@ -232,11 +232,12 @@ def test_reference_gradient_matches_oracle_finite_differences(case):
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-16, (i, j, fd, ref)
 
 
-@pytest.mark.parametrize("case", ["grad3d", "grad3d_sigma"])
+@pytest.mark.parametrize("case", ["grad3d", "grad3d_sigma", "grad3d_poles"])
 def test_reference_3d_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps of run_3d_adjoint (float64) against central finite
     differences of the oracle's float64 3D run at two cells; the sigma case adds a
-    lossy slab (sigma_d) and a magnetically lossy patch (sigma_b)."""
+    lossy slab (sigma_d) and a magnetically lossy patch (sigma_b), the poles case a
+    Lorentz and a Drude pole on two boxes (cells inside both are probed)."""
     g = load_golden(f"{case}_f64")
     n, dx, npml, steps = int(g["n"]), float(g["dx"]), int(g["npml"]), int(g["n_steps"])
     freqs = [float(f) for f in g["freqs"]]
@@ -245,8 +246,12 @@ def test_reference_3d_gradient_matches_oracle_finite_differences(case):
     w = np.array([1.0, -0.7, 0.4])
 
     def J_of(eps):
+        kw = {}
+        if "poles" in g:
+            kw = dict(poles=[tuple(p) for p in json.loads(str(g["poles"]))],
+                      pole_masks=[g["pm0"], g["pm1"]])
         c = O.coeffs_3d(n, n, n, dx, eps=eps, npml=npml, dtype=np.float64,
-                        sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"))
+                        sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"), **kw)
         dt = c["dt"]
         mons = [lambda s, t: O.flux3d_sample(s, t, dt, freqs, "x", 15, (5, 15, 5, 15)),
                 lambda s, t: O.flux3d_sample(s, t, dt, freqs, "z", 6, (5, 15, 5, 15))]
@@ -258,7 +263,8 @@ def test_reference_3d_gradient_matches_oracle_finite_differences(case):
     eps = g["eps"].astype(np.float64)
     assert abs(J_of(eps) - float(g["L"])) <= 1e-9 * abs(float(g["L"]))
     h = 1e-4
-    for (i, j, k) in [(12, 9, 11), (14, 12, 8)]:
+    cells = [(12, 9, 11), (14, 12, 8)] + ([(9, 7, 10), (12, 11, 8)] if "poles" in g else [])
+    for (i, j, k) in cells:
         ep, em = eps.copy(), eps.copy()
         ep[i, j, k] += h
         em[i, j, k] -= h
