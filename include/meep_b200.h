@@ -502,7 +502,7 @@ typedef struct mtb_yee3d_struct {
     /* PMC walls instead of PEC on these axes (bit 0 x, 1 y, 2 z; core/stepper_3d.py
      * _term_pmc :99-121): the tangential E stays live at the wall and the curl term
      * that differentiates along the axis is zero there. Split and one-pass kernels;
-     * the register-staged march and the adjoint refuse it. */
+     * the adjoint take it; the register-staged march refuses it. */
     int32_t pmc_axes;
     float *pol_p[3][2];
     const float *pol_c3[3];

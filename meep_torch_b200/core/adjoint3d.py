@@ -11,7 +11,7 @@ E' = E + (dt curl + s) / eps_c needs the increment); the adjoint plan then sweep
 chunk's steps in reverse. ``chunk`` bounds that record (at most 32 steps are kept at a
 time); the gradient does not depend on it. Conductive damping and dispersive poles are
 transposed with the step (the pole recurrence is linear, so its adjoint needs no record
-of P); PMC walls are refused by the library.
+of P), and so are PMC walls.
 """
 from __future__ import annotations
 
@@ -34,9 +34,6 @@ def run_3d_adjoint(c, n_steps: int, chunk: int, source, monitors, loss_fn, state
     eps_src = c.eps
     cd = c._replace(eps=eps_src.detach())
     eng = Engine3D(state0, cd, source, monitors, point_sign=+1, ring_slots=K)
-    if eng.S.pmc_axes:
-        eng.close()
-        raise L.MtbUnsupported("3D adjoint: PMC walls are forward-only on the B200 path")
     rec = adj = None
     try:
         chunks = [(s0, min(K, n - s0)) for s0 in range(0, n, K)]
@@ -108,4 +105,4 @@ def run_3d_adjoint(c, n_steps: int, chunk: int, source, monitors, loss_fn, state
         eng.close()
     if eps_src.requires_grad:
         torch.autograd.backward(eps_src, g_eps.to(eps_src.dtype))
-    return float(loss), accs
+    return float(loss.detach()), accs

@@ -1,6 +1,6 @@
 // Discrete adjoint of the 3D CPML step for sm_100a (with conductive damping:
-// H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps, and dispersive poles, whose
-// recurrence is linear with eps-free coefficients): the exact transpose of
+// H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps, dispersive poles, whose
+// recurrence is linear with eps-free coefficients, and PMC walls): the exact transpose of
 // the split H / E update (core/stepper_3d.py:363-437, the same arithmetic as
 // k_yee3d_h / k_yee3d_e) and of the plane sampling (core/monitors_3d.py:70-189)
 // -- the reverse sweep of the reference's run_3d_adjoint
@@ -42,6 +42,7 @@ struct Adj3 {
     const float *c3[3];           // pole drives per E component (np box planes each)
     float c1[MTB_MAX_POLES], c2[MTB_MAX_POLES];
     int np;                       // dispersive poles (0: none)
+    int pmc;                      // PMC walls: bit 0 x, 1 y, 2 z
     int nx, ny, nz, zp;
     float dt, rdx;
 };
@@ -165,6 +166,9 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             }
         }
     }
+    // PMC walls (core/stepper_3d.py _term_pmc :99-121): the tangential E on the wall is
+    // live, and there the term differentiating along the wall's axis is zero
+    const bool iL = iin || (P.pmc & 1), jL = jin || (P.pmc & 2);
     // E-side profiles (1, 0) on inert nodes
     const float exb = prof(P.pb[0][1], iin, 1.f, i), exa = prof(P.pa[0][1], iin, 0.f, i);
     const float eyb = prof(P.pb[1][1], jin, 1.f, j), eya = prof(P.pa[1][1], jin, 0.f, j);
@@ -173,10 +177,11 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
     for (int q = 0; q < 4; ++q) {
         const int k = kb + q;
         const bool vzE = k < nz, vz = k <= nz - 2, kin = k >= 1 && k <= nz - 2;
+        const bool kL = kin || (P.pmc & 4);
         const float ezb = prof(P.pb[2][1], kin, 1.f, k), eza = prof(P.pa[2][1], kin, 0.f, k);
         // Ex: valid i <= nx-2, k < nz; curl on j, k interior
         {
-            const bool v = xok && vzE, in = v && jin && kin;
+            const bool v = xok && vzE, in = v && jL && kL;
             const float e_x = 0.5f * (ep[q] + epi[q]);
             const float gE = ge[0][q];
             t[6][q] = v ? -gE * (en[0][q] - d1[0][q] * eo[0][q]) / e_x : 0.f;
@@ -186,12 +191,12 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const bool u6 = v && jin, u7 = v && kin;
             gp[0][q] = u6 ? eyb * g6 : gp[0][q];
             gp[1][q] = u7 ? ezb * g7 : gp[1][q];
-            t[0][q] = (v ? gc : 0.f) + (u6 ? eya * g6 : 0.f);      // dy(Hz)
-            t[1][q] = (v ? -gc : 0.f) + (u7 ? eza * g7 : 0.f);     // dz(Hy)
+            t[0][q] = u6 ? gc + eya * g6 : 0.f;                    // dy(Hz)
+            t[1][q] = u7 ? -gc + eza * g7 : 0.f;                   // dz(Hy)
         }
         // Ey: valid j <= ny-2, k < nz; curl on i, k interior
         {
-            const bool v = vyH && vzE, in = v && iin && kin;
+            const bool v = vyH && vzE, in = v && iL && kL;
             const float e_y = 0.5f * (ep[q] + epj[q]);
             const float gE = ge[1][q];
             t[7][q] = v ? -gE * (en[1][q] - d1[1][q] * eo[1][q]) / e_y : 0.f;
@@ -201,12 +206,12 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const bool u8 = v && kin, u9 = v && iin;
             gp[2][q] = u8 ? ezb * g8 : gp[2][q];
             gp[3][q] = u9 ? exb * g9 : gp[3][q];
-            t[2][q] = (v ? gc : 0.f) + (u8 ? eza * g8 : 0.f);      // dz(Hx)
-            t[3][q] = (v ? -gc : 0.f) + (u9 ? exa * g9 : 0.f);     // dx(Hz)
+            t[2][q] = u8 ? gc + eza * g8 : 0.f;                    // dz(Hx)
+            t[3][q] = u9 ? -gc + exa * g9 : 0.f;                   // dx(Hz)
         }
         // Ez: valid k <= nz-2; curl on i, j interior
         {
-            const bool v = vz, in = v && iin && jin;
+            const bool v = vz, in = v && iL && jL;
             const float e_z = 0.5f * (ep[q] + ((q < 3) ? ep[q + 1] : epk));
             const float gE = ge[2][q];
             t[8][q] = v ? -gE * (en[2][q] - d1[2][q] * eo[2][q]) / e_z : 0.f;
@@ -216,8 +221,8 @@ __global__ void __launch_bounds__(32 * A3Y) k_adj3_e(const __grid_constant__ Adj
             const bool u10 = v && iin, u11 = v && jin;
             gp[4][q] = u10 ? exb * g10 : gp[4][q];
             gp[5][q] = u11 ? eyb * g11 : gp[5][q];
-            t[4][q] = (v ? gc : 0.f) + (u10 ? exa * g10 : 0.f);    // dx(Hy)
-            t[5][q] = (v ? -gc : 0.f) + (u11 ? eya * g11 : 0.f);   // dy(Hx)
+            t[4][q] = u10 ? gc + exa * g10 : 0.f;                  // dx(Hy)
+            t[5][q] = u11 ? -gc + eya * g11 : 0.f;                 // dy(Hx)
         }
     }
     for (int c = 0; c < 6; ++c) s4(B.g_psi[6 + c] + g, gp[c]);
@@ -404,7 +409,7 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
                             "16-byte aligned");
     if (S.n_poles < 0 || S.n_poles > MTB_MAX_POLES)
         return fail(MTB_INVALID_ARG, "3D adjoint: n_poles %d", S.n_poles);
-    if (S.pmc_axes) return fail(MTB_UNSUPPORTED, "3D adjoint: PMC walls are forward-only");
+    if (S.pmc_axes & ~7) return fail(MTB_INVALID_ARG, "3D adjoint: pmc_axes %d", S.pmc_axes);
     if (S.nx < 3 || S.ny < 3 || S.nz < 3 || S.zpitch < S.nz || (S.zpitch & 3))
         return fail(MTB_INVALID_ARG, "3D adjoint: bad grid");
     if ((int64_t)S.nx * S.ny * S.zpitch >= (1LL << 31) || S.nx > 65535 ||
@@ -442,6 +447,7 @@ int mtb_yee3d_adjoint_create(const mtb_yee3d_struct *s, const mtb_adj3d_buffers 
     for (int c = 0; c < 6; ++c)
         for (int h = 0; h < 2; ++h) A.dmp[c][h] = S.damp[c][h];
     A.np = S.n_poles;
+    A.pmc = S.pmc_axes;
     for (int c = 0; c < 3; ++c) A.c3[c] = S.n_poles ? S.pol_c3[c] : nullptr;
     for (int p = 0; p < MTB_MAX_POLES; ++p) {
         A.c1[p] = p < S.n_poles ? S.pol_c1[p] : 0.f;

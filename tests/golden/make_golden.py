@@ -15,7 +15,8 @@ cases of the hot path through its own public functions:
 * the design chain (``conic_filter``, ``tanh_projection``, ``MaterialGrid``,
   ``DesignRegion``, ``OptimizationProblem``; ``python make_golden.py design``)
 * d J / d eps of ``run_3d_adjoint`` (core/adjoint3d.py:56; ``make_golden.py grad3d``,
-  with conductive damping ``grad3d_sigma``, with poles ``grad3d_poles``) and of ``run_te``
+  with conductive damping ``grad3d_sigma``, with poles ``grad3d_poles``, with PMC walls
+  ``grad3d_pmc``) and of ``run_te``
   (``make_golden.py grad_te``)
 * the TM and TE cases with an electric conductivity map (``sigma_d``;
   ``make_golden.py sigma``) and with magnetic conductivity and permeability maps
@@ -567,11 +568,12 @@ def design_case():
                 box=np.array(reg.box), rho0=_np(rho0), f0=f0, grad=grad)
 
 
-def grad3d_case(prec, sigma=False, poles=False):
+def grad3d_case(prec, sigma=False, poles=False, pmc=False):
     """d J / d eps of the reference's run_3d_adjoint (core/adjoint3d.py:56) on a
     small CPML grid with spheres, an Ez point dipole and two flux faces; ``sigma`` adds a
     lossy slab (sigma_d) and a magnetically lossy patch (sigma_b), ``poles`` a Lorentz
-    and a Drude pole on two boxes inside the CPML layers."""
+    and a Drude pole on two boxes inside the CPML layers, ``pmc`` PMC walls on y (no y
+    CPML) with the dipole moved next to the low wall."""
     from meep_torch.core.adjoint3d import run_3d_adjoint
     rng = np.random.default_rng(13)
     n, dx, npml = 20, 1.0 / 16, 4
@@ -598,8 +600,13 @@ def grad3d_case(prec, sigma=False, poles=False):
         pm[1][11:15, 9:15, 6:11] = 1.0
         kw = dict(poles=POLES3, pole_masks=[torch.tensor(m, dtype=DT[prec]) for m in pm])
         out_extra = dict(pm0=pm[0], pm1=pm[1], poles=json.dumps(POLES3))
+    src_ijk = (10, 9, 11)
+    if pmc:
+        kw = dict(pmc_axes=(1,))
+        out_extra = dict(pmc_axes=np.array([1]))
+        src_ijk = (10, 1, 11)
     c = build_3d_coeffs(n, n, n, dx, eps=e, npml=npml, device="cpu", **kw)
-    src = PointSource3D(c.dt, "Ez", 10, 9, 11, GaussianPulse(0.9, 0.6))
+    src = PointSource3D(c.dt, "Ez", *src_ijk, GaussianPulse(0.9, 0.6))
     freqs = [0.7, 0.9, 1.1]
     mons = [FluxMonitor3D(c.dt, freqs, normal="x", idx=15, win=(5, 15, 5, 15)),
             FluxMonitor3D(c.dt, freqs, normal="z", idx=6, win=(5, 15, 5, 15))]
@@ -614,7 +621,7 @@ def grad3d_case(prec, sigma=False, poles=False):
                        n_poles=len(POLES3) if poles else 0)
     n_steps, chunk = 70, 25
     L, accs = run_3d_adjoint(c, n_steps, chunk, src, mons, loss_fn, s0)
-    return dict(n=n, dx=dx, npml=npml, eps=eps, freqs=np.array(freqs), src=np.array([10, 9, 11]),
+    return dict(n=n, dx=dx, npml=npml, eps=eps, freqs=np.array(freqs), src=np.array(src_ijk),
                 fcen=0.9, fwidth=0.6, n_steps=n_steps, chunk=chunk, L=float(L),
                 grad=_np(e.grad), acc_0=_np(accs[0]), acc_1=_np(accs[1]), **out_extra)
 
@@ -707,6 +714,10 @@ def main():
     if sys.argv[1:] == ["grad3d_poles"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad3d_poles_f64.npz"),
                             **grad3d_case("f64", poles=True))
+        return
+    if sys.argv[1:] == ["grad3d_pmc"]:
+        np.savez_compressed(os.path.join(HERE, "golden_grad3d_pmc_f64.npz"),
+                            **grad3d_case("f64", pmc=True))
         return
     if sys.argv[1:] == ["grad_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad_tm_pmc_f64.npz"),

@@ -870,13 +870,14 @@ def test_magnetic_sheet_sources_match_oracle(case):
     assert all(v < TOL for v in errs.values()), errs
 
 
-@pytest.mark.parametrize("case", ["sigma", "poles"])
+@pytest.mark.parametrize("case", ["sigma", "poles", "pmc"])
 def test_3d_lossy_gradient_matches_reference_run_3d_adjoint(case):
     """d J / d eps of run_3d_adjoint with conductive damping (a sigma_d slab, a sigma_b
-    patch: H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps) or with a Lorentz and a Drude
-    pole (P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n), folded-D E update) on the 3D adjoint
-    kernels against the reference's float64 run_3d_adjoint (tests/golden/make_golden.py
-    grad3d_sigma / grad3d_poles, pinned by central differences of the oracle)."""
+    patch: H' = d1 H - d2 curl, E' = d1 E + d2 curl / eps), with a Lorentz and a Drude
+    pole (P(n+1) = c1 P(n) + c2 P(n-1) + c3 E(n), folded-D E update) or with PMC walls on
+    y (the dipole next to one) on the 3D adjoint kernels against the reference's float64
+    run_3d_adjoint (tests/golden/make_golden.py grad3d_sigma / grad3d_poles / grad3d_pmc,
+    pinned by central differences of the oracle)."""
     from meep_torch_b200.core.adjoint3d import run_3d_adjoint
     from meep_torch_b200.core.monitors_3d import FluxMonitor3D, PointSource3D
     from meep_torch_b200.core.sources import GaussianPulse
@@ -887,6 +888,9 @@ def test_3d_lossy_gradient_matches_reference_run_3d_adjoint(case):
     if case == "sigma":
         kw = dict(sigma_d=torch.tensor(g64["sigma_d"], dtype=torch.float32),
                   sigma_b=torch.tensor(g64["sigma_b"], dtype=torch.float32))
+        n_p = 0
+    elif case == "pmc":
+        kw = dict(pmc_axes=tuple(int(a) for a in g64["pmc_axes"]))
         n_p = 0
     else:
         poles = [tuple(p) for p in json.loads(str(g64["poles"]))]
@@ -1394,11 +1398,10 @@ def test_te_poles_batched_tiles_match_oracle_from_random_state():
     eng.close()
 
 
-def test_3d_damping_refused_by_fused_kernel_and_adjoint():
+def test_3d_damping_refused_by_fused_kernel():
     """Conductive damping runs on the split kernels only (the fused x-march refuses it
-    with MTB_UNSUPPORTED); the 3D adjoint takes damping and poles but refuses PMC walls."""
+    with MTB_UNSUPPORTED)."""
     from meep_torch_b200._lib import MtbUnsupported
-    from meep_torch_b200.core.adjoint3d import run_3d_adjoint
     from meep_torch_b200.core.monitors_3d import run_3d
     from meep_torch_b200.core.stepper_3d import build_3d_coeffs, init_3d_state
     n = 12
@@ -1408,10 +1411,6 @@ def test_3d_damping_refused_by_fused_kernel_and_adjoint():
     s0 = init_3d_state(n, n, n, npml=3, device=dev())
     with pytest.raises(MtbUnsupported):
         run_3d(s0, c, 2, variant=1)
-    cp = build_3d_coeffs(n, n, n, 0.0625, npml=3, device=dev(), pmc_axes=(1,))
-    sp = init_3d_state(n, n, n, npml=3, device=dev())
-    with pytest.raises(MtbUnsupported):
-        run_3d_adjoint(cp, 4, 2, None, [], lambda accs: torch.zeros(()), sp)
 
 
 def test_3d_poles_slabs_bitwise_equal_to_whole_grid():

@@ -232,12 +232,13 @@ def test_reference_gradient_matches_oracle_finite_differences(case):
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-16, (i, j, fd, ref)
 
 
-@pytest.mark.parametrize("case", ["grad3d", "grad3d_sigma", "grad3d_poles"])
+@pytest.mark.parametrize("case", ["grad3d", "grad3d_sigma", "grad3d_poles", "grad3d_pmc"])
 def test_reference_3d_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps of run_3d_adjoint (float64) against central finite
     differences of the oracle's float64 3D run at two cells; the sigma case adds a
     lossy slab (sigma_d) and a magnetically lossy patch (sigma_b), the poles case a
-    Lorentz and a Drude pole on two boxes (cells inside both are probed)."""
+    Lorentz and a Drude pole on two boxes (cells inside both are probed), the pmc case
+    PMC walls on y (cells on and next to the wall are probed)."""
     g = load_golden(f"{case}_f64")
     n, dx, npml, steps = int(g["n"]), float(g["dx"]), int(g["npml"]), int(g["n_steps"])
     freqs = [float(f) for f in g["freqs"]]
@@ -250,6 +251,8 @@ def test_reference_3d_gradient_matches_oracle_finite_differences(case):
         if "poles" in g:
             kw = dict(poles=[tuple(p) for p in json.loads(str(g["poles"]))],
                       pole_masks=[g["pm0"], g["pm1"]])
+        if "pmc_axes" in g:
+            kw = dict(pmc_axes=tuple(int(a) for a in g["pmc_axes"]))
         c = O.coeffs_3d(n, n, n, dx, eps=eps, npml=npml, dtype=np.float64,
                         sigma_d=g.get("sigma_d"), sigma_b=g.get("sigma_b"), **kw)
         dt = c["dt"]
@@ -263,7 +266,8 @@ def test_reference_3d_gradient_matches_oracle_finite_differences(case):
     eps = g["eps"].astype(np.float64)
     assert abs(J_of(eps) - float(g["L"])) <= 1e-9 * abs(float(g["L"]))
     h = 1e-4
-    cells = [(12, 9, 11), (14, 12, 8)] + ([(9, 7, 10), (12, 11, 8)] if "poles" in g else [])
+    cells = [(12, 9, 11), (14, 12, 8)] + ([(9, 7, 10), (12, 11, 8)] if "poles" in g else []) \
+        + ([(10, 0, 11), (11, 1, 10), (9, 19, 12)] if "pmc_axes" in g else [])
     for (i, j, k) in cells:
         ep, em = eps.copy(), eps.copy()
         ep[i, j, k] += h
