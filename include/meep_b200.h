@@ -194,7 +194,8 @@ typedef struct mtb_yee2d_struct {
      *      cell of the other cut (Rotate4, square grids).
      * The caller packs the E-side CPML memory and the (b, a) node profiles
      * from the cut row (offset 0). Tile kernels only (variant 2); the other
-     * variants, the no-alloc entry and the adjoint return MTB_UNSUPPORTED. */
+     * variants and the no-alloc entry return MTB_UNSUPPORTED, the adjoint takes
+     * TM cut 1 and returns MTB_UNSUPPORTED for cut 2 and for TE cuts. */
     int32_t cut_y, cut_x;
     int32_t cut_map_y, cut_map_x;
     float cut_ph_y, cut_ph_x;
@@ -501,8 +502,8 @@ typedef struct mtb_yee3d_struct {
     int32_t n_poles;
     /* PMC walls instead of PEC on these axes (bit 0 x, 1 y, 2 z; core/stepper_3d.py
      * _term_pmc :99-121): the tangential E stays live at the wall and the curl term
-     * that differentiates along the axis is zero there. Split and one-pass kernels;
-     * the adjoint take it; the register-staged march refuses it. */
+     * that differentiates along the axis is zero there. The split and one-pass
+     * kernels and the adjoint take it; the register-staged march refuses it. */
     int32_t pmc_axes;
     float *pol_p[3][2];
     const float *pol_c3[3];

@@ -23,7 +23,7 @@ import ctypes as C
 import torch
 
 from . import _lib as L
-from .engine2d import Engine2D
+from .engine2d import Engine2D, _cuts
 
 STATE_TM = ("Ez", "Hx", "Hy", "Dz", "psi_Ezy", "psi_Ezx", "psi_Hyx", "psi_Hxy")
 STATE_TE = ("Hz", "Ex", "Ey", "Dx", "Dy", "psi_Hzy", "psi_Hzx", "psi_Eyx", "psi_Exy")
@@ -49,9 +49,12 @@ class GradRun2D:
     def __init__(self, state, coeffs, n_steps, source, monitors, chunk=32,
                  phase_mode="exact"):
         self.te = hasattr(state, "Hz")
-        if any(getattr(coeffs, k, 0) for k in ("y_mirror_lo", "x_mirror_lo", "y_rot2_lo",
-                                               "rot4_lo")):
-            raise L.MtbUnsupported("gradients: symmetry cuts are forward-only")
+        # TM even mirrors (zero H ghost) and TE odd mirrors (CPML profiles only) have
+        # gradients; the live on-plane lines and the TE even-mirror row do not
+        cy, cx = _cuts(coeffs, self.te)
+        if 2 in (cy[0], cx[0]) or (self.te and (cy[0] or cx[0])):
+            raise L.MtbUnsupported("gradients: odd TM mirrors, rotations and TE even mirrors "
+                                   "are forward-only")
         self.names = STATE_TE if self.te else STATE_TM
         self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
         self.source, self.monitors = source, list(monitors)

@@ -106,7 +106,8 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
     ldv(S.inv_eps_a + g, ie);
     ldv(B.g_eps[0] + g, ge);
     inject(S, L, MTB_C2_MAIN, i, jb, g, radj, gez);
-    const bool rowin = i >= 1 && i <= nx - 2;
+    // an even x mirror (cut_x 1, zero H ghost beyond the cut) makes the cut row live
+    const bool rowin = (i >= 1 || S.cut_x) && i <= nx - 2;
     float bex = 1.f, aex = 0.f;
     if (rowin) { bex = S.ex_b[i]; aex = S.ex_a[i]; }
     // electric conductivity: D' = d1 D + d2 pad(curl)
@@ -140,9 +141,10 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
         const bool inside = j < ny;
-        // the curl of the D update: interior columns, or every column under PMC walls in
-        // y (zero H beyond both walls, core/stepper_tm.py:143-145)
-        const bool interior = rowin && (S.y_pmc ? j < ny : (j >= 1 && j <= ny - 2));
+        // the curl of the D update: interior columns, every column under PMC walls in y
+        // (zero H beyond both walls, core/stepper_tm.py:143-145), or from the cut column
+        // up under an even y mirror (zero H ghost beyond the cut, :146-148)
+        const bool interior = rowin && (S.y_pmc ? j < ny : ((j >= 1 || S.cut_y) && j <= ny - 2));
         const float gd = gdz[q] + gez[q] * ie[q];
         ge[q] -= gez[q] * ez[q] * ie[q];
         const float gc = interior ? d2[q] * gd : 0.f;
@@ -594,8 +596,13 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     *out = nullptr;
     const mtb_yee2d_struct &S = *s;
     if (S.pol != MTB_TM && S.pol != MTB_TE) return fail(MTB_INVALID_ARG, "adjoint: bad pol");
-    if (S.cut_y || S.cut_x)
-        return fail(MTB_UNSUPPORTED, "adjoint: symmetry cuts are forward-only");
+    if (S.cut_y < 0 || S.cut_y > 2 || S.cut_x < 0 || S.cut_x > 2)
+        return fail(MTB_INVALID_ARG, "adjoint: cut_y / cut_x must be 0, 1 or 2");
+    if (S.cut_y == 2 || S.cut_x == 2)
+        return fail(MTB_UNSUPPORTED, "adjoint: odd mirrors and rotations are forward-only");
+    if ((S.cut_y || S.cut_x) && S.pol != MTB_TM)
+        return fail(MTB_UNSUPPORTED, "adjoint: TE even mirrors are forward-only");
+    if (S.cut_y && S.y_pmc) return fail(MTB_INVALID_ARG, "adjoint: cut_y with y_pmc");
     if (S.y_pmc && S.pol != MTB_TM) return fail(MTB_INVALID_ARG, "adjoint: y_pmc is TM only");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");
     if (S.n_mpoles) return fail(MTB_UNSUPPORTED, "adjoint: magnetic poles are forward-only");

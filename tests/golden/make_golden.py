@@ -490,7 +490,8 @@ def grad_tm_case(prec, extra=None):
     """d J / d eps through the reference's autograd (run_tm with
     checkpoint_every, core/run.py:81-120) on the TM case's geometry; ``extra`` =
     "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole,
-    "pmc" PMC walls in y."""
+    "pmc" PMC walls in y, "mirror" even mirror cuts on the low x and y edges (the CPML
+    only on the far sides)."""
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
     eps = np.ones((nx, ny))
@@ -512,6 +513,9 @@ def grad_tm_case(prec, extra=None):
         out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
     if extra == "pmc":
         kw, out_extra = dict(y_pmc=True), dict(y_pmc=1)
+    folds = dict(y_mirror=1, x_mirror=1) if extra == "mirror" else {}
+    if folds:
+        kw, out_extra = dict(folds), dict(fold=json.dumps(folds))
     m = build_tm_coeffs(g, eps_inf=e, npml=npml, **kw)
     src = LineSource(g, ix=12, j0=10, j1=26, profile=GaussianPulse(0.65, 0.4))
     freqs = [0.55, 0.65, 0.75]
@@ -520,7 +524,7 @@ def grad_tm_case(prec, extra=None):
     dft = DFTFieldsMonitor(g, freqs, component="Ez")
     n, ce = 200, 50
     s0 = init_tm_state(g, n_poles=len(POLES) if extra == "poles" else 0,
-                       y_pmc=extra == "pmc")
+                       y_pmc=extra == "pmc", **folds)
     st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft],
                               checkpoint_every=ce)
     J = grad_loss(st, ax, ay, ad, monx, mony, dx)
@@ -639,7 +643,7 @@ def grad_te_case(prec, extra=None):
     """d J / d eps_inf through the reference's autograd of run_te
     (checkpoint_every, core/run.py:81-120) on the TE case's geometry; ``extra`` =
     "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole on
-    both E axes."""
+    both E axes, "mirror" odd mirror cuts on the low x and y edges."""
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -658,6 +662,9 @@ def grad_te_case(prec, extra=None):
         pm = pole_masks(nx, ny)
         kw = dict(poles=POLES, pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
         out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
+    elif extra == "mirror":
+        folds = dict(y_mirror=-1, x_mirror=-1)
+        kw, out_extra = dict(folds), dict(fold=json.dumps(folds))
     m = build_te_coeffs(g, eps_inf=e, npml=npml, **kw)
     line = LineSource(g, ix=12, j0=14, j1=26, profile=GaussianPulse(0.65, 0.4))
 
@@ -718,6 +725,12 @@ def main():
     if sys.argv[1:] == ["grad3d_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad3d_pmc_f64.npz"),
                             **grad3d_case("f64", pmc=True))
+        return
+    if sys.argv[1:] == ["grad_mirror"]:
+        np.savez_compressed(os.path.join(HERE, "golden_grad_tm_mirror_f64.npz"),
+                            **grad_tm_case("f64", "mirror"))
+        np.savez_compressed(os.path.join(HERE, "golden_grad_te_mirror_f64.npz"),
+                            **grad_te_case("f64", "mirror"))
         return
     if sys.argv[1:] == ["grad_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad_tm_pmc_f64.npz"),

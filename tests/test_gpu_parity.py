@@ -728,6 +728,8 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
     pmc = extra == "pmc"
     if pmc:
         kw = dict(y_pmc=True)
+    folds = json.loads(str(g["fold"])) if "fold" in g else {}
+    kw.update(folds)
     m = build_tm_coeffs(grid, eps_inf=e, npml=npml, **kw)
     src = LineSource(grid, ix=int(g["src_ix"]), j0=int(g["src_j0"]), j1=int(g["src_j1"]),
                      profile=GaussianPulse(float(g["fcen"]), float(g["fwidth"])))
@@ -737,7 +739,7 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
     monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=mx[0], lo=mx[1], hi=mx[2])
     mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=my[0], lo=my[1], hi=my[2])
     dft = DFTFieldsMonitor(grid, freqs, "Ez")
-    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p, y_pmc=pmc), dx
+    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p, y_pmc=pmc, **folds), dx
 
 
 def _grad_loss(st, ax, ay, ad, mx, my, dx):
@@ -768,11 +770,12 @@ def test_tm_gradient_matches_reference_autograd(chunk):
     assert e32 < 1e-4, e32
 
 
-@pytest.mark.parametrize("extra", ["lossy", "poles", "pmc"])
+@pytest.mark.parametrize("extra", ["lossy", "poles", "pmc", "mirror"])
 @pytest.mark.parametrize("chunk", [50, 13])
 def test_tm_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
     """d J / d eps of lossy (sigma_d on E, sigma_b and mu on H), dispersive (a
-    Lorentz and a Drude pole) and y-PMC TM runs from the adjoint kernels, against the reference's
+    Lorentz and a Drude pole), y-PMC and even-mirror (cuts on the low x and y edges) TM
+    runs from the adjoint kernels, against the reference's
     float64 autograd through run_tm(checkpoint_every=50) (tests/golden/make_golden.py
     grad_extra); the float32 forward and adjoint agree with it to 1e-4."""
     from meep_torch_b200.core.run import run_tm
@@ -994,11 +997,33 @@ def test_te_gradient_matches_reference_autograd(chunk):
     assert e32 < TOL, e32
 
 
+def test_gradients_of_live_cut_lines_refused():
+    """Gradients of TM odd mirrors (a live on-plane H line) and of TE even mirrors (the
+    2 Hz / dx cut row) raise MtbUnsupported before any device work."""
+    from meep_torch_b200._lib import MtbUnsupported
+    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.grid import Grid
+    from meep_torch_b200.core.monitors import DFTFieldsMonitor
+    from meep_torch_b200.core.run import run_te, run_tm
+    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.stepper_tm import init_tm_state
+    grid = Grid(nx=32, ny=32, dx=0.05, device=dev())
+    eps = torch.ones(32, 32, device=dev(), requires_grad=True)
+    m = build_tm_coeffs(grid, eps_inf=eps, npml=6, y_mirror=-1)
+    with pytest.raises(MtbUnsupported):
+        run_tm(init_tm_state(grid, y_mirror=-1), m, 4,
+               monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
+    m = build_te_coeffs(grid, eps_inf=eps, npml=6, x_mirror=1)
+    with pytest.raises(MtbUnsupported):
+        run_te(init_te_state(grid), m, 4, monitors=[DFTFieldsMonitor(grid, [0.5], "Hz")])
+
+
 @pytest.mark.parametrize("chunk", [60, 32])
-@pytest.mark.parametrize("extra", ["lossy", "poles"])
+@pytest.mark.parametrize("extra", ["lossy", "poles", "mirror"])
 def test_te_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
-    """d J / d eps_inf of lossy (sigma_d on Dx / Dy, sigma_b and mu on Hz) and
-    dispersive (a Lorentz and a Drude pole on Ex and Ey) TE runs from the adjoint kernels,
+    """d J / d eps_inf of lossy (sigma_d on Dx / Dy, sigma_b and mu on Hz), dispersive
+    (a Lorentz and a Drude pole on Ex and Ey) and odd-mirror (cuts on the low x and y
+    edges: CPML profiles only) TE runs from the adjoint kernels,
     against the reference's float64 autograd through run_te(checkpoint_every=60)
     (tests/golden/make_golden.py grad_extra_te, pinned by central differences of the
     oracle); the float32 forward and adjoint agree with it to 1e-4."""
@@ -1016,6 +1041,8 @@ def test_te_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk)
     kw, n_p = {}, 0
     if extra == "lossy":
         kw = dict(sigma_d=T(g64["sigma"]), sigma_b=T(g64["sigma_b"]), mu=T(g64["mu"]))
+    elif extra == "mirror":
+        kw = json.loads(str(g64["fold"]))
     else:
         poles = json.loads(str(g64["poles"]))
         kw = dict(poles=poles, pole_masks=[T(x) for x in g64["pole_masks"]])

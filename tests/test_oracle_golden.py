@@ -185,17 +185,20 @@ def test_3d_lean_sign_convention(case, prec):
         assert rel_l2(a, g[f"acc_{n}"]) < tol
 
 
-@pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles", "grad_tm_pmc"])
+@pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles", "grad_tm_pmc",
+                                  "grad_tm_mirror"])
 def test_reference_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps (reference autograd, float64) against central
     finite differences of the oracle's float64 run at a few pixels; the lossy case
-    adds sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole (the
-    gradients a future adjoint of those runs must reproduce)."""
+    adds sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole, the
+    mirror one even mirror cuts on the low edges (pixels on the cuts are probed)."""
     g = load_golden(f"{case}_f64")
     extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"),
                  y_pmc=bool(g.get("y_pmc", 0)))
     if "poles" in g:
         extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
+    if "fold" in g:
+        extra.update(json.loads(str(g["fold"])))
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
                            int(g["n_steps"]))
     freqs = [float(f) for f in g["freqs"]]
@@ -223,7 +226,8 @@ def test_reference_gradient_matches_oracle_finite_differences(case):
     eps = g["eps"].astype(np.float64)
     assert abs(J_of(eps) - float(g["J"])) <= 1e-9 * abs(float(g["J"]))
     h = 1e-4
-    for (i, j) in [(33, 24), (24, 17), (36, 12)]:
+    cells = [(33, 24), (24, 17), (36, 12)] + ([(0, 14), (10, 0), (0, 0)] if "fold" in g else [])
+    for (i, j) in cells:
         ep, em = eps.copy(), eps.copy()
         ep[i, j] += h
         em[i, j] -= h
@@ -277,16 +281,18 @@ def test_reference_3d_gradient_matches_oracle_finite_differences(case):
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-12, (i, j, k, fd, ref)
 
 
-@pytest.mark.parametrize("case", ["grad_te", "grad_te_lossy", "grad_te_poles"])
+@pytest.mark.parametrize("case", ["grad_te", "grad_te_lossy", "grad_te_poles", "grad_te_mirror"])
 def test_reference_te_gradient_matches_oracle_finite_differences(case):
     """The golden TE d J / d eps_inf (reference autograd, float64) against central
     finite differences of the oracle's float64 TE run at two pixels; the lossy case adds
     sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole on both E
-    axes."""
+    axes, the mirror one odd mirror cuts on the low edges (pixels on the cuts probed)."""
     g = load_golden(f"{case}_f64")
     extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"))
     if "poles" in g:
         extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
+    if "fold" in g:
+        extra.update(json.loads(str(g["fold"])))
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
                            int(g["n_steps"]))
     freqs = [float(f) for f in g["freqs"]]
@@ -314,7 +320,7 @@ def test_reference_te_gradient_matches_oracle_finite_differences(case):
     eps = g["eps"].astype(np.float64)
     assert abs(J_of(eps) - float(g["J"])) <= 1e-9 * abs(float(g["J"]))
     h = 1e-4
-    for (i, j) in [(30, 26), (20, 18)]:
+    for (i, j) in [(30, 26), (20, 18)] + ([(0, 15), (12, 0)] if "fold" in g else []):
         ep, em = eps.copy(), eps.copy()
         ep[i, j] += h
         em[i, j] -= h
