@@ -195,7 +195,7 @@ typedef struct mtb_yee2d_struct {
      * The caller packs the E-side CPML memory and the (b, a) node profiles
      * from the cut row (offset 0). Tile kernels only (variant 2); the other
      * variants and the no-alloc entry return MTB_UNSUPPORTED, the adjoint takes
-     * TM cut 1 and returns MTB_UNSUPPORTED for cut 2 and for TE cuts. */
+     * cut 1 and returns MTB_UNSUPPORTED for cut 2. */
     int32_t cut_y, cut_x;
     int32_t cut_map_y, cut_map_x;
     float cut_ph_y, cut_ph_x;

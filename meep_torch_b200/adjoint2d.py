@@ -49,12 +49,12 @@ class GradRun2D:
     def __init__(self, state, coeffs, n_steps, source, monitors, chunk=32,
                  phase_mode="exact"):
         self.te = hasattr(state, "Hz")
-        # TM even mirrors (zero H ghost) and TE odd mirrors (CPML profiles only) have
-        # gradients; the live on-plane lines and the TE even-mirror row do not
+        # TM even mirrors (zero H ghost) and TE mirrors (the even one's 2 Hz / dx cut row;
+        # the odd one changes only CPML profiles) have gradients; the TM live on-plane H
+        # lines (odd mirrors, rotations) do not
         cy, cx = _cuts(coeffs, self.te)
-        if 2 in (cy[0], cx[0]) or (self.te and (cy[0] or cx[0])):
-            raise L.MtbUnsupported("gradients: odd TM mirrors, rotations and TE even mirrors "
-                                   "are forward-only")
+        if 2 in (cy[0], cx[0]):
+            raise L.MtbUnsupported("gradients: odd TM mirrors and rotations are forward-only")
         self.names = STATE_TE if self.te else STATE_TM
         self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
         self.source, self.monitors = source, list(monitors)

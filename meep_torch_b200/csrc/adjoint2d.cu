@@ -421,16 +421,21 @@ __device__ __forceinline__ void adj_te_e_cell(const mtb_yee2d_struct &S, const m
         const float gdY = gdy[q] + gY[q] * iy[q];
         gex_e[q] -= xrow ? gX[q] * ex[q] * ix[q] : 0.f;
         gey_e[q] -= gY[q] * ey[q] * iy[q];
-        // Dx' = d1x Dx + d2x (d + psi0'): the curl on i <= nx-2, 1 <= j <= ny-2
+        // Dx' = d1x Dx + d2x (d + psi0'): the curl on i <= nx-2, 1 <= j <= ny-2; an even
+        // y mirror adds the cut row j = 0 with curl 2 Hz / dx and no psi
+        // (core/stepper_te.py:87-93), whose transpose is 2 c0 on the Hz difference slot
         const bool vx = xrow && j >= 1 && j <= ny - 2;
+        const bool cy = xrow && j == 0 && S.cut_y == 1;
         const float eyb = vx ? S.ey_b[j] : 1.f, eya = vx ? S.ey_a[j] : 0.f;
         const float c0 = dx2[q] * gdX, g0 = gp0[q] + c0;
-        t2[q] = vx ? c0 + eya * g0 : 0.f;
+        t2[q] = vx ? c0 + eya * g0 : (cy ? 2.f * c0 : 0.f);
         gp0[q] = vx ? eyb * g0 : gp0[q];
-        // Dy' = d1y Dy - d2y (d + psi1'): the curl on 1 <= i <= nx-2, j <= ny-2
+        // Dy' = d1y Dy - d2y (d + psi1'): the curl on 1 <= i <= nx-2, j <= ny-2; an even
+        // x mirror adds the cut row i = 0 the same way (:94-96)
         const bool vy = yrow && j <= ny - 2;
+        const bool cx = i == 0 && S.cut_x == 1 && j <= ny - 2;
         const float c1 = -dy2[q] * gdY, g1 = gp1[q] + c1;
-        t3[q] = vy ? c1 + exa * g1 : 0.f;
+        t3[q] = vy ? c1 + exa * g1 : (cx ? 2.f * c1 : 0.f);
         gp1[q] = vy ? exb * g1 : gp1[q];
         gdx[q] = dx1[q] * gdX;
         gdy[q] = dy1[q] * gdY;
@@ -600,8 +605,6 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
         return fail(MTB_INVALID_ARG, "adjoint: cut_y / cut_x must be 0, 1 or 2");
     if (S.cut_y == 2 || S.cut_x == 2)
         return fail(MTB_UNSUPPORTED, "adjoint: odd mirrors and rotations are forward-only");
-    if ((S.cut_y || S.cut_x) && S.pol != MTB_TM)
-        return fail(MTB_UNSUPPORTED, "adjoint: TE even mirrors are forward-only");
     if (S.cut_y && S.y_pmc) return fail(MTB_INVALID_ARG, "adjoint: cut_y with y_pmc");
     if (S.y_pmc && S.pol != MTB_TM) return fail(MTB_INVALID_ARG, "adjoint: y_pmc is TM only");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");

@@ -643,7 +643,8 @@ def grad_te_case(prec, extra=None):
     """d J / d eps_inf through the reference's autograd of run_te
     (checkpoint_every, core/run.py:81-120) on the TE case's geometry; ``extra`` =
     "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole on
-    both E axes, "mirror" odd mirror cuts on the low x and y edges."""
+    both E axes, "mirror" / "mirror_even" odd / even mirror cuts on the low x and y
+    edges."""
     rng = np.random.default_rng(12)
     nx, ny, dx, npml = 44, 40, 0.05, 8
     eps = np.ones((nx, ny))
@@ -662,8 +663,9 @@ def grad_te_case(prec, extra=None):
         pm = pole_masks(nx, ny)
         kw = dict(poles=POLES, pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
         out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
-    elif extra == "mirror":
-        folds = dict(y_mirror=-1, x_mirror=-1)
+    elif extra in ("mirror", "mirror_even"):
+        folds = dict(y_mirror=-1, x_mirror=-1) if extra == "mirror" else dict(y_mirror=1,
+                                                                              x_mirror=1)
         kw, out_extra = dict(folds), dict(fold=json.dumps(folds))
     m = build_te_coeffs(g, eps_inf=e, npml=npml, **kw)
     line = LineSource(g, ix=12, j0=14, j1=26, profile=GaussianPulse(0.65, 0.4))
@@ -731,6 +733,8 @@ def main():
                             **grad_tm_case("f64", "mirror"))
         np.savez_compressed(os.path.join(HERE, "golden_grad_te_mirror_f64.npz"),
                             **grad_te_case("f64", "mirror"))
+        np.savez_compressed(os.path.join(HERE, "golden_grad_te_mirror_even_f64.npz"),
+                            **grad_te_case("f64", "mirror_even"))
         return
     if sys.argv[1:] == ["grad_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad_tm_pmc_f64.npz"),

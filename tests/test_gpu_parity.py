@@ -998,14 +998,13 @@ def test_te_gradient_matches_reference_autograd(chunk):
 
 
 def test_gradients_of_live_cut_lines_refused():
-    """Gradients of TM odd mirrors (a live on-plane H line) and of TE even mirrors (the
-    2 Hz / dx cut row) raise MtbUnsupported before any device work."""
+    """Gradients of TM odd mirrors and rotations (a live on-plane H line) raise
+    MtbUnsupported before any device work."""
     from meep_torch_b200._lib import MtbUnsupported
-    from meep_torch_b200.core.coeffs import build_te_coeffs, build_tm_coeffs
+    from meep_torch_b200.core.coeffs import build_tm_coeffs
     from meep_torch_b200.core.grid import Grid
     from meep_torch_b200.core.monitors import DFTFieldsMonitor
-    from meep_torch_b200.core.run import run_te, run_tm
-    from meep_torch_b200.core.stepper_te import init_te_state
+    from meep_torch_b200.core.run import run_tm
     from meep_torch_b200.core.stepper_tm import init_tm_state
     grid = Grid(nx=32, ny=32, dx=0.05, device=dev())
     eps = torch.ones(32, 32, device=dev(), requires_grad=True)
@@ -1013,17 +1012,18 @@ def test_gradients_of_live_cut_lines_refused():
     with pytest.raises(MtbUnsupported):
         run_tm(init_tm_state(grid, y_mirror=-1), m, 4,
                monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
-    m = build_te_coeffs(grid, eps_inf=eps, npml=6, x_mirror=1)
+    m = build_tm_coeffs(grid, eps_inf=eps, npml=6, rot4=1)
     with pytest.raises(MtbUnsupported):
-        run_te(init_te_state(grid), m, 4, monitors=[DFTFieldsMonitor(grid, [0.5], "Hz")])
+        run_tm(init_tm_state(grid, rot4=1), m, 4, monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
 
 
 @pytest.mark.parametrize("chunk", [60, 32])
-@pytest.mark.parametrize("extra", ["lossy", "poles", "mirror"])
+@pytest.mark.parametrize("extra", ["lossy", "poles", "mirror", "mirror_even"])
 def test_te_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
     """d J / d eps_inf of lossy (sigma_d on Dx / Dy, sigma_b and mu on Hz), dispersive
-    (a Lorentz and a Drude pole on Ex and Ey) and odd-mirror (cuts on the low x and y
-    edges: CPML profiles only) TE runs from the adjoint kernels,
+    (a Lorentz and a Drude pole on Ex and Ey), odd-mirror (cuts on the low x and y edges:
+    CPML profiles only) and even-mirror (the cut rows' 2 Hz / dx) TE runs from the
+    adjoint kernels,
     against the reference's float64 autograd through run_te(checkpoint_every=60)
     (tests/golden/make_golden.py grad_extra_te, pinned by central differences of the
     oracle); the float32 forward and adjoint agree with it to 1e-4."""
@@ -1041,7 +1041,7 @@ def test_te_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk)
     kw, n_p = {}, 0
     if extra == "lossy":
         kw = dict(sigma_d=T(g64["sigma"]), sigma_b=T(g64["sigma_b"]), mu=T(g64["mu"]))
-    elif extra == "mirror":
+    elif extra.startswith("mirror"):
         kw = json.loads(str(g64["fold"]))
     else:
         poles = json.loads(str(g64["poles"]))

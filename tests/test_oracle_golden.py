@@ -281,7 +281,8 @@ def test_reference_3d_gradient_matches_oracle_finite_differences(case):
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-12, (i, j, k, fd, ref)
 
 
-@pytest.mark.parametrize("case", ["grad_te", "grad_te_lossy", "grad_te_poles", "grad_te_mirror"])
+@pytest.mark.parametrize("case", ["grad_te", "grad_te_lossy", "grad_te_poles", "grad_te_mirror",
+                                  "grad_te_mirror_even"])
 def test_reference_te_gradient_matches_oracle_finite_differences(case):
     """The golden TE d J / d eps_inf (reference autograd, float64) against central
     finite differences of the oracle's float64 TE run at two pixels; the lossy case adds
