@@ -194,8 +194,8 @@ typedef struct mtb_yee2d_struct {
      *      cell of the other cut (Rotate4, square grids).
      * The caller packs the E-side CPML memory and the (b, a) node profiles
      * from the cut row (offset 0). Tile kernels only (variant 2); the other
-     * variants and the no-alloc entry return MTB_UNSUPPORTED, the adjoint takes
-     * cut 1 and returns MTB_UNSUPPORTED for cut 2. */
+     * variants and the no-alloc entry return MTB_UNSUPPORTED; the adjoint takes
+     * every cut (cut 2 with mtb_adj2d_buffers.g_cut). */
     int32_t cut_y, cut_x;
     int32_t cut_map_y, cut_map_x;
     float cut_ph_y, cut_ph_x;
@@ -431,6 +431,11 @@ typedef struct mtb_adj2d_buffers {
      * Ex); g_pol_y the same for TE's Py stack (n_poles_y planes); null otherwise */
     float *g_pol[2];
     float *g_pol_y[2];
+    /* With a live on-plane H line (cut_y / cut_x 2: TM odd mirrors, Rotate2,
+     * Rotate4): d J / d Hx0 (g_cut[0], nx floats) and d J / d Hy0 (g_cut[1], ny
+     * floats), two buffers each (alternate reverse steps); zero at creation,
+     * null otherwise */
+    float *g_cut[2][2];
 } mtb_adj2d_buffers;
 
 typedef struct mtb_yee2d_adjoint mtb_yee2d_adjoint;

@@ -49,13 +49,11 @@ class GradRun2D:
     def __init__(self, state, coeffs, n_steps, source, monitors, chunk=32,
                  phase_mode="exact"):
         self.te = hasattr(state, "Hz")
-        # TM even mirrors (zero H ghost) and TE mirrors (the even one's 2 Hz / dx cut row;
-        # the odd one changes only CPML profiles) have gradients; the TM live on-plane H
-        # lines (odd mirrors, rotations) do not
-        cy, cx = _cuts(coeffs, self.te)
-        if 2 in (cy[0], cx[0]):
-            raise L.MtbUnsupported("gradients: odd TM mirrors and rotations are forward-only")
-        self.names = STATE_TE if self.te else STATE_TM
+        # symmetry cuts: TM mirrors and rotations (a live on-plane H line for the odd ones,
+        # whose adjoint lines the backward pass allocates) and TE mirrors
+        self.cuts = _cuts(coeffs, self.te)
+        lines = tuple(n for c, n in zip(self.cuts, ("Hx0", "Hy0")) if c[0] == 2)
+        self.names = (STATE_TE if self.te else STATE_TM) + lines
         self.state0, self.coeffs, self.n = state, coeffs, int(n_steps)
         self.source, self.monitors = source, list(monitors)
         self.chunk = max(1, int(chunk))
@@ -95,6 +93,12 @@ class GradRun2D:
             if n_p else []
         gpol_y = [torch.zeros((n_py * nx, P), dtype=torch.float32, device=dev)
                   for _ in range(2)] if n_py else []
+        # live on-plane H lines (cut 2): d J / d Hx0 (nx) and d J / d Hy0 (ny), two buffers
+        gcut = [[torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(2)]
+                if c[0] == 2 else None for c, n in zip(self.cuts, (nx, ny))]
+        for a, name in enumerate(("Hx0", "Hy0")):     # d J / d (the final line) -> buffer 0
+            if gcut[a] is not None and grads[self.names.index(name)] is not None:
+                gcut[a][0].copy_(grads[self.names.index(name)].reshape(-1))
         targets = g + gpsi
         if self.te:
             offs = [(0, 0)] * 5 + [(0, 1), (1, 0), (0, 0), (0, 0)]
@@ -104,7 +108,7 @@ class GradRun2D:
         ns = len(self.names)
         for q, name in enumerate(self.names):
             gr = grads[q]
-            if gr is None or gr.numel() == 0:
+            if q >= len(targets) or gr is None or gr.numel() == 0:   # lines: seeded above
                 continue
             targets[q].copy_(eng._pack(gr, nx, P, offs[q]))
         # d J / d acc in the forward regions' layout
@@ -130,12 +134,15 @@ class GradRun2D:
             bufs.g_pol[q] = L.ptr(gpol[q])
         for q in range(len(gpol_y)):
             bufs.g_pol_y[q] = L.ptr(gpol_y[q])
+        for a, pair in enumerate(gcut):
+            for h in range(2 if pair else 0):
+                bufs.g_cut[a][h] = L.ptr(pair[h])
         adj = C.c_void_p()
         L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
                                              regs if nreg else None, nreg, eng.groups,
                                              eng.n_groups, eng.ring_elems, self.sub,
                                              C.byref(adj)), "mtb_yee2d_adjoint_create")
-        keep = [gaccs, g, gpsi, tmp, geps, gpol, gpol_y]
+        keep = [gaccs, g, gpsi, tmp, geps, gpol, gpol_y, gcut]
         stream = eng._sptr()
         try:
             rec_mons = _record_monitors(float(self.coeffs.dt), dev, self.te)

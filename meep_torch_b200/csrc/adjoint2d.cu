@@ -92,7 +92,7 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
                                               const mtb_line_sample *L,
                                               const float *__restrict__ radj,
                                               const float *__restrict__ rec, const int i,
-                                              const int jb) {
+                                              const int jb, const int cpar) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -157,6 +157,15 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
         gdz[q] = inside ? d1[q] * gd : 0.f;
         gpe[q] = inside ? gpe[q] : 0.f;
     }
+    // live on-plane H lines (core/stepper_tm.py:100-115, :139-152): the cut row / column
+    // of Dz differences against Hx0 / Hy0, so d J / d line(n+1/2) = (the next step's,
+    // buffer cpar ^ 1) - (the difference adjoint) / dx, into buffer cpar
+    if (S.cut_y == 2 && jb == 0)
+        B.g_cut[0][cpar][i] = B.g_cut[0][cpar ^ 1][i] - t2[0] / S.dx;
+    if (S.cut_x == 2 && i == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (jb + q < ny) B.g_cut[1][cpar][jb + q] = B.g_cut[1][cpar ^ 1][jb + q] - t1[q] / S.dx;
     if (S.n_poles > 0) stv(B.g[0] + g, gpe);     // gEz(n) from the poles; k_adj_tm_ez adds
     stv(B.g[3] + g, gdz);
     stv(B.g_psi[2] + g, gp2);
@@ -169,11 +178,11 @@ __device__ __forceinline__ void adj_tm_e_cell(const mtb_yee2d_struct &S, const m
 __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_e(const __grid_constant__ mtb_yee2d_struct S,
                                                          const __grid_constant__ mtb_adj2d_buffers B,
                                                          const float *__restrict__ radj,
-                                                         const float *__restrict__ rec) {
+                                                         const float *__restrict__ rec, int cpar) {
     __shared__ mtb_line_sample sl[AMAXL];
     const mtb_line_sample *L = stage_lines(S, sl);
     adj_tm_e_cell(S, B, L, radj, rec, blockIdx.y * AROWS + threadIdx.y,
-                  (blockIdx.x * 32 + threadIdx.x) * 4);
+                  (blockIdx.x * 32 + threadIdx.x) * 4, cpar);
 }
 
 __device__ __forceinline__ void adj_tm_h_cell(const mtb_yee2d_struct &S, const mtb_adj2d_buffers &B,
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_h(const __grid_constant__
 
 __device__ __forceinline__ void adj_tm_ez_cell(const mtb_yee2d_struct &S,
                                                const mtb_adj2d_buffers &B, const int i,
-                                               const int jb) {
+                                               const int jb, const int cpar) {
     const int nx = S.nx, ny = S.ny, P = S.pitch;
     if (i >= nx || jb >= P) return;
     const uint32_t g = (uint32_t)i * P + jb;
@@ -263,13 +272,45 @@ __device__ __forceinline__ void adj_tm_ez_cell(const mtb_yee2d_struct &S,
         const float t4m = (q == 0) ? t4l : t4[q - 1];
         gez[q] = (jb + q < ny) ? gez[q] + ((t3p[q] - t3[q]) * rdx + (t4m - t4[q]) * rdx) : 0.f;
     }
+    // the on-plane H line updates of this step read Ez(n) (core/stepper_tm.py:100-115):
+    //   Hx0' = Hx0 - dt (Ez(i, 0) - ph_y Ez(partner)) / dx, partner (i, 0), (nx-1-i, 0) or (0, i)
+    //   Hy0' = Hy0 + dt (Ez(0, j) - ph_x Ez(partner)) / dx, partner (0, j) or (j, 0)
+    if ((S.cut_y == 2 && (i == 0 || jb == 0)) || (S.cut_x == 2 && (i == 0 || jb == 0))) {
+        const float k = S.dt * rdx;
+        const float *gx = B.g_cut[0][cpar], *gy = B.g_cut[1][cpar];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = jb + q;
+            if (j >= ny) continue;
+            float a = 0.f;
+            if (S.cut_y == 2) {
+                const float ph = S.cut_ph_y;
+                if (j == 0) {
+                    a -= k * gx[i];
+                    if (S.cut_map_y == 0) a += k * ph * gx[i];
+                    else if (S.cut_map_y == 1) a += k * ph * gx[nx - 1 - i];
+                }
+                if (S.cut_map_y == 2 && i == 0 && j < nx) a += k * ph * gx[j];
+            }
+            if (S.cut_x == 2) {
+                const float ph = S.cut_ph_x;
+                if (i == 0) {
+                    a += k * gy[j];
+                    if (S.cut_map_x == 0) a -= k * ph * gy[j];
+                }
+                if (S.cut_map_x == 2 && j == 0 && i < ny) a -= k * ph * gy[i];
+            }
+            gez[q] += a;
+        }
+    }
     stv(B.g[0] + g, gez);
 }
 
 __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_ez(const __grid_constant__ mtb_yee2d_struct S,
-                                                          const __grid_constant__ mtb_adj2d_buffers B) {
+                                                          const __grid_constant__ mtb_adj2d_buffers B,
+                                                          int cpar) {
     adj_tm_ez_cell(S, B, blockIdx.y * AROWS + threadIdx.y,
-                  (blockIdx.x * 32 + threadIdx.x) * 4);
+                  (blockIdx.x * 32 + threadIdx.x) * 4, cpar);
 }
 
 // ------------------------------------------------------------------ TE
@@ -502,12 +543,14 @@ __global__ void __launch_bounds__(32 * AROWS) k_adj_te_hz(const __grid_constant_
 __global__ void __launch_bounds__(32 * AROWS) k_adj_tm_eze(const __grid_constant__ mtb_yee2d_struct S,
                                                            const __grid_constant__ mtb_adj2d_buffers B,
                                                            const float *__restrict__ radj,
-                                                           const float *__restrict__ rec) {
+                                                           const float *__restrict__ rec, int cpar) {
     __shared__ mtb_line_sample sl[AMAXL];
     const mtb_line_sample *L = stage_lines(S, sl);
     const int i = blockIdx.y * AROWS + threadIdx.y, jb = (blockIdx.x * 32 + threadIdx.x) * 4;
-    adj_tm_ez_cell(S, B, i, jb);
-    adj_tm_e_cell(S, B, L, radj, rec, i, jb);
+    // cpar is the earlier step's buffer: this step's line gradient is in cpar ^ 1, which
+    // no thread of this launch writes
+    adj_tm_ez_cell(S, B, i, jb, cpar ^ 1);
+    adj_tm_e_cell(S, B, L, radj, rec, i, jb, cpar);
 }
 
 __global__ void __launch_bounds__(32 * AROWS) k_adj_te_hzh(const __grid_constant__ mtb_yee2d_struct S,
@@ -556,21 +599,30 @@ static int adjoint_chunk(mtb_yee2d_adjoint *p, int k, const float *rec, int64_t 
     // middle kernel, and the last kernel alone only at q = 0
     auto radj_of = [&](int q) { return p->dft.ring_d.as<float>() + (size_t)q * p->dft.slot_elems; };
     auto rec_of = [&](int q) { return rec + (size_t)q * rec_slot_elems; };
+    // live on-plane H lines: step q of the chunk writes line gradient buffer q & 1 and
+    // reads the later step's from (q + 1) & 1; the previous chunk ended in buffer 0, so an
+    // odd chunk starts with that copied to buffer 1 (device copies of nx / ny floats)
+    if (S.pol == MTB_TM && (k & 1))
+        for (int a = 0; a < 2; ++a)
+            if ((a ? S.cut_x : S.cut_y) == 2)
+                MTB_CUDA_TRY(cudaMemcpyAsync(p->b.g_cut[a][1], p->b.g_cut[a][0],
+                                             sizeof(float) * (a ? S.ny : S.nx),
+                                             cudaMemcpyDeviceToDevice, st));
     for (int q = k - 1; q >= 0; --q) {
         const float *radj = radj_of(q);
         const float *rq = rec_of(q);
         if (S.pol == MTB_TM) {
             if (q == k - 1) {
-                k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0]);
+                k_adj_tm_e<<<grid, blk, 0, st>>>(S, p->b, radj, rq + rec_offset[0], q & 1);
                 MTB_CHECK_LAUNCH();
             }
             k_adj_tm_h<<<grid, blk, 0, st>>>(S, p->b, radj);
             MTB_CHECK_LAUNCH();
             if (q > 0)
                 k_adj_tm_eze<<<grid, blk, 0, st>>>(S, p->b, radj_of(q - 1),
-                                                   rec_of(q - 1) + rec_offset[0]);
+                                                   rec_of(q - 1) + rec_offset[0], (q - 1) & 1);
             else
-                k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b);
+                k_adj_tm_ez<<<grid, blk, 0, st>>>(S, p->b, 0);
             MTB_CHECK_LAUNCH();
         } else {
             if (q == k - 1) {
@@ -603,8 +655,10 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     if (S.pol != MTB_TM && S.pol != MTB_TE) return fail(MTB_INVALID_ARG, "adjoint: bad pol");
     if (S.cut_y < 0 || S.cut_y > 2 || S.cut_x < 0 || S.cut_x > 2)
         return fail(MTB_INVALID_ARG, "adjoint: cut_y / cut_x must be 0, 1 or 2");
-    if (S.cut_y == 2 || S.cut_x == 2)
-        return fail(MTB_UNSUPPORTED, "adjoint: odd mirrors and rotations are forward-only");
+    for (int a = 0; a < 2; ++a)
+        if ((a ? S.cut_x : S.cut_y) == 2 &&
+            (S.pol != MTB_TM || !bufs->g_cut[a][0] || !bufs->g_cut[a][1]))
+            return fail(MTB_INVALID_ARG, "adjoint: a live cut line needs TM and g_cut[%d][0..1]", a);
     if (S.cut_y && S.y_pmc) return fail(MTB_INVALID_ARG, "adjoint: cut_y with y_pmc");
     if (S.y_pmc && S.pol != MTB_TM) return fail(MTB_INVALID_ARG, "adjoint: y_pmc is TM only");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");

@@ -862,13 +862,15 @@ class Engine2D:
         it.box["inv_a"].copy_(self._pack(torch.reciprocal(e), it.nx, it.pitch))
 
     def _live_buffers(self, b: int):
-        """The buffers of structure b the next step reads: fields, then CPML memory."""
+        """The buffers of structure b the next step reads: fields, CPML memory, pole
+        stacks and the live on-plane H lines of symmetry cuts."""
         it, cur = self.items[b], self.current
         pols = [it.box[k] for k in ("pol", "pol_x", "pol_y") if k in it.box]
         ps = self.pole_slot
         return [it.box["main"][cur], it.box["x"][cur], it.box["y"][cur]] + \
             [p[cur] for p in it.box["psi"]] + \
-            [b for pol in pols for b in (pol[ps], pol[(ps + 2) % 3])]
+            [b for pol in pols for b in (pol[ps], pol[(ps + 2) % 3])] + \
+            [it.box[n][cur] for n in ("Hx0", "Hy0") if n in it.box]
 
     def snapshot(self, b: int = 0):
         """Copy of structure b's live state (box layout) for restore()."""

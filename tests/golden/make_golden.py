@@ -125,6 +125,8 @@ def tm_case(prec, y_pmc=False, point=False, sigma=False, poles=False, magnetic=F
             nonlinear=False, mpoles=False):
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
+    if extra == "rot4":                          # Rotate4 needs a square grid
+        nx = ny = 40
     eps = np.ones((nx, ny))
     eps[:, 15:21] = 12.0                          # guide along x
     eps[20:30, 8:14] = rng.uniform(2.0, 6.0)      # a block
@@ -481,19 +483,26 @@ def grad_loss(st, ax, ay, ad, mx, my, dx):
     """The scalar loss of the gradient fixtures: both flux lines (frequency
     weights), the energy of the full-grid DFT and of the final fields."""
     w = torch.tensor([1.0, -0.5, 0.25], dtype=ax.dtype)
-    return ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
-            + 1e-3 * (ad * ad).sum() + 0.1 * (st.Ez * st.Ez).sum()
-            + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
+    J = ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
+         + 1e-3 * (ad * ad).sum() + 0.1 * (st.Ez * st.Ez).sum()
+         + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
+    for k, c in (("Hx0", 0.3), ("Hy0", -0.2)):     # the live on-plane lines of odd cuts
+        if getattr(st, k, None) is not None:
+            J = J + c * (getattr(st, k) ** 2).sum()
+    return J
 
 
 def grad_tm_case(prec, extra=None):
     """d J / d eps through the reference's autograd (run_tm with
     checkpoint_every, core/run.py:81-120) on the TM case's geometry; ``extra`` =
     "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole,
-    "pmc" PMC walls in y, "mirror" even mirror cuts on the low x and y edges (the CPML
-    only on the far sides)."""
+    "pmc" PMC walls in y, "mirror" / "mirror_odd" even / odd mirror cuts on the low x and
+    y edges (the CPML only on the far sides), "rot2" / "rot4" an odd Rotate2 (y cut) /
+    Rotate4 (both cuts, 40 x 40)."""
     rng = np.random.default_rng(11)
     nx, ny, dx, npml = 48, 36, 0.05, 8
+    if extra == "rot4":                          # Rotate4 needs a square grid
+        nx = ny = 40
     eps = np.ones((nx, ny))
     eps[:, 15:21] = 12.0
     eps[20:30, 8:14] = rng.uniform(2.0, 6.0)
@@ -513,7 +522,8 @@ def grad_tm_case(prec, extra=None):
         out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
     if extra == "pmc":
         kw, out_extra = dict(y_pmc=True), dict(y_pmc=1)
-    folds = dict(y_mirror=1, x_mirror=1) if extra == "mirror" else {}
+    folds = {"mirror": dict(y_mirror=1, x_mirror=1), "mirror_odd": dict(y_mirror=-1, x_mirror=-1),
+             "rot2": dict(y_rot2=-1), "rot4": dict(rot4=-1)}.get(extra, {})
     if folds:
         kw, out_extra = dict(folds), dict(fold=json.dumps(folds))
     m = build_tm_coeffs(g, eps_inf=e, npml=npml, **kw)
@@ -727,6 +737,11 @@ def main():
     if sys.argv[1:] == ["grad3d_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad3d_pmc_f64.npz"),
                             **grad3d_case("f64", pmc=True))
+        return
+    if sys.argv[1:] == ["grad_cut_lines"]:
+        for name in ("mirror_odd", "rot2", "rot4"):
+            np.savez_compressed(os.path.join(HERE, f"golden_grad_tm_{name}_f64.npz"),
+                                **grad_tm_case("f64", name))
         return
     if sys.argv[1:] == ["grad_mirror"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad_tm_mirror_f64.npz"),

@@ -745,9 +745,13 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
 def _grad_loss(st, ax, ay, ad, mx, my, dx):
     """The fixtures' loss (tests/golden/make_golden.py grad_loss)."""
     w = torch.tensor([1.0, -0.5, 0.25], dtype=ax.dtype, device=ax.device)
-    return ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
-            + 1e-3 * (ad * ad).sum() + 0.1 * (st.Ez * st.Ez).sum()
-            + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
+    J = ((w * mx.flux(ax, dx)).sum() + (w.flip(0) * my.flux(ay, dx)).sum()
+         + 1e-3 * (ad * ad).sum() + 0.1 * (st.Ez * st.Ez).sum()
+         + 0.05 * (st.Hy * st.Hy).sum() - 0.02 * (st.Hx * st.Hx).sum())
+    for k, c in (("Hx0", 0.3), ("Hy0", -0.2)):     # the live on-plane lines of odd cuts
+        if getattr(st, k, None) is not None:
+            J = J + c * (getattr(st, k) ** 2).sum()
+    return J
 
 
 @pytest.mark.parametrize("chunk", [50, 32, 7])
@@ -770,12 +774,14 @@ def test_tm_gradient_matches_reference_autograd(chunk):
     assert e32 < 1e-4, e32
 
 
-@pytest.mark.parametrize("extra", ["lossy", "poles", "pmc", "mirror"])
+@pytest.mark.parametrize("extra", ["lossy", "poles", "pmc", "mirror", "mirror_odd", "rot2",
+                                   "rot4"])
 @pytest.mark.parametrize("chunk", [50, 13])
 def test_tm_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
     """d J / d eps of lossy (sigma_d on E, sigma_b and mu on H), dispersive (a
-    Lorentz and a Drude pole), y-PMC and even-mirror (cuts on the low x and y edges) TM
-    runs from the adjoint kernels, against the reference's
+    Lorentz and a Drude pole), y-PMC, even- and odd-mirror (cuts on the low x and y edges)
+    and odd Rotate2 / Rotate4 TM runs (the live on-plane H lines, their final values in
+    the loss) from the adjoint kernels, against the reference's
     float64 autograd through run_tm(checkpoint_every=50) (tests/golden/make_golden.py
     grad_extra); the float32 forward and adjoint agree with it to 1e-4."""
     from meep_torch_b200.core.run import run_tm
@@ -995,26 +1001,6 @@ def test_te_gradient_matches_reference_autograd(chunk):
           f"J {float(J):.6e} vs {float(g32['J']):.6e}")
     assert abs(float(J) - float(g32["J"])) <= 1e-4 * abs(float(g32["J"]))
     assert e32 < TOL, e32
-
-
-def test_gradients_of_live_cut_lines_refused():
-    """Gradients of TM odd mirrors and rotations (a live on-plane H line) raise
-    MtbUnsupported before any device work."""
-    from meep_torch_b200._lib import MtbUnsupported
-    from meep_torch_b200.core.coeffs import build_tm_coeffs
-    from meep_torch_b200.core.grid import Grid
-    from meep_torch_b200.core.monitors import DFTFieldsMonitor
-    from meep_torch_b200.core.run import run_tm
-    from meep_torch_b200.core.stepper_tm import init_tm_state
-    grid = Grid(nx=32, ny=32, dx=0.05, device=dev())
-    eps = torch.ones(32, 32, device=dev(), requires_grad=True)
-    m = build_tm_coeffs(grid, eps_inf=eps, npml=6, y_mirror=-1)
-    with pytest.raises(MtbUnsupported):
-        run_tm(init_tm_state(grid, y_mirror=-1), m, 4,
-               monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
-    m = build_tm_coeffs(grid, eps_inf=eps, npml=6, rot4=1)
-    with pytest.raises(MtbUnsupported):
-        run_tm(init_tm_state(grid, rot4=1), m, 4, monitors=[DFTFieldsMonitor(grid, [0.5], "Ez")])
 
 
 @pytest.mark.parametrize("chunk", [60, 32])

@@ -186,12 +186,14 @@ def test_3d_lean_sign_convention(case, prec):
 
 
 @pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles", "grad_tm_pmc",
-                                  "grad_tm_mirror"])
+                                  "grad_tm_mirror", "grad_tm_mirror_odd", "grad_tm_rot2",
+                                  "grad_tm_rot4"])
 def test_reference_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps (reference autograd, float64) against central
     finite differences of the oracle's float64 run at a few pixels; the lossy case
     adds sigma_d, sigma_b and mu, the dispersive one a Lorentz and a Drude pole, the
-    mirror one even mirror cuts on the low edges (pixels on the cuts are probed)."""
+    mirror ones even / odd mirror cuts on the low edges, the rotation ones an odd Rotate2
+    / Rotate4 (pixels on the cuts are probed; the loss adds the final on-plane lines)."""
     g = load_golden(f"{case}_f64")
     extra = dict(sigma=g.get("sigma"), sigma_b=g.get("sigma_b"), mu=g.get("mu"),
                  y_pmc=bool(g.get("y_pmc", 0)))
@@ -221,7 +223,9 @@ def test_reference_gradient_matches_oracle_finite_differences(case):
         fx, fy = O.line_flux(ax, dx, -1.0), O.line_flux(ay, dx, +1.0)
         return float((w * fx).sum() + (w[::-1] * fy).sum() + 1e-3 * (ad * ad).sum()
                      + 0.1 * (s["Ez"] ** 2).sum() + 0.05 * (s["Hy"] ** 2).sum()
-                     - 0.02 * (s["Hx"] ** 2).sum())
+                     - 0.02 * (s["Hx"] ** 2).sum()
+                     + sum(c * (s[k] ** 2).sum() for k, c in (("Hx0", 0.3), ("Hy0", -0.2))
+                           if k in s))
 
     eps = g["eps"].astype(np.float64)
     assert abs(J_of(eps) - float(g["J"])) <= 1e-9 * abs(float(g["J"]))
