@@ -219,8 +219,8 @@ typedef struct mtb_yee2d_struct {
      * mtb_yee2d_pole_slot holds M(n), (s+2)%3 M(n-1), (s+1)%3 receives M(n+1));
      * mpc[c][3]: mc1, mc2, mc3 stacks. No magnetic conductivity pairs and no live
      * symmetry-cut lines with them (core/coeffs.py:177-179, :240-244). Tile kernels
-     * only (variant 2); other variants, the no-alloc entry and the adjoint return
-     * MTB_UNSUPPORTED. */
+     * only (variant 2) and the adjoint (mtb_adj2d_buffers.g_b / g_mpol); other
+     * variants and the no-alloc entry return MTB_UNSUPPORTED. */
     int32_t n_mpoles;
     int32_t pad4_[3];
     float *f_b[2][2];
@@ -436,6 +436,11 @@ typedef struct mtb_adj2d_buffers {
      * floats), two buffers each (alternate reverse steps); zero at creation,
      * null otherwise */
     float *g_cut[2][2];
+    /* With TM magnetic poles: d J / d B (g_b[0] Bx, g_b[1] By, box arrays) and
+     * d J / d M(n), d J / d M(n-1) (g_mpol[c][0], g_mpol[c][1], n_mpoles planes
+     * each); null otherwise */
+    float *g_b[2];
+    float *g_mpol[2][2];
 } mtb_adj2d_buffers;
 
 typedef struct mtb_yee2d_adjoint mtb_yee2d_adjoint;

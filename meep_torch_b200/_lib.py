@@ -94,7 +94,8 @@ class Yee3DStruct(C.Structure):
 
 class Adj2DBuffers(C.Structure):
     _fields_ = [("g", vp * 5), ("g_psi", vp * 4), ("tmp", vp * 4), ("g_eps", vp * 2),
-                ("g_pol", vp * 2), ("g_pol_y", vp * 2), ("g_cut", (vp * 2) * 2)]
+                ("g_pol", vp * 2), ("g_pol_y", vp * 2), ("g_cut", (vp * 2) * 2),
+                ("g_b", vp * 2), ("g_mpol", (vp * 2) * 2)]
 
 
 class Adj3DBuffers(C.Structure):

@@ -96,6 +96,11 @@ class GradRun2D:
         # live on-plane H lines (cut 2): d J / d Hx0 (nx) and d J / d Hy0 (ny), two buffers
         gcut = [[torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(2)]
                 if c[0] == 2 else None for c, n in zip(self.cuts, (nx, ny))]
+        # magnetic poles: d J / d B (Bx, By) and d J / d M(n), M(n-1) per component
+        n_m = int(eng.structs[0].n_mpoles)
+        gb = [box() for _ in range(2)] if n_m else []
+        gmp = [[torch.zeros((n_m * nx, P), dtype=torch.float32, device=dev) for _ in range(2)]
+               for _ in range(2)] if n_m else []
         for a, name in enumerate(("Hx0", "Hy0")):     # d J / d (the final line) -> buffer 0
             if gcut[a] is not None and grads[self.names.index(name)] is not None:
                 gcut[a][0].copy_(grads[self.names.index(name)].reshape(-1))
@@ -137,12 +142,16 @@ class GradRun2D:
         for a, pair in enumerate(gcut):
             for h in range(2 if pair else 0):
                 bufs.g_cut[a][h] = L.ptr(pair[h])
+        for c in range(len(gb)):
+            bufs.g_b[c] = L.ptr(gb[c])
+            for h in range(2):
+                bufs.g_mpol[c][h] = L.ptr(gmp[c][h])
         adj = C.c_void_p()
         L.check(lib.mtb_yee2d_adjoint_create(C.byref(eng.structs[0]), C.byref(bufs),
                                              regs if nreg else None, nreg, eng.groups,
                                              eng.n_groups, eng.ring_elems, self.sub,
                                              C.byref(adj)), "mtb_yee2d_adjoint_create")
-        keep = [gaccs, g, gpsi, tmp, geps, gpol, gpol_y, gcut]
+        keep = [gaccs, g, gpsi, tmp, geps, gpol, gpol_y, gcut, gb, gmp]
         stream = eng._sptr()
         try:
             rec_mons = _record_monitors(float(self.coeffs.dt), dev, self.te)

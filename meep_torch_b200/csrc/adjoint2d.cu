@@ -213,28 +213,68 @@ __device__ __forceinline__ void adj_tm_h_cell(const mtb_yee2d_struct &S, const m
     float h1y[4] = {1.f, 1.f, 1.f, 1.f}, h2y[4] = {dt, dt, dt, dt};
     if (S.mag_h1[0]) { ldv(S.mag_h1[0] + g, h1x); ldv(S.mag_h2[0] + g, h2x); }
     if (S.mag_h1[1]) { ldv(S.mag_h1[1] + g, h1y); ldv(S.mag_h2[1] + g, h2y); }
+    float gxa[4], gya[4];                          // d J / d H(n+1/2)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float t2n = (q < 3) ? t2[q + 1] : t2r;
+        gya[q] = ghy[q] + (t1[q] - t1n[q]) * rdx;
+        gxa[q] = ghx[q] + (t2[q] - t2n) * rdx;
+    }
+    // magnetic poles (core/stepper_tm.py:209-219): B' = B -/+ dt curl, M(n+1) = mc1 M(n)
+    // + mc2 M(n-1) + mc3 H(n-1/2), H(n+1/2) = B' - sum M(n+1). gN = gM(n)' - gH' per pole;
+    // gM(n) = mc1 gN + gM(n-1)', gM(n-1) = mc2 gN, H(n-1/2) gets sum mc3 gN (its only use),
+    // and the curl sees gB' + gH'
+    const bool mp = S.n_mpoles > 0;
+    float hxo[4] = {0.f, 0.f, 0.f, 0.f}, hyo[4] = {0.f, 0.f, 0.f, 0.f};
+    if (mp) {
+        float gbx[4], gby[4];
+        ldv(B.g_b[0] + g, gbx);
+        ldv(B.g_b[1] + g, gby);
+        const uint32_t pl = (uint32_t)nx * P;
+        for (int c = 0; c < 2; ++c) {
+            const float(&gh)[4] = c ? gya : gxa;
+            float(&acc)[4] = c ? hyo : hxo;
+            for (int k = 0; k < S.n_mpoles; ++k) {
+                const uint32_t o = k * pl + g;
+                float ga[4], gb[4], m1[4], m2[4], m3[4];
+                ldv(B.g_mpol[c][0] + o, ga); ldv(B.g_mpol[c][1] + o, gb);
+                ldv(S.mpc[c][0] + o, m1); ldv(S.mpc[c][1] + o, m2); ldv(S.mpc[c][2] + o, m3);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float gn = ga[q] - gh[q];
+                    ga[q] = m1[q] * gn + gb[q];
+                    gb[q] = m2[q] * gn;
+                    acc[q] += m3[q] * gn;
+                }
+                stv(B.g_mpol[c][0] + o, ga); stv(B.g_mpol[c][1] + o, gb);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { gxa[q] += gbx[q]; gya[q] += gby[q]; }
+    }
     float t3[4], t4[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int j = jb + q;
-        const float t2n = (q < 3) ? t2[q + 1] : t2r;
-        const float gyp = ghy[q] + (t1[q] - t1n[q]) * rdx;
-        const float gxp = ghx[q] + (t2[q] - t2n) * rdx;
+        const float gyp = gya[q], gxp = gxa[q];
         const bool vy = vrow && j < ny, vx = j <= ny - 2;
         // Hy = h1 Hy + h2 (dEz/dx + psi_Ezx'), psi_Ezx' = b_hx psi + a_hx dEz/dx
         const float cy = h2y[q] * gyp;
         const float g1 = gp1[q] + cy;
         t3[q] = vy ? cy + ahx * g1 : 0.f;
         gp1[q] = vy ? bhx * g1 : gp1[q];
-        ghy[q] = vy ? h1y[q] * gyp : 0.f;
+        ghy[q] = vy ? (mp ? hyo[q] : h1y[q] * gyp) : 0.f;
+        gya[q] = vy ? gyp : 0.f;                       // d J / d B(n-1/2) with poles
         // Hx = h1 Hx - h2 (dEz/dy + psi_Ezy'), psi_Ezy' = b_hy psi + a_hy dEz/dy
         const float bhy = vx ? S.hy_b[j] : 1.f, ahy = vx ? S.hy_a[j] : 0.f;
         const float cx = -h2x[q] * gxp;
         const float g0 = gp0[q] + cx;
         t4[q] = vx ? cx + ahy * g0 : 0.f;
         gp0[q] = vx ? bhy * g0 : gp0[q];
-        ghx[q] = vx ? h1x[q] * gxp : 0.f;
+        ghx[q] = vx ? (mp ? hxo[q] : h1x[q] * gxp) : 0.f;
+        gxa[q] = vx ? gxp : 0.f;
     }
+    if (mp) { stv(B.g_b[0] + g, gxa); stv(B.g_b[1] + g, gya); }
     stv(B.g[1] + g, ghx);
     stv(B.g[2] + g, ghy);
     stv(B.g_psi[0] + g, gp0);
@@ -662,7 +702,17 @@ int mtb_yee2d_adjoint_create(const mtb_yee2d_struct *s, const mtb_adj2d_buffers 
     if (S.cut_y && S.y_pmc) return fail(MTB_INVALID_ARG, "adjoint: cut_y with y_pmc");
     if (S.y_pmc && S.pol != MTB_TM) return fail(MTB_INVALID_ARG, "adjoint: y_pmc is TM only");
     if (S.chi2) return fail(MTB_UNSUPPORTED, "adjoint: chi2 / chi3 (a nonlinear step)");
-    if (S.n_mpoles) return fail(MTB_UNSUPPORTED, "adjoint: magnetic poles are forward-only");
+    if (S.n_mpoles < 0 || S.n_mpoles > MTB_MAX_POLES ||
+        (S.n_mpoles && (S.pol != MTB_TM || S.mag_h1[0] || S.mag_h1[1])))
+        return fail(MTB_INVALID_ARG, "adjoint: n_mpoles %d (TM, without magnetic pairs)",
+                    S.n_mpoles);
+    if (S.n_mpoles)
+        for (int c = 0; c < 2; ++c)
+            if (!bufs->g_b[c] || !bufs->g_mpol[c][0] || !bufs->g_mpol[c][1] || !S.mpc[c][0] ||
+                !S.mpc[c][1] || !S.mpc[c][2] || (reinterpret_cast<uintptr_t>(bufs->g_b[c]) & 15) ||
+                (reinterpret_cast<uintptr_t>(bufs->g_mpol[c][0]) & 15) ||
+                (reinterpret_cast<uintptr_t>(bufs->g_mpol[c][1]) & 15))
+                return fail(MTB_INVALID_ARG, "adjoint: magnetic poles need g_b, g_mpol and mc1..3");
     if (S.te3) return fail(MTB_UNSUPPORTED, "adjoint: TE tensor eps / oriented poles");
     if (S.n_lines < 0 || S.n_lines > AMAXL || (S.n_lines > 0 && !S.lines))
         return fail(MTB_INVALID_ARG, "adjoint: %d line samples (at most %d)", S.n_lines, AMAXL);

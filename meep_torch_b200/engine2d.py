@@ -863,14 +863,17 @@ class Engine2D:
 
     def _live_buffers(self, b: int):
         """The buffers of structure b the next step reads: fields, CPML memory, pole
-        stacks and the live on-plane H lines of symmetry cuts."""
+        stacks, the live on-plane H lines of symmetry cuts, and B with the magnetic pole
+        stacks."""
         it, cur = self.items[b], self.current
         pols = [it.box[k] for k in ("pol", "pol_x", "pol_y") if k in it.box]
         ps = self.pole_slot
         return [it.box["main"][cur], it.box["x"][cur], it.box["y"][cur]] + \
             [p[cur] for p in it.box["psi"]] + \
             [b for pol in pols for b in (pol[ps], pol[(ps + 2) % 3])] + \
-            [it.box[n][cur] for n in ("Hx0", "Hy0") if n in it.box]
+            [it.box[n][cur] for n in ("Hx0", "Hy0") if n in it.box] + \
+            [fb[cur] for fb in it.box.get("B", ())] + \
+            [b for m in it.box.get("M", ()) for b in (m[ps], m[(ps + 2) % 3])]
 
     def snapshot(self, b: int = 0):
         """Copy of structure b's live state (box layout) for restore()."""

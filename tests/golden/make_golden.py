@@ -496,6 +496,7 @@ def grad_tm_case(prec, extra=None):
     """d J / d eps through the reference's autograd (run_tm with
     checkpoint_every, core/run.py:81-120) on the TM case's geometry; ``extra`` =
     "lossy" adds sigma_d, sigma_b and mu maps, "poles" a Lorentz and a Drude pole,
+    "mpoles" two magnetic Lorentz poles,
     "pmc" PMC walls in y, "mirror" / "mirror_odd" even / odd mirror cuts on the low x and
     y edges (the CPML only on the far sides), "rot2" / "rot4" an odd Rotate2 (y cut) /
     Rotate4 (both cuts, 40 x 40)."""
@@ -520,6 +521,10 @@ def grad_tm_case(prec, extra=None):
         pm = pole_masks(nx, ny)
         kw = dict(poles=POLES, pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
         out_extra = dict(poles=json.dumps(POLES), pole_masks=np.stack(pm))
+    elif extra == "mpoles":
+        pm = pole_masks(nx, ny)
+        kw = dict(m_poles=M_POLES, m_pole_masks=[torch.tensor(v, dtype=DT[prec]) for v in pm])
+        out_extra = dict(m_poles=json.dumps(M_POLES), m_pole_masks=np.stack(pm))
     if extra == "pmc":
         kw, out_extra = dict(y_pmc=True), dict(y_pmc=1)
     folds = {"mirror": dict(y_mirror=1, x_mirror=1), "mirror_odd": dict(y_mirror=-1, x_mirror=-1),
@@ -534,6 +539,7 @@ def grad_tm_case(prec, extra=None):
     dft = DFTFieldsMonitor(g, freqs, component="Ez")
     n, ce = 200, 50
     s0 = init_tm_state(g, n_poles=len(POLES) if extra == "poles" else 0,
+                       n_mpoles=len(M_POLES) if extra == "mpoles" else 0,
                        y_pmc=extra == "pmc", **folds)
     st, (ax, ay, ad) = run_tm(s0, m, n, source=src, monitors=[monx, mony, dft],
                               checkpoint_every=ce)
@@ -737,6 +743,10 @@ def main():
     if sys.argv[1:] == ["grad3d_pmc"]:
         np.savez_compressed(os.path.join(HERE, "golden_grad3d_pmc_f64.npz"),
                             **grad3d_case("f64", pmc=True))
+        return
+    if sys.argv[1:] == ["grad_mpoles"]:
+        np.savez_compressed(os.path.join(HERE, "golden_grad_tm_mpoles_f64.npz"),
+                            **grad_tm_case("f64", "mpoles"))
         return
     if sys.argv[1:] == ["grad_cut_lines"]:
         for name in ("mirror_odd", "rot2", "rot4"):

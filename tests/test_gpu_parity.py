@@ -725,6 +725,11 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
         kw = dict(poles=poles, pole_masks=[torch.tensor(v, dtype=torch.float32, device=dev_)
                                            for v in g["pole_masks"]])
         n_p = len(poles)
+    elif extra == "mpoles":
+        kw = dict(m_poles=[tuple(p) for p in json.loads(str(g["m_poles"]))],
+                  m_pole_masks=[torch.tensor(v, dtype=torch.float32, device=dev_)
+                                for v in g["m_pole_masks"]])
+    n_m = len(kw.get("m_poles", ()))
     pmc = extra == "pmc"
     if pmc:
         kw = dict(y_pmc=True)
@@ -739,7 +744,8 @@ def _grad_setup(g, dev_, requires_grad=True, extra=None):
     monx = FluxMonitorTM(grid, freqs, x_normal=True, idx=mx[0], lo=mx[1], hi=mx[2])
     mony = FluxMonitorTM(grid, freqs, x_normal=False, idx=my[0], lo=my[1], hi=my[2])
     dft = DFTFieldsMonitor(grid, freqs, "Ez")
-    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p, y_pmc=pmc, **folds), dx
+    return e, m, src, [monx, mony, dft], init_tm_state(grid, n_poles=n_p, n_mpoles=n_m, y_pmc=pmc,
+                                                       **folds), dx
 
 
 def _grad_loss(st, ax, ay, ad, mx, my, dx):
@@ -775,13 +781,14 @@ def test_tm_gradient_matches_reference_autograd(chunk):
 
 
 @pytest.mark.parametrize("extra", ["lossy", "poles", "pmc", "mirror", "mirror_odd", "rot2",
-                                   "rot4"])
+                                   "rot4", "mpoles"])
 @pytest.mark.parametrize("chunk", [50, 13])
 def test_tm_gradient_lossy_and_dispersive_match_reference_autograd(extra, chunk):
     """d J / d eps of lossy (sigma_d on E, sigma_b and mu on H), dispersive (a
     Lorentz and a Drude pole), y-PMC, even- and odd-mirror (cuts on the low x and y edges)
     and odd Rotate2 / Rotate4 TM runs (the live on-plane H lines, their final values in
-    the loss) from the adjoint kernels, against the reference's
+    the loss) and TM runs with two magnetic Lorentz poles (H = B - sum M) from the adjoint
+    kernels, against the reference's
     float64 autograd through run_tm(checkpoint_every=50) (tests/golden/make_golden.py
     grad_extra); the float32 forward and adjoint agree with it to 1e-4."""
     from meep_torch_b200.core.run import run_tm

@@ -187,7 +187,7 @@ def test_3d_lean_sign_convention(case, prec):
 
 @pytest.mark.parametrize("case", ["grad_tm", "grad_tm_lossy", "grad_tm_poles", "grad_tm_pmc",
                                   "grad_tm_mirror", "grad_tm_mirror_odd", "grad_tm_rot2",
-                                  "grad_tm_rot4"])
+                                  "grad_tm_rot4", "grad_tm_mpoles"])
 def test_reference_gradient_matches_oracle_finite_differences(case):
     """The golden d J / d eps (reference autograd, float64) against central
     finite differences of the oracle's float64 run at a few pixels; the lossy case
@@ -201,6 +201,9 @@ def test_reference_gradient_matches_oracle_finite_differences(case):
         extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
     if "fold" in g:
         extra.update(json.loads(str(g["fold"])))
+    if "m_poles" in g:
+        extra.update(m_poles=[tuple(p) for p in json.loads(str(g["m_poles"]))],
+                     m_pole_masks=g["m_pole_masks"])
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
                            int(g["n_steps"]))
     freqs = [float(f) for f in g["freqs"]]
@@ -298,6 +301,9 @@ def test_reference_te_gradient_matches_oracle_finite_differences(case):
         extra.update(poles=json.loads(str(g["poles"])), pole_masks=g["pole_masks"])
     if "fold" in g:
         extra.update(json.loads(str(g["fold"])))
+    if "m_poles" in g:
+        extra.update(m_poles=[tuple(p) for p in json.loads(str(g["m_poles"]))],
+                     m_pole_masks=g["m_pole_masks"])
     nx, ny, dx, npml, n = (int(g["nx"]), int(g["ny"]), float(g["dx"]), int(g["npml"]),
                            int(g["n_steps"]))
     freqs = [float(f) for f in g["freqs"]]
