@@ -900,8 +900,8 @@ def reference_cpu(wl, args, threads):
     """(value, unit, cores, sample, kind) of the reference's own CPU path on a bounded
     sample of workload `wl`, or None when the reference is not installed (cfg5: the
     reference has no surrogate, so None). The reference runs on every host thread; the
-    process's own torch thread count is put back afterwards, so the host-side work of
-    the measurements that follow (the other configurations) is not slowed by it."""
+    process's own torch thread count is put back afterwards. It runs after every GPU
+    measurement of the line."""
     import torch
     prev = torch.get_num_threads()
     try:
@@ -1380,6 +1380,11 @@ def main():
         "clocks": r["clocks"],
         "gpu_launches": r["launches"],
     }
+    # the other configs run before the host-side reference sample: that sample keeps every
+    # host thread busy, and cfg4 (host-launch bound) measured 2.9 instead of 5.0
+    # gradients/s right after it
+    if args.workload == "cfg2" and world == 1 and not args.no_suite:
+        line["other_configs"] = config_suite(args, rank, world, dev)
     ref_cpu = (reference_cpu(args.workload, args, threads)
                if rank == 0 and not args.no_cpu else None)
     if ref_cpu is not None:
@@ -1403,8 +1408,6 @@ def main():
                                               f"thread, {sec:.1f} s"}
         else:
             line["cpu_baseline"] = cpu_baseline_line(args.cpu_structs, args.cpu_steps, threads)
-    if args.workload == "cfg2" and world == 1 and not args.no_suite:
-        line["other_configs"] = config_suite(args, rank, world, dev)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
